@@ -1,0 +1,120 @@
+/*
+ * bnc_b200.h -- C ABI of the B200 backend for BioNeuronCore's per-tick loop.
+ *
+ * Two groups of entry points:
+ *
+ * 1. The drop-in set.  Same names, signatures and error conventions as the
+ *    reference CUDA backend's `extern "C"` block (src/gpu_backend_cuda.cu:316-390;
+ *    the set a loader must find is listed in tests/smoke_cuda.sh:24-29).  A caller
+ *    that dlopen()s the reference's libbiocore_gpu_backend_cuda.so can dlopen
+ *    this library instead.
+ *
+ * 2. New entry points (prefix bnc_) for what the reference has no call for:
+ *    multi-tick runs without a host round trip, field reads of the device
+ *    structure-of-arrays, the synthetic generator, ensembles and the adjoint.
+ *
+ * Handles are opaque `void*` as in the reference.  Functions returning int use
+ * 0 for success and a negative BNC_ERR_* code otherwise; bnc_last_error()
+ * returns a message for the most recent failure on the calling thread.
+ */
+#ifndef BNC_B200_H
+#define BNC_B200_H
+
+#include <stdint.h>
+#include <stddef.h>
+#include "bnc_abi.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* error codes (the loader codes mirror reference src/bion_loader_host.cpp:13-24) */
+#define BNC_OK 0
+#define BNC_ERR_ARG -1
+#define BNC_ERR_FILE -2
+#define BNC_ERR_FORMAT -3
+#define BNC_ERR_VERSION -4
+#define BNC_ERR_ALLOC -5
+#define BNC_ERR_INDEX -6
+#define BNC_ERR_UNSUPPORTED -7
+#define BNC_ERR_CUDA -8
+#define BNC_ERR_STATE -9
+#define BNC_ERR_DEVICE_TIMEOUT -10
+
+/* ------------------------------------------------------------------ */
+/* 1. drop-in set (reference src/gpu_backend_cuda.cu:316-390)          */
+/* ------------------------------------------------------------------ */
+
+/* Replaces gpu_backend_create (gpu_backend_cuda.cu:325-327): backend on device 0;
+ * NULL when no CUDA device exists. */
+void* gpu_backend_create(void);
+/* Replaces gpu_backend_create_on_device (gpu_backend_cuda.cu:316-323); an
+ * out-of-range index falls back to device 0 as in the reference. */
+void* gpu_backend_create_on_device(int device_index);
+/* Replaces gpu_backend_destroy (gpu_backend_cuda.cu:329-331). */
+void gpu_backend_destroy(void* sim);
+/* Replaces gpu_backend_load_bion (gpu_backend_cuda.cu:333-336): loads a .bion
+ * v3..v14 file; 0 on success, negative on failure. */
+int gpu_backend_load_bion(void* sim, const char* filename);
+/* Replaces gpu_backend_run_tick (gpu_backend_cuda.cu:338-341): one tick of dt
+ * ms; afterwards the AoS view returned by gpu_backend_bion_data is coherent
+ * (the reference synchronises every tick, gpu_backend_cuda.cu:308). */
+void gpu_backend_run_tick(void* sim, float dt);
+/* Replaces gpu_backend_bion_data (gpu_backend_cuda.cu:343-346): host AoS view
+ * (BncBionData*, layout of reference include/bion_loader.h:16-28). */
+void* gpu_backend_bion_data(void* sim);
+/* Replaces gpu_backend_upload_stimuli (gpu_backend_cuda.cu:348-351). */
+void gpu_backend_upload_stimuli(void* sim, const BncGpuStimulusData* src);
+/* Replaces gpu_backend_device_count (gpu_backend_cuda.cu:353-357). */
+int gpu_backend_device_count(void);
+/* Replaces gpu_backend_get_device_info (gpu_backend_cuda.cu:359-380). */
+int gpu_backend_get_device_info(int index, BncGpuDeviceInfo* info);
+/* Replace the ABI probes gpu_backend_ibuf_offset/vm_offset/seg_size
+ * (gpu_backend_cuda.cu:384-386). */
+int gpu_backend_ibuf_offset(void);
+int gpu_backend_vm_offset(void);
+int gpu_backend_seg_size(void);
+
+/* ------------------------------------------------------------------ */
+/* 2. new entry points                                                 */
+/* ------------------------------------------------------------------ */
+
+/* Synthetic workload families (seeded). */
+#define BNC_NET_SMALL 1        /* 64 x 32-segment neurons, 6 modifiers, 400 synapses */
+#define BNC_NET_LARGE 2        /* 100k x 64-segment neurons, 16 of 24 types, 10M synapses */
+#define BNC_NET_TREES 3        /* depth-10 binary dendritic trees, electrodiffusion */
+#define BNC_NET_ENSEMBLE_MEMBER 4 /* one network of an uneven ensemble */
+#define BNC_NET_ADJOINT 5      /* 256 x 64-segment neurons, 2000 synapses */
+
+typedef struct {
+    uint32_t family;          /* BNC_NET_* */
+    uint32_t n_neurons;       /* 0: family default */
+    uint64_t n_synapses;      /* 0: family default, scaled with n_neurons */
+    uint64_t seed;
+    uint32_t segs_per_neuron; /* 0: family default (ignored for trees) */
+    uint32_t tree_depth;      /* trees only; 0: 10 */
+    float conductance_scale[4]; /* gNa, gK, gleak, gCa multipliers (0 = 1.0) */
+    uint32_t flags;           /* BNC_NETGEN_* */
+    float stim_pA;            /* 0: family default */
+    float stim_duration_ms;   /* 0: whole run (1e9 ms) */
+} BncNetgenParams;
+
+#define BNC_NETGEN_NO_SYNAPSES 1u
+#define BNC_NETGEN_NO_CONNECTIONS 2u
+#define BNC_NETGEN_NO_STIMULI 4u
+#define BNC_NETGEN_PERTURB_IONS 8u
+
+/* Generates a network into host AoS arrays in the reference layout.  The arrays
+ * are owned by the library; release with bnc_netgen_free.  *stim receives the
+ * current stimuli (may be NULL when none). */
+int bnc_netgen_aos(const BncNetgenParams* p, BncBionData* out,
+                   BncCurrentStimulus** stim, uint32_t* n_stim);
+void bnc_netgen_free(BncBionData* data, BncCurrentStimulus* stim);
+
+/* Message for the last error on this thread ("" when none). */
+const char* bnc_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BNC_B200_H */

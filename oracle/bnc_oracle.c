@@ -1,0 +1,794 @@
+/*
+ * bnc_oracle.c -- CPU oracle (TEST INFRASTRUCTURE ONLY; never part of the
+ * product path): the reference's per-tick loop restated in C with FP32 state.
+ *
+ * Follows reference src/simulation_host.cpp:174-657 (core_run_tick_impl) step by
+ * step, include/diffusion_kernel.h:41-364 (step 2.5), include/modifier_helpers.h
+ * and include/kernel_dispatch.h for the helpers, with the same loop orders.  The
+ * only intended difference from the reference is storage precision: V_m, ions,
+ * modifier densities/states are float here (double in the reference); I_buffer
+ * stays double.  Parity of this file against the reference itself is pinned by
+ * tests/test_oracle_vs_reference.py (reference built by oracle/Makefile) and the
+ * golden fixtures in tests/golden/.
+ *
+ * Supported subset (the loader rejects the rest with an error): modifier types
+ * listed in bo_type_supported(), chemical synapses, pre-autoreceptors that are
+ * bouton K/Na channels, no mechano stimuli, no consolidation/nuclei.
+ */
+#include <stdlib.h>
+#include <string.h>
+#include <stdio.h>
+#include "../include/bnc_abi.h"
+#include "bo_modifiers.h"
+
+typedef struct {
+    uint32_t id, pre, post;
+    uint8_t type;
+    float weight, delay, pre_area, post_area;
+    OMod pre_ar[8];
+    uint8_t n_pre_ar;
+    OMod post_r[8];
+    uint8_t n_post_r;
+    float p_rel, amt, cleft[15], facil, depr, tau_clear;
+    uint8_t refractory;
+    float RRP, RRP_max, RRP_rec, bouton_Ca, spine_Ca, spine_camkii, spine_calcineurin;
+    float w_scale;   /* receptor density scale (1 in plain runs) */
+} OSyn;
+
+typedef struct {
+    uint64_t arrival;
+    float amount;
+    uint8_t nt;
+} ODelay;
+
+typedef struct BoSim {
+    uint32_t n, m, k;
+    OSeg* seg;
+    BncIntraConnection* conn;
+    OSyn* syn;
+    ODelay* delay;          /* k * 4 slots */
+    uint64_t tick;
+    BncCurrentStimulus* stim;
+    uint32_t n_stim;
+    uint32_t* spike_count;  /* per segment, threshold -40 mV upward crossings */
+    float nt_D[15];
+    char err[256];
+} BoSim;
+
+/* ---- diffusion scratch (reference keeps these as function statics) ---- */
+typedef struct {
+    double *phi, *phi_new, *sigma, *diag, *goff_d;
+    float *goff, *gdiag, *inp, *Vold, *Vnew, *offd;
+    double *intra_acc, *extra_acc;
+    float *ntd_in, *ntd_out, *atpd, *tempd, *txnd;
+} BoScratch;
+
+static BoScratch g_scr;
+static uint32_t g_scr_n = 0, g_scr_m = 0;
+
+static void scratch_reserve(uint32_t n, uint32_t m) {
+    if (n <= g_scr_n && m <= g_scr_m) return;
+    BoScratch* s = &g_scr;
+    free(s->phi); free(s->phi_new); free(s->sigma); free(s->diag); free(s->goff_d);
+    free(s->goff); free(s->gdiag); free(s->inp); free(s->Vold); free(s->Vnew); free(s->offd);
+    free(s->intra_acc); free(s->extra_acc); free(s->ntd_in); free(s->ntd_out);
+    free(s->atpd); free(s->tempd); free(s->txnd);
+    size_t N = n + 1, M = m + 1;
+    s->phi = calloc(N, 8); s->phi_new = calloc(N, 8); s->sigma = calloc(N, 8); s->diag = calloc(N, 8);
+    s->goff_d = calloc(M, 8); s->goff = calloc(M, 4); s->gdiag = calloc(N, 4); s->inp = calloc(N, 4);
+    s->Vold = calloc(N, 4); s->Vnew = calloc(N, 4); s->offd = calloc(N, 4);
+    s->intra_acc = calloc(N * 7, 8); s->extra_acc = calloc(N * 7, 8);
+    s->ntd_in = calloc(N * 15, 4); s->ntd_out = calloc(N * 15, 4);
+    s->atpd = calloc(N, 4); s->tempd = calloc(N, 4); s->txnd = calloc(N, 4);
+    g_scr_n = n; g_scr_m = m;
+}
+
+/* run_tick_common.h:216-231 */
+static float bo_capacitance(const OSeg* s) {
+    float area = bo_seg_area(s);
+    float C_m = area * 0.01f;
+    if (C_m < 1e-4f) C_m = 1e-4f;
+    for (uint8_t j = 0; j < s->nmod && j < 16; j++) {
+        if (s->mods[j].type == 4) {
+            float gr = s->mods[j].st[0];
+            if (gr <= 0.0f || gr >= 1.0f) gr = 0.6f;
+            float factor = 100.0f * (1.0f / gr - 1.0f) / (1.0f / 0.6f - 1.0f);
+            C_m /= factor;
+            break;
+        }
+    }
+    return C_m;
+}
+
+/* diffusion_kernel.h:108-113 */
+static inline float bo_sg_bernoulli(float x) {
+    if (fabsf(x) < 1e-3f) return 1.0f - 0.5f * x;
+    if (x > 50.0f) return 0.0f;
+    if (x < -50.0f) return -x;
+    return x / (bo_expf(x) - 1.0f);
+}
+
+static const float NP_Z[7] = {1.0f, 1.0f, 2.0f, -1.0f, 2.0f, -1.0f, 1.0f};
+static const float DIFF_C[7] = {1.33f, 1.96f, 0.22f, 2.03f, 0.10f, 0.0f, 9.31f};
+static const float BATH_ION[7] = {140.0f, 3.0f, 1.2f, 130.0f, 1.0f, 0.0f, 4.0e-5f};
+
+/* diffusion_kernel.h:41-104 */
+static void bo_solve_phi_e(BoSim* S) {
+    OSeg* sg = S->seg;
+    uint32_t n = S->n, m = S->m;
+    BoScratch* c = &g_scr;
+    for (uint32_t i = 0; i < n; i++) c->phi[i] = 0.0;
+    for (uint32_t i = 0; i < n; i++) {
+        double s = 0.0;
+        for (int ion = 0; ion < 7; ion++)
+            s += NP_Z[ion] * NP_Z[ion] * DIFF_C[ion] * (double)sg[i].out[ion];
+        c->sigma[i] = 3.612f * s;
+        double g_bath = c->sigma[i] * bo_seg_area(&sg[i]) / 1.0f;
+        c->diag[i] = g_bath;
+    }
+    for (uint32_t i = 0; i < m; i++) {
+        uint32_t a = S->conn[i].segment_a, b = S->conn[i].segment_b;
+        c->goff_d[i] = 0.0;
+        if (a >= n || b >= n) continue;
+        float r_min = sg[a].radius < sg[b].radius ? sg[a].radius : sg[b].radius;
+        float area_conn = PI_F * r_min * r_min;
+        if (area_conn < 1e-6f) area_conn = 1e-6f;
+        float dist = (sg[a].length + sg[b].length) * 0.5f;
+        if (dist < 0.1f) dist = 0.1f;
+        double g = 0.5 * (c->sigma[a] + c->sigma[b]) * area_conn / dist;
+        c->goff_d[i] = g;
+        c->diag[a] += g;
+        c->diag[b] += g;
+    }
+    for (int iter = 0; iter < 50; iter++) {
+        for (uint32_t i = 0; i < n; i++) c->phi_new[i] = 0.0;
+        for (uint32_t i = 0; i < m; i++) {
+            uint32_t a = S->conn[i].segment_a, b = S->conn[i].segment_b;
+            if (a >= n || b >= n) continue;
+            double g = c->goff_d[i];
+            if (g <= 0.0) continue;
+            c->phi_new[a] += g * c->phi[b];
+            c->phi_new[b] += g * c->phi[a];
+        }
+        for (uint32_t i = 0; i < n; i++) {
+            c->phi[i] = (c->diag[i] > 1e-9) ? (c->phi_new[i] - sg[i].ibuf) / c->diag[i] : 0.0;
+            if (c->phi[i] > 10.0) c->phi[i] = 10.0;
+            if (c->phi[i] < -10.0) c->phi[i] = -10.0;
+        }
+    }
+}
+
+/* diffusion_kernel.h:115-364 */
+static void bo_diffusion(BoSim* S, float dt) {
+    uint32_t n = S->n, m = S->m;
+    if (m == 0) return;
+    OSeg* sg = S->seg;
+    BoScratch* c = &g_scr;
+    for (size_t i = 0; i < (size_t)n * 7; i++) { c->extra_acc[i] = 0.0; c->intra_acc[i] = 0.0; }
+    for (size_t i = 0; i < (size_t)n * 15; i++) { c->ntd_in[i] = 0.0f; c->ntd_out[i] = 0.0f; }
+    for (uint32_t i = 0; i < n; i++) { c->atpd[i] = 0.0f; c->tempd[i] = 0.0f; c->txnd[i] = 0.0f; }
+    bo_solve_phi_e(S);
+
+    /* intracellular Nernst-Planck, 5 substeps (diffusion_kernel.h:152-238) */
+    const float dt_sub = dt / 5;
+    for (int sub = 0; sub < 5; sub++) {
+        for (size_t i = 0; i < (size_t)n * 7; i++) c->intra_acc[i] = 0.0;
+        for (uint32_t i = 0; i < n; i++) { c->gdiag[i] = 0.0f; c->inp[i] = 0.0f; }
+        for (uint32_t i = 0; i < m; i++) {
+            BncIntraConnection* cn = &S->conn[i];
+            uint32_t a = cn->segment_a, b = cn->segment_b;
+            if (a >= n || b >= n) continue;
+            if (cn->is_intracellular == 0) continue;
+            float r_min = sg[a].radius < sg[b].radius ? sg[a].radius : sg[b].radius;
+            float area_conn = PI_F * r_min * r_min;
+            if (area_conn < 1e-6f) area_conn = 1e-6f;
+            float dist = (sg[a].length + sg[b].length) * 0.5f;
+            if (dist < 0.1f) dist = 0.1f;
+            float vol_a = (float)bo_seg_volume(&sg[a]);
+            float vol_b = (float)bo_seg_volume(&sg[b]);
+            if (vol_a < 1e-6f) vol_a = 1e-6f;
+            if (vol_b < 1e-6f) vol_b = 1e-6f;
+            float sigma_i = 0.0f;
+            for (int ion = 0; ion < 7; ion++) {
+                float C_bar = (float)(0.5f * ((double)sg[a].in[ion] + (double)sg[b].in[ion]));
+                sigma_i += NP_Z[ion] * NP_Z[ion] * DIFF_C[ion] * C_bar;
+            }
+            float g_ax = 3.612f * sigma_i * area_conn / dist;
+            c->goff[i] = g_ax;
+            c->gdiag[a] += g_ax;
+            c->gdiag[b] += g_ax;
+            float dV = (float)(((double)sg[a].V + c->phi[a]) - ((double)sg[b].V + c->phi[b]));
+            float I_np = 0.0f;
+            for (int ion = 0; ion < 7; ion++) {
+                float C_a = sg[a].in[ion];
+                float C_b = sg[b].in[ion];
+                float x = NP_Z[ion] * 0.03742f * dV;
+                float flux = DIFF_C[ion] * area_conn * dt_sub / dist *
+                             (C_a * bo_sg_bernoulli(-x) - C_b * bo_sg_bernoulli(x));
+                c->intra_acc[a * 7 + ion] -= (double)flux / vol_a;
+                c->intra_acc[b * 7 + ion] += (double)flux / vol_b;
+                I_np += NP_Z[ion] * 96.485f * flux / dt_sub;
+            }
+            c->inp[a] += I_np - g_ax * dV;
+            c->inp[b] -= I_np - g_ax * dV;
+        }
+        for (uint32_t i = 0; i < n; i++) { c->Vold[i] = sg[i].V; c->Vnew[i] = sg[i].V; }
+        for (int iter = 0; iter < 50; iter++) {
+            for (uint32_t i = 0; i < n; i++) c->offd[i] = 0.0f;
+            for (uint32_t i = 0; i < m; i++) {
+                BncIntraConnection* cn = &S->conn[i];
+                uint32_t a = cn->segment_a, b = cn->segment_b;
+                if (a >= n || b >= n) continue;
+                if (cn->is_intracellular == 0) continue;
+                c->offd[a] += c->goff[i] * c->Vnew[b];
+                c->offd[b] += c->goff[i] * c->Vnew[a];
+            }
+            for (uint32_t i = 0; i < n; i++) {
+                float C_dt = bo_capacitance(&sg[i]) / dt_sub;
+                if (C_dt < 1e-9f) C_dt = 1e-9f;
+                c->Vnew[i] = (C_dt * c->Vold[i] + c->inp[i] + c->offd[i]) / (C_dt + c->gdiag[i]);
+            }
+        }
+        for (uint32_t i = 0; i < n; i++) sg[i].V = c->Vnew[i];
+        for (uint32_t i = 0; i < n; i++)
+            for (int ion = 0; ion < 7; ion++)
+                sg[i].in[ion] = (float)((double)sg[i].in[ion] + (double)(float)c->intra_acc[i * 7 + ion]);
+    }
+
+    /* extracellular Nernst-Planck, 5 substeps (diffusion_kernel.h:244-281) */
+    for (int sub = 0; sub < 5; sub++) {
+        for (size_t i = 0; i < (size_t)n * 7; i++) c->extra_acc[i] = 0.0;
+        for (uint32_t i = 0; i < m; i++) {
+            BncIntraConnection* cn = &S->conn[i];
+            uint32_t a = cn->segment_a, b = cn->segment_b;
+            if (a >= n || b >= n) continue;
+            float r_min = sg[a].radius < sg[b].radius ? sg[a].radius : sg[b].radius;
+            float area_conn = PI_F * r_min * r_min;
+            if (area_conn < 1e-6f) area_conn = 1e-6f;
+            float dist = (sg[a].length + sg[b].length) * 0.5f;
+            if (dist < 0.1f) dist = 0.1f;
+            float vol_a = (float)bo_seg_volume(&sg[a]);
+            float vol_b = (float)bo_seg_volume(&sg[b]);
+            if (vol_a < 1e-6f) vol_a = 1e-6f;
+            if (vol_b < 1e-6f) vol_b = 1e-6f;
+            for (int ion = 0; ion < 7; ion++) {
+                double Ca = sg[a].out[ion];
+                double Cb = sg[b].out[ion];
+                double dphi = c->phi[a] - c->phi[b];
+                float x = (float)(NP_Z[ion] * 0.03742f * dphi);
+                double flux = DIFF_C[ion] * area_conn * dt_sub / dist *
+                              (Ca * bo_sg_bernoulli(-x) - Cb * bo_sg_bernoulli(x));
+                c->extra_acc[a * 7 + ion] -= flux / (vol_a * EXTRA_VOLUME_RATIO);
+                c->extra_acc[b * 7 + ion] += flux / (vol_b * EXTRA_VOLUME_RATIO);
+            }
+        }
+        for (uint32_t i = 0; i < n; i++)
+            for (int ion = 0; ion < 7; ion++)
+                sg[i].out[ion] = (float)((double)sg[i].out[ion] + c->extra_acc[i * 7 + ion]);
+    }
+
+    /* NT / ATP / heat / transcription (diffusion_kernel.h:284-345) */
+    for (uint32_t i = 0; i < m; i++) {
+        BncIntraConnection* cn = &S->conn[i];
+        uint32_t a = cn->segment_a, b = cn->segment_b;
+        if (a >= n || b >= n) continue;
+        float r_min = sg[a].radius < sg[b].radius ? sg[a].radius : sg[b].radius;
+        float area_conn = PI_F * r_min * r_min;
+        if (area_conn < 1e-6f) area_conn = 1e-6f;
+        float dist = (sg[a].length + sg[b].length) * 0.5f;
+        if (dist < 0.1f) dist = 0.1f;
+        float vol_a = (float)bo_seg_volume(&sg[a]);
+        float vol_b = (float)bo_seg_volume(&sg[b]);
+        if (vol_a < 1e-6f) vol_a = 1e-6f;
+        if (vol_b < 1e-6f) vol_b = 1e-6f;
+        int extra_only = (cn->is_intracellular == 0);
+        if (!extra_only) {
+            for (int nt = 0; nt < 15; nt++) {
+                float dC = sg[a].intra_nt[nt] - sg[b].intra_nt[nt];
+                if (dC < 1e-12f && dC > -1e-12f) continue;
+                float D = S->nt_D[nt];
+                float flux = D * area_conn * dC * dt / dist;
+                c->ntd_in[a * 15 + nt] -= flux / vol_a;
+                c->ntd_in[b * 15 + nt] += flux / vol_b;
+            }
+        }
+        for (int nt = 0; nt < 15; nt++) {
+            float dC = sg[a].nt[nt] - sg[b].nt[nt];
+            if (dC < 1e-12f && dC > -1e-12f) continue;
+            float D = S->nt_D[nt];
+            float flux = D * area_conn * dC * dt / dist;
+            c->ntd_out[a * 15 + nt] -= flux / vol_a;
+            c->ntd_out[b * 15 + nt] += flux / vol_b;
+        }
+        if (!extra_only) {
+            float dATP = sg[a].atp - sg[b].atp;
+            if (dATP > 1e-12f || dATP < -1e-12f) {
+                float f = 0.14f * area_conn * dATP * dt / dist;
+                c->atpd[a] -= f / vol_a;
+                c->atpd[b] += f / vol_b;
+            }
+            float dT = sg[a].temp - sg[b].temp;
+            if (dT > 0.001f || dT < -0.001f) {
+                float f = 0.0014f * area_conn * dT * dt / dist;
+                c->tempd[a] -= f / vol_a;
+                c->tempd[b] += f / vol_b;
+            }
+            float dTx = sg[a].txn - sg[b].txn;
+            if (dTx > 1e-9f || dTx < -1e-9f) {
+                float f = 0.01f * area_conn * dTx * dt / dist;
+                c->txnd[a] -= f / vol_a;
+                c->txnd[b] += f / vol_b;
+            }
+        }
+    }
+    for (uint32_t i = 0; i < n; i++) {
+        for (int ion = 0; ion < 7; ion++) {
+            double e = (double)sg[i].out[ion];
+            e += (BATH_ION[ion] - e) * dt / 1.0f;
+            if (e < 1e-9) e = 1e-9;
+            if (e > 1000.0) e = 1000.0;
+            sg[i].out[ion] = (float)e;
+        }
+        for (int nt = 0; nt < 15; nt++) {
+            sg[i].intra_nt[nt] += c->ntd_in[i * 15 + nt];
+            sg[i].nt[nt] += c->ntd_out[i * 15 + nt];
+        }
+        sg[i].atp += c->atpd[i];
+        sg[i].temp += c->tempd[i];
+        sg[i].txn += c->txnd[i];
+    }
+}
+
+static int bo_has_myelin(const OSeg* s) {
+    for (uint8_t j = 0; j < s->nmod; j++) if (s->mods[j].type == 4) return 1;
+    return 0;
+}
+
+/* xorshift32 release draw, simulation_host.cpp:150-156 */
+static inline float bo_xorshift32_rnd(uint32_t seed) {
+    uint32_t x = seed;
+    x ^= x << 13;
+    x ^= x >> 17;
+    x ^= x << 5;
+    return (float)(x & 0x7FFFFFFFu) / (float)0x7FFFFFFFu;
+}
+
+/* (uint32_t)(V_m * 1000.0f) with V_m double, as x86-64 g++ evaluates it:
+ * truncation to a 64-bit integer, then modulo 2^32 (simulation_host.cpp:438-440). */
+static inline uint32_t bo_vm_seed_bits(float V) {
+    double x = (double)V * 1000.0f;
+    return (uint32_t)(int64_t)x;
+}
+
+/* modifier_helpers.h:747-806 */
+static float bo_bouton_gamma(uint8_t t) {
+    switch (t) {
+        case 156: return 10.0f;
+        case 157: return 16.0f;
+        case 123: return 11.0f;
+        case 150: return 27.0f;
+        case 112: return 7.0f;
+        case 107: return 100.0f;
+        case 141: return 20.7f;
+        case 142: return 20.8f;
+        default: return 0.0f;
+    }
+}
+
+static void bo_bouton_ca_step(const OSeg* pre, OSyn* syn, float dt) {
+    float g_K = 0.0f, g_Na = 0.0f;
+    for (uint8_t j = 0; j < syn->n_pre_ar; j++) {
+        uint8_t t = syn->pre_ar[j].type;
+        float g = (float)((double)syn->pre_ar[j].density * bo_bouton_gamma(t));
+        if (t == 141 || t == 142) g_Na += g;
+        else g_K += g;
+    }
+    float V_bouton = pre->V;
+    if (g_K > 0.0f || g_Na > 0.0f) {
+        float E_K = bo_nernst(pre->in[1], pre->out[1], 1.0f);
+        float E_Na = bo_nernst(pre->in[0], pre->out[0], 1.0f);
+        V_bouton = (float)((300.0f * (double)pre->V + g_K * E_K + g_Na * E_Na) / (300.0f + g_K + g_Na));
+    }
+    float cav21_dens = 0.0f, mm = 0.0f, h = 0.0f;
+    for (uint8_t j = 0; j < pre->nmod; j++) {
+        if (pre->mods[j].type == 140) {
+            cav21_dens = pre->mods[j].density;
+            float m_inf = cav21_m_inf(V_bouton);
+            float h_inf = cav21_h_inf(V_bouton, syn->bouton_Ca * MM_TO_UM);
+            mm = m_inf;
+            h = (float)(h_inf + ((double)pre->mods[j].st[1] - h_inf) * bo_expf(-dt / 300.0f));
+        }
+    }
+    float cav21_open = mm * mm * h;
+    double P_single = bo_ghk_P(15.0f, 2.0f, GHK_CBAR_CA_MM);
+    double flux = bo_ghk_div(V_bouton, syn->bouton_Ca, (double)pre->out[2]);
+    double I_A = P_single * flux * (cav21_dens * syn->pre_area) * cav21_open;
+    float I_Ca = (float)(I_A * A_TO_PA);
+    syn->bouton_Ca = (float)(syn->bouton_Ca - I_Ca * dt * 1000.0f / (2.0f * FARADAY_CONST * 0.1f));
+    syn->bouton_Ca += (0.0001f - syn->bouton_Ca) * dt / 5.0f;
+    if (syn->bouton_Ca < 0.0f) syn->bouton_Ca = 0.0f;
+}
+
+/* modifier_helpers.h:808-817 */
+static void bo_spine_ca_step(OSyn* syn, float I_syn, float dt) {
+    float I_abs = I_syn < 0.0f ? -I_syn : I_syn;
+    float I_Ca = I_abs * 0.1f;
+    float influx = (float)(I_Ca * dt * 1000.0f / (2.0f * FARADAY_CONST * 0.05f * 100.0f));
+    syn->spine_Ca += influx;
+    syn->spine_Ca += (0.0001f - syn->spine_Ca) * dt / 50.0f;
+    if (syn->spine_Ca < 0.0f) syn->spine_Ca = 0.0f;
+}
+
+/* modifier_helpers.h:819-833 */
+static void bo_spine_plasticity_step(OSyn* syn, float dt) {
+    float Ca_uM = syn->spine_Ca * MM_TO_UM;
+    float Ca4 = Ca_uM * Ca_uM * Ca_uM * Ca_uM;
+    float camkii_inf = Ca4 / (Ca4 + 1.0f + 1e-9f);
+    syn->spine_camkii += (camkii_inf - syn->spine_camkii) * dt / 2000.0f;
+    if (syn->spine_camkii < 0.0f) syn->spine_camkii = 0.0f;
+    if (syn->spine_camkii > 1.0f) syn->spine_camkii = 1.0f;
+    float Ca2 = Ca_uM * Ca_uM;
+    float calcineurin_inf = Ca2 / (Ca2 + 0.05f * 0.05f + 1e-9f);
+    syn->spine_calcineurin += (calcineurin_inf - syn->spine_calcineurin) * dt / 300.0f;
+    if (syn->spine_calcineurin < 0.0f) syn->spine_calcineurin = 0.0f;
+    if (syn->spine_calcineurin > 1.0f) syn->spine_calcineurin = 1.0f;
+}
+
+/* run_tick_common.h:199-206 */
+static uint8_t bo_nt_from_receptor(uint8_t rt) {
+    if (rt == 11 || rt == 17) return 1;
+    if (rt == 12) return 7;
+    if (rt == 14) return 3;
+    if (rt == 13) return 4;
+    if (rt == 44 || rt == 22) return 2;
+    return 0;
+}
+
+static double bo_receptor(uint8_t rtype, OMod* m, OSeg* post, float dt, float scale) {
+    switch (rtype) {
+        case 8: return bo_ampa_current(m, post, dt, scale);
+        case 9: return bo_nmda_current(m, post, dt, scale);
+        case 11: return bo_gabaa_current(m, post, dt, scale);
+        case 12: return bo_glycine_current(m, post, dt, scale);
+        default: return bo_dispatch(rtype, m, post, dt);
+    }
+}
+
+/* simulation_host.cpp:174-657 (steps 1, 2.5, 3, 4; no mechano, no consolidation) */
+static void bo_tick(BoSim* S, float dt) {
+    uint64_t tick = S->tick++;
+    OSeg* sg = S->seg;
+    uint32_t n = S->n;
+    /* expiry of current stimuli (:189-209) */
+    {
+        uint32_t w = 0;
+        for (uint32_t r = 0; r < S->n_stim; r++) {
+            BncCurrentStimulus st = S->stim[r];
+            if (!(tick >= st.start_tick + (uint64_t)(st.duration_ms / dt))) S->stim[w++] = st;
+        }
+        S->n_stim = w;
+    }
+    /* step 1 (:234-303) */
+    for (uint32_t i = 0; i < n; i++) {
+        OSeg* s = &sg[i];
+        double I_total = 0.0;
+        int myel = bo_has_myelin(s);
+        for (uint8_t j = 0; j < s->nmod; j++) {
+            uint8_t type = s->mods[j].type;
+            if (myel && type != 4 && bo_is_myelin_blocked(type)) continue;
+            s->mods[j].st[7] = bo_seg_area(s);
+            I_total += bo_dispatch(type, &s->mods[j], s, dt);
+        }
+        for (uint32_t k = 0; k < S->n_stim; k++) {
+            const BncCurrentStimulus* st = &S->stim[k];
+            if (st->segment_id == s->id) {
+                uint64_t dur_ticks = (uint64_t)(st->duration_ms / dt);
+                if (tick >= st->start_tick && tick < st->start_tick + dur_ticks)
+                    I_total += st->amplitude_pA;
+            }
+        }
+        s->ibuf = I_total;
+    }
+    /* step 2.5 */
+    bo_diffusion(S, dt);
+    /* step 3 (:322-593) */
+    if (S->k > 0)
+        for (uint32_t i = 0; i < n; i++)
+            for (int q = 0; q < 15; q++) sg[i].nt[q] = 0.0f;
+    for (uint32_t i = 0; i < n; i++)
+        for (uint8_t j = 0; j < sg[i].nmod; j++)
+            if (sg[i].mods[j].type == 9) sg[i].nt[0] = 1.0f;
+    for (uint32_t i = 0; i < n; i++)
+        for (uint8_t j = 0; j < sg[i].nmod; j++)
+            if (sg[i].mods[j].type == 43) sg[i].nt[3] = 0.0f;
+    for (uint32_t i = 0; i < S->k; i++) {
+        OSyn* syn = &S->syn[i];
+        if (syn->pre >= n || syn->post >= n) continue;
+        OSeg* pre = &sg[syn->pre];
+        OSeg* post = &sg[syn->post];
+        if (syn->delay > 0.0f) {
+            ODelay* slots = &S->delay[(size_t)i * 4];
+            for (int q = 0; q < 4; q++) {
+                if (slots[q].arrival == 0) continue;
+                if (slots[q].arrival <= tick) {
+                    syn->cleft[slots[q].nt] += slots[q].amount;
+                    slots[q].arrival = 0;
+                }
+            }
+        }
+        /* rrp_do_recovery (kernel_dispatch.h:612-630); no CaMKII/calcineurin modifiers */
+        if (!(syn->RRP_max <= 0.0f || syn->RRP >= syn->RRP_max)) {
+            float ca_pre = pre->in[2];
+            float ca_f = ca_pre / (0.0005f + ca_pre);
+            float camkii = 0, calcn = 0;
+            float priming = syn->RRP_rec + camkii * 0.02f + calcn * 0.01f;
+            priming *= ca_f;
+            float rec = (syn->RRP_max - syn->RRP) * priming * dt;
+            syn->RRP += rec;
+            if (syn->RRP > syn->RRP_max) syn->RRP = syn->RRP_max;
+        }
+        bo_bouton_ca_step(pre, syn, dt);
+        if (syn->refractory == 0) {
+            float Ca_uM = syn->bouton_Ca * MM_TO_UM;
+            float ca_act = bo_powf(Ca_uM, 4.0f) / (bo_powf(Ca_uM, 4.0f) + bo_powf(10.0f, 4.0f));
+            float p = syn->p_rel * ca_act;
+            for (int j = 0; j < syn->n_pre_ar; j++) {
+                syn->pre_ar[j].st[7] = syn->pre_area;
+                p *= 1.0f;   /* bouton channels carry no release modulator (dispatch default 1.0) */
+            }
+            uint32_t seed = syn->id ^ ((uint32_t)tick) ^ bo_vm_seed_bits(pre->V);
+            if (bo_xorshift32_rnd(seed) < p) {
+                uint8_t nt_type = (syn->n_post_r > 0) ? bo_nt_from_receptor(syn->post_r[0].type) : 0;
+                float release_amt;
+                if (syn->RRP_max <= 0.0f) release_amt = syn->amt * p;
+                else {
+                    float avail = syn->amt;
+                    if (avail > syn->RRP) avail = syn->RRP;
+                    release_amt = avail * p;
+                    syn->RRP -= release_amt;
+                    if (syn->RRP < 0) syn->RRP = 0;
+                }
+                uint64_t delay_ticks = (syn->delay <= 0.0f || dt <= 0.0f) ? 0
+                                       : (uint64_t)((syn->delay / dt) + 0.5f);
+                if (delay_ticks > 0) {
+                    ODelay* slots = &S->delay[(size_t)i * 4];
+                    for (int q = 0; q < 4; q++) {
+                        if (slots[q].arrival == 0) {
+                            slots[q].arrival = tick + delay_ticks;
+                            slots[q].amount = release_amt;
+                            slots[q].nt = nt_type;
+                            break;
+                        }
+                    }
+                } else {
+                    syn->cleft[nt_type] += release_amt;
+                }
+                syn->refractory = (uint8_t)(uint32_t)(20.0f / dt + 0.5f);
+            }
+        }
+        for (int q = 0; q < 15; q++) post->nt[q] += syn->cleft[q];
+        int myel_post = bo_has_myelin(post);
+        float I_syn = 0.0f;
+        for (int j = 0; j < syn->n_post_r; j++) {
+            uint8_t rtype = syn->post_r[j].type;
+            if (myel_post && bo_is_ionotropic(rtype)) continue;
+            syn->post_r[j].st[7] = syn->post_area;
+            I_syn = (float)(I_syn + bo_receptor(rtype, &syn->post_r[j], post, dt, syn->w_scale));
+        }
+        post->ibuf += I_syn;
+        bo_spine_ca_step(syn, I_syn, dt);
+        for (int q = 0; q < 15; q++) {
+            syn->cleft[q] *= bo_expf(-dt / syn->tau_clear);
+            if (syn->cleft[q] < 0.0f) syn->cleft[q] = 0.0f;
+        }
+        float Ca_uM = syn->spine_Ca * 1000.0f;
+        float Ca_sq = Ca_uM * Ca_uM;
+        float tau_theta = 300000.0f;
+        syn->facil += (Ca_sq - syn->facil) * dt / tau_theta;
+        if (syn->facil < 0.0f) syn->facil = 0.0f;
+        syn->depr = syn->facil + 0.01f;
+        bo_spine_plasticity_step(syn, dt);
+        float camkii_act = syn->spine_camkii;
+        float calcineurin_act = syn->spine_calcineurin;
+        int inhib = 0;
+        for (int j = 0; j < syn->n_post_r; j++) {
+            uint8_t rt = syn->post_r[j].type;
+            if (rt == 11 || rt == 17 || rt == 12) { inhib = 1; break; }
+        }
+        float dw = 0.0f;
+        if (camkii_act > 0.0f) dw += 0.0003f * camkii_act * dt;
+        float pp1_active = 0.5f;
+        if (calcineurin_act > 0.0f) dw -= 0.0001f * calcineurin_act * pp1_active * dt;
+        if (inhib) dw = -dw;
+        syn->weight += dw;
+        if (syn->weight != syn->weight) syn->weight = 0.5f;
+        if (syn->facil != syn->facil) syn->facil = 0.0f;
+        if (syn->depr != syn->depr) syn->depr = 0.01f;
+        if (syn->weight < 0.01f) syn->weight = 0.01f;
+        if (syn->weight > 10.0f) syn->weight = 10.0f;
+        if (syn->refractory > 0) syn->refractory--;
+    }
+    /* step 4 (:596-649) */
+    for (uint32_t i = 0; i < n; i++) {
+        OSeg* s = &sg[i];
+        if (s->ibuf != s->ibuf) s->ibuf = 0.0f;
+        if (s->ibuf > 10000.0f) s->ibuf = 10000.0f;
+        if (s->ibuf < -10000.0f) s->ibuf = -10000.0f;
+        float C_m = bo_capacitance(s);
+        float prev_V = s->V;
+        float dV = (float)(s->ibuf / C_m * dt);
+        if (dV > 50.0f) dV = 50.0f;
+        if (dV < -50.0f) dV = -50.0f;
+        s->V = (float)((double)s->V + dV);
+        if (S->spike_count && prev_V <= -40.0f && s->V > -40.0f) S->spike_count[i]++;
+        s->ibuf = 0.0f;
+        if (s->V != s->V) { s->V = -65.0f; }
+        else {
+            if (s->V < -120.0f) s->V = -120.0f;
+            if (s->V > 150.0f) s->V = 150.0f;
+        }
+    }
+}
+
+/* ------------------------------------------------------------------ */
+/* C API used by the tests (through ctypes)                            */
+/* ------------------------------------------------------------------ */
+
+static void load_mod(OMod* o, const BncModifier* m) {
+    o->type = m->type;
+    o->active_vars = m->active_vars;
+    o->density = (float)m->density;
+    for (int k = 0; k < 8; k++) o->st[k] = (float)m->state[k];
+}
+
+BoSim* bo_create(const BncBionData* d, const BncCurrentStimulus* stim, uint32_t n_stim,
+                 char* err, int errlen) {
+    BoSim* S = calloc(1, sizeof(BoSim));
+    S->n = d->num_segments;
+    S->m = d->num_connections;
+    S->k = d->num_synapses;
+    S->seg = calloc(S->n ? S->n : 1, sizeof(OSeg));
+    S->conn = calloc(S->m ? S->m : 1, sizeof(BncIntraConnection));
+    S->syn = calloc(S->k ? S->k : 1, sizeof(OSyn));
+    S->delay = calloc((size_t)(S->k ? S->k : 1) * 4, sizeof(ODelay));
+    S->stim = calloc(n_stim ? n_stim : 1, sizeof(BncCurrentStimulus));
+    S->spike_count = calloc(S->n ? S->n : 1, sizeof(uint32_t));
+    if (n_stim) memcpy(S->stim, stim, n_stim * sizeof(BncCurrentStimulus));
+    S->n_stim = n_stim;
+    const float mass[15] = {147.0f, 103.0f, 153.0f, 176.0f, 146.0f, 267.0f, 169.0f, 75.0f, 111.0f,
+                            348.0f, 507.0f, 232.0f, 24.0f, 162.0f, 0.0f};
+    for (int q = 0; q < 15; q++) {
+        float ms = mass[q];
+        if (ms < 1.0f) ms = 1.0f;
+        S->nt_D[q] = 1.33f * bo_powf(23.0f / ms, 1.0f / 3.0f);
+    }
+    for (uint32_t i = 0; i < S->n; i++) {
+        const BncSegment* a = &d->segments[i];
+        OSeg* s = &S->seg[i];
+        s->id = a->id;
+        s->type = a->segment_type;
+        s->length = a->length;
+        s->radius = a->radius;
+        s->px = a->position.x; s->py = a->position.y; s->pz = a->position.z;
+        s->V = (float)a->V_m;
+        for (int q = 0; q < 8; q++) { s->in[q] = (float)a->intra_ions[q]; s->out[q] = (float)a->extra_ions[q]; }
+        for (int q = 0; q < 15; q++) { s->intra_nt[q] = a->intra_nt[q]; s->nt[q] = a->neurotransmitter[q]; }
+        s->atp = a->ATP_level;
+        s->temp = a->temperature;
+        s->txn = a->transcription_signal;
+        s->ibuf = a->I_buffer;
+        s->nmod = a->modifier_count > 32 ? 32 : a->modifier_count;
+        for (uint8_t j = 0; j < s->nmod; j++) {
+            if (!bo_type_supported(a->modifiers[j].type)) {
+                snprintf(err, errlen, "segment %u: modifier type %u not supported", i, a->modifiers[j].type);
+                return S;
+            }
+            load_mod(&s->mods[j], &a->modifiers[j]);
+        }
+    }
+    if (S->m) memcpy(S->conn, d->connections, S->m * sizeof(BncIntraConnection));
+    for (uint32_t i = 0; i < S->k; i++) {
+        const BncSynapse* a = &d->synapses[i];
+        OSyn* y = &S->syn[i];
+        if (a->type != BNC_SYN_CHEMICAL) {
+            snprintf(err, errlen, "synapse %u: only chemical synapses are supported", i);
+            return S;
+        }
+        y->id = a->id; y->pre = a->pre_segment; y->post = a->post_segment; y->type = a->type;
+        y->weight = a->weight; y->delay = a->delay; y->pre_area = a->pre_area; y->post_area = a->post_area;
+        y->n_pre_ar = a->pre_autoreceptor_count > 8 ? 8 : a->pre_autoreceptor_count;
+        for (int j = 0; j < y->n_pre_ar; j++) load_mod(&y->pre_ar[j], &a->pre_autoreceptors[j]);
+        y->n_post_r = a->post_receptor_count > 8 ? 8 : a->post_receptor_count;
+        for (int j = 0; j < y->n_post_r; j++) load_mod(&y->post_r[j], &a->post_receptors[j]);
+        y->p_rel = a->release_probability; y->amt = a->release_amount;
+        for (int q = 0; q < 15; q++) y->cleft[q] = a->cleft_neurotransmitter[q];
+        y->facil = a->facilitation; y->depr = a->depression; y->tau_clear = a->tau_clearance;
+        y->refractory = a->refractory;
+        y->RRP = a->RRP; y->RRP_max = a->RRP_max; y->RRP_rec = a->RRP_recovery;
+        y->bouton_Ca = a->bouton_Ca; y->spine_Ca = a->spine_Ca;
+        y->spine_camkii = a->spine_camkii; y->spine_calcineurin = a->spine_calcineurin;
+        y->w_scale = 1.0f;
+    }
+    scratch_reserve(S->n, S->m);
+    return S;
+}
+
+void bo_destroy(BoSim* S) {
+    if (!S) return;
+    free(S->seg); free(S->conn); free(S->syn); free(S->delay); free(S->stim); free(S->spike_count);
+    free(S);
+}
+
+void bo_run(BoSim* S, uint32_t ticks, float dt) {
+    for (uint32_t t = 0; t < ticks; t++) bo_tick(S, dt);
+}
+
+/* Runs `ticks` ticks and records V of the listed segments after every tick
+ * into out[t * n_rec + r]. */
+void bo_run_trace(BoSim* S, uint32_t ticks, float dt, const uint32_t* rec, uint32_t n_rec, float* out) {
+    for (uint32_t t = 0; t < ticks; t++) {
+        bo_tick(S, dt);
+        for (uint32_t r = 0; r < n_rec; r++) out[(size_t)t * n_rec + r] = S->seg[rec[r]].V;
+    }
+}
+
+uint64_t bo_tick_count(const BoSim* S) { return S->tick; }
+
+/* Field export.  field: 0 V, 1 in[ion], 2 out[ion], 3 atp, 4 temp, 5 txn,
+ * 6 intra_nt[idx], 7 nt[idx], 8 modifier state (idx = slot*8+k), 9 spike count. */
+void bo_get_seg_field(const BoSim* S, int field, int idx, float* out) {
+    for (uint32_t i = 0; i < S->n; i++) {
+        const OSeg* s = &S->seg[i];
+        float v = 0.0f;
+        switch (field) {
+            case 0: v = s->V; break;
+            case 1: v = s->in[idx]; break;
+            case 2: v = s->out[idx]; break;
+            case 3: v = s->atp; break;
+            case 4: v = s->temp; break;
+            case 5: v = s->txn; break;
+            case 6: v = s->intra_nt[idx]; break;
+            case 7: v = s->nt[idx]; break;
+            case 8: v = ((idx >> 3) < s->nmod) ? s->mods[idx >> 3].st[idx & 7] : 0.0f; break;
+            case 9: v = (float)S->spike_count[i]; break;
+        }
+        out[i] = v;
+    }
+}
+
+/* Synapse export.  field: 0 bouton_Ca, 1 spine_Ca, 2 weight, 3 refractory,
+ * 4 cleft[idx], 5 receptor state (idx = j*8+k), 6 facilitation, 7 spine_camkii,
+ * 8 spine_calcineurin, 9 RRP. */
+void bo_get_syn_field(const BoSim* S, int field, int idx, float* out) {
+    for (uint32_t i = 0; i < S->k; i++) {
+        const OSyn* y = &S->syn[i];
+        float v = 0.0f;
+        switch (field) {
+            case 0: v = y->bouton_Ca; break;
+            case 1: v = y->spine_Ca; break;
+            case 2: v = y->weight; break;
+            case 3: v = (float)y->refractory; break;
+            case 4: v = y->cleft[idx]; break;
+            case 5: v = ((idx >> 3) < y->n_post_r) ? y->post_r[idx >> 3].st[idx & 7] : 0.0f; break;
+            case 6: v = y->facil; break;
+            case 7: v = y->spine_camkii; break;
+            case 8: v = y->spine_calcineurin; break;
+            case 9: v = y->RRP; break;
+        }
+        out[i] = v;
+    }
+}
+
+/* Receptor density scale per synapse (the differentiable synaptic weight;
+ * 1.0 reproduces the reference). */
+void bo_set_syn_scale(BoSim* S, const float* scale) {
+    for (uint32_t i = 0; i < S->k; i++) S->syn[i].w_scale = scale[i];
+}
+
+/* Elementary functions, exported for the accuracy tests. */
+double bo_exp_d(double x) { return bo_exp(x); }
+float bo_expf_f(float x) { return bo_expf(x); }
+double bo_log_d(double x) { return bo_log(x); }
+double bo_pow_d(double x, double y) { return bo_pow(x, y); }
+float bo_xorshift_f(uint32_t seed) { return bo_xorshift32_rnd(seed); }
+uint32_t bo_seed_bits(float V) { return bo_vm_seed_bits(V); }
