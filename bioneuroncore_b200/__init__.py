@@ -1,0 +1,224 @@
+"""bioneuroncore_b200 -- B200 backend for BioNeuronCore's per-tick simulation loop.
+
+Python view of the C ABI in include/bnc_b200.h.  The compute path is the CUDA
+library libbnc_b200.so built in-tree (``python -m bioneuroncore_b200.build``);
+there is no CPU fallback: `Backend` raises when the library or a device is missing.
+
+    from bioneuroncore_b200 import Backend, NetgenParams
+    b = Backend()                                  # gpu_backend_create
+    b.load_generated(NetgenParams(family=2))       # 6.4M-segment network on device
+    b.run_ticks(100, 0.025)
+    v = b.segment_field("V")                       # V_m in original segment order
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from .abi import (BionData, NetgenParams, SEGMENT_DTYPE, SYNAPSE_DTYPE, CONN_DTYPE, STIM_DTYPE, view,
+                  NET_SMALL, NET_LARGE, NET_TREES, NET_ENSEMBLE_MEMBER, NET_ADJOINT, NETGEN_NO_SYNAPSES,
+                  NETGEN_NO_CONNECTIONS, NETGEN_NO_STIMULI, NETGEN_PERTURB_IONS)
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libbnc_b200.so")
+
+SEG_FIELDS = {"V": 0, "ion_in": 1, "ion_out": 2, "ATP": 3, "temperature": 4, "transcription": 5,
+              "intra_nt": 6, "neurotransmitter": 7, "mod_state": 8, "spikes": 9}
+SYN_FIELDS = {"bouton_Ca": 0, "spine_Ca": 1, "weight": 2, "refractory": 3, "cleft": 4, "receptor_state": 5,
+              "facilitation": 6, "spine_camkii": 7, "spine_calcineurin": 8, "RRP": 9}
+
+# Symbols the reference's loader requires (reference tests/smoke_cuda.sh:24-29) plus the
+# ABI probes and this backend's own entry points; include/*.h declares every one.
+DROPIN_SYMBOLS = ["gpu_backend_create", "gpu_backend_create_on_device", "gpu_backend_destroy",
+                  "gpu_backend_load_bion", "gpu_backend_run_tick", "gpu_backend_bion_data",
+                  "gpu_backend_upload_stimuli", "gpu_backend_device_count", "gpu_backend_get_device_info",
+                  "gpu_backend_ibuf_offset", "gpu_backend_vm_offset", "gpu_backend_seg_size"]
+NEW_SYMBOLS = ["bnc_netgen_aos", "bnc_netgen_free", "bnc_last_error", "bnc_load_aos", "bnc_load_generated",
+               "bnc_run_ticks", "bnc_time_ticks", "bnc_sync_to_host", "bnc_read_segment_field",
+               "bnc_read_synapse_field", "bnc_set_synapse_scale", "bnc_network_info", "bnc_save_bion"]
+
+
+class NetInfo(C.Structure):
+    _fields_ = [(n, C.c_uint32) for n in ("n_segments", "n_connections", "n_synapses", "n_tiles", "n_items",
+                                          "n_phases", "n_receptors", "max_tile_segs", "max_tile_edges",
+                                          "smem_bytes", "flags")] + [
+        ("ticks", C.c_uint64), ("algo_bytes_per_tick", C.c_double), ("seg_bytes_per_tick", C.c_double),
+        ("syn_bytes_per_tick", C.c_double)]
+
+
+class BackendError(RuntimeError):
+    pass
+
+
+_lib = None
+
+
+def load_library(path=LIB_PATH):
+    """Loads libbnc_b200.so; raises if it has not been built (no fallback path exists)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise BackendError("libbnc_b200.so is not built; run `python -m bioneuroncore_b200.build`")
+    lib = C.CDLL(path)
+    vp, i32, u32, f32 = C.c_void_p, C.c_int, C.c_uint32, C.c_float
+    sig = {
+        "gpu_backend_create": ([], vp), "gpu_backend_create_on_device": ([i32], vp),
+        "gpu_backend_destroy": ([vp], None), "gpu_backend_load_bion": ([vp, C.c_char_p], i32),
+        "gpu_backend_run_tick": ([vp, f32], None), "gpu_backend_bion_data": ([vp], vp),
+        "gpu_backend_upload_stimuli": ([vp, vp], None), "gpu_backend_device_count": ([], i32),
+        "gpu_backend_get_device_info": ([i32, vp], i32), "gpu_backend_ibuf_offset": ([], i32),
+        "gpu_backend_vm_offset": ([], i32), "gpu_backend_seg_size": ([], i32),
+        "bnc_netgen_aos": ([vp, vp, vp, vp], i32), "bnc_netgen_free": ([vp, vp], None),
+        "bnc_last_error": ([], C.c_char_p), "bnc_load_aos": ([vp, vp, vp, u32], i32),
+        "bnc_load_generated": ([vp, vp], i32), "bnc_run_ticks": ([vp, u32, f32], i32),
+        "bnc_time_ticks": ([vp, u32, f32, vp], i32), "bnc_sync_to_host": ([vp], i32),
+        "bnc_read_segment_field": ([vp, i32, i32, vp, u32], i32),
+        "bnc_read_synapse_field": ([vp, i32, i32, vp, u32], i32),
+        "bnc_set_synapse_scale": ([vp, vp, u32], i32), "bnc_network_info": ([vp, vp], i32),
+        "bnc_save_bion": ([vp, C.c_char_p], i32),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = res
+    _lib = lib
+    return lib
+
+
+def last_error():
+    return load_library().bnc_last_error().decode()
+
+
+def _check(rc, what):
+    if rc != 0:
+        raise BackendError("%s failed (%d): %s" % (what, rc, last_error()))
+
+
+class Network:
+    """A generated network in host AoS arrays (reference layout), owned by the library."""
+
+    def __init__(self, params):
+        lib = load_library()
+        self.params = params
+        self.data = BionData()
+        self._stim = C.c_void_p()
+        ns = C.c_uint32()
+        _check(lib.bnc_netgen_aos(C.byref(params), C.byref(self.data), C.byref(self._stim), C.byref(ns)),
+               "bnc_netgen_aos")
+        self.n_stim = ns.value
+
+    @property
+    def segments(self):
+        return view(self.data.segments, SEGMENT_DTYPE, self.data.num_segments)
+
+    @property
+    def synapses(self):
+        return view(self.data.synapses, SYNAPSE_DTYPE, self.data.num_synapses)
+
+    @property
+    def connections(self):
+        return view(self.data.connections, CONN_DTYPE, self.data.num_connections)
+
+    @property
+    def stimuli(self):
+        return view(self._stim.value, STIM_DTYPE, self.n_stim)
+
+    @property
+    def stim_ptr(self):
+        return self._stim.value
+
+    def close(self):
+        if self.data.segments:
+            load_library().bnc_netgen_free(C.byref(self.data), self._stim)
+            self._stim = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Backend:
+    """One simulation on one GPU (the reference's `Simulation` behind gpu_backend_*)."""
+
+    def __init__(self, device=0):
+        self.lib = load_library()
+        if self.lib.gpu_backend_device_count() <= 0:
+            raise BackendError("no CUDA device visible")
+        self.h = self.lib.gpu_backend_create_on_device(device)
+        if not self.h:
+            raise BackendError("gpu_backend_create_on_device failed: " + last_error())
+
+    def close(self):
+        if self.h:
+            self.lib.gpu_backend_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # drop-in calls
+    def load_bion(self, path):
+        _check(self.lib.gpu_backend_load_bion(self.h, path.encode()), "gpu_backend_load_bion")
+
+    def run_tick(self, dt):
+        self.lib.gpu_backend_run_tick(self.h, C.c_float(dt))
+
+    def bion_data(self):
+        p = self.lib.gpu_backend_bion_data(self.h)
+        return BionData.from_address(p) if p else None
+
+    # new calls
+    def load_network(self, net):
+        _check(self.lib.bnc_load_aos(self.h, C.byref(net.data), net.stim_ptr, net.n_stim), "bnc_load_aos")
+
+    def load_generated(self, params):
+        _check(self.lib.bnc_load_generated(self.h, C.byref(params)), "bnc_load_generated")
+
+    def run_ticks(self, n, dt):
+        _check(self.lib.bnc_run_ticks(self.h, n, C.c_float(dt)), "bnc_run_ticks")
+
+    def time_ticks(self, n, dt):
+        ms = C.c_float()
+        _check(self.lib.bnc_time_ticks(self.h, n, C.c_float(dt), C.byref(ms)), "bnc_time_ticks")
+        return ms.value
+
+    def sync_to_host(self):
+        _check(self.lib.bnc_sync_to_host(self.h), "bnc_sync_to_host")
+
+    def info(self):
+        inf = NetInfo()
+        _check(self.lib.bnc_network_info(self.h, C.byref(inf)), "bnc_network_info")
+        return inf
+
+    def segment_field(self, field, index=0):
+        n = self.info().n_segments
+        out = np.empty(n, np.float32)
+        _check(self.lib.bnc_read_segment_field(self.h, SEG_FIELDS.get(field, field), index,
+                                               out.ctypes.data, n), "bnc_read_segment_field")
+        return out
+
+    def synapse_field(self, field, index=0, n_total=None):
+        n = n_total if n_total is not None else self.info().n_synapses
+        out = np.empty(max(n, 1), np.float32)
+        _check(self.lib.bnc_read_synapse_field(self.h, SYN_FIELDS.get(field, field), index,
+                                               out.ctypes.data, n), "bnc_read_synapse_field")
+        return out[:n]
+
+    def set_synapse_scale(self, scale):
+        s = np.ascontiguousarray(scale, np.float32)
+        _check(self.lib.bnc_set_synapse_scale(self.h, s.ctypes.data, s.size), "bnc_set_synapse_scale")
+
+    def save_bion(self, path):
+        _check(self.lib.bnc_save_bion(self.h, path.encode()), "bnc_save_bion")
+
+
+__all__ = ["Backend", "Network", "NetgenParams", "BionData", "BackendError", "load_library", "last_error",
+           "NET_SMALL", "NET_LARGE", "NET_TREES", "NET_ENSEMBLE_MEMBER", "NET_ADJOINT", "NETGEN_NO_SYNAPSES",
+           "NETGEN_NO_CONNECTIONS", "NETGEN_NO_STIMULI", "NETGEN_PERTURB_IONS", "SEG_FIELDS", "SYN_FIELDS",
+           "DROPIN_SYMBOLS", "NEW_SYMBOLS"]

@@ -1,0 +1,125 @@
+"""Builds the backend's shared library (and, for tests, the CPU oracle).
+
+    python -m bioneuroncore_b200.build            # product library only
+    python -m bioneuroncore_b200.build --oracle   # also oracle/liboracle.so (+ reference if present)
+
+The CUDA translation units are compiled for sm_100a only, with --fmad=false so no
+multiply-add is contracted behind the source's back (the kernels restate the
+reference's arithmetic operation by operation).  Outputs stay in the source tree.
+"""
+import argparse
+import concurrent.futures as cf
+import os
+import shutil
+import subprocess
+import sys
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG)
+CSRC = os.path.join(PKG, "csrc")
+BUILD = os.path.join(PKG, "_build")
+LIB = os.path.join(PKG, "libbnc_b200.so")
+ORACLE_DIR = os.path.join(ROOT, "oracle")
+ORACLE_LIB = os.path.join(ORACLE_DIR, "liboracle.so")
+REFERENCE = "/root/reference"
+
+CU_SOURCES = ["kernels.cu", "backend.cu"]
+CPP_SOURCES = ["netgen.cpp", "capi_host.cpp", "builder.cpp"]
+HEADERS = ["common.h", "net.h", "netgen.h", "physics.cuh", "device_math.cuh"]
+
+GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--fmad=false", "-Xcompiler", "-fPIC,-ffp-contract=off",
+              "-I" + os.path.join(ROOT, "include")]
+
+
+def _nvcc():
+    for cand in (shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
+        if cand and os.path.exists(cand):
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def _stale(target, deps):
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
+
+
+def _run(cmd):
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("command failed: %s\n%s%s" % (" ".join(cmd), r.stdout, r.stderr))
+    return r.stdout + r.stderr
+
+
+def build_library(verbose=False, ptxas_info=False):
+    """Compiles libbnc_b200.so (sm_100a) if any source changed; returns its path."""
+    os.makedirs(BUILD, exist_ok=True)
+    nvcc = _nvcc()
+    headers = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(ROOT, "include", f)
+                                                        for f in ("bnc_abi.h", "bnc_b200.h")]
+    jobs = []
+    objs = []
+    for src in CU_SOURCES + CPP_SOURCES:
+        s = os.path.join(CSRC, src)
+        o = os.path.join(BUILD, src + ".o")
+        objs.append(o)
+        if _stale(o, [s] + headers + [__file__]):
+            cmd = [nvcc] + GENCODE + NVCC_FLAGS + ["-c", s, "-o", o]
+            if src.endswith(".cpp"):
+                cmd = [nvcc] + GENCODE + NVCC_FLAGS + ["-x", "c++", "-c", s, "-o", o]
+            if ptxas_info and src.endswith(".cu"):
+                cmd += ["-Xptxas", "-v"]
+            jobs.append(cmd)
+    logs = []
+    if jobs:
+        with cf.ThreadPoolExecutor(max_workers=min(8, len(jobs))) as ex:
+            logs = list(ex.map(_run, jobs))
+    if jobs or _stale(LIB, objs):
+        _run([nvcc] + GENCODE + ["-shared", "-o", LIB] + objs + ["-lcudart_static", "-lrt", "-ldl", "-lpthread"])
+    if verbose:
+        for l in logs:
+            if l.strip():
+                print(l)
+    return LIB
+
+
+def build_oracle():
+    """Compiles the CPU oracle (test infrastructure) with contraction disabled."""
+    srcs = [os.path.join(ORACLE_DIR, f) for f in ("bnc_oracle.c", "bo_math.h", "bo_physics.h", "bo_modifiers.h")]
+    if _stale(ORACLE_LIB, srcs + [os.path.join(ROOT, "include", "bnc_abi.h")]):
+        _run(["gcc", "-std=c11", "-O2", "-ffp-contract=off", "-fPIC", "-shared", "-o", ORACLE_LIB,
+              os.path.join(ORACLE_DIR, "bnc_oracle.c"), "-lm"])
+    return ORACLE_LIB
+
+
+def build_reference():
+    """Builds the reference CPU library into oracle/_ref/ when its sources are present."""
+    if not os.path.isdir(os.path.join(REFERENCE, "src")):
+        return None
+    _run(["make", "-s", "-C", ORACLE_DIR, "-j8"])
+    return os.path.join(ORACLE_DIR, "_ref", "libbiocore_ref.so")
+
+
+def ensure_built():
+    """Builds the product library and the oracle only when their files are missing."""
+    if not os.path.exists(LIB):
+        build_library()
+    if not os.path.exists(ORACLE_LIB):
+        build_oracle()
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--oracle", action="store_true")
+    ap.add_argument("--ptxas", action="store_true")
+    a = ap.parse_args(argv)
+    print(build_library(verbose=True, ptxas_info=a.ptxas))
+    if a.oracle:
+        print(build_oracle())
+        print(build_reference())
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,592 @@
+// backend.cu -- the backend object behind the C ABI of include/bnc_b200.h.
+//
+// One Backend per handle, bound to one device and one stream.  The drop-in
+// gpu_backend_* calls keep the reference's semantics (gpu_backend_cuda.cu:316-390):
+// the host AoS view returned by gpu_backend_bion_data is refreshed after every
+// gpu_backend_run_tick.  bnc_run_ticks runs many ticks without that refresh.
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <new>
+#include <string>
+#include <vector>
+#include <cuda_runtime.h>
+#include "net.h"
+#include "netgen.h"
+
+namespace bnc {
+
+struct Backend {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool loaded = false;
+    bool failed = false;
+    bool owns_aos = false;
+    BncBionData aos{};        // host AoS view (drop-in)
+    NetDev dev{};
+    NetHost host;
+    DeviceAllocs allocs;
+    DeviceAllocs stim_allocs;
+    Stimuli stim;
+    uint64_t tick = 0;
+    uint64_t ticks_run = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+
+    ~Backend() {
+        cudaSetDevice(device);
+        allocs.release();
+        stim_allocs.release();
+        free_aos();
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        if (stream) cudaStreamDestroy(stream);
+    }
+    void free_aos() {
+        if (owns_aos) {
+            delete[] aos.neurons; delete[] aos.segments; delete[] aos.connections; delete[] aos.synapses;
+        }
+        std::memset(&aos, 0, sizeof(aos));
+        owns_aos = false;
+    }
+    void reset_network() {
+        allocs.release();
+        stim_allocs.release();
+        free_aos();
+        std::memset(&dev, 0, sizeof(dev));
+        host = NetHost();
+        stim = Stimuli();
+        loaded = false;
+        failed = false;
+        tick = 0;
+        ticks_run = 0;
+    }
+};
+
+static int cuda_fail(cudaError_t e, const char* what) {
+    set_error("%s: %s", what, cudaGetErrorString(e));
+    return BNC_ERR_CUDA;
+}
+
+// ---- AoS <- device export ----
+template <typename T>
+static bool d2h(std::vector<T>& v, const T* p, size_t n) {
+    v.resize(n);
+    if (n == 0) return true;
+    return cudaMemcpy(v.data(), p, n * sizeof(T), cudaMemcpyDeviceToHost) == cudaSuccess;
+}
+
+int export_network(const NetDev& d, const NetHost& h, uint64_t ticks_run, BncBionData* aos) {
+    if (!aos || !aos->segments) return BNC_OK;
+    const uint32_t n = d.n_seg;
+    std::vector<float> V, in, out, intra_nt, nt, atp, temp, txn, it_st;
+    bool ok = d2h(V, d.V, n) && d2h(in, d.ion_in, (size_t)7 * n) && d2h(out, d.ion_out, (size_t)7 * n) &&
+              d2h(intra_nt, d.intra_nt, (size_t)15 * n) && d2h(nt, d.nt, (size_t)15 * n) && d2h(atp, d.atp, n) &&
+              d2h(temp, d.temp, n) && d2h(txn, d.txn, n) && d2h(it_st, d.it_st, (size_t)7 * d.n_items);
+    if (!ok) { set_error("export: device read failed"); return BNC_ERR_CUDA; }
+    for (uint32_t dd = 0; dd < n; dd++) {
+        BncSegment& s = aos->segments[h.perm[dd]];
+        s.V_m = V[dd];
+        for (int q = 0; q < 7; q++) {
+            s.intra_ions[q] = in[(size_t)q * n + dd];
+            s.extra_ions[q] = out[(size_t)q * n + dd];
+        }
+        for (int q = 0; q < 15; q++) {
+            s.intra_nt[q] = intra_nt[(size_t)q * n + dd];
+            s.neurotransmitter[q] = nt[(size_t)q * n + dd];
+        }
+        s.ATP_level = atp[dd];
+        s.temperature = temp[dd];
+        s.transcription_signal = txn[dd];
+        if (ticks_run > 0) s.I_buffer = 0.0;   // step 4 clears it (simulation_host.cpp:624)
+    }
+    const uint32_t NI = d.n_items;
+    for (uint32_t q = 0; q < NI; q++) {
+        BncModifier& m = aos->segments[h.item_seg[q]].modifiers[h.item_slot[q]];
+        for (int k = 0; k < 7; k++) m.state[k] = it_st[(size_t)k * NI + q];
+        if (ticks_run > 0) {
+            const BncSegment& s = aos->segments[h.item_seg[q]];
+            m.state[7] = (s.segment_type == 1 || s.segment_type == 3 || s.segment_type == 4)
+                ? 4.0f * 3.14159265f * s.radius * s.radius : 2.0f * 3.14159265f * s.radius * s.length;
+        }
+    }
+    const uint32_t K = d.n_syn;
+    if (K) {
+        std::vector<float> bouton, spine, camkii, calcn, facil, weight, cleft, rrp, rst;
+        std::vector<uint8_t> refr;
+        ok = d2h(bouton, d.sy_bouton, K) && d2h(spine, d.sy_spine, K) && d2h(camkii, d.sy_camkii, K) &&
+             d2h(calcn, d.sy_calcn, K) && d2h(facil, d.sy_facil, K) && d2h(weight, d.sy_weight, K) &&
+             d2h(cleft, d.sy_cleft, K) && d2h(rrp, d.sy_rrp, K) && d2h(refr, d.sy_refr, K) &&
+             d2h(rst, d.rc_st, (size_t)3 * d.n_rec);
+        if (!ok) { set_error("export: device read failed"); return BNC_ERR_CUDA; }
+        for (uint32_t q = 0; q < K; q++) {
+            BncSynapse& y = aos->synapses[h.syn_orig[q]];
+            y.bouton_Ca = bouton[q]; y.spine_Ca = spine[q]; y.spine_camkii = camkii[q];
+            y.spine_calcineurin = calcn[q]; y.facilitation = facil[q]; y.weight = weight[q];
+            y.cleft_neurotransmitter[h.syn_nt[q]] = cleft[q];
+            y.RRP = rrp[q]; y.refractory = refr[q];
+            if (ticks_run > 0) y.depression = facil[q] + 0.01f;
+        }
+        for (uint32_t r = 0; r < d.n_rec; r++) {
+            BncSynapse& y = aos->synapses[h.syn_orig[h.rec_syn[r]]];
+            BncModifier& m = y.post_receptors[h.rec_slot[r]];
+            m.state[0] = rst[r]; m.state[1] = rst[(size_t)d.n_rec + r]; m.state[2] = rst[(size_t)2 * d.n_rec + r];
+            if (ticks_run > 0) m.state[7] = y.post_area;
+        }
+    }
+    return BNC_OK;
+}
+
+// ---- builder sink for generated networks: AoS chunks are never held whole ----
+namespace {
+struct CollectSink : NetSink {
+    BncBionData* out;
+    std::vector<BncCurrentStimulus>* stim;
+    uint32_t ni = 0, si = 0, ci = 0;
+    uint64_t yi = 0;
+    bool ok = true;
+    void begin(uint32_t n_neurons, uint32_t n_segments, uint32_t n_connections, uint64_t n_synapses,
+               uint32_t) override {
+        std::memset(out, 0, sizeof(*out));
+        out->num_neurons = n_neurons; out->num_segments = n_segments;
+        out->num_connections = n_connections; out->num_synapses = (uint32_t)n_synapses;
+        out->header.magic = 0x42494F4Eu; out->header.version = 14;
+        out->header.num_neurons = n_neurons; out->header.num_segments = n_segments;
+        out->header.num_intra_connections = n_connections; out->header.num_synapses = (uint32_t)n_synapses;
+        out->neurons = new (std::nothrow) BncNeuron[n_neurons ? n_neurons : 1];
+        out->segments = new (std::nothrow) BncSegment[n_segments ? n_segments : 1];
+        out->connections = new (std::nothrow) BncIntraConnection[n_connections ? n_connections : 1];
+        out->synapses = new (std::nothrow) BncSynapse[n_synapses ? n_synapses : 1];
+        ok = out->neurons && out->segments && out->connections && out->synapses;
+    }
+    void neuron(const BncNeuron& n) override { if (ok) out->neurons[ni++] = n; }
+    void segment(const BncSegment& s) override { if (ok) out->segments[si++] = s; }
+    void connection(const BncIntraConnection& c) override { if (ok) out->connections[ci++] = c; }
+    void synapse(const BncSynapse& s) override { if (ok) out->synapses[yi++] = s; }
+    void stimulus(const BncCurrentStimulus& st) override { stim->push_back(st); }
+};
+}  // namespace
+
+static int load_common(Backend* b, BncBionData& aos, bool keep_aos) {
+    cudaSetDevice(b->device);
+    int rc = build_network(aos, b->stim, &b->dev, &b->host, &b->allocs);
+    if (rc != BNC_OK) { b->reset_network(); if (!keep_aos) {} return rc; }
+    if (keep_aos) { b->aos = aos; b->owns_aos = true; }
+    b->loaded = true;
+    return BNC_OK;
+}
+
+static void free_aos_arrays(BncBionData& a) {
+    delete[] a.neurons; delete[] a.segments; delete[] a.connections; delete[] a.synapses;
+    std::memset(&a, 0, sizeof(a));
+}
+
+static int copy_aos(const BncBionData* src, BncBionData* dst) {
+    std::memset(dst, 0, sizeof(*dst));
+    dst->header = src->header;
+    dst->num_neurons = src->num_neurons; dst->num_segments = src->num_segments;
+    dst->num_connections = src->num_connections; dst->num_synapses = src->num_synapses;
+    dst->neurons = new (std::nothrow) BncNeuron[src->num_neurons ? src->num_neurons : 1];
+    dst->segments = new (std::nothrow) BncSegment[src->num_segments ? src->num_segments : 1];
+    dst->connections = new (std::nothrow) BncIntraConnection[src->num_connections ? src->num_connections : 1];
+    dst->synapses = new (std::nothrow) BncSynapse[src->num_synapses ? src->num_synapses : 1];
+    if (!dst->neurons || !dst->segments || !dst->connections || !dst->synapses) { free_aos_arrays(*dst); return BNC_ERR_ALLOC; }
+    if (src->num_neurons && src->neurons) std::memcpy(dst->neurons, src->neurons, sizeof(BncNeuron) * src->num_neurons);
+    if (src->num_segments) std::memcpy(dst->segments, src->segments, sizeof(BncSegment) * src->num_segments);
+    if (src->num_connections) std::memcpy(dst->connections, src->connections, sizeof(BncIntraConnection) * src->num_connections);
+    if (src->num_synapses) std::memcpy(dst->synapses, src->synapses, sizeof(BncSynapse) * src->num_synapses);
+    return BNC_OK;
+}
+
+static int run_ticks(Backend* b, uint32_t n, float dt) {
+    if (!b->loaded) { set_error("no network loaded"); return BNC_ERR_STATE; }
+    if (b->failed) { set_error("backend is in a failed state after a device error"); return BNC_ERR_STATE; }
+    cudaSetDevice(b->device);
+    for (uint32_t t = 0; t < n; t++) {
+        cudaError_t e = launch_tick(b->dev, b->host, dt, b->tick, b->ticks_run == 0 ? 1 : 0, b->stream);
+        if (e != cudaSuccess) { b->failed = true; return cuda_fail(e, "tick launch"); }
+        b->tick++;
+        b->ticks_run++;
+    }
+    return BNC_OK;
+}
+
+static int sync_stream(Backend* b) {
+    cudaError_t e = cudaStreamSynchronize(b->stream);
+    if (e != cudaSuccess) { b->failed = true; return cuda_fail(e, "tick execution"); }
+    return BNC_OK;
+}
+
+// .bion v14 writer (reference bion_loader_host.cpp:449-504 layout)
+static int save_bion(const BncBionData& d, const char* path) {
+    FILE* f = fopen(path, "wb");
+    if (!f) { set_error("cannot open %s for writing", path); return BNC_BION_ERR_FILE_OPEN; }
+    BncNetworkHeader hdr = d.header;
+    hdr.magic = 0x42494F4Eu; hdr.version = 14; hdr.mode = 0; hdr.diffusion_type = 0;
+    hdr.num_neurons = d.num_neurons; hdr.num_segments = d.num_segments;
+    hdr.num_intra_connections = d.num_connections; hdr.num_synapses = d.num_synapses;
+    hdr.grid_dim_x = hdr.grid_dim_y = hdr.grid_dim_z = 0; hdr.voxel_size = 1.0f;
+    hdr.num_nuclei = 0; hdr.nucleus_version = 1;
+    hdr.file_sz_segment = sizeof(BncSegment); hdr.file_sz_synapse = sizeof(BncSynapse);
+    hdr.file_sz_nucleus = 500; hdr.file_sz_intraconnection = sizeof(BncIntraConnection);
+    hdr.file_sz_neuron = sizeof(BncNeuron); hdr.file_sz_modifier = sizeof(BncModifier);
+    bool ok = fwrite(&hdr, sizeof(hdr), 1, f) == 1;
+    if (ok && d.num_neurons) ok = fwrite(d.neurons, sizeof(BncNeuron), d.num_neurons, f) == d.num_neurons;
+    if (ok) ok = fwrite(d.segments, sizeof(BncSegment), d.num_segments, f) == d.num_segments;
+    if (ok && d.num_connections) ok = fwrite(d.connections, sizeof(BncIntraConnection), d.num_connections, f) == d.num_connections;
+    if (ok && d.num_synapses) ok = fwrite(d.synapses, sizeof(BncSynapse), d.num_synapses, f) == d.num_synapses;
+    fclose(f);
+    if (!ok) { set_error("write to %s failed", path); return BNC_BION_ERR_WRITE_FAIL; }
+    return BNC_OK;
+}
+
+// .bion reader for v10+ files with the v14 record sizes (bion_loader_host.cpp:26-428
+// is the reference; its v3-v13 migrations are not restated here).
+static int load_bion_file(const char* path, BncBionData* d) {
+    std::memset(d, 0, sizeof(*d));
+    FILE* f = fopen(path, "rb");
+    if (!f) { set_error("cannot open %s", path); return BNC_BION_ERR_FILE_OPEN; }
+    auto fail = [&](int code, const char* msg) { fclose(f); free_aos_arrays(*d); set_error("%s: %s", path, msg); return code; };
+    if (fread(&d->header, 68, 1, f) != 1) return fail(BNC_BION_ERR_FILE_READ, "short header");
+    if (d->header.magic != 0x42494F4Eu) return fail(BNC_BION_ERR_BAD_MAGIC, "bad magic");
+    if (d->header.version < 3 || d->header.version > 14) return fail(BNC_BION_ERR_BAD_VERSION, "unsupported version");
+    if (d->header.version < 10) return fail(BNC_BION_ERR_BAD_VERSION, "pre-v10 layouts need the reference's migration");
+    if (fread(((uint8_t*)&d->header) + 68, 32, 1, f) != 1) return fail(BNC_BION_ERR_FILE_READ, "short header");
+    if (d->header.num_segments == 0) return fail(BNC_BION_ERR_ZERO_SEGS, "zero segments");
+    if (d->header.file_sz_segment != sizeof(BncSegment) || d->header.file_sz_synapse != sizeof(BncSynapse) ||
+        d->header.file_sz_intraconnection != sizeof(BncIntraConnection) || d->header.file_sz_neuron != sizeof(BncNeuron))
+        return fail(BNC_BION_ERR_BAD_VERSION, "record sizes differ from v14");
+    d->num_neurons = d->header.num_neurons; d->num_segments = d->header.num_segments;
+    d->num_connections = d->header.num_intra_connections; d->num_synapses = d->header.num_synapses;
+    d->neurons = new (std::nothrow) BncNeuron[d->num_neurons ? d->num_neurons : 1];
+    d->segments = new (std::nothrow) BncSegment[d->num_segments];
+    d->connections = new (std::nothrow) BncIntraConnection[d->num_connections ? d->num_connections : 1];
+    d->synapses = new (std::nothrow) BncSynapse[d->num_synapses ? d->num_synapses : 1];
+    if (!d->neurons || !d->segments || !d->connections || !d->synapses) return fail(BNC_ERR_ALLOC, "out of memory");
+    if (d->num_neurons && fread(d->neurons, sizeof(BncNeuron), d->num_neurons, f) != d->num_neurons) return fail(BNC_BION_ERR_FILE_READ, "short neurons");
+    if (fread(d->segments, sizeof(BncSegment), d->num_segments, f) != d->num_segments) return fail(BNC_BION_ERR_FILE_READ, "short segments");
+    if (d->num_connections && fread(d->connections, sizeof(BncIntraConnection), d->num_connections, f) != d->num_connections) return fail(BNC_BION_ERR_FILE_READ, "short connections");
+    if (d->num_synapses && fread(d->synapses, sizeof(BncSynapse), d->num_synapses, f) != d->num_synapses) return fail(BNC_BION_ERR_FILE_READ, "short synapses");
+    fclose(f);
+    // validation (bion_loader_host.cpp:359-408)
+    for (uint32_t i = 0; i < d->num_connections; i++)
+        if (d->connections[i].segment_a >= d->num_segments || d->connections[i].segment_b >= d->num_segments) {
+            free_aos_arrays(*d); set_error("connection %u out of range", i); return BNC_BION_ERR_BAD_CONN;
+        }
+    for (uint32_t i = 0; i < d->num_synapses; i++) {
+        const BncSynapse& y = d->synapses[i];
+        if (y.pre_segment >= d->num_segments || y.post_segment >= d->num_segments || y.type >= 3) {
+            free_aos_arrays(*d); set_error("synapse %u invalid", i); return BNC_BION_ERR_BAD_SYNAPSE;
+        }
+        if (y.pre_autoreceptor_count > 8 || y.post_receptor_count > 8) {
+            free_aos_arrays(*d); set_error("synapse %u: too many receptors", i); return BNC_ERR_FORMAT;
+        }
+    }
+    for (uint32_t i = 0; i < d->num_neurons; i++)
+        if ((uint64_t)d->neurons[i].segment_start + d->neurons[i].segment_count > d->num_segments) {
+            free_aos_arrays(*d); set_error("neuron %u range", i); return BNC_BION_ERR_BAD_NEURON;
+        }
+    for (uint32_t i = 0; i < d->num_segments; i++)
+        if (d->segments[i].modifier_count > 32) { free_aos_arrays(*d); set_error("segment %u modifiers", i); return BNC_ERR_FORMAT; }
+    for (uint32_t i = 0; i < d->num_segments; i++) d->segments[i].intra_connection_count = 0;
+    for (uint32_t i = 0; i < d->num_connections; i++) {
+        uint32_t a = d->connections[i].segment_a, b = d->connections[i].segment_b;
+        if (d->segments[a].intra_connection_count < 16) d->segments[a].intra_connection_ids[d->segments[a].intra_connection_count++] = i;
+        if (d->segments[b].intra_connection_count < 16) d->segments[b].intra_connection_ids[d->segments[b].intra_connection_count++] = i;
+    }
+    return BNC_OK;
+}
+
+}  // namespace bnc
+
+using namespace bnc;
+
+extern "C" {
+
+void* gpu_backend_create_on_device(int device_index) {
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) { set_error("no CUDA device"); return nullptr; }
+    if (device_index < 0 || device_index >= ndev) device_index = 0;
+    Backend* b = new (std::nothrow) Backend();
+    if (!b) return nullptr;
+    b->device = device_index;
+    if (cudaSetDevice(device_index) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess) {
+        set_error("CUDA context creation failed");
+        delete b;
+        return nullptr;
+    }
+    return b;
+}
+
+void* gpu_backend_create(void) { return gpu_backend_create_on_device(0); }
+
+void gpu_backend_destroy(void* sim) { delete static_cast<Backend*>(sim); }
+
+int gpu_backend_load_bion(void* sim, const char* filename) {
+    if (!sim || !filename) return -1;
+    Backend* b = static_cast<Backend*>(sim);
+    b->reset_network();
+    BncBionData d;
+    int rc = load_bion_file(filename, &d);
+    if (rc != BNC_OK) return rc;
+    rc = load_common(b, d, true);
+    if (rc != BNC_OK) free_aos_arrays(d);
+    return rc;
+}
+
+void gpu_backend_run_tick(void* sim, float dt) {
+    if (!sim) return;
+    Backend* b = static_cast<Backend*>(sim);
+    if (run_ticks(b, 1, dt) != BNC_OK) return;
+    if (sync_stream(b) != BNC_OK) return;
+    export_network(b->dev, b->host, b->ticks_run, &b->aos);
+}
+
+void* gpu_backend_bion_data(void* sim) {
+    if (!sim) return nullptr;
+    Backend* b = static_cast<Backend*>(sim);
+    return b->owns_aos ? &b->aos : nullptr;
+}
+
+void gpu_backend_upload_stimuli(void* sim, const BncGpuStimulusData* src) {
+    if (!sim || !src) return;
+    Backend* b = static_cast<Backend*>(sim);
+    if (!b->loaded) { set_error("no network loaded"); return; }
+    if (src->ramp_count || src->ion_inj_count || src->lig_inj_count) {
+        set_error("ramp stimuli and ion/ligand injections have no device implementation in this backend");
+        return;
+    }
+    b->stim.current.assign(src->current_stim, src->current_stim + std::min<uint32_t>(src->current_stim_count, BNC_GPU_MAX_STIMULI));
+    b->stim.vclamp.assign(src->vclamps, src->vclamps + std::min<uint32_t>(src->vclamp_count, BNC_GPU_MAX_STIMULI));
+    cudaSetDevice(b->device);
+    cudaStreamSynchronize(b->stream);
+    b->stim_allocs.release();
+    upload_stimuli(b->stim, b->host, &b->dev, &b->stim_allocs);
+}
+
+int gpu_backend_device_count(void) {
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess) return 0;
+    return ndev;
+}
+
+int gpu_backend_get_device_info(int index, BncGpuDeviceInfo* info) {
+    if (!info) return -1;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess) return -1;
+    if (index < 0 || index >= ndev) return -1;
+    std::memset(info, 0, sizeof(*info));
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, index) != cudaSuccess) return -1;
+    std::strncpy(info->name, prop.name, 127);
+    info->vendor_id = 0x10DE;
+    info->is_cpu = 0;
+    info->global_mem_bytes = prop.totalGlobalMem;
+    info->max_compute_units = prop.multiProcessorCount;
+    info->device_index = index;
+    std::strncpy(info->backend_type, "cuda", 15);
+    return 0;
+}
+
+int gpu_backend_ibuf_offset(void) { return (int)offsetof(BncSegment, I_buffer); }
+int gpu_backend_vm_offset(void) { return (int)offsetof(BncSegment, V_m); }
+int gpu_backend_seg_size(void) { return (int)sizeof(BncSegment); }
+
+int bnc_load_aos(void* sim, const BncBionData* data, const BncCurrentStimulus* stim, uint32_t n_stim) {
+    if (!sim || !data) { set_error("bnc_load_aos: null argument"); return BNC_ERR_ARG; }
+    Backend* b = static_cast<Backend*>(sim);
+    b->reset_network();
+    if (stim && n_stim) b->stim.current.assign(stim, stim + n_stim);
+    BncBionData d;
+    int rc = copy_aos(data, &d);
+    if (rc != BNC_OK) { set_error("bnc_load_aos: out of host memory"); return rc; }
+    rc = load_common(b, d, true);
+    if (rc != BNC_OK) free_aos_arrays(d);
+    return rc;
+}
+
+int bnc_load_generated(void* sim, const BncNetgenParams* p) {
+    if (!sim || !p) { set_error("bnc_load_generated: null argument"); return BNC_ERR_ARG; }
+    Backend* b = static_cast<Backend*>(sim);
+    b->reset_network();
+    BncBionData d;
+    CollectSink sink;
+    sink.out = &d;
+    sink.stim = &b->stim.current;
+    NetShape shape;
+    int rc = generate_network(*p, sink, &shape);
+    if (rc != BNC_OK) { free_aos_arrays(d); set_error("bnc_load_generated: invalid parameters"); return rc; }
+    if (!sink.ok) { free_aos_arrays(d); set_error("bnc_load_generated: out of host memory"); return BNC_ERR_ALLOC; }
+    rc = load_common(b, d, false);
+    free_aos_arrays(d);
+    return rc;
+}
+
+int bnc_run_ticks(void* sim, uint32_t n_ticks, float dt) {
+    if (!sim) { set_error("null handle"); return BNC_ERR_ARG; }
+    Backend* b = static_cast<Backend*>(sim);
+    int rc = run_ticks(b, n_ticks, dt);
+    if (rc != BNC_OK) return rc;
+    return sync_stream(b);
+}
+
+int bnc_time_ticks(void* sim, uint32_t n_ticks, float dt, float* ms) {
+    if (!sim || !ms) { set_error("null argument"); return BNC_ERR_ARG; }
+    Backend* b = static_cast<Backend*>(sim);
+    cudaSetDevice(b->device);
+    cudaEventRecord(b->ev0, b->stream);
+    int rc = run_ticks(b, n_ticks, dt);
+    if (rc != BNC_OK) return rc;
+    cudaEventRecord(b->ev1, b->stream);
+    rc = sync_stream(b);
+    if (rc != BNC_OK) return rc;
+    cudaEventElapsedTime(ms, b->ev0, b->ev1);
+    return BNC_OK;
+}
+
+int bnc_sync_to_host(void* sim) {
+    if (!sim) { set_error("null handle"); return BNC_ERR_ARG; }
+    Backend* b = static_cast<Backend*>(sim);
+    cudaSetDevice(b->device);
+    int rc = sync_stream(b);
+    if (rc != BNC_OK) return rc;
+    return export_network(b->dev, b->host, b->ticks_run, &b->aos);
+}
+
+int bnc_read_segment_field(void* sim, int field, int index, float* out, uint32_t n) {
+    if (!sim || !out) { set_error("null argument"); return BNC_ERR_ARG; }
+    Backend* b = static_cast<Backend*>(sim);
+    if (!b->loaded) { set_error("no network loaded"); return BNC_ERR_STATE; }
+    const NetDev& d = b->dev;
+    const uint32_t N = d.n_seg;
+    if (n < N) { set_error("output buffer holds %u values, %u needed", n, N); return BNC_ERR_ARG; }
+    cudaSetDevice(b->device);
+    int rc = sync_stream(b);
+    if (rc != BNC_OK) return rc;
+    std::vector<float> v(N);
+    const float* src = nullptr;
+    switch (field) {
+        case 0: src = d.V; break;
+        case 1: if (index < 0 || index > 6) return BNC_ERR_ARG; src = d.ion_in + (size_t)index * N; break;
+        case 2: if (index < 0 || index > 6) return BNC_ERR_ARG; src = d.ion_out + (size_t)index * N; break;
+        case 3: src = d.atp; break;
+        case 4: src = d.temp; break;
+        case 5: src = d.txn; break;
+        case 6: if (index < 0 || index > 14) return BNC_ERR_ARG; src = d.intra_nt + (size_t)index * N; break;
+        case 7: if (index < 0 || index > 14) return BNC_ERR_ARG; src = d.nt + (size_t)index * N; break;
+        case 8: {
+            int slot = index >> 3, k = index & 7;
+            if (k > 6) { set_error("state[7] is the effective area"); return BNC_ERR_ARG; }
+            std::vector<float> st;
+            if (!d2h(st, d.it_st + (size_t)k * d.n_items, d.n_items)) return cuda_fail(cudaGetLastError(), "read");
+            for (uint32_t i = 0; i < N; i++) {
+                out[i] = 0.0f;
+                if (b->owns_aos && slot < b->aos.segments[i].modifier_count)
+                    out[i] = (float)b->aos.segments[i].modifiers[slot].state[k];
+            }
+            for (uint32_t q = 0; q < d.n_items; q++)
+                if (b->host.item_slot[q] == slot) out[b->host.item_seg[q]] = st[q];
+            return BNC_OK;
+        }
+        case 9: {
+            std::vector<uint32_t> c;
+            if (!d2h(c, d.spike_count, N)) return cuda_fail(cudaGetLastError(), "read");
+            for (uint32_t dd = 0; dd < N; dd++) out[b->host.perm[dd]] = (float)c[dd];
+            return BNC_OK;
+        }
+        default: set_error("unknown segment field %d", field); return BNC_ERR_ARG;
+    }
+    if (cudaMemcpy(v.data(), src, N * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return cuda_fail(cudaGetLastError(), "read");
+    for (uint32_t dd = 0; dd < N; dd++) out[b->host.perm[dd]] = v[dd];
+    return BNC_OK;
+}
+
+int bnc_read_synapse_field(void* sim, int field, int index, float* out, uint32_t n) {
+    if (!sim || !out) { set_error("null argument"); return BNC_ERR_ARG; }
+    Backend* b = static_cast<Backend*>(sim);
+    if (!b->loaded) { set_error("no network loaded"); return BNC_ERR_STATE; }
+    const NetDev& d = b->dev;
+    const uint32_t K = d.n_syn, KT = b->host.n_syn_total;
+    if (n < KT) { set_error("output buffer holds %u values, %u needed", n, KT); return BNC_ERR_ARG; }
+    cudaSetDevice(b->device);
+    int rc = sync_stream(b);
+    if (rc != BNC_OK) return rc;
+    for (uint32_t i = 0; i < KT; i++) out[i] = 0.0f;
+    std::vector<float> v;
+    const float* src = nullptr;
+    switch (field) {
+        case 0: src = d.sy_bouton; break;
+        case 1: src = d.sy_spine; break;
+        case 2: src = d.sy_weight; break;
+        case 3: {
+            std::vector<uint8_t> r;
+            if (!d2h(r, d.sy_refr, K)) return cuda_fail(cudaGetLastError(), "read");
+            for (uint32_t q = 0; q < K; q++) out[b->host.syn_orig[q]] = (float)r[q];
+            return BNC_OK;
+        }
+        case 4: {
+            if (!d2h(v, d.sy_cleft, K)) return cuda_fail(cudaGetLastError(), "read");
+            for (uint32_t q = 0; q < K; q++) out[b->host.syn_orig[q]] = (b->host.syn_nt[q] == index) ? v[q] : 0.0f;
+            return BNC_OK;
+        }
+        case 5: {
+            int j = index >> 3, k = index & 7;
+            if (k > 2) { set_error("receptor states above 2 are not tracked"); return BNC_ERR_ARG; }
+            if (!d2h(v, d.rc_st + (size_t)k * d.n_rec, d.n_rec)) return cuda_fail(cudaGetLastError(), "read");
+            for (uint32_t r = 0; r < d.n_rec; r++)
+                if (b->host.rec_slot[r] == j) out[b->host.syn_orig[b->host.rec_syn[r]]] = v[r];
+            return BNC_OK;
+        }
+        case 6: src = d.sy_facil; break;
+        case 7: src = d.sy_camkii; break;
+        case 8: src = d.sy_calcn; break;
+        case 9: src = d.sy_rrp; break;
+        default: set_error("unknown synapse field %d", field); return BNC_ERR_ARG;
+    }
+    if (!d2h(v, src, K)) return cuda_fail(cudaGetLastError(), "read");
+    for (uint32_t q = 0; q < K; q++) out[b->host.syn_orig[q]] = v[q];
+    return BNC_OK;
+}
+
+int bnc_set_synapse_scale(void* sim, const float* scale, uint32_t n) {
+    if (!sim || !scale) { set_error("null argument"); return BNC_ERR_ARG; }
+    Backend* b = static_cast<Backend*>(sim);
+    if (!b->loaded) { set_error("no network loaded"); return BNC_ERR_STATE; }
+    if (n < b->host.n_syn_total) { set_error("scale array too short"); return BNC_ERR_ARG; }
+    std::vector<float> v(b->dev.n_syn);
+    for (uint32_t q = 0; q < b->dev.n_syn; q++) v[q] = scale[b->host.syn_orig[q]];
+    cudaSetDevice(b->device);
+    if (cudaMemcpy(b->dev.sy_scale, v.data(), v.size() * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess)
+        return cuda_fail(cudaGetLastError(), "scale upload");
+    return BNC_OK;
+}
+
+int bnc_network_info(void* sim, BncNetInfo* info) {
+    if (!sim || !info) { set_error("null argument"); return BNC_ERR_ARG; }
+    Backend* b = static_cast<Backend*>(sim);
+    std::memset(info, 0, sizeof(*info));
+    if (!b->loaded) return BNC_ERR_STATE;
+    const NetDev& d = b->dev;
+    info->n_segments = d.n_seg; info->n_connections = b->host.n_conn; info->n_synapses = d.n_syn;
+    info->n_tiles = d.n_tiles; info->n_items = d.n_items; info->n_phases = d.n_phases; info->n_receptors = d.n_rec;
+    info->max_tile_segs = b->host.max_tile_segs; info->max_tile_edges = b->host.max_tile_edges;
+    info->smem_bytes = (uint32_t)b->host.smem_bytes; info->flags = d.flags;
+    info->ticks = b->ticks_run;
+    info->algo_bytes_per_tick = b->host.algo_bytes_per_tick;
+    info->seg_bytes_per_tick = b->host.seg_bytes;
+    info->syn_bytes_per_tick = b->host.syn_bytes;
+    return BNC_OK;
+}
+
+int bnc_save_bion(void* sim, const char* filename) {
+    if (!sim || !filename) { set_error("null argument"); return BNC_ERR_ARG; }
+    Backend* b = static_cast<Backend*>(sim);
+    if (!b->owns_aos) { set_error("no host AoS view (network was generated on the device)"); return BNC_ERR_STATE; }
+    int rc = bnc_sync_to_host(sim);
+    if (rc != BNC_OK) return rc;
+    return save_bion(b->aos, filename);
+}
+
+}  // extern "C"

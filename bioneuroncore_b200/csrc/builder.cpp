@@ -1,0 +1,780 @@
+// builder.cpp -- AoS (reference layout) -> device structure-of-arrays.
+//
+// What the builder decides, once per load:
+//  * tiles: connected components of the intra-connection graph (whole neurons),
+//    packed into tiles of <= kMaxTileSegs segments with each component owned by one
+//    warp; the device segment order is the concatenation of tiles;
+//  * the modifier phase schedule: a global sequence of phases such that every
+//    segment's active modifiers appear in increasing slot order, each phase holding
+//    at most one modifier per segment.  A greedy shortest-common-supersequence
+//    pass picks, at each step, the type that is next for the most segments, so a
+//    phase is a single modifier type when slot orders allow it (warp-uniform
+//    dispatch); otherwise phases fall back to slot order with items sorted by type;
+//  * incidence lists per segment in original connection order, so every gather in
+//    the kernels sums in the reference's scatter order (diffusion_kernel.h loops
+//    over connections in index order);
+//  * the post-segment CSR of synapses in original synapse order, so per-post
+//    accumulation follows simulation_host.cpp:357-592.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <vector>
+#include "net.h"
+
+namespace bnc {
+
+DeviceAllocs::~DeviceAllocs() { release(); }
+
+void* DeviceAllocs::alloc(size_t bytes) {
+    void* p = nullptr;
+    if (bytes == 0) bytes = 16;
+    if (cudaMalloc(&p, bytes) != cudaSuccess) return nullptr;
+    ptrs.push_back(p);
+    return p;
+}
+
+void DeviceAllocs::release() {
+    for (void* p : ptrs) cudaFree(p);
+    ptrs.clear();
+}
+
+namespace {
+
+// ---- host restatements of the static per-segment helpers ----
+// run_tick_common.h:209-214
+float seg_area(const BncSegment& s) {
+    return (s.segment_type == 1 || s.segment_type == 3 || s.segment_type == 4)
+        ? 4.0f * 3.14159265f * s.radius * s.radius
+        : 2.0f * 3.14159265f * s.radius * s.length;
+}
+// run_tick_common.h:262-266
+double seg_volume(const BncSegment& s) {
+    if (s.segment_type == 1 || s.segment_type == 3 || s.segment_type == 4)
+        return (4.0 / 3.0) * 3.14159265f * (double)s.radius * (double)s.radius * (double)s.radius;
+    return 3.14159265f * (double)s.radius * (double)s.radius * (double)s.length;
+}
+// run_tick_common.h:216-231 (C_m in pF; myelin state[0] = g-ratio is static)
+float seg_capacitance(const BncSegment& s) {
+    float area = seg_area(s);
+    float C_m = area * 0.01f;
+    if (C_m < 1e-4f) C_m = 1e-4f;
+    for (uint8_t j = 0; j < s.modifier_count && j < 16; j++) {
+        if (s.modifiers[j].type == BNC_MOD_MYELIN) {
+            float gr = (float)s.modifiers[j].state[0];
+            if (gr <= 0.0f || gr >= 1.0f) gr = 0.6f;
+            float factor = 100.0f * (1.0f / gr - 1.0f) / (1.0f / 0.6f - 1.0f);
+            C_m /= factor;
+            break;
+        }
+    }
+    return C_m;
+}
+
+bool type_supported(uint8_t t) {
+    switch (t) {
+        case 1: case 4: case 7: case 8: case 9: case 11: case 12: case 85: case 98: case 99:
+        case 100: case 102: case 103: case 104: case 105: case 106: case 107: case 112:
+        case 123: case 129: case 133: case 140: case 141: case 142: case 150: case 200:
+            return true;
+        default: return false;
+    }
+}
+bool receptor_supported(uint8_t t) { return t == 8 || t == 9 || t == 11 || t == 12; }
+// kernel_dispatch.h:283-309
+bool is_ionotropic(uint8_t t) { return t <= 2 || (t >= 8 && t <= 16) || t == 97 || t == 134 || t == 194; }
+bool is_myelin_blocked(uint8_t t) {
+    static const uint8_t list[] = {107, 151, 152, 153, 133, 85, 202, 203, 204, 150, 205, 206, 207, 154, 156,
+                                   157, 159, 112, 123, 121, 105, 195, 84, 96, 191, 200, 201, 140, 158, 168,
+                                   129, 130, 131, 132, 103, 209, 104};
+    if (is_ionotropic(t)) return true;
+    for (uint8_t x : list) if (x == t) return true;
+    return false;
+}
+// modifier_helpers.h:747-758
+float bouton_gamma(uint8_t t) {
+    switch (t) {
+        case 156: return 10.0f; case 157: return 16.0f; case 123: return 11.0f; case 150: return 27.0f;
+        case 112: return 7.0f; case 107: return 100.0f; case 141: return 20.7f; case 142: return 20.8f;
+        default: return 0.0f;
+    }
+}
+// run_tick_common.h:199-206
+uint8_t nt_from_receptor(uint8_t rt) {
+    if (rt == 11 || rt == 17) return 1;
+    if (rt == 12) return 7;
+    if (rt == 14) return 3;
+    if (rt == 13) return 4;
+    if (rt == 44 || rt == 22) return 2;
+    return 0;
+}
+// state indices that are parameters (read-only, default when 0) per type
+uint8_t param_mask(uint8_t t) {
+    switch (t) {
+        case 1: return 0x1C;      // 2,3,4
+        case 85: return 0x34;     // 2,4,5
+        case 98: return 0x06;     // 1,2
+        case 100: return 0x06;
+        case 102: return 0x1D;    // 0,2,3,4
+        case 103: return 0x38;    // 3,4,5
+        case 104: return 0x06;    // 1,2
+        case 105: return 0x3E;    // 1..5
+        case 106: return 0x08;    // 3
+        case 107: return 0x03;    // 0,1
+        case 112: return 0x76;    // 1,2,4,5,6
+        case 123: return 0x16;    // 1,2,4
+        case 129: return 0x3E;    // 1..5
+        case 133: return 0x01;    // 0
+        case 141: case 142: return 0x20;  // 5
+        case 150: return 0x20;    // 5
+        case 200: return 0x7C;    // 2..6
+        default: return 0;
+    }
+}
+
+template <typename T>
+T* up(DeviceAllocs* a, const std::vector<T>& v, int* rc) {
+    T* p = (T*)a->alloc(v.size() * sizeof(T));
+    if (!p) { *rc = BNC_ERR_ALLOC; return nullptr; }
+    if (!v.empty() && cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice) != cudaSuccess)
+        *rc = BNC_ERR_CUDA;
+    return p;
+}
+template <typename T>
+T* zeros(DeviceAllocs* a, size_t n, int* rc) {
+    T* p = (T*)a->alloc(n * sizeof(T));
+    if (!p) { *rc = BNC_ERR_ALLOC; return nullptr; }
+    if (cudaMemset(p, 0, n * sizeof(T)) != cudaSuccess) *rc = BNC_ERR_CUDA;
+    return p;
+}
+
+struct UF {
+    std::vector<uint32_t> p;
+    explicit UF(uint32_t n) : p(n) { std::iota(p.begin(), p.end(), 0u); }
+    uint32_t f(uint32_t x) { while (p[x] != x) { p[x] = p[p[x]]; x = p[x]; } return x; }
+    void u(uint32_t a, uint32_t b) { a = f(a); b = f(b); if (a != b) { if (a < b) p[b] = a; else p[a] = b; } }
+};
+
+}  // namespace
+
+int upload_stimuli(const Stimuli& stim, const NetHost& host, NetDev* dev, DeviceAllocs* allocs) {
+    int rc = BNC_OK;
+    uint32_t n = host.n_seg;
+    // current stimuli: the reference matches segments[i].id (simulation_host.cpp:250-258);
+    // ids equal original indices for generated and well-formed networks, others are mapped
+    // through the id list at load time by the caller.
+    {
+        std::vector<uint32_t> cnt(n + 1, 0);
+        for (const auto& s : stim.current) if (s.segment_id < n) cnt[host.inv[s.segment_id] + 1]++;
+        for (uint32_t i = 0; i < n; i++) cnt[i + 1] += cnt[i];
+        std::vector<float> amp(cnt[n]), dur(cnt[n]);
+        std::vector<unsigned long long> start(cnt[n]);
+        std::vector<uint8_t> alive(cnt[n], 1);
+        std::vector<uint32_t> pos(cnt.begin(), cnt.end() - 1);
+        for (const auto& s : stim.current) {
+            if (s.segment_id >= n) continue;
+            uint32_t k = pos[host.inv[s.segment_id]]++;
+            amp[k] = s.amplitude_pA; dur[k] = s.duration_ms; start[k] = s.start_tick;
+        }
+        if (cnt[n]) {
+            dev->cs_off = up(allocs, cnt, &rc);
+            dev->cs_amp = up(allocs, amp, &rc);
+            dev->cs_dur = up(allocs, dur, &rc);
+            dev->cs_start = up(allocs, start, &rc);
+            dev->cs_alive = up(allocs, alive, &rc);
+        } else {
+            dev->cs_off = nullptr;
+        }
+    }
+    {
+        std::vector<uint32_t> cnt(n + 1, 0);
+        for (const auto& s : stim.vclamp) if (s.segment_id < n) cnt[host.inv[s.segment_id] + 1]++;
+        for (uint32_t i = 0; i < n; i++) cnt[i + 1] += cnt[i];
+        std::vector<float> tgt(cnt[n]);
+        std::vector<unsigned long long> st(cnt[n]), en(cnt[n]);
+        std::vector<uint32_t> pos(cnt.begin(), cnt.end() - 1);
+        for (const auto& s : stim.vclamp) {
+            if (s.segment_id >= n) continue;
+            uint32_t k = pos[host.inv[s.segment_id]]++;
+            tgt[k] = s.target_mV; st[k] = s.start_tick; en[k] = s.end_tick;
+        }
+        if (cnt[n]) {
+            dev->vc_off = up(allocs, cnt, &rc);
+            dev->vc_target = up(allocs, tgt, &rc);
+            dev->vc_start = up(allocs, st, &rc);
+            dev->vc_end = up(allocs, en, &rc);
+        } else {
+            dev->vc_off = nullptr;
+        }
+    }
+    return rc;
+}
+
+int build_network(const BncBionData& aos, const Stimuli& stim, NetDev* dev, NetHost* host,
+                  DeviceAllocs* allocs) {
+    std::memset(dev, 0, sizeof(*dev));
+    const uint32_t n = aos.num_segments;
+    const BncSegment* S = aos.segments;
+    if (n == 0 || !S) { set_error("network has no segments"); return BNC_ERR_ARG; }
+    if (n >= (1u << 31)) { set_error("too many segments"); return BNC_ERR_ARG; }
+    host->n_seg = n;
+    host->n_conn = aos.num_connections;
+    host->n_syn_total = aos.num_synapses;
+    // segment ids must be the positions (stimuli and the reference match on id)
+    for (uint32_t i = 0; i < n; i++) {
+        if (S[i].modifier_count > BNC_MAX_MODIFIERS) { set_error("segment %u: modifier_count %u > 32", i, S[i].modifier_count); return BNC_ERR_FORMAT; }
+        for (uint8_t j = 0; j < S[i].modifier_count; j++)
+            if (!type_supported(S[i].modifiers[j].type)) {
+                set_error("segment %u slot %u: modifier type %u has no device implementation in this backend",
+                          i, j, S[i].modifiers[j].type);
+                return BNC_ERR_UNSUPPORTED;
+            }
+    }
+    // ---- valid connections and components ----
+    std::vector<uint32_t> conn_ok;
+    conn_ok.reserve(aos.num_connections);
+    UF uf(n);
+    for (uint32_t c = 0; c < aos.num_connections; c++) {
+        const auto& cn = aos.connections[c];
+        if (cn.segment_a >= n || cn.segment_b >= n) continue;  // skipped by every reference loop
+        conn_ok.push_back(c);
+        uf.u(cn.segment_a, cn.segment_b);
+    }
+    std::vector<uint32_t> comp_of(n);
+    std::vector<uint32_t> comp_size(n, 0);
+    for (uint32_t i = 0; i < n; i++) { comp_of[i] = uf.f(i); comp_size[comp_of[i]]++; }
+    // components ordered by their smallest segment (root of the union-find is the minimum)
+    std::vector<uint32_t> roots;
+    for (uint32_t i = 0; i < n; i++) if (comp_of[i] == i) roots.push_back(i);
+    std::vector<uint32_t> comp_members_off(n + 1, 0);
+    {
+        std::vector<uint32_t> rank(n, 0);
+        for (uint32_t r = 0; r < roots.size(); r++) rank[roots[r]] = r;
+        std::vector<uint32_t> cnt(roots.size() + 1, 0);
+        for (uint32_t i = 0; i < n; i++) cnt[rank[comp_of[i]] + 1]++;
+        for (size_t r = 0; r < roots.size(); r++) cnt[r + 1] += cnt[r];
+        host->perm.assign(n, 0);
+        std::vector<uint32_t> pos(cnt.begin(), cnt.end() - 1);
+        for (uint32_t i = 0; i < n; i++) host->perm[pos[rank[comp_of[i]]]++] = i;
+        comp_members_off.assign(cnt.begin(), cnt.end());
+    }
+    host->inv.assign(n, 0);
+    for (uint32_t d = 0; d < n; d++) host->inv[host->perm[d]] = d;
+    // ---- tile packing: whole components, one component per warp slot ----
+    const uint32_t warp_cap = 64;
+    std::vector<uint32_t> tile_seg_beg{0};
+    std::vector<uint16_t> warp_seg;   // per tile kTileWarps+1 entries
+    {
+        uint32_t cur_tile_segs = 0, cur_warp = 0, cur_warp_segs = 0;
+        std::vector<uint16_t> wb(kTileWarps + 1, 0);
+        auto close_tile = [&]() {
+            for (int w = (int)cur_warp + 1; w <= kTileWarps; w++) wb[w] = (uint16_t)cur_tile_segs;
+            warp_seg.insert(warp_seg.end(), wb.begin(), wb.end());
+            tile_seg_beg.push_back(tile_seg_beg.back() + cur_tile_segs);
+            cur_tile_segs = 0; cur_warp = 0; cur_warp_segs = 0;
+            std::fill(wb.begin(), wb.end(), 0);
+        };
+        for (size_t r = 0; r < roots.size(); r++) {
+            uint32_t sz = comp_members_off[r + 1] - comp_members_off[r];
+            if (sz > (uint32_t)kMaxTileSegs) {
+                set_error("connected component of %u segments exceeds the %d-segment tile", sz, kMaxTileSegs);
+                return BNC_ERR_UNSUPPORTED;
+            }
+            bool fits_warp = cur_warp_segs > 0 && cur_warp_segs + sz <= warp_cap;
+            if (!fits_warp && cur_warp_segs > 0) {  // move to the next warp
+                cur_warp++;
+                wb[cur_warp] = (uint16_t)cur_tile_segs;
+                cur_warp_segs = 0;
+            }
+            if (cur_warp >= (uint32_t)kTileWarps || cur_tile_segs + sz > (uint32_t)kMaxTileSegs) {
+                // the open warp index is past the end or the tile is full: close it
+                if (cur_warp >= (uint32_t)kTileWarps) cur_warp = kTileWarps - 1;
+                close_tile();
+            }
+            cur_tile_segs += sz;
+            cur_warp_segs += sz;
+            wb[cur_warp + 1] = (uint16_t)cur_tile_segs;
+        }
+        if (cur_tile_segs > 0) close_tile();
+    }
+    const uint32_t T = (uint32_t)tile_seg_beg.size() - 1;
+    std::vector<uint32_t> tile_of(n);
+    for (uint32_t t = 0; t < T; t++)
+        for (uint32_t d = tile_seg_beg[t]; d < tile_seg_beg[t + 1]; d++) tile_of[d] = t;
+    // ---- edges grouped by tile and warp, in original connection order ----
+    std::vector<uint32_t> tile_edge_beg(T + 1, 0);
+    std::vector<uint16_t> warp_edge(T * (kTileWarps + 1), 0);
+    std::vector<uint32_t> edge_conn;   // device edge -> original connection index
+    {
+        std::vector<std::vector<uint32_t>> per_tile_warp((size_t)T * kTileWarps);
+        for (uint32_t c : conn_ok) {
+            uint32_t da = host->inv[aos.connections[c].segment_a];
+            uint32_t t = tile_of[da];
+            uint32_t la = da - tile_seg_beg[t];
+            int w = 0;
+            while (w < kTileWarps - 1 && la >= warp_seg[t * (kTileWarps + 1) + w + 1]) w++;
+            per_tile_warp[(size_t)t * kTileWarps + w].push_back(c);
+        }
+        for (uint32_t t = 0; t < T; t++) {
+            uint32_t e0 = (uint32_t)edge_conn.size();
+            for (int w = 0; w < kTileWarps; w++) {
+                warp_edge[t * (kTileWarps + 1) + w] = (uint16_t)(edge_conn.size() - e0);
+                auto& v = per_tile_warp[(size_t)t * kTileWarps + w];
+                edge_conn.insert(edge_conn.end(), v.begin(), v.end());
+            }
+            warp_edge[t * (kTileWarps + 1) + kTileWarps] = (uint16_t)(edge_conn.size() - e0);
+            tile_edge_beg[t + 1] = (uint32_t)edge_conn.size();
+            if (edge_conn.size() - e0 > 32767) { set_error("tile %u has more than 32767 connections", t); return BNC_ERR_UNSUPPORTED; }
+        }
+    }
+    const uint32_t E = (uint32_t)edge_conn.size();
+    std::vector<uint16_t> e_a(E), e_b(E);
+    std::vector<uint8_t> e_intra(E);
+    std::vector<float> e_area(E), e_dist(E);
+    for (uint32_t e = 0; e < E; e++) {
+        const auto& cn = aos.connections[edge_conn[e]];
+        uint32_t da = host->inv[cn.segment_a], db = host->inv[cn.segment_b];
+        uint32_t t = tile_of[da];
+        e_a[e] = (uint16_t)(da - tile_seg_beg[t]);
+        e_b[e] = (uint16_t)(db - tile_seg_beg[t]);
+        e_intra[e] = cn.is_intracellular;
+        const BncSegment& A = S[cn.segment_a];
+        const BncSegment& B = S[cn.segment_b];
+        float r_min = A.radius < B.radius ? A.radius : B.radius;
+        float area_conn = 3.14159265f * r_min * r_min;
+        if (area_conn < 1e-6f) area_conn = 1e-6f;
+        float dist = (A.length + B.length) * 0.5f;
+        if (dist < 0.1f) dist = 0.1f;
+        e_area[e] = area_conn;
+        e_dist[e] = dist;
+    }
+    // incidence lists per device segment: original connection order, a-role before b-role
+    std::vector<uint32_t> inc_off(n + 1, 0);
+    for (uint32_t e = 0; e < E; e++) {
+        const auto& cn = aos.connections[edge_conn[e]];
+        inc_off[host->inv[cn.segment_a] + 1]++;
+        inc_off[host->inv[cn.segment_b] + 1]++;
+    }
+    for (uint32_t i = 0; i < n; i++) inc_off[i + 1] += inc_off[i];
+    std::vector<uint16_t> inc(inc_off[n]);
+    {
+        // edges of a tile are sorted by warp then connection index; the gather needs
+        // connection order, so sort each segment's list by original connection index.
+        std::vector<uint32_t> pos(inc_off.begin(), inc_off.end() - 1);
+        std::vector<std::pair<uint32_t, uint16_t>> tmp;
+        std::vector<uint64_t> key(inc_off[n]);
+        for (uint32_t e = 0; e < E; e++) {
+            const auto& cn = aos.connections[edge_conn[e]];
+            uint32_t t = tile_of[host->inv[cn.segment_a]];
+            uint16_t le = (uint16_t)(e - tile_edge_beg[t]);
+            uint32_t da = host->inv[cn.segment_a], db = host->inv[cn.segment_b];
+            uint32_t ka = pos[da]++;
+            inc[ka] = le;
+            key[ka] = ((uint64_t)edge_conn[e] << 1) | 0u;
+            uint32_t kb = pos[db]++;
+            inc[kb] = (uint16_t)(le | 0x8000u);
+            key[kb] = ((uint64_t)edge_conn[e] << 1) | 1u;
+        }
+        std::vector<uint32_t> idx;
+        for (uint32_t d = 0; d < n; d++) {
+            uint32_t b = inc_off[d], e = inc_off[d + 1];
+            if (e - b < 2) continue;
+            idx.resize(e - b);
+            std::iota(idx.begin(), idx.end(), b);
+            std::sort(idx.begin(), idx.end(), [&](uint32_t x, uint32_t y) { return key[x] < key[y]; });
+            std::vector<uint16_t> tmpi(e - b);
+            for (uint32_t k = 0; k < e - b; k++) tmpi[k] = inc[idx[k]];
+            std::copy(tmpi.begin(), tmpi.end(), inc.begin() + b);
+        }
+    }
+    // ---- phase schedule (greedy shortest common supersequence over active types) ----
+    std::vector<uint32_t> act_off(n + 1, 0);   // per original segment active slot list
+    std::vector<uint8_t> act_slot;
+    act_slot.reserve((size_t)n * 8);
+    std::vector<uint8_t> sflags(n, 0);
+    uint32_t max_active = 0;
+    for (uint32_t i = 0; i < n; i++) {
+        const BncSegment& s = S[i];
+        bool myel = false, nmda = false;
+        for (uint8_t j = 0; j < s.modifier_count; j++) {
+            if (s.modifiers[j].type == BNC_MOD_MYELIN) myel = true;
+            if (s.modifiers[j].type == BNC_MOD_NMDA) nmda = true;
+        }
+        uint32_t c = 0;
+        for (uint8_t j = 0; j < s.modifier_count; j++) {
+            uint8_t t = s.modifiers[j].type;
+            if (myel && t != BNC_MOD_MYELIN && is_myelin_blocked(t)) continue;  // simulation_host.cpp:241
+            if (t == BNC_MOD_MYELIN) continue;  // myelin_modulator returns 0 and touches nothing
+            act_slot.push_back(j);
+            c++;
+        }
+        act_off[i + 1] = act_off[i] + c;
+        max_active = std::max(max_active, c);
+        sflags[i] = (uint8_t)((myel ? SF_MYELIN : 0) | (nmda ? SF_NMDA : 0));
+    }
+    std::vector<uint16_t> item_phase(act_slot.size(), 0);
+    uint32_t n_phases = 0;
+    {
+        std::vector<uint32_t> ptr(n, 0);
+        uint32_t remaining = (uint32_t)act_slot.size();
+        std::vector<uint64_t> count(256);
+        const uint32_t cap = std::max<uint32_t>(2 * max_active + 4, 8);
+        bool greedy_ok = true;
+        while (remaining > 0) {
+            std::fill(count.begin(), count.end(), 0);
+            for (uint32_t i = 0; i < n; i++) {
+                uint32_t k = act_off[i] + ptr[i];
+                if (k < act_off[i + 1]) count[S[i].modifiers[act_slot[k]].type]++;
+            }
+            int best = (int)(std::max_element(count.begin(), count.end()) - count.begin());
+            for (uint32_t i = 0; i < n; i++) {
+                uint32_t k = act_off[i] + ptr[i];
+                if (k < act_off[i + 1] && S[i].modifiers[act_slot[k]].type == best) {
+                    item_phase[k] = (uint16_t)n_phases;
+                    ptr[i]++;
+                    remaining--;
+                }
+            }
+            n_phases++;
+            if (n_phases > cap) { greedy_ok = false; break; }
+        }
+        if (!greedy_ok) {  // slot-order phases: phase = rank among the segment's active modifiers
+            for (uint32_t i = 0; i < n; i++)
+                for (uint32_t k = act_off[i]; k < act_off[i + 1]; k++) item_phase[k] = (uint16_t)(k - act_off[i]);
+            n_phases = max_active;
+        }
+    }
+    if (n_phases == 0) n_phases = 1;
+    // ---- items sorted by (tile, phase, type, device segment) ----
+    struct ItemKey { uint32_t tile; uint16_t phase; uint8_t type; uint32_t dseg; uint32_t k; };
+    std::vector<ItemKey> keys(act_slot.size());
+    for (uint32_t i = 0; i < n; i++) {
+        uint32_t d = host->inv[i];
+        for (uint32_t k = act_off[i]; k < act_off[i + 1]; k++)
+            keys[k] = {tile_of[d], item_phase[k], S[i].modifiers[act_slot[k]].type, d, k};
+    }
+    std::sort(keys.begin(), keys.end(), [](const ItemKey& x, const ItemKey& y) {
+        if (x.tile != y.tile) return x.tile < y.tile;
+        if (x.phase != y.phase) return x.phase < y.phase;
+        if (x.type != y.type) return x.type < y.type;
+        return x.dseg < y.dseg;
+    });
+    const uint32_t NI = (uint32_t)keys.size();
+    std::vector<uint32_t> it_meta(NI);
+    std::vector<float> it_den(NI), it_st((size_t)7 * NI);
+    std::vector<uint32_t> phase_off((size_t)T * (n_phases + 1), 0);
+    host->item_seg.assign(NI, 0);
+    host->item_slot.assign(NI, 0);
+    {
+        uint32_t k = 0;
+        for (uint32_t t = 0; t < T; t++) {
+            for (uint32_t p = 0; p <= n_phases; p++) {
+                while (k < NI && keys[k].tile == t && keys[k].phase < p) k++;
+                phase_off[(size_t)t * (n_phases + 1) + p] = k;
+            }
+            while (k < NI && keys[k].tile == t) k++;
+        }
+    }
+    for (uint32_t q = 0; q < NI; q++) {
+        const ItemKey& kk = keys[q];
+        uint32_t orig = host->perm[kk.dseg];
+        uint8_t slot = act_slot[kk.k];
+        const BncModifier& m = S[orig].modifiers[slot];
+        uint8_t fl = 0;
+        uint8_t pm = param_mask(m.type);
+        for (int b = 0; b < 7; b++) if ((pm >> b) & 1) if (m.state[b] != 0.0) fl |= 1;
+        if (receptor_supported(m.type) && m.active_vars > 0) {
+            if (m.active_vars >= 8) { set_error("segment %u slot %u: active_vars %u out of range", orig, slot, m.active_vars); return BNC_ERR_FORMAT; }
+            fl |= (uint8_t)(2u | ((uint32_t)m.active_vars << 2));
+        }
+        uint32_t local = kk.dseg - tile_seg_beg[kk.tile];
+        it_meta[q] = local | ((uint32_t)m.type << 16) | ((uint32_t)fl << 24);
+        it_den[q] = (float)m.density;
+        for (int b = 0; b < 7; b++) it_st[(size_t)b * NI + q] = (float)m.state[b];
+        host->item_seg[q] = orig;
+        host->item_slot[q] = slot;
+    }
+    // ---- per-segment state and statics in device order ----
+    std::vector<float> V(n), ion_in((size_t)7 * n), ion_out((size_t)7 * n), intra_nt((size_t)15 * n),
+        nt((size_t)15 * n), atp(n), temp(n), txn(n), radius(n), length(n), area(n), cm(n);
+    std::vector<double> vol(n), ibuf(n);
+    std::vector<uint8_t> stype(n), dflags(n);
+    std::vector<float2> c21(n);
+    bool intra_nt_grad = false, temp_grad = false, txn_grad = false;
+    for (uint32_t d = 0; d < n; d++) {
+        const BncSegment& s = S[host->perm[d]];
+        V[d] = (float)s.V_m;
+        for (int q = 0; q < 7; q++) {
+            ion_in[(size_t)q * n + d] = (float)s.intra_ions[q];
+            ion_out[(size_t)q * n + d] = (float)s.extra_ions[q];
+        }
+        for (int q = 0; q < 15; q++) {
+            intra_nt[(size_t)q * n + d] = s.intra_nt[q];
+            nt[(size_t)q * n + d] = s.neurotransmitter[q];
+        }
+        atp[d] = s.ATP_level; temp[d] = s.temperature; txn[d] = s.transcription_signal;
+        radius[d] = s.radius; length[d] = s.length; stype[d] = s.segment_type;
+        area[d] = seg_area(s); vol[d] = seg_volume(s); cm[d] = seg_capacitance(s);
+        ibuf[d] = s.I_buffer;
+        dflags[d] = sflags[host->perm[d]];
+        c21[d] = make_float2(0.0f, 0.0f);
+        for (uint8_t j = 0; j < s.modifier_count; j++)
+            if (s.modifiers[j].type == BNC_MOD_CAV21)
+                c21[d] = make_float2((float)s.modifiers[j].density, (float)s.modifiers[j].state[1]);
+    }
+    for (uint32_t c : conn_ok) {
+        const auto& cn = aos.connections[c];
+        const BncSegment& A = S[cn.segment_a];
+        const BncSegment& B = S[cn.segment_b];
+        if (cn.is_intracellular) {
+            for (int q = 0; q < 15; q++) if (A.intra_nt[q] != B.intra_nt[q]) intra_nt_grad = true;
+            if (A.temperature != B.temperature) temp_grad = true;
+            if (A.transcription_signal != B.transcription_signal) txn_grad = true;
+        }
+    }
+    // ---- synapses: valid chemical ones in post-segment CSR order ----
+    std::vector<uint32_t> syn_valid;
+    bool need_pre_ext = false, any_delay = false;
+    uint32_t nt_mask = 0;
+    for (uint32_t k = 0; k < aos.num_synapses; k++) {
+        const BncSynapse& y = aos.synapses[k];
+        if (y.pre_segment >= n || y.post_segment >= n) continue;   // simulation_host.cpp:362
+        if (y.type != BNC_SYN_CHEMICAL) {
+            set_error("synapse %u: electrical synapses have no device implementation in this backend", k);
+            return BNC_ERR_UNSUPPORTED;
+        }
+        if (y.post_receptor_count > BNC_MAX_POST_RECEPTORS || y.pre_autoreceptor_count > BNC_MAX_PRE_AUTORECEPTORS) {
+            set_error("synapse %u: receptor count out of range", k); return BNC_ERR_FORMAT;
+        }
+        for (uint8_t j = 0; j < y.post_receptor_count; j++)
+            if (!receptor_supported(y.post_receptors[j].type)) {
+                set_error("synapse %u receptor %u: type %u has no device implementation as a receptor", k, j,
+                          y.post_receptors[j].type);
+                return BNC_ERR_UNSUPPORTED;
+            }
+        for (uint8_t j = 0; j < y.pre_autoreceptor_count; j++)
+            if (bouton_gamma(y.pre_autoreceptors[j].type) == 0.0f) {
+                set_error("synapse %u autoreceptor %u: type %u (release modulators are not supported)", k, j,
+                          y.pre_autoreceptors[j].type);
+                return BNC_ERR_UNSUPPORTED;
+            }
+        uint8_t ntt = y.post_receptor_count > 0 ? nt_from_receptor(y.post_receptors[0].type) : 0;
+        for (int q = 0; q < 15; q++)
+            if (q != ntt && y.cleft_neurotransmitter[q] != 0.0f) {
+                set_error("synapse %u: cleft holds neurotransmitter %d other than the one it releases", k, q);
+                return BNC_ERR_UNSUPPORTED;
+            }
+        if (y.pre_autoreceptor_count > 0 || y.RRP_max > 0.0f) need_pre_ext = true;
+        if (y.delay > 0.0f) any_delay = true;
+        nt_mask |= 1u << ntt;
+        syn_valid.push_back(k);
+    }
+    std::stable_sort(syn_valid.begin(), syn_valid.end(), [&](uint32_t x, uint32_t y) {
+        return host->inv[aos.synapses[x].post_segment] < host->inv[aos.synapses[y].post_segment];
+    });
+    const uint32_t K = (uint32_t)syn_valid.size();
+    std::vector<uint32_t> post_off(n + 1, 0);
+    for (uint32_t k : syn_valid) post_off[host->inv[aos.synapses[k].post_segment] + 1]++;
+    for (uint32_t i = 0; i < n; i++) post_off[i + 1] += post_off[i];
+    std::vector<uint32_t> sy_pre(K), sy_id(K), rc_off(K + 1, 0);
+    std::vector<float> sy_prel(K), sy_amt(K), sy_tauc(K), sy_delay(K), sy_prea(K), sy_posta(K), sy_gK(K),
+        sy_gNa(K), sy_bouton(K), sy_spine(K), sy_camkii(K), sy_calcn(K), sy_facil(K), sy_weight(K), sy_cleft(K),
+        sy_rrp(K), sy_rrpm(K), sy_rrpr(K), sy_scale(K, 1.0f);
+    std::vector<uint8_t> sy_refr(K), sy_flags(K);
+    std::vector<uint8_t> rc_type, rc_av;
+    std::vector<float> rc_den, rc_st0, rc_st1, rc_st2;
+    host->syn_orig = syn_valid;
+    host->rec_syn.clear(); host->rec_slot.clear();
+    host->syn_nt.assign(K, 0);
+    for (uint32_t q = 0; q < K; q++) {
+        const BncSynapse& y = aos.synapses[syn_valid[q]];
+        sy_pre[q] = host->inv[y.pre_segment];
+        sy_id[q] = y.id;
+        sy_prel[q] = y.release_probability; sy_amt[q] = y.release_amount; sy_tauc[q] = y.tau_clearance;
+        sy_delay[q] = y.delay; sy_prea[q] = y.pre_area; sy_posta[q] = y.post_area;
+        float gK = 0.0f, gNa = 0.0f;
+        for (uint8_t j = 0; j < y.pre_autoreceptor_count; j++) {   // modifier_helpers.h:767-773
+            uint8_t t = y.pre_autoreceptors[j].type;
+            float g = (float)(y.pre_autoreceptors[j].density * bouton_gamma(t));
+            if (t == 141 || t == 142) gNa += g; else gK += g;
+        }
+        sy_gK[q] = gK; sy_gNa[q] = gNa;
+        sy_refr[q] = y.refractory;
+        uint8_t ntt = y.post_receptor_count > 0 ? nt_from_receptor(y.post_receptors[0].type) : 0;
+        bool inhib = false;
+        for (uint8_t j = 0; j < y.post_receptor_count; j++) {
+            uint8_t rt = y.post_receptors[j].type;
+            if (rt == 11 || rt == 17 || rt == 12) { inhib = true; break; }
+        }
+        sy_flags[q] = (uint8_t)((inhib ? 1u : 0u) | ((uint32_t)ntt << 4));
+        host->syn_nt[q] = ntt;
+        sy_bouton[q] = y.bouton_Ca; sy_spine[q] = y.spine_Ca; sy_camkii[q] = y.spine_camkii;
+        sy_calcn[q] = y.spine_calcineurin; sy_facil[q] = y.facilitation; sy_weight[q] = y.weight;
+        sy_cleft[q] = y.cleft_neurotransmitter[ntt];
+        sy_rrp[q] = y.RRP; sy_rrpm[q] = y.RRP_max; sy_rrpr[q] = y.RRP_recovery;
+        bool myel_post = (sflags[y.post_segment] & SF_MYELIN) != 0;
+        for (uint8_t j = 0; j < y.post_receptor_count; j++) {
+            const BncModifier& r = y.post_receptors[j];
+            if (myel_post && is_ionotropic(r.type)) continue;   // simulation_host.cpp:495
+            if (r.active_vars >= 8) { set_error("synapse %u receptor %u: active_vars out of range", syn_valid[q], j); return BNC_ERR_FORMAT; }
+            rc_type.push_back(r.type);
+            rc_av.push_back(r.active_vars);
+            rc_den.push_back((float)r.density);
+            rc_st0.push_back((float)r.state[0]);
+            rc_st1.push_back((float)r.state[1]);
+            rc_st2.push_back((float)r.state[2]);
+            if (r.active_vars >= 3 && r.active_vars <= 6) {
+                set_error("synapse %u receptor %u: active_vars %u not supported", syn_valid[q], j, r.active_vars);
+                return BNC_ERR_UNSUPPORTED;
+            }
+            host->rec_syn.push_back(q);
+            host->rec_slot.push_back(j);
+        }
+        rc_off[q + 1] = (uint32_t)rc_type.size();
+    }
+    const uint32_t NR = (uint32_t)rc_type.size();
+    std::vector<float> rc_st((size_t)3 * NR);
+    for (uint32_t r = 0; r < NR; r++) {
+        rc_st[r] = rc_st0[r]; rc_st[(size_t)NR + r] = rc_st1[r]; rc_st[(size_t)2 * NR + r] = rc_st2[r];
+    }
+    // ---- upload ----
+    int rc = BNC_OK;
+    dev->n_seg = n; dev->n_tiles = T; dev->n_items = NI; dev->n_phases = n_phases;
+    dev->n_syn = K; dev->n_rec = NR; dev->n_edges = E;
+    uint32_t flags = 0;
+    if (!conn_ok.empty()) flags |= NF_DIFFUSION;
+    if (aos.num_synapses > 0) flags |= NF_SYNAPSES;     // the reset keys on num_synapses, valid or not
+    if (intra_nt_grad) flags |= NF_INTRA_NT;
+    if (temp_grad) flags |= NF_TEMP;
+    if (txn_grad) flags |= NF_TXN;
+    if (need_pre_ext) flags |= NF_PRE_EXT;
+    if (any_delay) flags |= NF_DELAY;
+    if (!(flags & NF_SYNAPSES)) flags |= NF_NT_DIFFUSE_OUT;
+    dev->flags = flags;
+    bool any_nmda = false;
+    for (uint32_t i = 0; i < n; i++) if (sflags[i] & SF_NMDA) any_nmda = true;
+    dev->nt_used_mask = nt_mask | (any_nmda ? 1u : 0u);
+    dev->V = up(allocs, V, &rc);
+    dev->ion_in = up(allocs, ion_in, &rc);
+    dev->ion_out = up(allocs, ion_out, &rc);
+    dev->intra_nt = up(allocs, intra_nt, &rc);
+    dev->nt = up(allocs, nt, &rc);
+    dev->atp = up(allocs, atp, &rc);
+    dev->temp = up(allocs, temp, &rc);
+    dev->txn = up(allocs, txn, &rc);
+    dev->ibuf = up(allocs, ibuf, &rc);
+    dev->radius = up(allocs, radius, &rc);
+    dev->length = up(allocs, length, &rc);
+    dev->area = up(allocs, area, &rc);
+    dev->vol = up(allocs, vol, &rc);
+    dev->cm = up(allocs, cm, &rc);
+    dev->stype = up(allocs, stype, &rc);
+    dev->sflags = up(allocs, dflags, &rc);
+    dev->cav21_static = up(allocs, c21, &rc);
+    dev->pre_rec = zeros<float4>(allocs, n, &rc);
+    if (need_pre_ext) {
+        dev->pre_ext = zeros<float4>(allocs, n, &rc);
+        dev->pre_ext2 = zeros<float>(allocs, n, &rc);
+    }
+    dev->tile_seg_beg = up(allocs, tile_seg_beg, &rc);
+    dev->tile_edge_beg = up(allocs, tile_edge_beg, &rc);
+    dev->phase_off = up(allocs, phase_off, &rc);
+    dev->warp_seg = up(allocs, warp_seg, &rc);
+    dev->warp_edge = up(allocs, warp_edge, &rc);
+    dev->e_a = up(allocs, e_a, &rc);
+    dev->e_b = up(allocs, e_b, &rc);
+    dev->e_intra = up(allocs, e_intra, &rc);
+    dev->e_area = up(allocs, e_area, &rc);
+    dev->e_dist = up(allocs, e_dist, &rc);
+    dev->inc_off = up(allocs, inc_off, &rc);
+    dev->inc = up(allocs, inc, &rc);
+    dev->it_meta = up(allocs, it_meta, &rc);
+    dev->it_den = up(allocs, it_den, &rc);
+    dev->it_st = up(allocs, it_st, &rc);
+    dev->post_off = up(allocs, post_off, &rc);
+    dev->sy_pre = up(allocs, sy_pre, &rc);
+    dev->sy_id = up(allocs, sy_id, &rc);
+    dev->sy_prel = up(allocs, sy_prel, &rc);
+    dev->sy_amt = up(allocs, sy_amt, &rc);
+    dev->sy_tauc = up(allocs, sy_tauc, &rc);
+    dev->sy_delay = up(allocs, sy_delay, &rc);
+    dev->sy_pre_area = up(allocs, sy_prea, &rc);
+    dev->sy_post_area = up(allocs, sy_posta, &rc);
+    dev->sy_gK = up(allocs, sy_gK, &rc);
+    dev->sy_gNa = up(allocs, sy_gNa, &rc);
+    dev->sy_refr = up(allocs, sy_refr, &rc);
+    dev->sy_flags = up(allocs, sy_flags, &rc);
+    dev->sy_bouton = up(allocs, sy_bouton, &rc);
+    dev->sy_spine = up(allocs, sy_spine, &rc);
+    dev->sy_camkii = up(allocs, sy_camkii, &rc);
+    dev->sy_calcn = up(allocs, sy_calcn, &rc);
+    dev->sy_facil = up(allocs, sy_facil, &rc);
+    dev->sy_weight = up(allocs, sy_weight, &rc);
+    dev->sy_cleft = up(allocs, sy_cleft, &rc);
+    dev->sy_rrp = up(allocs, sy_rrp, &rc);
+    dev->sy_rrp_max = up(allocs, sy_rrpm, &rc);
+    dev->sy_rrp_rec = up(allocs, sy_rrpr, &rc);
+    dev->sy_scale = up(allocs, sy_scale, &rc);
+    dev->rc_off = up(allocs, rc_off, &rc);
+    dev->rc_type = up(allocs, rc_type, &rc);
+    dev->rc_av = up(allocs, rc_av, &rc);
+    dev->rc_den = up(allocs, rc_den, &rc);
+    dev->rc_st = up(allocs, rc_st, &rc);
+    if (any_delay) {
+        dev->dl_arr = zeros<unsigned long long>(allocs, (size_t)4 * K, &rc);
+        dev->dl_amt = zeros<float>(allocs, (size_t)4 * K, &rc);
+        dev->dl_nt = zeros<uint8_t>(allocs, (size_t)4 * K, &rc);
+    }
+    dev->spike_count = zeros<uint32_t>(allocs, n, &rc);
+    dev->err_flag = zeros<int>(allocs, 1, &rc);
+    if (rc == BNC_OK) rc = upload_stimuli(stim, *host, dev, allocs);
+    if (rc != BNC_OK) { set_error("device allocation/upload failed (%d)", rc); return rc; }
+    // tile sizes for the shared-memory plan
+    uint32_t mts = 0, mte = 0;
+    for (uint32_t t = 0; t < T; t++) {
+        mts = std::max(mts, tile_seg_beg[t + 1] - tile_seg_beg[t]);
+        mte = std::max(mte, tile_edge_beg[t + 1] - tile_edge_beg[t]);
+    }
+    host->max_tile_segs = mts;
+    host->max_tile_edges = mte;
+    host->smem_bytes = tile_smem_bytes(mts, mte);
+    // ---- algorithmic bytes per tick of this schema (what one tick must move at minimum) ----
+    {
+        // kernel A per segment: read V, 14 ions, ATP, geometry+C_m (radius, length, area,
+        // vol, cm, type, flags), write V, 14 ions, ATP, I_buffer, pre-record.
+        double seg_a = 4 * 2 + 56 * 2 + 4 * 2 + (4 + 4 + 4 + 8 + 4 + 1 + 1) + 8 + 16;
+        if (flags & NF_INTRA_NT) seg_a += 120;
+        if (flags & NF_TEMP) seg_a += 8;
+        if (flags & NF_TXN) seg_a += 8;
+        if (flags & NF_DIFFUSION) seg_a += 4 * 2.0 * E / n + 8 * 2.0 * E / n;   // incidence + edge statics
+        // modifier items: meta + density read, dynamic state read+write
+        double items = 0;
+        for (uint32_t q = 0; q < NI; q++) {
+            uint8_t t = (uint8_t)(it_meta[q] >> 16);
+            int dyn = 0;
+            switch (t) {
+                case 1: case 8: case 11: case 12: case 85: case 140: case 141: case 142: case 200: dyn = 2; break;
+                case 9: dyn = 2; break;
+                case 150: dyn = 3; break;
+                case 102: case 103: case 104: case 105: case 112: case 123: case 129: dyn = 1; break;
+                default: dyn = 0;
+            }
+            if (t == 85) dyn = 3;
+            items += 4 + 4 + 8.0 * dyn;
+        }
+        // kernel B per segment: I_buffer, V rw, 7 intra ions rw, 4 extra ions, C_m, flags,
+        // used neurotransmitters written, CSR offset
+        int nt_used = __builtin_popcount(dev->nt_used_mask);
+        double seg_b = 8 + 4 * 2 + 28 * 2 + 16 + 4 + 1 + 4.0 * nt_used + 4;
+        // per synapse: pre index, id, pre-record, scalar params, dynamic state rw, receptors
+        double syn = 4 + 4 + 16 + 4 * 5 + 1 + 1 + (4 * 6 + 1) * 2 + 4;
+        double rec = 0;
+        for (uint32_t r = 0; r < NR; r++) rec += 1 + 4 + 8.0 * (rc_type[r] == 9 ? 2 : 2);
+        host->seg_bytes = (seg_a + seg_b) * n + items;
+        host->syn_bytes = syn * K + rec + 4.0 * (K + 1);
+        host->algo_bytes_per_tick = host->seg_bytes + host->syn_bytes;
+    }
+    return BNC_OK;
+}
+
+}  // namespace bnc

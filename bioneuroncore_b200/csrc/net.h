@@ -1,0 +1,170 @@
+// net.h -- the device-resident network: structure-of-arrays state, static
+// geometry, tile/phase schedule and synapse CSR, plus the host-side maps needed
+// to export back to the reference's AoS layout.
+#pragma once
+#include <cstdint>
+#include <vector>
+#include <cuda_runtime.h>
+#include "common.h"
+
+namespace bnc {
+
+// Launch geometry of the tile kernel (segments per tile, warps per tile).
+constexpr int kTileWarps = 8;
+constexpr int kTileThreads = kTileWarps * 32;
+constexpr int kMaxTileSegs = 1024;
+
+// Network-level flags.
+enum : uint32_t {
+    NF_DIFFUSION = 1u,      // any valid connection: step 2.5 runs (diffusion_kernel.h:118)
+    NF_SYNAPSES = 2u,       // any synapse: step 3 resets neurotransmitter (simulation_host.cpp:328)
+    NF_INTRA_NT = 4u,       // some intra_nt gradient exists: intracellular NT diffusion needed
+    NF_TEMP = 8u,           // some temperature gradient exists
+    NF_TXN = 16u,           // some transcription-signal gradient exists
+    NF_PRE_EXT = 32u,       // synapses read presynaptic intracellular ions (RRP or bouton channels)
+    NF_DELAY = 64u,         // some synapse has a transmission delay
+    NF_NT_DIFFUSE_OUT = 128u, // neurotransmitter diffusion result is live (no synapses reset it)
+};
+
+// Per-segment flags.
+enum : uint8_t { SF_MYELIN = 1u, SF_NMDA = 2u };
+
+// Plain-old-data descriptor passed by value to the kernels.
+struct NetDev {
+    uint32_t n_seg, n_tiles, n_items, n_phases, n_syn, n_rec, n_edges;
+    uint32_t flags;
+    uint32_t nt_used_mask;  // neurotransmitter indices that synapses/bath can make nonzero
+    // segment state (device order, ion-major for the 7-ion arrays)
+    float* V;
+    float* ion_in;    // [7][n_seg]
+    float* ion_out;   // [7][n_seg]
+    float* intra_nt;  // [15][n_seg]
+    float* nt;        // [15][n_seg]
+    float* atp;
+    float* temp;
+    float* txn;
+    double* ibuf;
+    // segment statics
+    float* radius;
+    float* length;
+    float* area;
+    double* vol;
+    float* cm;
+    uint8_t* stype;
+    uint8_t* sflags;
+    float2* cav21_static;   // (density, state[1]) of the last Cav2.1 when it never updates
+    float4* pre_rec;        // V, Ca_out, Cav2.1 density, Cav2.1 h  (after step 2.5)
+    float4* pre_ext;        // Na_in, K_in, Ca_in, Na_out
+    float* pre_ext2;        // K_out
+    // tiles
+    uint32_t* tile_seg_beg;   // [n_tiles+1] device segment offsets
+    uint32_t* tile_edge_beg;  // [n_tiles+1]
+    uint32_t* phase_off;      // [n_tiles*(n_phases+1)] absolute item offsets
+    uint16_t* warp_seg;       // [n_tiles*(kTileWarps+1)] tile-local offsets
+    uint16_t* warp_edge;      // [n_tiles*(kTileWarps+1)]
+    // edges (tile-grouped, tile-local endpoints)
+    uint16_t* e_a;
+    uint16_t* e_b;
+    uint8_t* e_intra;
+    float* e_area;
+    float* e_dist;
+    uint32_t* inc_off;        // [n_seg+1]
+    uint16_t* inc;            // tile-local edge index | (endpoint-is-b << 15)
+    // modifier items
+    uint32_t* it_meta;        // tile-local segment (16) | type (8) | flags (8)
+    float* it_den;
+    float* it_st;             // [7][n_items]
+    // current stimuli, per-segment CSR in stimulus order
+    uint32_t* cs_off;         // [n_seg+1] (nullptr when none)
+    float* cs_amp;
+    float* cs_dur;
+    unsigned long long* cs_start;
+    uint8_t* cs_alive;
+    // voltage clamps, per-segment CSR
+    uint32_t* vc_off;         // (nullptr when none)
+    float* vc_target;
+    unsigned long long* vc_start;
+    unsigned long long* vc_end;
+    // synapses in post-segment CSR order
+    uint32_t* post_off;       // [n_seg+1]
+    uint32_t* sy_pre;         // device index of the presynaptic segment
+    uint32_t* sy_id;
+    float* sy_prel;
+    float* sy_amt;
+    float* sy_tauc;
+    float* sy_delay;
+    float* sy_pre_area;
+    float* sy_post_area;
+    float* sy_gK;
+    float* sy_gNa;
+    uint8_t* sy_refr;
+    uint8_t* sy_flags;        // bit0 inhibitory, bits 4..7 released NT index
+    float* sy_bouton;
+    float* sy_spine;
+    float* sy_camkii;
+    float* sy_calcn;
+    float* sy_facil;
+    float* sy_weight;
+    float* sy_cleft;          // cleft concentration of the released NT
+    float* sy_rrp;
+    float* sy_rrp_max;
+    float* sy_rrp_rec;
+    float* sy_scale;          // receptor density scale (1 reproduces the reference)
+    uint32_t* rc_off;         // [n_syn+1]
+    uint8_t* rc_type;
+    uint8_t* rc_av;
+    float* rc_den;
+    float* rc_st;             // [3][n_rec]
+    unsigned long long* dl_arr;  // [4][n_syn]
+    float* dl_amt;
+    uint8_t* dl_nt;
+    uint32_t* spike_count;    // [n_seg]
+    int* err_flag;            // device-side error report (0 = ok)
+};
+
+// Host copy of everything the exporter needs to map device state back.
+struct NetHost {
+    uint32_t n_seg = 0, n_conn = 0, n_syn_total = 0;
+    std::vector<uint32_t> perm;      // device index -> original segment index
+    std::vector<uint32_t> inv;       // original segment index -> device index
+    std::vector<uint32_t> item_seg;  // item -> original segment index
+    std::vector<uint8_t> item_slot;  // item -> modifier slot
+    std::vector<uint32_t> syn_orig;  // device synapse -> original synapse index
+    std::vector<uint32_t> rec_syn;   // device receptor -> device synapse
+    std::vector<uint8_t> rec_slot;   // device receptor -> receptor slot
+    std::vector<uint8_t> syn_nt;     // released NT per device synapse
+    uint32_t max_tile_segs = 0, max_tile_edges = 0;
+    size_t smem_bytes = 0;
+    double algo_bytes_per_tick = 0;  // algorithmic HBM bytes per tick (see bytes_model)
+    double seg_bytes = 0, syn_bytes = 0;
+};
+
+struct Stimuli {
+    std::vector<BncCurrentStimulus> current;
+    std::vector<BncVoltageClamp> vclamp;
+};
+
+// Builds host-side SoA from AoS and uploads it.  Returns 0 or BNC_ERR_*; on error
+// bnc_last_error() explains.  `dev` receives device pointers (owned by `allocs`).
+struct DeviceAllocs {
+    std::vector<void*> ptrs;
+    ~DeviceAllocs();
+    void* alloc(size_t bytes);
+    void release();
+};
+
+int build_network(const BncBionData& aos, const Stimuli& stim, NetDev* dev, NetHost* host,
+                  DeviceAllocs* allocs);
+
+// Rebuilds the per-segment stimulus CSRs after an upload of new stimuli.
+int upload_stimuli(const Stimuli& stim, const NetHost& host, NetDev* dev, DeviceAllocs* allocs);
+
+// Writes device state back into the AoS arrays.
+int export_network(const NetDev& dev, const NetHost& host, uint64_t ticks_run, BncBionData* aos);
+
+// Kernel launchers (kernels.cu).
+cudaError_t launch_tick(const NetDev& dev, const NetHost& host, float dt, unsigned long long tick,
+                        int first_tick, cudaStream_t stream);
+size_t tile_smem_bytes(uint32_t max_segs, uint32_t max_edges);
+
+}  // namespace bnc

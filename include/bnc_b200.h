@@ -28,18 +28,26 @@
 extern "C" {
 #endif
 
-/* error codes (the loader codes mirror reference src/bion_loader_host.cpp:13-24) */
+/* .bion loader codes: the reference's BION_ERR_* values (src/bion_loader_host.cpp:13-24),
+ * so gpu_backend_load_bion fails with the same numbers as the reference backend. */
 #define BNC_OK 0
-#define BNC_ERR_ARG -1
-#define BNC_ERR_FILE -2
-#define BNC_ERR_FORMAT -3
-#define BNC_ERR_VERSION -4
+#define BNC_BION_ERR_FILE_OPEN -1
+#define BNC_BION_ERR_BAD_MAGIC -2
+#define BNC_BION_ERR_BAD_VERSION -3
+#define BNC_BION_ERR_ZERO_SEGS -4
 #define BNC_ERR_ALLOC -5
-#define BNC_ERR_INDEX -6
-#define BNC_ERR_UNSUPPORTED -7
-#define BNC_ERR_CUDA -8
-#define BNC_ERR_STATE -9
-#define BNC_ERR_DEVICE_TIMEOUT -10
+#define BNC_BION_ERR_BAD_CONN -6
+#define BNC_BION_ERR_BAD_SYNAPSE -7
+#define BNC_BION_ERR_BAD_NEURON -8
+#define BNC_ERR_FORMAT -9
+#define BNC_BION_ERR_WRITE_FAIL -10
+#define BNC_BION_ERR_FILE_READ -11
+/* backend codes */
+#define BNC_ERR_ARG -20
+#define BNC_ERR_UNSUPPORTED -21
+#define BNC_ERR_CUDA -22
+#define BNC_ERR_STATE -23
+#define BNC_ERR_DEVICE_TIMEOUT -24
 
 /* ------------------------------------------------------------------ */
 /* 1. drop-in set (reference src/gpu_backend_cuda.cu:316-390)          */
@@ -54,7 +62,11 @@ void* gpu_backend_create_on_device(int device_index);
 /* Replaces gpu_backend_destroy (gpu_backend_cuda.cu:329-331). */
 void gpu_backend_destroy(void* sim);
 /* Replaces gpu_backend_load_bion (gpu_backend_cuda.cu:333-336): loads a .bion
- * v3..v14 file; 0 on success, negative on failure. */
+ * file written with the v14 record sizes (v10+ header; the reference's loader
+ * also migrates v3-v13 layouts, bion_loader_host.cpp:99-263; those fail here with
+ * BNC_BION_ERR_BAD_VERSION).  0 on success, the reference's BION_ERR_* codes on
+ * file errors, BNC_ERR_UNSUPPORTED when the network uses something the device
+ * path does not implement (message in bnc_last_error). */
 int gpu_backend_load_bion(void* sim, const char* filename);
 /* Replaces gpu_backend_run_tick (gpu_backend_cuda.cu:338-341): one tick of dt
  * ms; afterwards the AoS view returned by gpu_backend_bion_data is coherent
@@ -110,6 +122,50 @@ typedef struct {
 int bnc_netgen_aos(const BncNetgenParams* p, BncBionData* out,
                    BncCurrentStimulus** stim, uint32_t* n_stim);
 void bnc_netgen_free(BncBionData* data, BncCurrentStimulus* stim);
+
+/* Loads a network from host AoS arrays in the reference layout (copied; the
+ * backend keeps its own AoS for gpu_backend_bion_data).  `stim` may be NULL. */
+int bnc_load_aos(void* sim, const BncBionData* data, const BncCurrentStimulus* stim, uint32_t n_stim);
+
+/* Generates a network and builds it on the device without keeping a host AoS
+ * copy (gpu_backend_bion_data then returns NULL); for networks too large for it. */
+int bnc_load_generated(void* sim, const BncNetgenParams* p);
+
+/* Runs n ticks of dt ms on the device without refreshing the host AoS view. */
+int bnc_run_ticks(void* sim, uint32_t n_ticks, float dt);
+
+/* Runs n ticks bracketed by CUDA events on the backend's stream; *ms receives the
+ * elapsed device time. */
+int bnc_time_ticks(void* sim, uint32_t n_ticks, float dt, float* ms);
+
+/* Copies device state into the host AoS view (no-op when none is held). */
+int bnc_sync_to_host(void* sim);
+
+/* Field reads in original segment / synapse order (host float arrays of n).
+ * Segment fields: 0 V_m, 1 intra ion[index], 2 extra ion[index], 3 ATP,
+ *   4 temperature, 5 transcription, 6 intra_nt[index], 7 neurotransmitter[index],
+ *   8 modifier state (index = slot*8 + k), 9 spike count (V crossing -40 mV upward).
+ * Synapse fields: 0 bouton_Ca, 1 spine_Ca, 2 weight, 3 refractory,
+ *   4 cleft_neurotransmitter[index], 5 receptor state (index = j*8 + k),
+ *   6 facilitation, 7 spine_camkii, 8 spine_calcineurin, 9 RRP. */
+int bnc_read_segment_field(void* sim, int field, int index, float* out, uint32_t n);
+int bnc_read_synapse_field(void* sim, int field, int index, float* out, uint32_t n);
+
+/* Per-synapse multiplicative scale of the receptor density (the differentiable
+ * synaptic weight; 1.0 everywhere reproduces the reference). */
+int bnc_set_synapse_scale(void* sim, const float* scale, uint32_t n);
+
+typedef struct {
+    uint32_t n_segments, n_connections, n_synapses, n_tiles, n_items, n_phases, n_receptors;
+    uint32_t max_tile_segs, max_tile_edges, smem_bytes, flags;
+    uint64_t ticks;
+    double algo_bytes_per_tick;   /* algorithmic HBM bytes one tick moves (state schema) */
+    double seg_bytes_per_tick, syn_bytes_per_tick;
+} BncNetInfo;
+int bnc_network_info(void* sim, BncNetInfo* info);
+
+/* Writes the host AoS view to a .bion v14 file (reference bion_save layout). */
+int bnc_save_bion(void* sim, const char* filename);
 
 /* Message for the last error on this thread ("" when none). */
 const char* bnc_last_error(void);

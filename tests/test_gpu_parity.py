@@ -1,0 +1,77 @@
+"""GPU tick vs the CPU oracle, through the C ABI.
+
+The kernels restate the reference's arithmetic operation by operation with FP32
+state (the oracle's precision rule), the same elementary functions and no fused
+multiply-adds, and every accumulation follows the reference's loop order.  So the
+bar here is bit-exact equality of every state variable, tick by tick: V_m, ions,
+modifier gates, synapse state, spike counts and release decisions.  Networks are
+small seeded instances of the workload families.
+"""
+import numpy as np
+import pytest
+
+from oracle.oracle import Oracle
+
+pytestmark = pytest.mark.gpu
+
+DT = 0.025
+
+
+def _pair(params):
+    from bioneuroncore_b200 import Backend, Network
+    net_o = Network(params)
+    net_g = Network(params)
+    ora = Oracle(net_o)
+    gpu = Backend()
+    gpu.load_network(net_g)
+    return ora, gpu, net_g
+
+
+def _assert_same(a, b, what):
+    a = np.asarray(a, np.float32)
+    b = np.asarray(b, np.float32)
+    same = (a.view(np.uint32) == b.view(np.uint32)) | (np.isnan(a) & np.isnan(b))
+    if not same.all():
+        i = int(np.argmax(~same))
+        raise AssertionError("%s differs at %d of %d: gpu %r oracle %r (%d mismatches)"
+                             % (what, i, a.size, a[i], b[i], int((~same).sum())))
+
+
+SEG_CHECKS = [("V", 0)] + [("ion_in", q) for q in range(7)] + [("ion_out", q) for q in range(7)] + [
+    ("ATP", 0), ("temperature", 0), ("transcription", 0), ("spikes", 0)] + [("neurotransmitter", q) for q in (0, 1, 7)]
+SYN_CHECKS = [("bouton_Ca", 0), ("spine_Ca", 0), ("weight", 0), ("refractory", 0), ("facilitation", 0),
+              ("spine_camkii", 0), ("spine_calcineurin", 0), ("cleft", 0), ("cleft", 1),
+              ("receptor_state", 0), ("receptor_state", 1)]
+
+
+def _compare_all(ora, gpu, n_syn, label):
+    for f, i in SEG_CHECKS:
+        _assert_same(gpu.segment_field(f, i), ora.segment_field(f, i), "%s %s[%d]" % (label, f, i))
+    for slot in range(6):
+        for k in range(3):
+            _assert_same(gpu.segment_field("mod_state", slot * 8 + k), ora.segment_field("mod_state", slot * 8 + k),
+                         "%s modifier slot %d state %d" % (label, slot, k))
+    if n_syn:
+        for f, i in SYN_CHECKS:
+            _assert_same(gpu.synapse_field(f, i, n_syn), ora.synapse_field(f, i), "%s synapse %s[%d]" % (label, f, i))
+
+
+@pytest.mark.parametrize("flags", [0, 1 | 2, 1, 2])
+def test_small_network_bitexact(flags):
+    from bioneuroncore_b200 import NetgenParams, NET_SMALL
+    p = NetgenParams(family=NET_SMALL, n_neurons=16, seed=11, flags=flags)
+    ora, gpu, net = _pair(p)
+    for step in (1, 9, 40):
+        ora.run(step, DT)
+        gpu.run_ticks(step, DT)
+        _compare_all(ora, gpu, net.data.num_synapses, "small flags=%d after +%d" % (flags, step))
+
+
+def test_large_set_bitexact():
+    from bioneuroncore_b200 import NetgenParams, NET_LARGE
+    p = NetgenParams(family=NET_LARGE, n_neurons=12, n_synapses=300, seed=5)
+    ora, gpu, net = _pair(p)
+    for step in (1, 20, 30):
+        ora.run(step, DT)
+        gpu.run_ticks(step, DT)
+        _compare_all(ora, gpu, net.data.num_synapses, "large after +%d" % step)
