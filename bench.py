@@ -1,0 +1,304 @@
+#!/usr/bin/env python
+"""Benchmark of the per-tick simulation loop on B200.
+
+Workload: the large plain network -- 100,000 neurons x 64 segments (6.4M segments),
+16 modifiers per segment drawn from 24 channel/receptor/pump types, Cav2.1 on axon
+segments, 10M chemical synapses with 8 receptors each, dt = 0.025 ms -- generated
+from a seed (synthetic data; no dataset exists for this path).  A step is one tick.
+
+    python bench.py [--gpus N --steps K --warmup W]          # this backend
+    python bench.py --impl reference [--steps K --warmup W]  # reference CPU tick
+
+value       segment-ticks/s of the whole job, device-timed with CUDA events on the
+            backend's stream around exactly K ticks (max over ranks for N > 1;
+            each rank runs its own network, weak scaling, no collective).
+e2e         the same metric through bnc_step_io: per tick, an H2D copy of the
+            stimulus amplitudes from pinned memory and a D2H copy of every
+            segment's V_m into pinned memory, wall clock around K steps.
+roofline    the dominant kernel's algorithmic bytes per launch over its average
+            CUDA-event duration, against the measured copy bandwidth.
+cpu_baseline the reference's own CPU tick (oracle/_ref, built from the reference
+            sources) on a bounded sample of the same workload, 1 core.
+"""
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+DT = 0.025
+WORKLOAD = ("large plain network: 100000 neurons x 64 segments (6.4M segments), 16 modifiers/segment "
+            "from 24 types, 10M synapses x 8 receptors, dt 0.025 ms")
+METRIC = "segment-ticks/s (plain 6.4M-segment network)"
+UNIT = "segment-ticks/s"
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=400)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--neurons", type=int, default=100000)
+    ap.add_argument("--seed", type=int, default=20260)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=100)
+    return ap.parse_args()
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples every 200 ms while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(prefix="bnc_clocks_", suffix=".csv")
+        os.close(fd)
+        try:
+            self.out = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.out, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.out.close()
+        sms, maxes, reasons, power = [], [], set(), []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                p = [x.strip() for x in line.split(",")]
+                if len(p) < 9:
+                    continue
+                try:
+                    sms.append(float(p[1]))
+                    maxes.append(float(p[2]))
+                    power.append(float(p[3]))
+                except ValueError:
+                    continue
+                for n, v in zip(names, p[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sms) if sms else None, "sm_max_mhz": max(maxes) if maxes else None,
+                "reasons": sorted(reasons), "samples": len(sms),
+                "power_w_max": max(power) if power else None}
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def ncu_traffic(kernel):
+    """DRAM bytes per launch recorded in the committed ncu summary of `kernel`, if any."""
+    path = os.path.join(ROOT, "profiles", "%s_large_network.md" % kernel)
+    try:
+        with open(path) as f:
+            m = re.search(r"dram_bytes_per_launch_full_size:\s*([0-9.eE+]+)", f.read())
+            return float(m.group(1)) if m else None
+    except OSError:
+        return None
+
+
+def cpu_reference_rate(neurons, ticks, warm, seed):
+    """Reference CPU tick (or the oracle port when the reference build is absent) on a
+    generated network; returns (segment-ticks/s, kind, segments)."""
+    import ctypes as C
+    from bioneuroncore_b200 import Network, NetgenParams, NET_LARGE
+    from oracle import oracle as orc
+    net = Network(NetgenParams(family=NET_LARGE, n_neurons=neurons, seed=seed))
+    nseg = net.data.num_segments
+    if orc.reference_available():
+        runner, kind = orc.Reference(net), "reference"
+    else:
+        runner, kind = orc.Oracle(net), "port"
+    runner.run(warm, DT)
+    t0 = time.perf_counter()
+    runner.run(ticks, DT)
+    dt = time.perf_counter() - t0
+    return nseg * ticks / dt, kind, nseg
+
+
+def _ref_worker(args):
+    neurons, ticks, warm, seed = args
+    return cpu_reference_rate(neurons, ticks, warm, seed)
+
+
+def run_reference_arm(a):
+    rank, _, world = dist_env()
+    if rank != 0:
+        return 0
+    import multiprocessing as mp
+    ncores = os.cpu_count() or 1
+    neurons = 128   # 8192 segments, 12,800 synapses per process and step
+    ctx = mp.get_context("spawn")
+    t0 = time.perf_counter()
+    with ctx.Pool(ncores) as pool:
+        res = pool.map(_ref_worker, [(neurons, a.steps, a.warmup, a.seed + i) for i in range(ncores)])
+    wall = time.perf_counter() - t0
+    value = sum(r[0] for r in res)
+    kind = res[0][1]
+    seg = res[0][2]
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": 1000.0 * seg * ncores / value if value else None,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "sample_per_process": "%d neurons x 64 segments" % neurons,
+                   "processes": ncores, "parallelism": "independent processes (the reference tick is single-threaded "
+                                                         "and not re-entrant)"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": ncores, "kind": kind,
+                         "sample": "%d processes x (%d neurons x 64 segments, %d ticks after %d warm-up)"
+                                   % (ncores, neurons, a.steps, a.warmup)},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "wall_s": wall,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    a = parse_args()
+    if a.impl == "reference":
+        return run_reference_arm(a)
+    rank, local_rank, world = dist_env()
+    dist = None
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local_rank))
+    from bioneuroncore_b200 import Backend, NetgenParams, NET_LARGE
+    b = Backend(local_rank if world > 1 else 0)
+    t0 = time.perf_counter()
+    b.load_generated(NetgenParams(family=NET_LARGE, n_neurons=a.neurons, seed=a.seed + rank))
+    setup_s = time.perf_counter() - t0
+    info = b.info()
+    b.run_ticks(a.warmup, DT)
+    n_prof = max(3, min(10, a.steps))
+    ms_tile, ms_syn = b.profile_ticks(n_prof, DT)
+
+    def barrier():
+        if dist is not None:
+            import torch
+            t = torch.zeros(1, device="cuda")
+            dist.all_reduce(t)
+            torch.cuda.synchronize()
+
+    barrier()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    ms = b.time_ticks(a.steps, DT)
+    clk = clocks.stop()
+    barrier()
+    ms_max = ms
+    if dist is not None:
+        import torch
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+    seg_ticks = float(info.n_segments) * a.steps * world
+    value = seg_ticks / (ms_max / 1000.0)
+
+    # end-to-end through the public step call with pinned host buffers
+    e2e = None
+    if not a.no_e2e:
+        import torch
+        n_stim = int(info.n_segments // 64 * 0.1 + 0.5)
+        amp = torch.full((n_stim,), 200.0, dtype=torch.float32).pin_memory()
+        vout = torch.empty(info.n_segments, dtype=torch.float32).pin_memory()
+        b.step_io(DT, amp.data_ptr(), n_stim, vout.data_ptr(), info.n_segments)
+        barrier()
+        t1 = time.perf_counter()
+        for _ in range(a.e2e_steps):
+            b.step_io(DT, amp.data_ptr(), n_stim, vout.data_ptr(), info.n_segments)
+        el = time.perf_counter() - t1
+        if dist is not None:
+            t = torch.tensor([el], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            el = float(t.item())
+        e2e = {"value": float(info.n_segments) * a.e2e_steps * world / el, "unit": UNIT,
+               "h2d_bytes_per_step": 4 * n_stim, "d2h_bytes_per_step": 4 * info.n_segments,
+               "steps": a.e2e_steps, "timing": "host wall clock around the steps, max over ranks"}
+
+    # roofline of the dominant kernel
+    peak, peak_kind = measured_peak()
+    tile_avg = ms_tile / n_prof
+    syn_avg = ms_syn / n_prof
+    if tile_avg >= syn_avg:
+        kname, kbytes, kms = "k_tile", info.tile_bytes_per_tick, tile_avg
+    else:
+        kname, kbytes, kms = "k_synapse", info.synapse_kernel_bytes_per_tick, syn_avg
+    achieved = kbytes / (kms / 1000.0) / 1e9
+    roofline = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": peak_kind, "traffic": ncu_traffic(kname),
+                "algo_bytes_per_launch": kbytes, "avg_launch_ms": kms,
+                "kernels_ms": {"k_tile": tile_avg, "k_synapse": syn_avg},
+                "tick_bytes": info.algo_bytes_per_tick,
+                "tick_frac": info.algo_bytes_per_tick / (ms_max / a.steps / 1000.0) / 1e9 / peak}
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        try:
+            rate, kind, nseg = cpu_reference_rate(1000, 5, 1, a.seed)
+            cpu = {"value": rate, "unit": UNIT, "cores": 1, "kind": kind,
+                   "sample": "1000 neurons x 64 segments (%d segments, 100,000 synapses) of the same generator, "
+                             "5 ticks after 1 warm-up tick" % nseg}
+        except Exception as exc:  # the baseline is reported, never required
+            cpu = {"value": None, "unit": UNIT, "cores": 1, "kind": "unavailable", "sample": str(exc)[:200]}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": ms_max / a.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 state, f64 GHK/accumulators", "data": "synthetic (seeded generator)",
+            "config": {"workload": WORKLOAD, "segments_per_gpu": info.n_segments,
+                       "synapses_per_gpu": info.n_synapses, "parallelism": "replicas" if world > 1 else "single",
+                       "l2": "inputs larger than L2 (device state ~8 GB per GPU)",
+                       "tiles": info.n_tiles, "phases": info.n_phases, "setup_s": round(setup_s, 1)},
+            "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,
+            "gpu_launches": 2 * a.steps,
+        }
+        print(json.dumps(line), flush=True)
+    b.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -35,7 +35,8 @@ DROPIN_SYMBOLS = ["gpu_backend_create", "gpu_backend_create_on_device", "gpu_bac
                   "gpu_backend_ibuf_offset", "gpu_backend_vm_offset", "gpu_backend_seg_size"]
 NEW_SYMBOLS = ["bnc_netgen_aos", "bnc_netgen_free", "bnc_last_error", "bnc_load_aos", "bnc_load_generated",
                "bnc_run_ticks", "bnc_time_ticks", "bnc_sync_to_host", "bnc_read_segment_field",
-               "bnc_read_synapse_field", "bnc_set_synapse_scale", "bnc_network_info", "bnc_save_bion"]
+               "bnc_read_synapse_field", "bnc_set_synapse_scale", "bnc_network_info", "bnc_save_bion",
+               "bnc_plan_generated", "bnc_step_io", "bnc_profile_ticks"]
 
 
 class NetInfo(C.Structure):
@@ -43,7 +44,15 @@ class NetInfo(C.Structure):
                                           "n_phases", "n_receptors", "max_tile_segs", "max_tile_edges",
                                           "smem_bytes", "flags")] + [
         ("ticks", C.c_uint64), ("algo_bytes_per_tick", C.c_double), ("seg_bytes_per_tick", C.c_double),
-        ("syn_bytes_per_tick", C.c_double)]
+        ("syn_bytes_per_tick", C.c_double), ("tile_bytes_per_tick", C.c_double),
+        ("synapse_kernel_bytes_per_tick", C.c_double)]
+
+
+def plan_generated(params):
+    """Host-only planning of a generated network (no device needed); returns NetInfo."""
+    inf = NetInfo()
+    _check(load_library().bnc_plan_generated(C.byref(params), C.byref(inf)), "bnc_plan_generated")
+    return inf
 
 
 class BackendError(RuntimeError):
@@ -76,7 +85,8 @@ def load_library(path=LIB_PATH):
         "bnc_read_segment_field": ([vp, i32, i32, vp, u32], i32),
         "bnc_read_synapse_field": ([vp, i32, i32, vp, u32], i32),
         "bnc_set_synapse_scale": ([vp, vp, u32], i32), "bnc_network_info": ([vp, vp], i32),
-        "bnc_save_bion": ([vp, C.c_char_p], i32),
+        "bnc_save_bion": ([vp, C.c_char_p], i32), "bnc_plan_generated": ([vp, vp], i32),
+        "bnc_step_io": ([vp, f32, vp, u32, vp, u32], i32), "bnc_profile_ticks": ([vp, u32, f32, vp, vp], i32),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -187,6 +197,17 @@ class Backend:
         ms = C.c_float()
         _check(self.lib.bnc_time_ticks(self.h, n, C.c_float(dt), C.byref(ms)), "bnc_time_ticks")
         return ms.value
+
+    def step_io(self, dt, stim_amp_ptr=0, n_amp=0, v_out_ptr=0, n_v=0):
+        """One tick with host<->device copies (pointers to host buffers, pinned for async)."""
+        _check(self.lib.bnc_step_io(self.h, C.c_float(dt), stim_amp_ptr or None, n_amp, v_out_ptr or None, n_v),
+               "bnc_step_io")
+
+    def profile_ticks(self, n, dt):
+        """Runs n ticks; returns (ms in the tile kernel, ms in the synapse kernel)."""
+        a, b = C.c_float(), C.c_float()
+        _check(self.lib.bnc_profile_ticks(self.h, n, C.c_float(dt), C.byref(a), C.byref(b)), "bnc_profile_ticks")
+        return a.value, b.value
 
     def sync_to_host(self):
         _check(self.lib.bnc_sync_to_host(self.h), "bnc_sync_to_host")

@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 #include "net.h"
 #include "netgen.h"
+#include "hostnet.h"
 
 namespace bnc {
 
@@ -136,40 +137,34 @@ int export_network(const NetDev& d, const NetHost& h, uint64_t ticks_run, BncBio
     return BNC_OK;
 }
 
-// ---- builder sink for generated networks: AoS chunks are never held whole ----
+// ---- generator -> compact host network (no AoS materialised) ----
 namespace {
-struct CollectSink : NetSink {
-    BncBionData* out;
+struct HostNetSink : NetSink {
+    HostNet* hn;
     std::vector<BncCurrentStimulus>* stim;
-    uint32_t ni = 0, si = 0, ci = 0;
-    uint64_t yi = 0;
-    bool ok = true;
-    void begin(uint32_t n_neurons, uint32_t n_segments, uint32_t n_connections, uint64_t n_synapses,
-               uint32_t) override {
-        std::memset(out, 0, sizeof(*out));
-        out->num_neurons = n_neurons; out->num_segments = n_segments;
-        out->num_connections = n_connections; out->num_synapses = (uint32_t)n_synapses;
-        out->header.magic = 0x42494F4Eu; out->header.version = 14;
-        out->header.num_neurons = n_neurons; out->header.num_segments = n_segments;
-        out->header.num_intra_connections = n_connections; out->header.num_synapses = (uint32_t)n_synapses;
-        out->neurons = new (std::nothrow) BncNeuron[n_neurons ? n_neurons : 1];
-        out->segments = new (std::nothrow) BncSegment[n_segments ? n_segments : 1];
-        out->connections = new (std::nothrow) BncIntraConnection[n_connections ? n_connections : 1];
-        out->synapses = new (std::nothrow) BncSynapse[n_synapses ? n_synapses : 1];
-        ok = out->neurons && out->segments && out->connections && out->synapses;
+    void begin(uint32_t, uint32_t n_segments, uint32_t n_connections, uint64_t n_synapses, uint32_t) override {
+        *hn = HostNet();
+        hn->seg.reserve(n_segments);
+        hn->mods.reserve((size_t)n_segments * 17);
+        hn->conn.reserve(n_connections);
+        hn->syn.reserve(n_synapses);
+        hn->recs.reserve(n_synapses * 8);
+        hn->num_connections = n_connections;
     }
-    void neuron(const BncNeuron& n) override { if (ok) out->neurons[ni++] = n; }
-    void segment(const BncSegment& s) override { if (ok) out->segments[si++] = s; }
-    void connection(const BncIntraConnection& c) override { if (ok) out->connections[ci++] = c; }
-    void synapse(const BncSynapse& s) override { if (ok) out->synapses[yi++] = s; }
+    void neuron(const BncNeuron&) override {}
+    void segment(const BncSegment& s) override { hostnet_add_segment(*hn, s); }
+    void connection(const BncIntraConnection& c) override { hn->conn.push_back(c); }
+    void synapse(const BncSynapse& s) override { hostnet_add_synapse(*hn, s); }
     void stimulus(const BncCurrentStimulus& st) override { stim->push_back(st); }
 };
 }  // namespace
 
 static int load_common(Backend* b, BncBionData& aos, bool keep_aos) {
     cudaSetDevice(b->device);
-    int rc = build_network(aos, b->stim, &b->dev, &b->host, &b->allocs);
-    if (rc != BNC_OK) { b->reset_network(); if (!keep_aos) {} return rc; }
+    HostNet hn;
+    hostnet_from_aos(aos, &hn);
+    int rc = build_network(hn, b->stim, &b->dev, &b->host, &b->allocs);
+    if (rc != BNC_OK) { b->reset_network(); return rc; }
     if (keep_aos) { b->aos = aos; b->owns_aos = true; }
     b->loaded = true;
     return BNC_OK;
@@ -410,17 +405,43 @@ int bnc_load_generated(void* sim, const BncNetgenParams* p) {
     if (!sim || !p) { set_error("bnc_load_generated: null argument"); return BNC_ERR_ARG; }
     Backend* b = static_cast<Backend*>(sim);
     b->reset_network();
-    BncBionData d;
-    CollectSink sink;
-    sink.out = &d;
+    HostNet hn;
+    HostNetSink sink;
+    sink.hn = &hn;
     sink.stim = &b->stim.current;
     NetShape shape;
     int rc = generate_network(*p, sink, &shape);
-    if (rc != BNC_OK) { free_aos_arrays(d); set_error("bnc_load_generated: invalid parameters"); return rc; }
-    if (!sink.ok) { free_aos_arrays(d); set_error("bnc_load_generated: out of host memory"); return BNC_ERR_ALLOC; }
-    rc = load_common(b, d, false);
-    free_aos_arrays(d);
-    return rc;
+    if (rc != BNC_OK) { set_error("bnc_load_generated: invalid parameters"); return rc; }
+    cudaSetDevice(b->device);
+    rc = build_network(hn, b->stim, &b->dev, &b->host, &b->allocs);
+    if (rc != BNC_OK) { b->reset_network(); return rc; }
+    b->loaded = true;
+    return BNC_OK;
+}
+
+int bnc_plan_generated(const BncNetgenParams* p, BncNetInfo* info) {
+    if (!p || !info) { set_error("bnc_plan_generated: null argument"); return BNC_ERR_ARG; }
+    HostNet hn;
+    Stimuli stim;
+    HostNetSink sink;
+    sink.hn = &hn;
+    sink.stim = &stim.current;
+    NetShape shape;
+    int rc = generate_network(*p, sink, &shape);
+    if (rc != BNC_OK) { set_error("bnc_plan_generated: invalid parameters"); return rc; }
+    NetDev dev;
+    NetHost host;
+    rc = build_network(hn, stim, &dev, &host, nullptr);
+    if (rc != BNC_OK) return rc;
+    std::memset(info, 0, sizeof(*info));
+    info->n_segments = dev.n_seg; info->n_connections = host.n_conn; info->n_synapses = dev.n_syn;
+    info->n_tiles = dev.n_tiles; info->n_items = dev.n_items; info->n_phases = dev.n_phases;
+    info->n_receptors = dev.n_rec; info->max_tile_segs = host.max_tile_segs;
+    info->max_tile_edges = host.max_tile_edges; info->smem_bytes = (uint32_t)host.smem_bytes;
+    info->flags = dev.flags; info->algo_bytes_per_tick = host.algo_bytes_per_tick;
+    info->seg_bytes_per_tick = host.seg_bytes; info->syn_bytes_per_tick = host.syn_bytes;
+    info->tile_bytes_per_tick = host.tile_bytes; info->synapse_kernel_bytes_per_tick = host.synk_bytes;
+    return BNC_OK;
 }
 
 int bnc_run_ticks(void* sim, uint32_t n_ticks, float dt) {
@@ -443,6 +464,70 @@ int bnc_time_ticks(void* sim, uint32_t n_ticks, float dt, float* ms) {
     if (rc != BNC_OK) return rc;
     cudaEventElapsedTime(ms, b->ev0, b->ev1);
     return BNC_OK;
+}
+
+int bnc_step_io(void* sim, float dt, const float* stim_amp, uint32_t n_amp, float* v_out, uint32_t n_v) {
+    if (!sim) { set_error("null handle"); return BNC_ERR_ARG; }
+    Backend* b = static_cast<Backend*>(sim);
+    if (!b->loaded) { set_error("no network loaded"); return BNC_ERR_STATE; }
+    cudaSetDevice(b->device);
+    cudaError_t e;
+    if (stim_amp && n_amp) {
+        if (!b->dev.cs_off || n_amp != (uint32_t)b->stim.current.size()) {
+            set_error("stimulus amplitude count %u does not match the %zu loaded current stimuli", n_amp,
+                      b->stim.current.size());
+            return BNC_ERR_ARG;
+        }
+        if (b->host.stim_identity) {
+            e = cudaMemcpyAsync(b->dev.cs_amp, stim_amp, n_amp * sizeof(float), cudaMemcpyHostToDevice, b->stream);
+            if (e != cudaSuccess) return cuda_fail(e, "stimulus upload");
+        } else {
+            set_error("per-step amplitudes need stimuli uploaded in per-segment order");
+            return BNC_ERR_UNSUPPORTED;
+        }
+    }
+    int rc = run_ticks(b, 1, dt);
+    if (rc != BNC_OK) return rc;
+    if (v_out && n_v) {
+        if (n_v < b->dev.n_seg) { set_error("V buffer too short"); return BNC_ERR_ARG; }
+        if (!b->host.perm_identity) { set_error("V read-back in step_io needs an identity segment order"); return BNC_ERR_UNSUPPORTED; }
+        e = cudaMemcpyAsync(v_out, b->dev.V, b->dev.n_seg * sizeof(float), cudaMemcpyDeviceToHost, b->stream);
+        if (e != cudaSuccess) return cuda_fail(e, "V read-back");
+    }
+    return sync_stream(b);
+}
+
+int bnc_profile_ticks(void* sim, uint32_t n_ticks, float dt, float* ms_tile, float* ms_synapse) {
+    if (!sim || !ms_tile || !ms_synapse) { set_error("null argument"); return BNC_ERR_ARG; }
+    Backend* b = static_cast<Backend*>(sim);
+    if (!b->loaded) { set_error("no network loaded"); return BNC_ERR_STATE; }
+    cudaSetDevice(b->device);
+    cudaEvent_t e[3];
+    for (auto& x : e) cudaEventCreate(&x);
+    float tt = 0.0f, ts = 0.0f;
+    int rc = BNC_OK;
+    for (uint32_t t = 0; t < n_ticks && rc == BNC_OK; t++) {
+        cudaEventRecord(e[0], b->stream);
+        cudaError_t er = launch_tile(b->dev, b->host, dt, b->tick, b->stream);
+        if (er != cudaSuccess) { rc = cuda_fail(er, "tile launch"); break; }
+        cudaEventRecord(e[1], b->stream);
+        er = launch_synapse(b->dev, dt, b->tick, b->ticks_run == 0 ? 1 : 0, b->stream);
+        if (er != cudaSuccess) { rc = cuda_fail(er, "synapse launch"); break; }
+        cudaEventRecord(e[2], b->stream);
+        b->tick++;
+        b->ticks_run++;
+        rc = sync_stream(b);
+        if (rc != BNC_OK) break;
+        float a = 0.0f, c = 0.0f;
+        cudaEventElapsedTime(&a, e[0], e[1]);
+        cudaEventElapsedTime(&c, e[1], e[2]);
+        tt += a;
+        ts += c;
+    }
+    for (auto& x : e) cudaEventDestroy(x);
+    *ms_tile = tt;
+    *ms_synapse = ts;
+    return rc;
 }
 
 int bnc_sync_to_host(void* sim) {
@@ -577,6 +662,8 @@ int bnc_network_info(void* sim, BncNetInfo* info) {
     info->algo_bytes_per_tick = b->host.algo_bytes_per_tick;
     info->seg_bytes_per_tick = b->host.seg_bytes;
     info->syn_bytes_per_tick = b->host.syn_bytes;
+    info->tile_bytes_per_tick = b->host.tile_bytes;
+    info->synapse_kernel_bytes_per_tick = b->host.synk_bytes;
     return BNC_OK;
 }
 

@@ -20,7 +20,11 @@
 #include <cstring>
 #include <numeric>
 #include <vector>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
 #include "net.h"
+#include "hostnet.h"
 
 namespace bnc {
 
@@ -43,25 +47,26 @@ namespace {
 
 // ---- host restatements of the static per-segment helpers ----
 // run_tick_common.h:209-214
-float seg_area(const BncSegment& s) {
+float seg_area(const SegLite& s) {
     return (s.segment_type == 1 || s.segment_type == 3 || s.segment_type == 4)
         ? 4.0f * 3.14159265f * s.radius * s.radius
         : 2.0f * 3.14159265f * s.radius * s.length;
 }
 // run_tick_common.h:262-266
-double seg_volume(const BncSegment& s) {
+double seg_volume(const SegLite& s) {
     if (s.segment_type == 1 || s.segment_type == 3 || s.segment_type == 4)
         return (4.0 / 3.0) * 3.14159265f * (double)s.radius * (double)s.radius * (double)s.radius;
     return 3.14159265f * (double)s.radius * (double)s.radius * (double)s.length;
 }
 // run_tick_common.h:216-231 (C_m in pF; myelin state[0] = g-ratio is static)
-float seg_capacitance(const BncSegment& s) {
+float seg_capacitance(const HostNet& hn, uint32_t i) {
+    const SegLite& s = hn.seg[i];
     float area = seg_area(s);
     float C_m = area * 0.01f;
     if (C_m < 1e-4f) C_m = 1e-4f;
     for (uint8_t j = 0; j < s.modifier_count && j < 16; j++) {
-        if (s.modifiers[j].type == BNC_MOD_MYELIN) {
-            float gr = (float)s.modifiers[j].state[0];
+        if (hn.mod(i, j).type == BNC_MOD_MYELIN) {
+            float gr = hn.mod(i, j).state[0];
             if (gr <= 0.0f || gr >= 1.0f) gr = 0.6f;
             float factor = 100.0f * (1.0f / gr - 1.0f) / (1.0f / 0.6f - 1.0f);
             C_m /= factor;
@@ -157,7 +162,7 @@ struct UF {
 
 }  // namespace
 
-int upload_stimuli(const Stimuli& stim, const NetHost& host, NetDev* dev, DeviceAllocs* allocs) {
+int upload_stimuli(const Stimuli& stim, NetHost& host, NetDev* dev, DeviceAllocs* allocs) {
     int rc = BNC_OK;
     uint32_t n = host.n_seg;
     // current stimuli: the reference matches segments[i].id (simulation_host.cpp:250-258);
@@ -171,9 +176,12 @@ int upload_stimuli(const Stimuli& stim, const NetHost& host, NetDev* dev, Device
         std::vector<unsigned long long> start(cnt[n]);
         std::vector<uint8_t> alive(cnt[n], 1);
         std::vector<uint32_t> pos(cnt.begin(), cnt.end() - 1);
+        host.stim_identity = true;
+        uint32_t j = 0;
         for (const auto& s : stim.current) {
-            if (s.segment_id >= n) continue;
+            if (s.segment_id >= n) { host.stim_identity = false; continue; }
             uint32_t k = pos[host.inv[s.segment_id]]++;
+            if (k != j++) host.stim_identity = false;
             amp[k] = s.amplitude_pA; dur[k] = s.duration_ms; start[k] = s.start_tick;
         }
         if (cnt[n]) {
@@ -210,12 +218,82 @@ int upload_stimuli(const Stimuli& stim, const NetHost& host, NetDev* dev, Device
     return rc;
 }
 
-int build_network(const BncBionData& aos, const Stimuli& stim, NetDev* dev, NetHost* host,
+void hostnet_add_segment(HostNet& hn, const BncSegment& s) {
+    SegLite L;
+    std::memset(&L, 0, sizeof(L));
+    L.id = s.id;
+    L.segment_type = s.segment_type;
+    L.modifier_count = s.modifier_count > BNC_MAX_MODIFIERS ? (uint8_t)BNC_MAX_MODIFIERS : s.modifier_count;
+    L.radius = s.radius; L.length = s.length;
+    L.V_m = (float)s.V_m;
+    for (int q = 0; q < 7; q++) { L.intra_ions[q] = (float)s.intra_ions[q]; L.extra_ions[q] = (float)s.extra_ions[q]; }
+    for (int q = 0; q < 15; q++) { L.intra_nt[q] = s.intra_nt[q]; L.neurotransmitter[q] = s.neurotransmitter[q]; }
+    L.ATP_level = s.ATP_level; L.temperature = s.temperature; L.transcription_signal = s.transcription_signal;
+    L.I_buffer = s.I_buffer;
+    L.mod_off = hn.mods.size();
+    for (uint8_t j = 0; j < L.modifier_count; j++) {
+        const BncModifier& m = s.modifiers[j];
+        ModLite M;
+        M.type = m.type; M.active_vars = m.active_vars; M.density = (float)m.density;
+        for (int k = 0; k < 8; k++) M.state[k] = (float)m.state[k];
+        hn.mods.push_back(M);
+    }
+    hn.seg.push_back(L);
+    hn.num_segments = (uint32_t)hn.seg.size();
+}
+
+void hostnet_add_synapse(HostNet& hn, const BncSynapse& y) {
+    SynLite L;
+    std::memset(&L, 0, sizeof(L));
+    L.id = y.id; L.pre_segment = y.pre_segment; L.post_segment = y.post_segment; L.type = y.type;
+    L.pre_autoreceptor_count = y.pre_autoreceptor_count; L.post_receptor_count = y.post_receptor_count;
+    L.refractory = y.refractory;
+    L.weight = y.weight; L.delay = y.delay; L.pre_area = y.pre_area; L.post_area = y.post_area;
+    L.release_probability = y.release_probability; L.release_amount = y.release_amount;
+    L.tau_clearance = y.tau_clearance; L.facilitation = y.facilitation; L.depression = y.depression;
+    L.RRP = y.RRP; L.RRP_max = y.RRP_max; L.RRP_recovery = y.RRP_recovery;
+    L.bouton_Ca = y.bouton_Ca; L.spine_Ca = y.spine_Ca; L.spine_camkii = y.spine_camkii;
+    L.spine_calcineurin = y.spine_calcineurin;
+    for (int q = 0; q < 15; q++) L.cleft_neurotransmitter[q] = y.cleft_neurotransmitter[q];
+    L.rec_off = hn.recs.size();
+    uint8_t npr = y.post_receptor_count > 8 ? 8 : y.post_receptor_count;
+    uint8_t npa = y.pre_autoreceptor_count > 8 ? 8 : y.pre_autoreceptor_count;
+    for (uint8_t j = 0; j < npr + npa; j++) {
+        const BncModifier& m = j < npr ? y.post_receptors[j] : y.pre_autoreceptors[j - npr];
+        ModLite M;
+        M.type = m.type; M.active_vars = m.active_vars; M.density = (float)m.density;
+        for (int k = 0; k < 8; k++) M.state[k] = (float)m.state[k];
+        hn.recs.push_back(M);
+    }
+    hn.syn.push_back(L);
+    hn.num_synapses = (uint32_t)hn.syn.size();
+}
+
+void hostnet_from_aos(const BncBionData& aos, HostNet* hn) {
+    *hn = HostNet();
+    hn->seg.reserve(aos.num_segments);
+    hn->syn.reserve(aos.num_synapses);
+    for (uint32_t i = 0; i < aos.num_segments; i++) hostnet_add_segment(*hn, aos.segments[i]);
+    hn->conn.assign(aos.connections, aos.connections + aos.num_connections);
+    hn->num_connections = aos.num_connections;
+    for (uint32_t k = 0; k < aos.num_synapses; k++) hostnet_add_synapse(*hn, aos.synapses[k]);
+}
+
+int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* host,
                   DeviceAllocs* allocs) {
+    const bool verbose = std::getenv("BNC_VERBOSE") != nullptr;
+    auto t_last = std::chrono::steady_clock::now();
+    auto lap = [&](const char* what) {
+        if (!verbose) return;
+        auto now = std::chrono::steady_clock::now();
+        fprintf(stderr, "[bnc build] %-28s %8.3f s\n", what, std::chrono::duration<double>(now - t_last).count());
+        t_last = now;
+    };
     std::memset(dev, 0, sizeof(*dev));
-    const uint32_t n = aos.num_segments;
-    const BncSegment* S = aos.segments;
-    if (n == 0 || !S) { set_error("network has no segments"); return BNC_ERR_ARG; }
+    const uint32_t n = hn.num_segments;
+    const std::vector<SegLite>& S = hn.seg;
+    const HostNet& aos = hn;
+    if (n == 0 || S.empty()) { set_error("network has no segments"); return BNC_ERR_ARG; }
     if (n >= (1u << 31)) { set_error("too many segments"); return BNC_ERR_ARG; }
     host->n_seg = n;
     host->n_conn = aos.num_connections;
@@ -224,9 +302,9 @@ int build_network(const BncBionData& aos, const Stimuli& stim, NetDev* dev, NetH
     for (uint32_t i = 0; i < n; i++) {
         if (S[i].modifier_count > BNC_MAX_MODIFIERS) { set_error("segment %u: modifier_count %u > 32", i, S[i].modifier_count); return BNC_ERR_FORMAT; }
         for (uint8_t j = 0; j < S[i].modifier_count; j++)
-            if (!type_supported(S[i].modifiers[j].type)) {
+            if (!type_supported(hn.mod(i, j).type)) {
                 set_error("segment %u slot %u: modifier type %u has no device implementation in this backend",
-                          i, j, S[i].modifiers[j].type);
+                          i, j, hn.mod(i, j).type);
                 return BNC_ERR_UNSUPPORTED;
             }
     }
@@ -235,7 +313,7 @@ int build_network(const BncBionData& aos, const Stimuli& stim, NetDev* dev, NetH
     conn_ok.reserve(aos.num_connections);
     UF uf(n);
     for (uint32_t c = 0; c < aos.num_connections; c++) {
-        const auto& cn = aos.connections[c];
+        const auto& cn = hn.conn[c];
         if (cn.segment_a >= n || cn.segment_b >= n) continue;  // skipped by every reference loop
         conn_ok.push_back(c);
         uf.u(cn.segment_a, cn.segment_b);
@@ -259,7 +337,12 @@ int build_network(const BncBionData& aos, const Stimuli& stim, NetDev* dev, NetH
         comp_members_off.assign(cnt.begin(), cnt.end());
     }
     host->inv.assign(n, 0);
-    for (uint32_t d = 0; d < n; d++) host->inv[host->perm[d]] = d;
+    host->perm_identity = true;
+    for (uint32_t d = 0; d < n; d++) {
+        host->inv[host->perm[d]] = d;
+        if (host->perm[d] != d) host->perm_identity = false;
+    }
+    lap("components");
     // ---- tile packing: whole components, one component per warp slot ----
     const uint32_t warp_cap = 64;
     std::vector<uint32_t> tile_seg_beg{0};
@@ -301,6 +384,7 @@ int build_network(const BncBionData& aos, const Stimuli& stim, NetDev* dev, NetH
     std::vector<uint32_t> tile_of(n);
     for (uint32_t t = 0; t < T; t++)
         for (uint32_t d = tile_seg_beg[t]; d < tile_seg_beg[t + 1]; d++) tile_of[d] = t;
+    lap("tiles");
     // ---- edges grouped by tile and warp, in original connection order ----
     std::vector<uint32_t> tile_edge_beg(T + 1, 0);
     std::vector<uint16_t> warp_edge(T * (kTileWarps + 1), 0);
@@ -308,7 +392,7 @@ int build_network(const BncBionData& aos, const Stimuli& stim, NetDev* dev, NetH
     {
         std::vector<std::vector<uint32_t>> per_tile_warp((size_t)T * kTileWarps);
         for (uint32_t c : conn_ok) {
-            uint32_t da = host->inv[aos.connections[c].segment_a];
+            uint32_t da = host->inv[hn.conn[c].segment_a];
             uint32_t t = tile_of[da];
             uint32_t la = da - tile_seg_beg[t];
             int w = 0;
@@ -332,14 +416,14 @@ int build_network(const BncBionData& aos, const Stimuli& stim, NetDev* dev, NetH
     std::vector<uint8_t> e_intra(E);
     std::vector<float> e_area(E), e_dist(E);
     for (uint32_t e = 0; e < E; e++) {
-        const auto& cn = aos.connections[edge_conn[e]];
+        const auto& cn = hn.conn[edge_conn[e]];
         uint32_t da = host->inv[cn.segment_a], db = host->inv[cn.segment_b];
         uint32_t t = tile_of[da];
         e_a[e] = (uint16_t)(da - tile_seg_beg[t]);
         e_b[e] = (uint16_t)(db - tile_seg_beg[t]);
         e_intra[e] = cn.is_intracellular;
-        const BncSegment& A = S[cn.segment_a];
-        const BncSegment& B = S[cn.segment_b];
+        const SegLite& A = S[cn.segment_a];
+        const SegLite& B = S[cn.segment_b];
         float r_min = A.radius < B.radius ? A.radius : B.radius;
         float area_conn = 3.14159265f * r_min * r_min;
         if (area_conn < 1e-6f) area_conn = 1e-6f;
@@ -348,10 +432,11 @@ int build_network(const BncBionData& aos, const Stimuli& stim, NetDev* dev, NetH
         e_area[e] = area_conn;
         e_dist[e] = dist;
     }
+    lap("edges");
     // incidence lists per device segment: original connection order, a-role before b-role
     std::vector<uint32_t> inc_off(n + 1, 0);
     for (uint32_t e = 0; e < E; e++) {
-        const auto& cn = aos.connections[edge_conn[e]];
+        const auto& cn = hn.conn[edge_conn[e]];
         inc_off[host->inv[cn.segment_a] + 1]++;
         inc_off[host->inv[cn.segment_b] + 1]++;
     }
@@ -364,7 +449,7 @@ int build_network(const BncBionData& aos, const Stimuli& stim, NetDev* dev, NetH
         std::vector<std::pair<uint32_t, uint16_t>> tmp;
         std::vector<uint64_t> key(inc_off[n]);
         for (uint32_t e = 0; e < E; e++) {
-            const auto& cn = aos.connections[edge_conn[e]];
+            const auto& cn = hn.conn[edge_conn[e]];
             uint32_t t = tile_of[host->inv[cn.segment_a]];
             uint16_t le = (uint16_t)(e - tile_edge_beg[t]);
             uint32_t da = host->inv[cn.segment_a], db = host->inv[cn.segment_b];
@@ -387,6 +472,7 @@ int build_network(const BncBionData& aos, const Stimuli& stim, NetDev* dev, NetH
             std::copy(tmpi.begin(), tmpi.end(), inc.begin() + b);
         }
     }
+    lap("incidence");
     // ---- phase schedule (greedy shortest common supersequence over active types) ----
     std::vector<uint32_t> act_off(n + 1, 0);   // per original segment active slot list
     std::vector<uint8_t> act_slot;
@@ -394,15 +480,15 @@ int build_network(const BncBionData& aos, const Stimuli& stim, NetDev* dev, NetH
     std::vector<uint8_t> sflags(n, 0);
     uint32_t max_active = 0;
     for (uint32_t i = 0; i < n; i++) {
-        const BncSegment& s = S[i];
+        const SegLite& s = S[i];
         bool myel = false, nmda = false;
         for (uint8_t j = 0; j < s.modifier_count; j++) {
-            if (s.modifiers[j].type == BNC_MOD_MYELIN) myel = true;
-            if (s.modifiers[j].type == BNC_MOD_NMDA) nmda = true;
+            if (hn.mod(i, j).type == BNC_MOD_MYELIN) myel = true;
+            if (hn.mod(i, j).type == BNC_MOD_NMDA) nmda = true;
         }
         uint32_t c = 0;
         for (uint8_t j = 0; j < s.modifier_count; j++) {
-            uint8_t t = s.modifiers[j].type;
+            uint8_t t = hn.mod(i, j).type;
             if (myel && t != BNC_MOD_MYELIN && is_myelin_blocked(t)) continue;  // simulation_host.cpp:241
             if (t == BNC_MOD_MYELIN) continue;  // myelin_modulator returns 0 and touches nothing
             act_slot.push_back(j);
@@ -413,10 +499,13 @@ int build_network(const BncBionData& aos, const Stimuli& stim, NetDev* dev, NetH
         sflags[i] = (uint8_t)((myel ? SF_MYELIN : 0) | (nmda ? SF_NMDA : 0));
     }
     std::vector<uint16_t> item_phase(act_slot.size(), 0);
+    std::vector<uint8_t> act_type(act_slot.size());
+    for (uint32_t i = 0; i < n; i++)
+        for (uint32_t k = act_off[i]; k < act_off[i + 1]; k++) act_type[k] = hn.mod(i, act_slot[k]).type;
     uint32_t n_phases = 0;
     {
         std::vector<uint32_t> ptr(n, 0);
-        uint32_t remaining = (uint32_t)act_slot.size();
+        uint64_t remaining = act_slot.size();
         std::vector<uint64_t> count(256);
         const uint32_t cap = std::max<uint32_t>(2 * max_active + 4, 8);
         bool greedy_ok = true;
@@ -424,12 +513,12 @@ int build_network(const BncBionData& aos, const Stimuli& stim, NetDev* dev, NetH
             std::fill(count.begin(), count.end(), 0);
             for (uint32_t i = 0; i < n; i++) {
                 uint32_t k = act_off[i] + ptr[i];
-                if (k < act_off[i + 1]) count[S[i].modifiers[act_slot[k]].type]++;
+                if (k < act_off[i + 1]) count[act_type[k]]++;
             }
             int best = (int)(std::max_element(count.begin(), count.end()) - count.begin());
             for (uint32_t i = 0; i < n; i++) {
                 uint32_t k = act_off[i] + ptr[i];
-                if (k < act_off[i + 1] && S[i].modifiers[act_slot[k]].type == best) {
+                if (k < act_off[i + 1] && act_type[k] == best) {
                     item_phase[k] = (uint16_t)n_phases;
                     ptr[i]++;
                     remaining--;
@@ -445,20 +534,44 @@ int build_network(const BncBionData& aos, const Stimuli& stim, NetDev* dev, NetH
         }
     }
     if (n_phases == 0) n_phases = 1;
-    // ---- items sorted by (tile, phase, type, device segment) ----
+    lap("phase schedule");
+    // ---- items ordered by (tile, phase, type, device segment): two counting passes ----
     struct ItemKey { uint32_t tile; uint16_t phase; uint8_t type; uint32_t dseg; uint32_t k; };
-    std::vector<ItemKey> keys(act_slot.size());
-    for (uint32_t i = 0; i < n; i++) {
-        uint32_t d = host->inv[i];
-        for (uint32_t k = act_off[i]; k < act_off[i + 1]; k++)
-            keys[k] = {tile_of[d], item_phase[k], S[i].modifiers[act_slot[k]].type, d, k};
+    const size_t NB = (size_t)T * n_phases;
+    std::vector<uint32_t> bucket_off(NB + 1, 0);
+    for (uint32_t d = 0; d < n; d++) {
+        uint32_t i = host->perm[d];
+        for (uint32_t k = act_off[i]; k < act_off[i + 1]; k++) bucket_off[(size_t)tile_of[d] * n_phases + item_phase[k] + 1]++;
     }
-    std::sort(keys.begin(), keys.end(), [](const ItemKey& x, const ItemKey& y) {
-        if (x.tile != y.tile) return x.tile < y.tile;
-        if (x.phase != y.phase) return x.phase < y.phase;
-        if (x.type != y.type) return x.type < y.type;
-        return x.dseg < y.dseg;
-    });
+    for (size_t b = 0; b < NB; b++) bucket_off[b + 1] += bucket_off[b];
+    std::vector<ItemKey> keys(act_slot.size());
+    {
+        std::vector<uint32_t> pos(bucket_off.begin(), bucket_off.end() - 1);
+        for (uint32_t d = 0; d < n; d++) {   // device order: each bucket fills in segment order
+            uint32_t i = host->perm[d];
+            for (uint32_t k = act_off[i]; k < act_off[i + 1]; k++) {
+                size_t b = (size_t)tile_of[d] * n_phases + item_phase[k];
+                keys[pos[b]++] = {tile_of[d], item_phase[k], act_type[k], d, k};
+            }
+        }
+        std::vector<ItemKey> tmp;
+        uint32_t tc[257];
+        for (size_t b = 0; b < NB; b++) {   // stable counting sort by type inside each bucket
+            uint32_t lo = bucket_off[b], hi = bucket_off[b + 1];
+            if (hi - lo < 2) continue;
+            std::fill(tc, tc + 257, 0u);
+            bool sorted = true;
+            for (uint32_t q = lo; q < hi; q++) {
+                tc[keys[q].type + 1]++;
+                if (q > lo && keys[q].type < keys[q - 1].type) sorted = false;
+            }
+            if (sorted) continue;
+            for (int t = 0; t < 256; t++) tc[t + 1] += tc[t];
+            tmp.assign(keys.begin() + lo, keys.begin() + hi);
+            for (const ItemKey& kk : tmp) keys[lo + tc[kk.type]++] = kk;
+        }
+    }
+    lap("item sort");
     const uint32_t NI = (uint32_t)keys.size();
     std::vector<uint32_t> it_meta(NI);
     std::vector<float> it_den(NI), it_st((size_t)7 * NI);
@@ -479,21 +592,22 @@ int build_network(const BncBionData& aos, const Stimuli& stim, NetDev* dev, NetH
         const ItemKey& kk = keys[q];
         uint32_t orig = host->perm[kk.dseg];
         uint8_t slot = act_slot[kk.k];
-        const BncModifier& m = S[orig].modifiers[slot];
+        const ModLite& m = hn.mod(orig, slot);
         uint8_t fl = 0;
         uint8_t pm = param_mask(m.type);
-        for (int b = 0; b < 7; b++) if ((pm >> b) & 1) if (m.state[b] != 0.0) fl |= 1;
+        for (int b = 0; b < 7; b++) if ((pm >> b) & 1) if (m.state[b] != 0.0f) fl |= 1;
         if (receptor_supported(m.type) && m.active_vars > 0) {
             if (m.active_vars >= 8) { set_error("segment %u slot %u: active_vars %u out of range", orig, slot, m.active_vars); return BNC_ERR_FORMAT; }
             fl |= (uint8_t)(2u | ((uint32_t)m.active_vars << 2));
         }
         uint32_t local = kk.dseg - tile_seg_beg[kk.tile];
         it_meta[q] = local | ((uint32_t)m.type << 16) | ((uint32_t)fl << 24);
-        it_den[q] = (float)m.density;
-        for (int b = 0; b < 7; b++) it_st[(size_t)b * NI + q] = (float)m.state[b];
+        it_den[q] = m.density;
+        for (int b = 0; b < 7; b++) it_st[(size_t)b * NI + q] = m.state[b];
         host->item_seg[q] = orig;
         host->item_slot[q] = slot;
     }
+    lap("items");
     // ---- per-segment state and statics in device order ----
     std::vector<float> V(n), ion_in((size_t)7 * n), ion_out((size_t)7 * n), intra_nt((size_t)15 * n),
         nt((size_t)15 * n), atp(n), temp(n), txn(n), radius(n), length(n), area(n), cm(n);
@@ -502,11 +616,11 @@ int build_network(const BncBionData& aos, const Stimuli& stim, NetDev* dev, NetH
     std::vector<float2> c21(n);
     bool intra_nt_grad = false, temp_grad = false, txn_grad = false;
     for (uint32_t d = 0; d < n; d++) {
-        const BncSegment& s = S[host->perm[d]];
-        V[d] = (float)s.V_m;
+        const SegLite& s = S[host->perm[d]];
+        V[d] = s.V_m;
         for (int q = 0; q < 7; q++) {
-            ion_in[(size_t)q * n + d] = (float)s.intra_ions[q];
-            ion_out[(size_t)q * n + d] = (float)s.extra_ions[q];
+            ion_in[(size_t)q * n + d] = s.intra_ions[q];
+            ion_out[(size_t)q * n + d] = s.extra_ions[q];
         }
         for (int q = 0; q < 15; q++) {
             intra_nt[(size_t)q * n + d] = s.intra_nt[q];
@@ -514,30 +628,31 @@ int build_network(const BncBionData& aos, const Stimuli& stim, NetDev* dev, NetH
         }
         atp[d] = s.ATP_level; temp[d] = s.temperature; txn[d] = s.transcription_signal;
         radius[d] = s.radius; length[d] = s.length; stype[d] = s.segment_type;
-        area[d] = seg_area(s); vol[d] = seg_volume(s); cm[d] = seg_capacitance(s);
+        area[d] = seg_area(s); vol[d] = seg_volume(s); cm[d] = seg_capacitance(hn, host->perm[d]);
         ibuf[d] = s.I_buffer;
         dflags[d] = sflags[host->perm[d]];
         c21[d] = make_float2(0.0f, 0.0f);
         for (uint8_t j = 0; j < s.modifier_count; j++)
-            if (s.modifiers[j].type == BNC_MOD_CAV21)
-                c21[d] = make_float2((float)s.modifiers[j].density, (float)s.modifiers[j].state[1]);
+            if (hn.mod(host->perm[d], j).type == BNC_MOD_CAV21)
+                c21[d] = make_float2(hn.mod(host->perm[d], j).density, hn.mod(host->perm[d], j).state[1]);
     }
     for (uint32_t c : conn_ok) {
-        const auto& cn = aos.connections[c];
-        const BncSegment& A = S[cn.segment_a];
-        const BncSegment& B = S[cn.segment_b];
+        const auto& cn = hn.conn[c];
+        const SegLite& A = S[cn.segment_a];
+        const SegLite& B = S[cn.segment_b];
         if (cn.is_intracellular) {
             for (int q = 0; q < 15; q++) if (A.intra_nt[q] != B.intra_nt[q]) intra_nt_grad = true;
             if (A.temperature != B.temperature) temp_grad = true;
             if (A.transcription_signal != B.transcription_signal) txn_grad = true;
         }
     }
+    lap("segment state");
     // ---- synapses: valid chemical ones in post-segment CSR order ----
     std::vector<uint32_t> syn_valid;
     bool need_pre_ext = false, any_delay = false;
     uint32_t nt_mask = 0;
     for (uint32_t k = 0; k < aos.num_synapses; k++) {
-        const BncSynapse& y = aos.synapses[k];
+        const SynLite& y = hn.syn[k];
         if (y.pre_segment >= n || y.post_segment >= n) continue;   // simulation_host.cpp:362
         if (y.type != BNC_SYN_CHEMICAL) {
             set_error("synapse %u: electrical synapses have no device implementation in this backend", k);
@@ -547,18 +662,18 @@ int build_network(const BncBionData& aos, const Stimuli& stim, NetDev* dev, NetH
             set_error("synapse %u: receptor count out of range", k); return BNC_ERR_FORMAT;
         }
         for (uint8_t j = 0; j < y.post_receptor_count; j++)
-            if (!receptor_supported(y.post_receptors[j].type)) {
+            if (!receptor_supported(hn.post_rec(k, j).type)) {
                 set_error("synapse %u receptor %u: type %u has no device implementation as a receptor", k, j,
-                          y.post_receptors[j].type);
+                          hn.post_rec(k, j).type);
                 return BNC_ERR_UNSUPPORTED;
             }
         for (uint8_t j = 0; j < y.pre_autoreceptor_count; j++)
-            if (bouton_gamma(y.pre_autoreceptors[j].type) == 0.0f) {
+            if (bouton_gamma(hn.pre_ar(k, j).type) == 0.0f) {
                 set_error("synapse %u autoreceptor %u: type %u (release modulators are not supported)", k, j,
-                          y.pre_autoreceptors[j].type);
+                          hn.pre_ar(k, j).type);
                 return BNC_ERR_UNSUPPORTED;
             }
-        uint8_t ntt = y.post_receptor_count > 0 ? nt_from_receptor(y.post_receptors[0].type) : 0;
+        uint8_t ntt = y.post_receptor_count > 0 ? nt_from_receptor(hn.post_rec(k, 0).type) : 0;
         for (int q = 0; q < 15; q++)
             if (q != ntt && y.cleft_neurotransmitter[q] != 0.0f) {
                 set_error("synapse %u: cleft holds neurotransmitter %d other than the one it releases", k, q);
@@ -569,13 +684,16 @@ int build_network(const BncBionData& aos, const Stimuli& stim, NetDev* dev, NetH
         nt_mask |= 1u << ntt;
         syn_valid.push_back(k);
     }
-    std::stable_sort(syn_valid.begin(), syn_valid.end(), [&](uint32_t x, uint32_t y) {
-        return host->inv[aos.synapses[x].post_segment] < host->inv[aos.synapses[y].post_segment];
-    });
     const uint32_t K = (uint32_t)syn_valid.size();
     std::vector<uint32_t> post_off(n + 1, 0);
-    for (uint32_t k : syn_valid) post_off[host->inv[aos.synapses[k].post_segment] + 1]++;
+    for (uint32_t k : syn_valid) post_off[host->inv[hn.syn[k].post_segment] + 1]++;
     for (uint32_t i = 0; i < n; i++) post_off[i + 1] += post_off[i];
+    {   // stable counting sort by postsynaptic device segment (original order within a post)
+        std::vector<uint32_t> pos(post_off.begin(), post_off.end() - 1);
+        std::vector<uint32_t> sorted(K);
+        for (uint32_t k : syn_valid) sorted[pos[host->inv[hn.syn[k].post_segment]]++] = k;
+        syn_valid.swap(sorted);
+    }
     std::vector<uint32_t> sy_pre(K), sy_id(K), rc_off(K + 1, 0);
     std::vector<float> sy_prel(K), sy_amt(K), sy_tauc(K), sy_delay(K), sy_prea(K), sy_posta(K), sy_gK(K),
         sy_gNa(K), sy_bouton(K), sy_spine(K), sy_camkii(K), sy_calcn(K), sy_facil(K), sy_weight(K), sy_cleft(K),
@@ -587,23 +705,23 @@ int build_network(const BncBionData& aos, const Stimuli& stim, NetDev* dev, NetH
     host->rec_syn.clear(); host->rec_slot.clear();
     host->syn_nt.assign(K, 0);
     for (uint32_t q = 0; q < K; q++) {
-        const BncSynapse& y = aos.synapses[syn_valid[q]];
+        const SynLite& y = hn.syn[syn_valid[q]];
         sy_pre[q] = host->inv[y.pre_segment];
         sy_id[q] = y.id;
         sy_prel[q] = y.release_probability; sy_amt[q] = y.release_amount; sy_tauc[q] = y.tau_clearance;
         sy_delay[q] = y.delay; sy_prea[q] = y.pre_area; sy_posta[q] = y.post_area;
         float gK = 0.0f, gNa = 0.0f;
         for (uint8_t j = 0; j < y.pre_autoreceptor_count; j++) {   // modifier_helpers.h:767-773
-            uint8_t t = y.pre_autoreceptors[j].type;
-            float g = (float)(y.pre_autoreceptors[j].density * bouton_gamma(t));
+            uint8_t t = hn.pre_ar(syn_valid[q], j).type;
+            float g = (float)((double)hn.pre_ar(syn_valid[q], j).density * bouton_gamma(t));
             if (t == 141 || t == 142) gNa += g; else gK += g;
         }
         sy_gK[q] = gK; sy_gNa[q] = gNa;
         sy_refr[q] = y.refractory;
-        uint8_t ntt = y.post_receptor_count > 0 ? nt_from_receptor(y.post_receptors[0].type) : 0;
+        uint8_t ntt = y.post_receptor_count > 0 ? nt_from_receptor(hn.post_rec(syn_valid[q], 0).type) : 0;
         bool inhib = false;
         for (uint8_t j = 0; j < y.post_receptor_count; j++) {
-            uint8_t rt = y.post_receptors[j].type;
+            uint8_t rt = hn.post_rec(syn_valid[q], j).type;
             if (rt == 11 || rt == 17 || rt == 12) { inhib = true; break; }
         }
         sy_flags[q] = (uint8_t)((inhib ? 1u : 0u) | ((uint32_t)ntt << 4));
@@ -614,15 +732,15 @@ int build_network(const BncBionData& aos, const Stimuli& stim, NetDev* dev, NetH
         sy_rrp[q] = y.RRP; sy_rrpm[q] = y.RRP_max; sy_rrpr[q] = y.RRP_recovery;
         bool myel_post = (sflags[y.post_segment] & SF_MYELIN) != 0;
         for (uint8_t j = 0; j < y.post_receptor_count; j++) {
-            const BncModifier& r = y.post_receptors[j];
+            const ModLite& r = hn.post_rec(syn_valid[q], j);
             if (myel_post && is_ionotropic(r.type)) continue;   // simulation_host.cpp:495
             if (r.active_vars >= 8) { set_error("synapse %u receptor %u: active_vars out of range", syn_valid[q], j); return BNC_ERR_FORMAT; }
             rc_type.push_back(r.type);
             rc_av.push_back(r.active_vars);
-            rc_den.push_back((float)r.density);
-            rc_st0.push_back((float)r.state[0]);
-            rc_st1.push_back((float)r.state[1]);
-            rc_st2.push_back((float)r.state[2]);
+            rc_den.push_back(r.density);
+            rc_st0.push_back(r.state[0]);
+            rc_st1.push_back(r.state[1]);
+            rc_st2.push_back(r.state[2]);
             if (r.active_vars >= 3 && r.active_vars <= 6) {
                 set_error("synapse %u receptor %u: active_vars %u not supported", syn_valid[q], j, r.active_vars);
                 return BNC_ERR_UNSUPPORTED;
@@ -632,12 +750,14 @@ int build_network(const BncBionData& aos, const Stimuli& stim, NetDev* dev, NetH
         }
         rc_off[q + 1] = (uint32_t)rc_type.size();
     }
+    lap("synapses");
     const uint32_t NR = (uint32_t)rc_type.size();
     std::vector<float> rc_st((size_t)3 * NR);
     for (uint32_t r = 0; r < NR; r++) {
         rc_st[r] = rc_st0[r]; rc_st[(size_t)NR + r] = rc_st1[r]; rc_st[(size_t)2 * NR + r] = rc_st2[r];
     }
-    // ---- upload ----
+    lap("receptors");
+    // ---- upload (skipped for a host-only plan) ----
     int rc = BNC_OK;
     dev->n_seg = n; dev->n_tiles = T; dev->n_items = NI; dev->n_phases = n_phases;
     dev->n_syn = K; dev->n_rec = NR; dev->n_edges = E;
@@ -654,81 +774,84 @@ int build_network(const BncBionData& aos, const Stimuli& stim, NetDev* dev, NetH
     bool any_nmda = false;
     for (uint32_t i = 0; i < n; i++) if (sflags[i] & SF_NMDA) any_nmda = true;
     dev->nt_used_mask = nt_mask | (any_nmda ? 1u : 0u);
-    dev->V = up(allocs, V, &rc);
-    dev->ion_in = up(allocs, ion_in, &rc);
-    dev->ion_out = up(allocs, ion_out, &rc);
-    dev->intra_nt = up(allocs, intra_nt, &rc);
-    dev->nt = up(allocs, nt, &rc);
-    dev->atp = up(allocs, atp, &rc);
-    dev->temp = up(allocs, temp, &rc);
-    dev->txn = up(allocs, txn, &rc);
-    dev->ibuf = up(allocs, ibuf, &rc);
-    dev->radius = up(allocs, radius, &rc);
-    dev->length = up(allocs, length, &rc);
-    dev->area = up(allocs, area, &rc);
-    dev->vol = up(allocs, vol, &rc);
-    dev->cm = up(allocs, cm, &rc);
-    dev->stype = up(allocs, stype, &rc);
-    dev->sflags = up(allocs, dflags, &rc);
-    dev->cav21_static = up(allocs, c21, &rc);
-    dev->pre_rec = zeros<float4>(allocs, n, &rc);
-    if (need_pre_ext) {
-        dev->pre_ext = zeros<float4>(allocs, n, &rc);
-        dev->pre_ext2 = zeros<float>(allocs, n, &rc);
+    if (allocs) {
+        dev->V = up(allocs, V, &rc);
+        dev->ion_in = up(allocs, ion_in, &rc);
+        dev->ion_out = up(allocs, ion_out, &rc);
+        dev->intra_nt = up(allocs, intra_nt, &rc);
+        dev->nt = up(allocs, nt, &rc);
+        dev->atp = up(allocs, atp, &rc);
+        dev->temp = up(allocs, temp, &rc);
+        dev->txn = up(allocs, txn, &rc);
+        dev->ibuf = up(allocs, ibuf, &rc);
+        dev->radius = up(allocs, radius, &rc);
+        dev->length = up(allocs, length, &rc);
+        dev->area = up(allocs, area, &rc);
+        dev->vol = up(allocs, vol, &rc);
+        dev->cm = up(allocs, cm, &rc);
+        dev->stype = up(allocs, stype, &rc);
+        dev->sflags = up(allocs, dflags, &rc);
+        dev->cav21_static = up(allocs, c21, &rc);
+        dev->pre_rec = zeros<float4>(allocs, n, &rc);
+        if (need_pre_ext) {
+            dev->pre_ext = zeros<float4>(allocs, n, &rc);
+            dev->pre_ext2 = zeros<float>(allocs, n, &rc);
+        }
+        dev->tile_seg_beg = up(allocs, tile_seg_beg, &rc);
+        dev->tile_edge_beg = up(allocs, tile_edge_beg, &rc);
+        dev->phase_off = up(allocs, phase_off, &rc);
+        dev->warp_seg = up(allocs, warp_seg, &rc);
+        dev->warp_edge = up(allocs, warp_edge, &rc);
+        dev->e_a = up(allocs, e_a, &rc);
+        dev->e_b = up(allocs, e_b, &rc);
+        dev->e_intra = up(allocs, e_intra, &rc);
+        dev->e_area = up(allocs, e_area, &rc);
+        dev->e_dist = up(allocs, e_dist, &rc);
+        dev->inc_off = up(allocs, inc_off, &rc);
+        dev->inc = up(allocs, inc, &rc);
+        dev->it_meta = up(allocs, it_meta, &rc);
+        dev->it_den = up(allocs, it_den, &rc);
+        dev->it_st = up(allocs, it_st, &rc);
+        dev->post_off = up(allocs, post_off, &rc);
+        dev->sy_pre = up(allocs, sy_pre, &rc);
+        dev->sy_id = up(allocs, sy_id, &rc);
+        dev->sy_prel = up(allocs, sy_prel, &rc);
+        dev->sy_amt = up(allocs, sy_amt, &rc);
+        dev->sy_tauc = up(allocs, sy_tauc, &rc);
+        dev->sy_delay = up(allocs, sy_delay, &rc);
+        dev->sy_pre_area = up(allocs, sy_prea, &rc);
+        dev->sy_post_area = up(allocs, sy_posta, &rc);
+        dev->sy_gK = up(allocs, sy_gK, &rc);
+        dev->sy_gNa = up(allocs, sy_gNa, &rc);
+        dev->sy_refr = up(allocs, sy_refr, &rc);
+        dev->sy_flags = up(allocs, sy_flags, &rc);
+        dev->sy_bouton = up(allocs, sy_bouton, &rc);
+        dev->sy_spine = up(allocs, sy_spine, &rc);
+        dev->sy_camkii = up(allocs, sy_camkii, &rc);
+        dev->sy_calcn = up(allocs, sy_calcn, &rc);
+        dev->sy_facil = up(allocs, sy_facil, &rc);
+        dev->sy_weight = up(allocs, sy_weight, &rc);
+        dev->sy_cleft = up(allocs, sy_cleft, &rc);
+        dev->sy_rrp = up(allocs, sy_rrp, &rc);
+        dev->sy_rrp_max = up(allocs, sy_rrpm, &rc);
+        dev->sy_rrp_rec = up(allocs, sy_rrpr, &rc);
+        dev->sy_scale = up(allocs, sy_scale, &rc);
+        dev->rc_off = up(allocs, rc_off, &rc);
+        dev->rc_type = up(allocs, rc_type, &rc);
+        dev->rc_av = up(allocs, rc_av, &rc);
+        dev->rc_den = up(allocs, rc_den, &rc);
+        dev->rc_st = up(allocs, rc_st, &rc);
+        if (any_delay) {
+            dev->dl_arr = zeros<unsigned long long>(allocs, (size_t)4 * K, &rc);
+            dev->dl_amt = zeros<float>(allocs, (size_t)4 * K, &rc);
+            dev->dl_nt = zeros<uint8_t>(allocs, (size_t)4 * K, &rc);
+        }
+        dev->spike_count = zeros<uint32_t>(allocs, n, &rc);
+        dev->err_flag = zeros<int>(allocs, 1, &rc);
+        if (rc == BNC_OK) rc = upload_stimuli(stim, *host, dev, allocs);
+        if (rc != BNC_OK) { set_error("device allocation/upload failed (%d)", rc); return rc; }
     }
-    dev->tile_seg_beg = up(allocs, tile_seg_beg, &rc);
-    dev->tile_edge_beg = up(allocs, tile_edge_beg, &rc);
-    dev->phase_off = up(allocs, phase_off, &rc);
-    dev->warp_seg = up(allocs, warp_seg, &rc);
-    dev->warp_edge = up(allocs, warp_edge, &rc);
-    dev->e_a = up(allocs, e_a, &rc);
-    dev->e_b = up(allocs, e_b, &rc);
-    dev->e_intra = up(allocs, e_intra, &rc);
-    dev->e_area = up(allocs, e_area, &rc);
-    dev->e_dist = up(allocs, e_dist, &rc);
-    dev->inc_off = up(allocs, inc_off, &rc);
-    dev->inc = up(allocs, inc, &rc);
-    dev->it_meta = up(allocs, it_meta, &rc);
-    dev->it_den = up(allocs, it_den, &rc);
-    dev->it_st = up(allocs, it_st, &rc);
-    dev->post_off = up(allocs, post_off, &rc);
-    dev->sy_pre = up(allocs, sy_pre, &rc);
-    dev->sy_id = up(allocs, sy_id, &rc);
-    dev->sy_prel = up(allocs, sy_prel, &rc);
-    dev->sy_amt = up(allocs, sy_amt, &rc);
-    dev->sy_tauc = up(allocs, sy_tauc, &rc);
-    dev->sy_delay = up(allocs, sy_delay, &rc);
-    dev->sy_pre_area = up(allocs, sy_prea, &rc);
-    dev->sy_post_area = up(allocs, sy_posta, &rc);
-    dev->sy_gK = up(allocs, sy_gK, &rc);
-    dev->sy_gNa = up(allocs, sy_gNa, &rc);
-    dev->sy_refr = up(allocs, sy_refr, &rc);
-    dev->sy_flags = up(allocs, sy_flags, &rc);
-    dev->sy_bouton = up(allocs, sy_bouton, &rc);
-    dev->sy_spine = up(allocs, sy_spine, &rc);
-    dev->sy_camkii = up(allocs, sy_camkii, &rc);
-    dev->sy_calcn = up(allocs, sy_calcn, &rc);
-    dev->sy_facil = up(allocs, sy_facil, &rc);
-    dev->sy_weight = up(allocs, sy_weight, &rc);
-    dev->sy_cleft = up(allocs, sy_cleft, &rc);
-    dev->sy_rrp = up(allocs, sy_rrp, &rc);
-    dev->sy_rrp_max = up(allocs, sy_rrpm, &rc);
-    dev->sy_rrp_rec = up(allocs, sy_rrpr, &rc);
-    dev->sy_scale = up(allocs, sy_scale, &rc);
-    dev->rc_off = up(allocs, rc_off, &rc);
-    dev->rc_type = up(allocs, rc_type, &rc);
-    dev->rc_av = up(allocs, rc_av, &rc);
-    dev->rc_den = up(allocs, rc_den, &rc);
-    dev->rc_st = up(allocs, rc_st, &rc);
-    if (any_delay) {
-        dev->dl_arr = zeros<unsigned long long>(allocs, (size_t)4 * K, &rc);
-        dev->dl_amt = zeros<float>(allocs, (size_t)4 * K, &rc);
-        dev->dl_nt = zeros<uint8_t>(allocs, (size_t)4 * K, &rc);
-    }
-    dev->spike_count = zeros<uint32_t>(allocs, n, &rc);
-    dev->err_flag = zeros<int>(allocs, 1, &rc);
-    if (rc == BNC_OK) rc = upload_stimuli(stim, *host, dev, allocs);
-    if (rc != BNC_OK) { set_error("device allocation/upload failed (%d)", rc); return rc; }
+    lap("upload");
     // tile sizes for the shared-memory plan
     uint32_t mts = 0, mte = 0;
     for (uint32_t t = 0; t < T; t++) {
@@ -772,6 +895,8 @@ int build_network(const BncBionData& aos, const Stimuli& stim, NetDev* dev, NetH
         for (uint32_t r = 0; r < NR; r++) rec += 1 + 4 + 8.0 * (rc_type[r] == 9 ? 2 : 2);
         host->seg_bytes = (seg_a + seg_b) * n + items;
         host->syn_bytes = syn * K + rec + 4.0 * (K + 1);
+        host->tile_bytes = seg_a * n + items;
+        host->synk_bytes = seg_b * n + host->syn_bytes;
         host->algo_bytes_per_tick = host->seg_bytes + host->syn_bytes;
     }
     return BNC_OK;

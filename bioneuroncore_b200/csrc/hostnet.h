@@ -1,0 +1,63 @@
+// hostnet.h -- compact host-side network, the builder's input.
+//
+// The reference's AoS records reserve room for 32 modifiers per segment and 8+8
+// receptors per synapse (3216 B and 1568 B).  A 6.4M-segment, 10M-synapse network
+// would need 36 GB of host memory in that layout; these records keep only the
+// occupied modifier/receptor slots, with state in the precision the device keeps.
+// Filled from AoS arrays (drop-in loads) or directly by the generator.
+#pragma once
+#include <cstdint>
+#include <vector>
+#include "common.h"
+
+namespace bnc {
+
+struct ModLite {
+    uint8_t type;
+    uint8_t active_vars;
+    float density;
+    float state[8];
+};
+
+struct SegLite {
+    uint32_t id;
+    uint8_t segment_type;
+    uint8_t modifier_count;
+    float radius, length;
+    float V_m;
+    float intra_ions[7], extra_ions[7];
+    float intra_nt[15], neurotransmitter[15];
+    float ATP_level, temperature, transcription_signal;
+    double I_buffer;
+    uint64_t mod_off;
+};
+
+struct SynLite {
+    uint32_t id, pre_segment, post_segment;
+    uint8_t type, pre_autoreceptor_count, post_receptor_count, refractory;
+    float weight, delay, pre_area, post_area, release_probability, release_amount, tau_clearance;
+    float facilitation, depression, RRP, RRP_max, RRP_recovery;
+    float bouton_Ca, spine_Ca, spine_camkii, spine_calcineurin;
+    float cleft_neurotransmitter[15];
+    uint64_t rec_off;   // post receptors, then pre autoreceptors, in HostNet::recs
+};
+
+struct HostNet {
+    uint32_t num_segments = 0, num_connections = 0, num_synapses = 0;
+    std::vector<SegLite> seg;
+    std::vector<ModLite> mods;
+    std::vector<BncIntraConnection> conn;
+    std::vector<SynLite> syn;
+    std::vector<ModLite> recs;
+    const ModLite& mod(uint32_t i, uint32_t j) const { return mods[seg[i].mod_off + j]; }
+    const ModLite& post_rec(uint32_t k, uint32_t j) const { return recs[syn[k].rec_off + j]; }
+    const ModLite& pre_ar(uint32_t k, uint32_t j) const {
+        return recs[syn[k].rec_off + syn[k].post_receptor_count + j];
+    }
+};
+
+void hostnet_add_segment(HostNet& hn, const BncSegment& s);
+void hostnet_add_synapse(HostNet& hn, const BncSynapse& y);
+void hostnet_from_aos(const BncBionData& aos, HostNet* hn);
+
+}  // namespace bnc

@@ -783,7 +783,7 @@ static cudaError_t init_tables(cudaStream_t stream) {
     return e;
 }
 
-cudaError_t launch_tick(const NetDev& dev, const NetHost& host, float dt, unsigned long long tick, int first_tick,
+cudaError_t launch_tile(const NetDev& dev, const NetHost& host, float dt, unsigned long long tick,
                         cudaStream_t stream) {
     cudaError_t e = init_tables(stream);
     if (e != cudaSuccess) return e;
@@ -794,10 +794,20 @@ cudaError_t launch_tick(const NetDev& dev, const NetHost& host, float dt, unsign
         if (e != cudaSuccess) return e;
     }
     k_tile<<<dev.n_tiles, kTileThreads, smem, stream>>>(dev, dt, tick, S, E);
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_synapse(const NetDev& dev, float dt, unsigned long long tick, int first_tick,
+                           cudaStream_t stream) {
     k_synapse<<<(dev.n_seg + 255) / 256, 256, 0, stream>>>(dev, dt, tick, first_tick);
     return cudaGetLastError();
+}
+
+cudaError_t launch_tick(const NetDev& dev, const NetHost& host, float dt, unsigned long long tick, int first_tick,
+                        cudaStream_t stream) {
+    cudaError_t e = launch_tile(dev, host, dt, tick, stream);
+    if (e != cudaSuccess) return e;
+    return launch_synapse(dev, dt, tick, first_tick, stream);
 }
 
 }  // namespace bnc

@@ -135,8 +135,11 @@ struct NetHost {
     std::vector<uint8_t> syn_nt;     // released NT per device synapse
     uint32_t max_tile_segs = 0, max_tile_edges = 0;
     size_t smem_bytes = 0;
-    double algo_bytes_per_tick = 0;  // algorithmic HBM bytes per tick (see bytes_model)
-    double seg_bytes = 0, syn_bytes = 0;
+    double algo_bytes_per_tick = 0;  // algorithmic HBM bytes per tick of this state schema
+    double seg_bytes = 0, syn_bytes = 0;     // split by owner: segment state vs synapse state
+    double tile_bytes = 0, synk_bytes = 0;   // split by kernel: k_tile vs k_synapse
+    bool perm_identity = true;               // device segment order equals the original order
+    bool stim_identity = true;               // per-segment stimulus CSR order equals upload order
 };
 
 struct Stimuli {
@@ -153,11 +156,12 @@ struct DeviceAllocs {
     void release();
 };
 
-int build_network(const BncBionData& aos, const Stimuli& stim, NetDev* dev, NetHost* host,
+struct HostNet;
+int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* host,
                   DeviceAllocs* allocs);
 
 // Rebuilds the per-segment stimulus CSRs after an upload of new stimuli.
-int upload_stimuli(const Stimuli& stim, const NetHost& host, NetDev* dev, DeviceAllocs* allocs);
+int upload_stimuli(const Stimuli& stim, NetHost& host, NetDev* dev, DeviceAllocs* allocs);
 
 // Writes device state back into the AoS arrays.
 int export_network(const NetDev& dev, const NetHost& host, uint64_t ticks_run, BncBionData* aos);
@@ -165,6 +169,10 @@ int export_network(const NetDev& dev, const NetHost& host, uint64_t ticks_run, B
 // Kernel launchers (kernels.cu).
 cudaError_t launch_tick(const NetDev& dev, const NetHost& host, float dt, unsigned long long tick,
                         int first_tick, cudaStream_t stream);
+cudaError_t launch_tile(const NetDev& dev, const NetHost& host, float dt, unsigned long long tick,
+                        cudaStream_t stream);
+cudaError_t launch_synapse(const NetDev& dev, float dt, unsigned long long tick, int first_tick,
+                           cudaStream_t stream);
 size_t tile_smem_bytes(uint32_t max_segs, uint32_t max_edges);
 
 }  // namespace bnc

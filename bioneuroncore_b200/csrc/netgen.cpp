@@ -11,7 +11,8 @@
 //  * Small set per segment: Nav1.6 (141; Nav1.2 142 on dendrites), Kv delayed
 //    rectifier (123), K2P leak (107), Cav1.3 (1), Na/K pump (7), myelin (4) on odd
 //    axon segments.  Large set: 16 draws with replacement from 24 types with the
-//    weights in kLargeTypes, in draw order.
+//    weights in kLargeTypes, listed by type ID (BNC_NETGEN_DRAW_ORDER keeps draw order);
+//    the tick processes a segment's modifiers in slot order either way.
 //  * Synapses: presynaptic segment uniform over axon segments, postsynaptic
 //    uniform over soma+dendrite segments; 80 % AMPA / 20 % GABA-A receptor class;
 //    release probability 0.3, tau_clearance 1 ms, release_amount 1, areas 0.1 um2.
@@ -174,6 +175,7 @@ int generate_network(const BncNetgenParams& p, NetSink& sink, NetShape* shape_ou
             seg.ER_Ca2 = 0.4f;
             int mc = 0;
             if (f.large_set) {
+                int picks[16];
                 for (int d = 0; d < 16; d++) {
                     float r = (float)rng_mod.u01() * wsum;
                     int pick = 23;
@@ -181,7 +183,12 @@ int generate_network(const BncNetgenParams& p, NetSink& sink, NetShape* shape_ou
                         if (r < kLargeTypes[t].weight) { pick = t; break; }
                         r -= kLargeTypes[t].weight;
                     }
-                    const TypeSpec& ts = kLargeTypes[pick];
+                    picks[d] = pick;
+                }
+                if (!(p.flags & BNC_NETGEN_DRAW_ORDER))   // list the drawn modifiers by type ID
+                    std::sort(picks, picks + 16, [](int a, int b) { return kLargeTypes[a].type < kLargeTypes[b].type; });
+                for (int d = 0; d < 16; d++) {
+                    const TypeSpec& ts = kLargeTypes[picks[d]];
                     set_mod(seg.modifiers[mc++], ts.type, ts.density * scale_of(p, ts.cls));
                 }
             } else {

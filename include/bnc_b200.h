@@ -115,6 +115,7 @@ typedef struct {
 #define BNC_NETGEN_NO_CONNECTIONS 2u
 #define BNC_NETGEN_NO_STIMULI 4u
 #define BNC_NETGEN_PERTURB_IONS 8u
+#define BNC_NETGEN_DRAW_ORDER 16u   /* large set: keep modifiers in draw order (default: by type ID) */
 
 /* Generates a network into host AoS arrays in the reference layout.  The arrays
  * are owned by the library; release with bnc_netgen_free.  *stim receives the
@@ -138,6 +139,17 @@ int bnc_run_ticks(void* sim, uint32_t n_ticks, float dt);
  * elapsed device time. */
 int bnc_time_ticks(void* sim, uint32_t n_ticks, float dt, float* ms);
 
+/* One serving step: uploads per-stimulus amplitudes (pA, one per loaded current
+ * stimulus, host memory -- pinned for an asynchronous copy), runs one tick and
+ * copies V_m of every segment into v_out (host, original order).  Either buffer
+ * may be NULL to skip that copy. */
+int bnc_step_io(void* sim, float dt, const float* stim_amp, uint32_t n_amp, float* v_out, uint32_t n_v);
+
+/* Runs n ticks with CUDA events around each kernel; returns the summed device
+ * time of the tile kernel (modifiers + electrodiffusion) and of the synapse +
+ * membrane kernel. */
+int bnc_profile_ticks(void* sim, uint32_t n_ticks, float dt, float* ms_tile, float* ms_synapse);
+
 /* Copies device state into the host AoS view (no-op when none is held). */
 int bnc_sync_to_host(void* sim);
 
@@ -160,9 +172,14 @@ typedef struct {
     uint32_t max_tile_segs, max_tile_edges, smem_bytes, flags;
     uint64_t ticks;
     double algo_bytes_per_tick;   /* algorithmic HBM bytes one tick moves (state schema) */
-    double seg_bytes_per_tick, syn_bytes_per_tick;
+    double seg_bytes_per_tick, syn_bytes_per_tick;          /* split by state owner */
+    double tile_bytes_per_tick, synapse_kernel_bytes_per_tick; /* split by kernel */
 } BncNetInfo;
 int bnc_network_info(void* sim, BncNetInfo* info);
+
+/* Host-only: generates a network and runs the builder's planning (tiles, phase
+ * schedule, CSRs) without a device; fills `info` (no upload, no CUDA call). */
+int bnc_plan_generated(const BncNetgenParams* p, BncNetInfo* info);
 
 /* Writes the host AoS view to a .bion v14 file (reference bion_save layout). */
 int bnc_save_bion(void* sim, const char* filename);
