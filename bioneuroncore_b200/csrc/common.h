@@ -2,8 +2,8 @@
 #pragma once
 #include <cstdarg>
 #include <cstdint>
-#include "../../include/bnc_abi.h"
-#include "../../include/bnc_b200.h"
+#include "bnc_abi.h"
+#include "bnc_b200.h"
 
 namespace bnc {
 // Records the message returned by bnc_last_error() on this thread.

@@ -15,9 +15,19 @@
 #pragma once
 #include <cstdint>
 
+// Translation units whose kernels run many different channel models in one launch
+// define BNC_MATH_OUTLINE before including this header: the elementary functions are
+// then called, not inlined at every call site, which keeps the kernel's instruction
+// footprint within the instruction cache.  Results are the same either way.
+#ifdef BNC_MATH_OUTLINE
+#define BNC_MATH_FN static __device__ __noinline__
+#else
+#define BNC_MATH_FN static __device__ __forceinline__
+#endif
+
 namespace bnc {
 
-__device__ __forceinline__ double dm_scale2(double p, int k) {
+static __device__ __forceinline__ double dm_scale2(double p, int k) {
     if (k > 1023)
         return p * __longlong_as_double((long long)(1023 + 1023) << 52) *
                __longlong_as_double((long long)(k - 1023 + 1023) << 52);
@@ -26,7 +36,7 @@ __device__ __forceinline__ double dm_scale2(double p, int k) {
            __longlong_as_double((long long)(-54 + 1023) << 52);
 }
 
-__device__ __forceinline__ double dm_exp(double x) {
+BNC_MATH_FN double dm_exp(double x) {
     if (x != x) return x;
     if (x > 709.782712893384) return __longlong_as_double(0x7FF0000000000000ll);
     if (x < -745.1332191019412) return 0.0;
@@ -53,14 +63,14 @@ __device__ __forceinline__ double dm_exp(double x) {
     return dm_scale2(p, (int)kd);
 }
 
-__device__ __forceinline__ float dm_scale2f(float p, int k) {
+static __device__ __forceinline__ float dm_scale2f(float p, int k) {
     if (k > 127)
         return p * __uint_as_float((uint32_t)(127 + 127) << 23) * __uint_as_float((uint32_t)(k - 127 + 127) << 23);
     if (k >= -126) return p * __uint_as_float((uint32_t)(k + 127) << 23);
     return (p * __uint_as_float((uint32_t)(k + 25 + 127) << 23)) * __uint_as_float((uint32_t)(-25 + 127) << 23);
 }
 
-__device__ __forceinline__ float dm_expf(float x) {
+BNC_MATH_FN float dm_expf(float x) {
     if (x != x) return x;
     if (x > 88.7228394f) return __uint_as_float(0x7F800000u);
     if (x < -103.972084f) return 0.0f;
@@ -81,7 +91,7 @@ __device__ __forceinline__ float dm_expf(float x) {
     return dm_scale2f(p, (int)kf);
 }
 
-__device__ __forceinline__ double dm_log(double x) {
+BNC_MATH_FN double dm_log(double x) {
     if (x != x) return x;
     if (x < 0.0) return __longlong_as_double(0x7FF8000000000000ll);
     if (x == 0.0) return -__longlong_as_double(0x7FF0000000000000ll);
@@ -114,9 +124,9 @@ __device__ __forceinline__ double dm_log(double x) {
     return ed * LN2_HI + (ed * LN2_LO + lm);
 }
 
-__device__ __forceinline__ float dm_logf(float x) { return (float)dm_log((double)x); }
+static __device__ __forceinline__ float dm_logf(float x) { return (float)dm_log((double)x); }
 
-__device__ __forceinline__ double dm_pow(double x, double y) {
+BNC_MATH_FN double dm_pow(double x, double y) {
     if (y == 0.0) return 1.0;
     if (x != x || y != y) return x + y;
     double yi = floor(y);
@@ -137,6 +147,6 @@ __device__ __forceinline__ double dm_pow(double x, double y) {
     return dm_exp(y * dm_log(x));
 }
 
-__device__ __forceinline__ float dm_powf(float x, float y) { return (float)dm_pow((double)x, (double)y); }
+static __device__ __forceinline__ float dm_powf(float x, float y) { return (float)dm_pow((double)x, (double)y); }
 
 }  // namespace bnc

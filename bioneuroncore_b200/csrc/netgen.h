@@ -9,8 +9,8 @@
 #pragma once
 #include <cstdint>
 #include <vector>
-#include "../../include/bnc_abi.h"
-#include "../../include/bnc_b200.h"
+#include "bnc_abi.h"
+#include "bnc_b200.h"
 
 namespace bnc {
 

@@ -14,6 +14,19 @@
 
 namespace bnc {
 
+// GHK factors that depend on V_m only.  V_m is constant while a segment's modifiers
+// (step 1) or a postsynaptic segment's receptors (step 3) run, so exp(-V_norm) and the
+// prefactor of run_tick_common.h:274-312 are evaluated once per segment and tick.  The
+// cached values are the same doubles the full functions compute, so every GHK result is
+// unchanged; a call with another V (the bouton voltage divider, a clamped V) falls back
+// to the full evaluation.
+struct GhkCache {
+    float Vc;          // V the factors belong to
+    uint8_t m1, m2;    // branch: 0 general, 1 |V_norm| < 1e-6, 2 V_norm > 20, 3 V_norm < -20
+    double A1, e1, D1; // monovalent/anion: k*F*V*0.001, exp(-V_norm), 1 - exp(-V_norm)
+    double A2, e2, D2; // divalent
+};
+
 // Segment state visible to a modifier while it runs (registers).
 struct DSeg {
     float V;
@@ -22,6 +35,7 @@ struct DSeg {
     float atp;
     float area;    // geometric membrane area, um^2 (run_tick_common.h:209-214)
     double vol;    // segment volume, um^3 (run_tick_common.h:262-266)
+    GhkCache gc;
 };
 
 // One modifier (or receptor) instance.  st[0..6] are the reference's state[0..6];
@@ -63,7 +77,7 @@ __device__ __forceinline__ void dp_clamp_ions(float* arr) {
         if ((double)arr[i] < 1e-9) arr[i] = (float)1e-9;
 }
 /* run_tick_common.h:274-312 */
-__device__ __forceinline__ double dp_ghk_mono(double V, double c_in, double c_out) {
+static __device__ __forceinline__ double dp_ghk_mono(double V, double c_in, double c_out) {
     double V_norm = FARADAY_CONST * V * 0.001 / (GAS_CONST * CELSIUS_37);
     if (fabs(V_norm) < 1e-6) return FARADAY_CONST * (c_in - c_out);
     double k = FARADAY_CONST / (GAS_CONST * CELSIUS_37);
@@ -71,7 +85,7 @@ __device__ __forceinline__ double dp_ghk_mono(double V, double c_in, double c_ou
     if (V_norm < -20.0) return k * FARADAY_CONST * V * 0.001 * c_out;
     return k * FARADAY_CONST * V * 0.001 * (c_in - c_out * dm_exp(-V_norm)) / (1.0 - dm_exp(-V_norm));
 }
-__device__ __forceinline__ double dp_ghk_div(double V, double c_in, double c_out) {
+static __device__ __forceinline__ double dp_ghk_div(double V, double c_in, double c_out) {
     double V_norm = 2.0 * FARADAY_CONST * V * 0.001 / (GAS_CONST * CELSIUS_37);
     if (fabs(V_norm) < 1e-6) return 2.0 * FARADAY_CONST * (c_in - c_out);
     double k = 4.0 * FARADAY_CONST / (GAS_CONST * CELSIUS_37);
@@ -79,7 +93,7 @@ __device__ __forceinline__ double dp_ghk_div(double V, double c_in, double c_out
     if (V_norm < -20.0) return k * FARADAY_CONST * V * 0.001 * c_out;
     return k * FARADAY_CONST * V * 0.001 * (c_in - c_out * dm_exp(-V_norm)) / (1.0 - dm_exp(-V_norm));
 }
-__device__ __forceinline__ double dp_ghk_anion(double V, double c_in, double c_out) {
+static __device__ __forceinline__ double dp_ghk_anion(double V, double c_in, double c_out) {
     double V_norm = FARADAY_CONST * V * 0.001 / (GAS_CONST * CELSIUS_37);
     if (fabs(V_norm) < 1e-6) return FARADAY_CONST * (c_out - c_in);
     double k = FARADAY_CONST / (GAS_CONST * CELSIUS_37);
@@ -87,6 +101,53 @@ __device__ __forceinline__ double dp_ghk_anion(double V, double c_in, double c_o
     if (V_norm < -20.0) return k * FARADAY_CONST * V * 0.001 * c_in;
     return k * FARADAY_CONST * V * 0.001 * (c_out - c_in * dm_exp(-V_norm)) / (1.0 - dm_exp(-V_norm));
 }
+
+/* GHK with the per-segment factors (see GhkCache); identical results to
+ * dp_ghk_mono/div/anion above. */
+static __device__ __forceinline__ void ghk_cache_fill(GhkCache& c, float Vf) {
+    double V = Vf;
+    c.Vc = Vf;
+    double Vn1 = FARADAY_CONST * V * 0.001 / (GAS_CONST * CELSIUS_37);
+    c.m1 = (fabs(Vn1) < 1e-6) ? 1 : (Vn1 > 20.0) ? 2 : (Vn1 < -20.0) ? 3 : 0;
+    double k1 = FARADAY_CONST / (GAS_CONST * CELSIUS_37);
+    c.A1 = k1 * FARADAY_CONST * V * 0.001;
+    c.e1 = (c.m1 == 0) ? dm_exp(-Vn1) : 0.0;
+    c.D1 = 1.0 - c.e1;
+    double Vn2 = 2.0 * FARADAY_CONST * V * 0.001 / (GAS_CONST * CELSIUS_37);
+    c.m2 = (fabs(Vn2) < 1e-6) ? 1 : (Vn2 > 20.0) ? 2 : (Vn2 < -20.0) ? 3 : 0;
+    double k2 = 4.0 * FARADAY_CONST / (GAS_CONST * CELSIUS_37);
+    c.A2 = k2 * FARADAY_CONST * V * 0.001;
+    c.e2 = (c.m2 == 0) ? dm_exp(-Vn2) : 0.0;
+    c.D2 = 1.0 - c.e2;
+}
+static __device__ __forceinline__ double dp_ghk_mono_c(const GhkCache& c, double V, double c_in, double c_out) {
+    if ((float)V != c.Vc) return dp_ghk_mono(V, c_in, c_out);
+    switch (c.m1) {
+        case 1: return FARADAY_CONST * (c_in - c_out);
+        case 2: return c.A1 * c_in;
+        case 3: return c.A1 * c_out;
+        default: return c.A1 * (c_in - c_out * c.e1) / c.D1;
+    }
+}
+static __device__ __forceinline__ double dp_ghk_div_c(const GhkCache& c, double V, double c_in, double c_out) {
+    if ((float)V != c.Vc) return dp_ghk_div(V, c_in, c_out);
+    switch (c.m2) {
+        case 1: return 2.0 * FARADAY_CONST * (c_in - c_out);
+        case 2: return c.A2 * c_in;
+        case 3: return c.A2 * c_out;
+        default: return c.A2 * (c_in - c_out * c.e2) / c.D2;
+    }
+}
+static __device__ __forceinline__ double dp_ghk_anion_c(const GhkCache& c, double V, double c_in, double c_out) {
+    if ((float)V != c.Vc) return dp_ghk_anion(V, c_in, c_out);
+    switch (c.m1) {
+        case 1: return FARADAY_CONST * (c_out - c_in);
+        case 2: return c.A1 * c_out;
+        case 3: return c.A1 * c_in;
+        default: return c.A1 * (c_out - c_in * c.e1) / c.D1;
+    }
+}
+
 /* modifier_helpers.h:48-54 */
 __device__ __forceinline__ double dp_ghk_P(float gamma_pS, float z, float cbar_mM) {
     double gamma_S = gamma_pS * PS_TO_S;
@@ -239,6 +300,7 @@ __device__ __forceinline__ float ncx_flux_norm(float V_mV, float Na_i, float Na_
  */
 
 /* hh_biological.cpp:193-232 (Nav1.6) and :238-277 (Nav1.2) */
+template <bool kDef>
 __device__ __forceinline__ double dp_nav_current(DMod& m, DSeg& s, float dt, int is12) {
     float V = s.V;
     float area = m.area;
@@ -258,13 +320,13 @@ __device__ __forceinline__ double dp_nav_current(DMod& m, DSeg& s, float dt, int
     m.st[0] = (float)m_val;
     m.st[1] = (float)h_val;
     float open_prob = (float)(m_val * m_val * m_val * h_val);
-    double ttx = (((double)m.st[5]) > 0.0f) ? ((double)m.st[5]) : 0.0f;
+    double ttx = ((kDef ? 0.0 : ((double)m.st[5])) > 0.0f) ? (kDef ? 0.0 : ((double)m.st[5])) : 0.0f;
     open_prob = (float)(open_prob / (1.0f + ttx / (is12 ? 10.0f : 5.0f)));
     float pkc = 0.0f, pka = 0.0f;   /* no PKC/PKA modifiers in supported networks */
     open_prob *= (1.0f - (is12 ? 0.7f : 0.2f) * (pkc + pka) * 0.5f);
     if (open_prob < 0.0f) open_prob = 0.0f;
     double P_single = dp_ghk_P(is12 ? 20.8f : 20.7f, 1.0f, GHK_CBAR_NA_MM);
-    double flux = dp_ghk_mono(V, ((double)s.in[0]), ((double)s.out[0]));
+    double flux = dp_ghk_mono_c(s.gc, V, ((double)s.in[0]), ((double)s.out[0]));
     double I_A = P_single * flux * (((double)m.den) * area) * open_prob;
     double I_Na = I_A * A_TO_PA;
     double vol = s.vol;
@@ -277,12 +339,13 @@ __device__ __forceinline__ double dp_nav_current(DMod& m, DSeg& s, float dt, int
 }
 
 /* hh_biological.cpp:142-187 (Cav1.3) */
+template <bool kDef>
 __device__ __forceinline__ double dp_cav13_current(DMod& m, DSeg& s, float dt) {
     float V = s.V;
     float area = m.area;
-    double Vhalf = (((double)m.st[3]) != 0.0f) ? -fabs(((double)m.st[3])) : -35.0f;
-    double k = (((double)m.st[4]) > 0.0f) ? ((double)m.st[4]) : 7.0f;
-    double gamma_ps = (((double)m.st[2]) > 0.0f) ? ((double)m.st[2]) : 25.0f;
+    double Vhalf = ((kDef ? 0.0 : ((double)m.st[3])) != 0.0f) ? -fabs((kDef ? 0.0 : ((double)m.st[3]))) : -35.0f;
+    double k = ((kDef ? 0.0 : ((double)m.st[4])) > 0.0f) ? (kDef ? 0.0 : ((double)m.st[4])) : 7.0f;
+    double gamma_ps = ((kDef ? 0.0 : ((double)m.st[2])) > 0.0f) ? (kDef ? 0.0 : ((double)m.st[2])) : 25.0f;
     float m_inf = (float)(1.0f / (1.0f + dm_exp(-(V - Vhalf) / (k + 1e-6f))));
     float tau_m = 2.0f;
     m.st[0] = (float)(((double)m.st[0]) + (m_inf - ((double)m.st[0])) * dt / tau_m);
@@ -299,7 +362,7 @@ __device__ __forceinline__ double dp_cav13_current(DMod& m, DSeg& s, float dt) {
     float ca_out = s.out[2];
     double P_single = dp_ghk_P((float)gamma_ps, 2.0f, GHK_CBAR_CA_MM);
     double open_prob = ((double)m.st[0]) * ((double)m.st[0]) * ((double)m.st[1]);
-    double flux = dp_ghk_div(V, ca_in, ca_out);
+    double flux = dp_ghk_div_c(s.gc, V, ca_in, ca_out);
     double I_A = P_single * flux * (((double)m.den) * area) * open_prob;
     double I_Ca = I_A * A_TO_PA;
     double vol = s.vol;
@@ -360,12 +423,13 @@ __device__ __forceinline__ void dp_k_flux(DSeg& s, double I_K, float dt, double 
 }
 
 /* hh_biological.cpp:789-841 (Kv4.2) */
+template <bool kDef>
 __device__ __forceinline__ double dp_kv42_current(DMod& m, DSeg& s, float dt) {
     float V = s.V;
     float area = m.area;
-    double Vhalf = (((double)m.st[4]) != 0.0f) ? -fabs(((double)m.st[4])) : -10.0f;
-    double k = (((double)m.st[5]) > 0.0f) ? ((double)m.st[5]) : 13.5f;
-    double gamma_ps = (((double)m.st[2]) > 0.0f) ? ((double)m.st[2]) : 5.0f;
+    double Vhalf = ((kDef ? 0.0 : ((double)m.st[4])) != 0.0f) ? -fabs((kDef ? 0.0 : ((double)m.st[4]))) : -10.0f;
+    double k = ((kDef ? 0.0 : ((double)m.st[5])) > 0.0f) ? (kDef ? 0.0 : ((double)m.st[5])) : 13.5f;
+    double gamma_ps = ((kDef ? 0.0 : ((double)m.st[2])) > 0.0f) ? (kDef ? 0.0 : ((double)m.st[2])) : 5.0f;
     float m_inf = (float)(1.0f / (1.0f + dm_exp(-(V - Vhalf) / (k + 1e-6f))));
     float tau_m = 1.5f;
     m.st[0] = (float)(((double)m.st[0]) + (m_inf - ((double)m.st[0])) * dt / tau_m);
@@ -385,7 +449,7 @@ __device__ __forceinline__ double dp_kv42_current(DMod& m, DSeg& s, float dt) {
     float K_o = s.out[1];
     double P_single = dp_ghk_P((float)gamma_eff, 1.0f, GHK_CBAR_K_MM);
     double open_prob = ((double)m.st[0]) * ((double)m.st[0]) * ((double)m.st[0]) * ((double)m.st[1]);
-    double flux = dp_ghk_mono(V, K_i, K_o);
+    double flux = dp_ghk_mono_c(s.gc, V, K_i, K_o);
     double I_A = P_single * flux * (((double)m.den) * area) * open_prob;
     double I_K = I_A * A_TO_PA;
     double vol = s.vol;
@@ -395,6 +459,7 @@ __device__ __forceinline__ double dp_kv42_current(DMod& m, DSeg& s, float dt) {
 }
 
 /* hh_biological.cpp:1043-1100 (Kv3.1) */
+template <bool kDef>
 __device__ __forceinline__ double dp_kv31_current(DMod& m, DSeg& s, float dt) {
     float V = s.V;
     float area = m.area;
@@ -413,7 +478,7 @@ __device__ __forceinline__ double dp_kv31_current(DMod& m, DSeg& s, float dt) {
     float K_o = s.out[1];
     double P_single = dp_ghk_P(gamma_ps, 1.0f, GHK_CBAR_K_MM);
     double open_prob = ((double)m.st[0]) * ((double)m.st[0]) * ((double)m.st[0]) * ((double)m.st[1]);
-    double tea = (((double)m.st[5]) > 0.0f) ? ((double)m.st[5]) : 0.0f;
+    double tea = ((kDef ? 0.0 : ((double)m.st[5])) > 0.0f) ? (kDef ? 0.0 : ((double)m.st[5])) : 0.0f;
     open_prob /= (1.0f + tea / 0.2f);
     float pkc = 0.0f;
     float k_phos = 5.6e-6f;
@@ -422,7 +487,7 @@ __device__ __forceinline__ double dp_kv31_current(DMod& m, DSeg& s, float dt) {
     if (((double)m.st[2]) < 0.0f) m.st[2] = 0.0f;
     if (((double)m.st[2]) > 1.0f) m.st[2] = 1.0f;
     open_prob *= (1.0f - 0.27f * ((double)m.st[2]));
-    double flux = dp_ghk_mono(V, K_i, K_o);
+    double flux = dp_ghk_mono_c(s.gc, V, K_i, K_o);
     double I_A = P_single * flux * (((double)m.den) * area) * open_prob;
     double I_K = I_A * A_TO_PA;
     double vol = s.vol;
@@ -432,10 +497,11 @@ __device__ __forceinline__ double dp_kv31_current(DMod& m, DSeg& s, float dt) {
 }
 
 /* hh_biological.cpp:2070-2105 (Cav3.1) */
+template <bool kDef>
 __device__ __forceinline__ double dp_cav31_current(DMod& m, DSeg& s, float dt) {
     float V = s.V;
     float area = m.area;
-    double gamma_ps = (((double)m.st[2]) > 0.0f) ? ((double)m.st[2]) : 7.5f;
+    double gamma_ps = ((kDef ? 0.0 : ((double)m.st[2])) > 0.0f) ? (kDef ? 0.0 : ((double)m.st[2])) : 7.5f;
     double m_val = ((double)m.st[0]), h_val = ((double)m.st[1]);
     float m_inf = dp_bz_act(V, -45.0f, 5.5f);
     float h_inf = dp_bz_inact(V, -77.0f, 6.0f);
@@ -453,14 +519,14 @@ __device__ __forceinline__ double dp_cav31_current(DMod& m, DSeg& s, float dt) {
     m.st[0] = (float)m_val;
     m.st[1] = (float)h_val;
     float open_prob = (float)(m_val * m_val * m_val * h_val);
-    double ni = (((double)m.st[3]) > 0.0f) ? ((double)m.st[3]) : 0.0f;
-    double mib = (((double)m.st[4]) > 0.0f) ? ((double)m.st[4]) : 0.0f;
-    double tta = (((double)m.st[5]) > 0.0f) ? ((double)m.st[5]) : 0.0f;
-    double z944 = (((double)m.st[6]) > 0.0f) ? ((double)m.st[6]) : 0.0f;
+    double ni = ((kDef ? 0.0 : ((double)m.st[3])) > 0.0f) ? (kDef ? 0.0 : ((double)m.st[3])) : 0.0f;
+    double mib = ((kDef ? 0.0 : ((double)m.st[4])) > 0.0f) ? (kDef ? 0.0 : ((double)m.st[4])) : 0.0f;
+    double tta = ((kDef ? 0.0 : ((double)m.st[5])) > 0.0f) ? (kDef ? 0.0 : ((double)m.st[5])) : 0.0f;
+    double z944 = ((kDef ? 0.0 : ((double)m.st[6])) > 0.0f) ? (kDef ? 0.0 : ((double)m.st[6])) : 0.0f;
     open_prob = (float)(open_prob / ((1.0f + ni / 250.0f) * (1.0f + mib / 1.6f)
                                      * (1.0f + tta / 82.0f) * (1.0f + z944 / 100.0f)));
     double P_single = dp_ghk_P((float)gamma_ps, 2.0f, GHK_CBAR_CA_MM);
-    double flux = dp_ghk_div(V, ((double)s.in[2]), ((double)s.out[2]));
+    double flux = dp_ghk_div_c(s.gc, V, ((double)s.in[2]), ((double)s.out[2]));
     double I_A = P_single * flux * (((double)m.den) * area) * open_prob;
     double I_CaT = I_A * A_TO_PA;
     float volume = (float)s.vol;
@@ -470,10 +536,11 @@ __device__ __forceinline__ double dp_cav31_current(DMod& m, DSeg& s, float dt) {
 }
 
 /* hh_biological.cpp:2574-2613 (PMCA) */
+template <bool kDef>
 __device__ __forceinline__ double dp_pmca_current(DMod& m, DSeg& s, float dt) {
     float area = m.area;
-    double K_m_Ca = (((double)m.st[1]) > 0.0f) ? ((double)m.st[1]) : 0.0003f;
-    double hill_n = (((double)m.st[2]) > 0.0f) ? ((double)m.st[2]) : 2.0f;
+    double K_m_Ca = ((kDef ? 0.0 : ((double)m.st[1])) > 0.0f) ? (kDef ? 0.0 : ((double)m.st[1])) : 0.0003f;
+    double hill_n = ((kDef ? 0.0 : ((double)m.st[2])) > 0.0f) ? (kDef ? 0.0 : ((double)m.st[2])) : 2.0f;
     float atp = s.atp;
     if (atp < 0.0f) atp = 0.0f;
     float f_ATP = atp / (atp + 0.2f);
@@ -521,10 +588,11 @@ __device__ __forceinline__ double dp_ncx_current(DMod& m, DSeg& s, float dt) {
 }
 
 /* hh_biological.cpp:2648-2702 (KCC2) */
+template <bool kDef>
 __device__ __forceinline__ double dp_kcc2_current(DMod& m, DSeg& s, float dt) {
     float area = m.area;
-    double Km_K_i = (((double)m.st[1]) > 0.0f) ? ((double)m.st[1]) : 6.5f;
-    double Km_Cl_i = (((double)m.st[2]) > 0.0f) ? ((double)m.st[2]) : 6.5f;
+    double Km_K_i = ((kDef ? 0.0 : ((double)m.st[1])) > 0.0f) ? (kDef ? 0.0 : ((double)m.st[1])) : 6.5f;
+    double Km_Cl_i = ((kDef ? 0.0 : ((double)m.st[2])) > 0.0f) ? (kDef ? 0.0 : ((double)m.st[2])) : 6.5f;
     float K_i = s.in[1]; if (K_i < 1e-9f) K_i = 1e-9f;
     float Cl_i = s.in[3]; if (Cl_i < 1e-9f) Cl_i = 1e-9f;
     float K_o = s.out[1]; if (K_o < 1e-9f) K_o = 1e-9f;
@@ -560,12 +628,13 @@ __device__ __forceinline__ double dp_kcc2_current(DMod& m, DSeg& s, float dt) {
 }
 
 /* hh_biological.cpp:2825-2857 (Ca2+ buffer) */
+template <bool kDef>
 __device__ __forceinline__ double dp_ca_buffer_current(DMod& m, DSeg& s, float dt) {
-    double B_total_ref = (((double)m.st[0]) > 0.0f) ? ((double)m.st[0]) : 0.15f;
+    double B_total_ref = ((kDef ? 0.0 : ((double)m.st[0])) > 0.0f) ? (kDef ? 0.0 : ((double)m.st[0])) : 0.15f;
     double B_total = B_total_ref * ((double)m.den);
-    double K_d = (((double)m.st[2]) > 0.0f) ? ((double)m.st[2]) : 0.0005f;
-    double k_on = (((double)m.st[3]) > 0.0f) ? ((double)m.st[3]) : 0.1f;
-    double k_off = (((double)m.st[4]) > 0.0f) ? ((double)m.st[4]) : (K_d * k_on);
+    double K_d = ((kDef ? 0.0 : ((double)m.st[2])) > 0.0f) ? (kDef ? 0.0 : ((double)m.st[2])) : 0.0005f;
+    double k_on = ((kDef ? 0.0 : ((double)m.st[3])) > 0.0f) ? (kDef ? 0.0 : ((double)m.st[3])) : 0.1f;
+    double k_off = ((kDef ? 0.0 : ((double)m.st[4])) > 0.0f) ? (kDef ? 0.0 : ((double)m.st[4])) : (K_d * k_on);
     double Ca_bound = ((double)m.st[1]);
     if (Ca_bound <= 0.0f && B_total > 0.0f) {
         float Ca_free0 = s.in[2];
@@ -592,13 +661,14 @@ __device__ __forceinline__ double dp_ca_buffer_current(DMod& m, DSeg& s, float d
 }
 
 /* hh_biological.cpp:2859-2888 (SK) */
+template <bool kDef>
 __device__ __forceinline__ double dp_sk_current(DMod& m, DSeg& s, float dt) {
     float V = s.V;
     float area = m.area;
     double open_prob = ((double)m.st[0]);
-    double gamma_ps = (((double)m.st[3]) > 0.0f) ? ((double)m.st[3]) : 10.0f;
-    double tau_open = (((double)m.st[4]) > 0.0f) ? ((double)m.st[4]) : 5.0f;
-    double tau_close = (((double)m.st[5]) > 0.0f) ? ((double)m.st[5]) : 50.0f;
+    double gamma_ps = ((kDef ? 0.0 : ((double)m.st[3])) > 0.0f) ? (kDef ? 0.0 : ((double)m.st[3])) : 10.0f;
+    double tau_open = ((kDef ? 0.0 : ((double)m.st[4])) > 0.0f) ? (kDef ? 0.0 : ((double)m.st[4])) : 5.0f;
+    double tau_close = ((kDef ? 0.0 : ((double)m.st[5])) > 0.0f) ? (kDef ? 0.0 : ((double)m.st[5])) : 50.0f;
     float ca = s.in[2];
     float p_inf = sk_p_inf(ca);
     float tau = (float)((p_inf > open_prob) ? tau_open : tau_close);
@@ -608,7 +678,7 @@ __device__ __forceinline__ double dp_sk_current(DMod& m, DSeg& s, float dt) {
     m.st[0] = (float)open_prob;
     float K_i = s.in[1], K_o = s.out[1];
     double P_single = dp_ghk_P((float)gamma_ps, 1.0f, GHK_CBAR_K_MM);
-    double flux = dp_ghk_mono(V, K_i, K_o);
+    double flux = dp_ghk_mono_c(s.gc, V, K_i, K_o);
     double I_A = P_single * flux * (((double)m.den) * area) * open_prob;
     float I_K = (float)(I_A * A_TO_PA);
     double vol = s.vol;
@@ -620,12 +690,13 @@ __device__ __forceinline__ double dp_sk_current(DMod& m, DSeg& s, float dt) {
 }
 
 /* hh_biological.cpp:2922-2949 (BK) */
+template <bool kDef>
 __device__ __forceinline__ double dp_bk_current(DMod& m, DSeg& s, float dt) {
     float V = s.V;
     float area = m.area;
     double open_prob = ((double)m.st[0]);
-    double gamma_ps = (((double)m.st[1]) > 0.0f) ? ((double)m.st[1]) : 250.0f;
-    double tau_ch = (((double)m.st[2]) > 0.0f) ? ((double)m.st[2]) : 1.0f;
+    double gamma_ps = ((kDef ? 0.0 : ((double)m.st[1])) > 0.0f) ? (kDef ? 0.0 : ((double)m.st[1])) : 250.0f;
+    double tau_ch = ((kDef ? 0.0 : ((double)m.st[2])) > 0.0f) ? (kDef ? 0.0 : ((double)m.st[2])) : 1.0f;
     float Ca = s.in[2];
     float po_inf = bk_ha_po(V, Ca);
     open_prob += (po_inf - open_prob) * dt / tau_ch;
@@ -634,7 +705,7 @@ __device__ __forceinline__ double dp_bk_current(DMod& m, DSeg& s, float dt) {
     m.st[0] = (float)open_prob;
     float K_i = s.in[1], K_o = s.out[1];
     double P_single = dp_ghk_P((float)gamma_ps, 1.0f, GHK_CBAR_K_MM);
-    double flux = dp_ghk_mono(V, K_i, K_o);
+    double flux = dp_ghk_mono_c(s.gc, V, K_i, K_o);
     double I_A = P_single * flux * (((double)m.den) * area) * open_prob;
     float I_K = (float)(I_A * A_TO_PA);
     double vol = s.vol;
@@ -646,15 +717,16 @@ __device__ __forceinline__ double dp_bk_current(DMod& m, DSeg& s, float dt) {
 }
 
 /* hh_biological.cpp:2951-2978 (NaP) */
+template <bool kDef>
 __device__ __forceinline__ double dp_nap_current(DMod& m, DSeg& s, float dt) {
     float V = s.V;
     float area = m.area;
     double m_val = ((double)m.st[0]);
-    double V_half = (((double)m.st[1]) != 0.0f) ? ((double)m.st[1]) : -58.7f;
-    double k_m = (((double)m.st[2]) > 0.0f) ? ((double)m.st[2]) : 6.0f;
-    double gamma_ps = (((double)m.st[3]) > 0.0f) ? ((double)m.st[3]) : 20.7f;
-    double tau_m = (((double)m.st[4]) > 0.0f) ? ((double)m.st[4]) : 5.0f;
-    double Po = (((double)m.st[5]) > 0.0f) ? ((double)m.st[5]) : 0.016f;
+    double V_half = ((kDef ? 0.0 : ((double)m.st[1])) != 0.0f) ? (kDef ? 0.0 : ((double)m.st[1])) : -58.7f;
+    double k_m = ((kDef ? 0.0 : ((double)m.st[2])) > 0.0f) ? (kDef ? 0.0 : ((double)m.st[2])) : 6.0f;
+    double gamma_ps = ((kDef ? 0.0 : ((double)m.st[3])) > 0.0f) ? (kDef ? 0.0 : ((double)m.st[3])) : 20.7f;
+    double tau_m = ((kDef ? 0.0 : ((double)m.st[4])) > 0.0f) ? (kDef ? 0.0 : ((double)m.st[4])) : 5.0f;
+    double Po = ((kDef ? 0.0 : ((double)m.st[5])) > 0.0f) ? (kDef ? 0.0 : ((double)m.st[5])) : 0.016f;
     float m_inf = dp_bz_act(V, (float)V_half, (float)k_m);
     m_val += (m_inf - m_val) * dt / tau_m;
     if (m_val < 0.0f) m_val = 0.0f;
@@ -662,7 +734,7 @@ __device__ __forceinline__ double dp_nap_current(DMod& m, DSeg& s, float dt) {
     m.st[0] = (float)m_val;
     float Na_i = s.in[0], Na_o = s.out[0];
     double P_single = dp_ghk_P((float)gamma_ps, 1.0f, GHK_CBAR_NA_MM);
-    double flux = dp_ghk_mono(V, Na_i, Na_o);
+    double flux = dp_ghk_mono_c(s.gc, V, Na_i, Na_o);
     double I_A = P_single * flux * (((double)m.den) * area) * (m_val * Po);
     float I_Na = (float)(I_A * A_TO_PA);
     double vol = s.vol;
@@ -673,14 +745,15 @@ __device__ __forceinline__ double dp_nap_current(DMod& m, DSeg& s, float dt) {
 }
 
 /* hh_biological.cpp:3018-3038 (Kir2.1) */
+template <bool kDef>
 __device__ __forceinline__ double dp_kir_current(DMod& m, DSeg& s, float dt) {
     float V = s.V;
     float area = m.area;
-    double gamma_ps = (((double)m.st[3]) > 0.0f) ? ((double)m.st[3]) : 30.0f;
+    double gamma_ps = ((kDef ? 0.0 : ((double)m.st[3])) > 0.0f) ? (kDef ? 0.0 : ((double)m.st[3])) : 30.0f;
     float K_i = s.in[1], K_o = s.out[1];
     float f_open = kir_f_open(V);
     double P_single = dp_ghk_P((float)gamma_ps, 1.0f, GHK_CBAR_K_MM);
-    double flux = dp_ghk_mono(V, K_i, K_o);
+    double flux = dp_ghk_mono_c(s.gc, V, K_i, K_o);
     double I_A = P_single * flux * (((double)m.den) * area) * f_open;
     double I_K = I_A * A_TO_PA;
     double vol = s.vol;
@@ -690,15 +763,16 @@ __device__ __forceinline__ double dp_kir_current(DMod& m, DSeg& s, float dt) {
 }
 
 /* hh_biological.cpp:3063-3084 (K2P leak) */
+template <bool kDef>
 __device__ __forceinline__ double dp_k2p_current(DMod& m, DSeg& s, float dt) {
     float V = s.V;
     float area = m.area;
-    double gamma_ps = (((double)m.st[0]) > 0.0f) ? ((double)m.st[0]) : 100.0f;
-    double Po = (((double)m.st[1]) > 0.0f) ? ((double)m.st[1]) : 0.012f;
+    double gamma_ps = ((kDef ? 0.0 : ((double)m.st[0])) > 0.0f) ? (kDef ? 0.0 : ((double)m.st[0])) : 100.0f;
+    double Po = ((kDef ? 0.0 : ((double)m.st[1])) > 0.0f) ? (kDef ? 0.0 : ((double)m.st[1])) : 0.012f;
     float K_i = s.in[1];
     float K_o = s.out[1];
     double P_single = dp_ghk_P((float)gamma_ps, 1.0f, GHK_CBAR_K_MM);
-    double flux = dp_ghk_mono(V, K_i, K_o);
+    double flux = dp_ghk_mono_c(s.gc, V, K_i, K_o);
     double I_A = P_single * flux * (((double)m.den) * area) * Po;
     double I_K = I_A * A_TO_PA;
     double vol = s.vol;
@@ -708,15 +782,16 @@ __device__ __forceinline__ double dp_k2p_current(DMod& m, DSeg& s, float dt) {
 }
 
 /* hh_biological.cpp:3158-3202 (Kv7 M-current) */
+template <bool kDef>
 __device__ __forceinline__ double dp_kv7_current(DMod& m, DSeg& s, float dt) {
     float V = s.V;
     float area = m.area;
     double m_val = ((double)m.st[0]);
-    double V_half = (((double)m.st[1]) != 0.0f) ? ((double)m.st[1]) : -38.0f;
-    double k_slope = (((double)m.st[2]) > 0.0f) ? ((double)m.st[2]) : 10.0f;
-    double tau_act = (((double)m.st[4]) > 0.0f) ? ((double)m.st[4]) : 100.0f;
-    double tau_deact = (((double)m.st[5]) > 0.0f) ? ((double)m.st[5]) : 60.0f;
-    double pip2 = (((double)m.st[6]) >= 0.0f) ? ((double)m.st[6]) : 1.0f;
+    double V_half = ((kDef ? 0.0 : ((double)m.st[1])) != 0.0f) ? (kDef ? 0.0 : ((double)m.st[1])) : -38.0f;
+    double k_slope = ((kDef ? 0.0 : ((double)m.st[2])) > 0.0f) ? (kDef ? 0.0 : ((double)m.st[2])) : 10.0f;
+    double tau_act = ((kDef ? 0.0 : ((double)m.st[4])) > 0.0f) ? (kDef ? 0.0 : ((double)m.st[4])) : 100.0f;
+    double tau_deact = ((kDef ? 0.0 : ((double)m.st[5])) > 0.0f) ? (kDef ? 0.0 : ((double)m.st[5])) : 60.0f;
+    double pip2 = ((kDef ? 1.0 : ((double)m.st[6])) >= 0.0f) ? (kDef ? 1.0 : ((double)m.st[6])) : 1.0f;
     float m_inf = (float)(1.0f / (1.0f + dm_exp(-(V - V_half) / k_slope)));
     float tau_m = (float)(tau_deact + (tau_act - tau_deact) * m_inf);
     if (tau_m < 1.0f) tau_m = 1.0f;
@@ -731,7 +806,7 @@ __device__ __forceinline__ double dp_kv7_current(DMod& m, DSeg& s, float dt) {
     float pkc = 0.0f;
     float pkc_suppress = 1.0f - 0.8f * pkc;
     if (pkc_suppress < 0.0f) pkc_suppress = 0.0f;
-    double flux = dp_ghk_mono(V, K_i, K_o);
+    double flux = dp_ghk_mono_c(s.gc, V, K_i, K_o);
     double I_A = P_single * flux * (((double)m.den) * area) * (m_val * pip2 * pkc_suppress);
     double I_K = I_A * A_TO_PA;
     double vol = s.vol;
@@ -741,13 +816,14 @@ __device__ __forceinline__ double dp_kv7_current(DMod& m, DSeg& s, float dt) {
 }
 
 /* hh_biological.cpp:2763-2797 (Kv1.1 delayed rectifier) */
+template <bool kDef>
 __device__ __forceinline__ double dp_kvdr_current(DMod& m, DSeg& s, float dt) {
     float V = s.V;
     float area = m.area;
     double m_val = ((double)m.st[0]);
-    double V_half = (((double)m.st[1]) != 0.0f) ? ((double)m.st[1]) : -30.0f;
-    double k = (((double)m.st[2]) > 0.0f) ? ((double)m.st[2]) : 6.0f;
-    double tau = (((double)m.st[4]) > 0.0f) ? ((double)m.st[4]) : kv_dr_m_tau(V, (float)V_half);
+    double V_half = ((kDef ? 0.0 : ((double)m.st[1])) != 0.0f) ? (kDef ? 0.0 : ((double)m.st[1])) : -30.0f;
+    double k = ((kDef ? 0.0 : ((double)m.st[2])) > 0.0f) ? (kDef ? 0.0 : ((double)m.st[2])) : 6.0f;
+    double tau = ((kDef ? 0.0 : ((double)m.st[4])) > 0.0f) ? (kDef ? 0.0 : ((double)m.st[4])) : kv_dr_m_tau(V, (float)V_half);
     float m_inf = (float)(1.0f / (1.0f + dm_exp(-(V - V_half) / (k + 1e-6f))));
     m_val += (m_inf - m_val) * dt / (tau + 1e-6f);
     if (m_val < 0.0f) m_val = 0.0f;
@@ -756,7 +832,7 @@ __device__ __forceinline__ double dp_kvdr_current(DMod& m, DSeg& s, float dt) {
     float K_i = s.in[1];
     float K_o = s.out[1];
     double P_single = dp_ghk_P(12.0f, 1.0f, GHK_CBAR_K_MM);
-    double flux = dp_ghk_mono(V, K_i, K_o);
+    double flux = dp_ghk_mono_c(s.gc, V, K_i, K_o);
     double I_A = P_single * flux * (((double)m.den) * area) * m_val;
     double I_K = I_A * A_TO_PA;
     double vol = s.vol;
@@ -769,14 +845,15 @@ __device__ __forceinline__ double dp_kvdr_current(DMod& m, DSeg& s, float dt) {
 }
 
 /* modifier_helpers.h:1442-1484 (hcn_generic_current) via hh_biological.cpp:3598 (HCN1) */
+template <bool kDef>
 __device__ __forceinline__ double dp_hcn1_current(DMod& m, DSeg& s, float dt) {
     double V = ((double)s.V);
     float area = m.area;
-    float V_half = (((double)m.st[1]) != 0) ? (float)((double)m.st[1]) : -69.0f;
-    float k = (((double)m.st[2]) > 0) ? (float)((double)m.st[2]) : 6.0f;
-    float gamma_ps = (((double)m.st[3]) > 0) ? (float)((double)m.st[3]) : 0.84f;
-    float tau_open = (((double)m.st[4]) > 0) ? (float)((double)m.st[4]) : 84.0f;
-    float tau_close = (((double)m.st[5]) > 0) ? (float)((double)m.st[5]) : 300.0f;
+    float V_half = ((kDef ? 0.0 : ((double)m.st[1])) != 0) ? (float)(kDef ? 0.0 : ((double)m.st[1])) : -69.0f;
+    float k = ((kDef ? 0.0 : ((double)m.st[2])) > 0) ? (float)(kDef ? 0.0 : ((double)m.st[2])) : 6.0f;
+    float gamma_ps = ((kDef ? 0.0 : ((double)m.st[3])) > 0) ? (float)(kDef ? 0.0 : ((double)m.st[3])) : 0.84f;
+    float tau_open = ((kDef ? 0.0 : ((double)m.st[4])) > 0) ? (float)(kDef ? 0.0 : ((double)m.st[4])) : 84.0f;
+    float tau_close = ((kDef ? 0.0 : ((double)m.st[5])) > 0) ? (float)(kDef ? 0.0 : ((double)m.st[5])) : 300.0f;
     float camp = 0.1f;  /* segment_camp_um: no cAMP/PKA modifier -> basal 0.1 uM (units.h:324) */
     float Ve = V_half + 15.0f * camp / (camp + 0.5f);
     float mv = m.st[0];
@@ -789,8 +866,8 @@ __device__ __forceinline__ double dp_hcn1_current(DMod& m, DSeg& s, float dt) {
     double P_Na, P_K, P_Ca;
     dp_partial_P(gamma_ps, 0.2f, 0.8f, 0.0f, &P_Na, &P_K, &P_Ca);
     double N = ((double)m.den) * area;
-    double flux_Na = dp_ghk_mono(V, ((double)s.in[0]), ((double)s.out[0]));
-    double flux_K = dp_ghk_mono(V, ((double)s.in[1]), ((double)s.out[1]));
+    double flux_Na = dp_ghk_mono_c(s.gc, V, ((double)s.in[0]), ((double)s.out[0]));
+    double flux_K = dp_ghk_mono_c(s.gc, V, ((double)s.in[1]), ((double)s.out[1]));
     double In = P_Na * flux_Na * N * mv * A_TO_PA;
     double Ik = P_K * flux_K * N * mv * A_TO_PA;
     double vol = s.vol;
@@ -805,16 +882,17 @@ __device__ __forceinline__ double dp_hcn1_current(DMod& m, DSeg& s, float dt) {
 }
 
 /* hh_biological.cpp:3609-3641 (NALCN; the returned sign follows the reference) */
+template <bool kDef>
 __device__ __forceinline__ double dp_nalcn_current(DMod& m, DSeg& s, float dt) {
     float V = s.V;
     float area = m.area;
-    double gamma_ps = (((double)m.st[0]) > 0.0f) ? ((double)m.st[0]) : 27.0f;
+    double gamma_ps = ((kDef ? 0.0 : ((double)m.st[0])) > 0.0f) ? (kDef ? 0.0 : ((double)m.st[0])) : 27.0f;
     double P_Na, P_K, P_Ca;
     dp_nalcn_partial_P((float)gamma_ps, &P_Na, &P_K, &P_Ca);
     double N = ((double)m.den) * area;
-    float Ina = (float)(P_Na * dp_ghk_mono(V, ((double)s.in[0]), ((double)s.out[0])) * N * A_TO_PA);
-    float Ik = (float)(P_K * dp_ghk_mono(V, ((double)s.in[1]), ((double)s.out[1])) * N * A_TO_PA);
-    float Ica = (float)(P_Ca * dp_ghk_div(V, ((double)s.in[2]), ((double)s.out[2])) * N * A_TO_PA);
+    float Ina = (float)(P_Na * dp_ghk_mono_c(s.gc, V, ((double)s.in[0]), ((double)s.out[0])) * N * A_TO_PA);
+    float Ik = (float)(P_K * dp_ghk_mono_c(s.gc, V, ((double)s.in[1]), ((double)s.out[1])) * N * A_TO_PA);
+    float Ica = (float)(P_Ca * dp_ghk_div_c(s.gc, V, ((double)s.in[2]), ((double)s.out[2])) * N * A_TO_PA);
     double vol = s.vol;
     double cpm = FARADAY_CONST * vol / 1000.0;
     s.in[0] = (float)(((double)s.in[0]) - (Ina * dt) / cpm);
@@ -829,6 +907,7 @@ __device__ __forceinline__ double dp_nalcn_current(DMod& m, DSeg& s, float dt) {
 }
 
 /* modifier_helpers.h:1213-1278 (ionotropic_ghk_current) */
+template <bool kDef>
 __device__ __forceinline__ double dp_ionotropic(DMod& m, DSeg& s, float dt, float nt, float gamma_ps, float EC50, float tau_rise,
                             float tau_decay, float P_Na_ratio, float P_K_ratio,
                             float P_Ca_ratio, int is_anion, float tau_desens, float K_desens,
@@ -837,8 +916,11 @@ __device__ __forceinline__ double dp_ionotropic(DMod& m, DSeg& s, float dt, floa
     double V = ((double)s.V);
     double vol = s.vol;
     double cpm = FARADAY_CONST * vol / 1000.0;
-    float stav = (m.av == 7) ? m.area : ((m.av > 0 && m.av < 7) ? m.st[m.av] : 0.0f);
-    float p_gamma_ps = (m.av > 0 && m.av < 8 && ((double)stav) > 0.0f) ? (float)((double)stav) : gamma_ps;
+    float p_gamma_ps = gamma_ps;
+    if (!kDef) {
+        float stav = (m.av == 7) ? m.area : ((m.av > 0 && m.av < 7) ? m.st[m.av] : 0.0f);
+        p_gamma_ps = (m.av > 0 && m.av < 8 && ((double)stav) > 0.0f) ? (float)((double)stav) : gamma_ps;
+    }
     float r_inf = nt / (nt + EC50);
     float r = m.st[0];
     float tau = (r_inf > r) ? tau_rise : tau_decay;
@@ -860,7 +942,7 @@ __device__ __forceinline__ double dp_ionotropic(DMod& m, DSeg& s, float dt, floa
     double I_total = 0.0;
     if (is_anion) {
         double P_Cl = dp_ghk_P(p_gamma_ps, 1.0f, GHK_CBAR_CL_MM);
-        double flux_Cl = dp_ghk_anion(V, ((double)s.in[3]), ((double)s.out[3]));
+        double flux_Cl = dp_ghk_anion_c(s.gc, V, ((double)s.in[3]), ((double)s.out[3]));
         double I_Cl = P_Cl * flux_Cl * N * open_prob * mod_scale * A_TO_PA;
         s.in[3] = (float)(((double)s.in[3]) + (I_Cl * dt) / cpm);
         dp_clamp_ions(s.in);
@@ -868,13 +950,13 @@ __device__ __forceinline__ double dp_ionotropic(DMod& m, DSeg& s, float dt, floa
     }
     double P_Na, P_K, P_Ca;
     dp_partial_P(p_gamma_ps, P_Na_ratio, P_K_ratio, P_Ca_ratio, &P_Na, &P_K, &P_Ca);
-    double I_Na = P_Na * dp_ghk_mono(V, ((double)s.in[0]), ((double)s.out[0])) * N * open_prob * mod_scale * A_TO_PA;
-    double I_K = P_K * dp_ghk_mono(V, ((double)s.in[1]), ((double)s.out[1])) * N * open_prob * mod_scale * A_TO_PA;
+    double I_Na = P_Na * dp_ghk_mono_c(s.gc, V, ((double)s.in[0]), ((double)s.out[0])) * N * open_prob * mod_scale * A_TO_PA;
+    double I_K = P_K * dp_ghk_mono_c(s.gc, V, ((double)s.in[1]), ((double)s.out[1])) * N * open_prob * mod_scale * A_TO_PA;
     I_total = I_Na + I_K;
     s.in[0] = (float)(((double)s.in[0]) - (I_Na * dt) / cpm);
     s.in[1] = (float)(((double)s.in[1]) - (I_K * dt) / cpm);
     if (P_Ca_ratio > 0.0f) {
-        double I_Ca = P_Ca * dp_ghk_div(V, ((double)s.in[2]), ((double)s.out[2])) * N * open_prob * mod_scale * A_TO_PA;
+        double I_Ca = P_Ca * dp_ghk_div_c(s.gc, V, ((double)s.in[2]), ((double)s.out[2])) * N * open_prob * mod_scale * A_TO_PA;
         I_total += I_Ca;
         s.in[2] = (float)(((double)s.in[2]) - (I_Ca * dt) / (2.0f * cpm));
     }
@@ -895,55 +977,69 @@ __device__ __forceinline__ double dp_nmda_cdi_coagonist(DMod& m, DSeg& s, float 
 }
 
 /* receptors_biological.cpp:42-82 (AMPA, NMDA, GABA-A, glycine) */
+template <bool kDef>
 __device__ __forceinline__ double dp_ampa_current(DMod& m, DSeg& s, float dt, float nt, float scale) {
-    return dp_ionotropic(m, s, dt, nt, 8.0f, 0.5f, 0.5f, 3.0f, 0.5f, 0.5f, 0.0f, 0, 3.0f, 0.0f, scale);
+    return dp_ionotropic<kDef>(m, s, dt, nt, 8.0f, 0.5f, 0.5f, 3.0f, 0.5f, 0.5f, 0.0f, 0, 3.0f, 0.0f, scale);
 }
+template <bool kDef>
 __device__ __forceinline__ double dp_nmda_current(DMod& m, DSeg& s, float dt, float nt, float scale) {
-    double I = dp_ionotropic(m, s, dt, nt, 50.0f, 1.0f, 5.0f, 50.0f, 0.08f, 0.08f, 0.84f, 0, 0.0f, 0.0f, scale);
+    double I = dp_ionotropic<kDef>(m, s, dt, nt, 50.0f, 1.0f, 5.0f, 50.0f, 0.08f, 0.08f, 0.84f, 0, 0.0f, 0.0f, scale);
     float mg_block = (float)(1.0f / (1.0f + (1.0f / 3.57f) * dm_exp(-0.062f * ((double)s.V))));
     double c = dp_nmda_cdi_coagonist(m, s, dt);
     return I * mg_block * c;
 }
+template <bool kDef>
 __device__ __forceinline__ double dp_gabaa_current(DMod& m, DSeg& s, float dt, float nt, float scale) {
-    return dp_ionotropic(m, s, dt, nt, 28.0f, 1.0f, 1.0f, 5.0f, 0.0f, 0.0f, 0.0f, 1, 2000.0f, 0.0f, scale);
+    return dp_ionotropic<kDef>(m, s, dt, nt, 28.0f, 1.0f, 1.0f, 5.0f, 0.0f, 0.0f, 0.0f, 1, 2000.0f, 0.0f, scale);
 }
+template <bool kDef>
 __device__ __forceinline__ double dp_glycine_current(DMod& m, DSeg& s, float dt, float nt, float scale) {
-    return dp_ionotropic(m, s, dt, nt, 60.0f, 0.5f, 0.3f, 5.0f, 0.0f, 0.0f, 0.0f, 1, 2000.0f, 0.0f, scale);
+    return dp_ionotropic<kDef>(m, s, dt, nt, 60.0f, 0.5f, 0.3f, 5.0f, 0.0f, 0.0f, 0.0f, 1, 2000.0f, 0.0f, scale);
 }
 
 /* kernel_dispatch.h:337-570 restricted to the supported types; 0 for unknown types
  * (the oracle's loader rejects them, so this branch is never taken). */
-__device__ __forceinline__ double dp_dispatch(uint8_t type, DMod& m, DSeg& s, float dt,
+template <bool kDef>
+__device__ __forceinline__ double dp_dispatch_t(uint8_t type, DMod& m, DSeg& s, float dt,
                                                 float nt_glu, float nt_gaba, float nt_gly) {
     switch (type) {
-        case 1: return dp_cav13_current(m, s, dt);
+        case 1: return dp_cav13_current<kDef>(m, s, dt);
         case 4: return 0.0f;
         case 7: return dp_nak_pump_current(m, s, dt);
-        case 8: return dp_ampa_current(m, s, dt, nt_glu, 1.0f);
-        case 9: return dp_nmda_current(m, s, dt, nt_glu, 1.0f);
-        case 11: return dp_gabaa_current(m, s, dt, nt_gaba, 1.0f);
-        case 12: return dp_glycine_current(m, s, dt, nt_gly, 1.0f);
-        case 85: return dp_kv42_current(m, s, dt);
-        case 98: return dp_pmca_current(m, s, dt);
+        case 8: return dp_ampa_current<kDef>(m, s, dt, nt_glu, 1.0f);
+        case 9: return dp_nmda_current<kDef>(m, s, dt, nt_glu, 1.0f);
+        case 11: return dp_gabaa_current<kDef>(m, s, dt, nt_gaba, 1.0f);
+        case 12: return dp_glycine_current<kDef>(m, s, dt, nt_gly, 1.0f);
+        case 85: return dp_kv42_current<kDef>(m, s, dt);
+        case 98: return dp_pmca_current<kDef>(m, s, dt);
         case 99: return dp_ncx_current(m, s, dt);
-        case 100: return dp_kcc2_current(m, s, dt);
-        case 102: return dp_ca_buffer_current(m, s, dt);
-        case 103: return dp_sk_current(m, s, dt);
-        case 104: return dp_bk_current(m, s, dt);
-        case 105: return dp_nap_current(m, s, dt);
-        case 106: return dp_kir_current(m, s, dt);
-        case 107: return dp_k2p_current(m, s, dt);
-        case 112: return dp_kv7_current(m, s, dt);
-        case 123: return dp_kvdr_current(m, s, dt);
-        case 129: return dp_hcn1_current(m, s, dt);
-        case 133: return dp_nalcn_current(m, s, dt);
+        case 100: return dp_kcc2_current<kDef>(m, s, dt);
+        case 102: return dp_ca_buffer_current<kDef>(m, s, dt);
+        case 103: return dp_sk_current<kDef>(m, s, dt);
+        case 104: return dp_bk_current<kDef>(m, s, dt);
+        case 105: return dp_nap_current<kDef>(m, s, dt);
+        case 106: return dp_kir_current<kDef>(m, s, dt);
+        case 107: return dp_k2p_current<kDef>(m, s, dt);
+        case 112: return dp_kv7_current<kDef>(m, s, dt);
+        case 123: return dp_kvdr_current<kDef>(m, s, dt);
+        case 129: return dp_hcn1_current<kDef>(m, s, dt);
+        case 133: return dp_nalcn_current<kDef>(m, s, dt);
         case 140: return dp_cav21_current(m, s, dt);
-        case 141: return dp_nav_current(m, s, dt, 0);
-        case 142: return dp_nav_current(m, s, dt, 1);
-        case 150: return dp_kv31_current(m, s, dt);
-        case 200: return dp_cav31_current(m, s, dt);
+        case 141: return dp_nav_current<kDef>(m, s, dt, 0);
+        case 142: return dp_nav_current<kDef>(m, s, dt, 1);
+        case 150: return dp_kv31_current<kDef>(m, s, dt);
+        case 200: return dp_cav31_current<kDef>(m, s, dt);
         default: return 0.0f;
     }
+}
+
+// kernel_dispatch.h:337-570 restricted to the device-implemented types.  `defaults`:
+// every parameter state of this modifier holds its default, so the specialisation
+// with constant parameters runs.
+__device__ __forceinline__ double dp_dispatch(uint8_t type, DMod& m, DSeg& s, float dt,
+                                              float nt_glu, float nt_gaba, float nt_gly, bool defaults) {
+    return defaults ? dp_dispatch_t<true>(type, m, s, dt, nt_glu, nt_gaba, nt_gly)
+                    : dp_dispatch_t<false>(type, m, s, dt, nt_glu, nt_gaba, nt_gly);
 }
 
 __device__ __forceinline__ int dp_type_supported(uint8_t t) {

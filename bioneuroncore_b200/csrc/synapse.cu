@@ -1,0 +1,282 @@
+// synapse.cu -- the synapse + membrane kernel of a tick (steps 3 and 4).
+//
+// One thread per segment (device order): the segment's incoming synapses in original
+// synapse order (post-segment CSR, no atomics), then the membrane update of the same
+// segment.  Presynaptic values come from the record the tile kernel wrote after step
+// 2.5 (V, Ca_out, the Cav2.1 gate), so a synapse never reads state another thread is
+// writing.
+#include <cuda_runtime.h>
+#include "net.h"
+#include "physics.cuh"
+
+namespace bnc {
+
+// modifier_helpers.h:1213-1279 via receptors_biological.cpp:42-82
+__device__ __forceinline__ double receptor_current(uint8_t type, DMod& m, DSeg& s, float dt, const float* ntv,
+                                                   float scale) {
+    switch (type) {
+        case 8: return m.av ? dp_ampa_current<false>(m, s, dt, ntv[0], scale) : dp_ampa_current<true>(m, s, dt, ntv[0], scale);
+        case 9: return m.av ? dp_nmda_current<false>(m, s, dt, ntv[0], scale) : dp_nmda_current<true>(m, s, dt, ntv[0], scale);
+        case 11: return m.av ? dp_gabaa_current<false>(m, s, dt, ntv[1], scale) : dp_gabaa_current<true>(m, s, dt, ntv[1], scale);
+        default: return m.av ? dp_glycine_current<false>(m, s, dt, ntv[7], scale) : dp_glycine_current<true>(m, s, dt, ntv[7], scale);
+    }
+}
+
+__device__ __forceinline__ float xorshift32_rnd(uint32_t seed) {
+    uint32_t x = seed;
+    x ^= x << 13;
+    x ^= x >> 17;
+    x ^= x << 5;
+    return (float)(x & 0x7FFFFFFFu) / (float)0x7FFFFFFFu;
+}
+
+__global__ void __launch_bounds__(256)
+k_synapse(NetDev d, float dt, unsigned long long tick, int first_tick) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t N = d.n_seg;
+    if (i >= N) return;
+    const uint8_t sfl = d.sflags[i];
+    const bool syn_on = (d.flags & NF_SYNAPSES) != 0;
+    float ntv[15];
+#pragma unroll
+    for (int q = 0; q < 15; q++) ntv[q] = 0.0f;
+    if (sfl & SF_NMDA) ntv[0] = 1.0f;   // bath NMDA (simulation_host.cpp:337-340)
+    double ib = d.ibuf[i];
+    DSeg s;
+    s.V = d.V[i];
+    const uint32_t k0 = d.post_off[i], k1 = d.post_off[i + 1];
+    bool touched = false;
+    if (k1 > k0) {
+#pragma unroll
+        for (int q = 0; q < 7; q++) s.in[q] = d.ion_in[(size_t)q * N + i];
+#pragma unroll
+        for (int q = 0; q < 4; q++) s.out[q] = d.ion_out[(size_t)q * N + i];
+        s.out[4] = s.out[5] = s.out[6] = 0.0f;
+        s.atp = 0.0f;
+        s.area = d.area[i];
+        s.vol = d.vol[i];
+        ghk_cache_fill(s.gc, s.V);   // V_m is constant through step 3
+    }
+    const uint32_t K = d.n_syn;
+    for (uint32_t k = k0; k < k1; k++) {
+        const uint32_t pre = d.sy_pre[k];
+        const float4 pr = d.pre_rec[pre];
+        const uint8_t sf = d.sy_flags[k];
+        const int ntt = sf >> 4;
+        float cleft = d.sy_cleft[k];
+        const float delay = d.sy_delay[k];
+        // delayed releases (delay_buffer.h:31-44)
+        if ((d.flags & NF_DELAY) && delay > 0.0f) {
+            for (int q = 0; q < 4; q++) {
+                unsigned long long arr = d.dl_arr[(size_t)q * K + k];
+                if (arr == 0) continue;
+                if (arr <= tick) {
+                    cleft += d.dl_amt[(size_t)q * K + k];
+                    d.dl_arr[(size_t)q * K + k] = 0;
+                }
+            }
+        }
+        // RRP recovery (kernel_dispatch.h:612-630); no CaMKII/calcineurin modifiers
+        float rrp = 0.0f, rrp_max = d.sy_rrp_max[k];
+        if (rrp_max > 0.0f) rrp = d.sy_rrp[k];
+        if (!(rrp_max <= 0.0f || rrp >= rrp_max)) {
+            float ca_pre = d.pre_ext[pre].z;
+            float ca_f = ca_pre / (0.0005f + ca_pre);
+            float priming = d.sy_rrp_rec[k] + 0.0f * 0.02f + 0.0f * 0.01f;
+            priming *= ca_f;
+            float rec = (rrp_max - rrp) * priming * dt;
+            rrp += rec;
+            if (rrp > rrp_max) rrp = rrp_max;
+        }
+        // bouton Ca2+ (modifier_helpers.h:764-806)
+        float bouton = d.sy_bouton[k];
+        const float pre_area = d.sy_pre_area[k];
+        {
+            const float g_K = d.sy_gK[k], g_Na = d.sy_gNa[k];
+            float V_bouton = pr.x;
+            if (g_K > 0.0f || g_Na > 0.0f) {
+                float4 ex = d.pre_ext[pre];
+                float koe = d.pre_ext2[pre];
+                float E_K = dp_nernst(ex.y, koe, 1.0f);
+                float E_Na = dp_nernst(ex.x, ex.w, 1.0f);
+                V_bouton = (float)((300.0f * (double)pr.x + g_K * E_K + g_Na * E_Na) / (300.0f + g_K + g_Na));
+            }
+            float cav21_dens = 0.0f, mm = 0.0f, h = 0.0f;
+            if (pr.z != 0.0f) {
+                cav21_dens = pr.z;
+                float m_inf = cav21_m_inf(V_bouton);
+                float h_inf = cav21_h_inf(V_bouton, bouton * MM_TO_UM);
+                mm = m_inf;
+                h = (float)(h_inf + ((double)pr.w - h_inf) * dm_expf(-dt / 300.0f));
+            }
+            float cav21_open = mm * mm * h;
+            double P_single = dp_ghk_P(15.0f, 2.0f, GHK_CBAR_CA_MM);
+            double flux = dp_ghk_div(V_bouton, bouton, (double)pr.y);
+            double I_A = P_single * flux * (cav21_dens * pre_area) * cav21_open;
+            float I_Ca = (float)(I_A * A_TO_PA);
+            bouton = (float)(bouton - I_Ca * dt * 1000.0f / (2.0f * FARADAY_CONST * 0.1f));
+            bouton += (0.0001f - bouton) * dt / 5.0f;
+            if (bouton < 0.0f) bouton = 0.0f;
+        }
+        // Ca2+-dependent release (simulation_host.cpp:421-460)
+        uint8_t refr = d.sy_refr[k];
+        if (refr == 0) {
+            float Ca_uM = bouton * MM_TO_UM;
+            float ca_act = dm_powf(Ca_uM, 4.0f) / (dm_powf(Ca_uM, 4.0f) + dm_powf(10.0f, 4.0f));
+            float p = d.sy_prel[k] * ca_act;
+            uint32_t vbits = (uint32_t)(long long)((double)pr.x * 1000.0f);
+            uint32_t seed = d.sy_id[k] ^ (uint32_t)tick ^ vbits;
+            if (xorshift32_rnd(seed) < p) {
+                const float amt = d.sy_amt[k];
+                float release_amt;
+                if (rrp_max <= 0.0f) release_amt = amt * p;
+                else {
+                    float avail = amt;
+                    if (avail > rrp) avail = rrp;
+                    release_amt = avail * p;
+                    rrp -= release_amt;
+                    if (rrp < 0) rrp = 0;
+                }
+                unsigned long long delay_ticks = (delay <= 0.0f || dt <= 0.0f) ? 0ull
+                    : (unsigned long long)((delay / dt) + 0.5f);
+                if (delay_ticks > 0) {
+                    for (int q = 0; q < 4; q++) {
+                        if (d.dl_arr[(size_t)q * K + k] == 0) {
+                            d.dl_arr[(size_t)q * K + k] = tick + delay_ticks;
+                            d.dl_amt[(size_t)q * K + k] = release_amt;
+                            d.dl_nt[(size_t)q * K + k] = (uint8_t)ntt;
+                            break;
+                        }
+                    }
+                } else {
+                    cleft += release_amt;
+                }
+                refr = (uint8_t)(uint32_t)(20.0f / dt + 0.5f);
+            }
+        }
+        // NT into the postsynaptic segment (simulation_host.cpp:463-465)
+        ntv[ntt] += cleft;
+        // receptors (simulation_host.cpp:490-500)
+        float I_syn = 0.0f;
+        const float post_area = d.sy_post_area[k];
+        const float scale = d.sy_scale[k];
+        const uint32_t NR = d.n_rec;
+        for (uint32_t r = d.rc_off[k]; r < d.rc_off[k + 1]; r++) {
+            DMod m;
+            m.den = d.rc_den[r];
+            m.st[0] = d.rc_st[r];
+            m.st[1] = d.rc_st[(size_t)NR + r];
+            m.st[2] = d.rc_st[(size_t)2 * NR + r];
+            m.st[3] = m.st[4] = m.st[5] = m.st[6] = 0.0f;
+            m.area = (post_area > 0.0f) ? post_area : s.area;
+            m.av = d.rc_av[r];
+            const uint8_t rt = d.rc_type[r];
+            I_syn = (float)(I_syn + receptor_current(rt, m, s, dt, ntv, scale));
+            d.rc_st[r] = m.st[0];
+            d.rc_st[(size_t)NR + r] = m.st[1];
+            d.rc_st[(size_t)2 * NR + r] = m.st[2];
+            touched = true;
+        }
+        ib += I_syn;
+        // spine Ca2+ (modifier_helpers.h:808-817)
+        float spine = d.sy_spine[k];
+        {
+            float I_abs = I_syn < 0.0f ? -I_syn : I_syn;
+            float I_Ca = I_abs * 0.1f;
+            float influx = (float)(I_Ca * dt * 1000.0f / (2.0f * FARADAY_CONST * 0.05f * 100.0f));
+            spine += influx;
+            spine += (0.0001f - spine) * dt / 50.0f;
+            if (spine < 0.0f) spine = 0.0f;
+        }
+        // clearance (simulation_host.cpp:505-510)
+        cleft *= dm_expf(-dt / d.sy_tauc[k]);
+        if (cleft < 0.0f) cleft = 0.0f;
+        // BCM threshold, spine CaMKII/calcineurin, weight (simulation_host.cpp:527-576)
+        float facil = d.sy_facil[k];
+        {
+            float Ca_uM = spine * 1000.0f;
+            float Ca_sq = Ca_uM * Ca_uM;
+            facil += (Ca_sq - facil) * dt / 300000.0f;
+            if (facil < 0.0f) facil = 0.0f;
+        }
+        float camkii = d.sy_camkii[k], calcn = d.sy_calcn[k];
+        {
+            float Ca_uM = spine * MM_TO_UM;
+            float Ca4 = Ca_uM * Ca_uM * Ca_uM * Ca_uM;
+            float camkii_inf = Ca4 / (Ca4 + 1.0f + 1e-9f);
+            camkii += (camkii_inf - camkii) * dt / 2000.0f;
+            if (camkii < 0.0f) camkii = 0.0f;
+            if (camkii > 1.0f) camkii = 1.0f;
+            float Ca2 = Ca_uM * Ca_uM;
+            float calcineurin_inf = Ca2 / (Ca2 + 0.05f * 0.05f + 1e-9f);
+            calcn += (calcineurin_inf - calcn) * dt / 300.0f;
+            if (calcn < 0.0f) calcn = 0.0f;
+            if (calcn > 1.0f) calcn = 1.0f;
+        }
+        float weight = d.sy_weight[k];
+        {
+            float dw = 0.0f;
+            if (camkii > 0.0f) dw += 0.0003f * camkii * dt;
+            float pp1_active = 0.5f;
+            if (calcn > 0.0f) dw -= 0.0001f * calcn * pp1_active * dt;
+            if (sf & 1) dw = -dw;
+            weight += dw;
+            if (weight != weight) weight = 0.5f;
+            if (facil != facil) facil = 0.0f;
+            if (weight < 0.01f) weight = 0.01f;
+            if (weight > 10.0f) weight = 10.0f;
+        }
+        if (refr > 0) refr--;
+        d.sy_cleft[k] = cleft;
+        d.sy_refr[k] = refr;
+        d.sy_bouton[k] = bouton;
+        d.sy_spine[k] = spine;
+        d.sy_camkii[k] = camkii;
+        d.sy_calcn[k] = calcn;
+        d.sy_facil[k] = facil;
+        d.sy_weight[k] = weight;
+        if (rrp_max > 0.0f) d.sy_rrp[k] = rrp;
+    }
+    // step 4: membrane update (simulation_host.cpp:596-649)
+    float V = s.V;
+    if (ib != ib) ib = 0.0f;
+    if (ib > 10000.0f) ib = 10000.0f;
+    if (ib < -10000.0f) ib = -10000.0f;
+    const float C_m = d.cm[i];
+    const float prev_V = V;
+    float dV = (float)(ib / C_m * dt);
+    if (dV > 50.0f) dV = 50.0f;
+    if (dV < -50.0f) dV = -50.0f;
+    V = (float)((double)V + dV);
+    if (prev_V <= -40.0f && V > -40.0f) d.spike_count[i]++;
+    if (d.vc_off) {
+        for (uint32_t k = d.vc_off[i]; k < d.vc_off[i + 1]; k++)
+            if (tick >= d.vc_start[k] && tick < d.vc_end[k]) V = d.vc_target[k];
+    }
+    if (V != V) V = -65.0f;
+    else {
+        if (V < -120.0f) V = -120.0f;
+        if (V > 150.0f) V = 150.0f;
+    }
+    d.V[i] = V;
+    if (touched) {
+#pragma unroll
+        for (int q = 0; q < 7; q++) d.ion_in[(size_t)q * N + i] = s.in[q];
+    }
+    if (syn_on) {
+        const uint32_t mask = first_tick ? 0x7FFFu : d.nt_used_mask;
+#pragma unroll
+        for (int q = 0; q < 15; q++)
+            if ((mask >> q) & 1u) d.nt[(size_t)q * N + i] = ntv[q];
+    } else if (sfl & SF_NMDA) {
+        d.nt[i] = 1.0f;
+    }
+}
+
+cudaError_t launch_synapse(const NetDev& dev, float dt, unsigned long long tick, int first_tick,
+                           cudaStream_t stream) {
+    k_synapse<<<(dev.n_seg + 255) / 256, 256, 0, stream>>>(dev, dt, tick, first_tick);
+    return cudaGetLastError();
+}
+
+}  // namespace bnc
