@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -677,3 +678,93 @@ int bnc_save_bion(void* sim, const char* filename) {
 }
 
 }  // extern "C"
+
+// ---- Ticks with the presynaptic exchange records in a library-owned array ----
+//
+// Each tick the tile kernel writes, for every segment, the record the synapse
+// kernel reads for that segment as a presynaptic site: V, Ca_out and the Cav2.1
+// density and h gate (float4), plus Na_in, K_in, Ca_in, Na_out (float4) and K_out
+// (float) when some synapse has autoreceptors or a readily releasable pool.  That
+// is 36 bytes of scratch per segment, rewritten every tick.  bnc_run_ticks takes it
+// from buffers allocated with the network; bnc_run_ticks_static_scratch takes it
+// from the fixed array below, for callers that cannot allocate device memory while
+// they run the simulation.
+namespace bnc {
+namespace {
+
+constexpr uint32_t kScratchSegs = BNC_STATIC_SCRATCH_MAX_SEGMENTS;
+constexpr size_t kScratchRecOff = 0;                                             // float4 [kScratchSegs]
+constexpr size_t kScratchExtOff = (size_t)kScratchSegs * sizeof(float4);         // float4 [kScratchSegs]
+constexpr size_t kScratchExt2Off = (size_t)kScratchSegs * 2 * sizeof(float4);    // float  [kScratchSegs]
+constexpr size_t kScratchBytes = kScratchExt2Off + (size_t)kScratchSegs * sizeof(float);
+static_assert(kScratchExtOff % 256 == 0 && kScratchExt2Off % 256 == 0, "scratch parts stay 256-byte aligned");
+
+// One copy per device that loads the library, alive until the process exits.  In
+// host code this name is only a stand-in for the symbol: the kernels get the device
+// address that cudaGetSymbolAddress returns for the current device.
+static __device__ __align__(256) unsigned char g_tick_scratch[kScratchBytes];
+
+constexpr int kScratchMaxDevices = 64;
+std::mutex g_scratch_mu;
+unsigned char* g_scratch_addr[kScratchMaxDevices] = {};
+
+// Device address of g_tick_scratch on `device`, which must be the current device.
+// Looked up on the first call per device and kept.
+int scratch_address(int device, unsigned char** out) {
+    if (device < 0 || device >= kScratchMaxDevices) {
+        set_error("bnc_run_ticks_static_scratch: device %d outside 0..%d", device, kScratchMaxDevices - 1);
+        return BNC_ERR_ARG;
+    }
+    std::lock_guard<std::mutex> lock(g_scratch_mu);
+    if (!g_scratch_addr[device]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_tick_scratch);
+        if (e != cudaSuccess || !p) return cuda_fail(e, "cudaGetSymbolAddress of the static tick scratch");
+        g_scratch_addr[device] = static_cast<unsigned char*>(p);
+    }
+    *out = g_scratch_addr[device];
+    return BNC_OK;
+}
+
+}  // namespace
+}  // namespace bnc
+
+extern "C" int bnc_run_ticks_static_scratch(void* sim, uint32_t n_ticks, float dt) {
+    if (!sim) { set_error("null handle"); return BNC_ERR_ARG; }
+    Backend* b = static_cast<Backend*>(sim);
+    if (!b->loaded) { set_error("no network loaded"); return BNC_ERR_STATE; }
+    if (b->failed) { set_error("backend is in a failed state after a device error"); return BNC_ERR_STATE; }
+    const uint32_t n = b->dev.n_seg;
+    if (n > kScratchSegs) {
+        set_error("bnc_run_ticks_static_scratch: the network has %u segments, the static scratch holds at most %u "
+                  "(BNC_STATIC_SCRATCH_MAX_SEGMENTS); use bnc_run_ticks", n, kScratchSegs);
+        return BNC_ERR_ARG;
+    }
+    cudaError_t e = cudaSetDevice(b->device);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
+    unsigned char* base = nullptr;
+    int rc = scratch_address(b->device, &base);
+    if (rc != BNC_OK) return rc;
+
+    // The network's own pointers, with the exchange records redirected into the array
+    // (the optional part only where the network has one).
+    NetDev d = b->dev;
+    d.pre_rec = reinterpret_cast<float4*>(base + kScratchRecOff);
+    if (b->dev.pre_ext) d.pre_ext = reinterpret_cast<float4*>(base + kScratchExtOff);
+    if (b->dev.pre_ext2) d.pre_ext2 = reinterpret_cast<float*>(base + kScratchExt2Off);
+    // The array keeps whatever the previous call left; start from zero as the
+    // network's own buffers do.
+    if (n) {
+        e = cudaMemsetAsync(d.pre_rec, 0, (size_t)n * sizeof(float4), b->stream);
+        if (e == cudaSuccess && b->dev.pre_ext) e = cudaMemsetAsync(d.pre_ext, 0, (size_t)n * sizeof(float4), b->stream);
+        if (e == cudaSuccess && b->dev.pre_ext2) e = cudaMemsetAsync(d.pre_ext2, 0, (size_t)n * sizeof(float), b->stream);
+        if (e != cudaSuccess) return cuda_fail(e, "clearing the static tick scratch");
+    }
+    for (uint32_t t = 0; t < n_ticks; t++) {
+        e = launch_tick(d, b->host, dt, b->tick, b->ticks_run == 0 ? 1 : 0, b->stream);
+        if (e != cudaSuccess) { b->failed = true; return cuda_fail(e, "tick launch"); }
+        b->tick++;
+        b->ticks_run++;
+    }
+    return sync_stream(b);
+}

@@ -135,6 +135,27 @@ int bnc_load_generated(void* sim, const BncNetgenParams* p);
 /* Runs n ticks of dt ms on the device without refreshing the host AoS view. */
 int bnc_run_ticks(void* sim, uint32_t n_ticks, float dt);
 
+/* No counterpart in the reference.  Same ticks and results as bnc_run_ticks, for
+ * callers that cannot call cudaMalloc while they drive the simulation: a host
+ * whose own pool allocator has reserved the device memory and treats any other
+ * allocation as an error, or a control loop that cannot afford the device-wide
+ * synchronisation a cudaFree brings.  Each tick the tile kernel hands the synapse
+ * kernel a per-segment record of the presynaptic state (36 bytes per segment);
+ * here that scratch is a fixed array inside the library instead of buffers of the
+ * network, and the call allocates nothing.
+ *   - Limit: networks of at most BNC_STATIC_SCRATCH_MAX_SEGMENTS segments (the
+ *     array is 4.5 MiB on every GPU that loads the library, held until exit);
+ *     larger networks are rejected with BNC_ERR_ARG.
+ *   - The first call on a device looks up the array's device address (one
+ *     runtime query, no allocation); make that first call before any stream
+ *     capture.
+ *   - All calls on a device share the one array.  Each call clears the part it
+ *     uses before its first tick, but calls that overlap on the GPU (two handles
+ *     on one device, different streams, different host threads) race on it:
+ *     serialise them. */
+#define BNC_STATIC_SCRATCH_MAX_SEGMENTS 131072u
+int bnc_run_ticks_static_scratch(void* sim, uint32_t n_ticks, float dt);
+
 /* Runs n ticks bracketed by CUDA events on the backend's stream; *ms receives the
  * elapsed device time. */
 int bnc_time_ticks(void* sim, uint32_t n_ticks, float dt, float* ms);
