@@ -58,6 +58,32 @@ def dist_env():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
 
 
+def rank_seed(seed, rank):
+    """Each rank simulates its own network (replicas, weak scaling): seed + rank."""
+    return seed + rank
+
+
+def max_over_ranks(value, dist, device):
+    """Max of a float over all ranks; every rank must call it (one all-reduce)."""
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def rank_barrier(dist, device):
+    """Barrier as an all-reduce on the backend's device, then a device synchronize."""
+    if dist is None:
+        return
+    import torch
+    t = torch.zeros(1, device=device)
+    dist.all_reduce(t)
+    if device != "cpu":
+        torch.cuda.synchronize()
+
+
 class ClockSampler:
     """nvidia-smi clock/throttle samples every 200 ms while the timed region runs."""
 
@@ -204,7 +230,7 @@ def main():
     from bioneuroncore_b200 import Backend, NetgenParams, NET_LARGE
     b = Backend(local_rank if world > 1 else 0)
     t0 = time.perf_counter()
-    b.load_generated(NetgenParams(family=NET_LARGE, n_neurons=a.neurons, seed=a.seed + rank))
+    b.load_generated(NetgenParams(family=NET_LARGE, n_neurons=a.neurons, seed=rank_seed(a.seed, rank)))
     setup_s = time.perf_counter() - t0
     info = b.info()
     b.run_ticks(a.warmup, DT)
@@ -212,11 +238,7 @@ def main():
     ms_tile, ms_syn = b.profile_ticks(n_prof, DT)
 
     def barrier():
-        if dist is not None:
-            import torch
-            t = torch.zeros(1, device="cuda")
-            dist.all_reduce(t)
-            torch.cuda.synchronize()
+        rank_barrier(dist, "cuda")
 
     barrier()
     clocks = ClockSampler(local_rank)
@@ -224,12 +246,7 @@ def main():
     ms = b.time_ticks(a.steps, DT)
     clk = clocks.stop()
     barrier()
-    ms_max = ms
-    if dist is not None:
-        import torch
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_max = float(t.item())
+    ms_max = max_over_ranks(ms, dist, "cuda")
     seg_ticks = float(info.n_segments) * a.steps * world
     value = seg_ticks / (ms_max / 1000.0)
 
@@ -245,11 +262,7 @@ def main():
         t1 = time.perf_counter()
         for _ in range(a.e2e_steps):
             b.step_io(DT, amp.data_ptr(), n_stim, vout.data_ptr(), info.n_segments)
-        el = time.perf_counter() - t1
-        if dist is not None:
-            t = torch.tensor([el], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            el = float(t.item())
+        el = max_over_ranks(time.perf_counter() - t1, dist, "cuda")
         e2e = {"value": float(info.n_segments) * a.e2e_steps * world / el, "unit": UNIT,
                "h2d_bytes_per_step": 4 * n_stim, "d2h_bytes_per_step": 4 * info.n_segments,
                "steps": a.e2e_steps, "timing": "host wall clock around the steps, max over ranks"}

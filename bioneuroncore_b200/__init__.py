@@ -36,7 +36,8 @@ DROPIN_SYMBOLS = ["gpu_backend_create", "gpu_backend_create_on_device", "gpu_bac
 NEW_SYMBOLS = ["bnc_netgen_aos", "bnc_netgen_free", "bnc_last_error", "bnc_load_aos", "bnc_load_generated",
                "bnc_run_ticks", "bnc_time_ticks", "bnc_sync_to_host", "bnc_read_segment_field",
                "bnc_read_synapse_field", "bnc_set_synapse_scale", "bnc_network_info", "bnc_save_bion",
-               "bnc_plan_generated", "bnc_step_io", "bnc_profile_ticks", "bnc_run_ticks_static_scratch"]
+               "bnc_plan_generated", "bnc_step_io", "bnc_profile_ticks", "bnc_run_ticks_static_scratch",
+               "bnc_plan_aos", "bnc_bion_load", "bnc_bion_unload", "bnc_bion_save"]
 
 
 class NetInfo(C.Structure):
@@ -88,6 +89,8 @@ def load_library(path=LIB_PATH):
         "bnc_save_bion": ([vp, C.c_char_p], i32), "bnc_plan_generated": ([vp, vp], i32),
         "bnc_step_io": ([vp, f32, vp, u32, vp, u32], i32), "bnc_profile_ticks": ([vp, u32, f32, vp, vp], i32),
         "bnc_run_ticks_static_scratch": ([vp, u32, f32], i32),
+        "bnc_plan_aos": ([vp, vp, u32, vp], i32), "bnc_bion_load": ([C.c_char_p, vp], i32),
+        "bnc_bion_unload": ([vp], None), "bnc_bion_save": ([C.c_char_p, vp], i32),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)

@@ -25,7 +25,7 @@ REFERENCE = "/root/reference"
 
 CU_SOURCES = ["tile.cu", "synapse.cu", "backend.cu"]
 CPP_SOURCES = ["netgen.cpp", "capi_host.cpp", "builder.cpp"]
-HEADERS = ["common.h", "net.h", "netgen.h", "physics.cuh", "device_math.cuh"]
+HEADERS = sorted(f for f in os.listdir(CSRC) if f.endswith((".h", ".cuh")))
 
 GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--fmad=false", "-Xcompiler", "-fPIC,-ffp-contract=off",

@@ -420,19 +420,10 @@ int bnc_load_generated(void* sim, const BncNetgenParams* p) {
     return BNC_OK;
 }
 
-int bnc_plan_generated(const BncNetgenParams* p, BncNetInfo* info) {
-    if (!p || !info) { set_error("bnc_plan_generated: null argument"); return BNC_ERR_ARG; }
-    HostNet hn;
-    Stimuli stim;
-    HostNetSink sink;
-    sink.hn = &hn;
-    sink.stim = &stim.current;
-    NetShape shape;
-    int rc = generate_network(*p, sink, &shape);
-    if (rc != BNC_OK) { set_error("bnc_plan_generated: invalid parameters"); return rc; }
+static int plan_info(const HostNet& hn, const Stimuli& stim, BncNetInfo* info) {
     NetDev dev;
     NetHost host;
-    rc = build_network(hn, stim, &dev, &host, nullptr);
+    int rc = build_network(hn, stim, &dev, &host, nullptr);
     if (rc != BNC_OK) return rc;
     std::memset(info, 0, sizeof(*info));
     info->n_segments = dev.n_seg; info->n_connections = host.n_conn; info->n_synapses = dev.n_syn;
@@ -443,6 +434,42 @@ int bnc_plan_generated(const BncNetgenParams* p, BncNetInfo* info) {
     info->seg_bytes_per_tick = host.seg_bytes; info->syn_bytes_per_tick = host.syn_bytes;
     info->tile_bytes_per_tick = host.tile_bytes; info->synapse_kernel_bytes_per_tick = host.synk_bytes;
     return BNC_OK;
+}
+
+int bnc_plan_generated(const BncNetgenParams* p, BncNetInfo* info) {
+    if (!p || !info) { set_error("bnc_plan_generated: null argument"); return BNC_ERR_ARG; }
+    HostNet hn;
+    Stimuli stim;
+    HostNetSink sink;
+    sink.hn = &hn;
+    sink.stim = &stim.current;
+    NetShape shape;
+    int rc = generate_network(*p, sink, &shape);
+    if (rc != BNC_OK) { set_error("bnc_plan_generated: invalid parameters"); return rc; }
+    return plan_info(hn, stim, info);
+}
+
+int bnc_plan_aos(const BncBionData* data, const BncCurrentStimulus* stim, uint32_t n_stim, BncNetInfo* info) {
+    if (!data || !info || (!data->segments && data->num_segments)) { set_error("bnc_plan_aos: null argument"); return BNC_ERR_ARG; }
+    HostNet hn;
+    hostnet_from_aos(*data, &hn);
+    Stimuli st;
+    if (stim && n_stim) st.current.assign(stim, stim + n_stim);
+    return plan_info(hn, st, info);
+}
+
+int bnc_bion_load(const char* filename, BncBionData* out) {
+    if (!filename || !out) { set_error("bnc_bion_load: null argument"); return BNC_ERR_ARG; }
+    return load_bion_file(filename, out);
+}
+
+void bnc_bion_unload(BncBionData* data) {
+    if (data) free_aos_arrays(*data);
+}
+
+int bnc_bion_save(const char* filename, const BncBionData* data) {
+    if (!filename || !data || !data->segments) { set_error("bnc_bion_save: null argument"); return BNC_ERR_ARG; }
+    return save_bion(*data, filename);
 }
 
 int bnc_run_ticks(void* sim, uint32_t n_ticks, float dt) {

@@ -224,6 +224,8 @@ void hostnet_add_segment(HostNet& hn, const BncSegment& s) {
     L.id = s.id;
     L.segment_type = s.segment_type;
     L.modifier_count = s.modifier_count > BNC_MAX_MODIFIERS ? (uint8_t)BNC_MAX_MODIFIERS : s.modifier_count;
+    if (s.modifier_count > BNC_MAX_MODIFIERS && hn.bad_modifier_count_seg == UINT32_MAX)
+        hn.bad_modifier_count_seg = (uint32_t)hn.seg.size();
     L.radius = s.radius; L.length = s.length;
     L.V_m = (float)s.V_m;
     for (int q = 0; q < 7; q++) { L.intra_ions[q] = (float)s.intra_ions[q]; L.extra_ions[q] = (float)s.extra_ions[q]; }
@@ -298,6 +300,10 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
     host->n_seg = n;
     host->n_conn = aos.num_connections;
     host->n_syn_total = aos.num_synapses;
+    if (hn.bad_modifier_count_seg != UINT32_MAX) {
+        set_error("segment %u: modifier_count > %d", hn.bad_modifier_count_seg, BNC_MAX_MODIFIERS);
+        return BNC_ERR_FORMAT;
+    }
     // segment ids must be the positions (stimuli and the reference match on id)
     for (uint32_t i = 0; i < n; i++) {
         if (S[i].modifier_count > BNC_MAX_MODIFIERS) { set_error("segment %u: modifier_count %u > 32", i, S[i].modifier_count); return BNC_ERR_FORMAT; }

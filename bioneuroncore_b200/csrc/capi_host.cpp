@@ -33,7 +33,7 @@ struct AosSink : NetSink {
     void begin(uint32_t n_neurons, uint32_t n_segments, uint32_t n_connections, uint64_t n_synapses,
                uint32_t n_stimuli) override {
         std::memset(out, 0, sizeof(*out));
-        out->header.magic = 0x4E4F4942u;  // "BION"
+        out->header.magic = 0x42494F4Eu;  // BION_MAGIC (bion_format.h:12)
         out->header.version = 14;
         out->header.num_neurons = n_neurons;
         out->header.num_segments = n_segments;

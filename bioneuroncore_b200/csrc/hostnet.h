@@ -49,6 +49,9 @@ struct HostNet {
     std::vector<BncIntraConnection> conn;
     std::vector<SynLite> syn;
     std::vector<ModLite> recs;
+    // First segment whose modifier_count exceeded BNC_MAX_MODIFIERS (UINT32_MAX: none);
+    // its modifier list is truncated here and the builder rejects the network.
+    uint32_t bad_modifier_count_seg = UINT32_MAX;
     const ModLite& mod(uint32_t i, uint32_t j) const { return mods[seg[i].mod_off + j]; }
     const ModLite& post_rec(uint32_t k, uint32_t j) const { return recs[syn[k].rec_off + j]; }
     const ModLite& pre_ar(uint32_t k, uint32_t j) const {

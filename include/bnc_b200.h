@@ -202,6 +202,20 @@ int bnc_network_info(void* sim, BncNetInfo* info);
  * schedule, CSRs) without a device; fills `info` (no upload, no CUDA call). */
 int bnc_plan_generated(const BncNetgenParams* p, BncNetInfo* info);
 
+/* Host-only: runs the builder's planning on AoS arrays in memory (validation,
+ * supported-type checks, tiles, schedule) without a device.  Returns the same
+ * codes a load of that network would. */
+int bnc_plan_aos(const BncBionData* data, const BncCurrentStimulus* stim, uint32_t n_stim, BncNetInfo* info);
+
+/* Host-only .bion I/O with the reference loader's semantics: bnc_bion_load
+ * replaces bion_load_host (src/bion_loader_host.cpp:26-428; v10-v14 files with
+ * the v14 record sizes; same BION_ERR_* codes and index validation; arrays owned
+ * by the library until bnc_bion_unload, which replaces bion_unload_host);
+ * bnc_bion_save replaces bion_save (src/bion_loader_host.cpp:449-504, writes v14). */
+int bnc_bion_load(const char* filename, BncBionData* out);
+void bnc_bion_unload(BncBionData* data);
+int bnc_bion_save(const char* filename, const BncBionData* data);
+
 /* Writes the host AoS view to a .bion v14 file (reference bion_save layout). */
 int bnc_save_bion(void* sim, const char* filename);
 

@@ -792,3 +792,19 @@ double bo_log_d(double x) { return bo_log(x); }
 double bo_pow_d(double x, double y) { return bo_pow(x, y); }
 float bo_xorshift_f(uint32_t seed) { return bo_xorshift32_rnd(seed); }
 uint32_t bo_seed_bits(float V) { return bo_vm_seed_bits(V); }
+
+/* Known-answer hooks for the tests (reference tests/test_ghk_reference.cpp,
+ * tests/test_reference_ionics.cpp): the oracle's GHK flux terms and Nernst
+ * potential, and the physical constants they use (types.h:400-402). */
+double bo_ghk_mono_d(double V, double c_in, double c_out) { return bo_ghk_mono(V, c_in, c_out); }
+double bo_ghk_div_d(double V, double c_in, double c_out) { return bo_ghk_div(V, c_in, c_out); }
+double bo_ghk_anion_d(double V, double c_in, double c_out) { return bo_ghk_anion(V, c_in, c_out); }
+float bo_nernst_f(float intra, float extra, float valence) { return bo_nernst(intra, extra, valence); }
+double bo_const(int which) {
+    switch (which) {
+        case 0: return FARADAY_CONST;
+        case 1: return GAS_CONST;
+        case 2: return CELSIUS_37;
+        default: return 0.0;
+    }
+}

@@ -43,6 +43,11 @@ def oracle_lib():
         lib.bo_pow_d.argtypes = [C.c_double, C.c_double]; lib.bo_pow_d.restype = C.c_double
         lib.bo_xorshift_f.argtypes = [C.c_uint32]; lib.bo_xorshift_f.restype = C.c_float
         lib.bo_seed_bits.argtypes = [C.c_float]; lib.bo_seed_bits.restype = C.c_uint32
+        for name in ("bo_ghk_mono_d", "bo_ghk_div_d", "bo_ghk_anion_d"):
+            getattr(lib, name).argtypes = [C.c_double] * 3
+            getattr(lib, name).restype = C.c_double
+        lib.bo_nernst_f.argtypes = [C.c_float] * 3; lib.bo_nernst_f.restype = C.c_float
+        lib.bo_const.argtypes = [C.c_int]; lib.bo_const.restype = C.c_double
         _ora = lib
     return _ora
 

@@ -1,0 +1,72 @@
+"""Generates the golden fixtures in this folder from the reference's own CPU tick.
+
+The reference's core_run_tick (src/simulation_host.cpp:660-669) is compiled from
+its sources into oracle/_ref/libbiocore_ref.so by oracle/Makefile and run here on
+seeded networks from the project's generator; the resulting state is stored as
+.npz so that tests can pin the oracle (and the GPU path) to the reference on
+machines where the reference sources are absent.
+
+    python tests/golden/make_golden.py
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+DT = 0.025
+
+# name -> (generator parameters, ticks)
+CASES = {
+    "small_n8_s7": (dict(family=1, n_neurons=8, seed=7), 200),
+    "large_n4_s3": (dict(family=2, n_neurons=4, n_synapses=80, seed=3), 100),
+}
+
+
+def params(spec):
+    from bioneuroncore_b200 import NetgenParams
+    return NetgenParams(**spec)
+
+
+def run_reference(spec, ticks):
+    import ctypes as C
+    from bioneuroncore_b200 import Network
+    from oracle.oracle import Reference, reference_lib
+    net = Network(params(spec))
+    ref = Reference(net)
+    lib = reference_lib()
+    spikes = np.zeros(net.data.num_segments, np.uint32)
+    lib.core_enable_spike_count(spikes.ctypes.data, net.data.num_segments)
+    somata = np.flatnonzero(net.segments["segment_type"] == 1).astype(np.uint32)
+    trace = np.empty((ticks, somata.size), np.float64)
+    for t in range(ticks):
+        ref.run(1, DT)
+        trace[t] = net.segments["V_m"][somata]
+    lib.core_disable_spike_tracking()
+    seg = net.segments
+    syn = net.synapses
+    out = dict(
+        ticks=np.int64(ticks), dt=np.float32(DT), somata=somata, soma_trace=trace,
+        V=seg["V_m"].copy(), ion_in=seg["intra_ions"][:, :7].copy(), ion_out=seg["extra_ions"][:, :7].copy(),
+        ATP=seg["ATP_level"].astype(np.float64), spikes=spikes.copy(),
+        syn_weight=syn["weight"].astype(np.float64), syn_spine_Ca=syn["spine_Ca"].astype(np.float64),
+        syn_bouton_Ca=syn["bouton_Ca"].astype(np.float64),
+    )
+    out.update({"param_" + k: np.int64(v) for k, v in spec.items()})
+    return out
+
+
+def main():
+    from oracle.oracle import reference_available
+    if not reference_available():
+        raise SystemExit("oracle/_ref/libbiocore_ref.so is not built (make -C oracle)")
+    for name, (spec, ticks) in CASES.items():
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), **run_reference(spec, ticks))
+        print("wrote", name)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,40 @@
+"""The oracle against the reference-generated fixtures in tests/golden/.
+
+The fixtures hold the reference's own state (FP64 V_m and ions) after a few
+hundred ticks of seeded networks; the oracle keeps FP32 state, so the bar is
+the relative tolerance in tests/golden_cases.py, and spike counts must be equal.
+"""
+import numpy as np
+import pytest
+
+import golden_cases
+from oracle.oracle import Oracle, reference_available
+
+
+@pytest.mark.parametrize("name", golden_cases.cases())
+def test_oracle_matches_reference_fixture(name):
+    from bioneuroncore_b200 import Network, NetgenParams
+    g, spec = golden_cases.load(name)
+    net = Network(NetgenParams(**spec))
+    o = Oracle(net)
+    trace = o.trace(int(g["ticks"]), float(g["dt"]), g["somata"])
+    golden_cases.compare(g, trace, o.segment_field, o.synapse_field)
+
+
+def test_fixtures_exist():
+    assert set(golden_cases.cases()) >= {"small_n8_s7", "large_n4_s3"}
+
+
+@pytest.mark.skipif(not reference_available(), reason="reference CPU library not built here")
+def test_fixtures_are_reproducible_from_the_reference():
+    """Re-runs the reference for the smallest fixture and checks it reproduces bit for bit."""
+    import importlib.util
+    import os
+    spec_ = importlib.util.spec_from_file_location(
+        "make_golden", os.path.join(golden_cases.GOLDEN, "make_golden.py"))
+    mg = importlib.util.module_from_spec(spec_)
+    spec_.loader.exec_module(mg)
+    g, spec = golden_cases.load("large_n4_s3")
+    fresh = mg.run_reference(spec, int(g["ticks"]))
+    for k in ("V", "ion_in", "ion_out", "soma_trace", "spikes", "syn_weight"):
+        assert np.array_equal(fresh[k], g[k]), k

@@ -75,3 +75,22 @@ def test_large_set_bitexact():
         ora.run(step, DT)
         gpu.run_ticks(step, DT)
         _compare_all(ora, gpu, net.data.num_synapses, "large after +%d" % step)
+
+
+@pytest.mark.parametrize("name", __import__("golden_cases").cases())
+def test_gpu_matches_reference_fixture(name):
+    """The GPU path against the reference's own FP64 CPU tick (fixtures made by
+    tests/golden/make_golden.py), within the relative tolerance of golden_cases."""
+    import golden_cases
+    from bioneuroncore_b200 import Backend, Network, NetgenParams
+    g, spec = golden_cases.load(name)
+    net = Network(NetgenParams(**spec))
+    gpu = Backend()
+    gpu.load_network(net)
+    somata = g["somata"]
+    trace = np.empty((int(g["ticks"]), somata.size), np.float64)
+    for t in range(int(g["ticks"])):
+        gpu.run_ticks(1, float(g["dt"]))
+        trace[t] = gpu.segment_field("V")[somata]
+    n_syn = net.data.num_synapses
+    golden_cases.compare(g, trace, gpu.segment_field, lambda f: gpu.synapse_field(f, 0, n_syn))

@@ -1,0 +1,180 @@
+"""Host-side logic without a GPU: the seeded generator, the builder's planning
+(tiles, phase schedule, validation and the supported-type checks), and .bion
+I/O, the latter also against the reference's own loader when it is built here
+(bion_load_host / bion_save, src/bion_loader_host.cpp:26-504).
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from oracle.oracle import reference_available, REF_LIB
+
+BNC_ERR_UNSUPPORTED = -21
+BNC_ERR_FORMAT = -9
+BNC_BION_ERR_BAD_CONN = -6
+BNC_BION_ERR_BAD_MAGIC = -2
+BNC_BION_ERR_FILE_OPEN = -1
+
+
+def _net(**kw):
+    from bioneuroncore_b200 import Network, NetgenParams
+    return Network(NetgenParams(**kw))
+
+
+def _plan_aos(net):
+    from bioneuroncore_b200 import load_library, NetInfo
+    info = NetInfo()
+    rc = load_library().bnc_plan_aos(C.byref(net.data), net.stim_ptr, net.n_stim, C.byref(info))
+    return rc, info
+
+
+def _bytes(net):
+    return (net.segments.tobytes(), net.synapses.tobytes(), net.connections.tobytes(), net.stimuli.tobytes())
+
+
+def test_generator_is_deterministic_per_seed():
+    a = _net(family=1, n_neurons=6, seed=42)
+    b = _net(family=1, n_neurons=6, seed=42)
+    c = _net(family=1, n_neurons=6, seed=43)
+    assert _bytes(a) == _bytes(b)
+    assert _bytes(a)[0] != _bytes(c)[0]
+
+
+def test_small_family_shape():
+    """64 x 32-segment neurons: soma + 15-segment dendrite chain + 16-segment axon,
+    6 modifier kinds, 80% AMPA / 20% GABA-A synapses, stimuli on 10% of somata."""
+    net = _net(family=1, n_neurons=20, seed=1)
+    seg = net.segments
+    assert net.data.num_segments == 20 * 32
+    assert (seg["segment_type"][::32] == 1).all()
+    assert np.allclose(seg["V_m"], -65.0)
+    assert np.allclose(seg["intra_ions"][:, 0], 12.0) and np.allclose(seg["extra_ions"][:, 1], 4.0)
+    assert net.data.num_connections == 20 * 31
+    rtype = net.synapses["post_receptors"]["type"][:, 0]
+    assert set(np.unique(rtype)) <= {8, 11}
+    assert net.n_stim == 2
+    assert (net.stimuli["amplitude_pA"] == 200.0).all()
+
+
+def test_plan_of_generated_networks():
+    from bioneuroncore_b200 import plan_generated, NetgenParams, NET_SMALL, NET_LARGE, NET_TREES
+    inf = plan_generated(NetgenParams(family=NET_SMALL, n_neurons=64, seed=1))
+    assert inf.n_segments == 2048 and inf.n_connections == 64 * 31
+    assert inf.max_tile_segs <= 1024 and inf.n_tiles >= 2
+    assert inf.n_synapses == 400 and inf.flags & 1 and inf.flags & 2
+    big = plan_generated(NetgenParams(family=NET_LARGE, n_neurons=200, seed=1))
+    assert big.n_segments == 200 * 64 and big.n_receptors == big.n_synapses * 8
+    # 16 modifiers per segment from the large set, plus Cav2.1 on axon segments
+    assert big.n_items >= 16 * big.n_segments
+    assert big.algo_bytes_per_tick == pytest.approx(big.tile_bytes_per_tick + big.synapse_kernel_bytes_per_tick)
+    trees = plan_generated(NetgenParams(family=NET_TREES, n_neurons=2, tree_depth=9, seed=1))
+    assert trees.n_segments == 2 * 1023 and trees.max_tile_segs <= 1024
+
+
+def test_plan_aos_accepts_generated_network():
+    net = _net(family=1, n_neurons=4, seed=5)
+    rc, info = _plan_aos(net)
+    assert rc == 0
+    assert info.n_segments == 128
+
+
+def test_unsupported_modifier_type_is_rejected_not_skipped():
+    from bioneuroncore_b200 import last_error
+    net = _net(family=1, n_neurons=2, seed=5)
+    net.segments["modifiers"][3, 0]["type"] = 50   # no device model for this built-in ID
+    rc, _ = _plan_aos(net)
+    assert rc == BNC_ERR_UNSUPPORTED
+    assert "50" in last_error()
+
+
+def test_user_plugin_type_is_rejected():
+    from bioneuroncore_b200 import last_error
+    net = _net(family=1, n_neurons=2, seed=5)
+    net.segments["modifiers"][0, 1]["type"] = 7 + 0   # NaK pump is supported
+    assert _plan_aos(net)[0] == 0
+    net.segments["modifiers"][0, 1]["type"] = 20      # user ID range 0-127 without a device entry
+    assert _plan_aos(net)[0] == BNC_ERR_UNSUPPORTED
+    assert last_error()
+
+
+def test_electrical_synapse_is_rejected():
+    net = _net(family=1, n_neurons=4, seed=5)
+    net.synapses["type"][0] = 1
+    assert _plan_aos(net)[0] == BNC_ERR_UNSUPPORTED
+
+
+def test_modifier_count_out_of_range_is_a_format_error():
+    net = _net(family=1, n_neurons=2, seed=5)
+    net.segments["modifier_count"][1] = 33
+    assert _plan_aos(net)[0] == BNC_ERR_FORMAT
+
+
+def _lib():
+    from bioneuroncore_b200 import load_library
+    return load_library()
+
+
+def test_bion_roundtrip(tmp_path):
+    from bioneuroncore_b200.abi import BionData
+    net = _net(family=2, n_neurons=3, n_synapses=40, seed=9)
+    path = str(tmp_path / "net.bion").encode()
+    assert _lib().bnc_bion_save(path, C.byref(net.data)) == 0
+    back = BionData()
+    assert _lib().bnc_bion_load(path, C.byref(back)) == 0
+    try:
+        from bioneuroncore_b200.abi import view, SEGMENT_DTYPE, SYNAPSE_DTYPE
+        s = view(back.segments, SEGMENT_DTYPE, back.num_segments)
+        y = view(back.synapses, SYNAPSE_DTYPE, back.num_synapses)
+        assert back.num_segments == net.data.num_segments and back.num_synapses == 40
+        # intra_connection_ids are rebuilt on load, as the reference loader does
+        fields = [f for f in SEGMENT_DTYPE.names if f not in ("intra_connection_ids", "intra_connection_count")]
+        for f in fields:
+            assert s[f].tobytes() == net.segments[f].tobytes(), f
+        assert y.tobytes() == net.synapses.tobytes()
+    finally:
+        _lib().bnc_bion_unload(C.byref(back))
+
+
+def test_bion_errors(tmp_path):
+    from bioneuroncore_b200.abi import BionData
+    d = BionData()
+    assert _lib().bnc_bion_load(str(tmp_path / "missing.bion").encode(), C.byref(d)) == BNC_BION_ERR_FILE_OPEN
+    bad = tmp_path / "bad.bion"
+    bad.write_bytes(b"\0" * 200)
+    assert _lib().bnc_bion_load(str(bad).encode(), C.byref(d)) == BNC_BION_ERR_BAD_MAGIC
+    net = _net(family=1, n_neurons=2, seed=5)
+    net.connections["segment_b"][0] = 10 ** 6
+    p = str(tmp_path / "conn.bion").encode()
+    assert _lib().bnc_bion_save(p, C.byref(net.data)) == 0
+    assert _lib().bnc_bion_load(p, C.byref(d)) == BNC_BION_ERR_BAD_CONN
+
+
+@pytest.mark.skipif(not reference_available(), reason="reference CPU library not built here")
+def test_bion_files_interchange_with_the_reference_loader(tmp_path):
+    from bioneuroncore_b200.abi import BionData, view, SEGMENT_DTYPE
+    ref = C.CDLL(REF_LIB)
+    load = getattr(ref, "_Z14bion_load_hostPKcP8BionData")
+    save = getattr(ref, "_Z9bion_savePKcPK8BionData")
+    unload = getattr(ref, "_Z16bion_unload_hostP8BionData")
+    for f in (load, save):
+        f.argtypes = [C.c_char_p, C.c_void_p]
+        f.restype = C.c_int
+    unload.argtypes = [C.c_void_p]
+    net = _net(family=1, n_neurons=3, seed=2)
+    ours = str(tmp_path / "ours.bion").encode()
+    theirs = str(tmp_path / "theirs.bion").encode()
+    assert _lib().bnc_bion_save(ours, C.byref(net.data)) == 0
+    r = BionData()
+    assert load(ours, C.byref(r)) == 0            # the reference reads our file
+    assert save(theirs, C.byref(r)) == 0          # and writes it back
+    unload(C.byref(r))
+    b = BionData()
+    assert _lib().bnc_bion_load(theirs, C.byref(b)) == 0   # we read the reference's file
+    try:
+        s = view(b.segments, SEGMENT_DTYPE, b.num_segments)
+        assert s["V_m"].tobytes() == net.segments["V_m"].tobytes()
+        assert s["modifiers"].tobytes() == net.segments["modifiers"].tobytes()
+        assert b.num_synapses == net.data.num_synapses
+    finally:
+        _lib().bnc_bion_unload(C.byref(b))
