@@ -37,7 +37,9 @@ NEW_SYMBOLS = ["bnc_netgen_aos", "bnc_netgen_free", "bnc_last_error", "bnc_load_
                "bnc_run_ticks", "bnc_time_ticks", "bnc_sync_to_host", "bnc_read_segment_field",
                "bnc_read_synapse_field", "bnc_set_synapse_scale", "bnc_network_info", "bnc_save_bion",
                "bnc_plan_generated", "bnc_step_io", "bnc_profile_ticks", "bnc_run_ticks_static_scratch",
-               "bnc_plan_aos", "bnc_bion_load", "bnc_bion_unload", "bnc_bion_save"]
+               "bnc_plan_aos", "bnc_bion_load", "bnc_bion_unload", "bnc_bion_save", "bnc_load_ensemble_generated",
+               "bnc_load_ensemble_aos", "bnc_ensemble_member", "bnc_plan_ensemble_generated", "bnc_ensemble_params",
+               "bnc_run_ticks_graph"]
 
 
 class NetInfo(C.Structure):
@@ -53,6 +55,28 @@ def plan_generated(params):
     """Host-only planning of a generated network (no device needed); returns NetInfo."""
     inf = NetInfo()
     _check(load_library().bnc_plan_generated(C.byref(params), C.byref(inf)), "bnc_plan_generated")
+    return inf
+
+
+class EnsembleMember(C.Structure):
+    _fields_ = [(n, C.c_uint32) for n in ("seg_begin", "n_segments", "syn_begin", "n_synapses", "stim_begin",
+                                          "n_stimuli")]
+
+
+def ensemble_params(seed, n_members, min_segments=200, max_segments=20000):
+    """Seeded uneven ensemble (sizes log-uniform, gNa/gK/gleak/gCa x U[0.5, 2]); returns a
+    ctypes array of NetgenParams."""
+    arr = (NetgenParams * n_members)()
+    _check(load_library().bnc_ensemble_params(seed, n_members, min_segments, max_segments, arr),
+           "bnc_ensemble_params")
+    return arr
+
+
+def plan_ensemble(params):
+    """Host-only planning of a generated ensemble; returns NetInfo."""
+    arr = params if isinstance(params, C.Array) else (NetgenParams * len(params))(*params)
+    inf = NetInfo()
+    _check(load_library().bnc_plan_ensemble_generated(arr, len(arr), C.byref(inf)), "bnc_plan_ensemble_generated")
     return inf
 
 
@@ -91,6 +115,9 @@ def load_library(path=LIB_PATH):
         "bnc_run_ticks_static_scratch": ([vp, u32, f32], i32),
         "bnc_plan_aos": ([vp, vp, u32, vp], i32), "bnc_bion_load": ([C.c_char_p, vp], i32),
         "bnc_bion_unload": ([vp], None), "bnc_bion_save": ([C.c_char_p, vp], i32),
+        "bnc_load_ensemble_generated": ([vp, vp, u32], i32), "bnc_load_ensemble_aos": ([vp, vp, vp, vp, u32], i32),
+        "bnc_ensemble_member": ([vp, u32, vp], i32), "bnc_plan_ensemble_generated": ([vp, u32, vp], i32),
+        "bnc_ensemble_params": ([C.c_uint64, u32, u32, u32, vp], i32), "bnc_run_ticks_graph": ([vp, u32, f32], i32),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -197,6 +224,26 @@ class Backend:
     def run_ticks(self, n, dt):
         _check(self.lib.bnc_run_ticks(self.h, n, C.c_float(dt)), "bnc_run_ticks")
 
+    def run_ticks_graph(self, n, dt):
+        _check(self.lib.bnc_run_ticks_graph(self.h, n, C.c_float(dt)), "bnc_run_ticks_graph")
+
+    def load_ensemble(self, params):
+        arr = params if isinstance(params, C.Array) else (NetgenParams * len(params))(*params)
+        _check(self.lib.bnc_load_ensemble_generated(self.h, arr, len(arr)), "bnc_load_ensemble_generated")
+
+    def load_ensemble_networks(self, nets):
+        """Ensemble of host-AoS Networks (copied; the Networks stay valid)."""
+        from .abi import BionData
+        data = (BionData * len(nets))(*[n.data for n in nets])
+        stims = (C.c_void_p * len(nets))(*[n.stim_ptr for n in nets])
+        counts = (C.c_uint32 * len(nets))(*[n.n_stim for n in nets])
+        _check(self.lib.bnc_load_ensemble_aos(self.h, data, stims, counts, len(nets)), "bnc_load_ensemble_aos")
+
+    def ensemble_member(self, m):
+        out = EnsembleMember()
+        _check(self.lib.bnc_ensemble_member(self.h, m, C.byref(out)), "bnc_ensemble_member")
+        return out
+
     def time_ticks(self, n, dt):
         ms = C.c_float()
         _check(self.lib.bnc_time_ticks(self.h, n, C.c_float(dt), C.byref(ms)), "bnc_time_ticks")
@@ -246,4 +293,4 @@ class Backend:
 __all__ = ["Backend", "Network", "NetgenParams", "BionData", "BackendError", "load_library", "last_error",
            "NET_SMALL", "NET_LARGE", "NET_TREES", "NET_ENSEMBLE_MEMBER", "NET_ADJOINT", "NETGEN_NO_SYNAPSES",
            "NETGEN_NO_CONNECTIONS", "NETGEN_NO_STIMULI", "NETGEN_PERTURB_IONS", "SEG_FIELDS", "SYN_FIELDS",
-           "DROPIN_SYMBOLS", "NEW_SYMBOLS"]
+           "DROPIN_SYMBOLS", "NEW_SYMBOLS", "EnsembleMember", "ensemble_params", "plan_ensemble", "plan_generated"]

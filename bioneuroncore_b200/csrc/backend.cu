@@ -33,9 +33,16 @@ struct Backend {
     uint64_t tick = 0;
     uint64_t ticks_run = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // ensemble members (empty for a single network): ranges in original order
+    std::vector<BncEnsembleMember> members;
+    // captured tick loop (bnc_run_ticks_graph)
+    unsigned long long* clock = nullptr;   // device [2], owned by allocs
+    cudaGraphExec_t graph_exec = nullptr;
+    float graph_dt = 0.0f;
 
     ~Backend() {
         cudaSetDevice(device);
+        drop_graph();
         allocs.release();
         stim_allocs.release();
         free_aos();
@@ -50,7 +57,14 @@ struct Backend {
         std::memset(&aos, 0, sizeof(aos));
         owns_aos = false;
     }
+    void drop_graph() {
+        if (graph_exec) cudaGraphExecDestroy(graph_exec);
+        graph_exec = nullptr;
+    }
     void reset_network() {
+        drop_graph();
+        clock = nullptr;
+        members.clear();
         allocs.release();
         stim_allocs.release();
         free_aos();
@@ -158,6 +172,97 @@ struct HostNetSink : NetSink {
     void synapse(const BncSynapse& s) override { hostnet_add_synapse(*hn, s); }
     void stimulus(const BncCurrentStimulus& st) override { stim->push_back(st); }
 };
+// Appends networks one after another into one HostNet: every index a member
+// holds (segment ids, connection endpoints, synapse pre/post, stimulus targets) is
+// offset by the member's first segment; synapse ids are kept.
+struct EnsembleSink : NetSink {
+    HostNet* hn;
+    std::vector<BncCurrentStimulus>* stim;
+    uint32_t base = 0;
+    uint64_t n_conn = 0, n_syn = 0;
+    void begin(uint32_t, uint32_t, uint32_t n_connections, uint64_t n_synapses, uint32_t) override {
+        base = (uint32_t)hn->seg.size();
+        hn->num_connections += n_connections;
+        n_conn = n_connections;
+        n_syn = n_synapses;
+    }
+    void neuron(const BncNeuron&) override {}
+    void segment(const BncSegment& s) override {
+        BncSegment t = s;
+        t.id += base;
+        hostnet_add_segment(*hn, t);
+    }
+    void connection(const BncIntraConnection& c) override {
+        BncIntraConnection t = c;
+        t.segment_a += base;
+        t.segment_b += base;
+        hn->conn.push_back(t);
+    }
+    void synapse(const BncSynapse& y) override {
+        BncSynapse t = y;
+        t.pre_segment += base;
+        t.post_segment += base;
+        hostnet_add_synapse(*hn, t);
+    }
+    void stimulus(const BncCurrentStimulus& st) override {
+        BncCurrentStimulus t = st;
+        t.segment_id += base;
+        stim->push_back(t);
+    }
+};
+
+// Whether a member has intra-connections and synapses: network-wide switches of the
+// reference tick (step 2.5 runs only with connections, diffusion_kernel.h:118; step 3
+// resets neurotransmitter only with synapses, simulation_host.cpp:328).
+struct MemberSwitches { bool conn, syn; };
+
+// Records the member that was just appended (its ranges start at the given offsets)
+// and checks that it agrees with member 0 on the switches.
+static int add_member(std::vector<BncEnsembleMember>& members, std::vector<MemberSwitches>& sw, const HostNet& hn,
+                      size_t n_stim_total, uint32_t seg_begin, uint32_t syn_begin, uint32_t stim_begin,
+                      uint64_t n_valid_conn) {
+    BncEnsembleMember m;
+    m.seg_begin = seg_begin;
+    m.n_segments = (uint32_t)hn.seg.size() - seg_begin;
+    m.syn_begin = syn_begin;
+    m.n_synapses = (uint32_t)hn.syn.size() - syn_begin;
+    m.stim_begin = stim_begin;
+    m.n_stimuli = (uint32_t)(n_stim_total - stim_begin);
+    if (m.n_segments == 0) { set_error("ensemble member %zu has no segments", members.size()); return BNC_ERR_ARG; }
+    MemberSwitches w{n_valid_conn > 0, m.n_synapses > 0};
+    if (!sw.empty() && (w.conn != sw[0].conn || w.syn != sw[0].syn)) {
+        set_error("ensemble member %zu %s intra-connections and %s synapses, member 0 %s and %s: members must "
+                  "agree on both", members.size(), w.conn ? "has" : "has no", w.syn ? "has" : "has no",
+                  sw[0].conn ? "has" : "has not", sw[0].syn ? "has" : "has not");
+        return BNC_ERR_UNSUPPORTED;
+    }
+    members.push_back(m);
+    sw.push_back(w);
+    return BNC_OK;
+}
+
+// Streams generated members into one HostNet.
+static int gather_generated(const BncNetgenParams* params, uint32_t n, HostNet* hn, std::vector<BncCurrentStimulus>* stim,
+                            std::vector<BncEnsembleMember>* members) {
+    if (!params || n == 0) { set_error("ensemble: no members"); return BNC_ERR_ARG; }
+    std::vector<MemberSwitches> sw;
+    EnsembleSink sink;
+    sink.hn = hn;
+    sink.stim = stim;
+    for (uint32_t m = 0; m < n; m++) {
+        const uint32_t seg0 = (uint32_t)hn->seg.size(), syn0 = (uint32_t)hn->syn.size(), st0 = (uint32_t)stim->size();
+        NetShape shape;
+        int rc = generate_network(params[m], sink, &shape);
+        if (rc != BNC_OK) { set_error("ensemble member %u: invalid generator parameters", m); return rc; }
+        if ((uint64_t)hn->seg.size() >= (1ull << 31)) { set_error("ensemble too large"); return BNC_ERR_ARG; }
+        rc = add_member(*members, sw, *hn, stim->size(), seg0, syn0, st0, sink.n_conn);
+        if (rc != BNC_OK) return rc;
+    }
+    hn->num_segments = (uint32_t)hn->seg.size();
+    hn->num_synapses = (uint32_t)hn->syn.size();
+    return BNC_OK;
+}
+
 }  // namespace
 
 static int load_common(Backend* b, BncBionData& aos, bool keep_aos) {
@@ -204,6 +309,59 @@ static int run_ticks(Backend* b, uint32_t n, float dt) {
         b->ticks_run++;
     }
     return BNC_OK;
+}
+
+// Ticks per captured graph: each replay covers this many ticks (two kernels and a
+// clock advance per tick); the remainder of a call runs as plain launches.
+constexpr uint32_t kGraphTicks = 32;
+
+static int capture_graph(Backend* b, float dt) {
+    b->drop_graph();
+    if (!b->clock) {
+        b->clock = static_cast<unsigned long long*>(b->allocs.alloc(2 * sizeof(unsigned long long)));
+        if (!b->clock) { set_error("device allocation of the tick clock failed"); return BNC_ERR_ALLOC; }
+    }
+    cudaError_t e = prepare_tick(b->dev, b->host, b->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "tick set-up");
+    NetDev d = b->dev;
+    d.clock = b->clock;
+    e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamBeginCapture");
+    cudaError_t le = cudaSuccess;
+    for (uint32_t t = 0; t < kGraphTicks && le == cudaSuccess; t++) {
+        le = enqueue_tick(d, b->host, dt, 0, 0, b->stream);
+        if (le == cudaSuccess) le = launch_advance_clock(b->clock, b->stream);
+    }
+    cudaGraph_t g = nullptr;
+    e = cudaStreamEndCapture(b->stream, &g);
+    if (le != cudaSuccess || e != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        return cuda_fail(le != cudaSuccess ? le : e, "tick loop capture");
+    }
+    e = cudaGraphInstantiate(&b->graph_exec, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) { b->graph_exec = nullptr; return cuda_fail(e, "cudaGraphInstantiate"); }
+    b->graph_dt = dt;
+    return BNC_OK;
+}
+
+static int run_ticks_graph(Backend* b, uint32_t n, float dt) {
+    if (!b->loaded) { set_error("no network loaded"); return BNC_ERR_STATE; }
+    if (b->failed) { set_error("backend is in a failed state after a device error"); return BNC_ERR_STATE; }
+    cudaSetDevice(b->device);
+    const uint32_t reps = n / kGraphTicks;
+    if (reps > 0) {
+        if (!b->graph_exec || b->graph_dt != dt) {
+            int rc = capture_graph(b, dt);
+            if (rc != BNC_OK) return rc;
+        }
+        cudaError_t e = launch_set_clock(b->clock, b->tick, b->ticks_run, b->stream);
+        for (uint32_t r = 0; r < reps && e == cudaSuccess; r++) e = cudaGraphLaunch(b->graph_exec, b->stream);
+        if (e != cudaSuccess) { b->failed = true; return cuda_fail(e, "graph launch"); }
+        b->tick += (uint64_t)reps * kGraphTicks;
+        b->ticks_run += (uint64_t)reps * kGraphTicks;
+    }
+    return run_ticks(b, n - reps * kGraphTicks, dt);
 }
 
 static int sync_stream(Backend* b) {
@@ -447,6 +605,88 @@ int bnc_plan_generated(const BncNetgenParams* p, BncNetInfo* info) {
     int rc = generate_network(*p, sink, &shape);
     if (rc != BNC_OK) { set_error("bnc_plan_generated: invalid parameters"); return rc; }
     return plan_info(hn, stim, info);
+}
+
+int bnc_load_ensemble_generated(void* sim, const BncNetgenParams* members, uint32_t n_members) {
+    if (!sim) { set_error("null handle"); return BNC_ERR_ARG; }
+    Backend* b = static_cast<Backend*>(sim);
+    b->reset_network();
+    HostNet hn;
+    std::vector<BncEnsembleMember> mem;
+    int rc = gather_generated(members, n_members, &hn, &b->stim.current, &mem);
+    if (rc != BNC_OK) { b->reset_network(); return rc; }
+    cudaSetDevice(b->device);
+    rc = build_network(hn, b->stim, &b->dev, &b->host, &b->allocs);
+    if (rc != BNC_OK) { b->reset_network(); return rc; }
+    b->members = std::move(mem);
+    b->loaded = true;
+    return BNC_OK;
+}
+
+int bnc_load_ensemble_aos(void* sim, const BncBionData* members, const BncCurrentStimulus* const* stim,
+                          const uint32_t* n_stim, uint32_t n_members) {
+    if (!sim || !members || n_members == 0) { set_error("bnc_load_ensemble_aos: null argument"); return BNC_ERR_ARG; }
+    Backend* b = static_cast<Backend*>(sim);
+    b->reset_network();
+    HostNet hn;
+    std::vector<BncEnsembleMember> mem;
+    std::vector<MemberSwitches> sw;
+    EnsembleSink sink;
+    sink.hn = &hn;
+    sink.stim = &b->stim.current;
+    for (uint32_t m = 0; m < n_members; m++) {
+        const BncBionData& d = members[m];
+        if (!d.segments || d.num_segments == 0) { b->reset_network(); set_error("ensemble member %u has no segments", m); return BNC_ERR_ARG; }
+        const uint32_t seg0 = (uint32_t)hn.seg.size(), syn0 = (uint32_t)hn.syn.size();
+        const uint32_t st0 = (uint32_t)b->stim.current.size();
+        uint32_t ns = (stim && n_stim && stim[m]) ? n_stim[m] : 0;
+        sink.begin(d.num_neurons, d.num_segments, d.num_connections, d.num_synapses, ns);
+        uint64_t valid_conn = 0;
+        for (uint32_t i = 0; i < d.num_segments; i++) sink.segment(d.segments[i]);
+        for (uint32_t c = 0; c < d.num_connections; c++) {
+            if (d.connections[c].segment_a < d.num_segments && d.connections[c].segment_b < d.num_segments) valid_conn++;
+            sink.connection(d.connections[c]);
+        }
+        for (uint32_t k = 0; k < d.num_synapses; k++) sink.synapse(d.synapses[k]);
+        for (uint32_t k = 0; k < ns; k++) sink.stimulus(stim[m][k]);
+        int rc = add_member(mem, sw, hn, b->stim.current.size(), seg0, syn0, st0, valid_conn);
+        if (rc != BNC_OK) { b->reset_network(); return rc; }
+    }
+    cudaSetDevice(b->device);
+    int rc = build_network(hn, b->stim, &b->dev, &b->host, &b->allocs);
+    if (rc != BNC_OK) { b->reset_network(); return rc; }
+    b->members = std::move(mem);
+    b->loaded = true;
+    return BNC_OK;
+}
+
+int bnc_ensemble_member(void* sim, uint32_t member, BncEnsembleMember* out) {
+    if (!sim || !out) { set_error("null argument"); return BNC_ERR_ARG; }
+    Backend* b = static_cast<Backend*>(sim);
+    if (member >= b->members.size()) {
+        set_error("ensemble member %u out of range (%zu members loaded)", member, b->members.size());
+        return BNC_ERR_ARG;
+    }
+    *out = b->members[member];
+    return BNC_OK;
+}
+
+int bnc_plan_ensemble_generated(const BncNetgenParams* members, uint32_t n_members, BncNetInfo* info) {
+    if (!members || !info) { set_error("bnc_plan_ensemble_generated: null argument"); return BNC_ERR_ARG; }
+    HostNet hn;
+    Stimuli st;
+    std::vector<BncEnsembleMember> mem;
+    int rc = gather_generated(members, n_members, &hn, &st.current, &mem);
+    if (rc != BNC_OK) return rc;
+    return plan_info(hn, st, info);
+}
+
+int bnc_run_ticks_graph(void* sim, uint32_t n_ticks, float dt) {
+    if (!sim) { set_error("null handle"); return BNC_ERR_ARG; }
+    Backend* b = static_cast<Backend*>(sim);
+    int rc = run_ticks_graph(b, n_ticks, dt);
+    if (rc != BNC_OK) return rc;
+    return sync_stream(b);
 }
 
 int bnc_plan_aos(const BncBionData* data, const BncCurrentStimulus* stim, uint32_t n_stim, BncNetInfo* info) {

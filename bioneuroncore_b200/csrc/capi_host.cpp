@@ -1,5 +1,6 @@
 // capi_host.cpp -- host-only C ABI: the synthetic generator's AoS output and the
 // per-thread error message.  No CUDA calls, so these work on a machine without a GPU.
+#include <cmath>
 #include <cstring>
 #include <cstdio>
 #include <new>
@@ -87,6 +88,38 @@ int bnc_netgen_aos(const BncNetgenParams* p, BncBionData* out, BncCurrentStimulu
         }
     }
     if (n_stim) *n_stim = (uint32_t)sink.stim.size();
+    return BNC_OK;
+}
+
+int bnc_ensemble_params(uint64_t seed, uint32_t n_members, uint32_t min_segments, uint32_t max_segments,
+                        BncNetgenParams* out) {
+    if (!out || n_members == 0 || min_segments < 32 || max_segments < min_segments) {
+        set_error("bnc_ensemble_params: need n_members > 0 and 32 <= min_segments <= max_segments");
+        return BNC_ERR_ARG;
+    }
+    // SplitMix64 over (seed, member): sizes, conductance factors and member seeds
+    auto mix = [](uint64_t z) {
+        z += 0x9E3779B97F4A7C15ull;
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        return z ^ (z >> 31);
+    };
+    auto u01 = [](uint64_t z) { return (double)(z >> 11) * (1.0 / 9007199254740992.0); };
+    const double lo = std::log((double)min_segments), hi = std::log((double)max_segments);
+    for (uint32_t m = 0; m < n_members; m++) {
+        uint64_t s = mix(seed * 0x100000001B3ull + m);
+        BncNetgenParams& p = out[m];
+        std::memset(&p, 0, sizeof(p));
+        p.family = BNC_NET_ENSEMBLE_MEMBER;
+        double segs = std::exp(lo + (hi - lo) * u01(s));
+        uint32_t nn = (uint32_t)(segs / 32.0 + 0.5);
+        p.n_neurons = nn < 1 ? 1 : nn;
+        for (int c = 0; c < 4; c++) {
+            s = mix(s);
+            p.conductance_scale[c] = (float)(0.5 + 1.5 * u01(s));   // U[0.5, 2]
+        }
+        p.seed = mix(s ^ 0xD1B54A32D192ED03ull);
+    }
     return BNC_OK;
 }
 

@@ -120,6 +120,10 @@ struct NetDev {
     uint8_t* dl_nt;
     uint32_t* spike_count;    // [n_seg]
     int* err_flag;            // device-side error report (0 = ok)
+    // Captured tick loops: when set, the kernels take the tick from clock[0] and the
+    // first-tick flag from clock[1] == 0 (ticks run so far) instead of their launch
+    // parameters, and k_advance_clock moves both on after each tick.
+    unsigned long long* clock;
 };
 
 // Host copy of everything the exporter needs to map device state back.
@@ -166,7 +170,15 @@ int upload_stimuli(const Stimuli& stim, NetHost& host, NetDev* dev, DeviceAllocs
 // Writes device state back into the AoS arrays.
 int export_network(const NetDev& dev, const NetHost& host, uint64_t ticks_run, BncBionData* aos);
 
-// Kernel launchers (kernels.cu).
+// Kernel launchers (tile.cu, synapse.cu).  prepare_tick does the per-device and
+// per-network set-up that must not happen inside a stream capture (constant tables,
+// the tile kernel's shared-memory limit); enqueue_tick only enqueues kernels.
+cudaError_t prepare_tick(const NetDev& dev, const NetHost& host, cudaStream_t stream);
+cudaError_t enqueue_tick(const NetDev& dev, const NetHost& host, float dt, unsigned long long tick, int first_tick,
+                         cudaStream_t stream);
+cudaError_t launch_set_clock(unsigned long long* clock, unsigned long long tick, unsigned long long ticks_run,
+                             cudaStream_t stream);
+cudaError_t launch_advance_clock(unsigned long long* clock, cudaStream_t stream);
 cudaError_t launch_tick(const NetDev& dev, const NetHost& host, float dt, unsigned long long tick,
                         int first_tick, cudaStream_t stream);
 cudaError_t launch_tile(const NetDev& dev, const NetHost& host, float dt, unsigned long long tick,

@@ -35,6 +35,10 @@ k_synapse(NetDev d, float dt, unsigned long long tick, int first_tick) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t N = d.n_seg;
     if (i >= N) return;
+    if (d.clock) {
+        tick = d.clock[0];
+        first_tick = d.clock[1] == 0 ? 1 : 0;
+    }
     const uint8_t sfl = d.sflags[i];
     const bool syn_on = (d.flags & NF_SYNAPSES) != 0;
     float ntv[15];
@@ -276,6 +280,28 @@ k_synapse(NetDev d, float dt, unsigned long long tick, int first_tick) {
 cudaError_t launch_synapse(const NetDev& dev, float dt, unsigned long long tick, int first_tick,
                            cudaStream_t stream) {
     k_synapse<<<(dev.n_seg + 255) / 256, 256, 0, stream>>>(dev, dt, tick, first_tick);
+    return cudaGetLastError();
+}
+
+// The device clock of captured tick loops: [0] the tick, [1] ticks run so far.
+__global__ void k_set_clock(unsigned long long* clock, unsigned long long tick, unsigned long long ticks_run) {
+    clock[0] = tick;
+    clock[1] = ticks_run;
+}
+
+__global__ void k_advance_clock(unsigned long long* clock) {
+    clock[0] += 1;
+    clock[1] += 1;
+}
+
+cudaError_t launch_set_clock(unsigned long long* clock, unsigned long long tick, unsigned long long ticks_run,
+                             cudaStream_t stream) {
+    k_set_clock<<<1, 1, 0, stream>>>(clock, tick, ticks_run);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_advance_clock(unsigned long long* clock, cudaStream_t stream) {
+    k_advance_clock<<<1, 1, 0, stream>>>(clock);
     return cudaGetLastError();
 }
 

@@ -165,6 +165,7 @@ k_tile(NetDev d, float dt, unsigned long long tick, uint32_t S, uint32_t E) {
     const int nth = blockDim.x;
     const uint32_t tile = blockIdx.x;
     const uint32_t N = d.n_seg;
+    if (d.clock) tick = d.clock[0];
     const uint32_t s0 = d.tile_seg_beg[tile];
     const int ns = (int)(d.tile_seg_beg[tile + 1] - s0);
     const uint32_t e0 = d.tile_edge_beg[tile];
@@ -567,18 +568,36 @@ static cudaError_t init_tables(cudaStream_t stream) {
     return e;
 }
 
-cudaError_t launch_tile(const NetDev& dev, const NetHost& host, float dt, unsigned long long tick,
-                        cudaStream_t stream) {
+cudaError_t prepare_tick(const NetDev& dev, const NetHost& host, cudaStream_t stream) {
+    (void)dev;
     cudaError_t e = init_tables(stream);
     if (e != cudaSuccess) return e;
-    const uint32_t S = host.max_tile_segs, E = host.max_tile_edges;
-    const size_t smem = tile_smem_bytes(S, E);
-    if (smem > 48 * 1024) {
+    const size_t smem = tile_smem_bytes(host.max_tile_segs, host.max_tile_edges);
+    if (smem > 48 * 1024)
         e = cudaFuncSetAttribute(k_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-    }
-    k_tile<<<dev.n_tiles, kTileThreads, smem, stream>>>(dev, dt, tick, S, E);
+    return e;
+}
+
+static void enqueue_tile(const NetDev& dev, const NetHost& host, float dt, unsigned long long tick,
+                         cudaStream_t stream) {
+    const uint32_t S = host.max_tile_segs, E = host.max_tile_edges;
+    k_tile<<<dev.n_tiles, kTileThreads, tile_smem_bytes(S, E), stream>>>(dev, dt, tick, S, E);
+}
+
+cudaError_t launch_tile(const NetDev& dev, const NetHost& host, float dt, unsigned long long tick,
+                        cudaStream_t stream) {
+    cudaError_t e = prepare_tick(dev, host, stream);
+    if (e != cudaSuccess) return e;
+    enqueue_tile(dev, host, dt, tick, stream);
     return cudaGetLastError();
+}
+
+cudaError_t enqueue_tick(const NetDev& dev, const NetHost& host, float dt, unsigned long long tick, int first_tick,
+                         cudaStream_t stream) {
+    enqueue_tile(dev, host, dt, tick, stream);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    return launch_synapse(dev, dt, tick, first_tick, stream);
 }
 
 cudaError_t launch_tick(const NetDev& dev, const NetHost& host, float dt, unsigned long long tick, int first_tick,

@@ -202,6 +202,41 @@ int bnc_network_info(void* sim, BncNetInfo* info);
  * schedule, CSRs) without a device; fills `info` (no upload, no CUDA call). */
 int bnc_plan_generated(const BncNetgenParams* p, BncNetInfo* info);
 
+/* ---- Batched ensembles: many independent networks in one device structure ----
+ * Members are concatenated in the given order (segments, connections, synapses
+ * and stimuli keep their order inside each member, indices offset by the member's
+ * first segment) and run by the same two kernels per tick: one launch covers every
+ * member.  Each member keeps its own synapse ids, so its release stream is the one
+ * it has when run alone, and every member's state evolves exactly as in a separate
+ * run.  The reference has no such call: it runs parameter sweeps as separate
+ * processes (src/daemon_server.cpp:1164-1290).  Members must agree on whether they
+ * have intra-connections and on whether they have synapses (network-wide switches
+ * of the reference tick); BNC_ERR_UNSUPPORTED otherwise.  Segment and synapse
+ * fields of a member are the ranges bnc_ensemble_member reports within the
+ * bnc_read_*_field arrays. */
+typedef struct {
+    uint32_t seg_begin, n_segments;
+    uint32_t syn_begin, n_synapses;
+    uint32_t stim_begin, n_stimuli;
+} BncEnsembleMember;
+int bnc_load_ensemble_generated(void* sim, const BncNetgenParams* members, uint32_t n_members);
+int bnc_load_ensemble_aos(void* sim, const BncBionData* members, const BncCurrentStimulus* const* stim,
+                          const uint32_t* n_stim, uint32_t n_members);
+int bnc_ensemble_member(void* sim, uint32_t member, BncEnsembleMember* out);
+/* Host-only planning of a generated ensemble (no device). */
+int bnc_plan_ensemble_generated(const BncNetgenParams* members, uint32_t n_members, BncNetInfo* info);
+/* Host-only: parameters of a seeded uneven ensemble: member sizes log-uniform in
+ * [min_segments, max_segments] (32-segment neurons of BNC_NET_ENSEMBLE_MEMBER),
+ * gNa/gK/gleak/gCa scaled by independent U[0.5, 2] factors, one seed per member. */
+int bnc_ensemble_params(uint64_t seed, uint32_t n_members, uint32_t min_segments, uint32_t max_segments,
+                        BncNetgenParams* out);
+
+/* Runs n ticks with the tick loop captured once in a CUDA graph (32 ticks per
+ * replay; the tick counter lives on the device) -- same results as bnc_run_ticks,
+ * fewer launch round trips for small networks and ensembles.  The graph is
+ * re-captured when dt changes or a network is loaded. */
+int bnc_run_ticks_graph(void* sim, uint32_t n_ticks, float dt);
+
 /* Host-only: runs the builder's planning on AoS arrays in memory (validation,
  * supported-type checks, tiles, schedule) without a device.  Returns the same
  * codes a load of that network would. */

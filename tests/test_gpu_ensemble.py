@@ -1,0 +1,86 @@
+"""Batched ensembles and the captured tick loop, on the GPU, through the C ABI.
+
+An ensemble is one device structure holding many independent networks; every
+member must evolve exactly as it does when simulated alone (same kernels, same
+per-member synapse ids and hence the same release stream), so the bar is bit
+equality per member.  The captured loop (bnc_run_ticks_graph) must equal plain
+launches bit for bit, including across calls (the tick counter lives on the
+device there).
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+DT = 0.025
+SEG = [("V", 0), ("ion_in", 0), ("ion_in", 1), ("ion_in", 2), ("ion_out", 1), ("ATP", 0), ("spikes", 0),
+       ("neurotransmitter", 0), ("mod_state", 0), ("mod_state", 1), ("mod_state", 9)]
+SYN = [("bouton_Ca", 0), ("spine_Ca", 0), ("weight", 0), ("refractory", 0), ("cleft", 0),
+       ("receptor_state", 0)]
+
+
+def _same(a, b, what):
+    a = np.asarray(a, np.float32)
+    b = np.asarray(b, np.float32)
+    eq = (a.view(np.uint32) == b.view(np.uint32)) | (np.isnan(a) & np.isnan(b))
+    assert eq.all(), "%s: %d of %d differ (first at %d: %r vs %r)" % (
+        what, int((~eq).sum()), a.size, int(np.argmax(~eq)), a[np.argmax(~eq)], b[np.argmax(~eq)])
+
+
+def test_ensemble_members_match_separate_runs():
+    from bioneuroncore_b200 import Backend, ensemble_params
+    ps = ensemble_params(11, 5, 64, 1200)
+    ens = Backend()
+    ens.load_ensemble(ps)
+    singles = []
+    for p in ps:
+        b = Backend()
+        b.load_generated(p)
+        singles.append(b)
+    for step in (1, 24):
+        ens.run_ticks(step, DT)
+        for b in singles:
+            b.run_ticks(step, DT)
+        for f, i in SEG:
+            whole = ens.segment_field(f, i)
+            for m, b in enumerate(singles):
+                r = ens.ensemble_member(m)
+                _same(whole[r.seg_begin:r.seg_begin + r.n_segments], b.segment_field(f, i),
+                      "member %d %s[%d] after +%d" % (m, f, i, step))
+        n_total = ens.info().n_synapses
+        for f, i in SYN:
+            whole = ens.synapse_field(f, i, n_total)
+            for m, b in enumerate(singles):
+                r = ens.ensemble_member(m)
+                _same(whole[r.syn_begin:r.syn_begin + r.n_synapses], b.synapse_field(f, i),
+                      "member %d synapse %s[%d] after +%d" % (m, f, i, step))
+
+
+def test_ensemble_of_host_networks_matches_generated_ensemble():
+    from bioneuroncore_b200 import Backend, Network, ensemble_params
+    ps = ensemble_params(5, 3, 64, 400)
+    a, b = Backend(), Backend()
+    a.load_ensemble(ps)
+    nets = [Network(p) for p in ps]
+    b.load_ensemble_networks(nets)
+    a.run_ticks(10, DT)
+    b.run_ticks(10, DT)
+    for f, i in SEG:
+        _same(a.segment_field(f, i), b.segment_field(f, i), "%s[%d]" % (f, i))
+
+
+@pytest.mark.parametrize("family", ["small", "large"])
+def test_graph_ticks_match_plain_ticks(family):
+    from bioneuroncore_b200 import Backend, NetgenParams, NET_SMALL, NET_LARGE
+    p = NetgenParams(family=NET_SMALL if family == "small" else NET_LARGE, n_neurons=10, n_synapses=200, seed=4)
+    g, r = Backend(), Backend()
+    g.load_generated(p)
+    r.load_generated(p)
+    for n in (70, 40, 3):        # two replays + 6 plain; one replay + 8 plain; plain only
+        g.run_ticks_graph(n, DT)
+        r.run_ticks(n, DT)
+        assert g.info().ticks == r.info().ticks
+        for f, i in SEG:
+            _same(g.segment_field(f, i), r.segment_field(f, i), "%s %s[%d] after %d" % (family, f, i, n))
+        for f, i in SYN:
+            _same(g.synapse_field(f, i), r.synapse_field(f, i), "%s synapse %s[%d]" % (family, f, i))

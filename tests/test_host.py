@@ -178,3 +178,37 @@ def test_bion_files_interchange_with_the_reference_loader(tmp_path):
         assert b.num_synapses == net.data.num_synapses
     finally:
         _lib().bnc_bion_unload(C.byref(b))
+
+
+def test_ensemble_params_are_seeded_and_in_range():
+    from bioneuroncore_b200 import ensemble_params
+    a = ensemble_params(7, 64, 200, 20000)
+    b = ensemble_params(7, 64, 200, 20000)
+    c = ensemble_params(8, 64, 200, 20000)
+    assert bytes(a) == bytes(b) and bytes(a) != bytes(c)
+    segs = np.array([m.n_neurons * 32 for m in a])
+    assert segs.min() >= 200 - 16 and segs.max() <= 20000 + 16
+    assert len(set(m.seed for m in a)) == 64
+    scales = np.array([list(m.conductance_scale) for m in a])
+    assert scales.min() >= 0.5 and scales.max() <= 2.0
+    assert all(m.family == 4 for m in a)
+
+
+def test_ensemble_plan_is_the_union_of_its_members():
+    from bioneuroncore_b200 import ensemble_params, plan_ensemble, plan_generated
+    ps = ensemble_params(3, 5, 64, 2000)
+    inf = plan_ensemble(ps)
+    singles = [plan_generated(p) for p in ps]
+    assert inf.n_segments == sum(x.n_segments for x in singles)
+    assert inf.n_synapses == sum(x.n_synapses for x in singles)
+    assert inf.n_items == sum(x.n_items for x in singles)
+    assert inf.n_tiles <= sum(x.n_tiles for x in singles)
+
+
+def test_ensemble_members_must_agree_on_the_network_switches():
+    from bioneuroncore_b200 import ensemble_params, plan_ensemble, BackendError, last_error
+    ps = ensemble_params(3, 3, 64, 600)
+    ps[1].flags = 1   # BNC_NETGEN_NO_SYNAPSES
+    with pytest.raises(BackendError):
+        plan_ensemble(ps)
+    assert "member 1" in last_error()
