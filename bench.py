@@ -51,6 +51,9 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=100)
+    ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--ens-members", type=int, default=512)
+    ap.add_argument("--ens-ticks", type=int, default=64)
     return ap.parse_args()
 
 
@@ -214,6 +217,48 @@ def run_reference_arm(a):
     return 0
 
 
+def run_ensemble(a, device):
+    """Batched ensemble: a.ens_members independent networks of uneven size (segments
+    log-uniform in [200, 20000], gNa/gK/gleak/gCa x U[0.5, 2], one seed each) in one
+    device structure -- grouping autotuned on a sample, tick loop captured in a CUDA
+    graph -- against the same networks run one after another with plain launches.
+    Both legs are device-timed with CUDA events over a.ens_ticks ticks after warm-up."""
+    from bioneuroncore_b200 import Backend, ensemble_params
+    ps = ensemble_params(a.seed, a.ens_members, 200, 20000)
+    ens = Backend(device)
+    t0 = time.perf_counter()
+    tune = ens.load_ensemble_tuned(ps, 32, DT)
+    setup_s = time.perf_counter() - t0
+    info = ens.info()
+    ens.run_ticks_graph(max(a.warmup, 3), DT)
+    ms_ens = ens.time_ticks_graph(a.ens_ticks, DT)
+    ens.close()
+    ms_seq = 0.0
+    seq_segments = 0
+    for p in ps:
+        b = Backend(device)
+        b.load_generated(p)
+        b.run_ticks(max(a.warmup, 3), DT)
+        ms_seq += b.time_ticks(a.ens_ticks, DT)
+        seq_segments += b.info().n_segments
+        b.close()
+    assert seq_segments == info.n_segments
+    rate_ens = info.n_segments * a.ens_ticks / (ms_ens / 1000.0)
+    rate_seq = info.n_segments * a.ens_ticks / (ms_seq / 1000.0)
+    return {
+        "workload": "%d networks, 200-20000 segments each (log-uniform), %d segments in total, conductances "
+                    "x U[0.5, 2], own seeds" % (a.ens_members, info.n_segments),
+        "metric": "segment-ticks/s", "ticks": a.ens_ticks, "value": rate_ens, "ms_per_tick": ms_ens / a.ens_ticks,
+        "sequential_value": rate_seq, "sequential_ms_per_tick": ms_seq / a.ens_ticks,
+        "speedup_vs_sequential": rate_ens / rate_seq,
+        "launch": "one structure, CUDA-graph tick loop (32 ticks per replay)",
+        "sequential_launch": "each network alone, plain launches (2 per tick), device time summed",
+        "grouping": {"warp_cap": tune.warp_cap, "tile_segs": tune.tile_segs,
+                     "candidates_tried": tune.candidates_tried, "sample_members": tune.sample_members},
+        "setup_s": round(setup_s, 1),
+    }
+
+
 def main():
     a = parse_args()
     if a.impl == "reference":
@@ -283,6 +328,11 @@ def main():
                 "tick_bytes": info.algo_bytes_per_tick,
                 "tick_frac": info.algo_bytes_per_tick / (ms_max / a.steps / 1000.0) / 1e9 / peak}
 
+    ensemble = None
+    if not a.no_ensemble:
+        b.close()   # free the large network's device memory first
+        ensemble = run_ensemble(a, local_rank if world > 1 else 0)
+
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         try:
@@ -303,7 +353,7 @@ def main():
                        "l2": "inputs larger than L2 (device state ~8 GB per GPU)",
                        "tiles": info.n_tiles, "phases": info.n_phases, "setup_s": round(setup_s, 1)},
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,
-            "gpu_launches": 2 * a.steps,
+            "gpu_launches": 2 * a.steps, "ensemble": ensemble,
         }
         print(json.dumps(line), flush=True)
     b.close()

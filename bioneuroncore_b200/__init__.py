@@ -39,7 +39,7 @@ NEW_SYMBOLS = ["bnc_netgen_aos", "bnc_netgen_free", "bnc_last_error", "bnc_load_
                "bnc_plan_generated", "bnc_step_io", "bnc_profile_ticks", "bnc_run_ticks_static_scratch",
                "bnc_plan_aos", "bnc_bion_load", "bnc_bion_unload", "bnc_bion_save", "bnc_load_ensemble_generated",
                "bnc_load_ensemble_aos", "bnc_ensemble_member", "bnc_plan_ensemble_generated", "bnc_ensemble_params",
-               "bnc_run_ticks_graph"]
+               "bnc_run_ticks_graph", "bnc_load_ensemble_tuned", "bnc_time_ticks_graph"]
 
 
 class NetInfo(C.Structure):
@@ -48,7 +48,12 @@ class NetInfo(C.Structure):
                                           "smem_bytes", "flags")] + [
         ("ticks", C.c_uint64), ("algo_bytes_per_tick", C.c_double), ("seg_bytes_per_tick", C.c_double),
         ("syn_bytes_per_tick", C.c_double), ("tile_bytes_per_tick", C.c_double),
-        ("synapse_kernel_bytes_per_tick", C.c_double)]
+        ("synapse_kernel_bytes_per_tick", C.c_double), ("warp_cap", C.c_uint32), ("tile_segs", C.c_uint32)]
+
+
+class Tuning(C.Structure):
+    _fields_ = [("warp_cap", C.c_uint32), ("tile_segs", C.c_uint32), ("ms_per_tick", C.c_float),
+                ("candidates_tried", C.c_uint32), ("sample_members", C.c_uint32)]
 
 
 def plan_generated(params):
@@ -118,6 +123,7 @@ def load_library(path=LIB_PATH):
         "bnc_load_ensemble_generated": ([vp, vp, u32], i32), "bnc_load_ensemble_aos": ([vp, vp, vp, vp, u32], i32),
         "bnc_ensemble_member": ([vp, u32, vp], i32), "bnc_plan_ensemble_generated": ([vp, u32, vp], i32),
         "bnc_ensemble_params": ([C.c_uint64, u32, u32, u32, vp], i32), "bnc_run_ticks_graph": ([vp, u32, f32], i32),
+        "bnc_load_ensemble_tuned": ([vp, vp, u32, u32, f32, vp], i32), "bnc_time_ticks_graph": ([vp, u32, f32, vp], i32),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -239,6 +245,18 @@ class Backend:
         counts = (C.c_uint32 * len(nets))(*[n.n_stim for n in nets])
         _check(self.lib.bnc_load_ensemble_aos(self.h, data, stims, counts, len(nets)), "bnc_load_ensemble_aos")
 
+    def load_ensemble_tuned(self, params, trial_ticks, dt):
+        arr = params if isinstance(params, C.Array) else (NetgenParams * len(params))(*params)
+        t = Tuning()
+        _check(self.lib.bnc_load_ensemble_tuned(self.h, arr, len(arr), trial_ticks, C.c_float(dt), C.byref(t)),
+               "bnc_load_ensemble_tuned")
+        return t
+
+    def time_ticks_graph(self, n, dt):
+        ms = C.c_float()
+        _check(self.lib.bnc_time_ticks_graph(self.h, n, C.c_float(dt), C.byref(ms)), "bnc_time_ticks_graph")
+        return ms.value
+
     def ensemble_member(self, m):
         out = EnsembleMember()
         _check(self.lib.bnc_ensemble_member(self.h, m, C.byref(out)), "bnc_ensemble_member")
@@ -293,4 +311,4 @@ class Backend:
 __all__ = ["Backend", "Network", "NetgenParams", "BionData", "BackendError", "load_library", "last_error",
            "NET_SMALL", "NET_LARGE", "NET_TREES", "NET_ENSEMBLE_MEMBER", "NET_ADJOINT", "NETGEN_NO_SYNAPSES",
            "NETGEN_NO_CONNECTIONS", "NETGEN_NO_STIMULI", "NETGEN_PERTURB_IONS", "SEG_FIELDS", "SYN_FIELDS",
-           "DROPIN_SYMBOLS", "NEW_SYMBOLS", "EnsembleMember", "ensemble_params", "plan_ensemble", "plan_generated"]
+           "DROPIN_SYMBOLS", "NEW_SYMBOLS", "EnsembleMember", "Tuning", "ensemble_params", "plan_ensemble", "plan_generated"]

@@ -591,6 +591,7 @@ static int plan_info(const HostNet& hn, const Stimuli& stim, BncNetInfo* info) {
     info->flags = dev.flags; info->algo_bytes_per_tick = host.algo_bytes_per_tick;
     info->seg_bytes_per_tick = host.seg_bytes; info->syn_bytes_per_tick = host.syn_bytes;
     info->tile_bytes_per_tick = host.tile_bytes; info->synapse_kernel_bytes_per_tick = host.synk_bytes;
+    info->warp_cap = host.opt.warp_cap; info->tile_segs = host.opt.tile_segs;
     return BNC_OK;
 }
 
@@ -607,20 +608,87 @@ int bnc_plan_generated(const BncNetgenParams* p, BncNetInfo* info) {
     return plan_info(hn, stim, info);
 }
 
-int bnc_load_ensemble_generated(void* sim, const BncNetgenParams* members, uint32_t n_members) {
-    if (!sim) { set_error("null handle"); return BNC_ERR_ARG; }
-    Backend* b = static_cast<Backend*>(sim);
+static int load_members(Backend* b, const BncNetgenParams* members, uint32_t n_members, const BuildOptions& opt) {
     b->reset_network();
     HostNet hn;
     std::vector<BncEnsembleMember> mem;
     int rc = gather_generated(members, n_members, &hn, &b->stim.current, &mem);
     if (rc != BNC_OK) { b->reset_network(); return rc; }
     cudaSetDevice(b->device);
-    rc = build_network(hn, b->stim, &b->dev, &b->host, &b->allocs);
+    rc = build_network(hn, b->stim, &b->dev, &b->host, &b->allocs, opt);
     if (rc != BNC_OK) { b->reset_network(); return rc; }
     b->members = std::move(mem);
     b->loaded = true;
     return BNC_OK;
+}
+
+int bnc_load_ensemble_generated(void* sim, const BncNetgenParams* members, uint32_t n_members) {
+    if (!sim) { set_error("null handle"); return BNC_ERR_ARG; }
+    return load_members(static_cast<Backend*>(sim), members, n_members, BuildOptions());
+}
+
+static int time_graph(Backend* b, uint32_t n, float dt, float* ms) {
+    cudaEventRecord(b->ev0, b->stream);
+    int rc = run_ticks_graph(b, n, dt);
+    if (rc != BNC_OK) return rc;
+    cudaEventRecord(b->ev1, b->stream);
+    rc = sync_stream(b);
+    if (rc != BNC_OK) return rc;
+    cudaEventElapsedTime(ms, b->ev0, b->ev1);
+    return BNC_OK;
+}
+
+// Groupings the autotuner tries: (segments per warp group, segments per tile).
+static const BuildOptions kTuneCandidates[] = {
+    {32, 256}, {64, 256}, {64, 512}, {128, 512}, {64, 1024}, {128, 1024}, {256, 1024},
+};
+
+int bnc_load_ensemble_tuned(void* sim, const BncNetgenParams* members, uint32_t n_members, uint32_t trial_ticks,
+                            float dt, BncTuning* out) {
+    if (!sim || !members || n_members == 0) { set_error("bnc_load_ensemble_tuned: null argument"); return BNC_ERR_ARG; }
+    Backend* b = static_cast<Backend*>(sim);
+    // Tune on an evenly strided sample of at most 64 members (every member's own
+    // sizes, so the sample keeps the ensemble's size mix), then build everything.
+    const uint32_t stride = n_members > 64 ? (n_members + 63) / 64 : 1;
+    std::vector<BncNetgenParams> sample;
+    for (uint32_t m = 0; m < n_members; m += stride) sample.push_back(members[m]);
+    if (trial_ticks < kGraphTicks) trial_ticks = kGraphTicks;
+    BncTuning best{};
+    best.ms_per_tick = -1.0f;
+    uint32_t tried = 0;
+    for (const BuildOptions& opt : kTuneCandidates) {
+        int rc = load_members(b, sample.data(), (uint32_t)sample.size(), opt);
+        if (rc == BNC_ERR_UNSUPPORTED) continue;   // a component larger than this tile
+        if (rc != BNC_OK) return rc;
+        float ms = 0.0f;
+        rc = run_ticks_graph(b, 1, dt);                     // first tick and set-up, untimed
+        if (rc == BNC_OK) rc = time_graph(b, trial_ticks, dt, &ms);
+        if (rc != BNC_OK) { b->reset_network(); return rc; }
+        tried++;
+        const float per_tick = ms / (float)trial_ticks;
+        if (best.ms_per_tick < 0.0f || per_tick < best.ms_per_tick) {
+            best.warp_cap = opt.warp_cap;
+            best.tile_segs = opt.tile_segs;
+            best.ms_per_tick = per_tick;
+        }
+    }
+    b->reset_network();
+    if (tried == 0) { set_error("no grouping fits the ensemble's largest component"); return BNC_ERR_UNSUPPORTED; }
+    best.candidates_tried = tried;
+    best.sample_members = (uint32_t)sample.size();
+    BuildOptions opt;
+    opt.warp_cap = best.warp_cap;
+    opt.tile_segs = best.tile_segs;
+    int rc = load_members(b, members, n_members, opt);
+    if (rc == BNC_OK && out) *out = best;
+    return rc;
+}
+
+int bnc_time_ticks_graph(void* sim, uint32_t n_ticks, float dt, float* ms) {
+    if (!sim || !ms) { set_error("null argument"); return BNC_ERR_ARG; }
+    Backend* b = static_cast<Backend*>(sim);
+    cudaSetDevice(b->device);
+    return time_graph(b, n_ticks, dt, ms);
 }
 
 int bnc_load_ensemble_aos(void* sim, const BncBionData* members, const BncCurrentStimulus* const* stim,
@@ -932,6 +1000,7 @@ int bnc_network_info(void* sim, BncNetInfo* info) {
     info->syn_bytes_per_tick = b->host.syn_bytes;
     info->tile_bytes_per_tick = b->host.tile_bytes;
     info->synapse_kernel_bytes_per_tick = b->host.synk_bytes;
+    info->warp_cap = b->host.opt.warp_cap; info->tile_segs = b->host.opt.tile_segs;
     return BNC_OK;
 }
 

@@ -282,7 +282,7 @@ void hostnet_from_aos(const BncBionData& aos, HostNet* hn) {
 }
 
 int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* host,
-                  DeviceAllocs* allocs) {
+                  DeviceAllocs* allocs, const BuildOptions& opt) {
     const bool verbose = std::getenv("BNC_VERBOSE") != nullptr;
     auto t_last = std::chrono::steady_clock::now();
     auto lap = [&](const char* what) {
@@ -350,7 +350,13 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
     }
     lap("components");
     // ---- tile packing: whole components, one component per warp slot ----
-    const uint32_t warp_cap = 64;
+    if (opt.warp_cap < 1 || opt.tile_segs < 32 || opt.tile_segs > (uint32_t)kMaxTileSegs) {
+        set_error("grouping options out of range (warp_cap %u, tile_segs %u)", opt.warp_cap, opt.tile_segs);
+        return BNC_ERR_ARG;
+    }
+    host->opt = opt;
+    const uint32_t warp_cap = opt.warp_cap;
+    const uint32_t tile_cap = opt.tile_segs;
     std::vector<uint32_t> tile_seg_beg{0};
     std::vector<uint16_t> warp_seg;   // per tile kTileWarps+1 entries
     {
@@ -365,8 +371,8 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
         };
         for (size_t r = 0; r < roots.size(); r++) {
             uint32_t sz = comp_members_off[r + 1] - comp_members_off[r];
-            if (sz > (uint32_t)kMaxTileSegs) {
-                set_error("connected component of %u segments exceeds the %d-segment tile", sz, kMaxTileSegs);
+            if (sz > tile_cap) {
+                set_error("connected component of %u segments exceeds the %u-segment tile", sz, tile_cap);
                 return BNC_ERR_UNSUPPORTED;
             }
             bool fits_warp = cur_warp_segs > 0 && cur_warp_segs + sz <= warp_cap;
@@ -375,7 +381,7 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
                 wb[cur_warp] = (uint16_t)cur_tile_segs;
                 cur_warp_segs = 0;
             }
-            if (cur_warp >= (uint32_t)kTileWarps || cur_tile_segs + sz > (uint32_t)kMaxTileSegs) {
+            if (cur_warp >= (uint32_t)kTileWarps || cur_tile_segs + sz > tile_cap) {
                 // the open warp index is past the end or the tile is full: close it
                 if (cur_warp >= (uint32_t)kTileWarps) cur_warp = kTileWarps - 1;
                 close_tile();

@@ -126,6 +126,15 @@ struct NetDev {
     unsigned long long* clock;
 };
 
+// How components are grouped: a warp group holds components until their segments
+// would exceed warp_cap (a larger component gets a warp group to itself), and a tile
+// holds up to kTileWarps warp groups and at most tile_segs segments.  The grouping
+// changes which CTA and warp handle a segment, never the arithmetic.
+struct BuildOptions {
+    uint32_t warp_cap = 64;
+    uint32_t tile_segs = kMaxTileSegs;
+};
+
 // Host copy of everything the exporter needs to map device state back.
 struct NetHost {
     uint32_t n_seg = 0, n_conn = 0, n_syn_total = 0;
@@ -139,6 +148,7 @@ struct NetHost {
     std::vector<uint8_t> syn_nt;     // released NT per device synapse
     uint32_t max_tile_segs = 0, max_tile_edges = 0;
     size_t smem_bytes = 0;
+    BuildOptions opt;                        // grouping the network was built with
     double algo_bytes_per_tick = 0;  // algorithmic HBM bytes per tick of this state schema
     double seg_bytes = 0, syn_bytes = 0;     // split by owner: segment state vs synapse state
     double tile_bytes = 0, synk_bytes = 0;   // split by kernel: k_tile vs k_synapse
@@ -162,7 +172,7 @@ struct DeviceAllocs {
 
 struct HostNet;
 int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* host,
-                  DeviceAllocs* allocs);
+                  DeviceAllocs* allocs, const BuildOptions& opt = BuildOptions());
 
 // Rebuilds the per-segment stimulus CSRs after an upload of new stimuli.
 int upload_stimuli(const Stimuli& stim, NetHost& host, NetDev* dev, DeviceAllocs* allocs);

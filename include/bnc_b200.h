@@ -195,6 +195,7 @@ typedef struct {
     double algo_bytes_per_tick;   /* algorithmic HBM bytes one tick moves (state schema) */
     double seg_bytes_per_tick, syn_bytes_per_tick;          /* split by state owner */
     double tile_bytes_per_tick, synapse_kernel_bytes_per_tick; /* split by kernel */
+    uint32_t warp_cap, tile_segs;  /* grouping the network was built with */
 } BncNetInfo;
 int bnc_network_info(void* sim, BncNetInfo* info);
 
@@ -230,6 +231,22 @@ int bnc_plan_ensemble_generated(const BncNetgenParams* members, uint32_t n_membe
  * gNa/gK/gleak/gCa scaled by independent U[0.5, 2] factors, one seed per member. */
 int bnc_ensemble_params(uint64_t seed, uint32_t n_members, uint32_t min_segments, uint32_t max_segments,
                         BncNetgenParams* out);
+
+/* Autotuned ensemble load: tries several groupings of components into warp
+ * groups and tiles on a strided sample of at most 64 members (build, one untimed
+ * tick, then trial_ticks timed with the captured loop), keeps the fastest and
+ * builds the whole ensemble with it.  The grouping never changes results.  `out`
+ * (may be NULL) receives the choice and its per-tick time on the sample. */
+typedef struct {
+    uint32_t warp_cap, tile_segs;   /* chosen grouping (segments per warp group / tile) */
+    float ms_per_tick;              /* on the sample */
+    uint32_t candidates_tried, sample_members;
+} BncTuning;
+int bnc_load_ensemble_tuned(void* sim, const BncNetgenParams* members, uint32_t n_members, uint32_t trial_ticks,
+                            float dt, BncTuning* out);
+
+/* bnc_run_ticks_graph bracketed by CUDA events; *ms receives the device time. */
+int bnc_time_ticks_graph(void* sim, uint32_t n_ticks, float dt, float* ms);
 
 /* Runs n ticks with the tick loop captured once in a CUDA graph (32 ticks per
  * replay; the tick counter lives on the device) -- same results as bnc_run_ticks,

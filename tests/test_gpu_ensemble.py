@@ -84,3 +84,21 @@ def test_graph_ticks_match_plain_ticks(family):
             _same(g.segment_field(f, i), r.segment_field(f, i), "%s %s[%d] after %d" % (family, f, i, n))
         for f, i in SYN:
             _same(g.synapse_field(f, i), r.synapse_field(f, i), "%s synapse %s[%d]" % (family, f, i))
+
+
+def test_autotuned_grouping_gives_identical_results():
+    from bioneuroncore_b200 import Backend, ensemble_params
+    ps = ensemble_params(21, 6, 64, 3000)
+    tuned, plain = Backend(), Backend()
+    t = tuned.load_ensemble_tuned(ps, 32, DT)
+    plain.load_ensemble(ps)
+    assert t.candidates_tried >= 3 and t.ms_per_tick > 0
+    assert (tuned.info().warp_cap, tuned.info().tile_segs) == (t.warp_cap, t.tile_segs)
+    for step in (1, 40):
+        tuned.run_ticks_graph(step, DT)
+        plain.run_ticks(step, DT)
+        for f, i in SEG:
+            _same(tuned.segment_field(f, i), plain.segment_field(f, i), "%s[%d] after +%d" % (f, i, step))
+        n = plain.info().n_synapses
+        for f, i in SYN:
+            _same(tuned.synapse_field(f, i, n), plain.synapse_field(f, i, n), "synapse %s[%d]" % (f, i))
