@@ -280,7 +280,7 @@ def main():
     info = b.info()
     b.run_ticks(a.warmup, DT)
     n_prof = max(3, min(10, a.steps))
-    ms_tile, ms_syn = b.profile_ticks(n_prof, DT)
+    ms_mod, ms_diff, ms_syn = b.profile_ticks(n_prof, DT)
 
     def barrier():
         rank_barrier(dist, "cuda")
@@ -314,17 +314,17 @@ def main():
 
     # roofline of the dominant kernel
     peak, peak_kind = measured_peak()
-    tile_avg = ms_tile / n_prof
-    syn_avg = ms_syn / n_prof
-    if tile_avg >= syn_avg:
-        kname, kbytes, kms = "k_tile", info.tile_bytes_per_tick, tile_avg
-    else:
-        kname, kbytes, kms = "k_synapse", info.synapse_kernel_bytes_per_tick, syn_avg
+    kernels = {"k_modifiers": (ms_mod / n_prof, info.modifier_kernel_bytes),
+               "k_diffusion": (ms_diff / n_prof, info.diffusion_kernel_bytes),
+               "k_synapse": (ms_syn / n_prof, info.synapse_kernel_bytes_per_tick)}
+    kname = max(kernels, key=lambda k: kernels[k][0])
+    kms, kbytes = kernels[kname]
     achieved = kbytes / (kms / 1000.0) / 1e9
     roofline = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_source": peak_kind, "traffic": ncu_traffic(kname),
                 "algo_bytes_per_launch": kbytes, "avg_launch_ms": kms,
-                "kernels_ms": {"k_tile": tile_avg, "k_synapse": syn_avg},
+                "kernels_ms": {k: v[0] for k, v in kernels.items()},
+                "kernels_frac": {k: v[1] / (v[0] / 1000.0) / 1e9 / peak for k, v in kernels.items()},
                 "tick_bytes": info.algo_bytes_per_tick,
                 "tick_frac": info.algo_bytes_per_tick / (ms_max / a.steps / 1000.0) / 1e9 / peak}
 
@@ -353,7 +353,7 @@ def main():
                        "l2": "inputs larger than L2 (device state ~8 GB per GPU)",
                        "tiles": info.n_tiles, "phases": info.n_phases, "setup_s": round(setup_s, 1)},
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,
-            "gpu_launches": 2 * a.steps, "ensemble": ensemble,
+            "gpu_launches": 3 * a.steps, "ensemble": ensemble,
         }
         print(json.dumps(line), flush=True)
     b.close()

@@ -48,7 +48,8 @@ class NetInfo(C.Structure):
                                           "smem_bytes", "flags")] + [
         ("ticks", C.c_uint64), ("algo_bytes_per_tick", C.c_double), ("seg_bytes_per_tick", C.c_double),
         ("syn_bytes_per_tick", C.c_double), ("tile_bytes_per_tick", C.c_double),
-        ("synapse_kernel_bytes_per_tick", C.c_double), ("warp_cap", C.c_uint32), ("tile_segs", C.c_uint32)]
+        ("synapse_kernel_bytes_per_tick", C.c_double), ("warp_cap", C.c_uint32), ("tile_segs", C.c_uint32),
+        ("modifier_kernel_bytes", C.c_double), ("diffusion_kernel_bytes", C.c_double)]
 
 
 class Tuning(C.Structure):
@@ -116,7 +117,7 @@ def load_library(path=LIB_PATH):
         "bnc_read_synapse_field": ([vp, i32, i32, vp, u32], i32),
         "bnc_set_synapse_scale": ([vp, vp, u32], i32), "bnc_network_info": ([vp, vp], i32),
         "bnc_save_bion": ([vp, C.c_char_p], i32), "bnc_plan_generated": ([vp, vp], i32),
-        "bnc_step_io": ([vp, f32, vp, u32, vp, u32], i32), "bnc_profile_ticks": ([vp, u32, f32, vp, vp], i32),
+        "bnc_step_io": ([vp, f32, vp, u32, vp, u32], i32), "bnc_profile_ticks": ([vp, u32, f32, vp, vp, vp], i32),
         "bnc_run_ticks_static_scratch": ([vp, u32, f32], i32),
         "bnc_plan_aos": ([vp, vp, u32, vp], i32), "bnc_bion_load": ([C.c_char_p, vp], i32),
         "bnc_bion_unload": ([vp], None), "bnc_bion_save": ([C.c_char_p, vp], i32),
@@ -273,10 +274,11 @@ class Backend:
                "bnc_step_io")
 
     def profile_ticks(self, n, dt):
-        """Runs n ticks; returns (ms in the tile kernel, ms in the synapse kernel)."""
-        a, b = C.c_float(), C.c_float()
-        _check(self.lib.bnc_profile_ticks(self.h, n, C.c_float(dt), C.byref(a), C.byref(b)), "bnc_profile_ticks")
-        return a.value, b.value
+        """Runs n ticks; returns summed ms in (k_modifiers, k_diffusion, k_synapse)."""
+        a, b, c = C.c_float(), C.c_float(), C.c_float()
+        _check(self.lib.bnc_profile_ticks(self.h, n, C.c_float(dt), C.byref(a), C.byref(b), C.byref(c)),
+               "bnc_profile_ticks")
+        return a.value, b.value, c.value
 
     def sync_to_host(self):
         _check(self.lib.bnc_sync_to_host(self.h), "bnc_sync_to_host")

@@ -592,6 +592,7 @@ static int plan_info(const HostNet& hn, const Stimuli& stim, BncNetInfo* info) {
     info->seg_bytes_per_tick = host.seg_bytes; info->syn_bytes_per_tick = host.syn_bytes;
     info->tile_bytes_per_tick = host.tile_bytes; info->synapse_kernel_bytes_per_tick = host.synk_bytes;
     info->warp_cap = host.opt.warp_cap; info->tile_segs = host.opt.tile_segs;
+    info->modifier_kernel_bytes = host.mod_bytes; info->diffusion_kernel_bytes = host.diff_bytes;
     return BNC_OK;
 }
 
@@ -833,35 +834,42 @@ int bnc_step_io(void* sim, float dt, const float* stim_amp, uint32_t n_amp, floa
     return sync_stream(b);
 }
 
-int bnc_profile_ticks(void* sim, uint32_t n_ticks, float dt, float* ms_tile, float* ms_synapse) {
-    if (!sim || !ms_tile || !ms_synapse) { set_error("null argument"); return BNC_ERR_ARG; }
+int bnc_profile_ticks(void* sim, uint32_t n_ticks, float dt, float* ms_modifiers, float* ms_diffusion,
+                      float* ms_synapse) {
+    if (!sim || !ms_modifiers || !ms_diffusion || !ms_synapse) { set_error("null argument"); return BNC_ERR_ARG; }
     Backend* b = static_cast<Backend*>(sim);
     if (!b->loaded) { set_error("no network loaded"); return BNC_ERR_STATE; }
     cudaSetDevice(b->device);
-    cudaEvent_t e[3];
+    cudaEvent_t e[4];
     for (auto& x : e) cudaEventCreate(&x);
-    float tt = 0.0f, ts = 0.0f;
+    float tm = 0.0f, td = 0.0f, ts = 0.0f;
     int rc = BNC_OK;
     for (uint32_t t = 0; t < n_ticks && rc == BNC_OK; t++) {
         cudaEventRecord(e[0], b->stream);
-        cudaError_t er = launch_tile(b->dev, b->host, dt, b->tick, b->stream);
-        if (er != cudaSuccess) { rc = cuda_fail(er, "tile launch"); break; }
+        cudaError_t er = launch_modifiers(b->dev, b->host, dt, b->tick, b->stream);
+        if (er != cudaSuccess) { rc = cuda_fail(er, "modifier kernel launch"); break; }
         cudaEventRecord(e[1], b->stream);
-        er = launch_synapse(b->dev, dt, b->tick, b->ticks_run == 0 ? 1 : 0, b->stream);
-        if (er != cudaSuccess) { rc = cuda_fail(er, "synapse launch"); break; }
+        er = launch_diffusion(b->dev, b->host, dt, b->stream);
+        if (er != cudaSuccess) { rc = cuda_fail(er, "diffusion kernel launch"); break; }
         cudaEventRecord(e[2], b->stream);
+        er = launch_synapse(b->dev, dt, b->tick, b->ticks_run == 0 ? 1 : 0, b->stream);
+        if (er != cudaSuccess) { rc = cuda_fail(er, "synapse kernel launch"); break; }
+        cudaEventRecord(e[3], b->stream);
         b->tick++;
         b->ticks_run++;
         rc = sync_stream(b);
         if (rc != BNC_OK) break;
-        float a = 0.0f, c = 0.0f;
-        cudaEventElapsedTime(&a, e[0], e[1]);
-        cudaEventElapsedTime(&c, e[1], e[2]);
-        tt += a;
-        ts += c;
+        float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f;
+        cudaEventElapsedTime(&a0, e[0], e[1]);
+        cudaEventElapsedTime(&a1, e[1], e[2]);
+        cudaEventElapsedTime(&a2, e[2], e[3]);
+        tm += a0;
+        td += a1;
+        ts += a2;
     }
     for (auto& x : e) cudaEventDestroy(x);
-    *ms_tile = tt;
+    *ms_modifiers = tm;
+    *ms_diffusion = td;
     *ms_synapse = ts;
     return rc;
 }
@@ -1001,6 +1009,7 @@ int bnc_network_info(void* sim, BncNetInfo* info) {
     info->tile_bytes_per_tick = b->host.tile_bytes;
     info->synapse_kernel_bytes_per_tick = b->host.synk_bytes;
     info->warp_cap = b->host.opt.warp_cap; info->tile_segs = b->host.opt.tile_segs;
+    info->modifier_kernel_bytes = b->host.mod_bytes; info->diffusion_kernel_bytes = b->host.diff_bytes;
     return BNC_OK;
 }
 

@@ -804,6 +804,7 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
         dev->stype = up(allocs, stype, &rc);
         dev->sflags = up(allocs, dflags, &rc);
         dev->cav21_static = up(allocs, c21, &rc);
+        dev->c21_cur = zeros<float2>(allocs, n, &rc);
         dev->pre_rec = zeros<float4>(allocs, n, &rc);
         if (need_pre_ext) {
             dev->pre_ext = zeros<float4>(allocs, n, &rc);
@@ -872,7 +873,12 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
     }
     host->max_tile_segs = mts;
     host->max_tile_edges = mte;
-    host->smem_bytes = tile_smem_bytes(mts, mte);
+    host->smem_bytes = std::max(tile_smem_bytes(mts), diffusion_smem_bytes(mts, mte));
+    if (host->smem_bytes > 227 * 1024) {
+        set_error("tile of %u segments and %u connections needs %zu bytes of shared memory (227 KB per CTA)", mts, mte,
+                  host->smem_bytes);
+        return BNC_ERR_UNSUPPORTED;
+    }
     // ---- algorithmic bytes per tick of this schema (what one tick must move at minimum) ----
     {
         // kernel A per segment: read V, 14 ions, ATP, geometry+C_m (radius, length, area,
@@ -910,6 +916,18 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
         host->tile_bytes = seg_a * n + items;
         host->synk_bytes = seg_b * n + host->syn_bytes;
         host->algo_bytes_per_tick = host->seg_bytes + host->syn_bytes;
+        // Per kernel of the three-kernel tick (the state between steps 1 and 2.5 makes
+        // one round trip through HBM, which the tick-level figure above does not count):
+        // k_modifiers reads V, 14 ions, ATP, area, vol, the static Cav2.1 gate and writes
+        // V, 14 ions, ATP, I_buffer, the Cav2.1 gate; k_diffusion reads them back with
+        // C_m and the connection statics and writes the state and the presynaptic record.
+        host->mod_bytes = (4 * 2 + 56 * 2 + 4 * 2 + 4 + 8 + 8 + 8 + 8) * (double)n + items;
+        double seg_d = 4 * 2 + 56 * 2 + 4 * 2 + 4 + 4 + 8 + 8 + 8 + 16;
+        if (flags & NF_INTRA_NT) seg_d += 120;
+        if (flags & NF_TEMP) seg_d += 8;
+        if (flags & NF_TXN) seg_d += 8;
+        if (flags & NF_DIFFUSION) seg_d += 4 * 2.0 * E / n + 8 * 2.0 * E / n;
+        host->diff_bytes = seg_d * n;
     }
     return BNC_OK;
 }

@@ -1,0 +1,569 @@
+// diffuse.cu -- step 2.5 of a tick, electrodiffusion (diffusion_kernel.h:115-364), and
+// the write-back of the tick's segment state.
+//
+// One CTA per tile of whole components (the same tiles as the modifier kernel), one
+// thread per segment and one per connection.  The 300 Jacobi sweeps of a tick (50 for
+// phi_e, 5 x 50 for V_m) are latency chains, not bandwidth: each thread keeps its
+// segment's stencil -- the incident connections in original connection order, the
+// other endpoint, the coefficient -- in registers for all sweeps of a solve, so a
+// sweep is a few independent shared-memory loads, the arithmetic and one barrier.
+// Every gather sums the segment's incident connections in original connection order,
+// the order of the reference's scatter loops, so results are bit-identical to them.
+#include <cuda_runtime.h>
+#include "net.h"
+#include "physics.cuh"
+
+namespace bnc {
+
+// valence, diffusion coefficient and bath concentration per ion (diffusion_kernel.h:23-33)
+__constant__ float kNpZ[7] = {1.0f, 1.0f, 2.0f, -1.0f, 2.0f, -1.0f, 1.0f};
+__constant__ float kDiffC[7] = {1.33f, 1.96f, 0.22f, 2.03f, 0.10f, 0.0f, 9.31f};
+__constant__ float kBathIon[7] = {140.0f, 3.0f, 1.2f, 130.0f, 1.0f, 0.0f, 4.0e-5f};
+__device__ float gNtD[15];   // Stokes-Einstein NT diffusion coefficients, set by k_init_ntd
+
+// D = 1.33 * (23/M)^(1/3) (types.h:428-445, nt_diffusion_coeff); the 15th entry has no
+// mass in the reference's table (0 -> 1)
+__global__ void k_init_ntd() {
+    const float mass[15] = {147.0f, 103.0f, 153.0f, 176.0f, 146.0f, 267.0f, 169.0f, 75.0f, 111.0f,
+                            348.0f, 507.0f, 232.0f, 24.0f, 162.0f, 0.0f};
+    for (int q = 0; q < 15; q++) {
+        float ms = mass[q];
+        if (ms < 1.0f) ms = 1.0f;
+        gNtD[q] = 1.33f * dm_powf(23.0f / ms, 1.0f / 3.0f);
+    }
+}
+
+static bool g_ntd_ready[64] = {false};   // per device
+
+namespace {
+
+// incidences held in registers per segment; segments with more use shared memory
+constexpr int kDeg = 4;
+
+// diffusion_kernel.h:108-113
+__device__ __forceinline__ float sg_bernoulli(float x) {
+    if (fabsf(x) < 1e-3f) return 1.0f - 0.5f * x;
+    if (x > 50.0f) return 0.0f;
+    if (x < -50.0f) return -x;
+    return x / (dm_expf(x) - 1.0f);
+}
+
+struct DiffSmem {
+    double *itot, *phiA, *phiB, *sig, *ed;
+    float *V, *in, *out, *atp, *area, *cm, *vf, *vnA, *vnB, *nb;
+    float *gax, *dve, *fl, *ie, *earea, *edist;
+    uint16_t *incoff, *inc, *ea, *eb;
+    uint8_t *ei, *es;
+};
+
+__host__ __device__ inline size_t al16(size_t x) { return (x + 15) & ~(size_t)15; }
+
+__host__ __device__ inline size_t diff_layout(uint32_t S, uint32_t E, unsigned char* base, DiffSmem* t) {
+    size_t off = 0;
+    auto take = [&](size_t bytes) { size_t o = off; off = al16(off + bytes); return base ? base + o : nullptr; };
+    const size_t Ee = E ? E : 1, Ii = 2 * Ee;   // each connection sits in two incidence lists
+    unsigned char* p;
+    p = take(8 * (size_t)S); if (t) t->itot = (double*)p;
+    p = take(8 * (size_t)S); if (t) t->phiA = (double*)p;
+    p = take(8 * (size_t)S); if (t) t->phiB = (double*)p;
+    p = take(8 * (size_t)S); if (t) t->sig = (double*)p;
+    p = take(4 * (size_t)S); if (t) t->V = (float*)p;
+    p = take(4 * 7 * (size_t)S); if (t) t->in = (float*)p;
+    p = take(4 * 7 * (size_t)S); if (t) t->out = (float*)p;
+    p = take(4 * (size_t)S); if (t) t->atp = (float*)p;
+    p = take(4 * (size_t)S); if (t) t->area = (float*)p;
+    p = take(4 * (size_t)S); if (t) t->cm = (float*)p;
+    p = take(4 * (size_t)S); if (t) t->vf = (float*)p;
+    p = take(4 * (size_t)S); if (t) t->vnA = (float*)p;
+    p = take(4 * (size_t)S); if (t) t->vnB = (float*)p;
+    p = take(4 * (size_t)S); if (t) t->nb = (float*)p;
+    p = take(2 * ((size_t)S + 1)); if (t) t->incoff = (uint16_t*)p;
+    p = take(2 * Ii); if (t) t->inc = (uint16_t*)p;
+    p = take(8 * Ee); if (t) t->ed = (double*)p;
+    p = take(4 * Ee); if (t) t->gax = (float*)p;
+    p = take(4 * Ee); if (t) t->dve = (float*)p;
+    p = take(4 * Ee); if (t) t->fl = (float*)p;
+    p = take(4 * Ee); if (t) t->ie = (float*)p;
+    p = take(4 * Ee); if (t) t->earea = (float*)p;
+    p = take(4 * Ee); if (t) t->edist = (float*)p;
+    p = take(2 * Ee); if (t) t->ea = (uint16_t*)p;
+    p = take(2 * Ee); if (t) t->eb = (uint16_t*)p;
+    p = take(Ee); if (t) t->ei = (uint8_t*)p;
+    p = take(Ee); if (t) t->es = (uint8_t*)p;
+    return off;
+}
+
+// A segment's incidences in original connection order: edge index, whether the
+// segment is the edge's b end, and the other endpoint.  n < 0: more than kDeg,
+// read t.inc instead.
+struct Stencil {
+    int n;
+    uint16_t e[kDeg];
+    uint16_t o[kDeg];
+    uint8_t bend;   // bit k: the segment is edge e[k]'s b end
+};
+
+// Fick pass for a float field in t.nb (diffusion_kernel.h:284-345): per-edge flux,
+// then per-segment gather in connection order, updating t.nb in place.
+template <bool kIntraOnly, bool kGradStrict>
+__device__ __forceinline__ void fick(const DiffSmem& t, int ns, int ne, int tid, int nth, int i, const Stencil& st,
+                                     float D, float thresh, float dt) {
+    for (int e = tid; e < ne; e += nth) {
+        t.es[e] = 1;
+        if (kIntraOnly && !t.ei[e]) continue;
+        float dC = t.nb[t.ea[e]] - t.nb[t.eb[e]];
+        if (kGradStrict) { if (!(dC > thresh || dC < -thresh)) continue; }
+        else if (dC < thresh && dC > -thresh) continue;
+        t.fl[e] = D * t.earea[e] * dC * dt / t.edist[e];
+        t.es[e] = 0;
+    }
+    __syncthreads();
+    // the gather reads only edge fluxes and the segment's own value: update in place
+    if (i < ns) {
+        const float vf = t.vf[i];
+        float acc = 0.0f;
+        if (st.n >= 0) {
+#pragma unroll
+            for (int k = 0; k < kDeg; k++) {
+                if (k >= st.n) break;
+                const int e = st.e[k];
+                if (t.es[e]) continue;
+                if ((st.bend >> k) & 1u) acc += t.fl[e] / vf; else acc -= t.fl[e] / vf;
+            }
+        } else {
+            for (int k = t.incoff[i]; k < t.incoff[i + 1]; k++) {
+                const uint16_t ent = t.inc[k];
+                const int e = ent & 0x7FFF;
+                if (t.es[e]) continue;
+                if (ent & 0x8000) acc += t.fl[e] / vf; else acc -= t.fl[e] / vf;
+            }
+        }
+        t.nb[i] = t.nb[i] + acc;
+    }
+    __syncthreads();
+}
+
+}  // namespace
+
+__global__ void __launch_bounds__(1024)
+k_diffusion(NetDev d, float dt, uint32_t S, uint32_t E) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    DiffSmem t;
+    diff_layout(S, E, smem, &t);
+    const int tid = threadIdx.x;
+    const int nth = blockDim.x;
+    const uint32_t tile = blockIdx.x;
+    const uint32_t N = d.n_seg;
+    const uint32_t s0 = d.tile_seg_beg[tile];
+    const int ns = (int)(d.tile_seg_beg[tile + 1] - s0);
+    const uint32_t e0 = d.tile_edge_beg[tile];
+    const int ne = (int)(d.tile_edge_beg[tile + 1] - e0);
+    const uint32_t inc0 = d.inc_off[s0];
+    const int ninc = (int)(d.inc_off[s0 + ns] - inc0);
+    const int i = tid;   // this thread's segment (when i < ns)
+
+    // ---- load: state after step 1 (modifier kernel), statics, connections ----
+    float c21d = 0.0f, c21h = 0.0f;
+    if (i < ns) {
+        const uint32_t g = s0 + i;
+        t.V[i] = d.V[g];
+#pragma unroll
+        for (int q = 0; q < 7; q++) {
+            t.in[q * S + i] = d.ion_in[(size_t)q * N + g];
+            t.out[q * S + i] = d.ion_out[(size_t)q * N + g];
+        }
+        t.atp[i] = d.atp[g];
+        t.area[i] = d.area[g];
+        t.cm[i] = d.cm[g];
+        float vf = (float)d.vol[g];
+        if (vf < 1e-6f) vf = 1e-6f;
+        t.vf[i] = vf;
+        t.itot[i] = d.ibuf[g];
+        t.incoff[i] = (uint16_t)(d.inc_off[g] - inc0);
+        const float2 c = d.c21_cur[g];
+        c21d = c.x;
+        c21h = c.y;
+    }
+    if (tid == 0) t.incoff[ns] = (uint16_t)ninc;
+    for (int e = tid; e < ne; e += nth) {
+        t.ea[e] = d.e_a[e0 + e];
+        t.eb[e] = d.e_b[e0 + e];
+        t.ei[e] = d.e_intra[e0 + e];
+        t.earea[e] = d.e_area[e0 + e];
+        t.edist[e] = d.e_dist[e0 + e];
+    }
+    for (int k = tid; k < ninc; k += nth) t.inc[k] = d.inc[inc0 + k];
+    __syncthreads();
+
+    if (d.flags & NF_DIFFUSION) {
+        // this segment's incidences in connection order
+        Stencil st;
+        st.n = 0;
+        st.bend = 0;
+        if (i < ns) {
+            const int k0 = t.incoff[i], k1 = t.incoff[i + 1];
+            if (k1 - k0 > kDeg) st.n = -1;
+            else {
+                st.n = k1 - k0;
+#pragma unroll
+                for (int k = 0; k < kDeg; k++) {
+                    st.e[k] = 0; st.o[k] = 0;
+                    if (k < st.n) {
+                        const uint16_t ent = t.inc[k0 + k];
+                        const int e = ent & 0x7FFF;
+                        st.e[k] = (uint16_t)e;
+                        if (ent & 0x8000) { st.bend |= (uint8_t)(1u << k); st.o[k] = t.ea[e]; }
+                        else st.o[k] = t.eb[e];
+                    }
+                }
+            }
+        }
+
+        // ---- phi_e (diffusion_kernel.h:41-104) ----
+        if (i < ns) {
+            double sacc = 0.0;
+#pragma unroll
+            for (int q = 0; q < 7; q++) sacc += kNpZ[q] * kNpZ[q] * kDiffC[q] * (double)t.out[q * S + i];
+            t.sig[i] = 3.612f * sacc;
+            t.phiA[i] = 0.0;
+        }
+        __syncthreads();
+        for (int e = tid; e < ne; e += nth) {
+            double g = 0.5 * (t.sig[t.ea[e]] + t.sig[t.eb[e]]) * t.earea[e] / t.edist[e];
+            t.ed[e] = g;
+        }
+        __syncthreads();
+        // diagonal and the sweep stencil (connections with g > 0, in order)
+        double diag = 0.0, itot = 0.0;
+        double pg[kDeg];
+        uint16_t po[kDeg];
+        int pn_cnt = 0;
+        if (i < ns) {
+            diag = t.sig[i] * t.area[i] / 1.0f;
+            itot = t.itot[i];
+            if (st.n >= 0) {
+#pragma unroll
+                for (int k = 0; k < kDeg; k++) {
+                    pg[k] = 0.0; po[k] = 0;
+                    if (k < st.n) diag += t.ed[st.e[k]];
+                }
+#pragma unroll
+                for (int k = 0; k < kDeg; k++) {
+                    if (k < st.n) {
+                        const double g = t.ed[st.e[k]];
+                        if (g > 0.0) {
+#pragma unroll
+                            for (int j = 0; j < kDeg; j++)
+                                if (j == pn_cnt) { pg[j] = g; po[j] = st.o[k]; }
+                            pn_cnt++;
+                        }
+                    }
+                }
+            } else {
+                for (int k = t.incoff[i]; k < t.incoff[i + 1]; k++) diag += t.ed[t.inc[k] & 0x7FFF];
+            }
+        }
+        double* phi = t.phiA;
+        double* phn = t.phiB;
+        for (int it = 0; it < 50; it++) {
+            if (i < ns) {
+                double pn = 0.0;
+                if (st.n >= 0) {
+#pragma unroll
+                    for (int k = 0; k < kDeg; k++)
+                        if (k < pn_cnt) pn += pg[k] * phi[po[k]];
+                } else {
+                    for (int k = t.incoff[i]; k < t.incoff[i + 1]; k++) {
+                        const uint16_t ent = t.inc[k];
+                        const int e = ent & 0x7FFF;
+                        const double g = t.ed[e];
+                        if (g <= 0.0) continue;
+                        const int o = (ent & 0x8000) ? t.ea[e] : t.eb[e];
+                        pn += g * phi[o];
+                    }
+                }
+                double v = (diag > 1e-9) ? (pn - itot) / diag : 0.0;
+                if (v > 10.0) v = 10.0;
+                if (v < -10.0) v = -10.0;
+                phn[i] = v;
+            }
+            __syncthreads();
+            double* tmp = phi; phi = phn; phn = tmp;
+        }
+
+        // ---- intracellular Nernst-Planck, 5 substeps (diffusion_kernel.h:152-238) ----
+        const float dt_sub = dt / 5;
+        for (int sub = 0; sub < 5; sub++) {
+            for (int e = tid; e < ne; e += nth) {
+                if (!t.ei[e]) continue;
+                const int a = t.ea[e], b = t.eb[e];
+                float sigma_i = 0.0f;
+#pragma unroll
+                for (int q = 0; q < 7; q++) {
+                    float C_bar = (float)(0.5f * ((double)t.in[q * S + a] + (double)t.in[q * S + b]));
+                    sigma_i += kNpZ[q] * kNpZ[q] * kDiffC[q] * C_bar;
+                }
+                t.gax[e] = 3.612f * sigma_i * t.earea[e] / t.edist[e];
+                t.dve[e] = (float)(((double)t.V[a] + phi[a]) - ((double)t.V[b] + phi[b]));
+                t.ie[e] = 0.0f;
+            }
+            __syncthreads();
+            // g_diag, and the V-sweep stencil (intracellular connections, in order)
+            float gd = 0.0f;
+            float vg[kDeg];
+            uint16_t vo[kDeg];
+            int vn_cnt = 0;
+            if (i < ns) {
+                if (st.n >= 0) {
+#pragma unroll
+                    for (int k = 0; k < kDeg; k++) {
+                        vg[k] = 0.0f; vo[k] = 0;
+                        if (k < st.n && t.ei[st.e[k]]) {
+                            const float g = t.gax[st.e[k]];
+                            gd += g;
+#pragma unroll
+                            for (int j = 0; j < kDeg; j++)
+                                if (j == vn_cnt) { vg[j] = g; vo[j] = st.o[k]; }
+                            vn_cnt++;
+                        }
+                    }
+                } else {
+                    for (int k = t.incoff[i]; k < t.incoff[i + 1]; k++) {
+                        const int e = t.inc[k] & 0x7FFF;
+                        if (t.ei[e]) gd += t.gax[e];
+                    }
+                }
+            }
+#pragma unroll 1
+            for (int q = 0; q < 7; q++) {
+                for (int e = tid; e < ne; e += nth) {
+                    if (!t.ei[e]) continue;
+                    const int a = t.ea[e], b = t.eb[e];
+                    const float C_a = t.in[q * S + a];
+                    const float C_b = t.in[q * S + b];
+                    const float x = kNpZ[q] * 0.03742f * t.dve[e];
+                    const float flux = kDiffC[q] * t.earea[e] * dt_sub / t.edist[e] *
+                                       (C_a * sg_bernoulli(-x) - C_b * sg_bernoulli(x));
+                    t.fl[e] = flux;
+                    t.ie[e] += kNpZ[q] * 96.485f * flux / dt_sub;
+                }
+                __syncthreads();
+                if (i < ns) {   // reads edge fluxes and its own concentration: in place
+                    const float vf = t.vf[i];
+                    double acc = 0.0;
+                    if (st.n >= 0) {
+#pragma unroll
+                        for (int k = 0; k < kDeg; k++) {
+                            if (k >= st.n) break;
+                            const int e = st.e[k];
+                            if (!t.ei[e]) continue;
+                            if ((st.bend >> k) & 1u) acc += (double)t.fl[e] / vf; else acc -= (double)t.fl[e] / vf;
+                        }
+                    } else {
+                        for (int k = t.incoff[i]; k < t.incoff[i + 1]; k++) {
+                            const uint16_t ent = t.inc[k];
+                            const int e = ent & 0x7FFF;
+                            if (!t.ei[e]) continue;
+                            if (ent & 0x8000) acc += (double)t.fl[e] / vf; else acc -= (double)t.fl[e] / vf;
+                        }
+                    }
+                    t.in[q * S + i] = (float)((double)t.in[q * S + i] + (double)(float)acc);
+                }
+                __syncthreads();
+            }
+            for (int e = tid; e < ne; e += nth) {
+                if (!t.ei[e]) continue;
+                t.ie[e] = t.ie[e] - t.gax[e] * t.dve[e];
+            }
+            __syncthreads();
+            float rhs = 0.0f, den = 1.0f;
+            if (i < ns) {
+                float inp = 0.0f;
+                if (st.n >= 0) {
+#pragma unroll
+                    for (int k = 0; k < kDeg; k++) {
+                        if (k >= st.n) break;
+                        const int e = st.e[k];
+                        if (!t.ei[e]) continue;
+                        if ((st.bend >> k) & 1u) inp -= t.ie[e]; else inp += t.ie[e];
+                    }
+                } else {
+                    for (int k = t.incoff[i]; k < t.incoff[i + 1]; k++) {
+                        const uint16_t ent = t.inc[k];
+                        const int e = ent & 0x7FFF;
+                        if (!t.ei[e]) continue;
+                        if (ent & 0x8000) inp -= t.ie[e]; else inp += t.ie[e];
+                    }
+                }
+                float C_dt = t.cm[i] / dt_sub;
+                if (C_dt < 1e-9f) C_dt = 1e-9f;
+                rhs = C_dt * t.V[i] + inp;
+                den = C_dt + gd;
+                t.vnA[i] = t.V[i];
+            }
+            __syncthreads();
+            float* vc = t.vnA;
+            float* vn = t.vnB;
+            for (int it = 0; it < 50; it++) {
+                if (i < ns) {
+                    float off = 0.0f;
+                    if (st.n >= 0) {
+#pragma unroll
+                        for (int k = 0; k < kDeg; k++)
+                            if (k < vn_cnt) off += vg[k] * vc[vo[k]];
+                    } else {
+                        for (int k = t.incoff[i]; k < t.incoff[i + 1]; k++) {
+                            const uint16_t ent = t.inc[k];
+                            const int e = ent & 0x7FFF;
+                            if (!t.ei[e]) continue;
+                            const int o = (ent & 0x8000) ? t.ea[e] : t.eb[e];
+                            off += t.gax[e] * vc[o];
+                        }
+                    }
+                    vn[i] = (rhs + off) / den;
+                }
+                __syncthreads();
+                float* tmp = vc; vc = vn; vn = tmp;
+            }
+            if (i < ns) t.V[i] = vc[i];
+            __syncthreads();
+        }
+
+        // ---- extracellular Nernst-Planck, 5 substeps (diffusion_kernel.h:244-281) ----
+        for (int sub = 0; sub < 5; sub++) {
+#pragma unroll 1
+            for (int q = 0; q < 7; q++) {
+                for (int e = tid; e < ne; e += nth) {
+                    const int a = t.ea[e], b = t.eb[e];
+                    const double Ca = t.out[q * S + a];
+                    const double Cb = t.out[q * S + b];
+                    const double dphi = phi[a] - phi[b];
+                    const float x = (float)(kNpZ[q] * 0.03742f * dphi);
+                    const double flux = kDiffC[q] * t.earea[e] * dt_sub / t.edist[e] *
+                                        (Ca * sg_bernoulli(-x) - Cb * sg_bernoulli(x));
+                    t.ed[e] = flux;
+                }
+                __syncthreads();
+                if (i < ns) {   // in place, as above
+                    const float vf = t.vf[i];
+                    double acc = 0.0;
+                    if (st.n >= 0) {
+#pragma unroll
+                        for (int k = 0; k < kDeg; k++) {
+                            if (k >= st.n) break;
+                            const int e = st.e[k];
+                            if ((st.bend >> k) & 1u) acc += t.ed[e] / (vf * EXTRA_VOLUME_RATIO);
+                            else acc -= t.ed[e] / (vf * EXTRA_VOLUME_RATIO);
+                        }
+                    } else {
+                        for (int k = t.incoff[i]; k < t.incoff[i + 1]; k++) {
+                            const uint16_t ent = t.inc[k];
+                            const int e = ent & 0x7FFF;
+                            if (ent & 0x8000) acc += t.ed[e] / (vf * EXTRA_VOLUME_RATIO);
+                            else acc -= t.ed[e] / (vf * EXTRA_VOLUME_RATIO);
+                        }
+                    }
+                    t.out[q * S + i] = (float)((double)t.out[q * S + i] + acc);
+                }
+                __syncthreads();
+            }
+        }
+
+        // ---- NT / ATP / heat / transcription (diffusion_kernel.h:284-363) ----
+        if (d.flags & NF_INTRA_NT) {
+            for (int nt = 0; nt < 15; nt++) {
+                if (i < ns) t.nb[i] = d.intra_nt[(size_t)nt * N + s0 + i];
+                __syncthreads();
+                fick<true, false>(t, ns, ne, tid, nth, i, st, gNtD[nt], 1e-12f, dt);
+                if (i < ns) d.intra_nt[(size_t)nt * N + s0 + i] = t.nb[i];
+            }
+        }
+        if (d.flags & NF_NT_DIFFUSE_OUT) {
+            for (int nt = 0; nt < 15; nt++) {
+                if (i < ns) t.nb[i] = d.nt[(size_t)nt * N + s0 + i];
+                __syncthreads();
+                fick<false, false>(t, ns, ne, tid, nth, i, st, gNtD[nt], 1e-12f, dt);
+                if (i < ns) d.nt[(size_t)nt * N + s0 + i] = t.nb[i];
+            }
+        }
+        {
+            if (i < ns) t.nb[i] = t.atp[i];
+            __syncthreads();
+            fick<true, true>(t, ns, ne, tid, nth, i, st, 0.14f, 1e-12f, dt);
+            if (i < ns) t.atp[i] = t.nb[i];
+        }
+        if (d.flags & NF_TEMP) {
+            if (i < ns) t.nb[i] = d.temp[s0 + i];
+            __syncthreads();
+            fick<true, true>(t, ns, ne, tid, nth, i, st, 0.0014f, 0.001f, dt);
+            if (i < ns) d.temp[s0 + i] = t.nb[i];
+        }
+        if (d.flags & NF_TXN) {
+            if (i < ns) t.nb[i] = d.txn[s0 + i];
+            __syncthreads();
+            fick<true, true>(t, ns, ne, tid, nth, i, st, 0.01f, 1e-9f, dt);
+            if (i < ns) d.txn[s0 + i] = t.nb[i];
+        }
+        if (i < ns) {
+#pragma unroll
+            for (int q = 0; q < 7; q++) {
+                double e = (double)t.out[q * S + i];
+                e += (kBathIon[q] - e) * dt / 1.0f;
+                if (e < 1e-9) e = 1e-9;
+                if (e > 1000.0) e = 1000.0;
+                t.out[q * S + i] = (float)e;
+            }
+        }
+    }
+
+    // ---- write back (each thread its own segment: no barrier needed) ----
+    if (i < ns) {
+        const uint32_t g = s0 + i;
+        d.V[g] = t.V[i];
+#pragma unroll
+        for (int q = 0; q < 7; q++) {
+            d.ion_in[(size_t)q * N + g] = t.in[q * S + i];
+            d.ion_out[(size_t)q * N + g] = t.out[q * S + i];
+        }
+        d.atp[g] = t.atp[i];
+        d.pre_rec[g] = make_float4(t.V[i], t.out[2 * S + i], c21d, c21h);
+        if (d.flags & NF_PRE_EXT) {
+            d.pre_ext[g] = make_float4(t.in[i], t.in[S + i], t.in[2 * S + i], t.out[i]);
+            d.pre_ext2[g] = t.out[S + i];
+        }
+    }
+}
+
+size_t diffusion_smem_bytes(uint32_t max_segs, uint32_t max_edges) {
+    return diff_layout(max_segs, max_edges, nullptr, nullptr);
+}
+
+uint32_t diffusion_threads(uint32_t max_segs) {
+    uint32_t t = (max_segs + 31) / 32 * 32;
+    return t < 32 ? 32 : t;
+}
+
+cudaError_t prepare_diffusion(const NetHost& host, cudaStream_t stream) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    if (!g_ntd_ready[dev]) {
+        k_init_ntd<<<1, 1, 0, stream>>>();
+        e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+        if (e != cudaSuccess) return e;
+        g_ntd_ready[dev] = true;
+    }
+    const size_t smem = diffusion_smem_bytes(host.max_tile_segs, host.max_tile_edges);
+    if (smem > 48 * 1024)
+        return cudaFuncSetAttribute(k_diffusion, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    return cudaSuccess;
+}
+
+void enqueue_diffusion(const NetDev& dev, const NetHost& host, float dt, cudaStream_t stream) {
+    const uint32_t S = host.max_tile_segs, E = host.max_tile_edges;
+    k_diffusion<<<dev.n_tiles, diffusion_threads(S), diffusion_smem_bytes(S, E), stream>>>(dev, dt, S, E);
+}
+
+}  // namespace bnc

@@ -53,6 +53,7 @@ struct NetDev {
     uint8_t* stype;
     uint8_t* sflags;
     float2* cav21_static;   // (density, state[1]) of the last Cav2.1 when it never updates
+    float2* c21_cur;        // the same after step 1 of the current tick (k_modifiers -> k_diffusion)
     float4* pre_rec;        // V, Ca_out, Cav2.1 density, Cav2.1 h  (after step 2.5)
     float4* pre_ext;        // Na_in, K_in, Ca_in, Na_out
     float* pre_ext2;        // K_out
@@ -151,7 +152,8 @@ struct NetHost {
     BuildOptions opt;                        // grouping the network was built with
     double algo_bytes_per_tick = 0;  // algorithmic HBM bytes per tick of this state schema
     double seg_bytes = 0, syn_bytes = 0;     // split by owner: segment state vs synapse state
-    double tile_bytes = 0, synk_bytes = 0;   // split by kernel: k_tile vs k_synapse
+    double tile_bytes = 0, synk_bytes = 0;   // tick figure split by step: 1 + 2.5 vs 3 + 4
+    double mod_bytes = 0, diff_bytes = 0;    // per launch of k_modifiers / k_diffusion
     bool perm_identity = true;               // device segment order equals the original order
     bool stim_identity = true;               // per-segment stimulus CSR order equals upload order
 };
@@ -186,15 +188,21 @@ int export_network(const NetDev& dev, const NetHost& host, uint64_t ticks_run, B
 cudaError_t prepare_tick(const NetDev& dev, const NetHost& host, cudaStream_t stream);
 cudaError_t enqueue_tick(const NetDev& dev, const NetHost& host, float dt, unsigned long long tick, int first_tick,
                          cudaStream_t stream);
+cudaError_t launch_tick(const NetDev& dev, const NetHost& host, float dt, unsigned long long tick, int first_tick,
+                        cudaStream_t stream);
+// the three kernels of a tick, one at a time (profiling)
+cudaError_t launch_modifiers(const NetDev& dev, const NetHost& host, float dt, unsigned long long tick,
+                             cudaStream_t stream);
+cudaError_t launch_diffusion(const NetDev& dev, const NetHost& host, float dt, cudaStream_t stream);
+cudaError_t launch_synapse(const NetDev& dev, float dt, unsigned long long tick, int first_tick,
+                           cudaStream_t stream);
 cudaError_t launch_set_clock(unsigned long long* clock, unsigned long long tick, unsigned long long ticks_run,
                              cudaStream_t stream);
 cudaError_t launch_advance_clock(unsigned long long* clock, cudaStream_t stream);
-cudaError_t launch_tick(const NetDev& dev, const NetHost& host, float dt, unsigned long long tick,
-                        int first_tick, cudaStream_t stream);
-cudaError_t launch_tile(const NetDev& dev, const NetHost& host, float dt, unsigned long long tick,
-                        cudaStream_t stream);
-cudaError_t launch_synapse(const NetDev& dev, float dt, unsigned long long tick, int first_tick,
-                           cudaStream_t stream);
-size_t tile_smem_bytes(uint32_t max_segs, uint32_t max_edges);
+// diffuse.cu
+cudaError_t prepare_diffusion(const NetHost& host, cudaStream_t stream);
+void enqueue_diffusion(const NetDev& dev, const NetHost& host, float dt, cudaStream_t stream);
+size_t diffusion_smem_bytes(uint32_t max_segs, uint32_t max_edges);
+size_t tile_smem_bytes(uint32_t max_segs);
 
 }  // namespace bnc

@@ -167,9 +167,10 @@ int bnc_time_ticks(void* sim, uint32_t n_ticks, float dt, float* ms);
 int bnc_step_io(void* sim, float dt, const float* stim_amp, uint32_t n_amp, float* v_out, uint32_t n_v);
 
 /* Runs n ticks with CUDA events around each kernel; returns the summed device
- * time of the tile kernel (modifiers + electrodiffusion) and of the synapse +
- * membrane kernel. */
-int bnc_profile_ticks(void* sim, uint32_t n_ticks, float dt, float* ms_tile, float* ms_synapse);
+ * time of the modifier kernel (step 1), the electrodiffusion kernel (step 2.5)
+ * and the synapse + membrane kernel (steps 3 and 4). */
+int bnc_profile_ticks(void* sim, uint32_t n_ticks, float dt, float* ms_modifiers, float* ms_diffusion,
+                      float* ms_synapse);
 
 /* Copies device state into the host AoS view (no-op when none is held). */
 int bnc_sync_to_host(void* sim);
@@ -194,8 +195,9 @@ typedef struct {
     uint64_t ticks;
     double algo_bytes_per_tick;   /* algorithmic HBM bytes one tick moves (state schema) */
     double seg_bytes_per_tick, syn_bytes_per_tick;          /* split by state owner */
-    double tile_bytes_per_tick, synapse_kernel_bytes_per_tick; /* split by kernel */
+    double tile_bytes_per_tick, synapse_kernel_bytes_per_tick; /* split: steps 1 + 2.5 / steps 3 + 4 */
     uint32_t warp_cap, tile_segs;  /* grouping the network was built with */
+    double modifier_kernel_bytes, diffusion_kernel_bytes;  /* per launch of each (state round trip included) */
 } BncNetInfo;
 int bnc_network_info(void* sim, BncNetInfo* info);
 
