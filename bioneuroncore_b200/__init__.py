@@ -39,7 +39,8 @@ NEW_SYMBOLS = ["bnc_netgen_aos", "bnc_netgen_free", "bnc_last_error", "bnc_load_
                "bnc_plan_generated", "bnc_step_io", "bnc_profile_ticks", "bnc_run_ticks_static_scratch",
                "bnc_plan_aos", "bnc_bion_load", "bnc_bion_unload", "bnc_bion_save", "bnc_load_ensemble_generated",
                "bnc_load_ensemble_aos", "bnc_ensemble_member", "bnc_plan_ensemble_generated", "bnc_ensemble_params",
-               "bnc_run_ticks_graph", "bnc_load_ensemble_tuned", "bnc_time_ticks_graph"]
+               "bnc_run_ticks_graph", "bnc_load_ensemble_tuned", "bnc_time_ticks_graph", "bnc_load_generated_opts",
+               "bnc_plan_generated_opts"]
 
 
 class NetInfo(C.Structure):
@@ -52,15 +53,25 @@ class NetInfo(C.Structure):
         ("modifier_kernel_bytes", C.c_double), ("diffusion_kernel_bytes", C.c_double)]
 
 
+class BuildOptions(C.Structure):
+    """Device-layout options (include/bnc_b200.h BncBuildOptions); 0 = default."""
+    _fields_ = [("warp_cap", C.c_uint32), ("tile_segs", C.c_uint32), ("phase_cap", C.c_uint32),
+                ("mod_ctas", C.c_uint32)]
+
+
 class Tuning(C.Structure):
     _fields_ = [("warp_cap", C.c_uint32), ("tile_segs", C.c_uint32), ("ms_per_tick", C.c_float),
                 ("candidates_tried", C.c_uint32), ("sample_members", C.c_uint32)]
 
 
-def plan_generated(params):
+def plan_generated(params, options=None):
     """Host-only planning of a generated network (no device needed); returns NetInfo."""
     inf = NetInfo()
-    _check(load_library().bnc_plan_generated(C.byref(params), C.byref(inf)), "bnc_plan_generated")
+    if options is None:
+        _check(load_library().bnc_plan_generated(C.byref(params), C.byref(inf)), "bnc_plan_generated")
+    else:
+        _check(load_library().bnc_plan_generated_opts(C.byref(params), C.byref(options), C.byref(inf)),
+               "bnc_plan_generated_opts")
     return inf
 
 
@@ -125,6 +136,7 @@ def load_library(path=LIB_PATH):
         "bnc_ensemble_member": ([vp, u32, vp], i32), "bnc_plan_ensemble_generated": ([vp, u32, vp], i32),
         "bnc_ensemble_params": ([C.c_uint64, u32, u32, u32, vp], i32), "bnc_run_ticks_graph": ([vp, u32, f32], i32),
         "bnc_load_ensemble_tuned": ([vp, vp, u32, u32, f32, vp], i32), "bnc_time_ticks_graph": ([vp, u32, f32, vp], i32),
+        "bnc_load_generated_opts": ([vp, vp, vp], i32), "bnc_plan_generated_opts": ([vp, vp, vp], i32),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -225,8 +237,12 @@ class Backend:
     def load_network(self, net):
         _check(self.lib.bnc_load_aos(self.h, C.byref(net.data), net.stim_ptr, net.n_stim), "bnc_load_aos")
 
-    def load_generated(self, params):
-        _check(self.lib.bnc_load_generated(self.h, C.byref(params)), "bnc_load_generated")
+    def load_generated(self, params, options=None):
+        if options is None:
+            _check(self.lib.bnc_load_generated(self.h, C.byref(params)), "bnc_load_generated")
+        else:
+            _check(self.lib.bnc_load_generated_opts(self.h, C.byref(params), C.byref(options)),
+                   "bnc_load_generated_opts")
 
     def run_ticks(self, n, dt):
         _check(self.lib.bnc_run_ticks(self.h, n, C.c_float(dt)), "bnc_run_ticks")
@@ -313,4 +329,4 @@ class Backend:
 __all__ = ["Backend", "Network", "NetgenParams", "BionData", "BackendError", "load_library", "last_error",
            "NET_SMALL", "NET_LARGE", "NET_TREES", "NET_ENSEMBLE_MEMBER", "NET_ADJOINT", "NETGEN_NO_SYNAPSES",
            "NETGEN_NO_CONNECTIONS", "NETGEN_NO_STIMULI", "NETGEN_PERTURB_IONS", "SEG_FIELDS", "SYN_FIELDS",
-           "DROPIN_SYMBOLS", "NEW_SYMBOLS", "EnsembleMember", "Tuning", "ensemble_params", "plan_ensemble", "plan_generated"]
+           "DROPIN_SYMBOLS", "NEW_SYMBOLS", "EnsembleMember", "Tuning", "BuildOptions", "ensemble_params", "plan_ensemble", "plan_generated"]

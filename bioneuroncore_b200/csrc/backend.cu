@@ -560,7 +560,18 @@ int bnc_load_aos(void* sim, const BncBionData* data, const BncCurrentStimulus* s
     return rc;
 }
 
-int bnc_load_generated(void* sim, const BncNetgenParams* p) {
+static BuildOptions to_options(const BncBuildOptions* o) {
+    BuildOptions opt;
+    if (o) {
+        if (o->warp_cap) opt.warp_cap = o->warp_cap;
+        if (o->tile_segs) opt.tile_segs = o->tile_segs;
+        opt.phase_cap = o->phase_cap;
+        if (o->mod_ctas) opt.mod_ctas = o->mod_ctas;
+    }
+    return opt;
+}
+
+int bnc_load_generated_opts(void* sim, const BncNetgenParams* p, const BncBuildOptions* o) {
     if (!sim || !p) { set_error("bnc_load_generated: null argument"); return BNC_ERR_ARG; }
     Backend* b = static_cast<Backend*>(sim);
     b->reset_network();
@@ -572,16 +583,19 @@ int bnc_load_generated(void* sim, const BncNetgenParams* p) {
     int rc = generate_network(*p, sink, &shape);
     if (rc != BNC_OK) { set_error("bnc_load_generated: invalid parameters"); return rc; }
     cudaSetDevice(b->device);
-    rc = build_network(hn, b->stim, &b->dev, &b->host, &b->allocs);
+    rc = build_network(hn, b->stim, &b->dev, &b->host, &b->allocs, to_options(o));
     if (rc != BNC_OK) { b->reset_network(); return rc; }
     b->loaded = true;
     return BNC_OK;
 }
 
-static int plan_info(const HostNet& hn, const Stimuli& stim, BncNetInfo* info) {
+int bnc_load_generated(void* sim, const BncNetgenParams* p) { return bnc_load_generated_opts(sim, p, nullptr); }
+
+static int plan_info(const HostNet& hn, const Stimuli& stim, BncNetInfo* info,
+                     const BuildOptions& opt = BuildOptions()) {
     NetDev dev;
     NetHost host;
-    int rc = build_network(hn, stim, &dev, &host, nullptr);
+    int rc = build_network(hn, stim, &dev, &host, nullptr, opt);
     if (rc != BNC_OK) return rc;
     std::memset(info, 0, sizeof(*info));
     info->n_segments = dev.n_seg; info->n_connections = host.n_conn; info->n_synapses = dev.n_syn;
@@ -596,7 +610,9 @@ static int plan_info(const HostNet& hn, const Stimuli& stim, BncNetInfo* info) {
     return BNC_OK;
 }
 
-int bnc_plan_generated(const BncNetgenParams* p, BncNetInfo* info) {
+int bnc_plan_generated(const BncNetgenParams* p, BncNetInfo* info) { return bnc_plan_generated_opts(p, nullptr, info); }
+
+int bnc_plan_generated_opts(const BncNetgenParams* p, const BncBuildOptions* o, BncNetInfo* info) {
     if (!p || !info) { set_error("bnc_plan_generated: null argument"); return BNC_ERR_ARG; }
     HostNet hn;
     Stimuli stim;
@@ -606,7 +622,7 @@ int bnc_plan_generated(const BncNetgenParams* p, BncNetInfo* info) {
     NetShape shape;
     int rc = generate_network(*p, sink, &shape);
     if (rc != BNC_OK) { set_error("bnc_plan_generated: invalid parameters"); return rc; }
-    return plan_info(hn, stim, info);
+    return plan_info(hn, stim, info, to_options(o));
 }
 
 static int load_members(Backend* b, const BncNetgenParams* members, uint32_t n_members, const BuildOptions& opt) {

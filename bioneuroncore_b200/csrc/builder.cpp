@@ -350,8 +350,10 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
     }
     lap("components");
     // ---- tile packing: whole components, one component per warp slot ----
-    if (opt.warp_cap < 1 || opt.tile_segs < 32 || opt.tile_segs > (uint32_t)kMaxTileSegs) {
-        set_error("grouping options out of range (warp_cap %u, tile_segs %u)", opt.warp_cap, opt.tile_segs);
+    if (opt.warp_cap < 1 || opt.tile_segs < 32 || opt.tile_segs > (uint32_t)kMaxTileSegs ||
+        opt.phase_cap > 4096 || (opt.mod_ctas != 2 && opt.mod_ctas != 3)) {
+        set_error("build options out of range (warp_cap %u, tile_segs %u, phase_cap %u, mod_ctas %u)", opt.warp_cap,
+                  opt.tile_segs, opt.phase_cap, opt.mod_ctas);
         return BNC_ERR_ARG;
     }
     host->opt = opt;
@@ -519,7 +521,7 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
         std::vector<uint32_t> ptr(n, 0);
         uint64_t remaining = act_slot.size();
         std::vector<uint64_t> count(256);
-        const uint32_t cap = std::max<uint32_t>(2 * max_active + 4, 8);
+        const uint32_t cap = opt.phase_cap ? opt.phase_cap : std::max<uint32_t>(2 * max_active + 4, 8);
         bool greedy_ok = true;
         while (remaining > 0) {
             std::fill(count.begin(), count.end(), 0);
@@ -706,7 +708,55 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
         for (uint32_t k : syn_valid) sorted[pos[host->inv[hn.syn[k].post_segment]]++] = k;
         syn_valid.swap(sorted);
     }
-    std::vector<uint32_t> sy_pre(K), sy_id(K), rc_off(K + 1, 0);
+    // ---- synapse-kernel threads and the sliced synapse order ----
+    // Thread t of the synapse kernel handles segment th_seg[t]: first every segment
+    // with synapses, by synapse count descending (stable in device order), then the
+    // rest.  Within a warp the lanes that still have a k-th synapse therefore form a
+    // prefix, and the k-th synapses of a warp's lanes sit next to each other: synapse
+    // (warp w, k, lane l) is at w_off[w] + sum over k' < k of the active lanes + l.
+    // Receptors of the synapses of slice (w, k): receptor j of each lane that has
+    // one, lanes in order, j ascending.  Each lane still walks its own synapses and
+    // receptors in original order.
+    std::vector<uint32_t> th_seg;
+    std::vector<uint16_t> th_cnt;
+    th_seg.reserve(n);
+    th_cnt.reserve(n);
+    {
+        std::vector<uint32_t> post_list, rest_list;
+        for (uint32_t d = 0; d < n; d++) (post_off[d + 1] > post_off[d] ? post_list : rest_list).push_back(d);
+        std::stable_sort(post_list.begin(), post_list.end(), [&](uint32_t a, uint32_t b) {
+            return post_off[a + 1] - post_off[a] > post_off[b + 1] - post_off[b];
+        });
+        for (uint32_t d : post_list) {
+            const uint32_t c = post_off[d + 1] - post_off[d];
+            if (c > 65535) { set_error("segment %u receives %u synapses (at most 65535)", host->perm[d], c); return BNC_ERR_UNSUPPORTED; }
+            th_seg.push_back(d);
+            th_cnt.push_back((uint16_t)c);
+        }
+        for (uint32_t d : rest_list) { th_seg.push_back(d); th_cnt.push_back(0); }
+    }
+    const uint32_t NW = (n + 31) / 32;
+    std::vector<uint32_t> w_off(NW + 1, 0), rw_off(NW + 1, 0);
+    std::vector<uint32_t> slot_syn;   // sliced position -> index into syn_valid (post-sorted)
+    slot_syn.reserve(K);
+    for (uint32_t w = 0; w < NW; w++) {
+        w_off[w] = (uint32_t)slot_syn.size();
+        uint32_t maxc = 0;
+        for (uint32_t l = 0; l < 32 && 32 * w + l < n; l++) maxc = std::max<uint32_t>(maxc, th_cnt[32 * w + l]);
+        for (uint32_t k = 0; k < maxc; k++)
+            for (uint32_t l = 0; l < 32 && 32 * w + l < n; l++) {
+                const uint32_t t = 32 * w + l;
+                if (th_cnt[t] > k) slot_syn.push_back(post_off[th_seg[t]] + k);
+            }
+    }
+    w_off[NW] = (uint32_t)slot_syn.size();
+    {
+        std::vector<uint32_t> sliced(K);
+        for (uint32_t q = 0; q < K; q++) sliced[q] = syn_valid[slot_syn[q]];
+        syn_valid.swap(sliced);
+    }
+    std::vector<uint32_t> sy_pre(K), sy_id(K);
+    std::vector<uint8_t> rc_cnt(K, 0), kept((size_t)K * 8, 0);
     std::vector<float> sy_prel(K), sy_amt(K), sy_tauc(K), sy_delay(K), sy_prea(K), sy_posta(K), sy_gK(K),
         sy_gNa(K), sy_bouton(K), sy_spine(K), sy_camkii(K), sy_calcn(K), sy_facil(K), sy_weight(K), sy_cleft(K),
         sy_rrp(K), sy_rrpm(K), sy_rrpr(K), sy_scale(K, 1.0f);
@@ -743,25 +793,51 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
         sy_cleft[q] = y.cleft_neurotransmitter[ntt];
         sy_rrp[q] = y.RRP; sy_rrpm[q] = y.RRP_max; sy_rrpr[q] = y.RRP_recovery;
         bool myel_post = (sflags[y.post_segment] & SF_MYELIN) != 0;
+        uint32_t nr = 0;
         for (uint8_t j = 0; j < y.post_receptor_count; j++) {
             const ModLite& r = hn.post_rec(syn_valid[q], j);
             if (myel_post && is_ionotropic(r.type)) continue;   // simulation_host.cpp:495
             if (r.active_vars >= 8) { set_error("synapse %u receptor %u: active_vars out of range", syn_valid[q], j); return BNC_ERR_FORMAT; }
-            rc_type.push_back(r.type);
-            rc_av.push_back(r.active_vars);
-            rc_den.push_back(r.density);
-            rc_st0.push_back(r.state[0]);
-            rc_st1.push_back(r.state[1]);
-            rc_st2.push_back(r.state[2]);
             if (r.active_vars >= 3 && r.active_vars <= 6) {
                 set_error("synapse %u receptor %u: active_vars %u not supported", syn_valid[q], j, r.active_vars);
                 return BNC_ERR_UNSUPPORTED;
             }
-            host->rec_syn.push_back(q);
-            host->rec_slot.push_back(j);
+            kept[(size_t)q * 8 + nr] = j;
+            nr++;
         }
-        rc_off[q + 1] = (uint32_t)rc_type.size();
+        rc_cnt[q] = (uint8_t)nr;
     }
+    // receptor order: slice by slice, receptor j of each lane that has one
+    for (uint32_t w = 0; w < NW; w++) {
+        rw_off[w] = (uint32_t)rc_type.size();
+        uint32_t maxc = 0;
+        for (uint32_t l = 0; l < 32 && 32 * w + l < n; l++) maxc = std::max<uint32_t>(maxc, th_cnt[32 * w + l]);
+        uint32_t q = w_off[w];
+        for (uint32_t k = 0; k < maxc; k++) {
+            uint32_t a = 0;   // lanes with a k-th synapse: a prefix of the warp
+            while (a < 32 && 32 * w + a < n && th_cnt[32 * w + a] > k) a++;
+            uint32_t maxr = 0;
+            for (uint32_t l = 0; l < a; l++) maxr = std::max<uint32_t>(maxr, rc_cnt[q + l]);
+            for (uint32_t j = 0; j < maxr; j++)
+                for (uint32_t l = 0; l < a; l++) {
+                    const uint32_t qq = q + l;
+                    if (rc_cnt[qq] <= j) continue;
+                    const uint8_t slot = kept[(size_t)qq * 8 + j];
+                    const ModLite& r = hn.post_rec(syn_valid[qq], slot);
+                    rc_type.push_back(r.type);
+                    rc_av.push_back(r.active_vars);
+                    rc_den.push_back(r.density);
+                    rc_st0.push_back(r.state[0]);
+                    rc_st1.push_back(r.state[1]);
+                    rc_st2.push_back(r.state[2]);
+                    host->rec_syn.push_back(qq);
+                    host->rec_slot.push_back(slot);
+                }
+            q += a;
+        }
+    }
+    rw_off[NW] = (uint32_t)rc_type.size();
+
     lap("synapses");
     const uint32_t NR = (uint32_t)rc_type.size();
     std::vector<float> rc_st((size_t)3 * NR);
@@ -825,7 +901,10 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
         dev->it_meta = up(allocs, it_meta, &rc);
         dev->it_den = up(allocs, it_den, &rc);
         dev->it_st = up(allocs, it_st, &rc);
-        dev->post_off = up(allocs, post_off, &rc);
+        dev->th_seg = up(allocs, th_seg, &rc);
+        dev->th_cnt = up(allocs, th_cnt, &rc);
+        dev->w_off = up(allocs, w_off, &rc);
+        dev->rw_off = up(allocs, rw_off, &rc);
         dev->sy_pre = up(allocs, sy_pre, &rc);
         dev->sy_id = up(allocs, sy_id, &rc);
         dev->sy_prel = up(allocs, sy_prel, &rc);
@@ -849,7 +928,7 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
         dev->sy_rrp_max = up(allocs, sy_rrpm, &rc);
         dev->sy_rrp_rec = up(allocs, sy_rrpr, &rc);
         dev->sy_scale = up(allocs, sy_scale, &rc);
-        dev->rc_off = up(allocs, rc_off, &rc);
+        dev->rc_cnt = up(allocs, rc_cnt, &rc);
         dev->rc_type = up(allocs, rc_type, &rc);
         dev->rc_av = up(allocs, rc_av, &rc);
         dev->rc_den = up(allocs, rc_den, &rc);

@@ -86,8 +86,12 @@ struct NetDev {
     float* vc_target;
     unsigned long long* vc_start;
     unsigned long long* vc_end;
-    // synapses in post-segment CSR order
-    uint32_t* post_off;       // [n_seg+1]
+    // synapse-kernel threads: segments with synapses by count descending, then the rest
+    uint32_t* th_seg;         // [n_seg] device segment of thread t
+    uint16_t* th_cnt;         // [n_seg] its synapse count
+    uint32_t* w_off;          // [warps+1] first sliced synapse of each warp
+    uint32_t* rw_off;         // [warps+1] first sliced receptor of each warp
+    // synapses in sliced order (warp, k-th synapse of the lane, lane)
     uint32_t* sy_pre;         // device index of the presynaptic segment
     uint32_t* sy_id;
     float* sy_prel;
@@ -111,7 +115,7 @@ struct NetDev {
     float* sy_rrp_max;
     float* sy_rrp_rec;
     float* sy_scale;          // receptor density scale (1 reproduces the reference)
-    uint32_t* rc_off;         // [n_syn+1]
+    uint8_t* rc_cnt;          // [n_syn] receptors of each synapse (receptors sliced likewise)
     uint8_t* rc_type;
     uint8_t* rc_av;
     float* rc_den;
@@ -134,6 +138,11 @@ struct NetDev {
 struct BuildOptions {
     uint32_t warp_cap = 64;
     uint32_t tile_segs = kMaxTileSegs;
+    // Modifier phases: the greedy type-uniform schedule is kept while it needs at most
+    // phase_cap phases (0: 2 x the longest active-modifier list + 4), else slot order.
+    uint32_t phase_cap = 0;
+    // Resident CTAs per SM the modifier kernel is compiled for (2 or 3: register budget).
+    uint32_t mod_ctas = 2;
 };
 
 // Host copy of everything the exporter needs to map device state back.
@@ -199,6 +208,8 @@ cudaError_t launch_synapse(const NetDev& dev, float dt, unsigned long long tick,
 cudaError_t launch_set_clock(unsigned long long* clock, unsigned long long tick, unsigned long long ticks_run,
                              cudaStream_t stream);
 cudaError_t launch_advance_clock(unsigned long long* clock, cudaStream_t stream);
+// synapse.cu: per-device receptor constants (outside stream capture)
+cudaError_t prepare_synapse(cudaStream_t stream);
 // diffuse.cu
 cudaError_t prepare_diffusion(const NetHost& host, cudaStream_t stream);
 void enqueue_diffusion(const NetDev& dev, const NetHost& host, float dt, cudaStream_t stream);

@@ -1,26 +1,124 @@
 // synapse.cu -- the synapse + membrane kernel of a tick (steps 3 and 4).
 //
-// One thread per segment (device order): the segment's incoming synapses in original
-// synapse order (post-segment CSR, no atomics), then the membrane update of the same
-// segment.  Presynaptic values come from the record the tile kernel wrote after step
-// 2.5 (V, Ca_out, the Cav2.1 gate), so a synapse never reads state another thread is
-// writing.
+// Thread t handles segment th_seg[t]: first the segments that receive synapses, by
+// synapse count descending, then the rest (membrane update only).  Each thread walks
+// its segment's incoming synapses in original synapse order, then updates the
+// membrane of that segment, so no atomics are involved and every sum keeps the
+// reference's order.  Synapse and receptor arrays are stored warp-sliced: the k-th
+// synapses of a warp's lanes are adjacent (lanes that still have one form a prefix of
+// the warp, since counts descend), and the j-th receptors of a slice's synapses are
+// adjacent, so the loads of a loop iteration are coalesced.  All four ionotropic
+// receptors run one code path with per-lane constants, so lanes holding different
+// receptor types do not serialise.  Presynaptic values come from the record the
+// diffusion kernel wrote after step 2.5 (V, Ca_out, the Cav2.1 gate).
 #include <cuda_runtime.h>
 #include "net.h"
 #include "physics.cuh"
 
 namespace bnc {
 
-// modifier_helpers.h:1213-1279 via receptors_biological.cpp:42-82
-__device__ __forceinline__ double receptor_current(uint8_t type, DMod& m, DSeg& s, float dt, const float* ntv,
-                                                   float scale) {
-    switch (type) {
-        case 8: return m.av ? dp_ampa_current<false>(m, s, dt, ntv[0], scale) : dp_ampa_current<true>(m, s, dt, ntv[0], scale);
-        case 9: return m.av ? dp_nmda_current<false>(m, s, dt, ntv[0], scale) : dp_nmda_current<true>(m, s, dt, ntv[0], scale);
-        case 11: return m.av ? dp_gabaa_current<false>(m, s, dt, ntv[1], scale) : dp_gabaa_current<true>(m, s, dt, ntv[1], scale);
-        default: return m.av ? dp_glycine_current<false>(m, s, dt, ntv[7], scale) : dp_glycine_current<true>(m, s, dt, ntv[7], scale);
+namespace {
+
+// Ionotropic receptor constants (receptors_biological.cpp:42-82 through
+// modifier_helpers.h:1213-1279): AMPA, NMDA, GABA-A, glycine.  The permeabilities at
+// the default conductance are computed once on the device with the same helpers the
+// models use, so they equal the constants a per-type specialisation folds.
+struct RecKind {
+    float gamma_ps, EC50, tau_rise, tau_decay, P_Na_ratio, P_K_ratio, P_Ca_ratio, tau_desens, K_desens;
+    int is_anion, nmda;
+    double P_Na, P_K, P_Ca, P_Cl;
+};
+
+__device__ RecKind gRec[4];
+
+__global__ void k_init_receptors() {
+    const float c[4][9] = {{8.0f, 0.5f, 0.5f, 3.0f, 0.5f, 0.5f, 0.0f, 3.0f, 0.0f},
+                           {50.0f, 1.0f, 5.0f, 50.0f, 0.08f, 0.08f, 0.84f, 0.0f, 0.0f},
+                           {28.0f, 1.0f, 1.0f, 5.0f, 0.0f, 0.0f, 0.0f, 2000.0f, 0.0f},
+                           {60.0f, 0.5f, 0.3f, 5.0f, 0.0f, 0.0f, 0.0f, 2000.0f, 0.0f}};
+    for (int k = 0; k < 4; k++) {
+        RecKind& r = gRec[k];
+        r.gamma_ps = c[k][0]; r.EC50 = c[k][1]; r.tau_rise = c[k][2]; r.tau_decay = c[k][3];
+        r.P_Na_ratio = c[k][4]; r.P_K_ratio = c[k][5]; r.P_Ca_ratio = c[k][6];
+        r.tau_desens = c[k][7]; r.K_desens = c[k][8];
+        r.is_anion = k >= 2;
+        r.nmda = k == 1;
+        dp_partial_P(r.gamma_ps, r.P_Na_ratio, r.P_K_ratio, r.P_Ca_ratio, &r.P_Na, &r.P_K, &r.P_Ca);
+        r.P_Cl = dp_ghk_P(r.gamma_ps, 1.0f, GHK_CBAR_CL_MM);
     }
 }
+
+static bool g_rec_ready[64] = {false};   // per device
+
+__device__ __forceinline__ int receptor_kind(uint8_t type) {
+    return type == 8 ? 0 : (type == 9 ? 1 : (type == 11 ? 2 : 3));
+}
+
+// modifier_helpers.h:1213-1279 (ionotropic_ghk_current) with the receptor's constants
+// as data; NMDA adds the Mg2+ block and CDI/co-agonist factor (receptors_biological.cpp:48-70).
+__device__ __forceinline__ double receptor_current(const RecKind& K, DMod& m, DSeg& s, float dt, float nt,
+                                                  float mod_scale) {
+    float area = m.area;
+    double V = ((double)s.V);
+    double vol = s.vol;
+    double cpm = FARADAY_CONST * vol / 1000.0;
+    const bool custom = m.av != 0;   // conductance override through active_vars
+    float p_gamma_ps = K.gamma_ps;
+    if (custom) {
+        float stav = (m.av == 7) ? m.area : (m.av == 1 ? m.st[1] : (m.av == 2 ? m.st[2] : 0.0f));
+        p_gamma_ps = (m.av > 0 && m.av < 8 && ((double)stav) > 0.0f) ? (float)((double)stav) : K.gamma_ps;
+    }
+    float r_inf = nt / (nt + K.EC50);
+    float r = m.st[0];
+    float tau = (r_inf > r) ? K.tau_rise : K.tau_decay;
+    m.st[0] = (float)(((double)m.st[0]) + (r_inf - r) * dt / tau);
+    if (((double)m.st[0]) < 0.0f) m.st[0] = 0.0f;
+    if (((double)m.st[0]) > 1.0f) m.st[0] = 1.0f;
+    float open_prob = m.st[0];
+    if (K.tau_desens > 0.0f) {
+        float kd = (K.K_desens > 0.0f) ? K.K_desens : K.EC50;
+        float dd = m.st[1];
+        float d_inf = nt / (nt + kd);
+        dd += (d_inf - dd) * dt / K.tau_desens;
+        if (dd < 0.0f) dd = 0.0f;
+        if (dd > 1.0f) dd = 1.0f;
+        m.st[1] = dd;
+        open_prob *= (1.0f - dd);
+    }
+    double N = ((double)m.den) * area;
+    double I;
+    if (K.is_anion) {
+        double P_Cl = custom ? dp_ghk_P(p_gamma_ps, 1.0f, GHK_CBAR_CL_MM) : K.P_Cl;
+        double flux_Cl = dp_ghk_anion_c(s.gc, V, ((double)s.in[3]), ((double)s.out[3]));
+        double I_Cl = P_Cl * flux_Cl * N * open_prob * mod_scale * A_TO_PA;
+        s.in[3] = (float)(((double)s.in[3]) + (I_Cl * dt) / cpm);
+        dp_clamp_ions(s.in);
+        I = -I_Cl;
+    } else {
+        double P_Na = K.P_Na, P_K = K.P_K, P_Ca = K.P_Ca;
+        if (custom) dp_partial_P(p_gamma_ps, K.P_Na_ratio, K.P_K_ratio, K.P_Ca_ratio, &P_Na, &P_K, &P_Ca);
+        double I_Na = P_Na * dp_ghk_mono_c(s.gc, V, ((double)s.in[0]), ((double)s.out[0])) * N * open_prob * mod_scale * A_TO_PA;
+        double I_K = P_K * dp_ghk_mono_c(s.gc, V, ((double)s.in[1]), ((double)s.out[1])) * N * open_prob * mod_scale * A_TO_PA;
+        double I_total = I_Na + I_K;
+        s.in[0] = (float)(((double)s.in[0]) - (I_Na * dt) / cpm);
+        s.in[1] = (float)(((double)s.in[1]) - (I_K * dt) / cpm);
+        if (K.P_Ca_ratio > 0.0f) {
+            double I_Ca = P_Ca * dp_ghk_div_c(s.gc, V, ((double)s.in[2]), ((double)s.out[2])) * N * open_prob * mod_scale * A_TO_PA;
+            I_total += I_Ca;
+            s.in[2] = (float)(((double)s.in[2]) - (I_Ca * dt) / (2.0f * cpm));
+        }
+        dp_clamp_ions(s.in);
+        I = -I_total;
+    }
+    if (K.nmda) {
+        float mg_block = (float)(1.0f / (1.0f + (1.0f / 3.57f) * dm_exp(-0.062f * ((double)s.V))));
+        double c = dp_nmda_cdi_coagonist(m, s, dt);
+        I = I * mg_block * c;
+    }
+    return I;
+}
+
+}  // namespace
 
 __device__ __forceinline__ float xorshift32_rnd(uint32_t seed) {
     uint32_t x = seed;
@@ -32,25 +130,29 @@ __device__ __forceinline__ float xorshift32_rnd(uint32_t seed) {
 
 __global__ void __launch_bounds__(256)
 k_synapse(NetDev d, float dt, unsigned long long tick, int first_tick) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t N = d.n_seg;
-    if (i >= N) return;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t lt_mask = (1u << lane) - 1u;
     if (d.clock) {
         tick = d.clock[0];
         first_tick = d.clock[1] == 0 ? 1 : 0;
     }
-    const uint8_t sfl = d.sflags[i];
+    // every lane of the warp takes part in the slice ballots below, valid or not
+    const bool valid = t < N;
+    const uint32_t i = valid ? d.th_seg[t] : 0u;
+    const uint32_t cnt = valid ? (uint32_t)d.th_cnt[t] : 0u;
+    const uint32_t maxc = __reduce_max_sync(0xFFFFFFFFu, cnt);
+    const uint8_t sfl = valid ? d.sflags[i] : (uint8_t)0;
     const bool syn_on = (d.flags & NF_SYNAPSES) != 0;
-    float ntv[15];
-#pragma unroll
-    for (int q = 0; q < 15; q++) ntv[q] = 0.0f;
-    if (sfl & SF_NMDA) ntv[0] = 1.0f;   // bath NMDA (simulation_host.cpp:337-340)
-    double ib = d.ibuf[i];
+    // the neurotransmitters a synapse can deliver: glutamate, GABA, glycine (0, 1, 7)
+    float nt_glu = (sfl & SF_NMDA) ? 1.0f : 0.0f;   // bath NMDA (simulation_host.cpp:337-340)
+    float nt_gaba = 0.0f, nt_gly = 0.0f;
+    double ib = valid ? d.ibuf[i] : 0.0;
     DSeg s;
-    s.V = d.V[i];
-    const uint32_t k0 = d.post_off[i], k1 = d.post_off[i + 1];
+    s.V = valid ? d.V[i] : 0.0f;
     bool touched = false;
-    if (k1 > k0) {
+    if (cnt > 0) {
 #pragma unroll
         for (int q = 0; q < 7; q++) s.in[q] = d.ion_in[(size_t)q * N + i];
 #pragma unroll
@@ -62,185 +164,213 @@ k_synapse(NetDev d, float dt, unsigned long long tick, int first_tick) {
         ghk_cache_fill(s.gc, s.V);   // V_m is constant through step 3
     }
     const uint32_t K = d.n_syn;
-    for (uint32_t k = k0; k < k1; k++) {
-        const uint32_t pre = d.sy_pre[k];
-        const float4 pr = d.pre_rec[pre];
-        const uint8_t sf = d.sy_flags[k];
-        const int ntt = sf >> 4;
-        float cleft = d.sy_cleft[k];
-        const float delay = d.sy_delay[k];
-        // delayed releases (delay_buffer.h:31-44)
-        if ((d.flags & NF_DELAY) && delay > 0.0f) {
-            for (int q = 0; q < 4; q++) {
-                unsigned long long arr = d.dl_arr[(size_t)q * K + k];
-                if (arr == 0) continue;
-                if (arr <= tick) {
-                    cleft += d.dl_amt[(size_t)q * K + k];
-                    d.dl_arr[(size_t)q * K + k] = 0;
-                }
-            }
-        }
-        // RRP recovery (kernel_dispatch.h:612-630); no CaMKII/calcineurin modifiers
-        float rrp = 0.0f, rrp_max = d.sy_rrp_max[k];
-        if (rrp_max > 0.0f) rrp = d.sy_rrp[k];
-        if (!(rrp_max <= 0.0f || rrp >= rrp_max)) {
-            float ca_pre = d.pre_ext[pre].z;
-            float ca_f = ca_pre / (0.0005f + ca_pre);
-            float priming = d.sy_rrp_rec[k] + 0.0f * 0.02f + 0.0f * 0.01f;
-            priming *= ca_f;
-            float rec = (rrp_max - rrp) * priming * dt;
-            rrp += rec;
-            if (rrp > rrp_max) rrp = rrp_max;
-        }
-        // bouton Ca2+ (modifier_helpers.h:764-806)
-        float bouton = d.sy_bouton[k];
-        const float pre_area = d.sy_pre_area[k];
-        {
-            const float g_K = d.sy_gK[k], g_Na = d.sy_gNa[k];
-            float V_bouton = pr.x;
-            if (g_K > 0.0f || g_Na > 0.0f) {
-                float4 ex = d.pre_ext[pre];
-                float koe = d.pre_ext2[pre];
-                float E_K = dp_nernst(ex.y, koe, 1.0f);
-                float E_Na = dp_nernst(ex.x, ex.w, 1.0f);
-                V_bouton = (float)((300.0f * (double)pr.x + g_K * E_K + g_Na * E_Na) / (300.0f + g_K + g_Na));
-            }
-            float cav21_dens = 0.0f, mm = 0.0f, h = 0.0f;
-            if (pr.z != 0.0f) {
-                cav21_dens = pr.z;
-                float m_inf = cav21_m_inf(V_bouton);
-                float h_inf = cav21_h_inf(V_bouton, bouton * MM_TO_UM);
-                mm = m_inf;
-                h = (float)(h_inf + ((double)pr.w - h_inf) * dm_expf(-dt / 300.0f));
-            }
-            float cav21_open = mm * mm * h;
-            double P_single = dp_ghk_P(15.0f, 2.0f, GHK_CBAR_CA_MM);
-            double flux = dp_ghk_div(V_bouton, bouton, (double)pr.y);
-            double I_A = P_single * flux * (cav21_dens * pre_area) * cav21_open;
-            float I_Ca = (float)(I_A * A_TO_PA);
-            bouton = (float)(bouton - I_Ca * dt * 1000.0f / (2.0f * FARADAY_CONST * 0.1f));
-            bouton += (0.0001f - bouton) * dt / 5.0f;
-            if (bouton < 0.0f) bouton = 0.0f;
-        }
-        // Ca2+-dependent release (simulation_host.cpp:421-460)
-        uint8_t refr = d.sy_refr[k];
-        if (refr == 0) {
-            float Ca_uM = bouton * MM_TO_UM;
-            float ca_act = dm_powf(Ca_uM, 4.0f) / (dm_powf(Ca_uM, 4.0f) + dm_powf(10.0f, 4.0f));
-            float p = d.sy_prel[k] * ca_act;
-            uint32_t vbits = (uint32_t)(long long)((double)pr.x * 1000.0f);
-            uint32_t seed = d.sy_id[k] ^ (uint32_t)tick ^ vbits;
-            if (xorshift32_rnd(seed) < p) {
-                const float amt = d.sy_amt[k];
-                float release_amt;
-                if (rrp_max <= 0.0f) release_amt = amt * p;
-                else {
-                    float avail = amt;
-                    if (avail > rrp) avail = rrp;
-                    release_amt = avail * p;
-                    rrp -= release_amt;
-                    if (rrp < 0) rrp = 0;
-                }
-                unsigned long long delay_ticks = (delay <= 0.0f || dt <= 0.0f) ? 0ull
-                    : (unsigned long long)((delay / dt) + 0.5f);
-                if (delay_ticks > 0) {
-                    for (int q = 0; q < 4; q++) {
-                        if (d.dl_arr[(size_t)q * K + k] == 0) {
-                            d.dl_arr[(size_t)q * K + k] = tick + delay_ticks;
-                            d.dl_amt[(size_t)q * K + k] = release_amt;
-                            d.dl_nt[(size_t)q * K + k] = (uint8_t)ntt;
-                            break;
-                        }
-                    }
-                } else {
-                    cleft += release_amt;
-                }
-                refr = (uint8_t)(uint32_t)(20.0f / dt + 0.5f);
-            }
-        }
-        // NT into the postsynaptic segment (simulation_host.cpp:463-465)
-        ntv[ntt] += cleft;
-        // receptors (simulation_host.cpp:490-500)
-        float I_syn = 0.0f;
-        const float post_area = d.sy_post_area[k];
-        const float scale = d.sy_scale[k];
-        const uint32_t NR = d.n_rec;
-        for (uint32_t r = d.rc_off[k]; r < d.rc_off[k + 1]; r++) {
-            DMod m;
-            m.den = d.rc_den[r];
-            m.st[0] = d.rc_st[r];
-            m.st[1] = d.rc_st[(size_t)NR + r];
-            m.st[2] = d.rc_st[(size_t)2 * NR + r];
-            m.st[3] = m.st[4] = m.st[5] = m.st[6] = 0.0f;
-            m.area = (post_area > 0.0f) ? post_area : s.area;
-            m.av = d.rc_av[r];
-            const uint8_t rt = d.rc_type[r];
-            I_syn = (float)(I_syn + receptor_current(rt, m, s, dt, ntv, scale));
-            d.rc_st[r] = m.st[0];
-            d.rc_st[(size_t)NR + r] = m.st[1];
-            d.rc_st[(size_t)2 * NR + r] = m.st[2];
-            touched = true;
-        }
-        ib += I_syn;
-        // spine Ca2+ (modifier_helpers.h:808-817)
-        float spine = d.sy_spine[k];
-        {
-            float I_abs = I_syn < 0.0f ? -I_syn : I_syn;
-            float I_Ca = I_abs * 0.1f;
-            float influx = (float)(I_Ca * dt * 1000.0f / (2.0f * FARADAY_CONST * 0.05f * 100.0f));
-            spine += influx;
-            spine += (0.0001f - spine) * dt / 50.0f;
-            if (spine < 0.0f) spine = 0.0f;
-        }
-        // clearance (simulation_host.cpp:505-510)
-        cleft *= dm_expf(-dt / d.sy_tauc[k]);
-        if (cleft < 0.0f) cleft = 0.0f;
-        // BCM threshold, spine CaMKII/calcineurin, weight (simulation_host.cpp:527-576)
-        float facil = d.sy_facil[k];
-        {
-            float Ca_uM = spine * 1000.0f;
-            float Ca_sq = Ca_uM * Ca_uM;
-            facil += (Ca_sq - facil) * dt / 300000.0f;
-            if (facil < 0.0f) facil = 0.0f;
-        }
-        float camkii = d.sy_camkii[k], calcn = d.sy_calcn[k];
-        {
-            float Ca_uM = spine * MM_TO_UM;
-            float Ca4 = Ca_uM * Ca_uM * Ca_uM * Ca_uM;
-            float camkii_inf = Ca4 / (Ca4 + 1.0f + 1e-9f);
-            camkii += (camkii_inf - camkii) * dt / 2000.0f;
-            if (camkii < 0.0f) camkii = 0.0f;
-            if (camkii > 1.0f) camkii = 1.0f;
-            float Ca2 = Ca_uM * Ca_uM;
-            float calcineurin_inf = Ca2 / (Ca2 + 0.05f * 0.05f + 1e-9f);
-            calcn += (calcineurin_inf - calcn) * dt / 300.0f;
-            if (calcn < 0.0f) calcn = 0.0f;
-            if (calcn > 1.0f) calcn = 1.0f;
-        }
-        float weight = d.sy_weight[k];
-        {
-            float dw = 0.0f;
-            if (camkii > 0.0f) dw += 0.0003f * camkii * dt;
-            float pp1_active = 0.5f;
-            if (calcn > 0.0f) dw -= 0.0001f * calcn * pp1_active * dt;
-            if (sf & 1) dw = -dw;
-            weight += dw;
-            if (weight != weight) weight = 0.5f;
-            if (facil != facil) facil = 0.0f;
-            if (weight < 0.01f) weight = 0.01f;
-            if (weight > 10.0f) weight = 10.0f;
-        }
-        if (refr > 0) refr--;
-        d.sy_cleft[k] = cleft;
-        d.sy_refr[k] = refr;
-        d.sy_bouton[k] = bouton;
-        d.sy_spine[k] = spine;
-        d.sy_camkii[k] = camkii;
-        d.sy_calcn[k] = calcn;
-        d.sy_facil[k] = facil;
-        d.sy_weight[k] = weight;
-        if (rrp_max > 0.0f) d.sy_rrp[k] = rrp;
+    const uint32_t NR = d.n_rec;
+    uint32_t base = 0, rbase = 0;
+    if (maxc > 0) {
+        base = d.w_off[t >> 5];
+        rbase = d.rw_off[t >> 5];
     }
+    for (uint32_t kk = 0; kk < maxc; kk++) {
+        const bool act = cnt > kk;
+        const uint32_t n_act = __popc(__ballot_sync(0xFFFFFFFFu, act));
+        const uint32_t k = base + lane;   // this lane's synapse in the slice (when act)
+        float cleft = 0.0f, rrp = 0.0f, rrp_max = 0.0f, bouton = 0.0f;
+        uint8_t refr = 0, sf = 0;
+        int ntt = 0;
+        uint32_t n_rc = 0;
+        if (act) {
+            const uint32_t pre = d.sy_pre[k];
+            const float4 pr = d.pre_rec[pre];
+            sf = d.sy_flags[k];
+            ntt = sf >> 4;
+            cleft = d.sy_cleft[k];
+            const float delay = d.sy_delay[k];
+            // delayed releases (delay_buffer.h:31-44)
+            if ((d.flags & NF_DELAY) && delay > 0.0f) {
+                for (int q = 0; q < 4; q++) {
+                    unsigned long long arr = d.dl_arr[(size_t)q * K + k];
+                    if (arr == 0) continue;
+                    if (arr <= tick) {
+                        cleft += d.dl_amt[(size_t)q * K + k];
+                        d.dl_arr[(size_t)q * K + k] = 0;
+                    }
+                }
+            }
+            // RRP recovery (kernel_dispatch.h:612-630); no CaMKII/calcineurin modifiers
+            rrp_max = d.sy_rrp_max[k];
+            if (rrp_max > 0.0f) rrp = d.sy_rrp[k];
+            if (!(rrp_max <= 0.0f || rrp >= rrp_max)) {
+                float ca_pre = d.pre_ext[pre].z;
+                float ca_f = ca_pre / (0.0005f + ca_pre);
+                float priming = d.sy_rrp_rec[k] + 0.0f * 0.02f + 0.0f * 0.01f;
+                priming *= ca_f;
+                float rec = (rrp_max - rrp) * priming * dt;
+                rrp += rec;
+                if (rrp > rrp_max) rrp = rrp_max;
+            }
+            // bouton Ca2+ (modifier_helpers.h:764-806)
+            bouton = d.sy_bouton[k];
+            const float pre_area = d.sy_pre_area[k];
+            {
+                const float g_K = d.sy_gK[k], g_Na = d.sy_gNa[k];
+                float V_bouton = pr.x;
+                if (g_K > 0.0f || g_Na > 0.0f) {
+                    float4 ex = d.pre_ext[pre];
+                    float koe = d.pre_ext2[pre];
+                    float E_K = dp_nernst(ex.y, koe, 1.0f);
+                    float E_Na = dp_nernst(ex.x, ex.w, 1.0f);
+                    V_bouton = (float)((300.0f * (double)pr.x + g_K * E_K + g_Na * E_Na) / (300.0f + g_K + g_Na));
+                }
+                float cav21_dens = 0.0f, mm = 0.0f, h = 0.0f;
+                if (pr.z != 0.0f) {
+                    cav21_dens = pr.z;
+                    float m_inf = cav21_m_inf(V_bouton);
+                    float h_inf = cav21_h_inf(V_bouton, bouton * MM_TO_UM);
+                    mm = m_inf;
+                    h = (float)(h_inf + ((double)pr.w - h_inf) * dm_expf(-dt / 300.0f));
+                }
+                float cav21_open = mm * mm * h;
+                double P_single = dp_ghk_P(15.0f, 2.0f, GHK_CBAR_CA_MM);
+                double flux = dp_ghk_div(V_bouton, bouton, (double)pr.y);
+                double I_A = P_single * flux * (cav21_dens * pre_area) * cav21_open;
+                float I_Ca = (float)(I_A * A_TO_PA);
+                bouton = (float)(bouton - I_Ca * dt * 1000.0f / (2.0f * FARADAY_CONST * 0.1f));
+                bouton += (0.0001f - bouton) * dt / 5.0f;
+                if (bouton < 0.0f) bouton = 0.0f;
+            }
+            // Ca2+-dependent release (simulation_host.cpp:421-460)
+            refr = d.sy_refr[k];
+            if (refr == 0) {
+                float Ca_uM = bouton * MM_TO_UM;
+                float ca_act = dm_powf(Ca_uM, 4.0f) / (dm_powf(Ca_uM, 4.0f) + dm_powf(10.0f, 4.0f));
+                float p = d.sy_prel[k] * ca_act;
+                uint32_t vbits = (uint32_t)(long long)((double)pr.x * 1000.0f);
+                uint32_t seed = d.sy_id[k] ^ (uint32_t)tick ^ vbits;
+                if (xorshift32_rnd(seed) < p) {
+                    const float amt = d.sy_amt[k];
+                    float release_amt;
+                    if (rrp_max <= 0.0f) release_amt = amt * p;
+                    else {
+                        float avail = amt;
+                        if (avail > rrp) avail = rrp;
+                        release_amt = avail * p;
+                        rrp -= release_amt;
+                        if (rrp < 0) rrp = 0;
+                    }
+                    unsigned long long delay_ticks = (delay <= 0.0f || dt <= 0.0f) ? 0ull
+                        : (unsigned long long)((delay / dt) + 0.5f);
+                    if (delay_ticks > 0) {
+                        for (int q = 0; q < 4; q++) {
+                            if (d.dl_arr[(size_t)q * K + k] == 0) {
+                                d.dl_arr[(size_t)q * K + k] = tick + delay_ticks;
+                                d.dl_amt[(size_t)q * K + k] = release_amt;
+                                d.dl_nt[(size_t)q * K + k] = (uint8_t)ntt;
+                                break;
+                            }
+                        }
+                    } else {
+                        cleft += release_amt;
+                    }
+                    refr = (uint8_t)(uint32_t)(20.0f / dt + 0.5f);
+                }
+            }
+            // NT into the postsynaptic segment (simulation_host.cpp:463-465)
+            if (ntt == 0) nt_glu += cleft;
+            else if (ntt == 1) nt_gaba += cleft;
+            else nt_gly += cleft;
+            n_rc = d.rc_cnt[k];
+        }
+        // receptors (simulation_host.cpp:490-500), j-th receptors of the slice side by side
+        float I_syn = 0.0f;
+        const float post_area = act ? d.sy_post_area[k] : 0.0f;
+        const float scale = act ? d.sy_scale[k] : 0.0f;
+        const uint32_t maxr = __reduce_max_sync(0xFFFFFFFFu, n_rc);
+        for (uint32_t j = 0; j < maxr; j++) {
+            const uint32_t has = __ballot_sync(0xFFFFFFFFu, n_rc > j);
+            if (n_rc > j) {
+                const uint32_t r = rbase + __popc(has & lt_mask);
+                DMod m;
+                m.den = d.rc_den[r];
+                m.st[0] = d.rc_st[r];
+                m.st[1] = d.rc_st[(size_t)NR + r];
+                m.st[2] = d.rc_st[(size_t)2 * NR + r];
+                m.st[3] = m.st[4] = m.st[5] = m.st[6] = 0.0f;
+                m.area = (post_area > 0.0f) ? post_area : s.area;
+                m.av = d.rc_av[r];
+                const int kind = receptor_kind(d.rc_type[r]);
+                const float ntr = kind <= 1 ? nt_glu : (kind == 2 ? nt_gaba : nt_gly);
+                I_syn = (float)(I_syn + receptor_current(gRec[kind], m, s, dt, ntr, scale));
+                d.rc_st[r] = m.st[0];
+                d.rc_st[(size_t)NR + r] = m.st[1];
+                d.rc_st[(size_t)2 * NR + r] = m.st[2];
+                touched = true;
+            }
+            rbase += __popc(has);
+        }
+        if (act) {
+            ib += I_syn;
+            // spine Ca2+ (modifier_helpers.h:808-817)
+            float spine = d.sy_spine[k];
+            {
+                float I_abs = I_syn < 0.0f ? -I_syn : I_syn;
+                float I_Ca = I_abs * 0.1f;
+                float influx = (float)(I_Ca * dt * 1000.0f / (2.0f * FARADAY_CONST * 0.05f * 100.0f));
+                spine += influx;
+                spine += (0.0001f - spine) * dt / 50.0f;
+                if (spine < 0.0f) spine = 0.0f;
+            }
+            // clearance (simulation_host.cpp:505-510)
+            cleft *= dm_expf(-dt / d.sy_tauc[k]);
+            if (cleft < 0.0f) cleft = 0.0f;
+            // BCM threshold, spine CaMKII/calcineurin, weight (simulation_host.cpp:527-576)
+            float facil = d.sy_facil[k];
+            {
+                float Ca_uM = spine * 1000.0f;
+                float Ca_sq = Ca_uM * Ca_uM;
+                facil += (Ca_sq - facil) * dt / 300000.0f;
+                if (facil < 0.0f) facil = 0.0f;
+            }
+            float camkii = d.sy_camkii[k], calcn = d.sy_calcn[k];
+            {
+                float Ca_uM = spine * MM_TO_UM;
+                float Ca4 = Ca_uM * Ca_uM * Ca_uM * Ca_uM;
+                float camkii_inf = Ca4 / (Ca4 + 1.0f + 1e-9f);
+                camkii += (camkii_inf - camkii) * dt / 2000.0f;
+                if (camkii < 0.0f) camkii = 0.0f;
+                if (camkii > 1.0f) camkii = 1.0f;
+                float Ca2 = Ca_uM * Ca_uM;
+                float calcineurin_inf = Ca2 / (Ca2 + 0.05f * 0.05f + 1e-9f);
+                calcn += (calcineurin_inf - calcn) * dt / 300.0f;
+                if (calcn < 0.0f) calcn = 0.0f;
+                if (calcn > 1.0f) calcn = 1.0f;
+            }
+            float weight = d.sy_weight[k];
+            {
+                float dw = 0.0f;
+                if (camkii > 0.0f) dw += 0.0003f * camkii * dt;
+                float pp1_active = 0.5f;
+                if (calcn > 0.0f) dw -= 0.0001f * calcn * pp1_active * dt;
+                if (sf & 1) dw = -dw;
+                weight += dw;
+                if (weight != weight) weight = 0.5f;
+                if (facil != facil) facil = 0.0f;
+                if (weight < 0.01f) weight = 0.01f;
+                if (weight > 10.0f) weight = 10.0f;
+            }
+            if (refr > 0) refr--;
+            d.sy_cleft[k] = cleft;
+            d.sy_refr[k] = refr;
+            d.sy_bouton[k] = bouton;
+            d.sy_spine[k] = spine;
+            d.sy_camkii[k] = camkii;
+            d.sy_calcn[k] = calcn;
+            d.sy_facil[k] = facil;
+            d.sy_weight[k] = weight;
+            if (rrp_max > 0.0f) d.sy_rrp[k] = rrp;
+        }
+        base += n_act;
+    }
+    if (!valid) return;
     // step 4: membrane update (simulation_host.cpp:596-649)
     float V = s.V;
     if (ib != ib) ib = 0.0f;
@@ -254,8 +384,8 @@ k_synapse(NetDev d, float dt, unsigned long long tick, int first_tick) {
     V = (float)((double)V + dV);
     if (prev_V <= -40.0f && V > -40.0f) d.spike_count[i]++;
     if (d.vc_off) {
-        for (uint32_t k = d.vc_off[i]; k < d.vc_off[i + 1]; k++)
-            if (tick >= d.vc_start[k] && tick < d.vc_end[k]) V = d.vc_target[k];
+        for (uint32_t q = d.vc_off[i]; q < d.vc_off[i + 1]; q++)
+            if (tick >= d.vc_start[q] && tick < d.vc_end[q]) V = d.vc_target[q];
     }
     if (V != V) V = -65.0f;
     else {
@@ -271,10 +401,24 @@ k_synapse(NetDev d, float dt, unsigned long long tick, int first_tick) {
         const uint32_t mask = first_tick ? 0x7FFFu : d.nt_used_mask;
 #pragma unroll
         for (int q = 0; q < 15; q++)
-            if ((mask >> q) & 1u) d.nt[(size_t)q * N + i] = ntv[q];
+            if ((mask >> q) & 1u)
+                d.nt[(size_t)q * N + i] = q == 0 ? nt_glu : (q == 1 ? nt_gaba : (q == 7 ? nt_gly : 0.0f));
     } else if (sfl & SF_NMDA) {
         d.nt[i] = 1.0f;
     }
+}
+
+cudaError_t prepare_synapse(cudaStream_t stream) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    if (g_rec_ready[dev]) return cudaSuccess;
+    k_init_receptors<<<1, 1, 0, stream>>>();
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e == cudaSuccess) g_rec_ready[dev] = true;
+    return e;
 }
 
 cudaError_t launch_synapse(const NetDev& dev, float dt, unsigned long long tick, int first_tick,

@@ -65,7 +65,8 @@ size_t tile_smem_bytes(uint32_t max_segs) {
     return tile_layout(max_segs, nullptr, nullptr);
 }
 
-__global__ void __launch_bounds__(kTileThreads)
+template <int kMinCtas>
+__global__ void __launch_bounds__(kTileThreads, kMinCtas)
 k_modifiers(NetDev d, float dt, unsigned long long tick, uint32_t S) {
     extern __shared__ __align__(16) unsigned char smem[];
     TileSmem t;
@@ -110,6 +111,7 @@ k_modifiers(NetDev d, float dt, unsigned long long tick, uint32_t S) {
     for (uint32_t p = 0; p < P; p++) {
         const uint32_t b = d.phase_off[(size_t)tile * (P + 1) + p];
         const uint32_t e = d.phase_off[(size_t)tile * (P + 1) + p + 1];
+        if (b == e) continue;   // empty for this tile (uniform across the CTA)
         for (uint32_t q = b + tid; q < e; q += nth) {
             const uint32_t meta = d.it_meta[q];
             const int ls = (int)(meta & 0xFFFFu);
@@ -228,16 +230,21 @@ cudaError_t prepare_tick(const NetDev& dev, const NetHost& host, cudaStream_t st
     if (e != cudaSuccess) return e;
     const size_t smem = tile_smem_bytes(host.max_tile_segs);
     if (smem > 48 * 1024) {
-        e = cudaFuncSetAttribute(k_modifiers, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        e = host.opt.mod_ctas == 3
+                ? cudaFuncSetAttribute(k_modifiers<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
+                : cudaFuncSetAttribute(k_modifiers<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
     }
+    e = prepare_synapse(stream);
+    if (e != cudaSuccess) return e;
     return prepare_diffusion(host, stream);
 }
 
 static void enqueue_modifiers(const NetDev& dev, const NetHost& host, float dt, unsigned long long tick,
                               cudaStream_t stream) {
     const uint32_t S = host.max_tile_segs;
-    k_modifiers<<<dev.n_tiles, kTileThreads, tile_smem_bytes(S), stream>>>(dev, dt, tick, S);
+    if (host.opt.mod_ctas == 3) k_modifiers<3><<<dev.n_tiles, kTileThreads, tile_smem_bytes(S), stream>>>(dev, dt, tick, S);
+    else k_modifiers<2><<<dev.n_tiles, kTileThreads, tile_smem_bytes(S), stream>>>(dev, dt, tick, S);
 }
 
 cudaError_t launch_modifiers(const NetDev& dev, const NetHost& host, float dt, unsigned long long tick,
