@@ -55,8 +55,7 @@ class NetInfo(C.Structure):
 
 class BuildOptions(C.Structure):
     """Device-layout options (include/bnc_b200.h BncBuildOptions); 0 = default."""
-    _fields_ = [("warp_cap", C.c_uint32), ("tile_segs", C.c_uint32), ("phase_cap", C.c_uint32),
-                ("mod_ctas", C.c_uint32)]
+    _fields_ = [("warp_cap", C.c_uint32), ("tile_segs", C.c_uint32), ("phase_cap", C.c_uint32)]
 
 
 class Tuning(C.Structure):

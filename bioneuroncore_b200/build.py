@@ -23,7 +23,7 @@ ORACLE_DIR = os.path.join(ROOT, "oracle")
 ORACLE_LIB = os.path.join(ORACLE_DIR, "liboracle.so")
 REFERENCE = "/root/reference"
 
-CU_SOURCES = ["tile.cu", "diffuse.cu", "synapse.cu", "backend.cu"]
+CU_SOURCES = ["modifiers.cu", "diffuse.cu", "synapse.cu", "backend.cu"]
 CPP_SOURCES = ["netgen.cpp", "capi_host.cpp", "builder.cpp"]
 HEADERS = sorted(f for f in os.listdir(CSRC) if f.endswith((".h", ".cuh")))
 

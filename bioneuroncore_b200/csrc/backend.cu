@@ -566,7 +566,6 @@ static BuildOptions to_options(const BncBuildOptions* o) {
         if (o->warp_cap) opt.warp_cap = o->warp_cap;
         if (o->tile_segs) opt.tile_segs = o->tile_segs;
         opt.phase_cap = o->phase_cap;
-        if (o->mod_ctas) opt.mod_ctas = o->mod_ctas;
     }
     return opt;
 }
@@ -865,7 +864,7 @@ int bnc_profile_ticks(void* sim, uint32_t n_ticks, float dt, float* ms_modifiers
         cudaError_t er = launch_modifiers(b->dev, b->host, dt, b->tick, b->stream);
         if (er != cudaSuccess) { rc = cuda_fail(er, "modifier kernel launch"); break; }
         cudaEventRecord(e[1], b->stream);
-        er = launch_diffusion(b->dev, b->host, dt, b->stream);
+        er = launch_diffusion(b->dev, b->host, dt, b->tick, b->stream);
         if (er != cudaSuccess) { rc = cuda_fail(er, "diffusion kernel launch"); break; }
         cudaEventRecord(e[2], b->stream);
         er = launch_synapse(b->dev, dt, b->tick, b->ticks_run == 0 ? 1 : 0, b->stream);

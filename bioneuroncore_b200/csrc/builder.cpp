@@ -350,10 +350,9 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
     }
     lap("components");
     // ---- tile packing: whole components, one component per warp slot ----
-    if (opt.warp_cap < 1 || opt.tile_segs < 32 || opt.tile_segs > (uint32_t)kMaxTileSegs ||
-        opt.phase_cap > 4096 || (opt.mod_ctas != 2 && opt.mod_ctas != 3)) {
-        set_error("build options out of range (warp_cap %u, tile_segs %u, phase_cap %u, mod_ctas %u)", opt.warp_cap,
-                  opt.tile_segs, opt.phase_cap, opt.mod_ctas);
+    if (opt.warp_cap < 1 || opt.tile_segs < 32 || opt.tile_segs > (uint32_t)kMaxTileSegs || opt.phase_cap > 4096) {
+        set_error("build options out of range (warp_cap %u, tile_segs %u, phase_cap %u)", opt.warp_cap,
+                  opt.tile_segs, opt.phase_cap);
         return BNC_ERR_ARG;
     }
     host->opt = opt;
@@ -549,13 +548,15 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
     }
     if (n_phases == 0) n_phases = 1;
     lap("phase schedule");
-    // ---- items ordered by (tile, phase, type, device segment): two counting passes ----
-    struct ItemKey { uint32_t tile; uint16_t phase; uint8_t type; uint32_t dseg; uint32_t k; };
-    const size_t NB = (size_t)T * n_phases;
+    // ---- items ordered by (phase, type, device segment): two counting passes ----
+    // A phase is one launch of the modifier kernel over the whole network; sorting
+    // by type inside it keeps warps, and the SMs at any moment, on few channel models.
+    struct ItemKey { uint16_t phase; uint8_t type; uint32_t dseg; uint32_t k; };
+    const size_t NB = n_phases;
     std::vector<uint32_t> bucket_off(NB + 1, 0);
     for (uint32_t d = 0; d < n; d++) {
         uint32_t i = host->perm[d];
-        for (uint32_t k = act_off[i]; k < act_off[i + 1]; k++) bucket_off[(size_t)tile_of[d] * n_phases + item_phase[k] + 1]++;
+        for (uint32_t k = act_off[i]; k < act_off[i + 1]; k++) bucket_off[item_phase[k] + 1]++;
     }
     for (size_t b = 0; b < NB; b++) bucket_off[b + 1] += bucket_off[b];
     std::vector<ItemKey> keys(act_slot.size());
@@ -563,23 +564,16 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
         std::vector<uint32_t> pos(bucket_off.begin(), bucket_off.end() - 1);
         for (uint32_t d = 0; d < n; d++) {   // device order: each bucket fills in segment order
             uint32_t i = host->perm[d];
-            for (uint32_t k = act_off[i]; k < act_off[i + 1]; k++) {
-                size_t b = (size_t)tile_of[d] * n_phases + item_phase[k];
-                keys[pos[b]++] = {tile_of[d], item_phase[k], act_type[k], d, k};
-            }
+            for (uint32_t k = act_off[i]; k < act_off[i + 1]; k++)
+                keys[pos[item_phase[k]]++] = {item_phase[k], act_type[k], d, k};
         }
         std::vector<ItemKey> tmp;
         uint32_t tc[257];
-        for (size_t b = 0; b < NB; b++) {   // stable counting sort by type inside each bucket
+        for (size_t b = 0; b < NB; b++) {   // stable counting sort by type inside each phase
             uint32_t lo = bucket_off[b], hi = bucket_off[b + 1];
             if (hi - lo < 2) continue;
             std::fill(tc, tc + 257, 0u);
-            bool sorted = true;
-            for (uint32_t q = lo; q < hi; q++) {
-                tc[keys[q].type + 1]++;
-                if (q > lo && keys[q].type < keys[q - 1].type) sorted = false;
-            }
-            if (sorted) continue;
+            for (uint32_t q = lo; q < hi; q++) tc[keys[q].type + 1]++;
             for (int t = 0; t < 256; t++) tc[t + 1] += tc[t];
             tmp.assign(keys.begin() + lo, keys.begin() + hi);
             for (const ItemKey& kk : tmp) keys[lo + tc[kk.type]++] = kk;
@@ -587,21 +581,13 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
     }
     lap("item sort");
     const uint32_t NI = (uint32_t)keys.size();
-    std::vector<uint32_t> it_meta(NI);
+    std::vector<uint32_t> it_seg(NI);
+    std::vector<uint16_t> it_tf(NI);
     std::vector<float> it_den(NI), it_st((size_t)7 * NI);
-    std::vector<uint32_t> phase_off((size_t)T * (n_phases + 1), 0);
+    std::vector<uint32_t> phase_off(bucket_off.begin(), bucket_off.end());
     host->item_seg.assign(NI, 0);
     host->item_slot.assign(NI, 0);
-    {
-        uint32_t k = 0;
-        for (uint32_t t = 0; t < T; t++) {
-            for (uint32_t p = 0; p <= n_phases; p++) {
-                while (k < NI && keys[k].tile == t && keys[k].phase < p) k++;
-                phase_off[(size_t)t * (n_phases + 1) + p] = k;
-            }
-            while (k < NI && keys[k].tile == t) k++;
-        }
-    }
+    host->phase_off = phase_off;
     for (uint32_t q = 0; q < NI; q++) {
         const ItemKey& kk = keys[q];
         uint32_t orig = host->perm[kk.dseg];
@@ -614,8 +600,8 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
             if (m.active_vars >= 8) { set_error("segment %u slot %u: active_vars %u out of range", orig, slot, m.active_vars); return BNC_ERR_FORMAT; }
             fl |= (uint8_t)(2u | ((uint32_t)m.active_vars << 2));
         }
-        uint32_t local = kk.dseg - tile_seg_beg[kk.tile];
-        it_meta[q] = local | ((uint32_t)m.type << 16) | ((uint32_t)fl << 24);
+        it_seg[q] = kk.dseg;
+        it_tf[q] = (uint16_t)(m.type | ((uint32_t)fl << 8));
         it_den[q] = m.density;
         for (int b = 0; b < 7; b++) it_st[(size_t)b * NI + q] = m.state[b];
         host->item_seg[q] = orig;
@@ -881,6 +867,7 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
         dev->sflags = up(allocs, dflags, &rc);
         dev->cav21_static = up(allocs, c21, &rc);
         dev->c21_cur = zeros<float2>(allocs, n, &rc);
+        dev->rec = zeros<SegRec>(allocs, n, &rc);
         dev->pre_rec = zeros<float4>(allocs, n, &rc);
         if (need_pre_ext) {
             dev->pre_ext = zeros<float4>(allocs, n, &rc);
@@ -898,7 +885,8 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
         dev->e_dist = up(allocs, e_dist, &rc);
         dev->inc_off = up(allocs, inc_off, &rc);
         dev->inc = up(allocs, inc, &rc);
-        dev->it_meta = up(allocs, it_meta, &rc);
+        dev->it_seg = up(allocs, it_seg, &rc);
+        dev->it_tf = up(allocs, it_tf, &rc);
         dev->it_den = up(allocs, it_den, &rc);
         dev->it_st = up(allocs, it_st, &rc);
         dev->th_seg = up(allocs, th_seg, &rc);
@@ -952,7 +940,7 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
     }
     host->max_tile_segs = mts;
     host->max_tile_edges = mte;
-    host->smem_bytes = std::max(tile_smem_bytes(mts), diffusion_smem_bytes(mts, mte));
+    host->smem_bytes = diffusion_smem_bytes(mts, mte);
     if (host->smem_bytes > 227 * 1024) {
         set_error("tile of %u segments and %u connections needs %zu bytes of shared memory (227 KB per CTA)", mts, mte,
                   host->smem_bytes);
@@ -970,7 +958,7 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
         // modifier items: meta + density read, dynamic state read+write
         double items = 0;
         for (uint32_t q = 0; q < NI; q++) {
-            uint8_t t = (uint8_t)(it_meta[q] >> 16);
+            uint8_t t = (uint8_t)(it_tf[q] & 0xFFu);
             int dyn = 0;
             switch (t) {
                 case 1: case 8: case 11: case 12: case 85: case 140: case 141: case 142: case 200: dyn = 2; break;

@@ -146,7 +146,7 @@ __device__ __forceinline__ void fick(const DiffSmem& t, int ns, int ne, int tid,
 }  // namespace
 
 __global__ void __launch_bounds__(1024)
-k_diffusion(NetDev d, float dt, uint32_t S, uint32_t E) {
+k_diffusion(NetDev d, float dt, unsigned long long tick, uint32_t S, uint32_t E) {
     extern __shared__ __align__(16) unsigned char smem[];
     DiffSmem t;
     diff_layout(S, E, smem, &t);
@@ -161,24 +161,38 @@ k_diffusion(NetDev d, float dt, uint32_t S, uint32_t E) {
     const uint32_t inc0 = d.inc_off[s0];
     const int ninc = (int)(d.inc_off[s0 + ns] - inc0);
     const int i = tid;   // this thread's segment (when i < ns)
+    if (d.clock) tick = d.clock[0];
 
-    // ---- load: state after step 1 (modifier kernel), statics, connections ----
+    // ---- load: state after step 1 (the modifier phases' records), stimuli, statics ----
     float c21d = 0.0f, c21h = 0.0f;
     if (i < ns) {
         const uint32_t g = s0 + i;
-        t.V[i] = d.V[g];
+        const SegRec* r = d.rec + g;
+        t.V[i] = r->V;
 #pragma unroll
         for (int q = 0; q < 7; q++) {
-            t.in[q * S + i] = d.ion_in[(size_t)q * N + g];
-            t.out[q * S + i] = d.ion_out[(size_t)q * N + g];
+            t.in[q * S + i] = r->in[q];
+            t.out[q * S + i] = r->out[q];
         }
-        t.atp[i] = d.atp[g];
+        t.atp[i] = r->atp;
         t.area[i] = d.area[g];
         t.cm[i] = d.cm[g];
-        float vf = (float)d.vol[g];
+        float vf = (float)r->vol;
         if (vf < 1e-6f) vf = 1e-6f;
         t.vf[i] = vf;
-        t.itot[i] = d.ibuf[g];
+        // current stimuli (simulation_host.cpp:189-209, 247-258): expiry, then add in order
+        double I = r->itot;
+        if (d.cs_off) {
+            for (uint32_t k = d.cs_off[g]; k < d.cs_off[g + 1]; k++) {
+                if (!d.cs_alive[k]) continue;
+                unsigned long long dur = (unsigned long long)(d.cs_dur[k] / dt);
+                unsigned long long st0 = d.cs_start[k];
+                if (tick >= st0 + dur) { d.cs_alive[k] = 0; continue; }
+                if (tick >= st0 && tick < st0 + dur) I += d.cs_amp[k];
+            }
+        }
+        t.itot[i] = I;
+        d.ibuf[g] = I;
         t.incoff[i] = (uint16_t)(d.inc_off[g] - inc0);
         const float2 c = d.c21_cur[g];
         c21d = c.x;
@@ -561,9 +575,10 @@ cudaError_t prepare_diffusion(const NetHost& host, cudaStream_t stream) {
     return cudaSuccess;
 }
 
-void enqueue_diffusion(const NetDev& dev, const NetHost& host, float dt, cudaStream_t stream) {
+void enqueue_diffusion(const NetDev& dev, const NetHost& host, float dt, unsigned long long tick,
+                       cudaStream_t stream) {
     const uint32_t S = host.max_tile_segs, E = host.max_tile_edges;
-    k_diffusion<<<dev.n_tiles, diffusion_threads(S), diffusion_smem_bytes(S, E), stream>>>(dev, dt, S, E);
+    k_diffusion<<<dev.n_tiles, diffusion_threads(S), diffusion_smem_bytes(S, E), stream>>>(dev, dt, tick, S, E);
 }
 
 }  // namespace bnc

@@ -1,0 +1,255 @@
+// modifiers.cu -- step 1 of a tick (modifier currents) and the tick launcher.
+//
+// One tick of the reference (simulation_host.cpp:174-657) is these launches:
+//
+//  k_gather      per segment: the step-1 working record (V, ions, ATP, area, volume,
+//                I_total = 0, the GHK factors of V), the Cav2.1 gate from its static copy.
+//  k_phase x P   one launch per modifier phase over the whole network.  Every segment's
+//                active modifiers sit in successive phases in slot order, at most one
+//                per phase, so a phase's items touch distinct segments and need no
+//                barrier; inside a phase items are ordered by type, so warps -- and the
+//                SMs at any moment -- run few channel models at a time, which keeps the
+//                many models' code within the instruction caches.  Each dispatch case
+//                loads and stores only the record fields its model uses.
+//  k_diffusion   (diffuse.cu) stimuli, step 2.5 electrodiffusion, the presynaptic record.
+//  k_synapse     (synapse.cu) steps 3 and 4.
+#define BNC_MATH_OUTLINE 1   // 26 channel models in one kernel: keep exp/log out of line
+#include <cuda_runtime.h>
+#include "net.h"
+#include "physics.cuh"
+
+namespace bnc {
+
+// state indices each modifier type updates every tick (read + write)
+__constant__ uint8_t c_dyn_mask[256];
+// state indices each type reads as parameters (default when 0)
+__constant__ uint8_t c_par_mask[256];
+
+__global__ void __launch_bounds__(256)
+k_gather(NetDev d) {
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t N = d.n_seg;
+    if (g >= N) return;
+    SegRec r;
+    r.V = d.V[g];
+#pragma unroll
+    for (int q = 0; q < 7; q++) {
+        r.in[q] = d.ion_in[(size_t)q * N + g];
+        r.out[q] = d.ion_out[(size_t)q * N + g];
+    }
+    r.atp = d.atp[g];
+    r.area = d.area[g];
+    r.vol = d.vol[g];
+    r.itot = 0.0;
+    GhkCache c;
+    ghk_cache_fill(c, r.V);
+    r.gV = c.Vc;
+    r.gm = (uint32_t)c.m1 | ((uint32_t)c.m2 << 8);
+    r.pad = 0;
+    r.A1 = c.A1; r.e1 = c.e1; r.D1 = c.D1;
+    r.A2 = c.A2; r.e2 = c.e2; r.D2 = c.D2;
+    d.rec[g] = r;
+    d.c21_cur[g] = d.cav21_static[g];
+}
+
+// The segment fields an item sees, loaded from the record and stored back inside the
+// model's own dispatch case: after inlining, the loads a model does not read are
+// dead, and stores of fields it leaves unchanged write back what was read.
+__device__ __forceinline__ void rec_load(DSeg& s, const SegRec* r) {
+    s.V = r->V;
+#pragma unroll
+    for (int k = 0; k < 7; k++) { s.in[k] = r->in[k]; s.out[k] = r->out[k]; }
+    s.atp = r->atp;
+    s.area = r->area;
+    s.vol = r->vol;
+    s.gc.Vc = r->gV;
+    const uint32_t gm = r->gm;
+    s.gc.m1 = (uint8_t)(gm & 0xFFu);
+    s.gc.m2 = (uint8_t)(gm >> 8);
+    s.gc.A1 = r->A1; s.gc.e1 = r->e1; s.gc.D1 = r->D1;
+    s.gc.A2 = r->A2; s.gc.e2 = r->e2; s.gc.D2 = r->D2;
+}
+
+__device__ __forceinline__ void rec_store(const DSeg& s, float v0, SegRec* r) {
+    if (s.V != v0) {   // a sodium channel clamped V to +-200 mV: refresh the GHK factors
+        GhkCache c;
+        ghk_cache_fill(c, s.V);
+        r->gV = c.Vc;
+        r->gm = (uint32_t)c.m1 | ((uint32_t)c.m2 << 8);
+        r->A1 = c.A1; r->e1 = c.e1; r->D1 = c.D1;
+        r->A2 = c.A2; r->e2 = c.e2; r->D2 = c.D2;
+    }
+    r->V = s.V;
+#pragma unroll
+    for (int k = 0; k < 7; k++) { r->in[k] = s.in[k]; r->out[k] = s.out[k]; }
+    r->atp = s.atp;
+}
+
+// kernel_dispatch.h:337-570 restricted to the device-implemented types (the builder
+// rejects every other type; myelin, type 4, is never an item: it returns 0 and
+// touches nothing).
+template <bool kDef>
+__device__ __forceinline__ double run_item(uint8_t type, DMod& m, SegRec* r, float dt, float glu, float gaba,
+                                           float gly) {
+    double I = 0.0;
+    switch (type) {
+#define BNC_ITEM(T, CALL)          \
+    case T: {                      \
+        DSeg s;                    \
+        rec_load(s, r);            \
+        const float v0 = s.V;      \
+        m.area = s.area;           \
+        I = (CALL);                \
+        rec_store(s, v0, r);       \
+        break;                     \
+    }
+        BNC_ITEM(1, dp_cav13_current<kDef>(m, s, dt))
+        BNC_ITEM(7, dp_nak_pump_current(m, s, dt))
+        BNC_ITEM(8, dp_ampa_current<kDef>(m, s, dt, glu, 1.0f))
+        BNC_ITEM(9, dp_nmda_current<kDef>(m, s, dt, glu, 1.0f))
+        BNC_ITEM(11, dp_gabaa_current<kDef>(m, s, dt, gaba, 1.0f))
+        BNC_ITEM(12, dp_glycine_current<kDef>(m, s, dt, gly, 1.0f))
+        BNC_ITEM(85, dp_kv42_current<kDef>(m, s, dt))
+        BNC_ITEM(98, dp_pmca_current<kDef>(m, s, dt))
+        BNC_ITEM(99, dp_ncx_current(m, s, dt))
+        BNC_ITEM(100, dp_kcc2_current<kDef>(m, s, dt))
+        BNC_ITEM(102, dp_ca_buffer_current<kDef>(m, s, dt))
+        BNC_ITEM(103, dp_sk_current<kDef>(m, s, dt))
+        BNC_ITEM(104, dp_bk_current<kDef>(m, s, dt))
+        BNC_ITEM(105, dp_nap_current<kDef>(m, s, dt))
+        BNC_ITEM(106, dp_kir_current<kDef>(m, s, dt))
+        BNC_ITEM(107, dp_k2p_current<kDef>(m, s, dt))
+        BNC_ITEM(112, dp_kv7_current<kDef>(m, s, dt))
+        BNC_ITEM(123, dp_kvdr_current<kDef>(m, s, dt))
+        BNC_ITEM(129, dp_hcn1_current<kDef>(m, s, dt))
+        BNC_ITEM(133, dp_nalcn_current<kDef>(m, s, dt))
+        BNC_ITEM(140, dp_cav21_current(m, s, dt))
+        BNC_ITEM(141, dp_nav_current<kDef>(m, s, dt, 0))
+        BNC_ITEM(142, dp_nav_current<kDef>(m, s, dt, 1))
+        BNC_ITEM(150, dp_kv31_current<kDef>(m, s, dt))
+        BNC_ITEM(200, dp_cav31_current<kDef>(m, s, dt))
+#undef BNC_ITEM
+        default: break;
+    }
+    return I;
+}
+
+// One modifier phase: items [b, e), one thread each (simulation_host.cpp:234-303 for
+// the item's segment and slot).
+__global__ void __launch_bounds__(256)
+k_phase(NetDev d, float dt, uint32_t b, uint32_t e) {
+    const uint32_t q = b + blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= e) return;
+    const uint32_t N = d.n_seg;
+    const uint32_t NI = d.n_items;
+    const uint32_t g = d.it_seg[q];
+    const uint32_t tf = d.it_tf[q];
+    const uint8_t type = (uint8_t)(tf & 0xFFu);
+    const uint8_t fl = (uint8_t)(tf >> 8);
+    DMod m;
+    m.den = d.it_den[q];
+    m.av = (fl & 2) ? (uint8_t)((fl >> 2) & 7) : (uint8_t)0;
+    uint32_t rm = c_dyn_mask[type] | ((fl & 1) ? c_par_mask[type] : 0u);
+    if (fl & 2) rm |= (1u << m.av) & 0x7Fu;
+#pragma unroll
+    for (int k = 0; k < 7; k++) m.st[k] = ((rm >> k) & 1u) ? d.it_st[(size_t)k * NI + q] : 0.0f;
+    float glu = 0.0f, gaba = 0.0f, gly = 0.0f;
+    if (type == 8 || type == 9) glu = d.nt[g];
+    else if (type == 11) gaba = d.nt[(size_t)1 * N + g];
+    else if (type == 12) gly = d.nt[(size_t)7 * N + g];
+    SegRec* r = d.rec + g;
+    const double I = ((fl & 3) == 0) ? run_item<true>(type, m, r, dt, glu, gaba, gly)
+                                     : run_item<false>(type, m, r, dt, glu, gaba, gly);
+    r->itot = r->itot + I;
+    const uint32_t wm = c_dyn_mask[type];
+#pragma unroll
+    for (int k = 0; k < 7; k++) if ((wm >> k) & 1u) d.it_st[(size_t)k * NI + q] = m.st[k];
+    if (type == 140) d.c21_cur[g] = make_float2(m.den, m.st[1]);
+}
+
+static bool g_tables_ready[64] = {false};   // per device: constant memory is per context
+
+static cudaError_t init_tables(cudaStream_t stream) {
+    int dev = 0;
+    cudaError_t ge = cudaGetDevice(&dev);
+    if (ge != cudaSuccess) return ge;
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    if (g_tables_ready[dev]) return cudaSuccess;
+    uint8_t dyn[256] = {0}, par[256] = {0};
+    dyn[1] = 0x03; par[1] = 0x1C;
+    dyn[8] = 0x03; dyn[9] = 0x05; dyn[11] = 0x03; dyn[12] = 0x03;
+    dyn[85] = 0x0B; par[85] = 0x34;
+    par[98] = 0x06; par[100] = 0x06;
+    dyn[102] = 0x02; par[102] = 0x1D;
+    dyn[103] = 0x01; par[103] = 0x38;
+    dyn[104] = 0x01; par[104] = 0x06;
+    dyn[105] = 0x01; par[105] = 0x3E;
+    par[106] = 0x08; par[107] = 0x03;
+    dyn[112] = 0x01; par[112] = 0x76;
+    dyn[123] = 0x01; par[123] = 0x16;
+    dyn[129] = 0x01; par[129] = 0x3E;
+    par[133] = 0x01;
+    dyn[140] = 0x03;
+    dyn[141] = 0x03; par[141] = 0x20;
+    dyn[142] = 0x03; par[142] = 0x20;
+    dyn[150] = 0x07; par[150] = 0x20;
+    dyn[200] = 0x03; par[200] = 0x7C;
+    cudaError_t e = cudaMemcpyToSymbol(c_dyn_mask, dyn, sizeof(dyn));
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_par_mask, par, sizeof(par));
+    if (e == cudaSuccess) g_tables_ready[dev] = true;
+    return e;
+}
+
+cudaError_t prepare_tick(const NetDev& dev, const NetHost& host, cudaStream_t stream) {
+    (void)dev;
+    cudaError_t e = init_tables(stream);
+    if (e != cudaSuccess) return e;
+    e = prepare_synapse(stream);
+    if (e != cudaSuccess) return e;
+    return prepare_diffusion(host, stream);
+}
+
+static cudaError_t enqueue_modifiers(const NetDev& dev, const NetHost& host, float dt, cudaStream_t stream) {
+    k_gather<<<(dev.n_seg + 255) / 256, 256, 0, stream>>>(dev);
+    const size_t P = host.phase_off.size() ? host.phase_off.size() - 1 : 0;
+    for (size_t p = 0; p < P; p++) {
+        const uint32_t b = host.phase_off[p], e = host.phase_off[p + 1];
+        if (e > b) k_phase<<<(e - b + 255) / 256, 256, 0, stream>>>(dev, dt, b, e);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_modifiers(const NetDev& dev, const NetHost& host, float dt, unsigned long long tick,
+                             cudaStream_t stream) {
+    (void)tick;
+    cudaError_t e = prepare_tick(dev, host, stream);
+    if (e != cudaSuccess) return e;
+    return enqueue_modifiers(dev, host, dt, stream);
+}
+
+cudaError_t launch_diffusion(const NetDev& dev, const NetHost& host, float dt, unsigned long long tick,
+                             cudaStream_t stream) {
+    cudaError_t e = prepare_tick(dev, host, stream);
+    if (e != cudaSuccess) return e;
+    enqueue_diffusion(dev, host, dt, tick, stream);
+    return cudaGetLastError();
+}
+
+cudaError_t enqueue_tick(const NetDev& dev, const NetHost& host, float dt, unsigned long long tick, int first_tick,
+                         cudaStream_t stream) {
+    cudaError_t e = enqueue_modifiers(dev, host, dt, stream);
+    if (e != cudaSuccess) return e;
+    enqueue_diffusion(dev, host, dt, tick, stream);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    return launch_synapse(dev, dt, tick, first_tick, stream);
+}
+
+cudaError_t launch_tick(const NetDev& dev, const NetHost& host, float dt, unsigned long long tick, int first_tick,
+                        cudaStream_t stream) {
+    cudaError_t e = prepare_tick(dev, host, stream);
+    if (e != cudaSuccess) return e;
+    return enqueue_tick(dev, host, dt, tick, first_tick, stream);
+}
+
+}  // namespace bnc

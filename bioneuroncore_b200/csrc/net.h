@@ -29,6 +29,25 @@ enum : uint32_t {
 // Per-segment flags.
 enum : uint8_t { SF_MYELIN = 1u, SF_NMDA = 2u };
 
+// The state a modifier reads and writes, gathered per segment for step 1 so that an
+// item touches one or two contiguous 32-byte runs instead of many scattered words:
+// V and the 7 intra ions | 7 extra ions and ATP | area, the V of the GHK factors and
+// their branch codes | volume and I_total | the GHK factors (144 bytes, 16-aligned).
+struct __align__(16) SegRec {
+    float V;
+    float in[7];
+    float out[7];
+    float atp;
+    float area;
+    float gV;
+    uint32_t gm;      // GHK branch codes: m1 | m2 << 8
+    uint32_t pad;
+    double vol;
+    double itot;
+    double A1, e1, D1, A2, e2, D2;
+};
+static_assert(sizeof(SegRec) == 144, "SegRec layout");
+
 // Plain-old-data descriptor passed by value to the kernels.
 struct NetDev {
     uint32_t n_seg, n_tiles, n_items, n_phases, n_syn, n_rec, n_edges;
@@ -54,13 +73,14 @@ struct NetDev {
     uint8_t* sflags;
     float2* cav21_static;   // (density, state[1]) of the last Cav2.1 when it never updates
     float2* c21_cur;        // the same after step 1 of the current tick (k_modifiers -> k_diffusion)
+    struct SegRec* rec;     // per-segment working record of step 1 (k_gather -> phases -> k_diffusion)
     float4* pre_rec;        // V, Ca_out, Cav2.1 density, Cav2.1 h  (after step 2.5)
     float4* pre_ext;        // Na_in, K_in, Ca_in, Na_out
     float* pre_ext2;        // K_out
     // tiles
     uint32_t* tile_seg_beg;   // [n_tiles+1] device segment offsets
     uint32_t* tile_edge_beg;  // [n_tiles+1]
-    uint32_t* phase_off;      // [n_tiles*(n_phases+1)] absolute item offsets
+    uint32_t* phase_off;      // [n_phases+1] item offsets of the modifier phases
     uint16_t* warp_seg;       // [n_tiles*(kTileWarps+1)] tile-local offsets
     uint16_t* warp_edge;      // [n_tiles*(kTileWarps+1)]
     // edges (tile-grouped, tile-local endpoints)
@@ -71,8 +91,9 @@ struct NetDev {
     float* e_dist;
     uint32_t* inc_off;        // [n_seg+1]
     uint16_t* inc;            // tile-local edge index | (endpoint-is-b << 15)
-    // modifier items
-    uint32_t* it_meta;        // tile-local segment (16) | type (8) | flags (8)
+    // modifier items, by (phase, type, device segment)
+    uint32_t* it_seg;         // device segment
+    uint16_t* it_tf;          // type (8) | flags (8): bit0 non-default parameters, bit1 receptor override, av << 2
     float* it_den;
     float* it_st;             // [7][n_items]
     // current stimuli, per-segment CSR in stimulus order
@@ -141,8 +162,6 @@ struct BuildOptions {
     // Modifier phases: the greedy type-uniform schedule is kept while it needs at most
     // phase_cap phases (0: 2 x the longest active-modifier list + 4), else slot order.
     uint32_t phase_cap = 0;
-    // Resident CTAs per SM the modifier kernel is compiled for (2 or 3: register budget).
-    uint32_t mod_ctas = 2;
 };
 
 // Host copy of everything the exporter needs to map device state back.
@@ -157,6 +176,7 @@ struct NetHost {
     std::vector<uint8_t> rec_slot;   // device receptor -> receptor slot
     std::vector<uint8_t> syn_nt;     // released NT per device synapse
     uint32_t max_tile_segs = 0, max_tile_edges = 0;
+    std::vector<uint32_t> phase_off;         // item range of each modifier phase (host copy)
     size_t smem_bytes = 0;
     BuildOptions opt;                        // grouping the network was built with
     double algo_bytes_per_tick = 0;  // algorithmic HBM bytes per tick of this state schema
@@ -202,7 +222,8 @@ cudaError_t launch_tick(const NetDev& dev, const NetHost& host, float dt, unsign
 // the three kernels of a tick, one at a time (profiling)
 cudaError_t launch_modifiers(const NetDev& dev, const NetHost& host, float dt, unsigned long long tick,
                              cudaStream_t stream);
-cudaError_t launch_diffusion(const NetDev& dev, const NetHost& host, float dt, cudaStream_t stream);
+cudaError_t launch_diffusion(const NetDev& dev, const NetHost& host, float dt, unsigned long long tick,
+                             cudaStream_t stream);
 cudaError_t launch_synapse(const NetDev& dev, float dt, unsigned long long tick, int first_tick,
                            cudaStream_t stream);
 cudaError_t launch_set_clock(unsigned long long* clock, unsigned long long tick, unsigned long long ticks_run,
@@ -212,8 +233,8 @@ cudaError_t launch_advance_clock(unsigned long long* clock, cudaStream_t stream)
 cudaError_t prepare_synapse(cudaStream_t stream);
 // diffuse.cu
 cudaError_t prepare_diffusion(const NetHost& host, cudaStream_t stream);
-void enqueue_diffusion(const NetDev& dev, const NetHost& host, float dt, cudaStream_t stream);
+void enqueue_diffusion(const NetDev& dev, const NetHost& host, float dt, unsigned long long tick,
+                       cudaStream_t stream);
 size_t diffusion_smem_bytes(uint32_t max_segs, uint32_t max_edges);
-size_t tile_smem_bytes(uint32_t max_segs);
 
 }  // namespace bnc

@@ -261,12 +261,10 @@ int bnc_run_ticks_graph(void* sim, uint32_t n_ticks, float dt);
  *                        (defaults 64 and 1024);
  *   phase_cap            the modifier schedule keeps the greedy type-uniform
  *                        phases while they number at most phase_cap (0: twice the
- *                        longest modifier list + 4), else phases follow slot order;
- *   mod_ctas             resident CTAs per SM the modifier kernel is compiled for
- *                        (2 or 3; 3 trades registers for occupancy).
+ *                        longest modifier list + 4), else phases follow slot order.
  * Zero fields take the defaults. */
 typedef struct {
-    uint32_t warp_cap, tile_segs, phase_cap, mod_ctas;
+    uint32_t warp_cap, tile_segs, phase_cap;
 } BncBuildOptions;
 int bnc_load_generated_opts(void* sim, const BncNetgenParams* p, const BncBuildOptions* opt);
 int bnc_plan_generated_opts(const BncNetgenParams* p, const BncBuildOptions* opt, BncNetInfo* info);
