@@ -252,7 +252,7 @@ def run_ensemble(a, device):
         "sequential_value": rate_seq, "sequential_ms_per_tick": ms_seq / a.ens_ticks,
         "speedup_vs_sequential": rate_ens / rate_seq,
         "launch": "one structure, CUDA-graph tick loop (32 ticks per replay)",
-        "sequential_launch": "each network alone, plain launches (2 per tick), device time summed",
+        "sequential_launch": "each network alone, plain launches (gather, one per modifier phase, diffusion, synapse: phases + 3 per tick), device time summed",
         "grouping": {"warp_cap": tune.warp_cap, "tile_segs": tune.tile_segs,
                      "candidates_tried": tune.candidates_tried, "sample_members": tune.sample_members},
         "setup_s": round(setup_s, 1),
@@ -353,7 +353,7 @@ def main():
                        "l2": "inputs larger than L2 (device state ~8 GB per GPU)",
                        "tiles": info.n_tiles, "phases": info.n_phases, "setup_s": round(setup_s, 1)},
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,
-            "gpu_launches": 3 * a.steps, "ensemble": ensemble,
+            "gpu_launches": (info.n_phases + 3) * a.steps, "ensemble": ensemble,
         }
         print(json.dumps(line), flush=True)
     b.close()

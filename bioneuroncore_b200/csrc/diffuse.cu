@@ -48,10 +48,20 @@ __device__ __forceinline__ float sg_bernoulli(float x) {
     return x / (dm_expf(x) - 1.0f);
 }
 
+// valence group of ion q (+1: 0, 1, 6; +2: 2, 4; -1: 3, 5) and the group's factor
+// z * 0.03742f of the Scharfetter-Gummel argument, as kNpZ[q] * 0.03742f evaluates it
+__device__ __forceinline__ int valence_group(int q) {
+    return (q == 2 || q == 4) ? 1 : ((q == 3 || q == 5) ? 2 : 0);
+}
+__device__ __forceinline__ float valence_factor(int g) {
+    return g == 0 ? 1.0f * 0.03742f : (g == 1 ? 2.0f * 0.03742f : -1.0f * 0.03742f);
+}
+
 struct DiffSmem {
     double *itot, *phiA, *phiB, *sig, *ed;
     float *V, *in, *out, *atp, *area, *cm, *vf, *vnA, *vnB, *nb;
     float *gax, *dve, *fl, *ie, *earea, *edist;
+    float *coef;   // [7][E]: kDiffC[q] * area * dt_sub / dist of each connection
     uint16_t *incoff, *inc, *ea, *eb;
     uint8_t *ei, *es;
 };
@@ -82,7 +92,8 @@ __host__ __device__ inline size_t diff_layout(uint32_t S, uint32_t E, unsigned c
     p = take(8 * Ee); if (t) t->ed = (double*)p;
     p = take(4 * Ee); if (t) t->gax = (float*)p;
     p = take(4 * Ee); if (t) t->dve = (float*)p;
-    p = take(4 * Ee); if (t) t->fl = (float*)p;
+    p = take(4 * 7 * Ee); if (t) t->fl = (float*)p;    // [7][E] (Fick passes use row 0)
+    p = take(4 * 7 * Ee); if (t) t->coef = (float*)p;
     p = take(4 * Ee); if (t) t->ie = (float*)p;
     p = take(4 * Ee); if (t) t->earea = (float*)p;
     p = take(4 * Ee); if (t) t->edist = (float*)p;
@@ -207,7 +218,18 @@ k_diffusion(NetDev d, float dt, unsigned long long tick, uint32_t S, uint32_t E)
         t.edist[e] = d.e_dist[e0 + e];
     }
     for (int k = tid; k < ninc; k += nth) t.inc[k] = d.inc[inc0 + k];
+    const float dt_sub = dt / 5;
+    // Nernst-Planck flux coefficient of each connection and ion: the reference's
+    // kDiffC[q] * area * dt_sub / dist, left to right, the same in every substep.
+    for (int e = tid; e < ne; e += nth) {
+        const float ar = d.e_area[e0 + e], di = d.e_dist[e0 + e];
+#pragma unroll
+        for (int q = 0; q < 7; q++) t.coef[q * E + e] = kDiffC[q] * ar * dt_sub / di;
+    }
     __syncthreads();
+    // when every connection has its own thread, that thread keeps its connection's
+    // extracellular Bernoulli values in registers for the whole tick
+    const bool edge_reg = ne <= nth;
 
     if (d.flags & NF_DIFFUSION) {
         // this segment's incidences in connection order
@@ -306,7 +328,6 @@ k_diffusion(NetDev d, float dt, unsigned long long tick, uint32_t S, uint32_t E)
         }
 
         // ---- intracellular Nernst-Planck, 5 substeps (diffusion_kernel.h:152-238) ----
-        const float dt_sub = dt / 5;
         for (int sub = 0; sub < 5; sub++) {
             for (int e = tid; e < ne; e += nth) {
                 if (!t.ei[e]) continue;
@@ -348,22 +369,36 @@ k_diffusion(NetDev d, float dt, unsigned long long tick, uint32_t S, uint32_t E)
                     }
                 }
             }
-#pragma unroll 1
-            for (int q = 0; q < 7; q++) {
-                for (int e = tid; e < ne; e += nth) {
-                    if (!t.ei[e]) continue;
-                    const int a = t.ea[e], b = t.eb[e];
+            // The 7 ions' fluxes in one connection pass (an ion's flux reads only that
+            // ion, which no other ion's update touches), then one gather for all 7.
+            // Ions of equal valence share x = (z * 0.03742f) * dV and so its Bernoulli values.
+            for (int e = tid; e < ne; e += nth) {
+                if (!t.ei[e]) continue;
+                const int a = t.ea[e], b = t.eb[e];
+                float bm[3], bp[3];
+#pragma unroll
+                for (int g = 0; g < 3; g++) {
+                    const float x = valence_factor(g) * t.dve[e];
+                    bm[g] = sg_bernoulli(-x);
+                    bp[g] = sg_bernoulli(x);
+                }
+                float ie = t.ie[e];
+#pragma unroll
+                for (int q = 0; q < 7; q++) {
                     const float C_a = t.in[q * S + a];
                     const float C_b = t.in[q * S + b];
-                    const float x = kNpZ[q] * 0.03742f * t.dve[e];
-                    const float flux = kDiffC[q] * t.earea[e] * dt_sub / t.edist[e] *
-                                       (C_a * sg_bernoulli(-x) - C_b * sg_bernoulli(x));
-                    t.fl[e] = flux;
-                    t.ie[e] += kNpZ[q] * 96.485f * flux / dt_sub;
+                    const int g = valence_group(q);
+                    const float flux = t.coef[q * E + e] * (C_a * bm[g] - C_b * bp[g]);
+                    t.fl[q * E + e] = flux;
+                    ie += kNpZ[q] * 96.485f * flux / dt_sub;
                 }
-                __syncthreads();
-                if (i < ns) {   // reads edge fluxes and its own concentration: in place
-                    const float vf = t.vf[i];
+                t.ie[e] = ie;
+            }
+            __syncthreads();
+            if (i < ns) {   // reads connection fluxes and its own concentrations: in place
+                const float vf = t.vf[i];
+#pragma unroll 1
+                for (int q = 0; q < 7; q++) {
                     double acc = 0.0;
                     if (st.n >= 0) {
 #pragma unroll
@@ -371,20 +406,22 @@ k_diffusion(NetDev d, float dt, unsigned long long tick, uint32_t S, uint32_t E)
                             if (k >= st.n) break;
                             const int e = st.e[k];
                             if (!t.ei[e]) continue;
-                            if ((st.bend >> k) & 1u) acc += (double)t.fl[e] / vf; else acc -= (double)t.fl[e] / vf;
+                            if ((st.bend >> k) & 1u) acc += (double)t.fl[q * E + e] / vf;
+                            else acc -= (double)t.fl[q * E + e] / vf;
                         }
                     } else {
                         for (int k = t.incoff[i]; k < t.incoff[i + 1]; k++) {
                             const uint16_t ent = t.inc[k];
                             const int e = ent & 0x7FFF;
                             if (!t.ei[e]) continue;
-                            if (ent & 0x8000) acc += (double)t.fl[e] / vf; else acc -= (double)t.fl[e] / vf;
+                            if (ent & 0x8000) acc += (double)t.fl[q * E + e] / vf;
+                            else acc -= (double)t.fl[q * E + e] / vf;
                         }
                     }
                     t.in[q * S + i] = (float)((double)t.in[q * S + i] + (double)(float)acc);
                 }
-                __syncthreads();
             }
+            __syncthreads();
             for (int e = tid; e < ne; e += nth) {
                 if (!t.ei[e]) continue;
                 t.ie[e] = t.ie[e] - t.gax[e] * t.dve[e];
@@ -444,17 +481,35 @@ k_diffusion(NetDev d, float dt, unsigned long long tick, uint32_t S, uint32_t E)
         }
 
         // ---- extracellular Nernst-Planck, 5 substeps (diffusion_kernel.h:244-281) ----
+        // phi_e is fixed for the tick, so each connection's Bernoulli values are too:
+        // x = (float)((z * 0.03742f) * dphi) per valence group.
+        float xbm0 = 0.0f, xbm1 = 0.0f, xbm2 = 0.0f, xbp0 = 0.0f, xbp1 = 0.0f, xbp2 = 0.0f;
+        if (edge_reg && tid < ne) {
+            const double dphi = phi[t.ea[tid]] - phi[t.eb[tid]];
+            float x = (float)(valence_factor(0) * dphi);
+            xbm0 = sg_bernoulli(-x); xbp0 = sg_bernoulli(x);
+            x = (float)(valence_factor(1) * dphi);
+            xbm1 = sg_bernoulli(-x); xbp1 = sg_bernoulli(x);
+            x = (float)(valence_factor(2) * dphi);
+            xbm2 = sg_bernoulli(-x); xbp2 = sg_bernoulli(x);
+        }
         for (int sub = 0; sub < 5; sub++) {
 #pragma unroll 1
             for (int q = 0; q < 7; q++) {
+                const int g = valence_group(q);
                 for (int e = tid; e < ne; e += nth) {
                     const int a = t.ea[e], b = t.eb[e];
                     const double Ca = t.out[q * S + a];
                     const double Cb = t.out[q * S + b];
-                    const double dphi = phi[a] - phi[b];
-                    const float x = (float)(kNpZ[q] * 0.03742f * dphi);
-                    const double flux = kDiffC[q] * t.earea[e] * dt_sub / t.edist[e] *
-                                        (Ca * sg_bernoulli(-x) - Cb * sg_bernoulli(x));
+                    float bm = g == 0 ? xbm0 : (g == 1 ? xbm1 : xbm2);
+                    float bp = g == 0 ? xbp0 : (g == 1 ? xbp1 : xbp2);
+                    if (!edge_reg) {
+                        const double dphi = phi[a] - phi[b];
+                        const float x = (float)(kNpZ[q] * 0.03742f * dphi);
+                        bm = sg_bernoulli(-x);
+                        bp = sg_bernoulli(x);
+                    }
+                    const double flux = t.coef[q * E + e] * (Ca * bm - Cb * bp);
                     t.ed[e] = flux;
                 }
                 __syncthreads();
