@@ -40,7 +40,8 @@ NEW_SYMBOLS = ["bnc_netgen_aos", "bnc_netgen_free", "bnc_last_error", "bnc_load_
                "bnc_plan_aos", "bnc_bion_load", "bnc_bion_unload", "bnc_bion_save", "bnc_load_ensemble_generated",
                "bnc_load_ensemble_aos", "bnc_ensemble_member", "bnc_plan_ensemble_generated", "bnc_ensemble_params",
                "bnc_run_ticks_graph", "bnc_load_ensemble_tuned", "bnc_time_ticks_graph", "bnc_load_generated_opts",
-               "bnc_plan_generated_opts"]
+               "bnc_plan_generated_opts", "biocore_gpu_register_device_modifier", "bnc_register_device_modifier",
+               "bnc_device_modifier_registered"]
 
 
 class NetInfo(C.Structure):
@@ -96,6 +97,13 @@ def plan_ensemble(params):
     return inf
 
 
+def register_device_modifier(type_id, source, entry):
+    """Compiles CUDA C++ `source` (see include/bnc_device_modifier.h) with NVRTC and
+    registers its extern "C" kernel `entry` for modifier type `type_id` (0-127)."""
+    _check(load_library().bnc_register_device_modifier(type_id, source.encode(), entry.encode()),
+           "bnc_register_device_modifier")
+
+
 class BackendError(RuntimeError):
     pass
 
@@ -136,6 +144,9 @@ def load_library(path=LIB_PATH):
         "bnc_ensemble_params": ([C.c_uint64, u32, u32, u32, vp], i32), "bnc_run_ticks_graph": ([vp, u32, f32], i32),
         "bnc_load_ensemble_tuned": ([vp, vp, u32, u32, f32, vp], i32), "bnc_time_ticks_graph": ([vp, u32, f32, vp], i32),
         "bnc_load_generated_opts": ([vp, vp, vp], i32), "bnc_plan_generated_opts": ([vp, vp, vp], i32),
+        "biocore_gpu_register_device_modifier": ([C.c_uint8, C.c_char_p, C.c_char_p], i32),
+        "bnc_register_device_modifier": ([C.c_uint8, C.c_char_p, C.c_char_p], i32),
+        "bnc_device_modifier_registered": ([C.c_uint8], i32),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -328,4 +339,4 @@ class Backend:
 __all__ = ["Backend", "Network", "NetgenParams", "BionData", "BackendError", "load_library", "last_error",
            "NET_SMALL", "NET_LARGE", "NET_TREES", "NET_ENSEMBLE_MEMBER", "NET_ADJOINT", "NETGEN_NO_SYNAPSES",
            "NETGEN_NO_CONNECTIONS", "NETGEN_NO_STIMULI", "NETGEN_PERTURB_IONS", "SEG_FIELDS", "SYN_FIELDS",
-           "DROPIN_SYMBOLS", "NEW_SYMBOLS", "EnsembleMember", "Tuning", "BuildOptions", "ensemble_params", "plan_ensemble", "plan_generated"]
+           "DROPIN_SYMBOLS", "NEW_SYMBOLS", "EnsembleMember", "Tuning", "BuildOptions", "register_device_modifier", "ensemble_params", "plan_ensemble", "plan_generated"]

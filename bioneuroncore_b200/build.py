@@ -23,13 +23,13 @@ ORACLE_DIR = os.path.join(ROOT, "oracle")
 ORACLE_LIB = os.path.join(ORACLE_DIR, "liboracle.so")
 REFERENCE = "/root/reference"
 
-CU_SOURCES = ["modifiers.cu", "diffuse.cu", "synapse.cu", "backend.cu"]
+CU_SOURCES = ["modifiers.cu", "diffuse.cu", "synapse.cu", "backend.cu", "plugins.cu"]
 CPP_SOURCES = ["netgen.cpp", "capi_host.cpp", "builder.cpp"]
 HEADERS = sorted(f for f in os.listdir(CSRC) if f.endswith((".h", ".cuh")))
 
 GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--fmad=false", "-Xcompiler", "-fPIC,-ffp-contract=off",
-              "-I" + os.path.join(ROOT, "include")]
+              "-I" + os.path.join(ROOT, "include"), "-I" + BUILD]
 
 
 def _nvcc():
@@ -53,12 +53,26 @@ def _run(cmd):
     return r.stdout + r.stderr
 
 
+def _embed_header():
+    """Writes include/bnc_device_modifier.h as a C++ raw string literal into the build
+    folder; plugins.cu hands it to NVRTC so user sources can include it."""
+    src = os.path.join(ROOT, "include", "bnc_device_modifier.h")
+    out = os.path.join(BUILD, "bnc_device_modifier_h.inc")
+    if _stale(out, [src]):
+        text = open(src).read()
+        assert ")BNCH\"" not in text
+        with open(out, "w") as f:
+            f.write('R"BNCH(' + text + ')BNCH"\n')
+
+
 def build_library(verbose=False, ptxas_info=False):
     """Compiles libbnc_b200.so (sm_100a) if any source changed; returns its path."""
     os.makedirs(BUILD, exist_ok=True)
     nvcc = _nvcc()
     headers = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(ROOT, "include", f)
-                                                        for f in ("bnc_abi.h", "bnc_b200.h")]
+                                                        for f in ("bnc_abi.h", "bnc_b200.h",
+                                                                  "bnc_device_modifier.h")]
+    _embed_header()
     jobs = []
     objs = []
     for src in CU_SOURCES + CPP_SOURCES:

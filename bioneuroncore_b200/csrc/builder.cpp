@@ -297,6 +297,10 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
     const HostNet& aos = hn;
     if (n == 0 || S.empty()) { set_error("network has no segments"); return BNC_ERR_ARG; }
     if (n >= (1u << 31)) { set_error("too many segments"); return BNC_ERR_ARG; }
+    // modifier IDs run by registered device modifiers (they override built-in models of
+    // the same ID, as the reference's plugin table does on its CPU path)
+    bool user_type[256] = {false};
+    for (int t = 0; t < 128; t++) user_type[t] = device_modifier_registered((uint8_t)t);
     host->n_seg = n;
     host->n_conn = aos.num_connections;
     host->n_syn_total = aos.num_synapses;
@@ -308,7 +312,7 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
     for (uint32_t i = 0; i < n; i++) {
         if (S[i].modifier_count > BNC_MAX_MODIFIERS) { set_error("segment %u: modifier_count %u > 32", i, S[i].modifier_count); return BNC_ERR_FORMAT; }
         for (uint8_t j = 0; j < S[i].modifier_count; j++)
-            if (!type_supported(hn.mod(i, j).type)) {
+            if (!type_supported(hn.mod(i, j).type) && !user_type[hn.mod(i, j).type]) {
                 set_error("segment %u slot %u: modifier type %u has no device implementation in this backend",
                           i, j, hn.mod(i, j).type);
                 return BNC_ERR_UNSUPPORTED;
@@ -607,6 +611,22 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
         host->item_seg[q] = orig;
         host->item_slot[q] = slot;
     }
+    // registered device modifiers: their items form one contiguous run per phase and type
+    host->user_ranges.clear();
+    std::memset(dev->user_mask, 0, sizeof(dev->user_mask));
+    for (uint32_t p = 0; p < n_phases; p++) {
+        uint32_t q = phase_off[p];
+        while (q < phase_off[p + 1]) {
+            const uint8_t t = (uint8_t)(it_tf[q] & 0xFFu);
+            uint32_t r = q;
+            while (r < phase_off[p + 1] && (uint8_t)(it_tf[r] & 0xFFu) == t) r++;
+            if (user_type[t]) {
+                host->user_ranges.push_back({p, t, q, r, nullptr});
+                dev->user_mask[t >> 5] |= 1u << (t & 31);
+            }
+            q = r;
+        }
+    }
     lap("items");
     // ---- per-segment state and statics in device order ----
     std::vector<float> V(n), ion_in((size_t)7 * n), ion_out((size_t)7 * n), intra_nt((size_t)15 * n),
@@ -885,6 +905,10 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
         dev->e_dist = up(allocs, e_dist, &rc);
         dev->inc_off = up(allocs, inc_off, &rc);
         dev->inc = up(allocs, inc, &rc);
+        for (auto& ur : host->user_ranges) {
+            int krc = device_modifier_kernel((uint8_t)ur.type, &ur.kernel);
+            if (krc != BNC_OK) return krc;
+        }
         dev->it_seg = up(allocs, it_seg, &rc);
         dev->it_tf = up(allocs, it_tf, &rc);
         dev->it_den = up(allocs, it_den, &rc);

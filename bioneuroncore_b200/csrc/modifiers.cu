@@ -146,6 +146,7 @@ k_phase(NetDev d, float dt, uint32_t b, uint32_t e) {
     const uint32_t tf = d.it_tf[q];
     const uint8_t type = (uint8_t)(tf & 0xFFu);
     const uint8_t fl = (uint8_t)(tf >> 8);
+    if (type < 128 && ((d.user_mask[type >> 5] >> (type & 31)) & 1u)) return;   // a registered device modifier
     DMod m;
     m.den = d.it_den[q];
     m.av = (fl & 2) ? (uint8_t)((fl >> 2) & 7) : (uint8_t)0;
@@ -212,9 +213,16 @@ cudaError_t prepare_tick(const NetDev& dev, const NetHost& host, cudaStream_t st
 static cudaError_t enqueue_modifiers(const NetDev& dev, const NetHost& host, float dt, cudaStream_t stream) {
     k_gather<<<(dev.n_seg + 255) / 256, 256, 0, stream>>>(dev);
     const size_t P = host.phase_off.size() ? host.phase_off.size() - 1 : 0;
+    size_t u = 0;
     for (size_t p = 0; p < P; p++) {
         const uint32_t b = host.phase_off[p], e = host.phase_off[p + 1];
         if (e > b) k_phase<<<(e - b + 255) / 256, 256, 0, stream>>>(dev, dt, b, e);
+        // items of registered device modifiers in this phase (k_phase skips them)
+        for (; u < host.user_ranges.size() && host.user_ranges[u].phase == p; u++) {
+            const auto& ur = host.user_ranges[u];
+            cudaError_t le = launch_device_modifier(ur.kernel, dev, (uint8_t)ur.type, ur.begin, ur.end, dt, stream);
+            if (le != cudaSuccess) return le;
+        }
     }
     return cudaGetLastError();
 }

@@ -53,6 +53,7 @@ struct NetDev {
     uint32_t n_seg, n_tiles, n_items, n_phases, n_syn, n_rec, n_edges;
     uint32_t flags;
     uint32_t nt_used_mask;  // neurotransmitter indices that synapses/bath can make nonzero
+    uint32_t user_mask[4];  // modifier IDs 0-127 run by registered device modifiers (plugins.cu)
     // segment state (device order, ion-major for the 7-ion arrays)
     float* V;
     float* ion_in;    // [7][n_seg]
@@ -177,6 +178,8 @@ struct NetHost {
     std::vector<uint8_t> syn_nt;     // released NT per device synapse
     uint32_t max_tile_segs = 0, max_tile_edges = 0;
     std::vector<uint32_t> phase_off;         // item range of each modifier phase (host copy)
+    struct UserRange { uint32_t phase, type, begin, end; const void* kernel; };
+    std::vector<UserRange> user_ranges;      // registered device modifiers' items, per phase
     size_t smem_bytes = 0;
     BuildOptions opt;                        // grouping the network was built with
     double algo_bytes_per_tick = 0;  // algorithmic HBM bytes per tick of this state schema
@@ -229,6 +232,11 @@ cudaError_t launch_synapse(const NetDev& dev, float dt, unsigned long long tick,
 cudaError_t launch_set_clock(unsigned long long* clock, unsigned long long tick, unsigned long long ticks_run,
                              cudaStream_t stream);
 cudaError_t launch_advance_clock(unsigned long long* clock, cudaStream_t stream);
+// plugins.cu: registered device modifiers (user modifier IDs 0-127)
+bool device_modifier_registered(uint8_t type);
+int device_modifier_kernel(uint8_t type, const void** kernel);   // loads on first use (needs a device)
+cudaError_t launch_device_modifier(const void* kernel, const NetDev& d, uint8_t type, uint32_t b, uint32_t e, float dt,
+                                   cudaStream_t stream);
 // synapse.cu: per-device receptor constants (outside stream capture)
 cudaError_t prepare_synapse(cudaStream_t stream);
 // diffuse.cu

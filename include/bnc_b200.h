@@ -269,6 +269,26 @@ typedef struct {
 int bnc_load_generated_opts(void* sim, const BncNetgenParams* p, const BncBuildOptions* opt);
 int bnc_plan_generated_opts(const BncNetgenParams* p, const BncBuildOptions* opt, BncNetInfo* info);
 
+/* ---- Device modifiers: user modifier IDs 0-127 on the GPU ----
+ * The reference registers plugin modifiers as host functions
+ * (register_modifier_current, modifier_interface.h:38, called from a plugin's
+ * biocore_plugin_init, plugin_manager.cpp:260-313); they override the built-in
+ * model of that ID on its CPU path only (kernel_dispatch.h:336-343).  These calls
+ * register device code instead: CUDA C++ source defining an extern "C" __global__
+ * entry with the interface of bnc_device_modifier.h, compiled here by NVRTC for
+ * sm_100a (no device needed to register).  Networks loaded afterwards run the
+ * entry on that type's items, overriding a built-in model of the same ID; a
+ * network that uses an ID with neither a built-in model nor a registration is
+ * rejected with BNC_ERR_UNSUPPORTED (no CPU fallback).  Registering an ID again
+ * replaces it for networks loaded later.
+ *   biocore_gpu_register_device_modifier: source from a file (cu_path).
+ *   Errors: BNC_ERR_ARG (ID >= 128, compile errors -- the NVRTC log is in
+ *   bnc_last_error), BNC_ERR_UNSUPPORTED (NVRTC not available). */
+int biocore_gpu_register_device_modifier(uint8_t type_id, const char* cu_path, const char* entry);
+int bnc_register_device_modifier(uint8_t type_id, const char* source, const char* entry);
+/* 1 when a device modifier is registered for the ID, else 0. */
+int bnc_device_modifier_registered(uint8_t type_id);
+
 /* Host-only: runs the builder's planning on AoS arrays in memory (validation,
  * supported-type checks, tiles, schedule) without a device.  Returns the same
  * codes a load of that network would. */

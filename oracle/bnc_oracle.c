@@ -353,6 +353,41 @@ static inline float bo_xorshift32_rnd(uint32_t seed) {
     return (float)(x & 0x7FFFFFFFu) / (float)0x7FFFFFFFu;
 }
 
+/* Plugin modifiers (modifier_interface.h:38 register_modifier_current; a registered
+ * function overrides the built-in model of its ID on the reference's CPU path,
+ * kernel_dispatch.h:336-343).  The oracle's plugins see the FP32 state through this
+ * view -- the same fields the device modifiers of the tested library see. */
+typedef struct {
+    float* V;
+    float* in;        /* 7 intracellular ions */
+    float* out;       /* 7 extracellular ions */
+    float* atp;
+    float area;       /* effective area, the reference's state[7] */
+    double vol;
+    float density;
+    float* state;     /* 8 state words; state[7] holds the area */
+    uint8_t type;
+} BoPluginView;
+typedef double (*BoPluginFn)(BoPluginView* v, float dt);
+static BoPluginFn g_bo_plugins[128];
+
+int bo_register_modifier(uint8_t type, BoPluginFn fn) {
+    if (type >= 128) return -1;
+    g_bo_plugins[type] = fn;
+    return 0;
+}
+
+static double bo_call_modifier(uint8_t type, OMod* m, OSeg* s, float dt) {
+    if (type < 128 && g_bo_plugins[type]) {
+        BoPluginView v;
+        v.V = &s->V; v.in = s->in; v.out = s->out; v.atp = &s->atp;
+        v.area = m->st[7]; v.vol = bo_seg_volume(s);
+        v.density = m->density; v.state = m->st; v.type = type;
+        return g_bo_plugins[type](&v, dt);
+    }
+    return bo_dispatch(type, m, s, dt);
+}
+
 /* (uint32_t)(V_m * 1000.0f) with V_m double, as x86-64 g++ evaluates it:
  * truncation to a 64-bit integer, then modulo 2^32 (simulation_host.cpp:438-440). */
 static inline uint32_t bo_vm_seed_bits(float V) {
@@ -477,7 +512,7 @@ static void bo_tick(BoSim* S, float dt) {
             uint8_t type = s->mods[j].type;
             if (myel && type != 4 && bo_is_myelin_blocked(type)) continue;
             s->mods[j].st[7] = bo_seg_area(s);
-            I_total += bo_dispatch(type, &s->mods[j], s, dt);
+            I_total += bo_call_modifier(type, &s->mods[j], s, dt);
         }
         for (uint32_t k = 0; k < S->n_stim; k++) {
             const BncCurrentStimulus* st = &S->stim[k];
@@ -679,7 +714,8 @@ BoSim* bo_create(const BncBionData* d, const BncCurrentStimulus* stim, uint32_t 
         s->ibuf = a->I_buffer;
         s->nmod = a->modifier_count > 32 ? 32 : a->modifier_count;
         for (uint8_t j = 0; j < s->nmod; j++) {
-            if (!bo_type_supported(a->modifiers[j].type)) {
+            const uint8_t mt = a->modifiers[j].type;
+            if (!bo_type_supported(mt) && !(mt < 128 && g_bo_plugins[mt])) {
                 snprintf(err, errlen, "segment %u: modifier type %u not supported", i, a->modifiers[j].type);
                 return S;
             }

@@ -48,6 +48,7 @@ def oracle_lib():
             getattr(lib, name).restype = C.c_double
         lib.bo_nernst_f.argtypes = [C.c_float] * 3; lib.bo_nernst_f.restype = C.c_float
         lib.bo_const.argtypes = [C.c_int]; lib.bo_const.restype = C.c_double
+        lib.bo_register_modifier.argtypes = [C.c_uint8, C.c_void_p]; lib.bo_register_modifier.restype = C.c_int
         _ora = lib
     return _ora
 

@@ -93,7 +93,8 @@ def test_user_plugin_type_is_rejected():
     net = _net(family=1, n_neurons=2, seed=5)
     net.segments["modifiers"][0, 1]["type"] = 7 + 0   # NaK pump is supported
     assert _plan_aos(net)[0] == 0
-    net.segments["modifiers"][0, 1]["type"] = 20      # user ID range 0-127 without a device entry
+    net.segments["modifiers"][0, 1]["type"] = 60      # user ID range 0-127 without a device entry
+    assert _lib().bnc_device_modifier_registered(60) == 0
     assert _plan_aos(net)[0] == BNC_ERR_UNSUPPORTED
     assert last_error()
 
