@@ -17,7 +17,7 @@ import numpy as np
 
 from .abi import (BionData, NetgenParams, SEGMENT_DTYPE, SYNAPSE_DTYPE, CONN_DTYPE, STIM_DTYPE, view,
                   NET_SMALL, NET_LARGE, NET_TREES, NET_ENSEMBLE_MEMBER, NET_ADJOINT, NETGEN_NO_SYNAPSES,
-                  NETGEN_NO_CONNECTIONS, NETGEN_NO_STIMULI, NETGEN_PERTURB_IONS)
+                  NETGEN_NO_CONNECTIONS, NETGEN_NO_STIMULI, NETGEN_PERTURB_IONS, NETGEN_SYNAPSE_EXTRAS)
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libbnc_b200.so")
@@ -56,7 +56,8 @@ class NetInfo(C.Structure):
 
 class BuildOptions(C.Structure):
     """Device-layout options (include/bnc_b200.h BncBuildOptions); 0 = default."""
-    _fields_ = [("warp_cap", C.c_uint32), ("tile_segs", C.c_uint32), ("phase_cap", C.c_uint32)]
+    _fields_ = [("warp_cap", C.c_uint32), ("tile_segs", C.c_uint32), ("phase_cap", C.c_uint32),
+                ("chunk_segs", C.c_uint32)]
 
 
 class Tuning(C.Structure):
@@ -338,5 +339,5 @@ class Backend:
 
 __all__ = ["Backend", "Network", "NetgenParams", "BionData", "BackendError", "load_library", "last_error",
            "NET_SMALL", "NET_LARGE", "NET_TREES", "NET_ENSEMBLE_MEMBER", "NET_ADJOINT", "NETGEN_NO_SYNAPSES",
-           "NETGEN_NO_CONNECTIONS", "NETGEN_NO_STIMULI", "NETGEN_PERTURB_IONS", "SEG_FIELDS", "SYN_FIELDS",
+           "NETGEN_NO_CONNECTIONS", "NETGEN_NO_STIMULI", "NETGEN_PERTURB_IONS", "NETGEN_SYNAPSE_EXTRAS", "SEG_FIELDS", "SYN_FIELDS",
            "DROPIN_SYMBOLS", "NEW_SYMBOLS", "EnsembleMember", "Tuning", "BuildOptions", "register_device_modifier", "ensemble_params", "plan_ensemble", "plan_generated"]

@@ -566,6 +566,7 @@ static BuildOptions to_options(const BncBuildOptions* o) {
         if (o->warp_cap) opt.warp_cap = o->warp_cap;
         if (o->tile_segs) opt.tile_segs = o->tile_segs;
         opt.phase_cap = o->phase_cap;
+        if (o->chunk_segs) opt.chunk_segs = o->chunk_segs;
     }
     return opt;
 }
@@ -1041,7 +1042,7 @@ int bnc_save_bion(void* sim, const char* filename) {
 
 // ---- Ticks with the presynaptic exchange records in a library-owned array ----
 //
-// Each tick the tile kernel writes, for every segment, the record the synapse
+// Each tick the diffusion kernel writes, for every segment, the record the synapse
 // kernel reads for that segment as a presynaptic site: V, Ca_out and the Cav2.1
 // density and h gate (float4), plus Na_in, K_in, Ca_in, Na_out (float4) and K_out
 // (float) when some synapse has autoreceptors or a readily releasable pool.  That

@@ -556,11 +556,18 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
     // A phase is one launch of the modifier kernel over the whole network; sorting
     // by type inside it keeps warps, and the SMs at any moment, on few channel models.
     struct ItemKey { uint16_t phase; uint8_t type; uint32_t dseg; uint32_t k; };
-    const size_t NB = n_phases;
+    // Items are bucketed by (chunk, phase): a chunk is a run of chunk_segs segments whose
+    // step-1 records stay resident in L2 while all phases of the chunk run.
+    const uint32_t chunk_segs = opt.chunk_segs ? std::min(opt.chunk_segs, n) : n;
+    const uint32_t n_chunks = (n + chunk_segs - 1) / chunk_segs;
+    host->chunk_segs = chunk_segs;
+    host->n_chunks = n_chunks;
+    const size_t NB = (size_t)n_chunks * n_phases;
     std::vector<uint32_t> bucket_off(NB + 1, 0);
     for (uint32_t d = 0; d < n; d++) {
         uint32_t i = host->perm[d];
-        for (uint32_t k = act_off[i]; k < act_off[i + 1]; k++) bucket_off[item_phase[k] + 1]++;
+        for (uint32_t k = act_off[i]; k < act_off[i + 1]; k++)
+            bucket_off[(size_t)(d / chunk_segs) * n_phases + item_phase[k] + 1]++;
     }
     for (size_t b = 0; b < NB; b++) bucket_off[b + 1] += bucket_off[b];
     std::vector<ItemKey> keys(act_slot.size());
@@ -569,11 +576,11 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
         for (uint32_t d = 0; d < n; d++) {   // device order: each bucket fills in segment order
             uint32_t i = host->perm[d];
             for (uint32_t k = act_off[i]; k < act_off[i + 1]; k++)
-                keys[pos[item_phase[k]]++] = {item_phase[k], act_type[k], d, k};
+                keys[pos[(size_t)(d / chunk_segs) * n_phases + item_phase[k]]++] = {item_phase[k], act_type[k], d, k};
         }
         std::vector<ItemKey> tmp;
         uint32_t tc[257];
-        for (size_t b = 0; b < NB; b++) {   // stable counting sort by type inside each phase
+        for (size_t b = 0; b < NB; b++) {   // stable counting sort by type inside each bucket
             uint32_t lo = bucket_off[b], hi = bucket_off[b + 1];
             if (hi - lo < 2) continue;
             std::fill(tc, tc + 257, 0u);
@@ -614,7 +621,7 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
     // registered device modifiers: their items form one contiguous run per phase and type
     host->user_ranges.clear();
     std::memset(dev->user_mask, 0, sizeof(dev->user_mask));
-    for (uint32_t p = 0; p < n_phases; p++) {
+    for (uint32_t p = 0; p < (uint32_t)NB; p++) {   // bucket: chunk * n_phases + phase
         uint32_t q = phase_off[p];
         while (q < phase_off[p + 1]) {
             const uint8_t t = (uint8_t)(it_tf[q] & 0xFFu);

@@ -14,6 +14,7 @@
 //  k_diffusion   (diffuse.cu) stimuli, step 2.5 electrodiffusion, the presynaptic record.
 //  k_synapse     (synapse.cu) steps 3 and 4.
 #define BNC_MATH_OUTLINE 1   // 26 channel models in one kernel: keep exp/log out of line
+#include <algorithm>
 #include <cuda_runtime.h>
 #include "net.h"
 #include "physics.cuh"
@@ -26,10 +27,10 @@ __constant__ uint8_t c_dyn_mask[256];
 __constant__ uint8_t c_par_mask[256];
 
 __global__ void __launch_bounds__(256)
-k_gather(NetDev d) {
-    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+k_gather(NetDev d, uint32_t s_begin, uint32_t s_end) {
+    const uint32_t g = s_begin + blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t N = d.n_seg;
-    if (g >= N) return;
+    if (g >= s_end) return;
     SegRec r;
     r.V = d.V[g];
 #pragma unroll
@@ -211,17 +212,23 @@ cudaError_t prepare_tick(const NetDev& dev, const NetHost& host, cudaStream_t st
 }
 
 static cudaError_t enqueue_modifiers(const NetDev& dev, const NetHost& host, float dt, cudaStream_t stream) {
-    k_gather<<<(dev.n_seg + 255) / 256, 256, 0, stream>>>(dev);
-    const size_t P = host.phase_off.size() ? host.phase_off.size() - 1 : 0;
+    const uint32_t P = dev.n_phases;
+    const uint32_t C = host.n_chunks ? host.n_chunks : 1;
+    const uint32_t cs = host.chunk_segs ? host.chunk_segs : dev.n_seg;
     size_t u = 0;
-    for (size_t p = 0; p < P; p++) {
-        const uint32_t b = host.phase_off[p], e = host.phase_off[p + 1];
-        if (e > b) k_phase<<<(e - b + 255) / 256, 256, 0, stream>>>(dev, dt, b, e);
-        // items of registered device modifiers in this phase (k_phase skips them)
-        for (; u < host.user_ranges.size() && host.user_ranges[u].phase == p; u++) {
-            const auto& ur = host.user_ranges[u];
-            cudaError_t le = launch_device_modifier(ur.kernel, dev, (uint8_t)ur.type, ur.begin, ur.end, dt, stream);
-            if (le != cudaSuccess) return le;
+    for (uint32_t c = 0; c < C; c++) {
+        const uint32_t s0 = c * cs, s1 = std::min(dev.n_seg, s0 + cs);
+        k_gather<<<(s1 - s0 + 255) / 256, 256, 0, stream>>>(dev, s0, s1);
+        for (uint32_t p = 0; p < P; p++) {
+            const uint32_t bk = c * P + p;
+            const uint32_t b = host.phase_off[bk], e = host.phase_off[bk + 1];
+            if (e > b) k_phase<<<(e - b + 255) / 256, 256, 0, stream>>>(dev, dt, b, e);
+            // items of registered device modifiers in this bucket (k_phase skips them)
+            for (; u < host.user_ranges.size() && host.user_ranges[u].bucket == bk; u++) {
+                const auto& ur = host.user_ranges[u];
+                cudaError_t le = launch_device_modifier(ur.kernel, dev, (uint8_t)ur.type, ur.begin, ur.end, dt, stream);
+                if (le != cudaSuccess) return le;
+            }
         }
     }
     return cudaGetLastError();

@@ -81,7 +81,7 @@ struct NetDev {
     // tiles
     uint32_t* tile_seg_beg;   // [n_tiles+1] device segment offsets
     uint32_t* tile_edge_beg;  // [n_tiles+1]
-    uint32_t* phase_off;      // [n_phases+1] item offsets of the modifier phases
+    uint32_t* phase_off;      // [n_chunks*n_phases+1] item offsets of the (chunk, phase) buckets
     uint16_t* warp_seg;       // [n_tiles*(kTileWarps+1)] tile-local offsets
     uint16_t* warp_edge;      // [n_tiles*(kTileWarps+1)]
     // edges (tile-grouped, tile-local endpoints)
@@ -163,6 +163,10 @@ struct BuildOptions {
     // Modifier phases: the greedy type-uniform schedule is kept while it needs at most
     // phase_cap phases (0: 2 x the longest active-modifier list + 4), else slot order.
     uint32_t phase_cap = 0;
+    // Segments per chunk of the modifier pass (0: the whole network in one chunk).
+    // All phases of a chunk run before the next chunk, so a chunk's step-1 records
+    // (144 bytes per segment) can stay in L2 between phases.
+    uint32_t chunk_segs = BNC_DEFAULT_CHUNK_SEGS;
 };
 
 // Host copy of everything the exporter needs to map device state back.
@@ -177,9 +181,10 @@ struct NetHost {
     std::vector<uint8_t> rec_slot;   // device receptor -> receptor slot
     std::vector<uint8_t> syn_nt;     // released NT per device synapse
     uint32_t max_tile_segs = 0, max_tile_edges = 0;
-    std::vector<uint32_t> phase_off;         // item range of each modifier phase (host copy)
-    struct UserRange { uint32_t phase, type, begin, end; const void* kernel; };
-    std::vector<UserRange> user_ranges;      // registered device modifiers' items, per phase
+    std::vector<uint32_t> phase_off;         // item range of each (chunk, phase) bucket (host copy)
+    uint32_t chunk_segs = 0, n_chunks = 1;   // modifier-pass chunks of consecutive segments
+    struct UserRange { uint32_t bucket, type, begin, end; const void* kernel; };
+    std::vector<UserRange> user_ranges;      // registered device modifiers' items, per bucket
     size_t smem_bytes = 0;
     BuildOptions opt;                        // grouping the network was built with
     double algo_bytes_per_tick = 0;  // algorithmic HBM bytes per tick of this state schema

@@ -133,6 +133,7 @@ int generate_network(const BncNetgenParams& p, NetSink& sink, NetShape* shape_ou
     if (shape_out) *shape_out = shape;
 
     Rng rng_geo(p.seed * 4 + 1), rng_mod(p.seed * 4 + 2), rng_syn(p.seed * 4 + 3), rng_stim(p.seed * 4 + 4);
+    Rng rng_extra(p.seed * 4 + 0x9E37);   // BNC_NETGEN_SYNAPSE_EXTRAS only
     float wsum = 0.0f;
     for (const auto& t : kLargeTypes) wsum += t.weight;
 
@@ -273,6 +274,19 @@ int generate_network(const BncNetgenParams& p, NetSink& sink, NetShape* shape_ou
                 set_mod(sy.post_receptors[j], rt, 200.0);
             }
             sy.post_receptor_count = (uint8_t)nr;
+            if (p.flags & BNC_NETGEN_SYNAPSE_EXTRAS) {
+                if (rng_extra.u01() < 0.3) {
+                    sy.RRP_max = 25.0f;
+                    sy.RRP = (float)(10.0 + 15.0 * rng_extra.u01());
+                    sy.RRP_recovery = 0.01f;
+                }
+                if (rng_extra.u01() < 0.3) {
+                    const bool nav = rng_extra.u01() < 0.5;
+                    set_mod(sy.pre_autoreceptors[0], nav ? BNC_MOD_NAV16 : BNC_MOD_KV_DR, nav ? 0.5 : 1.0);
+                    sy.pre_autoreceptor_count = 1;
+                }
+                if (rng_extra.u01() < 0.3) sy.delay = (float)(0.5 + 1.5 * rng_extra.u01());
+            }
             sy.release_probability = 0.3f;
             sy.release_amount = 1.0f;
             sy.tau_clearance = 1.0f;

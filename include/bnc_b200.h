@@ -116,6 +116,11 @@ typedef struct {
 #define BNC_NETGEN_NO_STIMULI 4u
 #define BNC_NETGEN_PERTURB_IONS 8u
 #define BNC_NETGEN_DRAW_ORDER 16u   /* large set: keep modifiers in draw order (default: by type ID) */
+/* Synapses also exercise the presynaptic machinery: about 30% each get a readily
+ * releasable pool (RRP_max 25, recovery 0.01), a presynaptic autoreceptor channel
+ * (Kv delayed rectifier 123 or Nav1.6 141 on the bouton) and a transmission delay
+ * of 0.5-2 ms (drawn from a stream of their own: other draws are unchanged). */
+#define BNC_NETGEN_SYNAPSE_EXTRAS 32u
 
 /* Generates a network into host AoS arrays in the reference layout.  The arrays
  * are owned by the library; release with bnc_netgen_free.  *stim receives the
@@ -139,8 +144,8 @@ int bnc_run_ticks(void* sim, uint32_t n_ticks, float dt);
  * callers that cannot call cudaMalloc while they drive the simulation: a host
  * whose own pool allocator has reserved the device memory and treats any other
  * allocation as an error, or a control loop that cannot afford the device-wide
- * synchronisation a cudaFree brings.  Each tick the tile kernel hands the synapse
- * kernel a per-segment record of the presynaptic state (36 bytes per segment);
+ * synchronisation a cudaFree brings.  Each tick the diffusion kernel hands the
+ * synapse kernel a per-segment record of the presynaptic state (36 bytes per segment);
  * here that scratch is a fixed array inside the library instead of buffers of the
  * network, and the call allocates nothing.
  *   - Limit: networks of at most BNC_STATIC_SCRATCH_MAX_SEGMENTS segments (the
@@ -261,11 +266,19 @@ int bnc_run_ticks_graph(void* sim, uint32_t n_ticks, float dt);
  *                        (defaults 64 and 1024);
  *   phase_cap            the modifier schedule keeps the greedy type-uniform
  *                        phases while they number at most phase_cap (0: twice the
- *                        longest modifier list + 4), else phases follow slot order.
+ *                        longest modifier list + 4), else phases follow slot order;
+ *   chunk_segs           the modifier pass runs all its phases on chunks of this
+ *                        many consecutive segments in turn, so a chunk's working
+ *                        records (144 bytes per segment) can stay in L2 between
+ *                        phases (0: BNC_DEFAULT_CHUNK_SEGS, one chunk).  On B200
+ *                        the extra launches cost more than L2 residency saves
+ *                        (6.4M segments: 9.4 ms per tick in one chunk, 9.5 ms in
+ *                        524,288-segment chunks, 11.6 ms in 262,144).
  * Zero fields take the defaults. */
 typedef struct {
-    uint32_t warp_cap, tile_segs, phase_cap;
+    uint32_t warp_cap, tile_segs, phase_cap, chunk_segs;
 } BncBuildOptions;
+#define BNC_DEFAULT_CHUNK_SEGS 0xFFFFFFFFu
 int bnc_load_generated_opts(void* sim, const BncNetgenParams* p, const BncBuildOptions* opt);
 int bnc_plan_generated_opts(const BncNetgenParams* p, const BncBuildOptions* opt, BncNetInfo* info);
 

@@ -23,6 +23,8 @@ DT = 0.025
 CASES = {
     "small_n8_s7": (dict(family=1, n_neurons=8, seed=7), 200),
     "large_n4_s3": (dict(family=2, n_neurons=4, n_synapses=80, seed=3), 100),
+    # RRP, presynaptic autoreceptors and transmission delays (BNC_NETGEN_SYNAPSE_EXTRAS)
+    "extras_n8_s7": (dict(family=1, n_neurons=8, seed=7, flags=32), 200),
 }
 
 
@@ -53,7 +55,7 @@ def run_reference(spec, ticks):
         V=seg["V_m"].copy(), ion_in=seg["intra_ions"][:, :7].copy(), ion_out=seg["extra_ions"][:, :7].copy(),
         ATP=seg["ATP_level"].astype(np.float64), spikes=spikes.copy(),
         syn_weight=syn["weight"].astype(np.float64), syn_spine_Ca=syn["spine_Ca"].astype(np.float64),
-        syn_bouton_Ca=syn["bouton_Ca"].astype(np.float64),
+        syn_bouton_Ca=syn["bouton_Ca"].astype(np.float64), syn_RRP=syn["RRP"].astype(np.float64),
     )
     out.update({"param_" + k: np.int64(v) for k, v in spec.items()})
     return out

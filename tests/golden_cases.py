@@ -37,6 +37,8 @@ def compare(g, trace, seg_field, syn_field):
     errs["syn_weight"] = _rel(syn_field("weight"), g["syn_weight"], 1e-9)
     errs["syn_spine_Ca"] = _rel(syn_field("spine_Ca"), g["syn_spine_Ca"], 1e-9)
     errs["syn_bouton_Ca"] = _rel(syn_field("bouton_Ca"), g["syn_bouton_Ca"], 1e-9)
+    if "syn_RRP" in g.files:
+        errs["syn_RRP"] = _rel(syn_field("RRP"), g["syn_RRP"], 1e-6)
     bad = {k: v for k, v in errs.items() if not v <= REL_TOL}
     assert not bad, "relative error above %g: %r" % (REL_TOL, bad)
     spikes = np.asarray(seg_field("spikes", 0)).astype(np.int64)

@@ -41,7 +41,7 @@ SEG_CHECKS = [("V", 0)] + [("ion_in", q) for q in range(7)] + [("ion_out", q) fo
     ("ATP", 0), ("temperature", 0), ("transcription", 0), ("spikes", 0)] + [("neurotransmitter", q) for q in (0, 1, 7)]
 SYN_CHECKS = [("bouton_Ca", 0), ("spine_Ca", 0), ("weight", 0), ("refractory", 0), ("facilitation", 0),
               ("spine_camkii", 0), ("spine_calcineurin", 0), ("cleft", 0), ("cleft", 1),
-              ("receptor_state", 0), ("receptor_state", 1)]
+              ("receptor_state", 0), ("receptor_state", 1), ("RRP", 0)]
 
 
 def _compare_all(ora, gpu, n_syn, label):
@@ -56,7 +56,7 @@ def _compare_all(ora, gpu, n_syn, label):
             _assert_same(gpu.synapse_field(f, i, n_syn), ora.synapse_field(f, i), "%s synapse %s[%d]" % (label, f, i))
 
 
-@pytest.mark.parametrize("flags", [0, 1 | 2, 1, 2])
+@pytest.mark.parametrize("flags", [0, 1 | 2, 1, 2, 32])
 def test_small_network_bitexact(flags):
     from bioneuroncore_b200 import NetgenParams, NET_SMALL
     p = NetgenParams(family=NET_SMALL, n_neurons=16, seed=11, flags=flags)
@@ -67,9 +67,10 @@ def test_small_network_bitexact(flags):
         _compare_all(ora, gpu, net.data.num_synapses, "small flags=%d after +%d" % (flags, step))
 
 
-def test_large_set_bitexact():
+@pytest.mark.parametrize("flags", [0, 32])
+def test_large_set_bitexact(flags):
     from bioneuroncore_b200 import NetgenParams, NET_LARGE
-    p = NetgenParams(family=NET_LARGE, n_neurons=12, n_synapses=300, seed=5)
+    p = NetgenParams(family=NET_LARGE, n_neurons=12, n_synapses=300, seed=5, flags=flags)
     ora, gpu, net = _pair(p)
     for step in (1, 20, 30):
         ora.run(step, DT)
@@ -94,3 +95,20 @@ def test_gpu_matches_reference_fixture(name):
         trace[t] = gpu.segment_field("V")[somata]
     n_syn = net.data.num_synapses
     golden_cases.compare(g, trace, gpu.segment_field, lambda f: gpu.synapse_field(f, 0, n_syn))
+
+
+@pytest.mark.parametrize("chunk", [64, 300])
+def test_chunked_modifier_pass_bitexact(chunk):
+    """The modifier pass run chunk by chunk (all phases of a chunk of segments before
+    the next) computes what the oracle computes: chunking only reorders independent
+    segments."""
+    from bioneuroncore_b200 import Backend, BuildOptions, Network, NetgenParams, NET_LARGE
+    p = NetgenParams(family=NET_LARGE, n_neurons=12, n_synapses=300, seed=5)
+    ora = Oracle(Network(p))
+    gpu = Backend()
+    gpu.load_generated(p, BuildOptions(chunk_segs=chunk))
+    n_syn = ora.n_syn
+    for step in (1, 20):
+        ora.run(step, DT)
+        gpu.run_ticks(step, DT)
+        _compare_all(ora, gpu, n_syn, "chunk %d after +%d" % (chunk, step))
