@@ -12,7 +12,6 @@
 #include <cuda_runtime.h>
 #include "net.h"
 #include "physics.cuh"
-#include "exact_div.h"
 
 namespace bnc {
 
@@ -300,7 +299,6 @@ k_diffusion(NetDev d, float dt, unsigned long long tick, uint32_t S, uint32_t E)
                 for (int k = t.incoff[i]; k < t.incoff[i + 1]; k++) diag += t.ed[t.inc[k] & 0x7FFF];
             }
         }
-        const double ydiag = recip_for_div(diag);   // the 50 sweeps divide by the same diagonal
         double* phi = t.phiA;
         double* phn = t.phiB;
         for (int it = 0; it < 50; it++) {
@@ -320,7 +318,7 @@ k_diffusion(NetDev d, float dt, unsigned long long tick, uint32_t S, uint32_t E)
                         pn += g * phi[o];
                     }
                 }
-                double v = (diag > 1e-9) ? div_by(pn - itot, diag, ydiag) : 0.0;
+                double v = (diag > 1e-9) ? (pn - itot) / diag : 0.0;
                 if (v > 10.0) v = 10.0;
                 if (v < -10.0) v = -10.0;
                 phn[i] = v;
@@ -399,7 +397,6 @@ k_diffusion(NetDev d, float dt, unsigned long long tick, uint32_t S, uint32_t E)
             __syncthreads();
             if (i < ns) {   // reads connection fluxes and its own concentrations: in place
                 const float vf = t.vf[i];
-                const double yvf = recip_for_div((double)vf);
 #pragma unroll 1
                 for (int q = 0; q < 7; q++) {
                     double acc = 0.0;
@@ -409,16 +406,16 @@ k_diffusion(NetDev d, float dt, unsigned long long tick, uint32_t S, uint32_t E)
                             if (k >= st.n) break;
                             const int e = st.e[k];
                             if (!t.ei[e]) continue;
-                            if ((st.bend >> k) & 1u) acc += div_by((double)t.fl[q * E + e], (double)vf, yvf);
-                            else acc -= div_by((double)t.fl[q * E + e], (double)vf, yvf);
+                            if ((st.bend >> k) & 1u) acc += (double)t.fl[q * E + e] / vf;
+                            else acc -= (double)t.fl[q * E + e] / vf;
                         }
                     } else {
                         for (int k = t.incoff[i]; k < t.incoff[i + 1]; k++) {
                             const uint16_t ent = t.inc[k];
                             const int e = ent & 0x7FFF;
                             if (!t.ei[e]) continue;
-                            if (ent & 0x8000) acc += div_by((double)t.fl[q * E + e], (double)vf, yvf);
-                            else acc -= div_by((double)t.fl[q * E + e], (double)vf, yvf);
+                            if (ent & 0x8000) acc += (double)t.fl[q * E + e] / vf;
+                            else acc -= (double)t.fl[q * E + e] / vf;
                         }
                     }
                     t.in[q * S + i] = (float)((double)t.in[q * S + i] + (double)(float)acc);
@@ -518,23 +515,21 @@ k_diffusion(NetDev d, float dt, unsigned long long tick, uint32_t S, uint32_t E)
                 __syncthreads();
                 if (i < ns) {   // in place, as above
                     const float vf = t.vf[i];
-                    const double vx = (double)(vf * EXTRA_VOLUME_RATIO);
-                    const double yvx = recip_for_div(vx);
                     double acc = 0.0;
                     if (st.n >= 0) {
 #pragma unroll
                         for (int k = 0; k < kDeg; k++) {
                             if (k >= st.n) break;
                             const int e = st.e[k];
-                            if ((st.bend >> k) & 1u) acc += div_by(t.ed[e], vx, yvx);
-                            else acc -= div_by(t.ed[e], vx, yvx);
+                            if ((st.bend >> k) & 1u) acc += t.ed[e] / (vf * EXTRA_VOLUME_RATIO);
+                            else acc -= t.ed[e] / (vf * EXTRA_VOLUME_RATIO);
                         }
                     } else {
                         for (int k = t.incoff[i]; k < t.incoff[i + 1]; k++) {
                             const uint16_t ent = t.inc[k];
                             const int e = ent & 0x7FFF;
-                            if (ent & 0x8000) acc += div_by(t.ed[e], vx, yvx);
-                            else acc -= div_by(t.ed[e], vx, yvx);
+                            if (ent & 0x8000) acc += t.ed[e] / (vf * EXTRA_VOLUME_RATIO);
+                            else acc -= t.ed[e] / (vf * EXTRA_VOLUME_RATIO);
                         }
                     }
                     t.out[q * S + i] = (float)((double)t.out[q * S + i] + acc);
