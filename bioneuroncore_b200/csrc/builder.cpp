@@ -346,14 +346,6 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
         for (uint32_t i = 0; i < n; i++) host->perm[pos[rank[comp_of[i]]]++] = i;
         comp_members_off.assign(cnt.begin(), cnt.end());
     }
-    host->inv.assign(n, 0);
-    host->perm_identity = true;
-    for (uint32_t d = 0; d < n; d++) {
-        host->inv[host->perm[d]] = d;
-        if (host->perm[d] != d) host->perm_identity = false;
-    }
-    lap("components");
-    // ---- tile packing: whole components, one component per warp slot ----
     if (opt.warp_cap < 1 || opt.tile_segs < 32 || opt.tile_segs > (uint32_t)kMaxTileSegs || opt.phase_cap > 4096) {
         set_error("build options out of range (warp_cap %u, tile_segs %u, phase_cap %u)", opt.warp_cap,
                   opt.tile_segs, opt.phase_cap);
@@ -362,6 +354,61 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
     host->opt = opt;
     const uint32_t warp_cap = opt.warp_cap;
     const uint32_t tile_cap = opt.tile_segs;
+    // A component larger than a tile spans a pair of tiles run by one 2-CTA cluster.
+    // Its segments are laid out depth first from its root (neighbours in ascending
+    // order), so cutting the list in half separates subtrees and few connections
+    // cross between the two tiles.  The order changes no arithmetic: every gather
+    // follows original connection order.
+    bool any_big = false;
+    for (size_t r = 0; r < roots.size(); r++)
+        if (comp_members_off[r + 1] - comp_members_off[r] > tile_cap) any_big = true;
+    if (any_big) {
+        std::vector<uint32_t> adj_off(n + 1, 0);
+        for (uint32_t c : conn_ok) {
+            const auto& cn = hn.conn[c];
+            if (comp_size[comp_of[cn.segment_a]] <= tile_cap) continue;
+            adj_off[cn.segment_a + 1]++;
+            adj_off[cn.segment_b + 1]++;
+        }
+        for (uint32_t i = 0; i < n; i++) adj_off[i + 1] += adj_off[i];
+        std::vector<uint32_t> adj(adj_off[n]);
+        {
+            std::vector<uint32_t> pos(adj_off.begin(), adj_off.end() - 1);
+            for (uint32_t c : conn_ok) {
+                const auto& cn = hn.conn[c];
+                if (comp_size[comp_of[cn.segment_a]] <= tile_cap) continue;
+                adj[pos[cn.segment_a]++] = cn.segment_b;
+                adj[pos[cn.segment_b]++] = cn.segment_a;
+            }
+        }
+        for (uint32_t i = 0; i < n; i++) std::sort(adj.begin() + adj_off[i], adj.begin() + adj_off[i + 1]);
+        std::vector<uint8_t> seen(n, 0);
+        std::vector<uint32_t> stack;
+        for (size_t r = 0; r < roots.size(); r++) {
+            const uint32_t b = comp_members_off[r], e = comp_members_off[r + 1];
+            if (e - b <= tile_cap) continue;
+            uint32_t k = b;
+            stack.assign(1, roots[r]);
+            while (!stack.empty()) {
+                const uint32_t x = stack.back();
+                stack.pop_back();
+                if (seen[x]) continue;
+                seen[x] = 1;
+                host->perm[k++] = x;
+                for (uint32_t j = adj_off[x + 1]; j > adj_off[x]; j--)   // smallest neighbour on top
+                    if (!seen[adj[j - 1]]) stack.push_back(adj[j - 1]);
+            }
+            if (k != e) { set_error("internal: depth-first layout of component %zu incomplete", r); return BNC_ERR_ARG; }
+        }
+    }
+    host->inv.assign(n, 0);
+    host->perm_identity = true;
+    for (uint32_t d = 0; d < n; d++) {
+        host->inv[host->perm[d]] = d;
+        if (host->perm[d] != d) host->perm_identity = false;
+    }
+    lap("components");
+    // ---- tile packing: whole components, one component per warp slot ----
     std::vector<uint32_t> tile_seg_beg{0};
     std::vector<uint16_t> warp_seg;   // per tile kTileWarps+1 entries
     {
@@ -374,11 +421,26 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
             cur_tile_segs = 0; cur_warp = 0; cur_warp_segs = 0;
             std::fill(wb.begin(), wb.end(), 0);
         };
+        // a tile of `segs` segments of one large component (one warp group)
+        auto push_tile = [&](uint32_t segs) {
+            std::vector<uint16_t> w(kTileWarps + 1, (uint16_t)segs);
+            w[0] = 0;
+            warp_seg.insert(warp_seg.end(), w.begin(), w.end());
+            tile_seg_beg.push_back(tile_seg_beg.back() + segs);
+        };
         for (size_t r = 0; r < roots.size(); r++) {
             uint32_t sz = comp_members_off[r + 1] - comp_members_off[r];
             if (sz > tile_cap) {
-                set_error("connected component of %u segments exceeds the %u-segment tile", sz, tile_cap);
-                return BNC_ERR_UNSUPPORTED;
+                if (sz > 2 * tile_cap) {
+                    set_error("connected component of %u segments exceeds two %u-segment tiles", sz, tile_cap);
+                    return BNC_ERR_UNSUPPORTED;
+                }
+                if (cur_tile_segs > 0) close_tile();
+                if ((tile_seg_beg.size() - 1) % 2 == 1) push_tile(0);   // the pair starts a cluster
+                const uint32_t h = (sz + 1) / 2;
+                push_tile(h);
+                push_tile(sz - h);
+                continue;
             }
             bool fits_warp = cur_warp_segs > 0 && cur_warp_segs + sz <= warp_cap;
             if (!fits_warp && cur_warp_segs > 0) {  // move to the next warp
@@ -396,48 +458,68 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
             wb[cur_warp + 1] = (uint16_t)cur_tile_segs;
         }
         if (cur_tile_segs > 0) close_tile();
+        if (any_big && (tile_seg_beg.size() - 1) % 2 == 1) push_tile(0);   // whole clusters only
     }
     const uint32_t T = (uint32_t)tile_seg_beg.size() - 1;
+    host->cluster = any_big ? 2 : 1;
     std::vector<uint32_t> tile_of(n);
     for (uint32_t t = 0; t < T; t++)
         for (uint32_t d = tile_seg_beg[t]; d < tile_seg_beg[t + 1]; d++) tile_of[d] = t;
     lap("tiles");
-    // ---- edges grouped by tile and warp, in original connection order ----
+    // ---- connections per tile, in original order ----
+    // A connection whose endpoints sit in the two tiles of a pair is in both tiles:
+    // each CTA computes it from identical values and gathers it for its own segment.
+    // A tile refers to the other tile's endpoint through a ghost slot after its own
+    // segments; the diffusion kernel refreshes ghosts from the owner after updates.
     std::vector<uint32_t> tile_edge_beg(T + 1, 0);
     std::vector<uint16_t> warp_edge(T * (kTileWarps + 1), 0);
     std::vector<uint32_t> edge_conn;   // device edge -> original connection index
+    std::vector<uint32_t> gh_off(T + 1, 0), gh_seg, gh_src;
+    std::vector<uint16_t> e_a, e_b;
     {
-        std::vector<std::vector<uint32_t>> per_tile_warp((size_t)T * kTileWarps);
+        std::vector<std::vector<uint32_t>> tile_conns(T);
         for (uint32_t c : conn_ok) {
-            uint32_t da = host->inv[hn.conn[c].segment_a];
-            uint32_t t = tile_of[da];
-            uint32_t la = da - tile_seg_beg[t];
-            int w = 0;
-            while (w < kTileWarps - 1 && la >= warp_seg[t * (kTileWarps + 1) + w + 1]) w++;
-            per_tile_warp[(size_t)t * kTileWarps + w].push_back(c);
-        }
-        for (uint32_t t = 0; t < T; t++) {
-            uint32_t e0 = (uint32_t)edge_conn.size();
-            for (int w = 0; w < kTileWarps; w++) {
-                warp_edge[t * (kTileWarps + 1) + w] = (uint16_t)(edge_conn.size() - e0);
-                auto& v = per_tile_warp[(size_t)t * kTileWarps + w];
-                edge_conn.insert(edge_conn.end(), v.begin(), v.end());
+            const uint32_t da = host->inv[hn.conn[c].segment_a], db = host->inv[hn.conn[c].segment_b];
+            const uint32_t ta = tile_of[da], tb = tile_of[db];
+            tile_conns[ta].push_back(c);
+            if (tb != ta) {
+                if ((ta ^ 1u) != tb) { set_error("internal: connection %u crosses unpaired tiles", c); return BNC_ERR_ARG; }
+                tile_conns[tb].push_back(c);
             }
-            warp_edge[t * (kTileWarps + 1) + kTileWarps] = (uint16_t)(edge_conn.size() - e0);
+        }
+        std::vector<uint32_t> ghosts;
+        for (uint32_t t = 0; t < T; t++) {
+            const uint32_t e0 = (uint32_t)edge_conn.size();
+            const uint32_t ns_t = tile_seg_beg[t + 1] - tile_seg_beg[t];
+            ghosts.clear();
+            auto local = [&](uint32_t x) -> uint16_t {
+                if (tile_of[x] == t) return (uint16_t)(x - tile_seg_beg[t]);
+                for (size_t g = 0; g < ghosts.size(); g++) if (ghosts[g] == x) return (uint16_t)(ns_t + g);
+                ghosts.push_back(x);
+                return (uint16_t)(ns_t + ghosts.size() - 1);
+            };
+            for (uint32_t c : tile_conns[t]) {
+                edge_conn.push_back(c);
+                e_a.push_back(local(host->inv[hn.conn[c].segment_a]));
+                e_b.push_back(local(host->inv[hn.conn[c].segment_b]));
+            }
+            for (uint32_t x : ghosts) {
+                gh_seg.push_back(x);
+                gh_src.push_back(x - tile_seg_beg[tile_of[x]]);   // owner tile is t ^ 1 (the pair)
+            }
+            gh_off[t + 1] = (uint32_t)gh_seg.size();
+            const uint32_t ne_t = (uint32_t)edge_conn.size() - e0;
+            for (int w = 0; w <= kTileWarps; w++) warp_edge[t * (kTileWarps + 1) + w] = (uint16_t)(w == 0 ? 0 : ne_t);
             tile_edge_beg[t + 1] = (uint32_t)edge_conn.size();
-            if (edge_conn.size() - e0 > 32767) { set_error("tile %u has more than 32767 connections", t); return BNC_ERR_UNSUPPORTED; }
+            if (ne_t > 32767) { set_error("tile %u has more than 32767 connections", t); return BNC_ERR_UNSUPPORTED; }
+            if (ns_t + ghosts.size() > 65535) { set_error("tile %u has too many ghost segments", t); return BNC_ERR_UNSUPPORTED; }
         }
     }
     const uint32_t E = (uint32_t)edge_conn.size();
-    std::vector<uint16_t> e_a(E), e_b(E);
     std::vector<uint8_t> e_intra(E);
     std::vector<float> e_area(E), e_dist(E);
     for (uint32_t e = 0; e < E; e++) {
         const auto& cn = hn.conn[edge_conn[e]];
-        uint32_t da = host->inv[cn.segment_a], db = host->inv[cn.segment_b];
-        uint32_t t = tile_of[da];
-        e_a[e] = (uint16_t)(da - tile_seg_beg[t]);
-        e_b[e] = (uint16_t)(db - tile_seg_beg[t]);
         e_intra[e] = cn.is_intracellular;
         const SegLite& A = S[cn.segment_a];
         const SegLite& B = S[cn.segment_b];
@@ -450,33 +532,37 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
         e_dist[e] = dist;
     }
     lap("edges");
-    // incidence lists per device segment: original connection order, a-role before b-role
+    // incidence lists per device segment: the connections of its own tile that touch
+    // it, in original connection order, a-role before b-role
     std::vector<uint32_t> inc_off(n + 1, 0);
-    for (uint32_t e = 0; e < E; e++) {
-        const auto& cn = hn.conn[edge_conn[e]];
-        inc_off[host->inv[cn.segment_a] + 1]++;
-        inc_off[host->inv[cn.segment_b] + 1]++;
-    }
+    for (uint32_t t = 0; t < T; t++)
+        for (uint32_t e = tile_edge_beg[t]; e < tile_edge_beg[t + 1]; e++) {
+            const auto& cn = hn.conn[edge_conn[e]];
+            const uint32_t da = host->inv[cn.segment_a], db = host->inv[cn.segment_b];
+            if (tile_of[da] == t) inc_off[da + 1]++;
+            if (tile_of[db] == t) inc_off[db + 1]++;
+        }
     for (uint32_t i = 0; i < n; i++) inc_off[i + 1] += inc_off[i];
     std::vector<uint16_t> inc(inc_off[n]);
     {
-        // edges of a tile are sorted by warp then connection index; the gather needs
-        // connection order, so sort each segment's list by original connection index.
         std::vector<uint32_t> pos(inc_off.begin(), inc_off.end() - 1);
-        std::vector<std::pair<uint32_t, uint16_t>> tmp;
         std::vector<uint64_t> key(inc_off[n]);
-        for (uint32_t e = 0; e < E; e++) {
-            const auto& cn = hn.conn[edge_conn[e]];
-            uint32_t t = tile_of[host->inv[cn.segment_a]];
-            uint16_t le = (uint16_t)(e - tile_edge_beg[t]);
-            uint32_t da = host->inv[cn.segment_a], db = host->inv[cn.segment_b];
-            uint32_t ka = pos[da]++;
-            inc[ka] = le;
-            key[ka] = ((uint64_t)edge_conn[e] << 1) | 0u;
-            uint32_t kb = pos[db]++;
-            inc[kb] = (uint16_t)(le | 0x8000u);
-            key[kb] = ((uint64_t)edge_conn[e] << 1) | 1u;
-        }
+        for (uint32_t t = 0; t < T; t++)
+            for (uint32_t e = tile_edge_beg[t]; e < tile_edge_beg[t + 1]; e++) {
+                const auto& cn = hn.conn[edge_conn[e]];
+                const uint16_t le = (uint16_t)(e - tile_edge_beg[t]);
+                const uint32_t da = host->inv[cn.segment_a], db = host->inv[cn.segment_b];
+                if (tile_of[da] == t) {
+                    const uint32_t ka = pos[da]++;
+                    inc[ka] = le;
+                    key[ka] = ((uint64_t)edge_conn[e] << 1) | 0u;
+                }
+                if (tile_of[db] == t) {
+                    const uint32_t kb = pos[db]++;
+                    inc[kb] = (uint16_t)(le | 0x8000u);
+                    key[kb] = ((uint64_t)edge_conn[e] << 1) | 1u;
+                }
+            }
         std::vector<uint32_t> idx;
         for (uint32_t d = 0; d < n; d++) {
             uint32_t b = inc_off[d], e = inc_off[d + 1];
@@ -858,6 +944,24 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
         rc_st[r] = rc_st0[r]; rc_st[(size_t)NR + r] = rc_st1[r]; rc_st[(size_t)2 * NR + r] = rc_st2[r];
     }
     lap("receptors");
+    // tile sizes for the shared-memory plan: own segments (threads), own + ghost
+    // segments (the per-segment array stride), connections
+    uint32_t mts = 0, mte = 0, mst = 0;
+    for (uint32_t t = 0; t < T; t++) {
+        const uint32_t ns_t = tile_seg_beg[t + 1] - tile_seg_beg[t];
+        mts = std::max(mts, ns_t);
+        mst = std::max(mst, ns_t + gh_off[t + 1] - gh_off[t]);
+        mte = std::max(mte, tile_edge_beg[t + 1] - tile_edge_beg[t]);
+    }
+    host->max_tile_segs = mts;
+    host->max_tile_stride = mst;
+    host->max_tile_edges = mte;
+    host->smem_bytes = diffusion_smem_bytes(mst, mte);
+    if (host->smem_bytes > 227 * 1024) {
+        set_error("tile of %u segments (%u with ghosts) and %u connections needs %zu bytes of shared memory "
+                  "(227 KB per CTA)", mts, mst, mte, host->smem_bytes);
+        return BNC_ERR_UNSUPPORTED;
+    }
     // ---- upload (skipped for a host-only plan) ----
     int rc = BNC_OK;
     dev->n_seg = n; dev->n_tiles = T; dev->n_items = NI; dev->n_phases = n_phases;
@@ -912,6 +1016,9 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
         dev->e_dist = up(allocs, e_dist, &rc);
         dev->inc_off = up(allocs, inc_off, &rc);
         dev->inc = up(allocs, inc, &rc);
+        dev->gh_off = up(allocs, gh_off, &rc);
+        dev->gh_seg = up(allocs, gh_seg, &rc);
+        dev->gh_src = up(allocs, gh_src, &rc);
         for (auto& ur : host->user_ranges) {
             int krc = device_modifier_kernel((uint8_t)ur.type, &ur.kernel);
             if (krc != BNC_OK) return krc;
@@ -963,20 +1070,6 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
         if (rc != BNC_OK) { set_error("device allocation/upload failed (%d)", rc); return rc; }
     }
     lap("upload");
-    // tile sizes for the shared-memory plan
-    uint32_t mts = 0, mte = 0;
-    for (uint32_t t = 0; t < T; t++) {
-        mts = std::max(mts, tile_seg_beg[t + 1] - tile_seg_beg[t]);
-        mte = std::max(mte, tile_edge_beg[t + 1] - tile_edge_beg[t]);
-    }
-    host->max_tile_segs = mts;
-    host->max_tile_edges = mte;
-    host->smem_bytes = diffusion_smem_bytes(mts, mte);
-    if (host->smem_bytes > 227 * 1024) {
-        set_error("tile of %u segments and %u connections needs %zu bytes of shared memory (227 KB per CTA)", mts, mte,
-                  host->smem_bytes);
-        return BNC_ERR_UNSUPPORTED;
-    }
     // ---- algorithmic bytes per tick of this schema (what one tick must move at minimum) ----
     {
         // kernel A per segment: read V, 14 ions, ATP, geometry+C_m (radius, length, area,

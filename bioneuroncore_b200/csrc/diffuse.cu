@@ -9,6 +9,7 @@
 // sweep is a few independent shared-memory loads, the arithmetic and one barrier.
 // Every gather sums the segment's incident connections in original connection order,
 // the order of the reference's scatter loops, so results are bit-identical to them.
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 #include "net.h"
 #include "physics.cuh"
@@ -63,6 +64,7 @@ struct DiffSmem {
     float *gax, *dve, *fl, *ie, *earea, *edist;
     float *coef;   // [7][E]: kDiffC[q] * area * dt_sub / dist of each connection
     uint16_t *incoff, *inc, *ea, *eb;
+    uint16_t *gsrc;   // ghost g's index in the paired tile
     uint8_t *ei, *es;
 };
 
@@ -88,6 +90,7 @@ __host__ __device__ inline size_t diff_layout(uint32_t S, uint32_t E, unsigned c
     p = take(4 * (size_t)S); if (t) t->vnB = (float*)p;
     p = take(4 * (size_t)S); if (t) t->nb = (float*)p;
     p = take(2 * ((size_t)S + 1)); if (t) t->incoff = (uint16_t*)p;
+    p = take(2 * (size_t)S); if (t) t->gsrc = (uint16_t*)p;
     p = take(2 * Ii); if (t) t->inc = (uint16_t*)p;
     p = take(8 * Ee); if (t) t->ed = (double*)p;
     p = take(4 * Ee); if (t) t->gax = (float*)p;
@@ -114,9 +117,35 @@ struct Stencil {
     uint8_t bend;   // bit k: the segment is edge e[k]'s b end
 };
 
+// Barrier of the CTAs that share a tile: the CTA itself, or both CTAs of a
+// 2-CTA cluster whose tiles hold the halves of one large component.
+template <int CL>
+__device__ __forceinline__ void tile_sync() {
+    if constexpr (CL == 2) cooperative_groups::this_cluster().sync();
+    else __syncthreads();
+}
+
+// After a tile_sync that follows an update: copy the paired CTA's values of this
+// tile's ghost segments (rows of stride S) into the ghost slots, then make them
+// visible to the CTA.  The peer does not change those values again before both
+// CTAs have passed another cluster barrier.
+template <int CL, typename T>
+__device__ __forceinline__ void halo(T* base, int rows, uint32_t S, int ns, int ng, const uint16_t* gsrc, int tid,
+                                     int nth) {
+    if constexpr (CL == 2) {
+        cooperative_groups::cluster_group cl = cooperative_groups::this_cluster();
+        const T* peer = cl.map_shared_rank(base, cl.block_rank() ^ 1u);
+        for (int k = tid; k < rows * ng; k += nth) {
+            const int r = k / ng, g = k - r * ng;
+            base[(size_t)r * S + ns + g] = peer[(size_t)r * S + gsrc[g]];
+        }
+        __syncthreads();
+    }
+}
+
 // Fick pass for a float field in t.nb (diffusion_kernel.h:284-345): per-edge flux,
 // then per-segment gather in connection order, updating t.nb in place.
-template <bool kIntraOnly, bool kGradStrict>
+template <int CL, bool kIntraOnly, bool kGradStrict>
 __device__ __forceinline__ void fick(const DiffSmem& t, int ns, int ne, int tid, int nth, int i, const Stencil& st,
                                      float D, float thresh, float dt) {
     for (int e = tid; e < ne; e += nth) {
@@ -128,7 +157,7 @@ __device__ __forceinline__ void fick(const DiffSmem& t, int ns, int ne, int tid,
         t.fl[e] = D * t.earea[e] * dC * dt / t.edist[e];
         t.es[e] = 0;
     }
-    __syncthreads();
+    tile_sync<CL>();
     // the gather reads only edge fluxes and the segment's own value: update in place
     if (i < ns) {
         const float vf = t.vf[i];
@@ -151,11 +180,12 @@ __device__ __forceinline__ void fick(const DiffSmem& t, int ns, int ne, int tid,
         }
         t.nb[i] = t.nb[i] + acc;
     }
-    __syncthreads();
+    tile_sync<CL>();
 }
 
 }  // namespace
 
+template <int CL>
 __global__ void __launch_bounds__(1024)
 k_diffusion(NetDev d, float dt, unsigned long long tick, uint32_t S, uint32_t E) {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -172,6 +202,8 @@ k_diffusion(NetDev d, float dt, unsigned long long tick, uint32_t S, uint32_t E)
     const uint32_t inc0 = d.inc_off[s0];
     const int ninc = (int)(d.inc_off[s0 + ns] - inc0);
     const int i = tid;   // this thread's segment (when i < ns)
+    const uint32_t gh0 = CL == 2 ? d.gh_off[tile] : 0u;
+    const int ng = CL == 2 ? (int)(d.gh_off[tile + 1] - gh0) : 0;   // ghost segments (clustered tiles only)
     if (d.clock) tick = d.clock[0];
 
     // ---- load: state after step 1 (the modifier phases' records), stimuli, statics ----
@@ -218,6 +250,19 @@ k_diffusion(NetDev d, float dt, unsigned long long tick, uint32_t S, uint32_t E)
         t.edist[e] = d.e_dist[e0 + e];
     }
     for (int k = tid; k < ninc; k += nth) t.inc[k] = d.inc[inc0 + k];
+    for (int g = tid; g < ng; g += nth) {   // ghosts: the paired tile's segments this tile's connections reach
+        const SegRec* r = d.rec + d.gh_seg[gh0 + g];
+        const int x = ns + g;
+        t.V[x] = r->V;
+#pragma unroll
+        for (int q = 0; q < 7; q++) {
+            t.in[q * S + x] = r->in[q];
+            t.out[q * S + x] = r->out[q];
+        }
+        t.atp[x] = r->atp;
+        t.phiA[x] = 0.0;
+        t.gsrc[g] = (uint16_t)d.gh_src[gh0 + g];
+    }
     const float dt_sub = dt / 5;
     // Nernst-Planck flux coefficient of each connection and ion: the reference's
     // kDiffC[q] * area * dt_sub / dist, left to right, the same in every substep.
@@ -226,7 +271,7 @@ k_diffusion(NetDev d, float dt, unsigned long long tick, uint32_t S, uint32_t E)
 #pragma unroll
         for (int q = 0; q < 7; q++) t.coef[q * E + e] = kDiffC[q] * ar * dt_sub / di;
     }
-    __syncthreads();
+    tile_sync<CL>();
     // when every connection has its own thread, that thread keeps its connection's
     // extracellular Bernoulli values in registers for the whole tick
     const bool edge_reg = ne <= nth;
@@ -263,12 +308,13 @@ k_diffusion(NetDev d, float dt, unsigned long long tick, uint32_t S, uint32_t E)
             t.sig[i] = 3.612f * sacc;
             t.phiA[i] = 0.0;
         }
-        __syncthreads();
+        tile_sync<CL>();
+        halo<CL>(t.sig, 1, S, ns, ng, t.gsrc, tid, nth);
         for (int e = tid; e < ne; e += nth) {
             double g = 0.5 * (t.sig[t.ea[e]] + t.sig[t.eb[e]]) * t.earea[e] / t.edist[e];
             t.ed[e] = g;
         }
-        __syncthreads();
+        tile_sync<CL>();
         // diagonal and the sweep stencil (connections with g > 0, in order)
         double diag = 0.0, itot = 0.0;
         double pg[kDeg];
@@ -323,7 +369,8 @@ k_diffusion(NetDev d, float dt, unsigned long long tick, uint32_t S, uint32_t E)
                 if (v < -10.0) v = -10.0;
                 phn[i] = v;
             }
-            __syncthreads();
+            tile_sync<CL>();
+            halo<CL>(phn, 1, S, ns, ng, t.gsrc, tid, nth);
             double* tmp = phi; phi = phn; phn = tmp;
         }
 
@@ -342,7 +389,7 @@ k_diffusion(NetDev d, float dt, unsigned long long tick, uint32_t S, uint32_t E)
                 t.dve[e] = (float)(((double)t.V[a] + phi[a]) - ((double)t.V[b] + phi[b]));
                 t.ie[e] = 0.0f;
             }
-            __syncthreads();
+            tile_sync<CL>();
             // g_diag, and the V-sweep stencil (intracellular connections, in order)
             float gd = 0.0f;
             float vg[kDeg];
@@ -394,7 +441,7 @@ k_diffusion(NetDev d, float dt, unsigned long long tick, uint32_t S, uint32_t E)
                 }
                 t.ie[e] = ie;
             }
-            __syncthreads();
+            tile_sync<CL>();
             if (i < ns) {   // reads connection fluxes and its own concentrations: in place
                 const float vf = t.vf[i];
 #pragma unroll 1
@@ -421,12 +468,12 @@ k_diffusion(NetDev d, float dt, unsigned long long tick, uint32_t S, uint32_t E)
                     t.in[q * S + i] = (float)((double)t.in[q * S + i] + (double)(float)acc);
                 }
             }
-            __syncthreads();
+            tile_sync<CL>();
             for (int e = tid; e < ne; e += nth) {
                 if (!t.ei[e]) continue;
                 t.ie[e] = t.ie[e] - t.gax[e] * t.dve[e];
             }
-            __syncthreads();
+            tile_sync<CL>();
             float rhs = 0.0f, den = 1.0f;
             if (i < ns) {
                 float inp = 0.0f;
@@ -452,7 +499,8 @@ k_diffusion(NetDev d, float dt, unsigned long long tick, uint32_t S, uint32_t E)
                 den = C_dt + gd;
                 t.vnA[i] = t.V[i];
             }
-            __syncthreads();
+            for (int g = tid; g < ng; g += nth) t.vnA[ns + g] = t.V[ns + g];
+            tile_sync<CL>();
             float* vc = t.vnA;
             float* vn = t.vnB;
             for (int it = 0; it < 50; it++) {
@@ -473,11 +521,14 @@ k_diffusion(NetDev d, float dt, unsigned long long tick, uint32_t S, uint32_t E)
                     }
                     vn[i] = (rhs + off) / den;
                 }
-                __syncthreads();
+                tile_sync<CL>();
+                halo<CL>(vn, 1, S, ns, ng, t.gsrc, tid, nth);
                 float* tmp = vc; vc = vn; vn = tmp;
             }
             if (i < ns) t.V[i] = vc[i];
-            __syncthreads();
+            tile_sync<CL>();
+            halo<CL>(t.V, 1, S, ns, ng, t.gsrc, tid, nth);
+            halo<CL>(t.in, 7, S, ns, ng, t.gsrc, tid, nth);
         }
 
         // ---- extracellular Nernst-Planck, 5 substeps (diffusion_kernel.h:244-281) ----
@@ -512,7 +563,7 @@ k_diffusion(NetDev d, float dt, unsigned long long tick, uint32_t S, uint32_t E)
                     const double flux = t.coef[q * E + e] * (Ca * bm - Cb * bp);
                     t.ed[e] = flux;
                 }
-                __syncthreads();
+                tile_sync<CL>();
                 if (i < ns) {   // in place, as above
                     const float vf = t.vf[i];
                     double acc = 0.0;
@@ -534,7 +585,8 @@ k_diffusion(NetDev d, float dt, unsigned long long tick, uint32_t S, uint32_t E)
                     }
                     t.out[q * S + i] = (float)((double)t.out[q * S + i] + acc);
                 }
-                __syncthreads();
+                tile_sync<CL>();
+                halo<CL>(t.out + (size_t)q * S, 1, S, ns, ng, t.gsrc, tid, nth);
             }
         }
 
@@ -542,35 +594,40 @@ k_diffusion(NetDev d, float dt, unsigned long long tick, uint32_t S, uint32_t E)
         if (d.flags & NF_INTRA_NT) {
             for (int nt = 0; nt < 15; nt++) {
                 if (i < ns) t.nb[i] = d.intra_nt[(size_t)nt * N + s0 + i];
-                __syncthreads();
-                fick<true, false>(t, ns, ne, tid, nth, i, st, gNtD[nt], 1e-12f, dt);
+                for (int g = tid; g < ng; g += nth) t.nb[ns + g] = d.intra_nt[(size_t)nt * N + d.gh_seg[gh0 + g]];
+                tile_sync<CL>();
+                fick<CL, true, false>(t, ns, ne, tid, nth, i, st, gNtD[nt], 1e-12f, dt);
                 if (i < ns) d.intra_nt[(size_t)nt * N + s0 + i] = t.nb[i];
             }
         }
         if (d.flags & NF_NT_DIFFUSE_OUT) {
             for (int nt = 0; nt < 15; nt++) {
                 if (i < ns) t.nb[i] = d.nt[(size_t)nt * N + s0 + i];
-                __syncthreads();
-                fick<false, false>(t, ns, ne, tid, nth, i, st, gNtD[nt], 1e-12f, dt);
+                for (int g = tid; g < ng; g += nth) t.nb[ns + g] = d.nt[(size_t)nt * N + d.gh_seg[gh0 + g]];
+                tile_sync<CL>();
+                fick<CL, false, false>(t, ns, ne, tid, nth, i, st, gNtD[nt], 1e-12f, dt);
                 if (i < ns) d.nt[(size_t)nt * N + s0 + i] = t.nb[i];
             }
         }
         {
             if (i < ns) t.nb[i] = t.atp[i];
-            __syncthreads();
-            fick<true, true>(t, ns, ne, tid, nth, i, st, 0.14f, 1e-12f, dt);
+            for (int g = tid; g < ng; g += nth) t.nb[ns + g] = t.atp[ns + g];
+            tile_sync<CL>();
+            fick<CL, true, true>(t, ns, ne, tid, nth, i, st, 0.14f, 1e-12f, dt);
             if (i < ns) t.atp[i] = t.nb[i];
         }
         if (d.flags & NF_TEMP) {
             if (i < ns) t.nb[i] = d.temp[s0 + i];
-            __syncthreads();
-            fick<true, true>(t, ns, ne, tid, nth, i, st, 0.0014f, 0.001f, dt);
+            for (int g = tid; g < ng; g += nth) t.nb[ns + g] = d.temp[d.gh_seg[gh0 + g]];
+            tile_sync<CL>();
+            fick<CL, true, true>(t, ns, ne, tid, nth, i, st, 0.0014f, 0.001f, dt);
             if (i < ns) d.temp[s0 + i] = t.nb[i];
         }
         if (d.flags & NF_TXN) {
             if (i < ns) t.nb[i] = d.txn[s0 + i];
-            __syncthreads();
-            fick<true, true>(t, ns, ne, tid, nth, i, st, 0.01f, 1e-9f, dt);
+            for (int g = tid; g < ng; g += nth) t.nb[ns + g] = d.txn[d.gh_seg[gh0 + g]];
+            tile_sync<CL>();
+            fick<CL, true, true>(t, ns, ne, tid, nth, i, st, 0.01f, 1e-9f, dt);
             if (i < ns) d.txn[s0 + i] = t.nb[i];
         }
         if (i < ns) {
@@ -624,16 +681,37 @@ cudaError_t prepare_diffusion(const NetHost& host, cudaStream_t stream) {
         if (e != cudaSuccess) return e;
         g_ntd_ready[dev] = true;
     }
-    const size_t smem = diffusion_smem_bytes(host.max_tile_segs, host.max_tile_edges);
+    const size_t smem = diffusion_smem_bytes(host.max_tile_stride, host.max_tile_edges);
     if (smem > 48 * 1024)
-        return cudaFuncSetAttribute(k_diffusion, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        return host.cluster == 2
+                   ? cudaFuncSetAttribute(k_diffusion<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
+                   : cudaFuncSetAttribute(k_diffusion<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     return cudaSuccess;
 }
 
-void enqueue_diffusion(const NetDev& dev, const NetHost& host, float dt, unsigned long long tick,
-                       cudaStream_t stream) {
-    const uint32_t S = host.max_tile_segs, E = host.max_tile_edges;
-    k_diffusion<<<dev.n_tiles, diffusion_threads(S), diffusion_smem_bytes(S, E), stream>>>(dev, dt, tick, S, E);
+cudaError_t enqueue_diffusion(const NetDev& dev, const NetHost& host, float dt, unsigned long long tick,
+                              cudaStream_t stream) {
+    const uint32_t S = host.max_tile_stride, E = host.max_tile_edges;
+    const size_t smem = diffusion_smem_bytes(S, E);
+    const uint32_t threads = diffusion_threads(host.max_tile_segs);
+    if (host.cluster == 2) {
+        // tiles in pairs: one 2-CTA cluster per pair (n_tiles is even)
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(dev.n_tiles);
+        cfg.blockDim = dim3(threads);
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = stream;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = 2;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        return cudaLaunchKernelEx(&cfg, k_diffusion<2>, dev, dt, tick, S, E);
+    }
+    k_diffusion<1><<<dev.n_tiles, threads, smem, stream>>>(dev, dt, tick, S, E);
+    return cudaGetLastError();
 }
 
 }  // namespace bnc

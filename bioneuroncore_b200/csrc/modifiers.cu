@@ -246,16 +246,14 @@ cudaError_t launch_diffusion(const NetDev& dev, const NetHost& host, float dt, u
                              cudaStream_t stream) {
     cudaError_t e = prepare_tick(dev, host, stream);
     if (e != cudaSuccess) return e;
-    enqueue_diffusion(dev, host, dt, tick, stream);
-    return cudaGetLastError();
+    return enqueue_diffusion(dev, host, dt, tick, stream);
 }
 
 cudaError_t enqueue_tick(const NetDev& dev, const NetHost& host, float dt, unsigned long long tick, int first_tick,
                          cudaStream_t stream) {
     cudaError_t e = enqueue_modifiers(dev, host, dt, stream);
     if (e != cudaSuccess) return e;
-    enqueue_diffusion(dev, host, dt, tick, stream);
-    e = cudaGetLastError();
+    e = enqueue_diffusion(dev, host, dt, tick, stream);
     if (e != cudaSuccess) return e;
     return launch_synapse(dev, dt, tick, first_tick, stream);
 }

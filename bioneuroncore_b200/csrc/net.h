@@ -92,6 +92,12 @@ struct NetDev {
     float* e_dist;
     uint32_t* inc_off;        // [n_seg+1]
     uint16_t* inc;            // tile-local edge index | (endpoint-is-b << 15)
+    // ghosts of tiles paired in a 2-CTA cluster (a component larger than one tile):
+    // tile t's ghost g is device segment gh_seg[gh_off[t] + g], at tile-local index
+    // n_own + g, owned by tile t ^ 1 at its local index gh_src[gh_off[t] + g]
+    uint32_t* gh_off;         // [n_tiles+1]
+    uint32_t* gh_seg;
+    uint32_t* gh_src;
     // modifier items, by (phase, type, device segment)
     uint32_t* it_seg;         // device segment
     uint16_t* it_tf;          // type (8) | flags (8): bit0 non-default parameters, bit1 receptor override, av << 2
@@ -181,6 +187,8 @@ struct NetHost {
     std::vector<uint8_t> rec_slot;   // device receptor -> receptor slot
     std::vector<uint8_t> syn_nt;     // released NT per device synapse
     uint32_t max_tile_segs = 0, max_tile_edges = 0;
+    uint32_t max_tile_stride = 0;            // own + ghost segments of the largest tile
+    uint32_t cluster = 1;                    // CTAs per diffusion cluster (2: tiles in pairs)
     std::vector<uint32_t> phase_off;         // item range of each (chunk, phase) bucket (host copy)
     uint32_t chunk_segs = 0, n_chunks = 1;   // modifier-pass chunks of consecutive segments
     struct UserRange { uint32_t bucket, type, begin, end; const void* kernel; };
@@ -246,8 +254,8 @@ cudaError_t launch_device_modifier(const void* kernel, const NetDev& d, uint8_t 
 cudaError_t prepare_synapse(cudaStream_t stream);
 // diffuse.cu
 cudaError_t prepare_diffusion(const NetHost& host, cudaStream_t stream);
-void enqueue_diffusion(const NetDev& dev, const NetHost& host, float dt, unsigned long long tick,
-                       cudaStream_t stream);
+cudaError_t enqueue_diffusion(const NetDev& dev, const NetHost& host, float dt, unsigned long long tick,
+                              cudaStream_t stream);
 size_t diffusion_smem_bytes(uint32_t max_segs, uint32_t max_edges);
 
 }  // namespace bnc

@@ -112,3 +112,32 @@ def test_chunked_modifier_pass_bitexact(chunk):
         ora.run(step, DT)
         gpu.run_ticks(step, DT)
         _compare_all(ora, gpu, n_syn, "chunk %d after +%d" % (chunk, step))
+
+
+def test_trees_bitexact():
+    """Depth-10 dendritic trees (2,047 segments each) exceed one CTA's tile: each tree
+    runs on a 2-CTA cluster, its halves exchanging ghost segments through distributed
+    shared memory.  The result must still be the oracle's, bit for bit."""
+    from bioneuroncore_b200 import NetgenParams, NET_TREES
+    p = NetgenParams(family=NET_TREES, n_neurons=3, tree_depth=10, seed=8, flags=8)   # perturbed ions
+    ora, gpu, net = _pair(p)
+    assert gpu.info().n_tiles % 2 == 0
+    for step in (1, 9, 20):
+        ora.run(step, DT)
+        gpu.run_ticks(step, DT)
+        _compare_all(ora, gpu, 0, "trees after +%d" % step)
+
+
+def test_components_split_across_a_cluster_bitexact():
+    """The large set with 48-segment tiles: every 64-segment neuron spans a tile pair,
+    with synapses, stimuli and all 24 channel types."""
+    from bioneuroncore_b200 import Backend, BuildOptions, Network, NetgenParams, NET_LARGE
+    p = NetgenParams(family=NET_LARGE, n_neurons=6, n_synapses=200, seed=9)
+    ora = Oracle(Network(p))
+    gpu = Backend()
+    gpu.load_generated(p, BuildOptions(tile_segs=48))
+    assert gpu.info().n_tiles == 12
+    for step in (1, 20):
+        ora.run(step, DT)
+        gpu.run_ticks(step, DT)
+        _compare_all(ora, gpu, ora.n_syn, "split components after +%d" % step)

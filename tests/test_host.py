@@ -70,6 +70,10 @@ def test_plan_of_generated_networks():
     assert big.algo_bytes_per_tick == pytest.approx(big.tile_bytes_per_tick + big.synapse_kernel_bytes_per_tick)
     trees = plan_generated(NetgenParams(family=NET_TREES, n_neurons=2, tree_depth=9, seed=1))
     assert trees.n_segments == 2 * 1023 and trees.max_tile_segs <= 1024
+    # depth 10: 2,047-segment trees split over tile pairs (2-CTA clusters)
+    big = plan_generated(NetgenParams(family=NET_TREES, n_neurons=3, tree_depth=10, seed=1))
+    assert big.n_segments == 3 * 2047 and big.n_tiles == 6 and big.max_tile_segs == 1024
+    assert big.smem_bytes <= 227 * 1024
 
 
 def test_plan_aos_accepts_generated_network():
