@@ -128,7 +128,7 @@ __device__ __forceinline__ float xorshift32_rnd(uint32_t seed) {
     return (float)(x & 0x7FFFFFFFu) / (float)0x7FFFFFFFu;
 }
 
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 4)
 k_synapse(NetDev d, float dt, unsigned long long tick, int first_tick) {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t N = d.n_seg;
