@@ -54,6 +54,9 @@ def parse_args():
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--ens-members", type=int, default=512)
     ap.add_argument("--ens-ticks", type=int, default=64)
+    ap.add_argument("--no-trees", action="store_true")
+    ap.add_argument("--trees", type=int, default=16384)
+    ap.add_argument("--tree-ticks", type=int, default=20)
     return ap.parse_args()
 
 
@@ -259,6 +262,33 @@ def run_ensemble(a, device):
     }
 
 
+def run_trees(a, device):
+    """Electrodiffusion-heavy workload: a.trees seeded binary dendritic trees of depth 10
+    (2,047 segments each; 16,384 trees = 33.5M segments), initial ions perturbed +-5%,
+    Nernst-Planck for 7 ions with the reference's fixed 50-sweep Jacobi solves.  Each
+    tree spans a 2-CTA cluster.  Device-timed with CUDA events over a.tree_ticks ticks."""
+    from bioneuroncore_b200 import Backend, NetgenParams, NET_TREES, NETGEN_PERTURB_IONS
+    b = Backend(device)
+    t0 = time.perf_counter()
+    b.load_generated(NetgenParams(family=NET_TREES, n_neurons=a.trees, tree_depth=10, seed=a.seed,
+                                  flags=NETGEN_PERTURB_IONS))
+    setup_s = time.perf_counter() - t0
+    info = b.info()
+    b.run_ticks(max(a.warmup, 3), DT)
+    n_prof = 3
+    ms_mod, ms_diff, ms_syn = b.profile_ticks(n_prof, DT)
+    ms = b.time_ticks(a.tree_ticks, DT)
+    b.close()
+    return {
+        "workload": "%d binary dendritic trees of depth 10 (%d segments), ions perturbed +-5%%, 50-sweep Jacobi"
+                    % (a.trees, info.n_segments),
+        "metric": "segment-ticks/s", "ticks": a.tree_ticks, "value": info.n_segments * a.tree_ticks / (ms / 1000.0),
+        "ms_per_tick": ms / a.tree_ticks,
+        "kernels_ms": {"k_modifiers": ms_mod / n_prof, "k_diffusion": ms_diff / n_prof, "k_synapse": ms_syn / n_prof},
+        "cluster": "2 CTAs per tree (distributed shared memory)", "setup_s": round(setup_s, 1),
+    }
+
+
 def main():
     a = parse_args()
     if a.impl == "reference":
@@ -333,6 +363,11 @@ def main():
         b.close()   # free the large network's device memory first
         ensemble = run_ensemble(a, local_rank if world > 1 else 0)
 
+    trees = None
+    if not a.no_trees:
+        b.close()
+        trees = run_trees(a, local_rank if world > 1 else 0)
+
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         try:
@@ -353,7 +388,7 @@ def main():
                        "l2": "inputs larger than L2 (device state ~8 GB per GPU)",
                        "tiles": info.n_tiles, "phases": info.n_phases, "setup_s": round(setup_s, 1)},
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,
-            "gpu_launches": (info.n_phases + 3) * a.steps, "ensemble": ensemble,
+            "gpu_launches": (info.n_phases + 3) * a.steps, "ensemble": ensemble, "trees": trees,
         }
         print(json.dumps(line), flush=True)
     b.close()
