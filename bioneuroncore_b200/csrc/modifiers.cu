@@ -3,7 +3,7 @@
 // One tick of the reference (simulation_host.cpp:174-657) is these launches:
 //
 //  k_gather      per segment: the step-1 working record (V, ions, ATP, area, volume,
-//                I_total = 0, the GHK factors of V), the Cav2.1 gate from its static copy.
+//                I_total = 0), the Cav2.1 gate from its static copy.
 //  k_phase x P   one launch per modifier phase over the whole network.  Every segment's
 //                active modifiers sit in successive phases in slot order, at most one
 //                per phase, so a phase's items touch distinct segments and need no
@@ -42,20 +42,16 @@ k_gather(NetDev d, uint32_t s_begin, uint32_t s_end) {
     r.area = d.area[g];
     r.vol = d.vol[g];
     r.itot = 0.0;
-    GhkCache c;
-    ghk_cache_fill(c, r.V);
-    r.gV = c.Vc;
-    r.gm = (uint32_t)c.m1 | ((uint32_t)c.m2 << 8);
     r.pad = 0;
-    r.A1 = c.A1; r.e1 = c.e1; r.D1 = c.D1;
-    r.A2 = c.A2; r.e2 = c.e2; r.D2 = c.D2;
+    r.pad2 = 0.0;
     d.rec[g] = r;
     d.c21_cur[g] = d.cav21_static[g];
 }
 
 // The segment fields an item sees, loaded from the record and stored back inside the
 // model's own dispatch case: after inlining, the loads a model does not read are
-// dead, and stores of fields it leaves unchanged write back what was read.
+// dead, and stores of fields it leaves unchanged write back what was read.  The GHK
+// factors of V are computed here, per item, from the record's V.
 __device__ __forceinline__ void rec_load(DSeg& s, const SegRec* r) {
     s.V = r->V;
 #pragma unroll
@@ -63,23 +59,11 @@ __device__ __forceinline__ void rec_load(DSeg& s, const SegRec* r) {
     s.atp = r->atp;
     s.area = r->area;
     s.vol = r->vol;
-    s.gc.Vc = r->gV;
-    const uint32_t gm = r->gm;
-    s.gc.m1 = (uint8_t)(gm & 0xFFu);
-    s.gc.m2 = (uint8_t)(gm >> 8);
-    s.gc.A1 = r->A1; s.gc.e1 = r->e1; s.gc.D1 = r->D1;
-    s.gc.A2 = r->A2; s.gc.e2 = r->e2; s.gc.D2 = r->D2;
+    ghk_cache_fill(s.gc, s.V);   // dead code for models without GHK currents
 }
 
 __device__ __forceinline__ void rec_store(const DSeg& s, float v0, SegRec* r) {
-    if (s.V != v0) {   // a sodium channel clamped V to +-200 mV: refresh the GHK factors
-        GhkCache c;
-        ghk_cache_fill(c, s.V);
-        r->gV = c.Vc;
-        r->gm = (uint32_t)c.m1 | ((uint32_t)c.m2 << 8);
-        r->A1 = c.A1; r->e1 = c.e1; r->D1 = c.D1;
-        r->A2 = c.A2; r->e2 = c.e2; r->D2 = c.D2;
-    }
+    (void)v0;
     r->V = s.V;
 #pragma unroll
     for (int k = 0; k < 7; k++) { r->in[k] = s.in[k]; r->out[k] = s.out[k]; }

@@ -30,23 +30,22 @@ enum : uint32_t {
 enum : uint8_t { SF_MYELIN = 1u, SF_NMDA = 2u };
 
 // The state a modifier reads and writes, gathered per segment for step 1 so that an
-// item touches one or two contiguous 32-byte runs instead of many scattered words:
-// V and the 7 intra ions | 7 extra ions and ATP | area, the V of the GHK factors and
-// their branch codes | volume and I_total | the GHK factors (144 bytes, 16-aligned).
+// item touches a few contiguous 32-byte runs instead of many scattered words:
+// V and the 7 intra ions | 7 extra ions and ATP | area | volume and I_total
+// (96 bytes, 16-aligned).  The GHK factors of V are recomputed per item: cheaper
+// than moving them through HBM in every phase.
 struct __align__(16) SegRec {
     float V;
     float in[7];
     float out[7];
     float atp;
     float area;
-    float gV;
-    uint32_t gm;      // GHK branch codes: m1 | m2 << 8
     uint32_t pad;
     double vol;
     double itot;
-    double A1, e1, D1, A2, e2, D2;
+    double pad2;
 };
-static_assert(sizeof(SegRec) == 144, "SegRec layout");
+static_assert(sizeof(SegRec) == 96, "SegRec layout");
 
 // Plain-old-data descriptor passed by value to the kernels.
 struct NetDev {
@@ -171,7 +170,7 @@ struct BuildOptions {
     uint32_t phase_cap = 0;
     // Segments per chunk of the modifier pass (0: the whole network in one chunk).
     // All phases of a chunk run before the next chunk, so a chunk's step-1 records
-    // (144 bytes per segment) can stay in L2 between phases.
+    // (96 bytes per segment) can stay in L2 between phases.
     uint32_t chunk_segs = BNC_DEFAULT_CHUNK_SEGS;
 };
 

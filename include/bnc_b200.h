@@ -269,7 +269,7 @@ int bnc_run_ticks_graph(void* sim, uint32_t n_ticks, float dt);
  *                        longest modifier list + 4), else phases follow slot order;
  *   chunk_segs           the modifier pass runs all its phases on chunks of this
  *                        many consecutive segments in turn, so a chunk's working
- *                        records (144 bytes per segment) can stay in L2 between
+ *                        records (96 bytes per segment) can stay in L2 between
  *                        phases (0: BNC_DEFAULT_CHUNK_SEGS, one chunk).  On B200
  *                        the extra launches cost more than L2 residency saves
  *                        (6.4M segments: 9.4 ms per tick in one chunk, 9.5 ms in

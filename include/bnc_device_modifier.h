@@ -32,7 +32,7 @@
 #ifndef BNC_DEVICE_MODIFIER_H
 #define BNC_DEVICE_MODIFIER_H
 
-/* Per-segment working state of step 1 (144 bytes). */
+/* Per-segment working state of step 1 (96 bytes). */
 typedef struct
 #ifdef __CUDACC__
 __align__(16)
@@ -43,12 +43,10 @@ __align__(16)
     float out[7];         /* extracellular, same order */
     float atp;            /* ATP level */
     float area;           /* membrane area, um^2 (the reference's state[7]) */
-    float ghk_V;          /* library-private: GHK factors below belong to this V */
-    unsigned int ghk_codes;   /* library-private */
     unsigned int reserved;
     double vol;           /* volume, um^3 */
     double itot;          /* I_total of step 1 so far, pA: add the modifier's current */
-    double ghk[6];        /* library-private */
+    double reserved2;
 } BncSegmentState;
 
 typedef struct {
