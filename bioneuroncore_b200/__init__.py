@@ -41,7 +41,10 @@ NEW_SYMBOLS = ["bnc_netgen_aos", "bnc_netgen_free", "bnc_last_error", "bnc_load_
                "bnc_load_ensemble_aos", "bnc_ensemble_member", "bnc_plan_ensemble_generated", "bnc_ensemble_params",
                "bnc_run_ticks_graph", "bnc_load_ensemble_tuned", "bnc_time_ticks_graph", "bnc_load_generated_opts",
                "bnc_plan_generated_opts", "biocore_gpu_register_device_modifier", "bnc_register_device_modifier",
-               "bnc_device_modifier_registered"]
+               "bnc_device_modifier_registered", "bnc_adjoint_create", "bnc_adjoint_destroy", "bnc_adjoint_info",
+               "bnc_adjoint_soma", "bnc_adjoint_record", "bnc_adjoint_release_count", "bnc_adjoint_set_params",
+               "bnc_adjoint_get_params", "bnc_adjoint_set_target", "bnc_adjoint_forward", "bnc_adjoint_backward",
+               "bnc_adjoint_timings"]
 
 
 class NetInfo(C.Structure):
@@ -148,6 +151,13 @@ def load_library(path=LIB_PATH):
         "biocore_gpu_register_device_modifier": ([C.c_uint8, C.c_char_p, C.c_char_p], i32),
         "bnc_register_device_modifier": ([C.c_uint8, C.c_char_p, C.c_char_p], i32),
         "bnc_device_modifier_registered": ([C.c_uint8], i32),
+        "bnc_adjoint_create": ([vp, vp], vp), "bnc_adjoint_destroy": ([vp], None),
+        "bnc_adjoint_info": ([vp, vp], i32), "bnc_adjoint_soma": ([vp, vp, u32], i32),
+        "bnc_adjoint_record": ([vp, vp], i32), "bnc_adjoint_release_count": ([vp, vp], i32),
+        "bnc_adjoint_set_params": ([vp, u32, vp, vp, vp, vp], i32),
+        "bnc_adjoint_get_params": ([vp, u32, vp, vp, vp, vp], i32),
+        "bnc_adjoint_set_target": ([vp, vp], i32), "bnc_adjoint_forward": ([vp, vp, vp], i32),
+        "bnc_adjoint_backward": ([vp, vp, vp, vp, vp], i32), "bnc_adjoint_timings": ([vp, vp, vp], i32),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -337,7 +347,106 @@ class Backend:
         _check(self.lib.bnc_save_bion(self.h, path.encode()), "bnc_save_bion")
 
 
-__all__ = ["Backend", "Network", "NetgenParams", "BionData", "BackendError", "load_library", "last_error",
+__all__ = ["Backend", "Network", "Adjoint", "AdjointConfig", "AdjointInfo", "NetgenParams", "BionData", "BackendError", "load_library", "last_error",
            "NET_SMALL", "NET_LARGE", "NET_TREES", "NET_ENSEMBLE_MEMBER", "NET_ADJOINT", "NETGEN_NO_SYNAPSES",
            "NETGEN_NO_CONNECTIONS", "NETGEN_NO_STIMULI", "NETGEN_PERTURB_IONS", "NETGEN_SYNAPSE_EXTRAS", "SEG_FIELDS", "SYN_FIELDS",
            "DROPIN_SYMBOLS", "NEW_SYMBOLS", "EnsembleMember", "Tuning", "BuildOptions", "register_device_modifier", "ensemble_params", "plan_ensemble", "plan_generated"]
+
+
+class AdjointConfig(C.Structure):
+    _fields_ = [("n_sets", C.c_uint32), ("ticks", C.c_uint32), ("checkpoint_every", C.c_uint32),
+                ("sample_every", C.c_uint32), ("dt", C.c_float)]
+
+
+class AdjointInfo(C.Structure):
+    _fields_ = [(n, C.c_uint32) for n in ("n_neurons", "n_segments", "n_synapses", "n_samples", "n_sets", "ticks",
+                                          "checkpoint_every", "threads", "smem_forward", "smem_backward")] + \
+               [(n, C.c_uint64) for n in ("checkpoint_bytes", "window_bytes", "scratch_bytes")]
+
+
+def _fptr(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+class Adjoint:
+    """Gradients of a somatic voltage-trace loss w.r.t. per-segment gNa/gK/gleak and
+    per-synapse weights, for `n_sets` parameter sets at once (bnc_adjoint_*).
+
+    Built from the network loaded in `backend` at its current tick; `record()` then runs
+    the plain tick for `ticks` ticks on that backend and keeps the release log that the
+    forward and backward passes replay (releases are pathwise fixed)."""
+
+    def __init__(self, backend, n_sets, ticks, dt, checkpoint_every=256, sample_every=1):
+        lib = load_library()
+        self.cfg = AdjointConfig(n_sets, ticks, checkpoint_every, sample_every, dt)
+        h = lib.bnc_adjoint_create(backend.h, C.byref(self.cfg))
+        if not h:
+            raise BackendError("bnc_adjoint_create failed: %s" % last_error())
+        self.h = h
+        self.backend = backend
+        inf = AdjointInfo()
+        _check(lib.bnc_adjoint_info(h, C.byref(inf)), "bnc_adjoint_info")
+        self.info = inf
+        import numpy as np
+        self.soma = np.zeros(inf.n_neurons, np.uint32)
+        _check(lib.bnc_adjoint_soma(h, _fptr(self.soma), inf.n_neurons), "bnc_adjoint_soma")
+
+    def close(self):
+        if getattr(self, "h", None):
+            load_library().bnc_adjoint_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def record(self):
+        _check(load_library().bnc_adjoint_record(self.h, self.backend.h), "bnc_adjoint_record")
+
+    def release_count(self):
+        n = C.c_uint64()
+        _check(load_library().bnc_adjoint_release_count(self.h, C.byref(n)), "bnc_adjoint_release_count")
+        return n.value
+
+    def set_params(self, p, gNa=None, gK=None, gleak=None, w=None):
+        import numpy as np
+        arr = [None if a is None else np.ascontiguousarray(a, np.float32) for a in (gNa, gK, gleak, w)]
+        _check(load_library().bnc_adjoint_set_params(self.h, p, *[_fptr(a) for a in arr]), "bnc_adjoint_set_params")
+
+    def get_params(self, p):
+        import numpy as np
+        i = self.info
+        out = [np.zeros(i.n_segments, np.float32) for _ in range(3)] + [np.zeros(max(i.n_synapses, 1), np.float32)]
+        _check(load_library().bnc_adjoint_get_params(self.h, p, *[_fptr(a) for a in out]), "bnc_adjoint_get_params")
+        out[3] = out[3][:i.n_synapses]
+        return out
+
+    def set_target(self, target):
+        import numpy as np
+        t = np.ascontiguousarray(target, np.float32).reshape(self.info.n_samples, self.info.n_neurons)
+        _check(load_library().bnc_adjoint_set_target(self.h, _fptr(t)), "bnc_adjoint_set_target")
+
+    def forward(self, trace=False):
+        """Returns (loss[n_sets], trace[n_sets][n_samples][n_neurons] or None)."""
+        import numpy as np
+        i = self.info
+        loss = np.zeros(i.n_sets, np.float64)
+        tr = np.zeros((i.n_sets, i.n_samples, i.n_neurons), np.float32) if trace else None
+        _check(load_library().bnc_adjoint_forward(self.h, _fptr(loss), _fptr(tr)), "bnc_adjoint_forward")
+        return loss, tr
+
+    def backward(self):
+        """Returns (g_gNa, g_gK, g_gleak) as [n_sets][n_segments] and g_w as [n_sets][n_synapses]."""
+        import numpy as np
+        i = self.info
+        g = [np.zeros((i.n_sets, i.n_segments), np.float32) for _ in range(3)]
+        gw = np.zeros((i.n_sets, max(i.n_synapses, 1)), np.float32)
+        _check(load_library().bnc_adjoint_backward(self.h, *[_fptr(a) for a in g], _fptr(gw)), "bnc_adjoint_backward")
+        return g[0], g[1], g[2], gw[:, :i.n_synapses]
+
+    def timings(self):
+        f, b = C.c_float(), C.c_float()
+        _check(load_library().bnc_adjoint_timings(self.h, C.byref(f), C.byref(b)), "bnc_adjoint_timings")
+        return f.value, b.value

@@ -23,7 +23,7 @@ ORACLE_DIR = os.path.join(ROOT, "oracle")
 ORACLE_LIB = os.path.join(ORACLE_DIR, "liboracle.so")
 REFERENCE = "/root/reference"
 
-CU_SOURCES = ["modifiers.cu", "diffuse.cu", "synapse.cu", "backend.cu", "plugins.cu"]
+CU_SOURCES = ["modifiers.cu", "diffuse.cu", "synapse.cu", "backend.cu", "plugins.cu", "adjoint.cu"]
 CPP_SOURCES = ["netgen.cpp", "capi_host.cpp", "builder.cpp"]
 HEADERS = sorted(f for f in os.listdir(CSRC) if f.endswith((".h", ".cuh")))
 
@@ -99,12 +99,20 @@ def build_library(verbose=False, ptxas_info=False):
     return LIB
 
 
+TANGENT_LIB = os.path.join(ORACLE_DIR, "libbo_tangent.so")
+
+
 def build_oracle():
-    """Compiles the CPU oracle (test infrastructure) with contraction disabled."""
+    """Compiles the CPU oracle (test infrastructure) with contraction disabled: the FP32
+    tick restatement and the FP64 forward-mode replay that checks the adjoint."""
     srcs = [os.path.join(ORACLE_DIR, f) for f in ("bnc_oracle.c", "bo_math.h", "bo_physics.h", "bo_modifiers.h")]
-    if _stale(ORACLE_LIB, srcs + [os.path.join(ROOT, "include", "bnc_abi.h")]):
+    abi = os.path.join(ROOT, "include", "bnc_abi.h")
+    if _stale(ORACLE_LIB, srcs + [abi]):
         _run(["gcc", "-std=c11", "-O2", "-ffp-contract=off", "-fPIC", "-shared", "-o", ORACLE_LIB,
               os.path.join(ORACLE_DIR, "bnc_oracle.c"), "-lm"])
+    tsrc = os.path.join(ORACLE_DIR, "bo_tangent.cpp")
+    if _stale(TANGENT_LIB, [tsrc, abi]):
+        _run(["g++", "-std=c++17", "-O2", "-ffp-contract=off", "-fPIC", "-shared", "-o", TANGENT_LIB, tsrc, "-lm"])
     return ORACLE_LIB
 
 
@@ -120,7 +128,7 @@ def ensure_built():
     """Builds the product library and the oracle only when their files are missing."""
     if not os.path.exists(LIB):
         build_library()
-    if not os.path.exists(ORACLE_LIB):
+    if not os.path.exists(ORACLE_LIB) or not os.path.exists(TANGENT_LIB):
         build_oracle()
 
 

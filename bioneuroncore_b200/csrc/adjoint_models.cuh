@@ -1,0 +1,446 @@
+// adjoint_models.cuh -- local derivatives of the pointwise pieces of a tick, for the
+// reverse tick in adjoint.cu.
+//
+// Each function restates one model of physics.cuh / synapse.cu over a forward-mode
+// dual number (value + N partial derivatives, double precision): evaluated once with
+// every input seeded, it yields the model's local Jacobian at the forward point, and
+// the reverse tick applies its transpose.  The values are not used for the forward
+// trajectory (that keeps the bit-exact device functions); only the derivatives are.
+// Float roundings of the forward code are identities here, clamps are subgradient
+// masks (derivative 0 where the clamp is active).
+#pragma once
+#include <cstdint>
+#include <cmath>
+
+namespace bnc {
+namespace adj {
+
+template <int N>
+struct Dual {
+    double v;
+    double d[N];
+    __device__ __forceinline__ Dual() : v(0.0) {
+#pragma unroll
+        for (int k = 0; k < N; k++) d[k] = 0.0;
+    }
+    __device__ __forceinline__ Dual(double x) : v(x) {   // NOLINT: constants promote implicitly
+#pragma unroll
+        for (int k = 0; k < N; k++) d[k] = 0.0;
+    }
+    __device__ __forceinline__ static Dual seed(double x, int k) {
+        Dual r(x);
+        r.d[k] = 1.0;
+        return r;
+    }
+};
+
+#define BNC_DUAL_OP(OP, EXPR_V, EXPR_D)                                                        \
+    template <int N>                                                                           \
+    __device__ __forceinline__ Dual<N> operator OP(const Dual<N>& a, const Dual<N>& b) {       \
+        Dual<N> r;                                                                             \
+        r.v = EXPR_V;                                                                          \
+        _Pragma("unroll") for (int k = 0; k < N; k++) r.d[k] = EXPR_D;                         \
+        return r;                                                                              \
+    }
+BNC_DUAL_OP(+, a.v + b.v, a.d[k] + b.d[k])
+BNC_DUAL_OP(-, a.v - b.v, a.d[k] - b.d[k])
+BNC_DUAL_OP(*, a.v * b.v, a.d[k] * b.v + a.v * b.d[k])
+#undef BNC_DUAL_OP
+template <int N>
+__device__ __forceinline__ Dual<N> operator/(const Dual<N>& a, const Dual<N>& b) {
+    Dual<N> r;
+    r.v = a.v / b.v;
+    const double ib = 1.0 / b.v;
+#pragma unroll
+    for (int k = 0; k < N; k++) r.d[k] = (a.d[k] - r.v * b.d[k]) * ib;
+    return r;
+}
+template <int N>
+__device__ __forceinline__ Dual<N> operator-(const Dual<N>& a) {
+    Dual<N> r;
+    r.v = -a.v;
+#pragma unroll
+    for (int k = 0; k < N; k++) r.d[k] = -a.d[k];
+    return r;
+}
+template <int N> __device__ __forceinline__ Dual<N> operator+(const Dual<N>& a, double b) { return a + Dual<N>(b); }
+template <int N> __device__ __forceinline__ Dual<N> operator+(double a, const Dual<N>& b) { return Dual<N>(a) + b; }
+template <int N> __device__ __forceinline__ Dual<N> operator-(const Dual<N>& a, double b) { return a - Dual<N>(b); }
+template <int N> __device__ __forceinline__ Dual<N> operator-(double a, const Dual<N>& b) { return Dual<N>(a) - b; }
+template <int N>
+__device__ __forceinline__ Dual<N> operator*(const Dual<N>& a, double b) {
+    Dual<N> r;
+    r.v = a.v * b;
+#pragma unroll
+    for (int k = 0; k < N; k++) r.d[k] = a.d[k] * b;
+    return r;
+}
+template <int N> __device__ __forceinline__ Dual<N> operator*(double a, const Dual<N>& b) { return b * a; }
+template <int N> __device__ __forceinline__ Dual<N> operator/(const Dual<N>& a, double b) { return a * (1.0 / b); }
+template <int N> __device__ __forceinline__ Dual<N> operator/(double a, const Dual<N>& b) { return Dual<N>(a) / b; }
+template <int N>
+__device__ __forceinline__ Dual<N> dexp(const Dual<N>& a) {
+    Dual<N> r;
+    r.v = exp(a.v);
+#pragma unroll
+    for (int k = 0; k < N; k++) r.d[k] = r.v * a.d[k];
+    return r;
+}
+template <int N>
+__device__ __forceinline__ Dual<N> dconst(const Dual<N>& a) { return Dual<N>(a.v); }   // a clamp in effect
+
+// clamp(x, lo, hi) with the derivative masked where the clamp is active
+template <int N>
+__device__ __forceinline__ Dual<N> dclamp(const Dual<N>& x, double lo, double hi) {
+    if (x.v < lo) return Dual<N>(lo);
+    if (x.v > hi) return Dual<N>(hi);
+    return x;
+}
+template <int N>
+__device__ __forceinline__ Dual<N> dfloor(const Dual<N>& x, double lo) { return (x.v < lo) ? Dual<N>(lo) : x; }
+
+/* ---- constants: the same literals as physics.cuh ---- */
+constexpr double kF = 96485.0;
+constexpr double kR = (double)8.314f;
+constexpr double kT = (double)310.15f;
+constexpr double kEVR = (double)(0.2f / (1.0f - 0.2f));
+
+// run_tick_common.h:274-312 (GHK flux, monovalent cation / anion) as a function of
+// (V, c_in, c_out); branch choice by value, as the forward code takes it.
+template <int N>
+__device__ __forceinline__ Dual<N> ghk_mono(const Dual<N>& V, const Dual<N>& cin, const Dual<N>& cout) {
+    const double kk = kF / (kR * kT);
+    Dual<N> Vn = V * (kF * 0.001 / (kR * kT));
+    if (fabs(Vn.v) < 1e-6) return (cin - cout) * kF;
+    Dual<N> A = V * (kk * kF * 0.001);
+    if (Vn.v > 20.0) return A * cin;
+    if (Vn.v < -20.0) return A * cout;
+    Dual<N> e = dexp(-Vn);
+    return A * (cin - cout * e) / (1.0 - e);
+}
+template <int N>
+__device__ __forceinline__ Dual<N> ghk_anion(const Dual<N>& V, const Dual<N>& cin, const Dual<N>& cout) {
+    return ghk_mono(V, cout, cin);
+}
+
+// modifier_helpers.h:132-135
+template <int N>
+__device__ __forceinline__ Dual<N> vtrap(const Dual<N>& x, double y) {
+    if (fabs(x.v / y) < 1e-6) return y * (1.0 - x / (2.0 * y));
+    return x / (1.0 - dexp(-x / y));
+}
+
+// Nav1.6 / Nav1.2 gating (modifier_helpers.h:145-215)
+struct NavK { double am, bm, ah, bh, hh; };
+__device__ __forceinline__ NavK nav_consts(int is12) {
+    return is12 ? NavK{(double)23.0f, (double)23.0f, (double)41.5f, (double)66.5f, (double)63.5f}
+                : NavK{(double)43.0f, (double)43.0f, (double)50.0f, (double)75.0f, (double)72.0f};
+}
+
+// Local Jacobians of the modifier items.  Inputs (seed order):
+//   0 V, 1 gate0, 2 gate1, 3 c_in, 4 c_out, 5 density
+// Outputs: V' (the Nav clamp), gate0', gate1', c_in', c_out', I (the returned current).
+struct ItemJac {
+    double dV[6], dg0[6], dg1[6], dcin[6], dcout[6], dI[6];
+};
+
+template <int N>
+__device__ __forceinline__ void store_row(double* row, const Dual<N>& x) {
+#pragma unroll
+    for (int k = 0; k < 6; k++) row[k] = (k < N) ? x.d[k] : 0.0;
+}
+
+// hh_biological.cpp:193-277 (dp_nav_current): c = Na
+__device__ __forceinline__ void jac_nav(ItemJac& J, float V0, float m0, float h0, float cin0, float cout0, float den0,
+                                        float area, double vol, float dt, int is12, float ttx) {
+    typedef Dual<6> D;
+    D V = D::seed(V0, 0), m = D::seed(m0, 1), h = D::seed(h0, 2);
+    D cin = D::seed(cin0, 3), cout = D::seed(cout0, 4), den = D::seed(den0, 5);
+    V = dclamp(V, -200.0, 200.0);
+    const NavK c = nav_consts(is12);
+    D am = (double)0.182f * vtrap(V + c.am, 6.0), bm = (double)0.124f * vtrap(-(V + c.bm), 6.0);
+    D ah = (double)0.024f * vtrap(V + c.ah, 5.0), bh = (double)0.0091f * vtrap(-(V + c.bh), 5.0);
+    D minf = am / (am + bm), mtau = 1.0 / (am + bm);
+    D hinf = 1.0 / (1.0 + dexp((V + c.hh) / (double)6.2f)), htau = 1.0 / (ah + bh);
+    D mv = dclamp(minf + (m - minf) * dexp(-(double)dt / mtau), 0.0, 1.0);
+    D hv = dclamp(hinf + (h - hinf) * dexp(-(double)dt / htau), 0.0, 1.0);
+    D open = mv * mv * mv * hv;
+    double ttxd = ttx > 0.0f ? (double)ttx : 0.0;
+    open = open / (1.0 + ttxd / (is12 ? 10.0 : 5.0));
+    if (open.v < 0.0) open = D(0.0);
+    const double gamma = is12 ? (double)20.8f : (double)20.7f;
+    const double P = gamma * 1e-12 * (kR * kT) / (kF * kF * (double)55.964f);
+    D flux = ghk_mono(V, cin, cout);
+    D I_Na = P * flux * (den * (double)area) * open * 1e12;
+    const double cpv = kF * vol / 1000.0;
+    D cin1 = dfloor(cin - (I_Na * (double)dt) / cpv, 1e-9);
+    D cout1 = dfloor(cout + (I_Na * (double)dt) / (cpv * kEVR), 1e-9);
+    store_row(J.dV, V); store_row(J.dg0, mv); store_row(J.dg1, hv);
+    store_row(J.dcin, cin1); store_row(J.dcout, cout1); store_row(J.dI, -I_Na);
+}
+
+// hh_biological.cpp:2763-2797 (dp_kvdr_current): gate0 = n, c = K
+__device__ __forceinline__ void jac_kvdr(ItemJac& J, float V0, float n0, float cin0, float cout0, float den0,
+                                         float area, double vol, float dt, const float* st) {
+    typedef Dual<6> D;
+    D V = D::seed(V0, 0), n = D::seed(n0, 1);
+    D cin = D::seed(cin0, 3), cout = D::seed(cout0, 4), den = D::seed(den0, 5);
+    const double V_half = (st[1] != 0.0f) ? (double)st[1] : -30.0;
+    const double k = (st[2] > 0.0f) ? (double)st[2] : 6.0;
+    D tau;
+    if (st[4] > 0.0f) tau = D((double)st[4]);
+    else {
+        tau = (double)14.6f * dexp(-(V - (double)(float)V_half) / (double)30.1f);
+        tau = dclamp(tau, (double)0.3f, 200.0);
+    }
+    D minf = 1.0 / (1.0 + dexp(-(V - V_half) / (k + (double)1e-6f)));
+    D nv = dclamp(n + (minf - n) * (double)dt / (tau + (double)1e-6f), 0.0, 1.0);
+    const double P = 12.0 * 1e-12 * (kR * kT) / (kF * kF * (double)40.514f);
+    D I_K = P * ghk_mono(V, cin, cout) * (den * (double)area) * nv * 1e12;
+    const double cpmv = (double)(float)(kF * vol / 1000.0);
+    D cin1 = dfloor(cin - (I_K * (double)dt) / cpmv, 1e-9);
+    D cout1 = dfloor(cout + (I_K * (double)dt) / (cpmv * kEVR), 1e-9);
+    store_row(J.dV, V); store_row(J.dg0, nv); store_row(J.dg1, D(0.0));
+    store_row(J.dcin, cin1); store_row(J.dcout, cout1); store_row(J.dI, -I_K);
+}
+
+// hh_biological.cpp:3063-3084 (dp_k2p_current): c = K, no gates
+__device__ __forceinline__ void jac_k2p(ItemJac& J, float V0, float cin0, float cout0, float den0,
+                                        float area, double vol, float dt, const float* st) {
+    typedef Dual<6> D;
+    D V = D::seed(V0, 0);
+    D cin = D::seed(cin0, 3), cout = D::seed(cout0, 4), den = D::seed(den0, 5);
+    const double gamma = (st[0] > 0.0f) ? (double)st[0] : 100.0;
+    const double Po = (st[1] > 0.0f) ? (double)st[1] : (double)0.012f;
+    const double P = (double)(float)gamma * 1e-12 * (kR * kT) / (kF * kF * (double)40.514f);
+    D I_K = P * ghk_mono(V, cin, cout) * (den * (double)area) * Po * 1e12;
+    const double cpv = kF * vol / 1000.0;
+    D cin1 = cin - (I_K * (double)dt) / cpv;   // dp_k_flux clamps the extracellular side only
+    D cout1 = dfloor(cout + (I_K * (double)dt) / (cpv * kEVR), 1e-9);
+    store_row(J.dV, V); store_row(J.dg0, D(0.0)); store_row(J.dg1, D(0.0));
+    store_row(J.dcin, cin1); store_row(J.dcout, cout1); store_row(J.dI, -I_K);
+}
+
+// Ionotropic receptor (modifier_helpers.h:1213-1278) with its gates given.  Inputs:
+//   0 V, 1 in[0], 2 in[1], 3 in[3], 4 out[0], 5 out[1], 6 out[3], 7 weight scale
+// Outputs: in[0]', in[1]', in[3]', I.
+struct RecJac {
+    double din0[8], din1[8], din3[8], dI[8];
+    double v0, v1, v3;   // the updated ions (values)
+};
+__device__ __forceinline__ void jac_receptor(RecJac& J, int anion, double P_a, double P_b, float V0,
+                                             const float* in, const float* out, float w0, float den,
+                                             float area, float open, double vol, float dt) {
+    typedef Dual<8> D;
+    D V = D::seed(V0, 0), i0 = D::seed(in[0], 1), i1 = D::seed(in[1], 2), i3 = D::seed(in[3], 3);
+    D o0 = D::seed(out[0], 4), o1 = D::seed(out[1], 5), o3 = D::seed(out[3], 6), w = D::seed(w0, 7);
+    const double cpm = kF * vol / 1000.0;
+    const double Nk = (double)den * (double)area * (double)open;
+    D n0 = i0, n1 = i1, n3 = i3, I;
+    if (anion) {
+        D I_Cl = P_a * ghk_anion(V, i3, o3) * Nk * w * 1e12;
+        n3 = dfloor(i3 + (I_Cl * (double)dt) / cpm, 1e-9);
+        I = -I_Cl;
+    } else {
+        D I_Na = P_a * ghk_mono(V, i0, o0) * Nk * w * 1e12;
+        D I_K = P_b * ghk_mono(V, i1, o1) * Nk * w * 1e12;
+        n0 = dfloor(i0 - (I_Na * (double)dt) / cpm, 1e-9);
+        n1 = dfloor(i1 - (I_K * (double)dt) / cpm, 1e-9);
+        I = -(I_Na + I_K);
+    }
+#pragma unroll
+    for (int k = 0; k < 8; k++) { J.din0[k] = n0.d[k]; J.din1[k] = n1.d[k]; J.din3[k] = n3.d[k]; J.dI[k] = I.d[k]; }
+    J.v0 = n0.v; J.v1 = n1.v; J.v3 = n3.v;
+}
+
+// ---- vector-Jacobian products of the items and receptors ----
+// The reverse tick needs lambda^T J, not J: these contract on the fly.  Quantities that
+// depend on V alone (gating rates, the GHK prefactor and exponential) carry a one-
+// component dual number; the rest of the chain rule is written out.
+
+// GHK flux (run_tick_common.h:274-312) and its partials in V, c_in, c_out.
+struct GhkD { double F, dV, dci, dco; };
+__device__ __forceinline__ GhkD ghk_mono_d(double Vd, double ci, double co) {
+    const double kk = kF / (kR * kT);
+    const double c1 = kF * 0.001 / (kR * kT);
+    const double Vn = Vd * c1;
+    GhkD r;
+    if (fabs(Vn) < 1e-6) { r.F = kF * (ci - co); r.dV = 0.0; r.dci = kF; r.dco = -kF; return r; }
+    const double A = Vd * (kk * kF * 0.001), dA = kk * kF * 0.001;
+    if (Vn > 20.0) { r.F = A * ci; r.dV = dA * ci; r.dci = A; r.dco = 0.0; return r; }
+    if (Vn < -20.0) { r.F = A * co; r.dV = dA * co; r.dci = 0.0; r.dco = A; return r; }
+    const double e = exp(-Vn), de = -e * c1;
+    const double D = 1.0 - e, Nn = ci - co * e;
+    r.F = A * Nn / D;
+    r.dV = dA * Nn / D + A * de * (ci - co) / (D * D);
+    r.dci = A / D;
+    r.dco = -A * e / D;
+    return r;
+}
+
+// lo = adjoints of (V', gate0', gate1', c_in', c_out', returned I); lx = adjoints of
+// (V, gate0, gate1, c_in, c_out, density).
+__device__ __forceinline__ void vjp_nav(const double* lo, double* lx, float V0, float m0, float h0, float cin,
+                                        float cout, float den, float area, double vol, float dt, int is12, float ttx) {
+    typedef Dual<1> D;
+    const bool mV = (double)V0 >= -200.0 && (double)V0 <= 200.0;
+    const double Vc = mV ? (double)V0 : ((double)V0 < -200.0 ? -200.0 : 200.0);
+    const D V = D::seed(Vc, 0);
+    const NavK c = nav_consts(is12);
+    const D am = (double)0.182f * vtrap(V + c.am, 6.0), bm = (double)0.124f * vtrap(-(V + c.bm), 6.0);
+    const D ah = (double)0.024f * vtrap(V + c.ah, 5.0), bh = (double)0.0091f * vtrap(-(V + c.bh), 5.0);
+    const D minf = am / (am + bm), mtau = 1.0 / (am + bm);
+    const D hinf = 1.0 / (1.0 + dexp((V + c.hh) / (double)6.2f)), htau = 1.0 / (ah + bh);
+    const D Em = dexp(-(double)dt / mtau), Eh = dexp(-(double)dt / htau);
+    const double mu_ = minf.v + ((double)m0 - minf.v) * Em.v, hu_ = hinf.v + ((double)h0 - hinf.v) * Eh.v;
+    const bool mm = mu_ >= 0.0 && mu_ <= 1.0, mh = hu_ >= 0.0 && hu_ <= 1.0;
+    const double mv = mm ? mu_ : (mu_ < 0.0 ? 0.0 : 1.0), hv = mh ? hu_ : (hu_ < 0.0 ? 0.0 : 1.0);
+    const double dm_dV = mm ? minf.d[0] * (1.0 - Em.v) + ((double)m0 - minf.v) * Em.d[0] : 0.0;
+    const double dh_dV = mh ? hinf.d[0] * (1.0 - Eh.v) + ((double)h0 - hinf.v) * Eh.d[0] : 0.0;
+    const double dm_dm = mm ? Em.v : 0.0, dh_dh = mh ? Eh.v : 0.0;
+    const double cdiv = 1.0 + (ttx > 0.0f ? (double)ttx : 0.0) / (is12 ? 10.0 : 5.0);
+    const double open = mv * mv * mv * hv / cdiv;
+    const double do_dm = 3.0 * mv * mv * hv / cdiv, do_dh = mv * mv * mv / cdiv;
+    const double gamma = is12 ? (double)20.8f : (double)20.7f;
+    const double Kc = gamma * 1e-12 * (kR * kT) / (kF * kF * (double)55.964f) * 1e12 * (double)area;
+    const GhkD G = ghk_mono_d(Vc, cin, cout);
+    const double I = Kc * G.F * (double)den * open;
+    const double cpv = kF * vol / 1000.0;
+    const bool mci = (double)cin - I * (double)dt / cpv >= 1e-9;
+    const bool mco = (double)cout + I * (double)dt / (cpv * kEVR) >= 1e-9;
+    const double lI = -lo[5] - (mci ? lo[3] * (double)dt / cpv : 0.0) + (mco ? lo[4] * (double)dt / (cpv * kEVR) : 0.0);
+    const double lopen = lI * Kc * G.F * (double)den;
+    const double lF = lI * Kc * (double)den * open;
+    const double lmv = lo[1] + lopen * do_dm, lhv = lo[2] + lopen * do_dh;
+    const double lVc = lo[0] + lF * G.dV + lmv * dm_dV + lhv * dh_dV;
+    lx[0] = mV ? lVc : 0.0;
+    lx[1] = lmv * dm_dm;
+    lx[2] = lhv * dh_dh;
+    lx[3] = (mci ? lo[3] : 0.0) + lF * G.dci;
+    lx[4] = (mco ? lo[4] : 0.0) + lF * G.dco;
+    lx[5] = lI * Kc * G.F * open;
+}
+
+__device__ __forceinline__ void vjp_kvdr(const double* lo, double* lx, float V0, float n0, float cin, float cout,
+                                         float den, float area, double vol, float dt, const float* st) {
+    typedef Dual<1> D;
+    const D V = D::seed((double)V0, 0);
+    const double V_half = (st[1] != 0.0f) ? (double)st[1] : -30.0;
+    const double k = (st[2] > 0.0f) ? (double)st[2] : 6.0;
+    D tau;
+    if (st[4] > 0.0f) tau = D((double)st[4]);
+    else tau = dclamp((double)14.6f * dexp(-(V - (double)(float)V_half) / (double)30.1f), (double)0.3f, 200.0);
+    const D minf = 1.0 / (1.0 + dexp(-(V - V_half) / (k + (double)1e-6f)));
+    const double tt = tau.v + (double)1e-6f;
+    const double nu = (double)n0 + (minf.v - (double)n0) * (double)dt / tt;
+    const bool mn = nu >= 0.0 && nu <= 1.0;
+    const double nv = mn ? nu : (nu < 0.0 ? 0.0 : 1.0);
+    const double dn_dV = mn ? (minf.d[0] * (double)dt / tt - (minf.v - (double)n0) * (double)dt * tau.d[0] / (tt * tt)) : 0.0;
+    const double dn_dn = mn ? 1.0 - (double)dt / tt : 0.0;
+    const double Kc = 12.0 * 1e-12 * (kR * kT) / (kF * kF * (double)40.514f) * 1e12 * (double)area;
+    const GhkD G = ghk_mono_d((double)V0, cin, cout);
+    const double I = Kc * G.F * (double)den * nv;
+    const double cpmv = (double)(float)(kF * vol / 1000.0);
+    const bool mci = (double)cin - I * (double)dt / cpmv >= 1e-9;
+    const bool mco = (double)cout + I * (double)dt / (cpmv * kEVR) >= 1e-9;
+    const double lI = -lo[5] - (mci ? lo[3] * (double)dt / cpmv : 0.0) + (mco ? lo[4] * (double)dt / (cpmv * kEVR) : 0.0);
+    const double lF = lI * Kc * (double)den * nv;
+    const double lnv = lo[1] + lI * Kc * G.F * (double)den;
+    lx[0] = lo[0] + lF * G.dV + lnv * dn_dV;
+    lx[1] = lnv * dn_dn;
+    lx[2] = 0.0;
+    lx[3] = (mci ? lo[3] : 0.0) + lF * G.dci;
+    lx[4] = (mco ? lo[4] : 0.0) + lF * G.dco;
+    lx[5] = lI * Kc * G.F * nv;
+}
+
+__device__ __forceinline__ void vjp_k2p(const double* lo, double* lx, float V0, float cin, float cout, float den,
+                                        float area, double vol, float dt, const float* st) {
+    const double gamma = (st[0] > 0.0f) ? (double)st[0] : 100.0;
+    const double Po = (st[1] > 0.0f) ? (double)st[1] : (double)0.012f;
+    const double Kc = (double)(float)gamma * 1e-12 * (kR * kT) / (kF * kF * (double)40.514f) * 1e12 * (double)area * Po;
+    const GhkD G = ghk_mono_d((double)V0, cin, cout);
+    const double I = Kc * G.F * (double)den;
+    const double cpv = kF * vol / 1000.0;
+    const bool mco = (double)cout + I * (double)dt / (cpv * kEVR) >= 1e-9;
+    const double lI = -lo[5] - lo[3] * (double)dt / cpv + (mco ? lo[4] * (double)dt / (cpv * kEVR) : 0.0);
+    const double lF = lI * Kc * (double)den;
+    lx[0] = lo[0] + lF * G.dV;
+    lx[1] = lx[2] = 0.0;
+    lx[3] = lo[3] + lF * G.dci;
+    lx[4] = (mco ? lo[4] : 0.0) + lF * G.dco;
+    lx[5] = lI * Kc * G.F;
+}
+
+// Ionotropic receptor with its open probability given.  lo = adjoints of (in[0]',
+// in[1]', in[3]', returned I); lx = adjoints of (V, in[0], in[1], in[3], out[0],
+// out[1], out[3], weight scale).  nv0/nv1/nv3 receive the updated ions (values).
+__device__ __forceinline__ void vjp_receptor(const double* lo, double* lx, int anion, double P_a, double P_b, float V0,
+                                             const float* in, const float* out, float w, float den, float area,
+                                             float open, double vol, float dt, float* nv) {
+    const double cpm = kF * vol / 1000.0;
+    const double Nk = (double)den * (double)area * (double)open * 1e12;
+    for (int k = 0; k < 8; k++) lx[k] = 0.0;
+    nv[0] = in[0]; nv[1] = in[1]; nv[2] = in[3];
+    if (anion) {
+        const GhkD G = ghk_mono_d((double)V0, out[3], in[3]);   // anion flux: c_in and c_out swapped
+        const double I = P_a * G.F * Nk * (double)w;
+        const double n3 = (double)in[3] + I * (double)dt / cpm;
+        const bool m3 = n3 >= 1e-9;
+        nv[2] = (float)(m3 ? n3 : 1e-9);
+        const double lI = -lo[3] + (m3 ? lo[2] * (double)dt / cpm : 0.0);
+        const double lF = lI * P_a * Nk * (double)w;
+        lx[0] = lF * G.dV;
+        lx[1] = lo[0]; lx[2] = lo[1];
+        lx[3] = (m3 ? lo[2] : 0.0) + lF * G.dco;
+        lx[6] = lF * G.dci;
+        lx[7] = lI * P_a * G.F * Nk;
+        return;
+    }
+    const GhkD Ga = ghk_mono_d((double)V0, in[0], out[0]);
+    const GhkD Gb = ghk_mono_d((double)V0, in[1], out[1]);
+    const double Ia = P_a * Ga.F * Nk * (double)w, Ib = P_b * Gb.F * Nk * (double)w;
+    const double n0 = (double)in[0] - Ia * (double)dt / cpm, n1 = (double)in[1] - Ib * (double)dt / cpm;
+    const bool m0 = n0 >= 1e-9, m1 = n1 >= 1e-9;
+    nv[0] = (float)(m0 ? n0 : 1e-9);
+    nv[1] = (float)(m1 ? n1 : 1e-9);
+    const double lIa = -lo[3] - (m0 ? lo[0] * (double)dt / cpm : 0.0);
+    const double lIb = -lo[3] - (m1 ? lo[1] * (double)dt / cpm : 0.0);
+    const double lFa = lIa * P_a * Nk * (double)w, lFb = lIb * P_b * Nk * (double)w;
+    lx[0] = lFa * Ga.dV + lFb * Gb.dV;
+    lx[1] = (m0 ? lo[0] : 0.0) + lFa * Ga.dci;
+    lx[2] = (m1 ? lo[1] : 0.0) + lFb * Gb.dci;
+    lx[3] = lo[2];
+    lx[4] = lFa * Ga.dco;
+    lx[5] = lFb * Gb.dco;
+    lx[7] = (lIa * P_a * Ga.F + lIb * P_b * Gb.F) * Nk;
+}
+
+// Scharfetter-Gummel Bernoulli function B(x) = x / (e^x - 1) and B'(x) in single
+// precision, one exponential for both; B(-x) = B(x) + x and B'(-x) = -(B'(x) + 1).
+__device__ __forceinline__ void bern_pair(float x, float ex, float* B, float* dB) {
+    if (fabsf(x) < 1e-3f) { *B = 1.0f - 0.5f * x; *dB = -0.5f; return; }
+    if (x > 50.0f) { *B = 0.0f; *dB = 0.0f; return; }
+    if (x < -50.0f) { *B = -x; *dB = -1.0f; return; }
+    const float em = ex - 1.0f;
+    *B = x / em;
+    *dB = (em - x * ex) / (em * em);
+}
+
+// diffusion_kernel.h:108-113 and its derivative
+__device__ __forceinline__ float bern(float x, float ex) {   // ex = exp(x) when needed
+    if (fabsf(x) < 1e-3f) return 1.0f - 0.5f * x;
+    if (x > 50.0f) return 0.0f;
+    if (x < -50.0f) return -x;
+    return x / (ex - 1.0f);
+}
+__device__ __forceinline__ double bern_d(float x) {
+    if (fabsf(x) < 1e-3f) return -0.5;
+    if (x > 50.0f) return 0.0;
+    if (x < -50.0f) return -1.0;
+    const double e = exp((double)x), em = e - 1.0;
+    return (em - (double)x * e) / (em * em);
+}
+
+}  // namespace adj
+}  // namespace bnc

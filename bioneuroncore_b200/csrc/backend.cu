@@ -15,6 +15,7 @@
 #include "net.h"
 #include "netgen.h"
 #include "hostnet.h"
+#include "hostnet.h"
 
 namespace bnc {
 
@@ -448,6 +449,90 @@ static int load_bion_file(const char* path, BncBionData* d) {
         if (d->segments[b].intra_connection_count < 16) d->segments[b].intra_connection_ids[d->segments[b].intra_connection_count++] = i;
     }
     return BNC_OK;
+}
+
+int backend_export_host(void* sim, HostNet* hn, std::vector<BncCurrentStimulus>* stim, uint64_t* tick,
+                        int* device, uint32_t* n_vclamp) {
+    if (!sim) { set_error("null handle"); return BNC_ERR_ARG; }
+    Backend* b = static_cast<Backend*>(sim);
+    if (!b->loaded) { set_error("no network loaded"); return BNC_ERR_STATE; }
+    if (!b->owns_aos || !b->aos.segments) {
+        set_error("the network must be loaded from AoS arrays (bnc_load_aos)");
+        return BNC_ERR_UNSUPPORTED;
+    }
+    if (!b->members.empty()) { set_error("an ensemble backend holds several networks"); return BNC_ERR_UNSUPPORTED; }
+    cudaSetDevice(b->device);
+    int rc = sync_stream(b);
+    if (rc != BNC_OK) return rc;
+    rc = export_network(b->dev, b->host, b->ticks_run, &b->aos);
+    if (rc != BNC_OK) return rc;
+    hostnet_from_aos(b->aos, hn);
+    *stim = b->stim.current;
+    *tick = b->tick;
+    *device = b->device;
+    *n_vclamp = (uint32_t)b->stim.vclamp.size();
+    return BNC_OK;
+}
+
+int backend_record_releases(void* sim, uint32_t ticks, float dt, std::vector<uint32_t>* syn,
+                            std::vector<uint64_t>* tick, std::vector<float>* amt, std::vector<uint8_t>* slot) {
+    if (!sim) { set_error("null handle"); return BNC_ERR_ARG; }
+    Backend* b = static_cast<Backend*>(sim);
+    if (!b->loaded) { set_error("no network loaded"); return BNC_ERR_STATE; }
+    cudaSetDevice(b->device);
+    syn->clear(); tick->clear(); amt->clear(); slot->clear();
+    const uint64_t t_begin = b->tick;
+    // Cleft entries per synapse: one immediate release per refractory period (the
+    // reference's uint8 refractory count, simulation_host.cpp:458) plus one delayed
+    // arrival per release.
+    uint32_t refr = (uint32_t)(uint8_t)(uint32_t)(20.0f / dt + 0.5f);
+    if (refr == 0) refr = 1;
+    const uint64_t per_syn = 2ull * ((uint64_t)ticks / refr + 1u);
+    const uint64_t cap64 = (uint64_t)b->dev.n_syn * per_syn + 16u;
+    if (cap64 > 0x7FFFFFFFull) { set_error("release log of %llu entries is too large", (unsigned long long)cap64); return BNC_ERR_ARG; }
+    {
+        const uint32_t cap = (uint32_t)cap64;
+        uint4* buf = nullptr;
+        uint32_t* n = nullptr;
+        if (cudaMalloc(&buf, (size_t)cap * sizeof(uint4)) != cudaSuccess ||
+            cudaMalloc(&n, sizeof(uint32_t)) != cudaSuccess) {
+            cudaFree(buf);
+            set_error("device allocation of the release log (%u entries) failed", cap);
+            return BNC_ERR_ALLOC;
+        }
+        cudaMemsetAsync(n, 0, sizeof(uint32_t), b->stream);
+        b->drop_graph();   // a captured tick holds the descriptor without the log
+        b->dev.ev_buf = buf; b->dev.ev_n = n; b->dev.ev_cap = cap;
+        int rc = run_ticks(b, ticks, dt);
+        b->dev.ev_buf = nullptr; b->dev.ev_n = nullptr; b->dev.ev_cap = 0;
+        if (rc == BNC_OK) rc = sync_stream(b);
+        uint32_t count = 0;
+        if (rc == BNC_OK && cudaMemcpy(&count, n, sizeof(uint32_t), cudaMemcpyDeviceToHost) != cudaSuccess)
+            rc = cuda_fail(cudaGetLastError(), "release log read");
+        if (rc == BNC_OK && count > cap) {
+            rc = BNC_ERR_STATE;
+            set_error("release log overflow (%u entries, room for %u)", count, cap);
+        }
+        std::vector<uint4> h(rc == BNC_OK ? count : 0);
+        if (rc == BNC_OK && count &&
+            cudaMemcpy(h.data(), buf, (size_t)count * sizeof(uint4), cudaMemcpyDeviceToHost) != cudaSuccess)
+            rc = cuda_fail(cudaGetLastError(), "release log read");
+        cudaFree(buf); cudaFree(n);
+        if (rc != BNC_OK) return rc;
+        syn->reserve(count); tick->reserve(count); amt->reserve(count); slot->reserve(count);
+        for (const uint4& e : h) {
+            // the low 32 bits of the tick, widened against the run's first tick
+            uint64_t t = (t_begin & ~0xFFFFFFFFull) | e.y;
+            if (t < t_begin) t += 0x100000000ull;
+            syn->push_back(b->host.syn_orig[e.x]);
+            tick->push_back(t);
+            float a;
+            std::memcpy(&a, &e.z, sizeof(a));
+            amt->push_back(a);
+            slot->push_back((uint8_t)e.w);
+        }
+        return BNC_OK;
+    }
 }
 
 }  // namespace bnc

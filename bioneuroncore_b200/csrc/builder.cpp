@@ -271,6 +271,13 @@ void hostnet_add_synapse(HostNet& hn, const BncSynapse& y) {
     hn.num_synapses = (uint32_t)hn.syn.size();
 }
 
+float host_seg_area(const SegLite& s) { return seg_area(s); }
+double host_seg_volume(const SegLite& s) { return seg_volume(s); }
+float host_seg_capacitance(const HostNet& hn, uint32_t i) { return seg_capacitance(hn, i); }
+bool host_is_myelin_blocked(uint8_t type) { return is_myelin_blocked(type); }
+bool host_is_ionotropic(uint8_t type) { return is_ionotropic(type); }
+uint8_t host_nt_from_receptor(uint8_t type) { return nt_from_receptor(type); }
+
 void hostnet_from_aos(const BncBionData& aos, HostNet* hn) {
     *hn = HostNet();
     hn->seg.reserve(aos.num_segments);

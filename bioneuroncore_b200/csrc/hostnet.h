@@ -59,6 +59,15 @@ struct HostNet {
     }
 };
 
+// Static per-segment quantities and type predicates of the reference, as the builder
+// computes them (run_tick_common.h:209-266, kernel_dispatch.h:283-309).
+float host_seg_area(const SegLite& s);
+double host_seg_volume(const SegLite& s);
+float host_seg_capacitance(const HostNet& hn, uint32_t i);
+bool host_is_myelin_blocked(uint8_t type);
+bool host_is_ionotropic(uint8_t type);
+uint8_t host_nt_from_receptor(uint8_t type);
+
 void hostnet_add_segment(HostNet& hn, const BncSegment& s);
 void hostnet_add_synapse(HostNet& hn, const BncSynapse& y);
 void hostnet_from_aos(const BncBionData& aos, HostNet* hn);

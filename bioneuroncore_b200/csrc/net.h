@@ -156,6 +156,13 @@ struct NetDev {
     // first-tick flag from clock[1] == 0 (ticks run so far) instead of their launch
     // parameters, and k_advance_clock moves both on after each tick.
     unsigned long long* clock;
+    // Release log (null: off).  Every transmitter amount that enters a synaptic cleft
+    // -- a delayed arrival (slot 0-3) or an immediate release (slot 4) -- is appended
+    // as {device synapse, tick (low 32 bits), amount bits, slot}; entries past ev_cap
+    // are counted but not written.
+    uint4* ev_buf;
+    uint32_t* ev_n;
+    uint32_t ev_cap;
 };
 
 // How components are grouped: a warp group holds components until their segments
@@ -251,6 +258,14 @@ cudaError_t launch_device_modifier(const void* kernel, const NetDev& d, uint8_t 
                                    cudaStream_t stream);
 // synapse.cu: per-device receptor constants (outside stream capture)
 cudaError_t prepare_synapse(cudaStream_t stream);
+// backend.cu: what the adjoint (adjoint.cu) takes from a loaded backend
+struct HostNet;
+int backend_export_host(void* sim, HostNet* hn, std::vector<BncCurrentStimulus>* stim, uint64_t* tick,
+                        int* device, uint32_t* n_vclamp);
+// Runs `ticks` plain ticks with the release log on; returns each cleft entry as
+// (original synapse index, tick, amount, slot) in the order the kernel wrote them.
+int backend_record_releases(void* sim, uint32_t ticks, float dt, std::vector<uint32_t>* syn,
+                            std::vector<uint64_t>* tick, std::vector<float>* amt, std::vector<uint8_t>* slot);
 // diffuse.cu
 cudaError_t prepare_diffusion(const NetHost& host, cudaStream_t stream);
 cudaError_t enqueue_diffusion(const NetDev& dev, const NetHost& host, float dt, unsigned long long tick,

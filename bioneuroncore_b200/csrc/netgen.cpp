@@ -84,7 +84,7 @@ Family family_defaults(uint32_t fam) {
         case BNC_NET_LARGE: return {100000, 64, 0, 10000000, false, true, 8, 200.0f};
         case BNC_NET_TREES: return {16384, 0, 10, 0, true, false, 1, 200.0f};
         case BNC_NET_ENSEMBLE_MEMBER: return {64, 32, 0, 400, false, false, 1, 200.0f};
-        case BNC_NET_ADJOINT: return {256, 64, 0, 2000, false, false, 1, 200.0f};
+        case BNC_NET_ADJOINT: return {256, 64, 0, 2000, false, false, 1, 1000.0f};
         default: return {0, 0, 0, 0, false, false, 0, 0.0f};
     }
 }
@@ -197,8 +197,10 @@ int generate_network(const BncNetgenParams& p, NetSink& sink, NetShape* shape_ou
                 set_mod(seg.modifiers[mc++], nav, 15.0 * scale_of(p, 0));
                 set_mod(seg.modifiers[mc++], BNC_MOD_KV_DR, 8.3 * scale_of(p, 1));
                 set_mod(seg.modifiers[mc++], BNC_MOD_K2P, 4.17 * scale_of(p, 2));
-                set_mod(seg.modifiers[mc++], BNC_MOD_CAV13, 0.04 * scale_of(p, 3));
-                set_mod(seg.modifiers[mc++], BNC_MOD_PUMP_NAK, 1500.0);
+                if (p.family != BNC_NET_ADJOINT) {   // the fitting family: the three fitted conductances only
+                    set_mod(seg.modifiers[mc++], BNC_MOD_CAV13, 0.04 * scale_of(p, 3));
+                    set_mod(seg.modifiers[mc++], BNC_MOD_PUMP_NAK, 1500.0);
+                }
                 if (axon && (axon_idx & 1u)) set_mod(seg.modifiers[mc++], BNC_MOD_MYELIN, 1.0);
             }
             if (axon) set_mod(seg.modifiers[mc++], BNC_MOD_CAV21, 100.0 * scale_of(p, 3));

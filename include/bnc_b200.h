@@ -96,7 +96,7 @@ int gpu_backend_seg_size(void);
 #define BNC_NET_LARGE 2        /* 100k x 64-segment neurons, 16 of 24 types, 10M synapses */
 #define BNC_NET_TREES 3        /* depth-10 binary dendritic trees, electrodiffusion */
 #define BNC_NET_ENSEMBLE_MEMBER 4 /* one network of an uneven ensemble */
-#define BNC_NET_ADJOINT 5      /* 256 x 64-segment neurons, 2000 synapses */
+#define BNC_NET_ADJOINT 5      /* 256 x 64-segment neurons, 2000 synapses; Nav, Kv_DR, K2P (+ myelin, Cav2.1); 1 nA steps */
 
 typedef struct {
     uint32_t family;          /* BNC_NET_* */
@@ -321,6 +321,74 @@ int bnc_save_bion(void* sim, const char* filename);
 
 /* Message for the last error on this thread ("" when none). */
 const char* bnc_last_error(void);
+
+/* ------------------------------------------------------------------ */
+/* 6. adjoint: gradients of a somatic voltage-trace loss               */
+/* ------------------------------------------------------------------ */
+/* The forward/backward pair differentiates the tick of simulation_host.cpp:174-657
+ * with respect to per-segment maximal conductances -- gNa, gK, gleak: the densities
+ * of the segment's Nav1.6/Nav1.2 (141/142), Kv delayed rectifier (123) and K2P leak
+ * (107) modifiers -- and per-synapse weights, a multiplicative scale on the density
+ * of the synapse's receptors (the `mod_scale` of ionotropic_ghk_current,
+ * modifier_helpers.h:421; 1 reproduces the reference).  The reference has no
+ * gradient path; these entry points are new.
+ *
+ * Loss of parameter set p: (1 / (S * n)) * sum over the S sampled ticks and the n
+ * neurons of (V_soma - target)^2, V_soma taken after every `sample_every`-th tick.
+ *
+ * Release events are pathwise: bnc_adjoint_record runs the plain tick on `sim` and
+ * logs every transmitter amount that enters a cleft; the forward and backward passes
+ * replay that log for every parameter set.  With the releases fixed each neuron
+ * evolves on its own, so a forward pass runs one CTA per (neuron, parameter set).
+ * The backward pass re-runs windows of `checkpoint_every` ticks from checkpoints and
+ * walks each window backwards.
+ *
+ * Modelled networks (others are rejected with BNC_ERR_UNSUPPORTED): segment
+ * modifiers Nav1.6, Nav1.2, Kv_DR, K2P (differentiated), myelin and Cav2.1 (no
+ * current); chemical synapses with AMPA and GABA-A receptors (at most 2 each);
+ * neurons of at most 128 segments, each a contiguous segment range joined by its
+ * connections; no voltage clamps. */
+typedef struct {
+    uint32_t n_sets;           /* parameter sets run side by side, 1..65535 */
+    uint32_t ticks;            /* ticks of the run */
+    uint32_t checkpoint_every; /* K: ticks between checkpoints (0: 256) */
+    uint32_t sample_every;     /* somatic V_m sampled after every this many ticks (0: 1) */
+    float dt;                  /* ms */
+} BncAdjointConfig;
+
+typedef struct {
+    uint32_t n_neurons, n_segments, n_synapses, n_samples, n_sets, ticks, checkpoint_every;
+    uint32_t threads, smem_forward, smem_backward;   /* per CTA */
+    uint64_t checkpoint_bytes, window_bytes, scratch_bytes;
+} BncAdjointInfo;
+
+/* Takes structure, state and parameters from the network loaded in `sim` (loaded
+ * from AoS arrays, at its current tick).  NULL on error (bnc_last_error).  Every
+ * parameter set starts from the network's densities and weight scale 1. */
+void* bnc_adjoint_create(void* sim, const BncAdjointConfig* cfg);
+void bnc_adjoint_destroy(void* adj);
+int bnc_adjoint_info(void* adj, BncAdjointInfo* info);
+/* The global segment index of each neuron's soma (the order of the loss's neurons). */
+int bnc_adjoint_soma(void* adj, uint32_t* soma, uint32_t n);
+/* Runs cfg.ticks plain ticks on `sim` (the network the adjoint was created from, at
+ * the same tick) and keeps the release log they produce. */
+int bnc_adjoint_record(void* adj, void* sim);
+int bnc_adjoint_release_count(void* adj, uint64_t* n);
+/* Parameters of one set, in original segment / synapse order; NULL leaves an array. */
+int bnc_adjoint_set_params(void* adj, uint32_t set, const float* gNa, const float* gK, const float* gleak,
+                           const float* w);
+int bnc_adjoint_get_params(void* adj, uint32_t set, float* gNa, float* gK, float* gleak, float* w);
+/* Target somatic traces [n_samples][n_neurons], shared by all sets. */
+int bnc_adjoint_set_target(void* adj, const float* target);
+/* Forward pass of every set from the network's state at creation: loss[n_sets]
+ * (may be NULL; needs a target), trace [n_sets][n_samples][n_neurons] (may be NULL). */
+int bnc_adjoint_forward(void* adj, double* loss, float* trace);
+/* Backward pass after a forward pass with the same parameters: gradients of each
+ * set's loss, [n_sets][n_segments] for each conductance and [n_sets][n_synapses] for
+ * the weights (any may be NULL).  A segment without the modifier gets 0. */
+int bnc_adjoint_backward(void* adj, float* g_gNa, float* g_gK, float* g_gleak, float* g_w);
+/* Device time of the last forward and backward pass (CUDA events). */
+int bnc_adjoint_timings(void* adj, float* forward_ms, float* backward_ms);
 
 #ifdef __cplusplus
 }

@@ -53,7 +53,24 @@ typedef struct BoSim {
     uint32_t* spike_count;  /* per segment, threshold -40 mV upward crossings */
     float nt_D[15];
     char err[256];
+    /* release log (bo_set_release_log): every amount that enters a cleft */
+    uint32_t *log_syn;
+    uint64_t *log_tick;
+    float *log_amt;
+    uint8_t *log_slot;
+    uint32_t log_cap, log_n;
 } BoSim;
+
+static void bo_log_release(BoSim* S, uint32_t syn, uint64_t tick, float amt, uint8_t slot) {
+    if (!S->log_syn) return;
+    if (S->log_n < S->log_cap) {
+        S->log_syn[S->log_n] = syn;
+        S->log_tick[S->log_n] = tick;
+        S->log_amt[S->log_n] = amt;
+        S->log_slot[S->log_n] = slot;
+    }
+    S->log_n++;
+}
 
 /* ---- diffusion scratch (reference keeps these as function statics) ---- */
 typedef struct {
@@ -547,6 +564,7 @@ static void bo_tick(BoSim* S, float dt) {
                 if (slots[q].arrival == 0) continue;
                 if (slots[q].arrival <= tick) {
                     syn->cleft[slots[q].nt] += slots[q].amount;
+                    bo_log_release(S, i, tick, slots[q].amount, (uint8_t)q);
                     slots[q].arrival = 0;
                 }
             }
@@ -597,6 +615,7 @@ static void bo_tick(BoSim* S, float dt) {
                     }
                 } else {
                     syn->cleft[nt_type] += release_amt;
+                    bo_log_release(S, i, tick, release_amt, 4);
                 }
                 syn->refractory = (uint8_t)(uint32_t)(20.0f / dt + 0.5f);
             }
@@ -769,6 +788,14 @@ void bo_run_trace(BoSim* S, uint32_t ticks, float dt, const uint32_t* rec, uint3
 }
 
 uint64_t bo_tick_count(const BoSim* S) { return S->tick; }
+
+/* Starts a release log into caller-owned arrays of `cap` entries (NULL stops it);
+ * returns nothing.  bo_release_log_count gives the entries seen (may exceed cap). */
+void bo_set_release_log(BoSim* S, uint32_t* syn, uint64_t* tick, float* amt, uint8_t* slot, uint32_t cap) {
+    S->log_syn = syn; S->log_tick = tick; S->log_amt = amt; S->log_slot = slot;
+    S->log_cap = cap; S->log_n = 0;
+}
+uint32_t bo_release_log_count(const BoSim* S) { return S->log_n; }
 
 /* Field export.  field: 0 V, 1 in[ion], 2 out[ion], 3 atp, 4 temp, 5 txn,
  * 6 intra_nt[idx], 7 nt[idx], 8 modifier state (idx = slot*8+k), 9 spike count. */

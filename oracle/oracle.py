@@ -49,6 +49,8 @@ def oracle_lib():
         lib.bo_nernst_f.argtypes = [C.c_float] * 3; lib.bo_nernst_f.restype = C.c_float
         lib.bo_const.argtypes = [C.c_int]; lib.bo_const.restype = C.c_double
         lib.bo_register_modifier.argtypes = [C.c_uint8, C.c_void_p]; lib.bo_register_modifier.restype = C.c_int
+        lib.bo_set_release_log.argtypes = [vp, vp, vp, vp, vp, C.c_uint32]
+        lib.bo_release_log_count.argtypes = [vp]; lib.bo_release_log_count.restype = C.c_uint32
         _ora = lib
     return _ora
 
@@ -114,6 +116,24 @@ class Oracle:
         s = np.ascontiguousarray(scale, np.float32)
         oracle_lib().bo_set_syn_scale(self.h, s.ctypes.data)
 
+    def run_logged(self, ticks, dt, cap=None):
+        """Runs `ticks` ticks and returns the release log they produce, sorted by
+        (synapse, tick, slot): every transmitter amount that entered a cleft."""
+        cap = cap or max(64, self.n_syn * (ticks // 16 + 4))
+        syn = np.zeros(cap, np.uint32)
+        tick = np.zeros(cap, np.uint64)
+        amt = np.zeros(cap, np.float32)
+        slot = np.zeros(cap, np.uint8)
+        lib = oracle_lib()
+        lib.bo_set_release_log(self.h, syn.ctypes.data, tick.ctypes.data, amt.ctypes.data, slot.ctypes.data, cap)
+        lib.bo_run(self.h, ticks, C.c_float(dt))
+        n = lib.bo_release_log_count(self.h)
+        lib.bo_set_release_log(self.h, None, None, None, None, 0)
+        if n > cap:
+            raise RuntimeError("release log overflow")
+        order = np.lexsort((slot[:n], tick[:n], syn[:n]))
+        return syn[:n][order], tick[:n][order], amt[:n][order]
+
     def close(self):
         if self.h:
             oracle_lib().bo_destroy(self.h)
@@ -148,3 +168,42 @@ class Reference:
             self.run(1, dt)
             out[t] = self.net.segments["V_m"][rec]
         return out
+
+
+_tan = None
+
+
+def tangent_lib():
+    """oracle/libbo_tangent.so: the FP64 forward-mode replay (bo_tangent.cpp)."""
+    global _tan
+    if _tan is None:
+        from bioneuroncore_b200 import build
+        path = build.TANGENT_LIB
+        if not os.path.exists(path):
+            build.build_oracle()
+        lib = C.CDLL(path)
+        vp = C.c_void_p
+        lib.bo_tangent_run.argtypes = [vp, vp, C.c_uint32, vp, vp, vp, C.c_uint32, C.c_uint64, C.c_uint32, C.c_float,
+                                       C.c_uint32] + [vp] * 8 + [vp, C.c_uint32, vp, vp, vp]
+        lib.bo_tangent_run.restype = C.c_int
+        _tan = lib
+    return _tan
+
+
+def tangent_loss(net, log, ticks, dt, params, direction, soma, target, stride=1):
+    """Loss and its derivative along `direction` (FP64 forward mode) for the replayed
+    tick.  params / direction: (gNa, gK, gleak per segment, w per synapse)."""
+    syn, tick, amt = [np.ascontiguousarray(a) for a in log]
+    syn = syn.astype(np.uint32); tick = tick.astype(np.uint64); amt = amt.astype(np.float32)
+    p = [np.ascontiguousarray(a, np.float64) for a in params]
+    d = [np.ascontiguousarray(a, np.float64) for a in direction]
+    soma = np.ascontiguousarray(soma, np.uint32)
+    target = np.ascontiguousarray(target, np.float32)
+    loss, dloss = C.c_double(), C.c_double()
+    rc = tangent_lib().bo_tangent_run(C.byref(net.data), net.stim_ptr, net.n_stim, syn.ctypes.data, tick.ctypes.data,
+                                      amt.ctypes.data, syn.size, 0, ticks, C.c_float(dt), stride,
+                                      *[a.ctypes.data for a in p], *[a.ctypes.data for a in d],
+                                      soma.ctypes.data, soma.size, target.ctypes.data, C.byref(loss), C.byref(dloss))
+    if rc != 0:
+        raise ValueError("network not modelled by the tangent replay")
+    return loss.value, dloss.value

@@ -1,0 +1,51 @@
+"""The FP64 forward-mode replay (oracle/bo_tangent.cpp) that checks the device adjoint:
+its directional derivatives against central differences of its own loss, on the CPU.
+Also the oracle's release log, which the replay feeds on."""
+import numpy as np
+
+from bioneuroncore_b200 import Network, NetgenParams, NET_ADJOINT
+
+DT = 0.025
+
+
+def _densities(net):
+    seg = net.segments
+    N, K = net.data.num_segments, net.data.num_synapses
+    out = [np.zeros(N) for _ in range(3)]
+    for i in range(N):
+        for j in range(seg["modifier_count"][i]):
+            c = {141: 0, 142: 0, 123: 1, 107: 2}.get(int(seg["modifiers"][i][j]["type"]))
+            if c is not None:
+                out[c][i] = float(np.float32(seg["modifiers"][i][j]["density"]))
+    return out + [np.ones(K)]
+
+
+def test_release_log_is_sorted_and_positive():
+    from oracle.oracle import Oracle
+    p = NetgenParams(family=NET_ADJOINT, n_neurons=4, seed=7)
+    syn, tick, amt = Oracle(Network(p)).run_logged(400, DT)
+    assert syn.size > 0
+    key = syn.astype(np.uint64) * np.uint64(1 << 32) + tick
+    assert (np.diff(key.astype(np.float64)) >= 0).all()
+    assert (amt > 0).all() and (tick < 400).all()
+
+
+def test_tangent_matches_its_central_differences():
+    from oracle.oracle import Oracle, tangent_loss
+    ticks = 300
+    p = NetgenParams(family=NET_ADJOINT, n_neurons=3, seed=11)
+    net = Network(p)
+    log = Oracle(Network(p)).run_logged(ticks, DT)
+    base = _densities(net)
+    soma = np.array([n * 64 for n in range(3)], np.uint32)
+    target = np.full((ticks, 3), -64.0, np.float32)
+    rng = np.random.default_rng(5)
+    dvec = [x * rng.standard_normal(x.shape) for x in base]
+    zero = [np.zeros_like(x) for x in base]
+    L, dL = tangent_loss(net, log, ticks, DT, base, dvec, soma, target)
+    h = 1e-4
+    Lp, _ = tangent_loss(net, log, ticks, DT, [x + h * v for x, v in zip(base, dvec)], zero, soma, target)
+    Lm, _ = tangent_loss(net, log, ticks, DT, [x - h * v for x, v in zip(base, dvec)], zero, soma, target)
+    fd = (Lp - Lm) / (2 * h)
+    assert L > 0 and abs(dL) > 0
+    assert abs(dL - fd) <= 1e-6 * abs(fd), (dL, fd)
