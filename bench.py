@@ -57,6 +57,10 @@ def parse_args():
     ap.add_argument("--no-trees", action="store_true")
     ap.add_argument("--trees", type=int, default=16384)
     ap.add_argument("--tree-ticks", type=int, default=20)
+    ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--adj-neurons", type=int, default=256)
+    ap.add_argument("--adj-sets", type=int, default=64)
+    ap.add_argument("--adj-ticks", type=int, default=1024)
     return ap.parse_args()
 
 
@@ -289,6 +293,55 @@ def run_trees(a, device):
     }
 
 
+def run_adjoint(a, device):
+    """Adjoint fitting workload: a.adj_neurons neurons x 64 segments with 2,000 synapses
+    per 256 neurons (the fitting family: Nav, Kv_DR, K2P leak, AMPA/GABA-A), a.adj_sets
+    parameter sets in one launch, checkpoints every 256 ticks.  Targets come from a
+    hidden parameter set; the forward and backward passes are device-timed (CUDA events
+    inside the library) and their ratio is the adjoint's cost in forward passes."""
+    import numpy as np
+    from bioneuroncore_b200 import Adjoint, Backend, Network, NetgenParams, NET_ADJOINT
+    t0 = time.perf_counter()
+    net = Network(NetgenParams(family=NET_ADJOINT, n_neurons=a.adj_neurons, seed=a.seed))
+    b = Backend(device)
+    b.load_network(net)
+    adj = Adjoint(b, a.adj_sets, a.adj_ticks, DT, checkpoint_every=256)
+    adj.record()
+    i = adj.info
+    base = adj.get_params(0)
+    hidden = [x * f for x, f in zip(base, (1.15, 0.85, 1.25, 0.8))]
+    adj.set_params(0, *hidden)
+    _, tr = adj.forward(trace=True)
+    adj.set_target(tr[0])
+    rng = np.random.default_rng(a.seed)
+    for p in range(a.adj_sets):   # parameter sets spread around the network's densities
+        adj.set_params(p, *[(x * np.exp(0.1 * rng.standard_normal(x.shape))).astype(np.float32) for x in base])
+    setup_s = time.perf_counter() - t0
+    loss, _ = adj.forward()       # the kernels are warm from the target pass
+    g = adj.backward()
+    fwd_ms, bwd_ms = adj.timings()
+    seg_ticks = float(i.n_segments) * a.adj_sets * a.adj_ticks
+    adj.close()
+    b.close()
+    spec_ticks = 20000
+    return {
+        "workload": "%d neurons x 64 segments (%d segments), %d synapses, %d parameter sets, %d ticks, "
+                    "checkpoints every 256 ticks; loss = MSE of somatic V_m against a hidden parameter set"
+                    % (a.adj_neurons, i.n_segments, i.n_synapses, a.adj_sets, a.adj_ticks),
+        "forward_ms": fwd_ms, "backward_ms": bwd_ms, "backward_over_forward": bwd_ms / fwd_ms,
+        "forward_segment_ticks_per_s": seg_ticks / (fwd_ms / 1000.0),
+        "gradient_segment_ticks_per_s": seg_ticks / ((fwd_ms + bwd_ms) / 1000.0),
+        "loss_mean": float(np.mean(loss)), "grad_abs_sum_gleak": float(np.abs(g[2]).sum()),
+        "extrapolated_20000_ticks_s": {"forward": fwd_ms / 1000.0 * spec_ticks / a.adj_ticks,
+                                       "backward": bwd_ms / 1000.0 * spec_ticks / a.adj_ticks,
+                                       "note": "linear in ticks; the timed run is %d ticks" % a.adj_ticks},
+        "memory_bytes": {"checkpoints": i.checkpoint_bytes, "window": i.window_bytes, "scratch": i.scratch_bytes},
+        "launch": "one CTA per (neuron, parameter set); forward %d threads, %d B shared; backward %d B shared"
+                  % (i.threads, i.smem_forward, i.smem_backward),
+        "setup_s": round(setup_s, 1),
+    }
+
+
 def main():
     a = parse_args()
     if a.impl == "reference":
@@ -368,6 +421,11 @@ def main():
         b.close()
         trees = run_trees(a, local_rank if world > 1 else 0)
 
+    adjoint = None
+    if not a.no_adjoint:
+        b.close()
+        adjoint = run_adjoint(a, local_rank if world > 1 else 0)
+
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         try:
@@ -389,6 +447,7 @@ def main():
                        "tiles": info.n_tiles, "phases": info.n_phases, "setup_s": round(setup_s, 1)},
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,
             "gpu_launches": (info.n_phases + 3) * a.steps, "ensemble": ensemble, "trees": trees,
+            "adjoint": adjoint,
         }
         print(json.dumps(line), flush=True)
     b.close()

@@ -26,11 +26,13 @@
 //   intracellular Nernst-Planck sub-steps (hand-derived: Bernoulli fluxes, chord
 //   conductances, the transposed Jacobi sweeps) -> the phi_e solve -> step 1 (local
 //   Jacobians of the channel models by dual numbers, slot order reversed).
+#define BNC_MATH_OUTLINE 1   // one copy of exp/log for the forward, the re-runs and the reverse
 #include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
 #include <cuda_runtime.h>
+#include <cuda_pipeline.h>
 #include "net.h"
 #include "hostnet.h"
 #include "physics.cuh"
@@ -44,7 +46,7 @@ namespace {
 constexpr int kMaxSeg = 128;     // segments (and connections) per neuron: threads per CTA
 constexpr int kItems = 3;        // differentiable items per segment (Nav, Kv_DR, K2P)
 constexpr int kGates = 4;        // dynamic gate words per segment
-constexpr int kMaxInc = 8;       // connections per segment
+constexpr int kMaxInc = 4;       // connections per segment (the generated families have at most 3)
 constexpr int kRecPerSyn = 2;    // receptors per synapse
 constexpr int kSegWords = 19;    // V, 7 intra, 7 extra, 4 gates
 constexpr int kSynWords = 5;     // receptor 0 (r, d), receptor 1 (r, d), cleft
@@ -118,7 +120,7 @@ struct Lay {
     unsigned long long* pmask;   // reverse pass: per segment, the phi_e sweeps that did not clamp
     float *st, *gax, *term, *vnA, *vnB;
     // reverse pass only
-    float *x0, *s2, *lam, *lphi, *lI, *mu, *lvA, *lvB, *linp, *lgdg, *eca, *ecb, *edv, *ldiag, *phs, *jsm;
+    float *s2, *lam, *lphi, *lI, *mu, *lvB, *linp, *lgdg, *eca, *ecb, *edv, *ldiag, *phs, *jsm;
 };
 
 __host__ __device__ inline size_t lay_bytes(uint32_t S, uint32_t E, uint32_t Y, bool bwd) {
@@ -126,8 +128,7 @@ __host__ __device__ inline size_t lay_bytes(uint32_t S, uint32_t E, uint32_t Y, 
     size_t flt = (size_t)kSegWords * S + kSynWords * Y + 2 * (size_t)E + 2 * (size_t)S;
     if (bwd) {
         dbl += S;   // pmask
-        flt += (size_t)kSegWords * S + kSynWords * Y + 15 * (size_t)S + kSegWords * (size_t)S + 8 * (size_t)S +
-               15 * (size_t)E + 102 * (size_t)S;
+        flt += 15 * (size_t)S + kSegWords * (size_t)S + 7 * (size_t)S + (size_t)E + 102 * (size_t)S + 4;
     }
     return dbl * 8 + flt * 4;
 }
@@ -144,17 +145,20 @@ __device__ inline Lay make_lay(unsigned char* base, uint32_t S, uint32_t E, uint
     l.gax = f; f += E; l.term = f; f += E;
     l.vnA = f; f += S; l.vnB = f; f += S;
     if (bwd) {
-        l.x0 = f; f += kSegWords * S + kSynWords * Y;
         l.s2 = f; f += 15 * S;
         l.lam = f; f += kSegWords * S;
-        l.lphi = f; f += S; l.lI = f; f += S; l.mu = f; f += S; l.lvA = f; f += S; l.lvB = f; f += S;
+        l.lphi = f; f += S; l.lI = f; f += S; l.mu = f; f += S; l.lvB = f; f += S;
         l.linp = f; f += S; l.lgdg = f; f += S; l.ldiag = f; f += S; l.edv = f; f += E;
-        l.eca = f; f += 7 * E; l.ecb = f; f += 7 * E;
+        // the reverse tick's per-connection adjoints reuse the forward's flux buffers
+        l.eca = reinterpret_cast<float*>(l.fa);
+        l.ecb = reinterpret_cast<float*>(l.fb);
         l.phs = f; f += 51 * S;
+        // 16-byte aligned for the asynchronous copies
+        f = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(f) + 15u) & ~(uintptr_t)15u);
         l.jsm = f; f += 51 * S;
     } else {
-        l.x0 = l.s2 = l.lam = l.lphi = l.lI = l.mu = l.lvA = l.lvB = l.linp = l.lgdg = l.eca = l.ecb = l.edv =
-            l.ldiag = l.phs = l.jsm = nullptr;
+        l.s2 = l.lam = l.lphi = l.lI = l.mu = l.lvB = l.linp = l.lgdg = l.eca = l.ecb = l.edv = l.ldiag = l.phs =
+            l.jsm = nullptr;
     }
     return l;
 }
@@ -268,6 +272,14 @@ __device__ inline float cleft_events(const AdjDev& d, uint32_t slot, unsigned lo
     return cleft;
 }
 
+// One differentiable item (kernel_dispatch.h:337-570 for its type), out of line so the
+// forward tick and the reverse tick's re-run share one copy of each model.
+__device__ __noinline__ double run_slot(uint8_t type, DMod& m, DSeg& s, float dt) {
+    if (type == 123) return dp_kvdr_current<false>(m, s, dt);
+    if (type == 107) return dp_k2p_current<false>(m, s, dt);
+    return dp_nav_current<false>(m, s, dt, type == 142 ? 1 : 0);
+}
+
 // Step 1 for this thread's segment: the differentiable items in slot order, then the
 // current stimuli (simulation_host.cpp:234-303).
 __device__ inline double step1_seg(const AdjDev& d, const Ctx& c, const Lay& L, unsigned long long tick, float dt) {
@@ -294,21 +306,12 @@ __device__ inline double step1_seg(const AdjDev& d, const Ctx& c, const Lay& L, 
         for (int k = 0; k < 7; k++) m.st[k] = d.it_st[((size_t)g * kItems + j) * 7 + k];
         m.area = s.area;
         m.av = 0;
-        double I;
-        if (type == 123) {
-            m.st[0] = st[(15 + go) * Sm + i];
-            I = dp_kvdr_current<false>(m, s, dt);
-            st[(15 + go) * Sm + i] = m.st[0];
-        } else if (type == 107) {
-            I = dp_k2p_current<false>(m, s, dt);
-        } else {
-            m.st[0] = st[(15 + go) * Sm + i];
-            m.st[1] = st[(16 + go) * Sm + i];
-            I = dp_nav_current<false>(m, s, dt, type == 142 ? 1 : 0);
-            st[(15 + go) * Sm + i] = m.st[0];
-            st[(16 + go) * Sm + i] = m.st[1];
-        }
-        I_total += I;
+        const int ng = (type == 123) ? 1 : (type == 107 ? 0 : 2);
+        if (ng > 0) m.st[0] = st[(15 + go) * Sm + i];
+        if (ng > 1) m.st[1] = st[(16 + go) * Sm + i];
+        I_total += run_slot(type, m, s, dt);
+        if (ng > 0) st[(15 + go) * Sm + i] = m.st[0];
+        if (ng > 1) st[(16 + go) * Sm + i] = m.st[1];
     }
     for (uint32_t q = d.stim_off[g]; q < d.stim_off[g + 1]; q++)
         if (tick >= d.stim_b[q] && tick < d.stim_e[q]) I_total += d.stim_amp[q];
@@ -327,7 +330,7 @@ struct Scr {
     float* syn;       // [Ymax][9]   in[7] before the synapse, receptor open probabilities
 };
 __host__ __device__ inline size_t scr_floats(uint32_t S, uint32_t Y) {
-    return (size_t)40 * S + (size_t)255 * S + (size_t)42 * S + (size_t)9 * Y + 4;
+    return ((size_t)40 * S + (size_t)255 * S + (size_t)42 * S + (size_t)9 * Y + 4 + 3) & ~(size_t)3;
 }
 __device__ inline Scr make_scr(const AdjDev& d) {
     Scr s;
@@ -341,10 +344,11 @@ __device__ inline Scr make_scr(const AdjDev& d) {
     return s;
 }
 
-// One tick of the neuron in shared memory.  kRec records the intermediates the reverse
+// One tick of the neuron in shared memory; each kernel has one call site, so one copy.
+// kRec records the intermediates the reverse
 // tick reads (into L.s2, L.ib3, L.pmask, L.phs and the CTA's scratch).
-template <bool kRec>
-__device__ void tick_fwd(const AdjDev& d, const Ctx& c, const Lay& L, const Scr& sc, uint32_t t) {
+__device__ __forceinline__ void tick_fwd(const AdjDev& d, const Ctx& c, const Lay& L, const Scr& sc, uint32_t t,
+                                         bool kRec) {
     const uint32_t tid = threadIdx.x;
     const uint32_t S = c.S, E = c.E, Sm = d.Smax, Em = d.Emax;
     const bool seg = tid < S, edge = tid < E;
@@ -609,12 +613,14 @@ __device__ void tick_fwd(const AdjDev& d, const Ctx& c, const Lay& L, const Scr&
     __syncthreads();
 }
 
-// Reverse of tick t.  On entry L.x0 holds the tick's starting state, L.st the state
+// Reverse of tick t.  On entry x0 is the tick's starting state (its block in the window
+// buffer, stride S), L.st the state
 // after the recorded re-run, L.s2 / L.ib3 / L.ibuf / L.pmask / L.phs and the scratch the
 // intermediates, and L.lam the adjoint of the state after the tick (V, ions, gates).
 // On exit L.lam holds the adjoint of the starting state; gp accumulates
 // d loss / d (gNa, gK, gleak) of this thread's segment.
-__device__ void tick_rev(const AdjDev& d, const Ctx& c, const Lay& L, const Scr& sc, uint32_t t, double* gp) {
+__device__ void tick_rev(const AdjDev& d, const Ctx& c, const Lay& L, const Scr& sc, const float* x0, uint32_t t,
+                         double* gp) {
     const uint32_t tid = threadIdx.x;
     const uint32_t S = c.S, E = c.E, Sm = d.Smax, Em = d.Emax;
     const bool seg = tid < S, edge = tid < E;
@@ -793,8 +799,15 @@ __device__ void tick_rev(const AdjDev& d, const Ctx& c, const Lay& L, const Scr&
                 }
             }
             const float rden = 1.0f / (C_dt + gdiag);
-            // the sub-step's 51 iterates into shared memory, one coalesced pass
-            for (uint32_t q = tid; q < 51u * Sm; q += blockDim.x) L.jsm[q] = jac[q];
+            // the sub-step's 51 iterates into shared memory: asynchronous 16-byte copies, all
+            // in flight at once (the stride Sm is a multiple of 4, the scratch 16-byte aligned)
+            {
+                const float4* src4 = reinterpret_cast<const float4*>(jac);
+                float4* dst4 = reinterpret_cast<float4*>(L.jsm);
+                for (uint32_t q = tid; q < 51u * Sm / 4u; q += blockDim.x) __pipeline_memcpy_async(dst4 + q, src4 + q, 16);
+                __pipeline_commit();
+                __pipeline_wait_prior(0);
+            }
             __syncthreads();
             // one barrier per sweep: this thread's adjoint stays in a register, the mu of
             // consecutive sweeps alternate between two buffers
@@ -946,13 +959,13 @@ __device__ void tick_rev(const AdjDev& d, const Ctx& c, const Lay& L, const Scr&
         const uint32_t g = c.g;
         const float lIt = L.lI[tid];
         DSeg s;
-        s.V = L.x0[tid];
-        for (int q = 0; q < 7; q++) { s.in[q] = L.x0[(1 + q) * Sm + tid]; s.out[q] = L.x0[(8 + q) * Sm + tid]; }
+        s.V = x0[tid];
+        for (int q = 0; q < 7; q++) { s.in[q] = x0[(1 + q) * S + tid]; s.out[q] = x0[(8 + q) * S + tid]; }
         s.atp = 0.0f;
         s.area = c.area;
         s.vol = c.vol;
         float gate[kGates];
-        for (int k = 0; k < kGates; k++) gate[k] = L.x0[(15 + k) * Sm + tid];
+        for (int k = 0; k < kGates; k++) gate[k] = x0[(15 + k) * S + tid];
         const uint32_t ni = d.n_it[g];
         float preV[kItems], preG0[kItems], preG1[kItems], preCi[kItems], preCo[kItems];
         for (uint32_t j = 0; j < ni; j++) {
@@ -968,13 +981,12 @@ __device__ void tick_rev(const AdjDev& d, const Ctx& c, const Lay& L, const Scr&
             for (int k = 0; k < 7; k++) m.st[k] = d.it_st[((size_t)g * kItems + j) * 7 + k];
             m.area = s.area;
             m.av = 0;
-            if (type == 123) { m.st[0] = gate[go]; dp_kvdr_current<false>(m, s, dt); gate[go] = m.st[0]; }
-            else if (type == 107) { dp_k2p_current<false>(m, s, dt); }
-            else {
-                m.st[0] = gate[go]; m.st[1] = gate[go + 1];
-                dp_nav_current<false>(m, s, dt, type == 142 ? 1 : 0);
-                gate[go] = m.st[0]; gate[go + 1] = m.st[1];
-            }
+            const int ng = (type == 123) ? 1 : (type == 107 ? 0 : 2);
+            if (ng > 0) m.st[0] = gate[go];
+            if (ng > 1) m.st[1] = gate[go + 1];
+            run_slot(type, m, s, dt);
+            if (ng > 0) gate[go] = m.st[0];
+            if (ng > 1) gate[go + 1] = m.st[1];
         }
         float lV = lam[tid];
         for (int j = (int)ni - 1; j >= 0; j--) {
@@ -1029,7 +1041,7 @@ __global__ void __launch_bounds__(kMaxSeg) k_adj_forward(AdjDev d, uint32_t t0, 
             block_store(d.ckpt + ((size_t)(t / d.K) * d.n_sets + c.p) * d.L + c.st_off, L.st, c, d.Smax);
             __syncthreads();
         }
-        tick_fwd<false>(d, c, L, sc, t);
+        tick_fwd(d, c, L, sc, t, false);
         if ((t + 1) % d.stride == 0 && threadIdx.x == c.soma) {
             const uint32_t smp = (t + 1) / d.stride - 1;
             const float V = L.st[c.soma];
@@ -1059,20 +1071,27 @@ __global__ void __launch_bounds__(kMaxSeg) k_adj_backward(AdjDev d, uint32_t w) 
     }
     block_load(L.st, d.ckpt + ((size_t)w * d.n_sets + c.p) * d.L + c.st_off, c, d.Smax);
     __syncthreads();
-    for (uint32_t t = tb; t < te; t++) {
-        block_store(d.win + ((size_t)(t - tb) * d.n_sets + c.p) * d.L + c.st_off, L.st, c, d.Smax);
-        __syncthreads();
-        if (t + 1 < te) tick_fwd<false>(d, c, L, sc, t);
-    }
-    __syncthreads();
+    // Steps [0, nA): re-run the window from its checkpoint, keeping each tick's starting
+    // state; steps [nA, nA + n): walk the ticks backwards, each re-run with its
+    // intermediates recorded and then reversed.  One call site of the tick keeps one
+    // copy of its code in the kernel.
+    const uint32_t n = te - tb;
+    const uint32_t nA = n - 1;
     double gp[3] = {0.0, 0.0, 0.0};
-    for (int t = (int)te - 1; t >= (int)tb; t--) {
-        const float* src = d.win + ((size_t)(t - tb) * d.n_sets + c.p) * d.L + c.st_off;
-        block_load(L.st, src, c, d.Smax);
-        block_load(L.x0, src, c, d.Smax);
+    for (uint32_t step = 0; step < nA + n; step++) {
+        const bool rec = step >= nA;
+        const uint32_t t = rec ? te - 1 - (step - nA) : tb + step;
+        float* blk = d.win + ((size_t)(t - tb) * d.n_sets + c.p) * d.L + c.st_off;
+        if (!rec) {
+            block_store(blk, L.st, c, d.Smax);
+        } else {
+            if (step == nA) block_store(blk, L.st, c, d.Smax);   // the window's last tick
+            __syncthreads();
+            block_load(L.st, blk, c, d.Smax);
+        }
         __syncthreads();
-        tick_fwd<true>(d, c, L, sc, (uint32_t)t);
-        tick_rev(d, c, L, sc, (uint32_t)t, gp);
+        tick_fwd(d, c, L, sc, t, rec);
+        if (rec) tick_rev(d, c, L, sc, blk, t, gp);
     }
     {
         float* dst = d.lam + (size_t)c.p * d.L + c.st_off;
@@ -1420,7 +1439,8 @@ int adj_build(Adjoint* A, void* sim, const BncAdjointConfig& cfg) {
     rc = BNC_OK;
     d.nn = nn; d.n_seg = N; d.n_edge = M; d.n_slot = n_slot; d.n_syn = KS; d.n_sets = cfg.n_sets;
     d.T = cfg.ticks; d.K = K; d.n_ckpt = (cfg.ticks + K - 1) / K; d.stride = stride; d.n_samples = cfg.ticks / stride;
-    d.Smax = Smax; d.Emax = std::max(Emax, 1u); d.Ymax = Ymax; d.L = L; d.dt = cfg.dt; d.has_conn = M > 0;
+    d.Smax = (Smax + 3u) & ~3u;   // stride of the per-segment arrays: a multiple of 4 (16-byte rows)
+    d.Emax = std::max(Emax, 1u); d.Ymax = Ymax; d.L = L; d.dt = cfg.dt; d.has_conn = M > 0;
     d.tick0 = tick0;
     std::vector<uint32_t> nr_seg_v(nr_seg.begin(), nr_seg.end());
     d.nr_seg = upload(al, nr_seg_v, &rc); d.nr_edge = upload(al, nr_edge, &rc); d.nr_slot = upload(al, nr_slot, &rc);
@@ -1453,7 +1473,7 @@ int adj_build(Adjoint* A, void* sim, const BncAdjointConfig& cfg) {
     d.loss_part = static_cast<double*>(al.alloc((size_t)cfg.n_sets * nn * sizeof(double)));
     d.g_par = static_cast<double*>(al.alloc((size_t)cfg.n_sets * 3 * N * sizeof(double)));
     d.g_w = static_cast<double*>(al.alloc((size_t)cfg.n_sets * std::max(KS, 1u) * sizeof(double)));
-    d.scr_floats = scr_floats(Smax, Ymax);
+    d.scr_floats = scr_floats(d.Smax, Ymax);
     d.scr = static_cast<float*>(al.alloc((size_t)nn * cfg.n_sets * d.scr_floats * sizeof(float)));
     if (!d.state || !d.lam || !d.ckpt || !d.win || !d.loss_part || !d.g_par || !d.g_w || !d.scr)
         return adj_fail(BNC_ERR_ALLOC, "state, checkpoints and scratch");
@@ -1468,9 +1488,9 @@ int adj_build(Adjoint* A, void* sim, const BncAdjointConfig& cfg) {
     d.ev_off = A->ev_off; d.ev_tick = A->ev_tick; d.ev_amt = A->ev_amt;
     d.target = nullptr;
     d.trace = nullptr;
-    A->threads = ((std::max(Smax, d.Emax) + 31u) / 32u) * 32u;
-    A->smem_fwd = lay_bytes(Smax, d.Emax, Ymax, false);
-    A->smem_bwd = lay_bytes(Smax, d.Emax, Ymax, true);
+    A->threads = ((std::max(d.Smax, d.Emax) + 31u) / 32u) * 32u;
+    A->smem_fwd = lay_bytes(d.Smax, d.Emax, Ymax, false);
+    A->smem_bwd = lay_bytes(d.Smax, d.Emax, Ymax, true);
     if (A->smem_bwd > 227u * 1024u) { set_error("adjoint: a neuron needs %zu bytes of shared memory", A->smem_bwd); return BNC_ERR_UNSUPPORTED; }
     if (cudaFuncSetAttribute(k_adj_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)A->smem_fwd) != cudaSuccess ||
         cudaFuncSetAttribute(k_adj_backward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)A->smem_bwd) != cudaSuccess)

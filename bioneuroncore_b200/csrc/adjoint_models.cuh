@@ -15,6 +15,12 @@
 namespace bnc {
 namespace adj {
 
+#ifndef BNC_ADJ_NOINLINE
+#define BNC_ADJ_NOINLINE __device__ __noinline__
+#endif
+// One out-of-line copy of the double exponential for every dual-number use.
+BNC_ADJ_NOINLINE double adj_exp(double x) { return exp(x); }
+
 template <int N>
 struct Dual {
     double v;
@@ -81,7 +87,7 @@ template <int N> __device__ __forceinline__ Dual<N> operator/(double a, const Du
 template <int N>
 __device__ __forceinline__ Dual<N> dexp(const Dual<N>& a) {
     Dual<N> r;
-    r.v = exp(a.v);
+    r.v = adj_exp(a.v);
 #pragma unroll
     for (int k = 0; k < N; k++) r.d[k] = r.v * a.d[k];
     return r;
@@ -269,7 +275,7 @@ __device__ __forceinline__ GhkD ghk_mono_d(double Vd, double ci, double co) {
     const double A = Vd * (kk * kF * 0.001), dA = kk * kF * 0.001;
     if (Vn > 20.0) { r.F = A * ci; r.dV = dA * ci; r.dci = A; r.dco = 0.0; return r; }
     if (Vn < -20.0) { r.F = A * co; r.dV = dA * co; r.dci = 0.0; r.dco = A; return r; }
-    const double e = exp(-Vn), de = -e * c1;
+    const double e = adj_exp(-Vn), de = -e * c1;
     const double D = 1.0 - e, Nn = ci - co * e;
     r.F = A * Nn / D;
     r.dV = dA * Nn / D + A * de * (ci - co) / (D * D);

@@ -346,7 +346,7 @@ const char* bnc_last_error(void);
  * Modelled networks (others are rejected with BNC_ERR_UNSUPPORTED): segment
  * modifiers Nav1.6, Nav1.2, Kv_DR, K2P (differentiated), myelin and Cav2.1 (no
  * current); chemical synapses with AMPA and GABA-A receptors (at most 2 each);
- * neurons of at most 128 segments, each a contiguous segment range joined by its
+ * neurons of at most 128 segments and 4 connections per segment, each a contiguous segment range joined by its
  * connections; no voltage clamps. */
 typedef struct {
     uint32_t n_sets;           /* parameter sets run side by side, 1..65535 */
