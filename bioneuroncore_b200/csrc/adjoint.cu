@@ -282,7 +282,8 @@ __device__ __noinline__ double run_slot(uint8_t type, DMod& m, DSeg& s, float dt
 
 // Step 1 for this thread's segment: the differentiable items in slot order, then the
 // current stimuli (simulation_host.cpp:234-303).
-__device__ inline double step1_seg(const AdjDev& d, const Ctx& c, const Lay& L, unsigned long long tick, float dt) {
+__device__ inline double step1_seg(const AdjDev& d, const Ctx& c, const Lay& L, unsigned long long tick, float dt,
+                                   float* pre) {
     const uint32_t Sm = d.Smax;
     const uint32_t i = threadIdx.x;
     const uint32_t g = c.g;
@@ -309,6 +310,14 @@ __device__ inline double step1_seg(const AdjDev& d, const Ctx& c, const Lay& L, 
         const int ng = (type == 123) ? 1 : (type == 107 ? 0 : 2);
         if (ng > 0) m.st[0] = st[(15 + go) * Sm + i];
         if (ng > 1) m.st[1] = st[(16 + go) * Sm + i];
+        if (pre) {   // the item's inputs, for the reverse tick
+            const int ion = (ng == 2) ? 0 : 1;
+            pre[(j * 5 + 0) * Sm + i] = s.V;
+            pre[(j * 5 + 1) * Sm + i] = m.st[0];
+            pre[(j * 5 + 2) * Sm + i] = m.st[1];
+            pre[(j * 5 + 3) * Sm + i] = s.in[ion];
+            pre[(j * 5 + 4) * Sm + i] = s.out[ion];
+        }
         I_total += run_slot(type, m, s, dt);
         if (ng > 0) st[(15 + go) * Sm + i] = m.st[0];
         if (ng > 1) st[(16 + go) * Sm + i] = m.st[1];
@@ -324,13 +333,15 @@ __device__ inline double step1_seg(const AdjDev& d, const Ctx& c, const Lay& L, 
 // Scratch of one CTA: intracellular sub-step starts, Jacobi
 // iterates, extracellular sub-step starts, synapse pre-states.
 struct Scr {
+    float* pre;       // [kItems][5][Sm]  V, gate 0, gate 1, c_in, c_out before each item
     float* istart;    // [5][8][Sm]  V, in[7]
     float* jac;       // [5][51][Sm]
     float* estart;    // [6][7][Sm]  out before each extra sub-step and before the bath
     float* syn;       // [Ymax][9]   in[7] before the synapse, receptor open probabilities
 };
 __host__ __device__ inline size_t scr_floats(uint32_t S, uint32_t Y) {
-    return ((size_t)40 * S + (size_t)255 * S + (size_t)42 * S + (size_t)9 * Y + 4 + 3) & ~(size_t)3;
+    return ((size_t)40 * S + (size_t)255 * S + (size_t)42 * S + (size_t)9 * Y + (size_t)kItems * 5 * S + 4 + 3) &
+           ~(size_t)3;
 }
 __device__ inline Scr make_scr(const AdjDev& d) {
     Scr s;
@@ -340,7 +351,8 @@ __device__ inline Scr make_scr(const AdjDev& d) {
     s.istart = f; f += 40 * S;
     s.jac = f; f += 255 * S;
     s.estart = f; f += 42 * S;
-    s.syn = f;
+    s.syn = f; f += 9 * d.Ymax;
+    s.pre = f;
     return s;
 }
 
@@ -358,7 +370,7 @@ __device__ __forceinline__ void tick_fwd(const AdjDev& d, const Ctx& c, const La
     float* st = L.st;
 
     // ---- step 1 ----
-    if (seg) L.ibuf[tid] = step1_seg(d, c, L, tick, dt);
+    if (seg) L.ibuf[tid] = step1_seg(d, c, L, tick, dt, kRec ? sc.pre : nullptr);
     __syncthreads();
 
     // ---- step 2.5 (diffusion_kernel.h:115-364) ----
@@ -613,14 +625,12 @@ __device__ __forceinline__ void tick_fwd(const AdjDev& d, const Ctx& c, const La
     __syncthreads();
 }
 
-// Reverse of tick t.  On entry x0 is the tick's starting state (its block in the window
-// buffer, stride S), L.st the state
+// Reverse of tick t.  On entry L.st holds the state
 // after the recorded re-run, L.s2 / L.ib3 / L.ibuf / L.pmask / L.phs and the scratch the
 // intermediates, and L.lam the adjoint of the state after the tick (V, ions, gates).
 // On exit L.lam holds the adjoint of the starting state; gp accumulates
 // d loss / d (gNa, gK, gleak) of this thread's segment.
-__device__ void tick_rev(const AdjDev& d, const Ctx& c, const Lay& L, const Scr& sc, const float* x0, uint32_t t,
-                         double* gp) {
+__device__ void tick_rev(const AdjDev& d, const Ctx& c, const Lay& L, const Scr& sc, uint32_t t, double* gp) {
     const uint32_t tid = threadIdx.x;
     const uint32_t S = c.S, E = c.E, Sm = d.Smax, Em = d.Emax;
     const bool seg = tid < S, edge = tid < E;
@@ -954,40 +964,12 @@ __device__ void tick_rev(const AdjDev& d, const Ctx& c, const Lay& L, const Scr&
         __syncthreads();
     }
 
-    // ---- step 1 reversed (thread = segment): items last first ----
+    // ---- step 1 reversed (thread = segment): items last first, from the inputs the
+    // recorded re-run kept ----
     if (seg) {
         const uint32_t g = c.g;
         const float lIt = L.lI[tid];
-        DSeg s;
-        s.V = x0[tid];
-        for (int q = 0; q < 7; q++) { s.in[q] = x0[(1 + q) * S + tid]; s.out[q] = x0[(8 + q) * S + tid]; }
-        s.atp = 0.0f;
-        s.area = c.area;
-        s.vol = c.vol;
-        float gate[kGates];
-        for (int k = 0; k < kGates; k++) gate[k] = x0[(15 + k) * S + tid];
         const uint32_t ni = d.n_it[g];
-        float preV[kItems], preG0[kItems], preG1[kItems], preCi[kItems], preCo[kItems];
-        for (uint32_t j = 0; j < ni; j++) {
-            const uint8_t type = d.it_type[g * kItems + j];
-            const uint32_t go = d.it_gate[g * kItems + j];
-            const int ion = (type == 141 || type == 142) ? 0 : 1;
-            preV[j] = s.V; preCi[j] = s.in[ion]; preCo[j] = s.out[ion];
-            preG0[j] = gate[go]; preG1[j] = (go + 1 < kGates) ? gate[go + 1] : 0.0f;
-            if (j + 1 == ni) break;   // the last item's outputs are not needed
-            ghk_cache_fill(s.gc, s.V);
-            DMod m;
-            m.den = par_of(d, c.p, cls_of(type), g);
-            for (int k = 0; k < 7; k++) m.st[k] = d.it_st[((size_t)g * kItems + j) * 7 + k];
-            m.area = s.area;
-            m.av = 0;
-            const int ng = (type == 123) ? 1 : (type == 107 ? 0 : 2);
-            if (ng > 0) m.st[0] = gate[go];
-            if (ng > 1) m.st[1] = gate[go + 1];
-            run_slot(type, m, s, dt);
-            if (ng > 0) gate[go] = m.st[0];
-            if (ng > 1) gate[go + 1] = m.st[1];
-        }
         float lV = lam[tid];
         for (int j = (int)ni - 1; j >= 0; j--) {
             const uint8_t type = d.it_type[g * kItems + j];
@@ -996,24 +978,26 @@ __device__ void tick_rev(const AdjDev& d, const Ctx& c, const Lay& L, const Scr&
             const int cls = cls_of(type);
             const float* pst = d.it_st + ((size_t)g * kItems + j) * 7;
             const float den = par_of(d, c.p, cls, g);
+            const float pV = sc.pre[(j * 5 + 0) * Sm + tid], pG0 = sc.pre[(j * 5 + 1) * Sm + tid],
+                        pG1 = sc.pre[(j * 5 + 2) * Sm + tid], pCi = sc.pre[(j * 5 + 3) * Sm + tid],
+                        pCo = sc.pre[(j * 5 + 4) * Sm + tid];
             const int ng = (type == 123) ? 1 : (type == 107 ? 0 : 2);
-            const double lo[6] = {(double)lV,
-                                  ng > 0 ? (double)lam[(15 + go) * Sm + tid] : 0.0,
-                                  ng > 1 ? (double)lam[(16 + go) * Sm + tid] : 0.0,
-                                  (double)lam[(1 + ion) * Sm + tid],
-                                  (double)lam[(8 + ion) * Sm + tid],
-                                  (double)lIt};
-            double lx[6];
-            if (type == 123) adj::vjp_kvdr(lo, lx, preV[j], preG0[j], preCi[j], preCo[j], den, c.area, c.vol, dt, pst);
-            else if (type == 107) adj::vjp_k2p(lo, lx, preV[j], preCi[j], preCo[j], den, c.area, c.vol, dt, pst);
-            else adj::vjp_nav(lo, lx, preV[j], preG0[j], preG1[j], preCi[j], preCo[j], den, c.area, c.vol, dt,
-                              type == 142 ? 1 : 0, pst[5]);
-            lV = (float)lx[0];
-            if (ng > 0) lam[(15 + go) * Sm + tid] = (float)lx[1];
-            if (ng > 1) lam[(16 + go) * Sm + tid] = (float)lx[2];
-            lam[(1 + ion) * Sm + tid] = (float)lx[3];
-            lam[(8 + ion) * Sm + tid] = (float)lx[4];
-            gp[cls] += lx[5];
+            const float lo[6] = {lV,
+                                 ng > 0 ? lam[(15 + go) * Sm + tid] : 0.0f,
+                                 ng > 1 ? lam[(16 + go) * Sm + tid] : 0.0f,
+                                 lam[(1 + ion) * Sm + tid],
+                                 lam[(8 + ion) * Sm + tid],
+                                 lIt};
+            float lx[6];
+            if (type == 123) adj::vjp_kvdr_f(lo, lx, pV, pG0, pCi, pCo, den, c.area, c.vol, dt, pst);
+            else if (type == 107) adj::vjp_k2p_f(lo, lx, pV, pCi, pCo, den, c.area, c.vol, dt, pst);
+            else adj::vjp_nav_f(lo, lx, pV, pG0, pG1, pCi, pCo, den, c.area, c.vol, dt, type == 142 ? 1 : 0, pst[5]);
+            lV = lx[0];
+            if (ng > 0) lam[(15 + go) * Sm + tid] = lx[1];
+            if (ng > 1) lam[(16 + go) * Sm + tid] = lx[2];
+            lam[(1 + ion) * Sm + tid] = lx[3];
+            lam[(8 + ion) * Sm + tid] = lx[4];
+            gp[cls] += (double)lx[5];
         }
         lam[tid] = lV;
     }
@@ -1091,7 +1075,7 @@ __global__ void __launch_bounds__(kMaxSeg) k_adj_backward(AdjDev d, uint32_t w) 
         }
         __syncthreads();
         tick_fwd(d, c, L, sc, t, rec);
-        if (rec) tick_rev(d, c, L, sc, blk, t, gp);
+        if (rec) tick_rev(d, c, L, sc, t, gp);
     }
     {
         float* dst = d.lam + (size_t)c.p * d.L + c.st_off;

@@ -422,6 +422,160 @@ __device__ __forceinline__ void vjp_receptor(const double* lo, double* lx, int a
     lx[7] = (lIa * P_a * Ga.F + lIb * P_b * Gb.F) * Nk;
 }
 
+// ---- the same products in single precision ----
+// The reverse tick's hot path.  Differences that cancel near zero -- 1 - e^-u in
+// vtrap and in the GHK flux -- are formed with expm1f, so they keep full relative
+// precision; the products agree with the double-precision ones above to ~1e-5.
+struct GhkF { float F, dV, dci, dco; };
+__device__ __forceinline__ GhkF ghk_mono_f(float V, float ci, float co) {
+    const float c1 = (float)(kF * 0.001 / (kR * kT));
+    const float dA = (float)(kF / (kR * kT) * kF * 0.001);
+    const float Vn = V * c1;
+    GhkF r;
+    if (fabsf(Vn) < 1e-6f) { r.F = (float)kF * (ci - co); r.dV = 0.0f; r.dci = (float)kF; r.dco = -(float)kF; return r; }
+    const float A = V * dA;
+    if (Vn > 20.0f) { r.F = A * ci; r.dV = dA * ci; r.dci = A; r.dco = 0.0f; return r; }
+    if (Vn < -20.0f) { r.F = A * co; r.dV = dA * co; r.dci = 0.0f; r.dco = A; return r; }
+    const float D = -expm1f(-Vn);      // 1 - e^-Vn
+    const float e = 1.0f - D;
+    const float Nn = ci - co * e;
+    r.F = A * Nn / D;
+    if (fabsf(Vn) < 1e-2f) {
+        // F = kappa (ci g(Vn) - co g(-Vn)), g(u) = u / (1 - e^-u): the two terms of the
+        // closed-form derivative cancel here, so take g'(u) = 1/2 + u/6 - u^3/180
+        const float kappa = dA / c1;
+        const float g1 = 0.5f + Vn / 6.0f - Vn * Vn * Vn / 180.0f, g2 = 0.5f - Vn / 6.0f + Vn * Vn * Vn / 180.0f;
+        r.dV = c1 * kappa * (ci * g1 + co * g2);
+    } else {
+        r.dV = dA * Nn / D - A * e * c1 * (ci - co) / (D * D);
+    }
+    r.dci = A / D;
+    r.dco = -A * e / D;
+    return r;
+}
+
+// vtrap(x, y) (modifier_helpers.h:132-135) and its derivative in x
+__device__ __forceinline__ void vtrap_f(float x, float y, float* v, float* dv) {
+    const float u = x / y;
+    if (fabsf(u) < 1e-6f) { *v = y * (1.0f - x / (2.0f * y)); *dv = -0.5f; return; }
+    const float D = -expm1f(-u);       // 1 - e^-u
+    *v = x / D;
+    // d/dx = g'(u), g(u) = u / (1 - e^-u); near 0 the closed form cancels
+    *dv = (fabsf(u) < 1e-2f) ? 0.5f + u / 6.0f - u * u * u / 180.0f : (D - u * (1.0f - D)) / (D * D);
+}
+// 1 / (1 + e^z) and its derivative in z
+__device__ __forceinline__ void logistic_f(float z, float* v, float* dv) {
+    const float ez = expf(z);
+    const float den = 1.0f + ez;
+    *v = 1.0f / den;
+    *dv = -ez / (den * den);
+}
+
+__device__ __forceinline__ void vjp_nav_f(const float* lo, float* lx, float V0, float m0, float h0, float cin, float cout,
+                                          float den, float area, double vol, float dt, int is12, float ttx) {
+    const bool mV = V0 >= -200.0f && V0 <= 200.0f;
+    const float V = mV ? V0 : (V0 < -200.0f ? -200.0f : 200.0f);
+    const float cam = is12 ? 23.0f : 43.0f, cah = is12 ? 41.5f : 50.0f, cbh = is12 ? 66.5f : 75.0f,
+                chh = is12 ? 63.5f : 72.0f;
+    float am, dam, bm, dbm, ah, dah, bh, dbh;
+    vtrap_f(V + cam, 6.0f, &am, &dam); am *= 0.182f; dam *= 0.182f;
+    vtrap_f(-(V + cam), 6.0f, &bm, &dbm); bm *= 0.124f; dbm *= -0.124f;
+    vtrap_f(V + cah, 5.0f, &ah, &dah); ah *= 0.024f; dah *= 0.024f;
+    vtrap_f(-(V + cbh), 5.0f, &bh, &dbh); bh *= 0.0091f; dbh *= -0.0091f;
+    const float sm = am + bm, sh = ah + bh;
+    const float minf = am / sm, dminf = (dam * bm - am * dbm) / (sm * sm);
+    const float mtau = 1.0f / sm, dmtau = -(dam + dbm) / (sm * sm);
+    float hinf, dhinf;
+    logistic_f((V + chh) / 6.2f, &hinf, &dhinf);
+    dhinf /= 6.2f;
+    const float htau = 1.0f / sh, dhtau = -(dah + dbh) / (sh * sh);
+    const float Em = expf(-dt / mtau), dEm = Em * dt / (mtau * mtau) * dmtau;
+    const float Eh = expf(-dt / htau), dEh = Eh * dt / (htau * htau) * dhtau;
+    const float mu_ = minf + (m0 - minf) * Em, hu_ = hinf + (h0 - hinf) * Eh;
+    const bool mm = mu_ >= 0.0f && mu_ <= 1.0f, mh = hu_ >= 0.0f && hu_ <= 1.0f;
+    const float mv = mm ? mu_ : (mu_ < 0.0f ? 0.0f : 1.0f), hv = mh ? hu_ : (hu_ < 0.0f ? 0.0f : 1.0f);
+    const float dm_dV = mm ? dminf * (1.0f - Em) + (m0 - minf) * dEm : 0.0f;
+    const float dh_dV = mh ? dhinf * (1.0f - Eh) + (h0 - hinf) * dEh : 0.0f;
+    const float dm_dm = mm ? Em : 0.0f, dh_dh = mh ? Eh : 0.0f;
+    const float cdiv = 1.0f + (ttx > 0.0f ? ttx : 0.0f) / (is12 ? 10.0f : 5.0f);
+    const float open = mv * mv * mv * hv / cdiv;
+    const float do_dm = 3.0f * mv * mv * hv / cdiv, do_dh = mv * mv * mv / cdiv;
+    const float gamma = is12 ? 20.8f : 20.7f;
+    const float Kc = (float)((double)gamma * 1e-12 * (kR * kT) / (kF * kF * (double)55.964f) * 1e12) * area;
+    const GhkF G = ghk_mono_f(V, cin, cout);
+    const float I = Kc * G.F * den * open;
+    const float cpv = (float)(kF * vol / 1000.0);
+    const bool mci = cin - I * dt / cpv >= 1e-9f;
+    const bool mco = cout + I * dt / (cpv * (float)kEVR) >= 1e-9f;
+    const float lI = -lo[5] - (mci ? lo[3] * dt / cpv : 0.0f) + (mco ? lo[4] * dt / (cpv * (float)kEVR) : 0.0f);
+    const float lopen = lI * Kc * G.F * den;
+    const float lF = lI * Kc * den * open;
+    const float lmv = lo[1] + lopen * do_dm, lhv = lo[2] + lopen * do_dh;
+    const float lVc = lo[0] + lF * G.dV + lmv * dm_dV + lhv * dh_dV;
+    lx[0] = mV ? lVc : 0.0f;
+    lx[1] = lmv * dm_dm;
+    lx[2] = lhv * dh_dh;
+    lx[3] = (mci ? lo[3] : 0.0f) + lF * G.dci;
+    lx[4] = (mco ? lo[4] : 0.0f) + lF * G.dco;
+    lx[5] = lI * Kc * G.F * open;
+}
+
+__device__ __forceinline__ void vjp_kvdr_f(const float* lo, float* lx, float V, float n0, float cin, float cout,
+                                           float den, float area, double vol, float dt, const float* st) {
+    const float V_half = (st[1] != 0.0f) ? st[1] : -30.0f;
+    const float k = (st[2] > 0.0f) ? st[2] : 6.0f;
+    float tau, dtau;
+    if (st[4] > 0.0f) { tau = st[4]; dtau = 0.0f; }
+    else {
+        const float t0 = 14.6f * expf(-(V - V_half) / 30.1f);
+        if (t0 < 0.3f) { tau = 0.3f; dtau = 0.0f; }
+        else if (t0 > 200.0f) { tau = 200.0f; dtau = 0.0f; }
+        else { tau = t0; dtau = -t0 / 30.1f; }
+    }
+    float minf, dminf;
+    logistic_f(-(V - V_half) / (k + 1e-6f), &minf, &dminf);
+    dminf *= -1.0f / (k + 1e-6f);
+    const float tt = tau + 1e-6f;
+    const float nu = n0 + (minf - n0) * dt / tt;
+    const bool mn = nu >= 0.0f && nu <= 1.0f;
+    const float nv = mn ? nu : (nu < 0.0f ? 0.0f : 1.0f);
+    const float dn_dV = mn ? (dminf * dt / tt - (minf - n0) * dt * dtau / (tt * tt)) : 0.0f;
+    const float dn_dn = mn ? 1.0f - dt / tt : 0.0f;
+    const float Kc = (float)(12.0 * 1e-12 * (kR * kT) / (kF * kF * (double)40.514f) * 1e12) * area;
+    const GhkF G = ghk_mono_f(V, cin, cout);
+    const float I = Kc * G.F * den * nv;
+    const float cpmv = (float)(kF * vol / 1000.0);
+    const bool mci = cin - I * dt / cpmv >= 1e-9f;
+    const bool mco = cout + I * dt / (cpmv * (float)kEVR) >= 1e-9f;
+    const float lI = -lo[5] - (mci ? lo[3] * dt / cpmv : 0.0f) + (mco ? lo[4] * dt / (cpmv * (float)kEVR) : 0.0f);
+    const float lF = lI * Kc * den * nv;
+    const float lnv = lo[1] + lI * Kc * G.F * den;
+    lx[0] = lo[0] + lF * G.dV + lnv * dn_dV;
+    lx[1] = lnv * dn_dn;
+    lx[2] = 0.0f;
+    lx[3] = (mci ? lo[3] : 0.0f) + lF * G.dci;
+    lx[4] = (mco ? lo[4] : 0.0f) + lF * G.dco;
+    lx[5] = lI * Kc * G.F * nv;
+}
+
+__device__ __forceinline__ void vjp_k2p_f(const float* lo, float* lx, float V, float cin, float cout, float den,
+                                          float area, double vol, float dt, const float* st) {
+    const double gamma = (st[0] > 0.0f) ? (double)st[0] : 100.0;
+    const double Po = (st[1] > 0.0f) ? (double)st[1] : (double)0.012f;
+    const float Kc = (float)((double)(float)gamma * 1e-12 * (kR * kT) / (kF * kF * (double)40.514f) * 1e12 * Po) * area;
+    const GhkF G = ghk_mono_f(V, cin, cout);
+    const float I = Kc * G.F * den;
+    const float cpv = (float)(kF * vol / 1000.0);
+    const bool mco = cout + I * dt / (cpv * (float)kEVR) >= 1e-9f;
+    const float lI = -lo[5] - lo[3] * dt / cpv + (mco ? lo[4] * dt / (cpv * (float)kEVR) : 0.0f);
+    const float lF = lI * Kc * den;
+    lx[0] = lo[0] + lF * G.dV;
+    lx[1] = lx[2] = 0.0f;
+    lx[3] = lo[3] + lF * G.dci;
+    lx[4] = (mco ? lo[4] : 0.0f) + lF * G.dco;
+    lx[5] = lI * Kc * G.F;
+}
+
 // Scharfetter-Gummel Bernoulli function B(x) = x / (e^x - 1) and B'(x) in single
 // precision, one exponential for both; B(-x) = B(x) + x and B'(-x) = -(B'(x) + 1).
 __device__ __forceinline__ void bern_pair(float x, float ex, float* B, float* dB) {
