@@ -44,7 +44,7 @@ NEW_SYMBOLS = ["bnc_netgen_aos", "bnc_netgen_free", "bnc_last_error", "bnc_load_
                "bnc_device_modifier_registered", "bnc_adjoint_create", "bnc_adjoint_destroy", "bnc_adjoint_info",
                "bnc_adjoint_soma", "bnc_adjoint_record", "bnc_adjoint_release_count", "bnc_adjoint_set_params",
                "bnc_adjoint_get_params", "bnc_adjoint_set_target", "bnc_adjoint_forward", "bnc_adjoint_backward",
-               "bnc_adjoint_timings"]
+               "bnc_adjoint_timings", "bnc_sweep_parse_params", "bnc_sweep_apply", "bnc_sweep_run"]
 
 
 class NetInfo(C.Structure):
@@ -158,6 +158,9 @@ def load_library(path=LIB_PATH):
         "bnc_adjoint_get_params": ([vp, u32, vp, vp, vp, vp], i32),
         "bnc_adjoint_set_target": ([vp, vp], i32), "bnc_adjoint_forward": ([vp, vp, vp], i32),
         "bnc_adjoint_backward": ([vp, vp, vp, vp, vp], i32), "bnc_adjoint_timings": ([vp, vp, vp], i32),
+        "bnc_sweep_parse_params": ([C.c_char_p, vp, vp, u32, vp, vp, u32, vp], i32),
+        "bnc_sweep_apply": ([vp, vp], i32),
+        "bnc_sweep_run": ([vp, vp, vp, u32, vp, u32, u32, f32, u32, vp], i32),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -347,7 +350,8 @@ class Backend:
         _check(self.lib.bnc_save_bion(self.h, path.encode()), "bnc_save_bion")
 
 
-__all__ = ["Backend", "Network", "Adjoint", "AdjointConfig", "AdjointInfo", "NetgenParams", "BionData", "BackendError", "load_library", "last_error",
+__all__ = ["Backend", "Network", "Adjoint", "AdjointConfig", "AdjointInfo", "SweepTask", "SweepResult",
+           "sweep_parse_params", "sweep_tasks", "sweep_run", "SWEEP_SINGLE_TICK", "NetgenParams", "BionData", "BackendError", "load_library", "last_error",
            "NET_SMALL", "NET_LARGE", "NET_TREES", "NET_ENSEMBLE_MEMBER", "NET_ADJOINT", "NETGEN_NO_SYNAPSES",
            "NETGEN_NO_CONNECTIONS", "NETGEN_NO_STIMULI", "NETGEN_PERTURB_IONS", "NETGEN_SYNAPSE_EXTRAS", "SEG_FIELDS", "SYN_FIELDS",
            "DROPIN_SYMBOLS", "NEW_SYMBOLS", "EnsembleMember", "Tuning", "BuildOptions", "register_device_modifier", "ensemble_params", "plan_ensemble", "plan_generated"]
@@ -450,3 +454,55 @@ class Adjoint:
         f, b = C.c_float(), C.c_float()
         _check(load_library().bnc_adjoint_timings(self.h, C.byref(f), C.byref(b)), "bnc_adjoint_timings")
         return f.value, b.value
+
+
+SWEEP_SINGLE_TICK = 1
+
+
+class SweepTask(C.Structure):
+    _fields_ = [("type_ids", C.c_void_p), ("values", C.c_void_p), ("n_overrides", C.c_uint32), ("seed", C.c_uint32)]
+
+
+class SweepResult(C.Structure):
+    _fields_ = [("mean_vm", C.c_float), ("spike_count", C.c_uint32), ("synchrony", C.c_float), ("tick", C.c_uint64),
+                ("metrics_json", C.c_char * 2048)]
+
+
+def sweep_parse_params(text, names=None):
+    """The reference's parameter JSON as [(type_id, value), ...] (bnc_sweep_parse_params);
+    `names` maps modifier names to type IDs for non-numeric keys."""
+    import numpy as np
+    names = names or {}
+    nm = (C.c_char_p * max(len(names), 1))(*[k.encode() for k in names])
+    ids = np.array(list(names.values()) or [0], np.uint8)
+    cap = 256
+    tid = np.zeros(cap, np.uint8)
+    val = np.zeros(cap, np.float32)
+    n = C.c_uint32()
+    _check(load_library().bnc_sweep_parse_params(text.encode(), nm, ids.ctypes.data_as(C.c_void_p), len(names),
+                                                 tid.ctypes.data_as(C.c_void_p), val.ctypes.data_as(C.c_void_p),
+                                                 cap, C.byref(n)), "bnc_sweep_parse_params")
+    return [(int(tid[q]), float(val[q])) for q in range(n.value)]
+
+
+def sweep_tasks(tasks):
+    """[(overrides [(type_id, value)], seed), ...] -> (ctypes array of SweepTask, keep-alive arrays)."""
+    import numpy as np
+    keep = []
+    arr = (SweepTask * len(tasks))()
+    for q, (ov, seed) in enumerate(tasks):
+        ids = np.array([t for t, _ in ov] or [0], np.uint8)
+        vals = np.array([v for _, v in ov] or [0.0], np.float32)
+        keep += [ids, vals]
+        arr[q] = SweepTask(ids.ctypes.data_as(C.c_void_p), vals.ctypes.data_as(C.c_void_p), len(ov), seed)
+    return arr, keep
+
+
+def sweep_run(backend, net, tasks, ticks, dt=0.1, single_tick=False):
+    """Runs the tasks as one ensemble in `backend` (bnc_sweep_run); returns the
+    per-task SweepResult list."""
+    arr, keep = sweep_tasks(tasks)
+    res = (SweepResult * len(tasks))()
+    _check(load_library().bnc_sweep_run(backend.h, C.byref(net.data), net.stim_ptr, net.n_stim, arr, len(tasks), ticks,
+                                        C.c_float(dt), SWEEP_SINGLE_TICK if single_tick else 0, res), "bnc_sweep_run")
+    return list(res)

@@ -33,6 +33,7 @@ struct Backend {
     Stimuli stim;
     uint64_t tick = 0;
     uint64_t ticks_run = 0;
+    uint32_t tick_stride = 1;   // the tick counter's step per tick (2: the reference's batch mode)
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     // ensemble members (empty for a single network): ranges in original order
     std::vector<BncEnsembleMember> members;
@@ -306,7 +307,7 @@ static int run_ticks(Backend* b, uint32_t n, float dt) {
     for (uint32_t t = 0; t < n; t++) {
         cudaError_t e = launch_tick(b->dev, b->host, dt, b->tick, b->ticks_run == 0 ? 1 : 0, b->stream);
         if (e != cudaSuccess) { b->failed = true; return cuda_fail(e, "tick launch"); }
-        b->tick++;
+        b->tick += b->tick_stride;
         b->ticks_run++;
     }
     return BNC_OK;
@@ -349,6 +350,7 @@ static int capture_graph(Backend* b, float dt) {
 static int run_ticks_graph(Backend* b, uint32_t n, float dt) {
     if (!b->loaded) { set_error("no network loaded"); return BNC_ERR_STATE; }
     if (b->failed) { set_error("backend is in a failed state after a device error"); return BNC_ERR_STATE; }
+    if (b->tick_stride != 1) return run_ticks(b, n, dt);   // the captured clock steps by one
     cudaSetDevice(b->device);
     const uint32_t reps = n / kGraphTicks;
     if (reps > 0) {
@@ -471,6 +473,12 @@ int backend_export_host(void* sim, HostNet* hn, std::vector<BncCurrentStimulus>*
     *tick = b->tick;
     *device = b->device;
     *n_vclamp = (uint32_t)b->stim.vclamp.size();
+    return BNC_OK;
+}
+
+int backend_set_tick_stride(void* sim, uint32_t stride) {
+    if (!sim || stride == 0) { set_error("null handle or zero stride"); return BNC_ERR_ARG; }
+    static_cast<Backend*>(sim)->tick_stride = stride;
     return BNC_OK;
 }
 

@@ -262,6 +262,9 @@ cudaError_t prepare_synapse(cudaStream_t stream);
 struct HostNet;
 int backend_export_host(void* sim, HostNet* hn, std::vector<BncCurrentStimulus>* stim, uint64_t* tick,
                         int* device, uint32_t* n_vclamp);
+// Steps the tick counter by `stride` per tick (1: the reference tick; 2: its batch mode,
+// daemon_main.cpp:250-258, which increments the counter once more after each tick).
+int backend_set_tick_stride(void* sim, uint32_t stride);
 // Runs `ticks` plain ticks with the release log on; returns each cleft entry as
 // (original synapse index, tick, amount, slot) in the order the kernel wrote them.
 int backend_record_releases(void* sim, uint32_t ticks, float dt, std::vector<uint32_t>* syn,

@@ -323,6 +323,52 @@ int bnc_save_bion(void* sim, const char* filename);
 const char* bnc_last_error(void);
 
 /* ------------------------------------------------------------------ */
+/* 5b. parameter sweeps: many parameterised runs as one ensemble       */
+/* ------------------------------------------------------------------ */
+/* A task of the reference's parameterised runs (daemon_main.cpp:79-300, the batch
+ * mode with --params-json and --seed; daemon_server.cpp:1164-1310, MSG_RUN_TASK_PARAMS):
+ * parameter overrides -- state[0] of each segment's first modifier of the given type
+ * set to the value -- and a seed that scales every synapse's release probability by
+ * 1 + 0.02 * (hash(seed, id) & 0xFFFF) / 65536 (0: no variation). */
+typedef struct {
+    const uint8_t* type_ids;
+    const float* values;
+    uint32_t n_overrides;
+    uint32_t seed;
+} BncSweepTask;
+
+/* core_compute_metrics (simulation_host.cpp:825-880) of one task's final state. */
+typedef struct {
+    float mean_vm;          /* mean V_m over the member's segments, mV */
+    uint32_t spike_count;   /* segments with V_m > -20 mV */
+    float synchrony;        /* fraction of segments within 10 mV of the mean */
+    uint64_t tick;          /* the tick counter after the run */
+    char metrics_json[2048];/* the reference's metrics string, type_vm included */
+} BncSweepResult;
+
+/* Step the tick counter once per tick, as a daemon task does.  Without it the counter
+ * steps twice per tick, as the batch mode's loop does (core_run_tick increments it,
+ * then the loop again, daemon_main.cpp:250-258). */
+#define BNC_SWEEP_SINGLE_TICK 1u
+
+/* The reference's parameter-JSON reader (daemon_main.cpp:79-155): numeric keys are
+ * modifier type IDs (< 212); other keys resolve through the name table (a key that is
+ * a case-insensitive prefix of a name, the lowest ID first), as the plugin
+ * descriptors' names do.  Writes up to cap overrides; *n_out receives the count
+ * (BNC_ERR_ARG if above cap). */
+int bnc_sweep_parse_params(const char* json, const char* const* names, const uint8_t* name_ids, uint32_t n_names,
+                           uint8_t* type_ids, float* values, uint32_t cap, uint32_t* n_out);
+/* Applies one task to a network in place (host arrays). */
+int bnc_sweep_apply(BncBionData* net, const BncSweepTask* task);
+/* Runs every task on its own copy of `base` as one ensemble in `sim` (loaded by the
+ * call; the members are readable afterwards with bnc_ensemble_member and the
+ * bnc_read_*_field calls), `ticks` ticks of `dt`, and writes each task's metrics.
+ * `stim` (may be NULL) applies to every member. */
+int bnc_sweep_run(void* sim, const BncBionData* base, const BncCurrentStimulus* stim, uint32_t n_stim,
+                  const BncSweepTask* tasks, uint32_t n_tasks, uint32_t ticks, float dt, uint32_t flags,
+                  BncSweepResult* results);
+
+/* ------------------------------------------------------------------ */
 /* 6. adjoint: gradients of a somatic voltage-trace loss               */
 /* ------------------------------------------------------------------ */
 /* The forward/backward pair differentiates the tick of simulation_host.cpp:174-657

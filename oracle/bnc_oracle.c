@@ -778,6 +778,15 @@ void bo_run(BoSim* S, uint32_t ticks, float dt) {
     for (uint32_t t = 0; t < ticks; t++) bo_tick(S, dt);
 }
 
+/* The reference's batch loop (daemon_main.cpp:250-258): after each tick the loop
+ * increments the tick counter once more, so tick k runs with counter stride * k. */
+void bo_run_stride(BoSim* S, uint32_t ticks, float dt, uint32_t stride) {
+    for (uint32_t t = 0; t < ticks; t++) {
+        bo_tick(S, dt);
+        S->tick += stride - 1;
+    }
+}
+
 /* Runs `ticks` ticks and records V of the listed segments after every tick
  * into out[t * n_rec + r]. */
 void bo_run_trace(BoSim* S, uint32_t ticks, float dt, const uint32_t* rec, uint32_t n_rec, float* out) {

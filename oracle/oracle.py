@@ -50,6 +50,7 @@ def oracle_lib():
         lib.bo_const.argtypes = [C.c_int]; lib.bo_const.restype = C.c_double
         lib.bo_register_modifier.argtypes = [C.c_uint8, C.c_void_p]; lib.bo_register_modifier.restype = C.c_int
         lib.bo_set_release_log.argtypes = [vp, vp, vp, vp, vp, C.c_uint32]
+        lib.bo_run_stride.argtypes = [vp, C.c_uint32, C.c_float, C.c_uint32]
         lib.bo_release_log_count.argtypes = [vp]; lib.bo_release_log_count.restype = C.c_uint32
         _ora = lib
     return _ora
@@ -93,8 +94,11 @@ class Oracle:
         self.n_seg = net.data.num_segments
         self.n_syn = net.data.num_synapses
 
-    def run(self, ticks, dt):
-        oracle_lib().bo_run(self.h, ticks, C.c_float(dt))
+    def run(self, ticks, dt, tick_stride=1):
+        if tick_stride == 1:
+            oracle_lib().bo_run(self.h, ticks, C.c_float(dt))
+        else:
+            oracle_lib().bo_run_stride(self.h, ticks, C.c_float(dt), tick_stride)
 
     def trace(self, ticks, dt, rec):
         rec = np.ascontiguousarray(rec, np.uint32)
@@ -155,12 +159,13 @@ class Reference:
         self.tick = C.c_uint64(0)
         self.n_stim = C.c_uint32(net.n_stim)
 
-    def run(self, ticks, dt):
+    def run(self, ticks, dt, tick_stride=1):
         d = self.net.data
         for _ in range(ticks):
             self.lib.core_run_tick(d.segments, d.num_segments, d.connections, d.num_connections, d.synapses,
                                    d.num_synapses, 0, C.byref(self.tick), C.c_float(dt), self.net.stim_ptr,
                                    C.byref(self.n_stim), *([None] * 10))
+            self.tick.value += tick_stride - 1   # the batch mode's second increment
 
     def trace(self, ticks, dt, rec):
         out = np.empty((ticks, len(rec)), np.float64)
