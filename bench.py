@@ -58,6 +58,9 @@ def parse_args():
     ap.add_argument("--trees", type=int, default=16384)
     ap.add_argument("--tree-ticks", type=int, default=20)
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-sweep", action="store_true")
+    ap.add_argument("--sweep-tasks", type=int, default=256)
+    ap.add_argument("--sweep-ticks", type=int, default=1000)
     ap.add_argument("--adj-neurons", type=int, default=256)
     ap.add_argument("--adj-sets", type=int, default=64)
     ap.add_argument("--adj-ticks", type=int, default=1024)
@@ -342,6 +345,52 @@ def run_adjoint(a, device):
     }
 
 
+def run_sweep(a, device):
+    """Parameter sweep: a.sweep_tasks parameterised runs of one 64-neuron network (2,048
+    segments, 400 synapses) as one ensemble (bnc_sweep_run), each task with its own K2P
+    conductance and Kv gate overrides and release seed, a.sweep_ticks ticks of 0.1 ms
+    with the reference batch mode's tick counter.  Timed end to end by wall clock: host
+    network in, per-task metrics out.  The reference runs such tasks one process each;
+    its CPU tick is timed on a bounded sample of one task."""
+    import numpy as np
+    from bioneuroncore_b200 import Backend, Network, NetgenParams, NET_SMALL, sweep_run
+    spec = dict(family=NET_SMALL, n_neurons=64, seed=a.seed, stim_pA=3000.0, stim_duration_ms=10.0)
+    base = Network(NetgenParams(**spec))
+    rng = np.random.default_rng(a.seed)
+    tasks = [([(107, float(rng.uniform(50.0, 150.0))), (123, float(rng.uniform(0.0, 0.3)))], int(q + 1))
+             for q in range(a.sweep_tasks)]
+    b = Backend(device)
+    sweep_run(b, base, tasks[:2], 10, 0.1)                    # warm-up: module load, constant tables
+    t0 = time.perf_counter()
+    res = sweep_run(b, base, tasks, a.sweep_ticks, 0.1)
+    wall = time.perf_counter() - t0
+    b.close()
+    seg_ticks = float(base.data.num_segments) * a.sweep_tasks * a.sweep_ticks
+    cpu = None
+    try:
+        from oracle.oracle import Reference, reference_available
+        if reference_available():
+            net = Network(NetgenParams(**spec))
+            ref = Reference(net)
+            n_cpu = 20
+            c0 = time.perf_counter()
+            ref.run(n_cpu, 0.1, tick_stride=2)
+            per_tick = (time.perf_counter() - c0) / n_cpu
+            cpu = {"seconds_per_task": per_tick * a.sweep_ticks, "cores": 1,
+                   "sweep_seconds_one_process_per_task": per_tick * a.sweep_ticks * a.sweep_tasks,
+                   "sample": "%d ticks of one task (reference core_run_tick, FP64 state)" % n_cpu}
+    except Exception as exc:
+        cpu = {"unavailable": str(exc)[:200]}
+    return {
+        "workload": "%d tasks x 64 neurons (%d segments each), %d ticks of 0.1 ms, batch-mode tick counter"
+                    % (a.sweep_tasks, base.data.num_segments, a.sweep_ticks),
+        "seconds": wall, "tasks_per_s": a.sweep_tasks / wall, "segment_ticks_per_s": seg_ticks / wall,
+        "timing": "wall clock of bnc_sweep_run: copies, build, tick loop, metrics",
+        "spike_count_mean": float(np.mean([r.spike_count for r in res])),
+        "cpu_reference": cpu,
+    }
+
+
 def main():
     a = parse_args()
     if a.impl == "reference":
@@ -421,6 +470,11 @@ def main():
         b.close()
         trees = run_trees(a, local_rank if world > 1 else 0)
 
+    sweep = None
+    if not a.no_sweep:
+        b.close()
+        sweep = run_sweep(a, local_rank if world > 1 else 0)
+
     adjoint = None
     if not a.no_adjoint:
         b.close()
@@ -447,7 +501,7 @@ def main():
                        "tiles": info.n_tiles, "phases": info.n_phases, "setup_s": round(setup_s, 1)},
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,
             "gpu_launches": (info.n_phases + 3) * a.steps, "ensemble": ensemble, "trees": trees,
-            "adjoint": adjoint,
+            "adjoint": adjoint, "sweep": sweep,
         }
         print(json.dumps(line), flush=True)
     b.close()
