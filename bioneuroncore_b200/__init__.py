@@ -44,7 +44,8 @@ NEW_SYMBOLS = ["bnc_netgen_aos", "bnc_netgen_free", "bnc_last_error", "bnc_load_
                "bnc_device_modifier_registered", "bnc_adjoint_create", "bnc_adjoint_destroy", "bnc_adjoint_info",
                "bnc_adjoint_soma", "bnc_adjoint_record", "bnc_adjoint_release_count", "bnc_adjoint_set_params",
                "bnc_adjoint_get_params", "bnc_adjoint_set_target", "bnc_adjoint_forward", "bnc_adjoint_backward",
-               "bnc_adjoint_timings", "bnc_sweep_parse_params", "bnc_sweep_apply", "bnc_sweep_run"]
+               "bnc_adjoint_timings", "bnc_sweep_parse_params", "bnc_sweep_apply", "bnc_sweep_run",
+               "bnc_save_checkpoint", "bnc_load_checkpoint"]
 
 
 class NetInfo(C.Structure):
@@ -161,6 +162,7 @@ def load_library(path=LIB_PATH):
         "bnc_sweep_parse_params": ([C.c_char_p, vp, vp, u32, vp, vp, u32, vp], i32),
         "bnc_sweep_apply": ([vp, vp], i32),
         "bnc_sweep_run": ([vp, vp, vp, u32, vp, u32, u32, f32, u32, vp], i32),
+        "bnc_save_checkpoint": ([vp, C.c_char_p], i32), "bnc_load_checkpoint": ([vp, C.c_char_p], i32),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -345,6 +347,12 @@ class Backend:
     def set_synapse_scale(self, scale):
         s = np.ascontiguousarray(scale, np.float32)
         _check(self.lib.bnc_set_synapse_scale(self.h, s.ctypes.data, s.size), "bnc_set_synapse_scale")
+
+    def save_checkpoint(self, path):
+        _check(self.lib.bnc_save_checkpoint(self.h, str(path).encode()), "bnc_save_checkpoint")
+
+    def load_checkpoint(self, path):
+        _check(self.lib.bnc_load_checkpoint(self.h, str(path).encode()), "bnc_load_checkpoint")
 
     def save_bion(self, path):
         _check(self.lib.bnc_save_bion(self.h, path.encode()), "bnc_save_bion")

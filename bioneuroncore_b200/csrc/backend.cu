@@ -1131,6 +1131,142 @@ int bnc_save_bion(void* sim, const char* filename) {
     return save_bion(b->aos, filename);
 }
 
+// ---- Checkpoints: the .bion plus what it does not hold ----
+// The .bion records the AoS state.  A run also carries the tick counter (it seeds the
+// release draws and times the stimuli), whether the first tick has run, the stimuli,
+// the per-synapse receptor density scales and the pending delayed releases
+// (delay_buffer.h:15-64).  The sidecar `<path>.state` holds them, so a loaded
+// checkpoint continues bit for bit.
+namespace {
+const char kStateMagic[8] = {'B', 'N', 'C', 'S', 'T', 'A', 'T', 'E'};
+constexpr uint32_t kStateVersion = 1;
+struct DelaySlot {
+    unsigned long long arrival;
+    float amount;
+    uint8_t nt, pad[3];
+};
+}  // namespace
+
+int bnc_save_checkpoint(void* sim, const char* path) {
+    if (!sim || !path) { set_error("null argument"); return BNC_ERR_ARG; }
+    Backend* b = static_cast<Backend*>(sim);
+    if (!b->loaded) { set_error("no network loaded"); return BNC_ERR_STATE; }
+    if (!b->members.empty()) { set_error("checkpoints hold one network, not an ensemble"); return BNC_ERR_UNSUPPORTED; }
+    int rc = bnc_save_bion(sim, path);
+    if (rc != BNC_OK) return rc;
+    const NetDev& d = b->dev;
+    const uint32_t K = d.n_syn;
+    const uint32_t KS = b->host.n_syn_total;
+    std::vector<float> scale_dev, scale(KS, 1.0f);
+    if (K && !d2h(scale_dev, d.sy_scale, K)) return cuda_fail(cudaGetLastError(), "checkpoint read");
+    for (uint32_t k = 0; k < K; k++) scale[b->host.syn_orig[k]] = scale_dev[k];
+    std::vector<DelaySlot> slots;
+    uint32_t has_delay = d.dl_arr ? 1u : 0u;
+    if (has_delay) {
+        std::vector<unsigned long long> arr;
+        std::vector<float> amt;
+        std::vector<uint8_t> nt;
+        if (!d2h(arr, d.dl_arr, (size_t)4 * K) || !d2h(amt, d.dl_amt, (size_t)4 * K) || !d2h(nt, d.dl_nt, (size_t)4 * K))
+            return cuda_fail(cudaGetLastError(), "checkpoint read");
+        slots.assign((size_t)4 * KS, DelaySlot{0, 0.0f, 0, {0, 0, 0}});
+        for (uint32_t k = 0; k < K; k++)
+            for (int q = 0; q < 4; q++) {
+                DelaySlot& sl = slots[(size_t)b->host.syn_orig[k] * 4 + q];
+                sl.arrival = arr[(size_t)q * K + k];
+                sl.amount = amt[(size_t)q * K + k];
+                sl.nt = nt[(size_t)q * K + k];
+            }
+    }
+    const std::string sp = std::string(path) + ".state";
+    FILE* f = fopen(sp.c_str(), "wb");
+    if (!f) { set_error("cannot write %s", sp.c_str()); return BNC_BION_ERR_FILE_OPEN; }
+    const uint32_t n_cur = (uint32_t)b->stim.current.size(), n_vc = (uint32_t)b->stim.vclamp.size();
+    const uint32_t head[6] = {kStateVersion, b->host.n_seg, KS, n_cur, n_vc, has_delay};
+    const uint64_t ticks[2] = {b->tick, b->ticks_run};
+    bool ok = fwrite(kStateMagic, 1, 8, f) == 8 && fwrite(head, sizeof(head), 1, f) == 1 && fwrite(ticks, sizeof(ticks), 1, f) == 1;
+    if (ok && n_cur) ok = fwrite(b->stim.current.data(), sizeof(BncCurrentStimulus), n_cur, f) == n_cur;
+    if (ok && n_vc) ok = fwrite(b->stim.vclamp.data(), sizeof(BncVoltageClamp), n_vc, f) == n_vc;
+    if (ok && KS) ok = fwrite(scale.data(), sizeof(float), KS, f) == KS;
+    if (ok && has_delay && KS) ok = fwrite(slots.data(), sizeof(DelaySlot), slots.size(), f) == slots.size();
+    if (fclose(f) != 0) ok = false;
+    if (!ok) { set_error("write error on %s", sp.c_str()); return BNC_BION_ERR_WRITE_FAIL; }
+    return BNC_OK;
+}
+
+int bnc_load_checkpoint(void* sim, const char* path) {
+    if (!sim || !path) { set_error("null argument"); return BNC_ERR_ARG; }
+    Backend* b = static_cast<Backend*>(sim);
+    const std::string sp = std::string(path) + ".state";
+    FILE* f = fopen(sp.c_str(), "rb");
+    if (!f) { set_error("cannot read %s", sp.c_str()); return BNC_BION_ERR_FILE_OPEN; }
+    char magic[8];
+    uint32_t head[6];
+    uint64_t ticks[2];
+    bool ok = fread(magic, 1, 8, f) == 8 && std::memcmp(magic, kStateMagic, 8) == 0 && fread(head, sizeof(head), 1, f) == 1 &&
+              head[0] == kStateVersion && fread(ticks, sizeof(ticks), 1, f) == 1;
+    Stimuli stim;
+    std::vector<float> scale;
+    std::vector<DelaySlot> slots;
+    if (ok) {
+        stim.current.resize(head[3]);
+        stim.vclamp.resize(head[4]);
+        scale.resize(head[2]);
+        if (head[3]) ok = fread(stim.current.data(), sizeof(BncCurrentStimulus), head[3], f) == head[3];
+        if (ok && head[4]) ok = fread(stim.vclamp.data(), sizeof(BncVoltageClamp), head[4], f) == head[4];
+        if (ok && head[2]) ok = fread(scale.data(), sizeof(float), head[2], f) == head[2];
+        if (ok && head[5] && head[2]) {
+            slots.resize((size_t)4 * head[2]);
+            ok = fread(slots.data(), sizeof(DelaySlot), slots.size(), f) == slots.size();
+        }
+    }
+    fclose(f);
+    if (!ok) { set_error("%s is not a checkpoint state file of this version", sp.c_str()); return BNC_ERR_FORMAT; }
+    b->reset_network();
+    BncBionData aos;
+    int rc = load_bion_file(path, &aos);
+    if (rc != BNC_OK) return rc;
+    if (aos.num_segments != head[1] || aos.num_synapses != head[2]) {
+        free_aos_arrays(aos);
+        set_error("checkpoint state does not match %s", path);
+        return BNC_ERR_FORMAT;
+    }
+    b->stim = stim;
+    rc = load_common(b, aos, true);
+    if (rc != BNC_OK) { free_aos_arrays(aos); return rc; }
+    b->tick = ticks[0];
+    b->ticks_run = ticks[1];
+    const NetDev& d = b->dev;
+    const uint32_t K = d.n_syn;
+    if (K) {
+        std::vector<float> sdev(K);
+        for (uint32_t k = 0; k < K; k++) sdev[k] = scale[b->host.syn_orig[k]];
+        if (cudaMemcpy(d.sy_scale, sdev.data(), K * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess)
+            return cuda_fail(cudaGetLastError(), "checkpoint upload");
+    }
+    if (!slots.empty()) {
+        if (!d.dl_arr) {
+            for (const DelaySlot& sl : slots)
+                if (sl.arrival) { set_error("pending delayed releases, but the network has no delays"); return BNC_ERR_FORMAT; }
+        } else {
+            std::vector<unsigned long long> arr((size_t)4 * K);
+            std::vector<float> amt((size_t)4 * K);
+            std::vector<uint8_t> nt((size_t)4 * K);
+            for (uint32_t k = 0; k < K; k++)
+                for (int q = 0; q < 4; q++) {
+                    const DelaySlot& sl = slots[(size_t)b->host.syn_orig[k] * 4 + q];
+                    arr[(size_t)q * K + k] = sl.arrival;
+                    amt[(size_t)q * K + k] = sl.amount;
+                    nt[(size_t)q * K + k] = sl.nt;
+                }
+            if (cudaMemcpy(d.dl_arr, arr.data(), arr.size() * sizeof(unsigned long long), cudaMemcpyHostToDevice) != cudaSuccess ||
+                cudaMemcpy(d.dl_amt, amt.data(), amt.size() * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess ||
+                cudaMemcpy(d.dl_nt, nt.data(), nt.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+                return cuda_fail(cudaGetLastError(), "checkpoint upload");
+        }
+    }
+    return BNC_OK;
+}
+
 }  // extern "C"
 
 // ---- Ticks with the presynaptic exchange records in a library-owned array ----

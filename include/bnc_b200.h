@@ -322,6 +322,17 @@ int bnc_save_bion(void* sim, const char* filename);
 /* Message for the last error on this thread ("" when none). */
 const char* bnc_last_error(void);
 
+/* Checkpoints that resume bit for bit.  The .bion (bion_loader_host.cpp:26-504)
+ * records the AoS state; a running simulation also carries the tick counter (it seeds
+ * the release draws, simulation_host.cpp:438-459, and times the stimuli), whether its
+ * first tick has run, its stimuli, the receptor density scales
+ * (bnc_set_synapse_scale) and the pending delayed releases (delay_buffer.h:15-64).
+ * bnc_save_checkpoint writes `path` (.bion) and `path`.state with those;
+ * bnc_load_checkpoint loads both, and the next tick continues the saved run exactly.
+ * Single networks only (BNC_ERR_UNSUPPORTED for an ensemble). */
+int bnc_save_checkpoint(void* sim, const char* path);
+int bnc_load_checkpoint(void* sim, const char* path);
+
 /* ------------------------------------------------------------------ */
 /* 5b. parameter sweeps: many parameterised runs as one ensemble       */
 /* ------------------------------------------------------------------ */

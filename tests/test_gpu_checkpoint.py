@@ -1,0 +1,60 @@
+"""Checkpoints (bnc_save_checkpoint / bnc_load_checkpoint): a run saved half way and
+loaded into a fresh backend continues bit for bit as the uninterrupted run.  The
+network has transmission delays, readily releasable pools and presynaptic
+autoreceptors (BNC_NETGEN_SYNAPSE_EXTRAS), so pending delayed releases and the tick
+counter that seeds the release draws must both survive the checkpoint."""
+import numpy as np
+import pytest
+
+from bioneuroncore_b200 import Backend, Network, NetgenParams, NET_SMALL, BackendError
+
+pytestmark = pytest.mark.gpu
+
+DT = 0.025
+SEG_FIELDS = [("V", 0), ("ATP", 0)] + [("ion_in", q) for q in range(7)] + [("ion_out", q) for q in range(7)] + \
+             [("neurotransmitter", q) for q in (0, 1)] + [("mod_state", q) for q in (0, 1, 8, 9)]
+SYN_FIELDS = ["weight", "bouton_Ca", "spine_Ca", "RRP", "cleft", "refractory", "receptor_state"]
+
+
+def _state(b):
+    out = {"%s[%d]" % f: np.asarray(b.segment_field(*f), np.float32) for f in SEG_FIELDS}
+    out.update({f: np.asarray(b.synapse_field(f), np.float32) for f in SYN_FIELDS})
+    return out
+
+
+def _same(x, y):
+    for k in x:
+        eq = x[k].view(np.uint32) == y[k].view(np.uint32)
+        assert eq.all(), "%s: %d values differ" % (k, int((~eq).sum()))
+
+
+def test_checkpoint_resumes_bit_for_bit(tmp_path):
+    p = NetgenParams(family=NET_SMALL, n_neurons=8, seed=7, flags=32)
+    whole = Backend()
+    whole.load_network(Network(p))
+    whole.run_ticks(800, DT)
+    half = Backend()
+    half.load_network(Network(p))
+    half.run_ticks(400, DT)
+    path = tmp_path / "run.bion"
+    half.save_checkpoint(path)
+    assert path.exists() and (tmp_path / "run.bion.state").exists()
+    resumed = Backend()
+    resumed.load_checkpoint(path)
+    resumed.run_ticks(400, DT)
+    _same(_state(whole), _state(resumed))
+    # the .bion alone restarts the tick counter and drops the pending releases
+    plain = Backend()
+    plain.load_bion(str(path))
+    plain.run_ticks(400, DT)
+    a, c = _state(whole), _state(plain)
+    assert any((a[k].view(np.uint32) != c[k].view(np.uint32)).any() for k in a)
+
+
+def test_checkpoint_errors(tmp_path):
+    b = Backend()
+    with pytest.raises(BackendError):
+        b.load_checkpoint(tmp_path / "missing.bion")
+    (tmp_path / "bad.bion.state").write_bytes(b"not a state file")
+    with pytest.raises(BackendError):
+        b.load_checkpoint(tmp_path / "bad.bion")
