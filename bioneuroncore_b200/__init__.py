@@ -45,7 +45,7 @@ NEW_SYMBOLS = ["bnc_netgen_aos", "bnc_netgen_free", "bnc_last_error", "bnc_load_
                "bnc_adjoint_soma", "bnc_adjoint_record", "bnc_adjoint_release_count", "bnc_adjoint_set_params",
                "bnc_adjoint_get_params", "bnc_adjoint_set_target", "bnc_adjoint_forward", "bnc_adjoint_backward",
                "bnc_adjoint_timings", "bnc_sweep_parse_params", "bnc_sweep_apply", "bnc_sweep_run",
-               "bnc_save_checkpoint", "bnc_load_checkpoint"]
+               "bnc_save_checkpoint", "bnc_load_checkpoint", "bnc_state_frame"]
 
 
 class NetInfo(C.Structure):
@@ -163,6 +163,7 @@ def load_library(path=LIB_PATH):
         "bnc_sweep_apply": ([vp, vp], i32),
         "bnc_sweep_run": ([vp, vp, vp, u32, vp, u32, u32, f32, u32, vp], i32),
         "bnc_save_checkpoint": ([vp, C.c_char_p], i32), "bnc_load_checkpoint": ([vp, C.c_char_p], i32),
+        "bnc_state_frame": ([vp, vp, C.c_uint64, vp], i32),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -347,6 +348,14 @@ class Backend:
     def set_synapse_scale(self, scale):
         s = np.ascontiguousarray(scale, np.float32)
         _check(self.lib.bnc_set_synapse_scale(self.h, s.ctypes.data, s.size), "bnc_set_synapse_scale")
+
+    def state_frame(self):
+        """The daemon's state-frame payload (bytes) from the device state."""
+        n = C.c_uint64()
+        self.lib.bnc_state_frame(self.h, None, 0, C.byref(n))
+        buf = (C.c_uint8 * n.value)()
+        _check(self.lib.bnc_state_frame(self.h, buf, n.value, C.byref(n)), "bnc_state_frame")
+        return bytes(buf)
 
     def save_checkpoint(self, path):
         _check(self.lib.bnc_save_checkpoint(self.h, str(path).encode()), "bnc_save_checkpoint")

@@ -1131,6 +1131,36 @@ int bnc_save_bion(void* sim, const char* filename) {
     return save_bion(b->aos, filename);
 }
 
+// ---- The daemon's state frame (daemon_state.cpp:66-79) from the device state ----
+int bnc_state_frame(void* sim, void* buf, uint64_t cap, uint64_t* len) {
+    if (!sim || !len) { set_error("null argument"); return BNC_ERR_ARG; }
+    Backend* b = static_cast<Backend*>(sim);
+    if (!b->loaded) { set_error("no network loaded"); return BNC_ERR_STATE; }
+    if (!b->owns_aos || !b->aos.segments) { set_error("no host AoS view (network was generated on the device)"); return BNC_ERR_STATE; }
+    const uint32_t N = b->aos.num_segments, K = b->aos.num_synapses;
+    const uint64_t need = 16ull + (uint64_t)N * sizeof(BncSegment) + (uint64_t)K * sizeof(BncSynapse);
+    *len = need;
+    if (!buf || cap < need) { set_error("frame needs %llu bytes", (unsigned long long)need); return BNC_ERR_ARG; }
+    uint8_t* p = static_cast<uint8_t*>(buf);
+    // the records' static fields from the host copy, then the device state written over
+    // them in place
+    BncBionData view = b->aos;
+    view.segments = reinterpret_cast<BncSegment*>(p + 16);
+    view.synapses = reinterpret_cast<BncSynapse*>(p + 16 + (size_t)N * sizeof(BncSegment));
+    std::memcpy(view.segments, b->aos.segments, (size_t)N * sizeof(BncSegment));
+    if (K) std::memcpy(view.synapses, b->aos.synapses, (size_t)K * sizeof(BncSynapse));
+    cudaSetDevice(b->device);
+    int rc = sync_stream(b);
+    if (rc != BNC_OK) return rc;
+    rc = export_network(b->dev, b->host, b->ticks_run, &view);
+    if (rc != BNC_OK) return rc;
+    const uint64_t tick = b->tick;
+    std::memcpy(p, &tick, 8);
+    std::memcpy(p + 8, &N, 4);
+    std::memcpy(p + 12, &K, 4);
+    return BNC_OK;
+}
+
 // ---- Checkpoints: the .bion plus what it does not hold ----
 // The .bion records the AoS state.  A run also carries the tick counter (it seeds the
 // release draws and times the stimuli), whether the first tick has run, the stimuli,

@@ -322,6 +322,13 @@ int bnc_save_bion(void* sim, const char* filename);
 /* Message for the last error on this thread ("" when none). */
 const char* bnc_last_error(void);
 
+/* The daemon's MSG_STATE_FRAME payload (daemon_state.cpp:66-79): the tick counter
+ * (u64), the segment and synapse counts (u32 each), then the Segment and Synapse
+ * records of the current state, filled from the device state directly into `buf`.
+ * *len receives the frame's size; BNC_ERR_ARG when buf is NULL or cap is smaller
+ * (a size query). */
+int bnc_state_frame(void* sim, void* buf, uint64_t cap, uint64_t* len);
+
 /* Checkpoints that resume bit for bit.  The .bion (bion_loader_host.cpp:26-504)
  * records the AoS state; a running simulation also carries the tick counter (it seeds
  * the release draws, simulation_host.cpp:438-459, and times the stimuli), whether its

@@ -58,3 +58,26 @@ def test_checkpoint_errors(tmp_path):
     (tmp_path / "bad.bion.state").write_bytes(b"not a state file")
     with pytest.raises(BackendError):
         b.load_checkpoint(tmp_path / "bad.bion")
+
+
+def test_state_frame_is_the_daemon_layout():
+    """bnc_state_frame: tick, counts and the Segment/Synapse records of the current state,
+    byte for byte the records of the synced host arrays (the daemon's frame,
+    daemon_state.cpp:66-79)."""
+    import ctypes as C
+    import struct
+    from bioneuroncore_b200 import BionData
+    p = NetgenParams(family=NET_SMALL, n_neurons=4, seed=3)
+    b = Backend()
+    b.load_network(Network(p))
+    b.run_ticks(37, DT)
+    frame = b.state_frame()
+    tick, n_seg, n_syn = struct.unpack_from("<QII", frame, 0)
+    assert tick == 37
+    b.sync_to_host()
+    d = C.cast(b.lib.gpu_backend_bion_data(b.h), C.POINTER(BionData)).contents
+    seg_bytes = C.string_at(d.segments, n_seg * 3216)
+    syn_bytes = C.string_at(d.synapses, n_syn * 1568)
+    assert n_seg == d.num_segments and n_syn == d.num_synapses
+    assert frame[16:16 + len(seg_bytes)] == seg_bytes
+    assert frame[16 + len(seg_bytes):] == syn_bytes
