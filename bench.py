@@ -500,7 +500,7 @@ def main():
                        "l2": "inputs larger than L2 (device state ~8 GB per GPU)",
                        "tiles": info.n_tiles, "phases": info.n_phases, "setup_s": round(setup_s, 1)},
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,
-            "gpu_launches": (info.n_phases + 3) * a.steps, "ensemble": ensemble, "trees": trees,
+            "gpu_launches": (info.modifier_launches + 2) * a.steps, "ensemble": ensemble, "trees": trees,
             "adjoint": adjoint, "sweep": sweep,
         }
         print(json.dumps(line), flush=True)

@@ -660,6 +660,7 @@ static BuildOptions to_options(const BncBuildOptions* o) {
         if (o->tile_segs) opt.tile_segs = o->tile_segs;
         opt.phase_cap = o->phase_cap;
         if (o->chunk_segs) opt.chunk_segs = o->chunk_segs;
+        if (o->fuse_phases) opt.fuse_phases = o->fuse_phases;
     }
     return opt;
 }
@@ -700,6 +701,7 @@ static int plan_info(const HostNet& hn, const Stimuli& stim, BncNetInfo* info,
     info->tile_bytes_per_tick = host.tile_bytes; info->synapse_kernel_bytes_per_tick = host.synk_bytes;
     info->warp_cap = host.opt.warp_cap; info->tile_segs = host.opt.tile_segs;
     info->modifier_kernel_bytes = host.mod_bytes; info->diffusion_kernel_bytes = host.diff_bytes;
+    info->modifier_launches = modifier_launches(dev, host); info->fuse_phases = host.fuse;
     return BNC_OK;
 }
 
@@ -1117,6 +1119,7 @@ int bnc_network_info(void* sim, BncNetInfo* info) {
     info->syn_bytes_per_tick = b->host.syn_bytes;
     info->tile_bytes_per_tick = b->host.tile_bytes;
     info->synapse_kernel_bytes_per_tick = b->host.synk_bytes;
+    info->modifier_launches = modifier_launches(d, b->host); info->fuse_phases = b->host.fuse;
     info->warp_cap = b->host.opt.warp_cap; info->tile_segs = b->host.opt.tile_segs;
     info->modifier_kernel_bytes = b->host.mod_bytes; info->diffusion_kernel_bytes = b->host.diff_bytes;
     return BNC_OK;

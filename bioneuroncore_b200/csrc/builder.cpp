@@ -663,8 +663,73 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
             bucket_off[(size_t)(d / chunk_segs) * n_phases + item_phase[k] + 1]++;
     }
     for (size_t b = 0; b < NB; b++) bucket_off[b + 1] += bucket_off[b];
+    // Fused phase groups: F consecutive phases run in one launch, one thread per segment
+    // running its items of those phases in order with the step-1 record in registers.
+    // That needs every segment's items in phases 0..c-1 (the slot-order schedule), so
+    // that the segments with an item in phase p0 + j are the first rows of the group
+    // once rows are sorted by their item count, and item (row r, phase p0 + j) sits at
+    // bucket_off[p0 + j] + r.  Rows are sorted by (count descending, the types of their
+    // items) so that warps run one sequence of models.
+    uint32_t fuse = std::min<uint32_t>(std::max<uint32_t>(opt.fuse_phases, 1u), kMaxFuse);
+    if (n_chunks != 1 || n_phases < 2) fuse = 1;
+    for (uint32_t i = 0; i < n && fuse > 1; i++)
+        for (uint32_t k = act_off[i]; k < act_off[i + 1]; k++)
+            if (item_phase[k] != k - act_off[i] || user_type[act_type[k]]) { fuse = 1; break; }
+    host->fuse = fuse;
     std::vector<ItemKey> keys(act_slot.size());
-    {
+    if (fuse > 1) {
+        uint32_t rank[256];
+        uint32_t R = 0;
+        {
+            bool seen[256] = {false};
+            for (uint8_t t : act_type) seen[t] = true;
+            for (int t = 0; t < 256; t++) rank[t] = seen[t] ? ++R : 0u;   // 1..R; 0: no item
+        }
+        std::vector<uint32_t> rows, tmp, cnt;
+        for (uint32_t p0 = 0; p0 < n_phases; p0 += fuse) {
+            const uint32_t F = std::min(fuse, n_phases - p0);
+            rows.clear();
+            for (uint32_t d = 0; d < n; d++)   // device order: the order inside a class
+                if (act_off[host->perm[d] + 1] - act_off[host->perm[d]] > p0) rows.push_back(d);
+            if (rows.size() != bucket_off[p0 + 1] - bucket_off[p0]) {
+                set_error("fused phase schedule: phase %u holds %zu items, %zu segments reach it", p0,
+                          (size_t)(bucket_off[p0 + 1] - bucket_off[p0]), rows.size());
+                return BNC_ERR_FORMAT;
+            }
+            // stable counting sorts, least significant first: the type of each item from
+            // the last phase of the group to the first, then the item count (descending)
+            auto key_of = [&](uint32_t d, uint32_t j) -> uint32_t {   // j == F: the count key
+                const uint32_t i = host->perm[d];
+                const uint32_t m = std::min(F, act_off[i + 1] - act_off[i] - p0);
+                if (j == F) return F - m;
+                return j < m ? rank[act_type[act_off[i] + p0 + j]] : 0u;
+            };
+            tmp.resize(rows.size());
+            for (int pass = (int)F - 1; pass >= -1; pass--) {
+                const uint32_t j = pass < 0 ? F : (uint32_t)pass;
+                const uint32_t nb = (j == F ? F : R) + 2;
+                cnt.assign(nb, 0u);
+                for (uint32_t d : rows) cnt[key_of(d, j) + 1]++;
+                for (uint32_t c = 0; c + 1 < nb; c++) cnt[c + 1] += cnt[c];
+                for (uint32_t d : rows) tmp[cnt[key_of(d, j)]++] = d;
+                rows.swap(tmp);
+            }
+            for (uint32_t r = 0; r < (uint32_t)rows.size(); r++) {
+                const uint32_t d = rows[r];
+                const uint32_t i = host->perm[d];
+                const uint32_t m = std::min(F, act_off[i + 1] - act_off[i] - p0);
+                for (uint32_t j = 0; j < m; j++) {
+                    const uint32_t k = act_off[i] + p0 + j;
+                    const uint32_t pos = bucket_off[p0 + j] + r;
+                    if (pos >= bucket_off[p0 + j + 1]) {
+                        set_error("fused phase schedule: row %u has no slot in phase %u", r, p0 + j);
+                        return BNC_ERR_FORMAT;
+                    }
+                    keys[pos] = {(uint16_t)(p0 + j), act_type[k], d, k};
+                }
+            }
+        }
+    } else {
         std::vector<uint32_t> pos(bucket_off.begin(), bucket_off.end() - 1);
         for (uint32_t d = 0; d < n; d++) {   // device order: each bucket fills in segment order
             uint32_t i = host->perm[d];

@@ -11,6 +11,9 @@
 //                SMs at any moment -- run few channel models at a time, which keeps the
 //                many models' code within the instruction caches.  Each dispatch case
 //                loads and stores only the record fields its model uses.
+//  k_phase_group the same phases two or three to a launch (slot-order schedules): one
+//                thread per segment runs its items of those phases on the record held
+//                in registers, so the record crosses HBM once per group.
 //  k_diffusion   (diffuse.cu) stimuli, step 2.5 electrodiffusion, the presynaptic record.
 //  k_synapse     (synapse.cu) steps 3 and 4.
 #define BNC_MATH_OUTLINE 1   // 26 channel models in one kernel: keep exp/log out of line
@@ -18,6 +21,10 @@
 #include <cuda_runtime.h>
 #include "net.h"
 #include "physics.cuh"
+
+#ifndef BNC_GROUP_MIN_CTAS
+#define BNC_GROUP_MIN_CTAS 4
+#endif
 
 namespace bnc {
 
@@ -155,6 +162,114 @@ k_phase(NetDev d, float dt, uint32_t b, uint32_t e) {
     if (type == 140) d.c21_cur[g] = make_float2(m.den, m.st[1]);
 }
 
+// run_item on a segment held in registers: the same models in the same order, the GHK
+// factors computed from the V the item starts with, as rec_load computes them.
+template <bool kDef>
+__device__ __forceinline__ double run_item_s(uint8_t type, DMod& m, DSeg& s, float dt, float glu, float gaba,
+                                             float gly) {
+    double I = 0.0;
+    switch (type) {
+#define BNC_ITEM(T, CALL)            \
+    case T: {                        \
+        ghk_cache_fill(s.gc, s.V);   \
+        m.area = s.area;             \
+        I = (CALL);                  \
+        break;                       \
+    }
+        BNC_ITEM(1, dp_cav13_current<kDef>(m, s, dt))
+        BNC_ITEM(7, dp_nak_pump_current(m, s, dt))
+        BNC_ITEM(8, dp_ampa_current<kDef>(m, s, dt, glu, 1.0f))
+        BNC_ITEM(9, dp_nmda_current<kDef>(m, s, dt, glu, 1.0f))
+        BNC_ITEM(11, dp_gabaa_current<kDef>(m, s, dt, gaba, 1.0f))
+        BNC_ITEM(12, dp_glycine_current<kDef>(m, s, dt, gly, 1.0f))
+        BNC_ITEM(85, dp_kv42_current<kDef>(m, s, dt))
+        BNC_ITEM(98, dp_pmca_current<kDef>(m, s, dt))
+        BNC_ITEM(99, dp_ncx_current(m, s, dt))
+        BNC_ITEM(100, dp_kcc2_current<kDef>(m, s, dt))
+        BNC_ITEM(102, dp_ca_buffer_current<kDef>(m, s, dt))
+        BNC_ITEM(103, dp_sk_current<kDef>(m, s, dt))
+        BNC_ITEM(104, dp_bk_current<kDef>(m, s, dt))
+        BNC_ITEM(105, dp_nap_current<kDef>(m, s, dt))
+        BNC_ITEM(106, dp_kir_current<kDef>(m, s, dt))
+        BNC_ITEM(107, dp_k2p_current<kDef>(m, s, dt))
+        BNC_ITEM(112, dp_kv7_current<kDef>(m, s, dt))
+        BNC_ITEM(123, dp_kvdr_current<kDef>(m, s, dt))
+        BNC_ITEM(129, dp_hcn1_current<kDef>(m, s, dt))
+        BNC_ITEM(133, dp_nalcn_current<kDef>(m, s, dt))
+        BNC_ITEM(140, dp_cav21_current(m, s, dt))
+        BNC_ITEM(141, dp_nav_current<kDef>(m, s, dt, 0))
+        BNC_ITEM(142, dp_nav_current<kDef>(m, s, dt, 1))
+        BNC_ITEM(150, dp_kv31_current<kDef>(m, s, dt))
+        BNC_ITEM(200, dp_cav31_current<kDef>(m, s, dt))
+#undef BNC_ITEM
+        default: break;
+    }
+    return I;
+}
+
+// Item offsets of a group of consecutive phases: phase j of the group holds items
+// [off[j], off[j + 1]); row q of the group owns item off[j] + q of every phase j with
+// q < off[j + 1] - off[j].
+struct PhaseGroup {
+    uint32_t off[kMaxFuse + 1];
+    uint32_t n;   // phases in the group
+};
+
+// `grp.n` consecutive modifier phases in one launch, one thread per row (a segment):
+// the record is loaded once, the row's items run in phase order on it in registers,
+// and it is stored once.  Items of one segment run in the order and with the
+// arithmetic of the one-launch-per-phase path, so the results are the same bits.
+// The builder orders rows by (item count, item types), so a warp runs one sequence of
+// models; it forms groups only when no registered device modifier is present.
+__global__ void __launch_bounds__(256, BNC_GROUP_MIN_CTAS)
+k_phase_group(NetDev d, float dt, PhaseGroup grp) {
+    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= grp.off[1] - grp.off[0]) return;
+    const uint32_t N = d.n_seg;
+    const uint32_t NI = d.n_items;
+    const uint32_t g = d.it_seg[grp.off[0] + q];
+    SegRec* r = d.rec + g;
+    DSeg s;
+    s.V = r->V;
+#pragma unroll
+    for (int k = 0; k < 7; k++) { s.in[k] = r->in[k]; s.out[k] = r->out[k]; }
+    s.atp = r->atp;
+    s.area = r->area;
+    s.vol = r->vol;
+    double itot = r->itot;
+#pragma unroll 1
+    for (uint32_t j = 0; j < grp.n; j++) {
+        if (q >= grp.off[j + 1] - grp.off[j]) break;
+        const uint32_t qi = grp.off[j] + q;
+        const uint32_t tf = d.it_tf[qi];
+        const uint8_t type = (uint8_t)(tf & 0xFFu);
+        const uint8_t fl = (uint8_t)(tf >> 8);
+        DMod m;
+        m.den = d.it_den[qi];
+        m.av = (fl & 2) ? (uint8_t)((fl >> 2) & 7) : (uint8_t)0;
+        uint32_t rm = c_dyn_mask[type] | ((fl & 1) ? c_par_mask[type] : 0u);
+        if (fl & 2) rm |= (1u << m.av) & 0x7Fu;
+#pragma unroll
+        for (int k = 0; k < 7; k++) m.st[k] = ((rm >> k) & 1u) ? d.it_st[(size_t)k * NI + qi] : 0.0f;
+        float glu = 0.0f, gaba = 0.0f, gly = 0.0f;
+        if (type == 8 || type == 9) glu = d.nt[g];
+        else if (type == 11) gaba = d.nt[(size_t)1 * N + g];
+        else if (type == 12) gly = d.nt[(size_t)7 * N + g];
+        const double I = ((fl & 3) == 0) ? run_item_s<true>(type, m, s, dt, glu, gaba, gly)
+                                         : run_item_s<false>(type, m, s, dt, glu, gaba, gly);
+        itot = itot + I;
+        const uint32_t wm = c_dyn_mask[type];
+#pragma unroll
+        for (int k = 0; k < 7; k++) if ((wm >> k) & 1u) d.it_st[(size_t)k * NI + qi] = m.st[k];
+        if (type == 140) d.c21_cur[g] = make_float2(m.den, m.st[1]);
+    }
+    r->V = s.V;
+#pragma unroll
+    for (int k = 0; k < 7; k++) { r->in[k] = s.in[k]; r->out[k] = s.out[k]; }
+    r->atp = s.atp;
+    r->itot = itot;
+}
+
 static bool g_tables_ready[64] = {false};   // per device: constant memory is per context
 
 static cudaError_t init_tables(cudaStream_t stream) {
@@ -205,6 +320,18 @@ static cudaError_t enqueue_modifiers(const NetDev& dev, const NetHost& host, flo
     for (uint32_t c = 0; c < C; c++) {
         const uint32_t s0 = c * cs, s1 = std::min(dev.n_seg, s0 + cs);
         k_gather<<<(s1 - s0 + 255) / 256, 256, 0, stream>>>(dev, s0, s1);
+        if (host.fuse > 1) {   // one chunk, no registered device modifiers (the builder's rule)
+            for (uint32_t p0 = 0; p0 < P; p0 += host.fuse) {
+                PhaseGroup grp;
+                grp.n = std::min(host.fuse, P - p0);
+                for (uint32_t j = 0; j <= kMaxFuse; j++) grp.off[j] = host.phase_off[std::min(p0 + j, p0 + grp.n)];
+                const uint32_t rows = grp.off[1] - grp.off[0];
+                if (rows == 0) continue;
+                if (grp.n == 1) k_phase<<<(rows + 255) / 256, 256, 0, stream>>>(dev, dt, grp.off[0], grp.off[1]);
+                else k_phase_group<<<(rows + 255) / 256, 256, 0, stream>>>(dev, dt, grp);
+            }
+            continue;
+        }
         for (uint32_t p = 0; p < P; p++) {
             const uint32_t bk = c * P + p;
             const uint32_t b = host.phase_off[bk], e = host.phase_off[bk + 1];
@@ -218,6 +345,19 @@ static cudaError_t enqueue_modifiers(const NetDev& dev, const NetHost& host, flo
         }
     }
     return cudaGetLastError();
+}
+
+uint32_t modifier_launches(const NetDev& dev, const NetHost& host) {
+    const uint32_t P = dev.n_phases;
+    const uint32_t C = host.n_chunks ? host.n_chunks : 1;
+    if (host.phase_off.size() < (size_t)C * P + 1) return 0;
+    uint32_t n = C;   // k_gather
+    if (host.fuse > 1) {
+        for (uint32_t p0 = 0; p0 < P; p0 += host.fuse) n += host.phase_off[p0 + 1] > host.phase_off[p0] ? 1u : 0u;
+        return n;
+    }
+    for (uint32_t bk = 0; bk < C * P; bk++) n += host.phase_off[bk + 1] > host.phase_off[bk] ? 1u : 0u;
+    return n + (uint32_t)host.user_ranges.size();
 }
 
 cudaError_t launch_modifiers(const NetDev& dev, const NetHost& host, float dt, unsigned long long tick,

@@ -179,7 +179,14 @@ struct BuildOptions {
     // All phases of a chunk run before the next chunk, so a chunk's step-1 records
     // (96 bytes per segment) can stay in L2 between phases.
     uint32_t chunk_segs = BNC_DEFAULT_CHUNK_SEGS;
+    // Modifier phases per launch (1: one launch per phase).  Applies to slot-order
+    // schedules in one chunk without registered device modifiers; up to kMaxFuse.
+    // 6.4M-segment large set, step 1 per tick: 1 phase 7.8 ms; at 3.2M segments
+    // 1: 3.94, 2: 2.89, 3: 2.40, 4: 2.15, 6: 2.43, 9: 4.97, 17: 19.5 ms (deeper groups
+    // diverge: rows sorted by their items' types share fewer types further down).
+    uint32_t fuse_phases = 4;
 };
+constexpr uint32_t kMaxFuse = 32;
 
 // Host copy of everything the exporter needs to map device state back.
 struct NetHost {
@@ -197,6 +204,7 @@ struct NetHost {
     uint32_t cluster = 1;                    // CTAs per diffusion cluster (2: tiles in pairs)
     std::vector<uint32_t> phase_off;         // item range of each (chunk, phase) bucket (host copy)
     uint32_t chunk_segs = 0, n_chunks = 1;   // modifier-pass chunks of consecutive segments
+    uint32_t fuse = 1;                       // modifier phases per launch (item order follows)
     struct UserRange { uint32_t bucket, type, begin, end; const void* kernel; };
     std::vector<UserRange> user_ranges;      // registered device modifiers' items, per bucket
     size_t smem_bytes = 0;
@@ -242,6 +250,9 @@ cudaError_t enqueue_tick(const NetDev& dev, const NetHost& host, float dt, unsig
 cudaError_t launch_tick(const NetDev& dev, const NetHost& host, float dt, unsigned long long tick, int first_tick,
                         cudaStream_t stream);
 // the three kernels of a tick, one at a time (profiling)
+// Launches step 1 makes per tick (k_gather per chunk, phase or phase-group launches,
+// registered device modifiers), as enqueue_modifiers issues them.
+uint32_t modifier_launches(const NetDev& dev, const NetHost& host);
 cudaError_t launch_modifiers(const NetDev& dev, const NetHost& host, float dt, unsigned long long tick,
                              cudaStream_t stream);
 cudaError_t launch_diffusion(const NetDev& dev, const NetHost& host, float dt, unsigned long long tick,

@@ -203,6 +203,8 @@ typedef struct {
     double tile_bytes_per_tick, synapse_kernel_bytes_per_tick; /* split: steps 1 + 2.5 / steps 3 + 4 */
     uint32_t warp_cap, tile_segs;  /* grouping the network was built with */
     double modifier_kernel_bytes, diffusion_kernel_bytes;  /* per launch of each (state round trip included) */
+    uint32_t modifier_launches;   /* launches of step 1 per tick: k_gather, phase launches, device modifiers */
+    uint32_t fuse_phases;         /* modifier phases per launch the network runs with */
 } BncNetInfo;
 int bnc_network_info(void* sim, BncNetInfo* info);
 
@@ -274,9 +276,18 @@ int bnc_run_ticks_graph(void* sim, uint32_t n_ticks, float dt);
  *                        the extra launches cost more than L2 residency saves
  *                        (6.4M segments: 9.4 ms per tick in one chunk, 9.5 ms in
  *                        524,288-segment chunks, 11.6 ms in 262,144).
+ *   fuse_phases          modifier phases per launch (default 4, at most 32; 1: one
+ *                        launch per phase).  A launch runs each segment's items of
+ *                        its phases with the segment's working record in registers,
+ *                        so the record crosses HBM once per group instead of once per
+ *                        phase.  It applies to slot-order schedules in one chunk
+ *                        without registered device modifiers; others run one launch
+ *                        per phase.  At 3.2M segments of the large set, step 1 takes
+ *                        3.94 ms per tick with 1, 2.15 ms with 4 and 19.5 ms with 17
+ *                        (one launch: warps diverge over the later items).
  * Zero fields take the defaults. */
 typedef struct {
-    uint32_t warp_cap, tile_segs, phase_cap, chunk_segs;
+    uint32_t warp_cap, tile_segs, phase_cap, chunk_segs, fuse_phases;
 } BncBuildOptions;
 #define BNC_DEFAULT_CHUNK_SEGS 0xFFFFFFFFu
 int bnc_load_generated_opts(void* sim, const BncNetgenParams* p, const BncBuildOptions* opt);

@@ -114,6 +114,28 @@ def test_chunked_modifier_pass_bitexact(chunk):
         _compare_all(ora, gpu, n_syn, "chunk %d after +%d" % (chunk, step))
 
 
+@pytest.mark.parametrize("fuse", [1, 3, 4, 17])
+def test_fused_modifier_phases_bitexact(fuse):
+    """Several modifier phases per launch (each segment's items of those phases run on
+    its record in registers) compute what the oracle computes, bit for bit; so do one
+    launch per phase and one launch for all 17 phases.  The large set has 16 modifiers
+    per segment (17 on axon segments with Cav2.1), so groups of 3 and 4 leave a
+    shorter last group."""
+    from bioneuroncore_b200 import Backend, BuildOptions, Network, NetgenParams, NET_LARGE
+    p = NetgenParams(family=NET_LARGE, n_neurons=12, n_synapses=300, seed=6)
+    ora = Oracle(Network(p))
+    gpu = Backend()
+    gpu.load_generated(p, BuildOptions(fuse_phases=fuse))
+    info = gpu.info()
+    assert info.fuse_phases == fuse
+    assert info.modifier_launches == 1 + -(-info.n_phases // fuse)
+    n_syn = ora.n_syn
+    for step in (1, 20):
+        ora.run(step, DT)
+        gpu.run_ticks(step, DT)
+        _compare_all(ora, gpu, n_syn, "fuse %d after +%d" % (fuse, step))
+
+
 def test_trees_bitexact():
     """Depth-10 dendritic trees (2,047 segments each) exceed one CTA's tile: each tree
     runs on a 2-CTA cluster, its halves exchanging ghost segments through distributed

@@ -76,6 +76,24 @@ def test_plan_of_generated_networks():
     assert big.smem_bytes <= 227 * 1024
 
 
+def test_modifier_phase_groups():
+    """Phase groups form on slot-order schedules only: the large set (16 modifiers per
+    segment, slot order) runs 17 phases in ceil(17 / F) launches; the small set keeps
+    its greedy type-uniform phases, one launch each; F is capped at 32."""
+    from bioneuroncore_b200 import plan_generated, BuildOptions, NetgenParams, NET_SMALL, NET_LARGE
+    p = NetgenParams(family=NET_LARGE, n_neurons=50, seed=2)
+    for f, want in ((1, 1), (2, 2), (4, 4), (17, 17), (40, 32)):
+        inf = plan_generated(p, BuildOptions(fuse_phases=f))
+        assert inf.fuse_phases == want
+        assert inf.modifier_launches == 1 + -(-inf.n_phases // want)
+    assert plan_generated(p).fuse_phases == 4            # the default
+    small = plan_generated(NetgenParams(family=NET_SMALL, n_neurons=16, seed=2), BuildOptions(fuse_phases=3))
+    assert small.fuse_phases == 1 and small.modifier_launches == 1 + small.n_phases
+    # chunked modifier passes keep one launch per phase and chunk
+    ch = plan_generated(p, BuildOptions(fuse_phases=3, chunk_segs=1000))
+    assert ch.fuse_phases == 1
+
+
 def test_plan_aos_accepts_generated_network():
     net = _net(family=1, n_neurons=4, seed=5)
     rc, info = _plan_aos(net)
