@@ -41,6 +41,26 @@ namespace {
 // incidences held in registers per segment; segments with more use shared memory
 constexpr int kDeg = 4;
 
+// a / b rounded to nearest (the IEEE binary64 quotient) for a b that holds a float
+// value (a 24-bit significand), given y = 1 / b rounded to nearest.  q0 = a * y is
+// within 1.5 units in the last place of a / b; q0 + r * y with r = a - b * q0 (one fma,
+// exact) differs from a / b by r * (y - 1/b), under 2^-103 |a / b|.  a - m * b is a
+// nonzero multiple of 2^(exponent(a) - 77) for every rounding midpoint m of the binary64
+// grid near a / b (m has 54 significant bits, b 24), so a / b lies at least
+// 2^-79 |a / b| from any midpoint and fma(r, y, q0) rounds to the same neighbour.
+// Zero, non-finite and very small quotients (where r could underflow) take the
+// hardware division.  The gathers divide by the segment's volume (a float) every
+// substep, ion and incidence: this replaces those divisions with a multiply and two
+// fmas.
+__device__ __forceinline__ double div_by_float(double a, double b, double y) {
+    const double q0 = a * y;
+    const double r = fma(-q0, b, a);
+    const double aq = fabs(q0);
+    if (aq >= 0x1p-900 && aq <= 0x1.fffffffffffffp+1023) return fma(r, y, q0);
+    if (aq == 0.0) return q0;
+    return a / b;
+}
+
 // diffusion_kernel.h:108-113
 __device__ __forceinline__ float sg_bernoulli(float x) {
     if (fabsf(x) < 1e-3f) return 1.0f - 0.5f * x;
@@ -347,6 +367,37 @@ k_diffusion(NetDev d, float dt, unsigned long long tick, uint32_t S, uint32_t E)
         }
         double* phi = t.phiA;
         double* phn = t.phiB;
+        // Tiles whose every segment has at most two stencil entries (chains and their
+        // somata): the same sums over two registers' worth of entries, two sweeps per
+        // iteration so the buffers need no swap.  50 sweeps end in phiA either way.
+        if (CL == 1 && __syncthreads_and(st.n >= 0 && pn_cnt <= 2)) {
+            const bool h0 = pn_cnt > 0, h1 = pn_cnt > 1;
+            const double g0 = pg[0], g1 = pg[1];
+            const int o0 = po[0], o1 = po[1];
+            const bool live = i < ns && diag > 1e-9;
+            for (int it = 0; it < 50; it += 2) {
+                if (i < ns) {
+                    double pn = 0.0;
+                    if (h0) pn += g0 * t.phiA[o0];
+                    if (h1) pn += g1 * t.phiA[o1];
+                    double v = live ? (pn - itot) / diag : 0.0;
+                    if (v > 10.0) v = 10.0;
+                    if (v < -10.0) v = -10.0;
+                    t.phiB[i] = v;
+                }
+                __syncthreads();
+                if (i < ns) {
+                    double pn = 0.0;
+                    if (h0) pn += g0 * t.phiB[o0];
+                    if (h1) pn += g1 * t.phiB[o1];
+                    double v = live ? (pn - itot) / diag : 0.0;
+                    if (v > 10.0) v = 10.0;
+                    if (v < -10.0) v = -10.0;
+                    t.phiA[i] = v;
+                }
+                __syncthreads();
+            }
+        } else
         for (int it = 0; it < 50; it++) {
             if (i < ns) {
                 double pn = 0.0;
@@ -444,6 +495,7 @@ k_diffusion(NetDev d, float dt, unsigned long long tick, uint32_t S, uint32_t E)
             tile_sync<CL>();
             if (i < ns) {   // reads connection fluxes and its own concentrations: in place
                 const float vf = t.vf[i];
+                const double yv = 1.0 / (double)vf;
 #pragma unroll 1
                 for (int q = 0; q < 7; q++) {
                     double acc = 0.0;
@@ -453,8 +505,9 @@ k_diffusion(NetDev d, float dt, unsigned long long tick, uint32_t S, uint32_t E)
                             if (k >= st.n) break;
                             const int e = st.e[k];
                             if (!t.ei[e]) continue;
-                            if ((st.bend >> k) & 1u) acc += (double)t.fl[q * E + e] / vf;
-                            else acc -= (double)t.fl[q * E + e] / vf;
+                            const double dq = div_by_float((double)t.fl[q * E + e], (double)vf, yv);
+                            if ((st.bend >> k) & 1u) acc += dq;
+                            else acc -= dq;
                         }
                     } else {
                         for (int k = t.incoff[i]; k < t.incoff[i + 1]; k++) {
@@ -503,6 +556,28 @@ k_diffusion(NetDev d, float dt, unsigned long long tick, uint32_t S, uint32_t E)
             tile_sync<CL>();
             float* vc = t.vnA;
             float* vn = t.vnB;
+            // as for phi_e: two-entry stencils in registers, two sweeps per iteration
+            if (CL == 1 && __syncthreads_and(st.n >= 0 && vn_cnt <= 2)) {
+                const bool h0 = vn_cnt > 0, h1 = vn_cnt > 1;
+                const float g0 = vg[0], g1 = vg[1];
+                const int o0 = vo[0], o1 = vo[1];
+                for (int it = 0; it < 50; it += 2) {
+                    if (i < ns) {
+                        float off = 0.0f;
+                        if (h0) off += g0 * t.vnA[o0];
+                        if (h1) off += g1 * t.vnA[o1];
+                        t.vnB[i] = (rhs + off) / den;
+                    }
+                    __syncthreads();
+                    if (i < ns) {
+                        float off = 0.0f;
+                        if (h0) off += g0 * t.vnB[o0];
+                        if (h1) off += g1 * t.vnB[o1];
+                        t.vnA[i] = (rhs + off) / den;
+                    }
+                    __syncthreads();
+                }
+            } else
             for (int it = 0; it < 50; it++) {
                 if (i < ns) {
                     float off = 0.0f;
@@ -566,14 +641,17 @@ k_diffusion(NetDev d, float dt, unsigned long long tick, uint32_t S, uint32_t E)
                 tile_sync<CL>();
                 if (i < ns) {   // in place, as above
                     const float vf = t.vf[i];
+                    const float vx = vf * EXTRA_VOLUME_RATIO;
+                    const double yx = 1.0 / (double)vx;
                     double acc = 0.0;
                     if (st.n >= 0) {
 #pragma unroll
                         for (int k = 0; k < kDeg; k++) {
                             if (k >= st.n) break;
                             const int e = st.e[k];
-                            if ((st.bend >> k) & 1u) acc += t.ed[e] / (vf * EXTRA_VOLUME_RATIO);
-                            else acc -= t.ed[e] / (vf * EXTRA_VOLUME_RATIO);
+                            const double dq = div_by_float(t.ed[e], (double)vx, yx);
+                            if ((st.bend >> k) & 1u) acc += dq;
+                            else acc -= dq;
                         }
                     } else {
                         for (int k = t.incoff[i]; k < t.incoff[i + 1]; k++) {
