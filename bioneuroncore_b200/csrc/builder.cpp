@@ -23,6 +23,9 @@
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
+#include <atomic>
+#include <mutex>
+#include <thread>
 #include "net.h"
 #include "hostnet.h"
 
@@ -44,6 +47,36 @@ void DeviceAllocs::release() {
 }
 
 namespace {
+
+// Runs f(begin, end) over [0, n) in contiguous chunks on up to hardware_concurrency
+// threads (one chunk per thread); small ranges run inline.  Used for loops whose
+// iterations write disjoint outputs, so the result does not depend on the split.
+template <typename F>
+void parallel_for(size_t n, F&& f, size_t min_chunk = 1 << 16) {
+    unsigned T = std::thread::hardware_concurrency();
+    if (T == 0) T = 1;
+    T = std::min<unsigned>(T, 32u);
+    const size_t chunks = std::min<size_t>(T, (n + min_chunk - 1) / min_chunk);
+    if (chunks <= 1) { f((size_t)0, n); return; }
+    const size_t per = (n + chunks - 1) / chunks;
+    std::vector<std::thread> th;
+    th.reserve(chunks);
+    for (size_t c = 0; c < chunks; c++) {
+        const size_t b = c * per, e = std::min(n, b + per);
+        if (b < e) th.emplace_back([&f, b, e]() { f(b, e); });
+    }
+    for (auto& t : th) t.join();
+}
+
+// The lowest index at which a parallel loop found an error (UINT64_MAX: none).
+struct FirstError {
+    std::atomic<uint64_t> at{UINT64_MAX};
+    void note(uint64_t i) {
+        uint64_t cur = at.load();
+        while (i < cur && !at.compare_exchange_weak(cur, i)) {}
+    }
+    bool any() const { return at.load() != UINT64_MAX; }
+};
 
 // ---- host restatements of the static per-segment helpers ----
 // run_tick_common.h:209-214
@@ -585,33 +618,50 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
     lap("incidence");
     // ---- phase schedule (greedy shortest common supersequence over active types) ----
     std::vector<uint32_t> act_off(n + 1, 0);   // per original segment active slot list
-    std::vector<uint8_t> act_slot;
-    act_slot.reserve((size_t)n * 8);
     std::vector<uint8_t> sflags(n, 0);
-    uint32_t max_active = 0;
-    for (uint32_t i = 0; i < n; i++) {
-        const SegLite& s = S[i];
+    // a modifier is active unless it is myelin or a channel myelin blocks
+    // (simulation_host.cpp:241; myelin_modulator returns 0 and touches nothing)
+    auto seg_flags = [&](uint32_t i) -> uint8_t {
         bool myel = false, nmda = false;
-        for (uint8_t j = 0; j < s.modifier_count; j++) {
+        for (uint8_t j = 0; j < S[i].modifier_count; j++) {
             if (hn.mod(i, j).type == BNC_MOD_MYELIN) myel = true;
             if (hn.mod(i, j).type == BNC_MOD_NMDA) nmda = true;
         }
-        uint32_t c = 0;
-        for (uint8_t j = 0; j < s.modifier_count; j++) {
-            uint8_t t = hn.mod(i, j).type;
-            if (myel && t != BNC_MOD_MYELIN && is_myelin_blocked(t)) continue;  // simulation_host.cpp:241
-            if (t == BNC_MOD_MYELIN) continue;  // myelin_modulator returns 0 and touches nothing
-            act_slot.push_back(j);
-            c++;
+        return (uint8_t)((myel ? SF_MYELIN : 0) | (nmda ? SF_NMDA : 0));
+    };
+    auto active = [&](uint8_t t, uint8_t fl) {
+        return t != BNC_MOD_MYELIN && !((fl & SF_MYELIN) && is_myelin_blocked(t));
+    };
+    parallel_for(n, [&](size_t i0, size_t i1) {
+        for (uint32_t i = (uint32_t)i0; i < (uint32_t)i1; i++) {
+            const uint8_t fl = seg_flags(i);
+            uint32_t c = 0;
+            for (uint8_t j = 0; j < S[i].modifier_count; j++) c += active(hn.mod(i, j).type, fl) ? 1u : 0u;
+            act_off[i + 1] = c;
+            sflags[i] = fl;
         }
-        act_off[i + 1] = act_off[i] + c;
-        max_active = std::max(max_active, c);
-        sflags[i] = (uint8_t)((myel ? SF_MYELIN : 0) | (nmda ? SF_NMDA : 0));
+    });
+    uint32_t max_active = 0;
+    for (uint32_t i = 0; i < n; i++) {
+        max_active = std::max(max_active, act_off[i + 1]);
+        act_off[i + 1] += act_off[i];
     }
+    std::vector<uint8_t> act_slot(act_off[n]);
     std::vector<uint16_t> item_phase(act_slot.size(), 0);
     std::vector<uint8_t> act_type(act_slot.size());
-    for (uint32_t i = 0; i < n; i++)
-        for (uint32_t k = act_off[i]; k < act_off[i + 1]; k++) act_type[k] = hn.mod(i, act_slot[k]).type;
+    parallel_for(n, [&](size_t i0, size_t i1) {
+        for (uint32_t i = (uint32_t)i0; i < (uint32_t)i1; i++) {
+            uint32_t k = act_off[i];
+            for (uint8_t j = 0; j < S[i].modifier_count; j++) {
+                const uint8_t t = hn.mod(i, j).type;
+                if (!active(t, sflags[i])) continue;
+                act_slot[k] = j;
+                act_type[k] = t;
+                k++;
+            }
+        }
+    });
+    lap("active lists");
     uint32_t n_phases = 0;
     {
         std::vector<uint32_t> ptr(n, 0);
@@ -619,21 +669,33 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
         std::vector<uint64_t> count(256);
         const uint32_t cap = opt.phase_cap ? opt.phase_cap : std::max<uint32_t>(2 * max_active + 4, 8);
         bool greedy_ok = true;
+        std::mutex mu;
         while (remaining > 0) {
             std::fill(count.begin(), count.end(), 0);
-            for (uint32_t i = 0; i < n; i++) {
-                uint32_t k = act_off[i] + ptr[i];
-                if (k < act_off[i + 1]) count[act_type[k]]++;
-            }
-            int best = (int)(std::max_element(count.begin(), count.end()) - count.begin());
-            for (uint32_t i = 0; i < n; i++) {
-                uint32_t k = act_off[i] + ptr[i];
-                if (k < act_off[i + 1] && act_type[k] == best) {
-                    item_phase[k] = (uint16_t)n_phases;
-                    ptr[i]++;
-                    remaining--;
+            parallel_for(n, [&](size_t i0, size_t i1) {
+                uint64_t local[256] = {0};
+                for (size_t i = i0; i < i1; i++) {
+                    uint32_t k = act_off[i] + ptr[i];
+                    if (k < act_off[i + 1]) local[act_type[k]]++;
                 }
-            }
+                std::lock_guard<std::mutex> lock(mu);
+                for (int t = 0; t < 256; t++) count[t] += local[t];
+            });
+            int best = (int)(std::max_element(count.begin(), count.end()) - count.begin());
+            std::atomic<uint64_t> taken{0};
+            parallel_for(n, [&](size_t i0, size_t i1) {
+                uint64_t c = 0;
+                for (size_t i = i0; i < i1; i++) {
+                    uint32_t k = act_off[i] + ptr[i];
+                    if (k < act_off[i + 1] && act_type[k] == best) {
+                        item_phase[k] = (uint16_t)n_phases;
+                        ptr[i]++;
+                        c++;
+                    }
+                }
+                taken += c;
+            });
+            remaining -= taken.load();
             n_phases++;
             if (n_phases > cap) { greedy_ok = false; break; }
         }
@@ -685,50 +747,61 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
             for (uint8_t t : act_type) seen[t] = true;
             for (int t = 0; t < 256; t++) rank[t] = seen[t] ? ++R : 0u;   // 1..R; 0: no item
         }
-        std::vector<uint32_t> rows, tmp, cnt;
-        for (uint32_t p0 = 0; p0 < n_phases; p0 += fuse) {
-            const uint32_t F = std::min(fuse, n_phases - p0);
-            rows.clear();
-            for (uint32_t d = 0; d < n; d++)   // device order: the order inside a class
-                if (act_off[host->perm[d] + 1] - act_off[host->perm[d]] > p0) rows.push_back(d);
-            if (rows.size() != bucket_off[p0 + 1] - bucket_off[p0]) {
-                set_error("fused phase schedule: phase %u holds %zu items, %zu segments reach it", p0,
-                          (size_t)(bucket_off[p0 + 1] - bucket_off[p0]), rows.size());
-                return BNC_ERR_FORMAT;
-            }
-            // stable counting sorts, least significant first: the type of each item from
-            // the last phase of the group to the first, then the item count (descending)
-            auto key_of = [&](uint32_t d, uint32_t j) -> uint32_t {   // j == F: the count key
-                const uint32_t i = host->perm[d];
-                const uint32_t m = std::min(F, act_off[i + 1] - act_off[i] - p0);
-                if (j == F) return F - m;
-                return j < m ? rank[act_type[act_off[i] + p0 + j]] : 0u;
-            };
-            tmp.resize(rows.size());
-            for (int pass = (int)F - 1; pass >= -1; pass--) {
-                const uint32_t j = pass < 0 ? F : (uint32_t)pass;
-                const uint32_t nb = (j == F ? F : R) + 2;
-                cnt.assign(nb, 0u);
-                for (uint32_t d : rows) cnt[key_of(d, j) + 1]++;
-                for (uint32_t c = 0; c + 1 < nb; c++) cnt[c + 1] += cnt[c];
-                for (uint32_t d : rows) tmp[cnt[key_of(d, j)]++] = d;
-                rows.swap(tmp);
-            }
-            for (uint32_t r = 0; r < (uint32_t)rows.size(); r++) {
-                const uint32_t d = rows[r];
-                const uint32_t i = host->perm[d];
-                const uint32_t m = std::min(F, act_off[i + 1] - act_off[i] - p0);
-                for (uint32_t j = 0; j < m; j++) {
-                    const uint32_t k = act_off[i] + p0 + j;
-                    const uint32_t pos = bucket_off[p0 + j] + r;
-                    if (pos >= bucket_off[p0 + j + 1]) {
-                        set_error("fused phase schedule: row %u has no slot in phase %u", r, p0 + j);
-                        return BNC_ERR_FORMAT;
+        // groups are independent (their items go to disjoint phase ranges): one thread each
+        const uint32_t n_groups = (n_phases + fuse - 1) / fuse;
+        std::vector<int> group_err(n_groups, 0);
+        parallel_for(n_groups, [&](size_t g0, size_t g1) {
+            std::vector<uint32_t> rows, tmp, cnt;
+            std::vector<uint8_t> kb;
+            for (size_t gi = g0; gi < g1; gi++) {
+                const uint32_t p0 = (uint32_t)gi * fuse;
+                const uint32_t F = std::min(fuse, n_phases - p0);
+                const uint32_t W = F + 1;   // per row: the item types of the group, then the count key
+                rows.clear();
+                kb.clear();
+                for (uint32_t d = 0; d < n; d++) {   // device order: the order inside a class
+                    const uint32_t i = host->perm[d];
+                    const uint32_t c = act_off[i + 1] - act_off[i];
+                    if (c <= p0) continue;
+                    const uint32_t m = std::min(F, c - p0);
+                    rows.push_back(d);
+                    for (uint32_t j = 0; j < F; j++) kb.push_back(j < m ? (uint8_t)rank[act_type[act_off[i] + p0 + j]] : 0);
+                    kb.push_back((uint8_t)(F - m));
+                }
+                if (rows.size() != bucket_off[p0 + 1] - bucket_off[p0]) { group_err[gi] = 1; continue; }
+                // stable counting sorts, least significant first: the type of each item from
+                // the last phase of the group to the first, then the item count (descending)
+                std::vector<uint32_t> idx(rows.size());
+                std::iota(idx.begin(), idx.end(), 0u);
+                tmp.resize(rows.size());
+                for (int pass = (int)F - 1; pass >= -1; pass--) {
+                    const uint32_t j = pass < 0 ? F : (uint32_t)pass;
+                    const uint32_t nb = (j == F ? F : R) + 2;
+                    cnt.assign(nb, 0u);
+                    for (uint32_t x : idx) cnt[kb[(size_t)x * W + j] + 1]++;
+                    for (uint32_t c = 0; c + 1 < nb; c++) cnt[c + 1] += cnt[c];
+                    for (uint32_t x : idx) tmp[cnt[kb[(size_t)x * W + j]]++] = x;
+                    idx.swap(tmp);
+                }
+                for (uint32_t r = 0; r < (uint32_t)idx.size(); r++) {
+                    const uint32_t d = rows[idx[r]];
+                    const uint32_t i = host->perm[d];
+                    const uint32_t m = F - kb[(size_t)idx[r] * W + F];
+                    for (uint32_t j = 0; j < m; j++) {
+                        const uint32_t k = act_off[i] + p0 + j;
+                        const uint32_t pos = bucket_off[p0 + j] + r;
+                        if (pos >= bucket_off[p0 + j + 1]) { group_err[gi] = 2; break; }
+                        keys[pos] = {(uint16_t)(p0 + j), act_type[k], d, k};
                     }
-                    keys[pos] = {(uint16_t)(p0 + j), act_type[k], d, k};
+                    if (group_err[gi]) break;
                 }
             }
-        }
+        }, 1);
+        for (uint32_t gi = 0; gi < n_groups; gi++)
+            if (group_err[gi]) {
+                set_error("fused phase schedule: phase group %u does not nest (%d)", gi, group_err[gi]);
+                return BNC_ERR_FORMAT;
+            }
     } else {
         std::vector<uint32_t> pos(bucket_off.begin(), bucket_off.end() - 1);
         for (uint32_t d = 0; d < n; d++) {   // device order: each bucket fills in segment order
@@ -757,24 +830,36 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
     host->item_seg.assign(NI, 0);
     host->item_slot.assign(NI, 0);
     host->phase_off = phase_off;
-    for (uint32_t q = 0; q < NI; q++) {
-        const ItemKey& kk = keys[q];
-        uint32_t orig = host->perm[kk.dseg];
-        uint8_t slot = act_slot[kk.k];
-        const ModLite& m = hn.mod(orig, slot);
-        uint8_t fl = 0;
-        uint8_t pm = param_mask(m.type);
-        for (int b = 0; b < 7; b++) if ((pm >> b) & 1) if (m.state[b] != 0.0f) fl |= 1;
-        if (receptor_supported(m.type) && m.active_vars > 0) {
-            if (m.active_vars >= 8) { set_error("segment %u slot %u: active_vars %u out of range", orig, slot, m.active_vars); return BNC_ERR_FORMAT; }
-            fl |= (uint8_t)(2u | ((uint32_t)m.active_vars << 2));
+    {
+        FirstError bad;
+        parallel_for(NI, [&](size_t q0, size_t q1) {
+            for (uint32_t q = (uint32_t)q0; q < (uint32_t)q1; q++) {
+                const ItemKey& kk = keys[q];
+                uint32_t orig = host->perm[kk.dseg];
+                uint8_t slot = act_slot[kk.k];
+                const ModLite& m = hn.mod(orig, slot);
+                uint8_t fl = 0;
+                uint8_t pm = param_mask(m.type);
+                for (int b = 0; b < 7; b++) if ((pm >> b) & 1) if (m.state[b] != 0.0f) fl |= 1;
+                if (receptor_supported(m.type) && m.active_vars > 0) {
+                    if (m.active_vars >= 8) { bad.note(q); continue; }
+                    fl |= (uint8_t)(2u | ((uint32_t)m.active_vars << 2));
+                }
+                it_seg[q] = kk.dseg;
+                it_tf[q] = (uint16_t)(m.type | ((uint32_t)fl << 8));
+                it_den[q] = m.density;
+                for (int b = 0; b < 7; b++) it_st[(size_t)b * NI + q] = m.state[b];
+                host->item_seg[q] = orig;
+                host->item_slot[q] = slot;
+            }
+        });
+        if (bad.any()) {
+            const ItemKey& kk = keys[bad.at.load()];
+            const uint32_t orig = host->perm[kk.dseg];
+            const uint8_t slot = act_slot[kk.k];
+            set_error("segment %u slot %u: active_vars %u out of range", orig, slot, hn.mod(orig, slot).active_vars);
+            return BNC_ERR_FORMAT;
         }
-        it_seg[q] = kk.dseg;
-        it_tf[q] = (uint16_t)(m.type | ((uint32_t)fl << 8));
-        it_den[q] = m.density;
-        for (int b = 0; b < 7; b++) it_st[(size_t)b * NI + q] = m.state[b];
-        host->item_seg[q] = orig;
-        host->item_slot[q] = slot;
     }
     // registered device modifiers: their items form one contiguous run per phase and type
     host->user_ranges.clear();
@@ -800,7 +885,8 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
     std::vector<uint8_t> stype(n), dflags(n);
     std::vector<float2> c21(n);
     bool intra_nt_grad = false, temp_grad = false, txn_grad = false;
-    for (uint32_t d = 0; d < n; d++) {
+    parallel_for(n, [&](size_t d0, size_t d1) {
+    for (uint32_t d = (uint32_t)d0; d < (uint32_t)d1; d++) {
         const SegLite& s = S[host->perm[d]];
         V[d] = s.V_m;
         for (int q = 0; q < 7; q++) {
@@ -821,6 +907,7 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
             if (hn.mod(host->perm[d], j).type == BNC_MOD_CAV21)
                 c21[d] = make_float2(hn.mod(host->perm[d], j).density, hn.mod(host->perm[d], j).state[1]);
     }
+    });
     for (uint32_t c : conn_ok) {
         const auto& cn = hn.conn[c];
         const SegLite& A = S[cn.segment_a];
@@ -836,38 +923,55 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
     std::vector<uint32_t> syn_valid;
     bool need_pre_ext = false, any_delay = false;
     uint32_t nt_mask = 0;
-    for (uint32_t k = 0; k < aos.num_synapses; k++) {
+    // status of synapse k: 0 kept, 1 skipped (indices out of range), 2 and up an error,
+    // whose message is written when `report` is set
+    auto check_syn = [&](uint32_t k, bool report) -> int {
         const SynLite& y = hn.syn[k];
-        if (y.pre_segment >= n || y.post_segment >= n) continue;   // simulation_host.cpp:362
+        if (y.pre_segment >= n || y.post_segment >= n) return 1;   // simulation_host.cpp:362
         if (y.type != BNC_SYN_CHEMICAL) {
-            set_error("synapse %u: electrical synapses have no device implementation in this backend", k);
+            if (report) set_error("synapse %u: electrical synapses have no device implementation in this backend", k);
             return BNC_ERR_UNSUPPORTED;
         }
         if (y.post_receptor_count > BNC_MAX_POST_RECEPTORS || y.pre_autoreceptor_count > BNC_MAX_PRE_AUTORECEPTORS) {
-            set_error("synapse %u: receptor count out of range", k); return BNC_ERR_FORMAT;
+            if (report) set_error("synapse %u: receptor count out of range", k);
+            return BNC_ERR_FORMAT;
         }
         for (uint8_t j = 0; j < y.post_receptor_count; j++)
             if (!receptor_supported(hn.post_rec(k, j).type)) {
-                set_error("synapse %u receptor %u: type %u has no device implementation as a receptor", k, j,
-                          hn.post_rec(k, j).type);
+                if (report)
+                    set_error("synapse %u receptor %u: type %u has no device implementation as a receptor", k, j,
+                              hn.post_rec(k, j).type);
                 return BNC_ERR_UNSUPPORTED;
             }
         for (uint8_t j = 0; j < y.pre_autoreceptor_count; j++)
             if (bouton_gamma(hn.pre_ar(k, j).type) == 0.0f) {
-                set_error("synapse %u autoreceptor %u: type %u (release modulators are not supported)", k, j,
-                          hn.pre_ar(k, j).type);
+                if (report)
+                    set_error("synapse %u autoreceptor %u: type %u (release modulators are not supported)", k, j,
+                              hn.pre_ar(k, j).type);
                 return BNC_ERR_UNSUPPORTED;
             }
         uint8_t ntt = y.post_receptor_count > 0 ? nt_from_receptor(hn.post_rec(k, 0).type) : 0;
         for (int q = 0; q < 15; q++)
             if (q != ntt && y.cleft_neurotransmitter[q] != 0.0f) {
-                set_error("synapse %u: cleft holds neurotransmitter %d other than the one it releases", k, q);
+                if (report) set_error("synapse %u: cleft holds neurotransmitter %d other than the one it releases", k, q);
                 return BNC_ERR_UNSUPPORTED;
             }
-        if (y.pre_autoreceptor_count > 0 || y.RRP_max > 0.0f) need_pre_ext = true;
-        if (y.delay > 0.0f) any_delay = true;
-        nt_mask |= 1u << ntt;
-        syn_valid.push_back(k);
+        return 0;
+    };
+    {
+        std::vector<int8_t> status(aos.num_synapses);
+        parallel_for(aos.num_synapses, [&](size_t k0, size_t k1) {
+            for (size_t k = k0; k < k1; k++) status[k] = (int8_t)check_syn((uint32_t)k, false);
+        });
+        for (uint32_t k = 0; k < aos.num_synapses; k++) {
+            if (status[k] == 1) continue;
+            if (status[k] != 0) return check_syn(k, true);
+            const SynLite& y = hn.syn[k];
+            if (y.pre_autoreceptor_count > 0 || y.RRP_max > 0.0f) need_pre_ext = true;
+            if (y.delay > 0.0f) any_delay = true;
+            nt_mask |= 1u << (y.post_receptor_count > 0 ? nt_from_receptor(hn.post_rec(k, 0).type) : 0);
+            syn_valid.push_back(k);
+        }
     }
     const uint32_t K = (uint32_t)syn_valid.size();
     std::vector<uint32_t> post_off(n + 1, 0);
@@ -937,7 +1041,8 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
     host->syn_orig = syn_valid;
     host->rec_syn.clear(); host->rec_slot.clear();
     host->syn_nt.assign(K, 0);
-    for (uint32_t q = 0; q < K; q++) {
+    // per synapse: 0 or the error its receptors raise (the lowest such synapse is reported)
+    auto fill_syn = [&](uint32_t q, bool report) -> int {
         const SynLite& y = hn.syn[syn_valid[q]];
         sy_pre[q] = host->inv[y.pre_segment];
         sy_id[q] = y.id;
@@ -968,45 +1073,71 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
         for (uint8_t j = 0; j < y.post_receptor_count; j++) {
             const ModLite& r = hn.post_rec(syn_valid[q], j);
             if (myel_post && is_ionotropic(r.type)) continue;   // simulation_host.cpp:495
-            if (r.active_vars >= 8) { set_error("synapse %u receptor %u: active_vars out of range", syn_valid[q], j); return BNC_ERR_FORMAT; }
+            if (r.active_vars >= 8) {
+                if (report) set_error("synapse %u receptor %u: active_vars out of range", syn_valid[q], j);
+                return BNC_ERR_FORMAT;
+            }
             if (r.active_vars >= 3 && r.active_vars <= 6) {
-                set_error("synapse %u receptor %u: active_vars %u not supported", syn_valid[q], j, r.active_vars);
+                if (report) set_error("synapse %u receptor %u: active_vars %u not supported", syn_valid[q], j, r.active_vars);
                 return BNC_ERR_UNSUPPORTED;
             }
             kept[(size_t)q * 8 + nr] = j;
             nr++;
         }
         rc_cnt[q] = (uint8_t)nr;
+        return 0;
+    };
+    {
+        FirstError bad;
+        parallel_for(K, [&](size_t q0, size_t q1) {
+            for (size_t q = q0; q < q1; q++)
+                if (fill_syn((uint32_t)q, false) != 0) bad.note(q);
+        });
+        if (bad.any()) return fill_syn((uint32_t)bad.at.load(), true);
     }
-    // receptor order: slice by slice, receptor j of each lane that has one
+    // receptor order: slice by slice, receptor j of each lane that has one.  A warp's
+    // receptors are those of its synapses, so a prefix sum of per-warp counts places
+    // each warp's run and the warps fill in parallel.
     for (uint32_t w = 0; w < NW; w++) {
-        rw_off[w] = (uint32_t)rc_type.size();
-        uint32_t maxc = 0;
-        for (uint32_t l = 0; l < 32 && 32 * w + l < n; l++) maxc = std::max<uint32_t>(maxc, th_cnt[32 * w + l]);
-        uint32_t q = w_off[w];
-        for (uint32_t k = 0; k < maxc; k++) {
-            uint32_t a = 0;   // lanes with a k-th synapse: a prefix of the warp
-            while (a < 32 && 32 * w + a < n && th_cnt[32 * w + a] > k) a++;
-            uint32_t maxr = 0;
-            for (uint32_t l = 0; l < a; l++) maxr = std::max<uint32_t>(maxr, rc_cnt[q + l]);
-            for (uint32_t j = 0; j < maxr; j++)
-                for (uint32_t l = 0; l < a; l++) {
-                    const uint32_t qq = q + l;
-                    if (rc_cnt[qq] <= j) continue;
-                    const uint8_t slot = kept[(size_t)qq * 8 + j];
-                    const ModLite& r = hn.post_rec(syn_valid[qq], slot);
-                    rc_type.push_back(r.type);
-                    rc_av.push_back(r.active_vars);
-                    rc_den.push_back(r.density);
-                    rc_st0.push_back(r.state[0]);
-                    rc_st1.push_back(r.state[1]);
-                    rc_st2.push_back(r.state[2]);
-                    host->rec_syn.push_back(qq);
-                    host->rec_slot.push_back(slot);
-                }
-            q += a;
-        }
+        uint32_t c = 0;
+        for (uint32_t q = w_off[w]; q < w_off[w + 1]; q++) c += rc_cnt[q];
+        rw_off[w + 1] = rw_off[w] + c;
     }
+    const size_t NRC = rw_off[NW];
+    rc_type.resize(NRC); rc_av.resize(NRC); rc_den.resize(NRC);
+    rc_st0.resize(NRC); rc_st1.resize(NRC); rc_st2.resize(NRC);
+    host->rec_syn.resize(NRC); host->rec_slot.resize(NRC);
+    parallel_for(NW, [&](size_t w0, size_t w1) {
+        for (uint32_t w = (uint32_t)w0; w < (uint32_t)w1; w++) {
+            size_t o = rw_off[w];
+            uint32_t maxc = 0;
+            for (uint32_t l = 0; l < 32 && 32 * w + l < n; l++) maxc = std::max<uint32_t>(maxc, th_cnt[32 * w + l]);
+            uint32_t q = w_off[w];
+            for (uint32_t k = 0; k < maxc; k++) {
+                uint32_t a = 0;   // lanes with a k-th synapse: a prefix of the warp
+                while (a < 32 && 32 * w + a < n && th_cnt[32 * w + a] > k) a++;
+                uint32_t maxr = 0;
+                for (uint32_t l = 0; l < a; l++) maxr = std::max<uint32_t>(maxr, rc_cnt[q + l]);
+                for (uint32_t j = 0; j < maxr; j++)
+                    for (uint32_t l = 0; l < a; l++) {
+                        const uint32_t qq = q + l;
+                        if (rc_cnt[qq] <= j) continue;
+                        const uint8_t slot = kept[(size_t)qq * 8 + j];
+                        const ModLite& r = hn.post_rec(syn_valid[qq], slot);
+                        rc_type[o] = r.type;
+                        rc_av[o] = r.active_vars;
+                        rc_den[o] = r.density;
+                        rc_st0[o] = r.state[0];
+                        rc_st1[o] = r.state[1];
+                        rc_st2[o] = r.state[2];
+                        host->rec_syn[o] = qq;
+                        host->rec_slot[o] = slot;
+                        o++;
+                    }
+                q += a;
+            }
+        }
+    }, 1024);
     rw_off[NW] = (uint32_t)rc_type.size();
 
     lap("synapses");
