@@ -190,6 +190,47 @@ def cpu_reference_rate(neurons, ticks, warm, seed):
     return nseg * ticks / dt, kind, nseg
 
 
+def cpu_reference_params(params, ticks, warm):
+    """The reference CPU tick (oracle port when the reference build is absent) run
+    network by network over `params` (NetgenParams); returns (segment-ticks/s, seconds
+    of timed ticks, segments, kind).  Networks are built before the clock starts."""
+    from bioneuroncore_b200 import Network
+    from oracle import oracle as orc
+    total_s, seg_ticks, nseg, kind = 0.0, 0.0, 0, "port"
+    for p in params:
+        net = Network(p)
+        if orc.reference_available():
+            runner, kind = orc.Reference(net), "reference"
+        else:
+            runner, kind = orc.Oracle(net), "port"
+        runner.run(warm, DT)
+        t0 = time.perf_counter()
+        runner.run(ticks, DT)
+        total_s += time.perf_counter() - t0
+        seg_ticks += float(net.data.num_segments) * ticks
+        nseg += net.data.num_segments
+    return seg_ticks / total_s, total_s, nseg, kind
+
+
+def _ref_params_worker(args):
+    params, ticks, warm = args
+    return cpu_reference_params(params, ticks, warm)
+
+
+def cpu_reference_parallel(params, ticks, warm, procs):
+    """cpu_reference_params with the networks dealt round-robin to `procs` processes
+    (spawned: the reference tick is single-threaded and not re-entrant); returns the
+    aggregate segment-ticks/s over the wall clock of the timed ticks (max over
+    processes) and the process count."""
+    import multiprocessing as mp
+    procs = max(1, min(procs, len(params)))
+    chunks = [params[k::procs] for k in range(procs)]
+    with mp.get_context("spawn").Pool(procs) as pool:
+        res = pool.map(_ref_params_worker, [(c, ticks, warm) for c in chunks])
+    seg_ticks = sum(r[0] * r[1] for r in res)
+    return seg_ticks / max(r[1] for r in res), procs
+
+
 def _ref_worker(args):
     neurons, ticks, warm, seed = args
     return cpu_reference_rate(neurons, ticks, warm, seed)
@@ -253,6 +294,19 @@ def run_ensemble(a, device):
         seq_segments += b.info().n_segments
         b.close()
     assert seq_segments == info.n_segments
+    cpu = None
+    if not a.no_cpu_baseline:
+        try:   # a seeded sample of the members, then all 8 host cores on it
+            sample = ps[:: max(1, len(ps) // 32)][:32]
+            rate1, secs, nseg_s, kind = cpu_reference_params(sample, 2, 1)
+            rate8, procs = cpu_reference_parallel(sample, 2, 1, os.cpu_count() or 1)
+            cpu = {"value": rate1, "unit": "segment-ticks/s", "cores": 1, "kind": kind,
+                   "parallel_value": rate8, "parallel_processes": procs,
+                   "sample": "%d of the %d networks (%d segments), 2 ticks after 1 warm-up each" %
+                             (len(sample), len(ps), nseg_s),
+                   "sequential_512_ms_per_tick_extrapolated": 1000.0 * info.n_segments / rate1}
+        except Exception as exc:
+            cpu = {"unavailable": str(exc)[:200]}
     rate_ens = info.n_segments * a.ens_ticks / (ms_ens / 1000.0)
     rate_seq = info.n_segments * a.ens_ticks / (ms_seq / 1000.0)
     return {
@@ -266,6 +320,7 @@ def run_ensemble(a, device):
         "grouping": {"warp_cap": tune.warp_cap, "tile_segs": tune.tile_segs,
                      "candidates_tried": tune.candidates_tried, "sample_members": tune.sample_members},
         "setup_s": round(setup_s, 1),
+        "cpu_reference": cpu,
     }
 
 
@@ -286,6 +341,17 @@ def run_trees(a, device):
     ms_mod, ms_diff, ms_syn = b.profile_ticks(n_prof, DT)
     ms = b.time_ticks(a.tree_ticks, DT)
     b.close()
+    cpu = None
+    if not a.no_cpu_baseline:
+        try:   # a seeded subset of the trees, per-segment throughput
+            n_sub = 16
+            rate, secs, nseg_s, kind = cpu_reference_params(
+                [NetgenParams(family=NET_TREES, n_neurons=n_sub, tree_depth=10, seed=a.seed, flags=NETGEN_PERTURB_IONS)],
+                2, 1)
+            cpu = {"value": rate, "unit": "segment-ticks/s", "cores": 1, "kind": kind,
+                   "sample": "%d trees (%d segments), 2 ticks after 1 warm-up" % (n_sub, nseg_s)}
+        except Exception as exc:
+            cpu = {"unavailable": str(exc)[:200]}
     return {
         "workload": "%d binary dendritic trees of depth 10 (%d segments), ions perturbed +-5%%, 50-sweep Jacobi"
                     % (a.trees, info.n_segments),
@@ -293,6 +359,7 @@ def run_trees(a, device):
         "ms_per_tick": ms / a.tree_ticks,
         "kernels_ms": {"k_modifiers": ms_mod / n_prof, "k_diffusion": ms_diff / n_prof, "k_synapse": ms_syn / n_prof},
         "cluster": "2 CTAs per tree (distributed shared memory)", "setup_s": round(setup_s, 1),
+        "cpu_reference": cpu,
     }
 
 
@@ -327,6 +394,19 @@ def run_adjoint(a, device):
     adj.close()
     b.close()
     spec_ticks = 20000
+    cpu = None
+    if not a.no_cpu_baseline:
+        try:   # the reference's CPU tick on the same network: the forward pass of one set
+            n_cpu = 20
+            rate, secs, nseg_s, kind = cpu_reference_params(
+                [NetgenParams(family=NET_ADJOINT, n_neurons=a.adj_neurons, seed=a.seed)], n_cpu, 1)
+            per_tick = secs / n_cpu
+            cpu = {"forward_s_all_sets": per_tick * a.adj_ticks * a.adj_sets, "cores": 1, "kind": kind,
+                   "forward_over_gpu_forward": per_tick * a.adj_ticks * a.adj_sets / (fwd_ms / 1000.0),
+                   "sample": "%d ticks of one set (%d segments), scaled to %d ticks x %d sets" %
+                             (n_cpu, nseg_s, a.adj_ticks, a.adj_sets)}
+        except Exception as exc:
+            cpu = {"unavailable": str(exc)[:200]}
     return {
         "workload": "%d neurons x 64 segments (%d segments), %d synapses, %d parameter sets, %d ticks, "
                     "checkpoints every 256 ticks; loss = MSE of somatic V_m against a hidden parameter set"
@@ -342,6 +422,7 @@ def run_adjoint(a, device):
         "launch": "one CTA per (neuron, parameter set); forward %d threads, %d B shared; backward %d B shared"
                   % (i.threads, i.smem_forward, i.smem_backward),
         "setup_s": round(setup_s, 1),
+        "cpu_reference": cpu,
     }
 
 
