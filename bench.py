@@ -339,7 +339,15 @@ def run_trees(a, device):
     b.run_ticks(max(a.warmup, 3), DT)
     n_prof = 3
     ms_mod, ms_diff, ms_syn = b.profile_ticks(n_prof, DT)
+    ms_fixed = b.time_ticks(a.tree_ticks, DT)
+    # the workload's own solver: Jacobi to a residual of 1e-6 with FP64 iterates and
+    # the per-ion FP64 ledger (bnc_set_diffusion_mode), on the same network
+    from bioneuroncore_b200 import DIFFUSION_RESIDUAL, DIFFUSION_LEDGER
+    b.set_diffusion_mode(DIFFUSION_RESIDUAL | DIFFUSION_LEDGER, 1e-6, 100000)
+    b.run_ticks(1, DT)
+    b.diffusion_stats(reset=True)
     ms = b.time_ticks(a.tree_ticks, DT)
+    dst = b.diffusion_stats()
     b.close()
     cpu = None
     if not a.no_cpu_baseline:
@@ -353,10 +361,16 @@ def run_trees(a, device):
         except Exception as exc:
             cpu = {"unavailable": str(exc)[:200]}
     return {
-        "workload": "%d binary dendritic trees of depth 10 (%d segments), ions perturbed +-5%%, 50-sweep Jacobi"
-                    % (a.trees, info.n_segments),
+        "workload": "%d binary dendritic trees of depth 10 (%d segments), ions perturbed +-5%%, Jacobi solves to "
+                    "a residual of 1e-6 in FP64, FP64 per-ion ledger" % (a.trees, info.n_segments),
         "metric": "segment-ticks/s", "ticks": a.tree_ticks, "value": info.n_segments * a.tree_ticks / (ms / 1000.0),
         "ms_per_tick": ms / a.tree_ticks,
+        "solver": {"max_sweeps_v": dst.max_sweeps_v, "max_sweeps_phi": dst.max_sweeps_phi,
+                   "capped_group_solves": dst.capped_v + dst.capped_phi,
+                   "ledger_rounding_abs_sum": float(sum(abs(x) for x in dst.rounding))},
+        "fixed_50_sweeps": {"value": info.n_segments * a.tree_ticks / (ms_fixed / 1000.0),
+                            "ms_per_tick": ms_fixed / a.tree_ticks,
+                            "note": "the reference's fixed 50 sweeps per solve (parity mode)"},
         "kernels_ms": {"k_modifiers": ms_mod / n_prof, "k_diffusion": ms_diff / n_prof, "k_synapse": ms_syn / n_prof},
         "cluster": "2 CTAs per tree (distributed shared memory)", "setup_s": round(setup_s, 1),
         "cpu_reference": cpu,

@@ -45,7 +45,18 @@ NEW_SYMBOLS = ["bnc_netgen_aos", "bnc_netgen_free", "bnc_last_error", "bnc_load_
                "bnc_adjoint_soma", "bnc_adjoint_record", "bnc_adjoint_release_count", "bnc_adjoint_set_params",
                "bnc_adjoint_get_params", "bnc_adjoint_set_target", "bnc_adjoint_forward", "bnc_adjoint_backward",
                "bnc_adjoint_timings", "bnc_sweep_parse_params", "bnc_sweep_apply", "bnc_sweep_run",
-               "bnc_save_checkpoint", "bnc_load_checkpoint", "bnc_state_frame"]
+               "bnc_save_checkpoint", "bnc_load_checkpoint", "bnc_state_frame", "bnc_set_diffusion_mode",
+               "bnc_diffusion_stats"]
+
+DIFFUSION_RESIDUAL = 1
+DIFFUSION_LEDGER = 2
+
+
+class DiffusionStats(C.Structure):
+    """bnc_diffusion_stats: sweep counts of the residual-controlled solves and the
+    per-ion FP64 ledger of step 2.5 (rounding of the FP32 updates, bath exchange)."""
+    _fields_ = [("max_sweeps_v", C.c_uint32), ("max_sweeps_phi", C.c_uint32), ("capped_v", C.c_uint32),
+                ("capped_phi", C.c_uint32), ("rounding", C.c_double * 7), ("bath", C.c_double * 7)]
 
 
 class NetInfo(C.Structure):
@@ -165,6 +176,8 @@ def load_library(path=LIB_PATH):
         "bnc_sweep_run": ([vp, vp, vp, u32, vp, u32, u32, f32, u32, vp], i32),
         "bnc_save_checkpoint": ([vp, C.c_char_p], i32), "bnc_load_checkpoint": ([vp, C.c_char_p], i32),
         "bnc_state_frame": ([vp, vp, C.c_uint64, vp], i32),
+        "bnc_set_diffusion_mode": ([vp, u32, C.c_double, u32], i32),
+        "bnc_diffusion_stats": ([vp, vp, i32], i32),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -358,6 +371,17 @@ class Backend:
         _check(self.lib.bnc_state_frame(self.h, buf, n.value, C.byref(n)), "bnc_state_frame")
         return bytes(buf)
 
+    def set_diffusion_mode(self, flags, tol=1e-6, max_sweeps=100000):
+        """Step 2.5 options: DIFFUSION_RESIDUAL (FP64 Jacobi solves to `tol`, at most
+        `max_sweeps` sweeps) and DIFFUSION_LEDGER (the per-ion FP64 ledger); 0 restores
+        the reference's fixed 50 sweeps."""
+        _check(self.lib.bnc_set_diffusion_mode(self.h, flags, C.c_double(tol), max_sweeps), "bnc_set_diffusion_mode")
+
+    def diffusion_stats(self, reset=False):
+        out = DiffusionStats()
+        _check(self.lib.bnc_diffusion_stats(self.h, C.byref(out), 1 if reset else 0), "bnc_diffusion_stats")
+        return out
+
     def save_checkpoint(self, path):
         _check(self.lib.bnc_save_checkpoint(self.h, str(path).encode()), "bnc_save_checkpoint")
 
@@ -372,7 +396,8 @@ __all__ = ["Backend", "Network", "Adjoint", "AdjointConfig", "AdjointInfo", "Swe
            "sweep_parse_params", "sweep_tasks", "sweep_run", "SWEEP_SINGLE_TICK", "NetgenParams", "BionData", "BackendError", "load_library", "last_error",
            "NET_SMALL", "NET_LARGE", "NET_TREES", "NET_ENSEMBLE_MEMBER", "NET_ADJOINT", "NETGEN_NO_SYNAPSES",
            "NETGEN_NO_CONNECTIONS", "NETGEN_NO_STIMULI", "NETGEN_PERTURB_IONS", "NETGEN_SYNAPSE_EXTRAS", "SEG_FIELDS", "SYN_FIELDS",
-           "DROPIN_SYMBOLS", "NEW_SYMBOLS", "EnsembleMember", "Tuning", "BuildOptions", "register_device_modifier", "ensemble_params", "plan_ensemble", "plan_generated"]
+           "DROPIN_SYMBOLS", "NEW_SYMBOLS", "EnsembleMember", "Tuning", "BuildOptions", "register_device_modifier", "ensemble_params", "plan_ensemble", "plan_generated",
+           "DIFFUSION_RESIDUAL", "DIFFUSION_LEDGER", "DiffusionStats"]
 
 
 class AdjointConfig(C.Structure):

@@ -1134,6 +1134,51 @@ int bnc_save_bion(void* sim, const char* filename) {
     return save_bion(b->aos, filename);
 }
 
+// ---- Electrodiffusion options: residual-controlled Jacobi solves, the ion ledger ----
+int bnc_set_diffusion_mode(void* sim, uint32_t flags, double tol, uint32_t max_sweeps) {
+    if (!sim) { set_error("null argument"); return BNC_ERR_ARG; }
+    Backend* b = static_cast<Backend*>(sim);
+    if (!b->loaded) { set_error("no network loaded"); return BNC_ERR_STATE; }
+    if (flags & ~(uint32_t)(BNC_DIFFUSION_RESIDUAL | BNC_DIFFUSION_LEDGER)) {
+        set_error("unknown diffusion flags 0x%x", flags);
+        return BNC_ERR_ARG;
+    }
+    if ((flags & BNC_DIFFUSION_RESIDUAL) && (!(tol > 0.0) || max_sweeps == 0)) {
+        set_error("the residual mode needs tol > 0 and max_sweeps >= 1 (tol %g, max_sweeps %u)", tol, max_sweeps);
+        return BNC_ERR_ARG;
+    }
+    b->drop_graph();   // a captured tick holds the descriptor by value
+    b->dev.diff_mode = flags;
+    b->dev.jac_tol = (flags & BNC_DIFFUSION_RESIDUAL) ? tol : 0.0;
+    b->dev.jac_max = (flags & BNC_DIFFUSION_RESIDUAL) ? max_sweeps : 0u;
+    return BNC_OK;
+}
+
+int bnc_diffusion_stats(void* sim, BncDiffusionStats* out, int reset) {
+    if (!sim || !out) { set_error("null argument"); return BNC_ERR_ARG; }
+    Backend* b = static_cast<Backend*>(sim);
+    if (!b->loaded) { set_error("no network loaded"); return BNC_ERR_STATE; }
+    cudaSetDevice(b->device);
+    int rc = sync_stream(b);
+    if (rc != BNC_OK) return rc;
+    std::memset(out, 0, sizeof(*out));
+    uint32_t st[4] = {0, 0, 0, 0};
+    double led[14] = {0};
+    cudaError_t e = cudaMemcpy(st, b->dev.jac_stats, sizeof(st), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(led, b->dev.ledger, sizeof(led), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && reset) {
+        e = cudaMemset(b->dev.jac_stats, 0, sizeof(st));
+        if (e == cudaSuccess) e = cudaMemset(b->dev.ledger, 0, sizeof(led));
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "diffusion statistics");
+    out->max_sweeps_v = st[0];
+    out->max_sweeps_phi = st[1];
+    out->capped_v = st[2];
+    out->capped_phi = st[3];
+    for (int q = 0; q < 7; q++) { out->rounding[q] = led[q]; out->bath[q] = led[7 + q]; }
+    return BNC_OK;
+}
+
 // ---- The daemon's state frame (daemon_state.cpp:66-79) from the device state ----
 int bnc_state_frame(void* sim, void* buf, uint64_t cap, uint64_t* len) {
     if (!sim || !len) { set_error("null argument"); return BNC_ERR_ARG; }

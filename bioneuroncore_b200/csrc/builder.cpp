@@ -1165,6 +1165,30 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
                   "(227 KB per CTA)", mts, mst, mte, host->smem_bytes);
         return BNC_ERR_UNSUPPORTED;
     }
+    // ---- convergence groups of the residual-controlled Jacobi mode: the connected
+    // components, numbered in device order within each tile (within each tile pair for
+    // 2-CTA clusters, whose halves share one component); bit 15 marks a group's first
+    // segment ----
+    std::vector<uint16_t> seg_grp(n, 0);
+    {
+        const uint32_t span = host->cluster == 2 ? 2u : 1u;
+        std::vector<uint32_t> local(n, UINT32_MAX);   // component root -> group index of the current tile
+        for (uint32_t t0 = 0; t0 < T; t0 += span) {
+            const uint32_t d0 = tile_seg_beg[t0], d1 = tile_seg_beg[std::min(T, t0 + span)];
+            uint32_t next = 0;
+            for (uint32_t d = d0; d < d1; d++) {
+                const uint32_t root = comp_of[host->perm[d]];
+                bool first = false;
+                if (local[root] == UINT32_MAX) { local[root] = next++; first = true; }
+                if (local[root] >= 0x800u) {
+                    set_error("tile %u holds more than 2048 components", t0);
+                    return BNC_ERR_UNSUPPORTED;
+                }
+                seg_grp[d] = (uint16_t)(local[root] | (first ? 0x8000u : 0u));
+            }
+            for (uint32_t d = d0; d < d1; d++) local[comp_of[host->perm[d]]] = UINT32_MAX;
+        }
+    }
     // ---- upload (skipped for a host-only plan) ----
     int rc = BNC_OK;
     dev->n_seg = n; dev->n_tiles = T; dev->n_items = NI; dev->n_phases = n_phases;
@@ -1269,6 +1293,12 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
         }
         dev->spike_count = zeros<uint32_t>(allocs, n, &rc);
         dev->err_flag = zeros<int>(allocs, 1, &rc);
+        dev->seg_grp = up(allocs, seg_grp, &rc);
+        dev->jac_stats = zeros<uint32_t>(allocs, 4, &rc);
+        dev->ledger = zeros<double>(allocs, 14, &rc);
+        dev->diff_mode = 0;
+        dev->jac_max = 0;
+        dev->jac_tol = 0.0;
         if (rc == BNC_OK) rc = upload_stimuli(stim, *host, dev, allocs);
         if (rc != BNC_OK) { set_error("device allocation/upload failed (%d)", rc); return rc; }
     }

@@ -115,7 +115,10 @@ __host__ __device__ inline size_t diff_layout(uint32_t S, uint32_t E, unsigned c
     p = take(8 * Ee); if (t) t->ed = (double*)p;
     p = take(4 * Ee); if (t) t->gax = (float*)p;
     p = take(4 * Ee); if (t) t->dve = (float*)p;
-    p = take(4 * 7 * Ee); if (t) t->fl = (float*)p;    // [7][E] (Fick passes use row 0)
+    // [7][E] (Fick passes use row 0); during the Jacobi solves of the residual mode the
+    // FP64 iterates (2 x S doubles) and the convergence-group bits (130 words)
+    const size_t fl_words = 7 * Ee > 4 * (size_t)S + 130 ? 7 * Ee : 4 * (size_t)S + 130;
+    p = take(4 * fl_words); if (t) t->fl = (float*)p;
     p = take(4 * 7 * Ee); if (t) t->coef = (float*)p;
     p = take(4 * Ee); if (t) t->ie = (float*)p;
     p = take(4 * Ee); if (t) t->earea = (float*)p;
@@ -203,12 +206,117 @@ __device__ __forceinline__ void fick(const DiffSmem& t, int ns, int ne, int tid,
     tile_sync<CL>();
 }
 
-}  // namespace
+// ---- residual-controlled Jacobi (NetDev::diff_mode bit 0) ----
+// A convergence group is a connected component.  Each sweep updates the segments of
+// the groups still iterating; a segment whose value moved by more than jac_tol sets its
+// group's bit; a group whose bit stays clear is done (its last sweep kept).  The CTA
+// (the cluster, for tile pairs) stops when every group is done or after jac_max sweeps.
+struct ResidualBufs {
+    double* wa;
+    double* wb;
+    unsigned* bits;   // [2][64] group bits by sweep parity, then [2] cluster flags
+};
+
+__device__ __forceinline__ ResidualBufs residual_bufs(const DiffSmem& t, uint32_t S) {
+    ResidualBufs r;
+    r.wa = reinterpret_cast<double*>(t.fl);
+    r.wb = r.wa + S;
+    r.bits = reinterpret_cast<unsigned*>(r.wb + S);
+    return r;
+}
+
+// OR of a predicate over the CTA, or over both CTAs of a cluster pair (flag[parity] of
+// each CTA carries its half; the parity alternates between calls so a value is never
+// overwritten before the peer has read it).  A barrier of the tile either way.
+template <int CL>
+__device__ __forceinline__ bool tile_or(bool pred, unsigned* flag, unsigned parity, int tid) {
+    if constexpr (CL == 2) {
+        const int local = __syncthreads_or(pred ? 1 : 0);
+        cooperative_groups::cluster_group cl = cooperative_groups::this_cluster();
+        if (tid == 0) flag[parity] = (unsigned)local;
+        cl.sync();
+        const unsigned* pf = cl.map_shared_rank(flag, cl.block_rank() ^ 1u);
+        return local != 0 || pf[parity] != 0u;
+    } else {
+        return __syncthreads_or(pred ? 1 : 0) != 0;
+    }
+}
 
 template <int CL>
+__device__ __forceinline__ unsigned peer_bits(const unsigned* w) {
+    if constexpr (CL == 2) {
+        cooperative_groups::cluster_group cl = cooperative_groups::this_cluster();
+        return *cl.map_shared_rank(const_cast<unsigned*>(w), cl.block_rank() ^ 1u);
+    } else {
+        return 0u;
+    }
+}
+
+// Runs one residual-controlled solve starting from rb.wa (own and ghost values set);
+// update(w) returns this thread's new value from the iterate w.  Returns the buffer
+// holding the result.  slot 0: the V_m solve, 1: the phi_e solve (sweep statistics).
+template <int CL, bool kPhi, typename F>
+__device__ __forceinline__ const double* residual_solve(const NetDev& d, const DiffSmem& t, ResidualBufs rb,
+                                                        uint32_t gw, int i, int ns, int ng, uint32_t S, int tid,
+                                                        int nth, F&& update, int slot) {
+    (void)kPhi;
+    unsigned* bits = rb.bits;
+    for (int k = tid; k < 130; k += nth) bits[k] = 0u;
+    const uint32_t grp = gw & 0x7FFu;
+    const bool leader = (gw & 0x8000u) != 0u;
+    const unsigned gbit = 1u << (grp & 31u);
+    const uint32_t gword = grp >> 5;
+    double* wa = rb.wa;
+    double* wb = rb.wb;
+    bool done = !(i < ns);
+    uint32_t it = 0;
+    tile_sync<CL>();
+    while (it < d.jac_max) {
+        unsigned* cur = bits + (it & 1u) * 64;
+        if (i < ns) {
+            double nv = wa[i];
+            if (!done) {
+                nv = update(static_cast<const double*>(wa));
+                if (fabs(nv - wa[i]) > d.jac_tol) atomicOr(&cur[gword], gbit);
+            }
+            wb[i] = nv;
+        }
+        tile_sync<CL>();
+        halo<CL>(wb, 1, S, ns, ng, t.gsrc, tid, nth);
+        bool more = false;
+        if (!done) {
+            const unsigned w = cur[gword] | peer_bits<CL>(cur + gword);
+            more = (w & gbit) != 0u;
+            if (!more) done = true;
+        }
+        for (int k = tid; k < 64; k += nth) bits[((it + 1) & 1u) * 64 + k] = 0u;
+        it++;
+        const bool any = tile_or<CL>(more, bits + 128, it & 1u, tid);
+        double* tmp = wa; wa = wb; wb = tmp;
+        if (!any) break;
+    }
+    if (i < ns && leader && !done) atomicAdd(&d.jac_stats[2 + slot], 1u);
+    if (tid == 0) atomicMax(&d.jac_stats[slot], it);
+    return wa;
+}
+
+// Adds a warp's values to a per-CTA FP64 ledger slot (every thread of the CTA calls it).
+__device__ __forceinline__ void ledger_add(double* sh, int slot, double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xFFFFFFFFu, v, o);
+    if ((threadIdx.x & 31u) == 0u) atomicAdd(&sh[slot], v);
+}
+
+}  // namespace
+
+// OPT 0: the reference's fixed-sweep solves (the default); OPT 1: the options of
+// NetDev::diff_mode compiled in (residual-controlled solves, the ion ledger).
+template <int CL, int OPT>
 __global__ void __launch_bounds__(1024)
 k_diffusion(NetDev d, float dt, unsigned long long tick, uint32_t S, uint32_t E) {
     extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ double sh_ledger[14];   // per ion: FP32 rounding of the NP updates, bath exchange
+    if (threadIdx.x < 14) sh_ledger[threadIdx.x] = 0.0;
     DiffSmem t;
     diff_layout(S, E, smem, &t);
     const int tid = threadIdx.x;
@@ -367,6 +475,40 @@ k_diffusion(NetDev d, float dt, unsigned long long tick, uint32_t S, uint32_t E)
         }
         double* phi = t.phiA;
         double* phn = t.phiB;
+        if (OPT && (d.diff_mode & 1u)) {
+            // residual-controlled: sweeps in phiA/phiB until the group converges; the
+            // result is copied into phiA, where the fixed-sweep solve leaves it
+            ResidualBufs rb = residual_bufs(t, S);
+            rb.wa = t.phiA;
+            rb.wb = t.phiB;
+            const uint32_t gw = (i < ns) ? d.seg_grp[s0 + i] : 0u;
+            const double* res = residual_solve<CL, true>(d, t, rb, gw, i, ns, ng, S, tid, nth, [&](const double* w) {
+                double pn = 0.0;
+                if (st.n >= 0) {
+#pragma unroll
+                    for (int k = 0; k < kDeg; k++)
+                        if (k < pn_cnt) pn += pg[k] * w[po[k]];
+                } else {
+                    for (int k = t.incoff[i]; k < t.incoff[i + 1]; k++) {
+                        const uint16_t ent = t.inc[k];
+                        const int e = ent & 0x7FFF;
+                        const double g = t.ed[e];
+                        if (g <= 0.0) continue;
+                        const int o = (ent & 0x8000) ? t.ea[e] : t.eb[e];
+                        pn += g * w[o];
+                    }
+                }
+                double v = (diag > 1e-9) ? (pn - itot) / diag : 0.0;
+                if (v > 10.0) v = 10.0;
+                if (v < -10.0) v = -10.0;
+                return v;
+            }, 1);
+            if (res != t.phiA) {
+                if (i < ns) t.phiA[i] = res[i];
+                for (int g = tid; g < ng; g += nth) t.phiA[ns + g] = res[ns + g];
+            }
+            tile_sync<CL>();
+        } else
         // Tiles whose every segment has at most two stencil entries (chains and their
         // somata): the same sums over two registers' worth of entries, two sweeps per
         // iteration so the buffers need no swap.  50 sweeps end in phiA either way.
@@ -493,12 +635,13 @@ k_diffusion(NetDev d, float dt, unsigned long long tick, uint32_t S, uint32_t E)
                 t.ie[e] = ie;
             }
             tile_sync<CL>();
-            if (i < ns) {   // reads connection fluxes and its own concentrations: in place
-                const float vf = t.vf[i];
+            {   // reads connection fluxes and its own concentrations: in place
+                const float vf = i < ns ? t.vf[i] : 1.0f;
                 const double yv = 1.0 / (double)vf;
 #pragma unroll 1
                 for (int q = 0; q < 7; q++) {
-                    double acc = 0.0;
+                    double acc = 0.0, lost = 0.0;
+                    if (i < ns) {
                     if (st.n >= 0) {
 #pragma unroll
                         for (int k = 0; k < kDeg; k++) {
@@ -518,7 +661,12 @@ k_diffusion(NetDev d, float dt, unsigned long long tick, uint32_t S, uint32_t E)
                             else acc -= (double)t.fl[q * E + e] / vf;
                         }
                     }
-                    t.in[q * S + i] = (float)((double)t.in[q * S + i] + (double)(float)acc);
+                    const float old = t.in[q * S + i];
+                    const float upd = (float)((double)old + (double)(float)acc);
+                    t.in[q * S + i] = upd;
+                    lost = ((double)upd - (double)old - acc) * (double)vf;
+                    }
+                    if (OPT && (d.diff_mode & 2u)) ledger_add(sh_ledger, q, lost);
                 }
             }
             tile_sync<CL>();
@@ -527,7 +675,7 @@ k_diffusion(NetDev d, float dt, unsigned long long tick, uint32_t S, uint32_t E)
                 t.ie[e] = t.ie[e] - t.gax[e] * t.dve[e];
             }
             tile_sync<CL>();
-            float rhs = 0.0f, den = 1.0f;
+            float rhs = 0.0f, den = 1.0f, C_dtv = 1.0f, inpv = 0.0f;
             if (i < ns) {
                 float inp = 0.0f;
                 if (st.n >= 0) {
@@ -550,12 +698,42 @@ k_diffusion(NetDev d, float dt, unsigned long long tick, uint32_t S, uint32_t E)
                 if (C_dt < 1e-9f) C_dt = 1e-9f;
                 rhs = C_dt * t.V[i] + inp;
                 den = C_dt + gd;
+                C_dtv = C_dt;
+                inpv = inp;
                 t.vnA[i] = t.V[i];
             }
             for (int g = tid; g < ng; g += nth) t.vnA[ns + g] = t.V[ns + g];
             tile_sync<CL>();
             float* vc = t.vnA;
             float* vn = t.vnB;
+            if (OPT && (d.diff_mode & 1u)) {
+                // residual-controlled FP64 Jacobi: iterates in the (dead) flux buffer, the
+                // result rounded to float into vnA
+                ResidualBufs rb = residual_bufs(t, S);
+                if (i < ns) rb.wa[i] = (double)t.V[i];
+                for (int g = tid; g < ng; g += nth) rb.wa[ns + g] = (double)t.V[ns + g];
+                const double rhs_d = (double)C_dtv * (double)t.V[i < ns ? i : 0] + (double)inpv;
+                const double den_d = (double)C_dtv + (double)gd;
+                const uint32_t gw = (i < ns) ? d.seg_grp[s0 + i] : 0u;
+                const double* res = residual_solve<CL, false>(d, t, rb, gw, i, ns, ng, S, tid, nth, [&](const double* w) {
+                    double off = 0.0;
+                    if (st.n >= 0) {
+#pragma unroll
+                        for (int k = 0; k < kDeg; k++)
+                            if (k < vn_cnt) off += (double)vg[k] * w[vo[k]];
+                    } else {
+                        for (int k = t.incoff[i]; k < t.incoff[i + 1]; k++) {
+                            const uint16_t ent = t.inc[k];
+                            const int e = ent & 0x7FFF;
+                            if (!t.ei[e]) continue;
+                            const int o = (ent & 0x8000) ? t.ea[e] : t.eb[e];
+                            off += (double)t.gax[e] * w[o];
+                        }
+                    }
+                    return (rhs_d + off) / den_d;
+                }, 0);
+                if (i < ns) t.vnA[i] = (float)res[i];
+            } else
             // as for phi_e: two-entry stencils in registers, two sweeps per iteration
             if (CL == 1 && __syncthreads_and(st.n >= 0 && vn_cnt <= 2)) {
                 const bool h0 = vn_cnt > 0, h1 = vn_cnt > 1;
@@ -639,6 +817,7 @@ k_diffusion(NetDev d, float dt, unsigned long long tick, uint32_t S, uint32_t E)
                     t.ed[e] = flux;
                 }
                 tile_sync<CL>();
+                double lost = 0.0;
                 if (i < ns) {   // in place, as above
                     const float vf = t.vf[i];
                     const float vx = vf * EXTRA_VOLUME_RATIO;
@@ -661,8 +840,12 @@ k_diffusion(NetDev d, float dt, unsigned long long tick, uint32_t S, uint32_t E)
                             else acc -= t.ed[e] / (vf * EXTRA_VOLUME_RATIO);
                         }
                     }
-                    t.out[q * S + i] = (float)((double)t.out[q * S + i] + acc);
+                    const float old = t.out[q * S + i];
+                    const float upd = (float)((double)old + acc);
+                    t.out[q * S + i] = upd;
+                    lost = ((double)upd - (double)old - acc) * (double)vx;
                 }
+                if (OPT && (d.diff_mode & 2u)) ledger_add(sh_ledger, q, lost);
                 tile_sync<CL>();
                 halo<CL>(t.out + (size_t)q * S, 1, S, ns, ng, t.gsrc, tid, nth);
             }
@@ -708,7 +891,26 @@ k_diffusion(NetDev d, float dt, unsigned long long tick, uint32_t S, uint32_t E)
             fick<CL, true, true>(t, ns, ne, tid, nth, i, st, 0.01f, 1e-9f, dt);
             if (i < ns) d.txn[s0 + i] = t.nb[i];
         }
-        if (i < ns) {
+        if (OPT && (d.diff_mode & 2u)) {
+            // the same bath relaxation and clamp, with each ion's stored change times the
+            // segment's extracellular volume added to the ledger (the bath exchange)
+#pragma unroll 1
+            for (int q = 0; q < 7; q++) {
+                double x = 0.0;
+                if (i < ns) {
+                    const float old = t.out[q * S + i];
+                    double e = (double)old;
+                    e += (kBathIon[q] - e) * dt / 1.0f;
+                    if (e < 1e-9) e = 1e-9;
+                    if (e > 1000.0) e = 1000.0;
+                    t.out[q * S + i] = (float)e;
+                    x = ((double)t.out[q * S + i] - (double)old) * (double)(t.vf[i] * EXTRA_VOLUME_RATIO);
+                }
+                ledger_add(sh_ledger, 7 + q, x);
+            }
+            __syncthreads();
+            if (tid < 14) atomicAdd(&d.ledger[tid], sh_ledger[tid]);
+        } else if (i < ns) {
 #pragma unroll
             for (int q = 0; q < 7; q++) {
                 double e = (double)t.out[q * S + i];
@@ -760,10 +962,18 @@ cudaError_t prepare_diffusion(const NetHost& host, cudaStream_t stream) {
         g_ntd_ready[dev] = true;
     }
     const size_t smem = diffusion_smem_bytes(host.max_tile_stride, host.max_tile_edges);
-    if (smem > 48 * 1024)
-        return host.cluster == 2
-                   ? cudaFuncSetAttribute(k_diffusion<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
-                   : cudaFuncSetAttribute(k_diffusion<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (smem > 48 * 1024) {
+        if (host.cluster == 2) {
+            e = cudaFuncSetAttribute(k_diffusion<2, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e == cudaSuccess)
+                e = cudaFuncSetAttribute(k_diffusion<2, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        } else {
+            e = cudaFuncSetAttribute(k_diffusion<1, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e == cudaSuccess)
+                e = cudaFuncSetAttribute(k_diffusion<1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        }
+        return e;
+    }
     return cudaSuccess;
 }
 
@@ -772,6 +982,7 @@ cudaError_t enqueue_diffusion(const NetDev& dev, const NetHost& host, float dt, 
     const uint32_t S = host.max_tile_stride, E = host.max_tile_edges;
     const size_t smem = diffusion_smem_bytes(S, E);
     const uint32_t threads = diffusion_threads(host.max_tile_segs);
+    const bool opt = dev.diff_mode != 0u;
     if (host.cluster == 2) {
         // tiles in pairs: one 2-CTA cluster per pair (n_tiles is even)
         cudaLaunchConfig_t cfg = {};
@@ -786,9 +997,11 @@ cudaError_t enqueue_diffusion(const NetDev& dev, const NetHost& host, float dt, 
         attr[0].val.clusterDim.z = 1;
         cfg.attrs = attr;
         cfg.numAttrs = 1;
-        return cudaLaunchKernelEx(&cfg, k_diffusion<2>, dev, dt, tick, S, E);
+        return opt ? cudaLaunchKernelEx(&cfg, k_diffusion<2, 1>, dev, dt, tick, S, E)
+                   : cudaLaunchKernelEx(&cfg, k_diffusion<2, 0>, dev, dt, tick, S, E);
     }
-    k_diffusion<1><<<dev.n_tiles, threads, smem, stream>>>(dev, dt, tick, S, E);
+    if (opt) k_diffusion<1, 1><<<dev.n_tiles, threads, smem, stream>>>(dev, dt, tick, S, E);
+    else k_diffusion<1, 0><<<dev.n_tiles, threads, smem, stream>>>(dev, dt, tick, S, E);
     return cudaGetLastError();
 }
 

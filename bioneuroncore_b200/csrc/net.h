@@ -163,6 +163,17 @@ struct NetDev {
     uint4* ev_buf;
     uint32_t* ev_n;
     uint32_t ev_cap;
+    // Electrodiffusion options (bnc_set_diffusion_mode).  diff_mode bit 0: the Jacobi
+    // solves iterate in FP64 until no value of a convergence group changes by more than
+    // jac_tol in a sweep (at most jac_max sweeps) instead of the reference's fixed 50;
+    // bit 1: the per-ion FP64 ledger of step 2.5 is kept.
+    uint32_t diff_mode;
+    uint32_t jac_max;
+    double jac_tol;
+    uint16_t* seg_grp;        // [n_seg] convergence group (connected component) within the
+                              // tile or tile pair, bit 15: the group's first segment
+    uint32_t* jac_stats;      // [4] max V sweeps, max phi sweeps, V and phi group solves at the cap
+    double* ledger;           // [14] per ion: FP32 rounding of the Nernst-Planck updates, bath exchange
 };
 
 // How components are grouped: a warp group holds components until their segments

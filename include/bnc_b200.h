@@ -333,6 +333,34 @@ int bnc_save_bion(void* sim, const char* filename);
 /* Message for the last error on this thread ("" when none). */
 const char* bnc_last_error(void);
 
+/* Electrodiffusion options of step 2.5 for the loaded network.  They have no
+ * counterpart in the reference, which always runs 50 Jacobi sweeps per solve
+ * (diffusion_kernel.h:25,27); the default (flags 0) is that parity mode.
+ *   BNC_DIFFUSION_RESIDUAL  the phi_e solve and each V_m solve iterate in FP64
+ *                           until no value of a convergence group (a connected
+ *                           component) changes by more than `tol` in a sweep,
+ *                           at most `max_sweeps` sweeps.  V_m is stored as float.
+ *   BNC_DIFFUSION_LEDGER    an FP64 ledger per ion over the run: `rounding`, the
+ *                           amount (concentration x volume) that storing the
+ *                           Nernst-Planck updates in FP32 added, and `bath`, the
+ *                           amount the bath relaxation and clamps added to the
+ *                           extracellular space.  Step 2.5 changes each ion's total
+ *                           (intracellular + extracellular amount) by exactly their
+ *                           sum, up to FP64 rounding.
+ * Loading a network resets the mode to 0.  bnc_diffusion_stats reads the largest
+ * sweep counts of a solve, the group solves that reached max_sweeps and the ledger
+ * accumulated since the load or the last reset. */
+#define BNC_DIFFUSION_RESIDUAL 1u
+#define BNC_DIFFUSION_LEDGER 2u
+typedef struct {
+    uint32_t max_sweeps_v, max_sweeps_phi;   /* most sweeps of one V_m / phi_e solve */
+    uint32_t capped_v, capped_phi;           /* group solves that stopped at max_sweeps */
+    double rounding[7];                      /* per ion, amount units (mM x um^3) */
+    double bath[7];
+} BncDiffusionStats;
+int bnc_set_diffusion_mode(void* sim, uint32_t flags, double tol, uint32_t max_sweeps);
+int bnc_diffusion_stats(void* sim, BncDiffusionStats* out, int reset);
+
 /* The daemon's MSG_STATE_FRAME payload (daemon_state.cpp:66-79): the tick counter
  * (u64), the segment and synapse counts (u32 each), then the Segment and Synapse
  * records of the current state, filled from the device state directly into `buf`.

@@ -15,6 +15,8 @@
  * listed in bo_type_supported(), chemical synapses, pre-autoreceptors that are
  * bouton K/Na channels, no mechano stimuli, no consolidation/nuclei.
  */
+#include <math.h>
+#include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
 #include <stdio.h>
@@ -59,6 +61,15 @@ typedef struct BoSim {
     float *log_amt;
     uint8_t *log_slot;
     uint32_t log_cap, log_n;
+    /* electrodiffusion options (bo_set_diffusion_mode): bit 0 residual-controlled FP64
+     * Jacobi per convergence group (connected component), bit 1 the per-ion ledger */
+    uint32_t dmode, jmax;
+    double jtol;
+    uint32_t *grp, n_grp;   /* group of each segment */
+    uint8_t *gdone, *gmore; /* per group */
+    double *vd, *vnd, *offdd, *rhsd, *dend, *phin;
+    uint32_t jstats[4];     /* max V sweeps, max phi sweeps, V and phi group solves at the cap */
+    double ledger[14];      /* per ion: rounding of the FP32 NP updates, bath exchange */
 } BoSim;
 
 static void bo_log_release(BoSim* S, uint32_t syn, uint64_t tick, float amt, uint8_t slot) {
@@ -157,6 +168,39 @@ static void bo_solve_phi_e(BoSim* S) {
         c->diag[a] += g;
         c->diag[b] += g;
     }
+    if (S->dmode & 1u) {   /* residual-controlled: sweeps until every group converged */
+        memset(S->gdone, 0, S->n_grp);
+        uint32_t it = 0;
+        while (it < S->jmax) {
+            for (uint32_t i = 0; i < n; i++) c->phi_new[i] = 0.0;
+            for (uint32_t i = 0; i < m; i++) {
+                uint32_t a = S->conn[i].segment_a, b = S->conn[i].segment_b;
+                if (a >= n || b >= n) continue;
+                double g = c->goff_d[i];
+                if (g <= 0.0) continue;
+                c->phi_new[a] += g * c->phi[b];
+                c->phi_new[b] += g * c->phi[a];
+            }
+            memset(S->gmore, 0, S->n_grp);
+            for (uint32_t i = 0; i < n; i++) {
+                if (S->gdone[S->grp[i]]) { S->phin[i] = c->phi[i]; continue; }
+                double v = (c->diag[i] > 1e-9) ? (c->phi_new[i] - sg[i].ibuf) / c->diag[i] : 0.0;
+                if (v > 10.0) v = 10.0;
+                if (v < -10.0) v = -10.0;
+                if (fabs(v - c->phi[i]) > S->jtol) S->gmore[S->grp[i]] = 1;
+                S->phin[i] = v;
+            }
+            memcpy(c->phi, S->phin, (size_t)n * sizeof(double));
+            it++;
+            int any = 0;
+            for (uint32_t g = 0; g < S->n_grp; g++)
+                if (!S->gdone[g]) { if (S->gmore[g]) any = 1; else S->gdone[g] = 1; }
+            if (!any) break;
+        }
+        if (it > S->jstats[1]) S->jstats[1] = it;
+        for (uint32_t g = 0; g < S->n_grp; g++) S->jstats[3] += S->gdone[g] ? 0u : 1u;
+        return;
+    }
     for (int iter = 0; iter < 50; iter++) {
         for (uint32_t i = 0; i < n; i++) c->phi_new[i] = 0.0;
         for (uint32_t i = 0; i < m; i++) {
@@ -173,6 +217,12 @@ static void bo_solve_phi_e(BoSim* S) {
             if (c->phi[i] < -10.0) c->phi[i] = -10.0;
         }
     }
+}
+
+/* the volume the Nernst-Planck updates divide by: float, at least 1e-6 um^3 */
+static float bo_vol_f(const OSeg* s) {
+    float v = (float)bo_seg_volume(s);
+    return v < 1e-6f ? 1e-6f : v;
 }
 
 /* diffusion_kernel.h:115-364 */
@@ -230,6 +280,44 @@ static void bo_diffusion(BoSim* S, float dt) {
             c->inp[b] -= I_np - g_ax * dV;
         }
         for (uint32_t i = 0; i < n; i++) { c->Vold[i] = sg[i].V; c->Vnew[i] = sg[i].V; }
+        if (S->dmode & 1u) {   /* residual-controlled, FP64 iterates */
+            for (uint32_t i = 0; i < n; i++) {
+                float C_dt = bo_capacitance(&sg[i]) / dt_sub;
+                if (C_dt < 1e-9f) C_dt = 1e-9f;
+                S->vd[i] = (double)c->Vold[i];
+                S->rhsd[i] = (double)C_dt * (double)c->Vold[i] + (double)c->inp[i];
+                S->dend[i] = (double)C_dt + (double)c->gdiag[i];
+            }
+            memset(S->gdone, 0, S->n_grp);
+            uint32_t it = 0;
+            while (it < S->jmax) {
+                for (uint32_t i = 0; i < n; i++) S->offdd[i] = 0.0;
+                for (uint32_t i = 0; i < m; i++) {
+                    BncIntraConnection* cn = &S->conn[i];
+                    uint32_t a = cn->segment_a, b = cn->segment_b;
+                    if (a >= n || b >= n) continue;
+                    if (cn->is_intracellular == 0) continue;
+                    S->offdd[a] += (double)c->goff[i] * S->vd[b];
+                    S->offdd[b] += (double)c->goff[i] * S->vd[a];
+                }
+                memset(S->gmore, 0, S->n_grp);
+                for (uint32_t i = 0; i < n; i++) {
+                    if (S->gdone[S->grp[i]]) { S->vnd[i] = S->vd[i]; continue; }
+                    const double nv = (S->rhsd[i] + S->offdd[i]) / S->dend[i];
+                    if (fabs(nv - S->vd[i]) > S->jtol) S->gmore[S->grp[i]] = 1;
+                    S->vnd[i] = nv;
+                }
+                double* tmp = S->vd; S->vd = S->vnd; S->vnd = tmp;
+                it++;
+                int any = 0;
+                for (uint32_t g = 0; g < S->n_grp; g++)
+                    if (!S->gdone[g]) { if (S->gmore[g]) any = 1; else S->gdone[g] = 1; }
+                if (!any) break;
+            }
+            if (it > S->jstats[0]) S->jstats[0] = it;
+            for (uint32_t g = 0; g < S->n_grp; g++) S->jstats[2] += S->gdone[g] ? 0u : 1u;
+            for (uint32_t i = 0; i < n; i++) c->Vnew[i] = (float)S->vd[i];
+        } else
         for (int iter = 0; iter < 50; iter++) {
             for (uint32_t i = 0; i < n; i++) c->offd[i] = 0.0f;
             for (uint32_t i = 0; i < m; i++) {
@@ -248,8 +336,12 @@ static void bo_diffusion(BoSim* S, float dt) {
         }
         for (uint32_t i = 0; i < n; i++) sg[i].V = c->Vnew[i];
         for (uint32_t i = 0; i < n; i++)
-            for (int ion = 0; ion < 7; ion++)
-                sg[i].in[ion] = (float)((double)sg[i].in[ion] + (double)(float)c->intra_acc[i * 7 + ion]);
+            for (int ion = 0; ion < 7; ion++) {
+                const float old = sg[i].in[ion];
+                const double acc = c->intra_acc[i * 7 + ion];
+                sg[i].in[ion] = (float)((double)old + (double)(float)acc);
+                if (S->dmode & 2u) S->ledger[ion] += ((double)sg[i].in[ion] - (double)old - acc) * (double)bo_vol_f(&sg[i]);
+            }
     }
 
     /* extracellular Nernst-Planck, 5 substeps (diffusion_kernel.h:244-281) */
@@ -280,8 +372,14 @@ static void bo_diffusion(BoSim* S, float dt) {
             }
         }
         for (uint32_t i = 0; i < n; i++)
-            for (int ion = 0; ion < 7; ion++)
-                sg[i].out[ion] = (float)((double)sg[i].out[ion] + c->extra_acc[i * 7 + ion]);
+            for (int ion = 0; ion < 7; ion++) {
+                const float old = sg[i].out[ion];
+                const double acc = c->extra_acc[i * 7 + ion];
+                sg[i].out[ion] = (float)((double)old + acc);
+                if (S->dmode & 2u)
+                    S->ledger[ion] += ((double)sg[i].out[ion] - (double)old - acc) *
+                                      (double)(bo_vol_f(&sg[i]) * EXTRA_VOLUME_RATIO);
+            }
     }
 
     /* NT / ATP / heat / transcription (diffusion_kernel.h:284-345) */
@@ -340,11 +438,15 @@ static void bo_diffusion(BoSim* S, float dt) {
     }
     for (uint32_t i = 0; i < n; i++) {
         for (int ion = 0; ion < 7; ion++) {
+            const float old = sg[i].out[ion];
             double e = (double)sg[i].out[ion];
             e += (BATH_ION[ion] - e) * dt / 1.0f;
             if (e < 1e-9) e = 1e-9;
             if (e > 1000.0) e = 1000.0;
             sg[i].out[ion] = (float)e;
+            if (S->dmode & 2u)
+                S->ledger[7 + ion] += ((double)sg[i].out[ion] - (double)old) *
+                                      (double)(bo_vol_f(&sg[i]) * EXTRA_VOLUME_RATIO);
         }
         for (int nt = 0; nt < 15; nt++) {
             sg[i].intra_nt[nt] += c->ntd_in[i * 15 + nt];
@@ -771,7 +873,55 @@ BoSim* bo_create(const BncBionData* d, const BncCurrentStimulus* stim, uint32_t 
 void bo_destroy(BoSim* S) {
     if (!S) return;
     free(S->seg); free(S->conn); free(S->syn); free(S->delay); free(S->stim); free(S->spike_count);
+    free(S->grp); free(S->gdone); free(S->gmore);
+    free(S->vd); free(S->vnd); free(S->offdd); free(S->rhsd); free(S->dend); free(S->phin);
     free(S);
+}
+
+static uint32_t bo_find(uint32_t* p, uint32_t x) {
+    while (p[x] != x) { p[x] = p[p[x]]; x = p[x]; }
+    return x;
+}
+
+/* Options of step 2.5 beside the reference's fixed 50 sweeps: flags bit 0 makes the
+ * phi_e and V_m solves iterate in FP64 until no value of a convergence group (a
+ * connected component over all valid connections) changes by more than tol in a
+ * sweep, at most max_sweeps sweeps; bit 1 keeps the per-ion FP64 ledger. */
+void bo_set_diffusion_mode(BoSim* S, uint32_t flags, double tol, uint32_t max_sweeps) {
+    const uint32_t n = S->n;
+    S->dmode = flags;
+    S->jtol = tol;
+    S->jmax = max_sweeps;
+    if (!S->grp) {
+        uint32_t* p = malloc((size_t)(n ? n : 1) * sizeof(uint32_t));
+        for (uint32_t i = 0; i < n; i++) p[i] = i;
+        for (uint32_t c = 0; c < S->m; c++) {
+            uint32_t a = S->conn[c].segment_a, b = S->conn[c].segment_b;
+            if (a >= n || b >= n) continue;
+            a = bo_find(p, a); b = bo_find(p, b);
+            if (a != b) { if (a < b) p[b] = a; else p[a] = b; }
+        }
+        S->grp = malloc((size_t)(n ? n : 1) * sizeof(uint32_t));
+        uint32_t* id = malloc((size_t)(n ? n : 1) * sizeof(uint32_t));
+        for (uint32_t i = 0; i < n; i++) id[i] = UINT32_MAX;
+        S->n_grp = 0;
+        for (uint32_t i = 0; i < n; i++) {
+            uint32_t r = bo_find(p, i);
+            if (id[r] == UINT32_MAX) id[r] = S->n_grp++;
+            S->grp[i] = id[r];
+        }
+        free(p); free(id);
+        size_t G = S->n_grp ? S->n_grp : 1, N = n ? n : 1;
+        S->gdone = calloc(G, 1); S->gmore = calloc(G, 1);
+        S->vd = calloc(N, 8); S->vnd = calloc(N, 8); S->offdd = calloc(N, 8);
+        S->rhsd = calloc(N, 8); S->dend = calloc(N, 8); S->phin = calloc(N, 8);
+    }
+}
+
+void bo_diffusion_stats(BoSim* S, uint32_t* stats4, double* ledger14, int reset) {
+    memcpy(stats4, S->jstats, sizeof(S->jstats));
+    memcpy(ledger14, S->ledger, sizeof(S->ledger));
+    if (reset) { memset(S->jstats, 0, sizeof(S->jstats)); memset(S->ledger, 0, sizeof(S->ledger)); }
 }
 
 void bo_run(BoSim* S, uint32_t ticks, float dt) {
@@ -823,6 +973,7 @@ void bo_get_seg_field(const BoSim* S, int field, int idx, float* out) {
             case 7: v = s->nt[idx]; break;
             case 8: v = ((idx >> 3) < s->nmod) ? s->mods[idx >> 3].st[idx & 7] : 0.0f; break;
             case 9: v = (float)S->spike_count[i]; break;
+            case 10: v = bo_vol_f(s); break;   /* the volume the Nernst-Planck updates divide by */
         }
         out[i] = v;
     }

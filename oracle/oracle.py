@@ -31,6 +31,8 @@ def oracle_lib():
         lib.bo_create.restype = vp
         lib.bo_destroy.argtypes = [vp]
         lib.bo_run.argtypes = [vp, C.c_uint32, C.c_float]
+        lib.bo_set_diffusion_mode.argtypes = [vp, C.c_uint32, C.c_double, C.c_uint32]
+        lib.bo_diffusion_stats.argtypes = [vp, vp, vp, C.c_int]
         lib.bo_run_trace.argtypes = [vp, C.c_uint32, C.c_float, vp, C.c_uint32, vp]
         lib.bo_get_seg_field.argtypes = [vp, C.c_int, C.c_int, vp]
         lib.bo_get_syn_field.argtypes = [vp, C.c_int, C.c_int, vp]
@@ -93,6 +95,19 @@ class Oracle:
             raise ValueError(err.value.decode())
         self.n_seg = net.data.num_segments
         self.n_syn = net.data.num_synapses
+
+    def set_diffusion_mode(self, flags, tol=1e-6, max_sweeps=100000):
+        """bo_set_diffusion_mode: residual-controlled FP64 Jacobi solves (flag 1) and
+        the per-ion ledger (flag 2), as the backend's bnc_set_diffusion_mode."""
+        oracle_lib().bo_set_diffusion_mode(self.h, flags, C.c_double(tol), max_sweeps)
+
+    def diffusion_stats(self, reset=False):
+        """(stats[4], ledger[14]): max V and phi sweeps, capped V and phi group solves;
+        per ion the FP32 rounding of the Nernst-Planck updates, then the bath exchange."""
+        st = np.zeros(4, np.uint32)
+        led = np.zeros(14, np.float64)
+        oracle_lib().bo_diffusion_stats(self.h, st.ctypes.data, led.ctypes.data, 1 if reset else 0)
+        return st, led
 
     def run(self, ticks, dt, tick_stride=1):
         if tick_stride == 1:

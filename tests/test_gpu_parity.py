@@ -163,3 +163,75 @@ def test_components_split_across_a_cluster_bitexact():
         ora.run(step, DT)
         gpu.run_ticks(step, DT)
         _compare_all(ora, gpu, ora.n_syn, "split components after +%d" % step)
+
+
+def _mode_net(case):
+    from bioneuroncore_b200 import NetgenParams, NET_TREES, NET_LARGE, NET_SMALL, NETGEN_PERTURB_IONS
+    if case == "trees":   # 2,047-segment trees on 2-CTA clusters
+        return NetgenParams(family=NET_TREES, n_neurons=3, tree_depth=10, seed=8, flags=NETGEN_PERTURB_IONS)
+    if case == "large":   # one tile holding twelve neurons (twelve convergence groups)
+        return NetgenParams(family=NET_LARGE, n_neurons=12, n_synapses=300, seed=5)
+    if case == "split":   # 48-segment tiles: each 64-segment neuron on its own tile pair
+        return NetgenParams(family=NET_LARGE, n_neurons=6, n_synapses=200, seed=9)
+    return NetgenParams(family=NET_SMALL, n_neurons=16, seed=11)
+
+
+@pytest.mark.parametrize("case", ["trees", "large", "split", "small"])
+@pytest.mark.parametrize("cap", [100000, 5])
+def test_residual_diffusion_mode_bitexact(case, cap):
+    """The residual-controlled FP64 Jacobi mode and the ion ledger (bnc_set_diffusion_mode)
+    against the oracle's restatement of the same mode: the state bit for bit, the same
+    sweep counts and capped group solves (each convergence group -- a connected
+    component -- stops on its own, as the oracle's loop over groups does), and the FP64
+    ledger within summation-order rounding (1e-9 relative)."""
+    from bioneuroncore_b200 import Backend, BuildOptions, Network, DIFFUSION_RESIDUAL, DIFFUSION_LEDGER
+    p = _mode_net(case)
+    ora = Oracle(Network(p))
+    gpu = Backend()
+    if case == "split":
+        gpu.load_generated(p, BuildOptions(tile_segs=48))
+    else:
+        gpu.load_network(Network(p))
+    flags = DIFFUSION_RESIDUAL | DIFFUSION_LEDGER
+    ora.set_diffusion_mode(flags, 1e-6, cap)
+    gpu.set_diffusion_mode(flags, 1e-6, cap)
+    n_syn = ora.n_syn
+    for step in (1, 3):
+        ora.run(step, DT)
+        gpu.run_ticks(step, DT)
+        _compare_all(ora, gpu, n_syn, "%s residual cap %d after +%d" % (case, cap, step))
+    st_o, led_o = ora.diffusion_stats()
+    st = gpu.diffusion_stats()
+    assert (st.max_sweeps_v, st.max_sweeps_phi, st.capped_v, st.capped_phi) == tuple(int(x) for x in st_o)
+    if cap == 5:
+        assert st.capped_v > 0
+    else:
+        assert st.capped_v == 0 and st.capped_phi == 0
+    led = np.array(list(st.rounding) + list(st.bath))
+    assert np.all(np.abs(led - led_o) <= 1e-9 * np.abs(led_o).max() + 1e-300), (led, led_o)
+
+
+def test_ledger_closes_the_mass_balance_on_the_gpu():
+    """On a network where only step 2.5 moves ions, each ion's total amount in the
+    device state (FP32, summed in FP64) changes by the device ledger's rounding plus
+    bath terms, up to FP64 rounding of the sums."""
+    import test_diffusion_modes as tdm
+    from bioneuroncore_b200 import Backend, DIFFUSION_LEDGER
+    net = tdm.diffusion_only(depth=10)
+    ora = Oracle(tdm.diffusion_only(depth=10))   # the volumes the updates divide by
+    vol = ora.segment_field(10).astype(np.float64)
+    vx = (ora.segment_field(10) * tdm.EXTRA_VOLUME_RATIO).astype(np.float64)
+    gpu = Backend()
+    gpu.load_network(net)
+    gpu.set_diffusion_mode(DIFFUSION_LEDGER)
+
+    def amounts():
+        return np.array([(np.asarray(gpu.segment_field("ion_in", q), np.float64) * vol).sum() +
+                         (np.asarray(gpu.segment_field("ion_out", q), np.float64) * vx).sum() for q in range(7)])
+
+    before = amounts()
+    gpu.run_ticks(5, DT)
+    after = amounts()
+    st = gpu.diffusion_stats()
+    booked = np.array(st.rounding) + np.array(st.bath)
+    assert np.all(np.abs((after - before) - booked) <= 1e-11 * (np.abs(before) + 1.0)), (after - before, booked)
