@@ -59,6 +59,9 @@ def parse_args():
     ap.add_argument("--tree-ticks", type=int, default=20)
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-sweep", action="store_true")
+    ap.add_argument("--no-dropin", action="store_true")
+    ap.add_argument("--dropin-neurons", type=int, default=10000)
+    ap.add_argument("--dropin-ticks", type=int, default=10)
     ap.add_argument("--sweep-tasks", type=int, default=256)
     ap.add_argument("--sweep-ticks", type=int, default=1000)
     ap.add_argument("--adj-neurons", type=int, default=256)
@@ -440,6 +443,38 @@ def run_adjoint(a, device):
     }
 
 
+def run_dropin(a, device):
+    """The reference-facing drop-in call: gpu_backend_run_tick on a network loaded from
+    host Segment/Synapse records (bnc_load_aos).  After every tick the call leaves those
+    records coherent with the device state (the reference's callers read them between
+    ticks), so each tick includes the device-to-host copy of the changing state and its
+    scatter into the records.  Wall clock per tick, beside the device-only tick of the
+    same network."""
+    import numpy as np
+    from bioneuroncore_b200 import Backend, Network, NetgenParams, NET_LARGE
+    net = Network(NetgenParams(family=NET_LARGE, n_neurons=a.dropin_neurons, seed=a.seed))
+    b = Backend(device)
+    b.load_network(net)
+    b.run_tick(DT)                                  # first call: staging buffers
+    t0 = time.perf_counter()
+    for _ in range(a.dropin_ticks):
+        b.run_tick(DT)
+    el = time.perf_counter() - t0
+    d = b.bion_data()
+    from bioneuroncore_b200.abi import view, SEGMENT_DTYPE
+    seg = view(d.segments, SEGMENT_DTYPE, d.num_segments)
+    coherent = bool(np.array_equal(seg["V_m"].astype(np.float32), np.asarray(b.segment_field("V"), np.float32)))
+    dev_ms = b.time_ticks(a.dropin_ticks, DT) / a.dropin_ticks
+    nseg = net.data.num_segments
+    b.close()
+    return {"call": "gpu_backend_run_tick (host Segment/Synapse records written back every tick)",
+            "workload": "large plain network at %d neurons (%d segments, %d synapses x 8 receptors)"
+                        % (a.dropin_neurons, nseg, net.data.num_synapses),
+            "value": nseg * a.dropin_ticks / el, "unit": UNIT, "ms_per_tick": 1000.0 * el / a.dropin_ticks,
+            "device_ms_per_tick": dev_ms, "ticks": a.dropin_ticks, "host_view_coherent": coherent,
+            "timing": "host wall clock around the calls"}
+
+
 def run_sweep(a, device):
     """Parameter sweep: a.sweep_tasks parameterised runs of one 64-neuron network (2,048
     segments, 400 synapses) as one ensemble (bnc_sweep_run), each task with its own K2P
@@ -539,6 +574,10 @@ def main():
                "h2d_bytes_per_step": 4 * n_stim, "d2h_bytes_per_step": 4 * info.n_segments,
                "steps": a.e2e_steps, "timing": "host wall clock around the steps, max over ranks"}
 
+    dropin = None
+    if not a.no_dropin and rank == 0 and world == 1:
+        dropin = run_dropin(a, local_rank if world > 1 else 0)
+
     # roofline of the dominant kernel
     peak, peak_kind = measured_peak()
     kernels = {"k_modifiers": (ms_mod / n_prof, info.modifier_kernel_bytes),
@@ -594,7 +633,7 @@ def main():
                        "synapses_per_gpu": info.n_synapses, "parallelism": "replicas" if world > 1 else "single",
                        "l2": "inputs larger than L2 (device state ~8 GB per GPU)",
                        "tiles": info.n_tiles, "phases": info.n_phases, "setup_s": round(setup_s, 1)},
-            "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,
+            "e2e": e2e, "e2e_dropin": dropin, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,
             "gpu_launches": (info.modifier_launches + 2) * a.steps, "ensemble": ensemble, "trees": trees,
             "adjoint": adjoint, "sweep": sweep,
         }

@@ -13,6 +13,7 @@
 #include <vector>
 #include <cuda_runtime.h>
 #include "net.h"
+#include "par.h"
 #include "netgen.h"
 #include "hostnet.h"
 #include "hostnet.h"
@@ -93,63 +94,130 @@ static bool d2h(std::vector<T>& v, const T* p, size_t n) {
     return cudaMemcpy(v.data(), p, n * sizeof(T), cudaMemcpyDeviceToHost) == cudaSuccess;
 }
 
+// Pinned staging for exports, kept for the process and grown on demand (one exporter at
+// a time); pageable memory when a pinned allocation fails.
+namespace {
+std::mutex g_stage_mu;
+void* g_stage = nullptr;
+size_t g_stage_cap = 0;
+std::vector<unsigned char> g_stage_pageable;
+
+unsigned char* stage_reserve(size_t bytes) {
+    if (bytes <= g_stage_cap && g_stage) return static_cast<unsigned char*>(g_stage);
+    if (g_stage) cudaFreeHost(g_stage);
+    g_stage = nullptr;
+    g_stage_cap = 0;
+    if (cudaMallocHost(&g_stage, bytes) == cudaSuccess) {
+        g_stage_cap = bytes;
+        return static_cast<unsigned char*>(g_stage);
+    }
+    cudaGetLastError();
+    g_stage = nullptr;
+    g_stage_pageable.resize(bytes);
+    return g_stage_pageable.data();
+}
+}  // namespace
+
+// Device state -> the host AoS view.  Fields the network's flags show cannot change on
+// the device (intracellular NT, temperature, transcription without gradients) and the
+// modifier state words no item type updates are not copied; the scatter into the AoS
+// records runs on all host cores.
 int export_network(const NetDev& d, const NetHost& h, uint64_t ticks_run, BncBionData* aos) {
     if (!aos || !aos->segments) return BNC_OK;
-    const uint32_t n = d.n_seg;
-    std::vector<float> V, in, out, intra_nt, nt, atp, temp, txn, it_st;
-    bool ok = d2h(V, d.V, n) && d2h(in, d.ion_in, (size_t)7 * n) && d2h(out, d.ion_out, (size_t)7 * n) &&
-              d2h(intra_nt, d.intra_nt, (size_t)15 * n) && d2h(nt, d.nt, (size_t)15 * n) && d2h(atp, d.atp, n) &&
-              d2h(temp, d.temp, n) && d2h(txn, d.txn, n) && d2h(it_st, d.it_st, (size_t)7 * d.n_items);
-    if (!ok) { set_error("export: device read failed"); return BNC_ERR_CUDA; }
-    for (uint32_t dd = 0; dd < n; dd++) {
-        BncSegment& s = aos->segments[h.perm[dd]];
-        s.V_m = V[dd];
-        for (int q = 0; q < 7; q++) {
-            s.intra_ions[q] = in[(size_t)q * n + dd];
-            s.extra_ions[q] = out[(size_t)q * n + dd];
-        }
-        for (int q = 0; q < 15; q++) {
-            s.intra_nt[q] = intra_nt[(size_t)q * n + dd];
-            s.neurotransmitter[q] = nt[(size_t)q * n + dd];
-        }
-        s.ATP_level = atp[dd];
-        s.temperature = temp[dd];
-        s.transcription_signal = txn[dd];
-        if (ticks_run > 0) s.I_buffer = 0.0;   // step 4 clears it (simulation_host.cpp:624)
-    }
-    const uint32_t NI = d.n_items;
-    for (uint32_t q = 0; q < NI; q++) {
-        BncModifier& m = aos->segments[h.item_seg[q]].modifiers[h.item_slot[q]];
-        for (int k = 0; k < 7; k++) m.state[k] = it_st[(size_t)k * NI + q];
-        if (ticks_run > 0) {
-            const BncSegment& s = aos->segments[h.item_seg[q]];
-            m.state[7] = (s.segment_type == 1 || s.segment_type == 3 || s.segment_type == 4)
-                ? 4.0f * 3.14159265f * s.radius * s.radius : 2.0f * 3.14159265f * s.radius * s.length;
-        }
-    }
-    const uint32_t K = d.n_syn;
+    const uint32_t n = d.n_seg, NI = d.n_items, K = d.n_syn, NR = d.n_rec;
+    const bool x_int = (d.flags & NF_INTRA_NT) != 0, x_temp = (d.flags & NF_TEMP) != 0,
+               x_txn = (d.flags & NF_TXN) != 0;
+    const uint8_t rows = h.item_dyn_rows;
+    // staging layout (floats, then the refractory bytes)
+    size_t off = 0;
+    auto take = [&](size_t floats) { size_t o = off; off += floats; return o; };
+    const size_t oV = take(n), oIn = take((size_t)7 * n), oOut = take((size_t)7 * n), oNt = take((size_t)15 * n),
+                 oAtp = take(n), oInt = x_int ? take((size_t)15 * n) : 0, oTemp = x_temp ? take(n) : 0,
+                 oTxn = x_txn ? take(n) : 0;
+    size_t oSt[7];
+    for (int k = 0; k < 7; k++) oSt[k] = ((rows >> k) & 1u) ? take(NI) : 0;
+    size_t oSy[8] = {0}, oRc = 0;
     if (K) {
-        std::vector<float> bouton, spine, camkii, calcn, facil, weight, cleft, rrp, rst;
-        std::vector<uint8_t> refr;
-        ok = d2h(bouton, d.sy_bouton, K) && d2h(spine, d.sy_spine, K) && d2h(camkii, d.sy_camkii, K) &&
-             d2h(calcn, d.sy_calcn, K) && d2h(facil, d.sy_facil, K) && d2h(weight, d.sy_weight, K) &&
-             d2h(cleft, d.sy_cleft, K) && d2h(rrp, d.sy_rrp, K) && d2h(refr, d.sy_refr, K) &&
-             d2h(rst, d.rc_st, (size_t)3 * d.n_rec);
-        if (!ok) { set_error("export: device read failed"); return BNC_ERR_CUDA; }
-        for (uint32_t q = 0; q < K; q++) {
-            BncSynapse& y = aos->synapses[h.syn_orig[q]];
-            y.bouton_Ca = bouton[q]; y.spine_Ca = spine[q]; y.spine_camkii = camkii[q];
-            y.spine_calcineurin = calcn[q]; y.facilitation = facil[q]; y.weight = weight[q];
-            y.cleft_neurotransmitter[h.syn_nt[q]] = cleft[q];
-            y.RRP = rrp[q]; y.refractory = refr[q];
-            if (ticks_run > 0) y.depression = facil[q] + 0.01f;
+        for (int f = 0; f < 8; f++) oSy[f] = take(K);
+        oRc = take((size_t)3 * NR);
+    }
+    const size_t bytes = off * sizeof(float) + K;
+    std::lock_guard<std::mutex> lock(g_stage_mu);
+    unsigned char* base = stage_reserve(bytes);
+    float* F = reinterpret_cast<float*>(base);
+    uint8_t* refr = base + off * sizeof(float);
+    bool ok = true;
+    auto get = [&](size_t o, const void* src, size_t nbytes) {
+        if (ok && nbytes) ok = cudaMemcpy(F + o, src, nbytes, cudaMemcpyDeviceToHost) == cudaSuccess;
+    };
+    get(oV, d.V, (size_t)n * 4);
+    get(oIn, d.ion_in, (size_t)7 * n * 4);
+    get(oOut, d.ion_out, (size_t)7 * n * 4);
+    get(oNt, d.nt, (size_t)15 * n * 4);
+    get(oAtp, d.atp, (size_t)n * 4);
+    if (x_int) get(oInt, d.intra_nt, (size_t)15 * n * 4);
+    if (x_temp) get(oTemp, d.temp, (size_t)n * 4);
+    if (x_txn) get(oTxn, d.txn, (size_t)n * 4);
+    for (int k = 0; k < 7; k++)
+        if ((rows >> k) & 1u) get(oSt[k], d.it_st + (size_t)k * NI, (size_t)NI * 4);
+    if (K) {
+        const float* src[8] = {d.sy_bouton, d.sy_spine, d.sy_camkii, d.sy_calcn, d.sy_facil, d.sy_weight,
+                               d.sy_cleft, d.sy_rrp};
+        for (int f = 0; f < 8; f++) get(oSy[f], src[f], (size_t)K * 4);
+        get(oRc, d.rc_st, (size_t)3 * NR * 4);
+        if (ok) ok = cudaMemcpy(refr, d.sy_refr, K, cudaMemcpyDeviceToHost) == cudaSuccess;
+    }
+    if (!ok) { set_error("export: device read failed"); return BNC_ERR_CUDA; }
+    parallel_for(n, [&](size_t d0, size_t d1) {
+        for (size_t dd = d0; dd < d1; dd++) {
+            BncSegment& s = aos->segments[h.perm[dd]];
+            s.V_m = F[oV + dd];
+            for (int q = 0; q < 7; q++) {
+                s.intra_ions[q] = F[oIn + (size_t)q * n + dd];
+                s.extra_ions[q] = F[oOut + (size_t)q * n + dd];
+            }
+            for (int q = 0; q < 15; q++) s.neurotransmitter[q] = F[oNt + (size_t)q * n + dd];
+            if (x_int) for (int q = 0; q < 15; q++) s.intra_nt[q] = F[oInt + (size_t)q * n + dd];
+            s.ATP_level = F[oAtp + dd];
+            if (x_temp) s.temperature = F[oTemp + dd];
+            if (x_txn) s.transcription_signal = F[oTxn + dd];
+            if (ticks_run > 0) s.I_buffer = 0.0;   // step 4 clears it (simulation_host.cpp:624)
         }
-        for (uint32_t r = 0; r < d.n_rec; r++) {
-            BncSynapse& y = aos->synapses[h.syn_orig[h.rec_syn[r]]];
-            BncModifier& m = y.post_receptors[h.rec_slot[r]];
-            m.state[0] = rst[r]; m.state[1] = rst[(size_t)d.n_rec + r]; m.state[2] = rst[(size_t)2 * d.n_rec + r];
-            if (ticks_run > 0) m.state[7] = y.post_area;
+    });
+    parallel_for(NI, [&](size_t q0, size_t q1) {
+        for (size_t q = q0; q < q1; q++) {
+            BncSegment& s = aos->segments[h.item_seg[q]];
+            BncModifier& m = s.modifiers[h.item_slot[q]];
+            const uint8_t t = m.type;
+            const bool user = t < 128 && ((d.user_mask[t >> 5] >> (t & 31)) & 1u);
+            const uint8_t wm = user ? (uint8_t)0x7F : host_dyn_mask(t);
+            for (int k = 0; k < 7; k++)
+                if ((wm >> k) & 1u) m.state[k] = F[oSt[k] + q];
+            if (ticks_run > 0)
+                m.state[7] = (s.segment_type == 1 || s.segment_type == 3 || s.segment_type == 4)
+                    ? 4.0f * 3.14159265f * s.radius * s.radius : 2.0f * 3.14159265f * s.radius * s.length;
         }
+    });
+    if (K) {
+        parallel_for(K, [&](size_t q0, size_t q1) {
+            for (size_t q = q0; q < q1; q++) {
+                BncSynapse& y = aos->synapses[h.syn_orig[q]];
+                y.bouton_Ca = F[oSy[0] + q]; y.spine_Ca = F[oSy[1] + q]; y.spine_camkii = F[oSy[2] + q];
+                y.spine_calcineurin = F[oSy[3] + q]; y.facilitation = F[oSy[4] + q]; y.weight = F[oSy[5] + q];
+                y.cleft_neurotransmitter[h.syn_nt[q]] = F[oSy[6] + q];
+                y.RRP = F[oSy[7] + q]; y.refractory = refr[q];
+                if (ticks_run > 0) y.depression = F[oSy[4] + q] + 0.01f;
+            }
+        });
+        parallel_for(NR, [&](size_t r0, size_t r1) {
+            for (size_t r = r0; r < r1; r++) {
+                BncSynapse& y = aos->synapses[h.syn_orig[h.rec_syn[r]]];
+                BncModifier& m = y.post_receptors[h.rec_slot[r]];
+                m.state[0] = F[oRc + r]; m.state[1] = F[oRc + (size_t)NR + r];
+                m.state[2] = F[oRc + (size_t)2 * NR + r];
+                if (ticks_run > 0) m.state[7] = y.post_area;
+            }
+        });
     }
     return BNC_OK;
 }

@@ -28,6 +28,7 @@
 #include <thread>
 #include "net.h"
 #include "hostnet.h"
+#include "par.h"
 
 namespace bnc {
 
@@ -47,36 +48,6 @@ void DeviceAllocs::release() {
 }
 
 namespace {
-
-// Runs f(begin, end) over [0, n) in contiguous chunks on up to hardware_concurrency
-// threads (one chunk per thread); small ranges run inline.  Used for loops whose
-// iterations write disjoint outputs, so the result does not depend on the split.
-template <typename F>
-void parallel_for(size_t n, F&& f, size_t min_chunk = 1 << 16) {
-    unsigned T = std::thread::hardware_concurrency();
-    if (T == 0) T = 1;
-    T = std::min<unsigned>(T, 32u);
-    const size_t chunks = std::min<size_t>(T, (n + min_chunk - 1) / min_chunk);
-    if (chunks <= 1) { f((size_t)0, n); return; }
-    const size_t per = (n + chunks - 1) / chunks;
-    std::vector<std::thread> th;
-    th.reserve(chunks);
-    for (size_t c = 0; c < chunks; c++) {
-        const size_t b = c * per, e = std::min(n, b + per);
-        if (b < e) th.emplace_back([&f, b, e]() { f(b, e); });
-    }
-    for (auto& t : th) t.join();
-}
-
-// The lowest index at which a parallel loop found an error (UINT64_MAX: none).
-struct FirstError {
-    std::atomic<uint64_t> at{UINT64_MAX};
-    void note(uint64_t i) {
-        uint64_t cur = at.load();
-        while (i < cur && !at.compare_exchange_weak(cur, i)) {}
-    }
-    bool any() const { return at.load() != UINT64_MAX; }
-};
 
 // ---- host restatements of the static per-segment helpers ----
 // run_tick_common.h:209-214
@@ -860,6 +831,14 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
             set_error("segment %u slot %u: active_vars %u out of range", orig, slot, hn.mod(orig, slot).active_vars);
             return BNC_ERR_FORMAT;
         }
+    }
+    {   // the state words some item updates on the device (registered types: all 7)
+        uint8_t seen[256] = {0};
+        for (uint8_t t : act_type) seen[t] = 1;
+        uint8_t rows = 0;
+        for (int t = 0; t < 256; t++)
+            if (seen[t]) rows |= (t < 128 && user_type[t]) ? (uint8_t)0x7F : host_dyn_mask((uint8_t)t);
+        host->item_dyn_rows = rows;
     }
     // registered device modifiers: their items form one contiguous run per phase and type
     host->user_ranges.clear();

@@ -11,9 +11,9 @@
 //                SMs at any moment -- run few channel models at a time, which keeps the
 //                many models' code within the instruction caches.  Each dispatch case
 //                loads and stores only the record fields its model uses.
-//  k_phase_group the same phases two or three to a launch (slot-order schedules): one
-//                thread per segment runs its items of those phases on the record held
-//                in registers, so the record crosses HBM once per group.
+//  k_phase_group the same phases four to a launch by default (slot-order schedules):
+//                one thread per segment runs its items of those phases on the record
+//                held in registers, so the record crosses HBM once per group.
 //  k_diffusion   (diffuse.cu) stimuli, step 2.5 electrodiffusion, the presynaptic record.
 //  k_synapse     (synapse.cu) steps 3 and 4.
 #define BNC_MATH_OUTLINE 1   // 26 channel models in one kernel: keep exp/log out of line
@@ -272,13 +272,11 @@ k_phase_group(NetDev d, float dt, PhaseGroup grp) {
 
 static bool g_tables_ready[64] = {false};   // per device: constant memory is per context
 
-static cudaError_t init_tables(cudaStream_t stream) {
-    int dev = 0;
-    cudaError_t ge = cudaGetDevice(&dev);
-    if (ge != cudaSuccess) return ge;
-    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
-    if (g_tables_ready[dev]) return cudaSuccess;
-    uint8_t dyn[256] = {0}, par[256] = {0};
+// The state words each built-in type updates every tick (dyn) and reads as parameters
+// when non-zero (par), by state index bit.
+static void fill_mask_tables(uint8_t* dyn, uint8_t* par) {
+    std::fill(dyn, dyn + 256, (uint8_t)0);
+    std::fill(par, par + 256, (uint8_t)0);
     dyn[1] = 0x03; par[1] = 0x1C;
     dyn[8] = 0x03; dyn[9] = 0x05; dyn[11] = 0x03; dyn[12] = 0x03;
     dyn[85] = 0x0B; par[85] = 0x34;
@@ -297,6 +295,23 @@ static cudaError_t init_tables(cudaStream_t stream) {
     dyn[142] = 0x03; par[142] = 0x20;
     dyn[150] = 0x07; par[150] = 0x20;
     dyn[200] = 0x03; par[200] = 0x7C;
+}
+
+uint8_t host_dyn_mask(uint8_t type) {
+    static uint8_t dyn[256], par[256];
+    static bool ready = false;
+    if (!ready) { fill_mask_tables(dyn, par); ready = true; }
+    return dyn[type];
+}
+
+static cudaError_t init_tables(cudaStream_t stream) {
+    int dev = 0;
+    cudaError_t ge = cudaGetDevice(&dev);
+    if (ge != cudaSuccess) return ge;
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    if (g_tables_ready[dev]) return cudaSuccess;
+    uint8_t dyn[256], par[256];
+    fill_mask_tables(dyn, par);
     cudaError_t e = cudaMemcpyToSymbol(c_dyn_mask, dyn, sizeof(dyn));
     if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_par_mask, par, sizeof(par));
     if (e == cudaSuccess) g_tables_ready[dev] = true;

@@ -216,6 +216,7 @@ struct NetHost {
     std::vector<uint32_t> phase_off;         // item range of each (chunk, phase) bucket (host copy)
     uint32_t chunk_segs = 0, n_chunks = 1;   // modifier-pass chunks of consecutive segments
     uint32_t fuse = 1;                       // modifier phases per launch (item order follows)
+    uint8_t item_dyn_rows = 0;               // state words (bits) any item updates: the rows exported
     struct UserRange { uint32_t bucket, type, begin, end; const void* kernel; };
     std::vector<UserRange> user_ranges;      // registered device modifiers' items, per bucket
     size_t smem_bytes = 0;
@@ -251,6 +252,8 @@ int upload_stimuli(const Stimuli& stim, NetHost& host, NetDev* dev, DeviceAllocs
 
 // Writes device state back into the AoS arrays.
 int export_network(const NetDev& dev, const NetHost& host, uint64_t ticks_run, BncBionData* aos);
+// State words (bits) a built-in modifier type updates every tick; 0 for other types.
+uint8_t host_dyn_mask(uint8_t type);
 
 // Kernel launchers (tile.cu, synapse.cu).  prepare_tick does the per-device and
 // per-network set-up that must not happen inside a stream capture (constant tables,
