@@ -382,7 +382,8 @@ def run_trees(a, device):
 
 def run_adjoint(a, device):
     """Adjoint fitting workload: a.adj_neurons neurons x 64 segments with 2,000 synapses
-    per 256 neurons (the fitting family: Nav, Kv_DR, K2P leak, AMPA/GABA-A), a.adj_sets
+    per 256 neurons (the fitting family: Nav, Kv_DR, K2P leak, AMPA/GABA-A; also timed
+    with Cav1.3 and the Na/K pump added), a.adj_sets
     parameter sets in one launch, checkpoints every 256 ticks.  Targets come from a
     hidden parameter set; the forward and backward passes are device-timed (CUDA events
     inside the library) and their ratio is the adjoint's cost in forward passes."""
@@ -411,6 +412,27 @@ def run_adjoint(a, device):
     adj.close()
     b.close()
     spec_ticks = 20000
+    # the same workload with the whole small set (Cav1.3 and the Na/K pump on every
+    # segment, the pump's ATP diffusing): its cost ratio, beside the fitting family's
+    from bioneuroncore_b200 import NETGEN_FULL_SMALL_SET
+    netf = Network(NetgenParams(family=NET_ADJOINT, n_neurons=a.adj_neurons, seed=a.seed, flags=NETGEN_FULL_SMALL_SET))
+    bf = Backend(device)
+    bf.load_network(netf)
+    adjf = Adjoint(bf, a.adj_sets, a.adj_ticks, DT, checkpoint_every=256)
+    adjf.record()
+    basef = adjf.get_params(0)
+    adjf.set_params(0, *[x * f for x, f in zip(basef, (1.15, 0.85, 1.25, 0.8))])
+    _, trf = adjf.forward(trace=True)
+    adjf.set_target(trf[0])
+    for p in range(a.adj_sets):
+        adjf.set_params(p, *[(x * np.exp(0.1 * rng.standard_normal(x.shape))).astype(np.float32) for x in basef])
+    adjf.forward()
+    adjf.backward()
+    ffwd, fbwd = adjf.timings()
+    adjf.close()
+    bf.close()
+    full = {"forward_ms": ffwd, "backward_ms": fbwd, "backward_over_forward": fbwd / ffwd,
+            "note": "the same workload with Cav1.3 and the Na/K pump on every segment (BNC_NETGEN_FULL_SMALL_SET)"}
     cpu = None
     if not a.no_cpu_baseline:
         try:   # the reference's CPU tick on the same network: the forward pass of one set
@@ -439,6 +461,7 @@ def run_adjoint(a, device):
         "launch": "one CTA per (neuron, parameter set); forward %d threads, %d B shared; backward %d B shared"
                   % (i.threads, i.smem_forward, i.smem_backward),
         "setup_s": round(setup_s, 1),
+        "full_small_set": full,
         "cpu_reference": cpu,
     }
 

@@ -2,7 +2,10 @@
 // maximal conductances (gNa, gK, gleak: the densities of the Nav1.x, Kv delayed
 // rectifier and K2P leak modifiers) and per-synapse weights (the receptor density
 // scale), by a hand-written discrete adjoint of the reference tick
-// (simulation_host.cpp:174-657).
+// (simulation_host.cpp:174-657).  The network may hold the whole small set: Cav1.3 and
+// the Na/K pump run with their own densities and are differentiated too, with the ATP
+// the pump consumes (a state word, diffusing by Fick in step 2.5).  Networks without
+// them run kernel instantiations that leave that code out (kFull = false).
 //
 // Pathwise replay.  The transmitter a release puts into a cleft is taken from a log
 // recorded once by the plain tick (bnc_adjoint_record), so the sampled release
@@ -44,11 +47,18 @@ namespace bnc {
 namespace {
 
 constexpr int kMaxSeg = 128;     // segments (and connections) per neuron: threads per CTA
-constexpr int kItems = 3;        // differentiable items per segment (Nav, Kv_DR, K2P)
-constexpr int kGates = 4;        // dynamic gate words per segment
+constexpr int kItems = 5;        // differentiable items per segment (Nav, Kv_DR, K2P, Cav1.3, Na/K pump)
+// item arrays' stride per segment on the device: kItems with Cav1.3 or the pump, else 3
+template <bool kFull> struct ItemStride { static constexpr uint32_t v = kFull ? kItems : 3; };
+constexpr int kGates = 5;        // dynamic gate words per segment (Nav m, h; Kv_DR n; Cav1.3 m, h)
 constexpr int kMaxInc = 4;       // connections per segment (the generated families have at most 3)
 constexpr int kRecPerSyn = 2;    // receptors per synapse
-constexpr int kSegWords = 19;    // V, 7 intra, 7 extra, 4 gates
+// A segment's state words: V, 7 intra, 7 extra, then the gate words the network's
+// segments need (at most kGates) and ATP when some segment carries the pump
+// (AdjDev::W words; ATP at row AdjDev::atp_w).  Shared memory holds W rows twice in
+// the reverse pass, so W follows the network.  The fitting family's kernels (no
+// Cav1.3, no pump) use the fixed width kW3: three gate words.
+constexpr uint32_t kW3 = 18;
 constexpr int kSynWords = 5;     // receptor 0 (r, d), receptor 1 (r, d), cleft
 
 __constant__ float c_z2d[7];     // z^2 * D per ion, as the reference's float product
@@ -63,8 +73,11 @@ struct AdjDev {
     uint32_t T, K, n_ckpt, stride, n_samples;
     uint32_t Smax, Emax, Ymax;
     uint32_t L;                    // state floats of one parameter set
+    uint32_t W, atp_w;             // state words per segment, the ATP word
     float dt;
     int has_conn;
+    int has_atp;                   // some segment carries the Na/K pump: ATP changes and diffuses
+    int full;                      // some item is Cav1.3 or the pump: the kernels with their code
     unsigned long long tick0;
     // per neuron
     const uint32_t *nr_seg, *nr_edge, *nr_slot, *nr_st;   // [nn + 1] offsets
@@ -76,6 +89,7 @@ struct AdjDev {
     const uint8_t* it_type;        // [seg][kItems]
     const uint8_t* it_gate;        // first gate word of the item
     const float* it_st;            // [seg][kItems][7] parameter words
+    const float* it_den;           // [seg][kItems] densities of the items without a fitted conductance
     const uint8_t* inc_n;
     const uint16_t* inc_e;         // [seg][kMaxInc] local connection ids, ascending
     const uint32_t* stim_off;      // [seg + 1]
@@ -123,17 +137,17 @@ struct Lay {
     float *s2, *lam, *lphi, *lI, *mu, *lvB, *linp, *lgdg, *eca, *ecb, *edv, *ldiag, *phs, *jsm;
 };
 
-__host__ __device__ inline size_t lay_bytes(uint32_t S, uint32_t E, uint32_t Y, bool bwd) {
+__host__ __device__ inline size_t lay_bytes(uint32_t S, uint32_t E, uint32_t Y, bool bwd, uint32_t W) {
     size_t dbl = (size_t)6 * S + 15 * (size_t)E;
-    size_t flt = (size_t)kSegWords * S + kSynWords * Y + 2 * (size_t)E + 2 * (size_t)S;
+    size_t flt = (size_t)W * S + kSynWords * Y + 2 * (size_t)E + 2 * (size_t)S;
     if (bwd) {
         dbl += S;   // pmask
-        flt += 15 * (size_t)S + kSegWords * (size_t)S + 7 * (size_t)S + (size_t)E + 102 * (size_t)S + 4;
+        flt += 15 * (size_t)S + W * (size_t)S + 7 * (size_t)S + (size_t)E + 102 * (size_t)S + 4;
     }
     return dbl * 8 + flt * 4;
 }
 
-__device__ inline Lay make_lay(unsigned char* base, uint32_t S, uint32_t E, uint32_t Y, bool bwd) {
+__device__ inline Lay make_lay(unsigned char* base, uint32_t S, uint32_t E, uint32_t Y, bool bwd, uint32_t W) {
     Lay l;
     double* d = reinterpret_cast<double*>(base);
     l.ibuf = d; d += S; l.phiA = d; d += S; l.phiB = d; d += S; l.sig = d; d += S; l.diag = d; d += S;
@@ -141,12 +155,12 @@ __device__ inline Lay make_lay(unsigned char* base, uint32_t S, uint32_t E, uint
     l.pmask = nullptr;
     if (bwd) { l.pmask = reinterpret_cast<unsigned long long*>(d); d += S; }
     float* f = reinterpret_cast<float*>(d);
-    l.st = f; f += kSegWords * S + kSynWords * Y;
+    l.st = f; f += W * S + kSynWords * Y;
     l.gax = f; f += E; l.term = f; f += E;
     l.vnA = f; f += S; l.vnB = f; f += S;
     if (bwd) {
         l.s2 = f; f += 15 * S;
-        l.lam = f; f += kSegWords * S;
+        l.lam = f; f += W * S;
         l.lphi = f; f += S; l.lI = f; f += S; l.mu = f; f += S; l.lvB = f; f += S;
         l.linp = f; f += S; l.lgdg = f; f += S; l.ldiag = f; f += S; l.edv = f; f += E;
         // the reverse tick's per-connection adjoints reuse the forward's flux buffers
@@ -232,17 +246,17 @@ __device__ inline bool inc_intra(uint32_t w) { return (w >> 17) & 1u; }
 
 // The block of a neuron: V[S], in[7][S], out[7][S], gate[4][S], then per synapse slot
 // the receptor states and the cleft.  Shared memory keeps the stride Smax.
-__device__ inline void block_load(float* dst, const float* src, const Ctx& c, uint32_t Smax) {
-    const uint32_t seg_words = kSegWords * c.S;
+__device__ inline void block_load(float* dst, const float* src, const Ctx& c, uint32_t Smax, uint32_t W) {
+    const uint32_t seg_words = W * c.S;
     for (uint32_t q = threadIdx.x; q < c.L_n; q += blockDim.x) {
-        const uint32_t o = (q < seg_words) ? (q / c.S) * Smax + (q % c.S) : kSegWords * Smax + (q - seg_words);
+        const uint32_t o = (q < seg_words) ? (q / c.S) * Smax + (q % c.S) : W * Smax + (q - seg_words);
         dst[o] = src[q];
     }
 }
-__device__ inline void block_store(float* dst, const float* src, const Ctx& c, uint32_t Smax) {
-    const uint32_t seg_words = kSegWords * c.S;
+__device__ inline void block_store(float* dst, const float* src, const Ctx& c, uint32_t Smax, uint32_t W) {
+    const uint32_t seg_words = W * c.S;
     for (uint32_t q = threadIdx.x; q < c.L_n; q += blockDim.x) {
-        const uint32_t o = (q < seg_words) ? (q / c.S) * Smax + (q % c.S) : kSegWords * Smax + (q - seg_words);
+        const uint32_t o = (q < seg_words) ? (q / c.S) * Smax + (q % c.S) : W * Smax + (q - seg_words);
         dst[q] = src[o];
     }
 }
@@ -257,7 +271,25 @@ __device__ inline float bern_f(float x) {
 __device__ inline float par_of(const AdjDev& d, uint32_t p, int cls, uint32_t g) {
     return d.par[((size_t)p * 3 + cls) * d.n_seg + g];
 }
-__device__ inline int cls_of(uint8_t type) { return type == 123 ? 1 : (type == 107 ? 2 : 0); }
+// the fitted conductance class of an item type (-1: Cav1.3 and the pump run with their
+// network densities)
+__device__ inline int cls_of(uint8_t type) {
+    return type == 123 ? 1 : (type == 107 ? 2 : ((type == 141 || type == 142) ? 0 : -1));
+}
+__device__ inline int gates_of(uint8_t type) {
+    return type == 123 ? 1 : ((type == 107 || type == 7) ? 0 : 2);
+}
+// the same for the fitting family's kernels (Nav, Kv_DR, K2P only)
+template <bool kFull> __device__ inline int cls_k(uint8_t type) {
+    return kFull ? cls_of(type) : (type == 123 ? 1 : (type == 107 ? 2 : 0));
+}
+template <bool kFull> __device__ inline int gates_k(uint8_t type) {
+    return kFull ? gates_of(type) : (type == 123 ? 1 : (type == 107 ? 0 : 2));
+}
+__device__ inline float den_of(const AdjDev& d, uint32_t p, uint8_t type, uint32_t g, uint32_t j) {
+    const int cls = cls_of(type);
+    return cls >= 0 ? par_of(d, p, cls, g) : d.it_den[g * kItems + j];
+}
 
 // the logged cleft entries of `slot` at `tick` (sorted by tick, then the order the
 // tick added them)
@@ -277,11 +309,16 @@ __device__ inline float cleft_events(const AdjDev& d, uint32_t slot, unsigned lo
 __device__ __noinline__ double run_slot(uint8_t type, DMod& m, DSeg& s, float dt) {
     if (type == 123) return dp_kvdr_current<false>(m, s, dt);
     if (type == 107) return dp_k2p_current<false>(m, s, dt);
+    if (type == 1) return dp_cav13_current<false>(m, s, dt);
+    if (type == 7) return dp_nak_pump_current(m, s, dt);
     return dp_nav_current<false>(m, s, dt, type == 142 ? 1 : 0);
 }
 
 // Step 1 for this thread's segment: the differentiable items in slot order, then the
 // current stimuli (simulation_host.cpp:234-303).
+// kFull: the Cav1.3 / Na/K pump / ATP code is compiled in (networks with those items);
+// without it the kernels hold only the fitting family's code paths.
+template <bool kFull>
 __device__ inline double step1_seg(const AdjDev& d, const Ctx& c, const Lay& L, unsigned long long tick, float dt,
                                    float* pre) {
     const uint32_t Sm = d.Smax;
@@ -292,31 +329,39 @@ __device__ inline double step1_seg(const AdjDev& d, const Ctx& c, const Lay& L, 
     s.V = st[i];
 #pragma unroll
     for (int q = 0; q < 7; q++) { s.in[q] = st[(1 + q) * Sm + i]; s.out[q] = st[(8 + q) * Sm + i]; }
-    s.atp = 0.0f;
+    s.atp = (kFull && d.has_atp) ? st[d.atp_w * Sm + i] : 0.0f;
     s.area = c.area;
     s.vol = c.vol;
     ghk_cache_fill(s.gc, s.V);
     double I_total = 0.0;
     const uint32_t ni = d.n_it[g];
     for (uint32_t j = 0; j < ni; j++) {
-        const uint8_t type = d.it_type[g * kItems + j];
-        const uint32_t go = d.it_gate[g * kItems + j];
+        constexpr uint32_t IS = ItemStride<kFull>::v;
+        const uint8_t type = d.it_type[g * IS + j];
+        const uint32_t go = d.it_gate[g * IS + j];
         DMod m;
-        m.den = par_of(d, c.p, cls_of(type), g);
+        m.den = kFull ? den_of(d, c.p, type, g, j) : par_of(d, c.p, cls_k<kFull>(type), g);
 #pragma unroll
-        for (int k = 0; k < 7; k++) m.st[k] = d.it_st[((size_t)g * kItems + j) * 7 + k];
+        for (int k = 0; k < 7; k++) m.st[k] = d.it_st[((size_t)g * IS + j) * 7 + k];
         m.area = s.area;
         m.av = 0;
-        const int ng = (type == 123) ? 1 : (type == 107 ? 0 : 2);
+        const int ng = gates_k<kFull>(type);
         if (ng > 0) m.st[0] = st[(15 + go) * Sm + i];
         if (ng > 1) m.st[1] = st[(16 + go) * Sm + i];
         if (pre) {   // the item's inputs, for the reverse tick
-            const int ion = (ng == 2) ? 0 : 1;
             pre[(j * 5 + 0) * Sm + i] = s.V;
-            pre[(j * 5 + 1) * Sm + i] = m.st[0];
-            pre[(j * 5 + 2) * Sm + i] = m.st[1];
-            pre[(j * 5 + 3) * Sm + i] = s.in[ion];
-            pre[(j * 5 + 4) * Sm + i] = s.out[ion];
+            if (kFull && type == 7) {   // the pump: Na_in, K_out, ATP
+                pre[(j * 5 + 1) * Sm + i] = s.in[0];
+                pre[(j * 5 + 2) * Sm + i] = s.out[1];
+                pre[(j * 5 + 3) * Sm + i] = s.atp;
+                pre[(j * 5 + 4) * Sm + i] = 0.0f;
+            } else {   // the item's ion by selects (an index would move s.in / s.out to local memory)
+                const bool ca = kFull && type == 1, na = ng == 2 && !ca;
+                pre[(j * 5 + 1) * Sm + i] = m.st[0];
+                pre[(j * 5 + 2) * Sm + i] = m.st[1];
+                pre[(j * 5 + 3) * Sm + i] = ca ? s.in[2] : (na ? s.in[0] : s.in[1]);
+                pre[(j * 5 + 4) * Sm + i] = ca ? s.out[2] : (na ? s.out[0] : s.out[1]);
+            }
         }
         I_total += run_slot(type, m, s, dt);
         if (ng > 0) st[(15 + go) * Sm + i] = m.st[0];
@@ -327,6 +372,7 @@ __device__ inline double step1_seg(const AdjDev& d, const Ctx& c, const Lay& L, 
     st[i] = s.V;
 #pragma unroll
     for (int q = 0; q < 7; q++) { st[(1 + q) * Sm + i] = s.in[q]; st[(8 + q) * Sm + i] = s.out[q]; }
+    if (kFull && d.has_atp) st[d.atp_w * Sm + i] = s.atp;
     return I_total;
 }
 
@@ -338,11 +384,14 @@ struct Scr {
     float* jac;       // [5][51][Sm]
     float* estart;    // [6][7][Sm]  out before each extra sub-step and before the bath
     float* syn;       // [Ymax][9]   in[7] before the synapse, receptor open probabilities
+    float* atpf;      // [Sm]        ATP before the Fick pass
 };
-__host__ __device__ inline size_t scr_floats(uint32_t S, uint32_t Y) {
-    return ((size_t)40 * S + (size_t)255 * S + (size_t)42 * S + (size_t)9 * Y + (size_t)kItems * 5 * S + 4 + 3) &
-           ~(size_t)3;
+// items: the item stride of the kernels; atp: whether the ATP row is recorded
+__host__ __device__ inline size_t scr_floats(uint32_t S, uint32_t Y, uint32_t items, bool atp) {
+    return ((size_t)40 * S + (size_t)255 * S + (size_t)42 * S + (size_t)9 * Y + (size_t)items * 5 * S +
+            (atp ? S : 0u) + 4 + 3) & ~(size_t)3;
 }
+template <bool kFull>
 __device__ inline Scr make_scr(const AdjDev& d) {
     Scr s;
     float* base = d.scr + (size_t)(blockIdx.y * gridDim.x + blockIdx.x) * d.scr_floats;
@@ -352,13 +401,15 @@ __device__ inline Scr make_scr(const AdjDev& d) {
     s.jac = f; f += 255 * S;
     s.estart = f; f += 42 * S;
     s.syn = f; f += 9 * d.Ymax;
-    s.pre = f;
+    s.pre = f; f += (size_t)ItemStride<kFull>::v * 5 * S;
+    s.atpf = f;
     return s;
 }
 
 // One tick of the neuron in shared memory; each kernel has one call site, so one copy.
 // kRec records the intermediates the reverse
 // tick reads (into L.s2, L.ib3, L.pmask, L.phs and the CTA's scratch).
+template <bool kFull>
 __device__ __forceinline__ void tick_fwd(const AdjDev& d, const Ctx& c, const Lay& L, const Scr& sc, uint32_t t,
                                          bool kRec) {
     const uint32_t tid = threadIdx.x;
@@ -370,7 +421,7 @@ __device__ __forceinline__ void tick_fwd(const AdjDev& d, const Ctx& c, const La
     float* st = L.st;
 
     // ---- step 1 ----
-    if (seg) L.ibuf[tid] = step1_seg(d, c, L, tick, dt, kRec ? sc.pre : nullptr);
+    if (seg) L.ibuf[tid] = step1_seg<kFull>(d, c, L, tick, dt, kRec ? sc.pre : nullptr);
     __syncthreads();
 
     // ---- step 2.5 (diffusion_kernel.h:115-364) ----
@@ -547,6 +598,41 @@ __device__ __forceinline__ void tick_fwd(const AdjDev& d, const Ctx& c, const La
             }
             __syncthreads();
         }
+        // ATP (diffusion_kernel.h:284-345): on each intracellular connection whose ATP
+        // difference exceeds 1e-12, flux = 0.14 area dC dt / dist in float, left to right;
+        // each segment adds -+flux / its volume in connection order
+        if (kFull && d.has_atp) {   // without a pump ATP is uniform in time, and the pass moves nothing
+        if (kRec && seg) sc.atpf[tid] = st[d.atp_w * Sm + tid];
+        if (edge) {
+            float fl = 0.0f, on = 0.0f;
+            if (c.eintra) {
+                const float dC = st[d.atp_w * Sm + c.ea] - st[d.atp_w * Sm + c.eb];
+                if (dC > 1e-12f || dC < -1e-12f) {
+                    fl = 0.14f * c.earea * dC * dt / c.edist;
+                    on = 1.0f;
+                }
+            }
+            L.gax[tid] = fl;
+            L.term[tid] = on;
+        }
+        __syncthreads();
+        if (seg) {
+            float vf = (float)c.vol;
+            if (vf < 1e-6f) vf = 1e-6f;
+            float acc = 0.0f;
+#pragma unroll
+            for (int k = 0; k < kMaxInc; k++) {
+                if ((uint32_t)k >= c.ninc) break;
+                const uint32_t w = c.inc[k];
+                const uint32_t le = inc_le(w);
+                if (L.term[le] == 0.0f) continue;
+                if (inc_isa(w)) acc -= L.gax[le] / vf;
+                else acc += L.gax[le] / vf;
+            }
+            st[d.atp_w * Sm + tid] = st[d.atp_w * Sm + tid] + acc;
+        }
+        __syncthreads();
+        }
         // bath relaxation and clamp of the extracellular ions (diffusion_kernel.h:348-360)
         if (seg) {
             if (kRec)
@@ -576,7 +662,7 @@ __device__ __forceinline__ void tick_fwd(const AdjDev& d, const Ctx& c, const La
         s.area = c.area;
         s.vol = c.vol;
         ghk_cache_fill(s.gc, s.V);
-        float* rs = st + kSegWords * Sm;
+        float* rs = st + (kFull ? d.W : kW3) * Sm;
         for (uint32_t y = d.sp_off[g]; y < d.sp_off[g + 1]; y++) {
             const uint32_t ly = y - c.y0;
             float cleft = cleft_events(d, y, tick, rs[ly * kSynWords + 4]);
@@ -630,6 +716,7 @@ __device__ __forceinline__ void tick_fwd(const AdjDev& d, const Ctx& c, const La
 // intermediates, and L.lam the adjoint of the state after the tick (V, ions, gates).
 // On exit L.lam holds the adjoint of the starting state; gp accumulates
 // d loss / d (gNa, gK, gleak) of this thread's segment.
+template <bool kFull>
 __device__ void tick_rev(const AdjDev& d, const Ctx& c, const Lay& L, const Scr& sc, uint32_t t, double* gp) {
     const uint32_t tid = threadIdx.x;
     const uint32_t S = c.S, E = c.E, Sm = d.Smax, Em = d.Emax;
@@ -726,6 +813,33 @@ __device__ void tick_rev(const AdjDev& d, const Ctx& c, const Lay& L, const Scr&
             }
         }
         __syncthreads();
+        // ---- the ATP Fick pass reversed: atp_a -= f / v_a, atp_b += f / v_b with
+        // f = c (atp_a - atp_b) on the connections that passed the threshold ----
+        if (kFull && d.has_atp) {
+        if (edge) {
+            float v = 0.0f;
+            if (c.eintra) {
+                const float dC = sc.atpf[c.ea] - sc.atpf[c.eb];
+                if (dC > 1e-12f || dC < -1e-12f) {
+                    const float lfl = -lam[d.atp_w * Sm + c.ea] / c.eva + lam[d.atp_w * Sm + c.eb] / c.evb;
+                    v = lfl * (0.14f * c.earea * dt / c.edist);
+                }
+            }
+            L.edv[tid] = v;
+        }
+        __syncthreads();
+        if (seg) {
+            float acc = 0.0f;
+#pragma unroll
+            for (int k = 0; k < kMaxInc; k++) {
+                if ((uint32_t)k >= c.ninc) break;
+                const uint32_t w = c.inc[k];
+                acc += inc_isa(w) ? L.edv[inc_le(w)] : -L.edv[inc_le(w)];
+            }
+            lam[d.atp_w * Sm + tid] += acc;
+        }
+        __syncthreads();
+        }
         // ---- extracellular sub-steps, last first ----
         float elphi = 0.0f;
         float bm[7], bp[7], dbm[7], dbp[7], kq[7];
@@ -972,16 +1086,27 @@ __device__ void tick_rev(const AdjDev& d, const Ctx& c, const Lay& L, const Scr&
         const uint32_t ni = d.n_it[g];
         float lV = lam[tid];
         for (int j = (int)ni - 1; j >= 0; j--) {
-            const uint8_t type = d.it_type[g * kItems + j];
-            const uint32_t go = d.it_gate[g * kItems + j];
-            const int ion = (type == 141 || type == 142) ? 0 : 1;
-            const int cls = cls_of(type);
-            const float* pst = d.it_st + ((size_t)g * kItems + j) * 7;
-            const float den = par_of(d, c.p, cls, g);
+            constexpr uint32_t IS = ItemStride<kFull>::v;
+            const uint8_t type = d.it_type[g * IS + j];
+            const uint32_t go = d.it_gate[g * IS + j];
+            const float den = kFull ? den_of(d, c.p, type, g, j) : par_of(d, c.p, cls_k<kFull>(type), g);
             const float pV = sc.pre[(j * 5 + 0) * Sm + tid], pG0 = sc.pre[(j * 5 + 1) * Sm + tid],
                         pG1 = sc.pre[(j * 5 + 2) * Sm + tid], pCi = sc.pre[(j * 5 + 3) * Sm + tid],
                         pCo = sc.pre[(j * 5 + 4) * Sm + tid];
-            const int ng = (type == 123) ? 1 : (type == 107 ? 0 : 2);
+            if (kFull && type == 7) {   // the pump: inputs V, Na_in, K_out, ATP (recorded in that order)
+                float lp[7] = {lV, lam[1 * Sm + tid], lam[8 * Sm + tid], lam[2 * Sm + tid], lam[9 * Sm + tid],
+                               lam[d.atp_w * Sm + tid], lIt};
+                adj::vjp_pump(lp, pV, pG0, pG1, pCi, den, c.area, c.vol, dt);
+                lV = lp[0];
+                lam[1 * Sm + tid] = lp[1];
+                lam[9 * Sm + tid] = lp[4];
+                lam[d.atp_w * Sm + tid] = lp[5];
+                continue;
+            }
+            const int ion = (type == 141 || type == 142) ? 0 : ((kFull && type == 1) ? 2 : 1);
+            const int cls = cls_k<kFull>(type);
+            const float* pst = d.it_st + ((size_t)g * IS + j) * 7;
+            const int ng = gates_k<kFull>(type);
             const float lo[6] = {lV,
                                  ng > 0 ? lam[(15 + go) * Sm + tid] : 0.0f,
                                  ng > 1 ? lam[(16 + go) * Sm + tid] : 0.0f,
@@ -991,13 +1116,19 @@ __device__ void tick_rev(const AdjDev& d, const Ctx& c, const Lay& L, const Scr&
             float lx[6];
             if (type == 123) adj::vjp_kvdr_f(lo, lx, pV, pG0, pCi, pCo, den, c.area, c.vol, dt, pst);
             else if (type == 107) adj::vjp_k2p_f(lo, lx, pV, pCi, pCo, den, c.area, c.vol, dt, pst);
+            else if (kFull && type == 1) {   // out of line, through arrays of its own (lo / lx stay in registers)
+                float lo1[6], lx1[6];
+                for (int k = 0; k < 6; k++) lo1[k] = lo[k];
+                adj::vjp_cav13(lo1, lx1, pV, pG0, pG1, pCi, pCo, den, c.area, c.vol, dt, pst);
+                for (int k = 0; k < 6; k++) lx[k] = lx1[k];
+            }
             else adj::vjp_nav_f(lo, lx, pV, pG0, pG1, pCi, pCo, den, c.area, c.vol, dt, type == 142 ? 1 : 0, pst[5]);
             lV = lx[0];
             if (ng > 0) lam[(15 + go) * Sm + tid] = lx[1];
             if (ng > 1) lam[(16 + go) * Sm + tid] = lx[2];
             lam[(1 + ion) * Sm + tid] = lx[3];
             lam[(8 + ion) * Sm + tid] = lx[4];
-            gp[cls] += (double)lx[5];
+            if (!kFull || cls >= 0) gp[cls] += (double)lx[5];
         }
         lam[tid] = lV;
     }
@@ -1011,21 +1142,22 @@ __global__ void k_adj_init(AdjDev d) {
 }
 
 // Forward pass over ticks [t0, t1): checkpoints every K ticks, the loss and the traces.
+template <bool kFull>
 __global__ void __launch_bounds__(kMaxSeg) k_adj_forward(AdjDev d, uint32_t t0, uint32_t t1) {
     extern __shared__ __align__(16) unsigned char smem[];
     const Ctx c = make_ctx(d);
-    const Lay L = make_lay(smem, d.Smax, d.Emax, d.Ymax, false);
+    const Lay L = make_lay(smem, d.Smax, d.Emax, d.Ymax, false, d.W);
     const Scr sc{};
     float* gstate = d.state + (size_t)c.p * d.L + c.st_off;
-    block_load(L.st, gstate, c, d.Smax);
+    block_load(L.st, gstate, c, d.Smax, d.W);
     __syncthreads();
     double loss = 0.0;
     for (uint32_t t = t0; t < t1; t++) {
         if (t % d.K == 0) {
-            block_store(d.ckpt + ((size_t)(t / d.K) * d.n_sets + c.p) * d.L + c.st_off, L.st, c, d.Smax);
+            block_store(d.ckpt + ((size_t)(t / d.K) * d.n_sets + c.p) * d.L + c.st_off, L.st, c, d.Smax, d.W);
             __syncthreads();
         }
-        tick_fwd(d, c, L, sc, t, false);
+        tick_fwd<kFull>(d, c, L, sc, t, false);
         if ((t + 1) % d.stride == 0 && threadIdx.x == c.soma) {
             const uint32_t smp = (t + 1) / d.stride - 1;
             const float V = L.st[c.soma];
@@ -1036,24 +1168,26 @@ __global__ void __launch_bounds__(kMaxSeg) k_adj_forward(AdjDev d, uint32_t t0, 
             if (d.trace) d.trace[((size_t)c.p * d.n_samples + smp) * d.nn + c.n] = V;
         }
     }
-    block_store(gstate, L.st, c, d.Smax);
+    block_store(gstate, L.st, c, d.Smax, d.W);
     if (threadIdx.x == c.soma) d.loss_part[(size_t)c.p * d.nn + c.n] += loss;
 }
 
 // Reverse pass over window w (ticks [w K, min((w + 1) K, T))).
+template <bool kFull>
 __global__ void __launch_bounds__(kMaxSeg) k_adj_backward(AdjDev d, uint32_t w) {
     extern __shared__ __align__(16) unsigned char smem[];
     const Ctx c = make_ctx(d);
-    const Lay L = make_lay(smem, d.Smax, d.Emax, d.Ymax, true);
-    const Scr sc = make_scr(d);
+    const uint32_t W = kFull ? d.W : kW3;
+    const Lay L = make_lay(smem, d.Smax, d.Emax, d.Ymax, true, W);
+    const Scr sc = make_scr<kFull>(d);
     const uint32_t tb = w * d.K;
     const uint32_t te = min(d.T, tb + d.K);
     const uint32_t Sm = d.Smax;
     {   // adjoint of the state at the window's end
         const float* src = d.lam + (size_t)c.p * d.L + c.st_off;
-        for (uint32_t q = threadIdx.x; q < kSegWords * c.S; q += blockDim.x) L.lam[(q / c.S) * Sm + (q % c.S)] = src[q];
+        for (uint32_t q = threadIdx.x; q < W * c.S; q += blockDim.x) L.lam[(q / c.S) * Sm + (q % c.S)] = src[q];
     }
-    block_load(L.st, d.ckpt + ((size_t)w * d.n_sets + c.p) * d.L + c.st_off, c, d.Smax);
+    block_load(L.st, d.ckpt + ((size_t)w * d.n_sets + c.p) * d.L + c.st_off, c, d.Smax, W);
     __syncthreads();
     // Steps [0, nA): re-run the window from its checkpoint, keeping each tick's starting
     // state; steps [nA, nA + n): walk the ticks backwards, each re-run with its
@@ -1067,19 +1201,19 @@ __global__ void __launch_bounds__(kMaxSeg) k_adj_backward(AdjDev d, uint32_t w) 
         const uint32_t t = rec ? te - 1 - (step - nA) : tb + step;
         float* blk = d.win + ((size_t)(t - tb) * d.n_sets + c.p) * d.L + c.st_off;
         if (!rec) {
-            block_store(blk, L.st, c, d.Smax);
+            block_store(blk, L.st, c, d.Smax, W);
         } else {
-            if (step == nA) block_store(blk, L.st, c, d.Smax);   // the window's last tick
+            if (step == nA) block_store(blk, L.st, c, d.Smax, W);   // the window's last tick
             __syncthreads();
-            block_load(L.st, blk, c, d.Smax);
+            block_load(L.st, blk, c, d.Smax, W);
         }
         __syncthreads();
-        tick_fwd(d, c, L, sc, t, rec);
-        if (rec) tick_rev(d, c, L, sc, t, gp);
+        tick_fwd<kFull>(d, c, L, sc, t, rec);
+        if (rec) tick_rev<kFull>(d, c, L, sc, t, gp);
     }
     {
         float* dst = d.lam + (size_t)c.p * d.L + c.st_off;
-        for (uint32_t q = threadIdx.x; q < kSegWords * c.S; q += blockDim.x) dst[q] = L.lam[(q / c.S) * Sm + (q % c.S)];
+        for (uint32_t q = threadIdx.x; q < W * c.S; q += blockDim.x) dst[q] = L.lam[(q / c.S) * Sm + (q % c.S)];
     }
     if (threadIdx.x < c.S)
         for (int k = 0; k < 3; k++) d.g_par[((size_t)c.p * 3 + k) * d.n_seg + c.g] += gp[k];
@@ -1250,7 +1384,7 @@ int adj_build(Adjoint* A, void* sim, const BncAdjointConfig& cfg) {
     std::vector<float> area(N), cm(N);
     std::vector<double> vol(N);
     std::vector<uint8_t> n_it(N, 0), it_type((size_t)N * kItems, 0), it_gate((size_t)N * kItems, 0);
-    std::vector<float> it_st((size_t)N * kItems * 7, 0.0f);
+    std::vector<float> it_st((size_t)N * kItems * 7, 0.0f), it_den((size_t)N * kItems, 0.0f);
     A->par0.assign((size_t)3 * N, 0.0f);
     for (uint32_t i = 0; i < N; i++) {
         const SegLite& s = hn.seg[i];
@@ -1266,22 +1400,46 @@ int adj_build(Adjoint* A, void* sim, const BncAdjointConfig& cfg) {
             const uint8_t t = m.type;
             if (myel && t != BNC_MOD_MYELIN && host_is_myelin_blocked(t)) continue;   // simulation_host.cpp:241
             if (t == BNC_MOD_MYELIN || t == BNC_MOD_CAV21) continue;   // no current, nothing the replay reads
-            if (t != BNC_MOD_NAV16 && t != BNC_MOD_NAV12 && t != BNC_MOD_KV_DR && t != BNC_MOD_K2P) {
+            if (t != BNC_MOD_NAV16 && t != BNC_MOD_NAV12 && t != BNC_MOD_KV_DR && t != BNC_MOD_K2P &&
+                t != BNC_MOD_CAV13 && t != BNC_MOD_PUMP_NAK) {
                 set_error("adjoint: modifier type %u (segment %u) is not differentiated (Nav1.6/1.2, Kv_DR, K2P, "
-                          "myelin and Cav2.1 are)", (unsigned)t, i);
+                          "Cav1.3, the Na/K pump, myelin and Cav2.1 are)", (unsigned)t, i);
                 return BNC_ERR_UNSUPPORTED;
             }
-            const int cls = (t == BNC_MOD_KV_DR) ? 1 : (t == BNC_MOD_K2P ? 2 : 0);
-            if (cls_used[cls]) { set_error("adjoint: segment %u holds two modifiers of one conductance class", i); return BNC_ERR_UNSUPPORTED; }
-            cls_used[cls] = true;
+            const int ng = (t == BNC_MOD_KV_DR) ? 1 : ((t == BNC_MOD_K2P || t == BNC_MOD_PUMP_NAK) ? 0 : 2);
+            if (n_it[i] >= kItems || gates + ng > (uint32_t)kGates) {
+                set_error("adjoint: segment %u holds more differentiable modifiers than %d items and %d gate words",
+                          i, kItems, kGates);
+                return BNC_ERR_UNSUPPORTED;
+            }
+            const int cls = (t == BNC_MOD_KV_DR) ? 1 : (t == BNC_MOD_K2P ? 2 : ((t == BNC_MOD_NAV16 || t == BNC_MOD_NAV12) ? 0 : -1));
+            if (cls >= 0) {
+                if (cls_used[cls]) { set_error("adjoint: segment %u holds two modifiers of one conductance class", i); return BNC_ERR_UNSUPPORTED; }
+                cls_used[cls] = true;
+            }
             const uint32_t k = n_it[i]++;
             it_type[(size_t)i * kItems + k] = t;
             it_gate[(size_t)i * kItems + k] = (uint8_t)gates;
+            it_den[(size_t)i * kItems + k] = m.density;
             for (int q = 0; q < 7; q++) it_st[((size_t)i * kItems + k) * 7 + q] = m.state[q];
-            gates += (t == BNC_MOD_KV_DR) ? 1 : (t == BNC_MOD_K2P ? 0 : 2);
-            A->par0[(size_t)cls * N + i] = m.density;
+            gates += ng;
+            if (cls >= 0) A->par0[(size_t)cls * N + i] = m.density;
         }
     }
+
+    // state words per segment: the gate words the segments need, and ATP with a pump
+    uint32_t gmax = 0;
+    for (uint32_t i = 0; i < N; i++)
+        for (uint32_t j = 0; j < n_it[i]; j++) {
+            const uint8_t t = it_type[(size_t)i * kItems + j];
+            const uint32_t ng = (t == BNC_MOD_KV_DR) ? 1u : ((t == BNC_MOD_K2P || t == BNC_MOD_PUMP_NAK) ? 0u : 2u);
+            gmax = std::max<uint32_t>(gmax, it_gate[(size_t)i * kItems + j] + ng);
+        }
+    const bool has_atp = std::find(it_type.begin(), it_type.end(), (uint8_t)BNC_MOD_PUMP_NAK) != it_type.end();
+    const bool full_items = has_atp || std::find(it_type.begin(), it_type.end(), (uint8_t)BNC_MOD_CAV13) != it_type.end();
+    const uint32_t atp_w = 15 + gmax;
+    // the fitting family's kernels take kW3 words (gmax <= 3 without Cav1.3)
+    const uint32_t Wseg = full_items ? atp_w + (has_atp ? 1u : 0u) : kW3;
 
     // synapse slots by post segment (original order within a segment)
     const uint32_t KS = hn.num_synapses;
@@ -1352,7 +1510,7 @@ int adj_build(Adjoint* A, void* sim, const BncAdjointConfig& cfg) {
         nr_slot[n + 1] = sp_cnt[nr_seg[n + 1]];
         const uint32_t S = nr_seg[n + 1] - nr_seg[n], Y = nr_slot[n + 1] - nr_slot[n];
         Ymax = std::max(Ymax, Y);
-        nr_st[n + 1] = nr_st[n] + kSegWords * S + kSynWords * Y;
+        nr_st[n + 1] = nr_st[n] + Wseg * S + kSynWords * Y;
         uint32_t so = 0;
         for (uint32_t i = nr_seg[n]; i < nr_seg[n + 1]; i++)
             if (hn.seg[i].segment_type == BNC_SEG_SOMA) { so = i - nr_seg[n]; break; }
@@ -1368,6 +1526,7 @@ int adj_build(Adjoint* A, void* sim, const BncAdjointConfig& cfg) {
             const SegLite& s = hn.seg[s0 + i];
             b[i] = s.V_m;
             for (int q = 0; q < 7; q++) { b[(1 + q) * S + i] = s.intra_ions[q]; b[(8 + q) * S + i] = s.extra_ions[q]; }
+            if (has_atp) b[atp_w * S + i] = s.ATP_level;
             for (uint32_t j = 0; j < n_it[s0 + i]; j++) {
                 const uint8_t t = it_type[(size_t)(s0 + i) * kItems + j];
                 const uint32_t go = it_gate[(size_t)(s0 + i) * kItems + j];
@@ -1375,15 +1534,15 @@ int adj_build(Adjoint* A, void* sim, const BncAdjointConfig& cfg) {
                 for (uint32_t jj = 0; jj < s.modifier_count; jj++) {
                     const ModLite& m = hn.mod(s0 + i, jj);
                     if (m.type != t) continue;
-                    if (t != BNC_MOD_K2P) b[(15 + go) * S + i] = m.state[0];
-                    if (t == BNC_MOD_NAV16 || t == BNC_MOD_NAV12) b[(16 + go) * S + i] = m.state[1];
+                    if (t != BNC_MOD_K2P && t != BNC_MOD_PUMP_NAK) b[(15 + go) * S + i] = m.state[0];
+                    if (t == BNC_MOD_NAV16 || t == BNC_MOD_NAV12 || t == BNC_MOD_CAV13) b[(16 + go) * S + i] = m.state[1];
                     break;
                 }
             }
         }
         const uint32_t y0 = nr_slot[n], Y = nr_slot[n + 1] - y0;
         for (uint32_t y = 0; y < Y; y++)
-            for (int q = 0; q < kSynWords; q++) b[kSegWords * S + y * kSynWords + q] = rinit[(size_t)(y0 + y) * kSynWords + q];
+            for (int q = 0; q < kSynWords; q++) b[Wseg * S + y * kSynWords + q] = rinit[(size_t)(y0 + y) * kSynWords + q];
     }
 
     // current stimuli per segment, in list order (matched by segment id, simulation_host.cpp:285-297)
@@ -1425,13 +1584,28 @@ int adj_build(Adjoint* A, void* sim, const BncAdjointConfig& cfg) {
     d.T = cfg.ticks; d.K = K; d.n_ckpt = (cfg.ticks + K - 1) / K; d.stride = stride; d.n_samples = cfg.ticks / stride;
     d.Smax = (Smax + 3u) & ~3u;   // stride of the per-segment arrays: a multiple of 4 (16-byte rows)
     d.Emax = std::max(Emax, 1u); d.Ymax = Ymax; d.L = L; d.dt = cfg.dt; d.has_conn = M > 0;
+    d.has_atp = has_atp ? 1 : 0;
+    d.full = full_items ? 1 : 0;
+    d.W = Wseg;
+    d.atp_w = atp_w;
     d.tick0 = tick0;
     std::vector<uint32_t> nr_seg_v(nr_seg.begin(), nr_seg.end());
     d.nr_seg = upload(al, nr_seg_v, &rc); d.nr_edge = upload(al, nr_edge, &rc); d.nr_slot = upload(al, nr_slot, &rc);
     d.nr_st = upload(al, nr_st, &rc); d.nr_soma = upload(al, nr_soma, &rc);
     d.area = upload(al, area, &rc); d.cm = upload(al, cm, &rc); d.vol = upload(al, vol, &rc);
+    if (!full_items) {   // the fitting family's kernels index items with stride 3
+        std::vector<uint8_t> t3((size_t)N * 3), g3((size_t)N * 3);
+        std::vector<float> s3((size_t)N * 3 * 7), d3((size_t)N * 3);
+        for (uint32_t i = 0; i < N; i++)
+            for (uint32_t j = 0; j < 3; j++) {
+                const size_t a = (size_t)i * kItems + j, b3 = (size_t)i * 3 + j;
+                t3[b3] = it_type[a]; g3[b3] = it_gate[a]; d3[b3] = it_den[a];
+                for (int q = 0; q < 7; q++) s3[b3 * 7 + q] = it_st[a * 7 + q];
+            }
+        it_type.swap(t3); it_gate.swap(g3); it_st.swap(s3); it_den.swap(d3);
+    }
     d.n_it = upload(al, n_it, &rc); d.it_type = upload(al, it_type, &rc); d.it_gate = upload(al, it_gate, &rc);
-    d.it_st = upload(al, it_st, &rc); d.inc_n = upload(al, inc_n, &rc); d.inc_e = upload(al, inc_e, &rc);
+    d.it_st = upload(al, it_st, &rc); d.it_den = upload(al, it_den, &rc); d.inc_n = upload(al, inc_n, &rc); d.inc_e = upload(al, inc_e, &rc);
     d.stim_off = upload(al, stim_off, &rc); d.stim_b = upload(al, stim_b, &rc); d.stim_e = upload(al, stim_e, &rc);
     d.stim_amp = upload(al, stim_amp, &rc); d.sp_off = upload(al, sp_cnt, &rc);
     d.ed_a = upload(al, ed_a, &rc); d.ed_b = upload(al, ed_b, &rc); d.ed_intra = upload(al, ed_intra, &rc);
@@ -1457,7 +1631,7 @@ int adj_build(Adjoint* A, void* sim, const BncAdjointConfig& cfg) {
     d.loss_part = static_cast<double*>(al.alloc((size_t)cfg.n_sets * nn * sizeof(double)));
     d.g_par = static_cast<double*>(al.alloc((size_t)cfg.n_sets * 3 * N * sizeof(double)));
     d.g_w = static_cast<double*>(al.alloc((size_t)cfg.n_sets * std::max(KS, 1u) * sizeof(double)));
-    d.scr_floats = scr_floats(d.Smax, Ymax);
+    d.scr_floats = scr_floats(d.Smax, Ymax, full_items ? (uint32_t)kItems : 3u, has_atp);
     d.scr = static_cast<float*>(al.alloc((size_t)nn * cfg.n_sets * d.scr_floats * sizeof(float)));
     if (!d.state || !d.lam || !d.ckpt || !d.win || !d.loss_part || !d.g_par || !d.g_w || !d.scr)
         return adj_fail(BNC_ERR_ALLOC, "state, checkpoints and scratch");
@@ -1473,11 +1647,13 @@ int adj_build(Adjoint* A, void* sim, const BncAdjointConfig& cfg) {
     d.target = nullptr;
     d.trace = nullptr;
     A->threads = ((std::max(d.Smax, d.Emax) + 31u) / 32u) * 32u;
-    A->smem_fwd = lay_bytes(d.Smax, d.Emax, Ymax, false);
-    A->smem_bwd = lay_bytes(d.Smax, d.Emax, Ymax, true);
+    A->smem_fwd = lay_bytes(d.Smax, d.Emax, Ymax, false, Wseg);
+    A->smem_bwd = lay_bytes(d.Smax, d.Emax, Ymax, true, Wseg);
     if (A->smem_bwd > 227u * 1024u) { set_error("adjoint: a neuron needs %zu bytes of shared memory", A->smem_bwd); return BNC_ERR_UNSUPPORTED; }
-    if (cudaFuncSetAttribute(k_adj_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)A->smem_fwd) != cudaSuccess ||
-        cudaFuncSetAttribute(k_adj_backward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)A->smem_bwd) != cudaSuccess)
+    if (cudaFuncSetAttribute(k_adj_forward<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)A->smem_fwd) != cudaSuccess ||
+        cudaFuncSetAttribute(k_adj_forward<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)A->smem_fwd) != cudaSuccess ||
+        cudaFuncSetAttribute(k_adj_backward<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)A->smem_bwd) != cudaSuccess ||
+        cudaFuncSetAttribute(k_adj_backward<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)A->smem_bwd) != cudaSuccess)
         return adj_fail(BNC_ERR_CUDA, "shared-memory limit");
     return BNC_OK;
 }
@@ -1663,7 +1839,8 @@ int bnc_adjoint_forward(void* adj, double* loss, float* trace) {
     const dim3 grid(d.nn, d.n_sets);
     for (uint32_t t0 = 0; t0 < d.T; t0 += d.K) {
         const uint32_t t1 = std::min(d.T, t0 + d.K);
-        k_adj_forward<<<grid, A->threads, A->smem_fwd, A->stream>>>(d, t0, t1);
+        if (d.full) k_adj_forward<true><<<grid, A->threads, A->smem_fwd, A->stream>>>(d, t0, t1);
+        else k_adj_forward<false><<<grid, A->threads, A->smem_fwd, A->stream>>>(d, t0, t1);
     }
     cudaEventRecord(A->ev1, A->stream);
     cudaError_t e = cudaStreamSynchronize(A->stream);
@@ -1700,7 +1877,8 @@ int bnc_adjoint_backward(void* adj, float* g_gNa, float* g_gK, float* g_gleak, f
     cudaEventRecord(A->ev0, A->stream);
     const dim3 grid(d.nn, d.n_sets);
     for (int w = (int)d.n_ckpt - 1; w >= 0; w--)
-        k_adj_backward<<<grid, A->threads, A->smem_bwd, A->stream>>>(d, (uint32_t)w);
+        if (d.full) k_adj_backward<true><<<grid, A->threads, A->smem_bwd, A->stream>>>(d, (uint32_t)w);
+        else k_adj_backward<false><<<grid, A->threads, A->smem_bwd, A->stream>>>(d, (uint32_t)w);
     cudaEventRecord(A->ev1, A->stream);
     cudaError_t e = cudaStreamSynchronize(A->stream);
     if (e == cudaSuccess) e = cudaGetLastError();

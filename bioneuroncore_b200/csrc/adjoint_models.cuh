@@ -471,6 +471,109 @@ __device__ __forceinline__ void logistic_f(float z, float* v, float* dv) {
     *dv = -ez / (den * den);
 }
 
+// Cav1.3 (hh_biological.cpp:142-187): lambda^T J in single precision, contracted by
+// hand.  The divalent GHK flux is 2 x the monovalent one at 2V (the thresholds of
+// run_tick_common.h:274-312 coincide), so ghk_mono_f gives its value and partials
+// without cancellation near 0.  lo = adjoints of (V', m', h', Ca_in', Ca_out',
+// returned I); lx = adjoints of (V, m, h, Ca_in, Ca_out, density) -- the density is
+// not fitted and its entry is 0.
+__device__ __noinline__ void vjp_cav13(const float* lo, float* lx, float V, float m0, float h0, float cin, float cout,
+                                      float den, float area, double vol, float dt, const float* st) {
+    const float Vhalf = (st[3] != 0.0f) ? -fabsf(st[3]) : -35.0f;
+    const float kk = ((st[4] > 0.0f) ? st[4] : 7.0f) + 1e-6f;
+    const float gamma = (st[2] > 0.0f) ? st[2] : 25.0f;
+    const float a = dt / 2.0f, b = dt / 100.0f;
+    float mi, dmi, hi0, dhi0;
+    logistic_f(-(V - Vhalf) / kk, &mi, &dmi);   // d mi / dV = -dmi / kk
+    logistic_f((V + 52.0f) / 8.0f, &hi0, &dhi0);  // d hi0 / dV = dhi0 / 8
+    const float m1 = m0 + (mi - m0) * a;
+    const float hc = 1.0f / (1.0f + cin * (1000.0f / 3.0f));
+    const float h1 = h0 + (hi0 * hc - h0) * b;
+    const bool mm = m1 >= 0.0f && m1 <= 1.0f, mh = h1 >= 0.0f && h1 <= 1.0f;
+    const float mc = fminf(fmaxf(m1, 0.0f), 1.0f), hcl = fminf(fmaxf(h1, 0.0f), 1.0f);
+    const float open = mc * mc * hcl;
+    const GhkF g = ghk_mono_f(2.0f * V, cin, cout);
+    const float flux = 2.0f * g.F, fV = 4.0f * g.dV, fci = 2.0f * g.dci, fco = 2.0f * g.dco;
+    const float G = (float)((double)gamma * 1e-12 * (kR * kT) / (4.0 * kF * kF * (double)0.12775f) * 1e12) * den * area;
+    const float I = G * flux * open;
+    const float cpm = (float)(kF * vol / 1000.0);
+    const float s_in = dt / (2.0f * cpm), s_out = dt / (2.0f * cpm * (float)kEVR);
+    const float lcin1 = (cin - I * s_in >= 1e-9f) ? lo[3] : 0.0f, lcout1 = (cout - I * s_out >= 1e-9f) ? lo[4] : 0.0f;
+    const float lI = -lo[5] - lcin1 * s_in - lcout1 * s_out;
+    const float lopen = lI * G * flux, lflux = lI * G * open;
+    const float lm1 = mm ? (lo[1] + lopen * 2.0f * mc * hcl) : 0.0f;
+    const float lh1 = mh ? (lo[2] + lopen * mc * mc) : 0.0f;
+    const float lmi = lm1 * a, lhi = lh1 * b;
+    lx[0] = lo[0] - lmi * dmi / kk + lhi * hc * dhi0 / 8.0f + lflux * fV;
+    lx[1] = lm1 * (1.0f - a);
+    lx[2] = lh1 * (1.0f - b);
+    lx[3] = lcin1 + lflux * fci - lhi * hi0 * hc * hc * (1000.0f / 3.0f);
+    lx[4] = lcout1 + lflux * fco;
+    lx[5] = 0.0f;
+}
+
+// The Na/K pump (hh_biological.cpp:57-97, nak_pump_vnorm modifier_helpers.h:1135-1170)
+// reversed in single precision.  Inputs V, Na_in, K_out, ATP; outputs Na_in', Na_out',
+// K_in', K_out', ATP' and the returned current.  lp holds the adjoints of (V', Na_in',
+// Na_out', K_in', K_out', ATP', I) on entry and those of (V, Na_in, Na_out, K_in, K_out,
+// ATP) on exit (Na_out and K_in pass through; V is not changed).  The transport cap (the
+// available Na and K) is a branch by value; the ion floors of 1e-9 are not reached by
+// a capped transport and are left out.
+__device__ __noinline__ void vjp_pump(float* lp, float V, float Na, float Ko, float atp0, float den, float area,
+                                     double vol, float dt) {
+    const float Na3 = Na * Na * Na, K2 = Ko * Ko, KK2 = 1.5f * 1.5f;
+    const float fNa = Na3 / (Na3 + 1000.0f), fK = K2 / (K2 + KK2);
+    const float dfNa = 3000.0f * Na * Na / ((Na3 + 1000.0f) * (Na3 + 1000.0f));
+    const float dfK = 2.0f * Ko * KK2 / ((K2 + KK2) * (K2 + KK2));
+    const bool atp_pos = atp0 >= 0.0f;
+    const float at = atp_pos ? atp0 : 0.0f;
+    const float fATP = at / (at + 0.5f), dfATP = atp_pos ? 0.5f / ((at + 0.5f) * (at + 0.5f)) : 0.0f;
+    const float cV = (float)(0.8 * kF * 0.001 / (kR * kT));
+    const float a2 = 60.0f * expf(0.5f * cV * V), b2 = 6.0f * expf(-0.5f * cV * V);
+    const float a1 = 200.0f * fNa * fATP, a3 = 200.0f * fK;
+    const float vmax = 200.0f / (200.0f / 200.0f + 1.0f + 200.0f / 60.0f);
+    float dv[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    float vn = 0.0f;
+    if (a1 != 0.0f) {
+        const float dn = a3 / a1 + (b2 + a3) / a2 + 1.0f + a3 / 60.0f;
+        const float tv = a3 / dn, q = tv / dn;
+        vn = tv / vmax;
+        const float t_a1 = q * a3 / (a1 * a1), t_a2 = q * (b2 + a3) / (a2 * a2);
+        const float t_a3 = 1.0f / dn - q * (1.0f / a1 + 1.0f / a2 + 1.0f / 60.0f), t_b2 = -q / a2;
+        dv[0] = 0.5f * cV * (t_a2 * a2 - t_b2 * b2) / vmax;
+        dv[1] = t_a1 * 200.0f * dfNa * fATP / vmax;
+        dv[2] = t_a3 * 200.0f * dfK / vmax;
+        dv[3] = t_a1 * 200.0f * fNa * dfATP / vmax;
+    }
+    const float cI = (float)((double)den * (double)area * 75.0 * (double)1.602176634e-19f * 1e12);
+    const float I = vn * cI;
+    const float cdt = dt / (float)(kF * (double)(float)vol / 1000.0);
+    const float tr_raw = I * cdt;
+    float na = (Na - 1e-9f) / 3.0f, ka = (Ko - 1e-9f) * (float)(kEVR / 2.0);
+    const bool na_on = na >= 0.0f, ka_on = ka >= 0.0f;
+    na = fmaxf(na, 0.0f);
+    ka = fmaxf(ka, 0.0f);
+    float dtr[4];
+    if (tr_raw > fminf(na, ka)) {   // capped by the available Na or K
+        dtr[0] = dtr[3] = 0.0f;
+        dtr[1] = (na < ka && na_on) ? 1.0f / 3.0f : 0.0f;
+        dtr[2] = (na >= ka && ka_on) ? (float)(kEVR / 2.0) : 0.0f;
+    } else {
+#pragma unroll
+        for (int k = 0; k < 4; k++) dtr[k] = dv[k] * cI * cdt;
+    }
+    const float la1 = (atp0 - I * (dt * 1e-8f) >= 0.0f) ? lp[5] : 0.0f;
+    const float lt = -3.0f * lp[1] + (float)(3.0 / kEVR) * lp[2] + 2.0f * lp[3] - (float)(2.0 / kEVR) * lp[4];
+    const float lI = -lp[6] - la1 * (dt * 1e-8f);
+    float lx[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) lx[k] = lt * dtr[k] + lI * dv[k] * cI;
+    lp[0] += lx[0];
+    lp[1] += lx[1];
+    lp[4] += lx[2];
+    lp[5] = la1 + lx[3];
+}
+
 __device__ __forceinline__ void vjp_nav_f(const float* lo, float* lx, float V0, float m0, float h0, float cin, float cout,
                                           float den, float area, double vol, float dt, int is12, float ttx) {
     const bool mV = V0 >= -200.0f && V0 <= 200.0f;

@@ -197,7 +197,9 @@ int generate_network(const BncNetgenParams& p, NetSink& sink, NetShape* shape_ou
                 set_mod(seg.modifiers[mc++], nav, 15.0 * scale_of(p, 0));
                 set_mod(seg.modifiers[mc++], BNC_MOD_KV_DR, 8.3 * scale_of(p, 1));
                 set_mod(seg.modifiers[mc++], BNC_MOD_K2P, 4.17 * scale_of(p, 2));
-                if (p.family != BNC_NET_ADJOINT) {   // the fitting family: the three fitted conductances only
+                // the fitting family keeps the three fitted conductances unless asked for
+                // the whole small set
+                if (p.family != BNC_NET_ADJOINT || (p.flags & BNC_NETGEN_FULL_SMALL_SET)) {
                     set_mod(seg.modifiers[mc++], BNC_MOD_CAV13, 0.04 * scale_of(p, 3));
                     set_mod(seg.modifiers[mc++], BNC_MOD_PUMP_NAK, 1500.0);
                 }

@@ -96,7 +96,7 @@ int gpu_backend_seg_size(void);
 #define BNC_NET_LARGE 2        /* 100k x 64-segment neurons, 16 of 24 types, 10M synapses */
 #define BNC_NET_TREES 3        /* depth-10 binary dendritic trees, electrodiffusion */
 #define BNC_NET_ENSEMBLE_MEMBER 4 /* one network of an uneven ensemble */
-#define BNC_NET_ADJOINT 5      /* 256 x 64-segment neurons, 2000 synapses; Nav, Kv_DR, K2P (+ myelin, Cav2.1); 1 nA steps */
+#define BNC_NET_ADJOINT 5      /* 256 x 64-segment neurons, 2000 synapses; Nav, Kv_DR, K2P (+ myelin, Cav2.1; Cav1.3 and the pump with BNC_NETGEN_FULL_SMALL_SET); 1 nA steps */
 
 typedef struct {
     uint32_t family;          /* BNC_NET_* */
@@ -121,6 +121,9 @@ typedef struct {
  * (Kv delayed rectifier 123 or Nav1.6 141 on the bouton) and a transmission delay
  * of 0.5-2 ms (drawn from a stream of their own: other draws are unchanged). */
 #define BNC_NETGEN_SYNAPSE_EXTRAS 32u
+/* The fitting family (BNC_NET_ADJOINT) with the whole small set: Cav1.3 and the Na/K
+ * pump on every segment as well, beside the three fitted conductances. */
+#define BNC_NETGEN_FULL_SMALL_SET 64u
 
 /* Generates a network into host AoS arrays in the reference layout.  The arrays
  * are owned by the library; release with bnc_netgen_free.  *stim receives the

@@ -3,20 +3,23 @@
  * path): the tick of the reference with its releases replayed from a log, in FP64
  * forward mode.  Every quantity carries its value and one directional derivative
  * with respect to the per-segment conductances (the densities of Nav1.6/Nav1.2 141/
- * 142, Kv delayed rectifier 123, K2P leak 107) and the per-synapse receptor density
+ * 142, Kv delayed rectifier 123, K2P leak 107; Cav1.3 1 and the Na/K pump 7 run with
+ * their fixed densities) and the per-synapse receptor density
  * scale, so one run gives the loss and its derivative along a chosen direction.  It
  * is the independent check of the device adjoint's gradients (which must agree with
  * it up to the difference between FP32 and FP64 trajectories) and, against central
  * differences of its own loss, is itself checked on the CPU.
  *
  * The tick restated (simulation_host.cpp:174-657): step 1 with the modifiers in slot
- * order (hh_biological.cpp:193-277, 2763-2797, 3063-3084 through the GHK helpers of
- * run_tick_common.h:274-312 and modifier_helpers.h:48-76, 132-215, 1008-1018); the
+ * order (hh_biological.cpp:193-277, 2763-2797, 3063-3084, 142-187, 57-97 through the
+ * GHK helpers of run_tick_common.h:274-312 and modifier_helpers.h:48-76, 132-215,
+ * 1008-1018, 1135-1170); the
  * current stimuli; step 2.5 (diffusion_kernel.h:41-364: phi_e Jacobi solve,
  * intracellular and extracellular Nernst-Planck sub-steps with Scharfetter-Gummel
  * fluxes, the backward-Euler V_m sweeps, the bath relaxation); step 3 with the clefts
  * from the log and AMPA / GABA-A receptors (modifier_helpers.h:1213-1278, with the
- * density scale); step 4 (simulation_host.cpp:596-649).  Transmitter, ATP and heat
+ * density scale); step 4 (simulation_host.cpp:596-649).  ATP diffuses (Fick,
+ * diffusion_kernel.h:284-345) because the pump reads it; transmitter and heat
  * diffusion are left out: nothing in the modelled networks reads them.  Every
  * arithmetic step is in double (the reference mixes float and double); clamps pass
  * the derivative where inactive and zero where active.
@@ -77,13 +80,38 @@ T vtrap(T x, double y) {
     return x / (T(1.0) - texp(-x / y));
 }
 void clamp_ions(T* a) { for (int q = 0; q < 7; q++) a[q] = floorT(a[q], 1e-9); }
+// run_tick_common.h:274-312 (divalent cation)
+T ghk_div(T V, T ci, T co) {
+    T Vn = V * (2.0 * F * 0.001 / (R * TK));
+    if (std::fabs(Vn.v) < 1e-6) return (ci - co) * (2.0 * F);
+    T A = V * (4.0 * F / (R * TK) * F * 0.001);
+    if (Vn.v > 20.0) return A * ci;
+    if (Vn.v < -20.0) return A * co;
+    T e = texp(-Vn);
+    return A * (ci - co * e) / (T(1.0) - e);
+}
+// modifier_helpers.h:1135-1170 (nak_pump_vnorm, K_m_Na 10, K_m_K 1.5)
+T pump_vnorm(T V, T Na, T Ko, T atp) {
+    T Na3 = Na * Na * Na, K2 = Ko * Ko;
+    T fNa = Na3 / (Na3 + 1000.0), fK = K2 / (K2 + (double)(1.5f * 1.5f));
+    if (atp.v < 0.0) atp = T(0.0);
+    T fATP = atp / (atp + 0.5);
+    T eta = V * (0.8 * F * 0.001 / (R * TK));
+    T a2 = texp(eta * 0.5) * 60.0, b2 = texp(-(eta * 0.5)) * 6.0;
+    T a1 = fNa * fATP * 200.0, a3 = fK * 200.0;
+    if (a1.v == 0.0) return T(0.0);
+    T den = a3 / a1 + (b2 + a3) / a2 + 1.0 + a3 / 60.0;
+    const double vmax = 200.0 / (200.0 / 200.0 + 1.0 + 200.0 / 60.0);
+    return a3 / den / vmax;
+}
 
 struct Seg {
-    T V, in[7], out[7];
-    T gate[3];          // Nav m, h; Kv_DR n
+    T V, in[7], out[7], atp;
+    T gate[5];          // Nav m, h; Kv_DR n; Cav1.3 m, h
     uint8_t type, n_it;
-    uint8_t it[3];
-    float st[3][7];
+    uint8_t it[5];
+    float st[5][7];
+    double den[5];      // densities of the items without a fitted conductance
     double area, vol, cm, radius, length;
     uint32_t id;
 };
@@ -143,6 +171,7 @@ int bo_tangent_run(const BncBionData* net, const BncCurrentStimulus* stim, uint3
         Seg& g = sg[i];
         g.V = T(s.V_m);
         for (int q = 0; q < 7; q++) { g.in[q] = T(s.intra_ions[q]); g.out[q] = T(s.extra_ions[q]); }
+        g.atp = T((double)s.ATP_level);
         g.type = s.segment_type;
         g.area = seg_area(s);
         g.vol = seg_volume(s);
@@ -165,14 +194,17 @@ int bo_tangent_run(const BncBionData* net, const BncCurrentStimulus* stim, uint3
             const BncModifier& m = s.modifiers[j];
             if (myel && m.type != BNC_MOD_MYELIN && myelin_blocked(m.type)) continue;
             if (m.type == BNC_MOD_MYELIN || m.type == BNC_MOD_CAV21) continue;
-            if (m.type != BNC_MOD_NAV16 && m.type != BNC_MOD_NAV12 && m.type != BNC_MOD_KV_DR && m.type != BNC_MOD_K2P)
+            if (m.type != BNC_MOD_NAV16 && m.type != BNC_MOD_NAV12 && m.type != BNC_MOD_KV_DR && m.type != BNC_MOD_K2P &&
+                m.type != BNC_MOD_CAV13 && m.type != BNC_MOD_PUMP_NAK)
                 return -1;
-            if (g.n_it >= 3) return -1;
+            if (g.n_it >= 5) return -1;
             const int k = g.n_it++;
             g.it[k] = m.type;
+            g.den[k] = (double)(float)m.density;
             for (int q = 0; q < 7; q++) g.st[k][q] = (float)m.state[q];
             if (m.type == BNC_MOD_NAV16 || m.type == BNC_MOD_NAV12) { g.gate[0] = T(g.st[k][0]); g.gate[1] = T(g.st[k][1]); }
             if (m.type == BNC_MOD_KV_DR) g.gate[2] = T(g.st[k][0]);
+            if (m.type == BNC_MOD_CAV13) { g.gate[3] = T(g.st[k][0]); g.gate[4] = T(g.st[k][1]); }
         }
     }
     std::vector<Syn> sy(K);
@@ -279,6 +311,44 @@ int bo_tangent_run(const BncBionData* net, const BncCurrentStimulus* stim, uint3
                     s.out[1] = s.out[1] + I * (double)dt / (cpv * EVR);
                     clamp_ions(s.in);
                     clamp_ions(s.out);
+                    I_total = I_total - I;
+                } else if (ty == BNC_MOD_CAV13) {   // hh_biological.cpp:142-187
+                    T V = s.V;
+                    const double Vh = s.st[j][3] != 0.0f ? -std::fabs((double)s.st[j][3]) : -35.0;
+                    const double kk = s.st[j][4] > 0.0f ? (double)s.st[j][4] : 7.0;
+                    const double gam = s.st[j][2] > 0.0f ? (double)s.st[j][2] : 25.0;
+                    T minf = T(1.0) / (T(1.0) + texp(-(V - Vh) / (kk + (double)1e-6f)));
+                    T mv = s.gate[3] + (minf - s.gate[3]) * ((double)dt / 2.0);
+                    T hinf = T(1.0) / (T(1.0) + texp((V + 52.0) / 8.0));
+                    hinf = hinf * (T(1.0) / (T(1.0) + s.in[2] * (1000.0 / 3.0)));
+                    T hv = s.gate[4] + (hinf - s.gate[4]) * ((double)dt / 100.0);
+                    mv = clampT(mv, 0.0, 1.0);
+                    hv = clampT(hv, 0.0, 1.0);
+                    s.gate[3] = mv; s.gate[4] = hv;
+                    const double P = ghk_P((double)(float)gam, 2.0, (double)0.12775f);
+                    T I = T(P) * ghk_div(V, s.in[2], s.out[2]) * (s.den[j] * s.area) * (mv * mv * hv) * 1e12;
+                    s.in[2] = s.in[2] - I * (double)dt / (2.0 * cpv);
+                    s.out[2] = s.out[2] - I * (double)dt / (2.0 * cpv * EVR);
+                    clamp_ions(s.in);
+                    clamp_ions(s.out);
+                    I_total = I_total - I;
+                } else if (ty == BNC_MOD_PUMP_NAK) {   // hh_biological.cpp:57-97
+                    T v = pump_vnorm(s.V, s.in[0], s.out[1], s.atp);
+                    const double e = (double)1.602176634e-19f;
+                    T I = v * (s.den[j] * s.area * 75.0 * e * 1e12);
+                    const double cpm = F * (double)(float)s.vol / 1000.0;
+                    T tr = I * ((double)dt / cpm);
+                    T na = floorT((s.in[0] - (double)1e-9f) / 3.0, 0.0);
+                    T ka = floorT((s.out[1] - (double)1e-9f) * (EVR / 2.0), 0.0);
+                    T mx = na.v < ka.v ? na : ka;
+                    if (tr.v > mx.v) tr = mx;
+                    s.in[0] = s.in[0] - tr * 3.0;
+                    s.out[0] = s.out[0] + tr * (3.0 / EVR);
+                    s.in[1] = s.in[1] + tr * 2.0;
+                    s.out[1] = s.out[1] - tr * (2.0 / EVR);
+                    clamp_ions(s.in);
+                    clamp_ions(s.out);
+                    s.atp = floorT(s.atp - I * ((double)dt * (double)1e-8f), 0.0);
                     I_total = I_total - I;
                 } else {   // K2P leak
                     const double gam = s.st[j][0] > 0.0f ? (double)s.st[j][0] : 100.0;
@@ -394,6 +464,21 @@ int bo_tangent_run(const BncBionData* net, const BncCurrentStimulus* stim, uint3
                 }
                 for (uint32_t i = 0; i < N; i++)
                     for (int q = 0; q < 7; q++) sg[i].out[q] += acc[(size_t)i * 7 + q];
+            }
+            // ATP (diffusion_kernel.h:284-345): from the values before the pass, on
+            // intracellular connections whose difference exceeds 1e-12
+            {
+                std::vector<T> da(N);
+                for (uint32_t e = 0; e < M; e++) {
+                    const Edge& x = ed[e];
+                    if (!x.intra) continue;
+                    T dC = sg[x.a].atp - sg[x.b].atp;
+                    if (!(dC.v > (double)1e-12f || dC.v < -(double)1e-12f)) continue;
+                    T f = dC * ((double)0.14f * x.area * (double)dt / x.dist);
+                    da[x.a] -= f / (double)(float)x.va;
+                    da[x.b] += f / (double)(float)x.vb;
+                }
+                for (uint32_t i = 0; i < N; i++) sg[i].atp += da[i];
             }
             for (uint32_t i = 0; i < N; i++)
                 for (int q = 0; q < 7; q++) {

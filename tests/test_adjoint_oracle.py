@@ -2,8 +2,9 @@
 its directional derivatives against central differences of its own loss, on the CPU.
 Also the oracle's release log, which the replay feeds on."""
 import numpy as np
+import pytest
 
-from bioneuroncore_b200 import Network, NetgenParams, NET_ADJOINT
+from bioneuroncore_b200 import Network, NetgenParams, NET_ADJOINT, NETGEN_FULL_SMALL_SET
 
 DT = 0.025
 
@@ -30,10 +31,13 @@ def test_release_log_is_sorted_and_positive():
     assert (amt > 0).all() and (tick < 400).all()
 
 
-def test_tangent_matches_its_central_differences():
+@pytest.mark.parametrize("flags", [0, NETGEN_FULL_SMALL_SET])
+def test_tangent_matches_its_central_differences(flags):
+    """With the fitting family and with the whole small set (Cav1.3, the Na/K pump and
+    the ATP it consumes, which diffuses)."""
     from oracle.oracle import Oracle, tangent_loss
     ticks = 300
-    p = NetgenParams(family=NET_ADJOINT, n_neurons=3, seed=11)
+    p = NetgenParams(family=NET_ADJOINT, n_neurons=3, seed=11, flags=flags)
     net = Network(p)
     log = Oracle(Network(p)).run_logged(ticks, DT)
     base = _densities(net)

@@ -3,20 +3,22 @@ against central finite differences, and a fit that the gradients drive.
 
 The network is the fitting family (BNC_NET_ADJOINT: Nav1.x, Kv_DR and K2P leak per
 segment, myelin on alternate axon segments, Cav2.1 on axons, AMPA/GABA-A synapses,
-a 200 pA step into 10% of somata).  All tests are marked gpu.
+a 1 nA step into 10% of somata), and for the replay and the gradients also the same
+family with the whole small set (BNC_NETGEN_FULL_SMALL_SET: Cav1.3 and the Na/K pump
+on every segment, the pump's ATP diffusing).  All tests are marked gpu.
 """
 import numpy as np
 import pytest
 
-from bioneuroncore_b200 import Adjoint, Backend, Network, NetgenParams, NET_ADJOINT
+from bioneuroncore_b200 import Adjoint, Backend, Network, NetgenParams, NET_ADJOINT, NETGEN_FULL_SMALL_SET
 
 DT = 0.025
 
 pytestmark = pytest.mark.gpu
 
 
-def _setup(n_neurons, ticks, n_sets, seed=7, checkpoint_every=64, sample_every=1):
-    p = NetgenParams(family=NET_ADJOINT, n_neurons=n_neurons, seed=seed)
+def _setup(n_neurons, ticks, n_sets, seed=7, checkpoint_every=64, sample_every=1, flags=0):
+    p = NetgenParams(family=NET_ADJOINT, n_neurons=n_neurons, seed=seed, flags=flags)
     net = Network(p)
     b = Backend()
     b.load_network(net)
@@ -35,11 +37,12 @@ def _plain_soma_trace(p, soma, ticks):
     return out
 
 
-def test_replay_forward_is_the_plain_trajectory():
+@pytest.mark.parametrize("flags", [0, NETGEN_FULL_SMALL_SET])
+def test_replay_forward_is_the_plain_trajectory(flags):
     """The forward pass, replaying the release log, reproduces the plain tick's somatic
     voltages bit for bit (same device functions, same operation order)."""
     ticks = 300
-    p, net, b, adj = _setup(6, ticks, 2)
+    p, net, b, adj = _setup(6, ticks, 2, flags=flags)
     assert adj.release_count() > 0
     _, tr = adj.forward(trace=True)
     plain = _plain_soma_trace(p, adj.soma, ticks)
@@ -51,9 +54,9 @@ def test_replay_forward_is_the_plain_trajectory():
     assert plain.max() > -40.0
 
 
-def _fit_problem(ticks, n_sets, n_neurons=4, scale=(1.1, 0.9, 1.2, 0.8)):
+def _fit_problem(ticks, n_sets, n_neurons=4, scale=(1.1, 0.9, 1.2, 0.8), flags=0):
     """Targets from a hidden parameter set: the network's densities times `scale`."""
-    p, net, b, adj = _setup(n_neurons, ticks, n_sets, checkpoint_every=64)
+    p, net, b, adj = _setup(n_neurons, ticks, n_sets, checkpoint_every=64, flags=flags)
     base = [x.astype(np.float32) for x in adj.get_params(0)]
     adj.set_params(0, *[x * s for x, s in zip(base, scale)])
     _, tr = adj.forward(trace=True)
@@ -62,7 +65,8 @@ def _fit_problem(ticks, n_sets, n_neurons=4, scale=(1.1, 0.9, 1.2, 0.8)):
     return p, net, adj, base, tr[0]
 
 
-def test_gradient_matches_fp64_forward_mode_and_central_differences():
+@pytest.mark.parametrize("flags", [0, NETGEN_FULL_SMALL_SET])
+def test_gradient_matches_fp64_forward_mode_and_central_differences(flags):
     """The device adjoint's gradient along a random direction of all parameters (gNa,
     gK, gleak per segment, weight per synapse) against (a) the FP64 CPU forward-mode
     replay of the same tick (oracle/bo_tangent.cpp) and (b) central differences of that
@@ -72,7 +76,7 @@ def test_gradient_matches_fp64_forward_mode_and_central_differences():
     rounding-limited at this h and are not the reference."""
     from oracle.oracle import Oracle, tangent_loss
     ticks = 400
-    p, net, adj, base, target = _fit_problem(ticks, 1)
+    p, net, adj, base, target = _fit_problem(ticks, 1, flags=flags)
     _, _ = adj.forward()
     g = adj.backward()
     log = Oracle(Network(p)).run_logged(ticks, DT)
