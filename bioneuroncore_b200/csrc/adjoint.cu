@@ -30,6 +30,9 @@
 //   conductances, the transposed Jacobi sweeps) -> the phi_e solve -> step 1 (local
 //   Jacobians of the channel models by dual numbers, slot order reversed).
 #define BNC_MATH_OUTLINE 1   // one copy of exp/log for the forward, the re-runs and the reverse
+#ifndef BNC_ADJ_MIN_BLOCKS
+#define BNC_ADJ_MIN_BLOCKS 4   // CTAs per SM the 64-thread backward is bounded for (5 spills: slower)
+#endif
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -134,7 +137,7 @@ struct Lay {
     unsigned long long* pmask;   // reverse pass: per segment, the phi_e sweeps that did not clamp
     float *st, *gax, *term, *vnA, *vnB;
     // reverse pass only
-    float *s2, *lam, *lphi, *lI, *mu, *lvB, *linp, *lgdg, *eca, *ecb, *edv, *ldiag, *phs, *jsm;
+    float *s2, *lam, *lphi, *lI, *mu, *lvB, *linp, *lgdg, *eca, *ecb, *edv, *ldiag, *jsm;
 };
 
 __host__ __device__ inline size_t lay_bytes(uint32_t S, uint32_t E, uint32_t Y, bool bwd, uint32_t W) {
@@ -142,7 +145,7 @@ __host__ __device__ inline size_t lay_bytes(uint32_t S, uint32_t E, uint32_t Y, 
     size_t flt = (size_t)W * S + kSynWords * Y + 2 * (size_t)E + 2 * (size_t)S;
     if (bwd) {
         dbl += S;   // pmask
-        flt += 15 * (size_t)S + W * (size_t)S + 7 * (size_t)S + (size_t)E + 102 * (size_t)S + 4;
+        flt += 15 * (size_t)S + W * (size_t)S + 7 * (size_t)S + (size_t)E + 51 * (size_t)S + 4;
     }
     return dbl * 8 + flt * 4;
 }
@@ -166,12 +169,11 @@ __device__ inline Lay make_lay(unsigned char* base, uint32_t S, uint32_t E, uint
         // the reverse tick's per-connection adjoints reuse the forward's flux buffers
         l.eca = reinterpret_cast<float*>(l.fa);
         l.ecb = reinterpret_cast<float*>(l.fb);
-        l.phs = f; f += 51 * S;
         // 16-byte aligned for the asynchronous copies
         f = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(f) + 15u) & ~(uintptr_t)15u);
         l.jsm = f; f += 51 * S;
     } else {
-        l.s2 = l.lam = l.lphi = l.lI = l.mu = l.lvB = l.linp = l.lgdg = l.eca = l.ecb = l.edv = l.ldiag = l.phs =
+        l.s2 = l.lam = l.lphi = l.lI = l.mu = l.lvB = l.linp = l.lgdg = l.eca = l.ecb = l.edv = l.ldiag =
             l.jsm = nullptr;
     }
     return l;
@@ -382,13 +384,14 @@ struct Scr {
     float* pre;       // [kItems][5][Sm]  V, gate 0, gate 1, c_in, c_out before each item
     float* istart;    // [5][8][Sm]  V, in[7]
     float* jac;       // [5][51][Sm]
+    float* phs;       // [51][Sm]    phi_e before each of its sweeps
     float* estart;    // [6][7][Sm]  out before each extra sub-step and before the bath
     float* syn;       // [Ymax][9]   in[7] before the synapse, receptor open probabilities
     float* atpf;      // [Sm]        ATP before the Fick pass
 };
 // items: the item stride of the kernels; atp: whether the ATP row is recorded
 __host__ __device__ inline size_t scr_floats(uint32_t S, uint32_t Y, uint32_t items, bool atp) {
-    return ((size_t)40 * S + (size_t)255 * S + (size_t)42 * S + (size_t)9 * Y + (size_t)items * 5 * S +
+    return ((size_t)40 * S + (size_t)255 * S + (size_t)51 * S + (size_t)42 * S + (size_t)9 * Y + (size_t)items * 5 * S +
             (atp ? S : 0u) + 4 + 3) & ~(size_t)3;
 }
 template <bool kFull>
@@ -399,6 +402,7 @@ __device__ inline Scr make_scr(const AdjDev& d) {
     float* f = base;
     s.istart = f; f += 40 * S;
     s.jac = f; f += 255 * S;
+    s.phs = f; f += 51 * S;
     s.estart = f; f += 42 * S;
     s.syn = f; f += 9 * d.Ymax;
     s.pre = f; f += (size_t)ItemStride<kFull>::v * 5 * S;
@@ -408,7 +412,7 @@ __device__ inline Scr make_scr(const AdjDev& d) {
 
 // One tick of the neuron in shared memory; each kernel has one call site, so one copy.
 // kRec records the intermediates the reverse
-// tick reads (into L.s2, L.ib3, L.pmask, L.phs and the CTA's scratch).
+// tick reads (into L.s2, L.ib3, L.pmask and the CTA's scratch).
 template <bool kFull>
 __device__ __forceinline__ void tick_fwd(const AdjDev& d, const Ctx& c, const Lay& L, const Scr& sc, uint32_t t,
                                          bool kRec) {
@@ -453,7 +457,7 @@ __device__ __forceinline__ void tick_fwd(const AdjDev& d, const Ctx& c, const La
         unsigned long long unclamped = 0ull;
         for (int it = 0; it < 50; it++) {
             if (seg) {
-                if (kRec) L.phs[it * Sm + tid] = (float)ph[tid];
+                if (kRec) sc.phs[it * Sm + tid] = (float)ph[tid];
                 double acc = 0.0;
 #pragma unroll
                 for (int k = 0; k < kMaxInc; k++) {
@@ -712,7 +716,7 @@ __device__ __forceinline__ void tick_fwd(const AdjDev& d, const Ctx& c, const La
 }
 
 // Reverse of tick t.  On entry L.st holds the state
-// after the recorded re-run, L.s2 / L.ib3 / L.ibuf / L.pmask / L.phs and the scratch the
+// after the recorded re-run, L.s2 / L.ib3 / L.ibuf / L.pmask and the scratch the
 // intermediates, and L.lam the adjoint of the state after the tick (V, ions, gates).
 // On exit L.lam holds the adjoint of the starting state; gp accumulates
 // d loss / d (gNa, gK, gleak) of this thread's segment.
@@ -1029,14 +1033,24 @@ __device__ void tick_rev(const AdjDev& d, const Ctx& c, const Lay& L, const Scr&
         float lg = 0.0f;
         const double god = edge ? L.god[tid] : 0.0;
         const float godf = (float)god;
+        // the recorded iterates into shared memory (the Jacobi staging area is free here)
+        {
+            const float4* src4 = reinterpret_cast<const float4*>(sc.phs);
+            float4* dst4 = reinterpret_cast<float4*>(L.jsm);
+            for (uint32_t q = tid; q < 50u * Sm / 4u; q += blockDim.x) __pipeline_memcpy_async(dst4 + q, src4 + q, 16);
+            __pipeline_commit();
+            __pipeline_wait_prior(0);
+        }
+        __syncthreads();
+        const float* phs = L.jsm;
         for (int k = 49; k >= 0; k--) {
-            const float* ph = L.phs + (size_t)k * Sm;
+            const float* ph = phs + (size_t)k * Sm;
             float* mu = (k & 1) ? L.lvB : L.mu;
             if (seg) {
                 float m = 0.0f;
                 if ((pm >> k) & 1ull) {
                     m = lp * rdiag;
-                    const float unc = (k == 49) ? (float)L.phiA[tid] : L.phs[(k + 1) * Sm + tid];
+                    const float unc = (k == 49) ? (float)L.phiA[tid] : phs[(k + 1) * Sm + tid];
                     ldg -= m * unc;
                 }
                 lI -= m;
@@ -1173,8 +1187,10 @@ __global__ void __launch_bounds__(kMaxSeg) k_adj_forward(AdjDev d, uint32_t t0, 
 }
 
 // Reverse pass over window w (ticks [w K, min((w + 1) K, T))).
-template <bool kFull>
-__global__ void __launch_bounds__(kMaxSeg) k_adj_backward(AdjDev d, uint32_t w) {
+// kThreads / kMinBlocks: the launch bounds (neurons of at most 64 segments run a
+// 64-thread instantiation bounded for 5 CTAs per SM).
+template <bool kFull, int kThreads, int kMinBlocks>
+__global__ void __launch_bounds__(kThreads, kMinBlocks) k_adj_backward(AdjDev d, uint32_t w) {
     extern __shared__ __align__(16) unsigned char smem[];
     const Ctx c = make_ctx(d);
     const uint32_t W = kFull ? d.W : kW3;
@@ -1652,8 +1668,10 @@ int adj_build(Adjoint* A, void* sim, const BncAdjointConfig& cfg) {
     if (A->smem_bwd > 227u * 1024u) { set_error("adjoint: a neuron needs %zu bytes of shared memory", A->smem_bwd); return BNC_ERR_UNSUPPORTED; }
     if (cudaFuncSetAttribute(k_adj_forward<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)A->smem_fwd) != cudaSuccess ||
         cudaFuncSetAttribute(k_adj_forward<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)A->smem_fwd) != cudaSuccess ||
-        cudaFuncSetAttribute(k_adj_backward<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)A->smem_bwd) != cudaSuccess ||
-        cudaFuncSetAttribute(k_adj_backward<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)A->smem_bwd) != cudaSuccess)
+        cudaFuncSetAttribute(k_adj_backward<false, kMaxSeg, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)A->smem_bwd) != cudaSuccess ||
+        cudaFuncSetAttribute(k_adj_backward<true, kMaxSeg, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)A->smem_bwd) != cudaSuccess ||
+        cudaFuncSetAttribute(k_adj_backward<false, 64, BNC_ADJ_MIN_BLOCKS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)A->smem_bwd) != cudaSuccess ||
+        cudaFuncSetAttribute(k_adj_backward<true, 64, BNC_ADJ_MIN_BLOCKS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)A->smem_bwd) != cudaSuccess)
         return adj_fail(BNC_ERR_CUDA, "shared-memory limit");
     return BNC_OK;
 }
@@ -1877,8 +1895,13 @@ int bnc_adjoint_backward(void* adj, float* g_gNa, float* g_gK, float* g_gleak, f
     cudaEventRecord(A->ev0, A->stream);
     const dim3 grid(d.nn, d.n_sets);
     for (int w = (int)d.n_ckpt - 1; w >= 0; w--)
-        if (d.full) k_adj_backward<true><<<grid, A->threads, A->smem_bwd, A->stream>>>(d, (uint32_t)w);
-        else k_adj_backward<false><<<grid, A->threads, A->smem_bwd, A->stream>>>(d, (uint32_t)w);
+        if (A->threads <= 64) {
+            if (d.full) k_adj_backward<true, 64, BNC_ADJ_MIN_BLOCKS><<<grid, A->threads, A->smem_bwd, A->stream>>>(d, (uint32_t)w);
+            else k_adj_backward<false, 64, BNC_ADJ_MIN_BLOCKS><<<grid, A->threads, A->smem_bwd, A->stream>>>(d, (uint32_t)w);
+        } else {
+            if (d.full) k_adj_backward<true, kMaxSeg, 1><<<grid, A->threads, A->smem_bwd, A->stream>>>(d, (uint32_t)w);
+            else k_adj_backward<false, kMaxSeg, 1><<<grid, A->threads, A->smem_bwd, A->stream>>>(d, (uint32_t)w);
+        }
     cudaEventRecord(A->ev1, A->stream);
     cudaError_t e = cudaStreamSynchronize(A->stream);
     if (e == cudaSuccess) e = cudaGetLastError();
