@@ -978,8 +978,33 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
     {
         std::vector<uint32_t> post_list, rest_list;
         for (uint32_t d = 0; d < n; d++) (post_off[d + 1] > post_off[d] ? post_list : rest_list).push_back(d);
+        // Segments of equal count are ordered by the class sequence of their synapses
+        // (bit k: the k-th synapse, in original order, carries an inhibitory receptor),
+        // so the lanes of a warp take the same receptor path at each k.  Only which
+        // thread runs a segment changes; each thread still walks its segment's synapses
+        // in original order.
+        std::vector<uint32_t> sig(n, 0);
+        parallel_for(post_list.size(), [&](size_t a0, size_t a1) {
+            for (size_t a = a0; a < a1; a++) {
+                const uint32_t d = post_list[a];
+                uint32_t m = 0;
+                for (uint32_t q = post_off[d], k = 0; q < post_off[d + 1] && k < 32; q++, k++) {
+                    const uint32_t sk = syn_valid[q];
+                    const SynLite& y = hn.syn[sk];
+                    bool inh = false;
+                    for (uint8_t j = 0; j < y.post_receptor_count; j++) {
+                        const uint8_t rt = hn.post_rec(sk, j).type;
+                        if (rt == 11 || rt == 17 || rt == 12) { inh = true; break; }
+                    }
+                    if (inh) m |= 1u << k;
+                }
+                sig[d] = m;
+            }
+        });
         std::stable_sort(post_list.begin(), post_list.end(), [&](uint32_t a, uint32_t b) {
-            return post_off[a + 1] - post_off[a] > post_off[b + 1] - post_off[b];
+            const uint32_t ca = post_off[a + 1] - post_off[a], cb = post_off[b + 1] - post_off[b];
+            if (ca != cb) return ca > cb;
+            return sig[a] < sig[b];
         });
         for (uint32_t d : post_list) {
             const uint32_t c = post_off[d + 1] - post_off[d];
