@@ -286,6 +286,15 @@ class Backend:
             _check(self.lib.bnc_load_generated_opts(self.h, C.byref(params), C.byref(options)),
                    "bnc_load_generated_opts")
 
+    def upload_stimuli(self, data):
+        """gpu_backend_upload_stimuli with a GpuStimulusData (abi.stimulus_data): replaces
+        every stimulus list; ion and ligand injections apply once, at the next tick.  The
+        reference call returns nothing, so a rejected upload shows as bnc_last_error()."""
+        self.lib.gpu_backend_upload_stimuli(self.h, C.byref(data))
+        err = last_error()
+        if err:
+            raise BackendError("gpu_backend_upload_stimuli: " + err)
+
     def run_ticks(self, n, dt):
         _check(self.lib.bnc_run_ticks(self.h, n, C.c_float(dt)), "bnc_run_ticks")
 

@@ -56,6 +56,76 @@ STIM_DTYPE = np.dtype({
 })
 
 
+MAX_STIMULI = 256   # BNC_GPU_MAX_STIMULI
+
+
+class CurrentStimulus(C.Structure):
+    _pack_ = 1
+    _fields_ = [("segment_id", C.c_uint32), ("amplitude_pA", C.c_float), ("duration_ms", C.c_float),
+                ("start_tick", C.c_uint64)]
+
+
+class VoltageClamp(C.Structure):
+    _pack_ = 1
+    _fields_ = [("segment_id", C.c_uint32), ("target_mV", C.c_float), ("start_tick", C.c_uint64),
+                ("end_tick", C.c_uint64)]
+
+
+class RampStimulus(C.Structure):
+    _pack_ = 1
+    _fields_ = [("segment_id", C.c_uint32), ("start_pA", C.c_float), ("end_pA", C.c_float),
+                ("start_tick", C.c_uint64), ("end_tick", C.c_uint64)]
+
+
+class IonInjection(C.Structure):
+    _pack_ = 1
+    _fields_ = [("segment_id", C.c_uint32), ("ion_idx", C.c_int32), ("amount_mM", C.c_float),
+                ("extracellular", C.c_uint8), ("_pad", C.c_uint8 * 3)]
+
+
+class LigandInjection(C.Structure):
+    _pack_ = 1
+    _fields_ = [("segment_id", C.c_uint32), ("nt_idx", C.c_int32), ("amount", C.c_float),
+                ("intracellular", C.c_uint8), ("_pad2", C.c_uint8 * 3)]
+
+
+class GpuStimulusData(C.Structure):
+    """BncGpuStimulusData, the argument of gpu_backend_upload_stimuli (reference
+    include/types.h:662-674): up to 256 entries of each stimulus kind."""
+    _pack_ = 1
+    _fields_ = [("current_stim_count", C.c_uint32), ("vclamp_count", C.c_uint32), ("ramp_count", C.c_uint32),
+                ("ion_inj_count", C.c_uint32), ("lig_inj_count", C.c_uint32), ("current_tick", C.c_uint64),
+                ("current_stim", CurrentStimulus * MAX_STIMULI), ("vclamps", VoltageClamp * MAX_STIMULI),
+                ("ramps", RampStimulus * MAX_STIMULI), ("ion_inj", IonInjection * MAX_STIMULI),
+                ("lig_inj", LigandInjection * MAX_STIMULI)]
+
+
+def stimulus_data(current=(), vclamps=(), ramps=(), ion_inj=(), lig_inj=()):
+    """A GpuStimulusData from tuples in field order: current (segment_id, amplitude_pA,
+    duration_ms, start_tick), vclamps (segment_id, target_mV, start_tick, end_tick), ramps
+    (segment_id, start_pA, end_pA, start_tick, end_tick), ion_inj (segment_id, ion_idx,
+    amount_mM, extracellular), lig_inj (segment_id, nt_idx, amount, intracellular)."""
+    d = GpuStimulusData()
+    for name, cnt, rows, cls in (("current_stim", "current_stim_count", current, CurrentStimulus),
+                                 ("vclamps", "vclamp_count", vclamps, VoltageClamp),
+                                 ("ramps", "ramp_count", ramps, RampStimulus),
+                                 ("ion_inj", "ion_inj_count", ion_inj, IonInjection),
+                                 ("lig_inj", "lig_inj_count", lig_inj, LigandInjection)):
+        rows = list(rows)
+        if len(rows) > MAX_STIMULI:
+            raise ValueError("at most %d entries of each stimulus kind" % MAX_STIMULI)
+        arr = getattr(d, name)
+        for k, r in enumerate(rows):
+            arr[k] = cls(*r)
+        setattr(d, cnt, len(rows))
+    return d
+
+
+assert C.sizeof(CurrentStimulus) == 20 and C.sizeof(VoltageClamp) == 24 and C.sizeof(RampStimulus) == 28
+assert C.sizeof(IonInjection) == 16 and C.sizeof(LigandInjection) == 16
+assert C.sizeof(GpuStimulusData) == 28 + MAX_STIMULI * (20 + 24 + 28 + 16 + 16)
+
+
 class BionData(C.Structure):
     """Reference BionData (include/bion_loader.h:16-28); not packed."""
     _fields_ = [

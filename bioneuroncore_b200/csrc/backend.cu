@@ -368,6 +368,13 @@ static int copy_aos(const BncBionData* src, BncBionData* dst) {
     return BNC_OK;
 }
 
+// Pending injections are consumed by the first tick enqueued after their upload (the
+// kernel zeroes the device count); later ticks need not launch k_inject.
+static void injections_enqueued(Backend* b) {
+    b->dev.inj = nullptr;
+    b->dev.inj_n = nullptr;
+}
+
 static int run_ticks(Backend* b, uint32_t n, float dt) {
     if (!b->loaded) { set_error("no network loaded"); return BNC_ERR_STATE; }
     if (b->failed) { set_error("backend is in a failed state after a device error"); return BNC_ERR_STATE; }
@@ -377,6 +384,7 @@ static int run_ticks(Backend* b, uint32_t n, float dt) {
         if (e != cudaSuccess) { b->failed = true; return cuda_fail(e, "tick launch"); }
         b->tick += b->tick_stride;
         b->ticks_run++;
+        injections_enqueued(b);
     }
     return BNC_OK;
 }
@@ -419,6 +427,11 @@ static int run_ticks_graph(Backend* b, uint32_t n, float dt) {
     if (!b->loaded) { set_error("no network loaded"); return BNC_ERR_STATE; }
     if (b->failed) { set_error("backend is in a failed state after a device error"); return BNC_ERR_STATE; }
     if (b->tick_stride != 1) return run_ticks(b, n, dt);   // the captured clock steps by one
+    if (b->dev.inj && n > 0) {   // the tick that applies pending injections runs uncaptured
+        int rc = run_ticks(b, 1, dt);
+        if (rc != BNC_OK) return rc;
+        n--;
+    }
     cudaSetDevice(b->device);
     const uint32_t reps = n / kGraphTicks;
     if (reps > 0) {
@@ -667,17 +680,25 @@ void* gpu_backend_bion_data(void* sim) {
 void gpu_backend_upload_stimuli(void* sim, const BncGpuStimulusData* src) {
     if (!sim || !src) return;
     Backend* b = static_cast<Backend*>(sim);
+    set_error("%s", "");   // the call returns nothing: an empty error string means success
     if (!b->loaded) { set_error("no network loaded"); return; }
-    if (src->ramp_count || src->ion_inj_count || src->lig_inj_count) {
-        set_error("ramp stimuli and ion/ligand injections have no device implementation in this backend");
-        return;
-    }
-    b->stim.current.assign(src->current_stim, src->current_stim + std::min<uint32_t>(src->current_stim_count, BNC_GPU_MAX_STIMULI));
-    b->stim.vclamp.assign(src->vclamps, src->vclamps + std::min<uint32_t>(src->vclamp_count, BNC_GPU_MAX_STIMULI));
+    auto take = [](auto& dst, const auto* arr, uint32_t cnt) {
+        dst.assign(arr, arr + std::min<uint32_t>(cnt, BNC_GPU_MAX_STIMULI));
+    };
+    take(b->stim.current, src->current_stim, src->current_stim_count);
+    take(b->stim.vclamp, src->vclamps, src->vclamp_count);
+    take(b->stim.ramp, src->ramps, src->ramp_count);
+    take(b->stim.ion_inj, src->ion_inj, src->ion_inj_count);
+    take(b->stim.lig_inj, src->lig_inj, src->lig_inj_count);
     cudaSetDevice(b->device);
     cudaStreamSynchronize(b->stream);
+    b->drop_graph();   // a captured tick holds the stimulus arrays freed below
     b->stim_allocs.release();
-    upload_stimuli(b->stim, b->host, &b->dev, &b->stim_allocs);
+    if (upload_stimuli(b->stim, b->host, &b->dev, &b->stim_allocs) != BNC_OK)
+        set_error("device allocation of the stimulus arrays failed");
+    // injections are one-shot: a later rebuild from these lists must not repeat them
+    b->stim.ion_inj.clear();
+    b->stim.lig_inj.clear();
 }
 
 int gpu_backend_device_count(void) {
@@ -1036,6 +1057,7 @@ int bnc_profile_ticks(void* sim, uint32_t n_ticks, float dt, float* ms_modifiers
         cudaEventRecord(e[3], b->stream);
         b->tick++;
         b->ticks_run++;
+        injections_enqueued(b);
         rc = sync_stream(b);
         if (rc != BNC_OK) break;
         float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f;
@@ -1501,6 +1523,9 @@ extern "C" int bnc_run_ticks_static_scratch(void* sim, uint32_t n_ticks, float d
         if (e != cudaSuccess) { b->failed = true; return cuda_fail(e, "tick launch"); }
         b->tick++;
         b->ticks_run++;
+        injections_enqueued(b);
+        d.inj = nullptr;
+        d.inj_n = nullptr;
     }
     return sync_stream(b);
 }

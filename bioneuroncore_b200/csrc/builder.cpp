@@ -219,6 +219,62 @@ int upload_stimuli(const Stimuli& stim, NetHost& host, NetDev* dev, DeviceAllocs
             dev->vc_off = nullptr;
         }
     }
+    {
+        std::vector<uint32_t> cnt(n + 1, 0);
+        for (const auto& s : stim.ramp) if (s.segment_id < n) cnt[host.inv[s.segment_id] + 1]++;
+        for (uint32_t i = 0; i < n; i++) cnt[i + 1] += cnt[i];
+        std::vector<float> from(cnt[n]), to(cnt[n]);
+        std::vector<unsigned long long> st(cnt[n]), en(cnt[n]);
+        std::vector<uint32_t> pos(cnt.begin(), cnt.end() - 1);
+        for (const auto& s : stim.ramp) {
+            if (s.segment_id >= n) continue;
+            uint32_t k = pos[host.inv[s.segment_id]]++;
+            from[k] = s.start_pA; to[k] = s.end_pA; st[k] = s.start_tick; en[k] = s.end_tick;
+        }
+        if (cnt[n]) {
+            dev->rp_off = up(allocs, cnt, &rc);
+            dev->rp_from = up(allocs, from, &rc);
+            dev->rp_to = up(allocs, to, &rc);
+            dev->rp_start = up(allocs, st, &rc);
+            dev->rp_end = up(allocs, en, &rc);
+        } else {
+            dev->rp_off = nullptr;
+        }
+    }
+    {
+        // Injections (simulation_host.cpp:279-300) land after the segment's step-1
+        // currents and before step 2.5, per segment in upload order: ions first, then
+        // ligands, which touch other arrays.  With synapses, step 3 zeroes every
+        // extracellular neurotransmitter entry before it accumulates (:326-330) and
+        // nothing reads the entry in between but step 2.5's own diffusion of it, so an
+        // extracellular ligand injection leaves no trace and is dropped here.
+        std::vector<uint4> ops;
+        bool intra_nt = false;
+        for (const auto& j : stim.ion_inj) {
+            if (j.segment_id >= n || j.ion_idx < 0 || j.ion_idx >= 7) continue;
+            uint32_t a;
+            std::memcpy(&a, &j.amount_mM, 4);
+            ops.push_back(make_uint4(host.inv[j.segment_id], (uint32_t)j.ion_idx + (j.extracellular ? 8u : 0u), a, 0u));
+        }
+        for (const auto& j : stim.lig_inj) {
+            if (j.segment_id >= n || j.nt_idx < 0 || j.nt_idx >= 15) continue;
+            if (!j.intracellular && (dev->flags & NF_SYNAPSES)) continue;
+            uint32_t a;
+            std::memcpy(&a, &j.amount, 4);
+            ops.push_back(make_uint4(host.inv[j.segment_id], (uint32_t)j.nt_idx + (j.intracellular ? 16u : 32u), a, 0u));
+            if (j.intracellular) intra_nt = true;
+        }
+        // An injected intracellular transmitter is a gradient that step 2.5 diffuses.
+        if (intra_nt && (dev->flags & NF_DIFFUSION)) dev->flags |= NF_INTRA_NT;
+        if (!ops.empty()) {
+            std::vector<uint32_t> count(1, (uint32_t)ops.size());
+            dev->inj = up(allocs, ops, &rc);
+            dev->inj_n = up(allocs, count, &rc);
+        } else {
+            dev->inj = nullptr;
+            dev->inj_n = nullptr;
+        }
+    }
     return rc;
 }
 

@@ -362,6 +362,18 @@ k_diffusion(NetDev d, float dt, unsigned long long tick, uint32_t S, uint32_t E)
                 if (tick >= st0 && tick < st0 + dur) I += d.cs_amp[k];
             }
         }
+        // ramps (simulation_host.cpp:261-276): the amplitude interpolated in FP32
+        if (d.rp_off) {
+            for (uint32_t k = d.rp_off[g]; k < d.rp_off[g + 1]; k++) {
+                const unsigned long long st0 = d.rp_start[k], en = d.rp_end[k];
+                if (tick >= st0 && tick < en) {
+                    const float frac = en > st0 ? (float)(tick - st0) / (float)(en - st0) : 1.0f;
+                    const float a = d.rp_from[k];
+                    const float amp = a + (d.rp_to[k] - a) * frac;
+                    I += amp;
+                }
+            }
+        }
         t.itot[i] = I;
         d.ibuf[g] = I;
         t.incoff[i] = (uint16_t)(d.inc_off[g] - inc0);
@@ -977,8 +989,38 @@ cudaError_t prepare_diffusion(const NetHost& host, cudaStream_t stream) {
     return cudaSuccess;
 }
 
+// One-shot ion and ligand injections (simulation_host.cpp:279-300), applied after the
+// modifier phases wrote the step-1 records and before step 2.5 reads them (ghost
+// copies included).  One thread walks the list in upload order, so repeated
+// injections into one segment add in the reference's order.
+__global__ void k_inject(NetDev d) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const uint32_t n = *d.inj_n;
+    const size_t N = d.n_seg;
+    for (uint32_t j = 0; j < n; j++) {
+        const uint4 op = d.inj[j];
+        const uint32_t g = op.x, what = op.y;
+        const float amt = __uint_as_float(op.z);
+        if (g >= N) continue;
+        if (what < 16u) {
+            float* ion = what < 8u ? &d.rec[g].in[what] : &d.rec[g].out[what - 8u];
+            *ion = (float)((double)*ion + (double)amt);
+        } else if (what < 31u) {
+            d.intra_nt[(size_t)(what - 16u) * N + g] += amt;
+        } else if (what >= 32u && what < 47u) {
+            d.nt[(size_t)(what - 32u) * N + g] += amt;
+        }
+    }
+    *d.inj_n = 0u;
+}
+
 cudaError_t enqueue_diffusion(const NetDev& dev, const NetHost& host, float dt, unsigned long long tick,
                               cudaStream_t stream) {
+    if (dev.inj) {
+        k_inject<<<1, 32, 0, stream>>>(dev);
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
     const uint32_t S = host.max_tile_stride, E = host.max_tile_edges;
     const size_t smem = diffusion_smem_bytes(S, E);
     const uint32_t threads = diffusion_threads(host.max_tile_segs);

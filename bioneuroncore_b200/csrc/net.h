@@ -113,6 +113,17 @@ struct NetDev {
     float* vc_target;
     unsigned long long* vc_start;
     unsigned long long* vc_end;
+    // ramp stimuli, per-segment CSR in upload order (simulation_host.cpp:261-276)
+    uint32_t* rp_off;         // (nullptr when none)
+    float* rp_from;           // start_pA
+    float* rp_to;             // end_pA
+    unsigned long long* rp_start;
+    unsigned long long* rp_end;
+    // one-shot ion and ligand injections in upload order: (device segment, what, amount
+    // bits, 0); what = ion (0-6) | 8 extracellular ion, 16 + nt intra_nt, 32 + nt
+    // neurotransmitter.  k_inject applies *inj_n of them and sets *inj_n to 0.
+    uint4* inj;               // (nullptr when none is pending)
+    uint32_t* inj_n;
     // synapse-kernel threads: segments with synapses by count descending, then the rest
     uint32_t* th_seg;         // [n_seg] device segment of thread t
     uint16_t* th_cnt;         // [n_seg] its synapse count
@@ -232,6 +243,9 @@ struct NetHost {
 struct Stimuli {
     std::vector<BncCurrentStimulus> current;
     std::vector<BncVoltageClamp> vclamp;
+    std::vector<BncRampStimulus> ramp;
+    std::vector<BncIonInjection> ion_inj;       // one-shot: cleared once uploaded to the device
+    std::vector<BncLigandInjection> lig_inj;
 };
 
 // Builds host-side SoA from AoS and uploads it.  Returns 0 or BNC_ERR_*; on error

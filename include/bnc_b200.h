@@ -75,7 +75,12 @@ void gpu_backend_run_tick(void* sim, float dt);
 /* Replaces gpu_backend_bion_data (gpu_backend_cuda.cu:343-346): host AoS view
  * (BncBionData*, layout of reference include/bion_loader.h:16-28). */
 void* gpu_backend_bion_data(void* sim);
-/* Replaces gpu_backend_upload_stimuli (gpu_backend_cuda.cu:348-351). */
+/* Replaces gpu_backend_upload_stimuli (gpu_backend_cuda.cu:348-351).  Every list of
+ * `src` replaces the previous one (at most 256 entries each; `current_tick` is ignored,
+ * the tick counter is internal).  Current steps, clamps and ramps follow the CPU tick
+ * (simulation_host.cpp:189-276, 633-643); ion and ligand injections apply once, at the
+ * next tick, after the segment's modifier currents (:279-306).  Returns nothing, as the
+ * reference's does: bnc_last_error() is empty after a successful upload. */
 void gpu_backend_upload_stimuli(void* sim, const BncGpuStimulusData* src);
 /* Replaces gpu_backend_device_count (gpu_backend_cuda.cu:353-357). */
 int gpu_backend_device_count(void);

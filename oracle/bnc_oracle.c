@@ -13,7 +13,9 @@
  *
  * Supported subset (the loader rejects the rest with an error): modifier types
  * listed in bo_type_supported(), chemical synapses, pre-autoreceptors that are
- * bouton K/Na channels, no mechano stimuli, no consolidation/nuclei.
+ * bouton K/Na channels, every stimulus kind of GpuStimulusData (current steps,
+ * clamps, ramps, ion and ligand injections; bo_upload_stimuli), no mechano
+ * stimuli, no consolidation/nuclei.
  */
 #include <math.h>
 #include <stdint.h>
@@ -52,6 +54,16 @@ typedef struct BoSim {
     uint64_t tick;
     BncCurrentStimulus* stim;
     uint32_t n_stim;
+    /* the other stimulus kinds of GpuStimulusData (types.h:608-674), set by
+       bo_upload_stimuli; injections are one-shot (simulation_host.cpp:304-306) */
+    BncVoltageClamp vc[BNC_GPU_MAX_STIMULI];
+    uint32_t n_vc;
+    BncRampStimulus ramp[BNC_GPU_MAX_STIMULI];
+    uint32_t n_ramp;
+    BncIonInjection ion_inj[BNC_GPU_MAX_STIMULI];
+    uint32_t n_ion_inj;
+    BncLigandInjection lig_inj[BNC_GPU_MAX_STIMULI];
+    uint32_t n_lig_inj;
     uint32_t* spike_count;  /* per segment, threshold -40 mV upward crossings */
     float nt_D[15];
     char err[256];
@@ -621,6 +633,14 @@ static void bo_tick(BoSim* S, float dt) {
             if (!(tick >= st.start_tick + (uint64_t)(st.duration_ms / dt))) S->stim[w++] = st;
         }
         S->n_stim = w;
+        w = 0;
+        for (uint32_t r = 0; r < S->n_vc; r++)
+            if (!(tick >= S->vc[r].end_tick)) S->vc[w++] = S->vc[r];
+        S->n_vc = w;
+        w = 0;
+        for (uint32_t r = 0; r < S->n_ramp; r++)
+            if (!(tick >= S->ramp[r].end_tick)) S->ramp[w++] = S->ramp[r];
+        S->n_ramp = w;
     }
     /* step 1 (:234-303) */
     for (uint32_t i = 0; i < n; i++) {
@@ -641,8 +661,36 @@ static void bo_tick(BoSim* S, float dt) {
                     I_total += st->amplitude_pA;
             }
         }
+        /* ramps (:261-276): amplitude interpolated in FP32 */
+        for (uint32_t r = 0; r < S->n_ramp; r++) {
+            const BncRampStimulus* rs = &S->ramp[r];
+            if (rs->segment_id != s->id) continue;
+            if (tick >= rs->start_tick && tick < rs->end_tick) {
+                float frac = (rs->end_tick > rs->start_tick)
+                    ? (float)(tick - rs->start_tick) / (float)(rs->end_tick - rs->start_tick)
+                    : 1.0f;
+                float amp = rs->start_pA + (rs->end_pA - rs->start_pA) * frac;
+                I_total += amp;
+            }
+        }
+        /* ion injections (:279-287), in upload order */
+        for (uint32_t r = 0; r < S->n_ion_inj; r++) {
+            const BncIonInjection* ij = &S->ion_inj[r];
+            if (ij->segment_id != s->id || ij->ion_idx < 0 || ij->ion_idx >= 7) continue;
+            float* ions = ij->extracellular ? s->out : s->in;
+            ions[ij->ion_idx] = (float)((double)ions[ij->ion_idx] + (double)ij->amount_mM);
+        }
+        /* ligand injections (:289-300) */
+        for (uint32_t r = 0; r < S->n_lig_inj; r++) {
+            const BncLigandInjection* lj = &S->lig_inj[r];
+            if (lj->segment_id != s->id || lj->nt_idx < 0 || lj->nt_idx >= 15) continue;
+            if (lj->intracellular) s->intra_nt[lj->nt_idx] += lj->amount;
+            else s->nt[lj->nt_idx] += lj->amount;
+        }
         s->ibuf = I_total;
     }
+    S->n_ion_inj = 0;   /* one-shot (:304-306) */
+    S->n_lig_inj = 0;
     /* step 2.5 */
     bo_diffusion(S, dt);
     /* step 3 (:322-593) */
@@ -778,6 +826,11 @@ static void bo_tick(BoSim* S, float dt) {
         s->V = (float)((double)s->V + dV);
         if (S->spike_count && prev_V <= -40.0f && s->V > -40.0f) S->spike_count[i]++;
         s->ibuf = 0.0f;
+        /* voltage clamps (:633-643): the last active clamp of the segment wins */
+        for (uint32_t v = 0; v < S->n_vc; v++) {
+            const BncVoltageClamp* vc = &S->vc[v];
+            if (vc->segment_id == s->id && tick >= vc->start_tick && tick < vc->end_tick) s->V = vc->target_mV;
+        }
         if (s->V != s->V) { s->V = -65.0f; }
         else {
             if (s->V < -120.0f) s->V = -120.0f;
@@ -868,6 +921,24 @@ BoSim* bo_create(const BncBionData* d, const BncCurrentStimulus* stim, uint32_t 
     }
     scratch_reserve(S->n, S->m);
     return S;
+}
+
+/* gpu_backend_upload_stimuli (gpu_backend_cuda.cu:242-248): every list is replaced by
+   the uploaded one; the injections apply at the next tick, once. */
+void bo_upload_stimuli(BoSim* S, const BncGpuStimulusData* src) {
+    uint32_t nc = src->current_stim_count < BNC_GPU_MAX_STIMULI ? src->current_stim_count : BNC_GPU_MAX_STIMULI;
+    free(S->stim);
+    S->stim = calloc(nc ? nc : 1, sizeof(BncCurrentStimulus));
+    if (nc) memcpy(S->stim, src->current_stim, nc * sizeof(BncCurrentStimulus));
+    S->n_stim = nc;
+#define BO_TAKE(dst, n, srcarr, cnt) do { \
+        n = (cnt) < BNC_GPU_MAX_STIMULI ? (cnt) : BNC_GPU_MAX_STIMULI; \
+        memcpy(dst, srcarr, (size_t)(n) * sizeof(dst[0])); } while (0)
+    BO_TAKE(S->vc, S->n_vc, src->vclamps, src->vclamp_count);
+    BO_TAKE(S->ramp, S->n_ramp, src->ramps, src->ramp_count);
+    BO_TAKE(S->ion_inj, S->n_ion_inj, src->ion_inj, src->ion_inj_count);
+    BO_TAKE(S->lig_inj, S->n_lig_inj, src->lig_inj, src->lig_inj_count);
+#undef BO_TAKE
 }
 
 void bo_destroy(BoSim* S) {

@@ -30,6 +30,7 @@ def oracle_lib():
         lib.bo_create.argtypes = [vp, vp, C.c_uint32, C.c_char_p, C.c_int]
         lib.bo_create.restype = vp
         lib.bo_destroy.argtypes = [vp]
+        lib.bo_upload_stimuli.argtypes = [vp, vp]
         lib.bo_run.argtypes = [vp, C.c_uint32, C.c_float]
         lib.bo_set_diffusion_mode.argtypes = [vp, C.c_uint32, C.c_double, C.c_uint32]
         lib.bo_diffusion_stats.argtypes = [vp, vp, vp, C.c_int]
@@ -109,6 +110,10 @@ class Oracle:
         oracle_lib().bo_diffusion_stats(self.h, st.ctypes.data, led.ctypes.data, 1 if reset else 0)
         return st, led
 
+    def upload_stimuli(self, data):
+        """bo_upload_stimuli with a GpuStimulusData: every list replaced, injections once."""
+        oracle_lib().bo_upload_stimuli(self.h, C.byref(data))
+
     def run(self, ticks, dt, tick_stride=1):
         if tick_stride == 1:
             oracle_lib().bo_run(self.h, ticks, C.c_float(dt))
@@ -173,13 +178,29 @@ class Reference:
         self.lib = reference_lib()
         self.tick = C.c_uint64(0)
         self.n_stim = C.c_uint32(net.n_stim)
+        self.stim_ptr = net.stim_ptr
+        self.rest = [None] * 10   # vclamps, ramps, ion and ligand injections, mechano: array, count
+
+    def upload_stimuli(self, data):
+        """Hands the lists of a GpuStimulusData to core_run_tick's own stimulus arguments
+        (simulation_host.cpp:660-669), which it expires and clears in place."""
+        self._data = data
+        self.stim_ptr = C.addressof(data.current_stim)
+        self.n_stim = C.c_uint32(data.current_stim_count)
+        self._counts = [C.c_uint32(data.vclamp_count), C.c_uint32(data.ramp_count),
+                        C.c_uint32(data.ion_inj_count), C.c_uint32(data.lig_inj_count)]
+        arrs = [data.vclamps, data.ramps, data.ion_inj, data.lig_inj]
+        self.rest = []
+        for a, c in zip(arrs, self._counts):
+            self.rest += [C.addressof(a), C.cast(C.pointer(c), C.c_void_p)]
+        self.rest += [None, None]
 
     def run(self, ticks, dt, tick_stride=1):
         d = self.net.data
         for _ in range(ticks):
             self.lib.core_run_tick(d.segments, d.num_segments, d.connections, d.num_connections, d.synapses,
-                                   d.num_synapses, 0, C.byref(self.tick), C.c_float(dt), self.net.stim_ptr,
-                                   C.byref(self.n_stim), *([None] * 10))
+                                   d.num_synapses, 0, C.byref(self.tick), C.c_float(dt), self.stim_ptr,
+                                   C.byref(self.n_stim), *self.rest)
             self.tick.value += tick_stride - 1   # the batch mode's second increment
 
     def trace(self, ticks, dt, rec):

@@ -6,7 +6,7 @@ seeded networks from the project's generator; the resulting state is stored as
 .npz so that tests can pin the oracle (and the GPU path) to the reference on
 machines where the reference sources are absent.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [case ...]
 """
 import os
 import sys
@@ -25,6 +25,8 @@ CASES = {
     "large_n4_s3": (dict(family=2, n_neurons=4, n_synapses=80, seed=3), 100),
     # RRP, presynaptic autoreceptors and transmission delays (BNC_NETGEN_SYNAPSE_EXTRAS)
     "extras_n8_s7": (dict(family=1, n_neurons=8, seed=7, flags=32), 200),
+    # every stimulus kind of gpu_backend_upload_stimuli, two uploads (golden_cases.stimulus_schedule)
+    "stimuli_n8_s7": (dict(family=1, n_neurons=8, seed=7), 200),
 }
 
 
@@ -33,8 +35,10 @@ def params(spec):
     return NetgenParams(**spec)
 
 
-def run_reference(spec, ticks):
+def run_reference(spec, ticks, name=""):
     import ctypes as C
+    sys.path.insert(0, os.path.dirname(HERE))
+    import golden_cases
     from bioneuroncore_b200 import Network
     from oracle.oracle import Reference, reference_lib
     net = Network(params(spec))
@@ -43,10 +47,7 @@ def run_reference(spec, ticks):
     spikes = np.zeros(net.data.num_segments, np.uint32)
     lib.core_enable_spike_count(spikes.ctypes.data, net.data.num_segments)
     somata = np.flatnonzero(net.segments["segment_type"] == 1).astype(np.uint32)
-    trace = np.empty((ticks, somata.size), np.float64)
-    for t in range(ticks):
-        ref.run(1, DT)
-        trace[t] = net.segments["V_m"][somata]
+    trace = golden_cases.run_scheduled(ref, name, net, ticks, DT, somata, lambda: net.segments["V_m"])
     lib.core_disable_spike_tracking()
     seg = net.segments
     syn = net.synapses
@@ -57,6 +58,8 @@ def run_reference(spec, ticks):
         syn_weight=syn["weight"].astype(np.float64), syn_spine_Ca=syn["spine_Ca"].astype(np.float64),
         syn_bouton_Ca=syn["bouton_Ca"].astype(np.float64), syn_RRP=syn["RRP"].astype(np.float64),
     )
+    if golden_cases.stimulus_schedule(name, net):
+        out["intra_nt"] = seg["intra_nt"].astype(np.float64)
     out.update({"param_" + k: np.int64(v) for k, v in spec.items()})
     return out
 
@@ -65,8 +68,11 @@ def main():
     from oracle.oracle import reference_available
     if not reference_available():
         raise SystemExit("oracle/_ref/libbiocore_ref.so is not built (make -C oracle)")
+    only = set(sys.argv[1:])   # case names; all cases when none is given
     for name, (spec, ticks) in CASES.items():
-        np.savez_compressed(os.path.join(HERE, name + ".npz"), **run_reference(spec, ticks))
+        if only and name not in only:
+            continue
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), **run_reference(spec, ticks, name))
         print("wrote", name)
 
 

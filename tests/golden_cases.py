@@ -39,8 +39,56 @@ def compare(g, trace, seg_field, syn_field):
     errs["syn_bouton_Ca"] = _rel(syn_field("bouton_Ca"), g["syn_bouton_Ca"], 1e-9)
     if "syn_RRP" in g.files:
         errs["syn_RRP"] = _rel(syn_field("RRP"), g["syn_RRP"], 1e-6)
+    if "intra_nt" in g.files:
+        for q in range(15):
+            errs["intra_nt[%d]" % q] = _rel(seg_field("intra_nt", q), g["intra_nt"][:, q], 1e-6)
     bad = {k: v for k, v in errs.items() if not v <= REL_TOL}
     assert not bad, "relative error above %g: %r" % (REL_TOL, bad)
     spikes = np.asarray(seg_field("spikes", 0)).astype(np.int64)
     assert np.array_equal(spikes, g["spikes"].astype(np.int64)), "spike counts differ from the reference"
     return errs
+
+
+def stimulus_schedule(name, net):
+    """The uploads (gpu_backend_upload_stimuli / core_run_tick's stimulus arguments) a
+    fixture case makes: a list of (tick, GpuStimulusData), each uploaded before that
+    tick runs.  Empty for cases without one.  The "stimuli" case keeps the generator's
+    current steps and adds ramps (rising, falling, empty), voltage clamps, ion
+    injections (repeated into one ion, extracellular, out-of-range index and segment)
+    and ligand injections (intracellular, which then diffuses, and extracellular)."""
+    if not name.startswith("stimuli"):
+        return []
+    from bioneuroncore_b200.abi import stimulus_data
+    cur = [tuple(int(r[f]) if f in ("segment_id", "start_tick") else float(r[f])
+                 for f in ("segment_id", "amplitude_pA", "duration_ms", "start_tick")) for r in net.stimuli]
+    soma = [int(i) for i in np.flatnonzero(net.segments["segment_type"] == 1)]
+    n = int(net.data.num_segments)
+    first = stimulus_data(
+        current=cur,
+        ramps=[(soma[0], 0.0, 300.0, 10, 150), (soma[1], 200.0, -100.0, 50, 120), (soma[2], 50.0, 80.0, 30, 30),
+               (soma[0], 25.0, 25.0, 100, 180)],
+        vclamps=[(soma[3], -30.0, 60, 90), (soma[3] + 1, -80.0, 20, 200), (soma[3], -20.0, 80, 85)],
+        ion_inj=[(soma[4], 0, 2.0, 0), (soma[4], 0, 0.5, 0), (soma[5] + 2, 1, 1.5, 1), (soma[5], 9, 1.0, 0),
+                 (n + 5, 0, 1.0, 0), (soma[6], 2, 1e-4, 0)],
+        lig_inj=[(soma[1] + 3, 0, 0.5, 1), (soma[2], 1, 0.2, 0), (soma[2] + 1, 7, 0.3, 1)])
+    second = stimulus_data(
+        current=cur,
+        ramps=[(soma[1], -50.0, 150.0, 100, 190)],
+        ion_inj=[(soma[0], 3, 4.0, 0), (soma[7], 1, -0.5, 1)],
+        lig_inj=[(soma[0], 0, 0.25, 1)])
+    return [(0, first), (100, second)]
+
+
+def run_scheduled(sim, name, net, ticks, dt, somata, read_v):
+    """Runs `ticks` single ticks on `sim` (anything with run(n, dt) or run_ticks(n, dt)
+    and upload_stimuli), uploading the case's schedule; returns the soma V_m trace."""
+    sched = dict(stimulus_schedule(name, net))
+    step = getattr(sim, "run_ticks", None) or sim.run
+    trace = np.empty((ticks, len(somata)), np.float64)
+    for t in range(ticks):
+        if t in sched:
+            sim.upload_stimuli(sched[t])
+        step(1, dt)
+        trace[t] = read_v()[somata]
+    return trace
+

@@ -17,12 +17,16 @@ def test_oracle_matches_reference_fixture(name):
     g, spec = golden_cases.load(name)
     net = Network(NetgenParams(**spec))
     o = Oracle(net)
-    trace = o.trace(int(g["ticks"]), float(g["dt"]), g["somata"])
+    if golden_cases.stimulus_schedule(name, net):
+        trace = golden_cases.run_scheduled(o, name, net, int(g["ticks"]), float(g["dt"]), g["somata"],
+                                           lambda: o.segment_field("V"))
+    else:
+        trace = o.trace(int(g["ticks"]), float(g["dt"]), g["somata"])
     golden_cases.compare(g, trace, o.segment_field, o.synapse_field)
 
 
 def test_fixtures_exist():
-    assert set(golden_cases.cases()) >= {"small_n8_s7", "large_n4_s3"}
+    assert set(golden_cases.cases()) >= {"small_n8_s7", "large_n4_s3", "stimuli_n8_s7"}
 
 
 @pytest.mark.skipif(not reference_available(), reason="reference CPU library not built here")

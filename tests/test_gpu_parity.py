@@ -88,11 +88,8 @@ def test_gpu_matches_reference_fixture(name):
     net = Network(NetgenParams(**spec))
     gpu = Backend()
     gpu.load_network(net)
-    somata = g["somata"]
-    trace = np.empty((int(g["ticks"]), somata.size), np.float64)
-    for t in range(int(g["ticks"])):
-        gpu.run_ticks(1, float(g["dt"]))
-        trace[t] = gpu.segment_field("V")[somata]
+    trace = golden_cases.run_scheduled(gpu, name, net, int(g["ticks"]), float(g["dt"]), g["somata"],
+                                       lambda: gpu.segment_field("V"))
     n_syn = net.data.num_synapses
     golden_cases.compare(g, trace, gpu.segment_field, lambda f: gpu.synapse_field(f, 0, n_syn))
 
@@ -235,3 +232,64 @@ def test_ledger_closes_the_mass_balance_on_the_gpu():
     st = gpu.diffusion_stats()
     booked = np.array(st.rounding) + np.array(st.bath)
     assert np.all(np.abs((after - before) - booked) <= 1e-11 * (np.abs(before) + 1.0)), (after - before, booked)
+
+
+def _compare_nt(ora, gpu, label):
+    for f in ("intra_nt", "neurotransmitter"):
+        for q in range(15):
+            _assert_same(gpu.segment_field(f, q), ora.segment_field(f, q), "%s %s[%d]" % (label, f, q))
+
+
+@pytest.mark.parametrize("graph", [False, True])
+def test_stimulus_uploads_bitexact(graph):
+    """gpu_backend_upload_stimuli with every stimulus kind, twice: current steps, ramps
+    (rising, falling, empty, flat), voltage clamps (overlapping on one segment), ion
+    injections (repeated into one ion, extracellular, invalid index and segment) and
+    ligand injections (intracellular, which turns on intra_nt diffusion, and
+    extracellular, which the synapse pass wipes).  Injections apply once, at the next
+    tick; each upload replaces every list.  Through plain launches and through the
+    captured tick loop, which an upload must invalidate."""
+    import golden_cases
+    from bioneuroncore_b200 import NetgenParams, NET_SMALL
+    p = NetgenParams(family=NET_SMALL, n_neurons=8, seed=7)
+    ora, gpu, net = _pair(p)
+    (t0, first), (t1, second) = golden_cases.stimulus_schedule("stimuli", net)
+    assert (t0, t1) == (0, 100)
+    run = gpu.run_ticks_graph if graph else gpu.run_ticks
+    n_syn = net.data.num_synapses
+    ora.upload_stimuli(first)
+    gpu.upload_stimuli(first)
+    for step in (1, 40, 59):
+        ora.run(step, DT)
+        run(step, DT)
+        _compare_all(ora, gpu, n_syn, "first upload, graph=%s, +%d" % (graph, step))
+        _compare_nt(ora, gpu, "first upload +%d" % step)
+    ora.upload_stimuli(second)
+    gpu.upload_stimuli(second)
+    for step in (1, 64, 35):
+        ora.run(step, DT)
+        run(step, DT)
+        _compare_all(ora, gpu, n_syn, "second upload, graph=%s, +%d" % (graph, step))
+        _compare_nt(ora, gpu, "second upload +%d" % step)
+
+
+def test_injections_without_synapses_bitexact():
+    """On dendritic trees (no synapses) an extracellular ligand injection stays in the
+    neurotransmitter field and diffuses through step 2.5, as intracellular ones and
+    ions do; ramps and clamps act as on any network."""
+    from bioneuroncore_b200 import NetgenParams, NET_TREES
+    from bioneuroncore_b200.abi import stimulus_data
+    p = NetgenParams(family=NET_TREES, n_neurons=2, tree_depth=6, seed=4)
+    ora, gpu, net = _pair(p)
+    n = int(net.data.num_segments)
+    data = stimulus_data(ramps=[(0, 100.0, -40.0, 2, 60)], vclamps=[(n - 1, -50.0, 5, 40)],
+                         ion_inj=[(3, 1, 2.0, 1), (3, 1, -0.25, 1), (70, 0, 1.0, 0)],
+                         lig_inj=[(5, 1, 0.4, 0), (9, 0, 0.3, 1), (5, 14, 0.1, 0), (66, 7, 0.2, 0)])
+    ora.upload_stimuli(data)
+    gpu.upload_stimuli(data)
+    for step in (1, 10, 49):
+        ora.run(step, DT)
+        gpu.run_ticks(step, DT)
+        _compare_all(ora, gpu, 0, "trees with injections +%d" % step)
+        _compare_nt(ora, gpu, "trees with injections +%d" % step)
+    assert gpu.segment_field("neurotransmitter", 1).astype(np.float64).sum() > 0.3
