@@ -110,7 +110,7 @@ struct AdjDev {
     const float* sl_rden;          // [slot][kRecPerSyn]
     const uint8_t* sl_rav;         // [slot][kRecPerSyn]
     const float *sl_parea, *sl_tauc;
-    const uint8_t* sl_nt;          // 0 glutamate, 1 GABA
+    const uint8_t* sl_nt;          // 0 glutamate, 1 GABA, 2 glycine
     const uint32_t* ev_off;        // [slot + 1] logged cleft entries, by tick
     const unsigned long long* ev_tick;
     const float* ev_amt;
@@ -658,7 +658,7 @@ __device__ __forceinline__ void tick_fwd(const AdjDev& d, const Ctx& c, const La
             for (int q = 0; q < 15; q++) L.s2[q * Sm + tid] = st[q * Sm + tid];
         const uint32_t g = c.g;
         double ib = L.ibuf[tid];
-        float nt_glu = 0.0f, nt_gaba = 0.0f;
+        float nt_glu = 0.0f, nt_gaba = 0.0f, nt_gly = 0.0f;
         DSeg s;
         s.V = st[tid];
         for (int q = 0; q < 7; q++) { s.in[q] = st[(1 + q) * Sm + tid]; s.out[q] = st[(8 + q) * Sm + tid]; }
@@ -670,7 +670,9 @@ __device__ __forceinline__ void tick_fwd(const AdjDev& d, const Ctx& c, const La
         for (uint32_t y = d.sp_off[g]; y < d.sp_off[g + 1]; y++) {
             const uint32_t ly = y - c.y0;
             float cleft = cleft_events(d, y, tick, rs[ly * kSynWords + 4]);
-            if (d.sl_nt[y] == 0) nt_glu += cleft; else nt_gaba += cleft;
+            if (d.sl_nt[y] == 0) nt_glu += cleft;
+            else if (d.sl_nt[y] == 1) nt_gaba += cleft;
+            else nt_gly += cleft;
             if (kRec) for (int q = 0; q < 7; q++) sc.syn[ly * 9 + q] = s.in[q];
             float I_syn = 0.0f;
             const float scale = d.w[(size_t)c.p * d.n_syn + d.sl_syn[y]];
@@ -684,7 +686,7 @@ __device__ __forceinline__ void tick_fwd(const AdjDev& d, const Ctx& c, const La
                 m.st[2] = m.st[3] = m.st[4] = m.st[5] = m.st[6] = 0.0f;
                 m.area = (parea > 0.0f) ? parea : s.area;
                 m.av = d.sl_rav[y * kRecPerSyn + j];
-                const float ntr = kind <= 1 ? nt_glu : nt_gaba;
+                const float ntr = kind <= 1 ? nt_glu : (kind == 2 ? nt_gaba : nt_gly);
                 I_syn = (float)(I_syn + receptor_current(gRec[kind], m, s, dt, ntr, scale));
                 rs[ly * kSynWords + 2 * j] = m.st[0];
                 rs[ly * kSynWords + 2 * j + 1] = m.st[1];
@@ -1483,13 +1485,16 @@ int adj_build(Adjoint* A, void* sim, const BncAdjointConfig& cfg) {
         const SegLite& ps = hn.seg[s.post_segment];
         for (uint32_t j = 0; j < ps.modifier_count; j++) if (hn.mod(s.post_segment, j).type == BNC_MOD_MYELIN) myel_post = true;
         const uint8_t nt = s.post_receptor_count > 0 ? host_nt_from_receptor(hn.post_rec(k, 0).type) : 0;
-        if (nt > 1) { set_error("adjoint: synapse %u releases a transmitter other than glutamate or GABA", k); return BNC_ERR_UNSUPPORTED; }
+        if (nt > 1 && nt != BNC_NT_GLYCINE) {
+            set_error("adjoint: synapse %u releases a transmitter other than glutamate, GABA or glycine", k);
+            return BNC_ERR_UNSUPPORTED;
+        }
         for (int q = 0; q < 15; q++)
             if (q != nt && s.cleft_neurotransmitter[q] != 0.0f) {
                 set_error("adjoint: synapse %u holds a cleft transmitter it does not release", k);
                 return BNC_ERR_UNSUPPORTED;
             }
-        sl_nt[y] = nt;
+        sl_nt[y] = (nt == BNC_NT_GLYCINE) ? 2 : nt;
         sl_parea[y] = s.post_area;
         sl_tauc[y] = s.tau_clearance;
         rinit[(size_t)y * kSynWords + 4] = s.cleft_neurotransmitter[nt];
@@ -1497,14 +1502,14 @@ int adj_build(Adjoint* A, void* sim, const BncAdjointConfig& cfg) {
         for (uint32_t j = 0; j < s.post_receptor_count; j++) {
             const ModLite& m = hn.post_rec(k, j);
             if (myel_post && host_is_ionotropic(m.type)) continue;   // simulation_host.cpp:495
-            if (m.type != BNC_MOD_AMPA && m.type != BNC_MOD_GABAA) {
-                set_error("adjoint: receptor type %u on synapse %u is not differentiated (AMPA and GABA-A are)",
+            if (m.type != BNC_MOD_AMPA && m.type != BNC_MOD_GABAA && m.type != BNC_MOD_GLYCINE) {
+                set_error("adjoint: receptor type %u on synapse %u is not differentiated (AMPA, GABA-A and glycine are)",
                           (unsigned)m.type, k);
                 return BNC_ERR_UNSUPPORTED;
             }
             if (m.active_vars != 0) { set_error("adjoint: receptor conductance overrides are not modelled"); return BNC_ERR_UNSUPPORTED; }
             if (r >= (uint32_t)kRecPerSyn) { set_error("adjoint: synapse %u has more than %d receptors", k, kRecPerSyn); return BNC_ERR_UNSUPPORTED; }
-            sl_kind[(size_t)y * kRecPerSyn + r] = (m.type == BNC_MOD_AMPA) ? 0 : 2;
+            sl_kind[(size_t)y * kRecPerSyn + r] = (m.type == BNC_MOD_AMPA) ? 0 : (m.type == BNC_MOD_GABAA ? 2 : 3);
             sl_rden[(size_t)y * kRecPerSyn + r] = m.density;
             rinit[(size_t)y * kSynWords + 2 * r] = m.state[0];
             rinit[(size_t)y * kSynWords + 2 * r + 1] = m.state[1];

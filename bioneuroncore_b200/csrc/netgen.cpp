@@ -272,7 +272,8 @@ int generate_network(const BncNetgenParams& p, NetSink& sink, NetShape* shape_ou
             int nr = f.receptors_per_syn;
             for (int j = 0; j < nr; j++) {
                 uint8_t rt;
-                if (j == 0) rt = inhib ? BNC_MOD_GABAA : BNC_MOD_AMPA;
+                if (j == 0) rt = ((p.flags & BNC_NETGEN_GLYCINE) && (i & 1)) ? BNC_MOD_GLYCINE
+                                                                             : (inhib ? BNC_MOD_GABAA : BNC_MOD_AMPA);
                 else if (inhib) rt = (rng_syn.u01() < 0.5) ? BNC_MOD_GABAA : BNC_MOD_GLYCINE;
                 else rt = (rng_syn.u01() < 0.5) ? BNC_MOD_AMPA : BNC_MOD_NMDA;
                 set_mod(sy.post_receptors[j], rt, 200.0);

@@ -129,6 +129,9 @@ typedef struct {
 /* The fitting family (BNC_NET_ADJOINT) with the whole small set: Cav1.3 and the Na/K
  * pump on every segment as well, beside the three fitted conductances. */
 #define BNC_NETGEN_FULL_SMALL_SET 64u
+/* Synapses with an odd index take a glycine receptor (transmitter glycine) as their
+ * first receptor instead of AMPA or GABA-A; other draws are unchanged. */
+#define BNC_NETGEN_GLYCINE 128u
 
 /* Generates a network into host AoS arrays in the reference layout.  The arrays
  * are owned by the library; release with bnc_netgen_free.  *stim receives the

@@ -17,7 +17,7 @@
  * current stimuli; step 2.5 (diffusion_kernel.h:41-364: phi_e Jacobi solve,
  * intracellular and extracellular Nernst-Planck sub-steps with Scharfetter-Gummel
  * fluxes, the backward-Euler V_m sweeps, the bath relaxation); step 3 with the clefts
- * from the log and AMPA / GABA-A receptors (modifier_helpers.h:1213-1278, with the
+ * from the log and AMPA / GABA-A / glycine receptors (modifier_helpers.h:1213-1278, with the
  * density scale); step 4 (simulation_host.cpp:596-649).  ATP diffuses (Fick,
  * diffusion_kernel.h:284-345) because the pump reads it; transmitter and heat
  * diffusion are left out: nothing in the modelled networks reads them.  Every
@@ -217,19 +217,22 @@ int bo_tangent_run(const BncBionData* net, const BncCurrentStimulus* stim, uint3
         bool myel_post = false;
         const BncSegment& ps = net->segments[s.post];
         for (uint32_t j = 0; j < ps.modifier_count; j++) if (ps.modifiers[j].type == BNC_MOD_MYELIN) myel_post = true;
-        s.nt = (y.post_receptor_count > 0 && y.post_receptors[0].type == BNC_MOD_GABAA) ? 1 : 0;
+        // transmitter of the first receptor (run_tick_common.h:199-206): 0 glutamate,
+        // 1 GABA, 2 glycine (cleft entry BNC_NT_GLYCINE)
+        const uint8_t r0 = y.post_receptor_count > 0 ? y.post_receptors[0].type : 0;
+        s.nt = r0 == BNC_MOD_GABAA ? 1 : (r0 == BNC_MOD_GLYCINE ? 2 : 0);
         s.n_r = 0;
         for (uint32_t j = 0; j < y.post_receptor_count; j++) {
             const BncModifier& m = y.post_receptors[j];
             if (myel_post && is_ionotropic(m.type)) continue;
-            if (m.type != BNC_MOD_AMPA && m.type != BNC_MOD_GABAA) return -1;
+            if (m.type != BNC_MOD_AMPA && m.type != BNC_MOD_GABAA && m.type != BNC_MOD_GLYCINE) return -1;
             s.rtype[s.n_r] = m.type;
             s.rden[s.n_r] = (double)(float)m.density;
             s.r[s.n_r] = (double)(float)m.state[0];
             s.dd[s.n_r] = (double)(float)m.state[1];
             s.n_r++;
         }
-        s.cleft = y.cleft_neurotransmitter[s.nt];
+        s.cleft = y.cleft_neurotransmitter[s.nt == 2 ? BNC_NT_GLYCINE : s.nt];
         s.tauc = y.tau_clearance;
         s.parea = y.post_area;
         s.ev_b = ev;
@@ -488,21 +491,24 @@ int bo_tangent_run(const BncBionData* net, const BncCurrentStimulus* stim, uint3
                 }
         }
         // ---- step 3 ----
-        std::vector<double> nt_glu(N, 0.0), nt_gaba(N, 0.0);
+        std::vector<double> nt_glu(N, 0.0), nt_gaba(N, 0.0), nt_gly(N, 0.0);
         for (uint32_t k = 0; k < K; k++) {
             Syn& y = sy[k];
             Seg& s = sg[y.post];
             for (uint32_t q = y.ev_b; q < y.ev_e; q++)
                 if (ev_tick[q] == tick) y.cleft += (double)ev_amt[q];
-            if (y.nt == 0) nt_glu[y.post] += y.cleft; else nt_gaba[y.post] += y.cleft;
+            if (y.nt == 0) nt_glu[y.post] += y.cleft;
+            else if (y.nt == 1) nt_gaba[y.post] += y.cleft;
+            else nt_gly[y.post] += y.cleft;
             T I_syn(0.0);
             const T w(p_w[k], d_w[k]);
             const double cpm = F * s.vol / 1000.0;
             for (int j = 0; j < y.n_r; j++) {
-                const bool ampa = y.rtype[j] == BNC_MOD_AMPA;
-                const double EC50 = ampa ? 0.5 : 1.0, tr = ampa ? 0.5 : 1.0, td = ampa ? 3.0 : 5.0,
-                             tdes = ampa ? 3.0 : 2000.0;
-                const double nt = ampa ? nt_glu[y.post] : nt_gaba[y.post];
+                // receptors_biological.cpp:42-82: AMPA, GABA-A, glycine
+                const bool ampa = y.rtype[j] == BNC_MOD_AMPA, gly = y.rtype[j] == BNC_MOD_GLYCINE;
+                const double EC50 = ampa ? 0.5 : (gly ? 0.5 : 1.0), tr = ampa ? 0.5 : (gly ? 0.3 : 1.0),
+                             td = ampa ? 3.0 : 5.0, tdes = ampa ? 3.0 : 2000.0;
+                const double nt = ampa ? nt_glu[y.post] : (gly ? nt_gly[y.post] : nt_gaba[y.post]);
                 const double r_inf = nt / (nt + EC50);
                 const double tau = r_inf > y.r[j] ? tr : td;
                 y.r[j] = std::min(1.0, std::max(0.0, y.r[j] + (r_inf - y.r[j]) * (double)dt / tau));
@@ -522,7 +528,7 @@ int bo_tangent_run(const BncBionData* net, const BncCurrentStimulus* stim, uint3
                     clamp_ions(s.in);
                     I_syn = I_syn - (INa + IK);
                 } else {
-                    const double PCl = ghk_P(28.0, 1.0, (double)36.20f);
+                    const double PCl = ghk_P(gly ? 60.0 : 28.0, 1.0, (double)36.20f);
                     T ICl = T(PCl) * ghk_mono(s.V, s.out[3], s.in[3]) * Nk * w * 1e12;
                     s.in[3] = s.in[3] + ICl * (double)dt / cpm;
                     clamp_ions(s.in);

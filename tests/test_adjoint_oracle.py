@@ -4,7 +4,7 @@ Also the oracle's release log, which the replay feeds on."""
 import numpy as np
 import pytest
 
-from bioneuroncore_b200 import Network, NetgenParams, NET_ADJOINT, NETGEN_FULL_SMALL_SET
+from bioneuroncore_b200 import Network, NetgenParams, NET_ADJOINT, NETGEN_FULL_SMALL_SET, NETGEN_GLYCINE
 
 DT = 0.025
 
@@ -31,25 +31,35 @@ def test_release_log_is_sorted_and_positive():
     assert (amt > 0).all() and (tick < 400).all()
 
 
-@pytest.mark.parametrize("flags", [0, NETGEN_FULL_SMALL_SET])
+@pytest.mark.parametrize("flags", [0, NETGEN_FULL_SMALL_SET, NETGEN_GLYCINE])
 def test_tangent_matches_its_central_differences(flags):
-    """With the fitting family and with the whole small set (Cav1.3, the Na/K pump and
-    the ATP it consumes, which diffuses)."""
+    """With the fitting family, with the whole small set (Cav1.3, the Na/K pump and
+    the ATP it consumes, which diffuses), and with glycine receptors first on the
+    odd-numbered synapses (4 neurons over 400 ticks, where synapse 17, a glycine
+    synapse, releases)."""
     from oracle.oracle import Oracle, tangent_loss
-    ticks = 300
-    p = NetgenParams(family=NET_ADJOINT, n_neurons=3, seed=11, flags=flags)
+    gly = bool(flags & NETGEN_GLYCINE)
+    n, ticks = (4, 400) if gly else (3, 300)
+    p = NetgenParams(family=NET_ADJOINT, n_neurons=n, seed=7 if gly else 11, flags=flags)
     net = Network(p)
     log = Oracle(Network(p)).run_logged(ticks, DT)
     base = _densities(net)
-    soma = np.array([n * 64 for n in range(3)], np.uint32)
-    target = np.full((ticks, 3), -64.0, np.float32)
+    soma = np.array([k * 64 for k in range(n)], np.uint32)
+    target = np.full((ticks, n), -64.0, np.float32)
     rng = np.random.default_rng(5)
     dvec = [x * rng.standard_normal(x.shape) for x in base]
     zero = [np.zeros_like(x) for x in base]
-    L, dL = tangent_loss(net, log, ticks, DT, base, dvec, soma, target)
-    h = 1e-4
-    Lp, _ = tangent_loss(net, log, ticks, DT, [x + h * v for x, v in zip(base, dvec)], zero, soma, target)
-    Lm, _ = tangent_loss(net, log, ticks, DT, [x - h * v for x, v in zip(base, dvec)], zero, soma, target)
-    fd = (Lp - Lm) / (2 * h)
-    assert L > 0 and abs(dL) > 0
-    assert abs(dL - fd) <= 1e-6 * abs(fd), (dL, fd)
+    if gly:
+        is_gly = net.synapses["post_receptors"][:, 0]["type"] == 12
+        assert is_gly[np.unique(log[0])].any()          # a glycine synapse releases
+    dirs = [dvec]
+    if gly:   # the weights of the glycine synapses alone
+        dirs.append(zero[:3] + [np.where(is_gly, base[3], 0.0)])
+    for dv in dirs:
+        L, dL = tangent_loss(net, log, ticks, DT, base, dv, soma, target)
+        h = 1e-4
+        Lp, _ = tangent_loss(net, log, ticks, DT, [x + h * v for x, v in zip(base, dv)], zero, soma, target)
+        Lm, _ = tangent_loss(net, log, ticks, DT, [x - h * v for x, v in zip(base, dv)], zero, soma, target)
+        fd = (Lp - Lm) / (2 * h)
+        assert L > 0 and abs(dL) > 0
+        assert abs(dL - fd) <= 1e-6 * abs(fd), (dL, fd)

@@ -10,7 +10,8 @@ on every segment, the pump's ATP diffusing).  All tests are marked gpu.
 import numpy as np
 import pytest
 
-from bioneuroncore_b200 import Adjoint, Backend, Network, NetgenParams, NET_ADJOINT, NETGEN_FULL_SMALL_SET
+from bioneuroncore_b200 import (Adjoint, Backend, Network, NetgenParams, NET_ADJOINT, NETGEN_FULL_SMALL_SET,
+                                NETGEN_GLYCINE)
 
 DT = 0.025
 
@@ -37,7 +38,7 @@ def _plain_soma_trace(p, soma, ticks):
     return out
 
 
-@pytest.mark.parametrize("flags", [0, NETGEN_FULL_SMALL_SET])
+@pytest.mark.parametrize("flags", [0, NETGEN_FULL_SMALL_SET, NETGEN_GLYCINE])
 def test_replay_forward_is_the_plain_trajectory(flags):
     """The forward pass, replaying the release log, reproduces the plain tick's somatic
     voltages bit for bit (same device functions, same operation order)."""
@@ -65,7 +66,7 @@ def _fit_problem(ticks, n_sets, n_neurons=4, scale=(1.1, 0.9, 1.2, 0.8), flags=0
     return p, net, adj, base, tr[0]
 
 
-@pytest.mark.parametrize("flags", [0, NETGEN_FULL_SMALL_SET])
+@pytest.mark.parametrize("flags", [0, NETGEN_FULL_SMALL_SET, NETGEN_GLYCINE])
 def test_gradient_matches_fp64_forward_mode_and_central_differences(flags):
     """The device adjoint's gradient along a random direction of all parameters (gNa,
     gK, gleak per segment, weight per synapse) against (a) the FP64 CPU forward-mode
