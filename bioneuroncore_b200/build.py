@@ -21,7 +21,7 @@ BUILD = os.path.join(PKG, "_build")
 LIB = os.path.join(PKG, "libbnc_b200.so")
 ORACLE_DIR = os.path.join(ROOT, "oracle")
 ORACLE_LIB = os.path.join(ORACLE_DIR, "liboracle.so")
-REFERENCE = "/root/reference"
+ORACLE64_LIB = os.path.join(ORACLE_DIR, "liboracle64.so")
 
 CU_SOURCES = ["modifiers.cu", "diffuse.cu", "synapse.cu", "backend.cu", "plugins.cu", "adjoint.cu"]
 CPP_SOURCES = ["netgen.cpp", "capi_host.cpp", "builder.cpp", "sweep.cpp"]
@@ -104,23 +104,30 @@ TANGENT_LIB = os.path.join(ORACLE_DIR, "libbo_tangent.so")
 
 def build_oracle():
     """Compiles the CPU oracle (test infrastructure) with contraction disabled: the FP32
-    tick restatement and the FP64 forward-mode replay that checks the adjoint."""
+    tick restatement, the same source with FP64 state and the C library's elementary
+    functions (liboracle64.so, checked against the reference's own tick), and the FP64
+    forward-mode replay that checks the adjoint."""
     srcs = [os.path.join(ORACLE_DIR, f) for f in ("bnc_oracle.c", "bo_math.h", "bo_physics.h", "bo_modifiers.h")]
     abi = os.path.join(ROOT, "include", "bnc_abi.h")
     if _stale(ORACLE_LIB, srcs + [abi]):
         _run(["gcc", "-std=c11", "-O2", "-ffp-contract=off", "-fPIC", "-shared", "-o", ORACLE_LIB,
               os.path.join(ORACLE_DIR, "bnc_oracle.c"), "-lm"])
+    if _stale(ORACLE64_LIB, srcs + [abi]):
+        _run(["gcc", "-std=c11", "-O2", "-ffp-contract=off", "-DBO_FP64", "-DBO_LIBM", "-fPIC", "-shared",
+              "-o", ORACLE64_LIB, os.path.join(ORACLE_DIR, "bnc_oracle.c"), "-lm"])
     tsrc = os.path.join(ORACLE_DIR, "bo_tangent.cpp")
     if _stale(TANGENT_LIB, [tsrc, abi]):
         _run(["g++", "-std=c++17", "-O2", "-ffp-contract=off", "-fPIC", "-shared", "-o", TANGENT_LIB, tsrc, "-lm"])
     return ORACLE_LIB
 
 
-def build_reference():
-    """Builds the reference CPU library into oracle/_ref/ when its sources are present."""
-    if not os.path.isdir(os.path.join(REFERENCE, "src")):
+def build_reference(ref_dir=None):
+    """Builds the reference CPU library into oracle/_ref/ from the reference checkout
+    at `ref_dir` (else $BNC_REFERENCE_DIR); returns None when neither names one."""
+    ref_dir = ref_dir or os.environ.get("BNC_REFERENCE_DIR")
+    if not ref_dir or not os.path.isdir(os.path.join(ref_dir, "src")):
         return None
-    _run(["make", "-s", "-C", ORACLE_DIR, "-j8"])
+    _run(["make", "-s", "-C", ORACLE_DIR, "-j8", "REF=" + os.path.abspath(ref_dir)])
     return os.path.join(ORACLE_DIR, "_ref", "libbiocore_ref.so")
 
 
@@ -128,7 +135,7 @@ def ensure_built():
     """Builds the product library and the oracle only when their files are missing."""
     if not os.path.exists(LIB):
         build_library()
-    if not os.path.exists(ORACLE_LIB) or not os.path.exists(TANGENT_LIB):
+    if not all(os.path.exists(p) for p in (ORACLE_LIB, ORACLE64_LIB, TANGENT_LIB)):
         build_oracle()
 
 
@@ -136,11 +143,12 @@ def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--oracle", action="store_true")
     ap.add_argument("--ptxas", action="store_true")
+    ap.add_argument("--reference", default=None, help="reference checkout to build oracle/_ref/ from")
     a = ap.parse_args(argv)
     print(build_library(verbose=True, ptxas_info=a.ptxas))
     if a.oracle:
         print(build_oracle())
-        print(build_reference())
+        print(build_reference(a.reference))
 
 
 if __name__ == "__main__":

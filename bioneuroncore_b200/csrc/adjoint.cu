@@ -267,7 +267,7 @@ __device__ inline float bern_f(float x) {
     if (fabsf(x) < 1e-3f) return 1.0f - 0.5f * x;
     if (x > 50.0f) return 0.0f;
     if (x < -50.0f) return -x;
-    return x / (dm_expf(x) - 1.0f);
+    return x / (dm_exp(x) - 1.0f);
 }
 
 __device__ inline float par_of(const AdjDev& d, uint32_t p, int cls, uint32_t g) {
@@ -693,7 +693,7 @@ __device__ __forceinline__ void tick_fwd(const AdjDev& d, const Ctx& c, const La
                 if (kRec) sc.syn[ly * 9 + 7 + j] = m.st[0] * (1.0f - m.st[1]);
             }
             ib += I_syn;
-            cleft *= dm_expf(-dt / d.sl_tauc[y]);
+            cleft *= dm_exp(-dt / d.sl_tauc[y]);
             if (cleft < 0.0f) cleft = 0.0f;
             rs[ly * kSynWords + 4] = cleft;
         }

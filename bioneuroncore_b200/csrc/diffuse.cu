@@ -30,7 +30,7 @@ __global__ void k_init_ntd() {
     for (int q = 0; q < 15; q++) {
         float ms = mass[q];
         if (ms < 1.0f) ms = 1.0f;
-        gNtD[q] = 1.33f * dm_powf(23.0f / ms, 1.0f / 3.0f);
+        gNtD[q] = 1.33f * dm_powf(23.0f / ms, 1.0f / 3.0f);   // powf: types.h:442
     }
 }
 
@@ -66,7 +66,7 @@ __device__ __forceinline__ float sg_bernoulli(float x) {
     if (fabsf(x) < 1e-3f) return 1.0f - 0.5f * x;
     if (x > 50.0f) return 0.0f;
     if (x < -50.0f) return -x;
-    return x / (dm_expf(x) - 1.0f);
+    return x / (dm_exp(x) - 1.0f);
 }
 
 // valence group of ion q (+1: 0, 1, 6; +2: 2, 4; -1: 3, 5) and the group's factor

@@ -175,16 +175,16 @@ __device__ __forceinline__ void dp_partial_P(float gamma_pS, float fNa, float fK
 __device__ __forceinline__ float dp_nernst(float intra, float extra, float valence) {
     if (intra < 1e-9f) intra = 1e-9f;
     if (extra < 1e-9f) extra = 1e-9f;
-    return (float)((GAS_CONST * CELSIUS_37) / (valence * FARADAY_CONST) * dm_logf(extra / intra) * 1000.0f);
+    return (float)((GAS_CONST * CELSIUS_37) / (valence * FARADAY_CONST) * dm_log(extra / intra) * 1000.0f);
 }
 /* modifier_helpers.h:132-135 */
 __device__ __forceinline__ float dp_vtrap(float x, float y) {
     if (fabsf(x / y) < 1e-6f) return y * (1.0f - x / (2.0f * y));
-    return x / (1.0f - dm_expf(-x / y));
+    return x / (1.0f - dm_exp(-x / y));
 }
 /* modifier_helpers.h:1090-1095 */
-__device__ __forceinline__ float dp_bz_act(float V, float vh, float k) { return 1.0f / (1.0f + dm_expf(-(V - vh) / k)); }
-__device__ __forceinline__ float dp_bz_inact(float V, float vh, float k) { return 1.0f / (1.0f + dm_expf((V - vh) / k)); }
+__device__ __forceinline__ float dp_bz_act(float V, float vh, float k) { return 1.0f / (1.0f + dm_exp(-(V - vh) / k)); }
+__device__ __forceinline__ float dp_bz_inact(float V, float vh, float k) { return 1.0f / (1.0f + dm_exp((V - vh) / k)); }
 
 /* ---- gating helpers (modifier_helpers.h:145-215, 264-271, 468-472, 689-702, 1008-1018, 882-892, 909-913, 954-967, 1137-1170, 1188-1210) ---- */
 __device__ __forceinline__ float nav16_am(float V) { return 0.182f * dp_vtrap(V + 43.0f, 6.0f); }
@@ -193,7 +193,7 @@ __device__ __forceinline__ float nav16_ah(float V) { return 0.024f * dp_vtrap(V 
 __device__ __forceinline__ float nav16_bh(float V) { return 0.0091f * dp_vtrap(-(V + 75.0f), 5.0f); }
 __device__ __forceinline__ float nav16_m_inf(float V) { float a = nav16_am(V), b = nav16_bm(V); return a / (a + b); }
 __device__ __forceinline__ float nav16_m_tau(float V) { return 1.0f / (nav16_am(V) + nav16_bm(V)); }
-__device__ __forceinline__ float nav16_h_inf(float V) { return 1.0f / (1.0f + dm_expf((V + 72.0f) / 6.2f)); }
+__device__ __forceinline__ float nav16_h_inf(float V) { return 1.0f / (1.0f + dm_exp((V + 72.0f) / 6.2f)); }
 __device__ __forceinline__ float nav16_h_tau(float V) { return 1.0f / (nav16_ah(V) + nav16_bh(V)); }
 __device__ __forceinline__ float nav12_am(float V) { return 0.182f * dp_vtrap(V + 23.0f, 6.0f); }
 __device__ __forceinline__ float nav12_bm(float V) { return 0.124f * dp_vtrap(-(V + 23.0f), 6.0f); }
@@ -201,36 +201,36 @@ __device__ __forceinline__ float nav12_ah(float V) { return 0.024f * dp_vtrap(V 
 __device__ __forceinline__ float nav12_bh(float V) { return 0.0091f * dp_vtrap(-(V + 66.5f), 5.0f); }
 __device__ __forceinline__ float nav12_m_inf(float V) { float a = nav12_am(V), b = nav12_bm(V); return a / (a + b); }
 __device__ __forceinline__ float nav12_m_tau(float V) { return 1.0f / (nav12_am(V) + nav12_bm(V)); }
-__device__ __forceinline__ float nav12_h_inf(float V) { return 1.0f / (1.0f + dm_expf((V + 63.5f) / 6.2f)); }
+__device__ __forceinline__ float nav12_h_inf(float V) { return 1.0f / (1.0f + dm_exp((V + 63.5f) / 6.2f)); }
 __device__ __forceinline__ float nav12_h_tau(float V) { return 1.0f / (nav12_ah(V) + nav12_bh(V)); }
-__device__ __forceinline__ float cav21_m_inf(float V) { return 1.0f / (1.0f + dm_expf(-(V - -15.0f) / (6.0f + 1e-6f))); }
+__device__ __forceinline__ float cav21_m_inf(float V) { return 1.0f / (1.0f + dm_exp(-(V - -15.0f) / (6.0f + 1e-6f))); }
 __device__ __forceinline__ float cav21_h_inf(float V, float Ca_uM) {
-    float h = 1.0f / (1.0f + dm_expf((V - -50.0f) / 8.0f));
+    float h = 1.0f / (1.0f + dm_exp((V - -50.0f) / 8.0f));
     h *= 1.0f / (1.0f + Ca_uM / 3.0f);
     return h;
 }
 __device__ __forceinline__ float kv42_h_tau(float V) {
-    return 15.0f + (170.0f - 15.0f) / (1.0f + dm_expf((V - -60.0f) / 8.0f));
+    return 15.0f + (170.0f - 15.0f) / (1.0f + dm_exp((V - -60.0f) / 8.0f));
 }
 __device__ __forceinline__ float cav31_h_tau(float V) {
-    return 25.0f + (250.0f - 25.0f) / (1.0f + dm_expf((V - -65.0f) / 8.0f));
+    return 25.0f + (250.0f - 25.0f) / (1.0f + dm_exp((V - -65.0f) / 8.0f));
 }
 __device__ __forceinline__ float cav31_m_tau(float V) {
     float dv = V - -20.0f;
-    float g = dm_expf(-(dv * dv) / (2.0f * 22.0f * 22.0f));
+    float g = dm_exp(-(dv * dv) / (2.0f * 22.0f * 22.0f));
     return 1.25f + (15.0f - 1.25f) * g;
 }
 __device__ __forceinline__ float kv_dr_m_tau(float V, float V_half) {
-    float tau = 14.6f * dm_expf(-(V - V_half) / 30.1f);
+    float tau = 14.6f * dm_exp(-(V - V_half) / 30.1f);
     if (tau < 0.3f) tau = 0.3f;
     if (tau > 200.0f) tau = 200.0f;
     return tau;
 }
 __device__ __forceinline__ float kir_f_open(float V) {
     float Vn = (float)(FARADAY_CONST * V * 0.001f / (GAS_CONST * CELSIUS_37));
-    float Kd_Mg = 0.3f * dm_expf(-0.6f * 2.0f * Vn);
+    float Kd_Mg = 0.3f * dm_exp(-0.6f * 2.0f * Vn);
     float mg_block = 0.5f / Kd_Mg;
-    float Kd_spm = 0.0775f * dm_expf(-0.5f * 4.0f * Vn);
+    float Kd_spm = 0.0775f * dm_exp(-0.5f * 4.0f * Vn);
     float r = 0.001f / Kd_spm;
     float spm_block = 0.0f, rk = r;
     for (int k = 0; k < 3; k++) { spm_block += rk; rk *= r; }
@@ -239,12 +239,12 @@ __device__ __forceinline__ float kir_f_open(float V) {
 __device__ __forceinline__ float sk_p_inf(float Ca) {
     if (Ca < 1e-9f) Ca = 1e-9f;
     float r = 0.0004f / Ca;
-    return 1.0f / (1.0f + dm_powf(r, 4.0f));
+    return 1.0f / (1.0f + dm_pow(r, 4.0f));
 }
 __device__ __forceinline__ float bk_ha_po(float V_mV, float Ca) {
     float Vn = (float)(FARADAY_CONST * V_mV * MV_TO_V / (GAS_CONST * CELSIUS_37));
-    float J = 0.104f * dm_expf(0.55f * Vn);
-    float L = 3.7e-8f * dm_expf(0.30f * Vn);
+    float J = 0.104f * dm_exp(0.55f * Vn);
+    float L = 3.7e-8f * dm_exp(0.30f * Vn);
     if (Ca < 0.0f) Ca = 0.0f;
     float K = Ca / 0.044f;
     float o = 1.0f + K * 23.0f + J * 32.0f + J * K * 23.0f * 32.0f * 3.7f;
@@ -265,8 +265,8 @@ __device__ __forceinline__ float nak_pump_vnorm(float V_mV, float Na_i, float K_
     if (atp < 0.0f) atp = 0.0f;
     float f_ATP = atp / (atp + 0.5f);
     float eta = (float)(0.8f * FARADAY_CONST * (V_mV * MV_TO_V) / (GAS_CONST * CELSIUS_37));
-    float a2 = 60.0f * dm_expf(0.5f * eta);
-    float b2 = 6.0f * dm_expf(-(1.0f - 0.5f) * eta);
+    float a2 = 60.0f * dm_exp(0.5f * eta);
+    float b2 = 6.0f * dm_exp(-(1.0f - 0.5f) * eta);
     float a1 = 200.0f * f_Na * f_ATP;
     float a3 = 200.0f * f_K;
     float a4 = 60.0f;
@@ -279,8 +279,8 @@ __device__ __forceinline__ float nak_pump_vnorm(float V_mV, float Na_i, float K_
 __device__ __forceinline__ float ncx_flux_norm(float V_mV, float Na_i, float Na_o, float Ca_i, float Ca_o) {
     float V_v = V_mV * MV_TO_V;
     float FRT = (float)(FARADAY_CONST / (GAS_CONST * CELSIUS_37));
-    float e_eta = dm_expf(0.35f * FRT * V_v);
-    float e_eta1 = dm_expf((0.35f - 1.0f) * FRT * V_v);
+    float e_eta = dm_exp(0.35f * FRT * V_v);
+    float e_eta1 = dm_exp((0.35f - 1.0f) * FRT * V_v);
     float Na_i3 = Na_i * Na_i * Na_i;
     float Na_o3 = Na_o * Na_o * Na_o;
     float fwd = e_eta1 * Na_o3 * Ca_i;
@@ -311,8 +311,8 @@ __device__ __forceinline__ double dp_nav_current(DMod& m, DSeg& s, float dt, int
     float mtau = is12 ? nav12_m_tau(V) : nav16_m_tau(V);
     float hinf = is12 ? nav12_h_inf(V) : nav16_h_inf(V);
     float htau = is12 ? nav12_h_tau(V) : nav16_h_tau(V);
-    double m_val = minf + (((double)m.st[0]) - minf) * dm_expf(-dt / mtau);
-    double h_val = hinf + (((double)m.st[1]) - hinf) * dm_expf(-dt / htau);
+    double m_val = minf + (((double)m.st[0]) - minf) * dm_exp(-dt / mtau);
+    double h_val = hinf + (((double)m.st[1]) - hinf) * dm_exp(-dt / htau);
     if (m_val < 0.0f) m_val = 0.0f;
     if (m_val > 1.0f) m_val = 1.0f;
     if (h_val < 0.0f) h_val = 0.0f;
@@ -350,7 +350,7 @@ __device__ __forceinline__ double dp_cav13_current(DMod& m, DSeg& s, float dt) {
     float tau_m = 2.0f;
     m.st[0] = (float)(((double)m.st[0]) + (m_inf - ((double)m.st[0])) * dt / tau_m);
     float Ca = (float)(((double)s.in[2]) * MM_TO_UM);
-    float h_inf = 1.0f / (1.0f + dm_expf((V + 52.0f) / 8.0f));
+    float h_inf = 1.0f / (1.0f + dm_exp((V + 52.0f) / 8.0f));
     h_inf *= 1.0f / (1.0f + Ca / 3.0f);
     float tau_h = 100.0f;
     m.st[1] = (float)(((double)m.st[1]) + (h_inf - ((double)m.st[1])) * dt / tau_h);
@@ -433,7 +433,7 @@ __device__ __forceinline__ double dp_kv42_current(DMod& m, DSeg& s, float dt) {
     float m_inf = (float)(1.0f / (1.0f + dm_exp(-(V - Vhalf) / (k + 1e-6f))));
     float tau_m = 1.5f;
     m.st[0] = (float)(((double)m.st[0]) + (m_inf - ((double)m.st[0])) * dt / tau_m);
-    float h_inf = 1.0f / (1.0f + dm_expf((V + 65.0f) / 8.0f));
+    float h_inf = 1.0f / (1.0f + dm_exp((V + 65.0f) / 8.0f));
     float tau_h = kv42_h_tau(V);
     m.st[1] = (float)(((double)m.st[1]) + (h_inf - ((double)m.st[1])) * dt / tau_h);
     if (((double)m.st[0]) < 0.0f) m.st[0] = 0.0f;
@@ -464,12 +464,12 @@ __device__ __forceinline__ double dp_kv31_current(DMod& m, DSeg& s, float dt) {
     float V = s.V;
     float area = m.area;
     float Vhalf = 10.0f, k = 10.0f, gamma_ps = 27.0f;
-    float m_inf = 1.0f / (1.0f + dm_expf(-(V - Vhalf) / (k + 1e-6f)));
+    float m_inf = 1.0f / (1.0f + dm_exp(-(V - Vhalf) / (k + 1e-6f)));
     float tau_m = 1.0f;
     m.st[0] = (float)(((double)m.st[0]) + (m_inf - ((double)m.st[0])) * dt / tau_m);
     if (((double)m.st[0]) < 0.0f) m.st[0] = 0.0f;
     if (((double)m.st[0]) > 1.0f) m.st[0] = 1.0f;
-    float h_inf = 1.0f / (1.0f + dm_expf((V + 30.0f) / 6.0f));
+    float h_inf = 1.0f / (1.0f + dm_exp((V + 30.0f) / 6.0f));
     float tau_h = 2000.0f;
     m.st[1] = (float)(((double)m.st[1]) + (h_inf - ((double)m.st[1])) * dt / tau_h);
     if (((double)m.st[1]) < 0.0f) m.st[1] = 0.0f;
@@ -857,7 +857,7 @@ __device__ __forceinline__ double dp_hcn1_current(DMod& m, DSeg& s, float dt) {
     float camp = 0.1f;  /* segment_camp_um: no cAMP/PKA modifier -> basal 0.1 uM (units.h:324) */
     float Ve = V_half + 15.0f * camp / (camp + 0.5f);
     float mv = m.st[0];
-    float mi = 1.0f / (1.0f + dm_expf(((float)V - Ve) / k));
+    float mi = 1.0f / (1.0f + dm_exp(((float)V - Ve) / k));
     float tau_eff = (V < Ve) ? (float)(tau_open * dm_exp((V - Ve) / 15.0f)) : tau_close;
     mv += (mi - mv) * dt / tau_eff;
     if (mv < 0.0f) mv = 0.0f;

@@ -134,7 +134,7 @@ k_synapse(NetDev d, float dt, unsigned long long tick, int first_tick) {
                     float m_inf = cav21_m_inf(V_bouton);
                     float h_inf = cav21_h_inf(V_bouton, bouton * MM_TO_UM);
                     mm = m_inf;
-                    h = (float)(h_inf + ((double)pr.w - h_inf) * dm_expf(-dt / 300.0f));
+                    h = (float)(h_inf + ((double)pr.w - h_inf) * dm_exp(-dt / 300.0f));
                 }
                 float cav21_open = mm * mm * h;
                 double P_single = dp_ghk_P(15.0f, 2.0f, GHK_CBAR_CA_MM);
@@ -149,7 +149,7 @@ k_synapse(NetDev d, float dt, unsigned long long tick, int first_tick) {
             refr = d.sy_refr[k];
             if (refr == 0) {
                 float Ca_uM = bouton * MM_TO_UM;
-                float ca_act = dm_powf(Ca_uM, 4.0f) / (dm_powf(Ca_uM, 4.0f) + dm_powf(10.0f, 4.0f));
+                float ca_act = dm_pow(Ca_uM, 4.0f) / (dm_pow(Ca_uM, 4.0f) + dm_pow(10.0f, 4.0f));
                 float p = d.sy_prel[k] * ca_act;
                 uint32_t vbits = (uint32_t)(long long)((double)pr.x * 1000.0f);
                 uint32_t seed = d.sy_id[k] ^ (uint32_t)tick ^ vbits;
@@ -228,7 +228,7 @@ k_synapse(NetDev d, float dt, unsigned long long tick, int first_tick) {
                 if (spine < 0.0f) spine = 0.0f;
             }
             // clearance (simulation_host.cpp:505-510)
-            cleft *= dm_expf(-dt / d.sy_tauc[k]);
+            cleft *= dm_exp(-dt / d.sy_tauc[k]);
             if (cleft < 0.0f) cleft = 0.0f;
             // BCM threshold, spine CaMKII/calcineurin, weight (simulation_host.cpp:527-576)
             float facil = d.sy_facil[k];

@@ -145,7 +145,7 @@ static inline float bo_sg_bernoulli(float x) {
     if (fabsf(x) < 1e-3f) return 1.0f - 0.5f * x;
     if (x > 50.0f) return 0.0f;
     if (x < -50.0f) return -x;
-    return x / (bo_expf(x) - 1.0f);
+    return x / (bo_exp(x) - 1.0f);
 }
 
 static const float NP_Z[7] = {1.0f, 1.0f, 2.0f, -1.0f, 2.0f, -1.0f, 1.0f};
@@ -349,9 +349,9 @@ static void bo_diffusion(BoSim* S, float dt) {
         for (uint32_t i = 0; i < n; i++) sg[i].V = c->Vnew[i];
         for (uint32_t i = 0; i < n; i++)
             for (int ion = 0; ion < 7; ion++) {
-                const float old = sg[i].in[ion];
+                const bo_real old = sg[i].in[ion];
                 const double acc = c->intra_acc[i * 7 + ion];
-                sg[i].in[ion] = (float)((double)old + (double)(float)acc);
+                sg[i].in[ion] = BO_ST((double)old + (double)(float)acc);
                 if (S->dmode & 2u) S->ledger[ion] += ((double)sg[i].in[ion] - (double)old - acc) * (double)bo_vol_f(&sg[i]);
             }
     }
@@ -385,9 +385,9 @@ static void bo_diffusion(BoSim* S, float dt) {
         }
         for (uint32_t i = 0; i < n; i++)
             for (int ion = 0; ion < 7; ion++) {
-                const float old = sg[i].out[ion];
+                const bo_real old = sg[i].out[ion];
                 const double acc = c->extra_acc[i * 7 + ion];
-                sg[i].out[ion] = (float)((double)old + acc);
+                sg[i].out[ion] = BO_ST((double)old + acc);
                 if (S->dmode & 2u)
                     S->ledger[ion] += ((double)sg[i].out[ion] - (double)old - acc) *
                                       (double)(bo_vol_f(&sg[i]) * EXTRA_VOLUME_RATIO);
@@ -450,12 +450,12 @@ static void bo_diffusion(BoSim* S, float dt) {
     }
     for (uint32_t i = 0; i < n; i++) {
         for (int ion = 0; ion < 7; ion++) {
-            const float old = sg[i].out[ion];
+            const bo_real old = sg[i].out[ion];
             double e = (double)sg[i].out[ion];
             e += (BATH_ION[ion] - e) * dt / 1.0f;
             if (e < 1e-9) e = 1e-9;
             if (e > 1000.0) e = 1000.0;
-            sg[i].out[ion] = (float)e;
+            sg[i].out[ion] = BO_ST(e);
             if (S->dmode & 2u)
                 S->ledger[7 + ion] += ((double)sg[i].out[ion] - (double)old) *
                                       (double)(bo_vol_f(&sg[i]) * EXTRA_VOLUME_RATIO);
@@ -503,12 +503,17 @@ typedef double (*BoPluginFn)(BoPluginView* v, float dt);
 static BoPluginFn g_bo_plugins[128];
 
 int bo_register_modifier(uint8_t type, BoPluginFn fn) {
+#ifdef BO_FP64
+    (void)fn;
+    return -1;
+#endif
     if (type >= 128) return -1;
     g_bo_plugins[type] = fn;
     return 0;
 }
 
 static double bo_call_modifier(uint8_t type, OMod* m, OSeg* s, float dt) {
+#ifndef BO_FP64   /* the plugin view is the FP32 state; the FP64 build takes no plugins */
     if (type < 128 && g_bo_plugins[type]) {
         BoPluginView v;
         v.V = &s->V; v.in = s->in; v.out = s->out; v.atp = &s->atp;
@@ -516,12 +521,13 @@ static double bo_call_modifier(uint8_t type, OMod* m, OSeg* s, float dt) {
         v.density = m->density; v.state = m->st; v.type = type;
         return g_bo_plugins[type](&v, dt);
     }
+#endif
     return bo_dispatch(type, m, s, dt);
 }
 
 /* (uint32_t)(V_m * 1000.0f) with V_m double, as x86-64 g++ evaluates it:
  * truncation to a 64-bit integer, then modulo 2^32 (simulation_host.cpp:438-440). */
-static inline uint32_t bo_vm_seed_bits(float V) {
+static inline uint32_t bo_vm_seed_bits(bo_real V) {
     double x = (double)V * 1000.0f;
     return (uint32_t)(int64_t)x;
 }
@@ -562,7 +568,7 @@ static void bo_bouton_ca_step(const OSeg* pre, OSyn* syn, float dt) {
             float m_inf = cav21_m_inf(V_bouton);
             float h_inf = cav21_h_inf(V_bouton, syn->bouton_Ca * MM_TO_UM);
             mm = m_inf;
-            h = (float)(h_inf + ((double)pre->mods[j].st[1] - h_inf) * bo_expf(-dt / 300.0f));
+            h = (float)(h_inf + ((double)pre->mods[j].st[1] - h_inf) * bo_exp(-dt / 300.0f));
         }
     }
     float cav21_open = mm * mm * h;
@@ -677,8 +683,8 @@ static void bo_tick(BoSim* S, float dt) {
         for (uint32_t r = 0; r < S->n_ion_inj; r++) {
             const BncIonInjection* ij = &S->ion_inj[r];
             if (ij->segment_id != s->id || ij->ion_idx < 0 || ij->ion_idx >= 7) continue;
-            float* ions = ij->extracellular ? s->out : s->in;
-            ions[ij->ion_idx] = (float)((double)ions[ij->ion_idx] + (double)ij->amount_mM);
+            bo_real* ions = ij->extracellular ? s->out : s->in;
+            ions[ij->ion_idx] = BO_ST((double)ions[ij->ion_idx] + (double)ij->amount_mM);
         }
         /* ligand injections (:289-300) */
         for (uint32_t r = 0; r < S->n_lig_inj; r++) {
@@ -733,7 +739,7 @@ static void bo_tick(BoSim* S, float dt) {
         bo_bouton_ca_step(pre, syn, dt);
         if (syn->refractory == 0) {
             float Ca_uM = syn->bouton_Ca * MM_TO_UM;
-            float ca_act = bo_powf(Ca_uM, 4.0f) / (bo_powf(Ca_uM, 4.0f) + bo_powf(10.0f, 4.0f));
+            float ca_act = bo_pow(Ca_uM, 4.0f) / (bo_pow(Ca_uM, 4.0f) + bo_pow(10.0f, 4.0f));
             float p = syn->p_rel * ca_act;
             for (int j = 0; j < syn->n_pre_ar; j++) {
                 syn->pre_ar[j].st[7] = syn->pre_area;
@@ -782,7 +788,7 @@ static void bo_tick(BoSim* S, float dt) {
         post->ibuf += I_syn;
         bo_spine_ca_step(syn, I_syn, dt);
         for (int q = 0; q < 15; q++) {
-            syn->cleft[q] *= bo_expf(-dt / syn->tau_clear);
+            syn->cleft[q] *= bo_exp(-dt / syn->tau_clear);
             if (syn->cleft[q] < 0.0f) syn->cleft[q] = 0.0f;
         }
         float Ca_uM = syn->spine_Ca * 1000.0f;
@@ -823,7 +829,7 @@ static void bo_tick(BoSim* S, float dt) {
         float dV = (float)(s->ibuf / C_m * dt);
         if (dV > 50.0f) dV = 50.0f;
         if (dV < -50.0f) dV = -50.0f;
-        s->V = (float)((double)s->V + dV);
+        s->V = BO_ST((double)s->V + dV);
         if (S->spike_count && prev_V <= -40.0f && s->V > -40.0f) S->spike_count[i]++;
         s->ibuf = 0.0f;
         /* voltage clamps (:633-643): the last active clamp of the segment wins */
@@ -846,8 +852,8 @@ static void bo_tick(BoSim* S, float dt) {
 static void load_mod(OMod* o, const BncModifier* m) {
     o->type = m->type;
     o->active_vars = m->active_vars;
-    o->density = (float)m->density;
-    for (int k = 0; k < 8; k++) o->st[k] = (float)m->state[k];
+    o->density = BO_ST(m->density);
+    for (int k = 0; k < 8; k++) o->st[k] = BO_ST(m->state[k]);
 }
 
 BoSim* bo_create(const BncBionData* d, const BncCurrentStimulus* stim, uint32_t n_stim,
@@ -869,7 +875,7 @@ BoSim* bo_create(const BncBionData* d, const BncCurrentStimulus* stim, uint32_t 
     for (int q = 0; q < 15; q++) {
         float ms = mass[q];
         if (ms < 1.0f) ms = 1.0f;
-        S->nt_D[q] = 1.33f * bo_powf(23.0f / ms, 1.0f / 3.0f);
+        S->nt_D[q] = 1.33f * bo_powf(23.0f / ms, 1.0f / 3.0f);   /* powf: types.h:442 */
     }
     for (uint32_t i = 0; i < S->n; i++) {
         const BncSegment* a = &d->segments[i];
@@ -879,8 +885,8 @@ BoSim* bo_create(const BncBionData* d, const BncCurrentStimulus* stim, uint32_t 
         s->length = a->length;
         s->radius = a->radius;
         s->px = a->position.x; s->py = a->position.y; s->pz = a->position.z;
-        s->V = (float)a->V_m;
-        for (int q = 0; q < 8; q++) { s->in[q] = (float)a->intra_ions[q]; s->out[q] = (float)a->extra_ions[q]; }
+        s->V = BO_ST(a->V_m);
+        for (int q = 0; q < 8; q++) { s->in[q] = BO_ST(a->intra_ions[q]); s->out[q] = BO_ST(a->extra_ions[q]); }
         for (int q = 0; q < 15; q++) { s->intra_nt[q] = a->intra_nt[q]; s->nt[q] = a->neurotransmitter[q]; }
         s->atp = a->ATP_level;
         s->temp = a->temperature;
@@ -1029,48 +1035,56 @@ uint32_t bo_release_log_count(const BoSim* S) { return S->log_n; }
 
 /* Field export.  field: 0 V, 1 in[ion], 2 out[ion], 3 atp, 4 temp, 5 txn,
  * 6 intra_nt[idx], 7 nt[idx], 8 modifier state (idx = slot*8+k), 9 spike count. */
-void bo_get_seg_field(const BoSim* S, int field, int idx, float* out) {
-    for (uint32_t i = 0; i < S->n; i++) {
-        const OSeg* s = &S->seg[i];
-        float v = 0.0f;
-        switch (field) {
-            case 0: v = s->V; break;
-            case 1: v = s->in[idx]; break;
-            case 2: v = s->out[idx]; break;
-            case 3: v = s->atp; break;
-            case 4: v = s->temp; break;
-            case 5: v = s->txn; break;
-            case 6: v = s->intra_nt[idx]; break;
-            case 7: v = s->nt[idx]; break;
-            case 8: v = ((idx >> 3) < s->nmod) ? s->mods[idx >> 3].st[idx & 7] : 0.0f; break;
-            case 9: v = (float)S->spike_count[i]; break;
-            case 10: v = bo_vol_f(s); break;   /* the volume the Nernst-Planck updates divide by */
-        }
-        out[i] = v;
+static double bo_seg_value(const BoSim* S, uint32_t i, int field, int idx) {
+    const OSeg* s = &S->seg[i];
+    switch (field) {
+        case 0: return s->V;
+        case 1: return s->in[idx];
+        case 2: return s->out[idx];
+        case 3: return s->atp;
+        case 4: return s->temp;
+        case 5: return s->txn;
+        case 6: return s->intra_nt[idx];
+        case 7: return s->nt[idx];
+        case 8: return ((idx >> 3) < s->nmod) ? s->mods[idx >> 3].st[idx & 7] : 0.0;
+        case 9: return (double)S->spike_count[i];
+        case 10: return bo_vol_f(s);   /* the volume the Nernst-Planck updates divide by */
     }
+    return 0.0;
+}
+void bo_get_seg_field(const BoSim* S, int field, int idx, float* out) {
+    for (uint32_t i = 0; i < S->n; i++) out[i] = (float)bo_seg_value(S, i, field, idx);
+}
+/* the same at the storage precision of the build (exact for the FP64 build) */
+void bo_get_seg_field64(const BoSim* S, int field, int idx, double* out) {
+    for (uint32_t i = 0; i < S->n; i++) out[i] = bo_seg_value(S, i, field, idx);
 }
 
 /* Synapse export.  field: 0 bouton_Ca, 1 spine_Ca, 2 weight, 3 refractory,
  * 4 cleft[idx], 5 receptor state (idx = j*8+k), 6 facilitation, 7 spine_camkii,
- * 8 spine_calcineurin, 9 RRP. */
-void bo_get_syn_field(const BoSim* S, int field, int idx, float* out) {
-    for (uint32_t i = 0; i < S->k; i++) {
-        const OSyn* y = &S->syn[i];
-        float v = 0.0f;
-        switch (field) {
-            case 0: v = y->bouton_Ca; break;
-            case 1: v = y->spine_Ca; break;
-            case 2: v = y->weight; break;
-            case 3: v = (float)y->refractory; break;
-            case 4: v = y->cleft[idx]; break;
-            case 5: v = ((idx >> 3) < y->n_post_r) ? y->post_r[idx >> 3].st[idx & 7] : 0.0f; break;
-            case 6: v = y->facil; break;
-            case 7: v = y->spine_camkii; break;
-            case 8: v = y->spine_calcineurin; break;
-            case 9: v = y->RRP; break;
-        }
-        out[i] = v;
+ * 8 spine_calcineurin, 9 RRP, 10 depression. */
+static double bo_syn_value(const BoSim* S, uint32_t i, int field, int idx) {
+    const OSyn* y = &S->syn[i];
+    switch (field) {
+        case 0: return y->bouton_Ca;
+        case 1: return y->spine_Ca;
+        case 2: return y->weight;
+        case 3: return (double)y->refractory;
+        case 4: return y->cleft[idx];
+        case 5: return ((idx >> 3) < y->n_post_r) ? y->post_r[idx >> 3].st[idx & 7] : 0.0;
+        case 6: return y->facil;
+        case 7: return y->spine_camkii;
+        case 8: return y->spine_calcineurin;
+        case 9: return y->RRP;
+        case 10: return y->depr;
     }
+    return 0.0;
+}
+void bo_get_syn_field(const BoSim* S, int field, int idx, float* out) {
+    for (uint32_t i = 0; i < S->k; i++) out[i] = (float)bo_syn_value(S, i, field, idx);
+}
+void bo_get_syn_field64(const BoSim* S, int field, int idx, double* out) {
+    for (uint32_t i = 0; i < S->k; i++) out[i] = bo_syn_value(S, i, field, idx);
 }
 
 /* Receptor density scale per synapse (the differentiable synaptic weight;
@@ -1085,7 +1099,7 @@ float bo_expf_f(float x) { return bo_expf(x); }
 double bo_log_d(double x) { return bo_log(x); }
 double bo_pow_d(double x, double y) { return bo_pow(x, y); }
 float bo_xorshift_f(uint32_t seed) { return bo_xorshift32_rnd(seed); }
-uint32_t bo_seed_bits(float V) { return bo_vm_seed_bits(V); }
+uint32_t bo_seed_bits(double V) { return bo_vm_seed_bits((bo_real)V); }
 
 /* Known-answer hooks for the tests (reference tests/test_ghk_reference.cpp,
  * tests/test_reference_ionics.cpp): the oracle's GHK flux terms and Nernst

@@ -148,4 +148,16 @@ static inline double bo_pow(double x, double y) {
 
 static inline float bo_powf(float x, float y) { return (float)bo_pow((double)x, (double)y); }
 
+#ifdef BO_LIBM
+/* The FP64-state build (-DBO_FP64 -DBO_LIBM) calls the C library's functions,
+ * exactly as the reference's compiled tick does, so that it can be compared with
+ * the reference bit for bit. */
+#define bo_exp(x) exp(x)
+#define bo_expf(x) expf(x)
+#define bo_log(x) log(x)
+#define bo_logf(x) logf(x)
+#define bo_pow(x, y) pow(x, y)
+#define bo_powf(x, y) powf(x, y)
+#endif
+
 #endif

@@ -19,14 +19,14 @@ static double bo_nav_current(OMod* m, OSeg* s, float dt, int is12) {
     float mtau = is12 ? nav12_m_tau(V) : nav16_m_tau(V);
     float hinf = is12 ? nav12_h_inf(V) : nav16_h_inf(V);
     float htau = is12 ? nav12_h_tau(V) : nav16_h_tau(V);
-    double m_val = minf + (MST(0) - minf) * bo_expf(-dt / mtau);
-    double h_val = hinf + (MST(1) - hinf) * bo_expf(-dt / htau);
+    double m_val = minf + (MST(0) - minf) * bo_exp(-dt / mtau);
+    double h_val = hinf + (MST(1) - hinf) * bo_exp(-dt / htau);
     if (m_val < 0.0f) m_val = 0.0f;
     if (m_val > 1.0f) m_val = 1.0f;
     if (h_val < 0.0f) h_val = 0.0f;
     if (h_val > 1.0f) h_val = 1.0f;
-    m->st[0] = (float)m_val;
-    m->st[1] = (float)h_val;
+    m->st[0] = BO_ST(m_val);
+    m->st[1] = BO_ST(h_val);
     float open_prob = (float)(m_val * m_val * m_val * h_val);
     double ttx = (MST(5) > 0.0f) ? MST(5) : 0.0f;
     open_prob = (float)(open_prob / (1.0f + ttx / (is12 ? 10.0f : 5.0f)));
@@ -39,8 +39,8 @@ static double bo_nav_current(OMod* m, OSeg* s, float dt, int is12) {
     double I_Na = I_A * A_TO_PA;
     double vol = bo_seg_volume(s);
     double cpv = FARADAY_CONST * vol / 1000.0;
-    s->in[0] = (float)(SIN(0) - (I_Na * dt) / cpv);
-    s->out[0] = (float)(SOUT(0) + (I_Na * dt) / (cpv * EXTRA_VOLUME_RATIO));
+    s->in[0] = BO_ST(SIN(0) - (I_Na * dt) / cpv);
+    s->out[0] = BO_ST(SOUT(0) + (I_Na * dt) / (cpv * EXTRA_VOLUME_RATIO));
     bo_clamp_ions(s->in);
     bo_clamp_ions(s->out);
     return -I_Na;
@@ -55,12 +55,12 @@ static double bo_cav13_current(OMod* m, OSeg* s, float dt) {
     double gamma_ps = (MST(2) > 0.0f) ? MST(2) : 25.0f;
     float m_inf = (float)(1.0f / (1.0f + bo_exp(-(V - Vhalf) / (k + 1e-6f))));
     float tau_m = 2.0f;
-    m->st[0] = (float)(MST(0) + (m_inf - MST(0)) * dt / tau_m);
+    m->st[0] = BO_ST(MST(0) + (m_inf - MST(0)) * dt / tau_m);
     float Ca = (float)(SIN(2) * MM_TO_UM);
-    float h_inf = 1.0f / (1.0f + bo_expf((V + 52.0f) / 8.0f));
+    float h_inf = 1.0f / (1.0f + bo_exp((V + 52.0f) / 8.0f));
     h_inf *= 1.0f / (1.0f + Ca / 3.0f);
     float tau_h = 100.0f;
-    m->st[1] = (float)(MST(1) + (h_inf - MST(1)) * dt / tau_h);
+    m->st[1] = BO_ST(MST(1) + (h_inf - MST(1)) * dt / tau_h);
     if (MST(0) < 0.0f) m->st[0] = 0.0f;
     if (MST(1) < 0.0f) m->st[1] = 0.0f;
     if (MST(0) > 1.0f) m->st[0] = 1.0f;
@@ -74,8 +74,8 @@ static double bo_cav13_current(OMod* m, OSeg* s, float dt) {
     double I_Ca = I_A * A_TO_PA;
     double vol = bo_seg_volume(s);
     double cpm = FARADAY_CONST * vol / 1000.0;
-    s->in[2] = (float)(SIN(2) - (I_Ca * dt) / (2.0f * cpm));
-    s->out[2] = (float)(SOUT(2) - (I_Ca * dt) / (2.0f * cpm * EXTRA_VOLUME_RATIO));
+    s->in[2] = BO_ST(SIN(2) - (I_Ca * dt) / (2.0f * cpm));
+    s->out[2] = BO_ST(SOUT(2) - (I_Ca * dt) / (2.0f * cpm * EXTRA_VOLUME_RATIO));
     bo_clamp_ions(s->in);
     bo_clamp_ions(s->out);
     return -I_Ca;
@@ -85,10 +85,10 @@ static double bo_cav13_current(OMod* m, OSeg* s, float dt) {
 static double bo_cav21_current(OMod* m, OSeg* s, float dt) {
     float V = s->V;
     float m_inf = cav21_m_inf(V);
-    m->st[0] = (float)(MST(0) + (m_inf - MST(0)) * dt / 1.0f);
+    m->st[0] = BO_ST(MST(0) + (m_inf - MST(0)) * dt / 1.0f);
     float Ca = (float)(SIN(2) * MM_TO_UM);
     float h_inf = cav21_h_inf(V, Ca);
-    m->st[1] = (float)(MST(1) + (h_inf - MST(1)) * dt / 300.0f);
+    m->st[1] = BO_ST(MST(1) + (h_inf - MST(1)) * dt / 300.0f);
     if (MST(0) < 0.0f) m->st[0] = 0.0f;
     if (MST(1) < 0.0f) m->st[1] = 0.0f;
     if (MST(0) > 1.0f) m->st[0] = 1.0f;
@@ -111,10 +111,10 @@ static double bo_nak_pump_current(OMod* m, OSeg* s, float dt) {
     if (k_avail < 0.0f) k_avail = 0.0f;
     float max_t = (na_avail < k_avail) ? na_avail : k_avail;
     if (transport > max_t) transport = max_t;
-    s->in[0] = (float)(SIN(0) - 3.0f * transport);
-    s->out[0] = (float)(SOUT(0) + 3.0f * transport / EXTRA_VOLUME_RATIO);
-    s->in[1] = (float)(SIN(1) + 2.0f * transport);
-    s->out[1] = (float)(SOUT(1) - 2.0f * transport / EXTRA_VOLUME_RATIO);
+    s->in[0] = BO_ST(SIN(0) - 3.0f * transport);
+    s->out[0] = BO_ST(SOUT(0) + 3.0f * transport / EXTRA_VOLUME_RATIO);
+    s->in[1] = BO_ST(SIN(1) + 2.0f * transport);
+    s->out[1] = BO_ST(SOUT(1) - 2.0f * transport / EXTRA_VOLUME_RATIO);
     bo_clamp_ions(s->in);
     bo_clamp_ions(s->out);
     s->atp -= I_pump * dt * 1e-8f;
@@ -124,8 +124,8 @@ static double bo_nak_pump_current(OMod* m, OSeg* s, float dt) {
 
 /* shared K-channel ion bookkeeping: intra K -= I*dt/cpv, extra K += .../EVR, clamp extra */
 static inline void bo_k_flux(OSeg* s, double I_K, float dt, double cpv) {
-    s->in[1] = (float)(SIN(1) - (I_K * dt) / cpv);
-    s->out[1] = (float)(SOUT(1) + (I_K * dt) / (cpv * EXTRA_VOLUME_RATIO));
+    s->in[1] = BO_ST(SIN(1) - (I_K * dt) / cpv);
+    s->out[1] = BO_ST(SOUT(1) + (I_K * dt) / (cpv * EXTRA_VOLUME_RATIO));
     bo_clamp_ions(s->out);
 }
 
@@ -138,16 +138,16 @@ static double bo_kv42_current(OMod* m, OSeg* s, float dt) {
     double gamma_ps = (MST(2) > 0.0f) ? MST(2) : 5.0f;
     float m_inf = (float)(1.0f / (1.0f + bo_exp(-(V - Vhalf) / (k + 1e-6f))));
     float tau_m = 1.5f;
-    m->st[0] = (float)(MST(0) + (m_inf - MST(0)) * dt / tau_m);
-    float h_inf = 1.0f / (1.0f + bo_expf((V + 65.0f) / 8.0f));
+    m->st[0] = BO_ST(MST(0) + (m_inf - MST(0)) * dt / tau_m);
+    float h_inf = 1.0f / (1.0f + bo_exp((V + 65.0f) / 8.0f));
     float tau_h = kv42_h_tau(V);
-    m->st[1] = (float)(MST(1) + (h_inf - MST(1)) * dt / tau_h);
+    m->st[1] = BO_ST(MST(1) + (h_inf - MST(1)) * dt / tau_h);
     if (MST(0) < 0.0f) m->st[0] = 0.0f;
     if (MST(1) < 0.0f) m->st[1] = 0.0f;
     if (MST(0) > 1.0f) m->st[0] = 1.0f;
     if (MST(1) > 1.0f) m->st[1] = 1.0f;
     float camkii = 0.0f;   /* no CaMKII modifiers in supported networks */
-    m->st[3] = (float)(MST(3) + (camkii * 0.5f - MST(3)) * dt / 5000.0f);
+    m->st[3] = BO_ST(MST(3) + (camkii * 0.5f - MST(3)) * dt / 5000.0f);
     if (MST(3) < 0.0f) m->st[3] = 0.0f;
     if (MST(3) > 1.0f) m->st[3] = 1.0f;
     double gamma_eff = gamma_ps * (1.0f - MST(3) * 0.7f);
@@ -169,14 +169,14 @@ static double bo_kv31_current(OMod* m, OSeg* s, float dt) {
     float V = s->V;
     float area = bo_eff_area(m, s);
     float Vhalf = 10.0f, k = 10.0f, gamma_ps = 27.0f;
-    float m_inf = 1.0f / (1.0f + bo_expf(-(V - Vhalf) / (k + 1e-6f)));
+    float m_inf = 1.0f / (1.0f + bo_exp(-(V - Vhalf) / (k + 1e-6f)));
     float tau_m = 1.0f;
-    m->st[0] = (float)(MST(0) + (m_inf - MST(0)) * dt / tau_m);
+    m->st[0] = BO_ST(MST(0) + (m_inf - MST(0)) * dt / tau_m);
     if (MST(0) < 0.0f) m->st[0] = 0.0f;
     if (MST(0) > 1.0f) m->st[0] = 1.0f;
-    float h_inf = 1.0f / (1.0f + bo_expf((V + 30.0f) / 6.0f));
+    float h_inf = 1.0f / (1.0f + bo_exp((V + 30.0f) / 6.0f));
     float tau_h = 2000.0f;
-    m->st[1] = (float)(MST(1) + (h_inf - MST(1)) * dt / tau_h);
+    m->st[1] = BO_ST(MST(1) + (h_inf - MST(1)) * dt / tau_h);
     if (MST(1) < 0.0f) m->st[1] = 0.0f;
     if (MST(1) > 1.0f) m->st[1] = 1.0f;
     float K_i = s->in[1];
@@ -188,7 +188,7 @@ static double bo_kv31_current(OMod* m, OSeg* s, float dt) {
     float pkc = 0.0f;
     float k_phos = 5.6e-6f;
     float k_dephos = 1e-4f;
-    m->st[2] = (float)(MST(2) + (k_phos * pkc * (1.0f - MST(2)) - k_dephos * MST(2)) * dt);
+    m->st[2] = BO_ST(MST(2) + (k_phos * pkc * (1.0f - MST(2)) - k_dephos * MST(2)) * dt);
     if (MST(2) < 0.0f) m->st[2] = 0.0f;
     if (MST(2) > 1.0f) m->st[2] = 1.0f;
     open_prob *= (1.0f - 0.27f * MST(2));
@@ -220,8 +220,8 @@ static double bo_cav31_current(OMod* m, OSeg* s, float dt) {
     if (m_val > 1.0f) m_val = 1.0f;
     if (h_val < 0.0f) h_val = 0.0f;
     if (h_val > 1.0f) h_val = 1.0f;
-    m->st[0] = (float)m_val;
-    m->st[1] = (float)h_val;
+    m->st[0] = BO_ST(m_val);
+    m->st[1] = BO_ST(h_val);
     float open_prob = (float)(m_val * m_val * m_val * h_val);
     double ni = (MST(3) > 0.0f) ? MST(3) : 0.0f;
     double mib = (MST(4) > 0.0f) ? MST(4) : 0.0f;
@@ -235,7 +235,7 @@ static double bo_cav31_current(OMod* m, OSeg* s, float dt) {
     double I_CaT = I_A * A_TO_PA;
     float volume = (float)bo_seg_volume(s);
     float charge_per_mole = (float)(FARADAY_CONST * volume / 1000.0);
-    s->in[2] = (float)(SIN(2) - (I_CaT * dt) / (2.0f * charge_per_mole));
+    s->in[2] = BO_ST(SIN(2) - (I_CaT * dt) / (2.0f * charge_per_mole));
     return -I_CaT;
 }
 
@@ -259,8 +259,8 @@ static double bo_pmca_current(OMod* m, OSeg* s, float dt) {
     float ca_avail = (float)(SIN(2) - 1e-9f);
     if (ca_avail < 0.0f) ca_avail = 0.0f;
     if (transport > ca_avail) transport = ca_avail;
-    s->in[2] = (float)(SIN(2) - transport);
-    s->out[2] = (float)(SOUT(2) + transport / EXTRA_VOLUME_RATIO);
+    s->in[2] = BO_ST(SIN(2) - transport);
+    s->out[2] = BO_ST(SOUT(2) + transport / EXTRA_VOLUME_RATIO);
     bo_clamp_ions(s->in);
     s->atp -= I_pump * dt * 1e-8f;
     if (s->atp < 0.0f) s->atp = 0.0f;
@@ -282,10 +282,10 @@ static double bo_ncx_current(OMod* m, OSeg* s, float dt) {
     float transport = (float)(I_ncx * dt / cpv);
     if (transport > Ca_i) transport = Ca_i;
     if (transport < -Na_i / 3.0f) transport = -Na_i / 3.0f;
-    s->in[2] = (float)(SIN(2) - transport);
-    s->out[2] = (float)(SOUT(2) + transport / EXTRA_VOLUME_RATIO);
-    s->in[0] = (float)(SIN(0) + 3.0f * transport);
-    s->out[0] = (float)(SOUT(0) - 3.0f * transport / EXTRA_VOLUME_RATIO);
+    s->in[2] = BO_ST(SIN(2) - transport);
+    s->out[2] = BO_ST(SOUT(2) + transport / EXTRA_VOLUME_RATIO);
+    s->in[0] = BO_ST(SIN(0) + 3.0f * transport);
+    s->out[0] = BO_ST(SOUT(0) - 3.0f * transport / EXTRA_VOLUME_RATIO);
     bo_clamp_ions(s->in);
     return I_ncx;
 }
@@ -321,10 +321,10 @@ static double bo_kcc2_current(OMod* m, OSeg* s, float dt) {
         if (mag > min_avail) mag = min_avail;
         dconc = -mag;
     }
-    s->in[1] = (float)(SIN(1) - dconc);
-    s->in[3] = (float)(SIN(3) - dconc);
-    s->out[1] = (float)(SOUT(1) + dconc / EXTRA_VOLUME_RATIO);
-    s->out[3] = (float)(SOUT(3) + dconc / EXTRA_VOLUME_RATIO);
+    s->in[1] = BO_ST(SIN(1) - dconc);
+    s->in[3] = BO_ST(SIN(3) - dconc);
+    s->out[1] = BO_ST(SOUT(1) + dconc / EXTRA_VOLUME_RATIO);
+    s->out[3] = BO_ST(SOUT(3) + dconc / EXTRA_VOLUME_RATIO);
     bo_clamp_ions(s->in);
     return 0.0f;
 }
@@ -340,7 +340,7 @@ static double bo_ca_buffer_current(OMod* m, OSeg* s, float dt) {
     if (Ca_bound <= 0.0f && B_total > 0.0f) {
         float Ca_free0 = s->in[2];
         Ca_bound = B_total * Ca_free0 / (Ca_free0 + K_d);
-        m->st[1] = (float)Ca_bound;
+        m->st[1] = BO_ST(Ca_bound);
     }
     float Ca_free = s->in[2];
     if (Ca_free < 1e-9f) Ca_free = 1e-9f;
@@ -350,14 +350,14 @@ static double bo_ca_buffer_current(OMod* m, OSeg* s, float dt) {
     Ca_bound += dCa_bound;
     if (Ca_bound < 0.0f) Ca_bound = 0.0f;
     if (Ca_bound > B_total) Ca_bound = B_total;
-    s->in[2] = (float)(SIN(2) - dCa_bound);
+    s->in[2] = BO_ST(SIN(2) - dCa_bound);
     if (SIN(2) < 1e-9f) {
         float deficit = (float)(1e-9f - SIN(2));
         s->in[2] = 1e-9f;
         Ca_bound -= deficit;
         if (Ca_bound < 0.0f) Ca_bound = 0.0f;
     }
-    m->st[1] = (float)Ca_bound;
+    m->st[1] = BO_ST(Ca_bound);
     return 0.0f;
 }
 
@@ -375,7 +375,7 @@ static double bo_sk_current(OMod* m, OSeg* s, float dt) {
     open_prob += (p_inf - open_prob) * dt / tau;
     if (open_prob < 0.0f) open_prob = 0.0f;
     if (open_prob > 1.0f) open_prob = 1.0f;
-    m->st[0] = (float)open_prob;
+    m->st[0] = BO_ST(open_prob);
     float K_i = s->in[1], K_o = s->out[1];
     double P_single = bo_ghk_P((float)gamma_ps, 1.0f, GHK_CBAR_K_MM);
     double flux = bo_ghk_mono(V, K_i, K_o);
@@ -383,8 +383,8 @@ static double bo_sk_current(OMod* m, OSeg* s, float dt) {
     float I_K = (float)(I_A * A_TO_PA);
     double vol = bo_seg_volume(s);
     double cpv = FARADAY_CONST * vol / 1000.0f;
-    s->in[1] = (float)(SIN(1) - (I_K * dt) / cpv);
-    s->out[1] = (float)(SOUT(1) + (I_K * dt) / (cpv * EXTRA_VOLUME_RATIO));
+    s->in[1] = BO_ST(SIN(1) - (I_K * dt) / cpv);
+    s->out[1] = BO_ST(SOUT(1) + (I_K * dt) / (cpv * EXTRA_VOLUME_RATIO));
     bo_clamp_ions(s->out);
     return -I_K;
 }
@@ -401,7 +401,7 @@ static double bo_bk_current(OMod* m, OSeg* s, float dt) {
     open_prob += (po_inf - open_prob) * dt / tau_ch;
     if (open_prob < 0.0f) open_prob = 0.0f;
     if (open_prob > 1.0f) open_prob = 1.0f;
-    m->st[0] = (float)open_prob;
+    m->st[0] = BO_ST(open_prob);
     float K_i = s->in[1], K_o = s->out[1];
     double P_single = bo_ghk_P((float)gamma_ps, 1.0f, GHK_CBAR_K_MM);
     double flux = bo_ghk_mono(V, K_i, K_o);
@@ -409,8 +409,8 @@ static double bo_bk_current(OMod* m, OSeg* s, float dt) {
     float I_K = (float)(I_A * A_TO_PA);
     double vol = bo_seg_volume(s);
     double cpv = FARADAY_CONST * vol / 1000.0f;
-    s->in[1] = (float)(SIN(1) - (I_K * dt) / cpv);
-    s->out[1] = (float)(SOUT(1) + (I_K * dt) / (cpv * EXTRA_VOLUME_RATIO));
+    s->in[1] = BO_ST(SIN(1) - (I_K * dt) / cpv);
+    s->out[1] = BO_ST(SOUT(1) + (I_K * dt) / (cpv * EXTRA_VOLUME_RATIO));
     bo_clamp_ions(s->out);
     return -I_K;
 }
@@ -429,7 +429,7 @@ static double bo_nap_current(OMod* m, OSeg* s, float dt) {
     m_val += (m_inf - m_val) * dt / tau_m;
     if (m_val < 0.0f) m_val = 0.0f;
     if (m_val > 1.0f) m_val = 1.0f;
-    m->st[0] = (float)m_val;
+    m->st[0] = BO_ST(m_val);
     float Na_i = s->in[0], Na_o = s->out[0];
     double P_single = bo_ghk_P((float)gamma_ps, 1.0f, GHK_CBAR_NA_MM);
     double flux = bo_ghk_mono(V, Na_i, Na_o);
@@ -437,7 +437,7 @@ static double bo_nap_current(OMod* m, OSeg* s, float dt) {
     float I_Na = (float)(I_A * A_TO_PA);
     double vol = bo_seg_volume(s);
     double cpv = FARADAY_CONST * vol / 1000.0f;
-    s->in[0] = (float)(SIN(0) - (I_Na * dt) / cpv);
+    s->in[0] = BO_ST(SIN(0) - (I_Na * dt) / cpv);
     bo_clamp_ions(s->in);
     return -I_Na;
 }
@@ -493,7 +493,7 @@ static double bo_kv7_current(OMod* m, OSeg* s, float dt) {
     m_val += (m_inf - m_val) * dt / tau_m;
     if (m_val < 0.0f) m_val = 0.0f;
     if (m_val > 1.0f) m_val = 1.0f;
-    m->st[0] = (float)m_val;
+    m->st[0] = BO_ST(m_val);
     if (pip2 < 0.01f) return 0.0f;
     float K_i = s->in[1];
     float K_o = s->out[1];
@@ -522,7 +522,7 @@ static double bo_kvdr_current(OMod* m, OSeg* s, float dt) {
     m_val += (m_inf - m_val) * dt / (tau + 1e-6f);
     if (m_val < 0.0f) m_val = 0.0f;
     if (m_val > 1.0f) m_val = 1.0f;
-    m->st[0] = (float)m_val;
+    m->st[0] = BO_ST(m_val);
     float K_i = s->in[1];
     float K_o = s->out[1];
     double P_single = bo_ghk_P(12.0f, 1.0f, GHK_CBAR_K_MM);
@@ -531,8 +531,8 @@ static double bo_kvdr_current(OMod* m, OSeg* s, float dt) {
     double I_K = I_A * A_TO_PA;
     double vol = bo_seg_volume(s);
     float charge_per_mole_vol = (float)(FARADAY_CONST * vol / 1000.0);
-    s->in[1] = (float)(SIN(1) - (I_K * dt) / charge_per_mole_vol);
-    s->out[1] = (float)(SOUT(1) + (I_K * dt) / (charge_per_mole_vol * EXTRA_VOLUME_RATIO));
+    s->in[1] = BO_ST(SIN(1) - (I_K * dt) / charge_per_mole_vol);
+    s->out[1] = BO_ST(SOUT(1) + (I_K * dt) / (charge_per_mole_vol * EXTRA_VOLUME_RATIO));
     bo_clamp_ions(s->in);
     bo_clamp_ions(s->out);
     return -I_K;
@@ -550,7 +550,7 @@ static double bo_hcn1_current(OMod* m, OSeg* s, float dt) {
     float camp = 0.1f;  /* segment_camp_um: no cAMP/PKA modifier -> basal 0.1 uM (units.h:324) */
     float Ve = V_half + 15.0f * camp / (camp + 0.5f);
     float mv = m->st[0];
-    float mi = 1.0f / (1.0f + bo_expf(((float)V - Ve) / k));
+    float mi = 1.0f / (1.0f + bo_exp(((float)V - Ve) / k));
     float tau_eff = (V < Ve) ? (float)(tau_open * bo_exp((V - Ve) / 15.0f)) : tau_close;
     mv += (mi - mv) * dt / tau_eff;
     if (mv < 0.0f) mv = 0.0f;
@@ -565,10 +565,10 @@ static double bo_hcn1_current(OMod* m, OSeg* s, float dt) {
     double Ik = P_K * flux_K * N * mv * A_TO_PA;
     double vol = bo_seg_volume(s);
     double cpm = FARADAY_CONST * vol / 1000.0;
-    s->in[0] = (float)(SIN(0) - (In * dt) / cpm);
-    s->in[1] = (float)(SIN(1) - (Ik * dt) / cpm);
-    s->out[0] = (float)(SOUT(0) + (In * dt) / (cpm * EXTRA_VOLUME_RATIO));
-    s->out[1] = (float)(SOUT(1) + (Ik * dt) / (cpm * EXTRA_VOLUME_RATIO));
+    s->in[0] = BO_ST(SIN(0) - (In * dt) / cpm);
+    s->in[1] = BO_ST(SIN(1) - (Ik * dt) / cpm);
+    s->out[0] = BO_ST(SOUT(0) + (In * dt) / (cpm * EXTRA_VOLUME_RATIO));
+    s->out[1] = BO_ST(SOUT(1) + (Ik * dt) / (cpm * EXTRA_VOLUME_RATIO));
     bo_clamp_ions(s->in);
     bo_clamp_ions(s->out);
     return -(In + Ik);
@@ -587,12 +587,12 @@ static double bo_nalcn_current(OMod* m, OSeg* s, float dt) {
     float Ica = (float)(P_Ca * bo_ghk_div(V, SIN(2), SOUT(2)) * N * A_TO_PA);
     double vol = bo_seg_volume(s);
     double cpm = FARADAY_CONST * vol / 1000.0;
-    s->in[0] = (float)(SIN(0) - (Ina * dt) / cpm);
-    s->in[1] = (float)(SIN(1) - (Ik * dt) / cpm);
-    s->in[2] = (float)(SIN(2) - (Ica * dt) / (2.0f * cpm));
-    s->out[0] = (float)(SOUT(0) + (Ina * dt) / (cpm * EXTRA_VOLUME_RATIO));
-    s->out[1] = (float)(SOUT(1) + (Ik * dt) / (cpm * EXTRA_VOLUME_RATIO));
-    s->out[2] = (float)(SOUT(2) + (Ica * dt) / (2.0f * cpm * EXTRA_VOLUME_RATIO));
+    s->in[0] = BO_ST(SIN(0) - (Ina * dt) / cpm);
+    s->in[1] = BO_ST(SIN(1) - (Ik * dt) / cpm);
+    s->in[2] = BO_ST(SIN(2) - (Ica * dt) / (2.0f * cpm));
+    s->out[0] = BO_ST(SOUT(0) + (Ina * dt) / (cpm * EXTRA_VOLUME_RATIO));
+    s->out[1] = BO_ST(SOUT(1) + (Ik * dt) / (cpm * EXTRA_VOLUME_RATIO));
+    s->out[2] = BO_ST(SOUT(2) + (Ica * dt) / (2.0f * cpm * EXTRA_VOLUME_RATIO));
     bo_clamp_ions(s->in);
     bo_clamp_ions(s->out);
     return -(Ina - Ik + Ica);
@@ -613,7 +613,7 @@ static double bo_ionotropic(OMod* m, OSeg* s, float dt, float gamma_ps, float EC
     float r_inf = nt / (nt + EC50);
     float r = m->st[0];
     float tau = (r_inf > r) ? tau_rise : tau_decay;
-    m->st[0] = (float)(MST(0) + (r_inf - r) * dt / tau);
+    m->st[0] = BO_ST(MST(0) + (r_inf - r) * dt / tau);
     if (MST(0) < 0.0f) m->st[0] = 0.0f;
     if (MST(0) > 1.0f) m->st[0] = 1.0f;
     float open_prob = m->st[0];
@@ -633,7 +633,7 @@ static double bo_ionotropic(OMod* m, OSeg* s, float dt, float gamma_ps, float EC
         double P_Cl = bo_ghk_P(p_gamma_ps, 1.0f, GHK_CBAR_CL_MM);
         double flux_Cl = bo_ghk_anion(V, SIN(3), SOUT(3));
         double I_Cl = P_Cl * flux_Cl * N * open_prob * mod_scale * A_TO_PA;
-        s->in[3] = (float)(SIN(3) + (I_Cl * dt) / cpm);
+        s->in[3] = BO_ST(SIN(3) + (I_Cl * dt) / cpm);
         bo_clamp_ions(s->in);
         return -I_Cl;
     }
@@ -642,12 +642,12 @@ static double bo_ionotropic(OMod* m, OSeg* s, float dt, float gamma_ps, float EC
     double I_Na = P_Na * bo_ghk_mono(V, SIN(0), SOUT(0)) * N * open_prob * mod_scale * A_TO_PA;
     double I_K = P_K * bo_ghk_mono(V, SIN(1), SOUT(1)) * N * open_prob * mod_scale * A_TO_PA;
     I_total = I_Na + I_K;
-    s->in[0] = (float)(SIN(0) - (I_Na * dt) / cpm);
-    s->in[1] = (float)(SIN(1) - (I_K * dt) / cpm);
+    s->in[0] = BO_ST(SIN(0) - (I_Na * dt) / cpm);
+    s->in[1] = BO_ST(SIN(1) - (I_K * dt) / cpm);
     if (P_Ca_ratio > 0.0f) {
         double I_Ca = P_Ca * bo_ghk_div(V, SIN(2), SOUT(2)) * N * open_prob * mod_scale * A_TO_PA;
         I_total += I_Ca;
-        s->in[2] = (float)(SIN(2) - (I_Ca * dt) / (2.0f * cpm));
+        s->in[2] = BO_ST(SIN(2) - (I_Ca * dt) / (2.0f * cpm));
     }
     bo_clamp_ions(s->in);
     return -I_total;
@@ -658,7 +658,7 @@ static double bo_nmda_cdi_coagonist(OMod* m, OSeg* s, float dt) {
     double Ca_uM = SIN(2) * MM_TO_UM;
     double cdi_inf = 1.0 - 0.8f * Ca_uM / (Ca_uM + 1.0f);
     float tau = (cdi_inf < MST(2)) ? 500.0f : 9000.0f;
-    m->st[2] = (float)(MST(2) + (cdi_inf - MST(2)) * dt / tau);
+    m->st[2] = BO_ST(MST(2) + (cdi_inf - MST(2)) * dt / tau);
     if (MST(2) < 0.0f) m->st[2] = 0.0f;
     if (MST(2) > 1.0f) m->st[2] = 1.0f;
     float coagonist = 10.0f / (10.0f + 1.0f);

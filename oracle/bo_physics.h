@@ -32,11 +32,24 @@
 #define GHK_CBAR_CA_MM 0.12775f
 #define GHK_CBAR_CL_MM 36.20f
 
+/* State storage type.  The oracle proper stores FP32 state (bo_real = float).
+ * Built with -DBO_FP64 the same source stores double, as the reference's Segment
+ * and Modifier do (types.h:451-500), and with -DBO_LIBM it calls the C library's
+ * elementary functions as the reference does: that build (oracle/liboracle64.so)
+ * must then reproduce the reference's own core_run_tick, which pins this
+ * restatement's operation order independently of FP32 rounding. */
+#ifdef BO_FP64
+typedef double bo_real;
+#else
+typedef float bo_real;
+#endif
+#define BO_ST(x) ((bo_real)(x))
+
 typedef struct {
     uint8_t type;
     uint8_t active_vars;
-    float density;
-    float st[8];
+    bo_real density;
+    bo_real st[8];
 } OMod;
 
 typedef struct {
@@ -44,8 +57,8 @@ typedef struct {
     uint8_t type;
     float length, radius;
     float px, py, pz;
-    float V;
-    float in[8], out[8];
+    bo_real V;
+    bo_real in[8], out[8];
     float intra_nt[15], nt[15];
     float atp, temp, txn;
     double ibuf;
@@ -79,9 +92,9 @@ static inline float bo_eff_area(const OMod* m, const OSeg* s) {
     return bo_seg_area(s);
 }
 /* modifier_helpers.h:1117-1121: arrays are double in the reference */
-static inline void bo_clamp_ions(float* arr) {
+static inline void bo_clamp_ions(bo_real* arr) {
     for (int i = 0; i < 7; i++)
-        if ((double)arr[i] < 1e-9) arr[i] = (float)1e-9;
+        if ((double)arr[i] < 1e-9) arr[i] = BO_ST(1e-9);
 }
 /* run_tick_common.h:274-312 */
 static inline double bo_ghk_mono(double V, double c_in, double c_out) {
@@ -135,16 +148,16 @@ static inline void bo_partial_P(float gamma_pS, float fNa, float fK, float fCa,
 static inline float bo_nernst(float intra, float extra, float valence) {
     if (intra < 1e-9f) intra = 1e-9f;
     if (extra < 1e-9f) extra = 1e-9f;
-    return (float)((GAS_CONST * CELSIUS_37) / (valence * FARADAY_CONST) * bo_logf(extra / intra) * 1000.0f);
+    return (float)((GAS_CONST * CELSIUS_37) / (valence * FARADAY_CONST) * bo_log(extra / intra) * 1000.0f);
 }
 /* modifier_helpers.h:132-135 */
 static inline float bo_vtrap(float x, float y) {
     if (fabsf(x / y) < 1e-6f) return y * (1.0f - x / (2.0f * y));
-    return x / (1.0f - bo_expf(-x / y));
+    return x / (1.0f - bo_exp(-x / y));
 }
 /* modifier_helpers.h:1090-1095 */
-static inline float bo_bz_act(float V, float vh, float k) { return 1.0f / (1.0f + bo_expf(-(V - vh) / k)); }
-static inline float bo_bz_inact(float V, float vh, float k) { return 1.0f / (1.0f + bo_expf((V - vh) / k)); }
+static inline float bo_bz_act(float V, float vh, float k) { return 1.0f / (1.0f + bo_exp(-(V - vh) / k)); }
+static inline float bo_bz_inact(float V, float vh, float k) { return 1.0f / (1.0f + bo_exp((V - vh) / k)); }
 
 /* ---- gating helpers (modifier_helpers.h:145-215, 264-271, 468-472, 689-702, 1008-1018, 882-892, 909-913, 954-967, 1137-1170, 1188-1210) ---- */
 static inline float nav16_am(float V) { return 0.182f * bo_vtrap(V + 43.0f, 6.0f); }
@@ -153,7 +166,7 @@ static inline float nav16_ah(float V) { return 0.024f * bo_vtrap(V + 50.0f, 5.0f
 static inline float nav16_bh(float V) { return 0.0091f * bo_vtrap(-(V + 75.0f), 5.0f); }
 static inline float nav16_m_inf(float V) { float a = nav16_am(V), b = nav16_bm(V); return a / (a + b); }
 static inline float nav16_m_tau(float V) { return 1.0f / (nav16_am(V) + nav16_bm(V)); }
-static inline float nav16_h_inf(float V) { return 1.0f / (1.0f + bo_expf((V + 72.0f) / 6.2f)); }
+static inline float nav16_h_inf(float V) { return 1.0f / (1.0f + bo_exp((V + 72.0f) / 6.2f)); }
 static inline float nav16_h_tau(float V) { return 1.0f / (nav16_ah(V) + nav16_bh(V)); }
 static inline float nav12_am(float V) { return 0.182f * bo_vtrap(V + 23.0f, 6.0f); }
 static inline float nav12_bm(float V) { return 0.124f * bo_vtrap(-(V + 23.0f), 6.0f); }
@@ -161,36 +174,36 @@ static inline float nav12_ah(float V) { return 0.024f * bo_vtrap(V + 41.5f, 5.0f
 static inline float nav12_bh(float V) { return 0.0091f * bo_vtrap(-(V + 66.5f), 5.0f); }
 static inline float nav12_m_inf(float V) { float a = nav12_am(V), b = nav12_bm(V); return a / (a + b); }
 static inline float nav12_m_tau(float V) { return 1.0f / (nav12_am(V) + nav12_bm(V)); }
-static inline float nav12_h_inf(float V) { return 1.0f / (1.0f + bo_expf((V + 63.5f) / 6.2f)); }
+static inline float nav12_h_inf(float V) { return 1.0f / (1.0f + bo_exp((V + 63.5f) / 6.2f)); }
 static inline float nav12_h_tau(float V) { return 1.0f / (nav12_ah(V) + nav12_bh(V)); }
-static inline float cav21_m_inf(float V) { return 1.0f / (1.0f + bo_expf(-(V - -15.0f) / (6.0f + 1e-6f))); }
+static inline float cav21_m_inf(float V) { return 1.0f / (1.0f + bo_exp(-(V - -15.0f) / (6.0f + 1e-6f))); }
 static inline float cav21_h_inf(float V, float Ca_uM) {
-    float h = 1.0f / (1.0f + bo_expf((V - -50.0f) / 8.0f));
+    float h = 1.0f / (1.0f + bo_exp((V - -50.0f) / 8.0f));
     h *= 1.0f / (1.0f + Ca_uM / 3.0f);
     return h;
 }
 static inline float kv42_h_tau(float V) {
-    return 15.0f + (170.0f - 15.0f) / (1.0f + bo_expf((V - -60.0f) / 8.0f));
+    return 15.0f + (170.0f - 15.0f) / (1.0f + bo_exp((V - -60.0f) / 8.0f));
 }
 static inline float cav31_h_tau(float V) {
-    return 25.0f + (250.0f - 25.0f) / (1.0f + bo_expf((V - -65.0f) / 8.0f));
+    return 25.0f + (250.0f - 25.0f) / (1.0f + bo_exp((V - -65.0f) / 8.0f));
 }
 static inline float cav31_m_tau(float V) {
     float dv = V - -20.0f;
-    float g = bo_expf(-(dv * dv) / (2.0f * 22.0f * 22.0f));
+    float g = bo_exp(-(dv * dv) / (2.0f * 22.0f * 22.0f));
     return 1.25f + (15.0f - 1.25f) * g;
 }
 static inline float kv_dr_m_tau(float V, float V_half) {
-    float tau = 14.6f * bo_expf(-(V - V_half) / 30.1f);
+    float tau = 14.6f * bo_exp(-(V - V_half) / 30.1f);
     if (tau < 0.3f) tau = 0.3f;
     if (tau > 200.0f) tau = 200.0f;
     return tau;
 }
 static inline float kir_f_open(float V) {
     float Vn = (float)(FARADAY_CONST * V * 0.001f / (GAS_CONST * CELSIUS_37));
-    float Kd_Mg = 0.3f * bo_expf(-0.6f * 2.0f * Vn);
+    float Kd_Mg = 0.3f * bo_exp(-0.6f * 2.0f * Vn);
     float mg_block = 0.5f / Kd_Mg;
-    float Kd_spm = 0.0775f * bo_expf(-0.5f * 4.0f * Vn);
+    float Kd_spm = 0.0775f * bo_exp(-0.5f * 4.0f * Vn);
     float r = 0.001f / Kd_spm;
     float spm_block = 0.0f, rk = r;
     for (int k = 0; k < 3; k++) { spm_block += rk; rk *= r; }
@@ -199,12 +212,12 @@ static inline float kir_f_open(float V) {
 static inline float sk_p_inf(float Ca) {
     if (Ca < 1e-9f) Ca = 1e-9f;
     float r = 0.0004f / Ca;
-    return 1.0f / (1.0f + bo_powf(r, 4.0f));
+    return 1.0f / (1.0f + bo_pow(r, 4.0f));
 }
 static inline float bk_ha_po(float V_mV, float Ca) {
     float Vn = (float)(FARADAY_CONST * V_mV * MV_TO_V / (GAS_CONST * CELSIUS_37));
-    float J = 0.104f * bo_expf(0.55f * Vn);
-    float L = 3.7e-8f * bo_expf(0.30f * Vn);
+    float J = 0.104f * bo_exp(0.55f * Vn);
+    float L = 3.7e-8f * bo_exp(0.30f * Vn);
     if (Ca < 0.0f) Ca = 0.0f;
     float K = Ca / 0.044f;
     float o = 1.0f + K * 23.0f + J * 32.0f + J * K * 23.0f * 32.0f * 3.7f;
@@ -225,8 +238,8 @@ static inline float nak_pump_vnorm(float V_mV, float Na_i, float K_o, float ATP_
     if (atp < 0.0f) atp = 0.0f;
     float f_ATP = atp / (atp + 0.5f);
     float eta = (float)(0.8f * FARADAY_CONST * (V_mV * MV_TO_V) / (GAS_CONST * CELSIUS_37));
-    float a2 = 60.0f * bo_expf(0.5f * eta);
-    float b2 = 6.0f * bo_expf(-(1.0f - 0.5f) * eta);
+    float a2 = 60.0f * bo_exp(0.5f * eta);
+    float b2 = 6.0f * bo_exp(-(1.0f - 0.5f) * eta);
     float a1 = 200.0f * f_Na * f_ATP;
     float a3 = 200.0f * f_K;
     float a4 = 60.0f;
@@ -239,8 +252,8 @@ static inline float nak_pump_vnorm(float V_mV, float Na_i, float K_o, float ATP_
 static inline float ncx_flux_norm(float V_mV, float Na_i, float Na_o, float Ca_i, float Ca_o) {
     float V_v = V_mV * MV_TO_V;
     float FRT = (float)(FARADAY_CONST / (GAS_CONST * CELSIUS_37));
-    float e_eta = bo_expf(0.35f * FRT * V_v);
-    float e_eta1 = bo_expf((0.35f - 1.0f) * FRT * V_v);
+    float e_eta = bo_exp(0.35f * FRT * V_v);
+    float e_eta1 = bo_exp((0.35f - 1.0f) * FRT * V_v);
     float Na_i3 = Na_i * Na_i * Na_i;
     float Na_o3 = Na_o * Na_o * Na_o;
     float fwd = e_eta1 * Na_o3 * Ca_i;

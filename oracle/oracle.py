@@ -45,7 +45,7 @@ def oracle_lib():
         lib.bo_log_d.argtypes = [C.c_double]; lib.bo_log_d.restype = C.c_double
         lib.bo_pow_d.argtypes = [C.c_double, C.c_double]; lib.bo_pow_d.restype = C.c_double
         lib.bo_xorshift_f.argtypes = [C.c_uint32]; lib.bo_xorshift_f.restype = C.c_float
-        lib.bo_seed_bits.argtypes = [C.c_float]; lib.bo_seed_bits.restype = C.c_uint32
+        lib.bo_seed_bits.argtypes = [C.c_double]; lib.bo_seed_bits.restype = C.c_uint32
         for name in ("bo_ghk_mono_d", "bo_ghk_div_d", "bo_ghk_anion_d"):
             getattr(lib, name).argtypes = [C.c_double] * 3
             getattr(lib, name).restype = C.c_double
@@ -57,6 +57,38 @@ def oracle_lib():
         lib.bo_release_log_count.argtypes = [vp]; lib.bo_release_log_count.restype = C.c_uint32
         _ora = lib
     return _ora
+
+
+_ora64 = None
+
+
+def oracle64_lib():
+    """oracle/liboracle64.so: the same restatement built with FP64 state and the C
+    library's elementary functions (-DBO_FP64 -DBO_LIBM), the build that is compared
+    with the reference's own tick."""
+    global _ora64
+    if _ora64 is None:
+        from bioneuroncore_b200 import build
+        if not os.path.exists(build.ORACLE64_LIB):
+            build.build_oracle()
+        lib = C.CDLL(build.ORACLE64_LIB)
+        vp = C.c_void_p
+        lib.bo_create.argtypes = [vp, vp, C.c_uint32, C.c_char_p, C.c_int]
+        lib.bo_create.restype = vp
+        lib.bo_destroy.argtypes = [vp]
+        lib.bo_upload_stimuli.argtypes = [vp, vp]
+        lib.bo_run.argtypes = [vp, C.c_uint32, C.c_float]
+        lib.bo_run_stride.argtypes = [vp, C.c_uint32, C.c_float, C.c_uint32]
+        lib.bo_get_seg_field64.argtypes = [vp, C.c_int, C.c_int, vp]
+        lib.bo_get_syn_field64.argtypes = [vp, C.c_int, C.c_int, vp]
+        lib.bo_set_release_log.argtypes = [vp, vp, vp, vp, vp, C.c_uint32]
+        lib.bo_release_log_count.argtypes = [vp]; lib.bo_release_log_count.restype = C.c_uint32
+        lib.bo_tick_count.argtypes = [vp]
+        lib.bo_tick_count.restype = C.c_uint64
+        lib.bo_seed_bits.argtypes = [C.c_double]; lib.bo_seed_bits.restype = C.c_uint32
+        lib.bo_xorshift_f.argtypes = [C.c_uint32]; lib.bo_xorshift_f.restype = C.c_float
+        _ora64 = lib
+    return _ora64
 
 
 def reference_available():
@@ -80,14 +112,17 @@ def reference_lib():
 SEG = {"V": 0, "ion_in": 1, "ion_out": 2, "ATP": 3, "temperature": 4, "transcription": 5, "intra_nt": 6,
        "neurotransmitter": 7, "mod_state": 8, "spikes": 9}
 SYN = {"bouton_Ca": 0, "spine_Ca": 1, "weight": 2, "refractory": 3, "cleft": 4, "receptor_state": 5,
-       "facilitation": 6, "spine_camkii": 7, "spine_calcineurin": 8, "RRP": 9}
+       "facilitation": 6, "spine_camkii": 7, "spine_calcineurin": 8, "RRP": 9, "depression": 10}
 
 
 class Oracle:
-    """FP32-state CPU restatement of the reference tick over a generated Network."""
+    """FP32-state CPU restatement of the reference tick over a generated Network.
+    With fp64=True, the same restatement with FP64 state and the C library's
+    elementary functions (oracle64_lib); its fields then come back as float64."""
 
-    def __init__(self, net):
-        lib = oracle_lib()
+    def __init__(self, net, fp64=False):
+        self.fp64 = fp64
+        lib = self._lib()
         err = C.create_string_buffer(256)
         self.h = lib.bo_create(C.byref(net.data), net.stim_ptr, net.n_stim, err, 256)
         if err.value:
@@ -97,48 +132,59 @@ class Oracle:
         self.n_seg = net.data.num_segments
         self.n_syn = net.data.num_synapses
 
+    def _lib(self):
+        return oracle64_lib() if self.fp64 else oracle_lib()
+
     def set_diffusion_mode(self, flags, tol=1e-6, max_sweeps=100000):
         """bo_set_diffusion_mode: residual-controlled FP64 Jacobi solves (flag 1) and
         the per-ion ledger (flag 2), as the backend's bnc_set_diffusion_mode."""
-        oracle_lib().bo_set_diffusion_mode(self.h, flags, C.c_double(tol), max_sweeps)
+        self._lib().bo_set_diffusion_mode(self.h, flags, C.c_double(tol), max_sweeps)
 
     def diffusion_stats(self, reset=False):
         """(stats[4], ledger[14]): max V and phi sweeps, capped V and phi group solves;
         per ion the FP32 rounding of the Nernst-Planck updates, then the bath exchange."""
         st = np.zeros(4, np.uint32)
         led = np.zeros(14, np.float64)
-        oracle_lib().bo_diffusion_stats(self.h, st.ctypes.data, led.ctypes.data, 1 if reset else 0)
+        self._lib().bo_diffusion_stats(self.h, st.ctypes.data, led.ctypes.data, 1 if reset else 0)
         return st, led
 
     def upload_stimuli(self, data):
         """bo_upload_stimuli with a GpuStimulusData: every list replaced, injections once."""
-        oracle_lib().bo_upload_stimuli(self.h, C.byref(data))
+        self._lib().bo_upload_stimuli(self.h, C.byref(data))
 
     def run(self, ticks, dt, tick_stride=1):
         if tick_stride == 1:
-            oracle_lib().bo_run(self.h, ticks, C.c_float(dt))
+            self._lib().bo_run(self.h, ticks, C.c_float(dt))
         else:
-            oracle_lib().bo_run_stride(self.h, ticks, C.c_float(dt), tick_stride)
+            self._lib().bo_run_stride(self.h, ticks, C.c_float(dt), tick_stride)
 
     def trace(self, ticks, dt, rec):
         rec = np.ascontiguousarray(rec, np.uint32)
         out = np.empty((ticks, rec.size), np.float32)
-        oracle_lib().bo_run_trace(self.h, ticks, C.c_float(dt), rec.ctypes.data, rec.size, out.ctypes.data)
+        self._lib().bo_run_trace(self.h, ticks, C.c_float(dt), rec.ctypes.data, rec.size, out.ctypes.data)
         return out
 
     def segment_field(self, field, index=0):
+        if self.fp64:
+            out = np.empty(self.n_seg, np.float64)
+            self._lib().bo_get_seg_field64(self.h, SEG.get(field, field), index, out.ctypes.data)
+            return out
         out = np.empty(self.n_seg, np.float32)
-        oracle_lib().bo_get_seg_field(self.h, SEG.get(field, field), index, out.ctypes.data)
+        self._lib().bo_get_seg_field(self.h, SEG.get(field, field), index, out.ctypes.data)
         return out
 
     def synapse_field(self, field, index=0):
+        if self.fp64:
+            out = np.empty(max(self.n_syn, 1), np.float64)
+            self._lib().bo_get_syn_field64(self.h, SYN.get(field, field), index, out.ctypes.data)
+            return out[:self.n_syn]
         out = np.empty(max(self.n_syn, 1), np.float32)
-        oracle_lib().bo_get_syn_field(self.h, SYN.get(field, field), index, out.ctypes.data)
+        self._lib().bo_get_syn_field(self.h, SYN.get(field, field), index, out.ctypes.data)
         return out[:self.n_syn]
 
     def set_synapse_scale(self, scale):
         s = np.ascontiguousarray(scale, np.float32)
-        oracle_lib().bo_set_syn_scale(self.h, s.ctypes.data)
+        self._lib().bo_set_syn_scale(self.h, s.ctypes.data)
 
     def run_logged(self, ticks, dt, cap=None):
         """Runs `ticks` ticks and returns the release log they produce, sorted by
@@ -148,7 +194,7 @@ class Oracle:
         tick = np.zeros(cap, np.uint64)
         amt = np.zeros(cap, np.float32)
         slot = np.zeros(cap, np.uint8)
-        lib = oracle_lib()
+        lib = self._lib()
         lib.bo_set_release_log(self.h, syn.ctypes.data, tick.ctypes.data, amt.ctypes.data, slot.ctypes.data, cap)
         lib.bo_run(self.h, ticks, C.c_float(dt))
         n = lib.bo_release_log_count(self.h)
@@ -160,7 +206,7 @@ class Oracle:
 
     def close(self):
         if self.h:
-            oracle_lib().bo_destroy(self.h)
+            self._lib().bo_destroy(self.h)
             self.h = None
 
     def __del__(self):
