@@ -32,6 +32,10 @@ struct Backend {
     DeviceAllocs allocs;
     DeviceAllocs stim_allocs;
     Stimuli stim;
+    // injections uploaded but not yet applied by a tick (the device list is consumed by
+    // the next tick; these copies let a checkpoint carry them)
+    std::vector<BncIonInjection> pend_ion;
+    std::vector<BncLigandInjection> pend_lig;
     uint64_t tick = 0;
     uint64_t ticks_run = 0;
     uint32_t tick_stride = 1;   // the tick counter's step per tick (2: the reference's batch mode)
@@ -74,6 +78,8 @@ struct Backend {
         std::memset(&dev, 0, sizeof(dev));
         host = NetHost();
         stim = Stimuli();
+        pend_ion.clear();
+        pend_lig.clear();
         loaded = false;
         failed = false;
         tick = 0;
@@ -373,6 +379,15 @@ static int copy_aos(const BncBionData* src, BncBionData* dst) {
 static void injections_enqueued(Backend* b) {
     b->dev.inj = nullptr;
     b->dev.inj_n = nullptr;
+    b->pend_ion.clear();
+    b->pend_lig.clear();
+}
+
+// Counter bookkeeping after one tick is enqueued; every tick entry point uses it.
+static void tick_enqueued(Backend* b) {
+    b->tick += b->tick_stride;
+    b->ticks_run++;
+    injections_enqueued(b);
 }
 
 static int run_ticks(Backend* b, uint32_t n, float dt) {
@@ -382,9 +397,7 @@ static int run_ticks(Backend* b, uint32_t n, float dt) {
     for (uint32_t t = 0; t < n; t++) {
         cudaError_t e = launch_tick(b->dev, b->host, dt, b->tick, b->ticks_run == 0 ? 1 : 0, b->stream);
         if (e != cudaSuccess) { b->failed = true; return cuda_fail(e, "tick launch"); }
-        b->tick += b->tick_stride;
-        b->ticks_run++;
-        injections_enqueued(b);
+        tick_enqueued(b);
     }
     return BNC_OK;
 }
@@ -696,7 +709,10 @@ void gpu_backend_upload_stimuli(void* sim, const BncGpuStimulusData* src) {
     b->stim_allocs.release();
     if (upload_stimuli(b->stim, b->host, &b->dev, &b->stim_allocs) != BNC_OK)
         set_error("device allocation of the stimulus arrays failed");
-    // injections are one-shot: a later rebuild from these lists must not repeat them
+    // injections are one-shot: a later rebuild from these lists must not repeat them;
+    // the pending copies last until a tick applies them
+    b->pend_ion.swap(b->stim.ion_inj);
+    b->pend_lig.swap(b->stim.lig_inj);
     b->stim.ion_inj.clear();
     b->stim.lig_inj.clear();
 }
@@ -1055,9 +1071,7 @@ int bnc_profile_ticks(void* sim, uint32_t n_ticks, float dt, float* ms_modifiers
         er = launch_synapse(b->dev, dt, b->tick, b->ticks_run == 0 ? 1 : 0, b->stream);
         if (er != cudaSuccess) { rc = cuda_fail(er, "synapse kernel launch"); break; }
         cudaEventRecord(e[3], b->stream);
-        b->tick++;
-        b->ticks_run++;
-        injections_enqueued(b);
+        tick_enqueued(b);
         rc = sync_stream(b);
         if (rc != BNC_OK) break;
         float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f;
@@ -1301,13 +1315,15 @@ int bnc_state_frame(void* sim, void* buf, uint64_t cap, uint64_t* len) {
 
 // ---- Checkpoints: the .bion plus what it does not hold ----
 // The .bion records the AoS state.  A run also carries the tick counter (it seeds the
-// release draws and times the stimuli), whether the first tick has run, the stimuli,
-// the per-synapse receptor density scales and the pending delayed releases
-// (delay_buffer.h:15-64).  The sidecar `<path>.state` holds them, so a loaded
-// checkpoint continues bit for bit.
+// release draws and times the stimuli), whether the first tick has run, the stimuli
+// (current steps, voltage clamps, ramps, and ion and ligand injections uploaded but not
+// yet applied), the per-synapse receptor density scales and the pending delayed
+// releases (delay_buffer.h:15-64).  The sidecar `<path>.state` holds them, so a loaded
+// checkpoint continues bit for bit.  Version 1 files held no ramps and no pending
+// injections; they are refused, since a run with either would not resume exactly.
 namespace {
 const char kStateMagic[8] = {'B', 'N', 'C', 'S', 'T', 'A', 'T', 'E'};
-constexpr uint32_t kStateVersion = 1;
+constexpr uint32_t kStateVersion = 2;
 struct DelaySlot {
     unsigned long long arrival;
     float amount;
@@ -1349,11 +1365,16 @@ int bnc_save_checkpoint(void* sim, const char* path) {
     FILE* f = fopen(sp.c_str(), "wb");
     if (!f) { set_error("cannot write %s", sp.c_str()); return BNC_BION_ERR_FILE_OPEN; }
     const uint32_t n_cur = (uint32_t)b->stim.current.size(), n_vc = (uint32_t)b->stim.vclamp.size();
-    const uint32_t head[6] = {kStateVersion, b->host.n_seg, KS, n_cur, n_vc, has_delay};
+    const uint32_t n_ramp = (uint32_t)b->stim.ramp.size();
+    const uint32_t n_ion = (uint32_t)b->pend_ion.size(), n_lig = (uint32_t)b->pend_lig.size();
+    const uint32_t head[9] = {kStateVersion, b->host.n_seg, KS, n_cur, n_vc, has_delay, n_ramp, n_ion, n_lig};
     const uint64_t ticks[2] = {b->tick, b->ticks_run};
     bool ok = fwrite(kStateMagic, 1, 8, f) == 8 && fwrite(head, sizeof(head), 1, f) == 1 && fwrite(ticks, sizeof(ticks), 1, f) == 1;
     if (ok && n_cur) ok = fwrite(b->stim.current.data(), sizeof(BncCurrentStimulus), n_cur, f) == n_cur;
     if (ok && n_vc) ok = fwrite(b->stim.vclamp.data(), sizeof(BncVoltageClamp), n_vc, f) == n_vc;
+    if (ok && n_ramp) ok = fwrite(b->stim.ramp.data(), sizeof(BncRampStimulus), n_ramp, f) == n_ramp;
+    if (ok && n_ion) ok = fwrite(b->pend_ion.data(), sizeof(BncIonInjection), n_ion, f) == n_ion;
+    if (ok && n_lig) ok = fwrite(b->pend_lig.data(), sizeof(BncLigandInjection), n_lig, f) == n_lig;
     if (ok && KS) ok = fwrite(scale.data(), sizeof(float), KS, f) == KS;
     if (ok && has_delay && KS) ok = fwrite(slots.data(), sizeof(DelaySlot), slots.size(), f) == slots.size();
     if (fclose(f) != 0) ok = false;
@@ -1368,19 +1389,34 @@ int bnc_load_checkpoint(void* sim, const char* path) {
     FILE* f = fopen(sp.c_str(), "rb");
     if (!f) { set_error("cannot read %s", sp.c_str()); return BNC_BION_ERR_FILE_OPEN; }
     char magic[8];
-    uint32_t head[6];
+    uint32_t version = 0;
+    uint32_t head[9];
     uint64_t ticks[2];
-    bool ok = fread(magic, 1, 8, f) == 8 && std::memcmp(magic, kStateMagic, 8) == 0 && fread(head, sizeof(head), 1, f) == 1 &&
-              head[0] == kStateVersion && fread(ticks, sizeof(ticks), 1, f) == 1;
+    bool ok = fread(magic, 1, 8, f) == 8 && std::memcmp(magic, kStateMagic, 8) == 0 && fread(&version, 4, 1, f) == 1;
+    if (ok && version != kStateVersion) {
+        fclose(f);
+        set_error("%s is a version %u state file; this library reads version %u (version 1 held no ramps "
+                  "and no pending injections)", sp.c_str(), version, kStateVersion);
+        return BNC_ERR_FORMAT;
+    }
+    head[0] = version;
+    ok = ok && fread(head + 1, sizeof(head) - 4, 1, f) == 1 && fread(ticks, sizeof(ticks), 1, f) == 1 &&
+         head[6] <= BNC_GPU_MAX_STIMULI && head[7] <= BNC_GPU_MAX_STIMULI && head[8] <= BNC_GPU_MAX_STIMULI;
     Stimuli stim;
     std::vector<float> scale;
     std::vector<DelaySlot> slots;
     if (ok) {
         stim.current.resize(head[3]);
         stim.vclamp.resize(head[4]);
+        stim.ramp.resize(head[6]);
+        stim.ion_inj.resize(head[7]);
+        stim.lig_inj.resize(head[8]);
         scale.resize(head[2]);
         if (head[3]) ok = fread(stim.current.data(), sizeof(BncCurrentStimulus), head[3], f) == head[3];
         if (ok && head[4]) ok = fread(stim.vclamp.data(), sizeof(BncVoltageClamp), head[4], f) == head[4];
+        if (ok && head[6]) ok = fread(stim.ramp.data(), sizeof(BncRampStimulus), head[6], f) == head[6];
+        if (ok && head[7]) ok = fread(stim.ion_inj.data(), sizeof(BncIonInjection), head[7], f) == head[7];
+        if (ok && head[8]) ok = fread(stim.lig_inj.data(), sizeof(BncLigandInjection), head[8], f) == head[8];
         if (ok && head[2]) ok = fread(scale.data(), sizeof(float), head[2], f) == head[2];
         if (ok && head[5] && head[2]) {
             slots.resize((size_t)4 * head[2]);
@@ -1401,6 +1437,11 @@ int bnc_load_checkpoint(void* sim, const char* path) {
     b->stim = stim;
     rc = load_common(b, aos, true);
     if (rc != BNC_OK) { free_aos_arrays(aos); return rc; }
+    // the pending injections went to the device with the build; the next tick applies them
+    b->pend_ion.swap(b->stim.ion_inj);
+    b->pend_lig.swap(b->stim.lig_inj);
+    b->stim.ion_inj.clear();
+    b->stim.lig_inj.clear();
     b->tick = ticks[0];
     b->ticks_run = ticks[1];
     const NetDev& d = b->dev;
@@ -1516,14 +1557,12 @@ extern "C" int bnc_run_ticks_static_scratch(void* sim, uint32_t n_ticks, float d
         e = cudaMemsetAsync(d.pre_rec, 0, (size_t)n * sizeof(float4), b->stream);
         if (e == cudaSuccess && b->dev.pre_ext) e = cudaMemsetAsync(d.pre_ext, 0, (size_t)n * sizeof(float4), b->stream);
         if (e == cudaSuccess && b->dev.pre_ext2) e = cudaMemsetAsync(d.pre_ext2, 0, (size_t)n * sizeof(float), b->stream);
-        if (e != cudaSuccess) return cuda_fail(e, "clearing the static tick scratch");
+        if (e != cudaSuccess) { b->failed = true; return cuda_fail(e, "clearing the static tick scratch"); }
     }
     for (uint32_t t = 0; t < n_ticks; t++) {
         e = launch_tick(d, b->host, dt, b->tick, b->ticks_run == 0 ? 1 : 0, b->stream);
         if (e != cudaSuccess) { b->failed = true; return cuda_fail(e, "tick launch"); }
-        b->tick++;
-        b->ticks_run++;
-        injections_enqueued(b);
+        tick_enqueued(b);
         d.inj = nullptr;
         d.inj_n = nullptr;
     }

@@ -51,6 +51,61 @@ def test_checkpoint_resumes_bit_for_bit(tmp_path):
     assert any((a[k].view(np.uint32) != c[k].view(np.uint32)).any() for k in a)
 
 
+def test_checkpoint_keeps_ramps_and_pending_injections(tmp_path):
+    """A ramp that spans the save point and ion and ligand injections uploaded just
+    before the save (applied by the first tick after it) survive the checkpoint: the
+    resumed run equals the uninterrupted one bit for bit."""
+    from bioneuroncore_b200.abi import stimulus_data
+    p = NetgenParams(family=NET_SMALL, n_neurons=8, seed=7, flags=32)
+    soma = [32 * k for k in range(8)]   # segment 0 of each 32-segment neuron
+
+    def uploads(sim, net, t):
+        cur = [tuple(int(r[f]) if f in ("segment_id", "start_tick") else float(r[f])
+                     for f in ("segment_id", "amplitude_pA", "duration_ms", "start_tick")) for r in net.stimuli]
+        if t == 100:
+            sim.upload_stimuli(stimulus_data(current=cur, ramps=[(soma[1], 0.0, 400.0, 150, 350),
+                                                                 (soma[2], 300.0, -100.0, 180, 260)]))
+        if t == 200:
+            sim.upload_stimuli(stimulus_data(current=cur, ramps=[(soma[1], 0.0, 400.0, 150, 350)],
+                                             ion_inj=[(soma[3], 0, 1.5, 0), (soma[4], 1, 0.5, 1)],
+                                             lig_inj=[(soma[5], 0, 0.3, 1), (soma[6], 2, 0.1, 0)]))
+
+    net_w = Network(p)
+    whole = Backend()
+    whole.load_network(net_w)
+    for t in range(400):
+        uploads(whole, net_w, t)
+        whole.run_ticks(1, DT)
+    net_h = Network(p)
+    half = Backend()
+    half.load_network(net_h)
+    for t in range(200):
+        uploads(half, net_h, t)
+        half.run_ticks(1, DT)
+    uploads(half, net_h, 200)          # uploaded, not yet applied: pending at the save
+    path = tmp_path / "run.bion"
+    half.save_checkpoint(path)
+    resumed = Backend()
+    resumed.load_checkpoint(path)
+    resumed.run_ticks(200, DT)
+    _same(_state(whole), _state(resumed))
+
+
+def test_checkpoint_refuses_version_1_state_files(tmp_path):
+    import struct
+    p = NetgenParams(family=NET_SMALL, n_neurons=4, seed=3)
+    b = Backend()
+    b.load_network(Network(p))
+    b.run_ticks(5, DT)
+    path = tmp_path / "run.bion"
+    b.save_checkpoint(path)
+    raw = bytearray((tmp_path / "run.bion.state").read_bytes())
+    struct.pack_into("<I", raw, 8, 1)
+    (tmp_path / "run.bion.state").write_bytes(bytes(raw))
+    with pytest.raises(BackendError, match="version 1"):
+        Backend().load_checkpoint(path)
+
+
 def test_checkpoint_errors(tmp_path):
     b = Backend()
     with pytest.raises(BackendError):

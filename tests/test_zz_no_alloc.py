@@ -74,6 +74,39 @@ def test_static_scratch_matches_regular_ticks(family, n_neurons, n_synapses, see
         _compare(static, regular, n_syn, "%s network, call %d (+%d ticks)" % (family, call + 1, n))
 
 
+def test_static_scratch_with_presynaptic_ions_and_injections():
+    """Synapses with readily releasable pools and bouton autoreceptor channels make the
+    tile kernel also write the presynaptic ion records, which this entry point keeps in
+    the fixed array as well; ion and ligand injections uploaded before the first call
+    are applied by its first tick.  3 nA somatic steps make the network release within
+    the run.  Both calls must equal the regular ticks bit for bit."""
+    from bioneuroncore_b200 import Backend, Network, NetgenParams, NET_SMALL, NETGEN_SYNAPSE_EXTRAS
+    from bioneuroncore_b200.abi import stimulus_data
+    p = NetgenParams(family=NET_SMALL, n_neurons=16, seed=6, flags=NETGEN_SYNAPSE_EXTRAS, stim_pA=3000.0)
+    net_s, net_r = Network(p), Network(p)
+    syn = net_r.synapses
+    assert (syn["RRP_max"] > 0).any() and (syn["pre_autoreceptor_count"] > 0).any()
+    static, regular = Backend(), Backend()
+    static.load_network(net_s)
+    regular.load_network(net_r)
+    cur = [tuple(int(r[f]) if f in ("segment_id", "start_tick") else float(r[f])
+                 for f in ("segment_id", "amplitude_pA", "duration_ms", "start_tick")) for r in net_r.stimuli]
+    inj = stimulus_data(current=cur, ion_inj=[(32, 0, 2.0, 0), (64, 1, 0.5, 1)], lig_inj=[(96, 0, 0.4, 1)])
+    static.upload_stimuli(inj)
+    regular.upload_stimuli(inj)
+    n_syn = net_r.data.num_synapses
+    rrp0 = np.asarray(regular.synapse_field("RRP", 0, n_syn)).copy()
+    for call, n in enumerate((150, 350)):
+        _static_ticks(static, n)
+        regular.run_ticks(n, DT)
+        assert static.info().ticks == regular.info().ticks
+        _compare(static, regular, n_syn, "extras network, call %d (+%d ticks)" % (call + 1, n))
+        _assert_same(static.synapse_field("RRP", 0, n_syn), regular.synapse_field("RRP", 0, n_syn), "RRP")
+        for f, i in (("intra_nt", 0), ("ion_in", 0), ("ion_out", 1)):
+            _assert_same(static.segment_field(f, i), regular.segment_field(f, i), "%s[%d]" % (f, i))
+    assert (np.asarray(regular.synapse_field("RRP", 0, n_syn)) != rrp0).any(), "the run must release"
+
+
 def test_static_scratch_rejects_networks_above_its_limit():
     from bioneuroncore_b200 import Backend, NetgenParams, NET_LARGE, plan_generated
     p = NetgenParams(family=NET_LARGE, n_neurons=MAX_SEGMENTS // 64 + 1, n_synapses=1000, seed=3)
