@@ -68,13 +68,14 @@ class NetInfo(C.Structure):
         ("syn_bytes_per_tick", C.c_double), ("tile_bytes_per_tick", C.c_double),
         ("synapse_kernel_bytes_per_tick", C.c_double), ("warp_cap", C.c_uint32), ("tile_segs", C.c_uint32),
         ("modifier_kernel_bytes", C.c_double), ("diffusion_kernel_bytes", C.c_double),
-        ("modifier_launches", C.c_uint32), ("fuse_phases", C.c_uint32)]
+        ("modifier_launches", C.c_uint32), ("fuse_phases", C.c_uint32), ("group_tiles_32", C.c_uint32),
+        ("group_tiles_64", C.c_uint32), ("diffusion_threads", C.c_uint32)]
 
 
 class BuildOptions(C.Structure):
     """Device-layout options (include/bnc_b200.h BncBuildOptions); 0 = default."""
     _fields_ = [("warp_cap", C.c_uint32), ("tile_segs", C.c_uint32), ("phase_cap", C.c_uint32),
-                ("chunk_segs", C.c_uint32), ("fuse_phases", C.c_uint32)]
+                ("chunk_segs", C.c_uint32), ("fuse_phases", C.c_uint32), ("cta_barriers", C.c_uint32)]
 
 
 class Tuning(C.Structure):

@@ -766,6 +766,7 @@ static BuildOptions to_options(const BncBuildOptions* o) {
         opt.phase_cap = o->phase_cap;
         if (o->chunk_segs) opt.chunk_segs = o->chunk_segs;
         if (o->fuse_phases) opt.fuse_phases = o->fuse_phases;
+        opt.group_barriers = o->cta_barriers == 0;
     }
     return opt;
 }
@@ -807,6 +808,8 @@ static int plan_info(const HostNet& hn, const Stimuli& stim, BncNetInfo* info,
     info->warp_cap = host.opt.warp_cap; info->tile_segs = host.opt.tile_segs;
     info->modifier_kernel_bytes = host.mod_bytes; info->diffusion_kernel_bytes = host.diff_bytes;
     info->modifier_launches = modifier_launches(dev, host); info->fuse_phases = host.fuse;
+    info->group_tiles_32 = host.group_tiles_32; info->group_tiles_64 = host.group_tiles_64;
+    info->diffusion_threads = host.diff_threads;
     return BNC_OK;
 }
 
@@ -1224,6 +1227,8 @@ int bnc_network_info(void* sim, BncNetInfo* info) {
     info->tile_bytes_per_tick = b->host.tile_bytes;
     info->synapse_kernel_bytes_per_tick = b->host.synk_bytes;
     info->modifier_launches = modifier_launches(d, b->host); info->fuse_phases = b->host.fuse;
+    info->group_tiles_32 = b->host.group_tiles_32; info->group_tiles_64 = b->host.group_tiles_64;
+    info->diffusion_threads = b->host.diff_threads;
     info->warp_cap = b->host.opt.warp_cap; info->tile_segs = b->host.opt.tile_segs;
     info->modifier_kernel_bytes = b->host.mod_bytes; info->diffusion_kernel_bytes = b->host.diff_bytes;
     return BNC_OK;

@@ -583,6 +583,93 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
         }
     }
     const uint32_t E = (uint32_t)edge_conn.size();
+    // ---- barrier groups of the diffusion kernel ----
+    // Every pass of step 2.5 couples only the two ends of a connection.  Where no
+    // connection of a tile joins segments in different aligned groups of G threads
+    // (G = 32, else 64), a group synchronises only itself (a warp, or a 64-thread named
+    // barrier) instead of the CTA.  Each connection of such a tile is then handled by
+    // the thread of one of its segments: breadth first from each component's first
+    // segment, a segment owns the connection it was reached by, so a thread handles at
+    // most one.  A tile whose connections cannot all be owned so (a cycle, a repeated
+    // connection) keeps CTA-wide barriers.
+    std::vector<uint8_t> tile_gmode(T, 0);
+    std::vector<uint16_t> seg_edge(n, 0xFFFF);
+    host->group_tiles_32 = host->group_tiles_64 = 0;
+    if (host->cluster == 1 && opt.group_barriers) {
+        std::vector<uint32_t> adj_off, adj, queue;
+        std::vector<uint8_t> seen;
+        for (uint32_t t = 0; t < T; t++) {
+            const uint32_t s0 = tile_seg_beg[t], ns_t = tile_seg_beg[t + 1] - s0;
+            const uint32_t e0 = tile_edge_beg[t], ne_t = tile_edge_beg[t + 1] - e0;
+            uint32_t G = 0;
+            for (uint32_t g : {32u, 64u}) {
+                bool ok = true;
+                for (uint32_t e = e0; e < e0 + ne_t && ok; e++) ok = e_a[e] < ns_t && e_b[e] < ns_t && e_a[e] / g == e_b[e] / g;
+                if (ok) { G = g; break; }
+            }
+            if (ne_t == 0) { tile_gmode[t] = 32; continue; }   // nothing couples its segments
+            if (!G) continue;
+            adj_off.assign(ns_t + 1, 0);
+            for (uint32_t e = e0; e < e0 + ne_t; e++) { adj_off[e_a[e] + 1]++; adj_off[e_b[e] + 1]++; }
+            for (uint32_t x = 0; x < ns_t; x++) adj_off[x + 1] += adj_off[x];
+            adj.assign(2 * (size_t)ne_t, 0);
+            {
+                std::vector<uint32_t> pos(adj_off.begin(), adj_off.end() - 1);
+                for (uint32_t e = e0; e < e0 + ne_t; e++) {
+                    adj[pos[e_a[e]]++] = (e - e0) << 16 | e_b[e];
+                    adj[pos[e_b[e]]++] = (e - e0) << 16 | e_a[e];
+                }
+            }
+            seen.assign(ns_t, 0);
+            uint32_t owned = 0;
+            for (uint32_t r = 0; r < ns_t; r++) {
+                if (seen[r]) continue;
+                seen[r] = 1;
+                queue.assign(1, r);
+                for (size_t h = 0; h < queue.size(); h++) {
+                    const uint32_t x = queue[h];
+                    for (uint32_t k = adj_off[x]; k < adj_off[x + 1]; k++) {
+                        const uint32_t y = adj[k] & 0xFFFFu;
+                        if (seen[y]) continue;
+                        seen[y] = 1;
+                        seg_edge[s0 + y] = (uint16_t)(adj[k] >> 16);
+                        owned++;
+                        queue.push_back(y);
+                    }
+                }
+            }
+            if (owned != ne_t) {
+                for (uint32_t x = 0; x < ns_t; x++) seg_edge[s0 + x] = 0xFFFF;
+                continue;
+            }
+            tile_gmode[t] = (uint8_t)G;
+        }
+    }
+    {
+        // The kernel is compiled per barrier mode, so the mode is the network's: warps
+        // (32) when every tile's connections stay inside aligned warps, else 64-thread
+        // groups when every tile's stay inside those (a warp-grouped tile is also
+        // 64-grouped), else the CTA.  A 64-thread group is two whole warps: the CTA is
+        // a multiple of 64 threads, and its groups take named barriers 1..15.
+        uint32_t mts0 = 0;
+        for (uint32_t t = 0; t < T; t++) mts0 = std::max(mts0, tile_seg_beg[t + 1] - tile_seg_beg[t]);
+        bool all32 = T > 0, all_grouped = T > 0;
+        for (uint32_t t = 0; t < T; t++) {
+            all32 &= tile_gmode[t] == 32;
+            all_grouped &= tile_gmode[t] != 0;
+        }
+        uint32_t gm = all32 ? 32u : (all_grouped ? 64u : 0u);
+        uint32_t th = (mts0 + (gm == 64 ? 63 : 31)) / (gm == 64 ? 64 : 32) * (gm == 64 ? 64 : 32);
+        if (gm == 64 && th > 960) {
+            gm = 0;
+            th = (mts0 + 31) / 32 * 32;
+        }
+        if (gm == 0) std::fill(seg_edge.begin(), seg_edge.end(), (uint16_t)0xFFFF);
+        host->diff_gm = gm;
+        host->diff_threads = th < 32 ? 32 : th;
+        host->group_tiles_32 = gm == 32 ? T : 0;
+        host->group_tiles_64 = gm == 64 ? T : 0;
+    }
     std::vector<uint8_t> e_intra(E);
     std::vector<float> e_area(E), e_dist(E);
     for (uint32_t e = 0; e < E; e++) {
@@ -1296,6 +1383,7 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
         dev->phase_off = up(allocs, phase_off, &rc);
         dev->warp_seg = up(allocs, warp_seg, &rc);
         dev->warp_edge = up(allocs, warp_edge, &rc);
+        dev->seg_edge = host->diff_gm ? up(allocs, seg_edge, &rc) : nullptr;
         dev->e_a = up(allocs, e_a, &rc);
         dev->e_b = up(allocs, e_b, &rc);
         dev->e_intra = up(allocs, e_intra, &rc);

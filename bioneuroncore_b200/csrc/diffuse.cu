@@ -61,6 +61,41 @@ __device__ __forceinline__ double div_by_float(double a, double b, double y) {
     return a / b;
 }
 
+// a / b rounded to nearest in binary32, given y = 1 / b rounded to nearest (Markstein's
+// correction, Markstein 1990, IBM J. Res. Dev. 34(1)): q0 = a * y is within an ulp of
+// a / b, r = a - b * q0 is then exact (one fma), and fma(r, y, q0) is the correctly
+// rounded quotient.  Operands are kept well inside the normal range (|a| in
+// [2^-64, 2^64], |b| in [2^-32, 2^32], so q0 and r are normal); outside it the
+// hardware division runs.  Used where one divisor serves many divisions (a Jacobi
+// solve's diagonal, a segment's volume, a connection's length, the substep).
+__device__ __forceinline__ bool div_rn_f_range_b(float b) {
+    const float ab = fabsf(b);
+    return ab >= 0x1p-32f && ab <= 0x1p32f;
+}
+__device__ __forceinline__ bool div_rn_f_range_a(float a) {
+    const float aa = fabsf(a);
+    return aa >= 0x1p-64f && aa <= 0x1p64f;
+}
+__device__ __forceinline__ float div_rn_f(float a, float b, float y) {
+    if (div_rn_f_range_a(a) && div_rn_f_range_b(b)) {
+        const float q0 = a * y;
+        const float r = __fmaf_rn(-q0, b, a);
+        return __fmaf_rn(r, y, q0);
+    }
+    return a / b;
+}
+
+// The same in binary64 (|b| and |q0| in [2^-500, 2^500]).
+__device__ __forceinline__ double div_rn_d(double a, double b, double y) {
+    const double q0 = a * y;
+    const double aq = fabs(q0), ab = fabs(b);
+    if (aq >= 0x1p-500 && aq <= 0x1p500 && ab >= 0x1p-500 && ab <= 0x1p500) {
+        const double r = __fma_rn(-q0, b, a);
+        return __fma_rn(r, y, q0);
+    }
+    return a / b;
+}
+
 // diffusion_kernel.h:108-113
 __device__ __forceinline__ float sg_bernoulli(float x) {
     if (fabsf(x) < 1e-3f) return 1.0f - 0.5f * x;
@@ -140,12 +175,19 @@ struct Stencil {
     uint8_t bend;   // bit k: the segment is edge e[k]'s b end
 };
 
-// Barrier of the CTAs that share a tile: the CTA itself, or both CTAs of a
-// 2-CTA cluster whose tiles hold the halves of one large component.
+// Barrier of the threads that share a tile's data: the CTA itself, both CTAs of a
+// 2-CTA cluster whose tiles hold the halves of one large component, or -- in a tile
+// whose connections all stay inside aligned groups of gm threads -- the thread's own
+// group: its warp (gm 32) or its pair of warps, named barrier 1 + tid / 64 (gm 64).
 template <int CL>
-__device__ __forceinline__ void tile_sync() {
-    if constexpr (CL == 2) cooperative_groups::this_cluster().sync();
-    else __syncthreads();
+__device__ __forceinline__ void tile_sync(int gm = 0) {
+    if constexpr (CL == 2) {
+        cooperative_groups::this_cluster().sync();
+    } else {
+        if (gm == 32) __syncwarp();
+        else if (gm == 64) asm volatile("bar.sync %0, 64;" ::"r"(1 + (int)(threadIdx.x >> 6)) : "memory");
+        else __syncthreads();
+    }
 }
 
 // After a tile_sync that follows an update: copy the paired CTA's values of this
@@ -168,19 +210,24 @@ __device__ __forceinline__ void halo(T* base, int rows, uint32_t S, int ns, int 
 
 // Fick pass for a float field in t.nb (diffusion_kernel.h:284-345): per-edge flux,
 // then per-segment gather in connection order, updating t.nb in place.
+// yvf: 1 / (this segment's volume); rde: 1 / (the length of this thread's connection)
+// when each connection has its own thread (edge_reg), else unused.  The thread handles
+// connections ef, ef + es, ... below el; gm is the barrier group (tile_sync).
 template <int CL, bool kIntraOnly, bool kGradStrict>
-__device__ __forceinline__ void fick(const DiffSmem& t, int ns, int ne, int tid, int nth, int i, const Stencil& st,
-                                     float D, float thresh, float dt) {
-    for (int e = tid; e < ne; e += nth) {
+__device__ __forceinline__ void fick(const DiffSmem& t, int ns, int ef, int el, int es, int gm, int i,
+                                     const Stencil& st, float D, float thresh, float dt, float yvf, bool edge_reg,
+                                     float rde) {
+    for (int e = ef; e < el; e += es) {
         t.es[e] = 1;
         if (kIntraOnly && !t.ei[e]) continue;
         float dC = t.nb[t.ea[e]] - t.nb[t.eb[e]];
         if (kGradStrict) { if (!(dC > thresh || dC < -thresh)) continue; }
         else if (dC < thresh && dC > -thresh) continue;
-        t.fl[e] = D * t.earea[e] * dC * dt / t.edist[e];
+        const float num = D * t.earea[e] * dC * dt;
+        t.fl[e] = edge_reg ? div_rn_f(num, t.edist[e], rde) : num / t.edist[e];
         t.es[e] = 0;
     }
-    tile_sync<CL>();
+    tile_sync<CL>(gm);
     // the gather reads only edge fluxes and the segment's own value: update in place
     if (i < ns) {
         const float vf = t.vf[i];
@@ -191,19 +238,19 @@ __device__ __forceinline__ void fick(const DiffSmem& t, int ns, int ne, int tid,
                 if (k >= st.n) break;
                 const int e = st.e[k];
                 if (t.es[e]) continue;
-                if ((st.bend >> k) & 1u) acc += t.fl[e] / vf; else acc -= t.fl[e] / vf;
+                if ((st.bend >> k) & 1u) acc += div_rn_f(t.fl[e], vf, yvf); else acc -= div_rn_f(t.fl[e], vf, yvf);
             }
         } else {
             for (int k = t.incoff[i]; k < t.incoff[i + 1]; k++) {
                 const uint16_t ent = t.inc[k];
                 const int e = ent & 0x7FFF;
                 if (t.es[e]) continue;
-                if (ent & 0x8000) acc += t.fl[e] / vf; else acc -= t.fl[e] / vf;
+                if (ent & 0x8000) acc += div_rn_f(t.fl[e], vf, yvf); else acc -= div_rn_f(t.fl[e], vf, yvf);
             }
         }
         t.nb[i] = t.nb[i] + acc;
     }
-    tile_sync<CL>();
+    tile_sync<CL>(gm);
 }
 
 // ---- residual-controlled Jacobi (NetDev::diff_mode bit 0) ----
@@ -311,7 +358,9 @@ __device__ __forceinline__ void ledger_add(double* sh, int slot, double v) {
 
 // OPT 0: the reference's fixed-sweep solves (the default); OPT 1: the options of
 // NetDev::diff_mode compiled in (residual-controlled solves, the ion ledger).
-template <int CL, int OPT>
+// GM: barrier groups (0: the CTA or cluster; 32 or 64: aligned thread groups that hold
+// whole components, NetHost::diff_gm).
+template <int CL, int OPT, int GM>
 __global__ void __launch_bounds__(1024)
 k_diffusion(NetDev d, float dt, unsigned long long tick, uint32_t S, uint32_t E) {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -404,6 +453,7 @@ k_diffusion(NetDev d, float dt, unsigned long long tick, uint32_t S, uint32_t E)
         t.gsrc[g] = (uint16_t)d.gh_src[gh0 + g];
     }
     const float dt_sub = dt / 5;
+    const float ydts = 1.0f / dt_sub;
     // Nernst-Planck flux coefficient of each connection and ion: the reference's
     // kDiffC[q] * area * dt_sub / dist, left to right, the same in every substep.
     for (int e = tid; e < ne; e += nth) {
@@ -412,9 +462,21 @@ k_diffusion(NetDev d, float dt, unsigned long long tick, uint32_t S, uint32_t E)
         for (int q = 0; q < 7; q++) t.coef[q * E + e] = kDiffC[q] * ar * dt_sub / di;
     }
     tile_sync<CL>();
+    // Barrier group of this tile (tile_sync) and the connections this thread handles:
+    // in a grouped tile the one its segment owns (seg_edge), else tid, tid + nth, ...
+    constexpr int gm = (CL == 1 && OPT == 0) ? GM : 0;
+    int ef = tid, el = ne, es = nth;
+    if (gm) {
+        const uint16_t me = (i < ns) ? d.seg_edge[s0 + i] : (uint16_t)0xFFFF;
+        ef = me != 0xFFFF ? (int)me : 0;
+        el = me != 0xFFFF ? (int)me + 1 : 0;
+        es = 1;
+    }
     // when every connection has its own thread, that thread keeps its connection's
-    // extracellular Bernoulli values in registers for the whole tick
-    const bool edge_reg = ne <= nth;
+    // extracellular Bernoulli values and reciprocal length in registers for the tick
+    const bool edge_reg = gm != 0 || ne <= nth;
+    const int my_edge = ef < el ? ef : -1;
+    const float rde = (edge_reg && my_edge >= 0) ? 1.0f / t.edist[my_edge] : 1.0f;
 
     if (d.flags & NF_DIFFUSION) {
         // this segment's incidences in connection order
@@ -448,13 +510,13 @@ k_diffusion(NetDev d, float dt, unsigned long long tick, uint32_t S, uint32_t E)
             t.sig[i] = 3.612f * sacc;
             t.phiA[i] = 0.0;
         }
-        tile_sync<CL>();
+        tile_sync<CL>(gm);
         halo<CL>(t.sig, 1, S, ns, ng, t.gsrc, tid, nth);
-        for (int e = tid; e < ne; e += nth) {
+        for (int e = ef; e < el; e += es) {
             double g = 0.5 * (t.sig[t.ea[e]] + t.sig[t.eb[e]]) * t.earea[e] / t.edist[e];
             t.ed[e] = g;
         }
-        tile_sync<CL>();
+        tile_sync<CL>(gm);
         // diagonal and the sweep stencil (connections with g > 0, in order)
         double diag = 0.0, itot = 0.0;
         double pg[kDeg];
@@ -485,6 +547,7 @@ k_diffusion(NetDev d, float dt, unsigned long long tick, uint32_t S, uint32_t E)
                 for (int k = t.incoff[i]; k < t.incoff[i + 1]; k++) diag += t.ed[t.inc[k] & 0x7FFF];
             }
         }
+        const double ydiag = (i < ns && diag > 1e-9) ? 1.0 / diag : 1.0;
         double* phi = t.phiA;
         double* phn = t.phiB;
         if (OPT && (d.diff_mode & 1u)) {
@@ -519,7 +582,7 @@ k_diffusion(NetDev d, float dt, unsigned long long tick, uint32_t S, uint32_t E)
                 if (i < ns) t.phiA[i] = res[i];
                 for (int g = tid; g < ng; g += nth) t.phiA[ns + g] = res[ns + g];
             }
-            tile_sync<CL>();
+            tile_sync<CL>(gm);
         } else
         // Tiles whose every segment has at most two stencil entries (chains and their
         // somata): the same sums over two registers' worth of entries, two sweeps per
@@ -534,22 +597,22 @@ k_diffusion(NetDev d, float dt, unsigned long long tick, uint32_t S, uint32_t E)
                     double pn = 0.0;
                     if (h0) pn += g0 * t.phiA[o0];
                     if (h1) pn += g1 * t.phiA[o1];
-                    double v = live ? (pn - itot) / diag : 0.0;
+                    double v = live ? div_rn_d(pn - itot, diag, ydiag) : 0.0;
                     if (v > 10.0) v = 10.0;
                     if (v < -10.0) v = -10.0;
                     t.phiB[i] = v;
                 }
-                __syncthreads();
+                tile_sync<CL>(gm);
                 if (i < ns) {
                     double pn = 0.0;
                     if (h0) pn += g0 * t.phiB[o0];
                     if (h1) pn += g1 * t.phiB[o1];
-                    double v = live ? (pn - itot) / diag : 0.0;
+                    double v = live ? div_rn_d(pn - itot, diag, ydiag) : 0.0;
                     if (v > 10.0) v = 10.0;
                     if (v < -10.0) v = -10.0;
                     t.phiA[i] = v;
                 }
-                __syncthreads();
+                tile_sync<CL>(gm);
             }
         } else
         for (int it = 0; it < 50; it++) {
@@ -569,19 +632,19 @@ k_diffusion(NetDev d, float dt, unsigned long long tick, uint32_t S, uint32_t E)
                         pn += g * phi[o];
                     }
                 }
-                double v = (diag > 1e-9) ? (pn - itot) / diag : 0.0;
+                double v = (diag > 1e-9) ? div_rn_d(pn - itot, diag, ydiag) : 0.0;
                 if (v > 10.0) v = 10.0;
                 if (v < -10.0) v = -10.0;
                 phn[i] = v;
             }
-            tile_sync<CL>();
+            tile_sync<CL>(gm);
             halo<CL>(phn, 1, S, ns, ng, t.gsrc, tid, nth);
             double* tmp = phi; phi = phn; phn = tmp;
         }
 
         // ---- intracellular Nernst-Planck, 5 substeps (diffusion_kernel.h:152-238) ----
         for (int sub = 0; sub < 5; sub++) {
-            for (int e = tid; e < ne; e += nth) {
+            for (int e = ef; e < el; e += es) {
                 if (!t.ei[e]) continue;
                 const int a = t.ea[e], b = t.eb[e];
                 float sigma_i = 0.0f;
@@ -590,11 +653,12 @@ k_diffusion(NetDev d, float dt, unsigned long long tick, uint32_t S, uint32_t E)
                     float C_bar = (float)(0.5f * ((double)t.in[q * S + a] + (double)t.in[q * S + b]));
                     sigma_i += kNpZ[q] * kNpZ[q] * kDiffC[q] * C_bar;
                 }
-                t.gax[e] = 3.612f * sigma_i * t.earea[e] / t.edist[e];
+                const float gnum = 3.612f * sigma_i * t.earea[e];
+                t.gax[e] = edge_reg ? div_rn_f(gnum, t.edist[e], rde) : gnum / t.edist[e];
                 t.dve[e] = (float)(((double)t.V[a] + phi[a]) - ((double)t.V[b] + phi[b]));
                 t.ie[e] = 0.0f;
             }
-            tile_sync<CL>();
+            tile_sync<CL>(gm);
             // g_diag, and the V-sweep stencil (intracellular connections, in order)
             float gd = 0.0f;
             float vg[kDeg];
@@ -624,16 +688,21 @@ k_diffusion(NetDev d, float dt, unsigned long long tick, uint32_t S, uint32_t E)
             // The 7 ions' fluxes in one connection pass (an ion's flux reads only that
             // ion, which no other ion's update touches), then one gather for all 7.
             // Ions of equal valence share x = (z * 0.03742f) * dV and so its Bernoulli values.
-            for (int e = tid; e < ne; e += nth) {
+            for (int e = ef; e < el; e += es) {
                 if (!t.ei[e]) continue;
                 const int a = t.ea[e], b = t.eb[e];
+                // the z = -1 group's argument is exactly minus the z = +1 group's
+                // (x = (-0.03742f) * dV rounds symmetrically), so its two values are
+                // the z = +1 group's, swapped
                 float bm[3], bp[3];
 #pragma unroll
-                for (int g = 0; g < 3; g++) {
+                for (int g = 0; g < 2; g++) {
                     const float x = valence_factor(g) * t.dve[e];
                     bm[g] = sg_bernoulli(-x);
                     bp[g] = sg_bernoulli(x);
                 }
+                bm[2] = bp[0];
+                bp[2] = bm[0];
                 float ie = t.ie[e];
 #pragma unroll
                 for (int q = 0; q < 7; q++) {
@@ -642,11 +711,11 @@ k_diffusion(NetDev d, float dt, unsigned long long tick, uint32_t S, uint32_t E)
                     const int g = valence_group(q);
                     const float flux = t.coef[q * E + e] * (C_a * bm[g] - C_b * bp[g]);
                     t.fl[q * E + e] = flux;
-                    ie += kNpZ[q] * 96.485f * flux / dt_sub;
+                    ie += div_rn_f(kNpZ[q] * 96.485f * flux, dt_sub, ydts);
                 }
                 t.ie[e] = ie;
             }
-            tile_sync<CL>();
+            tile_sync<CL>(gm);
             {   // reads connection fluxes and its own concentrations: in place
                 const float vf = i < ns ? t.vf[i] : 1.0f;
                 const double yv = 1.0 / (double)vf;
@@ -681,13 +750,13 @@ k_diffusion(NetDev d, float dt, unsigned long long tick, uint32_t S, uint32_t E)
                     if (OPT && (d.diff_mode & 2u)) ledger_add(sh_ledger, q, lost);
                 }
             }
-            tile_sync<CL>();
-            for (int e = tid; e < ne; e += nth) {
+            tile_sync<CL>(gm);
+            for (int e = ef; e < el; e += es) {
                 if (!t.ei[e]) continue;
                 t.ie[e] = t.ie[e] - t.gax[e] * t.dve[e];
             }
-            tile_sync<CL>();
-            float rhs = 0.0f, den = 1.0f, C_dtv = 1.0f, inpv = 0.0f;
+            tile_sync<CL>(gm);
+            float rhs = 0.0f, den = 1.0f, yden = 1.0f, C_dtv = 1.0f, inpv = 0.0f;
             if (i < ns) {
                 float inp = 0.0f;
                 if (st.n >= 0) {
@@ -710,12 +779,13 @@ k_diffusion(NetDev d, float dt, unsigned long long tick, uint32_t S, uint32_t E)
                 if (C_dt < 1e-9f) C_dt = 1e-9f;
                 rhs = C_dt * t.V[i] + inp;
                 den = C_dt + gd;
+                yden = 1.0f / den;
                 C_dtv = C_dt;
                 inpv = inp;
                 t.vnA[i] = t.V[i];
             }
             for (int g = tid; g < ng; g += nth) t.vnA[ns + g] = t.V[ns + g];
-            tile_sync<CL>();
+            tile_sync<CL>(gm);
             float* vc = t.vnA;
             float* vn = t.vnB;
             if (OPT && (d.diff_mode & 1u)) {
@@ -756,16 +826,16 @@ k_diffusion(NetDev d, float dt, unsigned long long tick, uint32_t S, uint32_t E)
                         float off = 0.0f;
                         if (h0) off += g0 * t.vnA[o0];
                         if (h1) off += g1 * t.vnA[o1];
-                        t.vnB[i] = (rhs + off) / den;
+                        t.vnB[i] = div_rn_f(rhs + off, den, yden);
                     }
-                    __syncthreads();
+                    tile_sync<CL>(gm);
                     if (i < ns) {
                         float off = 0.0f;
                         if (h0) off += g0 * t.vnB[o0];
                         if (h1) off += g1 * t.vnB[o1];
-                        t.vnA[i] = (rhs + off) / den;
+                        t.vnA[i] = div_rn_f(rhs + off, den, yden);
                     }
-                    __syncthreads();
+                    tile_sync<CL>(gm);
                 }
             } else
             for (int it = 0; it < 50; it++) {
@@ -784,14 +854,14 @@ k_diffusion(NetDev d, float dt, unsigned long long tick, uint32_t S, uint32_t E)
                             off += t.gax[e] * vc[o];
                         }
                     }
-                    vn[i] = (rhs + off) / den;
+                    vn[i] = div_rn_f(rhs + off, den, yden);
                 }
-                tile_sync<CL>();
+                tile_sync<CL>(gm);
                 halo<CL>(vn, 1, S, ns, ng, t.gsrc, tid, nth);
                 float* tmp = vc; vc = vn; vn = tmp;
             }
             if (i < ns) t.V[i] = vc[i];
-            tile_sync<CL>();
+            tile_sync<CL>(gm);
             halo<CL>(t.V, 1, S, ns, ng, t.gsrc, tid, nth);
             halo<CL>(t.in, 7, S, ns, ng, t.gsrc, tid, nth);
         }
@@ -800,20 +870,21 @@ k_diffusion(NetDev d, float dt, unsigned long long tick, uint32_t S, uint32_t E)
         // phi_e is fixed for the tick, so each connection's Bernoulli values are too:
         // x = (float)((z * 0.03742f) * dphi) per valence group.
         float xbm0 = 0.0f, xbm1 = 0.0f, xbm2 = 0.0f, xbp0 = 0.0f, xbp1 = 0.0f, xbp2 = 0.0f;
-        if (edge_reg && tid < ne) {
-            const double dphi = phi[t.ea[tid]] - phi[t.eb[tid]];
+        if (edge_reg && my_edge >= 0) {
+            const double dphi = phi[t.ea[my_edge]] - phi[t.eb[my_edge]];
             float x = (float)(valence_factor(0) * dphi);
             xbm0 = sg_bernoulli(-x); xbp0 = sg_bernoulli(x);
             x = (float)(valence_factor(1) * dphi);
             xbm1 = sg_bernoulli(-x); xbp1 = sg_bernoulli(x);
-            x = (float)(valence_factor(2) * dphi);
-            xbm2 = sg_bernoulli(-x); xbp2 = sg_bernoulli(x);
+            xbm2 = xbp0; xbp2 = xbm0;   // the z = -1 argument is minus the z = +1 one
         }
         for (int sub = 0; sub < 5; sub++) {
+            const float vx_seg = (i < ns ? t.vf[i] : 1.0f) * EXTRA_VOLUME_RATIO;
+            const double yx_d = 1.0 / (double)vx_seg;
 #pragma unroll 1
             for (int q = 0; q < 7; q++) {
                 const int g = valence_group(q);
-                for (int e = tid; e < ne; e += nth) {
+                for (int e = ef; e < el; e += es) {
                     const int a = t.ea[e], b = t.eb[e];
                     const double Ca = t.out[q * S + a];
                     const double Cb = t.out[q * S + b];
@@ -828,12 +899,12 @@ k_diffusion(NetDev d, float dt, unsigned long long tick, uint32_t S, uint32_t E)
                     const double flux = t.coef[q * E + e] * (Ca * bm - Cb * bp);
                     t.ed[e] = flux;
                 }
-                tile_sync<CL>();
+                tile_sync<CL>(gm);
                 double lost = 0.0;
                 if (i < ns) {   // in place, as above
                     const float vf = t.vf[i];
-                    const float vx = vf * EXTRA_VOLUME_RATIO;
-                    const double yx = 1.0 / (double)vx;
+                    const float vx = vx_seg;
+                    const double yx = yx_d;
                     double acc = 0.0;
                     if (st.n >= 0) {
 #pragma unroll
@@ -858,18 +929,19 @@ k_diffusion(NetDev d, float dt, unsigned long long tick, uint32_t S, uint32_t E)
                     lost = ((double)upd - (double)old - acc) * (double)vx;
                 }
                 if (OPT && (d.diff_mode & 2u)) ledger_add(sh_ledger, q, lost);
-                tile_sync<CL>();
+                tile_sync<CL>(gm);
                 halo<CL>(t.out + (size_t)q * S, 1, S, ns, ng, t.gsrc, tid, nth);
             }
         }
 
         // ---- NT / ATP / heat / transcription (diffusion_kernel.h:284-363) ----
+        const float yvf = 1.0f / (i < ns ? t.vf[i] : 1.0f);
         if (d.flags & NF_INTRA_NT) {
             for (int nt = 0; nt < 15; nt++) {
                 if (i < ns) t.nb[i] = d.intra_nt[(size_t)nt * N + s0 + i];
                 for (int g = tid; g < ng; g += nth) t.nb[ns + g] = d.intra_nt[(size_t)nt * N + d.gh_seg[gh0 + g]];
-                tile_sync<CL>();
-                fick<CL, true, false>(t, ns, ne, tid, nth, i, st, gNtD[nt], 1e-12f, dt);
+                tile_sync<CL>(gm);
+                fick<CL, true, false>(t, ns, ef, el, es, gm, i, st, gNtD[nt], 1e-12f, dt, yvf, edge_reg, rde);
                 if (i < ns) d.intra_nt[(size_t)nt * N + s0 + i] = t.nb[i];
             }
         }
@@ -877,30 +949,30 @@ k_diffusion(NetDev d, float dt, unsigned long long tick, uint32_t S, uint32_t E)
             for (int nt = 0; nt < 15; nt++) {
                 if (i < ns) t.nb[i] = d.nt[(size_t)nt * N + s0 + i];
                 for (int g = tid; g < ng; g += nth) t.nb[ns + g] = d.nt[(size_t)nt * N + d.gh_seg[gh0 + g]];
-                tile_sync<CL>();
-                fick<CL, false, false>(t, ns, ne, tid, nth, i, st, gNtD[nt], 1e-12f, dt);
+                tile_sync<CL>(gm);
+                fick<CL, false, false>(t, ns, ef, el, es, gm, i, st, gNtD[nt], 1e-12f, dt, yvf, edge_reg, rde);
                 if (i < ns) d.nt[(size_t)nt * N + s0 + i] = t.nb[i];
             }
         }
         {
             if (i < ns) t.nb[i] = t.atp[i];
             for (int g = tid; g < ng; g += nth) t.nb[ns + g] = t.atp[ns + g];
-            tile_sync<CL>();
-            fick<CL, true, true>(t, ns, ne, tid, nth, i, st, 0.14f, 1e-12f, dt);
+            tile_sync<CL>(gm);
+            fick<CL, true, true>(t, ns, ef, el, es, gm, i, st, 0.14f, 1e-12f, dt, yvf, edge_reg, rde);
             if (i < ns) t.atp[i] = t.nb[i];
         }
         if (d.flags & NF_TEMP) {
             if (i < ns) t.nb[i] = d.temp[s0 + i];
             for (int g = tid; g < ng; g += nth) t.nb[ns + g] = d.temp[d.gh_seg[gh0 + g]];
-            tile_sync<CL>();
-            fick<CL, true, true>(t, ns, ne, tid, nth, i, st, 0.0014f, 0.001f, dt);
+            tile_sync<CL>(gm);
+            fick<CL, true, true>(t, ns, ef, el, es, gm, i, st, 0.0014f, 0.001f, dt, yvf, edge_reg, rde);
             if (i < ns) d.temp[s0 + i] = t.nb[i];
         }
         if (d.flags & NF_TXN) {
             if (i < ns) t.nb[i] = d.txn[s0 + i];
             for (int g = tid; g < ng; g += nth) t.nb[ns + g] = d.txn[d.gh_seg[gh0 + g]];
-            tile_sync<CL>();
-            fick<CL, true, true>(t, ns, ne, tid, nth, i, st, 0.01f, 1e-9f, dt);
+            tile_sync<CL>(gm);
+            fick<CL, true, true>(t, ns, ef, el, es, gm, i, st, 0.01f, 1e-9f, dt, yvf, edge_reg, rde);
             if (i < ns) d.txn[s0 + i] = t.nb[i];
         }
         if (OPT && (d.diff_mode & 2u)) {
@@ -975,14 +1047,15 @@ cudaError_t prepare_diffusion(const NetHost& host, cudaStream_t stream) {
     }
     const size_t smem = diffusion_smem_bytes(host.max_tile_stride, host.max_tile_edges);
     if (smem > 48 * 1024) {
+        const int a = cudaFuncAttributeMaxDynamicSharedMemorySize;
         if (host.cluster == 2) {
-            e = cudaFuncSetAttribute(k_diffusion<2, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            if (e == cudaSuccess)
-                e = cudaFuncSetAttribute(k_diffusion<2, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            e = cudaFuncSetAttribute(k_diffusion<2, 0, 0>, (cudaFuncAttribute)a, (int)smem);
+            if (e == cudaSuccess) e = cudaFuncSetAttribute(k_diffusion<2, 1, 0>, (cudaFuncAttribute)a, (int)smem);
         } else {
-            e = cudaFuncSetAttribute(k_diffusion<1, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            if (e == cudaSuccess)
-                e = cudaFuncSetAttribute(k_diffusion<1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            e = cudaFuncSetAttribute(k_diffusion<1, 0, 0>, (cudaFuncAttribute)a, (int)smem);
+            if (e == cudaSuccess) e = cudaFuncSetAttribute(k_diffusion<1, 1, 0>, (cudaFuncAttribute)a, (int)smem);
+            if (e == cudaSuccess) e = cudaFuncSetAttribute(k_diffusion<1, 0, 32>, (cudaFuncAttribute)a, (int)smem);
+            if (e == cudaSuccess) e = cudaFuncSetAttribute(k_diffusion<1, 0, 64>, (cudaFuncAttribute)a, (int)smem);
         }
         return e;
     }
@@ -1023,7 +1096,7 @@ cudaError_t enqueue_diffusion(const NetDev& dev, const NetHost& host, float dt, 
     }
     const uint32_t S = host.max_tile_stride, E = host.max_tile_edges;
     const size_t smem = diffusion_smem_bytes(S, E);
-    const uint32_t threads = diffusion_threads(host.max_tile_segs);
+    const uint32_t threads = std::max(host.diff_threads, diffusion_threads(host.max_tile_segs));
     const bool opt = dev.diff_mode != 0u;
     if (host.cluster == 2) {
         // tiles in pairs: one 2-CTA cluster per pair (n_tiles is even)
@@ -1039,11 +1112,17 @@ cudaError_t enqueue_diffusion(const NetDev& dev, const NetHost& host, float dt, 
         attr[0].val.clusterDim.z = 1;
         cfg.attrs = attr;
         cfg.numAttrs = 1;
-        return opt ? cudaLaunchKernelEx(&cfg, k_diffusion<2, 1>, dev, dt, tick, S, E)
-                   : cudaLaunchKernelEx(&cfg, k_diffusion<2, 0>, dev, dt, tick, S, E);
+        return opt ? cudaLaunchKernelEx(&cfg, k_diffusion<2, 1, 0>, dev, dt, tick, S, E)
+                   : cudaLaunchKernelEx(&cfg, k_diffusion<2, 0, 0>, dev, dt, tick, S, E);
     }
-    if (opt) k_diffusion<1, 1><<<dev.n_tiles, threads, smem, stream>>>(dev, dt, tick, S, E);
-    else k_diffusion<1, 0><<<dev.n_tiles, threads, smem, stream>>>(dev, dt, tick, S, E);
+    // barrier groups: only with each segment's connection assignment, and for 64-thread
+    // groups only with whole groups of two warps (named barriers 1..15)
+    int gm = (opt || !dev.seg_edge) ? 0 : (int)host.diff_gm;
+    if (gm == 64 && (threads % 64u != 0u || threads > 960u)) gm = 0;
+    if (opt) k_diffusion<1, 1, 0><<<dev.n_tiles, threads, smem, stream>>>(dev, dt, tick, S, E);
+    else if (gm == 64) k_diffusion<1, 0, 64><<<dev.n_tiles, threads, smem, stream>>>(dev, dt, tick, S, E);
+    else if (gm == 32) k_diffusion<1, 0, 32><<<dev.n_tiles, threads, smem, stream>>>(dev, dt, tick, S, E);
+    else k_diffusion<1, 0, 0><<<dev.n_tiles, threads, smem, stream>>>(dev, dt, tick, S, E);
     return cudaGetLastError();
 }
 

@@ -83,6 +83,9 @@ struct NetDev {
     uint32_t* phase_off;      // [n_chunks*n_phases+1] item offsets of the (chunk, phase) buckets
     uint16_t* warp_seg;       // [n_tiles*(kTileWarps+1)] tile-local offsets
     uint16_t* warp_edge;      // [n_tiles*(kTileWarps+1)]
+    // diffusion barrier groups (NetHost::diff_gm nonzero): per segment the tile-local
+    // connection its thread handles (0xFFFF: none); null otherwise
+    uint16_t* seg_edge;
     // edges (tile-grouped, tile-local endpoints)
     uint16_t* e_a;
     uint16_t* e_b;
@@ -207,6 +210,9 @@ struct BuildOptions {
     // 1: 3.94, 2: 2.89, 3: 2.40, 4: 2.15, 6: 2.43, 9: 4.97, 17: 19.5 ms (deeper groups
     // diverge: rows sorted by their items' types share fewer types further down).
     uint32_t fuse_phases = 4;
+    // Diffusion barriers over aligned thread groups where the tile allows (false: always
+    // the whole CTA).
+    bool group_barriers = true;
 };
 constexpr uint32_t kMaxFuse = 32;
 
@@ -224,6 +230,9 @@ struct NetHost {
     uint32_t max_tile_segs = 0, max_tile_edges = 0;
     uint32_t max_tile_stride = 0;            // own + ghost segments of the largest tile
     uint32_t cluster = 1;                    // CTAs per diffusion cluster (2: tiles in pairs)
+    uint32_t diff_threads = 32;              // threads per diffusion CTA
+    uint32_t diff_gm = 0;                    // diffusion barrier groups: 0 (CTA), 32 or 64 threads
+    uint32_t group_tiles_32 = 0, group_tiles_64 = 0;   // tiles with warp / 64-thread barrier groups
     std::vector<uint32_t> phase_off;         // item range of each (chunk, phase) bucket (host copy)
     uint32_t chunk_segs = 0, n_chunks = 1;   // modifier-pass chunks of consecutive segments
     uint32_t fuse = 1;                       // modifier phases per launch (item order follows)

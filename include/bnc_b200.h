@@ -216,6 +216,8 @@ typedef struct {
     double modifier_kernel_bytes, diffusion_kernel_bytes;  /* per launch of each (state round trip included) */
     uint32_t modifier_launches;   /* launches of step 1 per tick: k_gather, phase launches, device modifiers */
     uint32_t fuse_phases;         /* modifier phases per launch the network runs with */
+    uint32_t group_tiles_32, group_tiles_64;  /* tiles whose diffusion barriers span one warp / 64 threads */
+    uint32_t diffusion_threads;   /* threads per diffusion CTA */
 } BncNetInfo;
 int bnc_network_info(void* sim, BncNetInfo* info);
 
@@ -299,6 +301,9 @@ int bnc_run_ticks_graph(void* sim, uint32_t n_ticks, float dt);
  * Zero fields take the defaults. */
 typedef struct {
     uint32_t warp_cap, tile_segs, phase_cap, chunk_segs, fuse_phases;
+    /* nonzero: the diffusion kernel synchronises whole CTAs even where every
+     * connection stays inside an aligned group of 32 or 64 threads (for tests) */
+    uint32_t cta_barriers;
 } BncBuildOptions;
 #define BNC_DEFAULT_CHUNK_SEGS 0xFFFFFFFFu
 int bnc_load_generated_opts(void* sim, const BncNetgenParams* p, const BncBuildOptions* opt);

@@ -111,6 +111,39 @@ def test_chunked_modifier_pass_bitexact(chunk):
         _compare_all(ora, gpu, n_syn, "chunk %d after +%d" % (chunk, step))
 
 
+@pytest.mark.parametrize("family,cta_barriers", [("small", 0), ("small", 1), ("large", 0), ("large", 1)])
+def test_diffusion_barrier_groups_bitexact(family, cta_barriers):
+    """The diffusion kernel with barriers over a warp (32-segment neurons) or a pair of
+    warps (64-segment neurons), and with CTA-wide barriers: both are the oracle's tick,
+    bit for bit, through releases."""
+    from bioneuroncore_b200 import Backend, BuildOptions, Network, NetgenParams, NET_LARGE, NET_SMALL
+    if family == "small":
+        p = NetgenParams(family=NET_SMALL, n_neurons=40, seed=6, flags=32, stim_pA=3000.0)
+    else:
+        p = NetgenParams(family=NET_LARGE, n_neurons=20, seed=3)
+    ora = Oracle(Network(p))
+    gpu = Backend()
+    gpu.load_generated(p, BuildOptions(cta_barriers=cta_barriers))
+    info = gpu.info()
+    grouped = info.group_tiles_32 + info.group_tiles_64
+    assert (grouped == 0) if cta_barriers else (grouped == info.n_tiles)
+    n_syn = ora.n_syn
+    for step in (1, 99, 200):
+        ora.run(step, DT)
+        gpu.run_ticks(step, DT)
+        label = "%s cta_barriers=%d after +%d" % (family, cta_barriers, step)
+        for f, i in SEG_CHECKS:
+            _assert_same(gpu.segment_field(f, i), ora.segment_field(f, i), "%s %s[%d]" % (label, f, i))
+        # gate words of the channel slots (a generated network loaded without host
+        # records reads back only the state words its models update)
+        for slot in range(5):
+            for k in range(2):
+                _assert_same(gpu.segment_field("mod_state", slot * 8 + k), ora.segment_field("mod_state", slot * 8 + k),
+                             "%s modifier slot %d state %d" % (label, slot, k))
+        for f, i in SYN_CHECKS:
+            _assert_same(gpu.synapse_field(f, i, n_syn), ora.synapse_field(f, i), "%s synapse %s[%d]" % (label, f, i))
+
+
 @pytest.mark.parametrize("fuse", [1, 3, 4, 17])
 def test_fused_modifier_phases_bitexact(fuse):
     """Several modifier phases per launch (each segment's items of those phases run on

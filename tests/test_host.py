@@ -94,6 +94,23 @@ def test_modifier_phase_groups():
     assert ch.fuse_phases == 1
 
 
+def test_diffusion_barrier_groups():
+    """Tiles whose connections stay inside aligned groups of 32 or 64 threads get
+    barriers of that group (32-segment neurons: a warp each; 64-segment neurons: a
+    named 64-thread barrier), with a CTA of whole 64-thread groups; trees split over
+    2-CTA clusters keep cluster barriers; the option turns the groups off."""
+    from bioneuroncore_b200 import BuildOptions, plan_generated, NetgenParams, NET_SMALL, NET_LARGE, NET_TREES
+    small = plan_generated(NetgenParams(family=NET_SMALL, n_neurons=64, seed=1))
+    assert small.group_tiles_32 == small.n_tiles and small.group_tiles_64 == 0
+    large = plan_generated(NetgenParams(family=NET_LARGE, n_neurons=100, seed=1))
+    assert large.group_tiles_64 == large.n_tiles and large.group_tiles_32 == 0
+    assert large.diffusion_threads % 64 == 0 and large.diffusion_threads <= 960
+    off = plan_generated(NetgenParams(family=NET_LARGE, n_neurons=100, seed=1), BuildOptions(cta_barriers=1))
+    assert off.group_tiles_32 == off.group_tiles_64 == 0
+    trees = plan_generated(NetgenParams(family=NET_TREES, n_neurons=2, tree_depth=10, seed=1))
+    assert trees.group_tiles_32 == trees.group_tiles_64 == 0
+
+
 def test_plan_aos_accepts_generated_network():
     net = _net(family=1, n_neurons=4, seed=5)
     rc, info = _plan_aos(net)
