@@ -35,7 +35,8 @@ DROPIN_SYMBOLS = ["gpu_backend_create", "gpu_backend_create_on_device", "gpu_bac
                   "gpu_backend_upload_stimuli", "gpu_backend_device_count", "gpu_backend_get_device_info",
                   "gpu_backend_ibuf_offset", "gpu_backend_vm_offset", "gpu_backend_seg_size"]
 NEW_SYMBOLS = ["bnc_netgen_aos", "bnc_netgen_free", "bnc_last_error", "bnc_load_aos", "bnc_load_generated",
-               "bnc_run_ticks", "bnc_time_ticks", "bnc_sync_to_host", "bnc_read_segment_field",
+               "bnc_run_ticks", "bnc_time_ticks", "bnc_sync_to_host", "bnc_records_managed", "bnc_set_records_residency",
+               "bnc_read_segment_field",
                "bnc_read_synapse_field", "bnc_set_synapse_scale", "bnc_network_info", "bnc_save_bion",
                "bnc_plan_generated", "bnc_step_io", "bnc_profile_ticks", "bnc_run_ticks_static_scratch",
                "bnc_plan_aos", "bnc_bion_load", "bnc_bion_unload", "bnc_bion_save", "bnc_load_ensemble_generated",
@@ -149,7 +150,8 @@ def load_library(path=LIB_PATH):
         "bnc_netgen_aos": ([vp, vp, vp, vp], i32), "bnc_netgen_free": ([vp, vp], None),
         "bnc_last_error": ([], C.c_char_p), "bnc_load_aos": ([vp, vp, vp, u32], i32),
         "bnc_load_generated": ([vp, vp], i32), "bnc_run_ticks": ([vp, u32, f32], i32),
-        "bnc_time_ticks": ([vp, u32, f32, vp], i32), "bnc_sync_to_host": ([vp], i32),
+        "bnc_time_ticks": ([vp, u32, f32, vp], i32), "bnc_sync_to_host": ([vp], i32), "bnc_records_managed": ([vp], i32),
+        "bnc_set_records_residency": ([vp, i32], i32),
         "bnc_read_segment_field": ([vp, i32, i32, vp, u32], i32),
         "bnc_read_synapse_field": ([vp, i32, i32, vp, u32], i32),
         "bnc_set_synapse_scale": ([vp, vp, u32], i32), "bnc_network_info": ([vp, vp], i32),

@@ -38,6 +38,18 @@ struct Backend {
     std::vector<BncLigandInjection> pend_lig;
     uint64_t tick = 0;
     uint64_t ticks_run = 0;
+    // Drop-in records (aos.segments, aos.synapses) in managed memory, written on the
+    // device after each tick; the index maps the export kernels need (owned by allocs)
+    bool aos_managed = false;
+    struct {
+        uint32_t* perm;       // device segment -> record
+        uint32_t* item_seg;   // item -> record
+        uint16_t* item_sm;    // item -> modifier slot | state words it updates << 8
+        uint32_t* syn_orig;   // device synapse -> record
+        uint8_t* syn_nt;      // device synapse -> the cleft entry it carries
+        uint32_t* rec_syn;    // device receptor -> device synapse
+        uint8_t* rec_slot;    // device receptor -> receptor slot
+    } xm{};
     uint32_t tick_stride = 1;   // the tick counter's step per tick (2: the reference's batch mode)
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     // ensemble members (empty for a single network): ranges in original order
@@ -59,10 +71,20 @@ struct Backend {
     }
     void free_aos() {
         if (owns_aos) {
-            delete[] aos.neurons; delete[] aos.segments; delete[] aos.connections; delete[] aos.synapses;
+            delete[] aos.neurons;
+            delete[] aos.connections;
+            if (aos_managed) {
+                cudaFree(aos.segments);
+                cudaFree(aos.synapses);
+            } else {
+                delete[] aos.segments;
+                delete[] aos.synapses;
+            }
         }
         std::memset(&aos, 0, sizeof(aos));
         owns_aos = false;
+        aos_managed = false;
+        std::memset(&xm, 0, sizeof(xm));
     }
     void drop_graph() {
         if (graph_exec) cudaGraphExecDestroy(graph_exec);
@@ -341,6 +363,198 @@ static int gather_generated(const BncNetgenParams* params, uint32_t n, HostNet* 
 
 }  // namespace
 
+static int sync_stream(Backend* b);
+
+// ---- Drop-in records in managed memory ----
+// The reference's backend keeps the Segment and Synapse records in managed memory and
+// its kernels update them in place (bion_loader.cpp:634, gpu_backend_cuda.cu:250-308):
+// after a tick the records are coherent, and a host read migrates only the pages it
+// touches.  The same here: the records of a network loaded for the drop-in calls move
+// to managed memory, and after each tick these kernels write the changing words of
+// the device state into them (the words export_network writes on the host path).
+// Records are packed structs; every word written sits at its natural alignment
+// (BncSegment V_m at 40, ions at 48 and 112, modifier states at 296 + 88 j + 16, ...).
+namespace {
+template <typename T>
+__device__ __forceinline__ void put(unsigned char* rec, size_t off, T v) { *reinterpret_cast<T*>(rec + off) = v; }
+
+constexpr size_t kSegBytes = sizeof(BncSegment), kSynBytes = sizeof(BncSynapse), kModBytes = sizeof(BncModifier);
+constexpr size_t kOffMods = offsetof(BncSegment, modifiers), kOffModState = offsetof(BncModifier, state);
+static_assert(offsetof(BncSegment, V_m) % 8 == 0 && offsetof(BncSegment, intra_ions) % 8 == 0 &&
+              offsetof(BncSegment, extra_ions) % 8 == 0 && offsetof(BncSegment, I_buffer) % 8 == 0 &&
+              kOffMods % 8 == 0 && kModBytes % 8 == 0 && kOffModState % 8 == 0 && kSegBytes % 8 == 0 &&
+              offsetof(BncSynapse, post_receptors) % 8 == 0 && kSynBytes % 8 == 0 &&
+              offsetof(BncSegment, neurotransmitter) % 4 == 0 && offsetof(BncSegment, intra_nt) % 4 == 0 &&
+              offsetof(BncSegment, ATP_level) % 4 == 0 && offsetof(BncSegment, temperature) % 4 == 0 &&
+              offsetof(BncSegment, transcription_signal) % 4 == 0 && offsetof(BncSynapse, bouton_Ca) % 4 == 0 &&
+              offsetof(BncSynapse, cleft_neurotransmitter) % 4 == 0,
+              "record words are naturally aligned");
+
+__global__ void k_export_segments(NetDev d, const uint32_t* perm, unsigned char* seg, int x_int, int x_temp,
+                                  int x_txn, int clear_ibuf) {
+    const uint32_t n = d.n_seg;
+    for (uint32_t dd = blockIdx.x * blockDim.x + threadIdx.x; dd < n; dd += gridDim.x * blockDim.x) {
+        unsigned char* r = seg + (size_t)perm[dd] * kSegBytes;
+        put<double>(r, offsetof(BncSegment, V_m), (double)d.V[dd]);
+        for (int q = 0; q < 7; q++) {
+            put<double>(r, offsetof(BncSegment, intra_ions) + 8 * q, (double)d.ion_in[(size_t)q * n + dd]);
+            put<double>(r, offsetof(BncSegment, extra_ions) + 8 * q, (double)d.ion_out[(size_t)q * n + dd]);
+        }
+        for (int q = 0; q < 15; q++) put<float>(r, offsetof(BncSegment, neurotransmitter) + 4 * q, d.nt[(size_t)q * n + dd]);
+        if (x_int)
+            for (int q = 0; q < 15; q++) put<float>(r, offsetof(BncSegment, intra_nt) + 4 * q, d.intra_nt[(size_t)q * n + dd]);
+        put<float>(r, offsetof(BncSegment, ATP_level), d.atp[dd]);
+        if (x_temp) put<float>(r, offsetof(BncSegment, temperature), d.temp[dd]);
+        if (x_txn) put<float>(r, offsetof(BncSegment, transcription_signal), d.txn[dd]);
+        if (clear_ibuf) put<double>(r, offsetof(BncSegment, I_buffer), 0.0);   // step 4 clears it
+    }
+}
+
+// One thread per modifier item: the state words its type updates, and (after a tick)
+// state[7], the effective area the tick wrote (run_tick_common.h:234-238), computed
+// from the record's geometry as the host export does.
+__global__ void k_export_items(NetDev d, const uint32_t* item_seg, const uint16_t* item_sm, unsigned char* seg,
+                               int set_area) {
+    const uint32_t NI = d.n_items;
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < NI; q += gridDim.x * blockDim.x) {
+        unsigned char* r = seg + (size_t)item_seg[q] * kSegBytes;
+        const uint32_t sm = item_sm[q];
+        unsigned char* m = r + kOffMods + (size_t)(sm & 0xFFu) * kModBytes;
+        const uint32_t wm = sm >> 8;
+        for (int k = 0; k < 7; k++)
+            if ((wm >> k) & 1u) put<double>(m, kOffModState + 8 * k, (double)d.it_st[(size_t)k * NI + q]);
+        if (set_area) {
+            const uint8_t st = r[offsetof(BncSegment, segment_type)];
+            const float rad = *reinterpret_cast<const float*>(r + offsetof(BncSegment, radius));
+            const float len = *reinterpret_cast<const float*>(r + offsetof(BncSegment, length));
+            const float area = (st == 1 || st == 3 || st == 4) ? 4.0f * 3.14159265f * rad * rad
+                                                                : 2.0f * 3.14159265f * rad * len;
+            put<double>(m, kOffModState + 8 * 7, (double)area);
+        }
+    }
+}
+
+__global__ void k_export_synapses(NetDev d, const uint32_t* syn_orig, const uint8_t* syn_nt, unsigned char* syn,
+                                  int after_tick) {
+    const uint32_t K = d.n_syn;
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < K; q += gridDim.x * blockDim.x) {
+        unsigned char* y = syn + (size_t)syn_orig[q] * kSynBytes;
+        put<float>(y, offsetof(BncSynapse, bouton_Ca), d.sy_bouton[q]);
+        put<float>(y, offsetof(BncSynapse, spine_Ca), d.sy_spine[q]);
+        put<float>(y, offsetof(BncSynapse, spine_camkii), d.sy_camkii[q]);
+        put<float>(y, offsetof(BncSynapse, spine_calcineurin), d.sy_calcn[q]);
+        put<float>(y, offsetof(BncSynapse, facilitation), d.sy_facil[q]);
+        put<float>(y, offsetof(BncSynapse, weight), d.sy_weight[q]);
+        put<float>(y, offsetof(BncSynapse, cleft_neurotransmitter) + 4 * (size_t)syn_nt[q], d.sy_cleft[q]);
+        put<float>(y, offsetof(BncSynapse, RRP), d.sy_rrp[q]);
+        y[offsetof(BncSynapse, refractory)] = d.sy_refr[q];
+        if (after_tick) put<float>(y, offsetof(BncSynapse, depression), d.sy_facil[q] + 0.01f);
+    }
+}
+
+__global__ void k_export_receptors(NetDev d, const uint32_t* rec_syn, const uint8_t* rec_slot, const uint32_t* syn_orig,
+                                   unsigned char* syn, int after_tick) {
+    const uint32_t NR = d.n_rec;
+    for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < NR; r += gridDim.x * blockDim.x) {
+        unsigned char* y = syn + (size_t)syn_orig[rec_syn[r]] * kSynBytes;
+        unsigned char* m = y + offsetof(BncSynapse, post_receptors) + (size_t)rec_slot[r] * kModBytes;
+        for (int k = 0; k < 3; k++) put<double>(m, kOffModState + 8 * k, (double)d.rc_st[(size_t)k * NR + r]);
+        if (after_tick)
+            put<double>(m, kOffModState + 8 * 7, (double)*reinterpret_cast<const float*>(y + offsetof(BncSynapse, post_area)));
+    }
+}
+
+template <typename T>
+T* upload_map(Backend* b, const std::vector<T>& v, bool* ok) {
+    if (!*ok || v.empty()) return nullptr;
+    T* p = static_cast<T*>(b->allocs.alloc(v.size() * sizeof(T)));
+    if (!p || cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice) != cudaSuccess) *ok = false;
+    return p;
+}
+}  // namespace
+
+// Moves the records of a loaded single network into managed memory and uploads the
+// export maps.  Where the device cannot share managed memory with the host
+// concurrently the records stay in host memory and export_network updates them.
+static int make_records_managed(Backend* b) {
+    if (!b->owns_aos || !b->members.empty() || b->aos_managed) return BNC_OK;
+    int cma = 0;
+    if (cudaDeviceGetAttribute(&cma, cudaDevAttrConcurrentManagedAccess, b->device) != cudaSuccess || !cma) {
+        cudaGetLastError();
+        return BNC_OK;
+    }
+    const size_t n = b->aos.num_segments, k = b->aos.num_synapses;
+    void *ms = nullptr, *my = nullptr;
+    if (cudaMallocManaged(&ms, (n ? n : 1) * kSegBytes) != cudaSuccess ||
+        cudaMallocManaged(&my, (k ? k : 1) * kSynBytes) != cudaSuccess) {
+        cudaGetLastError();
+        if (ms) cudaFree(ms);
+        return BNC_OK;   // host records, host export
+    }
+    auto& x = b->xm;
+    if (!x.perm) {   // the export maps, once per network
+        const NetHost& h = b->host;
+        std::vector<uint16_t> sm(h.item_seg.size());
+        for (size_t q = 0; q < sm.size(); q++) {
+            const uint8_t t = b->aos.segments[h.item_seg[q]].modifiers[h.item_slot[q]].type;
+            const bool user = t < 128 && ((b->dev.user_mask[t >> 5] >> (t & 31)) & 1u);
+            sm[q] = (uint16_t)(h.item_slot[q] | ((user ? 0x7Fu : host_dyn_mask(t)) << 8));
+        }
+        bool ok = true;
+        x.perm = upload_map(b, h.perm, &ok);
+        x.item_seg = upload_map(b, h.item_seg, &ok);
+        x.item_sm = upload_map(b, sm, &ok);
+        x.syn_orig = upload_map(b, h.syn_orig, &ok);
+        x.syn_nt = upload_map(b, h.syn_nt, &ok);
+        x.rec_syn = upload_map(b, h.rec_syn, &ok);
+        x.rec_slot = upload_map(b, h.rec_slot, &ok);
+        if (!ok) {
+            cudaFree(ms);
+            cudaFree(my);
+            std::memset(&x, 0, sizeof(x));
+            return cuda_fail(cudaGetLastError(), "upload of the record export maps");
+        }
+    }
+    if (n) std::memcpy(ms, b->aos.segments, n * kSegBytes);
+    if (k) std::memcpy(my, b->aos.synapses, k * kSynBytes);
+    delete[] b->aos.segments;
+    delete[] b->aos.synapses;
+    b->aos.segments = static_cast<BncSegment*>(ms);
+    b->aos.synapses = static_cast<BncSynapse*>(my);
+    b->aos_managed = true;
+    // the device writes the records every tick: start them resident there
+    cudaMemPrefetchAsync(ms, (n ? n : 1) * kSegBytes, b->device, b->stream);
+    cudaMemPrefetchAsync(my, (k ? k : 1) * kSynBytes, b->device, b->stream);
+    cudaGetLastError();
+    return BNC_OK;
+}
+
+// The records coherent with the device state: on the device into managed records,
+// else by the host export.  The stream is synchronised on return.
+static int export_records(Backend* b) {
+    if (!b->aos_managed) {
+        int rc = sync_stream(b);
+        if (rc != BNC_OK) return rc;
+        return export_network(b->dev, b->host, b->ticks_run, &b->aos);
+    }
+    const NetDev& d = b->dev;
+    const int after = b->ticks_run > 0 ? 1 : 0;
+    unsigned char* seg = reinterpret_cast<unsigned char*>(b->aos.segments);
+    unsigned char* syn = reinterpret_cast<unsigned char*>(b->aos.synapses);
+    auto grid = [](uint32_t m) { return (unsigned)std::min<uint32_t>((m + 255) / 256, 148u * 16u); };
+    if (d.n_seg)
+        k_export_segments<<<grid(d.n_seg), 256, 0, b->stream>>>(d, b->xm.perm, seg, (d.flags & NF_INTRA_NT) != 0,
+                                                                (d.flags & NF_TEMP) != 0, (d.flags & NF_TXN) != 0, after);
+    if (d.n_items) k_export_items<<<grid(d.n_items), 256, 0, b->stream>>>(d, b->xm.item_seg, b->xm.item_sm, seg, after);
+    if (d.n_syn) k_export_synapses<<<grid(d.n_syn), 256, 0, b->stream>>>(d, b->xm.syn_orig, b->xm.syn_nt, syn, after);
+    if (d.n_rec)
+        k_export_receptors<<<grid(d.n_rec), 256, 0, b->stream>>>(d, b->xm.rec_syn, b->xm.rec_slot, b->xm.syn_orig, syn,
+                                                                 after);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) { b->failed = true; return cuda_fail(e, "record export launch"); }
+    return sync_stream(b);
+}
+
 static int load_common(Backend* b, BncBionData& aos, bool keep_aos) {
     cudaSetDevice(b->device);
     HostNet hn;
@@ -349,6 +563,7 @@ static int load_common(Backend* b, BncBionData& aos, bool keep_aos) {
     if (rc != BNC_OK) { b->reset_network(); return rc; }
     if (keep_aos) { b->aos = aos; b->owns_aos = true; }
     b->loaded = true;
+    if (keep_aos) return make_records_managed(b);
     return BNC_OK;
 }
 
@@ -558,9 +773,7 @@ int backend_export_host(void* sim, HostNet* hn, std::vector<BncCurrentStimulus>*
     }
     if (!b->members.empty()) { set_error("an ensemble backend holds several networks"); return BNC_ERR_UNSUPPORTED; }
     cudaSetDevice(b->device);
-    int rc = sync_stream(b);
-    if (rc != BNC_OK) return rc;
-    rc = export_network(b->dev, b->host, b->ticks_run, &b->aos);
+    int rc = export_records(b);
     if (rc != BNC_OK) return rc;
     hostnet_from_aos(b->aos, hn);
     *stim = b->stim.current;
@@ -680,8 +893,7 @@ void gpu_backend_run_tick(void* sim, float dt) {
     if (!sim) return;
     Backend* b = static_cast<Backend*>(sim);
     if (run_ticks(b, 1, dt) != BNC_OK) return;
-    if (sync_stream(b) != BNC_OK) return;
-    export_network(b->dev, b->host, b->ticks_run, &b->aos);
+    export_records(b);
 }
 
 void* gpu_backend_bion_data(void* sim) {
@@ -1096,9 +1308,35 @@ int bnc_sync_to_host(void* sim) {
     if (!sim) { set_error("null handle"); return BNC_ERR_ARG; }
     Backend* b = static_cast<Backend*>(sim);
     cudaSetDevice(b->device);
+    return export_records(b);
+}
+
+int bnc_records_managed(void* sim) {
+    return (sim && static_cast<Backend*>(sim)->aos_managed) ? 1 : 0;
+}
+
+int bnc_set_records_residency(void* sim, int on_host) {
+    if (!sim) { set_error("null handle"); return BNC_ERR_ARG; }
+    Backend* b = static_cast<Backend*>(sim);
+    if (!b->loaded || !b->owns_aos) { set_error("no drop-in records"); return BNC_ERR_STATE; }
+    cudaSetDevice(b->device);
     int rc = sync_stream(b);
     if (rc != BNC_OK) return rc;
-    return export_network(b->dev, b->host, b->ticks_run, &b->aos);
+    if (!on_host) return b->aos_managed ? BNC_OK : make_records_managed(b);
+    if (!b->aos_managed) return BNC_OK;
+    // back to host records, updated by the bulk host export after each tick
+    const size_t n = b->aos.num_segments, k = b->aos.num_synapses;
+    BncSegment* hs = new (std::nothrow) BncSegment[n ? n : 1];
+    BncSynapse* hy = new (std::nothrow) BncSynapse[k ? k : 1];
+    if (!hs || !hy) { delete[] hs; delete[] hy; set_error("host record allocation failed"); return BNC_ERR_ALLOC; }
+    if (n) std::memcpy(hs, b->aos.segments, n * sizeof(BncSegment));
+    if (k) std::memcpy(hy, b->aos.synapses, k * sizeof(BncSynapse));
+    cudaFree(b->aos.segments);
+    cudaFree(b->aos.synapses);
+    b->aos.segments = hs;
+    b->aos.synapses = hy;
+    b->aos_managed = false;
+    return BNC_OK;
 }
 
 int bnc_read_segment_field(void* sim, int field, int index, float* out, uint32_t n) {

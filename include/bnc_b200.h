@@ -190,6 +190,21 @@ int bnc_profile_ticks(void* sim, uint32_t n_ticks, float dt, float* ms_modifiers
 
 /* Copies device state into the host AoS view (no-op when none is held). */
 int bnc_sync_to_host(void* sim);
+/* 1 when the handle's Segment/Synapse records (gpu_backend_bion_data) live in managed
+ * memory and are written on the device after each tick, as the reference's backend
+ * keeps them (bion_loader.cpp:634); 0 when they are host memory updated by a host
+ * export (devices without concurrent managed access) or there are none. */
+int bnc_records_managed(void* sim);
+/* Where the drop-in records live between ticks.  on_host = 0 (the default where the
+ * device supports concurrent managed access, as the reference's backend keeps them):
+ * managed memory resident on the device, written there after each tick; a host read
+ * migrates the pages it touches, and the next tick brings them back.  on_host = 1:
+ * plain host memory, updated after each tick by copying the changing state to the
+ * host and scattering it into the records on all host cores; for callers that read
+ * every record every tick.  A switch moves the records: the segments and synapses
+ * pointers of gpu_backend_bion_data change, and pointers taken before are invalid.
+ * BNC_ERR_STATE when the handle has no drop-in records. */
+int bnc_set_records_residency(void* sim, int on_host);
 
 /* Field reads in original segment / synapse order (host float arrays of n).
  * Segment fields: 0 V_m, 1 intra ion[index], 2 extra ion[index], 3 ATP,
