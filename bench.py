@@ -234,37 +234,121 @@ def cpu_reference_parallel(params, ticks, warm, procs):
     return seg_ticks / max(r[1] for r in res), procs
 
 
-def _ref_worker(args):
-    neurons, ticks, warm, seed = args
-    return cpu_reference_rate(neurons, ticks, warm, seed)
+class _RefBionData:
+    """The reference's BionData (include/bion_loader.h:16-28) for its own loader, defined
+    here so that the reference arm imports nothing of this backend."""
+    @staticmethod
+    def make():
+        import ctypes as C
+
+        class BionData(C.Structure):
+            _fields_ = [("header", C.c_uint8 * 100), ("neurons", C.c_void_p), ("segments", C.c_void_p),
+                        ("connections", C.c_void_p), ("synapses", C.c_void_p), ("nuclei", C.c_void_p),
+                        ("num_neurons", C.c_uint32), ("num_segments", C.c_uint32),
+                        ("num_connections", C.c_uint32), ("num_synapses", C.c_uint32), ("num_nuclei", C.c_uint32)]
+        return BionData()
+
+
+def write_reference_samples(out_dir, neurons, seeds):
+    """Child process of the reference arm: generates the sample networks with this
+    backend's seeded generator and writes each as a .bion with the reference's own
+    bion_save, plus its current steps (CurrentStimulus records) beside it."""
+    import ctypes as C
+    from bioneuroncore_b200 import Network, NetgenParams, NET_LARGE
+    from oracle import oracle as orc
+    ref = orc.reference_lib()
+    save = getattr(ref, "_Z9bion_savePKcPK8BionData")
+    save.argtypes = [C.c_char_p, C.c_void_p]
+    save.restype = C.c_int
+    for sd in seeds:
+        net = Network(NetgenParams(family=NET_LARGE, n_neurons=neurons, seed=sd))
+        path = os.path.join(out_dir, "sample_%d.bion" % sd)
+        if save(path.encode(), C.byref(net.data)) != 0:
+            raise RuntimeError("bion_save failed for %s" % path)
+        with open(path + ".stim", "wb") as f:
+            f.write(net.stimuli.tobytes())
+        net.close()
+
+
+def _ref_bion_worker(args):
+    """One reference-arm process: the reference's bion_load_host reads a sample .bion,
+    then its core_run_tick runs warm-up and timed ticks on it.  Returns (segment-ticks/s,
+    segments, whether this backend's library is mapped in the process)."""
+    path, ticks, warm = args
+    import ctypes as C
+    from oracle import oracle as orc
+    ref = orc.reference_lib()
+    load = getattr(ref, "_Z14bion_load_hostPKcP8BionData")
+    load.argtypes = [C.c_char_p, C.c_void_p]
+    load.restype = C.c_int
+    d = _RefBionData.make()
+    if load(path.encode(), C.byref(d)) != 0:
+        raise RuntimeError("bion_load_host failed for %s" % path)
+    raw = open(path + ".stim", "rb").read()
+    stim = (C.c_uint8 * max(len(raw), 1)).from_buffer_copy(raw or b"\0")
+    n_stim = C.c_uint32(len(raw) // 20)
+    tick = C.c_uint64(0)
+
+    def run(n):
+        for _ in range(n):
+            ref.core_run_tick(d.segments, d.num_segments, d.connections, d.num_connections, d.synapses,
+                              d.num_synapses, 0, C.byref(tick), C.c_float(DT), C.addressof(stim), C.byref(n_stim),
+                              *([None] * 10))
+    run(warm)
+    t0 = time.perf_counter()
+    run(ticks)
+    el = time.perf_counter() - t0
+    with open("/proc/self/maps") as f:
+        mapped = any("libbnc_b200" in line for line in f)
+    return d.num_segments * ticks / el, d.num_segments, mapped
+
+
+def workload_config(neurons):
+    """The workload as both arms name it (the large plain network at `neurons`)."""
+    return {"workload": WORKLOAD if neurons == 100000 else WORKLOAD.replace("100000 neurons", "%d neurons" % neurons),
+            "segments_per_gpu": neurons * 64, "synapses_per_gpu": neurons * 100, "dt_ms": DT}
 
 
 def run_reference_arm(a):
+    """The reference's own CPU tick (oracle/_ref, compiled from the reference's sources)
+    on the workload, one process per host core: the tick is single-threaded and not
+    re-entrant (function-local statics, diffusion_kernel.h:50,124-128).  Each process
+    runs a bounded sample of the workload (128 neurons x 64 segments of the same
+    generator, its own seed) read from a .bion by the reference's loader; the samples
+    are written beforehand by a separate process, so no process of this arm maps this
+    backend's library."""
     rank, _, world = dist_env()
     if rank != 0:
         return 0
     import multiprocessing as mp
+    import shutil
     ncores = os.cpu_count() or 1
     neurons = 128   # 8192 segments, 12,800 synapses per process and step
-    ctx = mp.get_context("spawn")
-    t0 = time.perf_counter()
-    with ctx.Pool(ncores) as pool:
-        res = pool.map(_ref_worker, [(neurons, a.steps, a.warmup, a.seed + i) for i in range(ncores)])
-    wall = time.perf_counter() - t0
+    tmp = tempfile.mkdtemp(prefix="bnc_ref_samples_")
+    try:
+        seeds = [a.seed + i for i in range(ncores)]
+        subprocess.run([sys.executable, os.path.abspath(__file__), "--write-reference-samples", tmp, str(neurons)]
+                       + [str(x) for x in seeds], check=True)
+        paths = [os.path.join(tmp, "sample_%d.bion" % sd) for sd in seeds]
+        t0 = time.perf_counter()
+        with mp.get_context("spawn").Pool(ncores) as pool:
+            res = pool.map(_ref_bion_worker, [(p, a.steps, a.warmup) for p in paths])
+        wall = time.perf_counter() - t0
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
     value = sum(r[0] for r in res)
-    kind = res[0][1]
-    seg = res[0][2]
+    seg = res[0][1]
+    sample = ("%d processes, each the reference's tick on its own %d-neuron x 64-segment sample of the generator "
+              "(%d segments, %d synapses x 8 receptors) read by its bion_load_host; %d ticks after %d warm-up"
+              % (ncores, neurons, seg, neurons * 100, a.steps, a.warmup))
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": 1000.0 * seg * ncores / value if value else None,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "sample_per_process": "%d neurons x 64 segments" % neurons,
-                   "processes": ncores, "parallelism": "independent processes (the reference tick is single-threaded "
-                                                         "and not re-entrant)"},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": ncores, "kind": kind,
-                         "sample": "%d processes x (%d neurons x 64 segments, %d ticks after %d warm-up)"
-                                   % (ncores, neurons, a.steps, a.warmup)},
+        "config": workload_config(a.neurons),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": ncores, "kind": "reference", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "this_backend_mapped_in_reference_processes": any(r[2] for r in res),
         "wall_s": wall,
     }
     print(json.dumps(line), flush=True)
@@ -577,6 +661,9 @@ def run_sweep(a, device):
 
 
 def main():
+    if len(sys.argv) > 1 and sys.argv[1] == "--write-reference-samples":
+        write_reference_samples(sys.argv[2], int(sys.argv[3]), [int(x) for x in sys.argv[4:]])
+        return 0
     a = parse_args()
     if a.impl == "reference":
         return run_reference_arm(a)
@@ -684,10 +771,11 @@ def main():
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": ms_max / a.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 state, f64 GHK/accumulators", "data": "synthetic (seeded generator)",
-            "config": {"workload": WORKLOAD, "segments_per_gpu": info.n_segments,
-                       "synapses_per_gpu": info.n_synapses, "parallelism": "replicas" if world > 1 else "single",
-                       "l2": "inputs larger than L2 (device state ~8 GB per GPU)",
-                       "tiles": info.n_tiles, "phases": info.n_phases, "setup_s": round(setup_s, 1)},
+            "config": workload_config(a.neurons),
+            "build": {"parallelism": "replicas" if world > 1 else "single",
+                      "l2": "inputs larger than L2 (device state ~8 GB per GPU)", "tiles": info.n_tiles,
+                      "phases": info.n_phases, "diffusion_barrier_group": info.group_tiles_64 and 64 or
+                      (info.group_tiles_32 and 32 or 0), "setup_s": round(setup_s, 1)},
             "e2e": e2e, "e2e_dropin": dropin, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,
             "gpu_launches": (info.modifier_launches + 2) * a.steps, "ensemble": ensemble, "trees": trees,
             "adjoint": adjoint, "sweep": sweep,
