@@ -617,31 +617,64 @@ static int run_ticks(Backend* b, uint32_t n, float dt) {
     return BNC_OK;
 }
 
-// Ticks per captured graph: each replay covers this many ticks (two kernels and a
-// clock advance per tick); the remainder of a call runs as plain launches.
-constexpr uint32_t kGraphTicks = 32;
+// The captured tick loop: one graph whose conditional WHILE node runs its body -- one
+// tick, the device clock advance, and a countdown -- until the countdown reaches zero,
+// so one graph launch runs all ticks of a call.  The countdown is set before each
+// launch; it is capped at kLoopMax iterations, and any count outside 1..kLoopMax ends
+// the loop, so the loop always ends.
+constexpr uint32_t kGraphTicks = 32;           // minimum trial length of the tuner
+constexpr unsigned long long kLoopMax = 1ull << 24;
+
+namespace {
+__global__ void k_loop_countdown(cudaGraphConditionalHandle h, unsigned long long* count) {
+    const unsigned long long c = *count;
+    if (c <= 1 || c > kLoopMax) {
+        *count = 0;
+        cudaGraphSetConditional(h, 0);
+    } else {
+        *count = c - 1;
+    }
+}
+__global__ void k_loop_set(unsigned long long* count, unsigned long long n) { *count = n; }
+}  // namespace
 
 static int capture_graph(Backend* b, float dt) {
     b->drop_graph();
     if (!b->clock) {
-        b->clock = static_cast<unsigned long long*>(b->allocs.alloc(2 * sizeof(unsigned long long)));
+        // clock[0] tick counter, clock[1] ticks run, clock[2] the loop's countdown
+        b->clock = static_cast<unsigned long long*>(b->allocs.alloc(3 * sizeof(unsigned long long)));
         if (!b->clock) { set_error("device allocation of the tick clock failed"); return BNC_ERR_ALLOC; }
     }
     cudaError_t e = prepare_tick(b->dev, b->host, b->stream);
     if (e != cudaSuccess) return cuda_fail(e, "tick set-up");
     NetDev d = b->dev;
     d.clock = b->clock;
-    e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamBeginCapture");
-    cudaError_t le = cudaSuccess;
-    for (uint32_t t = 0; t < kGraphTicks && le == cudaSuccess; t++) {
-        le = enqueue_tick(d, b->host, dt, 0, 0, b->stream);
-        if (le == cudaSuccess) le = launch_advance_clock(b->clock, b->stream);
-    }
     cudaGraph_t g = nullptr;
-    e = cudaStreamEndCapture(b->stream, &g);
+    e = cudaGraphCreate(&g, 0);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGraphCreate");
+    cudaGraphConditionalHandle h;
+    e = cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault);
+    cudaGraphNode_t node = nullptr;
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    if (e == cudaSuccess) e = cudaGraphAddNode(&node, g, nullptr, 0, &cp);
+    if (e != cudaSuccess) { cudaGraphDestroy(g); return cuda_fail(e, "conditional graph node"); }
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    e = cudaStreamBeginCaptureToGraph(b->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) { cudaGraphDestroy(g); return cuda_fail(e, "capture of the loop body"); }
+    cudaError_t le = enqueue_tick(d, b->host, dt, 0, 0, b->stream);
+    if (le == cudaSuccess) le = launch_advance_clock(b->clock, b->stream);
+    if (le == cudaSuccess) {
+        k_loop_countdown<<<1, 1, 0, b->stream>>>(h, b->clock + 2);
+        le = cudaGetLastError();
+    }
+    cudaGraph_t cap = nullptr;
+    e = cudaStreamEndCapture(b->stream, &cap);
     if (le != cudaSuccess || e != cudaSuccess) {
-        if (g) cudaGraphDestroy(g);
+        cudaGraphDestroy(g);
         return cuda_fail(le != cudaSuccess ? le : e, "tick loop capture");
     }
     e = cudaGraphInstantiate(&b->graph_exec, g, 0);
@@ -660,20 +693,26 @@ static int run_ticks_graph(Backend* b, uint32_t n, float dt) {
         if (rc != BNC_OK) return rc;
         n--;
     }
-    cudaSetDevice(b->device);
-    const uint32_t reps = n / kGraphTicks;
-    if (reps > 0) {
-        if (!b->graph_exec || b->graph_dt != dt) {
-            int rc = capture_graph(b, dt);
-            if (rc != BNC_OK) return rc;
-        }
-        cudaError_t e = launch_set_clock(b->clock, b->tick, b->ticks_run, b->stream);
-        for (uint32_t r = 0; r < reps && e == cudaSuccess; r++) e = cudaGraphLaunch(b->graph_exec, b->stream);
-        if (e != cudaSuccess) { b->failed = true; return cuda_fail(e, "graph launch"); }
-        b->tick += (uint64_t)reps * kGraphTicks;
-        b->ticks_run += (uint64_t)reps * kGraphTicks;
+    if (n == 0) return BNC_OK;
+    if ((unsigned long long)n > kLoopMax) {
+        int rc = run_ticks_graph(b, (uint32_t)kLoopMax, dt);
+        return rc != BNC_OK ? rc : run_ticks_graph(b, n - (uint32_t)kLoopMax, dt);
     }
-    return run_ticks(b, n - reps * kGraphTicks, dt);
+    cudaSetDevice(b->device);
+    if (!b->graph_exec || b->graph_dt != dt) {
+        int rc = capture_graph(b, dt);
+        if (rc != BNC_OK) return rc;
+    }
+    cudaError_t e = launch_set_clock(b->clock, b->tick, b->ticks_run, b->stream);
+    if (e == cudaSuccess) {
+        k_loop_set<<<1, 1, 0, b->stream>>>(b->clock + 2, (unsigned long long)n);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaGraphLaunch(b->graph_exec, b->stream);
+    if (e != cudaSuccess) { b->failed = true; return cuda_fail(e, "graph launch"); }
+    b->tick += n;
+    b->ticks_run += n;
+    return BNC_OK;
 }
 
 static int sync_stream(Backend* b) {

@@ -285,10 +285,12 @@ int bnc_load_ensemble_tuned(void* sim, const BncNetgenParams* members, uint32_t 
 /* bnc_run_ticks_graph bracketed by CUDA events; *ms receives the device time. */
 int bnc_time_ticks_graph(void* sim, uint32_t n_ticks, float dt, float* ms);
 
-/* Runs n ticks with the tick loop captured once in a CUDA graph (32 ticks per
- * replay; the tick counter lives on the device) -- same results as bnc_run_ticks,
- * fewer launch round trips for small networks and ensembles.  The graph is
- * re-captured when dt changes or a network is loaded. */
+/* Runs n ticks as one launch of a CUDA graph captured once: a conditional while node
+ * around one tick, the device-side clock advance and a countdown set before each
+ * launch (the tick counter lives on the device) -- same results as bnc_run_ticks,
+ * one launch per call whatever n.  The tick that applies pending injections runs
+ * before the graph as a plain launch.  The graph is re-captured when dt changes, a
+ * network is loaded or stimuli are uploaded. */
 int bnc_run_ticks_graph(void* sim, uint32_t n_ticks, float dt);
 
 /* Build options of a network's device layout.  None of them changes results:

@@ -102,3 +102,33 @@ def test_autotuned_grouping_gives_identical_results():
         n = plain.info().n_synapses
         for f, i in SYN:
             _same(tuned.synapse_field(f, i, n), plain.synapse_field(f, i, n), "synapse %s[%d]" % (f, i))
+
+
+def test_ensemble_members_equal_the_oracle_with_releases():
+    """Each member of a seeded uneven ensemble (own conductance scales and seed), with
+    3 nA somatic steps so that members release, run through the captured tick loop,
+    equals the CPU oracle's run of that member alone, bit for bit, after 600 ticks."""
+    from bioneuroncore_b200 import Backend, Network, ensemble_params
+    from oracle.oracle import Oracle
+    ps = ensemble_params(23, 6, 64, 900)
+    for p in ps:
+        p.stim_pA = 3000.0
+    ens = Backend()
+    ens.load_ensemble(ps)
+    ticks = 600
+    ens.run_ticks_graph(ticks, DT)
+    n_total = ens.info().n_synapses
+    released = 0
+    for m, p in enumerate(ps):
+        ora = Oracle(Network(p))
+        log = ora.run_logged(ticks, DT)
+        released += len(log[0])
+        r = ens.ensemble_member(m)
+        for f, i in SEG + [("ion_out", 0), ("ion_in", 3)]:
+            whole = ens.segment_field(f, i)
+            _same(whole[r.seg_begin:r.seg_begin + r.n_segments], ora.segment_field(f, i), "member %d %s[%d]" % (m, f, i))
+        for f, i in SYN + [("RRP", 0), ("receptor_state", 1)]:
+            whole = ens.synapse_field(f, i, n_total)
+            _same(whole[r.syn_begin:r.syn_begin + r.n_synapses], ora.synapse_field(f, i),
+                  "member %d synapse %s[%d]" % (m, f, i))
+    assert released > 0, "the members must release transmitter"
