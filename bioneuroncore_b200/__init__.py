@@ -36,6 +36,8 @@ DROPIN_SYMBOLS = ["gpu_backend_create", "gpu_backend_create_on_device", "gpu_bac
                   "gpu_backend_ibuf_offset", "gpu_backend_vm_offset", "gpu_backend_seg_size"]
 NEW_SYMBOLS = ["bnc_netgen_aos", "bnc_netgen_free", "bnc_last_error", "bnc_load_aos", "bnc_load_generated",
                "bnc_run_ticks", "bnc_time_ticks", "bnc_sync_to_host", "bnc_records_managed", "bnc_set_records_residency",
+               "register_modifier_current", "register_modulator_release", "bnc_plugin_load",
+               "bnc_plugin_load_directory", "bnc_plugin_registered", "bnc_plugin_count", "bnc_plugin_unregister_all",
                "bnc_read_segment_field",
                "bnc_read_synapse_field", "bnc_set_synapse_scale", "bnc_network_info", "bnc_save_bion",
                "bnc_plan_generated", "bnc_step_io", "bnc_profile_ticks", "bnc_run_ticks_static_scratch",

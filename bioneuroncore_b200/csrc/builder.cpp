@@ -378,12 +378,21 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
     // segment ids must be the positions (stimuli and the reference match on id)
     for (uint32_t i = 0; i < n; i++) {
         if (S[i].modifier_count > BNC_MAX_MODIFIERS) { set_error("segment %u: modifier_count %u > 32", i, S[i].modifier_count); return BNC_ERR_FORMAT; }
-        for (uint8_t j = 0; j < S[i].modifier_count; j++)
-            if (!type_supported(hn.mod(i, j).type) && !user_type[hn.mod(i, j).type]) {
-                set_error("segment %u slot %u: modifier type %u has no device implementation in this backend",
-                          i, j, hn.mod(i, j).type);
+        for (uint8_t j = 0; j < S[i].modifier_count; j++) {
+            const uint8_t t = hn.mod(i, j).type;
+            if (!user_type[t] && host_plugin_registered(t)) {
+                // the reference would run the plugin's CPU function for this ID
+                // (kernel_dispatch.h:336-343); there is no CPU path here
+                set_error("segment %u slot %u: modifier type %u is registered by a host plugin (a CPU function); "
+                          "register device code for it (biocore_gpu_register_device_modifier)", i, j, t);
                 return BNC_ERR_UNSUPPORTED;
             }
+            if (!type_supported(t) && !user_type[t]) {
+                set_error("segment %u slot %u: modifier type %u has no device implementation in this backend",
+                          i, j, t);
+                return BNC_ERR_UNSUPPORTED;
+            }
+        }
     }
     // ---- valid connections and components ----
     std::vector<uint32_t> conn_ok;
@@ -1059,14 +1068,24 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
             return BNC_ERR_FORMAT;
         }
         for (uint8_t j = 0; j < y.post_receptor_count; j++)
-            if (!receptor_supported(hn.post_rec(k, j).type)) {
+            if (host_plugin_registered(hn.post_rec(k, j).type)) {
+                if (report)
+                    set_error("synapse %u receptor %u: type %u is registered by a host plugin (a CPU function), "
+                              "which this backend cannot run", k, j, hn.post_rec(k, j).type);
+                return BNC_ERR_UNSUPPORTED;
+            } else if (!receptor_supported(hn.post_rec(k, j).type)) {
                 if (report)
                     set_error("synapse %u receptor %u: type %u has no device implementation as a receptor", k, j,
                               hn.post_rec(k, j).type);
                 return BNC_ERR_UNSUPPORTED;
             }
         for (uint8_t j = 0; j < y.pre_autoreceptor_count; j++)
-            if (bouton_gamma(hn.pre_ar(k, j).type) == 0.0f) {
+            if (host_plugin_registered(hn.pre_ar(k, j).type)) {
+                if (report)
+                    set_error("synapse %u autoreceptor %u: type %u is registered by a host plugin (a CPU function), "
+                              "which this backend cannot run", k, j, hn.pre_ar(k, j).type);
+                return BNC_ERR_UNSUPPORTED;
+            } else if (bouton_gamma(hn.pre_ar(k, j).type) == 0.0f) {
                 if (report)
                     set_error("synapse %u autoreceptor %u: type %u (release modulators are not supported)", k, j,
                               hn.pre_ar(k, j).type);

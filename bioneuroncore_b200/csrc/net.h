@@ -301,6 +301,8 @@ cudaError_t launch_set_clock(unsigned long long* clock, unsigned long long tick,
 cudaError_t launch_advance_clock(unsigned long long* clock, cudaStream_t stream);
 // plugins.cu: registered device modifiers (user modifier IDs 0-127)
 bool device_modifier_registered(uint8_t type);
+// A host plugin registered a CPU function for the ID (plugin_host.cpp).
+bool host_plugin_registered(uint8_t type);
 int device_modifier_kernel(uint8_t type, const void** kernel);   // loads on first use (needs a device)
 cudaError_t launch_device_modifier(const void* kernel, const NetDev& d, uint8_t type, uint32_t b, uint32_t e, float dt,
                                    cudaStream_t stream);

@@ -346,6 +346,36 @@ int bnc_register_device_modifier(uint8_t type_id, const char* source, const char
 /* 1 when a device modifier is registered for the ID, else 0. */
 int bnc_device_modifier_registered(uint8_t type_id);
 
+/* ---- Reference modifier plugins (plugin_host.cpp) ----
+ * The registration functions a reference plugin's biocore_plugin_init calls, with the
+ * reference's names and linkage (modifier_interface.h:38-39 and, C++ linkage,
+ * plugin_manager.h:98-99: register_user_modifier / register_user_modulator): they
+ * record the CPU function per ID 0-127 (types >= 128 ignored, as the reference does).
+ * ModifierFunc / ReleaseModulatorFunc are the reference's function types; this
+ * backend never calls them.  A network using an ID that a host plugin registered is
+ * refused with BNC_ERR_UNSUPPORTED unless device code is registered for the ID
+ * (biocore_gpu_register_device_modifier): no CPU fallback. */
+#ifndef BNC_PLUGIN_HOST_IMPL   /* plugin_host.cpp defines them with the reference's types */
+typedef void (*BncPluginFunc)(void);   /* stands for ModifierFunc / ReleaseModulatorFunc */
+void register_modifier_current(uint8_t type, BncPluginFunc func);
+void register_modulator_release(uint8_t type, BncPluginFunc func);
+#endif
+/* plugin_load (plugin_manager.cpp:208-258): dlopen(RTLD_LAZY | RTLD_GLOBAL), this
+ * library first made visible to the plugin; biocore_plugin_desc parsed when present;
+ * biocore_plugin_init called.  Returns what init returned (> 0), or -1 (dlopen
+ * failed), -2 (no biocore_plugin_init), -3 (init returned <= 0); the message is in
+ * bnc_last_error().  The handle stays open for the process. */
+int bnc_plugin_load(const char* so_path);
+/* Every regular *.so file of a directory (plugin_load_directory,
+ * plugin_manager.cpp:260-300); returns the sum of the positive registration counts. */
+int bnc_plugin_load_directory(const char* dir_path);
+/* bit 0: a current function is registered for the ID, bit 1: a release modulator. */
+int bnc_plugin_registered(uint8_t type_id);
+/* Plugins loaded so far. */
+int bnc_plugin_count(void);
+/* Forgets every registration (the libraries stay loaded). */
+void bnc_plugin_unregister_all(void);
+
 /* Host-only: runs the builder's planning on AoS arrays in memory (validation,
  * supported-type checks, tiles, schedule) without a device.  Returns the same
  * codes a load of that network would. */

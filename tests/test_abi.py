@@ -39,7 +39,7 @@ DROPIN = ["gpu_backend_create", "gpu_backend_create_on_device", "gpu_backend_des
 def declared_functions():
     text = open(os.path.join(INCLUDE, "bnc_b200.h")).read()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
-    names = re.findall(r"^\s*(?:const\s+)?[A-Za-z_][A-Za-z0-9_]*\s*\**\s*\b((?:gpu_backend|bnc|biocore_gpu)_[a-z0-9_]+)\s*\(",
+    names = re.findall(r"^\s*(?:const\s+)?[A-Za-z_][A-Za-z0-9_]*\s*\**\s*\b((?:gpu_backend|bnc|biocore_gpu|register)_[a-z0-9_]+)\s*\(",
                        text, flags=re.M)
     return sorted(set(names))
 
