@@ -356,7 +356,7 @@ def run_reference_arm(a):
     return 0
 
 
-def run_ensemble(a, device):
+def run_ensemble(a, device, dist=None):
     """Batched ensemble: a.ens_members independent networks of uneven size (segments
     log-uniform in [200, 20000], gNa/gK/gleak/gCa x U[0.5, 2], one seed each) in one
     device structure -- grouping autotuned on a sample, tick loop captured in a CUDA
@@ -365,14 +365,21 @@ def run_ensemble(a, device):
     captured loop; the sequential leg runs a.ens_seq_ticks ticks per network.  Both are
     device-timed with CUDA events after warm-up and compared per tick."""
     from bioneuroncore_b200 import Backend, ensemble_params
-    ps = ensemble_params(a.seed, a.ens_members, 200, 20000)
+    from bioneuroncore_b200.shard import deal_members, member_segments
+    ps_all = list(ensemble_params(a.seed, a.ens_members, 200, 20000))
+    world = dist.get_world_size() if dist is not None else 1
+    rank = dist.get_rank() if dist is not None else 0
+    sizes = member_segments(ps_all)
+    deal = deal_members(sizes, world)   # whole members per rank, greedy size balance
+    ps = [ps_all[m] for m in deal[rank]]
+    total_segments = sum(sizes)
     ens = Backend(device)
     t0 = time.perf_counter()
     tune = ens.load_ensemble_tuned(ps, 32, DT)
     setup_s = time.perf_counter() - t0
     info = ens.info()
     ens.run_ticks_graph(max(a.warmup, 3), DT)
-    ms_ens = ens.time_ticks_graph(a.ens_ticks, DT)
+    ms_ens = max_over_ranks(ens.time_ticks_graph(a.ens_ticks, DT), dist, "cuda")
     ens.close()
     ms_seq = 0.0
     seq_segments = 0
@@ -384,8 +391,9 @@ def run_ensemble(a, device):
         seq_segments += b.info().n_segments
         b.close()
     assert seq_segments == info.n_segments
+    ms_seq = max_over_ranks(ms_seq, dist, "cuda")
     cpu = None
-    if not a.no_cpu_baseline:
+    if not a.no_cpu_baseline and world == 1:
         try:   # a seeded sample of the members, then all 8 host cores on it
             sample = ps[:: max(1, len(ps) // 32)][:32]
             rate1, secs, nseg_s, kind = cpu_reference_params(sample, 2, 1)
@@ -397,11 +405,13 @@ def run_ensemble(a, device):
                    "sequential_512_ms_per_tick_extrapolated": 1000.0 * info.n_segments / rate1}
         except Exception as exc:
             cpu = {"unavailable": str(exc)[:200]}
-    rate_ens = info.n_segments * a.ens_ticks / (ms_ens / 1000.0)
-    rate_seq = info.n_segments * a.ens_seq_ticks / (ms_seq / 1000.0)
+    rate_ens = total_segments * a.ens_ticks / (ms_ens / 1000.0)
+    rate_seq = total_segments * a.ens_seq_ticks / (ms_seq / 1000.0)
     return {
         "workload": "%d networks, 200-20000 segments each (log-uniform), %d segments in total, conductances "
-                    "x U[0.5, 2], own seeds" % (a.ens_members, info.n_segments),
+                    "x U[0.5, 2], own seeds" % (a.ens_members, total_segments),
+        "ranks": world, "members_per_rank": [len(x) for x in deal],
+        "segments_per_rank": [sum(sizes[m] for m in x) for x in deal],
         "metric": "segment-ticks/s", "ticks": a.ens_ticks, "value": rate_ens, "ms_per_tick": ms_ens / a.ens_ticks,
         "sequential_value": rate_seq, "sequential_ms_per_tick": ms_seq / a.ens_seq_ticks,
         "sequential_ticks": a.ens_seq_ticks,
@@ -744,7 +754,7 @@ def main():
     ensemble = None
     if not a.no_ensemble:
         b.close()   # free the large network's device memory first
-        ensemble = run_ensemble(a, local_rank if world > 1 else 0)
+        ensemble = run_ensemble(a, local_rank if world > 1 else 0, dist)
 
     trees = None
     if not a.no_trees:
