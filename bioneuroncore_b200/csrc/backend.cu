@@ -73,6 +73,7 @@ struct Backend {
         if (owns_aos) {
             delete[] aos.neurons;
             delete[] aos.connections;
+            delete[] static_cast<uint8_t*>(aos.nuclei);
             if (aos_managed) {
                 cudaFree(aos.segments);
                 cudaFree(aos.synapses);
@@ -363,6 +364,14 @@ static int gather_generated(const BncNetgenParams* params, uint32_t n, HostNet* 
 
 }  // namespace
 
+// Nucleus records (types.h:508-524, 500 bytes with 57 genes): protein_level at 244; the
+// 46-gene records of older v7-v14 files (412 bytes) hold it at 200
+// (bion_format.h:492-535).  Gene indices of the protein -> parameter mapping
+// (types.h:357-361).
+constexpr size_t kNucleusBytes = 500, kNucleus46Bytes = 412;
+constexpr size_t kProteinOff = 244, kProtein46Off = 200, kGeneActOff = 16, kTail46Off = 384, kTailOff = 472;
+constexpr int kGeneSYT1 = 40, kGeneUNC13A = 42, kGeneCPLX1 = 44;
+
 static int sync_stream(Backend* b);
 
 // ---- Drop-in records in managed memory ----
@@ -555,8 +564,37 @@ static int export_records(Backend* b) {
     return sync_stream(b);
 }
 
+// The reference's GPU backend maps the nucleus protein levels of each synapse's
+// presynaptic neuron onto its release parameters before every synaptic step
+// (gpu_backend_cuda.cu:275-289, rrp_apply_protein_mapping, kernel_dispatch.h:651-663):
+// synapses with id 0 are skipped, the nucleus is the one at the position of the
+// presynaptic segment's neuron_id.  Nothing on that path changes protein levels, so the
+// mapping gives the same values every tick: it is applied once, to the records, when a
+// network with nuclei is loaded.
+static void apply_protein_mapping(BncBionData& d) {
+    if (!d.nuclei || d.num_nuclei == 0) return;
+    const uint8_t* nu = static_cast<const uint8_t*>(d.nuclei);
+    for (uint32_t i = 0; i < d.num_synapses; i++) {
+        BncSynapse& y = d.synapses[i];
+        if (y.id == 0) continue;
+        if (y.pre_segment >= d.num_segments) continue;
+        const uint32_t nid = d.segments[y.pre_segment].neuron_id;
+        if (nid >= d.num_nuclei) continue;
+        const float* pl = reinterpret_cast<const float*>(nu + (size_t)nid * kNucleusBytes + kProteinOff);
+        const float munc13 = pl[kGeneUNC13A];
+        y.RRP_max = 10.0f + munc13 * 40.0f;
+        const float syt1 = pl[kGeneSYT1];
+        y.release_probability = 0.3f + syt1 * 0.7f;
+        const float cplx1 = pl[kGeneCPLX1];
+        y.RRP_recovery = 0.02f + munc13 * 0.08f - cplx1 * 0.01f;
+        if (y.RRP_recovery < 0.005f) y.RRP_recovery = 0.005f;
+        if (y.RRP_recovery > 0.2f) y.RRP_recovery = 0.2f;
+    }
+}
+
 static int load_common(Backend* b, BncBionData& aos, bool keep_aos) {
     cudaSetDevice(b->device);
+    apply_protein_mapping(aos);
     HostNet hn;
     hostnet_from_aos(aos, &hn);
     int rc = build_network(hn, b->stim, &b->dev, &b->host, &b->allocs);
@@ -569,6 +607,7 @@ static int load_common(Backend* b, BncBionData& aos, bool keep_aos) {
 
 static void free_aos_arrays(BncBionData& a) {
     delete[] a.neurons; delete[] a.segments; delete[] a.connections; delete[] a.synapses;
+    delete[] static_cast<uint8_t*>(a.nuclei);
     std::memset(&a, 0, sizeof(a));
 }
 
@@ -586,6 +625,15 @@ static int copy_aos(const BncBionData* src, BncBionData* dst) {
     if (src->num_segments) std::memcpy(dst->segments, src->segments, sizeof(BncSegment) * src->num_segments);
     if (src->num_connections) std::memcpy(dst->connections, src->connections, sizeof(BncIntraConnection) * src->num_connections);
     if (src->num_synapses) std::memcpy(dst->synapses, src->synapses, sizeof(BncSynapse) * src->num_synapses);
+    dst->nuclei = nullptr;
+    dst->num_nuclei = 0;
+    if (src->num_nuclei && src->nuclei) {
+        uint8_t* nu = new (std::nothrow) uint8_t[(size_t)src->num_nuclei * kNucleusBytes];
+        if (!nu) { free_aos_arrays(*dst); return BNC_ERR_ALLOC; }
+        std::memcpy(nu, src->nuclei, (size_t)src->num_nuclei * kNucleusBytes);
+        dst->nuclei = nu;
+        dst->num_nuclei = src->num_nuclei;
+    }
     return BNC_OK;
 }
 
@@ -730,7 +778,7 @@ static int save_bion(const BncBionData& d, const char* path) {
     hdr.num_neurons = d.num_neurons; hdr.num_segments = d.num_segments;
     hdr.num_intra_connections = d.num_connections; hdr.num_synapses = d.num_synapses;
     hdr.grid_dim_x = hdr.grid_dim_y = hdr.grid_dim_z = 0; hdr.voxel_size = 1.0f;
-    hdr.num_nuclei = 0; hdr.nucleus_version = 1;
+    hdr.num_nuclei = d.nuclei ? d.num_nuclei : 0; hdr.nucleus_version = 1;
     hdr.file_sz_segment = sizeof(BncSegment); hdr.file_sz_synapse = sizeof(BncSynapse);
     hdr.file_sz_nucleus = 500; hdr.file_sz_intraconnection = sizeof(BncIntraConnection);
     hdr.file_sz_neuron = sizeof(BncNeuron); hdr.file_sz_modifier = sizeof(BncModifier);
@@ -739,6 +787,7 @@ static int save_bion(const BncBionData& d, const char* path) {
     if (ok) ok = fwrite(d.segments, sizeof(BncSegment), d.num_segments, f) == d.num_segments;
     if (ok && d.num_connections) ok = fwrite(d.connections, sizeof(BncIntraConnection), d.num_connections, f) == d.num_connections;
     if (ok && d.num_synapses) ok = fwrite(d.synapses, sizeof(BncSynapse), d.num_synapses, f) == d.num_synapses;
+    if (ok && hdr.num_nuclei) ok = fwrite(d.nuclei, kNucleusBytes, hdr.num_nuclei, f) == hdr.num_nuclei;
     fclose(f);
     if (!ok) { set_error("write to %s failed", path); return BNC_BION_ERR_WRITE_FAIL; }
     return BNC_OK;
@@ -771,6 +820,28 @@ static int load_bion_file(const char* path, BncBionData* d) {
     if (fread(d->segments, sizeof(BncSegment), d->num_segments, f) != d->num_segments) return fail(BNC_BION_ERR_FILE_READ, "short segments");
     if (d->num_connections && fread(d->connections, sizeof(BncIntraConnection), d->num_connections, f) != d->num_connections) return fail(BNC_BION_ERR_FILE_READ, "short connections");
     if (d->num_synapses && fread(d->synapses, sizeof(BncSynapse), d->num_synapses, f) != d->num_synapses) return fail(BNC_BION_ERR_FILE_READ, "short synapses");
+    if (d->header.num_nuclei > 0) {   // bion_loader_host.cpp:276-339 (v7-v14 records)
+        const size_t fsz = d->header.file_sz_nucleus;
+        if (fsz != kNucleusBytes && fsz != kNucleus46Bytes) return fail(BNC_BION_ERR_BAD_VERSION, "nucleus record size");
+        const uint32_t nn = d->header.num_nuclei;
+        uint8_t* nu = new (std::nothrow) uint8_t[(size_t)nn * kNucleusBytes];
+        if (!nu) return fail(BNC_ERR_ALLOC, "out of memory");
+        d->nuclei = nu;
+        d->num_nuclei = nn;
+        std::memset(nu, 0, (size_t)nn * kNucleusBytes);
+        std::vector<uint8_t> rec(fsz);
+        for (uint32_t i = 0; i < nn; i++) {
+            if (fread(rec.data(), fsz, 1, f) != 1) return fail(BNC_BION_ERR_FILE_READ, "short nuclei");
+            uint8_t* dst = nu + (size_t)i * kNucleusBytes;
+            if (fsz == kNucleusBytes) { std::memcpy(dst, rec.data(), kNucleusBytes); continue; }
+            // 46 genes -> 57: ids and counters, genes 0..45 of both arrays, the six
+            // levels after them; genes 46..56 stay 0 (bion_format.h:515-535)
+            std::memcpy(dst, rec.data(), kGeneActOff);
+            std::memcpy(dst + kGeneActOff, rec.data() + kGeneActOff, 46 * 4);
+            std::memcpy(dst + kProteinOff, rec.data() + kProtein46Off, 46 * 4);
+            std::memcpy(dst + kTailOff, rec.data() + kTail46Off, 6 * 4);
+        }
+    }
     fclose(f);
     // validation (bion_loader_host.cpp:359-408)
     for (uint32_t i = 0; i < d->num_connections; i++)

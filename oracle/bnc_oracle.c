@@ -856,6 +856,20 @@ static void load_mod(OMod* o, const BncModifier* m) {
     for (int k = 0; k < 8; k++) o->st[k] = BO_ST(m->state[k]);
 }
 
+/* rrp_apply_protein_mapping (kernel_dispatch.h:651-663): protein levels of genes
+   UNC13A (42), SYT1 (40) and CPLX1 (44) (types.h:357-361) set RRP_max, the release
+   probability and RRP recovery. */
+void bo_protein_mapping(const float* protein_level, float* rrp_max, float* p_rel, float* rrp_rec) {
+    float munc13 = protein_level[42];
+    *rrp_max = 10.0f + munc13 * 40.0f;
+    float syt1 = protein_level[40];
+    *p_rel = 0.3f + syt1 * 0.7f;
+    float cplx1 = protein_level[44];
+    *rrp_rec = 0.02f + munc13 * 0.08f - cplx1 * 0.01f;
+    if (*rrp_rec < 0.005f) *rrp_rec = 0.005f;
+    if (*rrp_rec > 0.2f) *rrp_rec = 0.2f;
+}
+
 BoSim* bo_create(const BncBionData* d, const BncCurrentStimulus* stim, uint32_t n_stim,
                  char* err, int errlen) {
     BoSim* S = calloc(1, sizeof(BoSim));
@@ -924,6 +938,16 @@ BoSim* bo_create(const BncBionData* d, const BncCurrentStimulus* stim, uint32_t 
         y->bouton_Ca = a->bouton_Ca; y->spine_Ca = a->spine_Ca;
         y->spine_camkii = a->spine_camkii; y->spine_calcineurin = a->spine_calcineurin;
         y->w_scale = 1.0f;
+        /* nucleus protein levels of the presynaptic neuron (gpu_backend_cuda.cu:275-289:
+           synapses with id 0 skipped, nucleus at the position of the pre segment's
+           neuron_id); with fixed protein levels the per-tick mapping is the same every
+           tick, so it is applied here once */
+        if (d->nuclei && d->num_nuclei && a->id != 0 && a->pre_segment < d->num_segments) {
+            uint32_t nid = d->segments[a->pre_segment].neuron_id;
+            if (nid < d->num_nuclei)
+                bo_protein_mapping((const float*)((const uint8_t*)d->nuclei + (size_t)nid * 500 + 244),
+                                   &y->RRP_max, &y->p_rel, &y->RRP_rec);
+        }
     }
     scratch_reserve(S->n, S->m);
     return S;

@@ -24,3 +24,14 @@ extern "C" uint32_t ref_release_seed(uint32_t syn_id, uint64_t tick, double V_m)
 extern "C" int ref_release_decision(uint32_t syn_id, uint64_t tick, double V_m, float p) {
     return xorshift32_rnd(ref_release_seed(syn_id, tick, V_m)) < p ? 1 : 0;
 }
+
+// rrp_apply_protein_mapping (kernel_dispatch.h:651-663) on a synapse whose other fields
+// are zero: returns RRP_max, release_probability and RRP_recovery.
+extern "C" void ref_protein_mapping(const float* protein_level, float* out3) {
+    Synapse syn;
+    memset(&syn, 0, sizeof(syn));
+    rrp_apply_protein_mapping(&syn, protein_level);
+    out3[0] = syn.RRP_max;
+    out3[1] = syn.release_probability;
+    out3[2] = syn.RRP_recovery;
+}

@@ -196,3 +196,50 @@ def test_dropin_sequence_within_tolerance_of_the_reference(tmp_path):
         errs["extra[%d]" % q] = _rel(seg["extra_ions"][:, q], rseg["extra_ions"][:, q], 1e-6)
     bad = {k: v for k, v in errs.items() if not v <= REL_TOL_FP64}
     assert not bad, bad
+
+
+def test_dropin_with_nuclei_applies_the_protein_mapping(tmp_path):
+    """A .bion with nucleus records: the reference's backend maps each synapse's
+    presynaptic nucleus protein levels onto RRP_max, the release probability and RRP
+    recovery (gpu_backend_cuda.cu:275-289).  The records after loading carry the mapped
+    values, and 300 ticks equal the oracle given the same nuclei, bit for bit."""
+    from bioneuroncore_b200 import Backend, Network, NetgenParams, NET_SMALL, NETGEN_SYNAPSE_EXTRAS
+    p = NetgenParams(family=NET_SMALL, n_neurons=16, seed=6, flags=NETGEN_SYNAPSE_EXTRAS, stim_pA=3000.0)
+    rng = np.random.default_rng(5)
+    nu = np.zeros(16 * 500, np.uint8)
+    for i in range(16):
+        nu[i * 500:i * 500 + 4] = np.frombuffer(np.uint32(i).tobytes(), np.uint8)
+        nu[i * 500 + 244:i * 500 + 244 + 228] = np.frombuffer(rng.uniform(0.0, 1.0, 57).astype(np.float32).tobytes(),
+                                                             np.uint8)
+    net = Network(p)
+    net_o = Network(p)
+    for n in (net, net_o):
+        n.data.nuclei = nu.ctypes.data
+        n.data.num_nuclei = 16
+    path = tmp_path / "nuclei.bion"
+    try:
+        _save(net, path)
+        ora = Oracle(net_o)
+    finally:
+        for n in (net, net_o):
+            n.data.nuclei = None
+            n.data.num_nuclei = 0
+    from bioneuroncore_b200.abi import stimulus_data
+    b = Backend()
+    b.load_bion(str(path))
+    cur = [tuple(int(r[f]) if f in ("segment_id", "start_tick") else float(r[f])
+                 for f in ("segment_id", "amplitude_pA", "duration_ms", "start_tick")) for r in net.stimuli]
+    b.upload_stimuli(stimulus_data(current=cur))   # the oracle has the generator's steps
+    n_seg, n_syn = net.data.num_segments, net.data.num_synapses
+    seg, syn = _records(b, n_seg, n_syn)
+    pre_neuron = net.segments["neuron_id"][net.synapses["pre_segment"]]
+    pl = nu.reshape(16, 500)[:, 244:244 + 228].copy().view(np.float32)
+    mapped = net.synapses["id"] != 0
+    want_max = (np.float32(10.0) + pl[pre_neuron, 42] * np.float32(40.0)).astype(np.float32)
+    assert np.array_equal(syn["RRP_max"][mapped], want_max[mapped])
+    assert np.array_equal(syn["RRP_max"][~mapped], net.synapses["RRP_max"][~mapped])
+    for t in range(300):
+        b.run_tick(DT)
+        ora.run(1, DT)
+        seg, syn = _records(b, n_seg, n_syn)
+        _compare(seg, syn, ora, full=(t + 1) % 100 == 0, label="nuclei tick %d" % (t + 1))

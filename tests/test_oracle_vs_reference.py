@@ -222,3 +222,87 @@ def test_release_draw_matches_the_reference():
         assert h.ref_xorshift32_rnd(seed_ref) == o32.bo_xorshift_f(seed_ref)
         assert h.ref_release_decision(sid, tk, float(V32[i]), float(p[i])) == \
             int(o32.bo_xorshift_f(seed_ref) < float(p[i]))
+
+
+def test_protein_mapping_matches_the_reference():
+    """The nucleus protein -> release parameter mapping of the oracle against the
+    reference's own rrp_apply_protein_mapping (kernel_dispatch.h:651-663), through
+    oracle/ref_harness.cpp, on random protein levels that reach both clamps."""
+    h = C.CDLL(REF_LIB.replace("libbiocore_ref.so", "libref_harness.so"))
+    h.ref_protein_mapping.argtypes = [C.c_void_p, C.c_void_p]
+    from oracle.oracle import oracle_lib
+    o = oracle_lib()
+    o.bo_protein_mapping.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    rng = np.random.default_rng(7)
+    for _ in range(2000):
+        pl = rng.uniform(-3.0, 3.0, 57).astype(np.float32)
+        want = np.zeros(3, np.float32)
+        h.ref_protein_mapping(pl.ctypes.data, want.ctypes.data)
+        got = np.zeros(3, np.float32)
+        o.bo_protein_mapping(pl.ctypes.data, got[0:].ctypes.data, got[1:].ctypes.data, got[2:].ctypes.data)
+        assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+
+
+def _nuclei(n, seed):
+    """n 500-byte nucleus records (types.h:508-524) with random protein levels."""
+    rng = np.random.default_rng(seed)
+    buf = np.zeros(n * 500, np.uint8)
+    for i in range(n):
+        buf[i * 500:i * 500 + 4] = np.frombuffer(np.uint32(i).tobytes(), np.uint8)
+        buf[i * 500 + 244:i * 500 + 244 + 57 * 4] = np.frombuffer(rng.uniform(0.0, 1.5, 57).astype(np.float32).tobytes(),
+                                                                 np.uint8)
+    return buf
+
+
+def test_nuclei_are_read_as_the_reference_reads_them(tmp_path):
+    """A .bion with nuclei written by the reference's bion_save (500-byte records), and
+    the same file rewritten with the 46-gene 412-byte records of older files: this
+    library's reader returns the reference loader's nucleus records byte for byte."""
+    from bioneuroncore_b200 import Network, NetgenParams, NET_SMALL, load_library
+    from bioneuroncore_b200.abi import BionData
+    ref = C.CDLL(REF_LIB)
+    load = getattr(ref, "_Z14bion_load_hostPKcP8BionData")
+    save = getattr(ref, "_Z9bion_savePKcPK8BionData")
+    unload = getattr(ref, "_Z16bion_unload_hostP8BionData")
+    for f in (load, save):
+        f.argtypes = [C.c_char_p, C.c_void_p]
+        f.restype = C.c_int
+    unload.argtypes = [C.c_void_p]
+    net = Network(NetgenParams(family=NET_SMALL, n_neurons=4, seed=2))
+    nu = _nuclei(4, 3)
+    net.data.nuclei = nu.ctypes.data
+    net.data.num_nuclei = 4
+    p500 = tmp_path / "n500.bion"
+    try:
+        assert save(str(p500).encode(), C.byref(net.data)) == 0
+    finally:
+        net.data.nuclei = None
+        net.data.num_nuclei = 0
+    raw = bytearray(p500.read_bytes())
+    hdr = 100
+    n_nuc_off = len(raw) - 4 * 500
+    old = bytearray()
+    for i in range(4):
+        r = raw[n_nuc_off + i * 500:n_nuc_off + (i + 1) * 500]
+        rec = bytearray(412)
+        rec[0:16] = r[0:16]
+        rec[16:16 + 184] = r[16:16 + 184]          # genes 0..45 of gene_activity
+        rec[200:200 + 184] = r[244:244 + 184]      # genes 0..45 of protein_level
+        rec[384:408] = r[472:496]                  # the six levels after them
+        old += rec
+    raw412 = raw[:n_nuc_off] + old
+    struct_off = 84   # NetworkHeader.file_sz_nucleus (types.h:577-599)
+    raw412[struct_off:struct_off + 4] = np.uint32(412).tobytes()
+    p412 = tmp_path / "n412.bion"
+    p412.write_bytes(bytes(raw412))
+    lib = load_library()
+    for path in (p500, p412):
+        r, o = BionData(), BionData()
+        assert load(str(path).encode(), C.byref(r)) == 0
+        assert lib.bnc_bion_load(str(path).encode(), C.byref(o)) == 0
+        try:
+            assert r.num_nuclei == o.num_nuclei == 4
+            assert C.string_at(r.nuclei, 4 * 500) == C.string_at(o.nuclei, 4 * 500), path.name
+        finally:
+            unload(C.byref(r))
+            lib.bnc_bion_unload(C.byref(o))
