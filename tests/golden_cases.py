@@ -10,8 +10,52 @@ GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 REL_TOL = 1e-4   # relative, V_m floored at 1 mV and concentrations at 1e-6 mM
 
 
-def cases():
+# State words a release fixture holds in full (the reference's FP64 values), by the
+# field names of Oracle.segment_field / synapse_field.
+SEG_FULL = [("V", 0), ("ATP", 0), ("temperature", 0), ("transcription", 0)] + \
+    [("ion_in", q) for q in range(7)] + [("ion_out", q) for q in range(7)] + \
+    [("intra_nt", q) for q in range(15)] + [("neurotransmitter", q) for q in range(15)]
+SYN_FULL = [(f, 0) for f in ("bouton_Ca", "spine_Ca", "weight", "refractory", "facilitation", "depression",
+                             "spine_camkii", "spine_calcineurin", "RRP")] + [("cleft", q) for q in range(15)]
+
+
+def _all():
     return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "*.npz")))
+
+
+def cases():
+    """Fixtures an FP32-state path must match within REL_TOL.  A fixture whose release
+    draws an FP32 V_m can flip (the seed truncates V_m * 1000 to an integer) is a pin
+    for the FP64 restatement only (release_cases), and is left out here."""
+    out = []
+    for name in _all():
+        with np.load(os.path.join(GOLDEN, name + ".npz")) as g:
+            if "fp32_tolerance" not in g.files or int(g["fp32_tolerance"]):
+                out.append(name)
+    return out
+
+
+def release_cases():
+    """Fixtures that hold the reference's release decisions and its full FP64 state."""
+    out = []
+    for name in _all():
+        with np.load(os.path.join(GOLDEN, name + ".npz")) as g:
+            if "release_syn" in g.files:
+                out.append(name)
+    return out
+
+
+def release_log(g):
+    return list(zip((int(x) for x in g["release_syn"]), (int(x) for x in g["release_tick"])))
+
+
+def decisions(before, after, tick):
+    """(synapse, tick) of every release decided in a tick: a synapse releases only while
+    its refractory counter is 0 (simulation_host.cpp:458), and a release leaves it
+    above 0 (it counts down every tick, :591)."""
+    before = np.asarray(before)
+    after = np.asarray(after)
+    return [(int(i), tick) for i in np.flatnonzero((before == 0) & (after > 0))]
 
 
 def load(name):
@@ -26,9 +70,14 @@ def _rel(a, b, floor):
     return float((np.abs(a - b) / np.maximum(np.abs(b), floor)).max()) if b.size else 0.0
 
 
-def compare(g, trace, seg_field, syn_field):
-    """Returns a dict of max relative errors; raises AssertionError past REL_TOL or on
-    any spike-count difference."""
+def compare(g, trace, seg_field, syn_field, log=None):
+    """Returns a dict of max relative errors; raises AssertionError past REL_TOL, on
+    any spike-count difference, or (given the run's release decisions `log` and a
+    fixture that holds the reference's) on any release decision that differs."""
+    if log is not None and "release_syn" in g.files:
+        want = release_log(g)
+        assert log == want, "release decisions differ from the reference: %d vs %d, first difference %r" % (
+            len(log), len(want), next(((a, b) for a, b in zip(log, want) if a != b), None))
     errs = {"soma_trace": _rel(trace, g["soma_trace"], 1.0), "V": _rel(seg_field("V", 0), g["V"], 1.0),
             "ATP": _rel(seg_field("ATP", 0), g["ATP"], 1e-6)}
     for q in range(7):
@@ -79,16 +128,22 @@ def stimulus_schedule(name, net):
     return [(0, first), (100, second)]
 
 
-def run_scheduled(sim, name, net, ticks, dt, somata, read_v):
+def run_scheduled(sim, name, net, ticks, dt, somata, read_v, read_refractory=None):
     """Runs `ticks` single ticks on `sim` (anything with run(n, dt) or run_ticks(n, dt)
-    and upload_stimuli), uploading the case's schedule; returns the soma V_m trace."""
+    and upload_stimuli), uploading the case's schedule; returns the soma V_m trace, and
+    with read_refractory (the synapses' refractory counters) also the release decisions
+    (synapse, tick) in tick order."""
     sched = dict(stimulus_schedule(name, net))
     step = getattr(sim, "run_ticks", None) or sim.run
     trace = np.empty((ticks, len(somata)), np.float64)
+    log = []
     for t in range(ticks):
         if t in sched:
             sim.upload_stimuli(sched[t])
+        before = np.array(read_refractory(), copy=True) if read_refractory else None
         step(1, dt)
+        if read_refractory:
+            log += decisions(before, read_refractory(), t)
         trace[t] = read_v()[somata]
-    return trace
+    return (trace, log) if read_refractory else trace
 
