@@ -19,6 +19,9 @@ roofline    the dominant kernel's algorithmic bytes per launch over its average
             CUDA-event duration, against the measured copy bandwidth.
 cpu_baseline the reference's own CPU tick (oracle/_ref, built from the reference
             sources) on a bounded sample of the same workload, 1 core.
+draw_order  the same network with each segment's modifiers kept in the order the
+            seeded draw produced them instead of listed by type ID (the default):
+            another slot order, so other physics from the same distribution.
 """
 import argparse
 import json
@@ -61,6 +64,8 @@ def parse_args():
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-sweep", action="store_true")
     ap.add_argument("--no-dropin", action="store_true")
+    ap.add_argument("--no-draw-order", action="store_true")
+    ap.add_argument("--draw-ticks", type=int, default=50)
     ap.add_argument("--dropin-neurons", type=int, default=10000)
     ap.add_argument("--dropin-ticks", type=int, default=10)
     ap.add_argument("--sweep-tasks", type=int, default=256)
@@ -354,6 +359,33 @@ def run_reference_arm(a):
     }
     print(json.dumps(line), flush=True)
     return 0
+
+
+def run_draw_order(a, device):
+    """The headline network with each segment's 16 large-set modifiers kept in the order
+    the seeded categorical draw produced them (BNC_NETGEN_DRAW_ORDER), instead of
+    listed by type ID.  The slot order is the order the tick applies them in, so this
+    is different physics of the same distribution, and the phase groups' warps see less
+    uniform model sequences.  Device-timed with CUDA events over a.draw_ticks ticks."""
+    from bioneuroncore_b200 import Backend, NetgenParams, NET_LARGE, NETGEN_DRAW_ORDER
+    b = Backend(device)
+    try:
+        t0 = time.perf_counter()
+        b.load_generated(NetgenParams(family=NET_LARGE, n_neurons=a.neurons, seed=a.seed, flags=NETGEN_DRAW_ORDER))
+        setup = time.perf_counter() - t0
+        info = b.info()
+        b.run_ticks(a.warmup, DT)
+        n_prof = 5
+        ms_mod, ms_diff, ms_syn = b.profile_ticks(n_prof, DT)
+        ms = b.time_ticks(a.draw_ticks, DT)
+        return {"workload": workload_config(a.neurons)["workload"] + ", modifiers in draw order",
+                "metric": UNIT, "ticks": a.draw_ticks, "value": float(info.n_segments) * a.draw_ticks / (ms / 1000.0),
+                "ms_per_tick": ms / a.draw_ticks, "phases": info.n_phases,
+                "kernels_ms": {"k_modifiers": ms_mod / n_prof, "k_diffusion": ms_diff / n_prof,
+                               "k_synapse": ms_syn / n_prof},
+                "setup_s": round(setup, 1)}
+    finally:
+        b.close()
 
 
 def run_ensemble(a, device, dist=None):
@@ -751,9 +783,14 @@ def main():
                 "tick_bytes": info.algo_bytes_per_tick,
                 "tick_frac": info.algo_bytes_per_tick / (ms_max / a.steps / 1000.0) / 1e9 / peak}
 
+    draw_order = None
+    if not a.no_draw_order and rank == 0 and world == 1:
+        b.close()   # free the large network's device memory first
+        draw_order = run_draw_order(a, 0)
+
     ensemble = None
     if not a.no_ensemble:
-        b.close()   # free the large network's device memory first
+        b.close()
         ensemble = run_ensemble(a, local_rank if world > 1 else 0, dist)
 
     trees = None
@@ -793,7 +830,7 @@ def main():
                       (info.group_tiles_32 and 32 or 0), "setup_s": round(setup_s, 1)},
             "e2e": e2e, "e2e_dropin": dropin, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,
             "gpu_launches": (info.modifier_launches + 2) * a.steps, "ensemble": ensemble, "trees": trees,
-            "adjoint": adjoint, "sweep": sweep,
+            "adjoint": adjoint, "sweep": sweep, "draw_order": draw_order,
         }
         print(json.dumps(line), flush=True)
     b.close()

@@ -16,7 +16,7 @@
 #include "par.h"
 #include "netgen.h"
 #include "hostnet.h"
-#include "hostnet.h"
+#include "bion_file.h"
 
 namespace bnc {
 
@@ -605,11 +605,7 @@ static int load_common(Backend* b, BncBionData& aos, bool keep_aos) {
     return BNC_OK;
 }
 
-static void free_aos_arrays(BncBionData& a) {
-    delete[] a.neurons; delete[] a.segments; delete[] a.connections; delete[] a.synapses;
-    delete[] static_cast<uint8_t*>(a.nuclei);
-    std::memset(&a, 0, sizeof(a));
-}
+static void free_aos_arrays(BncBionData& a) { bion_free(a); }
 
 static int copy_aos(const BncBionData* src, BncBionData* dst) {
     std::memset(dst, 0, sizeof(*dst));
@@ -769,107 +765,10 @@ static int sync_stream(Backend* b) {
     return BNC_OK;
 }
 
-// .bion v14 writer (reference bion_loader_host.cpp:449-504 layout)
-static int save_bion(const BncBionData& d, const char* path) {
-    FILE* f = fopen(path, "wb");
-    if (!f) { set_error("cannot open %s for writing", path); return BNC_BION_ERR_FILE_OPEN; }
-    BncNetworkHeader hdr = d.header;
-    hdr.magic = 0x42494F4Eu; hdr.version = 14; hdr.mode = 0; hdr.diffusion_type = 0;
-    hdr.num_neurons = d.num_neurons; hdr.num_segments = d.num_segments;
-    hdr.num_intra_connections = d.num_connections; hdr.num_synapses = d.num_synapses;
-    hdr.grid_dim_x = hdr.grid_dim_y = hdr.grid_dim_z = 0; hdr.voxel_size = 1.0f;
-    hdr.num_nuclei = d.nuclei ? d.num_nuclei : 0; hdr.nucleus_version = 1;
-    hdr.file_sz_segment = sizeof(BncSegment); hdr.file_sz_synapse = sizeof(BncSynapse);
-    hdr.file_sz_nucleus = 500; hdr.file_sz_intraconnection = sizeof(BncIntraConnection);
-    hdr.file_sz_neuron = sizeof(BncNeuron); hdr.file_sz_modifier = sizeof(BncModifier);
-    bool ok = fwrite(&hdr, sizeof(hdr), 1, f) == 1;
-    if (ok && d.num_neurons) ok = fwrite(d.neurons, sizeof(BncNeuron), d.num_neurons, f) == d.num_neurons;
-    if (ok) ok = fwrite(d.segments, sizeof(BncSegment), d.num_segments, f) == d.num_segments;
-    if (ok && d.num_connections) ok = fwrite(d.connections, sizeof(BncIntraConnection), d.num_connections, f) == d.num_connections;
-    if (ok && d.num_synapses) ok = fwrite(d.synapses, sizeof(BncSynapse), d.num_synapses, f) == d.num_synapses;
-    if (ok && hdr.num_nuclei) ok = fwrite(d.nuclei, kNucleusBytes, hdr.num_nuclei, f) == hdr.num_nuclei;
-    fclose(f);
-    if (!ok) { set_error("write to %s failed", path); return BNC_BION_ERR_WRITE_FAIL; }
-    return BNC_OK;
-}
-
-// .bion reader for v10+ files with the v14 record sizes (bion_loader_host.cpp:26-428
-// is the reference; its v3-v13 migrations are not restated here).
-static int load_bion_file(const char* path, BncBionData* d) {
-    std::memset(d, 0, sizeof(*d));
-    FILE* f = fopen(path, "rb");
-    if (!f) { set_error("cannot open %s", path); return BNC_BION_ERR_FILE_OPEN; }
-    auto fail = [&](int code, const char* msg) { fclose(f); free_aos_arrays(*d); set_error("%s: %s", path, msg); return code; };
-    if (fread(&d->header, 68, 1, f) != 1) return fail(BNC_BION_ERR_FILE_READ, "short header");
-    if (d->header.magic != 0x42494F4Eu) return fail(BNC_BION_ERR_BAD_MAGIC, "bad magic");
-    if (d->header.version < 3 || d->header.version > 14) return fail(BNC_BION_ERR_BAD_VERSION, "unsupported version");
-    if (d->header.version < 10) return fail(BNC_BION_ERR_BAD_VERSION, "pre-v10 layouts need the reference's migration");
-    if (fread(((uint8_t*)&d->header) + 68, 32, 1, f) != 1) return fail(BNC_BION_ERR_FILE_READ, "short header");
-    if (d->header.num_segments == 0) return fail(BNC_BION_ERR_ZERO_SEGS, "zero segments");
-    if (d->header.file_sz_segment != sizeof(BncSegment) || d->header.file_sz_synapse != sizeof(BncSynapse) ||
-        d->header.file_sz_intraconnection != sizeof(BncIntraConnection) || d->header.file_sz_neuron != sizeof(BncNeuron))
-        return fail(BNC_BION_ERR_BAD_VERSION, "record sizes differ from v14");
-    d->num_neurons = d->header.num_neurons; d->num_segments = d->header.num_segments;
-    d->num_connections = d->header.num_intra_connections; d->num_synapses = d->header.num_synapses;
-    d->neurons = new (std::nothrow) BncNeuron[d->num_neurons ? d->num_neurons : 1];
-    d->segments = new (std::nothrow) BncSegment[d->num_segments];
-    d->connections = new (std::nothrow) BncIntraConnection[d->num_connections ? d->num_connections : 1];
-    d->synapses = new (std::nothrow) BncSynapse[d->num_synapses ? d->num_synapses : 1];
-    if (!d->neurons || !d->segments || !d->connections || !d->synapses) return fail(BNC_ERR_ALLOC, "out of memory");
-    if (d->num_neurons && fread(d->neurons, sizeof(BncNeuron), d->num_neurons, f) != d->num_neurons) return fail(BNC_BION_ERR_FILE_READ, "short neurons");
-    if (fread(d->segments, sizeof(BncSegment), d->num_segments, f) != d->num_segments) return fail(BNC_BION_ERR_FILE_READ, "short segments");
-    if (d->num_connections && fread(d->connections, sizeof(BncIntraConnection), d->num_connections, f) != d->num_connections) return fail(BNC_BION_ERR_FILE_READ, "short connections");
-    if (d->num_synapses && fread(d->synapses, sizeof(BncSynapse), d->num_synapses, f) != d->num_synapses) return fail(BNC_BION_ERR_FILE_READ, "short synapses");
-    if (d->header.num_nuclei > 0) {   // bion_loader_host.cpp:276-339 (v7-v14 records)
-        const size_t fsz = d->header.file_sz_nucleus;
-        if (fsz != kNucleusBytes && fsz != kNucleus46Bytes) return fail(BNC_BION_ERR_BAD_VERSION, "nucleus record size");
-        const uint32_t nn = d->header.num_nuclei;
-        uint8_t* nu = new (std::nothrow) uint8_t[(size_t)nn * kNucleusBytes];
-        if (!nu) return fail(BNC_ERR_ALLOC, "out of memory");
-        d->nuclei = nu;
-        d->num_nuclei = nn;
-        std::memset(nu, 0, (size_t)nn * kNucleusBytes);
-        std::vector<uint8_t> rec(fsz);
-        for (uint32_t i = 0; i < nn; i++) {
-            if (fread(rec.data(), fsz, 1, f) != 1) return fail(BNC_BION_ERR_FILE_READ, "short nuclei");
-            uint8_t* dst = nu + (size_t)i * kNucleusBytes;
-            if (fsz == kNucleusBytes) { std::memcpy(dst, rec.data(), kNucleusBytes); continue; }
-            // 46 genes -> 57: ids and counters, genes 0..45 of both arrays, the six
-            // levels after them; genes 46..56 stay 0 (bion_format.h:515-535)
-            std::memcpy(dst, rec.data(), kGeneActOff);
-            std::memcpy(dst + kGeneActOff, rec.data() + kGeneActOff, 46 * 4);
-            std::memcpy(dst + kProteinOff, rec.data() + kProtein46Off, 46 * 4);
-            std::memcpy(dst + kTailOff, rec.data() + kTail46Off, 6 * 4);
-        }
-    }
-    fclose(f);
-    // validation (bion_loader_host.cpp:359-408)
-    for (uint32_t i = 0; i < d->num_connections; i++)
-        if (d->connections[i].segment_a >= d->num_segments || d->connections[i].segment_b >= d->num_segments) {
-            free_aos_arrays(*d); set_error("connection %u out of range", i); return BNC_BION_ERR_BAD_CONN;
-        }
-    for (uint32_t i = 0; i < d->num_synapses; i++) {
-        const BncSynapse& y = d->synapses[i];
-        if (y.pre_segment >= d->num_segments || y.post_segment >= d->num_segments || y.type >= 3) {
-            free_aos_arrays(*d); set_error("synapse %u invalid", i); return BNC_BION_ERR_BAD_SYNAPSE;
-        }
-        if (y.pre_autoreceptor_count > 8 || y.post_receptor_count > 8) {
-            free_aos_arrays(*d); set_error("synapse %u: too many receptors", i); return BNC_ERR_FORMAT;
-        }
-    }
-    for (uint32_t i = 0; i < d->num_neurons; i++)
-        if ((uint64_t)d->neurons[i].segment_start + d->neurons[i].segment_count > d->num_segments) {
-            free_aos_arrays(*d); set_error("neuron %u range", i); return BNC_BION_ERR_BAD_NEURON;
-        }
-    for (uint32_t i = 0; i < d->num_segments; i++)
-        if (d->segments[i].modifier_count > 32) { free_aos_arrays(*d); set_error("segment %u modifiers", i); return BNC_ERR_FORMAT; }
-    for (uint32_t i = 0; i < d->num_segments; i++) d->segments[i].intra_connection_count = 0;
-    for (uint32_t i = 0; i < d->num_connections; i++) {
-        uint32_t a = d->connections[i].segment_a, b = d->connections[i].segment_b;
-        if (d->segments[a].intra_connection_count < 16) d->segments[a].intra_connection_ids[d->segments[a].intra_connection_count++] = i;
-        if (d->segments[b].intra_connection_count < 16) d->segments[b].intra_connection_ids[d->segments[b].intra_connection_count++] = i;
-    }
-    return BNC_OK;
+// .bion files: bion_file.cpp (every version the reference reads; the v14 writer).
+static int save_bion(const BncBionData& d, const char* path) { return bion_write(d, path); }
+static int load_bion_file(const char* path, BncBionData* d, bool default_nuclei = true) {
+    return bion_read(path, d, default_nuclei);
 }
 
 int backend_export_host(void* sim, HostNet* hn, std::vector<BncCurrentStimulus>* stim, uint64_t* tick,
@@ -1780,7 +1679,7 @@ int bnc_load_checkpoint(void* sim, const char* path) {
     if (!ok) { set_error("%s is not a checkpoint state file of this version", sp.c_str()); return BNC_ERR_FORMAT; }
     b->reset_network();
     BncBionData aos;
-    int rc = load_bion_file(path, &aos);
+    int rc = load_bion_file(path, &aos, false);   // the nuclei the run had, none added
     if (rc != BNC_OK) return rc;
     if (aos.num_segments != head[1] || aos.num_synapses != head[2]) {
         free_aos_arrays(aos);

@@ -62,11 +62,15 @@ void* gpu_backend_create_on_device(int device_index);
 /* Replaces gpu_backend_destroy (gpu_backend_cuda.cu:329-331). */
 void gpu_backend_destroy(void* sim);
 /* Replaces gpu_backend_load_bion (gpu_backend_cuda.cu:333-336): loads a .bion
- * file written with the v14 record sizes (v10+ header; the reference's loader
- * also migrates v3-v13 layouts, bion_loader_host.cpp:99-263; those fail here with
- * BNC_BION_ERR_BAD_VERSION).  0 on success, the reference's BION_ERR_* codes on
- * file errors, BNC_ERR_UNSUPPORTED when the network uses something the device
- * path does not implement (message in bnc_last_error). */
+ * file of any version the reference reads (3-14, with its migrations,
+ * bion_loader_host.cpp:26-428, bion_format.h:59-340).  A file without nucleus
+ * records gets one default nucleus per neuron, as the reference's loader creates
+ * them; the nucleus protein levels are mapped onto each synapse's RRP_max, release
+ * probability and RRP recovery as the reference's backend does every tick
+ * (gpu_backend_cuda.cu:275-289), so with default nuclei every synapse whose id is not
+ * 0 takes 10, 0.3 and 0.02.  0 on success, the reference's BION_ERR_* codes on file
+ * errors, BNC_ERR_UNSUPPORTED when the network uses something the device path does
+ * not implement (message in bnc_last_error). */
 int gpu_backend_load_bion(void* sim, const char* filename);
 /* Replaces gpu_backend_run_tick (gpu_backend_cuda.cu:338-341): one tick of dt
  * ms; afterwards the AoS view returned by gpu_backend_bion_data is coherent
@@ -382,10 +386,12 @@ void bnc_plugin_unregister_all(void);
 int bnc_plan_aos(const BncBionData* data, const BncCurrentStimulus* stim, uint32_t n_stim, BncNetInfo* info);
 
 /* Host-only .bion I/O with the reference loader's semantics: bnc_bion_load
- * replaces bion_load_host (src/bion_loader_host.cpp:26-428; v10-v14 files with
- * the v14 record sizes; same BION_ERR_* codes and index validation; arrays owned
- * by the library until bnc_bion_unload, which replaces bion_unload_host);
- * bnc_bion_save replaces bion_save (src/bion_loader_host.cpp:449-504, writes v14). */
+ * replaces bion_load_host (src/bion_loader_host.cpp:26-428: versions 3-14 with the
+ * same migrations, default nuclei for a file without any, the same BION_ERR_* codes
+ * and validation; arrays owned by the library until bnc_bion_unload, which replaces
+ * bion_unload_host).  Bytes the reference's migrations leave unwritten are zero
+ * here.  bnc_bion_save replaces bion_save (src/bion_loader_host.cpp:449-504, writes
+ * v14). */
 int bnc_bion_load(const char* filename, BncBionData* out);
 void bnc_bion_unload(BncBionData* data);
 int bnc_bion_save(const char* filename, const BncBionData* data);

@@ -61,6 +61,38 @@ def _schedule(net):
     return {0: first, 120: second}
 
 
+def _default_nuclei(net):
+    """The nucleus records both reference loaders create for a file without any
+    (bion_loader.cpp:902-914, bion_loader_host.cpp:340-353): one per neuron, its id,
+    enabled, consolidation mode 3, amino-acid level 0.5, protein levels 0.  The
+    reference's GPU backend maps them onto the synapses every tick
+    (gpu_backend_cuda.cu:275-289): RRP_max 10, release probability 0.3, RRP recovery
+    0.02 for every synapse whose id is not 0."""
+    n = int(net.data.num_neurons)
+    nu = np.zeros((n, 500), np.uint8)
+    neurons = np.ctypeslib.as_array(C.cast(net.data.neurons, C.POINTER(C.c_uint8)), (n * 24,)).reshape(n, 24)
+    nu[:, 0:4] = neurons[:, 0:4]   # Neuron.id
+    nu[:, 4] = 1
+    nu[:, 5] = 3
+    nu[:, 492:496] = np.full(n, 0.5, np.float32).view(np.uint8).reshape(n, 4)
+    return nu.reshape(-1)
+
+
+def _oracle_as_loaded(p, nuclei=None):
+    """The oracle on the network as gpu_backend_load_bion holds it: with the file's
+    nuclei, or the default ones, whose protein mapping the oracle applies at creation."""
+    from bioneuroncore_b200 import Network
+    net_o = Network(p)
+    nu = _default_nuclei(net_o) if nuclei is None else nuclei
+    net_o.data.nuclei = nu.ctypes.data
+    net_o.data.num_nuclei = len(nu) // 500
+    try:
+        return Oracle(net_o), net_o
+    finally:
+        net_o.data.nuclei = None
+        net_o.data.num_nuclei = 0
+
+
 def _records(b, n_seg, n_syn):
     from bioneuroncore_b200.abi import SEGMENT_DTYPE, SYNAPSE_DTYPE, view
     d = b.bion_data()
@@ -133,7 +165,7 @@ def test_dropin_sequence_equals_the_oracle(tmp_path, family, on_host):
     if on_host:
         assert b.lib.bnc_records_managed(b.h) == 1
         assert b.lib.bnc_set_records_residency(b.h, 1) == 0
-    ora = Oracle(Network(p))
+    ora, _keep = _oracle_as_loaded(p)
     n_seg, n_syn = net.data.num_segments, net.data.num_synapses
     ticks = 300
     refr_prev = None
@@ -161,7 +193,7 @@ def test_dropin_sequence_within_tolerance_of_the_reference(tmp_path):
     records its own bion_load_host read from the same file): V_m and every ion within
     REL_TOL_FP64 after 200 ticks (FP32 state against FP64 state)."""
     from bioneuroncore_b200 import Backend, Network, NetgenParams, NET_LARGE
-    from bioneuroncore_b200.abi import BionData, SEGMENT_DTYPE, view
+    from bioneuroncore_b200.abi import BionData, SEGMENT_DTYPE, SYNAPSE_DTYPE, view
     p = NetgenParams(family=NET_LARGE, n_neurons=12, seed=3)
     net = Network(p)
     path = tmp_path / "net.bion"
@@ -178,6 +210,24 @@ def test_dropin_sequence_within_tolerance_of_the_reference(tmp_path):
         def segments(self):
             return view(self.data.segments, SEGMENT_DTYPE, self.data.num_segments)
 
+    # what the reference's backend does with the default nuclei its loader created: the
+    # protein mapping (the reference's own function, through oracle/ref_harness.cpp)
+    h = C.CDLL(REF_LIB.replace("libbiocore_ref.so", "libref_harness.so"))
+    h.ref_protein_mapping.argtypes = [C.c_void_p, C.c_void_p]
+    assert rd.num_nuclei == rd.num_neurons > 0
+    nu = np.ctypeslib.as_array(C.cast(rd.nuclei, C.POINTER(C.c_uint8)), (rd.num_nuclei * 500,)).reshape(-1, 500)
+    rsyn = view(rd.synapses, SYNAPSE_DTYPE, rd.num_synapses)
+    rseg0 = view(rd.segments, SEGMENT_DTYPE, rd.num_segments)
+    mapped = 0
+    for k in range(rd.num_synapses):
+        nid = int(rseg0["neuron_id"][rsyn["pre_segment"][k]])
+        if rsyn["id"][k] == 0 or nid >= rd.num_nuclei:
+            continue
+        out = np.zeros(3, np.float32)
+        h.ref_protein_mapping(nu[nid, 244:472].copy().ctypes.data, out.ctypes.data)
+        rsyn["RRP_max"][k], rsyn["release_probability"][k], rsyn["RRP_recovery"][k] = out
+        mapped += 1
+    assert mapped > 0
     ref = Reference(_Held(rd, net.n_stim, net.stim_ptr))
     b = Backend()
     b.load_bion(str(path))
@@ -212,18 +262,15 @@ def test_dropin_with_nuclei_applies_the_protein_mapping(tmp_path):
         nu[i * 500 + 244:i * 500 + 244 + 228] = np.frombuffer(rng.uniform(0.0, 1.0, 57).astype(np.float32).tobytes(),
                                                              np.uint8)
     net = Network(p)
-    net_o = Network(p)
-    for n in (net, net_o):
-        n.data.nuclei = nu.ctypes.data
-        n.data.num_nuclei = 16
+    net.data.nuclei = nu.ctypes.data
+    net.data.num_nuclei = 16
     path = tmp_path / "nuclei.bion"
     try:
         _save(net, path)
-        ora = Oracle(net_o)
     finally:
-        for n in (net, net_o):
-            n.data.nuclei = None
-            n.data.num_nuclei = 0
+        net.data.nuclei = None
+        net.data.num_nuclei = 0
+    ora, _keep = _oracle_as_loaded(p, nu)
     from bioneuroncore_b200.abi import stimulus_data
     b = Backend()
     b.load_bion(str(path))
