@@ -986,7 +986,10 @@ static BuildOptions to_options(const BncBuildOptions* o) {
         if (o->tile_segs) opt.tile_segs = o->tile_segs;
         opt.phase_cap = o->phase_cap;
         if (o->chunk_segs) opt.chunk_segs = o->chunk_segs;
-        if (o->fuse_phases) opt.fuse_phases = o->fuse_phases;
+        if (o->fuse_phases) {
+            opt.fuse_phases = o->fuse_phases;
+            opt.fuse_adaptive = false;
+        }
         opt.group_barriers = o->cta_barriers == 0;
     }
     return opt;

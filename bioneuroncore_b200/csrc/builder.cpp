@@ -860,7 +860,6 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
     for (uint32_t i = 0; i < n && fuse > 1; i++)
         for (uint32_t k = act_off[i]; k < act_off[i + 1]; k++)
             if (item_phase[k] != k - act_off[i] || user_type[act_type[k]]) { fuse = 1; break; }
-    host->fuse = fuse;
     std::vector<ItemKey> keys(act_slot.size());
     if (fuse > 1) {
         uint32_t rank[256];
@@ -870,61 +869,91 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
             for (uint8_t t : act_type) seen[t] = true;
             for (int t = 0; t < 256; t++) rank[t] = seen[t] ? ++R : 0u;   // 1..R; 0: no item
         }
-        // groups are independent (their items go to disjoint phase ranges): one thread each
-        const uint32_t n_groups = (n_phases + fuse - 1) / fuse;
-        std::vector<int> group_err(n_groups, 0);
-        parallel_for(n_groups, [&](size_t g0, size_t g1) {
-            std::vector<uint32_t> rows, tmp, cnt;
-            std::vector<uint8_t> kb;
-            for (size_t gi = g0; gi < g1; gi++) {
-                const uint32_t p0 = (uint32_t)gi * fuse;
-                const uint32_t F = std::min(fuse, n_phases - p0);
-                const uint32_t W = F + 1;   // per row: the item types of the group, then the count key
-                rows.clear();
-                kb.clear();
-                for (uint32_t d = 0; d < n; d++) {   // device order: the order inside a class
-                    const uint32_t i = host->perm[d];
-                    const uint32_t c = act_off[i + 1] - act_off[i];
-                    if (c <= p0) continue;
-                    const uint32_t m = std::min(F, c - p0);
-                    rows.push_back(d);
-                    for (uint32_t j = 0; j < F; j++) kb.push_back(j < m ? (uint8_t)rank[act_type[act_off[i] + p0 + j]] : 0);
-                    kb.push_back((uint8_t)(F - m));
-                }
-                if (rows.size() != bucket_off[p0 + 1] - bucket_off[p0]) { group_err[gi] = 1; continue; }
-                // stable counting sorts, least significant first: the type of each item from
-                // the last phase of the group to the first, then the item count (descending)
-                std::vector<uint32_t> idx(rows.size());
-                std::iota(idx.begin(), idx.end(), 0u);
-                tmp.resize(rows.size());
-                for (int pass = (int)F - 1; pass >= -1; pass--) {
-                    const uint32_t j = pass < 0 ? F : (uint32_t)pass;
-                    const uint32_t nb = (j == F ? F : R) + 2;
-                    cnt.assign(nb, 0u);
-                    for (uint32_t x : idx) cnt[kb[(size_t)x * W + j] + 1]++;
-                    for (uint32_t c = 0; c + 1 < nb; c++) cnt[c + 1] += cnt[c];
-                    for (uint32_t x : idx) tmp[cnt[kb[(size_t)x * W + j]]++] = x;
-                    idx.swap(tmp);
-                }
-                for (uint32_t r = 0; r < (uint32_t)idx.size(); r++) {
-                    const uint32_t d = rows[idx[r]];
-                    const uint32_t i = host->perm[d];
-                    const uint32_t m = F - kb[(size_t)idx[r] * W + F];
-                    for (uint32_t j = 0; j < m; j++) {
-                        const uint32_t k = act_off[i] + p0 + j;
-                        const uint32_t pos = bucket_off[p0 + j] + r;
-                        if (pos >= bucket_off[p0 + j + 1]) { group_err[gi] = 2; break; }
-                        keys[pos] = {(uint16_t)(p0 + j), act_type[k], d, k};
+        // A warp of the group kernel runs, for each item, every model its 32 rows hold
+        // there in turn.  Rows sorted by their items' types share a model while enough
+        // rows share the types before it; when slots are in no particular order (drawn
+        // types listed as drawn), deep groups leave warps on several models per item and
+        // the SMs on most of the 26 models' code at once.  The grouping is redone with
+        // one phase fewer per group while the mean distinct models per warp and item
+        // exceeds kMaxWarpTypes.
+        for (;;) {
+            // groups are independent (their items go to disjoint phase ranges): one thread each
+            const uint32_t n_groups = (n_phases + fuse - 1) / fuse;
+            std::vector<int> group_err(n_groups, 0);
+            std::vector<uint64_t> g_models(n_groups, 0), g_warp_items(n_groups, 0);
+            parallel_for(n_groups, [&](size_t g0, size_t g1) {
+                std::vector<uint32_t> rows, tmp, cnt;
+                std::vector<uint8_t> kb;
+                for (size_t gi = g0; gi < g1; gi++) {
+                    const uint32_t p0 = (uint32_t)gi * fuse;
+                    const uint32_t F = std::min(fuse, n_phases - p0);
+                    const uint32_t W = F + 1;   // per row: the item types of the group, then the count key
+                    rows.clear();
+                    kb.clear();
+                    for (uint32_t d = 0; d < n; d++) {   // device order: the order inside a class
+                        const uint32_t i = host->perm[d];
+                        const uint32_t c = act_off[i + 1] - act_off[i];
+                        if (c <= p0) continue;
+                        const uint32_t m = std::min(F, c - p0);
+                        rows.push_back(d);
+                        for (uint32_t j = 0; j < F; j++) kb.push_back(j < m ? (uint8_t)rank[act_type[act_off[i] + p0 + j]] : 0);
+                        kb.push_back((uint8_t)(F - m));
                     }
-                    if (group_err[gi]) break;
+                    if (rows.size() != bucket_off[p0 + 1] - bucket_off[p0]) { group_err[gi] = 1; continue; }
+                    // stable counting sorts, least significant first: the type of each item from
+                    // the last phase of the group to the first, then the item count (descending)
+                    std::vector<uint32_t> idx(rows.size());
+                    std::iota(idx.begin(), idx.end(), 0u);
+                    tmp.resize(rows.size());
+                    for (int pass = (int)F - 1; pass >= -1; pass--) {
+                        const uint32_t j = pass < 0 ? F : (uint32_t)pass;
+                        const uint32_t nb = (j == F ? F : R) + 2;
+                        cnt.assign(nb, 0u);
+                        for (uint32_t x : idx) cnt[kb[(size_t)x * W + j] + 1]++;
+                        for (uint32_t c = 0; c + 1 < nb; c++) cnt[c + 1] += cnt[c];
+                        for (uint32_t x : idx) tmp[cnt[kb[(size_t)x * W + j]]++] = x;
+                        idx.swap(tmp);
+                    }
+                    for (uint32_t r = 0; r < (uint32_t)idx.size(); r++) {
+                        const uint32_t d = rows[idx[r]];
+                        const uint32_t i = host->perm[d];
+                        const uint32_t m = F - kb[(size_t)idx[r] * W + F];
+                        for (uint32_t j = 0; j < m; j++) {
+                            const uint32_t k = act_off[i] + p0 + j;
+                            const uint32_t pos = bucket_off[p0 + j] + r;
+                            if (pos >= bucket_off[p0 + j + 1]) { group_err[gi] = 2; break; }
+                            keys[pos] = {(uint16_t)(p0 + j), act_type[k], d, k};
+                        }
+                        if (group_err[gi]) break;
+                    }
+                    // distinct models per warp (32 consecutive rows) and item
+                    for (size_t w0 = 0; w0 < idx.size(); w0 += 32) {
+                        const size_t w1 = std::min(idx.size(), w0 + 32);
+                        for (uint32_t j = 0; j < F; j++) {
+                            uint64_t bits[4] = {0, 0, 0, 0};
+                            for (size_t r = w0; r < w1; r++) {
+                                const uint32_t t = kb[(size_t)idx[r] * W + j];
+                                if (t) bits[t >> 6] |= 1ull << (t & 63);
+                            }
+                            const uint32_t c = __builtin_popcountll(bits[0]) + __builtin_popcountll(bits[1]) +
+                                               __builtin_popcountll(bits[2]) + __builtin_popcountll(bits[3]);
+                            if (c) { g_models[gi] += c; g_warp_items[gi]++; }
+                        }
+                    }
                 }
-            }
-        }, 1);
-        for (uint32_t gi = 0; gi < n_groups; gi++)
-            if (group_err[gi]) {
-                set_error("fused phase schedule: phase group %u does not nest (%d)", gi, group_err[gi]);
-                return BNC_ERR_FORMAT;
-            }
+            }, 1);
+            for (uint32_t gi = 0; gi < n_groups; gi++)
+                if (group_err[gi]) {
+                    set_error("fused phase schedule: phase group %u does not nest (%d)", gi, group_err[gi]);
+                    return BNC_ERR_FORMAT;
+                }
+            uint64_t models = 0, warp_items = 0;
+            for (uint32_t gi = 0; gi < n_groups; gi++) { models += g_models[gi]; warp_items += g_warp_items[gi]; }
+            host->warp_models = warp_items ? (double)models / (double)warp_items : 1.0;
+            if (!opt.fuse_adaptive || fuse <= 2 || n < kAdaptiveFuseMinSegs || host->warp_models <= kMaxWarpTypes)
+                break;
+            fuse--;
+        }
     } else {
         std::vector<uint32_t> pos(bucket_off.begin(), bucket_off.end() - 1);
         for (uint32_t d = 0; d < n; d++) {   // device order: each bucket fills in segment order
@@ -944,6 +973,7 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
             for (const ItemKey& kk : tmp) keys[lo + tc[kk.type]++] = kk;
         }
     }
+    host->fuse = fuse;
     lap("item sort");
     const uint32_t NI = (uint32_t)keys.size();
     std::vector<uint32_t> it_seg(NI);

@@ -210,11 +210,24 @@ struct BuildOptions {
     // 1: 3.94, 2: 2.89, 3: 2.40, 4: 2.15, 6: 2.43, 9: 4.97, 17: 19.5 ms (deeper groups
     // diverge: rows sorted by their items' types share fewer types further down).
     uint32_t fuse_phases = 4;
+    // Lower fuse_phases while the rows sorted for its groups leave warps on more than
+    // kMaxWarpTypes distinct models per item on average (an explicit fuse_phases option
+    // turns this off).
+    bool fuse_adaptive = true;
     // Diffusion barriers over aligned thread groups where the tile allows (false: always
     // the whole CTA).
     bool group_barriers = true;
 };
 constexpr uint32_t kMaxFuse = 32;
+// Distinct channel models a warp may run per item of a phase group, on average over
+// the group's warps and items, before a shallower group is preferred.  Large set,
+// 640k segments: slots listed by type ID give 1.05 at 4 phases per group; slots in
+// draw order 1.21 at 3 and 3.36 at 4, where step 1 took 3.0x longer at 6.4M segments
+// (16.1 against 5.5 ms per tick: instruction-cache misses, 12 of 32 lanes active).
+constexpr double kMaxWarpTypes = 1.3;
+// Below this many segments a modifier launch is a few microseconds of work, its count
+// matters more than divergence, and the requested depth is kept.
+constexpr uint32_t kAdaptiveFuseMinSegs = 1u << 16;
 
 // Host copy of everything the exporter needs to map device state back.
 struct NetHost {
@@ -236,6 +249,7 @@ struct NetHost {
     std::vector<uint32_t> phase_off;         // item range of each (chunk, phase) bucket (host copy)
     uint32_t chunk_segs = 0, n_chunks = 1;   // modifier-pass chunks of consecutive segments
     uint32_t fuse = 1;                       // modifier phases per launch (item order follows)
+    double warp_models = 1.0;                // mean distinct models per warp and item of a group
     uint8_t item_dyn_rows = 0;               // state words (bits) any item updates: the rows exported
     struct UserRange { uint32_t bucket, type, begin, end; const void* kernel; };
     std::vector<UserRange> user_ranges;      // registered device modifiers' items, per bucket

@@ -87,6 +87,14 @@ def test_modifier_phase_groups():
         assert inf.fuse_phases == want
         assert inf.modifier_launches == 1 + -(-inf.n_phases // want)
     assert plan_generated(p).fuse_phases == 4            # the default
+    # from 65,536 segments on, the depth drops while warps would run more than 1.3
+    # models per item on average: slots listed by type ID keep 4, slots in draw order
+    # (no common order between segments) get 2 at 128k segments
+    from bioneuroncore_b200 import NETGEN_DRAW_ORDER
+    assert plan_generated(NetgenParams(family=NET_LARGE, n_neurons=2000, seed=2)).fuse_phases == 4
+    assert plan_generated(NetgenParams(family=NET_LARGE, n_neurons=2000, seed=2, flags=NETGEN_DRAW_ORDER)).fuse_phases == 2
+    assert plan_generated(NetgenParams(family=NET_LARGE, n_neurons=2000, seed=2, flags=NETGEN_DRAW_ORDER),
+                          BuildOptions(fuse_phases=4)).fuse_phases == 4   # an explicit depth is kept
     small = plan_generated(NetgenParams(family=NET_SMALL, n_neurons=16, seed=2), BuildOptions(fuse_phases=3))
     assert small.fuse_phases == 1 and small.modifier_launches == 1 + small.n_phases
     # chunked modifier passes keep one launch per phase and chunk
