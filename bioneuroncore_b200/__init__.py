@@ -18,7 +18,7 @@ import numpy as np
 from .abi import (BionData, NetgenParams, SEGMENT_DTYPE, SYNAPSE_DTYPE, CONN_DTYPE, STIM_DTYPE, view,
                   NET_SMALL, NET_LARGE, NET_TREES, NET_ENSEMBLE_MEMBER, NET_ADJOINT, NETGEN_NO_SYNAPSES,
                   NETGEN_NO_CONNECTIONS, NETGEN_NO_STIMULI, NETGEN_PERTURB_IONS, NETGEN_SYNAPSE_EXTRAS,
-                  NETGEN_FULL_SMALL_SET, NETGEN_GLYCINE, NETGEN_DRAW_ORDER)
+                  NETGEN_FULL_SMALL_SET, NETGEN_GLYCINE, NETGEN_DRAW_ORDER, NETGEN_RELEASE_MODULATORS)
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libbnc_b200.so")
@@ -26,7 +26,7 @@ LIB_PATH = os.path.join(_HERE, "libbnc_b200.so")
 SEG_FIELDS = {"V": 0, "ion_in": 1, "ion_out": 2, "ATP": 3, "temperature": 4, "transcription": 5,
               "intra_nt": 6, "neurotransmitter": 7, "mod_state": 8, "spikes": 9}
 SYN_FIELDS = {"bouton_Ca": 0, "spine_Ca": 1, "weight": 2, "refractory": 3, "cleft": 4, "receptor_state": 5,
-              "facilitation": 6, "spine_camkii": 7, "spine_calcineurin": 8, "RRP": 9}
+              "facilitation": 6, "spine_camkii": 7, "spine_calcineurin": 8, "RRP": 9, "autoreceptor_state": 11}
 
 # Symbols the reference's loader requires (reference tests/smoke_cuda.sh:24-29) plus the
 # ABI probes and this backend's own entry points; include/*.h declares every one.
@@ -410,7 +410,7 @@ class Backend:
 __all__ = ["Backend", "Network", "Adjoint", "AdjointConfig", "AdjointInfo", "SweepTask", "SweepResult",
            "sweep_parse_params", "sweep_tasks", "sweep_run", "SWEEP_SINGLE_TICK", "NetgenParams", "BionData", "BackendError", "load_library", "last_error",
            "NET_SMALL", "NET_LARGE", "NET_TREES", "NET_ENSEMBLE_MEMBER", "NET_ADJOINT", "NETGEN_NO_SYNAPSES",
-           "NETGEN_NO_CONNECTIONS", "NETGEN_NO_STIMULI", "NETGEN_PERTURB_IONS", "NETGEN_SYNAPSE_EXTRAS", "NETGEN_FULL_SMALL_SET", "NETGEN_GLYCINE", "NETGEN_DRAW_ORDER", "SEG_FIELDS", "SYN_FIELDS",
+           "NETGEN_NO_CONNECTIONS", "NETGEN_NO_STIMULI", "NETGEN_PERTURB_IONS", "NETGEN_SYNAPSE_EXTRAS", "NETGEN_FULL_SMALL_SET", "NETGEN_GLYCINE", "NETGEN_DRAW_ORDER", "NETGEN_RELEASE_MODULATORS", "SEG_FIELDS", "SYN_FIELDS",
            "DROPIN_SYMBOLS", "NEW_SYMBOLS", "EnsembleMember", "Tuning", "BuildOptions", "register_device_modifier", "ensemble_params", "plan_ensemble", "plan_generated",
            "DIFFUSION_RESIDUAL", "DIFFUSION_LEDGER", "DiffusionStats"]
 

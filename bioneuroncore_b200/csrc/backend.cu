@@ -49,6 +49,8 @@ struct Backend {
         uint8_t* syn_nt;      // device synapse -> the cleft entry it carries
         uint32_t* rec_syn;    // device receptor -> device synapse
         uint8_t* rec_slot;    // device receptor -> receptor slot
+        uint32_t* md_syn;     // release modulator -> record
+        uint8_t* md_slot;     // release modulator -> autoreceptor slot
     } xm{};
     uint32_t tick_stride = 1;   // the tick counter's step per tick (2: the reference's batch mode)
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -165,10 +167,11 @@ int export_network(const NetDev& d, const NetHost& h, uint64_t ticks_run, BncBio
                  oTxn = x_txn ? take(n) : 0;
     size_t oSt[7];
     for (int k = 0; k < 7; k++) oSt[k] = ((rows >> k) & 1u) ? take(NI) : 0;
-    size_t oSy[8] = {0}, oRc = 0;
+    size_t oSy[8] = {0}, oRc = 0, oMd = 0;
     if (K) {
         for (int f = 0; f < 8; f++) oSy[f] = take(K);
         oRc = take((size_t)3 * NR);
+        oMd = take(d.n_md);
     }
     const size_t bytes = off * sizeof(float) + K;
     std::lock_guard<std::mutex> lock(g_stage_mu);
@@ -194,6 +197,7 @@ int export_network(const NetDev& d, const NetHost& h, uint64_t ticks_run, BncBio
                                d.sy_cleft, d.sy_rrp};
         for (int f = 0; f < 8; f++) get(oSy[f], src[f], (size_t)K * 4);
         get(oRc, d.rc_st, (size_t)3 * NR * 4);
+        get(oMd, d.md_st, (size_t)d.n_md * 4);
         if (ok) ok = cudaMemcpy(refr, d.sy_refr, K, cudaMemcpyDeviceToHost) == cudaSuccess;
     }
     if (!ok) { set_error("export: device read failed"); return BNC_ERR_CUDA; }
@@ -247,6 +251,12 @@ int export_network(const NetDev& d, const NetHost& h, uint64_t ticks_run, BncBio
                 if (ticks_run > 0) m.state[7] = y.post_area;
             }
         });
+        for (uint32_t q = 0; q < d.n_md; q++) {
+            BncSynapse& y = aos->synapses[h.md_syn[q]];
+            BncModifier& m = y.pre_autoreceptors[h.md_slot[q]];
+            m.state[0] = F[oMd + q];
+            if (ticks_run > 0) m.state[7] = y.pre_area;
+        }
     }
     return BNC_OK;
 }
@@ -473,6 +483,17 @@ __global__ void k_export_receptors(NetDev d, const uint32_t* rec_syn, const uint
     }
 }
 
+__global__ void k_export_modulators(NetDev d, const uint32_t* md_syn, const uint8_t* md_slot, unsigned char* syn,
+                                    int after_tick) {
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < d.n_md; q += gridDim.x * blockDim.x) {
+        unsigned char* y = syn + (size_t)md_syn[q] * kSynBytes;
+        unsigned char* m = y + offsetof(BncSynapse, pre_autoreceptors) + (size_t)md_slot[q] * kModBytes;
+        put<double>(m, kOffModState, (double)d.md_st[q]);
+        if (after_tick)
+            put<double>(m, kOffModState + 8 * 7, (double)*reinterpret_cast<const float*>(y + offsetof(BncSynapse, pre_area)));
+    }
+}
+
 template <typename T>
 T* upload_map(Backend* b, const std::vector<T>& v, bool* ok) {
     if (!*ok || v.empty()) return nullptr;
@@ -517,6 +538,8 @@ static int make_records_managed(Backend* b) {
         x.syn_nt = upload_map(b, h.syn_nt, &ok);
         x.rec_syn = upload_map(b, h.rec_syn, &ok);
         x.rec_slot = upload_map(b, h.rec_slot, &ok);
+        x.md_syn = upload_map(b, h.md_syn, &ok);
+        x.md_slot = upload_map(b, h.md_slot, &ok);
         if (!ok) {
             cudaFree(ms);
             cudaFree(my);
@@ -559,6 +582,7 @@ static int export_records(Backend* b) {
     if (d.n_rec)
         k_export_receptors<<<grid(d.n_rec), 256, 0, b->stream>>>(d, b->xm.rec_syn, b->xm.rec_slot, b->xm.syn_orig, syn,
                                                                  after);
+    if (d.n_md) k_export_modulators<<<grid(d.n_md), 256, 0, b->stream>>>(d, b->xm.md_syn, b->xm.md_slot, syn, after);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) { b->failed = true; return cuda_fail(e, "record export launch"); }
     return sync_stream(b);
@@ -1440,6 +1464,14 @@ int bnc_read_synapse_field(void* sim, int field, int index, float* out, uint32_t
         case 7: src = d.sy_camkii; break;
         case 8: src = d.sy_calcn; break;
         case 9: src = d.sy_rrp; break;
+        case 11: {   // autoreceptor state: index = slot * 8 + word; word 0 of release modulators
+            const int j = index >> 3, w = index & 7;
+            if (w != 0) { set_error("autoreceptor states other than word 0 of release modulators are not tracked"); return BNC_ERR_ARG; }
+            if (d.n_md && !d2h(v, d.md_st, d.n_md)) return cuda_fail(cudaGetLastError(), "read");
+            for (uint32_t q = 0; q < d.n_md; q++)
+                if (b->host.md_slot[q] == j) out[b->host.md_syn[q]] = v[q];
+            return BNC_OK;
+        }
         default: set_error("unknown synapse field %d", field); return BNC_ERR_ARG;
     }
     if (!d2h(v, src, K)) return cuda_fail(cudaGetLastError(), "read");

@@ -108,6 +108,24 @@ float bouton_gamma(uint8_t t) {
         default: return 0.0f;
     }
 }
+// Presynaptic release modulators (receptors_biological.cpp:428-509, dispatched by
+// kernel_dispatch.h:575-604): kind << 4 | the cleft transmitter the type reads; kind 1
+// Gi/o, 2 Gs, 3 ionotropic; 0 for every other type (the dispatch's default factor 1).
+uint8_t modulator_code(uint8_t t) {
+    switch (t) {
+        case 18: case 19: return 0x13;   // 5-HT1A, 5-HT1B: serotonin
+        case 22: return 0x12;            // D2: dopamine
+        case 27: return 0x15;            // A1: adenosine
+        case 29: case 30: return 0x10;   // mGluR2, mGluR3: glutamate
+        case 35: return 0x16;            // alpha2: noradrenaline
+        case 36: return 0x19;            // CB1: endocannabinoid
+        case 38: return 0x18;            // H3: histamine
+        case 44: return 0x22;            // D1: dopamine
+        case 46: return 0x25;            // A2A: adenosine
+        case 13: return 0x34;            // nicotinic: acetylcholine
+        default: return 0;
+    }
+}
 // run_tick_common.h:199-206
 uint8_t nt_from_receptor(uint8_t rt) {
     if (rt == 11 || rt == 17) return 1;
@@ -1115,10 +1133,10 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
                     set_error("synapse %u autoreceptor %u: type %u is registered by a host plugin (a CPU function), "
                               "which this backend cannot run", k, j, hn.pre_ar(k, j).type);
                 return BNC_ERR_UNSUPPORTED;
-            } else if (bouton_gamma(hn.pre_ar(k, j).type) == 0.0f) {
+            } else if (bouton_gamma(hn.pre_ar(k, j).type) == 0.0f && modulator_code(hn.pre_ar(k, j).type) == 0) {
                 if (report)
-                    set_error("synapse %u autoreceptor %u: type %u (release modulators are not supported)", k, j,
-                              hn.pre_ar(k, j).type);
+                    set_error("synapse %u autoreceptor %u: type %u is neither a bouton channel nor a release modulator",
+                              k, j, hn.pre_ar(k, j).type);
                 return BNC_ERR_UNSUPPORTED;
             }
         uint8_t ntt = y.post_receptor_count > 0 ? nt_from_receptor(hn.post_rec(k, 0).type) : 0;
@@ -1290,6 +1308,45 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
                 if (fill_syn((uint32_t)q, false) != 0) bad.note(q);
         });
         if (bad.any()) return fill_syn((uint32_t)bad.at.load(), true);
+    }
+    // release modulators of the autoreceptors, per sliced synapse in autoreceptor order
+    std::vector<uint32_t> md_off;
+    std::vector<uint8_t> md_code;
+    std::vector<double> md_scale;
+    std::vector<float> md_st;
+    host->md_syn.clear(); host->md_slot.clear();
+    {
+        uint32_t total = 0;
+        std::vector<uint32_t> cnt(K, 0);
+        for (uint32_t q = 0; q < K; q++) {
+            const SynLite& y = hn.syn[syn_valid[q]];
+            for (uint8_t j = 0; j < y.pre_autoreceptor_count; j++)
+                if (modulator_code(hn.pre_ar(syn_valid[q], j).type)) cnt[q]++;
+            total += cnt[q];
+        }
+        if (total) {
+            md_off.assign(K + 1, 0);
+            for (uint32_t q = 0; q < K; q++) md_off[q + 1] = md_off[q] + cnt[q];
+            md_code.resize(total); md_scale.resize(total); md_st.resize(total);
+            host->md_syn.resize(total); host->md_slot.resize(total);
+            for (uint32_t q = 0; q < K; q++) {
+                const SynLite& y = hn.syn[syn_valid[q]];
+                uint32_t o = md_off[q];
+                // effective_area_mod: state[7], which the release step sets to pre_area, if > 0
+                const float area = y.pre_area > 0.0f ? y.pre_area : 1.0f;
+                for (uint8_t j = 0; j < y.pre_autoreceptor_count; j++) {
+                    const ModLite& m = hn.pre_ar(syn_valid[q], j);
+                    const uint8_t code = modulator_code(m.type);
+                    if (!code) continue;
+                    md_code[o] = code;
+                    md_scale[o] = (double)m.density * (double)area;
+                    md_st[o] = m.state[0];
+                    host->md_syn[o] = syn_valid[q];
+                    host->md_slot[o] = j;
+                    o++;
+                }
+            }
+        }
     }
     // receptor order: slice by slice, receptor j of each lane that has one.  A warp's
     // receptors are those of its synapses, so a prefix sum of per-warp counts places
@@ -1483,6 +1540,13 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
         dev->rc_av = up(allocs, rc_av, &rc);
         dev->rc_den = up(allocs, rc_den, &rc);
         dev->rc_st = up(allocs, rc_st, &rc);
+        if (!md_off.empty()) {
+            dev->md_off = up(allocs, md_off, &rc);
+            dev->md_code = up(allocs, md_code, &rc);
+            dev->md_scale = up(allocs, md_scale, &rc);
+            dev->md_st = up(allocs, md_st, &rc);
+            dev->n_md = (uint32_t)md_st.size();
+        }
         if (any_delay) {
             dev->dl_arr = zeros<unsigned long long>(allocs, (size_t)4 * K, &rc);
             dev->dl_amt = zeros<float>(allocs, (size_t)4 * K, &rc);

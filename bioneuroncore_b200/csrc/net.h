@@ -164,6 +164,14 @@ struct NetDev {
     unsigned long long* dl_arr;  // [4][n_syn]
     float* dl_amt;
     uint8_t* dl_nt;
+    // Release modulators among the presynaptic autoreceptors (md_off null when the
+    // network has none): those of sliced synapse k are [md_off[k], md_off[k + 1]), in
+    // autoreceptor order.
+    uint32_t* md_off;         // [n_syn + 1]
+    uint8_t* md_code;         // kind << 4 | cleft NT index; kind 1 Gi/o, 2 Gs, 3 ionotropic
+    double* md_scale;         // density x effective area (pre_area, or 1 when not positive)
+    float* md_st;             // state[0]
+    uint32_t n_md;
     uint32_t* spike_count;    // [n_seg]
     int* err_flag;            // device-side error report (0 = ok)
     // Captured tick loops: when set, the kernels take the tick from clock[0] and the
@@ -240,6 +248,8 @@ struct NetHost {
     std::vector<uint32_t> rec_syn;   // device receptor -> device synapse
     std::vector<uint8_t> rec_slot;   // device receptor -> receptor slot
     std::vector<uint8_t> syn_nt;     // released NT per device synapse
+    std::vector<uint32_t> md_syn;    // release modulator -> original synapse index
+    std::vector<uint8_t> md_slot;    // release modulator -> autoreceptor slot
     uint32_t max_tile_segs = 0, max_tile_edges = 0;
     uint32_t max_tile_stride = 0;            // own + ghost segments of the largest tile
     uint32_t cluster = 1;                    // CTAs per diffusion cluster (2: tiles in pairs)

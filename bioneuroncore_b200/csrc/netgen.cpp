@@ -134,6 +134,7 @@ int generate_network(const BncNetgenParams& p, NetSink& sink, NetShape* shape_ou
 
     Rng rng_geo(p.seed * 4 + 1), rng_mod(p.seed * 4 + 2), rng_syn(p.seed * 4 + 3), rng_stim(p.seed * 4 + 4);
     Rng rng_extra(p.seed * 4 + 0x9E37);   // BNC_NETGEN_SYNAPSE_EXTRAS only
+    Rng rng_modul(p.seed * 4 + 0x5BD1);   // BNC_NETGEN_RELEASE_MODULATORS only
     float wsum = 0.0f;
     for (const auto& t : kLargeTypes) wsum += t.weight;
 
@@ -291,6 +292,17 @@ int generate_network(const BncNetgenParams& p, NetSink& sink, NetShape* shape_ou
                     sy.pre_autoreceptor_count = 1;
                 }
                 if (rng_extra.u01() < 0.3) sy.delay = (float)(0.5 + 1.5 * rng_extra.u01());
+            }
+            if (p.flags & BNC_NETGEN_RELEASE_MODULATORS) {
+                static const uint8_t kModulators[12] = {18, 19, 22, 27, 29, 30, 35, 36, 38, 44, 46, 13};
+                if (rng_modul.u01() < 0.5) {
+                    const int nm = rng_modul.u01() < 0.5 ? 1 : 2;
+                    for (int q = 0; q < nm && sy.pre_autoreceptor_count < BNC_MAX_PRE_AUTORECEPTORS; q++) {
+                        BncModifier& m = sy.pre_autoreceptors[sy.pre_autoreceptor_count++];
+                        set_mod(m, kModulators[rng_modul.below(12)], (double)(float)(0.2 + 0.8 * rng_modul.u01()));
+                        m.state[0] = (double)(float)(0.5 * rng_modul.u01());
+                    }
+                }
             }
             sy.release_probability = 0.3f;
             sy.release_amount = 1.0f;

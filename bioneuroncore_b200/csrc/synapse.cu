@@ -151,6 +151,31 @@ k_synapse(NetDev d, float dt, unsigned long long tick, int first_tick) {
                 float Ca_uM = bouton * MM_TO_UM;
                 float ca_act = dm_pow(Ca_uM, 4.0f) / (dm_pow(Ca_uM, 4.0f) + dm_pow(10.0f, 4.0f));
                 float p = d.sy_prel[k] * ca_act;
+                // release modulators of the autoreceptors, in autoreceptor order
+                // (kernel_dispatch.h:575-604, receptors_biological.cpp:428-509); the
+                // bouton channels take the dispatch's default factor 1
+                if (d.md_off) {
+                    const uint32_t m1 = d.md_off[k + 1];
+                    for (uint32_t mi = d.md_off[k]; mi < m1; mi++) {
+                        const uint32_t code = d.md_code[mi];
+                        const uint32_t kind = code >> 4;
+                        const float c = ((int)(code & 15u) == ntt) ? cleft : 0.0f;
+                        const float activation = c / (c + 0.5f);
+                        const double scale = d.md_scale[mi];
+                        float f;
+                        if (kind == 3) {
+                            f = (float)(1.0f + (double)(0.3f * activation) * scale);
+                        } else {
+                            float s0 = d.md_st[mi];
+                            s0 = (float)((double)s0 + ((double)activation - (double)s0) * (double)dt /
+                                         (kind == 1 ? 50.0 : 30.0));
+                            d.md_st[mi] = s0;
+                            f = (kind == 1) ? (float)(1.0f - (double)0.7f * (double)s0 * scale)
+                                            : (float)(1.0f + (double)0.5f * (double)s0 * scale);
+                        }
+                        p *= f;
+                    }
+                }
                 uint32_t vbits = (uint32_t)(long long)((double)pr.x * 1000.0f);
                 uint32_t seed = d.sy_id[k] ^ (uint32_t)tick ^ vbits;
                 if (xorshift32_rnd(seed) < p) {

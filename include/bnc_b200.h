@@ -136,6 +136,11 @@ typedef struct {
 /* Synapses with an odd index take a glycine receptor (transmitter glycine) as their
  * first receptor instead of AMPA or GABA-A; other draws are unchanged. */
 #define BNC_NETGEN_GLYCINE 128u
+/* About half the synapses also get one or two presynaptic release-modulator
+ * autoreceptors (Gi/o, Gs and ionotropic types: 5-HT1A/1B, D1, D2, A1, A2A, mGluR2/3,
+ * alpha2, CB1, H3, nicotinic), density 0.2-1, state[0] 0-0.5, after any bouton
+ * channel (drawn from a stream of their own: other draws are unchanged). */
+#define BNC_NETGEN_RELEASE_MODULATORS 256u
 
 /* Generates a network into host AoS arrays in the reference layout.  The arrays
  * are owned by the library; release with bnc_netgen_free.  *stim receives the

@@ -13,7 +13,7 @@
  *
  * Supported subset (the loader rejects the rest with an error): modifier types
  * listed in bo_type_supported(), chemical synapses, pre-autoreceptors that are
- * bouton K/Na channels, every stimulus kind of GpuStimulusData (current steps,
+ * bouton K/Na channels or release modulators, every stimulus kind of GpuStimulusData (current steps,
  * clamps, ramps, ion and ligand injections; bo_upload_stimuli), no mechano
  * stimuli, no consolidation/nuclei.
  */
@@ -547,6 +547,44 @@ static float bo_bouton_gamma(uint8_t t) {
     }
 }
 
+/* Release modulators of presynaptic autoreceptors (receptors_biological.cpp:428-509,
+ * dispatched by kernel_dispatch.h:575-604): kind 1 Gi/o (state[0] relaxes to the
+ * activation with tau 50 ms, factor 1 - 0.7 s0 scale), kind 2 Gs (tau 30 ms, factor
+ * 1 + 0.5 s0 scale), kind 3 ionotropic (factor 1 + 0.3 activation scale), with
+ * activation = nt / (nt + 0.5) of the cleft transmitter the type reads and scale =
+ * density x effective_area_mod (state[7] if > 0, else 1).  Other types (the bouton
+ * channels) take the dispatch's default, 1. */
+static int bo_modulator_kind(uint8_t t, int* nt) {
+    switch (t) {
+        case 18: case 19: *nt = 3; return 1;   /* 5-HT1A, 5-HT1B: serotonin */
+        case 22: *nt = 2; return 1;            /* D2: dopamine */
+        case 27: *nt = 5; return 1;            /* A1: adenosine */
+        case 29: case 30: *nt = 0; return 1;   /* mGluR2, mGluR3: glutamate */
+        case 35: *nt = 6; return 1;            /* alpha2: noradrenaline */
+        case 36: *nt = 9; return 1;            /* CB1: endocannabinoid */
+        case 38: *nt = 8; return 1;            /* H3: histamine */
+        case 44: *nt = 2; return 2;            /* D1: dopamine */
+        case 46: *nt = 5; return 2;            /* A2A: adenosine */
+        case 13: *nt = 4; return 3;            /* nicotinic: acetylcholine */
+        default: *nt = 0; return 0;
+    }
+}
+
+static float bo_release_modulator(OMod* m, const float* cleft, float dt) {
+    int nt;
+    const int kind = bo_modulator_kind(m->type, &nt);
+    if (!kind) return 1.0f;
+    const float c = cleft[nt];
+    const float activation = c / (c + 0.5f);
+    const float area = (m->st[7] > 0.0f) ? (float)m->st[7] : 1.0f;
+    const double scale = (double)m->density * (double)area;
+    if (kind == 3) return (float)(1.0f + (double)(0.3f * activation) * scale);
+    const float tau = (kind == 1) ? 50.0f : 30.0f;
+    m->st[0] = BO_ST((double)m->st[0] + ((double)activation - (double)m->st[0]) * (double)dt / (double)tau);
+    if (kind == 1) return (float)(1.0f - (double)0.7f * (double)m->st[0] * scale);
+    return (float)(1.0f + (double)0.5f * (double)m->st[0] * scale);
+}
+
 static void bo_bouton_ca_step(const OSeg* pre, OSyn* syn, float dt) {
     float g_K = 0.0f, g_Na = 0.0f;
     for (uint8_t j = 0; j < syn->n_pre_ar; j++) {
@@ -743,7 +781,7 @@ static void bo_tick(BoSim* S, float dt) {
             float p = syn->p_rel * ca_act;
             for (int j = 0; j < syn->n_pre_ar; j++) {
                 syn->pre_ar[j].st[7] = syn->pre_area;
-                p *= 1.0f;   /* bouton channels carry no release modulator (dispatch default 1.0) */
+                p *= bo_release_modulator(&syn->pre_ar[j], syn->cleft, dt);
             }
             uint32_t seed = syn->id ^ ((uint32_t)tick) ^ bo_vm_seed_bits(pre->V);
             if (bo_xorshift32_rnd(seed) < p) {
@@ -1101,6 +1139,7 @@ static double bo_syn_value(const BoSim* S, uint32_t i, int field, int idx) {
         case 8: return y->spine_calcineurin;
         case 9: return y->RRP;
         case 10: return y->depr;
+        case 11: return ((idx >> 3) < y->n_pre_ar) ? y->pre_ar[idx >> 3].st[idx & 7] : 0.0;
     }
     return 0.0;
 }

@@ -139,6 +139,12 @@ def _compare(seg, syn, ora, full, label):
                 _eq(np.where(has, syn["post_receptors"][:, j]["state"][:, k], 0.0),
                     np.where(has, ora.synapse_field("receptor_state", j * 8 + k), 0.0),
                     "%s receptor %d state %d" % (label, j, k))
+        for j in range(int(syn["pre_autoreceptor_count"].max())):   # release modulators' state[0]
+            types = np.where(syn["pre_autoreceptor_count"] > j, syn["pre_autoreceptors"][:, j]["type"], 0)
+            mod = np.isin(types, [13, 18, 19, 22, 27, 29, 30, 35, 36, 38, 44, 46])
+            if mod.any():
+                _eq(syn["pre_autoreceptors"][:, j]["state"][:, 0][mod],
+                    ora.synapse_field("autoreceptor_state", j * 8)[mod], "%s autoreceptor %d state 0" % (label, j))
 
 
 def _rel(a, b, floor):
@@ -147,15 +153,18 @@ def _rel(a, b, floor):
     return float((np.abs(a - b) / np.maximum(np.abs(b), floor)).max())
 
 
-@pytest.mark.parametrize("family,on_host", [("large", 0), ("large", 1), ("extras", 0)])
+@pytest.mark.parametrize("family,on_host", [("large", 0), ("large", 1), ("extras", 0), ("modulators", 0),
+                                           ("modulators", 1)])
 def test_dropin_sequence_equals_the_oracle(tmp_path, family, on_host):
     """on_host: the records moved to plain host memory and updated by the host export
     (bnc_set_records_residency), instead of managed memory written on the device."""
-    from bioneuroncore_b200 import Backend, Network, NetgenParams, NET_LARGE, NET_SMALL, NETGEN_SYNAPSE_EXTRAS
+    from bioneuroncore_b200 import (Backend, Network, NetgenParams, NET_LARGE, NET_SMALL, NETGEN_SYNAPSE_EXTRAS,
+                                    NETGEN_RELEASE_MODULATORS)
     if family == "large":
         p = NetgenParams(family=NET_LARGE, n_neurons=12, seed=3)
     else:
-        p = NetgenParams(family=NET_SMALL, n_neurons=16, seed=6, flags=NETGEN_SYNAPSE_EXTRAS, stim_pA=3000.0)
+        flags = NETGEN_SYNAPSE_EXTRAS | (NETGEN_RELEASE_MODULATORS if family == "modulators" else 0)
+        p = NetgenParams(family=NET_SMALL, n_neurons=16, seed=6, flags=flags, stim_pA=3000.0)
     net = Network(p)
     path = tmp_path / "net.bion"
     _save(net, path)

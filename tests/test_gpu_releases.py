@@ -121,3 +121,27 @@ def test_full_small_workload_bitexact():
     synapses, 4,000 ticks at dt 0.025 ms, 0.2 nA steps on 10% of somata."""
     from bioneuroncore_b200 import NetgenParams, NET_SMALL
     _run(NetgenParams(family=NET_SMALL, n_neurons=64, seed=7), 4000, 1000)
+
+
+def test_release_modulators_bitexact():
+    """Presynaptic release modulators (Gi/o, Gs and ionotropic autoreceptors) beside
+    bouton channels, pools and delays, 1,000 ticks: the modulators' state words, the
+    release decisions and all other state equal the oracle's bit for bit."""
+    from bioneuroncore_b200 import NetgenParams, NET_SMALL, NETGEN_SYNAPSE_EXTRAS, NETGEN_RELEASE_MODULATORS
+    p = NetgenParams(family=NET_SMALL, n_neurons=16, seed=6,
+                     flags=NETGEN_SYNAPSE_EXTRAS | NETGEN_RELEASE_MODULATORS, stim_pA=3000.0)
+    log, net = _run(p, 1000, 100)
+    assert len(log) > 0
+    ora, gpu, net = _pair(p)
+    ora.run(400, DT)
+    gpu.run_ticks(400, DT)
+    n_syn = net.data.num_synapses
+    nmod = 0
+    for j in range(int(net.synapses["pre_autoreceptor_count"].max())):
+        g = gpu.synapse_field("autoreceptor_state", j * 8, n_syn)
+        o = ora.synapse_field("autoreceptor_state", j * 8)
+        types = np.where(net.synapses["pre_autoreceptor_count"] > j, net.synapses["pre_autoreceptors"][:, j]["type"], 0)
+        is_mod = np.isin(types, [13, 18, 19, 22, 27, 29, 30, 35, 36, 38, 44, 46])
+        nmod += int(is_mod.sum())
+        _same(g[is_mod], o[is_mod], "modulator state, autoreceptor %d" % j)
+    assert nmod > 0

@@ -178,6 +178,32 @@ def test_synapse_extras_with_releases_bit_identical():
     assert any(syn["pre_autoreceptor_count"][s] > 0 for s in released), "a synapse with autoreceptors must release"
 
 
+def test_release_modulators_bit_identical():
+    """Presynaptic release-modulator autoreceptors (Gi/o, Gs and ionotropic types,
+    receptors_biological.cpp:428-509) beside bouton channels, pools and delays: the
+    modulators' state[0] and every release decision, 1,000 ticks."""
+    from bioneuroncore_b200 import NET_SMALL, NETGEN_SYNAPSE_EXTRAS, NETGEN_RELEASE_MODULATORS
+    spec = dict(family=NET_SMALL, n=16, seed=6, flags=NETGEN_SYNAPSE_EXTRAS | NETGEN_RELEASE_MODULATORS,
+                stim_pA=3000.0)
+    net_r = _net(**spec)
+    syn = net_r.synapses
+    types = {int(syn["pre_autoreceptors"][k, j]["type"]) for k in range(len(syn))
+             for j in range(int(syn["pre_autoreceptor_count"][k]))}
+    assert {29, 30} & types and types & {18, 19, 22, 27, 35, 36, 38} and types & {44, 46}
+    log = _run_pinned(net_r, _net(**spec), 1000, full_every=100)
+    assert len(log) > 0, "the case must release"
+    ora_net = _net(**spec)
+    ora = Oracle(ora_net, fp64=True)
+    ref = _fresh_reference(net_r2 := _net(**spec))
+    ora.run(300, DT)
+    ref.run(300, DT)
+    for j in range(3):
+        want = np.where(net_r2.synapses["pre_autoreceptor_count"] > j,
+                        net_r2.synapses["pre_autoreceptors"][:, j]["state"][:, 0], 0.0)
+        assert np.array_equal(ora.synapse_field("autoreceptor_state", j * 8), want), j
+    ora.close()
+
+
 def test_stimulus_uploads_bit_identical():
     """Every stimulus kind of GpuStimulusData, uploaded twice (the stimuli fixture's schedule)."""
     import golden_cases
