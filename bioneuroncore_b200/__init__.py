@@ -36,6 +36,7 @@ DROPIN_SYMBOLS = ["gpu_backend_create", "gpu_backend_create_on_device", "gpu_bac
                   "gpu_backend_ibuf_offset", "gpu_backend_vm_offset", "gpu_backend_seg_size"]
 NEW_SYMBOLS = ["bnc_netgen_aos", "bnc_netgen_free", "bnc_last_error", "bnc_load_aos", "bnc_load_generated",
                "bnc_run_ticks", "bnc_time_ticks", "bnc_sync_to_host", "bnc_records_managed", "bnc_set_records_residency",
+               "bnc_upload_mechano",
                "register_modifier_current", "register_modulator_release", "bnc_plugin_load",
                "bnc_plugin_load_directory", "bnc_plugin_registered", "bnc_plugin_count", "bnc_plugin_unregister_all",
                "bnc_read_segment_field",
@@ -153,7 +154,7 @@ def load_library(path=LIB_PATH):
         "bnc_last_error": ([], C.c_char_p), "bnc_load_aos": ([vp, vp, vp, u32], i32),
         "bnc_load_generated": ([vp, vp], i32), "bnc_run_ticks": ([vp, u32, f32], i32),
         "bnc_time_ticks": ([vp, u32, f32, vp], i32), "bnc_sync_to_host": ([vp], i32), "bnc_records_managed": ([vp], i32),
-        "bnc_set_records_residency": ([vp, i32], i32),
+        "bnc_set_records_residency": ([vp, i32], i32), "bnc_upload_mechano": ([vp, vp, u32], i32),
         "bnc_read_segment_field": ([vp, i32, i32, vp, u32], i32),
         "bnc_read_synapse_field": ([vp, i32, i32, vp, u32], i32),
         "bnc_set_synapse_scale": ([vp, vp, u32], i32), "bnc_network_info": ([vp, vp], i32),
@@ -290,6 +291,12 @@ class Backend:
         else:
             _check(self.lib.bnc_load_generated_opts(self.h, C.byref(params), C.byref(options)),
                    "bnc_load_generated_opts")
+
+    def upload_mechano(self, items):
+        """bnc_upload_mechano with (segment_id, mod_type, state_idx, value) tuples."""
+        from .abi import mechano_data
+        arr, n = mechano_data(items)
+        _check(self.lib.bnc_upload_mechano(self.h, arr, n), "bnc_upload_mechano")
 
     def upload_stimuli(self, data):
         """gpu_backend_upload_stimuli with a GpuStimulusData (abi.stimulus_data): replaces

@@ -89,6 +89,20 @@ class LigandInjection(C.Structure):
                 ("intracellular", C.c_uint8), ("_pad2", C.c_uint8 * 3)]
 
 
+class MechanoStimulus(C.Structure):
+    """types.h:645-655 (packed, 13 bytes)."""
+    _pack_ = 1
+    _fields_ = [("segment_id", C.c_uint32), ("mod_type", C.c_uint8), ("state_idx", C.c_int32), ("value", C.c_float)]
+
+
+def mechano_data(items):
+    """A ctypes array of MechanoStimulus from (segment_id, mod_type, state_idx, value)."""
+    arr = (MechanoStimulus * max(len(items), 1))()
+    for i, (sid, t, idx, v) in enumerate(items):
+        arr[i].segment_id, arr[i].mod_type, arr[i].state_idx, arr[i].value = sid, t, idx, v
+    return arr, len(items)
+
+
 class GpuStimulusData(C.Structure):
     """BncGpuStimulusData, the argument of gpu_backend_upload_stimuli (reference
     include/types.h:662-674): up to 256 entries of each stimulus kind."""

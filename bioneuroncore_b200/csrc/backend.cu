@@ -962,6 +962,63 @@ void gpu_backend_upload_stimuli(void* sim, const BncGpuStimulusData* src) {
     b->stim.lig_inj.clear();
 }
 
+int bnc_upload_mechano(void* sim, const BncMechanoStimulus* ms, uint32_t n) {
+    if (!sim || (n && !ms)) { set_error("null argument"); return BNC_ERR_ARG; }
+    Backend* b = static_cast<Backend*>(sim);
+    if (!b->loaded) { set_error("no network loaded"); return BNC_ERR_STATE; }
+    if (!b->members.empty()) { set_error("mechano stimuli address one network, not an ensemble"); return BNC_ERR_UNSUPPORTED; }
+    if (!b->owns_aos || !b->aos.segments) {
+        set_error("mechano stimuli need the network's records (load it from AoS arrays or a .bion)");
+        return BNC_ERR_UNSUPPORTED;
+    }
+    if (!n) return BNC_OK;
+    cudaSetDevice(b->device);
+    int rc = sync_stream(b);
+    if (rc != BNC_OK) return rc;
+    // each stimulus -> (record, slot), as simulation_host.cpp:213-228 searches them
+    struct Hit { uint32_t seg; uint8_t slot; int idx; float value; uint32_t item; };
+    std::vector<Hit> hits;
+    BncBionData& a = b->aos;
+    for (uint32_t m = 0; m < n; m++) {
+        BncMechanoStimulus st;
+        std::memcpy(&st, reinterpret_cast<const unsigned char*>(ms) + (size_t)m * sizeof(BncMechanoStimulus), sizeof(st));
+        for (uint32_t i = 0; i < a.num_segments; i++) {
+            if (a.segments[i].id != st.segment_id) continue;
+            const uint8_t mc = a.segments[i].modifier_count;
+            for (uint8_t j = 0; j < mc && j < BNC_MAX_MODIFIERS; j++)
+                if (a.segments[i].modifiers[j].type == st.mod_type) {
+                    if (st.state_idx >= 0 && st.state_idx < BNC_MAX_STATE) hits.push_back({i, j, st.state_idx, st.value, UINT32_MAX});
+                    break;
+                }
+            break;
+        }
+    }
+    if (hits.empty()) return BNC_OK;
+    // the items of those slots (a slot myelin blocks has none: only its record changes)
+    const NetHost& h = b->host;
+    parallel_for(h.item_seg.size(), [&](size_t q0, size_t q1) {
+        for (size_t q = q0; q < q1; q++)
+            for (Hit& x : hits)
+                if (h.item_seg[q] == x.seg && h.item_slot[q] == x.slot) x.item = (uint32_t)q;
+    });
+    const NetDev& d = b->dev;
+    for (const Hit& x : hits) {
+        a.segments[x.seg].modifiers[x.slot].state[x.idx] = (double)x.value;
+        if (x.item == UINT32_MAX || x.idx >= 7) continue;
+        cudaError_t e = cudaMemcpy(d.it_st + (size_t)x.idx * d.n_items + x.item, &x.value, 4, cudaMemcpyHostToDevice);
+        const uint8_t type = a.segments[x.seg].modifiers[x.slot].type;
+        if (e == cudaSuccess && x.value != 0.0f && ((param_mask(type) >> x.idx) & 1u)) {
+            // a parameter word now set: the item reads its parameters
+            uint16_t tf = 0;
+            e = cudaMemcpy(&tf, d.it_tf + x.item, 2, cudaMemcpyDeviceToHost);
+            tf = (uint16_t)(tf | (1u << 8));
+            if (e == cudaSuccess) e = cudaMemcpy(d.it_tf + x.item, &tf, 2, cudaMemcpyHostToDevice);
+        }
+        if (e != cudaSuccess) return cuda_fail(e, "mechano stimulus write");
+    }
+    return BNC_OK;
+}
+
 int gpu_backend_device_count(void) {
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess) return 0;

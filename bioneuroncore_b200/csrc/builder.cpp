@@ -136,7 +136,7 @@ uint8_t nt_from_receptor(uint8_t rt) {
     return 0;
 }
 // state indices that are parameters (read-only, default when 0) per type
-uint8_t param_mask(uint8_t t) {
+uint8_t param_words(uint8_t t) {
     switch (t) {
         case 1: return 0x1C;      // 2,3,4
         case 85: return 0x34;     // 2,4,5
@@ -183,6 +183,8 @@ struct UF {
 };
 
 }  // namespace
+
+uint8_t param_mask(uint8_t type) { return param_words(type); }
 
 int upload_stimuli(const Stimuli& stim, NetHost& host, NetDev* dev, DeviceAllocs* allocs) {
     int rc = BNC_OK;
@@ -1010,7 +1012,7 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
                 uint8_t slot = act_slot[kk.k];
                 const ModLite& m = hn.mod(orig, slot);
                 uint8_t fl = 0;
-                uint8_t pm = param_mask(m.type);
+                uint8_t pm = param_words(m.type);
                 for (int b = 0; b < 7; b++) if ((pm >> b) & 1) if (m.state[b] != 0.0f) fl |= 1;
                 if (receptor_supported(m.type) && m.active_vars > 0) {
                     if (m.active_vars >= 8) { bad.note(q); continue; }

@@ -301,6 +301,8 @@ int upload_stimuli(const Stimuli& stim, NetHost& host, NetDev* dev, DeviceAllocs
 int export_network(const NetDev& dev, const NetHost& host, uint64_t ticks_run, BncBionData* aos);
 // State words (bits) a built-in modifier type updates every tick; 0 for other types.
 uint8_t host_dyn_mask(uint8_t type);
+// State words (bits) a built-in type reads as parameters (its default when 0).
+uint8_t param_mask(uint8_t type);
 
 // Kernel launchers (tile.cu, synapse.cu).  prepare_tick does the per-device and
 // per-network set-up that must not happen inside a stream capture (constant tables,

@@ -290,6 +290,15 @@ typedef struct {
     BncLigandInjection lig_inj[BNC_GPU_MAX_STIMULI];
 } BncGpuStimulusData;
 
+/* Mechano stimulus (types.h:645-655): value written into state[state_idx] of the
+ * first modifier of type mod_type on the segment whose id is segment_id. */
+typedef struct {
+    uint32_t segment_id;
+    uint8_t mod_type;
+    int32_t state_idx;
+    float value;
+} BncMechanoStimulus;
+
 typedef struct {
     char name[128];
     uint32_t vendor_id;
@@ -325,6 +334,7 @@ BNC_STATIC_ASSERT(sizeof(BncSynapse) == 1568, synapse_size);
 BNC_STATIC_ASSERT(sizeof(BncIntraConnection) == 16, conn_size);
 BNC_STATIC_ASSERT(sizeof(BncNeuron) == 24, neuron_size);
 BNC_STATIC_ASSERT(sizeof(BncNetworkHeader) == 100, header_size);
+BNC_STATIC_ASSERT(sizeof(BncMechanoStimulus) == 13, mechano_size);
 BNC_STATIC_ASSERT(offsetof(BncSegment, V_m) == 40, seg_vm);
 BNC_STATIC_ASSERT(offsetof(BncSegment, intra_ions) == 48, seg_intra);
 BNC_STATIC_ASSERT(offsetof(BncSegment, extra_ions) == 112, seg_extra);

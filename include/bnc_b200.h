@@ -385,6 +385,18 @@ int bnc_plugin_count(void);
 /* Forgets every registration (the libraries stay loaded). */
 void bnc_plugin_unregister_all(void);
 
+/* Mechano stimuli: the mechano argument of the reference's core_run_tick
+ * (simulation_host.cpp:211-230), which the GPU backend's GpuStimulusData does not
+ * carry.  Each stimulus writes its value into state[state_idx] of the first modifier
+ * of type mod_type on the first segment whose id is segment_id, in the order given,
+ * before the next tick's modifier currents (one-shot).  A stimulus whose segment,
+ * type or index (0-7) does not exist does nothing; state[7] is the effective area,
+ * which every tick rewrites, so a write there reaches only the records.  Nothing
+ * reads modifier state between ticks, so the writes are made at once (device state
+ * and records).  Needs the network's records (a network loaded from AoS arrays or a
+ * .bion); BNC_ERR_UNSUPPORTED for generated networks and ensembles. */
+int bnc_upload_mechano(void* sim, const BncMechanoStimulus* stimuli, uint32_t n);
+
 /* Host-only: runs the builder's planning on AoS arrays in memory (validation,
  * supported-type checks, tiles, schedule) without a device.  Returns the same
  * codes a load of that network would. */

@@ -14,8 +14,8 @@
  * Supported subset (the loader rejects the rest with an error): modifier types
  * listed in bo_type_supported(), chemical synapses, pre-autoreceptors that are
  * bouton K/Na channels or release modulators, every stimulus kind of GpuStimulusData (current steps,
- * clamps, ramps, ion and ligand injections; bo_upload_stimuli), no mechano
- * stimuli, no consolidation/nuclei.
+ * clamps, ramps, ion and ligand injections; bo_upload_stimuli), mechano stimuli
+ * (bo_upload_mechano), no consolidation.
  */
 #include <math.h>
 #include <stdint.h>
@@ -64,6 +64,9 @@ typedef struct BoSim {
     uint32_t n_ion_inj;
     BncLigandInjection lig_inj[BNC_GPU_MAX_STIMULI];
     uint32_t n_lig_inj;
+    /* mechano stimuli for the next tick (simulation_host.cpp:211-230), one-shot */
+    BncMechanoStimulus* mech;
+    uint32_t n_mech;
     uint32_t* spike_count;  /* per segment, threshold -40 mV upward crossings */
     float nt_D[15];
     char err[256];
@@ -664,7 +667,7 @@ static double bo_receptor(uint8_t rtype, OMod* m, OSeg* post, float dt, float sc
     }
 }
 
-/* simulation_host.cpp:174-657 (steps 1, 2.5, 3, 4; no mechano, no consolidation) */
+/* simulation_host.cpp:174-657 (mechano stimuli, steps 1, 2.5, 3, 4; no consolidation) */
 static void bo_tick(BoSim* S, float dt) {
     uint64_t tick = S->tick++;
     OSeg* sg = S->seg;
@@ -686,6 +689,21 @@ static void bo_tick(BoSim* S, float dt) {
             if (!(tick >= S->ramp[r].end_tick)) S->ramp[w++] = S->ramp[r];
         S->n_ramp = w;
     }
+    /* mechano stimuli (:211-230): the value into state[state_idx] of the first modifier
+       of the type on the first segment with the id, in order, then cleared */
+    for (uint32_t m = 0; m < S->n_mech; m++) {
+        const BncMechanoStimulus* ms = &S->mech[m];
+        for (uint32_t i = 0; i < n; i++) {
+            if (sg[i].id != ms->segment_id) continue;
+            for (uint8_t j = 0; j < sg[i].nmod; j++)
+                if (sg[i].mods[j].type == ms->mod_type) {
+                    if (ms->state_idx >= 0 && ms->state_idx < 8) sg[i].mods[j].st[ms->state_idx] = BO_ST(ms->value);
+                    break;
+                }
+            break;
+        }
+    }
+    S->n_mech = 0;
     /* step 1 (:234-303) */
     for (uint32_t i = 0; i < n; i++) {
         OSeg* s = &sg[i];
@@ -993,6 +1011,14 @@ BoSim* bo_create(const BncBionData* d, const BncCurrentStimulus* stim, uint32_t 
 
 /* gpu_backend_upload_stimuli (gpu_backend_cuda.cu:242-248): every list is replaced by
    the uploaded one; the injections apply at the next tick, once. */
+/* The mechano argument of core_run_tick for the next tick (replaces any pending). */
+void bo_upload_mechano(BoSim* S, const BncMechanoStimulus* ms, uint32_t n) {
+    free(S->mech);
+    S->mech = n ? malloc((size_t)n * sizeof(BncMechanoStimulus)) : NULL;
+    if (n) memcpy(S->mech, ms, (size_t)n * sizeof(BncMechanoStimulus));
+    S->n_mech = n;
+}
+
 void bo_upload_stimuli(BoSim* S, const BncGpuStimulusData* src) {
     uint32_t nc = src->current_stim_count < BNC_GPU_MAX_STIMULI ? src->current_stim_count : BNC_GPU_MAX_STIMULI;
     free(S->stim);
@@ -1011,7 +1037,7 @@ void bo_upload_stimuli(BoSim* S, const BncGpuStimulusData* src) {
 
 void bo_destroy(BoSim* S) {
     if (!S) return;
-    free(S->seg); free(S->conn); free(S->syn); free(S->delay); free(S->stim); free(S->spike_count);
+    free(S->seg); free(S->conn); free(S->syn); free(S->delay); free(S->stim); free(S->spike_count); free(S->mech);
     free(S->grp); free(S->gdone); free(S->gmore);
     free(S->vd); free(S->vnd); free(S->offdd); free(S->rhsd); free(S->dend); free(S->phin);
     free(S);

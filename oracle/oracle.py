@@ -31,6 +31,7 @@ def oracle_lib():
         lib.bo_create.restype = vp
         lib.bo_destroy.argtypes = [vp]
         lib.bo_upload_stimuli.argtypes = [vp, vp]
+        lib.bo_upload_mechano.argtypes = [vp, vp, C.c_uint32]
         lib.bo_run.argtypes = [vp, C.c_uint32, C.c_float]
         lib.bo_set_diffusion_mode.argtypes = [vp, C.c_uint32, C.c_double, C.c_uint32]
         lib.bo_diffusion_stats.argtypes = [vp, vp, vp, C.c_int]
@@ -77,6 +78,7 @@ def oracle64_lib():
         lib.bo_create.restype = vp
         lib.bo_destroy.argtypes = [vp]
         lib.bo_upload_stimuli.argtypes = [vp, vp]
+        lib.bo_upload_mechano.argtypes = [vp, vp, C.c_uint32]
         lib.bo_run.argtypes = [vp, C.c_uint32, C.c_float]
         lib.bo_run_stride.argtypes = [vp, C.c_uint32, C.c_float, C.c_uint32]
         lib.bo_get_seg_field64.argtypes = [vp, C.c_int, C.c_int, vp]
@@ -152,6 +154,12 @@ class Oracle:
     def upload_stimuli(self, data):
         """bo_upload_stimuli with a GpuStimulusData: every list replaced, injections once."""
         self._lib().bo_upload_stimuli(self.h, C.byref(data))
+
+    def upload_mechano(self, items):
+        """bo_upload_mechano: (segment_id, mod_type, state_idx, value) for the next tick."""
+        from bioneuroncore_b200.abi import mechano_data
+        arr, n = mechano_data(items)
+        self._lib().bo_upload_mechano(self.h, arr, C.c_uint32(n))
 
     def run(self, ticks, dt, tick_stride=1):
         if tick_stride == 1:
@@ -241,6 +249,14 @@ class Reference:
         for a, c in zip(arrs, self._counts):
             self.rest += [C.addressof(a), C.cast(C.pointer(c), C.c_void_p)]
         self.rest += [None, None]
+
+    def upload_mechano(self, items):
+        """The mechano argument of the next core_run_tick call (simulation_host.cpp:211-230),
+        which applies the stimuli and sets the count to 0."""
+        from bioneuroncore_b200.abi import mechano_data
+        self._mech, n = mechano_data(items)
+        self._mech_n = C.c_uint32(n)
+        self.rest = list(self.rest[:8]) + [C.addressof(self._mech), C.cast(C.pointer(self._mech_n), C.c_void_p)]
 
     def run(self, ticks, dt, tick_stride=1):
         d = self.net.data

@@ -204,6 +204,54 @@ def test_release_modulators_bit_identical():
     ora.close()
 
 
+def mechano_schedule(net):
+    """Mechano stimuli at three ticks of the small family (tick -> (segment_id, mod_type,
+    state_idx, value) list): a gate (dynamic word), parameter words of Nav1.x and K2P,
+    the effective-area word 7, the Kv delayed rectifier of a myelinated axon segment
+    (myelin blocks it: kernel_dispatch.h:301-309, so its modifier never runs), and
+    stimuli that match nothing (absent type, index out of range, absent segment id);
+    two on one slot in one call, the later winning."""
+    seg = net.segments
+    types = seg["modifiers"]["type"]
+    cnt = seg["modifier_count"]
+
+    def first(t, pred=lambda i: True):
+        for i in range(len(seg)):
+            if pred(i) and t in types[i, :cnt[i]]:
+                return int(seg["id"][i])
+        raise AssertionError("no segment with type %d" % t)
+    myel = lambda i: 4 in types[i, :cnt[i]]                        # noqa: E731
+    nav = 141 if (types == 141).any() else 142
+    s_kv, s_k2p, s_nav = first(123), first(107), first(nav, lambda i: not myel(i))
+    s_blocked = first(123, myel)
+    return {
+        20: [(s_kv, 123, 0, 0.9), (s_nav, nav, 5, 4.0), (s_k2p, 107, 0, 3.5), (s_k2p, 107, 7, 123.0),
+             (s_blocked, 123, 0, 0.7), (s_kv, 200, 0, 1.0), (s_kv, 123, 9, 1.0), (10 ** 7, 123, 0, 1.0)],
+        60: [(s_kv, 123, 0, 0.2), (s_kv, 123, 0, 0.95), (s_nav, nav, 1, 0.1)],
+        61: [(s_k2p, 107, 1, 2.0)],
+    }
+
+
+def test_mechano_stimuli_bit_identical():
+    """Mechano stimuli, core_run_tick's own argument (simulation_host.cpp:211-230): one
+    shot, before the tick's modifier currents; every state word after each call and
+    200 ticks equal."""
+    from bioneuroncore_b200 import NET_SMALL
+    net_r, net_o = _net(NET_SMALL, 8, 7, stim_pA=3000.0), _net(NET_SMALL, 8, 7, stim_pA=3000.0)
+    sched = mechano_schedule(net_r)
+    ref = _fresh_reference(net_r)
+    ora = Oracle(net_o, fp64=True)
+    for t in range(200):
+        if t in sched:
+            ref.upload_mechano(sched[t])
+            ora.upload_mechano(sched[t])
+        ref.run(1, DT)
+        ora.run(1, DT)
+        if t in sched or t + 1 == 200:
+            _assert_same(net_r, ora)
+    ora.close()
+
+
 def test_stimulus_uploads_bit_identical():
     """Every stimulus kind of GpuStimulusData, uploaded twice (the stimuli fixture's schedule)."""
     import golden_cases
