@@ -169,15 +169,45 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def ncu_traffic(kernel):
-    """DRAM bytes per launch recorded in the committed ncu summary of `kernel`, if any."""
+def ncu_figure(kernel, key):
+    """A per-launch figure (`key: value` line) recorded in the committed ncu summary of
+    `kernel`, scaled to the full network, if any."""
     path = os.path.join(ROOT, "profiles", "%s_large_network.md" % kernel)
     try:
         with open(path) as f:
-            m = re.search(r"dram_bytes_per_launch_full_size:\s*([0-9.eE+]+)", f.read())
+            m = re.search(r"%s:\s*([0-9.eE+]+)" % key, f.read())
             return float(m.group(1)) if m else None
     except OSError:
         return None
+
+
+def ncu_traffic(kernel):
+    """DRAM bytes per launch recorded in the committed ncu summary of `kernel`, if any."""
+    return ncu_figure(kernel, "dram_bytes_per_launch_full_size")
+
+
+def issue_roofline(kernels, sm_mhz, n_gpus_neurons_scale=1.0):
+    """The bound these kernels hit: instruction issue.  Warp instructions per launch
+    (ncu, committed summaries, scaled to the full network) over the CUDA-event time,
+    against the issue peak of the GPU at the SM clock sampled in the timed region (one
+    warp instruction per cycle per scheduler, four schedulers per SM)."""
+    try:
+        import torch
+        sms = torch.cuda.get_device_properties(0).multi_processor_count
+    except Exception:
+        return None
+    if not sm_mhz:
+        return None
+    peak = sms * 4 * sm_mhz * 1e6
+    out = {"unit": "warp instructions/s", "peak": peak, "sms": sms, "sm_mhz": sm_mhz,
+           "peak_source": "4 schedulers x SMs x median SM clock in the timed region", "kernels": {}}
+    for k, ms in kernels.items():
+        w = ncu_figure(k, "warp_instructions_per_launch_full_size")
+        if w is None or not ms:
+            continue
+        w *= n_gpus_neurons_scale
+        out["kernels"][k] = {"warp_instructions": w, "achieved": w / (ms / 1000.0), "frac": w / (ms / 1000.0) / peak}
+    return out
 
 
 def cpu_reference_rate(neurons, ticks, warm, seed):
@@ -782,6 +812,9 @@ def main():
                 "kernels_frac": {k: v[1] / (v[0] / 1000.0) / 1e9 / peak for k, v in kernels.items()},
                 "tick_bytes": info.algo_bytes_per_tick,
                 "tick_frac": info.algo_bytes_per_tick / (ms_max / a.steps / 1000.0) / 1e9 / peak}
+    # the summaries' instruction counts are per launch of the 6.4M-segment network
+    roofline["issue"] = issue_roofline({k: v[0] for k, v in kernels.items()}, clk.get("sm_mhz"),
+                                       info.n_segments / 6.4e6)
 
     draw_order = None
     if not a.no_draw_order and rank == 0 and world == 1:
