@@ -73,6 +73,7 @@ def parse_args():
     ap.add_argument("--adj-neurons", type=int, default=256)
     ap.add_argument("--adj-sets", type=int, default=64)
     ap.add_argument("--adj-ticks", type=int, default=1024)
+    ap.add_argument("--adj-fitting-only", action="store_true", help="skip the whole-small-set adjoint run")
     return ap.parse_args()
 
 
@@ -541,6 +542,31 @@ def run_trees(a, device):
     }
 
 
+def run_adjoint_full_small_set(a, device, rng):
+    """The adjoint workload with the whole small set (Cav1.3 and the Na/K pump on every
+    segment, the pump's ATP diffusing): its cost ratio, beside the fitting family's."""
+    import numpy as np
+    from bioneuroncore_b200 import Adjoint, Backend, Network, NetgenParams, NET_ADJOINT, NETGEN_FULL_SMALL_SET
+    netf = Network(NetgenParams(family=NET_ADJOINT, n_neurons=a.adj_neurons, seed=a.seed, flags=NETGEN_FULL_SMALL_SET))
+    bf = Backend(device)
+    bf.load_network(netf)
+    adjf = Adjoint(bf, a.adj_sets, a.adj_ticks, DT, checkpoint_every=256)
+    adjf.record()
+    basef = adjf.get_params(0)
+    adjf.set_params(0, *[x * f for x, f in zip(basef, (1.15, 0.85, 1.25, 0.8))])
+    _, trf = adjf.forward(trace=True)
+    adjf.set_target(trf[0])
+    for p in range(a.adj_sets):
+        adjf.set_params(p, *[(x * np.exp(0.1 * rng.standard_normal(x.shape))).astype(np.float32) for x in basef])
+    adjf.forward()
+    adjf.backward()
+    ffwd, fbwd = adjf.timings()
+    adjf.close()
+    bf.close()
+    return {"forward_ms": ffwd, "backward_ms": fbwd, "backward_over_forward": fbwd / ffwd,
+            "note": "the same workload with Cav1.3 and the Na/K pump on every segment (BNC_NETGEN_FULL_SMALL_SET)"}
+
+
 def run_adjoint(a, device):
     """Adjoint fitting workload: a.adj_neurons neurons x 64 segments with 2,000 synapses
     per 256 neurons (the fitting family: Nav, Kv_DR, K2P leak, AMPA/GABA-A; also timed
@@ -573,27 +599,9 @@ def run_adjoint(a, device):
     adj.close()
     b.close()
     spec_ticks = 20000
-    # the same workload with the whole small set (Cav1.3 and the Na/K pump on every
-    # segment, the pump's ATP diffusing): its cost ratio, beside the fitting family's
-    from bioneuroncore_b200 import NETGEN_FULL_SMALL_SET
-    netf = Network(NetgenParams(family=NET_ADJOINT, n_neurons=a.adj_neurons, seed=a.seed, flags=NETGEN_FULL_SMALL_SET))
-    bf = Backend(device)
-    bf.load_network(netf)
-    adjf = Adjoint(bf, a.adj_sets, a.adj_ticks, DT, checkpoint_every=256)
-    adjf.record()
-    basef = adjf.get_params(0)
-    adjf.set_params(0, *[x * f for x, f in zip(basef, (1.15, 0.85, 1.25, 0.8))])
-    _, trf = adjf.forward(trace=True)
-    adjf.set_target(trf[0])
-    for p in range(a.adj_sets):
-        adjf.set_params(p, *[(x * np.exp(0.1 * rng.standard_normal(x.shape))).astype(np.float32) for x in basef])
-    adjf.forward()
-    adjf.backward()
-    ffwd, fbwd = adjf.timings()
-    adjf.close()
-    bf.close()
-    full = {"forward_ms": ffwd, "backward_ms": fbwd, "backward_over_forward": fbwd / ffwd,
-            "note": "the same workload with Cav1.3 and the Na/K pump on every segment (BNC_NETGEN_FULL_SMALL_SET)"}
+    full = None
+    if not a.adj_fitting_only:
+        full = run_adjoint_full_small_set(a, device, rng)
     cpu = None
     if not a.no_cpu_baseline:
         try:   # the reference's CPU tick on the same network: the forward pass of one set
@@ -733,6 +741,8 @@ def run_sweep(a, device):
         "seconds": wall, "tasks_per_s": a.sweep_tasks / wall, "segment_ticks_per_s": seg_ticks / wall,
         "timing": "wall clock of bnc_sweep_run: copies, build, tick loop, metrics",
         "spike_count_mean": float(np.mean([r.spike_count for r in res])),
+        "spike_count_note": "the reference's metric (core_compute_metrics, simulation_host.cpp:825-880): "
+                            "segments above -20 mV at the last tick, a snapshot, not the spikes of the run",
         "cpu_reference": cpu,
     }
 
