@@ -167,11 +167,12 @@ int export_network(const NetDev& d, const NetHost& h, uint64_t ticks_run, BncBio
                  oTxn = x_txn ? take(n) : 0;
     size_t oSt[7];
     for (int k = 0; k < 7; k++) oSt[k] = ((rows >> k) & 1u) ? take(NI) : 0;
-    size_t oSy[8] = {0}, oRc = 0, oMd = 0;
+    size_t oSy[8] = {0}, oRc = 0, oMd = 0, oEc = 0;
     if (K) {
         for (int f = 0; f < 8; f++) oSy[f] = take(K);
         oRc = take((size_t)3 * NR);
         oMd = take(d.n_md);
+        oEc = d.sy_cleft_ecb ? take(K) : 0;
     }
     const size_t bytes = off * sizeof(float) + K;
     std::lock_guard<std::mutex> lock(g_stage_mu);
@@ -198,6 +199,7 @@ int export_network(const NetDev& d, const NetHost& h, uint64_t ticks_run, BncBio
         for (int f = 0; f < 8; f++) get(oSy[f], src[f], (size_t)K * 4);
         get(oRc, d.rc_st, (size_t)3 * NR * 4);
         get(oMd, d.md_st, (size_t)d.n_md * 4);
+        if (d.sy_cleft_ecb) get(oEc, d.sy_cleft_ecb, (size_t)K * 4);
         if (ok) ok = cudaMemcpy(refr, d.sy_refr, K, cudaMemcpyDeviceToHost) == cudaSuccess;
     }
     if (!ok) { set_error("export: device read failed"); return BNC_ERR_CUDA; }
@@ -239,6 +241,7 @@ int export_network(const NetDev& d, const NetHost& h, uint64_t ticks_run, BncBio
                 y.spine_calcineurin = F[oSy[3] + q]; y.facilitation = F[oSy[4] + q]; y.weight = F[oSy[5] + q];
                 y.cleft_neurotransmitter[h.syn_nt[q]] = F[oSy[6] + q];
                 y.RRP = F[oSy[7] + q]; y.refractory = refr[q];
+                if (d.sy_cleft_ecb) y.cleft_neurotransmitter[9] = F[oEc + q];
                 if (ticks_run > 0) y.depression = F[oSy[4] + q] + 0.01f;
             }
         });
@@ -466,6 +469,7 @@ __global__ void k_export_synapses(NetDev d, const uint32_t* syn_orig, const uint
         put<float>(y, offsetof(BncSynapse, weight), d.sy_weight[q]);
         put<float>(y, offsetof(BncSynapse, cleft_neurotransmitter) + 4 * (size_t)syn_nt[q], d.sy_cleft[q]);
         put<float>(y, offsetof(BncSynapse, RRP), d.sy_rrp[q]);
+        if (d.sy_cleft_ecb) put<float>(y, offsetof(BncSynapse, cleft_neurotransmitter) + 4 * 9, d.sy_cleft_ecb[q]);
         y[offsetof(BncSynapse, refractory)] = d.sy_refr[q];
         if (after_tick) put<float>(y, offsetof(BncSynapse, depression), d.sy_facil[q] + 0.01f);
     }
@@ -1505,6 +1509,11 @@ int bnc_read_synapse_field(void* sim, int field, int index, float* out, uint32_t
             return BNC_OK;
         }
         case 4: {
+            if (index == 9 && d.sy_cleft_ecb) {   // the endocannabinoid entry
+                if (!d2h(v, d.sy_cleft_ecb, K)) return cuda_fail(cudaGetLastError(), "read");
+                for (uint32_t q = 0; q < K; q++) out[b->host.syn_orig[q]] = v[q];
+                return BNC_OK;
+            }
             if (!d2h(v, d.sy_cleft, K)) return cuda_fail(cudaGetLastError(), "read");
             for (uint32_t q = 0; q < K; q++) out[b->host.syn_orig[q]] = (b->host.syn_nt[q] == index) ? v[q] : 0.0f;
             return BNC_OK;

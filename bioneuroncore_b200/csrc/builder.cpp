@@ -84,7 +84,7 @@ bool type_supported(uint8_t t) {
     switch (t) {
         case 1: case 4: case 7: case 8: case 9: case 11: case 12: case 85: case 98: case 99:
         case 100: case 102: case 103: case 104: case 105: case 106: case 107: case 112:
-        case 123: case 129: case 133: case 140: case 141: case 142: case 150: case 200:
+        case 123: case 129: case 133: case 140: case 141: case 142: case 150: case 200: case 86:
             return true;
         default: return false;
     }
@@ -155,6 +155,7 @@ uint8_t param_words(uint8_t t) {
         case 141: case 142: return 0x20;  // 5
         case 150: return 0x20;    // 5
         case 200: return 0x7C;    // 2..6
+        case 86: return 0x06;     // 1,2
         default: return 0;
     }
 }
@@ -1143,7 +1144,7 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
             }
         uint8_t ntt = y.post_receptor_count > 0 ? nt_from_receptor(hn.post_rec(k, 0).type) : 0;
         for (int q = 0; q < 15; q++)
-            if (q != ntt && y.cleft_neurotransmitter[q] != 0.0f) {
+            if (q != ntt && q != 9 && y.cleft_neurotransmitter[q] != 0.0f) {   // 9: endocannabinoid
                 if (report) set_error("synapse %u: cleft holds neurotransmitter %d other than the one it releases", k, q);
                 return BNC_ERR_UNSUPPORTED;
             }
@@ -1311,6 +1312,26 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
         });
         if (bad.any()) return fill_syn((uint32_t)bad.at.load(), true);
     }
+    // endocannabinoid retrograde signalling (simulation_host.cpp:578-589): each post
+    // segment's first eCB-synthesis modifier (its item) and each synapse's eCB cleft entry
+    std::vector<uint32_t> seg_ecb_item;
+    std::vector<float> sy_cleft_ecb;
+    {
+        bool any_ecb = false;
+        std::vector<uint8_t> best_slot;
+        for (uint32_t q = 0; q < NI; q++) {
+            if ((uint8_t)(it_tf[q] & 0xFFu) != 86) continue;
+            if (!any_ecb) { any_ecb = true; seg_ecb_item.assign(n, UINT32_MAX); best_slot.assign(n, 0xFF); }
+            const uint32_t dseg = host->inv[host->item_seg[q]];
+            if (host->item_slot[q] < best_slot[dseg]) { best_slot[dseg] = host->item_slot[q]; seg_ecb_item[dseg] = q; }
+        }
+        for (uint32_t q = 0; q < K && !any_ecb; q++)
+            if (hn.syn[syn_valid[q]].cleft_neurotransmitter[9] != 0.0f) any_ecb = true;
+        if (any_ecb) {
+            sy_cleft_ecb.resize(K);
+            for (uint32_t q = 0; q < K; q++) sy_cleft_ecb[q] = hn.syn[syn_valid[q]].cleft_neurotransmitter[9];
+        }
+    }
     // release modulators of the autoreceptors, per sliced synapse in autoreceptor order
     std::vector<uint32_t> md_off;
     std::vector<uint8_t> md_code;
@@ -1460,7 +1481,7 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
     dev->flags = flags;
     bool any_nmda = false;
     for (uint32_t i = 0; i < n; i++) if (sflags[i] & SF_NMDA) any_nmda = true;
-    dev->nt_used_mask = nt_mask | (any_nmda ? 1u : 0u);
+    dev->nt_used_mask = nt_mask | (any_nmda ? 1u : 0u) | (sy_cleft_ecb.empty() ? 0u : 1u << 9);
     if (allocs) {
         dev->V = up(allocs, V, &rc);
         dev->ion_in = up(allocs, ion_in, &rc);
@@ -1542,6 +1563,10 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
         dev->rc_av = up(allocs, rc_av, &rc);
         dev->rc_den = up(allocs, rc_den, &rc);
         dev->rc_st = up(allocs, rc_st, &rc);
+        if (!sy_cleft_ecb.empty()) {
+            dev->sy_cleft_ecb = up(allocs, sy_cleft_ecb, &rc);
+            if (!seg_ecb_item.empty()) dev->seg_ecb_item = up(allocs, seg_ecb_item, &rc);
+        }
         if (!md_off.empty()) {
             dev->md_off = up(allocs, md_off, &rc);
             dev->md_code = up(allocs, md_code, &rc);

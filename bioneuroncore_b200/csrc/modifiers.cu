@@ -120,6 +120,7 @@ __device__ __forceinline__ double run_item(uint8_t type, DMod& m, SegRec* r, flo
         BNC_ITEM(142, dp_nav_current<kDef>(m, s, dt, 1))
         BNC_ITEM(150, dp_kv31_current<kDef>(m, s, dt))
         BNC_ITEM(200, dp_cav31_current<kDef>(m, s, dt))
+        BNC_ITEM(86, dp_ecb_synthesis_current<kDef>(m, s, dt))
 #undef BNC_ITEM
         default: break;
     }
@@ -201,6 +202,7 @@ __device__ __forceinline__ double run_item_s(uint8_t type, DMod& m, DSeg& s, flo
         BNC_ITEM(142, dp_nav_current<kDef>(m, s, dt, 1))
         BNC_ITEM(150, dp_kv31_current<kDef>(m, s, dt))
         BNC_ITEM(200, dp_cav31_current<kDef>(m, s, dt))
+        BNC_ITEM(86, dp_ecb_synthesis_current<kDef>(m, s, dt))
 #undef BNC_ITEM
         default: break;
     }
@@ -279,6 +281,7 @@ static void fill_mask_tables(uint8_t* dyn, uint8_t* par) {
     std::fill(par, par + 256, (uint8_t)0);
     dyn[1] = 0x03; par[1] = 0x1C;
     dyn[8] = 0x03; dyn[9] = 0x05; dyn[11] = 0x03; dyn[12] = 0x03;
+    dyn[86] = 0x01; par[86] = 0x06;
     dyn[85] = 0x0B; par[85] = 0x34;
     par[98] = 0x06; par[100] = 0x06;
     dyn[102] = 0x02; par[102] = 0x1D;

@@ -167,6 +167,11 @@ struct NetDev {
     // Release modulators among the presynaptic autoreceptors (md_off null when the
     // network has none): those of sliced synapse k are [md_off[k], md_off[k + 1]), in
     // autoreceptor order.
+    // Endocannabinoid signalling (null when the network has none): each synapse's eCB
+    // cleft entry, and per device segment the item of its first eCB-synthesis modifier
+    // (UINT32_MAX: none)
+    float* sy_cleft_ecb;      // [n_syn]
+    uint32_t* seg_ecb_item;   // [n_seg] (null when no segment has one)
     uint32_t* md_off;         // [n_syn + 1]
     uint8_t* md_code;         // kind << 4 | cleft NT index; kind 1 Gi/o, 2 Gs, 3 ionotropic
     double* md_scale;         // density x effective area (pre_area, or 1 when not positive)

@@ -207,6 +207,11 @@ int generate_network(const BncNetgenParams& p, NetSink& sink, NetShape* shape_ou
                 if (axon && (axon_idx & 1u)) set_mod(seg.modifiers[mc++], BNC_MOD_MYELIN, 1.0);
             }
             if (axon) set_mod(seg.modifiers[mc++], BNC_MOD_CAV21, 100.0 * scale_of(p, 3));
+            if ((p.flags & BNC_NETGEN_ECB) && !axon && mc < BNC_MAX_MODIFIERS) {
+                set_mod(seg.modifiers[mc], 86, 1.0);   // eCB synthesis
+                seg.modifiers[mc].state[0] = (double)0.5f;
+                mc++;
+            }
             seg.modifier_count = (uint8_t)mc;
             // intra_connection_ids: the connections touching this segment (the reference
             // loader fills the same list, bion_loader_host.cpp:410-425)
@@ -292,6 +297,11 @@ int generate_network(const BncNetgenParams& p, NetSink& sink, NetShape* shape_ou
                     sy.pre_autoreceptor_count = 1;
                 }
                 if (rng_extra.u01() < 0.3) sy.delay = (float)(0.5 + 1.5 * rng_extra.u01());
+            }
+            if ((p.flags & BNC_NETGEN_ECB) && rng_modul.u01() < 0.5 &&
+                sy.pre_autoreceptor_count < BNC_MAX_PRE_AUTORECEPTORS) {
+                BncModifier& m = sy.pre_autoreceptors[sy.pre_autoreceptor_count++];
+                set_mod(m, 36, (double)(float)(0.5 + 0.5 * rng_modul.u01()));   // CB1
             }
             if (p.flags & BNC_NETGEN_RELEASE_MODULATORS) {
                 static const uint8_t kModulators[12] = {18, 19, 22, 27, 29, 30, 35, 36, 38, 44, 46, 13};

@@ -997,6 +997,24 @@ __device__ __forceinline__ double dp_glycine_current(DMod& m, DSeg& s, float dt,
     return dp_ionotropic<kDef>(m, s, dt, nt, 60.0f, 0.5f, 0.3f, 5.0f, 0.0f, 0.0f, 0.0f, 1, 2000.0f, 0.0f, scale);
 }
 
+/* hh_biological.cpp:1746-1767 (eCB synthesis: 2-AG from Ca2+; segment_dag is 0, as no
+ * supported network carries the PLC/IP3/DAG modifier).  No current; the retrograde
+ * release into the clefts runs in the synapse kernel. */
+template <bool kDef>
+__device__ __forceinline__ double dp_ecb_synthesis_current(DMod& m, DSeg& s, float dt) {
+    float Ca = (float)((double)s.in[2] * (double)MM_TO_UM);
+    double synth_rate = ((kDef ? 0.0 : ((double)m.st[1])) > 0.0f) ? (kDef ? 0.0 : ((double)m.st[1])) : (double)0.01f;
+    double degrad_rate = ((kDef ? 0.0 : ((double)m.st[2])) > 0.0f) ? (kDef ? 0.0 : ((double)m.st[2])) : (double)0.005f;
+    float dag = 0.0f;
+    dt = (float)((double)dt * (double)m.den);
+    float Ca_n = Ca * Ca;
+    float synth = (float)(synth_rate * (double)Ca_n / (double)(Ca_n + 0.25f + 1e-9f) * (double)(1.0f + dag));
+    m.st[0] = (float)((double)m.st[0] + ((double)synth - (double)m.st[0] * degrad_rate) * (double)dt);
+    if (m.st[0] < 0.0f) m.st[0] = 0.0f;
+    if (m.st[0] > 10.0f) m.st[0] = 10.0f;
+    return 0.0;
+}
+
 /* kernel_dispatch.h:337-570 restricted to the supported types; 0 for unknown types
  * (the oracle's loader rejects them, so this branch is never taken). */
 template <bool kDef>
@@ -1029,6 +1047,7 @@ __device__ __forceinline__ double dp_dispatch_t(uint8_t type, DMod& m, DSeg& s, 
         case 142: return dp_nav_current<kDef>(m, s, dt, 1);
         case 150: return dp_kv31_current<kDef>(m, s, dt);
         case 200: return dp_cav31_current<kDef>(m, s, dt);
+        case 86: return dp_ecb_synthesis_current<kDef>(m, s, dt);
         default: return 0.0f;
     }
 }

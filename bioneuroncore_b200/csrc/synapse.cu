@@ -53,7 +53,11 @@ k_synapse(NetDev d, float dt, unsigned long long tick, int first_tick) {
     const bool syn_on = (d.flags & NF_SYNAPSES) != 0;
     // the neurotransmitters a synapse can deliver: glutamate, GABA, glycine (0, 1, 7)
     float nt_glu = (sfl & SF_NMDA) ? 1.0f : 0.0f;   // bath NMDA (simulation_host.cpp:337-340)
-    float nt_gaba = 0.0f, nt_gly = 0.0f;
+    float nt_gaba = 0.0f, nt_gly = 0.0f, nt_ecb = 0.0f;
+    // the segment's eCB-synthesis modifier (its first), whose state[0] each of its
+    // synapses draws on in order (simulation_host.cpp:578-589)
+    const uint32_t ecb_q = (valid && d.seg_ecb_item) ? d.seg_ecb_item[i] : UINT32_MAX;
+    float ecb_st = ecb_q != UINT32_MAX ? d.it_st[ecb_q] : 0.0f;
     double ib = valid ? d.ibuf[i] : 0.0;
     DSeg s;
     s.V = valid ? d.V[i] : 0.0f;
@@ -80,7 +84,7 @@ k_synapse(NetDev d, float dt, unsigned long long tick, int first_tick) {
         const bool act = cnt > kk;
         const uint32_t n_act = __popc(__ballot_sync(0xFFFFFFFFu, act));
         const uint32_t k = base + lane;   // this lane's synapse in the slice (when act)
-        float cleft = 0.0f, rrp = 0.0f, rrp_max = 0.0f, bouton = 0.0f;
+        float cleft = 0.0f, cleft_e = 0.0f, rrp = 0.0f, rrp_max = 0.0f, bouton = 0.0f;
         uint8_t refr = 0, sf = 0;
         int ntt = 0;
         uint32_t n_rc = 0;
@@ -90,6 +94,7 @@ k_synapse(NetDev d, float dt, unsigned long long tick, int first_tick) {
             sf = d.sy_flags[k];
             ntt = sf >> 4;
             cleft = d.sy_cleft[k];
+            if (d.sy_cleft_ecb) cleft_e = d.sy_cleft_ecb[k];
             const float delay = d.sy_delay[k];
             // delayed releases (delay_buffer.h:31-44)
             if ((d.flags & NF_DELAY) && delay > 0.0f) {
@@ -159,7 +164,8 @@ k_synapse(NetDev d, float dt, unsigned long long tick, int first_tick) {
                     for (uint32_t mi = d.md_off[k]; mi < m1; mi++) {
                         const uint32_t code = d.md_code[mi];
                         const uint32_t kind = code >> 4;
-                        const float c = ((int)(code & 15u) == ntt) ? cleft : 0.0f;
+                        const int mnt = (int)(code & 15u);
+                        const float c = mnt == ntt ? cleft : (mnt == 9 ? cleft_e : 0.0f);
                         const float activation = c / (c + 0.5f);
                         const double scale = d.md_scale[mi];
                         float f;
@@ -211,6 +217,7 @@ k_synapse(NetDev d, float dt, unsigned long long tick, int first_tick) {
             if (ntt == 0) nt_glu += cleft;
             else if (ntt == 1) nt_gaba += cleft;
             else nt_gly += cleft;
+            nt_ecb += cleft_e;
             n_rc = d.rc_cnt[k];
         }
         // receptors (simulation_host.cpp:490-500), j-th receptors of the slice side by side
@@ -253,8 +260,11 @@ k_synapse(NetDev d, float dt, unsigned long long tick, int first_tick) {
                 if (spine < 0.0f) spine = 0.0f;
             }
             // clearance (simulation_host.cpp:505-510)
-            cleft *= dm_exp(-dt / d.sy_tauc[k]);
+            const auto clear_f = dm_exp(-dt / d.sy_tauc[k]);
+            cleft *= clear_f;
             if (cleft < 0.0f) cleft = 0.0f;
+            cleft_e *= clear_f;
+            if (cleft_e < 0.0f) cleft_e = 0.0f;
             // BCM threshold, spine CaMKII/calcineurin, weight (simulation_host.cpp:527-576)
             float facil = d.sy_facil[k];
             {
@@ -290,8 +300,17 @@ k_synapse(NetDev d, float dt, unsigned long long tick, int first_tick) {
                 if (weight < 0.01f) weight = 0.01f;
                 if (weight > 10.0f) weight = 10.0f;
             }
+            // eCB retrograde release (simulation_host.cpp:578-589)
+            if (ecb_q != UINT32_MAX) {
+                const float ecb = ecb_st;
+                if (ecb > 0.0f) {
+                    cleft_e += ecb * 0.1f * dt;
+                    ecb_st = (float)((double)ecb_st * (double)0.9f);
+                }
+            }
             if (refr > 0) refr--;
             d.sy_cleft[k] = cleft;
+            if (d.sy_cleft_ecb) d.sy_cleft_ecb[k] = cleft_e;
             d.sy_refr[k] = refr;
             d.sy_bouton[k] = bouton;
             d.sy_spine[k] = spine;
@@ -303,6 +322,7 @@ k_synapse(NetDev d, float dt, unsigned long long tick, int first_tick) {
         }
         base += n_act;
     }
+    if (ecb_q != UINT32_MAX) d.it_st[ecb_q] = ecb_st;
     if (!valid) return;
     // step 4: membrane update (simulation_host.cpp:596-649)
     float V = s.V;
@@ -335,7 +355,7 @@ k_synapse(NetDev d, float dt, unsigned long long tick, int first_tick) {
 #pragma unroll
         for (int q = 0; q < 15; q++)
             if ((mask >> q) & 1u)
-                d.nt[(size_t)q * N + i] = q == 0 ? nt_glu : (q == 1 ? nt_gaba : (q == 7 ? nt_gly : 0.0f));
+                d.nt[(size_t)q * N + i] = q == 0 ? nt_glu : (q == 1 ? nt_gaba : (q == 7 ? nt_gly : (q == 9 ? nt_ecb : 0.0f)));
     } else if (sfl & SF_NMDA) {
         d.nt[i] = 1.0f;
     }

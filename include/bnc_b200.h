@@ -141,6 +141,10 @@ typedef struct {
  * alpha2, CB1, H3, nicotinic), density 0.2-1, state[0] 0-0.5, after any bouton
  * channel (drawn from a stream of their own: other draws are unchanged). */
 #define BNC_NETGEN_RELEASE_MODULATORS 256u
+/* Endocannabinoid retrograde signalling: an eCB-synthesis modifier (86, density 1,
+ * state[0] 0.5) on every soma and dendrite segment, and a CB1 release modulator on
+ * about half the synapses (from the release-modulator stream). */
+#define BNC_NETGEN_ECB 512u
 
 /* Generates a network into host AoS arrays in the reference layout.  The arrays
  * are owned by the library; release with bnc_netgen_free.  *stim receives the

@@ -872,6 +872,17 @@ static void bo_tick(BoSim* S, float dt) {
         if (syn->depr != syn->depr) syn->depr = 0.01f;
         if (syn->weight < 0.01f) syn->weight = 0.01f;
         if (syn->weight > 10.0f) syn->weight = 10.0f;
+        /* eCB retrograde signalling (:578-589): the post segment's first eCB-synthesis
+           modifier puts 2-AG into this cleft and loses a tenth of it */
+        for (uint8_t j = 0; j < post->nmod; j++) {
+            if (post->mods[j].type != 86) continue;
+            float ecb = (float)post->mods[j].st[0];
+            if (ecb > 0.0f) {
+                syn->cleft[9] += ecb * 0.1f * dt;
+                post->mods[j].st[0] = BO_ST((double)post->mods[j].st[0] * (double)0.9f);
+            }
+            break;
+        }
         if (syn->refractory > 0) syn->refractory--;
     }
     /* step 4 (:596-649) */

@@ -684,6 +684,23 @@ static double bo_glycine_current(OMod* m, OSeg* s, float dt, float scale) {
 
 /* kernel_dispatch.h:337-570 restricted to the supported types; 0 for unknown types
  * (the oracle's loader rejects them, so this branch is never taken). */
+/* hh_biological.cpp:1746-1767 (eCB synthesis, 2-AG from Ca2+ and DAG).  segment_dag
+ * (modifier_helpers.h:1496-1500) reads a PLC/IP3/DAG modifier, which no supported
+ * network carries, so DAG is 0 here. */
+static double bo_ecb_synthesis_current(OMod* m, OSeg* s, float dt) {
+    float Ca = (float)((double)s->in[2] * (double)MM_TO_UM);
+    double synth_rate = (m->st[1] > 0.0f) ? (double)m->st[1] : (double)0.01f;
+    double degrad_rate = (m->st[2] > 0.0f) ? (double)m->st[2] : (double)0.005f;
+    float dag = 0.0f;
+    dt = (float)((double)dt * (double)m->density);
+    float Ca_n = Ca * Ca;
+    float synth = (float)(synth_rate * (double)Ca_n / (double)(Ca_n + 0.25f + 1e-9f) * (double)(1.0f + dag));
+    m->st[0] = BO_ST((double)m->st[0] + ((double)synth - (double)m->st[0] * degrad_rate) * (double)dt);
+    if (m->st[0] < 0.0f) m->st[0] = 0.0f;
+    if (m->st[0] > 10.0f) m->st[0] = 10.0f;
+    return 0.0;
+}
+
 static double bo_dispatch(uint8_t type, OMod* m, OSeg* s, float dt) {
     switch (type) {
         case 1: return bo_cav13_current(m, s, dt);
@@ -712,6 +729,7 @@ static double bo_dispatch(uint8_t type, OMod* m, OSeg* s, float dt) {
         case 142: return bo_nav_current(m, s, dt, 1);
         case 150: return bo_kv31_current(m, s, dt);
         case 200: return bo_cav31_current(m, s, dt);
+        case 86: return bo_ecb_synthesis_current(m, s, dt);
         default: return 0.0f;
     }
 }
@@ -720,7 +738,7 @@ static int bo_type_supported(uint8_t t) {
     switch (t) {
         case 1: case 4: case 7: case 8: case 9: case 11: case 12: case 85: case 98: case 99:
         case 100: case 102: case 103: case 104: case 105: case 106: case 107: case 112:
-        case 123: case 129: case 133: case 140: case 141: case 142: case 150: case 200:
+        case 123: case 129: case 133: case 140: case 141: case 142: case 150: case 200: case 86:
             return 1;
         default: return 0;
     }

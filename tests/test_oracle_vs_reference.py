@@ -204,6 +204,20 @@ def test_release_modulators_bit_identical():
     ora.close()
 
 
+def test_endocannabinoid_signalling_bit_identical():
+    """eCB synthesis on the post segments (hh_biological.cpp:1746-1767), its retrograde
+    release into each cleft with the modifier's decay per synapse
+    (simulation_host.cpp:578-589), and CB1 autoreceptors reading it: 1,000 ticks with
+    releases, every state word and release decision equal."""
+    from bioneuroncore_b200 import NET_SMALL, NETGEN_SYNAPSE_EXTRAS, NETGEN_ECB
+    spec = dict(family=NET_SMALL, n=16, seed=6, flags=NETGEN_SYNAPSE_EXTRAS | NETGEN_ECB, stim_pA=3000.0)
+    net_r = _net(**spec)
+    assert (net_r.segments["modifiers"]["type"] == 86).any()
+    log = _run_pinned(net_r, _net(**spec), 1000, full_every=100)
+    assert len(log) > 0
+    assert (net_r.synapses["cleft_neurotransmitter"][:, 9] > 0).any(), "eCB must reach the clefts"
+
+
 def mechano_schedule(net):
     """Mechano stimuli at three ticks of the small family (tick -> (segment_id, mod_type,
     state_idx, value) list): a gate (dynamic word), parameter words of Nav1.x and K2P,
