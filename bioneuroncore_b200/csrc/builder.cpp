@@ -84,7 +84,7 @@ bool type_supported(uint8_t t) {
     switch (t) {
         case 1: case 4: case 7: case 8: case 9: case 11: case 12: case 85: case 98: case 99:
         case 100: case 102: case 103: case 104: case 105: case 106: case 107: case 112:
-        case 123: case 129: case 133: case 140: case 141: case 142: case 150: case 200: case 86:
+        case 123: case 129: case 133: case 140: case 141: case 142: case 150: case 200: case 86: case 147:
             return true;
         default: return false;
     }
@@ -308,6 +308,7 @@ void hostnet_add_segment(HostNet& hn, const BncSegment& s) {
     if (s.modifier_count > BNC_MAX_MODIFIERS && hn.bad_modifier_count_seg == UINT32_MAX)
         hn.bad_modifier_count_seg = (uint32_t)hn.seg.size();
     L.radius = s.radius; L.length = s.length;
+    L.pos_z = s.position.z;
     L.V_m = (float)s.V_m;
     for (int q = 0; q < 7; q++) { L.intra_ions[q] = (float)s.intra_ions[q]; L.extra_ions[q] = (float)s.extra_ions[q]; }
     for (int q = 0; q < 15; q++) { L.intra_nt[q] = s.intra_nt[q]; L.neurotransmitter[q] = s.neurotransmitter[q]; }
@@ -1332,6 +1333,50 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
             for (uint32_t q = 0; q < K; q++) sy_cleft_ecb[q] = hn.syn[syn_valid[q]].cleft_neurotransmitter[9];
         }
     }
+    // glia (simulation_host.cpp:351-355, 467-487): the first 256 segments with a GLAST
+    // transporter; each synapse gives its capture to the one nearest its post segment in z
+    std::vector<uint32_t> gl_seg, gl_off, gl_syn;
+    if (K) {
+        std::vector<uint32_t> glia;
+        for (uint32_t i = 0; i < n && glia.size() < 256; i++)
+            for (uint8_t j = 0; j < hn.seg[i].modifier_count; j++)
+                if (hn.mod(i, j).type == 147) { glia.push_back(i); break; }
+        if (!glia.empty()) {
+            std::vector<int32_t> near(n, -1);
+            for (uint32_t g : glia) near[g] = -2;
+            for (uint32_t q = 0; q < K; q++)
+                if (near[hn.syn[syn_valid[q]].post_segment] == -2) {
+                    // its own synapses' transmitter and the captures would interleave
+                    set_error("synapse %u targets glial segment %u (a segment with a GLAST transporter)",
+                              syn_valid[q], hn.syn[syn_valid[q]].post_segment);
+                    return BNC_ERR_UNSUPPORTED;
+                }
+            std::vector<uint32_t> order(K);
+            std::iota(order.begin(), order.end(), 0u);
+            std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return syn_valid[a] < syn_valid[b]; });
+            std::vector<uint32_t> of(K);
+            gl_off.assign(glia.size() + 1, 0);
+            for (uint32_t q = 0; q < K; q++) {
+                const uint32_t post = hn.syn[syn_valid[q]].post_segment;
+                if (near[post] < 0) {
+                    float best_dz = 1e30f;
+                    int32_t best = 0;
+                    for (uint32_t gi = 0; gi < glia.size(); gi++) {
+                        const float dz = std::fabs(hn.seg[glia[gi]].pos_z - hn.seg[post].pos_z);
+                        if (dz < best_dz) { best_dz = dz; best = (int32_t)gi; }
+                    }
+                    near[post] = best;
+                }
+                of[q] = (uint32_t)near[post];
+                gl_off[of[q] + 1]++;
+            }
+            for (size_t gi = 0; gi < glia.size(); gi++) gl_off[gi + 1] += gl_off[gi];
+            gl_syn.resize(K);
+            std::vector<uint32_t> pos(gl_off.begin(), gl_off.end() - 1);
+            for (uint32_t q : order) gl_syn[pos[of[q]]++] = q;   // original synapse order per glial segment
+            for (uint32_t g : glia) gl_seg.push_back(host->inv[g]);
+        }
+    }
     // release modulators of the autoreceptors, per sliced synapse in autoreceptor order
     std::vector<uint32_t> md_off;
     std::vector<uint8_t> md_code;
@@ -1563,6 +1608,13 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
         dev->rc_av = up(allocs, rc_av, &rc);
         dev->rc_den = up(allocs, rc_den, &rc);
         dev->rc_st = up(allocs, rc_st, &rc);
+        if (!gl_seg.empty()) {
+            dev->gl_cap = zeros<float>(allocs, K, &rc);
+            dev->gl_seg = up(allocs, gl_seg, &rc);
+            dev->gl_off = up(allocs, gl_off, &rc);
+            dev->gl_syn = up(allocs, gl_syn, &rc);
+            dev->n_glia = (uint32_t)gl_seg.size();
+        }
         if (!sy_cleft_ecb.empty()) {
             dev->sy_cleft_ecb = up(allocs, sy_cleft_ecb, &rc);
             if (!seg_ecb_item.empty()) dev->seg_ecb_item = up(allocs, seg_ecb_item, &rc);

@@ -24,6 +24,7 @@ struct SegLite {
     uint8_t segment_type;
     uint8_t modifier_count;
     float radius, length;
+    float pos_z;   // position.z (glial capture picks the nearest glial segment in z)
     float V_m;
     float intra_ions[7], extra_ions[7];
     float intra_nt[15], neurotransmitter[15];

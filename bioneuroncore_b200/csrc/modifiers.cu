@@ -81,7 +81,7 @@ __device__ __forceinline__ void rec_store(const DSeg& s, float v0, SegRec* r) {
 // rejects every other type; myelin, type 4, is never an item: it returns 0 and
 // touches nothing).
 template <bool kDef>
-__device__ __forceinline__ double run_item(uint8_t type, DMod& m, SegRec* r, float dt, float glu, float gaba,
+__device__ __forceinline__ double run_item(uint8_t type, DMod& m, SegRec* r, float dt, float& glu, float gaba,
                                            float gly) {
     double I = 0.0;
     switch (type) {
@@ -121,6 +121,7 @@ __device__ __forceinline__ double run_item(uint8_t type, DMod& m, SegRec* r, flo
         BNC_ITEM(150, dp_kv31_current<kDef>(m, s, dt))
         BNC_ITEM(200, dp_cav31_current<kDef>(m, s, dt))
         BNC_ITEM(86, dp_ecb_synthesis_current<kDef>(m, s, dt))
+        BNC_ITEM(147, dp_glast_current(m, s, dt, glu))
 #undef BNC_ITEM
         default: break;
     }
@@ -150,13 +151,14 @@ k_phase(NetDev d, float dt, uint32_t b, uint32_t e) {
 #pragma unroll
     for (int k = 0; k < 7; k++) m.st[k] = ((rm >> k) & 1u) ? d.it_st[(size_t)k * NI + q] : 0.0f;
     float glu = 0.0f, gaba = 0.0f, gly = 0.0f;
-    if (type == 8 || type == 9) glu = d.nt[g];
+    if (type == 8 || type == 9 || type == 147) glu = d.nt[g];
     else if (type == 11) gaba = d.nt[(size_t)1 * N + g];
     else if (type == 12) gly = d.nt[(size_t)7 * N + g];
     SegRec* r = d.rec + g;
     const double I = ((fl & 3) == 0) ? run_item<true>(type, m, r, dt, glu, gaba, gly)
                                      : run_item<false>(type, m, r, dt, glu, gaba, gly);
     r->itot = r->itot + I;
+    if (type == 147) d.nt[g] = glu;   // the transporter's uptake
     const uint32_t wm = c_dyn_mask[type];
 #pragma unroll
     for (int k = 0; k < 7; k++) if ((wm >> k) & 1u) d.it_st[(size_t)k * NI + q] = m.st[k];
@@ -166,7 +168,7 @@ k_phase(NetDev d, float dt, uint32_t b, uint32_t e) {
 // run_item on a segment held in registers: the same models in the same order, the GHK
 // factors computed from the V the item starts with, as rec_load computes them.
 template <bool kDef>
-__device__ __forceinline__ double run_item_s(uint8_t type, DMod& m, DSeg& s, float dt, float glu, float gaba,
+__device__ __forceinline__ double run_item_s(uint8_t type, DMod& m, DSeg& s, float dt, float& glu, float gaba,
                                              float gly) {
     double I = 0.0;
     switch (type) {
@@ -203,6 +205,7 @@ __device__ __forceinline__ double run_item_s(uint8_t type, DMod& m, DSeg& s, flo
         BNC_ITEM(150, dp_kv31_current<kDef>(m, s, dt))
         BNC_ITEM(200, dp_cav31_current<kDef>(m, s, dt))
         BNC_ITEM(86, dp_ecb_synthesis_current<kDef>(m, s, dt))
+        BNC_ITEM(147, dp_glast_current(m, s, dt, glu))
 #undef BNC_ITEM
         default: break;
     }
@@ -254,12 +257,13 @@ k_phase_group(NetDev d, float dt, PhaseGroup grp) {
 #pragma unroll
         for (int k = 0; k < 7; k++) m.st[k] = ((rm >> k) & 1u) ? d.it_st[(size_t)k * NI + qi] : 0.0f;
         float glu = 0.0f, gaba = 0.0f, gly = 0.0f;
-        if (type == 8 || type == 9) glu = d.nt[g];
+        if (type == 8 || type == 9 || type == 147) glu = d.nt[g];
         else if (type == 11) gaba = d.nt[(size_t)1 * N + g];
         else if (type == 12) gly = d.nt[(size_t)7 * N + g];
         const double I = ((fl & 3) == 0) ? run_item_s<true>(type, m, s, dt, glu, gaba, gly)
                                          : run_item_s<false>(type, m, s, dt, glu, gaba, gly);
         itot = itot + I;
+        if (type == 147) d.nt[g] = glu;   // the transporter's uptake
         const uint32_t wm = c_dyn_mask[type];
 #pragma unroll
         for (int k = 0; k < 7; k++) if ((wm >> k) & 1u) d.it_st[(size_t)k * NI + qi] = m.st[k];

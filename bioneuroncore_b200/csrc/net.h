@@ -172,6 +172,14 @@ struct NetDev {
     // (UINT32_MAX: none)
     float* sy_cleft_ecb;      // [n_syn]
     uint32_t* seg_ecb_item;   // [n_seg] (null when no segment has one)
+    // Glia (gl_cap null when no segment has a GLAST transporter): the first 256 such
+    // segments, each with the sliced synapses whose post segment is nearest to it in
+    // z, in original synapse order; gl_cap holds each synapse's capture of the tick
+    float* gl_cap;            // [n_syn]
+    uint32_t* gl_seg;         // [n_glia] device segment
+    uint32_t* gl_off;         // [n_glia + 1]
+    uint32_t* gl_syn;         // sliced synapse indices
+    uint32_t n_glia;
     uint32_t* md_off;         // [n_syn + 1]
     uint8_t* md_code;         // kind << 4 | cleft NT index; kind 1 Gi/o, 2 Gs, 3 ionotropic
     double* md_scale;         // density x effective area (pre_area, or 1 when not positive)

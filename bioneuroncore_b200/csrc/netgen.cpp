@@ -207,6 +207,9 @@ int generate_network(const BncNetgenParams& p, NetSink& sink, NetShape* shape_ou
                 if (axon && (axon_idx & 1u)) set_mod(seg.modifiers[mc++], BNC_MOD_MYELIN, 1.0);
             }
             if (axon) set_mod(seg.modifiers[mc++], BNC_MOD_CAV21, 100.0 * scale_of(p, 3));
+            if ((p.flags & BNC_NETGEN_GLIA) && axon && (axon_idx % 4u) == 0 && mc < BNC_MAX_MODIFIERS)
+                set_mod(seg.modifiers[mc++], 147, 1.0);   // GLAST: a glial segment
+            if (p.flags & BNC_NETGEN_GLIA) seg.position.z = (float)((nrn * 7u) % 13u) * 10.0f + (float)k;
             if ((p.flags & BNC_NETGEN_ECB) && !axon && mc < BNC_MAX_MODIFIERS) {
                 set_mod(seg.modifiers[mc], 86, 1.0);   // eCB synthesis
                 seg.modifiers[mc].state[0] = (double)0.5f;

@@ -1015,6 +1015,38 @@ __device__ __forceinline__ double dp_ecb_synthesis_current(DMod& m, DSeg& s, flo
     return 0.0;
 }
 
+/* hh_biological.cpp:725-733 (GLAST, glial glutamate transporter) through
+ * glial_nt_uptake_current (modifier_helpers.h:418-454): 3 Na+ in, 1 K+ out, net +2,
+ * glutamate taken from the segment's own neurotransmitter pool `glu`, which the
+ * caller stores back. */
+__device__ __forceinline__ double dp_glast_current(DMod& m, DSeg& s, float dt, float& glu) {
+    const float k_m_rel = 10.0f, imax = 2.0f, rel_per_mm = 667.0f;
+    const int na_in = 3, k_out = 1, net_charge = 2;
+    float area = m.area;
+    float NT = glu;
+    if (NT < 0.0f) NT = 0.0f;
+    float frac = NT / (NT + k_m_rel);
+    float I = (float)((double)imax * (double)m.den * (double)area * (double)(1e-8f * 1e6f) * (double)frac);
+    float volume = (float)s.vol;
+    double cpm = FARADAY_CONST * (double)volume / 1000.0;
+    float transport = (float)((double)(I * dt) / ((double)(float)net_charge * cpm));
+    float nt_avail = NT / rel_per_mm;
+    float na_avail = (float)((double)s.out[0] * (double)EXTRA_VOLUME_RATIO / (double)(float)na_in);
+    if (transport > nt_avail) transport = nt_avail;
+    if (transport > na_avail) transport = na_avail;
+    if (k_out && (double)transport > (double)s.in[1]) transport = s.in[1];
+    if (transport < 0.0f) transport = 0.0f;
+    s.in[0] = (float)((double)s.in[0] + (double)((float)na_in * transport));
+    s.out[0] = (float)((double)s.out[0] - (double)((float)na_in * transport / EXTRA_VOLUME_RATIO));
+    s.in[1] = (float)((double)s.in[1] - (double)((float)k_out * transport));
+    s.out[1] = (float)((double)s.out[1] + (double)((float)k_out * transport / EXTRA_VOLUME_RATIO));
+    glu -= transport * rel_per_mm;
+    if (glu < 0.0f) glu = 0.0f;
+    dp_clamp_ions(s.in);
+    dp_clamp_ions(s.out);
+    return I;
+}
+
 /* kernel_dispatch.h:337-570 restricted to the supported types; 0 for unknown types
  * (the oracle's loader rejects them, so this branch is never taken). */
 template <bool kDef>

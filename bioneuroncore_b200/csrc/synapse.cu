@@ -218,6 +218,18 @@ k_synapse(NetDev d, float dt, unsigned long long tick, int first_tick) {
             else if (ntt == 1) nt_gaba += cleft;
             else nt_gly += cleft;
             nt_ecb += cleft_e;
+            // glial capture (simulation_host.cpp:467-487): a share of the transmitter
+            // goes to the glial segment nearest the post segment in z; k_glia adds the
+            // shares to the glial segments in synapse order
+            if (d.gl_cap) {
+                float cap = 0.0f;
+                if (cleft > 0.0f) {
+                    const float tau = d.sy_tauc[k] > 0.0f ? d.sy_tauc[k] : 5.0f;
+                    cap = (float)((double)cleft * (1.0 - dm_exp(-dt / tau)));
+                    cleft -= cap;
+                }
+                d.gl_cap[k] = cap;
+            }
             n_rc = d.rc_cnt[k];
         }
         // receptors (simulation_host.cpp:490-500), j-th receptors of the slice side by side
@@ -261,8 +273,10 @@ k_synapse(NetDev d, float dt, unsigned long long tick, int first_tick) {
             }
             // clearance (simulation_host.cpp:505-510)
             const auto clear_f = dm_exp(-dt / d.sy_tauc[k]);
-            cleft *= clear_f;
-            if (cleft < 0.0f) cleft = 0.0f;
+            if (!d.gl_cap) {   // with glia, they take glutamate, GABA and glycine instead
+                cleft *= clear_f;
+                if (cleft < 0.0f) cleft = 0.0f;
+            }
             cleft_e *= clear_f;
             if (cleft_e < 0.0f) cleft_e = 0.0f;
             // BCM threshold, spine CaMKII/calcineurin, weight (simulation_host.cpp:527-576)
@@ -374,9 +388,32 @@ cudaError_t prepare_synapse(cudaStream_t stream) {
     return e;
 }
 
+// The glial segments' transmitter after step 3: what k_synapse left there (the reset,
+// no synapse targets a glial segment) plus each capture, in original synapse order
+// (simulation_host.cpp:480-481).  One thread per glial segment.
+__global__ void k_glia(NetDev d) {
+    const uint32_t gi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gi >= d.n_glia) return;
+    const uint32_t g = d.gl_seg[gi];
+    const uint32_t N = d.n_seg;
+    float glu = d.nt[g], gaba = d.nt[(size_t)1 * N + g], gly = d.nt[(size_t)7 * N + g];
+    for (uint32_t x = d.gl_off[gi]; x < d.gl_off[gi + 1]; x++) {
+        const uint32_t k = d.gl_syn[x];
+        const float c = d.gl_cap[k];
+        const int ntt = d.sy_flags[k] >> 4;
+        if (ntt == 0) glu += c;
+        else if (ntt == 1) gaba += c;
+        else gly += c;
+    }
+    d.nt[g] = glu;
+    d.nt[(size_t)1 * N + g] = gaba;
+    d.nt[(size_t)7 * N + g] = gly;
+}
+
 cudaError_t launch_synapse(const NetDev& dev, float dt, unsigned long long tick, int first_tick,
                            cudaStream_t stream) {
     k_synapse<<<(dev.n_seg + 255) / 256, 256, 0, stream>>>(dev, dt, tick, first_tick);
+    if (dev.gl_cap) k_glia<<<(dev.n_glia + 127) / 128, 128, 0, stream>>>(dev);
     return cudaGetLastError();
 }
 

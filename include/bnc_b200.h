@@ -145,6 +145,10 @@ typedef struct {
  * state[0] 0.5) on every soma and dendrite segment, and a CB1 release modulator on
  * about half the synapses (from the release-modulator stream). */
 #define BNC_NETGEN_ECB 512u
+/* Glia: a GLAST glutamate transporter (147) on every fourth axon segment, which makes
+ * it a glial segment that takes up transmitter from the clefts nearest to it in z;
+ * segments get spread z positions (neuron-dependent offsets). */
+#define BNC_NETGEN_GLIA 1024u
 
 /* Generates a network into host AoS arrays in the reference layout.  The arrays
  * are owned by the library; release with bnc_netgen_free.  *stim receives the

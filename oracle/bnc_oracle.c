@@ -765,6 +765,12 @@ static void bo_tick(BoSim* S, float dt) {
     for (uint32_t i = 0; i < n; i++)
         for (uint8_t j = 0; j < sg[i].nmod; j++)
             if (sg[i].mods[j].type == 43) sg[i].nt[3] = 0.0f;
+    /* glial segments (:351-355): the first 256 with a GLAST modifier */
+    uint32_t glia[256];
+    uint32_t n_glia = 0;
+    for (uint32_t g = 0; g < n && n_glia < 256; g++)
+        for (uint8_t j = 0; j < sg[g].nmod; j++)
+            if (sg[g].mods[j].type == 147) { glia[n_glia++] = g; break; }
     for (uint32_t i = 0; i < S->k; i++) {
         OSyn* syn = &S->syn[i];
         if (syn->pre >= n || syn->post >= n) continue;
@@ -833,6 +839,24 @@ static void bo_tick(BoSim* S, float dt) {
             }
         }
         for (int q = 0; q < 15; q++) post->nt[q] += syn->cleft[q];
+        /* glial capture (:467-487): a share of glutamate, glycine and GABA goes to the
+           glial segment nearest in z, rate-limited by the clearance time constant */
+        if (n_glia > 0) {
+            for (int kk = 0; kk < 3; kk++) {
+                int q = (kk == 0) ? 0 : (kk == 1) ? 7 : 1;
+                if (syn->cleft[q] <= 0.0f) continue;
+                float best_dz = 1e30f;
+                uint32_t best_g = glia[0];
+                for (uint32_t gi = 0; gi < n_glia; gi++) {
+                    float dz = fabsf(sg[glia[gi]].pz - post->pz);
+                    if (dz < best_dz) { best_dz = dz; best_g = glia[gi]; }
+                }
+                float tau = (syn->tau_clear > 0.0f) ? syn->tau_clear : 5.0f;
+                float capture = (float)((double)syn->cleft[q] * (1.0 - bo_exp(-dt / tau)));
+                sg[best_g].nt[q] += capture;
+                syn->cleft[q] -= capture;
+            }
+        }
         int myel_post = bo_has_myelin(post);
         float I_syn = 0.0f;
         for (int j = 0; j < syn->n_post_r; j++) {
@@ -844,6 +868,7 @@ static void bo_tick(BoSim* S, float dt) {
         post->ibuf += I_syn;
         bo_spine_ca_step(syn, I_syn, dt);
         for (int q = 0; q < 15; q++) {
+            if ((q == 0 || q == 7 || q == 1) && n_glia > 0) continue;   /* the glia took their share */
             syn->cleft[q] *= bo_exp(-dt / syn->tau_clear);
             if (syn->cleft[q] < 0.0f) syn->cleft[q] = 0.0f;
         }

@@ -701,6 +701,37 @@ static double bo_ecb_synthesis_current(OMod* m, OSeg* s, float dt) {
     return 0.0;
 }
 
+/* hh_biological.cpp:725-733 (GLAST, glial glutamate transporter) through
+ * glial_nt_uptake_current (modifier_helpers.h:418-454): 3 Na+ in, 1 K+ out, net +2,
+ * glutamate taken from the segment's own neurotransmitter pool. */
+static double bo_glast_current(OMod* m, OSeg* s, float dt) {
+    const float k_m_rel = 10.0f, imax = 2.0f, rel_per_mm = 667.0f;
+    const int na_in = 3, k_out = 1, net_charge = 2;
+    float area = (m->st[7] > 0.0f) ? (float)m->st[7] : bo_seg_area(s);
+    float NT = s->nt[0];
+    if (NT < 0.0f) NT = 0.0f;
+    float frac = NT / (NT + k_m_rel);
+    float I = (float)((double)imax * (double)m->density * (double)area * (double)(1e-8f * 1e6f) * (double)frac);
+    float volume = (float)bo_seg_volume(s);
+    double cpm = FARADAY_CONST * (double)volume / 1000.0;
+    float transport = (float)((double)(I * dt) / ((double)(float)net_charge * cpm));
+    float nt_avail = NT / rel_per_mm;
+    float na_avail = (float)((double)s->out[0] * (double)EXTRA_VOLUME_RATIO / (double)(float)na_in);
+    if (transport > nt_avail) transport = nt_avail;
+    if (transport > na_avail) transport = na_avail;
+    if (k_out && (double)transport > (double)s->in[1]) transport = (float)s->in[1];
+    if (transport < 0.0f) transport = 0.0f;
+    s->in[0] = BO_ST((double)s->in[0] + (double)((float)na_in * transport));
+    s->out[0] = BO_ST((double)s->out[0] - (double)((float)na_in * transport / EXTRA_VOLUME_RATIO));
+    s->in[1] = BO_ST((double)s->in[1] - (double)((float)k_out * transport));
+    s->out[1] = BO_ST((double)s->out[1] + (double)((float)k_out * transport / EXTRA_VOLUME_RATIO));
+    s->nt[0] -= transport * rel_per_mm;
+    if (s->nt[0] < 0.0f) s->nt[0] = 0.0f;
+    bo_clamp_ions(s->in);
+    bo_clamp_ions(s->out);
+    return I;
+}
+
 static double bo_dispatch(uint8_t type, OMod* m, OSeg* s, float dt) {
     switch (type) {
         case 1: return bo_cav13_current(m, s, dt);
@@ -730,6 +761,7 @@ static double bo_dispatch(uint8_t type, OMod* m, OSeg* s, float dt) {
         case 150: return bo_kv31_current(m, s, dt);
         case 200: return bo_cav31_current(m, s, dt);
         case 86: return bo_ecb_synthesis_current(m, s, dt);
+        case 147: return bo_glast_current(m, s, dt);
         default: return 0.0f;
     }
 }
@@ -738,7 +770,7 @@ static int bo_type_supported(uint8_t t) {
     switch (t) {
         case 1: case 4: case 7: case 8: case 9: case 11: case 12: case 85: case 98: case 99:
         case 100: case 102: case 103: case 104: case 105: case 106: case 107: case 112:
-        case 123: case 129: case 133: case 140: case 141: case 142: case 150: case 200: case 86:
+        case 123: case 129: case 133: case 140: case 141: case 142: case 150: case 200: case 86: case 147:
             return 1;
         default: return 0;
     }

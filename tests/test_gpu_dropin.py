@@ -154,16 +154,18 @@ def _rel(a, b, floor):
 
 
 @pytest.mark.parametrize("family,on_host", [("large", 0), ("large", 1), ("extras", 0), ("modulators", 0),
-                                           ("modulators", 1), ("ecb", 0), ("ecb", 1)])
+                                           ("modulators", 1), ("ecb", 0), ("ecb", 1),
+                                           ("glia", 0)])
 def test_dropin_sequence_equals_the_oracle(tmp_path, family, on_host):
     """on_host: the records moved to plain host memory and updated by the host export
     (bnc_set_records_residency), instead of managed memory written on the device."""
     from bioneuroncore_b200 import (Backend, Network, NetgenParams, NET_LARGE, NET_SMALL, NETGEN_SYNAPSE_EXTRAS,
-                                    NETGEN_RELEASE_MODULATORS, NETGEN_ECB)
+                                    NETGEN_RELEASE_MODULATORS, NETGEN_ECB, NETGEN_GLIA)
     if family == "large":
         p = NetgenParams(family=NET_LARGE, n_neurons=12, seed=3)
     else:
-        flags = NETGEN_SYNAPSE_EXTRAS | {"modulators": NETGEN_RELEASE_MODULATORS, "ecb": NETGEN_ECB}.get(family, 0)
+        flags = NETGEN_SYNAPSE_EXTRAS | {"modulators": NETGEN_RELEASE_MODULATORS, "ecb": NETGEN_ECB,
+                                         "glia": NETGEN_GLIA}.get(family, 0)
         p = NetgenParams(family=NET_SMALL, n_neurons=16, seed=6, flags=flags, stim_pA=3000.0)
     net = Network(p)
     path = tmp_path / "net.bion"

@@ -157,3 +157,15 @@ def test_endocannabinoid_signalling_bitexact():
                      stim_pA=3000.0)
     log, net = _run(p, 1000, 100)
     assert len(log) > 0
+
+
+def test_glial_capture_bitexact():
+    """Glial segments with a GLAST transporter: each cleft hands a share of its
+    transmitter to the glial segment nearest in z (summed there in synapse order),
+    the transporter takes it up in step 1, and no cleft clears it by its own time
+    constant; 1,000 ticks equal the oracle's bit for bit."""
+    from bioneuroncore_b200 import NetgenParams, NET_SMALL, NETGEN_SYNAPSE_EXTRAS, NETGEN_GLIA
+    p = NetgenParams(family=NET_SMALL, n_neurons=16, seed=6, flags=NETGEN_SYNAPSE_EXTRAS | NETGEN_GLIA,
+                     stim_pA=3000.0)
+    log, net = _run(p, 1000, 100)
+    assert len(log) > 0

@@ -218,6 +218,22 @@ def test_endocannabinoid_signalling_bit_identical():
     assert (net_r.synapses["cleft_neurotransmitter"][:, 9] > 0).any(), "eCB must reach the clefts"
 
 
+def test_glial_capture_bit_identical():
+    """Glial segments (a GLAST transporter, hh_biological.cpp:725-733): each cleft
+    hands a share of its glutamate, glycine or GABA to the glial segment nearest in z
+    instead of clearing it (simulation_host.cpp:467-487, 505-510), and the transporter
+    takes it up in step 1; 1,000 ticks with releases, everything equal."""
+    from bioneuroncore_b200 import NET_SMALL, NETGEN_SYNAPSE_EXTRAS, NETGEN_GLIA
+    spec = dict(family=NET_SMALL, n=16, seed=6, flags=NETGEN_SYNAPSE_EXTRAS | NETGEN_GLIA, stim_pA=3000.0)
+    net_r = _net(**spec)
+    glial = np.flatnonzero((net_r.segments["modifiers"]["type"] == 147).any(axis=1))
+    assert len(glial) > 1
+    log = _run_pinned(net_r, _net(**spec), 1000, full_every=100)
+    assert len(log) > 0
+    nt = net_r.segments["neurotransmitter"]
+    assert (nt[glial][:, [0, 1, 7]] > 0).any(), "the glia must have taken up transmitter"
+
+
 def mechano_schedule(net):
     """Mechano stimuli at three ticks of the small family (tick -> (segment_id, mod_type,
     state_idx, value) list): a gate (dynamic word), parameter words of Nav1.x and K2P,
