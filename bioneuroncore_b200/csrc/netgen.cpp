@@ -127,9 +127,13 @@ int generate_network(const BncNetgenParams& p, NetSink& sink, NetShape* shape_ou
     uint32_t n_stim = (p.flags & BNC_NETGEN_NO_STIMULI) ? 0 : (uint32_t)(0.1 * n_neurons + 0.5);
     if (n_stim == 0 && !(p.flags & BNC_NETGEN_NO_STIMULI) && n_neurons >= 1) n_stim = 1;
 
+    // electrical synapses between the somata of consecutive neurons, spread through
+    // the chemical ones in the synapse order
+    const uint64_t n_gj = ((p.flags & BNC_NETGEN_GAP_JUNCTIONS) && n_syn && n_neurons > 1 && !f.tree) ? n_neurons - 1 : 0;
+
     NetShape shape;
     shape.n_neurons = n_neurons; shape.n_segments = n_seg; shape.n_connections = n_conn;
-    shape.n_synapses = n_syn; shape.n_stimuli = n_stim;
+    shape.n_synapses = n_syn + n_gj; shape.n_stimuli = n_stim;
     if (shape_out) *shape_out = shape;
 
     Rng rng_geo(p.seed * 4 + 1), rng_mod(p.seed * 4 + 2), rng_syn(p.seed * 4 + 3), rng_stim(p.seed * 4 + 4);
@@ -138,7 +142,7 @@ int generate_network(const BncNetgenParams& p, NetSink& sink, NetShape* shape_ou
     float wsum = 0.0f;
     for (const auto& t : kLargeTypes) wsum += t.weight;
 
-    sink.begin(n_neurons, n_seg, n_conn, n_syn, n_stim);
+    sink.begin(n_neurons, n_seg, n_conn, n_syn + n_gj, n_stim);
 
     BncSegment seg;
     for (uint32_t nrn = 0; nrn < n_neurons; nrn++) {
@@ -207,6 +211,18 @@ int generate_network(const BncNetgenParams& p, NetSink& sink, NetShape* shape_ou
                 if (axon && (axon_idx & 1u)) set_mod(seg.modifiers[mc++], BNC_MOD_MYELIN, 1.0);
             }
             if (axon) set_mod(seg.modifiers[mc++], BNC_MOD_CAV21, 100.0 * scale_of(p, 3));
+            if ((p.flags & BNC_NETGEN_GAP_JUNCTIONS) && soma && mc + 2 <= BNC_MAX_MODIFIERS) {
+                set_mod(seg.modifiers[mc], 114, 1.0);   // connexin-36
+                seg.modifiers[mc].state[0] = (double)0.8f;
+                seg.modifiers[mc].state[4] = 1.0;
+                mc++;
+                if (nrn & 1u) {                         // connexin-43 on every other soma
+                    set_mod(seg.modifiers[mc], 198, 0.5);
+                    seg.modifiers[mc].state[0] = (double)0.6f;
+                    seg.modifiers[mc].state[4] = 1.0;
+                    mc++;
+                }
+            }
             if ((p.flags & BNC_NETGEN_GLIA) && axon && (axon_idx % 4u) == 0 && mc < BNC_MAX_MODIFIERS)
                 set_mod(seg.modifiers[mc++], 147, 1.0);   // GLAST: a glial segment
             if (p.flags & BNC_NETGEN_GLIA) seg.position.z = (float)((nrn * 7u) % 13u) * 10.0f + (float)k;
@@ -263,6 +279,7 @@ int generate_network(const BncNetgenParams& p, NetSink& sink, NetShape* shape_ou
         uint64_t n_axon_total = (uint64_t)n_neurons * n_axon;
         uint64_t n_post_total = (uint64_t)n_neurons * (1 + n_dend);
         BncSynapse sy;
+        uint64_t gj_done = 0;
         for (uint64_t i = 0; i < n_syn; i++) {
             std::memset(&sy, 0, sizeof(sy));
             uint64_t a = rng_syn.below(n_axon_total);
@@ -325,6 +342,18 @@ int generate_network(const BncNetgenParams& p, NetSink& sink, NetShape* shape_ou
             sy.bouton_Ca = 1e-4f;
             sy.spine_Ca = 1e-4f;
             sink.synapse(sy);
+            while (gj_done < n_gj && (i + 1) * (n_gj + 1) >= (gj_done + 1) * n_syn) {
+                std::memset(&sy, 0, sizeof(sy));
+                sy.id = (uint32_t)(n_syn + gj_done);
+                sy.pre_segment = (uint32_t)gj_done * segs;
+                sy.post_segment = (uint32_t)(gj_done + 1) * segs;
+                sy.type = (gj_done & 1u) ? 2 : BNC_SYN_ELECTRICAL;   // dendritic bridge, electrical
+                sy.delay = (gj_done % 3u == 0) ? 0.5f : 0.0f;        // 0.5 ms: the filtered current
+                sy.weight = 1.0f;
+                sy.tau_clearance = 1.0f;
+                sink.synapse(sy);
+                gj_done++;
+            }
         }
     }
 

@@ -149,6 +149,11 @@ typedef struct {
  * it a glial segment that takes up transmitter from the clefts nearest to it in z;
  * segments get spread z positions (neuron-dependent offsets). */
 #define BNC_NETGEN_GLIA 1024u
+/* Gap junctions: electrical synapses (alternately type 1 and 2, every third with a
+ * 0.5 ms delay) from the soma of each neuron to the next one's, spread through the
+ * chemical synapses in the synapse order; connexin-36 (114) on every soma and
+ * connexin-43 (198) on every other one. */
+#define BNC_NETGEN_GAP_JUNCTIONS 2048u
 
 /* Generates a network into host AoS arrays in the reference layout.  The arrays
  * are owned by the library; release with bnc_netgen_free.  *stim receives the

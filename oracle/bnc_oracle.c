@@ -588,6 +588,44 @@ static float bo_release_modulator(OMod* m, const float* cleft, float dt) {
     return (float)(1.0f + (double)0.5f * (double)m->st[0] * scale);
 }
 
+/* run_tick_common.h:114-122: the slow Ca2+/calmodulin gate of a gap junction */
+static float bo_gj_cam_update(float m_slow, float ca_pre, float ca_post, float dt) {
+    float ca_avg = 0.5f * (ca_pre + ca_post);
+    float cam_act = (ca_avg * ca_avg) / (ca_avg * ca_avg + 0.0003f * 0.0003f);
+    m_slow += (cam_act - m_slow) * dt / 100.0f;
+    if (m_slow < 0.0f) m_slow = 0.0f;
+    if (m_slow > 1.0f) m_slow = 1.0f;
+    return m_slow;
+}
+
+/* run_tick_common.h:79-110: the junction's conductance (nS) from the connexins of both
+ * segments (the density is the presynaptic segment's), Cx43's Vj gate and the slow gate */
+static float bo_gj_g_eff(const OSeg* pre, const OSeg* post, float m_slow, float Vj) {
+    float g_gap_ps = 0.0f;
+    for (int cx = 0; cx < 2; cx++) {
+        uint8_t cx_type = (cx == 0) ? 114 : 198;
+        float gamma = (cx == 0) ? 14.0f : 100.0f;
+        float density = 0.0f;
+        float f = 1.0f;
+        for (uint8_t j = 0; j < pre->nmod; j++)
+            if (pre->mods[j].type == cx_type) {
+                density = (float)pre->mods[j].density;
+                f = (float)((double)f * ((double)pre->mods[j].st[0] * (double)pre->mods[j].st[4]));
+            }
+        for (uint8_t j = 0; j < post->nmod; j++)
+            if (post->mods[j].type == cx_type)
+                f = (float)((double)f * ((double)post->mods[j].st[0] * (double)post->mods[j].st[4]));
+        if (cx == 1) {
+            float vj_abs = Vj < 0.0f ? -Vj : Vj;
+            float f_vj = (float)(1.0f / (1.0f + bo_exp((double)((vj_abs - 40.0f) / 5.0f))));
+            f *= f_vj;
+        }
+        if (f < 0.01f) f = 0.01f;
+        g_gap_ps += density * f * gamma;
+    }
+    return g_gap_ps * 1e-3f * (1.0f - m_slow);
+}
+
 static void bo_bouton_ca_step(const OSeg* pre, OSyn* syn, float dt) {
     float g_K = 0.0f, g_Na = 0.0f;
     for (uint8_t j = 0; j < syn->n_pre_ar; j++) {
@@ -786,6 +824,25 @@ static void bo_tick(BoSim* S, float dt) {
                     slots[q].arrival = 0;
                 }
             }
+        }
+        /* electrical synapse or dendritic bridge (:373-402, run_tick_common.h:79-122) */
+        if (syn->type == 1 || syn->type == 2) {
+            float Vj = (float)((double)pre->V - (double)post->V);
+            float m_slow = bo_gj_cam_update(syn->depr, (float)pre->in[2], (float)post->in[2], dt);
+            syn->depr = m_slow;
+            float g_eff = bo_gj_g_eff(pre, post, m_slow, Vj);
+            float I_gap_raw = g_eff * Vj;
+            if (syn->delay > 0.001f) {
+                float I_filtered = syn->cleft[0];
+                I_filtered += (I_gap_raw - I_filtered) * dt / syn->delay;
+                syn->cleft[0] = I_filtered;
+                pre->ibuf -= I_filtered;
+                post->ibuf += I_filtered;
+            } else {
+                pre->ibuf -= I_gap_raw;
+                post->ibuf += I_gap_raw;
+            }
+            continue;
         }
         /* rrp_do_recovery (kernel_dispatch.h:612-630); no CaMKII/calcineurin modifiers */
         if (!(syn->RRP_max <= 0.0f || syn->RRP >= syn->RRP_max)) {
@@ -1012,8 +1069,8 @@ BoSim* bo_create(const BncBionData* d, const BncCurrentStimulus* stim, uint32_t 
     for (uint32_t i = 0; i < S->k; i++) {
         const BncSynapse* a = &d->synapses[i];
         OSyn* y = &S->syn[i];
-        if (a->type != BNC_SYN_CHEMICAL) {
-            snprintf(err, errlen, "synapse %u: only chemical synapses are supported", i);
+        if (a->type > 2) {
+            snprintf(err, errlen, "synapse %u: type %u", i, (unsigned)a->type);
             return S;
         }
         y->id = a->id; y->pre = a->pre_segment; y->post = a->post_segment; y->type = a->type;

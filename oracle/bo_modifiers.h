@@ -732,6 +732,34 @@ static double bo_glast_current(OMod* m, OSeg* s, float dt) {
     return I;
 }
 
+/* hh_biological.cpp:3266-3308 (connexin-36) and 3310-3350 (connexin-43), the same
+ * steps: connexon turnover, phosphorylation toward CaMKII and cAMP drives, P_open from
+ * phosphorylation and pH.  No current; gap junctions read state[0] and state[4]. */
+static double bo_connexin_current(OMod* m, OSeg* s, float dt) {
+    double synth_rate = (m->st[2] > 0.0f) ? (double)m->st[2] : (double)0.001f;
+    double degrad_rate = (m->st[3] > 0.0f) ? (double)m->st[3] : (double)0.0005f;
+    double pH = (m->st[5] > 4.0f) ? (double)m->st[5] : (double)7.2f;
+    m->st[0] = BO_ST((double)m->st[0] + (synth_rate - degrad_rate * (double)m->st[0]) * (double)dt / (double)3600000.0f);
+    if (m->st[0] < 0.0f) m->st[0] = 0.0f;
+    if (m->st[0] > 1.0f) m->st[0] = 1.0f;
+    float camkii_act = 0.0f;
+    for (uint8_t j = 0; j < s->nmod; j++)
+        if (s->mods[j].type == 82) camkii_act = (float)s->mods[j].st[0];
+    double pka_drive = (double)m->st[6];
+    float p_target = (float)((double)(camkii_act * 0.6f) + pka_drive * (double)0.3f);
+    m->st[1] = BO_ST((double)m->st[1] + ((double)p_target - (double)m->st[1]) * (double)dt / (double)5000.0f);
+    if (m->st[1] < 0.0f) m->st[1] = 0.0f;
+    if (m->st[1] > 1.0f) m->st[1] = 1.0f;
+    float pH_factor = (pH < 6.8f) ? (float)((pH - (double)6.0f) / (double)0.8f) : 1.0f;
+    if (pH_factor < 0.0f) pH_factor = 0.0f;
+    double camkii_P_open = 1.0f - (double)m->st[1] * (double)0.5f;
+    double pka_P_open = 1.0f + (double)m->st[1] * (double)0.3f;
+    m->st[4] = BO_ST((camkii_P_open * (double)0.5f + pka_P_open * (double)0.5f) * (double)pH_factor);
+    if (m->st[4] < 0.05f) m->st[4] = 0.05f;
+    if (m->st[4] > 2.0f) m->st[4] = 2.0f;
+    return 0.0;
+}
+
 static double bo_dispatch(uint8_t type, OMod* m, OSeg* s, float dt) {
     switch (type) {
         case 1: return bo_cav13_current(m, s, dt);
@@ -762,6 +790,7 @@ static double bo_dispatch(uint8_t type, OMod* m, OSeg* s, float dt) {
         case 200: return bo_cav31_current(m, s, dt);
         case 86: return bo_ecb_synthesis_current(m, s, dt);
         case 147: return bo_glast_current(m, s, dt);
+        case 114: case 198: return bo_connexin_current(m, s, dt);
         default: return 0.0f;
     }
 }
@@ -770,7 +799,7 @@ static int bo_type_supported(uint8_t t) {
     switch (t) {
         case 1: case 4: case 7: case 8: case 9: case 11: case 12: case 85: case 98: case 99:
         case 100: case 102: case 103: case 104: case 105: case 106: case 107: case 112:
-        case 123: case 129: case 133: case 140: case 141: case 142: case 150: case 200: case 86: case 147:
+        case 123: case 129: case 133: case 140: case 141: case 142: case 150: case 200: case 86: case 147: case 114: case 198:
             return 1;
         default: return 0;
     }

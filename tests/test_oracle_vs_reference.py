@@ -234,6 +234,22 @@ def test_glial_capture_bit_identical():
     assert (nt[glial][:, [0, 1, 7]] > 0).any(), "the glia must have taken up transmitter"
 
 
+def test_gap_junctions_bit_identical():
+    """Electrical synapses and dendritic bridges between somata (simulation_host.cpp:
+    373-402; run_tick_common.h:79-122): connexin-36/43 models in step 1, the slow
+    Ca2+/CaM gate, Cx43's Vj gate, the filtered current of delayed junctions, both
+    segments' I_buffer in synapse order among the chemical synapses; 1,000 ticks."""
+    from bioneuroncore_b200 import NET_SMALL, NETGEN_GAP_JUNCTIONS
+    spec = dict(family=NET_SMALL, n=16, seed=6, flags=NETGEN_GAP_JUNCTIONS, stim_pA=3000.0)
+    net_r = _net(**spec)
+    syn = net_r.synapses
+    assert (syn["type"] == 1).any() and (syn["type"] == 2).any()
+    log = _run_pinned(net_r, _net(**spec), 1000, full_every=100)
+    assert len(log) > 0
+    gj = syn["type"] > 0
+    assert (syn["depression"][gj] > 0).all() and (syn["cleft_neurotransmitter"][gj & (syn["delay"] > 0), 0] != 0).any()
+
+
 def mechano_schedule(net):
     """Mechano stimuli at three ticks of the small family (tick -> (segment_id, mod_type,
     state_idx, value) list): a gate (dynamic word), parameter words of Nav1.x and K2P,
