@@ -26,7 +26,8 @@ LIB_PATH = os.path.join(_HERE, "libbnc_b200.so")
 SEG_FIELDS = {"V": 0, "ion_in": 1, "ion_out": 2, "ATP": 3, "temperature": 4, "transcription": 5,
               "intra_nt": 6, "neurotransmitter": 7, "mod_state": 8, "spikes": 9}
 SYN_FIELDS = {"bouton_Ca": 0, "spine_Ca": 1, "weight": 2, "refractory": 3, "cleft": 4, "receptor_state": 5,
-              "facilitation": 6, "spine_camkii": 7, "spine_calcineurin": 8, "RRP": 9, "autoreceptor_state": 11}
+              "facilitation": 6, "spine_camkii": 7, "spine_calcineurin": 8, "RRP": 9, "depression": 10,
+              "autoreceptor_state": 11}
 
 # Symbols the reference's loader requires (reference tests/smoke_cuda.sh:24-29) plus the
 # ABI probes and this backend's own entry points; include/*.h declares every one.

@@ -51,6 +51,7 @@ struct Backend {
         uint8_t* rec_slot;    // device receptor -> receptor slot
         uint32_t* md_syn;     // release modulator -> record
         uint8_t* md_slot;     // release modulator -> autoreceptor slot
+        uint32_t* gj_syn;     // gap junction -> record
     } xm{};
     uint32_t tick_stride = 1;   // the tick counter's step per tick (2: the reference's batch mode)
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -167,14 +168,17 @@ int export_network(const NetDev& d, const NetHost& h, uint64_t ticks_run, BncBio
                  oTxn = x_txn ? take(n) : 0;
     size_t oSt[7];
     for (int k = 0; k < 7; k++) oSt[k] = ((rows >> k) & 1u) ? take(NI) : 0;
-    size_t oSy[8] = {0}, oRc = 0, oMd = 0, oEc = 0;
+    size_t oSy[8] = {0}, oRc = 0, oMd = 0, oEc = 0, oGd = 0, oGf = 0;
     if (K) {
         for (int f = 0; f < 8; f++) oSy[f] = take(K);
         oRc = take((size_t)3 * NR);
         oMd = take(d.n_md);
         oEc = d.sy_cleft_ecb ? take(K) : 0;
+        oGd = take(d.n_gj);
+        oGf = take(d.n_gj);
     }
     const size_t bytes = off * sizeof(float) + K;
+    std::vector<uint32_t> gjv;   // the gap-junction sides among the entries
     std::lock_guard<std::mutex> lock(g_stage_mu);
     unsigned char* base = stage_reserve(bytes);
     float* F = reinterpret_cast<float*>(base);
@@ -200,6 +204,9 @@ int export_network(const NetDev& d, const NetHost& h, uint64_t ticks_run, BncBio
         get(oRc, d.rc_st, (size_t)3 * NR * 4);
         get(oMd, d.md_st, (size_t)d.n_md * 4);
         if (d.sy_cleft_ecb) get(oEc, d.sy_cleft_ecb, (size_t)K * 4);
+        get(oGd, d.gj_dep, (size_t)d.n_gj * 4);
+        get(oGf, d.gj_flt, (size_t)d.n_gj * 4);
+        if (ok && d.sy_gj) ok = d2h(gjv, d.sy_gj, K);
         if (ok) ok = cudaMemcpy(refr, d.sy_refr, K, cudaMemcpyDeviceToHost) == cudaSuccess;
     }
     if (!ok) { set_error("export: device read failed"); return BNC_ERR_CUDA; }
@@ -236,6 +243,7 @@ int export_network(const NetDev& d, const NetHost& h, uint64_t ticks_run, BncBio
     if (K) {
         parallel_for(K, [&](size_t q0, size_t q1) {
             for (size_t q = q0; q < q1; q++) {
+                if (!gjv.empty() && gjv[q] != UINT32_MAX) continue;   // a gap junction's side
                 BncSynapse& y = aos->synapses[h.syn_orig[q]];
                 y.bouton_Ca = F[oSy[0] + q]; y.spine_Ca = F[oSy[1] + q]; y.spine_camkii = F[oSy[2] + q];
                 y.spine_calcineurin = F[oSy[3] + q]; y.facilitation = F[oSy[4] + q]; y.weight = F[oSy[5] + q];
@@ -254,6 +262,11 @@ int export_network(const NetDev& d, const NetHost& h, uint64_t ticks_run, BncBio
                 if (ticks_run > 0) m.state[7] = y.post_area;
             }
         });
+        for (uint32_t g = 0; g < d.n_gj; g++) {
+            BncSynapse& y = aos->synapses[h.gj_syn[g]];
+            y.depression = F[oGd + g];
+            y.cleft_neurotransmitter[0] = F[oGf + g];
+        }
         for (uint32_t q = 0; q < d.n_md; q++) {
             BncSynapse& y = aos->synapses[h.md_syn[q]];
             BncModifier& m = y.pre_autoreceptors[h.md_slot[q]];
@@ -460,6 +473,7 @@ __global__ void k_export_synapses(NetDev d, const uint32_t* syn_orig, const uint
                                   int after_tick) {
     const uint32_t K = d.n_syn;
     for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < K; q += gridDim.x * blockDim.x) {
+        if (d.sy_gj && d.sy_gj[q] != UINT32_MAX) continue;   // a gap junction's side: k_export_gaps
         unsigned char* y = syn + (size_t)syn_orig[q] * kSynBytes;
         put<float>(y, offsetof(BncSynapse, bouton_Ca), d.sy_bouton[q]);
         put<float>(y, offsetof(BncSynapse, spine_Ca), d.sy_spine[q]);
@@ -484,6 +498,15 @@ __global__ void k_export_receptors(NetDev d, const uint32_t* rec_syn, const uint
         for (int k = 0; k < 3; k++) put<double>(m, kOffModState + 8 * k, (double)d.rc_st[(size_t)k * NR + r]);
         if (after_tick)
             put<double>(m, kOffModState + 8 * 7, (double)*reinterpret_cast<const float*>(y + offsetof(BncSynapse, post_area)));
+    }
+}
+
+// gap junctions: the slow gate in depression, the filtered current in cleft entry 0
+__global__ void k_export_gaps(NetDev d, const uint32_t* gj_syn, unsigned char* syn) {
+    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < d.n_gj; g += gridDim.x * blockDim.x) {
+        unsigned char* y = syn + (size_t)gj_syn[g] * kSynBytes;
+        put<float>(y, offsetof(BncSynapse, depression), d.gj_dep[g]);
+        put<float>(y, offsetof(BncSynapse, cleft_neurotransmitter), d.gj_flt[g]);
     }
 }
 
@@ -544,6 +567,7 @@ static int make_records_managed(Backend* b) {
         x.rec_slot = upload_map(b, h.rec_slot, &ok);
         x.md_syn = upload_map(b, h.md_syn, &ok);
         x.md_slot = upload_map(b, h.md_slot, &ok);
+        x.gj_syn = upload_map(b, h.gj_syn, &ok);
         if (!ok) {
             cudaFree(ms);
             cudaFree(my);
@@ -587,6 +611,7 @@ static int export_records(Backend* b) {
         k_export_receptors<<<grid(d.n_rec), 256, 0, b->stream>>>(d, b->xm.rec_syn, b->xm.rec_slot, b->xm.syn_orig, syn,
                                                                  after);
     if (d.n_md) k_export_modulators<<<grid(d.n_md), 256, 0, b->stream>>>(d, b->xm.md_syn, b->xm.md_slot, syn, after);
+    if (d.n_gj) k_export_gaps<<<grid(d.n_gj), 256, 0, b->stream>>>(d, b->xm.gj_syn, syn);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) { b->failed = true; return cuda_fail(e, "record export launch"); }
     return sync_stream(b);
@@ -1516,6 +1541,10 @@ int bnc_read_synapse_field(void* sim, int field, int index, float* out, uint32_t
             }
             if (!d2h(v, d.sy_cleft, K)) return cuda_fail(cudaGetLastError(), "read");
             for (uint32_t q = 0; q < K; q++) out[b->host.syn_orig[q]] = (b->host.syn_nt[q] == index) ? v[q] : 0.0f;
+            if (index == 0 && d.n_gj) {   // a gap junction's cleft entry 0 holds its filtered current
+                if (!d2h(v, d.gj_flt, d.n_gj)) return cuda_fail(cudaGetLastError(), "read");
+                for (uint32_t g = 0; g < d.n_gj; g++) out[b->host.gj_syn[g]] = v[g];
+            }
             return BNC_OK;
         }
         case 5: {
@@ -1530,6 +1559,19 @@ int bnc_read_synapse_field(void* sim, int field, int index, float* out, uint32_t
         case 7: src = d.sy_camkii; break;
         case 8: src = d.sy_calcn; break;
         case 9: src = d.sy_rrp; break;
+        case 10: {   // depression: BCM's threshold (facilitation + 0.01 after a tick), a gap junction's slow gate
+            if (!d2h(v, d.sy_facil, K)) return cuda_fail(cudaGetLastError(), "read");
+            for (uint32_t q = 0; q < K; q++) {
+                const uint32_t o = b->host.syn_orig[q];
+                out[o] = b->ticks_run > 0 ? v[q] + 0.01f
+                                          : ((b->owns_aos && b->aos.synapses) ? b->aos.synapses[o].depression : 0.0f);
+            }
+            if (d.n_gj) {
+                if (!d2h(v, d.gj_dep, d.n_gj)) return cuda_fail(cudaGetLastError(), "read");
+                for (uint32_t g = 0; g < d.n_gj; g++) out[b->host.gj_syn[g]] = v[g];
+            }
+            return BNC_OK;
+        }
         case 11: {   // autoreceptor state: index = slot * 8 + word; word 0 of release modulators
             const int j = index >> 3, w = index & 7;
             if (w != 0) { set_error("autoreceptor states other than word 0 of release modulators are not tracked"); return BNC_ERR_ARG; }

@@ -84,7 +84,7 @@ bool type_supported(uint8_t t) {
     switch (t) {
         case 1: case 4: case 7: case 8: case 9: case 11: case 12: case 85: case 98: case 99:
         case 100: case 102: case 103: case 104: case 105: case 106: case 107: case 112:
-        case 123: case 129: case 133: case 140: case 141: case 142: case 150: case 200: case 86: case 147:
+        case 123: case 129: case 133: case 140: case 141: case 142: case 150: case 200: case 86: case 147: case 114: case 198:
             return true;
         default: return false;
     }
@@ -156,6 +156,7 @@ uint8_t param_words(uint8_t t) {
         case 150: return 0x20;    // 5
         case 200: return 0x7C;    // 2..6
         case 86: return 0x06;     // 1,2
+        case 114: case 198: return 0x6C;   // 2,3,5,6
         default: return 0;
     }
 }
@@ -1111,14 +1112,17 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
     auto check_syn = [&](uint32_t k, bool report) -> int {
         const SynLite& y = hn.syn[k];
         if (y.pre_segment >= n || y.post_segment >= n) return 1;   // simulation_host.cpp:362
-        if (y.type != BNC_SYN_CHEMICAL) {
-            if (report) set_error("synapse %u: electrical synapses have no device implementation in this backend", k);
+        if (y.type > 2) {
+            if (report) set_error("synapse %u: type %u", k, (unsigned)y.type);
             return BNC_ERR_UNSUPPORTED;
         }
         if (y.post_receptor_count > BNC_MAX_POST_RECEPTORS || y.pre_autoreceptor_count > BNC_MAX_PRE_AUTORECEPTORS) {
             if (report) set_error("synapse %u: receptor count out of range", k);
             return BNC_ERR_FORMAT;
         }
+        // an electrical synapse or dendritic bridge runs only the gap-junction step
+        // (simulation_host.cpp:373-402): its receptors and transmitter are never read
+        if (y.type != BNC_SYN_CHEMICAL) return 0;
         for (uint8_t j = 0; j < y.post_receptor_count; j++)
             if (host_plugin_registered(hn.post_rec(k, j).type)) {
                 if (report)
@@ -1160,21 +1164,56 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
             if (status[k] == 1) continue;
             if (status[k] != 0) return check_syn(k, true);
             const SynLite& y = hn.syn[k];
+            if (y.type != BNC_SYN_CHEMICAL) {   // a gap junction reads both segments' Ca2+
+                need_pre_ext = true;
+                syn_valid.push_back(k);
+                continue;
+            }
             if (y.pre_autoreceptor_count > 0 || y.RRP_max > 0.0f) need_pre_ext = true;
             if (y.delay > 0.0f) any_delay = true;
             nt_mask |= 1u << (y.post_receptor_count > 0 ? nt_from_receptor(hn.post_rec(k, 0).type) : 0);
             syn_valid.push_back(k);
         }
     }
+    // The synapse kernel's entries: each chemical synapse once, for its post segment;
+    // each gap junction twice, for its pre segment (side 2) and then its post segment
+    // (side 1), since the reference's loop changes both segments' I_buffer
+    // (simulation_host.cpp:373-402).  Entries are kept in original synapse order per
+    // owning segment.
+    std::vector<uint8_t> ent_side;
+    {
+        bool any_gap = false;
+        for (uint32_t k : syn_valid) if (hn.syn[k].type != BNC_SYN_CHEMICAL) { any_gap = true; break; }
+        if (any_gap) {
+            std::vector<uint32_t> ent;
+            ent.reserve(syn_valid.size() + 64);
+            for (uint32_t k : syn_valid) {
+                if (hn.syn[k].type != BNC_SYN_CHEMICAL) { ent.push_back(k); ent_side.push_back(2); }
+                ent.push_back(k);
+                ent_side.push_back(hn.syn[k].type != BNC_SYN_CHEMICAL ? 1 : 0);
+            }
+            syn_valid.swap(ent);
+        }
+    }
+    auto owner = [&](uint32_t q) {   // device segment of entry q
+        const SynLite& y = hn.syn[syn_valid[q]];
+        return host->inv[(!ent_side.empty() && ent_side[q] == 2) ? y.pre_segment : y.post_segment];
+    };
     const uint32_t K = (uint32_t)syn_valid.size();
     std::vector<uint32_t> post_off(n + 1, 0);
-    for (uint32_t k : syn_valid) post_off[host->inv[hn.syn[k].post_segment] + 1]++;
+    for (uint32_t q = 0; q < K; q++) post_off[owner(q) + 1]++;
     for (uint32_t i = 0; i < n; i++) post_off[i + 1] += post_off[i];
-    {   // stable counting sort by postsynaptic device segment (original order within a post)
+    {   // stable counting sort by owning device segment (original order within a segment)
         std::vector<uint32_t> pos(post_off.begin(), post_off.end() - 1);
         std::vector<uint32_t> sorted(K);
-        for (uint32_t k : syn_valid) sorted[pos[host->inv[hn.syn[k].post_segment]]++] = k;
+        std::vector<uint8_t> sorted_side(ent_side.size());
+        for (uint32_t q = 0; q < K; q++) {
+            const uint32_t at = pos[owner(q)]++;
+            sorted[at] = syn_valid[q];
+            if (!ent_side.empty()) sorted_side[at] = ent_side[q];
+        }
         syn_valid.swap(sorted);
+        ent_side.swap(sorted_side);
     }
     // ---- synapse-kernel threads and the sliced synapse order ----
     // Thread t of the synapse kernel handles segment th_seg[t]: first every segment
@@ -1247,6 +1286,11 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
         std::vector<uint32_t> sliced(K);
         for (uint32_t q = 0; q < K; q++) sliced[q] = syn_valid[slot_syn[q]];
         syn_valid.swap(sliced);
+        if (!ent_side.empty()) {
+            std::vector<uint8_t> sliced_side(K);
+            for (uint32_t q = 0; q < K; q++) sliced_side[q] = ent_side[slot_syn[q]];
+            ent_side.swap(sliced_side);
+        }
     }
     std::vector<uint32_t> sy_pre(K), sy_id(K);
     std::vector<uint8_t> rc_cnt(K, 0), kept((size_t)K * 8, 0);
@@ -1333,6 +1377,57 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
             for (uint32_t q = 0; q < K; q++) sy_cleft_ecb[q] = hn.syn[syn_valid[q]].cleft_neurotransmitter[9];
         }
     }
+    // gap junctions (simulation_host.cpp:373-402, run_tick_common.h:79-122)
+    std::vector<uint32_t> sy_gj, gj_pre, gj_post, seg_cx;
+    std::vector<float> gj_delay, gj_dep, gj_flt;
+    host->gj_syn.clear();
+    if (!ent_side.empty()) {
+        std::vector<uint32_t>& gap_list = host->gj_syn;   // original indices, ascending
+        for (uint32_t q = 0; q < K; q++) if (ent_side[q] == 1) gap_list.push_back(syn_valid[q]);
+        std::sort(gap_list.begin(), gap_list.end());
+        std::vector<uint32_t> gidx(hn.syn.size(), UINT32_MAX);
+        for (uint32_t g = 0; g < gap_list.size(); g++) gidx[gap_list[g]] = g;
+        sy_gj.assign(K, UINT32_MAX);
+        for (uint32_t q = 0; q < K; q++)
+            if (ent_side[q]) sy_gj[q] = gidx[syn_valid[q]] | (ent_side[q] == 2 ? 0x80000000u : 0u);
+        // The junction reads both segments' Ca2+ as the loop has left it at its
+        // position; the kernel reads it as step 3 began, which is the same while no
+        // earlier synapse onto either segment carries an NMDA receptor (the only
+        // Ca2+-permeable receptor; a myelinated post segment skips it).
+        std::vector<uint32_t> first_nmda(n, UINT32_MAX);
+        for (uint32_t k = 0; k < hn.syn.size(); k++) {
+            const SynLite& y = hn.syn[k];
+            if (y.type != BNC_SYN_CHEMICAL || y.pre_segment >= n || y.post_segment >= n) continue;
+            if (sflags[y.post_segment] & SF_MYELIN) continue;
+            for (uint8_t j = 0; j < y.post_receptor_count; j++)
+                if (hn.post_rec(k, j).type == 9) { first_nmda[y.post_segment] = std::min(first_nmda[y.post_segment], k); break; }
+        }
+        for (uint32_t k : gap_list) {
+            const SynLite& y = hn.syn[k];
+            if (first_nmda[y.pre_segment] < k || first_nmda[y.post_segment] < k) {
+                set_error("gap junction %u: an earlier synapse onto one of its segments has an NMDA receptor, whose "
+                          "Ca2+ the junction would read mid-step", k);
+                return BNC_ERR_UNSUPPORTED;
+            }
+            gj_pre.push_back(host->inv[y.pre_segment]);
+            gj_post.push_back(host->inv[y.post_segment]);
+            gj_delay.push_back(y.delay);
+            gj_dep.push_back(y.depression);
+            gj_flt.push_back(y.cleft_neurotransmitter[0]);
+        }
+        // each segment's connexin-36 and connexin-43 items (at most one of each)
+        seg_cx.assign((size_t)2 * n, UINT32_MAX);
+        for (uint32_t q = 0; q < NI; q++) {
+            const uint8_t t = (uint8_t)(it_tf[q] & 0xFFu);
+            if (t != 114 && t != 198) continue;
+            const size_t at = (size_t)(t == 198 ? 1 : 0) * n + host->inv[host->item_seg[q]];
+            if (seg_cx[at] != UINT32_MAX) {
+                set_error("segment %u holds two connexin-%d modifiers", host->item_seg[q], t == 198 ? 43 : 36);
+                return BNC_ERR_UNSUPPORTED;
+            }
+            seg_cx[at] = q;
+        }
+    }
     // glia (simulation_host.cpp:351-355, 467-487): the first 256 segments with a GLAST
     // transporter; each synapse gives its capture to the one nearest its post segment in z
     std::vector<uint32_t> gl_seg, gl_off, gl_syn;
@@ -1345,7 +1440,7 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
             std::vector<int32_t> near(n, -1);
             for (uint32_t g : glia) near[g] = -2;
             for (uint32_t q = 0; q < K; q++)
-                if (near[hn.syn[syn_valid[q]].post_segment] == -2) {
+                if ((ent_side.empty() || ent_side[q] == 0) && near[hn.syn[syn_valid[q]].post_segment] == -2) {
                     // its own synapses' transmitter and the captures would interleave
                     set_error("synapse %u targets glial segment %u (a segment with a GLAST transporter)",
                               syn_valid[q], hn.syn[syn_valid[q]].post_segment);
@@ -1357,6 +1452,7 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
             std::vector<uint32_t> of(K);
             gl_off.assign(glia.size() + 1, 0);
             for (uint32_t q = 0; q < K; q++) {
+                if (!ent_side.empty() && ent_side[q] != 0) { of[q] = UINT32_MAX; continue; }   // a gap junction
                 const uint32_t post = hn.syn[syn_valid[q]].post_segment;
                 if (near[post] < 0) {
                     float best_dz = 1e30f;
@@ -1371,9 +1467,10 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
                 gl_off[of[q] + 1]++;
             }
             for (size_t gi = 0; gi < glia.size(); gi++) gl_off[gi + 1] += gl_off[gi];
-            gl_syn.resize(K);
+            gl_syn.resize(gl_off.back());
             std::vector<uint32_t> pos(gl_off.begin(), gl_off.end() - 1);
-            for (uint32_t q : order) gl_syn[pos[of[q]]++] = q;   // original synapse order per glial segment
+            for (uint32_t q : order)   // original synapse order per glial segment
+                if (of[q] != UINT32_MAX) gl_syn[pos[of[q]]++] = q;
             for (uint32_t g : glia) gl_seg.push_back(host->inv[g]);
         }
     }
@@ -1608,6 +1705,18 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
         dev->rc_av = up(allocs, rc_av, &rc);
         dev->rc_den = up(allocs, rc_den, &rc);
         dev->rc_st = up(allocs, rc_st, &rc);
+        if (!sy_gj.empty()) {
+            dev->sy_gj = up(allocs, sy_gj, &rc);
+            dev->gj_pre = up(allocs, gj_pre, &rc);
+            dev->gj_post = up(allocs, gj_post, &rc);
+            dev->gj_delay = up(allocs, gj_delay, &rc);
+            dev->gj_dep = up(allocs, gj_dep, &rc);
+            dev->gj_dep_new = up(allocs, gj_dep, &rc);
+            dev->gj_flt = up(allocs, gj_flt, &rc);
+            dev->gj_flt_new = up(allocs, gj_flt, &rc);
+            dev->seg_cx = up(allocs, seg_cx, &rc);
+            dev->n_gj = (uint32_t)gj_pre.size();
+        }
         if (!gl_seg.empty()) {
             dev->gl_cap = zeros<float>(allocs, K, &rc);
             dev->gl_seg = up(allocs, gl_seg, &rc);

@@ -122,6 +122,8 @@ __device__ __forceinline__ double run_item(uint8_t type, DMod& m, SegRec* r, flo
         BNC_ITEM(200, dp_cav31_current<kDef>(m, s, dt))
         BNC_ITEM(86, dp_ecb_synthesis_current<kDef>(m, s, dt))
         BNC_ITEM(147, dp_glast_current(m, s, dt, glu))
+        BNC_ITEM(114, dp_connexin_current<kDef>(m, s, dt))
+        BNC_ITEM(198, dp_connexin_current<kDef>(m, s, dt))
 #undef BNC_ITEM
         default: break;
     }
@@ -206,6 +208,8 @@ __device__ __forceinline__ double run_item_s(uint8_t type, DMod& m, DSeg& s, flo
         BNC_ITEM(200, dp_cav31_current<kDef>(m, s, dt))
         BNC_ITEM(86, dp_ecb_synthesis_current<kDef>(m, s, dt))
         BNC_ITEM(147, dp_glast_current(m, s, dt, glu))
+        BNC_ITEM(114, dp_connexin_current<kDef>(m, s, dt))
+        BNC_ITEM(198, dp_connexin_current<kDef>(m, s, dt))
 #undef BNC_ITEM
         default: break;
     }
@@ -286,6 +290,7 @@ static void fill_mask_tables(uint8_t* dyn, uint8_t* par) {
     dyn[1] = 0x03; par[1] = 0x1C;
     dyn[8] = 0x03; dyn[9] = 0x05; dyn[11] = 0x03; dyn[12] = 0x03;
     dyn[86] = 0x01; par[86] = 0x06;
+    dyn[114] = dyn[198] = 0x13; par[114] = par[198] = 0x6C;
     dyn[85] = 0x0B; par[85] = 0x34;
     par[98] = 0x06; par[100] = 0x06;
     dyn[102] = 0x02; par[102] = 0x1D;

@@ -175,6 +175,22 @@ struct NetDev {
     // Glia (gl_cap null when no segment has a GLAST transporter): the first 256 such
     // segments, each with the sliced synapses whose post segment is nearest to it in
     // z, in original synapse order; gl_cap holds each synapse's capture of the tick
+    // Gap junctions (sy_gj null when the network has none): per entry of the synapse
+    // kernel the junction it is a side of (bit 31: the pre side), UINT32_MAX for a
+    // chemical synapse; per junction its segments, delay (the filter's time constant),
+    // slow gate and filtered current as the tick began (gj_dep, gj_flt) and as the
+    // post side leaves them (gj_dep_new, gj_flt_new, copied back after step 3); per
+    // segment the items of its connexin-36 and connexin-43 ([2][n_seg], UINT32_MAX)
+    uint32_t* sy_gj;
+    uint32_t* gj_pre;
+    uint32_t* gj_post;
+    float* gj_delay;
+    float* gj_dep;
+    float* gj_dep_new;
+    float* gj_flt;
+    float* gj_flt_new;
+    uint32_t* seg_cx;
+    uint32_t n_gj;
     float* gl_cap;            // [n_syn]
     uint32_t* gl_seg;         // [n_glia] device segment
     uint32_t* gl_off;         // [n_glia + 1]
@@ -263,6 +279,7 @@ struct NetHost {
     std::vector<uint8_t> syn_nt;     // released NT per device synapse
     std::vector<uint32_t> md_syn;    // release modulator -> original synapse index
     std::vector<uint8_t> md_slot;    // release modulator -> autoreceptor slot
+    std::vector<uint32_t> gj_syn;    // gap junction -> original synapse index
     uint32_t max_tile_segs = 0, max_tile_edges = 0;
     uint32_t max_tile_stride = 0;            // own + ghost segments of the largest tile
     uint32_t cluster = 1;                    // CTAs per diffusion cluster (2: tiles in pairs)

@@ -1015,6 +1015,35 @@ __device__ __forceinline__ double dp_ecb_synthesis_current(DMod& m, DSeg& s, flo
     return 0.0;
 }
 
+/* hh_biological.cpp:3266-3308 (connexin-36) and 3310-3350 (connexin-43), the same
+ * steps: connexon turnover, phosphorylation toward the CaMKII drive (0: CaMKII is not
+ * a supported modifier) and the cAMP drive in state[6], P_open from phosphorylation
+ * and pH.  No current; gap junctions read state[0] and state[4]. */
+template <bool kDef>
+__device__ __forceinline__ double dp_connexin_current(DMod& m, DSeg& s, float dt) {
+    (void)s;
+    double synth_rate = ((kDef ? 0.0 : ((double)m.st[2])) > 0.0f) ? (kDef ? 0.0 : ((double)m.st[2])) : (double)0.001f;
+    double degrad_rate = ((kDef ? 0.0 : ((double)m.st[3])) > 0.0f) ? (kDef ? 0.0 : ((double)m.st[3])) : (double)0.0005f;
+    double pH = ((kDef ? 0.0 : ((double)m.st[5])) > 4.0f) ? (kDef ? 0.0 : ((double)m.st[5])) : (double)7.2f;
+    m.st[0] = (float)((double)m.st[0] + (synth_rate - degrad_rate * (double)m.st[0]) * (double)dt / (double)3600000.0f);
+    if (m.st[0] < 0.0f) m.st[0] = 0.0f;
+    if (m.st[0] > 1.0f) m.st[0] = 1.0f;
+    float camkii_act = 0.0f;
+    double pka_drive = kDef ? 0.0 : (double)m.st[6];
+    float p_target = (float)((double)(camkii_act * 0.6f) + pka_drive * (double)0.3f);
+    m.st[1] = (float)((double)m.st[1] + ((double)p_target - (double)m.st[1]) * (double)dt / (double)5000.0f);
+    if (m.st[1] < 0.0f) m.st[1] = 0.0f;
+    if (m.st[1] > 1.0f) m.st[1] = 1.0f;
+    float pH_factor = (pH < 6.8f) ? (float)((pH - (double)6.0f) / (double)0.8f) : 1.0f;
+    if (pH_factor < 0.0f) pH_factor = 0.0f;
+    double camkii_P_open = 1.0f - (double)m.st[1] * (double)0.5f;
+    double pka_P_open = 1.0f + (double)m.st[1] * (double)0.3f;
+    m.st[4] = (float)((camkii_P_open * (double)0.5f + pka_P_open * (double)0.5f) * (double)pH_factor);
+    if (m.st[4] < 0.05f) m.st[4] = 0.05f;
+    if (m.st[4] > 2.0f) m.st[4] = 2.0f;
+    return 0.0;
+}
+
 /* hh_biological.cpp:725-733 (GLAST, glial glutamate transporter) through
  * glial_nt_uptake_current (modifier_helpers.h:418-454): 3 Na+ in, 1 K+ out, net +2,
  * glutamate taken from the segment's own neurotransmitter pool `glu`, which the

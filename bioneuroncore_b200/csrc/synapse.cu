@@ -28,6 +28,53 @@ __device__ __forceinline__ float xorshift32_rnd(uint32_t seed) {
     return (float)(x & 0x7FFFFFFFu) / (float)0x7FFFFFFFu;
 }
 
+// run_tick_common.h:114-122: the slow Ca2+/calmodulin gate of a gap junction
+__device__ __forceinline__ float gj_cam_update(float m_slow, float ca_pre, float ca_post, float dt) {
+    float ca_avg = 0.5f * (ca_pre + ca_post);
+    float cam_act = (ca_avg * ca_avg) / (ca_avg * ca_avg + 0.0003f * 0.0003f);
+    m_slow += (cam_act - m_slow) * dt / 100.0f;
+    if (m_slow < 0.0f) m_slow = 0.0f;
+    if (m_slow > 1.0f) m_slow = 1.0f;
+    return m_slow;
+}
+
+// run_tick_common.h:79-110: the junction's conductance (nS) from the connexin-36 and
+// connexin-43 items of both segments (density from the pre segment's), Cx43's Vj gate
+// and the slow gate
+__device__ __forceinline__ float gj_g_eff(const NetDev& d, uint32_t gp, uint32_t gq, float m_slow, float Vj) {
+    const uint32_t N = d.n_seg, NI = d.n_items;
+    float g_gap_ps = 0.0f;
+    for (int cx = 0; cx < 2; cx++) {
+        const float gamma = cx == 0 ? 14.0f : 100.0f;
+        float density = 0.0f;
+        float f = 1.0f;
+        const uint32_t qp = d.seg_cx[(size_t)cx * N + gp];
+        if (qp != UINT32_MAX) {
+            density = d.it_den[qp];
+            f = (float)((double)f * ((double)d.it_st[qp] * (double)d.it_st[(size_t)4 * NI + qp]));
+        }
+        const uint32_t qq = d.seg_cx[(size_t)cx * N + gq];
+        if (qq != UINT32_MAX) f = (float)((double)f * ((double)d.it_st[qq] * (double)d.it_st[(size_t)4 * NI + qq]));
+        if (cx == 1) {
+            const float vj_abs = Vj < 0.0f ? -Vj : Vj;
+            const float f_vj = (float)(1.0f / (1.0f + dm_exp((double)((vj_abs - 40.0f) / 5.0f))));
+            f *= f_vj;
+        }
+        if (f < 0.01f) f = 0.01f;
+        g_gap_ps += density * f * gamma;
+    }
+    return g_gap_ps * 1e-3f * (1.0f - m_slow);
+}
+
+// After step 3: the junctions' state as the post sides left it becomes the next
+// tick's starting state.
+__global__ void k_gj_commit(NetDev d) {
+    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < d.n_gj; g += gridDim.x * blockDim.x) {
+        d.gj_dep[g] = d.gj_dep_new[g];
+        d.gj_flt[g] = d.gj_flt_new[g];
+    }
+}
+
 __device__ __forceinline__ void log_release(const NetDev& d, uint32_t k, unsigned long long tick, float amt,
                                          uint32_t slot) {
     const uint32_t at = atomicAdd(d.ev_n, 1u);
@@ -84,11 +131,14 @@ k_synapse(NetDev d, float dt, unsigned long long tick, int first_tick) {
         const bool act = cnt > kk;
         const uint32_t n_act = __popc(__ballot_sync(0xFFFFFFFFu, act));
         const uint32_t k = base + lane;   // this lane's synapse in the slice (when act)
+        // a gap junction's side (simulation_host.cpp:373-402) or a chemical synapse
+        const uint32_t gjv = (act && d.sy_gj) ? d.sy_gj[k] : UINT32_MAX;
+        const bool chem = act && gjv == UINT32_MAX;
         float cleft = 0.0f, cleft_e = 0.0f, rrp = 0.0f, rrp_max = 0.0f, bouton = 0.0f;
         uint8_t refr = 0, sf = 0;
         int ntt = 0;
         uint32_t n_rc = 0;
-        if (act) {
+        if (chem) {
             const uint32_t pre = d.sy_pre[k];
             const float4 pr = d.pre_rec[pre];
             sf = d.sy_flags[k];
@@ -259,7 +309,33 @@ k_synapse(NetDev d, float dt, unsigned long long tick, int first_tick) {
             }
             rbase += __popc(has);
         }
-        if (act) {
+        if (act && gjv != UINT32_MAX) {
+            // gap junction (simulation_host.cpp:373-402): both sides compute the same
+            // current from the segments' state as step 3 began (V is constant through
+            // step 3, and the builder refuses networks where an earlier synapse could
+            // move either segment's Ca2+); the post side records the junction's state
+            const uint32_t g = gjv & 0x7FFFFFFFu;
+            const uint32_t gp = d.gj_pre[g], gq = d.gj_post[g];
+            const float Vj = (float)((double)d.pre_rec[gp].x - (double)d.pre_rec[gq].x);
+            const float m_slow = gj_cam_update(d.gj_dep[g], d.pre_ext[gp].z, d.pre_ext[gq].z, dt);
+            const float g_eff = gj_g_eff(d, gp, gq, m_slow, Vj);
+            const float I_gap_raw = g_eff * Vj;
+            const float delay = d.gj_delay[g];
+            float I = I_gap_raw;
+            if (delay > 0.001f) {
+                float I_filtered = d.gj_flt[g];
+                I_filtered += (I_gap_raw - I_filtered) * dt / delay;
+                I = I_filtered;
+            }
+            if (gjv >> 31) {
+                ib -= I;
+            } else {
+                ib += I;
+                d.gj_dep_new[g] = m_slow;
+                if (delay > 0.001f) d.gj_flt_new[g] = I;
+            }
+        }
+        if (chem) {
             ib += I_syn;
             // spine Ca2+ (modifier_helpers.h:808-817)
             float spine = d.sy_spine[k];
@@ -414,6 +490,7 @@ cudaError_t launch_synapse(const NetDev& dev, float dt, unsigned long long tick,
                            cudaStream_t stream) {
     k_synapse<<<(dev.n_seg + 255) / 256, 256, 0, stream>>>(dev, dt, tick, first_tick);
     if (dev.gl_cap) k_glia<<<(dev.n_glia + 127) / 128, 128, 0, stream>>>(dev);
+    if (dev.sy_gj) k_gj_commit<<<(dev.n_gj + 255) / 256 < 1184 ? (dev.n_gj + 255) / 256 : 1184, 256, 0, stream>>>(dev);
     return cudaGetLastError();
 }
 

@@ -233,8 +233,10 @@ int bnc_set_records_residency(void* sim, int on_host);
  *   4 temperature, 5 transcription, 6 intra_nt[index], 7 neurotransmitter[index],
  *   8 modifier state (index = slot*8 + k), 9 spike count (V crossing -40 mV upward).
  * Synapse fields: 0 bouton_Ca, 1 spine_Ca, 2 weight, 3 refractory,
- *   4 cleft_neurotransmitter[index], 5 receptor state (index = j*8 + k),
- *   6 facilitation, 7 spine_camkii, 8 spine_calcineurin, 9 RRP. */
+ *   4 cleft_neurotransmitter[index] (a gap junction's entry 0: its filtered current),
+ *   5 receptor state (index = j*8 + k), 6 facilitation, 7 spine_camkii,
+ *   8 spine_calcineurin, 9 RRP, 10 depression (a gap junction's slow gate),
+ *   11 autoreceptor state (index = j*8, word 0 of release modulators). */
 int bnc_read_segment_field(void* sim, int field, int index, float* out, uint32_t n);
 int bnc_read_synapse_field(void* sim, int field, int index, float* out, uint32_t n);
 

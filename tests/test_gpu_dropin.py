@@ -139,6 +139,9 @@ def _compare(seg, syn, ora, full, label):
                 _eq(np.where(has, syn["post_receptors"][:, j]["state"][:, k], 0.0),
                     np.where(has, ora.synapse_field("receptor_state", j * 8 + k), 0.0),
                     "%s receptor %d state %d" % (label, j, k))
+        gap = syn["type"] > 0
+        if gap.any():   # gap junctions: the slow gate and the filtered current
+            _eq(syn["depression"][gap], ora.synapse_field("depression")[gap], "%s gap slow gate" % label)
         for j in range(int(syn["pre_autoreceptor_count"].max())):   # release modulators' state[0]
             types = np.where(syn["pre_autoreceptor_count"] > j, syn["pre_autoreceptors"][:, j]["type"], 0)
             mod = np.isin(types, [13, 18, 19, 22, 27, 29, 30, 35, 36, 38, 44, 46])
@@ -155,17 +158,17 @@ def _rel(a, b, floor):
 
 @pytest.mark.parametrize("family,on_host", [("large", 0), ("large", 1), ("extras", 0), ("modulators", 0),
                                            ("modulators", 1), ("ecb", 0), ("ecb", 1),
-                                           ("glia", 0)])
+                                           ("glia", 0), ("gaps", 0), ("gaps", 1)])
 def test_dropin_sequence_equals_the_oracle(tmp_path, family, on_host):
     """on_host: the records moved to plain host memory and updated by the host export
     (bnc_set_records_residency), instead of managed memory written on the device."""
     from bioneuroncore_b200 import (Backend, Network, NetgenParams, NET_LARGE, NET_SMALL, NETGEN_SYNAPSE_EXTRAS,
-                                    NETGEN_RELEASE_MODULATORS, NETGEN_ECB, NETGEN_GLIA)
+                                    NETGEN_RELEASE_MODULATORS, NETGEN_ECB, NETGEN_GLIA, NETGEN_GAP_JUNCTIONS)
     if family == "large":
         p = NetgenParams(family=NET_LARGE, n_neurons=12, seed=3)
     else:
         flags = NETGEN_SYNAPSE_EXTRAS | {"modulators": NETGEN_RELEASE_MODULATORS, "ecb": NETGEN_ECB,
-                                         "glia": NETGEN_GLIA}.get(family, 0)
+                                         "glia": NETGEN_GLIA, "gaps": NETGEN_GAP_JUNCTIONS}.get(family, 0)
         p = NetgenParams(family=NET_SMALL, n_neurons=16, seed=6, flags=flags, stim_pA=3000.0)
     net = Network(p)
     path = tmp_path / "net.bion"

@@ -169,3 +169,23 @@ def test_glial_capture_bitexact():
                      stim_pA=3000.0)
     log, net = _run(p, 1000, 100)
     assert len(log) > 0
+
+
+def test_gap_junctions_bitexact():
+    """Electrical synapses and dendritic bridges between somata, spread among the
+    chemical synapses: connexin items, the slow gate, Cx43's Vj gate, the filtered
+    current of delayed junctions, both segments' I_buffer in synapse order; 1,000 ticks
+    equal the oracle's bit for bit, the junctions' gate and filter included."""
+    from bioneuroncore_b200 import NetgenParams, NET_SMALL, NETGEN_GAP_JUNCTIONS
+    p = NetgenParams(family=NET_SMALL, n_neurons=16, seed=6, flags=NETGEN_GAP_JUNCTIONS, stim_pA=3000.0)
+    ora, gpu, net = _pair(p)
+    n_syn = net.data.num_synapses
+    gap = net.synapses["type"] > 0
+    assert gap.sum() == 15
+    for t in range(10):
+        ora.run(100, DT)
+        gpu.run_ticks(100, DT)
+        _compare_everything(ora, gpu, net, "tick %d" % (100 * (t + 1)))
+        _same(gpu.synapse_field("depression", 0, n_syn)[gap], ora.synapse_field("depression", 0)[gap],
+              "tick %d gap slow gate" % (100 * (t + 1)))
+    assert (ora.synapse_field("depression", 0)[gap] > 0).all()

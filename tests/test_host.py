@@ -146,10 +146,29 @@ def test_user_plugin_type_is_rejected():
     assert last_error()
 
 
-def test_electrical_synapse_is_rejected():
-    net = _net(family=1, n_neurons=4, seed=5)
-    net.synapses["type"][0] = 1
-    assert _plan_aos(net)[0] == BNC_ERR_UNSUPPORTED
+def test_gap_junction_rules():
+    """Electrical synapses and dendritic bridges are accepted; a junction whose segment
+    an earlier synapse with an NMDA receptor targets (its Ca2+ would move before the
+    junction reads it), a segment with two connexin-36, and synapse types above 2 are
+    refused."""
+    from bioneuroncore_b200 import NETGEN_GAP_JUNCTIONS, last_error
+    net = _net(family=1, n_neurons=4, seed=5, flags=NETGEN_GAP_JUNCTIONS)
+    syn = net.synapses
+    assert (syn["type"] > 0).sum() == 3 and _plan_aos(net)[0] == 0
+    g = int(np.flatnonzero(syn["type"] > 0)[-1])
+    k = int(np.flatnonzero(syn["type"][:g] == 0)[0])
+    syn["post_segment"][k] = syn["post_segment"][g]
+    syn["post_receptors"][k, 0]["type"] = 9                      # NMDA onto the junction's segment, earlier
+    assert _plan_aos(net)[0] == BNC_ERR_UNSUPPORTED and "NMDA" in last_error()
+    net2 = _net(family=1, n_neurons=4, seed=5, flags=NETGEN_GAP_JUNCTIONS)
+    seg = net2.segments
+    c = int(seg["modifier_count"][0])
+    seg["modifiers"][0, c] = seg["modifiers"][0, int(np.flatnonzero(seg["modifiers"][0]["type"] == 114)[0])]
+    seg["modifier_count"][0] = c + 1
+    assert _plan_aos(net2)[0] == BNC_ERR_UNSUPPORTED and "connexin" in last_error()
+    net3 = _net(family=1, n_neurons=4, seed=5)
+    net3.synapses["type"][0] = 3
+    assert _plan_aos(net3)[0] == BNC_ERR_UNSUPPORTED
 
 
 def test_modifier_count_out_of_range_is_a_format_error():
