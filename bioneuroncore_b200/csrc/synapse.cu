@@ -81,6 +81,9 @@ __device__ __forceinline__ void log_release(const NetDev& d, uint32_t k, unsigne
     if (at < d.ev_cap) d.ev_buf[at] = make_uint4(k, (uint32_t)tick, __float_as_uint(amt), slot);
 }
 
+// kX: the network has release modulators, eCB, glia or gap junctions; the plain
+// instantiation leaves their code (and registers) out.
+template <bool kX>
 __global__ void __launch_bounds__(256, 4)
 k_synapse(NetDev d, float dt, unsigned long long tick, int first_tick) {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -103,7 +106,7 @@ k_synapse(NetDev d, float dt, unsigned long long tick, int first_tick) {
     float nt_gaba = 0.0f, nt_gly = 0.0f, nt_ecb = 0.0f;
     // the segment's eCB-synthesis modifier (its first), whose state[0] each of its
     // synapses draws on in order (simulation_host.cpp:578-589)
-    const uint32_t ecb_q = (valid && d.seg_ecb_item) ? d.seg_ecb_item[i] : UINT32_MAX;
+    const uint32_t ecb_q = (kX && valid && d.seg_ecb_item) ? d.seg_ecb_item[i] : UINT32_MAX;
     float ecb_st = ecb_q != UINT32_MAX ? d.it_st[ecb_q] : 0.0f;
     double ib = valid ? d.ibuf[i] : 0.0;
     DSeg s;
@@ -132,7 +135,7 @@ k_synapse(NetDev d, float dt, unsigned long long tick, int first_tick) {
         const uint32_t n_act = __popc(__ballot_sync(0xFFFFFFFFu, act));
         const uint32_t k = base + lane;   // this lane's synapse in the slice (when act)
         // a gap junction's side (simulation_host.cpp:373-402) or a chemical synapse
-        const uint32_t gjv = (act && d.sy_gj) ? d.sy_gj[k] : UINT32_MAX;
+        const uint32_t gjv = (kX && act && d.sy_gj) ? d.sy_gj[k] : UINT32_MAX;
         const bool chem = act && gjv == UINT32_MAX;
         float cleft = 0.0f, cleft_e = 0.0f, rrp = 0.0f, rrp_max = 0.0f, bouton = 0.0f;
         uint8_t refr = 0, sf = 0;
@@ -144,7 +147,7 @@ k_synapse(NetDev d, float dt, unsigned long long tick, int first_tick) {
             sf = d.sy_flags[k];
             ntt = sf >> 4;
             cleft = d.sy_cleft[k];
-            if (d.sy_cleft_ecb) cleft_e = d.sy_cleft_ecb[k];
+            if (kX && d.sy_cleft_ecb) cleft_e = d.sy_cleft_ecb[k];
             const float delay = d.sy_delay[k];
             // delayed releases (delay_buffer.h:31-44)
             if ((d.flags & NF_DELAY) && delay > 0.0f) {
@@ -209,7 +212,7 @@ k_synapse(NetDev d, float dt, unsigned long long tick, int first_tick) {
                 // release modulators of the autoreceptors, in autoreceptor order
                 // (kernel_dispatch.h:575-604, receptors_biological.cpp:428-509); the
                 // bouton channels take the dispatch's default factor 1
-                if (d.md_off) {
+                if (kX && d.md_off) {
                     const uint32_t m1 = d.md_off[k + 1];
                     for (uint32_t mi = d.md_off[k]; mi < m1; mi++) {
                         const uint32_t code = d.md_code[mi];
@@ -267,11 +270,11 @@ k_synapse(NetDev d, float dt, unsigned long long tick, int first_tick) {
             if (ntt == 0) nt_glu += cleft;
             else if (ntt == 1) nt_gaba += cleft;
             else nt_gly += cleft;
-            nt_ecb += cleft_e;
+            if (kX) nt_ecb += cleft_e;
             // glial capture (simulation_host.cpp:467-487): a share of the transmitter
             // goes to the glial segment nearest the post segment in z; k_glia adds the
             // shares to the glial segments in synapse order
-            if (d.gl_cap) {
+            if (kX && d.gl_cap) {
                 float cap = 0.0f;
                 if (cleft > 0.0f) {
                     const float tau = d.sy_tauc[k] > 0.0f ? d.sy_tauc[k] : 5.0f;
@@ -349,12 +352,14 @@ k_synapse(NetDev d, float dt, unsigned long long tick, int first_tick) {
             }
             // clearance (simulation_host.cpp:505-510)
             const auto clear_f = dm_exp(-dt / d.sy_tauc[k]);
-            if (!d.gl_cap) {   // with glia, they take glutamate, GABA and glycine instead
+            if (!kX || !d.gl_cap) {   // with glia, they take glutamate, GABA and glycine instead
                 cleft *= clear_f;
                 if (cleft < 0.0f) cleft = 0.0f;
             }
-            cleft_e *= clear_f;
-            if (cleft_e < 0.0f) cleft_e = 0.0f;
+            if (kX) {
+                cleft_e *= clear_f;
+                if (cleft_e < 0.0f) cleft_e = 0.0f;
+            }
             // BCM threshold, spine CaMKII/calcineurin, weight (simulation_host.cpp:527-576)
             float facil = d.sy_facil[k];
             {
@@ -400,7 +405,7 @@ k_synapse(NetDev d, float dt, unsigned long long tick, int first_tick) {
             }
             if (refr > 0) refr--;
             d.sy_cleft[k] = cleft;
-            if (d.sy_cleft_ecb) d.sy_cleft_ecb[k] = cleft_e;
+            if (kX && d.sy_cleft_ecb) d.sy_cleft_ecb[k] = cleft_e;
             d.sy_refr[k] = refr;
             d.sy_bouton[k] = bouton;
             d.sy_spine[k] = spine;
@@ -488,7 +493,9 @@ __global__ void k_glia(NetDev d) {
 
 cudaError_t launch_synapse(const NetDev& dev, float dt, unsigned long long tick, int first_tick,
                            cudaStream_t stream) {
-    k_synapse<<<(dev.n_seg + 255) / 256, 256, 0, stream>>>(dev, dt, tick, first_tick);
+    const bool extras = dev.md_off || dev.sy_cleft_ecb || dev.gl_cap || dev.sy_gj;
+    if (extras) k_synapse<true><<<(dev.n_seg + 255) / 256, 256, 0, stream>>>(dev, dt, tick, first_tick);
+    else k_synapse<false><<<(dev.n_seg + 255) / 256, 256, 0, stream>>>(dev, dt, tick, first_tick);
     if (dev.gl_cap) k_glia<<<(dev.n_glia + 127) / 128, 128, 0, stream>>>(dev);
     if (dev.sy_gj) k_gj_commit<<<(dev.n_gj + 255) / 256 < 1184 ? (dev.n_gj + 255) / 256 : 1184, 256, 0, stream>>>(dev);
     return cudaGetLastError();
