@@ -1717,6 +1717,11 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
             dev->seg_cx = up(allocs, seg_cx, &rc);
             dev->n_gj = (uint32_t)gj_pre.size();
         }
+        dev->model_extras = 0;
+        for (uint32_t q = 0; q < NI && !dev->model_extras; q++) {
+            const uint8_t t = (uint8_t)(it_tf[q] & 0xFFu);
+            if (t == 86 || t == 114 || t == 147 || t == 198) dev->model_extras = 1;
+        }
         if (!gl_seg.empty()) {
             dev->gl_cap = zeros<float>(allocs, K, &rc);
             dev->gl_seg = up(allocs, gl_seg, &rc);

@@ -80,7 +80,7 @@ __device__ __forceinline__ void rec_store(const DSeg& s, float v0, SegRec* r) {
 // kernel_dispatch.h:337-570 restricted to the device-implemented types (the builder
 // rejects every other type; myelin, type 4, is never an item: it returns 0 and
 // touches nothing).
-template <bool kDef>
+template <bool kDef, bool kX>
 __device__ __forceinline__ double run_item(uint8_t type, DMod& m, SegRec* r, float dt, float& glu, float gaba,
                                            float gly) {
     double I = 0.0;
@@ -120,10 +120,11 @@ __device__ __forceinline__ double run_item(uint8_t type, DMod& m, SegRec* r, flo
         BNC_ITEM(142, dp_nav_current<kDef>(m, s, dt, 1))
         BNC_ITEM(150, dp_kv31_current<kDef>(m, s, dt))
         BNC_ITEM(200, dp_cav31_current<kDef>(m, s, dt))
-        BNC_ITEM(86, dp_ecb_synthesis_current<kDef>(m, s, dt))
-        BNC_ITEM(147, dp_glast_current(m, s, dt, glu))
-        BNC_ITEM(114, dp_connexin_current<kDef>(m, s, dt))
-        BNC_ITEM(198, dp_connexin_current<kDef>(m, s, dt))
+        // models only some networks carry: their code is in the kX instantiation alone
+        BNC_ITEM(86, kX ? dp_ecb_synthesis_current<kDef>(m, s, dt) : 0.0)
+        BNC_ITEM(147, kX ? dp_glast_current(m, s, dt, glu) : 0.0)
+        BNC_ITEM(114, kX ? dp_connexin_current<kDef>(m, s, dt) : 0.0)
+        BNC_ITEM(198, kX ? dp_connexin_current<kDef>(m, s, dt) : 0.0)
 #undef BNC_ITEM
         default: break;
     }
@@ -134,6 +135,7 @@ __device__ __forceinline__ double run_item(uint8_t type, DMod& m, SegRec* r, flo
 // the item's segment and slot).  Capped at 64 registers for 4 CTAs per SM: with the
 // 96-byte record the cap costs 16 bytes of spills and the extra warps hide more of the
 // record loads' latency (6.4M segments: 8.04 -> 7.80 ms per tick).
+template <bool kX>
 __global__ void __launch_bounds__(256, 4)
 k_phase(NetDev d, float dt, uint32_t b, uint32_t e) {
     const uint32_t q = b + blockIdx.x * blockDim.x + threadIdx.x;
@@ -153,14 +155,14 @@ k_phase(NetDev d, float dt, uint32_t b, uint32_t e) {
 #pragma unroll
     for (int k = 0; k < 7; k++) m.st[k] = ((rm >> k) & 1u) ? d.it_st[(size_t)k * NI + q] : 0.0f;
     float glu = 0.0f, gaba = 0.0f, gly = 0.0f;
-    if (type == 8 || type == 9 || type == 147) glu = d.nt[g];
+    if (type == 8 || type == 9 || (kX && type == 147)) glu = d.nt[g];
     else if (type == 11) gaba = d.nt[(size_t)1 * N + g];
     else if (type == 12) gly = d.nt[(size_t)7 * N + g];
     SegRec* r = d.rec + g;
-    const double I = ((fl & 3) == 0) ? run_item<true>(type, m, r, dt, glu, gaba, gly)
-                                     : run_item<false>(type, m, r, dt, glu, gaba, gly);
+    const double I = ((fl & 3) == 0) ? run_item<true, kX>(type, m, r, dt, glu, gaba, gly)
+                                     : run_item<false, kX>(type, m, r, dt, glu, gaba, gly);
     r->itot = r->itot + I;
-    if (type == 147) d.nt[g] = glu;   // the transporter's uptake
+    if (kX && type == 147) d.nt[g] = glu;   // the transporter's uptake
     const uint32_t wm = c_dyn_mask[type];
 #pragma unroll
     for (int k = 0; k < 7; k++) if ((wm >> k) & 1u) d.it_st[(size_t)k * NI + q] = m.st[k];
@@ -169,7 +171,7 @@ k_phase(NetDev d, float dt, uint32_t b, uint32_t e) {
 
 // run_item on a segment held in registers: the same models in the same order, the GHK
 // factors computed from the V the item starts with, as rec_load computes them.
-template <bool kDef>
+template <bool kDef, bool kX>
 __device__ __forceinline__ double run_item_s(uint8_t type, DMod& m, DSeg& s, float dt, float& glu, float gaba,
                                              float gly) {
     double I = 0.0;
@@ -206,10 +208,11 @@ __device__ __forceinline__ double run_item_s(uint8_t type, DMod& m, DSeg& s, flo
         BNC_ITEM(142, dp_nav_current<kDef>(m, s, dt, 1))
         BNC_ITEM(150, dp_kv31_current<kDef>(m, s, dt))
         BNC_ITEM(200, dp_cav31_current<kDef>(m, s, dt))
-        BNC_ITEM(86, dp_ecb_synthesis_current<kDef>(m, s, dt))
-        BNC_ITEM(147, dp_glast_current(m, s, dt, glu))
-        BNC_ITEM(114, dp_connexin_current<kDef>(m, s, dt))
-        BNC_ITEM(198, dp_connexin_current<kDef>(m, s, dt))
+        // models only some networks carry: their code is in the kX instantiation alone
+        BNC_ITEM(86, kX ? dp_ecb_synthesis_current<kDef>(m, s, dt) : 0.0)
+        BNC_ITEM(147, kX ? dp_glast_current(m, s, dt, glu) : 0.0)
+        BNC_ITEM(114, kX ? dp_connexin_current<kDef>(m, s, dt) : 0.0)
+        BNC_ITEM(198, kX ? dp_connexin_current<kDef>(m, s, dt) : 0.0)
 #undef BNC_ITEM
         default: break;
     }
@@ -230,6 +233,7 @@ struct PhaseGroup {
 // arithmetic of the one-launch-per-phase path, so the results are the same bits.
 // The builder orders rows by (item count, item types), so a warp runs one sequence of
 // models; it forms groups only when no registered device modifier is present.
+template <bool kX>
 __global__ void __launch_bounds__(256, BNC_GROUP_MIN_CTAS)
 k_phase_group(NetDev d, float dt, PhaseGroup grp) {
     const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
@@ -261,13 +265,13 @@ k_phase_group(NetDev d, float dt, PhaseGroup grp) {
 #pragma unroll
         for (int k = 0; k < 7; k++) m.st[k] = ((rm >> k) & 1u) ? d.it_st[(size_t)k * NI + qi] : 0.0f;
         float glu = 0.0f, gaba = 0.0f, gly = 0.0f;
-        if (type == 8 || type == 9 || type == 147) glu = d.nt[g];
+        if (type == 8 || type == 9 || (kX && type == 147)) glu = d.nt[g];
         else if (type == 11) gaba = d.nt[(size_t)1 * N + g];
         else if (type == 12) gly = d.nt[(size_t)7 * N + g];
-        const double I = ((fl & 3) == 0) ? run_item_s<true>(type, m, s, dt, glu, gaba, gly)
-                                         : run_item_s<false>(type, m, s, dt, glu, gaba, gly);
+        const double I = ((fl & 3) == 0) ? run_item_s<true, kX>(type, m, s, dt, glu, gaba, gly)
+                                         : run_item_s<false, kX>(type, m, s, dt, glu, gaba, gly);
         itot = itot + I;
-        if (type == 147) d.nt[g] = glu;   // the transporter's uptake
+        if (kX && type == 147) d.nt[g] = glu;   // the transporter's uptake
         const uint32_t wm = c_dyn_mask[type];
 #pragma unroll
         for (int k = 0; k < 7; k++) if ((wm >> k) & 1u) d.it_st[(size_t)k * NI + qi] = m.st[k];
@@ -354,15 +358,23 @@ static cudaError_t enqueue_modifiers(const NetDev& dev, const NetHost& host, flo
                 for (uint32_t j = 0; j <= kMaxFuse; j++) grp.off[j] = host.phase_off[std::min(p0 + j, p0 + grp.n)];
                 const uint32_t rows = grp.off[1] - grp.off[0];
                 if (rows == 0) continue;
-                if (grp.n == 1) k_phase<<<(rows + 255) / 256, 256, 0, stream>>>(dev, dt, grp.off[0], grp.off[1]);
-                else k_phase_group<<<(rows + 255) / 256, 256, 0, stream>>>(dev, dt, grp);
+                const dim3 gs((rows + 255) / 256);
+                if (grp.n == 1) {
+                    if (dev.model_extras) k_phase<true><<<gs, 256, 0, stream>>>(dev, dt, grp.off[0], grp.off[1]);
+                    else k_phase<false><<<gs, 256, 0, stream>>>(dev, dt, grp.off[0], grp.off[1]);
+                } else if (dev.model_extras) {
+                    k_phase_group<true><<<gs, 256, 0, stream>>>(dev, dt, grp);
+                } else {
+                    k_phase_group<false><<<gs, 256, 0, stream>>>(dev, dt, grp);
+                }
             }
             continue;
         }
         for (uint32_t p = 0; p < P; p++) {
             const uint32_t bk = c * P + p;
             const uint32_t b = host.phase_off[bk], e = host.phase_off[bk + 1];
-            if (e > b) k_phase<<<(e - b + 255) / 256, 256, 0, stream>>>(dev, dt, b, e);
+            if (e > b && dev.model_extras) k_phase<true><<<(e - b + 255) / 256, 256, 0, stream>>>(dev, dt, b, e);
+            else if (e > b) k_phase<false><<<(e - b + 255) / 256, 256, 0, stream>>>(dev, dt, b, e);
             // items of registered device modifiers in this bucket (k_phase skips them)
             for (; u < host.user_ranges.size() && host.user_ranges[u].bucket == bk; u++) {
                 const auto& ur = host.user_ranges[u];

@@ -196,6 +196,7 @@ struct NetDev {
     uint32_t* gl_off;         // [n_glia + 1]
     uint32_t* gl_syn;         // sliced synapse indices
     uint32_t n_glia;
+    uint32_t model_extras;    // 1: some item is eCB synthesis, GLAST or a connexin (86, 147, 114, 198)
     uint32_t* md_off;         // [n_syn + 1]
     uint8_t* md_code;         // kind << 4 | cleft NT index; kind 1 Gi/o, 2 Gs, 3 ionotropic
     double* md_scale;         // density x effective area (pre_area, or 1 when not positive)
