@@ -23,7 +23,7 @@ ORACLE_DIR = os.path.join(ROOT, "oracle")
 ORACLE_LIB = os.path.join(ORACLE_DIR, "liboracle.so")
 ORACLE64_LIB = os.path.join(ORACLE_DIR, "liboracle64.so")
 
-CU_SOURCES = ["modifiers.cu", "diffuse.cu", "synapse.cu", "backend.cu", "plugins.cu", "adjoint.cu"]
+CU_SOURCES = ["modifiers.cu", "diffuse.cu", "synapse.cu", "backend.cu", "plugins.cu", "adjoint.cu", "convert.cu"]
 CPP_SOURCES = ["netgen.cpp", "capi_host.cpp", "builder.cpp", "sweep.cpp", "plugin_host.cpp", "bion_file.cpp"]
 HEADERS = sorted(f for f in os.listdir(CSRC) if f.endswith((".h", ".cuh")))
 

@@ -186,7 +186,9 @@ struct UF {
 
 }  // namespace
 
+float host_bouton_gamma(uint8_t type) { return bouton_gamma(type); }
 uint8_t param_mask(uint8_t type) { return param_words(type); }
+bool host_receptor_supported(uint8_t type) { return receptor_supported(type); }
 
 int upload_stimuli(const Stimuli& stim, NetHost& host, NetDev* dev, DeviceAllocs* allocs) {
     int rc = BNC_OK;
@@ -999,44 +1001,35 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
     host->fuse = fuse;
     lap("item sort");
     const uint32_t NI = (uint32_t)keys.size();
-    std::vector<uint32_t> it_seg(NI);
-    std::vector<uint16_t> it_tf(NI);
-    std::vector<float> it_den(NI), it_st((size_t)7 * NI);
     std::vector<uint32_t> phase_off(bucket_off.begin(), bucket_off.end());
-    host->item_seg.assign(NI, 0);
-    host->item_slot.assign(NI, 0);
+    // The items' values (density, state, flags) are gathered on the device from the
+    // modifier records (device_convert_state); the host keeps each item's segment and slot.
+    host->item_seg.resize(NI);
+    host->item_slot.resize(NI);
     host->phase_off = phase_off;
-    {
+    parallel_for(NI, [&](size_t q0, size_t q1) {
+        for (size_t q = q0; q < q1; q++) {
+            host->item_seg[q] = host->perm[keys[q].dseg];
+            host->item_slot[q] = act_slot[keys[q].k];
+        }
+    });
+    auto item_type = [&](uint32_t q) { return keys[q].type; };
+    if (!allocs) {   // a host-only plan checks what the device conversion would
         FirstError bad;
         parallel_for(NI, [&](size_t q0, size_t q1) {
-            for (uint32_t q = (uint32_t)q0; q < (uint32_t)q1; q++) {
-                const ItemKey& kk = keys[q];
-                uint32_t orig = host->perm[kk.dseg];
-                uint8_t slot = act_slot[kk.k];
-                const ModLite& m = hn.mod(orig, slot);
-                uint8_t fl = 0;
-                uint8_t pm = param_words(m.type);
-                for (int b = 0; b < 7; b++) if ((pm >> b) & 1) if (m.state[b] != 0.0f) fl |= 1;
-                if (receptor_supported(m.type) && m.active_vars > 0) {
-                    if (m.active_vars >= 8) { bad.note(q); continue; }
-                    fl |= (uint8_t)(2u | ((uint32_t)m.active_vars << 2));
-                }
-                it_seg[q] = kk.dseg;
-                it_tf[q] = (uint16_t)(m.type | ((uint32_t)fl << 8));
-                it_den[q] = m.density;
-                for (int b = 0; b < 7; b++) it_st[(size_t)b * NI + q] = m.state[b];
-                host->item_seg[q] = orig;
-                host->item_slot[q] = slot;
+            for (size_t q = q0; q < q1; q++) {
+                const ModLite& m = hn.mod(host->item_seg[q], host->item_slot[q]);
+                if (receptor_supported(m.type) && m.active_vars >= 8) bad.note(q);
             }
         });
         if (bad.any()) {
-            const ItemKey& kk = keys[bad.at.load()];
-            const uint32_t orig = host->perm[kk.dseg];
-            const uint8_t slot = act_slot[kk.k];
-            set_error("segment %u slot %u: active_vars %u out of range", orig, slot, hn.mod(orig, slot).active_vars);
+            const uint32_t q = (uint32_t)bad.at.load();
+            set_error("segment %u slot %u: active_vars %u out of range", host->item_seg[q], host->item_slot[q],
+                      hn.mod(host->item_seg[q], host->item_slot[q]).active_vars);
             return BNC_ERR_FORMAT;
         }
     }
+    lap("item fill");
     {   // the state words some item updates on the device (registered types: all 7)
         uint8_t seen[256] = {0};
         for (uint8_t t : act_type) seen[t] = 1;
@@ -1051,9 +1044,9 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
     for (uint32_t p = 0; p < (uint32_t)NB; p++) {   // bucket: chunk * n_phases + phase
         uint32_t q = phase_off[p];
         while (q < phase_off[p + 1]) {
-            const uint8_t t = (uint8_t)(it_tf[q] & 0xFFu);
+            const uint8_t t = item_type(q);
             uint32_t r = q;
-            while (r < phase_off[p + 1] && (uint8_t)(it_tf[r] & 0xFFu) == t) r++;
+            while (r < phase_off[p + 1] && item_type(r) == t) r++;
             if (user_type[t]) {
                 host->user_ranges.push_back({p, t, q, r, nullptr});
                 dev->user_mask[t >> 5] |= 1u << (t & 31);
@@ -1062,34 +1055,16 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
         }
     }
     lap("items");
-    // ---- per-segment state and statics in device order ----
-    std::vector<float> V(n), ion_in((size_t)7 * n), ion_out((size_t)7 * n), intra_nt((size_t)15 * n),
-        nt((size_t)15 * n), atp(n), temp(n), txn(n), radius(n), length(n), area(n), cm(n);
-    std::vector<double> vol(n), ibuf(n);
-    std::vector<uint8_t> stype(n), dflags(n);
-    std::vector<float2> c21(n);
+    // ---- per-segment statics in device order (the state is gathered on the device) ----
+    std::vector<float> area(n), cm(n);
+    std::vector<double> vol(n);
+    std::vector<uint8_t> dflags(n);
     bool intra_nt_grad = false, temp_grad = false, txn_grad = false;
     parallel_for(n, [&](size_t d0, size_t d1) {
     for (uint32_t d = (uint32_t)d0; d < (uint32_t)d1; d++) {
         const SegLite& s = S[host->perm[d]];
-        V[d] = s.V_m;
-        for (int q = 0; q < 7; q++) {
-            ion_in[(size_t)q * n + d] = s.intra_ions[q];
-            ion_out[(size_t)q * n + d] = s.extra_ions[q];
-        }
-        for (int q = 0; q < 15; q++) {
-            intra_nt[(size_t)q * n + d] = s.intra_nt[q];
-            nt[(size_t)q * n + d] = s.neurotransmitter[q];
-        }
-        atp[d] = s.ATP_level; temp[d] = s.temperature; txn[d] = s.transcription_signal;
-        radius[d] = s.radius; length[d] = s.length; stype[d] = s.segment_type;
         area[d] = seg_area(s); vol[d] = seg_volume(s); cm[d] = seg_capacitance(hn, host->perm[d]);
-        ibuf[d] = s.I_buffer;
         dflags[d] = sflags[host->perm[d]];
-        c21[d] = make_float2(0.0f, 0.0f);
-        for (uint8_t j = 0; j < s.modifier_count; j++)
-            if (hn.mod(host->perm[d], j).type == BNC_MOD_CAV21)
-                c21[d] = make_float2(hn.mod(host->perm[d], j).density, hn.mod(host->perm[d], j).state[1]);
     }
     });
     for (uint32_t c : conn_ok) {
@@ -1175,6 +1150,7 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
             syn_valid.push_back(k);
         }
     }
+    lap("syn check");
     // The synapse kernel's entries: each chemical synapse once, for its post segment;
     // each gap junction twice, for its pre segment (side 2) and then its post segment
     // (side 1), since the reference's loop changes both segments' I_buffer
@@ -1215,6 +1191,7 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
         syn_valid.swap(sorted);
         ent_side.swap(sorted_side);
     }
+    lap("syn sort");
     // ---- synapse-kernel threads and the sliced synapse order ----
     // Thread t of the synapse kernel handles segment th_seg[t]: first every segment
     // with synapses, by synapse count descending (stable in device order), then the
@@ -1267,6 +1244,7 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
         }
         for (uint32_t d : rest_list) { th_seg.push_back(d); th_cnt.push_back(0); }
     }
+    lap("syn threads");
     const uint32_t NW = (n + 31) / 32;
     std::vector<uint32_t> w_off(NW + 1, 0), rw_off(NW + 1, 0);
     std::vector<uint32_t> slot_syn;   // sliced position -> index into syn_valid (post-sorted)
@@ -1292,44 +1270,17 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
             ent_side.swap(sliced_side);
         }
     }
-    std::vector<uint32_t> sy_pre(K), sy_id(K);
+    lap("syn slices");
+    // The synapses' and receptors' values are gathered on the device from their records
+    // (device_convert_synapses); the host decides which receptors each synapse keeps.
     std::vector<uint8_t> rc_cnt(K, 0), kept((size_t)K * 8, 0);
-    std::vector<float> sy_prel(K), sy_amt(K), sy_tauc(K), sy_delay(K), sy_prea(K), sy_posta(K), sy_gK(K),
-        sy_gNa(K), sy_bouton(K), sy_spine(K), sy_camkii(K), sy_calcn(K), sy_facil(K), sy_weight(K), sy_cleft(K),
-        sy_rrp(K), sy_rrpm(K), sy_rrpr(K), sy_scale(K, 1.0f);
-    std::vector<uint8_t> sy_refr(K), sy_flags(K);
-    std::vector<uint8_t> rc_type, rc_av;
-    std::vector<float> rc_den, rc_st0, rc_st1, rc_st2;
     host->syn_orig = syn_valid;
     host->rec_syn.clear(); host->rec_slot.clear();
     host->syn_nt.assign(K, 0);
     // per synapse: 0 or the error its receptors raise (the lowest such synapse is reported)
     auto fill_syn = [&](uint32_t q, bool report) -> int {
         const SynLite& y = hn.syn[syn_valid[q]];
-        sy_pre[q] = host->inv[y.pre_segment];
-        sy_id[q] = y.id;
-        sy_prel[q] = y.release_probability; sy_amt[q] = y.release_amount; sy_tauc[q] = y.tau_clearance;
-        sy_delay[q] = y.delay; sy_prea[q] = y.pre_area; sy_posta[q] = y.post_area;
-        float gK = 0.0f, gNa = 0.0f;
-        for (uint8_t j = 0; j < y.pre_autoreceptor_count; j++) {   // modifier_helpers.h:767-773
-            uint8_t t = hn.pre_ar(syn_valid[q], j).type;
-            float g = (float)((double)hn.pre_ar(syn_valid[q], j).density * bouton_gamma(t));
-            if (t == 141 || t == 142) gNa += g; else gK += g;
-        }
-        sy_gK[q] = gK; sy_gNa[q] = gNa;
-        sy_refr[q] = y.refractory;
-        uint8_t ntt = y.post_receptor_count > 0 ? nt_from_receptor(hn.post_rec(syn_valid[q], 0).type) : 0;
-        bool inhib = false;
-        for (uint8_t j = 0; j < y.post_receptor_count; j++) {
-            uint8_t rt = hn.post_rec(syn_valid[q], j).type;
-            if (rt == 11 || rt == 17 || rt == 12) { inhib = true; break; }
-        }
-        sy_flags[q] = (uint8_t)((inhib ? 1u : 0u) | ((uint32_t)ntt << 4));
-        host->syn_nt[q] = ntt;
-        sy_bouton[q] = y.bouton_Ca; sy_spine[q] = y.spine_Ca; sy_camkii[q] = y.spine_camkii;
-        sy_calcn[q] = y.spine_calcineurin; sy_facil[q] = y.facilitation; sy_weight[q] = y.weight;
-        sy_cleft[q] = y.cleft_neurotransmitter[ntt];
-        sy_rrp[q] = y.RRP; sy_rrpm[q] = y.RRP_max; sy_rrpr[q] = y.RRP_recovery;
+        host->syn_nt[q] = y.post_receptor_count > 0 ? nt_from_receptor(hn.post_rec(syn_valid[q], 0).type) : 0;
         bool myel_post = (sflags[y.post_segment] & SF_MYELIN) != 0;
         uint32_t nr = 0;
         for (uint8_t j = 0; j < y.post_receptor_count; j++) {
@@ -1357,6 +1308,7 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
         });
         if (bad.any()) return fill_syn((uint32_t)bad.at.load(), true);
     }
+    lap("syn fill");
     // endocannabinoid retrograde signalling (simulation_host.cpp:578-589): each post
     // segment's first eCB-synthesis modifier (its item) and each synapse's eCB cleft entry
     std::vector<uint32_t> seg_ecb_item;
@@ -1365,7 +1317,7 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
         bool any_ecb = false;
         std::vector<uint8_t> best_slot;
         for (uint32_t q = 0; q < NI; q++) {
-            if ((uint8_t)(it_tf[q] & 0xFFu) != 86) continue;
+            if (item_type(q) != 86) continue;
             if (!any_ecb) { any_ecb = true; seg_ecb_item.assign(n, UINT32_MAX); best_slot.assign(n, 0xFF); }
             const uint32_t dseg = host->inv[host->item_seg[q]];
             if (host->item_slot[q] < best_slot[dseg]) { best_slot[dseg] = host->item_slot[q]; seg_ecb_item[dseg] = q; }
@@ -1418,7 +1370,7 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
         // each segment's connexin-36 and connexin-43 items (at most one of each)
         seg_cx.assign((size_t)2 * n, UINT32_MAX);
         for (uint32_t q = 0; q < NI; q++) {
-            const uint8_t t = (uint8_t)(it_tf[q] & 0xFFu);
+            const uint8_t t = item_type(q);
             if (t != 114 && t != 198) continue;
             const size_t at = (size_t)(t == 198 ? 1 : 0) * n + host->inv[host->item_seg[q]];
             if (seg_cx[at] != UINT32_MAX) {
@@ -1474,6 +1426,7 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
             for (uint32_t g : glia) gl_seg.push_back(host->inv[g]);
         }
     }
+    lap("syn ecb gap glia");
     // release modulators of the autoreceptors, per sliced synapse in autoreceptor order
     std::vector<uint32_t> md_off;
     std::vector<uint8_t> md_code;
@@ -1513,6 +1466,7 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
             }
         }
     }
+    lap("syn modulators");
     // receptor order: slice by slice, receptor j of each lane that has one.  A warp's
     // receptors are those of its synapses, so a prefix sum of per-warp counts places
     // each warp's run and the warps fill in parallel.
@@ -1522,8 +1476,6 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
         rw_off[w + 1] = rw_off[w] + c;
     }
     const size_t NRC = rw_off[NW];
-    rc_type.resize(NRC); rc_av.resize(NRC); rc_den.resize(NRC);
-    rc_st0.resize(NRC); rc_st1.resize(NRC); rc_st2.resize(NRC);
     host->rec_syn.resize(NRC); host->rec_slot.resize(NRC);
     parallel_for(NW, [&](size_t w0, size_t w1) {
         for (uint32_t w = (uint32_t)w0; w < (uint32_t)w1; w++) {
@@ -1541,13 +1493,6 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
                         const uint32_t qq = q + l;
                         if (rc_cnt[qq] <= j) continue;
                         const uint8_t slot = kept[(size_t)qq * 8 + j];
-                        const ModLite& r = hn.post_rec(syn_valid[qq], slot);
-                        rc_type[o] = r.type;
-                        rc_av[o] = r.active_vars;
-                        rc_den[o] = r.density;
-                        rc_st0[o] = r.state[0];
-                        rc_st1[o] = r.state[1];
-                        rc_st2[o] = r.state[2];
                         host->rec_syn[o] = qq;
                         host->rec_slot[o] = slot;
                         o++;
@@ -1556,14 +1501,10 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
             }
         }
     }, 1024);
-    rw_off[NW] = (uint32_t)rc_type.size();
+    rw_off[NW] = (uint32_t)NRC;
 
     lap("synapses");
-    const uint32_t NR = (uint32_t)rc_type.size();
-    std::vector<float> rc_st((size_t)3 * NR);
-    for (uint32_t r = 0; r < NR; r++) {
-        rc_st[r] = rc_st0[r]; rc_st[(size_t)NR + r] = rc_st1[r]; rc_st[(size_t)2 * NR + r] = rc_st2[r];
-    }
+    const uint32_t NR = (uint32_t)NRC;
     lap("receptors");
     // tile sizes for the shared-memory plan: own segments (threads), own + ghost
     // segments (the per-segment array stride), connections
@@ -1625,23 +1566,20 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
     for (uint32_t i = 0; i < n; i++) if (sflags[i] & SF_NMDA) any_nmda = true;
     dev->nt_used_mask = nt_mask | (any_nmda ? 1u : 0u) | (sy_cleft_ecb.empty() ? 0u : 1u << 9);
     if (allocs) {
-        dev->V = up(allocs, V, &rc);
-        dev->ion_in = up(allocs, ion_in, &rc);
-        dev->ion_out = up(allocs, ion_out, &rc);
-        dev->intra_nt = up(allocs, intra_nt, &rc);
-        dev->nt = up(allocs, nt, &rc);
-        dev->atp = up(allocs, atp, &rc);
-        dev->temp = up(allocs, temp, &rc);
-        dev->txn = up(allocs, txn, &rc);
-        dev->ibuf = up(allocs, ibuf, &rc);
-        dev->radius = up(allocs, radius, &rc);
-        dev->length = up(allocs, length, &rc);
+        {
+            uint32_t bad = UINT32_MAX;
+            rc = device_convert_state(hn, host->perm, host->inv, host->item_seg, host->item_slot, dev, allocs, &bad);
+            if (rc != BNC_OK) return rc;
+            if (bad != UINT32_MAX) {
+                set_error("segment %u slot %u: active_vars %u out of range", host->item_seg[bad], host->item_slot[bad],
+                          hn.mod(host->item_seg[bad], host->item_slot[bad]).active_vars);
+                return BNC_ERR_FORMAT;
+            }
+        }
         dev->area = up(allocs, area, &rc);
         dev->vol = up(allocs, vol, &rc);
         dev->cm = up(allocs, cm, &rc);
-        dev->stype = up(allocs, stype, &rc);
         dev->sflags = up(allocs, dflags, &rc);
-        dev->cav21_static = up(allocs, c21, &rc);
         dev->c21_cur = zeros<float2>(allocs, n, &rc);
         dev->rec = zeros<SegRec>(allocs, n, &rc);
         dev->pre_rec = zeros<float4>(allocs, n, &rc);
@@ -1669,42 +1607,12 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
             int krc = device_modifier_kernel((uint8_t)ur.type, &ur.kernel);
             if (krc != BNC_OK) return krc;
         }
-        dev->it_seg = up(allocs, it_seg, &rc);
-        dev->it_tf = up(allocs, it_tf, &rc);
-        dev->it_den = up(allocs, it_den, &rc);
-        dev->it_st = up(allocs, it_st, &rc);
         dev->th_seg = up(allocs, th_seg, &rc);
         dev->th_cnt = up(allocs, th_cnt, &rc);
         dev->w_off = up(allocs, w_off, &rc);
         dev->rw_off = up(allocs, rw_off, &rc);
-        dev->sy_pre = up(allocs, sy_pre, &rc);
-        dev->sy_id = up(allocs, sy_id, &rc);
-        dev->sy_prel = up(allocs, sy_prel, &rc);
-        dev->sy_amt = up(allocs, sy_amt, &rc);
-        dev->sy_tauc = up(allocs, sy_tauc, &rc);
-        dev->sy_delay = up(allocs, sy_delay, &rc);
-        dev->sy_pre_area = up(allocs, sy_prea, &rc);
-        dev->sy_post_area = up(allocs, sy_posta, &rc);
-        dev->sy_gK = up(allocs, sy_gK, &rc);
-        dev->sy_gNa = up(allocs, sy_gNa, &rc);
-        dev->sy_refr = up(allocs, sy_refr, &rc);
-        dev->sy_flags = up(allocs, sy_flags, &rc);
-        dev->sy_bouton = up(allocs, sy_bouton, &rc);
-        dev->sy_spine = up(allocs, sy_spine, &rc);
-        dev->sy_camkii = up(allocs, sy_camkii, &rc);
-        dev->sy_calcn = up(allocs, sy_calcn, &rc);
-        dev->sy_facil = up(allocs, sy_facil, &rc);
-        dev->sy_weight = up(allocs, sy_weight, &rc);
-        dev->sy_cleft = up(allocs, sy_cleft, &rc);
-        dev->sy_rrp = up(allocs, sy_rrp, &rc);
-        dev->sy_rrp_max = up(allocs, sy_rrpm, &rc);
-        dev->sy_rrp_rec = up(allocs, sy_rrpr, &rc);
-        dev->sy_scale = up(allocs, sy_scale, &rc);
+        if (rc == BNC_OK) rc = device_convert_synapses(hn, host->syn_orig, host->inv, host->rec_syn, host->rec_slot, dev, allocs);
         dev->rc_cnt = up(allocs, rc_cnt, &rc);
-        dev->rc_type = up(allocs, rc_type, &rc);
-        dev->rc_av = up(allocs, rc_av, &rc);
-        dev->rc_den = up(allocs, rc_den, &rc);
-        dev->rc_st = up(allocs, rc_st, &rc);
         if (!sy_gj.empty()) {
             dev->sy_gj = up(allocs, sy_gj, &rc);
             dev->gj_pre = up(allocs, gj_pre, &rc);
@@ -1719,7 +1627,7 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
         }
         dev->model_extras = 0;
         for (uint32_t q = 0; q < NI && !dev->model_extras; q++) {
-            const uint8_t t = (uint8_t)(it_tf[q] & 0xFFu);
+            const uint8_t t = item_type(q);
             if (t == 86 || t == 114 || t == 147 || t == 198) dev->model_extras = 1;
         }
         if (!gl_seg.empty()) {
@@ -1769,7 +1677,7 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
         // modifier items: meta + density read, dynamic state read+write
         double items = 0;
         for (uint32_t q = 0; q < NI; q++) {
-            uint8_t t = (uint8_t)(it_tf[q] & 0xFFu);
+            const uint8_t t = item_type(q);
             int dyn = 0;
             switch (t) {
                 case 1: case 8: case 11: case 12: case 85: case 140: case 141: case 142: case 200: dyn = 2; break;
@@ -1788,7 +1696,7 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
         // per synapse: pre index, id, pre-record, scalar params, dynamic state rw, receptors
         double syn = 4 + 4 + 16 + 4 * 5 + 1 + 1 + (4 * 6 + 1) * 2 + 4;
         double rec = 0;
-        for (uint32_t r = 0; r < NR; r++) rec += 1 + 4 + 8.0 * (rc_type[r] == 9 ? 2 : 2);
+        rec += (1 + 4 + 8.0 * 2) * NR;
         host->seg_bytes = (seg_a + seg_b) * n + items;
         host->syn_bytes = syn * K + rec + 4.0 * (K + 1);
         host->tile_bytes = seg_a * n + items;

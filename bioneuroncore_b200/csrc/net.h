@@ -334,6 +334,24 @@ int export_network(const NetDev& dev, const NetHost& host, uint64_t ticks_run, B
 uint8_t host_dyn_mask(uint8_t type);
 // State words (bits) a built-in type reads as parameters (its default when 0).
 uint8_t param_mask(uint8_t type);
+// Receptor types the synapse and modifier kernels implement (AMPA, NMDA, GABA-A, glycine).
+bool host_receptor_supported(uint8_t type);
+// The bouton channel conductance (pS) an autoreceptor of this type adds (0: none).
+float host_bouton_gamma(uint8_t type);
+
+// The segment state and the modifier items in device order, gathered on the device
+// from the host records (convert.cu): perm maps device to original segments, inv the
+// reverse; item q belongs to original segment item_seg[q], slot item_slot[q].  Sets
+// *bad_item to the lowest item whose receptor override (active_vars) is out of range.
+int device_convert_state(const HostNet& hn, const std::vector<uint32_t>& perm, const std::vector<uint32_t>& inv,
+                         const std::vector<uint32_t>& item_seg, const std::vector<uint8_t>& item_slot, NetDev* dev,
+                         DeviceAllocs* allocs, uint32_t* bad_item);
+// The synapse and receptor arrays in device order, gathered on the device (convert.cu):
+// device synapse q is original synapse syn_orig[q]; device receptor r is slot
+// rec_slot[r] of device synapse rec_syn[r].
+int device_convert_synapses(const HostNet& hn, const std::vector<uint32_t>& syn_orig,
+                            const std::vector<uint32_t>& inv, const std::vector<uint32_t>& rec_syn,
+                            const std::vector<uint8_t>& rec_slot, NetDev* dev, DeviceAllocs* allocs);
 
 // Kernel launchers (tile.cu, synapse.cu).  prepare_tick does the per-device and
 // per-network set-up that must not happen inside a stream capture (constant tables,
