@@ -1188,7 +1188,32 @@ __global__ void __launch_bounds__(kMaxSeg) k_adj_forward(AdjDev d, uint32_t t0, 
     if (threadIdx.x == c.soma) d.loss_part[(size_t)c.p * d.nn + c.n] += loss;
 }
 
-// Reverse pass over window w (ticks [w K, min((w + 1) K, T))).
+// The re-run of window w from its checkpoint that the reverse pass needs: each tick's
+// starting state into the window buffer.  A launch of its own, before the window's
+// reverse launch: every CTA then runs the forward tick's code at the forward kernel's
+// occupancy, where in the reverse kernel CTAs re-running and CTAs reversing would share
+// an SM's instruction caches between the two ticks' code.
+template <bool kFull>
+__global__ void __launch_bounds__(kMaxSeg) k_adj_rerun(AdjDev d, uint32_t w) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const Ctx c = make_ctx(d);
+    const uint32_t W = kFull ? d.W : kW3;
+    const Lay L = make_lay(smem, d.Smax, d.Emax, d.Ymax, false, W);
+    const Scr sc{};
+    const uint32_t tb = w * d.K;
+    const uint32_t te = min(d.T, tb + d.K);
+    block_load(L.st, d.ckpt + ((size_t)w * d.n_sets + c.p) * d.L + c.st_off, c, d.Smax, W);
+    __syncthreads();
+    for (uint32_t t = tb; t < te; t++) {
+        block_store(d.win + ((size_t)(t - tb) * d.n_sets + c.p) * d.L + c.st_off, L.st, c, d.Smax, W);
+        if (t + 1 == te) break;   // the last tick is re-run by the reverse launch
+        __syncthreads();
+        tick_fwd<kFull>(d, c, L, sc, t, false);
+    }
+}
+
+// Reverse pass over window w (ticks [w K, min((w + 1) K, T))), after k_adj_rerun has
+// left each tick's starting state in the window buffer.
 // kThreads / kMinBlocks: the launch bounds (neurons of at most 64 segments run a
 // 64-thread instantiation bounded for 5 CTAs per SM).
 template <bool kFull, int kThreads, int kMinBlocks>
@@ -1205,29 +1230,17 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_adj_backward(AdjDev d,
         const float* src = d.lam + (size_t)c.p * d.L + c.st_off;
         for (uint32_t q = threadIdx.x; q < W * c.S; q += blockDim.x) L.lam[(q / c.S) * Sm + (q % c.S)] = src[q];
     }
-    block_load(L.st, d.ckpt + ((size_t)w * d.n_sets + c.p) * d.L + c.st_off, c, d.Smax, W);
-    __syncthreads();
-    // Steps [0, nA): re-run the window from its checkpoint, keeping each tick's starting
-    // state; steps [nA, nA + n): walk the ticks backwards, each re-run with its
-    // intermediates recorded and then reversed.  One call site of the tick keeps one
-    // copy of its code in the kernel.
+    // Walk the ticks backwards: each is re-run from its starting state with its
+    // intermediates recorded, then reversed.
     const uint32_t n = te - tb;
-    const uint32_t nA = n - 1;
     double gp[3] = {0.0, 0.0, 0.0};
-    for (uint32_t step = 0; step < nA + n; step++) {
-        const bool rec = step >= nA;
-        const uint32_t t = rec ? te - 1 - (step - nA) : tb + step;
-        float* blk = d.win + ((size_t)(t - tb) * d.n_sets + c.p) * d.L + c.st_off;
-        if (!rec) {
-            block_store(blk, L.st, c, d.Smax, W);
-        } else {
-            if (step == nA) block_store(blk, L.st, c, d.Smax, W);   // the window's last tick
-            __syncthreads();
-            block_load(L.st, blk, c, d.Smax, W);
-        }
+    for (uint32_t step = 0; step < n; step++) {
+        const uint32_t t = te - 1 - step;
         __syncthreads();
-        tick_fwd<kFull>(d, c, L, sc, t, rec);
-        if (rec) tick_rev<kFull>(d, c, L, sc, t, gp);
+        block_load(L.st, d.win + ((size_t)(t - tb) * d.n_sets + c.p) * d.L + c.st_off, c, d.Smax, W);
+        __syncthreads();
+        tick_fwd<kFull>(d, c, L, sc, t, true);
+        tick_rev<kFull>(d, c, L, sc, t, gp);
     }
     {
         float* dst = d.lam + (size_t)c.p * d.L + c.st_off;
@@ -1673,6 +1686,8 @@ int adj_build(Adjoint* A, void* sim, const BncAdjointConfig& cfg) {
     if (A->smem_bwd > 227u * 1024u) { set_error("adjoint: a neuron needs %zu bytes of shared memory", A->smem_bwd); return BNC_ERR_UNSUPPORTED; }
     if (cudaFuncSetAttribute(k_adj_forward<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)A->smem_fwd) != cudaSuccess ||
         cudaFuncSetAttribute(k_adj_forward<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)A->smem_fwd) != cudaSuccess ||
+        cudaFuncSetAttribute(k_adj_rerun<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)A->smem_fwd) != cudaSuccess ||
+        cudaFuncSetAttribute(k_adj_rerun<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)A->smem_fwd) != cudaSuccess ||
         cudaFuncSetAttribute(k_adj_backward<false, kMaxSeg, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)A->smem_bwd) != cudaSuccess ||
         cudaFuncSetAttribute(k_adj_backward<true, kMaxSeg, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)A->smem_bwd) != cudaSuccess ||
         cudaFuncSetAttribute(k_adj_backward<false, 64, BNC_ADJ_MIN_BLOCKS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)A->smem_bwd) != cudaSuccess ||
@@ -1899,7 +1914,9 @@ int bnc_adjoint_backward(void* adj, float* g_gNa, float* g_gK, float* g_gleak, f
     cudaMemsetAsync(d.g_w, 0, (size_t)d.n_sets * std::max(d.n_syn, 1u) * sizeof(double), A->stream);
     cudaEventRecord(A->ev0, A->stream);
     const dim3 grid(d.nn, d.n_sets);
-    for (int w = (int)d.n_ckpt - 1; w >= 0; w--)
+    for (int w = (int)d.n_ckpt - 1; w >= 0; w--) {
+        if (d.full) k_adj_rerun<true><<<grid, A->threads, A->smem_fwd, A->stream>>>(d, (uint32_t)w);
+        else k_adj_rerun<false><<<grid, A->threads, A->smem_fwd, A->stream>>>(d, (uint32_t)w);
         if (A->threads <= 64) {
             if (d.full) k_adj_backward<true, 64, BNC_ADJ_MIN_BLOCKS><<<grid, A->threads, A->smem_bwd, A->stream>>>(d, (uint32_t)w);
             else k_adj_backward<false, 64, BNC_ADJ_MIN_BLOCKS><<<grid, A->threads, A->smem_bwd, A->stream>>>(d, (uint32_t)w);
@@ -1907,6 +1924,7 @@ int bnc_adjoint_backward(void* adj, float* g_gNa, float* g_gK, float* g_gleak, f
             if (d.full) k_adj_backward<true, kMaxSeg, 1><<<grid, A->threads, A->smem_bwd, A->stream>>>(d, (uint32_t)w);
             else k_adj_backward<false, kMaxSeg, 1><<<grid, A->threads, A->smem_bwd, A->stream>>>(d, (uint32_t)w);
         }
+    }
     cudaEventRecord(A->ev1, A->stream);
     cudaError_t e = cudaStreamSynchronize(A->stream);
     if (e == cudaSuccess) e = cudaGetLastError();
