@@ -18,7 +18,8 @@ import numpy as np
 from .abi import (BionData, NetgenParams, SEGMENT_DTYPE, SYNAPSE_DTYPE, CONN_DTYPE, STIM_DTYPE, view,
                   NET_SMALL, NET_LARGE, NET_TREES, NET_ENSEMBLE_MEMBER, NET_ADJOINT, NETGEN_NO_SYNAPSES,
                   NETGEN_NO_CONNECTIONS, NETGEN_NO_STIMULI, NETGEN_PERTURB_IONS, NETGEN_SYNAPSE_EXTRAS,
-                  NETGEN_FULL_SMALL_SET, NETGEN_GLYCINE, NETGEN_DRAW_ORDER, NETGEN_RELEASE_MODULATORS, NETGEN_ECB, NETGEN_GLIA, NETGEN_GAP_JUNCTIONS)
+                  NETGEN_FULL_SMALL_SET, NETGEN_GLYCINE, NETGEN_DRAW_ORDER, NETGEN_RELEASE_MODULATORS, NETGEN_ECB, NETGEN_GLIA, NETGEN_GAP_JUNCTIONS,
+                  NETGEN_NMDA)
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libbnc_b200.so")
@@ -418,7 +419,7 @@ class Backend:
 __all__ = ["Backend", "Network", "Adjoint", "AdjointConfig", "AdjointInfo", "SweepTask", "SweepResult",
            "sweep_parse_params", "sweep_tasks", "sweep_run", "SWEEP_SINGLE_TICK", "NetgenParams", "BionData", "BackendError", "load_library", "last_error",
            "NET_SMALL", "NET_LARGE", "NET_TREES", "NET_ENSEMBLE_MEMBER", "NET_ADJOINT", "NETGEN_NO_SYNAPSES",
-           "NETGEN_NO_CONNECTIONS", "NETGEN_NO_STIMULI", "NETGEN_PERTURB_IONS", "NETGEN_SYNAPSE_EXTRAS", "NETGEN_FULL_SMALL_SET", "NETGEN_GLYCINE", "NETGEN_DRAW_ORDER", "NETGEN_RELEASE_MODULATORS", "NETGEN_ECB", "NETGEN_GLIA", "NETGEN_GAP_JUNCTIONS", "SEG_FIELDS", "SYN_FIELDS",
+           "NETGEN_NO_CONNECTIONS", "NETGEN_NO_STIMULI", "NETGEN_PERTURB_IONS", "NETGEN_SYNAPSE_EXTRAS", "NETGEN_FULL_SMALL_SET", "NETGEN_GLYCINE", "NETGEN_DRAW_ORDER", "NETGEN_RELEASE_MODULATORS", "NETGEN_ECB", "NETGEN_GLIA", "NETGEN_GAP_JUNCTIONS", "NETGEN_NMDA", "SEG_FIELDS", "SYN_FIELDS",
            "DROPIN_SYMBOLS", "NEW_SYMBOLS", "EnsembleMember", "Tuning", "BuildOptions", "register_device_modifier", "ensemble_params", "plan_ensemble", "plan_generated",
            "DIFFUSION_RESIDUAL", "DIFFUSION_LEDGER", "DiffusionStats"]
 

@@ -183,6 +183,7 @@ NETGEN_RELEASE_MODULATORS = 256
 NETGEN_ECB = 512
 NETGEN_GLIA = 1024
 NETGEN_GAP_JUNCTIONS = 2048
+NETGEN_NMDA = 4096
 
 assert SEGMENT_DTYPE.itemsize == 3216 and SYNAPSE_DTYPE.itemsize == 1568 and MOD_DTYPE.itemsize == 88
 assert BionData.segments.offset == 112 and BionData.num_segments.offset == 148

@@ -62,7 +62,9 @@ constexpr int kRecPerSyn = 2;    // receptors per synapse
 // the reverse pass, so W follows the network.  The fitting family's kernels (no
 // Cav1.3, no pump) use the fixed width kW3: three gate words.
 constexpr uint32_t kW3 = 18;
-constexpr int kSynWords = 5;     // receptor 0 (r, d), receptor 1 (r, d), cleft
+constexpr int kSynWords = 5;     // receptor 0 (r, d), receptor 1 (r, d), cleft; an NMDA receptor's d word holds
+                                 // its Ca2+-dependent inactivation gate (state[2]; it does not desensitise)
+constexpr int kSynScr = 11;      // per synapse in the scratch: in[7] before it, open probabilities, NMDA gates before
 
 __constant__ float c_z2d[7];     // z^2 * D per ion, as the reference's float product
 __constant__ float c_z[7];
@@ -145,7 +147,7 @@ __host__ __device__ inline size_t lay_bytes(uint32_t S, uint32_t E, uint32_t Y, 
     size_t flt = (size_t)W * S + kSynWords * Y + 2 * (size_t)E + 2 * (size_t)S;
     if (bwd) {
         dbl += S;   // pmask
-        flt += 15 * (size_t)S + W * (size_t)S + 7 * (size_t)S + (size_t)E + 51 * (size_t)S + 4;
+        flt += 15 * (size_t)S + W * (size_t)S + kSynWords * (size_t)Y + 7 * (size_t)S + (size_t)E + 51 * (size_t)S + 4;
     }
     return dbl * 8 + flt * 4;
 }
@@ -163,7 +165,7 @@ __device__ inline Lay make_lay(unsigned char* base, uint32_t S, uint32_t E, uint
     l.vnA = f; f += S; l.vnB = f; f += S;
     if (bwd) {
         l.s2 = f; f += 15 * S;
-        l.lam = f; f += W * S;
+        l.lam = f; f += W * S + kSynWords * Y;   // the state's layout: segment words, then synapse words
         l.lphi = f; f += S; l.lI = f; f += S; l.mu = f; f += S; l.lvB = f; f += S;
         l.linp = f; f += S; l.lgdg = f; f += S; l.ldiag = f; f += S; l.edv = f; f += E;
         // the reverse tick's per-connection adjoints reuse the forward's flux buffers
@@ -386,12 +388,12 @@ struct Scr {
     float* jac;       // [5][51][Sm]
     float* phs;       // [51][Sm]    phi_e before each of its sweeps
     float* estart;    // [6][7][Sm]  out before each extra sub-step and before the bath
-    float* syn;       // [Ymax][9]   in[7] before the synapse, receptor open probabilities
+    float* syn;       // [Ymax][kSynScr] in[7] before the synapse, receptor open probabilities, NMDA gates
     float* atpf;      // [Sm]        ATP before the Fick pass
 };
 // items: the item stride of the kernels; atp: whether the ATP row is recorded
 __host__ __device__ inline size_t scr_floats(uint32_t S, uint32_t Y, uint32_t items, bool atp) {
-    return ((size_t)40 * S + (size_t)255 * S + (size_t)51 * S + (size_t)42 * S + (size_t)9 * Y + (size_t)items * 5 * S +
+    return ((size_t)40 * S + (size_t)255 * S + (size_t)51 * S + (size_t)42 * S + (size_t)kSynScr * Y + (size_t)items * 5 * S +
             (atp ? S : 0u) + 4 + 3) & ~(size_t)3;
 }
 template <bool kFull>
@@ -404,7 +406,7 @@ __device__ inline Scr make_scr(const AdjDev& d) {
     s.jac = f; f += 255 * S;
     s.phs = f; f += 51 * S;
     s.estart = f; f += 42 * S;
-    s.syn = f; f += 9 * d.Ymax;
+    s.syn = f; f += kSynScr * d.Ymax;
     s.pre = f; f += (size_t)ItemStride<kFull>::v * 5 * S;
     s.atpf = f;
     return s;
@@ -673,7 +675,7 @@ __device__ __forceinline__ void tick_fwd(const AdjDev& d, const Ctx& c, const La
             if (d.sl_nt[y] == 0) nt_glu += cleft;
             else if (d.sl_nt[y] == 1) nt_gaba += cleft;
             else nt_gly += cleft;
-            if (kRec) for (int q = 0; q < 7; q++) sc.syn[ly * 9 + q] = s.in[q];
+            if (kRec) for (int q = 0; q < 7; q++) sc.syn[ly * kSynScr + q] = s.in[q];
             float I_syn = 0.0f;
             const float scale = d.w[(size_t)c.p * d.n_syn + d.sl_syn[y]];
             const float parea = d.sl_parea[y];
@@ -681,16 +683,19 @@ __device__ __forceinline__ void tick_fwd(const AdjDev& d, const Ctx& c, const La
                 const int kind = d.sl_kind[y * kRecPerSyn + j];
                 DMod m;
                 m.den = d.sl_rden[y * kRecPerSyn + j];
+                const bool nmda = kind == 1;
                 m.st[0] = rs[ly * kSynWords + 2 * j];
-                m.st[1] = rs[ly * kSynWords + 2 * j + 1];
-                m.st[2] = m.st[3] = m.st[4] = m.st[5] = m.st[6] = 0.0f;
+                m.st[1] = nmda ? 0.0f : rs[ly * kSynWords + 2 * j + 1];
+                m.st[2] = nmda ? rs[ly * kSynWords + 2 * j + 1] : 0.0f;
+                m.st[3] = m.st[4] = m.st[5] = m.st[6] = 0.0f;
+                if (kRec && nmda) sc.syn[ly * kSynScr + 9 + j] = m.st[2];
                 m.area = (parea > 0.0f) ? parea : s.area;
                 m.av = d.sl_rav[y * kRecPerSyn + j];
                 const float ntr = kind <= 1 ? nt_glu : (kind == 2 ? nt_gaba : nt_gly);
                 I_syn = (float)(I_syn + receptor_current(gRec[kind], m, s, dt, ntr, scale));
                 rs[ly * kSynWords + 2 * j] = m.st[0];
-                rs[ly * kSynWords + 2 * j + 1] = m.st[1];
-                if (kRec) sc.syn[ly * 9 + 7 + j] = m.st[0] * (1.0f - m.st[1]);
+                rs[ly * kSynWords + 2 * j + 1] = nmda ? m.st[2] : m.st[1];
+                if (kRec) sc.syn[ly * kSynScr + 7 + j] = m.st[0] * (1.0f - m.st[1]);
             }
             ib += I_syn;
             cleft *= dm_exp(-dt / d.sl_tauc[y]);
@@ -775,28 +780,56 @@ __device__ void tick_rev(const AdjDev& d, const Ctx& c, const Lay& L, const Scr&
             const float area = (parea > 0.0f) ? parea : c.area;
             // the ions before each receptor of the synapse (receptor 0: recorded)
             float pre[kRecPerSyn][7];
-            for (int q = 0; q < 7; q++) pre[0][q] = sc.syn[ly * 9 + q];
+            for (int q = 0; q < 7; q++) pre[0][q] = sc.syn[ly * kSynScr + q];
             for (uint32_t j = 0; j + 1 < nrec; j++) {
-                const RecKind& K = gRec[d.sl_kind[y * kRecPerSyn + j]];
-                double z4[4] = {0.0, 0.0, 0.0, 0.0}, zx[8];
-                float nv[3];
-                adj::vjp_receptor(z4, zx, K.is_anion, K.is_anion ? K.P_Cl : K.P_Na, K.P_K, V2, pre[j], out2, wv,
-                                  d.sl_rden[y * kRecPerSyn + j], area, sc.syn[ly * 9 + 7 + j], c.vol, dt, nv);
+                const int kind = d.sl_kind[y * kRecPerSyn + j];
+                const RecKind& K = gRec[kind];
+                const float open = sc.syn[ly * kSynScr + 7 + j];
                 for (int q = 0; q < 7; q++) pre[j + 1][q] = pre[j][q];
-                pre[j + 1][0] = nv[0]; pre[j + 1][1] = nv[1]; pre[j + 1][3] = nv[2];
+                if (kind == 1) {
+                    const double z5[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+                    double zx[9];
+                    float nv[3];
+                    adj::vjp_nmda(z5, zx, K.P_Na, K.P_K, K.P_Ca, V2, pre[j], out2, wv, d.sl_rden[y * kRecPerSyn + j],
+                                  area, open, sc.syn[ly * kSynScr + 9 + j], c.vol, dt, nv);
+                    pre[j + 1][0] = nv[0]; pre[j + 1][1] = nv[1]; pre[j + 1][2] = nv[2];
+                } else {
+                    double z4[4] = {0.0, 0.0, 0.0, 0.0}, zx[8];
+                    float nv[3];
+                    adj::vjp_receptor(z4, zx, K.is_anion, K.is_anion ? K.P_Cl : K.P_Na, K.P_K, V2, pre[j], out2, wv,
+                                      d.sl_rden[y * kRecPerSyn + j], area, open, c.vol, dt, nv);
+                    pre[j + 1][0] = nv[0]; pre[j + 1][1] = nv[1]; pre[j + 1][3] = nv[2];
+                }
             }
+            // the adjoints of the synapse's state words (an NMDA receptor's inactivation gate)
+            float* lsy = lam + (kFull ? d.W : kW3) * Sm + ly * kSynWords;
             double gw = 0.0;
             for (int j = (int)nrec - 1; j >= 0; j--) {
-                const RecKind& K = gRec[d.sl_kind[y * kRecPerSyn + j]];
-                const double l4[4] = {(double)lin[0], (double)lin[1], (double)lin[3], (double)lib};
-                double lx[8];
+                const int kind = d.sl_kind[y * kRecPerSyn + j];
+                const RecKind& K = gRec[kind];
+                const float open = sc.syn[ly * kSynScr + 7 + j];
                 float nv[3];
-                adj::vjp_receptor(l4, lx, K.is_anion, K.is_anion ? K.P_Cl : K.P_Na, K.P_K, V2, pre[j], out2, wv,
-                                  d.sl_rden[y * kRecPerSyn + j], area, sc.syn[ly * 9 + 7 + j], c.vol, dt, nv);
-                lV2 += (float)lx[0];
-                lin[0] = (float)lx[1]; lin[1] = (float)lx[2]; lin[3] = (float)lx[3];
-                lout[0] += (float)lx[4]; lout[1] += (float)lx[5]; lout[3] += (float)lx[6];
-                gw += lx[7];
+                if (kind == 1) {
+                    const double l5[5] = {(double)lin[0], (double)lin[1], (double)lin[2], (double)lib,
+                                          (double)lsy[2 * j + 1]};
+                    double lx[9];
+                    adj::vjp_nmda(l5, lx, K.P_Na, K.P_K, K.P_Ca, V2, pre[j], out2, wv, d.sl_rden[y * kRecPerSyn + j],
+                                  area, open, sc.syn[ly * kSynScr + 9 + j], c.vol, dt, nv);
+                    lV2 += (float)lx[0];
+                    lin[0] = (float)lx[1]; lin[1] = (float)lx[2]; lin[2] = (float)lx[3];
+                    lout[0] += (float)lx[4]; lout[1] += (float)lx[5]; lout[2] += (float)lx[6];
+                    gw += lx[7];
+                    lsy[2 * j + 1] = (float)lx[8];
+                } else {
+                    const double l4[4] = {(double)lin[0], (double)lin[1], (double)lin[3], (double)lib};
+                    double lx[8];
+                    adj::vjp_receptor(l4, lx, K.is_anion, K.is_anion ? K.P_Cl : K.P_Na, K.P_K, V2, pre[j], out2, wv,
+                                      d.sl_rden[y * kRecPerSyn + j], area, open, c.vol, dt, nv);
+                    lV2 += (float)lx[0];
+                    lin[0] = (float)lx[1]; lin[1] = (float)lx[2]; lin[3] = (float)lx[3];
+                    lout[0] += (float)lx[4]; lout[1] += (float)lx[5]; lout[3] += (float)lx[6];
+                    gw += lx[7];
+                }
             }
             d.g_w[(size_t)c.p * d.n_syn + syn] += gw;
         }
@@ -1228,7 +1261,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_adj_backward(AdjDev d,
     const uint32_t Sm = d.Smax;
     {   // adjoint of the state at the window's end
         const float* src = d.lam + (size_t)c.p * d.L + c.st_off;
-        for (uint32_t q = threadIdx.x; q < W * c.S; q += blockDim.x) L.lam[(q / c.S) * Sm + (q % c.S)] = src[q];
+        block_load(L.lam, src, c, Sm, W);
     }
     // Walk the ticks backwards: each is re-run from its starting state with its
     // intermediates recorded, then reversed.
@@ -1244,7 +1277,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_adj_backward(AdjDev d,
     }
     {
         float* dst = d.lam + (size_t)c.p * d.L + c.st_off;
-        for (uint32_t q = threadIdx.x; q < W * c.S; q += blockDim.x) dst[q] = L.lam[(q / c.S) * Sm + (q % c.S)];
+        block_store(dst, L.lam, c, Sm, W);
     }
     if (threadIdx.x < c.S)
         for (int k = 0; k < 3; k++) d.g_par[((size_t)c.p * 3 + k) * d.n_seg + c.g] += gp[k];
@@ -1515,17 +1548,19 @@ int adj_build(Adjoint* A, void* sim, const BncAdjointConfig& cfg) {
         for (uint32_t j = 0; j < s.post_receptor_count; j++) {
             const ModLite& m = hn.post_rec(k, j);
             if (myel_post && host_is_ionotropic(m.type)) continue;   // simulation_host.cpp:495
-            if (m.type != BNC_MOD_AMPA && m.type != BNC_MOD_GABAA && m.type != BNC_MOD_GLYCINE) {
-                set_error("adjoint: receptor type %u on synapse %u is not differentiated (AMPA, GABA-A and glycine are)",
+            if (m.type != BNC_MOD_AMPA && m.type != BNC_MOD_NMDA && m.type != BNC_MOD_GABAA && m.type != BNC_MOD_GLYCINE) {
+                set_error("adjoint: receptor type %u on synapse %u is not differentiated (AMPA, NMDA, GABA-A and glycine are)",
                           (unsigned)m.type, k);
                 return BNC_ERR_UNSUPPORTED;
             }
             if (m.active_vars != 0) { set_error("adjoint: receptor conductance overrides are not modelled"); return BNC_ERR_UNSUPPORTED; }
             if (r >= (uint32_t)kRecPerSyn) { set_error("adjoint: synapse %u has more than %d receptors", k, kRecPerSyn); return BNC_ERR_UNSUPPORTED; }
-            sl_kind[(size_t)y * kRecPerSyn + r] = (m.type == BNC_MOD_AMPA) ? 0 : (m.type == BNC_MOD_GABAA ? 2 : 3);
+            sl_kind[(size_t)y * kRecPerSyn + r] =
+                (m.type == BNC_MOD_AMPA) ? 0 : (m.type == BNC_MOD_NMDA ? 1 : (m.type == BNC_MOD_GABAA ? 2 : 3));
             sl_rden[(size_t)y * kRecPerSyn + r] = m.density;
             rinit[(size_t)y * kSynWords + 2 * r] = m.state[0];
-            rinit[(size_t)y * kSynWords + 2 * r + 1] = m.state[1];
+            // NMDA does not desensitise: its second word carries the inactivation gate
+            rinit[(size_t)y * kSynWords + 2 * r + 1] = m.type == BNC_MOD_NMDA ? m.state[2] : m.state[1];
             r++;
         }
         sl_nrec[y] = (uint8_t)r;

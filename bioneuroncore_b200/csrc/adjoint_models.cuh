@@ -422,6 +422,69 @@ __device__ __forceinline__ void vjp_receptor(const double* lo, double* lx, int a
     lx[7] = (lIa * P_a * Ga.F + lIb * P_b * Gb.F) * Nk;
 }
 
+// The NMDA receptor (receptors_biological.cpp:48-70): GHK Na+, K+ and Ca2+ currents of
+// the open receptors, each moving its ion (the ions clamped at 1e-9 as masks), the Mg2+
+// block of the membrane potential, and the Ca2+-dependent inactivation gate cdi
+// (modifier_helpers.h:1281-1290), which relaxes toward a value set by the Ca2+ the
+// receptor has just let in and scales the returned current with the co-agonist factor.
+// The divalent GHK flux is 2 x the monovalent one at 2V.  Float roundings are
+// identities and the gate's time constant is the branch the forward took.
+// lo = adjoints of (c_in Na', K', Ca', returned I, cdi'); lx = adjoints of (V, c_in Na,
+// K, Ca, c_out Na, K, Ca, weight, cdi); nv = c_in Na', K', Ca' as the forward leaves them.
+__device__ __forceinline__ void vjp_nmda(const double* lo, double* lx, double P_Na, double P_K, double P_Ca, float V0,
+                                         const float* in, const float* out, float w, float den, float area, float open,
+                                         float cdi0, double vol, float dt, float* nv) {
+    const double cpm = kF * vol / 1000.0;
+    const double Nk = (double)den * (double)area * (double)open * 1e12;
+    const double W = (double)w, T = (double)dt;
+    for (int k = 0; k < 9; k++) lx[k] = 0.0;
+    const GhkD Ga = ghk_mono_d((double)V0, in[0], out[0]);
+    const GhkD Gb = ghk_mono_d((double)V0, in[1], out[1]);
+    const GhkD Gh = ghk_mono_d(2.0 * (double)V0, in[2], out[2]);
+    const double Fc = 2.0 * Gh.F, dVc = 4.0 * Gh.dV, dcic = 2.0 * Gh.dci, dcoc = 2.0 * Gh.dco;
+    const double Ia = P_Na * Ga.F * Nk * W, Ib = P_K * Gb.F * Nk * W, Ic = P_Ca * Fc * Nk * W;
+    const double n0 = (double)in[0] - Ia * T / cpm, n1 = (double)in[1] - Ib * T / cpm;
+    const double n2 = (double)in[2] - Ic * T / (2.0 * cpm);
+    const bool m0 = n0 >= 1e-9, m1 = n1 >= 1e-9, m2 = n2 >= 1e-9;
+    nv[0] = (float)(m0 ? n0 : 1e-9);
+    nv[1] = (float)(m1 ? n1 : 1e-9);
+    nv[2] = (float)(m2 ? n2 : 1e-9);
+    const double I0 = -(Ia + Ib + Ic);
+    // Mg2+ block: 1 / (1 + e^(-0.062 V) / 3.57)
+    const double a = (double)(1.0f / 3.57f), b = (double)0.062f;
+    const double ex = adj_exp(-b * (double)V0);
+    const double mg = 1.0 / (1.0 + a * ex);
+    const double dmg = mg * mg * a * b * ex;
+    // inactivation gate from the Ca2+ after the receptor's own influx
+    const double u = (double)nv[2] * 1000.0;
+    const double cinf = 1.0 - (double)0.8f * u / (u + 1.0);
+    const double tau = (cinf < (double)cdi0) ? 500.0 : 9000.0;
+    const double craw = (double)cdi0 + (cinf - (double)cdi0) * T / tau;
+    const bool mc = craw >= 0.0 && craw <= 1.0;
+    const double cnew = mc ? craw : (craw < 0.0 ? 0.0 : 1.0);
+    const double coag = (double)(10.0f / 11.0f);
+    const double lI = lo[3];
+    const double lcnew = lo[4] + lI * I0 * mg * coag;
+    lx[0] = lI * I0 * cnew * coag * dmg;
+    const double lI0 = lI * mg * cnew * coag;
+    const double lcraw = mc ? lcnew : 0.0;
+    lx[8] = lcraw * (1.0 - T / tau);
+    const double lu = lcraw * (T / tau) * (-(double)0.8f / ((u + 1.0) * (u + 1.0)));
+    const double ln0 = lo[0], ln1 = lo[1], ln2 = lo[2] + lu * 1000.0;
+    const double lIa = -lI0 - (m0 ? ln0 * T / cpm : 0.0);
+    const double lIb = -lI0 - (m1 ? ln1 * T / cpm : 0.0);
+    const double lIc = -lI0 - (m2 ? ln2 * T / (2.0 * cpm) : 0.0);
+    const double lFa = lIa * P_Na * Nk * W, lFb = lIb * P_K * Nk * W, lFc = lIc * P_Ca * Nk * W;
+    lx[0] += lFa * Ga.dV + lFb * Gb.dV + lFc * dVc;
+    lx[1] = (m0 ? ln0 : 0.0) + lFa * Ga.dci;
+    lx[2] = (m1 ? ln1 : 0.0) + lFb * Gb.dci;
+    lx[3] = (m2 ? ln2 : 0.0) + lFc * dcic;
+    lx[4] = lFa * Ga.dco;
+    lx[5] = lFb * Gb.dco;
+    lx[6] = lFc * dcoc;
+    lx[7] = (lIa * P_Na * Ga.F + lIb * P_K * Gb.F + lIc * P_Ca * Fc) * Nk;
+}
+
 // ---- the same products in single precision ----
 // The reverse tick's hot path.  Differences that cancel near zero -- 1 - e^-u in
 // vtrap and in the GHK flux -- are formed with expm1f, so they keep full relative

@@ -304,6 +304,8 @@ int generate_network(const BncNetgenParams& p, NetSink& sink, NetShape* shape_ou
                 else rt = (rng_syn.u01() < 0.5) ? BNC_MOD_AMPA : BNC_MOD_NMDA;
                 set_mod(sy.post_receptors[j], rt, 200.0);
             }
+            if ((p.flags & BNC_NETGEN_NMDA) && sy.post_receptors[0].type == BNC_MOD_AMPA && nr < BNC_MAX_POST_RECEPTORS)
+                set_mod(sy.post_receptors[nr++], BNC_MOD_NMDA, 200.0);
             sy.post_receptor_count = (uint8_t)nr;
             if (p.flags & BNC_NETGEN_SYNAPSE_EXTRAS) {
                 if (rng_extra.u01() < 0.3) {

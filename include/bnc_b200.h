@@ -154,6 +154,9 @@ typedef struct {
  * chemical synapses in the synapse order; connexin-36 (114) on every soma and
  * connexin-43 (198) on every other one. */
 #define BNC_NETGEN_GAP_JUNCTIONS 2048u
+/* Synapses whose first receptor is AMPA also get an NMDA receptor (9) as their next
+ * one: density 200, CDI gate (state[2]) 1; other draws are unchanged. */
+#define BNC_NETGEN_NMDA 4096u
 
 /* Generates a network into host AoS arrays in the reference layout.  The arrays
  * are owned by the library; release with bnc_netgen_free.  *stim receives the

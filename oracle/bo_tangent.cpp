@@ -142,6 +142,7 @@ struct Syn {
     uint8_t n_r, rtype[8], nt;
     double rden[8];
     double r[8], dd[8];   // receptor gates (values: they depend on the clefts only)
+    T cdi[8];             // NMDA Ca2+-dependent inactivation gate (state[2]): follows Ca2+, so a tangent
     double cleft, tauc, parea;
     uint32_t ev_b, ev_e;  // log range
 };
@@ -225,11 +226,13 @@ int bo_tangent_run(const BncBionData* net, const BncCurrentStimulus* stim, uint3
         for (uint32_t j = 0; j < y.post_receptor_count; j++) {
             const BncModifier& m = y.post_receptors[j];
             if (myel_post && is_ionotropic(m.type)) continue;
-            if (m.type != BNC_MOD_AMPA && m.type != BNC_MOD_GABAA && m.type != BNC_MOD_GLYCINE) return -1;
+            if (m.type != BNC_MOD_AMPA && m.type != BNC_MOD_GABAA && m.type != BNC_MOD_GLYCINE && m.type != BNC_MOD_NMDA)
+                return -1;
             s.rtype[s.n_r] = m.type;
             s.rden[s.n_r] = (double)(float)m.density;
             s.r[s.n_r] = (double)(float)m.state[0];
             s.dd[s.n_r] = (double)(float)m.state[1];
+            s.cdi[s.n_r] = T((double)(float)m.state[2]);
             s.n_r++;
         }
         s.cleft = y.cleft_neurotransmitter[s.nt == 2 ? BNC_NT_GLYCINE : s.nt];
@@ -504,7 +507,40 @@ int bo_tangent_run(const BncBionData* net, const BncCurrentStimulus* stim, uint3
             const T w(p_w[k], d_w[k]);
             const double cpm = F * s.vol / 1000.0;
             for (int j = 0; j < y.n_r; j++) {
-                // receptors_biological.cpp:42-82: AMPA, GABA-A, glycine
+                // receptors_biological.cpp:42-82: AMPA, NMDA, GABA-A, glycine
+                const bool nmda = y.rtype[j] == BNC_MOD_NMDA;
+                if (nmda) {
+                    // gating on glutamate without desensitisation (EC50 1, rise 5 ms, decay 50
+                    // ms); GHK Na+, K+ and Ca2+ currents with the 0.08 / 0.08 / 0.84 split of
+                    // 50 pS (modifier_helpers.h:69-76, 1213-1279); the Mg2+ block of the
+                    // membrane potential and the Ca2+-dependent inactivation gate that follows
+                    // the Ca2+ the receptor has just let in (modifier_helpers.h:1281-1290)
+                    const double nt = nt_glu[y.post];
+                    const double r_inf = nt / (nt + 1.0);
+                    const double tau = r_inf > y.r[j] ? 5.0 : 50.0;
+                    y.r[j] = std::min(1.0, std::max(0.0, y.r[j] + (r_inf - y.r[j]) * (double)dt / tau));
+                    const double area = y.parea > 0.0 ? y.parea : s.area;
+                    const double Nk = y.rden[j] * area * y.r[j];
+                    const double cNa = (double)55.964f, cK = (double)40.514f, cCa = (double)0.12775f;
+                    const double wsum = (double)0.08f * cNa + (double)0.08f * cK + (double)0.84f * 4.0 * cCa;
+                    const double PNa = ghk_P(50.0 * (double)0.08f * cNa / wsum, 1.0, cNa);
+                    const double PK = ghk_P(50.0 * (double)0.08f * cK / wsum, 1.0, cK);
+                    const double PCa = ghk_P(50.0 * (double)0.84f * 4.0 * cCa / wsum, 2.0, cCa);
+                    T INa = T(PNa) * ghk_mono(s.V, s.in[0], s.out[0]) * Nk * w * 1e12;
+                    T IK = T(PK) * ghk_mono(s.V, s.in[1], s.out[1]) * Nk * w * 1e12;
+                    T ICa = T(PCa) * ghk_div(s.V, s.in[2], s.out[2]) * Nk * w * 1e12;
+                    s.in[0] = s.in[0] - INa * (double)dt / cpm;
+                    s.in[1] = s.in[1] - IK * (double)dt / cpm;
+                    s.in[2] = s.in[2] - ICa * (double)dt / (2.0 * cpm);
+                    clamp_ions(s.in);
+                    const T mg = T(1.0) / (T(1.0) + T((double)(1.0f / 3.57f)) * texp(s.V * -(double)0.062f));
+                    const T ca_uM = s.in[2] * 1000.0;
+                    const T cinf = T(1.0) - T((double)0.8f) * ca_uM / (ca_uM + 1.0);
+                    const double tcdi = cinf.v < y.cdi[j].v ? 500.0 : 9000.0;
+                    y.cdi[j] = clampT(y.cdi[j] + (cinf - y.cdi[j]) * ((double)dt / tcdi), 0.0, 1.0);
+                    I_syn = I_syn - (INa + IK + ICa) * mg * y.cdi[j] * (double)(10.0f / 11.0f);
+                    continue;
+                }
                 const bool ampa = y.rtype[j] == BNC_MOD_AMPA, gly = y.rtype[j] == BNC_MOD_GLYCINE;
                 const double EC50 = ampa ? 0.5 : (gly ? 0.5 : 1.0), tr = ampa ? 0.5 : (gly ? 0.3 : 1.0),
                              td = ampa ? 3.0 : 5.0, tdes = ampa ? 3.0 : 2000.0;

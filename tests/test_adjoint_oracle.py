@@ -4,7 +4,8 @@ Also the oracle's release log, which the replay feeds on."""
 import numpy as np
 import pytest
 
-from bioneuroncore_b200 import Network, NetgenParams, NET_ADJOINT, NETGEN_FULL_SMALL_SET, NETGEN_GLYCINE
+from bioneuroncore_b200 import (Network, NetgenParams, NET_ADJOINT, NETGEN_FULL_SMALL_SET, NETGEN_GLYCINE,
+                                NETGEN_NMDA)
 
 DT = 0.025
 
@@ -31,16 +32,19 @@ def test_release_log_is_sorted_and_positive():
     assert (amt > 0).all() and (tick < 400).all()
 
 
-@pytest.mark.parametrize("flags", [0, NETGEN_FULL_SMALL_SET, NETGEN_GLYCINE])
+@pytest.mark.parametrize("flags", [0, NETGEN_FULL_SMALL_SET, NETGEN_GLYCINE, NETGEN_NMDA])
 def test_tangent_matches_its_central_differences(flags):
     """With the fitting family, with the whole small set (Cav1.3, the Na/K pump and
-    the ATP it consumes, which diffuses), and with glycine receptors first on the
+    the ATP it consumes, which diffuses), with glycine receptors first on the
     odd-numbered synapses (4 neurons over 400 ticks, where synapse 17, a glycine
-    synapse, releases)."""
+    synapse, releases), and with an NMDA receptor after the AMPA one of every
+    excitatory synapse (its Ca2+ current, Mg2+ block and Ca2+-dependent inactivation
+    gate carry the tangent)."""
     from oracle.oracle import Oracle, tangent_loss
     gly = bool(flags & NETGEN_GLYCINE)
-    n, ticks = (4, 400) if gly else (3, 300)
-    p = NetgenParams(family=NET_ADJOINT, n_neurons=n, seed=7 if gly else 11, flags=flags)
+    nmda = bool(flags & NETGEN_NMDA)
+    n, ticks = (4, 400) if (gly or nmda) else (3, 300)
+    p = NetgenParams(family=NET_ADJOINT, n_neurons=n, seed=7 if (gly or nmda) else 11, flags=flags)
     net = Network(p)
     log = Oracle(Network(p)).run_logged(ticks, DT)
     base = _densities(net)
@@ -52,9 +56,14 @@ def test_tangent_matches_its_central_differences(flags):
     if gly:
         is_gly = net.synapses["post_receptors"][:, 0]["type"] == 12
         assert is_gly[np.unique(log[0])].any()          # a glycine synapse releases
+    if nmda:
+        is_nmda = net.synapses["post_receptors"][:, 1]["type"] == 9
+        assert is_nmda[np.unique(log[0])].any()         # an NMDA synapse releases
     dirs = [dvec]
     if gly:   # the weights of the glycine synapses alone
         dirs.append(zero[:3] + [np.where(is_gly, base[3], 0.0)])
+    if nmda:  # the weights of the synapses with an NMDA receptor alone
+        dirs.append(zero[:3] + [np.where(is_nmda, base[3], 0.0)])
     for dv in dirs:
         L, dL = tangent_loss(net, log, ticks, DT, base, dv, soma, target)
         h = 1e-4

@@ -5,13 +5,15 @@ The network is the fitting family (BNC_NET_ADJOINT: Nav1.x, Kv_DR and K2P leak p
 segment, myelin on alternate axon segments, Cav2.1 on axons, AMPA/GABA-A synapses,
 a 1 nA step into 10% of somata), and for the replay and the gradients also the same
 family with the whole small set (BNC_NETGEN_FULL_SMALL_SET: Cav1.3 and the Na/K pump
-on every segment, the pump's ATP diffusing).  All tests are marked gpu.
+on every segment, the pump's ATP diffusing), with glycine receptors, and with an NMDA
+receptor after the AMPA one of every excitatory synapse (BNC_NETGEN_NMDA: Ca2+ current,
+Mg2+ block, Ca2+-dependent inactivation gate).  All tests are marked gpu.
 """
 import numpy as np
 import pytest
 
 from bioneuroncore_b200 import (Adjoint, Backend, Network, NetgenParams, NET_ADJOINT, NETGEN_FULL_SMALL_SET,
-                                NETGEN_GLYCINE)
+                                NETGEN_GLYCINE, NETGEN_NMDA)
 
 DT = 0.025
 
@@ -38,7 +40,7 @@ def _plain_soma_trace(p, soma, ticks):
     return out
 
 
-@pytest.mark.parametrize("flags", [0, NETGEN_FULL_SMALL_SET, NETGEN_GLYCINE])
+@pytest.mark.parametrize("flags", [0, NETGEN_FULL_SMALL_SET, NETGEN_GLYCINE, NETGEN_NMDA])
 def test_replay_forward_is_the_plain_trajectory(flags):
     """The forward pass, replaying the release log, reproduces the plain tick's somatic
     voltages bit for bit (same device functions, same operation order)."""
@@ -66,7 +68,7 @@ def _fit_problem(ticks, n_sets, n_neurons=4, scale=(1.1, 0.9, 1.2, 0.8), flags=0
     return p, net, adj, base, tr[0]
 
 
-@pytest.mark.parametrize("flags", [0, NETGEN_FULL_SMALL_SET, NETGEN_GLYCINE])
+@pytest.mark.parametrize("flags", [0, NETGEN_FULL_SMALL_SET, NETGEN_GLYCINE, NETGEN_NMDA])
 def test_gradient_matches_fp64_forward_mode_and_central_differences(flags):
     """The device adjoint's gradient along a random direction of all parameters (gNa,
     gK, gleak per segment, weight per synapse) against (a) the FP64 CPU forward-mode
@@ -103,6 +105,16 @@ def test_gradient_matches_fp64_forward_mode_and_central_differences(flags):
         _, tk = tangent_loss(Network(p), log, ticks, DT, b64, dk, adj.soma, target)
         ak = float(np.dot(g[k][0].astype(np.float64), dvec[k]))
         assert abs(ak - tk) <= 1e-2 * abs(tk) + 1e-6, "class %d: adjoint %.9g vs FP64 forward mode %.9g" % (k, ak, tk)
+    if flags & NETGEN_NMDA:
+        # the weights of the synapses with an NMDA receptor, one of which releases
+        is_nmda = net.synapses["post_receptors"][:, 1]["type"] == 9
+        assert is_nmda[np.unique(log[0])].any()
+        dk = [np.zeros_like(x) for x in b64]
+        dk[3] = np.where(is_nmda, dvec[3], 0.0)
+        _, tk = tangent_loss(Network(p), log, ticks, DT, b64, dk, adj.soma, target)
+        ak = float(np.dot(g[3][0].astype(np.float64), dk[3]))
+        assert abs(tk) > 1e-4
+        assert abs(ak - tk) <= 1e-2 * abs(tk), "NMDA synapses' weights: adjoint %.9g vs FP64 forward mode %.9g" % (ak, tk)
 
 
 def test_fit_reduces_the_loss_from_the_untrained_parameters():
