@@ -552,7 +552,7 @@ int bnc_sweep_run(void* sim, const BncBionData* base, const BncCurrentStimulus* 
  *
  * Modelled networks (others are rejected with BNC_ERR_UNSUPPORTED): segment
  * modifiers Nav1.6, Nav1.2, Kv_DR, K2P (differentiated), myelin and Cav2.1 (no
- * current); chemical synapses with AMPA, GABA-A and glycine receptors (at most 2 each);
+ * current); chemical synapses with AMPA, NMDA, GABA-A and glycine receptors (at most 2 each);
  * neurons of at most 128 segments and 4 connections per segment, each a contiguous segment range joined by its
  * connections; no voltage clamps. */
 typedef struct {
