@@ -1014,6 +1014,8 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
         }
     });
     auto item_type = [&](uint32_t q) { return keys[q].type; };
+    bool type_present[256] = {false};   // item types of the network (the scans below skip absent ones)
+    for (uint8_t t : act_type) type_present[t] = true;
     if (!allocs) {   // a host-only plan checks what the device conversion would
         FirstError bad;
         parallel_for(NI, [&](size_t q0, size_t q1) {
@@ -1316,7 +1318,7 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
     {
         bool any_ecb = false;
         std::vector<uint8_t> best_slot;
-        for (uint32_t q = 0; q < NI; q++) {
+        for (uint32_t q = 0; q < NI && type_present[86]; q++) {
             if (item_type(q) != 86) continue;
             if (!any_ecb) { any_ecb = true; seg_ecb_item.assign(n, UINT32_MAX); best_slot.assign(n, 0xFF); }
             const uint32_t dseg = host->inv[host->item_seg[q]];
@@ -1369,7 +1371,7 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
         }
         // each segment's connexin-36 and connexin-43 items (at most one of each)
         seg_cx.assign((size_t)2 * n, UINT32_MAX);
-        for (uint32_t q = 0; q < NI; q++) {
+        for (uint32_t q = 0; q < NI && (type_present[114] || type_present[198]); q++) {
             const uint8_t t = item_type(q);
             if (t != 114 && t != 198) continue;
             const size_t at = (size_t)(t == 198 ? 1 : 0) * n + host->inv[host->item_seg[q]];
@@ -1385,7 +1387,7 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
     std::vector<uint32_t> gl_seg, gl_off, gl_syn;
     if (K) {
         std::vector<uint32_t> glia;
-        for (uint32_t i = 0; i < n && glia.size() < 256; i++)
+        for (uint32_t i = 0; i < n && glia.size() < 256 && type_present[147]; i++)
             for (uint8_t j = 0; j < hn.seg[i].modifier_count; j++)
                 if (hn.mod(i, j).type == 147) { glia.push_back(i); break; }
         if (!glia.empty()) {
@@ -1625,11 +1627,7 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
             dev->seg_cx = up(allocs, seg_cx, &rc);
             dev->n_gj = (uint32_t)gj_pre.size();
         }
-        dev->model_extras = 0;
-        for (uint32_t q = 0; q < NI && !dev->model_extras; q++) {
-            const uint8_t t = item_type(q);
-            if (t == 86 || t == 114 || t == 147 || t == 198) dev->model_extras = 1;
-        }
+        dev->model_extras = (type_present[86] || type_present[114] || type_present[147] || type_present[198]) ? 1u : 0u;
         if (!gl_seg.empty()) {
             dev->gl_cap = zeros<float>(allocs, K, &rc);
             dev->gl_seg = up(allocs, gl_seg, &rc);
