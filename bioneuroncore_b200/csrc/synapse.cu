@@ -83,6 +83,159 @@ __device__ __forceinline__ void log_release(const NetDev& d, uint32_t k, unsigne
 
 // kX: the network has release modulators, eCB, glia or gap junctions; the plain
 // instantiation leaves their code (and registers) out.
+// Step 3's presynaptic half of synapse k (simulation_host.cpp:322-460): delayed
+// arrivals, RRP recovery, bouton Ca2+, the Ca2+-dependent release and its delay slot.
+// It reads the presynaptic segment's record and the synapse's own state only, so the
+// synapses can take it in any order: networks without release modulators, eCB, glia
+// and gap junctions run it for all synapses at once (k_release) before the per-segment
+// half; the others run it in the segment's synapse loop.
+template <bool kX>
+__device__ __forceinline__ void presyn_step(const NetDev& d, uint32_t k, uint32_t K, unsigned long long tick, float dt,
+                                            float& cleft, float& cleft_e, float& rrp, float& rrp_max, float& bouton,
+                                            uint8_t& refr, uint8_t& sf, int& ntt) {
+    const uint32_t pre = d.sy_pre[k];
+    const float4 pr = d.pre_rec[pre];
+    sf = d.sy_flags[k];
+    ntt = sf >> 4;
+    cleft = d.sy_cleft[k];
+    if (kX && d.sy_cleft_ecb) cleft_e = d.sy_cleft_ecb[k];
+    const float delay = d.sy_delay[k];
+    // delayed releases (delay_buffer.h:31-44)
+    if ((d.flags & NF_DELAY) && delay > 0.0f) {
+        for (int q = 0; q < 4; q++) {
+            unsigned long long arr = d.dl_arr[(size_t)q * K + k];
+            if (arr == 0) continue;
+            if (arr <= tick) {
+                cleft += d.dl_amt[(size_t)q * K + k];
+                if (d.ev_buf) log_release(d, k, tick, d.dl_amt[(size_t)q * K + k], q);
+                d.dl_arr[(size_t)q * K + k] = 0;
+            }
+        }
+    }
+    // RRP recovery (kernel_dispatch.h:612-630); no CaMKII/calcineurin modifiers
+    rrp_max = d.sy_rrp_max[k];
+    if (rrp_max > 0.0f) rrp = d.sy_rrp[k];
+    if (!(rrp_max <= 0.0f || rrp >= rrp_max)) {
+        float ca_pre = d.pre_ext[pre].z;
+        float ca_f = ca_pre / (0.0005f + ca_pre);
+        float priming = d.sy_rrp_rec[k] + 0.0f * 0.02f + 0.0f * 0.01f;
+        priming *= ca_f;
+        float rec = (rrp_max - rrp) * priming * dt;
+        rrp += rec;
+        if (rrp > rrp_max) rrp = rrp_max;
+    }
+    // bouton Ca2+ (modifier_helpers.h:764-806)
+    bouton = d.sy_bouton[k];
+    const float pre_area = d.sy_pre_area[k];
+    {
+        const float g_K = d.sy_gK[k], g_Na = d.sy_gNa[k];
+        float V_bouton = pr.x;
+        if (g_K > 0.0f || g_Na > 0.0f) {
+            float4 ex = d.pre_ext[pre];
+            float koe = d.pre_ext2[pre];
+            float E_K = dp_nernst(ex.y, koe, 1.0f);
+            float E_Na = dp_nernst(ex.x, ex.w, 1.0f);
+            V_bouton = (float)((300.0f * (double)pr.x + g_K * E_K + g_Na * E_Na) / (300.0f + g_K + g_Na));
+        }
+        float cav21_dens = 0.0f, mm = 0.0f, h = 0.0f;
+        if (pr.z != 0.0f) {
+            cav21_dens = pr.z;
+            float m_inf = cav21_m_inf(V_bouton);
+            float h_inf = cav21_h_inf(V_bouton, bouton * MM_TO_UM);
+            mm = m_inf;
+            h = (float)(h_inf + ((double)pr.w - h_inf) * dm_exp(-dt / 300.0f));
+        }
+        float cav21_open = mm * mm * h;
+        double P_single = dp_ghk_P(15.0f, 2.0f, GHK_CBAR_CA_MM);
+        double flux = dp_ghk_div(V_bouton, bouton, (double)pr.y);
+        double I_A = P_single * flux * (cav21_dens * pre_area) * cav21_open;
+        float I_Ca = (float)(I_A * A_TO_PA);
+        bouton = (float)(bouton - I_Ca * dt * 1000.0f / (2.0f * FARADAY_CONST * 0.1f));
+        bouton += (0.0001f - bouton) * dt / 5.0f;
+        if (bouton < 0.0f) bouton = 0.0f;
+    }
+    // Ca2+-dependent release (simulation_host.cpp:421-460)
+    refr = d.sy_refr[k];
+    if (refr == 0) {
+        float Ca_uM = bouton * MM_TO_UM;
+        float ca_act = dm_pow(Ca_uM, 4.0f) / (dm_pow(Ca_uM, 4.0f) + dm_pow(10.0f, 4.0f));
+        float p = d.sy_prel[k] * ca_act;
+        // release modulators of the autoreceptors, in autoreceptor order
+        // (kernel_dispatch.h:575-604, receptors_biological.cpp:428-509); the
+        // bouton channels take the dispatch's default factor 1
+        if (kX && d.md_off) {
+            const uint32_t m1 = d.md_off[k + 1];
+            for (uint32_t mi = d.md_off[k]; mi < m1; mi++) {
+                const uint32_t code = d.md_code[mi];
+                const uint32_t kind = code >> 4;
+                const int mnt = (int)(code & 15u);
+                const float c = mnt == ntt ? cleft : (mnt == 9 ? cleft_e : 0.0f);
+                const float activation = c / (c + 0.5f);
+                const double scale = d.md_scale[mi];
+                float f;
+                if (kind == 3) {
+                    f = (float)(1.0f + (double)(0.3f * activation) * scale);
+                } else {
+                    float s0 = d.md_st[mi];
+                    s0 = (float)((double)s0 + ((double)activation - (double)s0) * (double)dt /
+                                 (kind == 1 ? 50.0 : 30.0));
+                    d.md_st[mi] = s0;
+                    f = (kind == 1) ? (float)(1.0f - (double)0.7f * (double)s0 * scale)
+                                    : (float)(1.0f + (double)0.5f * (double)s0 * scale);
+                }
+                p *= f;
+            }
+        }
+        uint32_t vbits = (uint32_t)(long long)((double)pr.x * 1000.0f);
+        uint32_t seed = d.sy_id[k] ^ (uint32_t)tick ^ vbits;
+        if (xorshift32_rnd(seed) < p) {
+            const float amt = d.sy_amt[k];
+            float release_amt;
+            if (rrp_max <= 0.0f) release_amt = amt * p;
+            else {
+                float avail = amt;
+                if (avail > rrp) avail = rrp;
+                release_amt = avail * p;
+                rrp -= release_amt;
+                if (rrp < 0) rrp = 0;
+            }
+            unsigned long long delay_ticks = (delay <= 0.0f || dt <= 0.0f) ? 0ull
+                : (unsigned long long)((delay / dt) + 0.5f);
+            if (delay_ticks > 0) {
+                for (int q = 0; q < 4; q++) {
+                    if (d.dl_arr[(size_t)q * K + k] == 0) {
+                        d.dl_arr[(size_t)q * K + k] = tick + delay_ticks;
+                        d.dl_amt[(size_t)q * K + k] = release_amt;
+                        d.dl_nt[(size_t)q * K + k] = (uint8_t)ntt;
+                        break;
+                    }
+                }
+            } else {
+                cleft += release_amt;
+                if (d.ev_buf) log_release(d, k, tick, release_amt, 4);
+            }
+            refr = (uint8_t)(uint32_t)(20.0f / dt + 0.5f);
+        }
+    }
+}
+
+// The presynaptic half of every synapse of a network without release modulators, eCB,
+// glia or gap junctions, one thread per synapse; k_synapse<false> reads the cleft,
+// refractory count, bouton Ca2+ and RRP it leaves.
+__global__ void __launch_bounds__(256) k_release(NetDev d, float dt, unsigned long long tick) {
+    if (d.clock) tick = d.clock[0];
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= d.n_syn) return;
+    float cleft = 0.0f, cleft_e = 0.0f, rrp = 0.0f, rrp_max = 0.0f, bouton = 0.0f;
+    uint8_t refr = 0, sf = 0;
+    int ntt = 0;
+    presyn_step<false>(d, k, d.n_syn, tick, dt, cleft, cleft_e, rrp, rrp_max, bouton, refr, sf, ntt);
+    d.sy_cleft[k] = cleft;
+    d.sy_refr[k] = refr;
+    d.sy_bouton[k] = bouton;
+    if (rrp_max > 0.0f) d.sy_rrp[k] = rrp;
+}
+
 template <bool kX>
 __global__ void __launch_bounds__(256, 4)
 k_synapse(NetDev d, float dt, unsigned long long tick, int first_tick) {
@@ -142,129 +295,13 @@ k_synapse(NetDev d, float dt, unsigned long long tick, int first_tick) {
         int ntt = 0;
         uint32_t n_rc = 0;
         if (chem) {
-            const uint32_t pre = d.sy_pre[k];
-            const float4 pr = d.pre_rec[pre];
-            sf = d.sy_flags[k];
-            ntt = sf >> 4;
-            cleft = d.sy_cleft[k];
-            if (kX && d.sy_cleft_ecb) cleft_e = d.sy_cleft_ecb[k];
-            const float delay = d.sy_delay[k];
-            // delayed releases (delay_buffer.h:31-44)
-            if ((d.flags & NF_DELAY) && delay > 0.0f) {
-                for (int q = 0; q < 4; q++) {
-                    unsigned long long arr = d.dl_arr[(size_t)q * K + k];
-                    if (arr == 0) continue;
-                    if (arr <= tick) {
-                        cleft += d.dl_amt[(size_t)q * K + k];
-                        if (d.ev_buf) log_release(d, k, tick, d.dl_amt[(size_t)q * K + k], q);
-                        d.dl_arr[(size_t)q * K + k] = 0;
-                    }
-                }
-            }
-            // RRP recovery (kernel_dispatch.h:612-630); no CaMKII/calcineurin modifiers
-            rrp_max = d.sy_rrp_max[k];
-            if (rrp_max > 0.0f) rrp = d.sy_rrp[k];
-            if (!(rrp_max <= 0.0f || rrp >= rrp_max)) {
-                float ca_pre = d.pre_ext[pre].z;
-                float ca_f = ca_pre / (0.0005f + ca_pre);
-                float priming = d.sy_rrp_rec[k] + 0.0f * 0.02f + 0.0f * 0.01f;
-                priming *= ca_f;
-                float rec = (rrp_max - rrp) * priming * dt;
-                rrp += rec;
-                if (rrp > rrp_max) rrp = rrp_max;
-            }
-            // bouton Ca2+ (modifier_helpers.h:764-806)
-            bouton = d.sy_bouton[k];
-            const float pre_area = d.sy_pre_area[k];
-            {
-                const float g_K = d.sy_gK[k], g_Na = d.sy_gNa[k];
-                float V_bouton = pr.x;
-                if (g_K > 0.0f || g_Na > 0.0f) {
-                    float4 ex = d.pre_ext[pre];
-                    float koe = d.pre_ext2[pre];
-                    float E_K = dp_nernst(ex.y, koe, 1.0f);
-                    float E_Na = dp_nernst(ex.x, ex.w, 1.0f);
-                    V_bouton = (float)((300.0f * (double)pr.x + g_K * E_K + g_Na * E_Na) / (300.0f + g_K + g_Na));
-                }
-                float cav21_dens = 0.0f, mm = 0.0f, h = 0.0f;
-                if (pr.z != 0.0f) {
-                    cav21_dens = pr.z;
-                    float m_inf = cav21_m_inf(V_bouton);
-                    float h_inf = cav21_h_inf(V_bouton, bouton * MM_TO_UM);
-                    mm = m_inf;
-                    h = (float)(h_inf + ((double)pr.w - h_inf) * dm_exp(-dt / 300.0f));
-                }
-                float cav21_open = mm * mm * h;
-                double P_single = dp_ghk_P(15.0f, 2.0f, GHK_CBAR_CA_MM);
-                double flux = dp_ghk_div(V_bouton, bouton, (double)pr.y);
-                double I_A = P_single * flux * (cav21_dens * pre_area) * cav21_open;
-                float I_Ca = (float)(I_A * A_TO_PA);
-                bouton = (float)(bouton - I_Ca * dt * 1000.0f / (2.0f * FARADAY_CONST * 0.1f));
-                bouton += (0.0001f - bouton) * dt / 5.0f;
-                if (bouton < 0.0f) bouton = 0.0f;
-            }
-            // Ca2+-dependent release (simulation_host.cpp:421-460)
-            refr = d.sy_refr[k];
-            if (refr == 0) {
-                float Ca_uM = bouton * MM_TO_UM;
-                float ca_act = dm_pow(Ca_uM, 4.0f) / (dm_pow(Ca_uM, 4.0f) + dm_pow(10.0f, 4.0f));
-                float p = d.sy_prel[k] * ca_act;
-                // release modulators of the autoreceptors, in autoreceptor order
-                // (kernel_dispatch.h:575-604, receptors_biological.cpp:428-509); the
-                // bouton channels take the dispatch's default factor 1
-                if (kX && d.md_off) {
-                    const uint32_t m1 = d.md_off[k + 1];
-                    for (uint32_t mi = d.md_off[k]; mi < m1; mi++) {
-                        const uint32_t code = d.md_code[mi];
-                        const uint32_t kind = code >> 4;
-                        const int mnt = (int)(code & 15u);
-                        const float c = mnt == ntt ? cleft : (mnt == 9 ? cleft_e : 0.0f);
-                        const float activation = c / (c + 0.5f);
-                        const double scale = d.md_scale[mi];
-                        float f;
-                        if (kind == 3) {
-                            f = (float)(1.0f + (double)(0.3f * activation) * scale);
-                        } else {
-                            float s0 = d.md_st[mi];
-                            s0 = (float)((double)s0 + ((double)activation - (double)s0) * (double)dt /
-                                         (kind == 1 ? 50.0 : 30.0));
-                            d.md_st[mi] = s0;
-                            f = (kind == 1) ? (float)(1.0f - (double)0.7f * (double)s0 * scale)
-                                            : (float)(1.0f + (double)0.5f * (double)s0 * scale);
-                        }
-                        p *= f;
-                    }
-                }
-                uint32_t vbits = (uint32_t)(long long)((double)pr.x * 1000.0f);
-                uint32_t seed = d.sy_id[k] ^ (uint32_t)tick ^ vbits;
-                if (xorshift32_rnd(seed) < p) {
-                    const float amt = d.sy_amt[k];
-                    float release_amt;
-                    if (rrp_max <= 0.0f) release_amt = amt * p;
-                    else {
-                        float avail = amt;
-                        if (avail > rrp) avail = rrp;
-                        release_amt = avail * p;
-                        rrp -= release_amt;
-                        if (rrp < 0) rrp = 0;
-                    }
-                    unsigned long long delay_ticks = (delay <= 0.0f || dt <= 0.0f) ? 0ull
-                        : (unsigned long long)((delay / dt) + 0.5f);
-                    if (delay_ticks > 0) {
-                        for (int q = 0; q < 4; q++) {
-                            if (d.dl_arr[(size_t)q * K + k] == 0) {
-                                d.dl_arr[(size_t)q * K + k] = tick + delay_ticks;
-                                d.dl_amt[(size_t)q * K + k] = release_amt;
-                                d.dl_nt[(size_t)q * K + k] = (uint8_t)ntt;
-                                break;
-                            }
-                        }
-                    } else {
-                        cleft += release_amt;
-                        if (d.ev_buf) log_release(d, k, tick, release_amt, 4);
-                    }
-                    refr = (uint8_t)(uint32_t)(20.0f / dt + 0.5f);
-                }
+            if (kX) {
+                presyn_step<true>(d, k, K, tick, dt, cleft, cleft_e, rrp, rrp_max, bouton, refr, sf, ntt);
+            } else {   // k_release ran the presynaptic half
+                sf = d.sy_flags[k];
+                ntt = sf >> 4;
+                cleft = d.sy_cleft[k];
+                refr = d.sy_refr[k];
             }
             // NT into the postsynaptic segment (simulation_host.cpp:463-465)
             if (ntt == 0) nt_glu += cleft;
@@ -407,13 +444,13 @@ k_synapse(NetDev d, float dt, unsigned long long tick, int first_tick) {
             d.sy_cleft[k] = cleft;
             if (kX && d.sy_cleft_ecb) d.sy_cleft_ecb[k] = cleft_e;
             d.sy_refr[k] = refr;
-            d.sy_bouton[k] = bouton;
+            if (kX) d.sy_bouton[k] = bouton;   // else k_release stored it
             d.sy_spine[k] = spine;
             d.sy_camkii[k] = camkii;
             d.sy_calcn[k] = calcn;
             d.sy_facil[k] = facil;
             d.sy_weight[k] = weight;
-            if (rrp_max > 0.0f) d.sy_rrp[k] = rrp;
+            if (kX && rrp_max > 0.0f) d.sy_rrp[k] = rrp;
         }
         base += n_act;
     }
@@ -495,7 +532,10 @@ cudaError_t launch_synapse(const NetDev& dev, float dt, unsigned long long tick,
                            cudaStream_t stream) {
     const bool extras = dev.md_off || dev.sy_cleft_ecb || dev.gl_cap || dev.sy_gj;
     if (extras) k_synapse<true><<<(dev.n_seg + 255) / 256, 256, 0, stream>>>(dev, dt, tick, first_tick);
-    else k_synapse<false><<<(dev.n_seg + 255) / 256, 256, 0, stream>>>(dev, dt, tick, first_tick);
+    else {
+        if (dev.n_syn) k_release<<<(dev.n_syn + 255) / 256, 256, 0, stream>>>(dev, dt, tick);
+        k_synapse<false><<<(dev.n_seg + 255) / 256, 256, 0, stream>>>(dev, dt, tick, first_tick);
+    }
     if (dev.gl_cap) k_glia<<<(dev.n_glia + 127) / 128, 128, 0, stream>>>(dev);
     if (dev.sy_gj) k_gj_commit<<<(dev.n_gj + 255) / 256 < 1184 ? (dev.n_gj + 255) / 256 : 1184, 256, 0, stream>>>(dev);
     return cudaGetLastError();
