@@ -872,7 +872,7 @@ def main():
                       "phases": info.n_phases, "diffusion_barrier_group": info.group_tiles_64 and 64 or
                       (info.group_tiles_32 and 32 or 0), "setup_s": round(setup_s, 1)},
             "e2e": e2e, "e2e_dropin": dropin, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,
-            "gpu_launches": (info.modifier_launches + 2) * a.steps, "ensemble": ensemble, "trees": trees,
+            "gpu_launches": (info.modifier_launches + 1 + info.synapse_launches) * a.steps, "ensemble": ensemble, "trees": trees,
             "adjoint": adjoint, "sweep": sweep, "draw_order": draw_order,
         }
         print(json.dumps(line), flush=True)

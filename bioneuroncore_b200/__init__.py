@@ -75,7 +75,7 @@ class NetInfo(C.Structure):
         ("synapse_kernel_bytes_per_tick", C.c_double), ("warp_cap", C.c_uint32), ("tile_segs", C.c_uint32),
         ("modifier_kernel_bytes", C.c_double), ("diffusion_kernel_bytes", C.c_double),
         ("modifier_launches", C.c_uint32), ("fuse_phases", C.c_uint32), ("group_tiles_32", C.c_uint32),
-        ("group_tiles_64", C.c_uint32), ("diffusion_threads", C.c_uint32)]
+        ("group_tiles_64", C.c_uint32), ("diffusion_threads", C.c_uint32), ("synapse_launches", C.c_uint32)]
 
 
 class BuildOptions(C.Structure):

@@ -1144,6 +1144,7 @@ static int plan_info(const HostNet& hn, const Stimuli& stim, BncNetInfo* info,
     info->modifier_launches = modifier_launches(dev, host); info->fuse_phases = host.fuse;
     info->group_tiles_32 = host.group_tiles_32; info->group_tiles_64 = host.group_tiles_64;
     info->diffusion_threads = host.diff_threads;
+    info->synapse_launches = synapse_launches(dev);
     return BNC_OK;
 }
 
@@ -1619,6 +1620,7 @@ int bnc_network_info(void* sim, BncNetInfo* info) {
     info->modifier_launches = modifier_launches(d, b->host); info->fuse_phases = b->host.fuse;
     info->group_tiles_32 = b->host.group_tiles_32; info->group_tiles_64 = b->host.group_tiles_64;
     info->diffusion_threads = b->host.diff_threads;
+    info->synapse_launches = synapse_launches(d);
     info->warp_cap = b->host.opt.warp_cap; info->tile_segs = b->host.opt.tile_segs;
     info->modifier_kernel_bytes = b->host.mod_bytes; info->diffusion_kernel_bytes = b->host.diff_bytes;
     return BNC_OK;

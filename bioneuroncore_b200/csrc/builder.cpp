@@ -1567,6 +1567,9 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
     bool any_nmda = false;
     for (uint32_t i = 0; i < n; i++) if (sflags[i] & SF_NMDA) any_nmda = true;
     dev->nt_used_mask = nt_mask | (any_nmda ? 1u : 0u) | (sy_cleft_ecb.empty() ? 0u : 1u << 9);
+    dev->syn_extras = (!md_off.empty() || !sy_cleft_ecb.empty() || !gl_seg.empty() || !sy_gj.empty()) ? 1u : 0u;
+    dev->n_gj = (uint32_t)gj_pre.size();
+    dev->n_glia = (uint32_t)gl_seg.size();
     if (allocs) {
         {
             uint32_t bad = UINT32_MAX;

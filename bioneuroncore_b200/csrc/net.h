@@ -197,6 +197,7 @@ struct NetDev {
     uint32_t* gl_syn;         // sliced synapse indices
     uint32_t n_glia;
     uint32_t model_extras;    // 1: some item is eCB synthesis, GLAST or a connexin (86, 147, 114, 198)
+    uint32_t syn_extras;      // 1: release modulators, eCB, glia or gap junctions (the fused synapse kernel)
     uint32_t* md_off;         // [n_syn + 1]
     uint8_t* md_code;         // kind << 4 | cleft NT index; kind 1 Gi/o, 2 Gs, 3 ionotropic
     double* md_scale;         // density x effective area (pre_area, or 1 when not positive)
@@ -365,6 +366,7 @@ cudaError_t launch_tick(const NetDev& dev, const NetHost& host, float dt, unsign
 // Launches step 1 makes per tick (k_gather per chunk, phase or phase-group launches,
 // registered device modifiers), as enqueue_modifiers issues them.
 uint32_t modifier_launches(const NetDev& dev, const NetHost& host);
+uint32_t synapse_launches(const NetDev& dev);
 cudaError_t launch_modifiers(const NetDev& dev, const NetHost& host, float dt, unsigned long long tick,
                              cudaStream_t stream);
 cudaError_t launch_diffusion(const NetDev& dev, const NetHost& host, float dt, unsigned long long tick,

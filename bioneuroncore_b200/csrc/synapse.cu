@@ -528,9 +528,15 @@ __global__ void k_glia(NetDev d) {
     d.nt[(size_t)7 * N + g] = gly;
 }
 
+// Launches of steps 3 and 4 per tick, as launch_synapse issues them.
+uint32_t synapse_launches(const NetDev& dev) {
+    const bool extras = dev.syn_extras != 0;
+    return 1u + ((!extras && dev.n_syn) ? 1u : 0u) + (dev.n_glia ? 1u : 0u) + (dev.n_gj ? 1u : 0u);
+}
+
 cudaError_t launch_synapse(const NetDev& dev, float dt, unsigned long long tick, int first_tick,
                            cudaStream_t stream) {
-    const bool extras = dev.md_off || dev.sy_cleft_ecb || dev.gl_cap || dev.sy_gj;
+    const bool extras = dev.syn_extras != 0;
     if (extras) k_synapse<true><<<(dev.n_seg + 255) / 256, 256, 0, stream>>>(dev, dt, tick, first_tick);
     else {
         if (dev.n_syn) k_release<<<(dev.n_syn + 255) / 256, 256, 0, stream>>>(dev, dt, tick);

@@ -260,6 +260,8 @@ typedef struct {
     uint32_t fuse_phases;         /* modifier phases per launch the network runs with */
     uint32_t group_tiles_32, group_tiles_64;  /* tiles whose diffusion barriers span one warp / 64 threads */
     uint32_t diffusion_threads;   /* threads per diffusion CTA */
+    uint32_t synapse_launches;    /* launches of steps 3-4 per tick: k_release (networks without release
+                                     modulators, eCB, glia or gap junctions), k_synapse, k_glia, k_gj_commit */
 } BncNetInfo;
 int bnc_network_info(void* sim, BncNetInfo* info);
 
