@@ -102,6 +102,22 @@ def test_modifier_phase_groups():
     assert ch.fuse_phases == 1
 
 
+def test_synapse_step_launches():
+    """Steps 3 and 4 run as k_release (the synapses' presynaptic half, one thread per
+    synapse) and k_synapse for networks without release modulators, eCB, glia or gap
+    junctions, and as one fused k_synapse (plus k_glia, k_gj_commit) otherwise."""
+    from bioneuroncore_b200 import (plan_generated, NetgenParams, NET_SMALL, NET_LARGE, NETGEN_NO_SYNAPSES,
+                                    NETGEN_GAP_JUNCTIONS, NETGEN_GLIA, NETGEN_RELEASE_MODULATORS)
+    assert plan_generated(NetgenParams(family=NET_LARGE, n_neurons=20, seed=1)).synapse_launches == 2
+    assert plan_generated(NetgenParams(family=NET_SMALL, n_neurons=8, seed=1)).synapse_launches == 2
+    assert plan_generated(NetgenParams(family=NET_SMALL, n_neurons=8, seed=1,
+                                       flags=NETGEN_NO_SYNAPSES)).synapse_launches == 1
+    assert plan_generated(NetgenParams(family=NET_SMALL, n_neurons=8, seed=1,
+                                       flags=NETGEN_RELEASE_MODULATORS)).synapse_launches == 1
+    assert plan_generated(NetgenParams(family=NET_SMALL, n_neurons=8, seed=1,
+                                       flags=NETGEN_GLIA | NETGEN_GAP_JUNCTIONS)).synapse_launches == 3
+
+
 def test_diffusion_barrier_groups():
     """Tiles whose connections stay inside aligned groups of 32 or 64 threads get
     barriers of that group (32-segment neurons: a warp each; 64-segment neurons: a
