@@ -878,59 +878,79 @@ k_diffusion(NetDev d, float dt, unsigned long long tick, uint32_t S, uint32_t E)
             xbm1 = sg_bernoulli(-x); xbp1 = sg_bernoulli(x);
             xbm2 = xbp0; xbp2 = xbm0;   // the z = -1 argument is minus the z = +1 one
         }
+        // The ions in two groups (0-3, 4-6): one connection pass writes a group's
+        // fluxes, one gather applies them.  An ion's flux reads only that ion, which no
+        // other ion's update touches, so each ion's arithmetic and its order are those
+        // of one pass per ion.  The fluxes of a group (4 x E doubles) take the
+        // connection buffers the intracellular sub-steps and the phi_e solve have
+        // finished with (ed, gax, dve and fl lie contiguous, 44 E bytes in all).
+        double* const xfl = t.ed;
         for (int sub = 0; sub < 5; sub++) {
             const float vx_seg = (i < ns ? t.vf[i] : 1.0f) * EXTRA_VOLUME_RATIO;
             const double yx_d = 1.0 / (double)vx_seg;
 #pragma unroll 1
-            for (int q = 0; q < 7; q++) {
-                const int g = valence_group(q);
+            for (int q0 = 0; q0 < 7; q0 += 4) {
+                const int nq = q0 == 0 ? 4 : 3;
                 for (int e = ef; e < el; e += es) {
                     const int a = t.ea[e], b = t.eb[e];
-                    const double Ca = t.out[q * S + a];
-                    const double Cb = t.out[q * S + b];
-                    float bm = g == 0 ? xbm0 : (g == 1 ? xbm1 : xbm2);
-                    float bp = g == 0 ? xbp0 : (g == 1 ? xbp1 : xbp2);
-                    if (!edge_reg) {
-                        const double dphi = phi[a] - phi[b];
-                        const float x = (float)(kNpZ[q] * 0.03742f * dphi);
-                        bm = sg_bernoulli(-x);
-                        bp = sg_bernoulli(x);
+                    double dphi = 0.0;
+                    if (!edge_reg) dphi = phi[a] - phi[b];
+#pragma unroll
+                    for (int j = 0; j < 4; j++) {
+                        if (j >= nq) break;
+                        const int q = q0 + j;
+                        const int g = valence_group(q);
+                        const double Ca = t.out[q * S + a];
+                        const double Cb = t.out[q * S + b];
+                        float bm = g == 0 ? xbm0 : (g == 1 ? xbm1 : xbm2);
+                        float bp = g == 0 ? xbp0 : (g == 1 ? xbp1 : xbp2);
+                        if (!edge_reg) {
+                            const float x = (float)(kNpZ[q] * 0.03742f * dphi);
+                            bm = sg_bernoulli(-x);
+                            bp = sg_bernoulli(x);
+                        }
+                        xfl[(size_t)j * E + e] = t.coef[q * E + e] * (Ca * bm - Cb * bp);
                     }
-                    const double flux = t.coef[q * E + e] * (Ca * bm - Cb * bp);
-                    t.ed[e] = flux;
                 }
                 tile_sync<CL>(gm);
-                double lost = 0.0;
+                double lost[4] = {0.0, 0.0, 0.0, 0.0};
                 if (i < ns) {   // in place, as above
                     const float vf = t.vf[i];
                     const float vx = vx_seg;
                     const double yx = yx_d;
-                    double acc = 0.0;
-                    if (st.n >= 0) {
 #pragma unroll
-                        for (int k = 0; k < kDeg; k++) {
-                            if (k >= st.n) break;
-                            const int e = st.e[k];
-                            const double dq = div_by_float(t.ed[e], (double)vx, yx);
-                            if ((st.bend >> k) & 1u) acc += dq;
-                            else acc -= dq;
+                    for (int j = 0; j < 4; j++) {
+                        if (j >= nq) break;
+                        const int q = q0 + j;
+                        const double* fq = xfl + (size_t)j * E;
+                        double acc = 0.0;
+                        if (st.n >= 0) {
+#pragma unroll
+                            for (int k = 0; k < kDeg; k++) {
+                                if (k >= st.n) break;
+                                const int e = st.e[k];
+                                const double dq = div_by_float(fq[e], (double)vx, yx);
+                                if ((st.bend >> k) & 1u) acc += dq;
+                                else acc -= dq;
+                            }
+                        } else {
+                            for (int k = t.incoff[i]; k < t.incoff[i + 1]; k++) {
+                                const uint16_t ent = t.inc[k];
+                                const int e = ent & 0x7FFF;
+                                if (ent & 0x8000) acc += fq[e] / (vf * EXTRA_VOLUME_RATIO);
+                                else acc -= fq[e] / (vf * EXTRA_VOLUME_RATIO);
+                            }
                         }
-                    } else {
-                        for (int k = t.incoff[i]; k < t.incoff[i + 1]; k++) {
-                            const uint16_t ent = t.inc[k];
-                            const int e = ent & 0x7FFF;
-                            if (ent & 0x8000) acc += t.ed[e] / (vf * EXTRA_VOLUME_RATIO);
-                            else acc -= t.ed[e] / (vf * EXTRA_VOLUME_RATIO);
-                        }
+                        const float old = t.out[q * S + i];
+                        const float upd = (float)((double)old + acc);
+                        t.out[q * S + i] = upd;
+                        lost[j] = ((double)upd - (double)old - acc) * (double)vx;
                     }
-                    const float old = t.out[q * S + i];
-                    const float upd = (float)((double)old + acc);
-                    t.out[q * S + i] = upd;
-                    lost = ((double)upd - (double)old - acc) * (double)vx;
                 }
-                if (OPT && (d.diff_mode & 2u)) ledger_add(sh_ledger, q, lost);
+                if (OPT && (d.diff_mode & 2u))   // every thread of the warp takes part
+                    for (int j = 0; j < nq; j++) ledger_add(sh_ledger, q0 + j, lost[j]);
                 tile_sync<CL>(gm);
-                halo<CL>(t.out + (size_t)q * S, 1, S, ns, ng, t.gsrc, tid, nth);
+                halo<CL>(t.out + (size_t)q0 * S, nq, S, ns, ng, t.gsrc, tid, nth);
             }
         }
 
