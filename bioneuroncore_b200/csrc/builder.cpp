@@ -365,8 +365,16 @@ uint8_t host_nt_from_receptor(uint8_t type) { return nt_from_receptor(type); }
 
 void hostnet_from_aos(const BncBionData& aos, HostNet* hn) {
     *hn = HostNet();
+    size_t n_mods = 0, n_recs = 0;
+    for (uint32_t i = 0; i < aos.num_segments; i++)
+        n_mods += aos.segments[i].modifier_count > BNC_MAX_MODIFIERS ? BNC_MAX_MODIFIERS : aos.segments[i].modifier_count;
+    for (uint32_t k = 0; k < aos.num_synapses; k++)
+        n_recs += (size_t)std::min<uint32_t>(aos.synapses[k].post_receptor_count, 8u) +
+                  std::min<uint32_t>(aos.synapses[k].pre_autoreceptor_count, 8u);
     hn->seg.reserve(aos.num_segments);
+    hn->mods.reserve(n_mods);
     hn->syn.reserve(aos.num_synapses);
+    hn->recs.reserve(n_recs);
     for (uint32_t i = 0; i < aos.num_segments; i++) hostnet_add_segment(*hn, aos.segments[i]);
     hn->conn.assign(aos.connections, aos.connections + aos.num_connections);
     hn->num_connections = aos.num_connections;
@@ -385,7 +393,7 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
     };
     std::memset(dev, 0, sizeof(*dev));
     const uint32_t n = hn.num_segments;
-    const std::vector<SegLite>& S = hn.seg;
+    const HostVec<SegLite>& S = hn.seg;
     const HostNet& aos = hn;
     if (n == 0 || S.empty()) { set_error("network has no segments"); return BNC_ERR_ARG; }
     if (n >= (1u << 31)) { set_error("too many segments"); return BNC_ERR_ARG; }
