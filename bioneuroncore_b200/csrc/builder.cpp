@@ -802,9 +802,9 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
         max_active = std::max(max_active, act_off[i + 1]);
         act_off[i + 1] += act_off[i];
     }
-    std::vector<uint8_t> act_slot(act_off[n]);
-    std::vector<uint16_t> item_phase(act_slot.size(), 0);
-    std::vector<uint8_t> act_type(act_slot.size());
+    HostVec<uint8_t> act_slot(act_off[n]);
+    HostVec<uint16_t> item_phase(act_slot.size(), 0);
+    HostVec<uint8_t> act_type(act_slot.size());
     parallel_for(n, [&](size_t i0, size_t i1) {
         for (uint32_t i = (uint32_t)i0; i < (uint32_t)i1; i++) {
             uint32_t k = act_off[i];
@@ -893,7 +893,7 @@ int build_network(const HostNet& hn, const Stimuli& stim, NetDev* dev, NetHost* 
     for (uint32_t i = 0; i < n && fuse > 1; i++)
         for (uint32_t k = act_off[i]; k < act_off[i + 1]; k++)
             if (item_phase[k] != k - act_off[i] || user_type[act_type[k]]) { fuse = 1; break; }
-    std::vector<ItemKey> keys(act_slot.size());
+    HostVec<ItemKey> keys(act_slot.size());
     if (fuse > 1) {
         uint32_t rank[256];
         uint32_t R = 0;
